@@ -1,0 +1,221 @@
+/*
+ * firepro.h — C ABI of the B200 sparse-brick fire simulation step.
+ *
+ * This is the drop-in boundary for Fire Pro's engine layer: one call per method of the
+ * reference's `FluidSimulation` class (src/engine/FluidSimulation.ts), with plain structs
+ * and pointers in place of WebGPU resources and JS objects. A Node-API addon (see
+ * INTEGRATION.md) or Python ctypes binds these symbols one to one.
+ *
+ * Conventions
+ *  - Every function returns an `int` status (FP_OK or a negative FP_E* code) and never
+ *    throws across the ABI. `fp_last_error` gives the message of the latest failure,
+ *    worded as the reference's thrown Error messages where one exists.
+ *  - Validation happens before any state changes, as in the reference.
+ *  - A handle is not thread safe: calls on one handle are serialised by the caller.
+ *  - Caller buffers are borrowed for the duration of a call only.
+ *  - All world-space quantities are meters, seconds and the reference's units.
+ */
+#ifndef FIREPRO_H
+#define FIREPRO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FP_ABI_VERSION 1
+
+/* Status codes. */
+#define FP_OK 0
+#define FP_EINVAL (-1)   /* invalid argument: the reference throws an Error */
+#define FP_ENOMEM (-2)   /* device memory or the session's HBM budget is exhausted */
+#define FP_ELIMIT (-3)   /* a reference limit is exceeded (tiles, storage) */
+#define FP_EDEVICE (-4)  /* CUDA error; the message names the call */
+#define FP_ETIMEOUT (-5) /* a bounded device wait gave up; the context stays usable */
+#define FP_EUNSUPPORTED (-6) /* a grid option this build does not implement */
+
+/* Storage precision of the pools. Arithmetic is FP32 in every mode. */
+#define FP_PRECISION_FP32 0  /* plain FP32 storage everywhere (the drop-in) */
+#define FP_PRECISION_MIXED 1 /* FP16 scalar pools, BF16 coarse multigrid, FP32 velocity */
+
+/* Source shapes (types.ts:248 SimulationSource.shape). */
+#define FP_SHAPE_SPHERE 0
+#define FP_SHAPE_BOX 1
+#define FP_SHAPE_MESH 2
+
+/* Force kinds (ForceFields.ts:64 — the index of the type name). */
+#define FP_FORCE_WIND 0
+#define FP_FORCE_TURBULENCE 1
+#define FP_FORCE_VORTEX 2
+#define FP_FORCE_RADIAL 3
+
+/* The simulation lattice: replaces `SimulationGrid` (src/engine/types.ts:26-36), validated
+ * as `FluidSimulation`'s constructor does (FluidSimulation.ts:359-379). */
+typedef struct fp_grid {
+  float voxel_size;        /* meters, [0.0001, 16] */
+  int32_t velocity_divisor;/* 1 (the reference also allows 2 and 4) */
+  int32_t brick_size;      /* fine cells per brick side: 8 or 16 */
+  int32_t smoke_divisor;   /* 1 (the reference also allows 2 and 4) */
+  int32_t scalar_maccormack; /* bounded MacCormack scalar transport: 0 or 1 */
+  int32_t precision;       /* FP_PRECISION_* */
+  double voxel_budget;     /* grid.maxVoxels; 0 means the reference default 8,000,000 */
+} fp_grid;
+
+/* `SimulationSettings` (types.ts:235-243). */
+typedef struct fp_settings {
+  float buoyancy, smoke_weight, velocity_damping, cooling, dissipation, vorticity;
+  uint32_t seed;
+} fp_settings;
+
+/* One flame response ramp: 2..8 knots [lifetime, response] (flame.ts:3, :66-85). */
+typedef struct fp_flame_ramp {
+  uint32_t count;
+  float knots[8][2];
+} fp_flame_ramp;
+
+/* `FlameSettings` (flame.ts:7-13); ramps are smoke, heat, expansion. */
+typedef struct fp_combustion {
+  float lifespan, smoke_rate, heat_rate, expansion_rate;
+  fp_flame_ramp ramps[3];
+} fp_combustion;
+
+/* `FuelSettings` (fuel.ts:7-14). */
+typedef struct fp_fuel {
+  int32_t enabled;
+  float ignition_heat, burn_rate;
+} fp_fuel;
+
+/* `SimulationSource` (types.ts:246-268). `id` replaces the string id: a source whose id
+ * was absent last step is new. Mesh sources carry no samples in this ABI version. */
+typedef struct fp_source {
+  uint64_t id;
+  int32_t shape;            /* FP_SHAPE_* */
+  float position[3];
+  float size[3];            /* sphere radii or box half extents */
+  float flame, heat_rate, smoke_rate, fuel_rate;
+  float velocity[3];
+  float velocity_response;
+  float outward_speed;
+  int32_t has_variation;    /* burst-only initial variation */
+  float variation_period, variation_strength;
+} fp_source;
+
+/* `SimulationForce` (types.ts:284-293). When `targeted` is set the force reaches only the
+ * union of the regions of `force_targets[first_target .. first_target+target_count)`. */
+typedef struct fp_force {
+  int32_t type;             /* FP_FORCE_* */
+  float vector[3];          /* wind direction or vortex axis, unit length */
+  float center[3];
+  float strength, scale, lift, inward;
+  int32_t targeted;
+  uint32_t first_target, target_count;
+} fp_force;
+
+/* `SimulationCollider` (types.ts:271-281). Spheres and boxes use position/size/axes
+ * (axes are the columns of the world rotation; spheres ignore them); mesh colliders use
+ * a cell-center occupancy mask of dims[0]*dims[1]*dims[2] bits from lattice cell `lo`,
+ * stored at collider_masks[mask_offset ...], one bit per cell, x fastest. */
+typedef struct fp_collider {
+  int32_t shape;            /* FP_SHAPE_SPHERE, FP_SHAPE_BOX or FP_SHAPE_MESH */
+  float position[3];
+  float size[3];
+  float axes[3][3];
+  int32_t lo[3];
+  int32_t dims[3];
+  uint32_t mask_offset;
+} fp_collider;
+
+/* `SimulationFrame` (types.ts:295-302). */
+typedef struct fp_frame {
+  fp_settings simulation;
+  fp_combustion combustion;
+  fp_fuel fuel;
+  const fp_source* sources;
+  uint32_t source_count;
+  const fp_force* forces;
+  uint32_t force_count;
+  const fp_source* force_targets;
+  uint32_t force_target_count;
+  const fp_collider* colliders;
+  uint32_t collider_count;
+  const uint32_t* collider_masks;
+  uint32_t collider_mask_words;
+} fp_frame;
+
+/* What `FireSimulation.stats` and `FluidSimulation`'s getters report
+ * (FireSimulation.ts:295-334; FluidSimulation.ts:230-245). */
+typedef struct fp_stats {
+  double time;              /* simulated seconds */
+  uint64_t steps;
+  uint32_t active_bricks;   /* at the latest measurement */
+  uint32_t brick_cells;     /* fine cells per brick */
+  int32_t pool_limited;     /* gridLimited */
+  uint32_t pool_slots;      /* slots the pools hold */
+  uint32_t used_slots;
+  uint32_t tiles;           /* live tiles */
+  uint32_t tile_capacity;   /* tile slots the per-brick tables hold */
+  uint32_t failures;        /* failed allocations at the latest measurement */
+  uint64_t memory_bytes;    /* device bytes this simulation owns */
+  uint32_t last_vcycles;    /* V-cycles the latest pressure solve ran */
+  double last_residual;     /* FP64 RMS residual after the latest solve (mixed mode), else -1 */
+} fp_stats;
+
+/* Per-slot field arrays a test or debug view may copy out (`fp_sim_read_field`). Each
+ * is [slot][channel][cell] in FP32, cells x fastest within a brick. */
+#define FP_FIELD_VELOCITY 0   /* 3 channels: MAC face velocities u, v, w */
+#define FP_FIELD_SCALARS 1    /* 4 channels: smoke, heat, flame lifetime, fuel */
+#define FP_FIELD_EXPANSION 2  /* 1 channel */
+#define FP_FIELD_PRESSURE 3   /* 1 channel: the latest solution */
+#define FP_FIELD_DIVERGENCE 4 /* 1 channel: the Poisson right-hand side */
+#define FP_FIELD_CURL 5       /* 4 channels: curl xyz and magnitude */
+
+/* Integer tables a test may copy out (`fp_sim_read_table`), bit-exact against the oracle. */
+#define FP_TABLE_ENTRIES 0     /* int32 per brick id: slot | FRESH (0x2000000), or -1 */
+#define FP_TABLE_PAGES 1       /* int32 per brick id: the allocator's slot, or -1 */
+#define FP_TABLE_STATE 2       /* uint32 per brick id */
+#define FP_TABLE_ACTIVITY 3    /* uint32 per brick id, then per tile slot */
+#define FP_TABLE_RECORDS 4     /* int32[28] per brick id: 27 neighbour entries + pressure flag */
+#define FP_TABLE_FREE 5        /* uint32: free count, failures, then the free stack */
+#define FP_TABLE_ACTIVE 6      /* uint32: count, then brick ids in ascending order */
+#define FP_TABLE_SOLIDS 7      /* uint32 words per slot: one bit per fine cell */
+#define FP_TABLE_TILES 8       /* int32[4] per tile slot: x, y, z, state (0 free 1 live 2 closing) */
+
+typedef struct fp_sim fp_sim;
+
+/* Library */
+int fp_abi_version(void);
+const char* fp_last_error(const fp_sim* sim); /* sim may be NULL: the thread's last error */
+
+/* `FluidSimulation.create(device, grid)` (FluidSimulation.ts:419-475). `device` is the CUDA
+ * ordinal. */
+int fp_sim_create(const fp_grid* grid, int device, fp_sim** out);
+/* `FluidSimulation.dispose()` (FluidSimulation.ts:1780-1802). */
+int fp_sim_destroy(fp_sim* sim);
+/* `FluidSimulation.reset()` (FluidSimulation.ts:768-779). */
+int fp_sim_reset(fp_sim* sim);
+/* The fields `FireSimulation.step` sets before each step (FireSimulation.ts:457-459):
+ * cutoff, voxelBudget (maxVoxels), ground. */
+int fp_sim_set_runtime(fp_sim* sim, float cutoff, double voxel_budget, int ground);
+/* `FluidSimulation.step(frame, dt)` (FluidSimulation.ts:1367-1373): dt in (0, 1/30].
+ * Enqueues the step on the simulation's CUDA stream; returns before it completes. */
+int fp_sim_step(fp_sim* sim, const fp_frame* frame, float dt);
+/* Wait for the simulation's queued work. */
+int fp_sim_synchronize(fp_sim* sim);
+/* Stats (waits for the latest step's measurement). */
+int fp_sim_stats(fp_sim* sim, fp_stats* out);
+/* Copy a per-slot field (FP_FIELD_*) into `host`, `bytes` long: slots*channels*cells*4. */
+int fp_sim_read_field(fp_sim* sim, int field, float* host, size_t bytes);
+/* Copy an integer table (FP_TABLE_*) into `host`; `*bytes` in: capacity, out: bytes written. */
+int fp_sim_read_table(fp_sim* sim, int table, void* host, size_t* bytes);
+/* `FluidSimulation.readBricks()` (FluidSimulation.ts:1749-1779): the world boxes of the
+ * bricks that hold a slot, six floats each (min xyz, max xyz). `*count` in: capacity in
+ * boxes, out: boxes written (or needed, with FP_ELIMIT). */
+int fp_sim_read_bricks(fp_sim* sim, float* boxes, uint32_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FIREPRO_H */

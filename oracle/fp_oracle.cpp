@@ -1,0 +1,2089 @@
+// TEST INFRASTRUCTURE — NOT PART OF THE PRODUCT.
+//
+// CPU oracle of Fire Pro's sparse-brick simulation step: a restatement, operation for
+// operation, of the reference's WGSL kernels and of the TypeScript engine host that drives
+// them. Templated on the real type: double is the FP64 error oracle; float is the FP32
+// CPU baseline (OpenMP over bricks). Storage rounding restates the reference's
+// half-precision pools when asked (mode "half"), or the mixed mode of this build.
+//
+// Only tests/, bench.py's `cpu_baseline` leg and __graft_entry__.smoke() may load this.
+// Parity unpinned: the reference ships no tests, golden vectors or CPU path, and cannot
+// run in this environment (TypeScript without Node; WGSL without a WebGPU device).
+//
+// Layout. Pools are slot-major: [slot][channel][cell], cells x fastest within a brick.
+// The reference keeps each slot in a 3D texture with a one-texel apron that copies the
+// first layer of the following bricks; reads through that apron equal reads of the
+// neighbour's cells (zero where the neighbour has no slot), so this oracle reads the
+// neighbour cells directly. Samples are trilinear with exact weights.
+//
+// Citations are path:line in the reference project.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/firepro.h"
+#include "fp_oracle_common.hpp"
+
+namespace orc {
+
+// ---------------------------------------------------------------------------------------
+// Tile directory: src/engine/TileDirectory.ts:61-186.
+// ---------------------------------------------------------------------------------------
+static const int TILE_BRICKS = 4;
+static const int LINGER_STEPS = 60;  // TileDirectory.ts:8
+static const int MIN_TILES = 16;     // FluidSimulation.ts:72
+static const int32_t FRESH_ENTRY = 0x2000000;  // tiles.wgsl:138
+static const int RECORD_WORDS = 28;            // FluidSimulation.ts:139
+
+struct Tile {
+  I3 coord;
+  int slot;
+  int64_t needed;
+  bool closing;
+};
+
+struct Directory {
+  // Insertion-ordered, like the JS Map of TileDirectory.ts:62.
+  std::map<uint64_t, Tile> bySeq;
+  std::map<std::tuple<int, int, int>, uint64_t> byCoord;
+  uint64_t nextSeq = 0;
+  std::vector<int> slotUsed;  // -1 free, else 1 (TileDirectory.ts:63 `slots`)
+  std::vector<int> created;
+  bool dirty = true;
+  bool ground = true;
+  int version = 0;
+
+  int count() const { return (int)bySeq.size(); }
+  Tile* find(int x, int y, int z) {
+    auto it = byCoord.find(std::make_tuple(x, y, z));
+    if (it == byCoord.end()) return nullptr;
+    return &bySeq[it->second];
+  }
+  // TileDirectory.ts:86-108
+  void need(I3 lo, I3 hi, int64_t step) {
+    for (int z = lo[2]; z <= hi[2]; z++)
+      for (int y = ground ? std::max(0, lo[1]) : lo[1]; y <= hi[1]; y++)
+        for (int x = lo[0]; x <= hi[0]; x++) {
+          Tile* t = find(x, y, z);
+          if (t) {
+            t->needed = step;
+            if (t->closing) {
+              t->closing = false;
+              dirty = true;
+            }
+            continue;
+          }
+          int slot = -1;
+          for (size_t i = 0; i < slotUsed.size(); i++)
+            if (slotUsed[i] < 0) {
+              slot = (int)i;
+              break;
+            }
+          if (slot < 0) {
+            slot = (int)slotUsed.size();
+            slotUsed.push_back(-1);
+          }
+          slotUsed[slot] = 1;
+          uint64_t seq = nextSeq++;
+          bySeq[seq] = Tile{i3(x, y, z), slot, step, false};
+          byCoord[std::make_tuple(x, y, z)] = seq;
+          created.push_back(slot);
+          dirty = true;
+        }
+  }
+  // TileDirectory.ts:111-123
+  void retire(int64_t step) {
+    for (auto it = bySeq.begin(); it != bySeq.end();) {
+      Tile& t = it->second;
+      if (t.closing) {
+        slotUsed[t.slot] = -1;
+        byCoord.erase(std::make_tuple(t.coord[0], t.coord[1], t.coord[2]));
+        it = bySeq.erase(it);
+        dirty = true;
+        continue;
+      }
+      if (step - t.needed > LINGER_STEPS) {
+        t.closing = true;
+        dirty = true;
+      }
+      ++it;
+    }
+    while (!slotUsed.empty() && slotUsed.back() < 0) slotUsed.pop_back();
+  }
+  void clear() {
+    bySeq.clear();
+    byCoord.clear();
+    slotUsed.clear();
+    created.clear();
+    dirty = true;
+  }
+  int slotAt(int x, int y, int z) {
+    Tile* t = find(x, y, z);
+    return t ? t->slot : -1;
+  }
+  std::vector<int> takeCreated() {
+    std::vector<int> out;
+    for (int s : created)
+      if (s < (int)slotUsed.size() && slotUsed[s] >= 0) out.push_back(s);
+    created.clear();
+    return out;
+  }
+};
+
+// ---------------------------------------------------------------------------------------
+// Packed scene records (fluid-common.wgsl:34-51; FluidSimulation.ts:1150-1366).
+// ---------------------------------------------------------------------------------------
+template <class R>
+struct Emitter {
+  R pos[3];
+  bool enabled;
+  R size[3];
+  bool box;
+  R flame, heat, smoke, response;  // rates.xyzw
+  R vel[3];
+  R outward;                       // velocity.w
+  R period, strength, fuel;        // variation.xyz
+};
+
+template <class R>
+struct Collider {
+  int kind;  // 0 ellipsoid, 1 box, 2 mesh
+  R center[3];
+  R extent[3];
+  R axes[3][3];  // columns
+  int lo[3];
+  int size[3];
+  uint32_t first;  // word offset of the mask
+};
+
+template <class R>
+struct Force {
+  R axis[3];
+  R strength;
+  R center[3];
+  int kind;
+  R scale, lift, inward;
+  int regionFirst, regionCount;
+  bool targeted;
+};
+template <class R>
+struct Region {
+  R center[3];
+  bool box;
+  R size[3];
+};
+
+template <class R>
+struct FlameP {
+  R dt, lifespan, smoke, heat, expansion;
+  int counts[3];
+  R knots[3][8][2];
+};
+
+struct Prec {
+  int vel = STORE_EXACT, scal = STORE_EXACT, expn = STORE_EXACT, p0 = STORE_EXACT, pc = STORE_EXACT;
+  int curl = STORE_EXACT, bounds = STORE_EXACT;
+  bool truncate = false;  // truncateHalf at the reference's hand-offs
+};
+
+// Activity flags (fluid-content.wgsl:11-13).
+static const uint32_t CONTENT = 1u, EXPANDS = 2u, MAY_EXPAND = 4u;
+static const uint32_t BRICK_FREES = 8u, BRICK_REQUESTS = 16u;  // fluid-allocation.wgsl:40-41
+static const uint8_t STORED_SOLID = 64u;                       // pressure.wgsl:159
+static const uint32_t SOLID = 1024u;                           // pressure.wgsl:168
+
+static inline int neighborIndex(int dx, int dy, int dz) { return (dz + 1) * 9 + (dy + 1) * 3 + dx + 1; }
+
+template <class R>
+struct Sim {
+  // --- configuration
+  int B, shift, N, W;  // brick cells per side, log2, cells per brick, solid words per slot
+  R h;                 // voxel size (float value)
+  bool maccormack;
+  Prec prec;
+  int brickLevels, bottom;
+  double voxelBudget = 8e6;
+  float cutoff = 0.0f;
+  bool ground = true;
+
+  // --- host state (FluidSimulation.ts fields)
+  Directory dir;
+  int capacity = 0;  // tile slots
+  std::vector<I3> snapshot;  // tile coordinates per slot at the last tables build
+  std::vector<int> snapshotState;
+  std::vector<int32_t> tileNeighbors;  // 27 per tile slot
+  double time = 0;
+  int64_t steps = 0;
+  bool mayHaveFlame = false;
+  bool solidsStale = true;
+  bool geometryDirty = true;
+  int colliderCount = 0;
+  std::vector<Collider<R>> prevColliders;
+  std::vector<uint32_t> prevMasks;
+  std::vector<std::pair<I3, uint32_t>> contentTiles;  // tile coord, brick bits
+  uint32_t activeBrickCount = 0, usedSlots = 0, lastFailures = 0;
+  bool poolLimited = false;
+
+  // --- per brick id (capacity * 64)
+  std::vector<int32_t> pages, entries, records;
+  std::vector<uint32_t> state, activity;  // activity: bricks then tile slots
+
+  // --- pool
+  uint32_t slots = 0;
+  std::vector<uint32_t> freeStack;
+  int32_t freeCount = 0;
+  uint32_t failures = 0;
+  std::vector<R> vel, velP, velC, velF, curl;  // [slot][3 or 4][N]
+  std::vector<R> fld, fldP, fldN;              // [slot][4][N]
+  std::vector<R> expn, div;                    // [slot][N]
+  std::vector<R> vmin, vmax;                   // velocity donor bounds [slot][3][N]
+  std::vector<R> sb;                           // scalar bounds [slot][8][N]
+  std::vector<int32_t> vdonor;                 // velocity donor bases [slot][3][N][3]
+  std::vector<uint32_t> solids;                // [slot][W]
+  // multigrid: per level p (ping-pong), rhs, topology
+  struct Level {
+    std::vector<R> p[2], rhs;
+    std::vector<uint8_t> topo;
+    int current = 0;
+  };
+  std::vector<Level> levels;
+  std::vector<R> pres[2];  // level 0 pressures
+  int latest = 0;
+
+  // --- per step scene
+  std::vector<Emitter<R>> emitters;
+  std::vector<Collider<R>> colliders;
+  std::vector<uint32_t> masks;
+  std::vector<Force<R>> forces;
+  std::vector<Region<R>> regions;
+  std::vector<std::vector<int>> lists[3];  // per kind, per tile slot
+  FlameP<R> flame;
+  std::vector<V3<float>> noiseTable;  // 64^3 curl noise (built once)
+  // uniforms of the step
+  R dt, buoyancy, coolingK, smokeWeight, damping, dissipation, vorticity;
+  R timeU, seedU;
+  uint32_t seedBits;
+  bool lifetimeZero;
+  bool fuelEnabled;
+  R ignition, burnRate;
+  int held = 0;
+  bool solidsAll = false;
+
+  // --- step-local lists
+  std::vector<uint32_t> active;                      // brick ids
+  std::vector<std::pair<uint32_t, uint32_t>> zeroed;  // id, slot | fresh<<31
+
+  // ================================================================================
+  Sim(const fp_grid& g, Prec p) {
+    B = g.brick_size;
+    shift = B == 8 ? 3 : 4;
+    N = B * B * B;
+    W = N / 32;
+    h = (R)(float)g.voxel_size;
+    maccormack = g.scalar_maccormack != 0;
+    prec = p;
+    brickLevels = shift;
+    bottom = brickLevels + 2;
+    if (g.voxel_budget > 0) voxelBudget = g.voxel_budget;
+    buildNoise();
+    allocate();
+  }
+
+  uint32_t slotLimit() const {
+    double v = std::floor(voxelBudget / (double)N);
+    return (uint32_t)std::max(1.0, v);
+  }
+  int levelShift(int level) const { return level < brickLevels ? brickLevels - level : brickLevels + 2 - level; }
+  int levelSide(int level) const { return 1 << levelShift(level); }
+  int levelCells(int level) const { int s = levelSide(level); return s * s * s; }
+
+  // FluidSimulation.ts:496-549 — empty pools and no tiles. The pool holds the whole
+  // voxel budget at once; it grows only when the budget does.
+  void allocate() {
+    slots = slotLimit();
+    freeStack.assign(slots, 0);
+    for (uint32_t i = 0; i < slots; i++) freeStack[i] = slots - 1 - i;  // pops slot 0 first
+    freeCount = (int32_t)slots;
+    failures = 0;
+    resizePools(slots);
+    dir.clear();
+    contentTiles.clear();
+    capacity = 0;
+    setCapacity(MIN_TILES);
+    applyTiles();
+    solidsStale = true;
+    geometryDirty = true;
+    usedSlots = 0;
+    poolLimited = false;
+  }
+  void resizePools(uint32_t n) {
+    size_t s = n;
+    vel.resize(s * 3 * N, 0); velP.resize(s * 3 * N, 0); velC.resize(s * 3 * N, 0); velF.resize(s * 3 * N, 0);
+    curl.resize(s * 4 * N, 0);
+    fld.resize(s * 4 * N, 0); fldP.resize(s * 4 * N, 0); fldN.resize(s * 4 * N, 0);
+    expn.resize(s * N, 0); div.resize(s * N, 0);
+    vmin.resize(s * 3 * N, 0); vmax.resize(s * 3 * N, 0);
+    sb.resize(s * 8 * N, 0);
+    vdonor.resize(s * 3 * N * 3, 0);
+    solids.resize(s * W, 0);
+    pres[0].resize(s * N, 0); pres[1].resize(s * N, 0);
+    levels.resize(bottom + 1);
+    levels[0].topo.resize(s * N, 0);
+    for (int l = 1; l < brickLevels; l++) {
+      size_t c = s * levelCells(l);
+      levels[l].p[0].resize(c, 0); levels[l].p[1].resize(c, 0); levels[l].rhs.resize(c, 0);
+      levels[l].topo.resize(c, 0);
+    }
+  }
+  // Grow the pool after the voxel budget rose: new slots go under the free stack
+  // (FluidSimulation.ts:1013-1093, fluid-pool-growth.wgsl:12-21).
+  void growPool(uint32_t target) {
+    if (target <= slots) return;
+    uint32_t added = target - slots;
+    std::vector<uint32_t> next(target, 0);
+    for (uint32_t i = 0; i < added; i++) next[i] = slots + added - 1 - i;
+    for (uint32_t i = 0; i < slots; i++) next[added + i] = freeStack[i];
+    freeStack.swap(next);
+    freeCount += (int32_t)added;
+    resizePools(target);
+    slots = target;
+    geometryDirty = true;
+  }
+  void setCapacity(int cap) {
+    int old = capacity;
+    capacity = cap;
+    size_t bricks = (size_t)cap * 64;
+    pages.resize(bricks, -1);
+    entries.resize(bricks, -1);
+    records.resize(bricks * RECORD_WORDS, -1);
+    state.resize(bricks, 0);
+    std::vector<uint32_t> act(bricks + cap, 0);
+    for (size_t i = 0; i < (size_t)old * 64 && i < activity.size(); i++) act[i] = activity[i];
+    activity.swap(act);
+    for (int l = brickLevels; l <= bottom; l++) {
+      size_t c = (size_t)cap * levelCells(l);
+      levels[l].p[0].resize(c, 0); levels[l].p[1].resize(c, 0); levels[l].rhs.resize(c, 0);
+      levels[l].topo.resize(c, 0);
+    }
+    snapshot.resize(cap, i3(0, 0, 0));
+    snapshotState.resize(cap, 0);
+    tileNeighbors.resize((size_t)cap * 27, -1);
+  }
+  // FluidSimulation.ts:629-678 applyTiles and TileDirectory.ts:151-186 tables.
+  void applyTiles() {
+    int needed = std::max(MIN_TILES, (int)dir.slotUsed.size());
+    if (needed > capacity) {
+      int cap = capacity;
+      while (cap < needed) cap *= 2;
+      setCapacity(cap);
+    }
+    std::fill(snapshotState.begin(), snapshotState.end(), 0);
+    std::fill(tileNeighbors.begin(), tileNeighbors.end(), -1);
+    for (int s = 0; s < capacity; s++) snapshot[s] = i3(0, 0, 0);
+    for (auto& kv : dir.bySeq) {
+      const Tile& t = kv.second;
+      snapshot[t.slot] = t.coord;
+      snapshotState[t.slot] = t.closing ? 2 : 1;
+      for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+          for (int dx = -1; dx <= 1; dx++) {
+            Tile* n = dir.find(t.coord[0] + dx, t.coord[1] + dy, t.coord[2] + dz);
+            if (n) tileNeighbors[(size_t)t.slot * 27 + neighborIndex(dx, dy, dz)] = n->slot;
+          }
+    }
+    dir.dirty = false;
+    dir.version++;
+    for (int slot : dir.takeCreated()) {
+      for (int k = 0; k < 64; k++) {
+        size_t id = (size_t)slot * 64 + k;
+        pages[id] = -1;
+        state[id] = 0;
+        activity[id] = 0;
+        entries[id] = -1;
+      }
+    }
+    geometryDirty = true;  // PressureSolver.setBricks -> resetPlans
+  }
+
+  // ---------------------------------------------------------------- addressing (tiles.wgsl)
+  int tileAt(int x, int y, int z) { return dir.slotAt(x, y, z); }
+  static int floordiv(int a, int s) { return a >> s; }
+  // The id of world brick b, or -1 (tiles.wgsl:266-272).
+  int brickId(int bx, int by, int bz) {
+    int t = tileAt(bx >> 2, by >> 2, bz >> 2);
+    if (t < 0) return -1;
+    return t * 64 + (((bz & 3) * 4 + (by & 3)) * 4 + (bx & 3));
+  }
+  int32_t brickEntry(int bx, int by, int bz) {
+    int id = brickId(bx, by, bz);
+    return id < 0 ? -1 : entries[id];
+  }
+  static int entryPage(int32_t e) { return e < 0 ? -1 : (e & 0xffffff); }
+  int brickSlot(int bx, int by, int bz) { return entryPage(brickEntry(bx, by, bz)); }
+  I3 brickOf(uint32_t id) {
+    I3 t = snapshot[id >> 6];
+    int l = id & 63;
+    return i3(t[0] * 4 + (l & 3), t[1] * 4 + ((l >> 2) & 3), t[2] * 4 + (l >> 4));
+  }
+  int local(int x, int y, int z) const { return ((z & (B - 1)) * B + (y & (B - 1))) * B + (x & (B - 1)); }
+  // Cell p of a pool of `ch` channels: zero in a brick without a slot (fluid-sampling.wgsl:68-75).
+  R cellAt(const std::vector<R>& pool, int ch, int c, int x, int y, int z) {
+    int s = brickSlot(x >> shift, y >> shift, z >> shift);
+    if (s < 0) return 0;
+    return pool[((size_t)s * ch + c) * N + local(x, y, z)];
+  }
+  // Trilinear sample at `pos` in cell units, centres at .5 (fluid-sampling.wgsl:85-114).
+  R sampleCells(const std::vector<R>& pool, int ch, int c, R px, R py, R pz) {
+    R q[3] = {px - R(0.5), py - R(0.5), pz - R(0.5)};
+    int b[3];
+    R f[3];
+    for (int a = 0; a < 3; a++) {
+      b[a] = floori((double)q[a]);
+      f[a] = q[a] - (R)b[a];
+    }
+    R value = 0;
+    for (int z = 0; z < 2; z++)
+      for (int y = 0; y < 2; y++)
+        for (int x = 0; x < 2; x++) {
+          R w = (x ? f[0] : R(1) - f[0]) * (y ? f[1] : R(1) - f[1]) * (z ? f[2] : R(1) - f[2]);
+          value += cellAt(pool, ch, c, b[0] + x, b[1] + y, b[2] + z) * w;
+        }
+    return value;
+  }
+  // Solid test of field cell c (solids.wgsl:15-31).
+  bool solidCell(int x, int y, int z) {
+    if (ground && y < 0) return true;
+    if (colliderCount == 0) return false;
+    int s = brickSlot(x >> shift, y >> shift, z >> shift);
+    if (s < 0) return false;
+    int bit = local(x, y, z);
+    return ((solids[(size_t)s * W + (bit >> 5)] >> (bit & 31)) & 1u) != 0;
+  }
+  // fieldCell (solids.wgsl:7-9): the quarter-cell bias picks one cell on shared corners.
+  bool solidAt(R wx, R wy, R wz) {
+    return solidCell(floori((double)(wx / h + R(0.25))), floori((double)(wy / h + R(0.25))),
+                     floori((double)(wz / h + R(0.25))));
+  }
+  V3<R> center(int x, int y, int z) { return v3<R>((R(x) + R(0.5)) * h, (R(y) + R(0.5)) * h, (R(z) + R(0.5)) * h); }
+
+  // ---------------------------------------------------------------- velocity sampling
+  // fluid-advection.wgsl:17-21: the MAC component at world position `p`.
+  R velComp(const std::vector<R>& pool, V3<R> p, int c) {
+    V3<R> q = p;
+    q[c] -= R(0.5) * h;
+    return sampleCells(pool, 3, c, q[0] / h, q[1] / h, q[2] / h);
+  }
+  V3<R> velocityAt(V3<R> p) { return v3<R>(velComp(vel, p, 0), velComp(vel, p, 1), velComp(vel, p, 2)); }
+  // fluid-advection.wgsl:26-44
+  V3<R> velocityOnFace(int x, int y, int z, int c, V3<R> orig) {
+    R fp[3] = {R(x) + R(0.5), R(y) + R(0.5), R(z) + R(0.5)};
+    fp[c] += R(0.5);
+    V3<R> r;
+    for (int k = 0; k < 3; k++) {
+      if (k == c) {
+        r[k] = orig[k];
+        continue;
+      }
+      R q[3] = {fp[0], fp[1], fp[2]};
+      q[k] -= R(0.5);
+      r[k] = sampleCells(vel, 3, k, q[0], q[1], q[2]);
+    }
+    return r;
+  }
+
+  // ---------------------------------------------------------------- scene packing
+  void checkFinite(float v, const char* name) {
+    if (!std::isfinite(v)) throw std::string(name) + " must be finite in f32.";
+  }
+  // flame.ts:43-87 packFlameStep
+  void packFlame(const fp_combustion& c, float dtf) {
+    float step = dtf, lifespan = c.lifespan;
+    checkFinite(step, "Flame timestep");
+    checkFinite(lifespan, "Flame lifespan");
+    if (step <= 0 || lifespan <= 0) throw std::string("Flame timestep and lifespan must be positive in f32.");
+    checkFinite(step / lifespan, "Lifetime decrement");
+    checkFinite(c.smoke_rate, "Smoke rate");
+    checkFinite(c.heat_rate, "Heat rate");
+    checkFinite(c.expansion_rate, "Expansion rate");
+    if (c.smoke_rate < 0 || c.heat_rate < 0) throw std::string("Smoke and heat rates must be nonnegative.");
+    const char* names[3] = {"smoke", "heat", "expansion"};
+    flame.dt = step; flame.lifespan = lifespan; flame.smoke = c.smoke_rate; flame.heat = c.heat_rate;
+    flame.expansion = c.expansion_rate;
+    for (int ch = 0; ch < 3; ch++) {
+      const fp_flame_ramp& r = c.ramps[ch];
+      if (r.count < 2 || r.count > 8) throw std::string(names[ch]) + " ramp needs 2–8 knots.";
+      float prev = -1;
+      for (uint32_t i = 0; i < r.count; i++) {
+        float x = r.knots[i][0], y = r.knots[i][1];
+        if (!std::isfinite(x)) throw std::string(names[ch]) + " lifetime must be finite in f32.";
+        if (!std::isfinite(y)) throw std::string(names[ch]) + " response must be finite in f32.";
+        if (x < 0 || x > 1 || y < 0 || y > 1 || x <= prev)
+          throw std::string(names[ch]) + " knots must increase in f32 with coordinates in [0,1].";
+        if ((i == 0 && x != 0) || (i == r.count - 1 && x != 1))
+          throw std::string(names[ch]) + " ramp must span lifetime 0–1.";
+        flame.knots[ch][i][0] = x;
+        flame.knots[ch][i][1] = y;
+        prev = x;
+      }
+      flame.counts[ch] = (int)r.count;
+    }
+  }
+  // Every tile within the world box, or every tile (FluidSimulation.ts:1163-1188).
+  void bin(int kind, int index, bool hasBox, const R* lo, const R* hi) {
+    R tileSize = R(TILE_BRICKS * B) * h;
+    if (!hasBox) {
+      for (int s = 0; s < capacity; s++)
+        if (snapshotState[s] != 0) lists[kind][s].push_back(index);
+      return;
+    }
+    int l[3], u[3];
+    for (int a = 0; a < 3; a++) {
+      l[a] = floori((double)(lo[a] / tileSize));
+      u[a] = floori((double)(hi[a] / tileSize));
+    }
+    for (int z = l[2]; z <= u[2]; z++)
+      for (int y = l[1]; y <= u[1]; y++)
+        for (int x = l[0]; x <= u[0]; x++) {
+          int s = dir.slotAt(x, y, z);
+          if (s >= 0) lists[kind][s].push_back(index);
+        }
+  }
+  bool packScene(const fp_frame& f) {
+    for (int k = 0; k < 3; k++) lists[k].assign(capacity, {});
+    R brick = R(B) * h;
+    emitters.clear();
+    for (uint32_t i = 0; i < f.source_count; i++) {
+      const fp_source& s = f.sources[i];
+      if (s.shape == FP_SHAPE_MESH) continue;
+      Emitter<R> e;
+      for (int a = 0; a < 3; a++) {
+        e.pos[a] = s.position[a];
+        e.size[a] = s.size[a];
+        e.vel[a] = s.velocity[a];
+      }
+      e.enabled = true;
+      e.box = s.shape == FP_SHAPE_BOX;
+      e.flame = s.flame; e.heat = s.heat_rate; e.smoke = s.smoke_rate; e.response = s.velocity_response;
+      e.outward = s.outward_speed;
+      e.period = s.has_variation ? s.variation_period : 0.5f;
+      e.strength = s.has_variation ? s.variation_strength : 0.0f;
+      e.fuel = s.fuel_rate;
+      int index = (int)emitters.size();
+      emitters.push_back(e);
+      R lo[3], hi[3];
+      for (int a = 0; a < 3; a++) {
+        R ext = std::max((R)s.size[a], (R)0.03f);
+        lo[a] = e.pos[a] - ext - 2 * brick;
+        hi[a] = e.pos[a] + ext + 2 * brick;
+      }
+      bin(0, index, true, lo, hi);
+    }
+    // Colliders (FluidSimulation.ts:1216-1295).
+    colliders.clear();
+    masks.assign(f.collider_masks, f.collider_masks + f.collider_mask_words);
+    for (uint32_t i = 0; i < f.collider_count; i++) {
+      const fp_collider& c = f.colliders[i];
+      Collider<R> k{};
+      R lo[3], hi[3];
+      if (c.shape == FP_SHAPE_MESH) {
+        k.kind = 2;
+        for (int a = 0; a < 3; a++) {
+          k.lo[a] = c.lo[a];
+          k.size[a] = c.dims[a];
+          lo[a] = (R)((float)c.lo[a] * (float)h);
+          hi[a] = (R)((float)(c.lo[a] + c.dims[a]) * (float)h);
+        }
+        k.first = c.mask_offset;
+      } else {
+        k.kind = c.shape == FP_SHAPE_BOX ? 1 : 0;
+        for (int a = 0; a < 3; a++) {
+          k.center[a] = c.position[a];
+          k.extent[a] = c.size[a];
+          for (int b = 0; b < 3; b++) k.axes[a][b] = c.axes[a][b];
+        }
+        for (int a = 0; a < 3; a++) {
+          R ext = c.size[a];
+          if (k.kind == 1)
+            ext = std::fabs((R)c.axes[0][a]) * (R)c.size[0] + std::fabs((R)c.axes[1][a]) * (R)c.size[1] +
+                  std::fabs((R)c.axes[2][a]) * (R)c.size[2];
+          lo[a] = (R)c.position[a] - ext;
+          hi[a] = (R)c.position[a] + ext;
+        }
+      }
+      colliders.push_back(k);
+      bin(2, (int)i, true, lo, hi);
+    }
+    bool changed = colliders.size() != prevColliders.size() || masks != prevMasks;
+    for (size_t i = 0; !changed && i < colliders.size(); i++)
+      changed = std::memcmp(&colliders[i], &prevColliders[i], sizeof(Collider<R>)) != 0;
+    prevColliders = colliders;
+    prevMasks = masks;
+    colliderCount = (int)colliders.size();
+    // Forces (ForceFields.ts:41-114).
+    forces.clear();
+    regions.clear();
+    for (uint32_t i = 0; i < f.force_count; i++) {
+      const fp_force& s = f.forces[i];
+      Force<R> k{};
+      for (int a = 0; a < 3; a++) {
+        k.axis[a] = s.vector[a];
+        k.center[a] = s.center[a];
+      }
+      k.strength = s.strength;
+      k.kind = s.type;
+      k.scale = s.scale; k.lift = s.lift; k.inward = s.inward;
+      k.targeted = s.targeted != 0;
+      k.regionFirst = (int)regions.size();
+      k.regionCount = 0;
+      bool hasReach = false;
+      R lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
+      if (k.targeted) {
+        for (uint32_t t = 0; t < s.target_count; t++) {
+          const fp_source& src = f.force_targets[s.first_target + t];
+          if (src.shape == FP_SHAPE_MESH) continue;
+          Region<R> r;
+          for (int a = 0; a < 3; a++) {
+            r.center[a] = src.position[a];
+            r.size[a] = src.size[a];
+          }
+          r.box = src.shape == FP_SHAPE_BOX;
+          regions.push_back(r);
+          k.regionCount++;
+          for (int a = 0; a < 3; a++) {
+            R ext = std::max((R)src.size[a], (R)0.03f);
+            R l = r.center[a] - ext, u = r.center[a] + ext;
+            if (!hasReach) { lo[a] = l; hi[a] = u; } else { lo[a] = std::min(lo[a], l); hi[a] = std::max(hi[a], u); }
+          }
+          hasReach = true;
+        }
+      }
+      forces.push_back(k);
+      if (!k.targeted) {
+        bin(1, (int)i, false, nullptr, nullptr);
+      } else {
+        R l[3], u[3];
+        for (int a = 0; a < 3; a++) {
+          l[a] = lo[a] - brick;
+          u[a] = hi[a] + brick;
+        }
+        bin(1, (int)i, true, l, u);
+      }
+    }
+    return changed;
+  }
+
+  // ---------------------------------------------------------------- host step
+  void needBox(const R* lo, const R* hi, R margin) {
+    R size = R(TILE_BRICKS * B) * h;
+    I3 l, u;
+    for (int a = 0; a < 3; a++) {
+      l[a] = floori((double)((lo[a] - margin) / size));
+      u[a] = floori((double)((hi[a] + margin) / size));
+    }
+    dir.need(l, u, steps);
+  }
+  // FluidSimulation.ts:873-912 updateTiles
+  void updateTiles(const fp_frame& f) {
+    dir.retire(steps);
+    R reach = R(2 * B) * h;
+    R margin = reach + R(TILE_BRICKS * B) * h;
+    for (uint32_t i = 0; i < f.source_count; i++) {
+      const fp_source& s = f.sources[i];
+      if (s.shape == FP_SHAPE_MESH) continue;
+      R ext = std::max(std::max(std::max((R)s.size[0], (R)s.size[1]), (R)s.size[2]), (R)0.03f) +
+              (R)s.outward_speed * R(0.25);
+      R lo[3], hi[3];
+      for (int a = 0; a < 3; a++) {
+        lo[a] = (R)s.position[a] - ext;
+        hi[a] = (R)s.position[a] + ext;
+      }
+      needBox(lo, hi, margin);
+    }
+    for (auto& ct : contentTiles)
+      dir.need(i3(ct.first[0] - 1, ct.first[1] - 1, ct.first[2] - 1),
+               i3(ct.first[0] + 1, ct.first[1] + 1, ct.first[2] + 1), steps);
+    if (dir.dirty) applyTiles();
+  }
+
+  std::string step(const fp_frame& f, float dtf) {
+    if (!std::isfinite(dtf) || dtf <= 0 || dtf > 1.0f / 30.0f)
+      return "Simulation step must be in (0, 1/30]. Use fixed substeps.";
+    try {
+      packFlame(f.combustion, dtf);
+    } catch (const std::string& e) {
+      return e;
+    }
+    if (dir.ground != ground) {
+      dir.ground = ground;
+      geometryDirty = true;
+    }
+    uint32_t limit = slotLimit();
+    if (limit > slots) growPool(limit);
+    updateTiles(f);
+    if (packScene(f)) {
+      solidsStale = true;
+      geometryDirty = true;
+    }
+    mayHaveFlame = mayHaveFlame || f.fuel.enabled;
+    for (uint32_t i = 0; i < f.source_count; i++) mayHaveFlame = mayHaveFlame || f.sources[i].flame > 0;
+    dt = (R)dtf;
+    buoyancy = f.simulation.buoyancy; coolingK = f.simulation.cooling; smokeWeight = f.simulation.smoke_weight;
+    damping = f.simulation.velocity_damping; dissipation = f.simulation.dissipation;
+    vorticity = f.simulation.vorticity;
+    timeU = (R)(float)time;
+    float seedf = (float)f.simulation.seed;
+    seedU = (R)seedf;
+    std::memcpy(&seedBits, &seedf, 4);
+    lifetimeZero = !mayHaveFlame;
+    fuelEnabled = f.fuel.enabled != 0;
+    ignition = f.fuel.ignition_heat;
+    burnRate = f.fuel.burn_rate;
+    held = (int)std::max<int64_t>(0, (int64_t)slots - (int64_t)slotLimit());
+    solidsAll = solidsStale;
+    for (int s = 0; s < capacity; s++) activity[(size_t)capacity * 64 + s] = 0;
+    allocation();
+    solidsStale = false;
+    zeroFresh();
+    transport();
+    forcesStep();
+    solvePressure();
+    projectStep();
+    readActivity();
+    time += dtf;
+    steps++;
+    return "";
+  }
+
+  // ---------------------------------------------------------------- allocation
+  // sourceNear (fluid-allocation.wgsl:90-108)
+  bool sourceNear(I3 b, int tile) {
+    R size = R(B) * h;
+    R lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+      lo[a] = R(b[a]) * size;
+      hi[a] = (R(b[a]) + R(1)) * size;
+    }
+    for (int i : lists[0][tile]) {
+      const Emitter<R>& e = emitters[i];
+      if (!e.enabled) continue;
+      bool inside = true;
+      for (int a = 0; a < 3; a++) {
+        R motion = std::fabs(e.vel[a]) + std::fabs(e.outward);
+        R pad = std::min(size, R(2) * h + motion * dt);
+        R extent = std::max(e.size[a], (R)0.03f) + pad;
+        if (!(e.pos[a] + extent > lo[a] && e.pos[a] - extent < hi[a])) inside = false;
+      }
+      if (inside) return true;
+    }
+    return false;
+  }
+  // buildBricks, freeBricks, allocateBricks, linkBricks, finishBricks, buildSolids
+  // (fluid-allocation.wgsl:129-387), serially in brick-id order.
+  void allocation() {
+    size_t count = (size_t)capacity * 64;
+    std::vector<uint32_t> st(count, 0);
+    std::vector<uint32_t> freeRank(count, 0), reqRank(count, 0);
+    uint32_t frees = 0, requests = 0;
+    for (size_t index = 0; index < count; index++) {
+      uint32_t s = 0;
+      int tile = (int)(index >> 6);
+      if (snapshotState[tile] != 0) {
+        I3 b = brickOf((uint32_t)index);
+        bool open = snapshotState[tile] != 2;
+        bool listed = false;
+        for (int z = -1; z <= 1 && open && !listed; z++)
+          for (int y = -1; y <= 1 && !listed; y++)
+            for (int x = -1; x <= 1 && !listed; x++) {
+              int nb = brickId(b[0] + x, b[1] + y, b[2] + z);
+              if (nb < 0) continue;
+              int toward = neighborIndex(-x, -y, -z);
+              listed = ((activity[nb] >> 3u) & (1u << toward)) != 0u;
+            }
+        if (open && !listed) listed = sourceNear(b, tile);
+        int32_t page = pages[index];
+        bool wasListed = (state[index] & 1u) != 0;
+        s = (uint32_t)listed | ((uint32_t)wasListed << 2);
+        if (!listed && page >= 0) s |= BRICK_FREES;
+        if (listed && page < 0) s |= BRICK_REQUESTS;
+      }
+      st[index] = s;
+      if (s & BRICK_FREES) freeRank[index] = frees++;
+      if (s & BRICK_REQUESTS) reqRank[index] = requests++;
+    }
+    zeroed.clear();
+    // freeBricks
+    for (size_t index = 0; index < count; index++) {
+      if (!(st[index] & BRICK_FREES)) continue;
+      int32_t page = pages[index];
+      freeStack[freeCount + freeRank[index]] = (uint32_t)page;
+      if (st[index] & 4u) zeroed.push_back({(uint32_t)index, (uint32_t)page});
+      pages[index] = -1;
+    }
+    // allocateBricks
+    active.clear();
+    for (size_t index = 0; index < count; index++) {
+      uint32_t s = st[index];
+      int32_t page = pages[index];
+      bool fresh = false;
+      if (s & BRICK_REQUESTS) {
+        int32_t top = freeCount + (int32_t)frees - (int32_t)reqRank[index];
+        if (top > held) {
+          page = (int32_t)freeStack[top - 1];
+          pages[index] = page;
+          zeroed.push_back({(uint32_t)index, (uint32_t)page | 0x80000000u});
+          fresh = true;
+        }
+      }
+      if (page >= 0) active.push_back((uint32_t)index);
+      state[index] = (uint32_t)(page >= 0);
+      entries[index] = page >= 0 ? (page | (fresh ? FRESH_ENTRY : 0)) : -1;
+      uint32_t flags = activity[index];
+      activity[index] = (flags & EXPANDS) ? MAY_EXPAND : 0u;
+    }
+    // The zero list holds frees, then grants, in brick order within each; its order is
+    // immaterial to the step.
+    // linkBricks
+    for (size_t index = 0; index < count; index++) {
+      if (entries[index] < 0) continue;
+      I3 b = brickOf((uint32_t)index);
+      int32_t* w = &records[index * RECORD_WORDS];
+      for (int k = 0; k < 27; k++) {
+        int dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = k / 9 - 1;
+        int nb = brickId(b[0] + dx, b[1] + dy, b[2] + dz);
+        w[k] = nb >= 0 ? entries[nb] : -1;
+      }
+      int unknowns = 1;
+      for (int k = 0; k < 8; k++) {
+        int dx = -(k & 1), dy = -((k >> 1) & 1), dz = -((k >> 2) & 1);
+        if (ground && b[1] + dy < 0) continue;
+        if (w[neighborIndex(dx, dy, dz)] < 0) unknowns = 0;
+      }
+      w[27] = unknowns;
+    }
+    // finishBricks
+    int32_t fr = freeCount + (int32_t)frees;
+    int32_t granted = std::min((int32_t)requests, std::max(fr - held, 0));
+    freeCount = fr - granted;
+    failures += requests - (uint32_t)granted;
+    // buildSolids
+    if (colliderCount > 0 || solidsAll) buildSolids();
+  }
+  bool insideCollider(const Collider<R>& c, int x, int y, int z) {
+    if (c.kind == 2) {
+      int q[3] = {x - c.lo[0], y - c.lo[1], z - c.lo[2]};
+      for (int a = 0; a < 3; a++)
+        if (q[a] < 0 || q[a] >= c.size[a]) return false;
+      uint32_t index = (uint32_t)((q[2] * c.size[1] + q[1]) * c.size[0] + q[0]);
+      return ((masks[c.first + (index >> 5)] >> (index & 31u)) & 1u) != 0;
+    }
+    R w[3] = {(R(x) + R(0.5)) * h, (R(y) + R(0.5)) * h, (R(z) + R(0.5)) * h};
+    R d[3];
+    for (int a = 0; a < 3; a++) {
+      // transpose(axes) * (w - center): row a = column a of axes.
+      R s = 0;
+      for (int k = 0; k < 3; k++) s += c.axes[a][k] * (w[k] - c.center[k]);
+      d[a] = std::fabs(s / c.extent[a]);
+    }
+    if (c.kind == 1) return d[0] < 1 && d[1] < 1 && d[2] < 1;
+    return d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < R(1);
+  }
+  void buildSolidsBrick(uint32_t id, int slot) {
+    I3 b = brickOf(id);
+    int tile = (int)(id >> 6);
+    for (int word = 0; word < W; word++) {
+      uint32_t bits = 0;
+      for (int k = 0; k < 32; k++) {
+        int bit = word * 32 + k;
+        int x = b[0] * B + (bit & (B - 1)), y = b[1] * B + ((bit >> shift) & (B - 1)), z = b[2] * B + (bit >> (2 * shift));
+        for (int i : lists[2][tile])
+          if (insideCollider(colliders[i], x, y, z)) {
+            bits |= 1u << k;
+            break;
+          }
+      }
+      solids[(size_t)slot * W + word] = bits;
+    }
+  }
+  void buildSolids() {
+    if (solidsAll) {
+      for (size_t id = 0; id < (size_t)capacity * 64; id++) {
+        int slot = entryPage(entries[id]);
+        if (slot >= 0) buildSolidsBrick((uint32_t)id, slot);
+      }
+    } else {
+      for (auto& z : zeroed)
+        if (z.second & 0x80000000u) buildSolidsBrick(z.first, (int)(z.second & 0xffffffu));
+    }
+  }
+  // fluid-zeroing.wgsl: a fresh slot starts as still, empty air. Pools every step
+  // rewrites before reading need no clearing.
+  void zeroFresh() {
+    for (auto& z : zeroed) {
+      if (!(z.second & 0x80000000u)) continue;
+      size_t s = z.second & 0xffffffu;
+      std::fill(vel.begin() + s * 3 * N, vel.begin() + (s + 1) * 3 * N, R(0));
+      std::fill(fld.begin() + s * 4 * N, fld.begin() + (s + 1) * 4 * N, R(0));
+      std::fill(expn.begin() + s * N, expn.begin() + (s + 1) * N, R(0));
+    }
+  }
+
+  // ---------------------------------------------------------------- transport
+  template <class F>
+  void forActiveCells(F fn) {
+    long n = (long)active.size();
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long i = 0; i < n; i++) {
+      uint32_t id = active[i];
+      int slot = entryPage(entries[id]);
+      I3 b = brickOf(id);
+      for (int c = 0; c < N; c++) {
+        int x = b[0] * B + (c & (B - 1)), y = b[1] * B + ((c >> shift) & (B - 1)), z = b[2] * B + (c >> (2 * shift));
+        fn(id, slot, c, x, y, z);
+      }
+    }
+  }
+  R sv(R x) { return store_round(x, prec.vel); }
+  R ss(R x) { return store_round(x, prec.scal); }
+
+  // advectVelocityWithBounds (fluid-velocity-transport.wgsl:28-100)
+  void advectVelocity() {
+    forActiveCells([&](uint32_t, int slot, int c, int x, int y, int z) {
+      // Bounds over the 2x2x2 forward block of the velocity.
+      for (int k = 0; k < 3; k++) {
+        R lo = R(1e5), hi = R(-1e5);
+        for (int dz = 0; dz < 2; dz++)
+          for (int dy = 0; dy < 2; dy++)
+            for (int dx = 0; dx < 2; dx++) {
+              R v = cellAt(vel, 3, k, x + dx, y + dy, z + dz);
+              lo = std::min(lo, v);
+              hi = std::max(hi, v);
+            }
+        vmin[((size_t)slot * 3 + k) * N + c] = store_round(lo, prec.bounds);
+        vmax[((size_t)slot * 3 + k) * N + c] = store_round(hi, prec.bounds);
+      }
+      V3<R> pos = center(x, y, z);
+      if (solidAt(pos[0], pos[1], pos[2])) {
+        for (int k = 0; k < 3; k++) velP[((size_t)slot * 3 + k) * N + c] = 0;
+        return;
+      }
+      V3<R> orig = v3<R>(vel[((size_t)slot * 3 + 0) * N + c], vel[((size_t)slot * 3 + 1) * N + c],
+                         vel[((size_t)slot * 3 + 2) * N + c]);
+      for (int comp = 0; comp < 3; comp++) {
+        V3<R> face = pos;
+        face[comp] += R(0.5) * h;
+        V3<R> fv = velocityOnFace(x, y, z, comp, orig);
+        V3<R> mid, dep;
+        for (int a = 0; a < 3; a++) mid[a] = face[a] - R(0.5) * dt * fv[a];
+        V3<R> vm = velocityAt(mid);
+        for (int a = 0; a < 3; a++) dep[a] = face[a] - dt * vm[a];
+        int32_t* d = &vdonor[(((size_t)slot * 3 + comp) * N + c) * 3];
+        V3<R> shifted = dep;
+        shifted[comp] -= R(0.5) * h;
+        for (int a = 0; a < 3; a++) d[a] = floori((double)(shifted[a] / h - R(0.5)));
+        velP[((size_t)slot * 3 + comp) * N + c] = sv(velComp(vel, dep, comp));
+      }
+    });
+  }
+  // correctVelocity (fluid-velocity-transport.wgsl:104-179)
+  void correctVelocity() {
+    forActiveCells([&](uint32_t, int slot, int c, int x, int y, int z) {
+      V3<R> pos = center(x, y, z);
+      if (solidAt(pos[0], pos[1], pos[2])) {
+        for (int k = 0; k < 3; k++) velC[((size_t)slot * 3 + k) * N + c] = 0;
+        return;
+      }
+      V3<R> orig;
+      for (int k = 0; k < 3; k++) orig[k] = vel[((size_t)slot * 3 + k) * N + c];
+      for (int comp = 0; comp < 3; comp++) {
+        R predicted = velP[((size_t)slot * 3 + comp) * N + c];
+        const int32_t* d = &vdonor[(((size_t)slot * 3 + comp) * N + c) * 3];
+        int bs = brickSlot(d[0] >> shift, d[1] >> shift, d[2] >> shift);
+        R lo = 0, hi = 0;
+        if (bs >= 0) {
+          int lc = local(d[0], d[1], d[2]);
+          lo = vmin[((size_t)bs * 3 + comp) * N + lc];
+          hi = vmax[((size_t)bs * 3 + comp) * N + lc];
+        }
+        R result;
+        if (lo == hi && predicted == lo) {
+          result = predicted;
+        } else {
+          V3<R> face = pos;
+          face[comp] += R(0.5) * h;
+          V3<R> fv = velocityOnFace(x, y, z, comp, orig);
+          V3<R> mid, fwd;
+          for (int a = 0; a < 3; a++) mid[a] = face[a] + R(0.5) * dt * fv[a];
+          V3<R> vm = velocityAt(mid);
+          for (int a = 0; a < 3; a++) fwd[a] = face[a] + dt * vm[a];
+          fwd[comp] -= R(0.5) * h;
+          R reversed = sampleCells(velP, 3, comp, fwd[0] / h, fwd[1] / h, fwd[2] / h);
+          R corrected = predicted + R(0.5) * (orig[comp] - reversed);
+          result = (corrected < lo || corrected > hi) ? predicted : corrected;
+        }
+        velC[((size_t)slot * 3 + comp) * N + c] = sv(result);
+      }
+    });
+  }
+  // fluid-advection.wgsl:53-61 traceBack / traceForward from a cell centre.
+  V3<R> trace(V3<R> p, V3<R> cv, R sign) {
+    V3<R> mid;
+    for (int a = 0; a < 3; a++) mid[a] = p[a] + sign * R(0.5) * dt * cv[a];
+    V3<R> vm = velocityAt(mid);
+    V3<R> out;
+    for (int a = 0; a < 3; a++) out[a] = p[a] + sign * dt * vm[a];
+    return out;
+  }
+  // advectScalars (fluid-scalar-transport.wgsl:38-142)
+  void advectScalars() {
+    forActiveCells([&](uint32_t, int slot, int c, int x, int y, int z) {
+      V3<R> pos = center(x, y, z);
+      V3<R> cv = velocityAt(pos);
+      V3<R> dep = trace(pos, cv, R(-1));
+      R out[4];
+      if (!maccormack) {
+        for (int k = 0; k < 4; k++) out[k] = sampleCells(fld, 4, k, dep[0] / h, dep[1] / h, dep[2] / h);
+        out[2] = clampr(out[2], R(0), R(1));
+      } else {
+        R dc[3] = {R(x) + (dep[0] - pos[0]) / h, R(y) + (dep[1] - pos[1]) / h, R(z) + (dep[2] - pos[2]) / h};
+        int base[3];
+        R fr[3];
+        for (int a = 0; a < 3; a++) {
+          base[a] = floori((double)dc[a]);
+          fr[a] = dc[a] - std::floor(dc[a]);
+        }
+        R mn[3] = {R(65504), R(65504), R(65504)}, mx[3] = {R(-65504), R(-65504), R(-65504)};
+        R lmin = 1, lmax = 0;
+        R value[4] = {0, 0, 0, 0};
+        for (int dz = 0; dz < 2; dz++)
+          for (int dy = 0; dy < 2; dy++)
+            for (int dx = 0; dx < 2; dx++) {
+              R s[4];
+              for (int k = 0; k < 4; k++) s[k] = cellAt(fld, 4, k, base[0] + dx, base[1] + dy, base[2] + dz);
+              R bsx = store_round(s[0], prec.bounds == STORE_EXACT ? prec.scal : STORE_F16);
+              R bsy = store_round(s[1], prec.bounds == STORE_EXACT ? prec.scal : STORE_F16);
+              R bsz = store_round(s[2], prec.bounds == STORE_EXACT ? prec.scal : STORE_F16);
+              R bsw = store_round(s[3], prec.bounds == STORE_EXACT ? prec.scal : STORE_F16);
+              mn[0] = std::min(mn[0], bsx); mn[1] = std::min(mn[1], bsy); mn[2] = std::min(mn[2], bsw);
+              mx[0] = std::max(mx[0], bsx); mx[1] = std::max(mx[1], bsy); mx[2] = std::max(mx[2], bsw);
+              lmin = std::min(lmin, bsz);
+              lmax = std::max(lmax, bsz);
+              R w = (dx ? fr[0] : R(1) - fr[0]) * (dy ? fr[1] : R(1) - fr[1]) * (dz ? fr[2] : R(1) - fr[2]);
+              for (int k = 0; k < 4; k++) value[k] += s[k] * w;
+            }
+        R* bnd = &sb[(size_t)slot * 8 * N];
+        bnd[0 * N + c] = mn[0]; bnd[1 * N + c] = mn[1]; bnd[2 * N + c] = mn[2]; bnd[3 * N + c] = lmin;
+        bnd[4 * N + c] = mx[0]; bnd[5 * N + c] = mx[1]; bnd[6 * N + c] = mx[2]; bnd[7 * N + c] = lmax;
+        out[0] = value[0];
+        out[1] = value[1];
+        out[2] = lifetimeZero ? R(0) : value[2];
+        out[3] = value[3];
+      }
+      for (int k = 0; k < 4; k++) fldP[((size_t)slot * 4 + k) * N + c] = ss(out[k]);
+    });
+  }
+  R rampIntegral(int ch, R lo, R hi) {
+    R area = 0;
+    for (int i = 1; i < flame.counts[ch]; i++) {
+      R ax = flame.knots[ch][i - 1][0], ay = flame.knots[ch][i - 1][1];
+      R bx = flame.knots[ch][i][0], by = flame.knots[ch][i][1];
+      R left = std::max(lo, ax), right = std::min(hi, bx);
+      if (right > left) {
+        R y0 = mixr(ay, by, (left - ax) / (bx - ax));
+        R y1 = mixr(ay, by, (right - ax) / (bx - ax));
+        area += (right - left) * (y0 + y1) * R(0.5);
+      }
+    }
+    return area;
+  }
+  // evaluateFlame (flame-common.wgsl:30-42)
+  void evaluateFlame(R before, R& after, R prod[3]) {
+    if (before <= 0) {
+      after = 0;
+      prod[0] = prod[1] = prod[2] = 0;
+      return;
+    }
+    after = std::max(R(0), before - flame.dt / flame.lifespan);
+    prod[0] = flame.smoke * flame.lifespan * rampIntegral(0, after, before);
+    prod[1] = flame.heat * flame.lifespan * rampIntegral(1, after, before);
+    prod[2] = flame.expansion * (flame.lifespan * rampIntegral(2, after, before) / flame.dt);
+  }
+  R emitterWeight(const Emitter<R>& e, V3<R> p) {
+    R d[3];
+    for (int a = 0; a < 3; a++) d[a] = (p[a] - e.pos[a]) / std::max(e.size[a], (R)0.03f);
+    R r = e.box ? std::max(std::fabs(d[0]), std::max(std::fabs(d[1]), std::fabs(d[2])))
+                : std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    if (r >= R(1) || !e.enabled) return 0;
+    return R(1) - smoothstep(R(0.5), R(1), r);
+  }
+  void burstVariation(const Emitter<R>& e, V3<R> p, R out[2]) {
+    if (e.strength == 0) {
+      out[0] = out[1] = 1;
+      return;
+    }
+    V3<R> q;
+    const R off[3] = {R(3.17), R(7.53), R(11.29)};
+    for (int a = 0; a < 3; a++) q[a] = (p[a] - e.pos[a]) / e.period + off[a];
+    V3<R> q2 = v3<R>(q[0] + R(17.3), q[1] + R(2.8), q[2] + R(8.6));
+    out[0] = R(1) - e.strength * burst_pattern(q, seedBits);
+    out[1] = R(1) - e.strength * burst_pattern(q2, seedBits);
+  }
+  // evolveFields (fluid-field-evolution.wgsl:9-84) with correctedScalars
+  // (fluid-scalar-transport.wgsl:144-199) and recordContent (fluid-content.wgsl:29-64).
+  void evolveFields() {
+    long n = (long)active.size();
+    std::vector<uint32_t> busyOut(n, 0), expandsOut(n, 0);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long i = 0; i < n; i++) {
+      uint32_t id = active[i];
+      int slot = entryPage(entries[id]);
+      I3 b = brickOf(id);
+      int tile = (int)(id >> 6);
+      uint32_t busy = 0;
+      bool expands = false;
+      for (int c = 0; c < N; c++) {
+        int x = b[0] * B + (c & (B - 1)), y = b[1] * B + ((c >> shift) & (B - 1)), z = b[2] * B + (c >> (2 * shift));
+        V3<R> pos = center(x, y, z);
+        bool cvSampled = false;
+        V3<R> cv;
+        auto traceVel = [&]() {
+          if (!cvSampled) {
+            cv = velocityAt(pos);
+            cvSampled = true;
+          }
+          return cv;
+        };
+        R value[4] = {0, 0, 0, 0};
+        R expansion = 0;
+        bool injected = false;
+        if (!solidAt(pos[0], pos[1], pos[2])) {
+          R tr[4];
+          const R* adv = &fldP[(size_t)slot * 4 * N];
+          if (!maccormack) {
+            for (int k = 0; k < 4; k++) tr[k] = adv[k * N + c];
+          } else {
+            const R* bnd = &sb[(size_t)slot * 8 * N];
+            R mn[3] = {bnd[0 * N + c], bnd[1 * N + c], bnd[2 * N + c]};
+            R mx[3] = {bnd[4 * N + c], bnd[5 * N + c], bnd[6 * N + c]};
+            R lmin = bnd[3 * N + c], lmax = bnd[7 * N + c];
+            if (mn[0] == mx[0] && mn[1] == mx[1] && mn[2] == mx[2] && lmin == lmax) {
+              tr[0] = mn[0]; tr[1] = mn[1]; tr[2] = clampr(lmin, R(0), R(1)); tr[3] = mn[2];
+            } else {
+              R a[4] = {adv[0 * N + c], adv[1 * N + c], adv[2 * N + c], adv[3 * N + c]};
+              V3<R> fwd = trace(pos, traceVel(), R(1));
+              R o[4];
+              for (int k = 0; k < 4; k++) o[k] = fld[((size_t)slot * 4 + k) * N + c];
+              R lifetime = a[2];
+              R rev[3];
+              if (lmin != lmax || a[2] != lmin) {
+                R fc[3] = {R(x) + (fwd[0] - pos[0]) / h, R(y) + (fwd[1] - pos[1]) / h, R(z) + (fwd[2] - pos[2]) / h};
+                int base[3];
+                R fr[3];
+                for (int ax = 0; ax < 3; ax++) {
+                  base[ax] = floori((double)fc[ax]);
+                  fr[ax] = fc[ax] - std::floor(fc[ax]);
+                }
+                R rs[4] = {0, 0, 0, 0};
+                for (int dz = 0; dz < 2; dz++)
+                  for (int dy = 0; dy < 2; dy++)
+                    for (int dx = 0; dx < 2; dx++) {
+                      R w = (dx ? fr[0] : R(1) - fr[0]) * (dy ? fr[1] : R(1) - fr[1]) * (dz ? fr[2] : R(1) - fr[2]);
+                      for (int k = 0; k < 4; k++) rs[k] += cellAt(fldP, 4, k, base[0] + dx, base[1] + dy, base[2] + dz) * w;
+                    }
+                rev[0] = rs[0]; rev[1] = rs[1]; rev[2] = rs[3];
+                R cl = a[2] + R(0.5) * (o[2] - rs[2]);
+                lifetime = (cl < lmin || cl > lmax) ? a[2] : cl;
+              } else {
+                rev[0] = sampleCells(fldP, 4, 0, fwd[0] / h, fwd[1] / h, fwd[2] / h);
+                rev[1] = sampleCells(fldP, 4, 1, fwd[0] / h, fwd[1] / h, fwd[2] / h);
+                rev[2] = sampleCells(fldP, 4, 3, fwd[0] / h, fwd[1] / h, fwd[2] / h);
+              }
+              R ax3[3] = {a[0], a[1], a[3]}, ox3[3] = {o[0], o[1], o[3]}, bd[3];
+              for (int k = 0; k < 3; k++) {
+                R corr = ax3[k] + R(0.5) * (ox3[k] - rev[k]);
+                bd[k] = (corr < mn[k] || corr > mx[k]) ? ax3[k] : corr;
+              }
+              tr[0] = bd[0]; tr[1] = bd[1]; tr[2] = clampr(lifetime, R(0), R(1)); tr[3] = bd[2];
+            }
+          }
+          // The corrected scalars as the half-float field held them.
+          for (int k = 0; k < 4; k++) tr[k] = prec.truncate ? (R)truncate_half((double)tr[k]) : ss(tr[k]);
+          R lifetime = tr[2];
+          R prodS = 0, prodH = 0, injectedFuel = 0;
+          for (int ei : lists[0][tile]) {
+            const Emitter<R>& e = emitters[ei];
+            R w = emitterWeight(e, pos);
+            if (w == 0) continue;
+            R var[2];
+            burstVariation(e, pos, var);
+            lifetime = std::max(lifetime, e.flame * w * var[1]);
+            prodS += e.smoke * w * dt;
+            prodH += e.heat * var[0] * w * dt;
+            injectedFuel += e.fuel * w * dt;
+          }
+          R remaining = 0, burned = 0;
+          if (fuelEnabled) {
+            remaining = tr[3] + injectedFuel;
+            if (tr[1] + prodH >= ignition) {
+              lifetime = std::max(lifetime, std::min(remaining, R(1)));
+              R unburned = remaining * std::exp(-burnRate * dt);
+              burned = remaining - unburned;
+              remaining = unburned;
+            }
+          }
+          R after, fp[3];
+          evaluateFlame(clampr(lifetime, R(0), R(1)), after, fp);
+          expansion = fp[2] + flame.expansion * burned / dt;
+          R dS = tr[0] * std::exp(-dissipation * dt) + (prodS + fp[0]) * std::exp(-dissipation * dt * R(0.5));
+          R dH = tr[1] * std::exp(-coolingK * dt) + (prodH + fp[1]) * std::exp(-coolingK * dt * R(0.5));
+          value[0] = std::max(dS, R(0));
+          value[1] = std::max(dH, R(0));
+          value[2] = after;
+          value[3] = remaining;
+          injected = prodS > 0 || prodH > 0 || lifetime > tr[2] || injectedFuel > 0;
+        }
+        // clearDormant (fluid-common.wgsl:8-13)
+        if (!injected && value[2] == 0 && value[0] < R(0.001) && value[1] < R(0.001) && value[3] < R(0.001))
+          value[0] = value[1] = value[2] = value[3] = 0;
+        for (int k = 0; k < 4; k++) fldN[((size_t)slot * 4 + k) * N + c] = ss(value[k]);
+        expn[(size_t)slot * N + c] = store_round(expansion, prec.expn);
+        if (expansion != 0) expands = true;
+        // holdsContent (fluid-content.wgsl:22-24) tests the value before its store rounds.
+        if (std::max(std::max(value[0], value[2]), value[3]) > (R)cutoff) {
+          V3<R> v = traceVel();
+          busy |= contentSupport(x, y, z, v);
+        }
+      }
+      busyOut[i] = busy;
+      expandsOut[i] = expands;
+    }
+    for (long i = 0; i < n; i++) {
+      uint32_t id = active[i];
+      uint32_t flags = 0;
+      if (busyOut[i]) {
+        flags = CONTENT | (busyOut[i] << 3);
+        uint32_t l = id & 63u;
+        uint32_t bits = (1u << (l & 3u)) | (16u << ((l >> 2) & 3u)) | (256u << (l >> 4));
+        activity[(size_t)capacity * 64 + (id >> 6)] |= bits;
+      }
+      if (expandsOut[i]) flags |= EXPANDS;
+      activity[id] |= flags;
+    }
+  }
+  // contentSupport (fluid-content.wgsl:29-39)
+  uint32_t contentSupport(int x, int y, int z, V3<R> v) {
+    int id[3] = {x, y, z};
+    bool low[3], high[3];
+    for (int a = 0; a < 3; a++) {
+      R side = R(B);
+      R loc = R(id[a] & (B - 1)) + R(0.5);
+      R pad = std::min(side, std::max(R(2), R(2)) + std::fabs(v[a]) * dt / h);
+      low[a] = loc < pad;
+      high[a] = loc + pad >= side;
+    }
+    uint32_t row = 2u | (low[0] ? 1u : 0u) | (high[0] ? 4u : 0u);
+    uint32_t plane = (row << 3u) | (low[1] ? row : 0u) | (high[1] ? (row << 6u) : 0u);
+    return (plane << 9u) | (low[2] ? plane : 0u) | (high[2] ? (plane << 18u) : 0u);
+  }
+  void transport() {
+    advectVelocity();
+    correctVelocity();
+    advectScalars();
+    evolveFields();
+    fld.swap(fldN);
+  }
+
+  // ---------------------------------------------------------------- forces
+  void buildNoise() {
+    noiseTable.resize(64 * 64 * 64);
+    for (int z = 0; z < 64; z++)
+      for (int y = 0; y < 64; y++)
+        for (int x = 0; x < 64; x++) {
+          V3<float> p = v3<float>((x + 0.5f) / 64.0f * 16.0f, (y + 0.5f) / 64.0f * 16.0f, (z + 0.5f) / 64.0f * 16.0f);
+          V3<float> dx = noise_gradient(p);
+          V3<float> dy = noise_gradient(v3<float>(p[0] + 7.1f, p[1] + 3.7f, p[2] + 11.3f));
+          V3<float> dz = noise_gradient(v3<float>(p[0] + 5.2f, p[1] + 7.9f, p[2] + 9.5f));
+          V3<float> c = v3<float>(dz[1] - dy[2], dx[2] - dz[0], dy[0] - dx[1]);
+          for (int a = 0; a < 3; a++) c[a] = (float)round_f16(c[a]);  // rgba16float texture
+          noiseTable[(z * 64 + y) * 64 + x] = c;
+        }
+  }
+  // curlNoise (fluid-forces.wgsl:3-9): a repeat-addressed trilinear fetch of the table.
+  V3<R> curlNoise(V3<R> p) {
+    static const R rot[3][3] = {{R(.36), R(-.8), R(.48)}, {R(.48), R(.6), R(.64)}, {R(-.8), R(0), R(.6)}};  // columns
+    R uvw[3];
+    for (int a = 0; a < 3; a++) uvw[a] = (rot[0][a] * p[0] + rot[1][a] * p[1] + rot[2][a] * p[2]) / R(16);
+    int i0[3];
+    R f[3];
+    for (int a = 0; a < 3; a++) {
+      R t = uvw[a] * R(64) - R(0.5);
+      i0[a] = floori((double)t);
+      f[a] = t - std::floor(t);
+    }
+    R s[3] = {0, 0, 0};
+    for (int dz = 0; dz < 2; dz++)
+      for (int dy = 0; dy < 2; dy++)
+        for (int dx = 0; dx < 2; dx++) {
+          int xi = (i0[0] + dx) & 63, yi = (i0[1] + dy) & 63, zi = (i0[2] + dz) & 63;
+          R w = (dx ? f[0] : R(1) - f[0]) * (dy ? f[1] : R(1) - f[1]) * (dz ? f[2] : R(1) - f[2]);
+          const V3<float>& v = noiseTable[(zi * 64 + yi) * 64 + xi];
+          for (int a = 0; a < 3; a++) s[a] += (R)v[a] * w;
+        }
+    V3<R> out;
+    for (int a = 0; a < 3; a++) out[a] = rot[a][0] * s[0] + rot[a][1] * s[1] + rot[a][2] * s[2];
+    return out;
+  }
+  // externalForces + coverage (force-fields.wgsl:312-365)
+  V3<R> externalForces(int tile, V3<R> p) {
+    V3<R> result = v3<R>(0, 0, 0);
+    for (int index : lists[1][tile]) {
+      const Force<R>& f = forces[index];
+      R weight = 1;
+      if (f.targeted) {
+        R covered = 0;
+        for (int r = 0; r < f.regionCount; r++) {
+          const Region<R>& g = regions[f.regionFirst + r];
+          R d[3];
+          for (int a = 0; a < 3; a++) d[a] = std::fabs((p[a] - g.center[a]) / std::max(g.size[a], (R)0.03f));
+          R dist = g.box ? std::max(d[0], std::max(d[1], d[2])) : std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+          covered = std::max(covered, R(1) - smoothstep(R(0.5), R(1), dist));
+        }
+        weight = covered;
+      }
+      if (weight == 0) continue;
+      V3<R> acc = v3<R>(f.axis[0] * f.strength, f.axis[1] * f.strength, f.axis[2] * f.strength);
+      if (f.kind == 1) {
+        V3<R> q;
+        R off[3] = {seedU, -timeU * R(0.7), seedU * R(0.25)};
+        for (int a = 0; a < 3; a++) q[a] = p[a] * f.scale * R(0.65) + off[a];
+        V3<R> q2 = v3<R>(q[0] * R(2.03) + R(13.7), q[1] * R(2.03) + R(5.3), q[2] * R(2.03) + R(19.1));
+        V3<R> n1 = curlNoise(q), n2 = curlNoise(q2);
+        for (int a = 0; a < 3; a++) acc[a] = (n1[a] + R(0.45) * n2[a]) * f.strength;
+      } else if (f.kind >= 2) {
+        R delta[3], radial[3];
+        for (int a = 0; a < 3; a++) radial[a] = delta[a] = p[a] - f.center[a];
+        if (f.kind == 2) {
+          R dd = delta[0] * f.axis[0] + delta[1] * f.axis[1] + delta[2] * f.axis[2];
+          for (int a = 0; a < 3; a++) radial[a] -= f.axis[a] * dd;
+        }
+        R rr = radial[0] * radial[0] + radial[1] * radial[1] + radial[2] * radial[2];
+        R distance = std::sqrt(rr);
+        R radius = std::max(f.scale, R(0.01));
+        R dir[3];
+        for (int a = 0; a < 3; a++) dir[a] = radial[a] / std::max(distance, radius * R(0.25));
+        R falloff = R(1) / (R(1) + rr / (radius * radius));
+        if (f.kind == 2) {
+          R cr[3] = {f.axis[1] * dir[2] - f.axis[2] * dir[1], f.axis[2] * dir[0] - f.axis[0] * dir[2],
+                     f.axis[0] * dir[1] - f.axis[1] * dir[0]};
+          for (int a = 0; a < 3; a++)
+            acc[a] = (cr[a] * f.strength - dir[a] * f.inward + f.axis[a] * f.lift) * falloff;
+        } else {
+          for (int a = 0; a < 3; a++) acc[a] = dir[a] * f.strength * falloff;
+        }
+      }
+      for (int a = 0; a < 3; a++) result[a] += acc[a] * weight;
+    }
+    return result;
+  }
+  // computeCurl (fluid-forces.wgsl:38-75) over the corrected velocity.
+  void computeCurl() {
+    forActiveCells([&](uint32_t, int slot, int c, int x, int y, int z) {
+      auto cc = [&](int px, int py, int pz, int comp) {
+        int q[3] = {px, py, pz};
+        q[comp] -= 1;
+        return R(0.5) * (cellAt(velC, 3, comp, px, py, pz) + cellAt(velC, 3, comp, q[0], q[1], q[2]));
+      };
+      R hh = R(0.5) / h;
+      R dx0 = (cc(x + 1, y, z, 1) - cc(x - 1, y, z, 1)) * hh, dx1 = (cc(x + 1, y, z, 2) - cc(x - 1, y, z, 2)) * hh;
+      R dy0 = (cc(x, y + 1, z, 0) - cc(x, y - 1, z, 0)) * hh, dy1 = (cc(x, y + 1, z, 2) - cc(x, y - 1, z, 2)) * hh;
+      R dz0 = (cc(x, y, z + 1, 0) - cc(x, y, z - 1, 0)) * hh, dz1 = (cc(x, y, z + 1, 1) - cc(x, y, z - 1, 1)) * hh;
+      R cv[3] = {dy1 - dz1, dz0 - dx1, dx0 - dy0};
+      R mag = std::sqrt(cv[0] * cv[0] + cv[1] * cv[1] + cv[2] * cv[2]);
+      for (int k = 0; k < 3; k++) curl[((size_t)slot * 4 + k) * N + c] = store_round(cv[k], prec.curl);
+      curl[((size_t)slot * 4 + 3) * N + c] = store_round(mag, prec.curl);
+    });
+  }
+  // centerForce (fluid-forces.wgsl:79-104), cellForce (:113-118)
+  V3<R> cellForce(int tile, int x, int y, int z) {
+    if (brickSlot(x >> shift, y >> shift, z >> shift) < 0) return v3<R>(0, 0, 0);
+    V3<R> w = center(x, y, z);
+    V3<R> F = v3<R>(0, 0, 0);
+    if (!solidAt(w[0], w[1], w[2])) {
+      R heat = cellAt(fld, 4, 1, x, y, z), density = cellAt(fld, 4, 0, x, y, z);
+      V3<R> conf = v3<R>(0, 0, 0);
+      if (vorticity != 0) {
+        R c[3] = {cellAt(curl, 4, 0, x, y, z), cellAt(curl, 4, 1, x, y, z), cellAt(curl, 4, 2, x, y, z)};
+        R eta[3] = {cellAt(curl, 4, 3, x + 1, y, z) - cellAt(curl, 4, 3, x - 1, y, z),
+                    cellAt(curl, 4, 3, x, y + 1, z) - cellAt(curl, 4, 3, x, y - 1, z),
+                    cellAt(curl, 4, 3, x, y, z + 1) - cellAt(curl, 4, 3, x, y, z - 1)};
+        R len = std::sqrt(eta[0] * eta[0] + eta[1] * eta[1] + eta[2] * eta[2]) + R(0.0001);
+        R n[3] = {eta[0] / len, eta[1] / len, eta[2] / len};
+        R s = vorticity * h;
+        conf = v3<R>((n[1] * c[2] - n[2] * c[1]) * s, (n[2] * c[0] - n[0] * c[2]) * s, (n[0] * c[1] - n[1] * c[0]) * s);
+      }
+      V3<R> ext = externalForces(tile, w);
+      for (int a = 0; a < 3; a++) F[a] = conf[a] + ext[a];
+      F[1] += buoyancy * heat - smokeWeight * density;
+    }
+    for (int a = 0; a < 3; a++) F[a] = prec.truncate ? (R)truncate_half((double)F[a]) : sv(F[a]);
+    return F;
+  }
+  // sourceVelocity (fluid-forces.wgsl:122-149)
+  R sourceVelocity(int tile, R value, V3<R> face, int comp) {
+    R result = value;
+    for (int ei : lists[0][tile]) {
+      const Emitter<R>& e = emitters[ei];
+      if (e.response == 0) continue;
+      R w = emitterWeight(e, face);
+      if (w == 0) continue;
+      R radial[3] = {0, 0, 0};
+      if (e.outward != 0) {
+        R d[3] = {face[0] - e.pos[0], face[1] - e.pos[1], face[2] - e.pos[2]};
+        R len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        for (int a = 0; a < 3; a++) radial[a] = d[a] / std::max(len, R(1e-6)) * e.outward;
+      }
+      result = mixr(result, e.vel[comp] + radial[comp], R(1) - std::exp(-e.response * w * dt));
+    }
+    return result;
+  }
+  // applyForces (fluid-forces.wgsl:151-182), then computeDivergence (:184-203).
+  void forcesStep() {
+    if (vorticity != 0) computeCurl();
+    forActiveCells([&](uint32_t id, int slot, int c, int x, int y, int z) {
+      int tile = (int)(id >> 6);
+      V3<R> F0 = cellForce(tile, x, y, z);
+      V3<R> Fx = cellForce(tile, x + 1, y, z), Fy = cellForce(tile, x, y + 1, z), Fz = cellForce(tile, x, y, z + 1);
+      R force[3] = {R(0.5) * (F0[0] + Fx[0]), R(0.5) * (F0[1] + Fy[1]), R(0.5) * (F0[2] + Fz[2])};
+      V3<R> pos = center(x, y, z);
+      R decay = std::exp(-damping * dt);
+      R v[3];
+      for (int a = 0; a < 3; a++) v[a] = velC[((size_t)slot * 3 + a) * N + c] * decay + dt * force[a];
+      R out[3];
+      for (int a = 0; a < 3; a++) {
+        V3<R> face = pos;
+        face[a] += R(0.5) * h;
+        out[a] = sourceVelocity(tile, v[a], face, a);
+      }
+      // enforceFaces (fluid-forces.wgsl:15-31)
+      if (solidAt(pos[0], pos[1], pos[2])) {
+        out[0] = out[1] = out[2] = 0;
+      } else {
+        if (solidAt(pos[0] + h, pos[1], pos[2])) out[0] = 0;
+        if (solidAt(pos[0], pos[1] + h, pos[2])) out[1] = 0;
+        if (solidAt(pos[0], pos[1], pos[2] + h)) out[2] = 0;
+      }
+      for (int a = 0; a < 3; a++) velF[((size_t)slot * 3 + a) * N + c] = sv(out[a]);
+    });
+    forActiveCells([&](uint32_t, int slot, int c, int x, int y, int z) {
+      R d = (velF[((size_t)slot * 3 + 0) * N + c] - cellAt(velF, 3, 0, x - 1, y, z)) / h +
+            (velF[((size_t)slot * 3 + 1) * N + c] - cellAt(velF, 3, 1, x, y - 1, z)) / h +
+            (velF[((size_t)slot * 3 + 2) * N + c] - cellAt(velF, 3, 2, x, y, z - 1)) / h;
+      div[(size_t)slot * N + c] = store_round(h * h * (d - expn[(size_t)slot * N + c]), prec.p0);
+    });
+  }
+
+  // ---------------------------------------------------------------- multigrid (pressure.wgsl)
+  int storeMode(int level) { return level == 0 ? prec.p0 : prec.pc; }
+  // cellAddress (pressure.wgsl:72-92): -1 without storage.
+  long cellAddress(int px, int py, int pz, int level) {
+    int s = levelShift(level), side = 1 << s;
+    int lx = px & (side - 1), ly = py & (side - 1), lz = pz & (side - 1);
+    long owner;
+    if (level < brickLevels) {
+      int slot = brickSlot(px >> s, py >> s, pz >> s);
+      if (slot < 0) return -1;
+      owner = slot;
+    } else {
+      int t = tileAt(px >> s, py >> s, pz >> s);
+      if (t < 0) return -1;
+      owner = t;
+    }
+    return owner * side * side * side + (lz * side + ly) * side + lx;
+  }
+  bool brickActive(int bx, int by, int bz) { return brickEntry(bx, by, bz) >= 0; }
+  // activeCell (pressure.wgsl:100-136)
+  bool activeCell(int px, int py, int pz, int level) {
+    if (level >= brickLevels) {
+      int n = 1 << (level - brickLevels);
+      for (int z = 0; z < n; z++)
+        for (int y = 0; y < n; y++)
+          for (int x = 0; x < n; x++) {
+            int id = brickId(px * n + x, py * n + y, pz * n + z);
+            if (id < 0 || entries[id] < 0 || records[(size_t)id * RECORD_WORDS + 27] == 0) return false;
+          }
+      return true;
+    }
+    int span = 1 << level;
+    int p[3] = {px, py, pz};
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+      lo[a] = (p[a] * span - 1) >> brickLevels;
+      hi[a] = (p[a] * span + span - 1) >> brickLevels;
+    }
+    if (ground) lo[1] = std::max(lo[1], 0);
+    for (int z = lo[2]; z <= hi[2]; z++)
+      for (int y = lo[1]; y <= hi[1]; y++)
+        for (int x = lo[0]; x <= hi[0]; x++)
+          if (!brickActive(x, y, z)) return false;
+    return true;
+  }
+  bool blockedAt(int px, int py, int pz, int level) {
+    R s = h * R(1 << level);
+    return solidAt((R(px) + R(0.5)) * s, (R(py) + R(0.5)) * s, (R(pz) + R(0.5)) * s);
+  }
+  uint8_t cellTopology(int px, int py, int pz, int level) {
+    if (blockedAt(px, py, pz, level)) return STORED_SOLID;
+    static const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    uint8_t flags = 0;
+    for (int s = 0; s < 6; s++)
+      if (!blockedAt(px + off[s][0], py + off[s][1], pz + off[s][2], level)) flags |= (uint8_t)(1u << s);
+    return flags;
+  }
+  std::vector<uint8_t>& topo(int level) { return levels[level].topo; }
+  void buildBrickTopology(uint32_t id, int slot, int level) {
+    I3 b = brickOf(id);
+    int side = levelSide(level), cells = side * side * side;
+    for (int o = 0; o < cells; o++) {
+      int lx = o % side, ly = (o / side) % side, lz = o / (side * side);
+      topo(level)[(size_t)slot * cells + o] = cellTopology(b[0] * side + lx, b[1] * side + ly, b[2] * side + lz, level);
+    }
+  }
+  void buildTopology() {
+    if (geometryDirty) {
+      for (size_t id = 0; id < (size_t)capacity * 64; id++) {
+        if (snapshotState[id >> 6] == 0) continue;
+        int slot = entryPage(entries[id]);
+        if (slot < 0) continue;
+        for (int l = 0; l < brickLevels; l++) buildBrickTopology((uint32_t)id, slot, l);
+      }
+      for (int l = brickLevels; l <= bottom; l++) {
+        int side = levelSide(l), cells = side * side * side;
+        for (int t = 0; t < capacity; t++) {
+          if (snapshotState[t] == 0) continue;
+          for (int o = 0; o < cells; o++) {
+            int lx = o % side, ly = (o / side) % side, lz = o / (side * side);
+            topo(l)[(size_t)t * cells + o] =
+                cellTopology(snapshot[t][0] * side + lx, snapshot[t][1] * side + ly, snapshot[t][2] * side + lz, l);
+          }
+        }
+      }
+      geometryDirty = false;
+    }
+  }
+  // Fresh slots need their topology every step (PressureSolver.ts:293-302).
+  void buildZeroedTopology() {
+    for (auto& z : zeroed) {
+      int slot = entryPage(entries[z.first]);
+      if (slot < 0) continue;
+      for (int l = 0; l < brickLevels; l++) buildBrickTopology(z.first, slot, l);
+    }
+  }
+  uint32_t flagsOf(int level, long addr) {
+    uint8_t s = topo(level)[addr];
+    if (s & STORED_SOLID) return SOLID;
+    return s & 63u;
+  }
+  static R axisDiag(uint32_t flags) {
+    return R((flags >> 0) & 1) + R((flags >> 1) & 1) + R((flags >> 2) & 1) + R((flags >> 3) & 1) +
+           R((flags >> 4) & 1) + R((flags >> 5) & 1);
+  }
+  std::vector<R>* inP;
+  std::vector<R>* outP;
+  std::vector<R>* inRhs;
+  R readAt(const std::vector<R>& arr, int px, int py, int pz, int level) {
+    long a = cellAddress(px, py, pz, level);
+    return a < 0 ? R(0) : arr[a];
+  }
+  // stencil (pressure.wgsl:360-402): sum of open neighbours and the diagonal; axis weights are
+  // 1 on the cubic lattice.
+  void stencil(int px, int py, int pz, uint32_t flags, int level, const std::vector<R>& p, R& sum, R& diag) {
+    static const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    R v[6];
+    for (int s = 0; s < 6; s++)
+      v[s] = (flags & (1u << s)) ? readAt(p, px + off[s][0], py + off[s][1], pz + off[s][2], level) : R(0);
+    sum = (v[0] + v[1]) + (v[2] + v[3]) + (v[4] + v[5]);
+    diag = R((flags >> 0) & 1) + R((flags >> 1) & 1) + (R((flags >> 2) & 1) + R((flags >> 3) & 1)) +
+           (R((flags >> 4) & 1) + R((flags >> 5) & 1));
+  }
+  // Cells a level's dispatch covers: every cell of every listed brick (brick levels), or of
+  // every tile (tile levels).
+  template <class F>
+  void forLevelCells(int level, F fn) {
+    int side = levelSide(level), cells = side * side * side;
+    if (level < brickLevels) {
+      long n = (long)active.size();
+#pragma omp parallel for schedule(dynamic, 8)
+      for (long i = 0; i < n; i++) {
+        I3 b = brickOf(active[i]);
+        for (int o = 0; o < cells; o++)
+          fn(b[0] * side + o % side, b[1] * side + (o / side) % side, b[2] * side + o / (side * side));
+      }
+    } else {
+#pragma omp parallel for schedule(dynamic, 8)
+      for (int t = 0; t < capacity; t++) {
+        if (snapshotState[t] == 0) continue;
+        for (int o = 0; o < cells; o++)
+          fn(snapshot[t][0] * side + o % side, snapshot[t][1] * side + (o / side) % side,
+             snapshot[t][2] * side + o / (side * side));
+      }
+    }
+  }
+  // relaxCell (pressure.wgsl:468-479); `first` is initializePressure (:485-505).
+  void relax(int level, const std::vector<R>& rhs, const std::vector<R>& pin, std::vector<R>& pout, bool first) {
+    forLevelCells(level, [&](int px, int py, int pz) {
+      long a = cellAddress(px, py, pz, level);
+      uint32_t flags = flagsOf(level, a);
+      if ((flags & SOLID) || !activeCell(px, py, pz, level)) {
+        pout[a] = 0;
+        return;
+      }
+      R sum, diag;
+      if (first) {
+        diag = R((flags >> 0) & 1) + R((flags >> 1) & 1) + (R((flags >> 2) & 1) + R((flags >> 3) & 1)) +
+               (R((flags >> 4) & 1) + R((flags >> 5) & 1));
+        pout[a] = store_round(mixr(R(0), (R(0) - rhs[a]) / std::max(diag, R(1e-12)), R(0.8)), storeMode(level));
+        return;
+      }
+      stencil(px, py, pz, flags, level, pin, sum, diag);
+      R cand = (sum - rhs[a]) / std::max(diag, R(1e-12));
+      pout[a] = store_round(mixr(pin[a], cand, R(0.8)), storeMode(level));
+    });
+  }
+  // restrictCell (pressure.wgsl:601-647): coarse right-hand side and its first iterate.
+  void restrictLevel(int fine, const std::vector<R>& rhs, const std::vector<R>& p, std::vector<R>& crhs,
+                     std::vector<R>& cfirst) {
+    int level = fine + 1;
+    forLevelCells(level, [&](int cx, int cy, int cz) {
+      R residual = 0;
+      bool every = true;
+      for (int z = 0; z < 2; z++)
+        for (int y = 0; y < 2; y++)
+          for (int x = 0; x < 2; x++) {
+            int px = cx * 2 + x, py = cy * 2 + y, pz = cz * 2 + z;
+            bool unknown = activeCell(px, py, pz, fine);
+            every = every && unknown;
+            if (unknown) {
+              long a = cellAddress(px, py, pz, fine);
+              uint32_t flags = flagsOf(fine, a);
+              if (!(flags & SOLID)) {
+                R sum, diag;
+                stencil(px, py, pz, flags, fine, p, sum, diag);
+                residual += rhs[a] - (sum - diag * p[a]);
+              }
+            }
+          }
+      R r = residual * R(0.5);
+      long out = cellAddress(cx, cy, cz, level);
+      R stored = store_round(r, storeMode(level));
+      crhs[out] = stored;
+      R first = 0;
+      if (every) {
+        uint32_t flags = flagsOf(level, out);
+        if (!(flags & SOLID)) {
+          R diag = R((flags >> 0) & 1) + R((flags >> 1) & 1) + (R((flags >> 2) & 1) + R((flags >> 3) & 1)) +
+                   (R((flags >> 4) & 1) + R((flags >> 5) & 1));
+          first = mixr(R(0), (R(0) - stored) / std::max(diag, R(1e-12)), R(0.8));
+        }
+      }
+      cfirst[out] = store_round(first, storeMode(level));
+    });
+  }
+  bool coarseSolid(int px, int py, int pz, int level) {
+    long a = cellAddress(px, py, pz, level);
+    if (a < 0) return false;
+    return (topo(level)[a] & STORED_SOLID) != 0;
+  }
+  R coarseValue(const std::vector<R>& coarse, int level, int px, int py, int pz) {
+    int groundY = ground ? 0 : -0x7fffffff;
+    int c[3] = {px, std::max(py, groundY), pz};
+    if (!coarseSolid(c[0], c[1], c[2], level)) return readAt(coarse, c[0], c[1], c[2], level);
+    R sum = 0, count = 0;
+    for (int axis = 0; axis < 3; axis++)
+      for (int side = -1; side <= 1; side += 2) {
+        int q[3] = {c[0], c[1], c[2]};
+        q[axis] += side;
+        q[1] = std::max(q[1], groundY);
+        if (!coarseSolid(q[0], q[1], q[2], level)) {
+          sum += readAt(coarse, q[0], q[1], q[2], level);
+          count += 1;
+        }
+      }
+    return sum / std::max(count, R(1));
+  }
+  // prolongateCell (pressure.wgsl:726-755)
+  void prolongate(int level, const std::vector<R>& pin, const std::vector<R>& coarse, std::vector<R>& pout) {
+    int cl = level + 1;
+    forLevelCells(level, [&](int px, int py, int pz) {
+      long a = cellAddress(px, py, pz, level);
+      uint32_t flags = flagsOf(level, a);
+      if ((flags & SOLID) || !activeCell(px, py, pz, level)) {
+        pout[a] = 0;
+        return;
+      }
+      R q[3] = {(R(px) + R(0.5)) * R(0.5) - R(0.5), (R(py) + R(0.5)) * R(0.5) - R(0.5), (R(pz) + R(0.5)) * R(0.5) - R(0.5)};
+      int i[3];
+      R f[3];
+      for (int k = 0; k < 3; k++) {
+        i[k] = floori((double)q[k]);
+        f[k] = q[k] - std::floor(q[k]);
+      }
+      bool fast = colliderCount == 0 && (!ground || i[1] >= 0);
+      auto cv = [&](int dx, int dy, int dz) {
+        return fast ? readAt(coarse, i[0] + dx, i[1] + dy, i[2] + dz, cl) : coarseValue(coarse, cl, i[0] + dx, i[1] + dy, i[2] + dz);
+      };
+      R corr = mixr(mixr(mixr(cv(0, 0, 0), cv(1, 0, 0), f[0]), mixr(cv(0, 1, 0), cv(1, 1, 0), f[0]), f[1]),
+                    mixr(mixr(cv(0, 0, 1), cv(1, 0, 1), f[0]), mixr(cv(0, 1, 1), cv(1, 1, 1), f[0]), f[1]), f[2]);
+      pout[a] = store_round(pin[a] + corr, storeMode(level));
+    });
+  }
+  // The level's pressure pair and right-hand side.
+  std::vector<R>& P(int level, int k) { return level == 0 ? pres[k] : levels[level].p[k]; }
+  std::vector<R>& RHS(int level) { return level == 0 ? div : levels[level].rhs; }
+  void smooth(int level, int n, bool& initialize) {
+    Level& L = levels[level];
+    for (int i = 0; i < n; i++) {
+      bool first = level == 0 && initialize;
+      relax(level, RHS(level), P(level, L.current), P(level, 1 - L.current), first);
+      L.current = 1 - L.current;
+      if (first) initialize = false;
+    }
+  }
+  // relaxCoarse (pressure.wgsl:549-599): the bottom level, iterations in one group.
+  void bottomSolve(int iterations) {
+    int level = bottom;
+    Level& L = levels[level];
+    std::vector<R>& pin = P(level, L.current);
+    std::vector<R> value(capacity, 0), source(capacity, 0);
+    std::vector<uint32_t> flags(capacity, SOLID);
+    std::vector<bool> valid(capacity, false);
+    for (int t = 0; t < capacity; t++) {
+      valid[t] = snapshotState[t] != 0;
+      if (valid[t] && activeCell(snapshot[t][0], snapshot[t][1], snapshot[t][2], level)) {
+        long a = cellAddress(snapshot[t][0], snapshot[t][1], snapshot[t][2], level);
+        flags[t] = flagsOf(level, a);
+        source[t] = RHS(level)[a];
+        value[t] = pin[a];
+      }
+    }
+    static const int nb[6] = {neighborIndex(1, 0, 0), neighborIndex(-1, 0, 0), neighborIndex(0, 1, 0),
+                              neighborIndex(0, -1, 0), neighborIndex(0, 0, 1), neighborIndex(0, 0, -1)};
+    for (int it = 0; it < iterations; it++) {
+      std::vector<R> next(capacity, 0);
+      for (int t = 0; t < capacity; t++) {
+        if (!valid[t] || (flags[t] & SOLID)) continue;
+        R v[6];
+        for (int s = 0; s < 6; s++) {
+          v[s] = 0;
+          if (!(flags[t] & (1u << s))) continue;
+          int n = tileNeighbors[(size_t)t * 27 + nb[s]];
+          if (n >= 0) v[s] = value[n];
+        }
+        R sum = (v[0] + v[1]) + (v[2] + v[3]) + (v[4] + v[5]);
+        uint32_t fl = flags[t];
+        R diag = R((fl >> 0) & 1) + R((fl >> 1) & 1) + (R((fl >> 2) & 1) + R((fl >> 3) & 1)) +
+                 (R((fl >> 4) & 1) + R((fl >> 5) & 1));
+        R cand = (sum - source[t]) / std::max(diag, R(1e-12));
+        next[t] = store_round(mixr(value[t], cand, R(0.8)), storeMode(level));
+      }
+      value.swap(next);
+    }
+    std::vector<R>& pout = P(level, 1 - L.current);
+    for (int t = 0; t < capacity; t++)
+      if (valid[t]) {
+        long a = cellAddress(snapshot[t][0], snapshot[t][1], snapshot[t][2], level);
+        if (a >= 0) pout[a] = value[t];
+      }
+    L.current = 1 - L.current;
+  }
+  void cycle(int index, bool& initialize) {
+    if (index == bottom) {
+      if (capacity <= 256) {
+        bottomSolve(19);
+      } else {
+        smooth(index, 19, initialize);
+      }
+      return;
+    }
+    smooth(index, index > 0 ? 2 : 1, initialize);
+    Level& L = levels[index];
+    Level& C = levels[index + 1];
+    restrictLevel(index, RHS(index), P(index, L.current), RHS(index + 1), P(index + 1, 1));
+    C.current = 1;
+    cycle(index + 1, initialize);
+    prolongate(index, P(index, L.current), P(index + 1, C.current), P(index, 1 - L.current));
+    L.current = 1 - L.current;
+    smooth(index, 3, initialize);
+  }
+  // PressureSolver.solve (PressureSolver.ts:371-402) with PRESSURE_CYCLES = 1.
+  void solvePressure() {
+    buildZeroedTopology();
+    buildTopology();
+    levels[0].current = latest;
+    bool initialize = true;
+    cycle(0, initialize);
+    latest = levels[0].current;
+  }
+
+  // ---------------------------------------------------------------- projection
+  bool pressureUnknown(int px, int py, int pz) {
+    int p[3] = {px, py, pz}, lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+      lo[a] = (p[a] - 1) >> shift;
+      hi[a] = p[a] >> shift;
+    }
+    if (ground) lo[1] = std::max(lo[1], 0);
+    for (int z = lo[2]; z <= hi[2]; z++)
+      for (int y = lo[1]; y <= hi[1]; y++)
+        for (int x = lo[0]; x <= hi[0]; x++)
+          if (brickEntry(x, y, z) < 0) return false;
+    return true;
+  }
+  R cellPressure(int x, int y, int z) {
+    int s = brickSlot(x >> shift, y >> shift, z >> shift);
+    if (s < 0) return 0;
+    return pres[latest][(size_t)s * N + local(x, y, z)];
+  }
+  // project (fluid-forces.wgsl:205-262) into the velocity pool of the next step.
+  void projectStep() {
+    std::vector<R> out(vel.size(), 0);
+    forActiveCells([&](uint32_t, int slot, int c, int x, int y, int z) {
+      V3<R> pos = center(x, y, z);
+      R res[3] = {0, 0, 0};
+      if (!solidAt(pos[0], pos[1], pos[2])) {
+        R cp = pres[latest][(size_t)slot * N + c];
+        bool pu = pressureUnknown(x, y, z);
+        for (int a = 0; a < 3; a++) {
+          int n[3] = {x, y, z};
+          n[a] += 1;
+          R v = velF[((size_t)slot * 3 + a) * N + c];
+          V3<R> nc = center(n[0], n[1], n[2]);
+          if (solidAt(nc[0], nc[1], nc[2])) {
+            res[a] = 0;
+          } else if (!pu && !pressureUnknown(n[0], n[1], n[2])) {
+            res[a] = 0;
+          } else {
+            res[a] = v - (cellPressure(n[0], n[1], n[2]) - cp) / h;
+          }
+        }
+      }
+      for (int a = 0; a < 3; a++) out[((size_t)slot * 3 + a) * N + c] = sv(res[a]);
+    });
+    vel.swap(out);
+  }
+
+  // ---------------------------------------------------------------- measurement
+  // readActivity (FluidSimulation.ts:1701-1746), applied before the next step.
+  void readActivity() {
+    contentTiles.clear();
+    for (int s = 0; s < capacity; s++) {
+      uint32_t f = activity[(size_t)capacity * 64 + s];
+      if (f && snapshotState[s] != 0) contentTiles.push_back({snapshot[s], f});
+    }
+    activeBrickCount = (uint32_t)active.size();
+    usedSlots = slots - (uint32_t)freeCount;
+    uint32_t limit = slotLimit();
+    lastFailures = failures;
+    poolLimited = failures > 0 && slots >= limit;
+    failures = 0;
+  }
+};
+
+}  // namespace orc
+
+// =========================================================================================
+// C API for ctypes (tests and the CPU baseline).
+// =========================================================================================
+struct or_sim {
+  int real;  // 0 double, 1 float
+  orc::Sim<double>* d = nullptr;
+  orc::Sim<float>* f = nullptr;
+  std::string error;
+};
+
+template <class S, class Fn>
+static auto with(or_sim* s, Fn fn) {
+  if (s->d) return fn(*s->d);
+  return fn(*s->f);
+}
+
+extern "C" {
+
+// mode: 0 storage as the grid's precision says (FP32 -> exact in the real type);
+//       2 the reference's half-precision storage with its truncations.
+or_sim* or_create(const fp_grid* g, int real, int mode) {
+  orc::Prec p;
+  if (mode == 2) {
+    p.vel = p.scal = p.expn = p.p0 = p.pc = p.curl = p.bounds = orc::STORE_F16;
+    p.truncate = true;
+  } else if (g->precision == FP_PRECISION_MIXED) {
+    p.scal = orc::STORE_F16;
+    p.pc = orc::STORE_BF16;
+  }
+  if (g->brick_size != 8 && g->brick_size != 16) return nullptr;
+  or_sim* s = new or_sim();
+  s->real = real;
+  if (real == 0)
+    s->d = new orc::Sim<double>(*g, p);
+  else
+    s->f = new orc::Sim<float>(*g, p);
+  return s;
+}
+void or_destroy(or_sim* s) {
+  if (!s) return;
+  delete s->d;
+  delete s->f;
+  delete s;
+}
+void or_set_threads(int n) {
+#ifdef _OPENMP
+  omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+void or_set_runtime(or_sim* s, float cutoff, double budget, int ground) {
+  auto fn = [&](auto& sim) {
+    sim.cutoff = cutoff;
+    if (budget > 0) sim.voxelBudget = budget;
+    sim.ground = ground != 0;
+    return 0;
+  };
+  if (s->d) fn(*s->d); else fn(*s->f);
+}
+int or_step(or_sim* s, const fp_frame* f, float dt) {
+  std::string e = s->d ? s->d->step(*f, dt) : s->f->step(*f, dt);
+  s->error = e;
+  return e.empty() ? 0 : -1;
+}
+const char* or_error(or_sim* s) { return s->error.c_str(); }
+
+// Sizes: 0 slots, 1 capacity (tile slots), 2 cells per brick, 3 active bricks, 4 steps,
+// 5 used slots, 6 pool limited, 7 failures at the last measurement, 8 tiles.
+int64_t or_info(or_sim* s, int what) {
+  auto fn = [&](auto& sim) -> int64_t {
+    switch (what) {
+      case 0: return sim.slots;
+      case 1: return sim.capacity;
+      case 2: return sim.N;
+      case 3: return sim.activeBrickCount;
+      case 4: return sim.steps;
+      case 5: return sim.usedSlots;
+      case 6: return sim.poolLimited;
+      case 7: return sim.lastFailures;
+      case 8: return sim.dir.count();
+    }
+    return -1;
+  };
+  return s->d ? fn(*s->d) : fn(*s->f);
+}
+
+// Field copy out/in as float, layout [slot][channel][cell] (FP_FIELD_*). `write` copies in.
+static int field_io(or_sim* s, int field, float* buf, size_t count, int write) {
+  auto fn = [&](auto& sim) -> int {
+    using R = typename std::remove_reference<decltype(sim.h)>::type;
+    std::vector<R>* v = nullptr;
+    switch (field) {
+      case FP_FIELD_VELOCITY: v = &sim.vel; break;
+      case FP_FIELD_SCALARS: v = &sim.fld; break;
+      case FP_FIELD_EXPANSION: v = &sim.expn; break;
+      case FP_FIELD_PRESSURE: v = &sim.pres[sim.latest]; break;
+      case FP_FIELD_DIVERGENCE: v = &sim.div; break;
+      case FP_FIELD_CURL: v = &sim.curl; break;
+      default: return -1;
+    }
+    if (count != v->size()) return -2;
+    if (write)
+      for (size_t i = 0; i < count; i++) (*v)[i] = (R)buf[i];
+    else
+      for (size_t i = 0; i < count; i++) buf[i] = (float)(*v)[i];
+    return 0;
+  };
+  return s->d ? fn(*s->d) : fn(*s->f);
+}
+int or_read_field(or_sim* s, int field, float* out, size_t count) { return field_io(s, field, out, count, 0); }
+int or_write_field(or_sim* s, int field, const float* in, size_t count) {
+  return field_io(s, field, const_cast<float*>(in), count, 1);
+}
+// Double-precision copy out, for the error oracle's comparisons.
+int or_read_field64(or_sim* s, int field, double* out, size_t count) {
+  if (!s->d) return -1;
+  auto& sim = *s->d;
+  std::vector<double>* v = nullptr;
+  switch (field) {
+    case FP_FIELD_VELOCITY: v = &sim.vel; break;
+    case FP_FIELD_SCALARS: v = &sim.fld; break;
+    case FP_FIELD_EXPANSION: v = &sim.expn; break;
+    case FP_FIELD_PRESSURE: v = &sim.pres[sim.latest]; break;
+    case FP_FIELD_DIVERGENCE: v = &sim.div; break;
+    case FP_FIELD_CURL: v = &sim.curl; break;
+    default: return -1;
+  }
+  if (count != v->size()) return -2;
+  std::memcpy(out, v->data(), count * 8);
+  return 0;
+}
+
+// Integer tables (FP_TABLE_*); returns the words written or needed.
+int64_t or_read_table(or_sim* s, int table, void* out, size_t capacityBytes) {
+  auto fn = [&](auto& sim) -> int64_t {
+    std::vector<uint32_t> w;
+    size_t bricks = (size_t)sim.capacity * 64;
+    switch (table) {
+      case FP_TABLE_ENTRIES: w.assign(sim.entries.begin(), sim.entries.end()); break;
+      case FP_TABLE_PAGES: w.assign(sim.pages.begin(), sim.pages.end()); break;
+      case FP_TABLE_STATE: w = sim.state; break;
+      case FP_TABLE_ACTIVITY: w = sim.activity; break;
+      case FP_TABLE_RECORDS: w.assign(sim.records.begin(), sim.records.end()); break;
+      case FP_TABLE_FREE:
+        w.push_back((uint32_t)sim.freeCount);
+        w.push_back(sim.lastFailures);
+        w.insert(w.end(), sim.freeStack.begin(), sim.freeStack.end());
+        break;
+      case FP_TABLE_ACTIVE:
+        w.push_back((uint32_t)sim.active.size());
+        w.insert(w.end(), sim.active.begin(), sim.active.end());
+        break;
+      case FP_TABLE_SOLIDS: w = sim.solids; break;
+      case FP_TABLE_TILES:
+        for (int t = 0; t < sim.capacity; t++) {
+          w.push_back((uint32_t)sim.snapshot[t][0]);
+          w.push_back((uint32_t)sim.snapshot[t][1]);
+          w.push_back((uint32_t)sim.snapshot[t][2]);
+          w.push_back((uint32_t)sim.snapshotState[t]);
+        }
+        break;
+      default: return -1;
+    }
+    (void)bricks;
+    size_t bytes = w.size() * 4;
+    if (out && capacityBytes >= bytes) std::memcpy(out, w.data(), bytes);
+    return (int64_t)w.size();
+  };
+  return s->d ? fn(*s->d) : fn(*s->f);
+}
+// Overwrite the activity flags (teacher forcing of the content measurement).
+int or_write_activity(or_sim* s, const uint32_t* in, size_t count) {
+  auto fn = [&](auto& sim) -> int {
+    if (count != sim.activity.size()) return -2;
+    std::memcpy(sim.activity.data(), in, count * 4);
+    sim.contentTiles.clear();
+    for (int t = 0; t < sim.capacity; t++) {
+      uint32_t f = sim.activity[(size_t)sim.capacity * 64 + t];
+      if (f && sim.snapshotState[t] != 0) sim.contentTiles.push_back({sim.snapshot[t], f});
+    }
+    return 0;
+  };
+  return s->d ? fn(*s->d) : fn(*s->f);
+}
+
+}  // extern "C"

@@ -1,0 +1,132 @@
+"""TEST INFRASTRUCTURE — ctypes wrapper of the CPU oracle (oracle/_ref/libfp_oracle.so).
+
+Only tests/, bench.py's `cpu_baseline` leg and __graft_entry__.smoke() may use this. The
+oracle restates the reference's step on the CPU: real=0 is the FP64 error oracle, real=1
+the FP32 CPU baseline. Parity unpinned: the reference has no tests or runnable CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_ref" / "libfp_oracle.so"
+
+
+def build() -> Path:
+    subprocess.run(["make", "-C", str(HERE)], check=True, stdout=subprocess.DEVNULL)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        L.or_create.restype = C.c_void_p
+        L.or_create.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.or_destroy.argtypes = [C.c_void_p]
+        L.or_set_threads.argtypes = [C.c_int]
+        L.or_set_runtime.argtypes = [C.c_void_p, C.c_float, C.c_double, C.c_int]
+        L.or_step.restype = C.c_int
+        L.or_step.argtypes = [C.c_void_p, C.c_void_p, C.c_float]
+        L.or_error.restype = C.c_char_p
+        L.or_error.argtypes = [C.c_void_p]
+        L.or_info.restype = C.c_int64
+        L.or_info.argtypes = [C.c_void_p, C.c_int]
+        L.or_read_field.restype = C.c_int
+        L.or_read_field.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+        L.or_write_field.restype = C.c_int
+        L.or_write_field.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+        L.or_read_field64.restype = C.c_int
+        L.or_read_field64.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+        L.or_read_table.restype = C.c_int64
+        L.or_read_table.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+        L.or_write_activity.restype = C.c_int
+        L.or_write_activity.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+        _lib = L
+    return _lib
+
+
+CHANNELS = {0: 3, 1: 4, 2: 1, 3: 1, 4: 1, 5: 4}
+
+
+class OracleSim:
+    """One oracle simulation. `real`: 0 FP64, 1 FP32. `mode`: 0 the grid's precision,
+    2 the reference's half-precision storage."""
+
+    def __init__(self, grid, real: int = 0, mode: int = 0):
+        self.L = lib()
+        self.h = self.L.or_create(C.byref(grid), real, mode)
+        if not self.h:
+            raise ValueError("oracle rejected the grid")
+        self.real = real
+
+    def close(self):
+        if self.h:
+            self.L.or_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_runtime(self, cutoff: float, budget: float, ground: bool):
+        self.L.or_set_runtime(self.h, cutoff, budget, int(ground))
+
+    def step(self, frame, dt: float = 1.0 / 60.0):
+        if self.L.or_step(self.h, C.byref(frame), dt) != 0:
+            raise ValueError(self.L.or_error(self.h).decode())
+
+    def info(self, what: int) -> int:
+        return int(self.L.or_info(self.h, what))
+
+    @property
+    def slots(self):
+        return self.info(0)
+
+    @property
+    def capacity(self):
+        return self.info(1)
+
+    @property
+    def cells(self):
+        return self.info(2)
+
+    @property
+    def active_bricks(self):
+        return self.info(3)
+
+    def field(self, fid: int, f64: bool = False) -> np.ndarray:
+        n = self.slots * CHANNELS[fid] * self.cells
+        if f64:
+            out = np.empty(n, np.float64)
+            assert self.L.or_read_field64(self.h, fid, out.ctypes.data, n) == 0
+        else:
+            out = np.empty(n, np.float32)
+            assert self.L.or_read_field(self.h, fid, out.ctypes.data, n) == 0
+        return out.reshape(self.slots, CHANNELS[fid], self.cells)
+
+    def write_field(self, fid: int, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, np.float32).ravel()
+        assert self.L.or_write_field(self.h, fid, a.ctypes.data, a.size) == 0
+
+    def table(self, tid: int) -> np.ndarray:
+        n = self.L.or_read_table(self.h, tid, None, 0)
+        out = np.empty(max(n, 1), np.uint32)
+        self.L.or_read_table(self.h, tid, out.ctypes.data, out.nbytes)
+        return out[:n]
+
+    def write_activity(self, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, np.uint32)
+        assert self.L.or_write_activity(self.h, a.ctypes.data, a.size) == 0
+
+
+def set_threads(n: int):
+    lib().or_set_threads(n)

@@ -1,0 +1,111 @@
+"""Lockstep parity harness: the CUDA step against the FP64 oracle from identical state.
+
+Each step both run the same frame from the same state. Integer tables must match bit for
+bit; each field must match within the relative-L2 tolerance. The CUDA fields and activity
+flags are then copied into the oracle (teacher forcing), so per-step differences never
+compound through the flow's chaos.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from firepro import abi
+from oracle.fp_oracle import OracleSim
+
+# north_star tolerance: relative L2 <= 1e-3 against the FP64 oracle per field per step.
+REL_L2_TOL = 1e-3
+
+CHECK_FIELDS = {
+    "velocity": abi.FP_FIELD_VELOCITY,
+    "scalars": abi.FP_FIELD_SCALARS,
+    "expansion": abi.FP_FIELD_EXPANSION,
+    "pressure": abi.FP_FIELD_PRESSURE,
+    "divergence": abi.FP_FIELD_DIVERGENCE,
+}
+
+
+def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
+    num = float(np.linalg.norm((a.astype(np.float64) - b).ravel()))
+    den = float(np.linalg.norm(b.ravel()))
+    if den == 0.0:
+        return 0.0 if num == 0.0 else float("inf")
+    return num / den
+
+
+def active_slots(entries: np.ndarray) -> np.ndarray:
+    e = entries.view(np.int32)
+    return np.unique(e[e >= 0] & 0xFFFFFF)
+
+
+def compare_tables(gpu, orc) -> dict:
+    """Bit-exact comparison of the allocation's integer tables. Returns mismatch counts."""
+    out = {}
+    for name, tid in (("entries", abi.FP_TABLE_ENTRIES), ("pages", abi.FP_TABLE_PAGES),
+                      ("state", abi.FP_TABLE_STATE), ("active", abi.FP_TABLE_ACTIVE),
+                      ("free", abi.FP_TABLE_FREE), ("tiles", abi.FP_TABLE_TILES)):
+        a, b = gpu.table(tid), orc.table(tid)
+        if name == "state":
+            a, b = a & 1, b & 1  # the persistent bit; the rank bits are scratch
+        out[name] = int(np.count_nonzero(a != b)) if a.shape == b.shape else -1
+    ea = gpu.table(abi.FP_TABLE_ENTRIES).view(np.int32)
+    ra = gpu.table(abi.FP_TABLE_RECORDS).reshape(-1, 28)
+    rb = orc.table(abi.FP_TABLE_RECORDS).reshape(-1, 28)
+    live = ea >= 0
+    out["records"] = int(np.count_nonzero(ra[live] != rb[live])) if ra.shape == rb.shape else -1
+    act_a = gpu.table(abi.FP_TABLE_ACTIVITY)
+    act_b = orc.table(abi.FP_TABLE_ACTIVITY)
+    out["activity"] = int(np.count_nonzero(act_a != act_b)) if act_a.shape == act_b.shape else -1
+    if gpu.table(abi.FP_TABLE_SOLIDS).shape == orc.table(abi.FP_TABLE_SOLIDS).shape:
+        slots = active_slots(ea)
+        sa = gpu.table(abi.FP_TABLE_SOLIDS).reshape(gpu_slots(gpu), -1)[slots]
+        sb = orc.table(abi.FP_TABLE_SOLIDS).reshape(orc.slots, -1)[slots]
+        out["solids"] = int(np.count_nonzero(sa != sb))
+    return out
+
+
+def gpu_slots(gpu) -> int:
+    return int(gpu.stats().pool_slots)
+
+
+def compare_fields(gpu, orc, slots: np.ndarray) -> dict:
+    out = {}
+    for name, fid in CHECK_FIELDS.items():
+        a = gpu.field(fid)[slots]
+        b = orc.field(fid, f64=orc.real == 0)[slots]
+        if fid == abi.FP_FIELD_SCALARS:
+            for k, ch in enumerate(("smoke", "heat", "lifetime", "fuel")):
+                out[ch] = rel_l2(a[:, k], b[:, k])
+        else:
+            out[name] = rel_l2(a, b)
+    return out
+
+
+def force(gpu, orc):
+    """Copy the CUDA state that carries into the next step into the oracle."""
+    for fid in (abi.FP_FIELD_VELOCITY, abi.FP_FIELD_SCALARS, abi.FP_FIELD_EXPANSION):
+        orc.write_field(fid, gpu.field(fid))
+    orc.write_activity(gpu.table(abi.FP_TABLE_ACTIVITY))
+
+
+def lockstep(scene, steps: int, gpu_factory, cutoff=0.05, budget=8e6, ground=True, start=0, log=None):
+    """Run `steps` steps in lockstep; returns per-step (tables, fields) reports."""
+    grid = scene.grid(budget=budget)
+    gpu = gpu_factory(grid)
+    orc = OracleSim(grid, real=0)
+    gpu.set_runtime(cutoff, budget, ground)
+    orc.set_runtime(cutoff, budget, ground)
+    reports = []
+    for s in range(start, start + steps):
+        fd = scene.frame(s)
+        gpu.step(fd.frame)
+        orc.step(fd.frame)
+        tables = compare_tables(gpu, orc)
+        slots = active_slots(gpu.table(abi.FP_TABLE_ENTRIES))
+        fields = compare_fields(gpu, orc, slots)
+        reports.append((s, tables, fields, len(slots)))
+        if log:
+            log(s, tables, fields, len(slots))
+        force(gpu, orc)
+    gpu.dispose()
+    orc.close()
+    return reports

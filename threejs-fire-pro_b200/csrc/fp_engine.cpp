@@ -1,0 +1,959 @@
+// Host engine: see fp_engine.hpp. Citations are path:line in the reference project.
+#include "fp_engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "fp_launch.h"
+
+namespace fp {
+
+static const int TILE_BRICKS = 4;
+static const int LINGER_STEPS = 60;  // TileDirectory.ts:8
+static const int MIN_TILES = 16;     // FluidSimulation.ts:72
+static const int HASH_ROW = 256;     // TileDirectory.ts:17
+
+// ------------------------------------------------------------------------ TileDirectory
+void TileDirectory::need(int lx, int ly, int lz, int hx, int hy, int hz, int64_t step) {
+  for (int z = lz; z <= hz; z++)
+    for (int y = ground ? std::max(0, ly) : ly; y <= hy; y++)
+      for (int x = lx; x <= hx; x++) {
+        auto it = index_.find(key(x, y, z));
+        if (it != index_.end()) {
+          Tile& t = slots_[it->second];
+          t.needed = step;
+          if (t.closing) {
+            t.closing = false;
+            dirty = true;
+          }
+          continue;
+        }
+        int slot = -1;
+        for (size_t i = 0; i < slots_.size(); i++)
+          if (!slots_[i].alive) {
+            slot = (int)i;
+            break;
+          }
+        if (slot < 0) {
+          slot = (int)slots_.size();
+          slots_.push_back(Tile{});
+        }
+        slots_[slot] = Tile{x, y, z, step, false, true};
+        index_[key(x, y, z)] = slot;
+        created_.push_back(slot);
+        dirty = true;
+      }
+}
+void TileDirectory::retire(int64_t step) {
+  for (size_t s = 0; s < slots_.size(); s++) {
+    Tile& t = slots_[s];
+    if (!t.alive) continue;
+    if (t.closing) {
+      index_.erase(key(t.x, t.y, t.z));
+      t.alive = false;
+      dirty = true;
+    } else if (step - t.needed > LINGER_STEPS) {
+      t.closing = true;
+      dirty = true;
+    }
+  }
+  while (!slots_.empty() && !slots_.back().alive) slots_.pop_back();
+}
+void TileDirectory::clear() {
+  slots_.clear();
+  index_.clear();
+  created_.clear();
+  dirty = true;
+}
+int TileDirectory::slotAt(int x, int y, int z) const {
+  auto it = index_.find(key(x, y, z));
+  return it == index_.end() ? -1 : it->second;
+}
+std::vector<int> TileDirectory::takeCreated() {
+  std::vector<int> out;
+  for (int s : created_)
+    if (s < (int)slots_.size() && slots_[s].alive) out.push_back(s);
+  created_.clear();
+  return out;
+}
+
+// ------------------------------------------------------------------------ Engine
+int Engine::check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return FP_OK;
+  error_ = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? FP_ENOMEM : FP_EDEVICE;
+}
+
+bool Engine::alloc(DeviceBuffer& b, size_t bytes, bool zero) {
+  if (b.ptr) cudaFree(b.ptr);
+  b.ptr = nullptr;
+  b.bytes = 0;
+  if (bytes == 0) bytes = 16;
+  if (cudaMalloc(&b.ptr, bytes) != cudaSuccess) {
+    b.ptr = nullptr;
+    error_ = "device memory exhausted";
+    return false;
+  }
+  b.bytes = bytes;
+  if (zero) cudaMemsetAsync(b.ptr, 0, bytes, stream_);
+  return true;
+}
+
+bool Engine::grow(DeviceBuffer& b, size_t bytes, int fill) {
+  if (bytes <= b.bytes && b.ptr) return true;
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    error_ = "device memory exhausted";
+    return false;
+  }
+  cudaMemsetAsync(p, fill, bytes, stream_);
+  if (b.ptr) {
+    cudaMemcpyAsync(p, b.ptr, b.bytes, cudaMemcpyDeviceToDevice, stream_);
+    cudaStreamSynchronize(stream_);
+    cudaFree(b.ptr);
+  }
+  b.ptr = p;
+  b.bytes = bytes;
+  return true;
+}
+
+bool Engine::upload(DeviceBuffer& b, const void* src, size_t bytes) {
+  if (bytes == 0) return true;
+  if (bytes > b.bytes) {
+    cudaStreamSynchronize(stream_);
+    if (!alloc(b, std::max(bytes + bytes / 2, (size_t)256), false)) return false;
+  }
+  // Synchronous from pageable memory: the source vectors change next step.
+  return cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, stream_) == cudaSuccess;
+}
+
+uint32_t Engine::slotLimit() const {
+  double v = std::floor(budget_ / (double)N_);
+  return (uint32_t)std::max(1.0, v);
+}
+
+Engine::Engine(const fp_grid& g, int device) : device_(device) {
+  B_ = g.brick_size;
+  shift_ = B_ == 8 ? 3 : 4;
+  N_ = B_ * B_ * B_;
+  W_ = N_ / 32;
+  brickLevels_ = shift_;
+  bottom_ = brickLevels_ + 2;
+  h_ = g.voxel_size;
+  maccormack_ = g.scalar_maccormack != 0;
+  precision_ = g.precision;
+  budget_ = g.voxel_budget > 0 ? g.voxel_budget : 8e6;
+}
+
+Engine::~Engine() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  freeAll();
+  if (paramsH_) cudaFreeHost(paramsH_);
+  if (readH_) cudaFreeHost(readH_);
+  if (readEvent_) cudaEventDestroy(readEvent_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::freeAll() {
+  DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_, &zeroList_,
+                         &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_, &donors_, &solids_,
+                         &tileRecD_, &tileNbrD_, &hashD_, &emittersD_, &collidersD_, &masksD_, &forcesD_,
+                         &regionsD_, &tileListsD_, &noise_, &paramsD_};
+  for (DeviceBuffer* b : all)
+    if (b->ptr) {
+      cudaFree(b->ptr);
+      b->ptr = nullptr;
+      b->bytes = 0;
+    }
+  for (auto& b : vel_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
+  for (auto& b : fld_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
+  for (auto& b : p0_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
+  for (int l = 0; l < FP_MAX_LEVELS; l++) {
+    if (topo_[l].ptr) { cudaFree(topo_[l].ptr); topo_[l] = DeviceBuffer{}; }
+    if (lrhs_[l].ptr) { cudaFree(lrhs_[l].ptr); lrhs_[l] = DeviceBuffer{}; }
+    for (auto& b : lp_[l]) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
+  }
+}
+
+// FluidSimulation.ts:496-549 allocate(): empty pools of the whole voxel budget, no tiles.
+int Engine::initialize() {
+  int rc;
+  if ((rc = check(cudaSetDevice(device_), "cudaSetDevice"))) return rc;
+  if (!stream_) {
+    if ((rc = check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
+    cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_);
+    if ((rc = check(cudaMallocHost(&paramsH_, sizeof(SimParams)), "cudaMallocHost"))) return rc;
+    if ((rc = check(cudaEventCreateWithFlags(&readEvent_, cudaEventDisableTiming), "cudaEventCreate"))) return rc;
+  }
+  freeAll();
+  if (!alloc(paramsD_, sizeof(SimParams)) || !alloc(counters_, sizeof(FpCounters)) ||
+      !alloc(noise_, 64 * 64 * 64 * sizeof(float4)))
+    return FP_ENOMEM;
+  fp_launch_noise((float4*)noise_.ptr, stream_);
+  slots_ = 0;
+  capacity_ = 0;
+  if ((rc = allocatePools(slotLimit()))) return rc;
+  dir_.clear();
+  dir_.ground = ground_;
+  contentTiles_.clear();
+  if ((rc = setCapacity(MIN_TILES))) return rc;
+  if ((rc = applyTiles())) return rc;
+  solidsStale_ = true;
+  geometryDirty_ = true;
+  mayHaveFlame_ = false;
+  time_ = 0;
+  steps_ = 0;
+  latest_ = 0;
+  activeBricks_ = usedSlots_ = lastFailures_ = 0;
+  poolLimited_ = false;
+  pendingRead_ = false;
+  colliderCount_ = 0;
+  prevColliders_.clear();
+  prevMasks_.clear();
+  for (int k = 0; k < 4; k++) velIdx_[k] = k;
+  for (int k = 0; k < 3; k++) fldIdx_[k] = k;
+  return check(cudaStreamSynchronize(stream_), "initialize");
+}
+
+// Pools of `slots` slots, all free: the stack pops slot 0 first.
+int Engine::allocatePools(uint32_t slots) {
+  size_t s = slots, N = N_;
+  bool ok = true;
+  for (auto& b : vel_) ok = ok && alloc(b, s * 3 * N * 4);
+  for (auto& b : fld_) ok = ok && alloc(b, s * 4 * N * 4);
+  ok = ok && alloc(curl_, s * 4 * N * 4) && alloc(expn_, s * N * 4) && alloc(div_, s * N * 4) &&
+       alloc(vmin_, s * 3 * N * 4) && alloc(vmax_, s * 3 * N * 4) && alloc(sb_, s * 8 * N * 4) &&
+       alloc(donors_, s * 3 * N * 2) && alloc(solids_, s * W_ * 4) && alloc(p0_[0], s * N * 4) &&
+       alloc(p0_[1], s * N * 4) && alloc(topo_[0], s * N) && alloc(freeStack_, s * 4);
+  for (int l = 1; l < brickLevels_ && ok; l++) {
+    size_t c = s * levelCells(l);
+    ok = alloc(lp_[l][0], c * 4) && alloc(lp_[l][1], c * 4) && alloc(lrhs_[l], c * 4) && alloc(topo_[l], c);
+  }
+  if (!ok) return FP_ENOMEM;
+  std::vector<uint32_t> stack(slots);
+  for (uint32_t i = 0; i < slots; i++) stack[i] = slots - 1 - i;
+  cudaMemcpy(freeStack_.ptr, stack.data(), s * 4, cudaMemcpyHostToDevice);
+  FpCounters c{};
+  c.freeCount = (int32_t)slots;
+  cudaMemcpy(counters_.ptr, &c, sizeof(c), cudaMemcpyHostToDevice);
+  slots_ = slots;
+  return FP_OK;
+}
+
+// After the budget rose: new slots go under the free stack (fluid-pool-growth.wgsl:12-21),
+// live pools keep their contents.
+int Engine::growPool(uint32_t target) {
+  if (target <= slots_) return FP_OK;
+  cudaStreamSynchronize(stream_);
+  size_t s = target, N = N_;
+  uint32_t added = target - slots_;
+  bool ok = true;
+  for (auto& b : vel_) ok = ok && grow(b, s * 3 * N * 4, 0);
+  for (auto& b : fld_) ok = ok && grow(b, s * 4 * N * 4, 0);
+  ok = ok && grow(curl_, s * 4 * N * 4, 0) && grow(expn_, s * N * 4, 0) && grow(div_, s * N * 4, 0) &&
+       grow(vmin_, s * 3 * N * 4, 0) && grow(vmax_, s * 3 * N * 4, 0) && grow(sb_, s * 8 * N * 4, 0) &&
+       grow(donors_, s * 3 * N * 2, 0) && grow(solids_, s * W_ * 4, 0) && grow(p0_[0], s * N * 4, 0) &&
+       grow(p0_[1], s * N * 4, 0) && grow(topo_[0], s * N, 0);
+  for (int l = 1; l < brickLevels_ && ok; l++) {
+    size_t c = s * levelCells(l);
+    ok = grow(lp_[l][0], c * 4, 0) && grow(lp_[l][1], c * 4, 0) && grow(lrhs_[l], c * 4, 0) && grow(topo_[l], c, 0);
+  }
+  if (!ok) return FP_ENOMEM;
+  std::vector<uint32_t> old(slots_);
+  cudaMemcpy(old.data(), freeStack_.ptr, (size_t)slots_ * 4, cudaMemcpyDeviceToHost);
+  std::vector<uint32_t> next(target);
+  for (uint32_t i = 0; i < added; i++) next[i] = slots_ + added - 1 - i;
+  for (uint32_t i = 0; i < slots_; i++) next[added + i] = old[i];
+  if (!alloc(freeStack_, s * 4, false)) return FP_ENOMEM;
+  cudaMemcpy(freeStack_.ptr, next.data(), s * 4, cudaMemcpyHostToDevice);
+  FpCounters c;
+  cudaMemcpy(&c, counters_.ptr, sizeof(c), cudaMemcpyDeviceToHost);
+  c.freeCount += (int32_t)added;
+  cudaMemcpy(counters_.ptr, &c, sizeof(c), cudaMemcpyHostToDevice);
+  slots_ = target;
+  geometryDirty_ = true;
+  return FP_OK;
+}
+
+// Per-brick and per-tile storage for `capacity` tile slots, keeping every brick's page,
+// state, flags, entry and record (FluidSimulation.ts:633-646).
+int Engine::setCapacity(int capacity) {
+  size_t bricks = (size_t)capacity * 64;
+  size_t oldBricks = (size_t)capacity_ * 64;
+  bool ok = grow(pages_, bricks * 4, 0xff) && grow(entries_, bricks * 4, 0xff) && grow(state_, bricks * 4, 0) &&
+            grow(records_, bricks * FP_RECORD_WORDS * 4, 0xff) && alloc(active_, bricks * 4) &&
+            alloc(zeroList_, bricks * 8) && alloc(blockCounts_, (bricks / 256 + 1) * 16);
+  if (!ok) return FP_ENOMEM;
+  // activity: bricks, then a word per tile slot.
+  {
+    DeviceBuffer next;
+    if (!alloc(next, (bricks + capacity) * 4)) return FP_ENOMEM;
+    if (activity_.ptr) {
+      cudaMemcpyAsync(next.ptr, activity_.ptr, oldBricks * 4, cudaMemcpyDeviceToDevice, stream_);
+      cudaStreamSynchronize(stream_);
+      cudaFree(activity_.ptr);
+    }
+    activity_ = next;
+  }
+  for (int l = brickLevels_; l <= bottom_; l++) {
+    size_t c = (size_t)capacity * levelCells(l);
+    ok = ok && grow(lp_[l][0], c * 4, 0) && grow(lp_[l][1], c * 4, 0) && grow(lrhs_[l], c * 4, 0) &&
+         grow(topo_[l], c, 0);
+  }
+  if (!ok) return FP_ENOMEM;
+  capacity_ = capacity;
+  return FP_OK;
+}
+
+// applyTiles (FluidSimulation.ts:629-678) with TileDirectory.tables (TileDirectory.ts:151-186).
+int Engine::applyTiles() {
+  int needed = std::max(MIN_TILES, dir_.slotsUsed());
+  if (needed > capacity_) {
+    int cap = capacity_;
+    while (cap < needed) cap *= 2;
+    int rc = setCapacity(cap);
+    if (rc) return rc;
+  }
+  tileRec_.assign(capacity_, make_int4(0, 0, 0, 0));
+  tileNbr_.assign((size_t)capacity_ * 27, -1);
+  int size = HASH_ROW;
+  while (size < dir_.count() * 2) size *= 2;
+  hash_.assign(size, make_int4(-1, -1, -1, -1));
+  const auto& slots = dir_.slots();
+  for (size_t s = 0; s < slots.size(); s++) {
+    const TileDirectory::Tile& t = slots[s];
+    if (!t.alive) continue;
+    tileRec_[s] = make_int4(t.x, t.y, t.z, t.closing ? 2 : 1);
+    uint32_t hsh = (((uint32_t)t.x * 73856093u) ^ ((uint32_t)t.y * 19349663u) ^ ((uint32_t)t.z * 83492791u)) & (size - 1);
+    while (hash_[hsh].w >= 0) hsh = (hsh + 1) & (size - 1);
+    hash_[hsh] = make_int4(t.x, t.y, t.z, (int)s);
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++)
+          tileNbr_[s * 27 + (dz + 1) * 9 + (dy + 1) * 3 + dx + 1] = dir_.slotAt(t.x + dx, t.y + dy, t.z + dz);
+  }
+  if (!upload(tileRecD_, tileRec_.data(), tileRec_.size() * sizeof(int4)) ||
+      !upload(tileNbrD_, tileNbr_.data(), tileNbr_.size() * 4) || !upload(hashD_, hash_.data(), hash_.size() * sizeof(int4)))
+    return FP_ENOMEM;
+  // New tiles' bricks start without slots.
+  for (int slot : dir_.takeCreated()) {
+    size_t off = (size_t)slot * 64 * 4;
+    cudaMemsetAsync((char*)pages_.ptr + off, 0xff, 64 * 4, stream_);
+    cudaMemsetAsync((char*)entries_.ptr + off, 0xff, 64 * 4, stream_);
+    cudaMemsetAsync((char*)state_.ptr + off, 0, 64 * 4, stream_);
+    cudaMemsetAsync((char*)activity_.ptr + off, 0, 64 * 4, stream_);
+  }
+  dir_.dirty = false;
+  geometryDirty_ = true;  // PressureSolver.setBricks -> resetPlans
+  cudaStreamSynchronize(stream_);  // the host tables are reused next step
+  return FP_OK;
+}
+
+// updateTiles (FluidSimulation.ts:873-912).
+void Engine::updateTiles(const fp_frame& f) {
+  dir_.retire(steps_);
+  float brick = (float)B_ * h_, tile = (float)(TILE_BRICKS * B_) * h_;
+  float margin = 2.f * brick + tile;
+  for (uint32_t i = 0; i < f.source_count; i++) {
+    const fp_source& s = f.sources[i];
+    if (s.shape == FP_SHAPE_MESH) continue;
+    float ext = std::max(std::max(std::max(s.size[0], s.size[1]), s.size[2]), 0.03f) + s.outward_speed * 0.25f;
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+      lo[a] = (int)std::floor((s.position[a] - ext - margin) / tile);
+      hi[a] = (int)std::floor((s.position[a] + ext + margin) / tile);
+    }
+    dir_.need(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], steps_);
+  }
+  for (auto& ct : contentTiles_)
+    dir_.need(ct.first.x - 1, ct.first.y - 1, ct.first.z - 1, ct.first.x + 1, ct.first.y + 1, ct.first.z + 1, steps_);
+}
+
+// packFlameStep (flame.ts:43-87): validate before any state changes.
+int Engine::packFlame(const fp_combustion& c, float dt) {
+  auto finite = [](float v) { return std::isfinite(v); };
+  if (!finite(dt)) return fail(FP_EINVAL, "Flame timestep must be finite in f32.");
+  if (!finite(c.lifespan)) return fail(FP_EINVAL, "Flame lifespan must be finite in f32.");
+  if (dt <= 0 || c.lifespan <= 0) return fail(FP_EINVAL, "Flame timestep and lifespan must be positive in f32.");
+  if (!finite(dt / c.lifespan)) return fail(FP_EINVAL, "Lifetime decrement must be finite in f32.");
+  if (!finite(c.smoke_rate)) return fail(FP_EINVAL, "Smoke rate must be finite in f32.");
+  if (!finite(c.heat_rate)) return fail(FP_EINVAL, "Heat rate must be finite in f32.");
+  if (!finite(c.expansion_rate)) return fail(FP_EINVAL, "Expansion rate must be finite in f32.");
+  if (c.smoke_rate < 0 || c.heat_rate < 0) return fail(FP_EINVAL, "Smoke and heat rates must be nonnegative.");
+  for (float r : {c.smoke_rate, c.heat_rate, c.expansion_rate})
+    if (!finite(r * c.lifespan)) return fail(FP_EINVAL, "Integrated flame output must be finite in f32.");
+  const char* names[3] = {"smoke", "heat", "expansion"};
+  FpFlame F{};
+  F.dt = dt;
+  F.lifespan = c.lifespan;
+  F.smoke = c.smoke_rate;
+  F.heat = c.heat_rate;
+  F.expansion = c.expansion_rate;
+  for (int ch = 0; ch < 3; ch++) {
+    const fp_flame_ramp& r = c.ramps[ch];
+    if (r.count < 2 || r.count > 8) return fail(FP_EINVAL, std::string(names[ch]) + " ramp needs 2–8 knots.");
+    float prev = -1;
+    for (uint32_t i = 0; i < r.count; i++) {
+      float x = r.knots[i][0], y = r.knots[i][1];
+      if (!finite(x)) return fail(FP_EINVAL, std::string(names[ch]) + " lifetime must be finite in f32.");
+      if (!finite(y)) return fail(FP_EINVAL, std::string(names[ch]) + " response must be finite in f32.");
+      if (x < 0 || x > 1 || y < 0 || y > 1 || x <= prev)
+        return fail(FP_EINVAL, std::string(names[ch]) + " knots must increase in f32 with coordinates in [0,1].");
+      if ((i == 0 && x != 0) || (i == r.count - 1 && x != 1))
+        return fail(FP_EINVAL, std::string(names[ch]) + " ramp must span lifetime 0–1.");
+      F.knots[ch][i][0] = x;
+      F.knots[ch][i][1] = y;
+      prev = x;
+    }
+    F.counts[ch] = (int)r.count;
+  }
+  flame_ = F;
+  return FP_OK;
+}
+
+// Every tile within the world box (FluidSimulation.ts:1163-1188); all tiles without one.
+void Engine::bin(int kind, int index, const float* lo, const float* hi, std::vector<std::vector<uint32_t>>& lists) {
+  const auto& slots = dir_.slots();
+  if (!lo) {
+    for (size_t s = 0; s < slots.size(); s++)
+      if (slots[s].alive) lists[(size_t)s * 3 + kind].push_back((uint32_t)index);
+    return;
+  }
+  float tile = (float)(TILE_BRICKS * B_) * h_;
+  int l[3], u[3];
+  for (int a = 0; a < 3; a++) {
+    l[a] = (int)std::floor(lo[a] / tile);
+    u[a] = (int)std::floor(hi[a] / tile);
+  }
+  long span = 1;
+  for (int a = 0; a < 3; a++) span *= std::max(0, u[a] - l[a] + 1);
+  if (span > dir_.count()) {
+    for (size_t s = 0; s < slots.size(); s++) {
+      const auto& t = slots[s];
+      if (t.alive && t.x >= l[0] && t.x <= u[0] && t.y >= l[1] && t.y <= u[1] && t.z >= l[2] && t.z <= u[2])
+        lists[s * 3 + kind].push_back((uint32_t)index);
+    }
+    return;
+  }
+  for (int z = l[2]; z <= u[2]; z++)
+    for (int y = l[1]; y <= u[1]; y++)
+      for (int x = l[0]; x <= u[0]; x++) {
+        int s = dir_.slotAt(x, y, z);
+        if (s >= 0) lists[(size_t)s * 3 + kind].push_back((uint32_t)index);
+      }
+}
+
+// packScene (FluidSimulation.ts:1150-1366) and ForceFields.prepare (ForceFields.ts:41-114).
+// Returns whether the colliders changed.
+bool Engine::packScene(const fp_frame& f) {
+  std::vector<std::vector<uint32_t>> lists((size_t)capacity_ * 3);
+  float brick = (float)B_ * h_;
+  emitters_.clear();
+  for (uint32_t i = 0; i < f.source_count; i++) {
+    const fp_source& s = f.sources[i];
+    if (s.shape == FP_SHAPE_MESH) continue;
+    FpEmitter e{};
+    for (int a = 0; a < 3; a++) {
+      e.pos[a] = s.position[a];
+      e.size[a] = s.size[a];
+      e.vel[a] = s.velocity[a];
+    }
+    e.enabled = 1.f;
+    e.box = s.shape == FP_SHAPE_BOX ? 1.f : 0.f;
+    e.flame = s.flame;
+    e.heat = s.heat_rate;
+    e.smoke = s.smoke_rate;
+    e.response = s.velocity_response;
+    e.outward = s.outward_speed;
+    e.period = s.has_variation ? s.variation_period : 0.5f;
+    e.strength = s.has_variation ? s.variation_strength : 0.f;
+    e.fuel = s.fuel_rate;
+    int index = (int)emitters_.size();
+    emitters_.push_back(e);
+    float lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+      float ext = std::max(s.size[a], 0.03f);
+      lo[a] = s.position[a] - ext - 2.f * brick;
+      hi[a] = s.position[a] + ext + 2.f * brick;
+    }
+    bin(0, index, lo, hi, lists);
+  }
+  colliders_.clear();
+  masks_.assign(f.collider_masks, f.collider_masks + f.collider_mask_words);
+  for (uint32_t i = 0; i < f.collider_count; i++) {
+    const fp_collider& c = f.colliders[i];
+    FpCollider k{};
+    float lo[3], hi[3];
+    if (c.shape == FP_SHAPE_MESH) {
+      k.kind = 2.f;
+      for (int a = 0; a < 3; a++) {
+        k.lo[a] = c.lo[a];
+        k.size[a] = c.dims[a];
+        lo[a] = (float)c.lo[a] * h_;
+        hi[a] = (float)(c.lo[a] + c.dims[a]) * h_;
+      }
+      k.first = (int)c.mask_offset;
+    } else {
+      k.kind = c.shape == FP_SHAPE_BOX ? 1.f : 0.f;
+      for (int a = 0; a < 3; a++) {
+        k.center[a] = c.position[a];
+        k.extent[a] = c.size[a];
+        for (int b = 0; b < 3; b++) k.axes[a][b] = c.axes[a][b];
+      }
+      for (int a = 0; a < 3; a++) {
+        float ext = c.size[a];
+        if (c.shape == FP_SHAPE_BOX)
+          ext = std::fabs(c.axes[0][a]) * c.size[0] + std::fabs(c.axes[1][a]) * c.size[1] + std::fabs(c.axes[2][a]) * c.size[2];
+        lo[a] = c.position[a] - ext;
+        hi[a] = c.position[a] + ext;
+      }
+    }
+    colliders_.push_back(k);
+    bin(2, (int)i, lo, hi, lists);
+  }
+  std::vector<uint8_t> packed(colliders_.size() * sizeof(FpCollider));
+  if (!packed.empty()) std::memcpy(packed.data(), colliders_.data(), packed.size());
+  bool changed = packed != prevColliders_ || masks_ != prevMasks_;
+  prevColliders_.swap(packed);
+  prevMasks_ = masks_;
+  colliderCount_ = (int)colliders_.size();
+  forces_.clear();
+  regions_.clear();
+  for (uint32_t i = 0; i < f.force_count; i++) {
+    const fp_force& s = f.forces[i];
+    FpForce k{};
+    for (int a = 0; a < 3; a++) {
+      k.axis[a] = s.vector[a];
+      k.center[a] = s.center[a];
+    }
+    k.strength = s.strength;
+    k.kind = (float)s.type;
+    k.scale = s.scale;
+    k.lift = s.lift;
+    k.inward = s.inward;
+    k.targeted = s.targeted ? 1.f : 0.f;
+    k.regionFirst = (float)regions_.size();
+    bool has = false;
+    float lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
+    int count = 0;
+    if (s.targeted) {
+      for (uint32_t t = 0; t < s.target_count && s.first_target + t < f.force_target_count; t++) {
+        const fp_source& src = f.force_targets[s.first_target + t];
+        if (src.shape == FP_SHAPE_MESH) continue;
+        FpRegion r{};
+        for (int a = 0; a < 3; a++) {
+          r.center[a] = src.position[a];
+          r.size[a] = src.size[a];
+        }
+        r.box = src.shape == FP_SHAPE_BOX ? 3.f : 1.f;
+        regions_.push_back(r);
+        count++;
+        for (int a = 0; a < 3; a++) {
+          float ext = std::max(src.size[a], 0.03f);
+          float l = src.position[a] - ext, u = src.position[a] + ext;
+          lo[a] = has ? std::min(lo[a], l) : l;
+          hi[a] = has ? std::max(hi[a], u) : u;
+        }
+        has = true;
+      }
+    }
+    k.regionCount = (float)count;
+    forces_.push_back(k);
+    if (!s.targeted) {
+      bin(1, (int)i, nullptr, nullptr, lists);
+    } else {
+      float l[3], u[3];
+      for (int a = 0; a < 3; a++) {
+        l[a] = lo[a] - brick;
+        u[a] = hi[a] + brick;
+      }
+      bin(1, (int)i, l, u, lists);
+    }
+  }
+  // What reaches each tile: an 8-word header per tile slot, then the indices.
+  size_t length = (size_t)capacity_ * 8;
+  for (auto& l : lists) length += l.size();
+  tileLists_.assign(length, 0);
+  size_t next = (size_t)capacity_ * 8;
+  for (int s = 0; s < capacity_; s++)
+    for (int k = 0; k < 3; k++) {
+      auto& l = lists[(size_t)s * 3 + k];
+      tileLists_[(size_t)s * 8 + 2 * k] = (uint32_t)next;
+      tileLists_[(size_t)s * 8 + 2 * k + 1] = (uint32_t)l.size();
+      std::copy(l.begin(), l.end(), tileLists_.begin() + next);
+      next += l.size();
+    }
+  return changed;
+}
+
+int Engine::uploadScene() {
+  if (!upload(emittersD_, emitters_.data(), emitters_.size() * sizeof(FpEmitter)) ||
+      !upload(collidersD_, colliders_.data(), colliders_.size() * sizeof(FpCollider)) ||
+      !upload(masksD_, masks_.data(), masks_.size() * 4) ||
+      !upload(forcesD_, forces_.data(), forces_.size() * sizeof(FpForce)) ||
+      !upload(regionsD_, regions_.data(), regions_.size() * sizeof(FpRegion)) ||
+      !upload(tileListsD_, tileLists_.data(), tileLists_.size() * 4))
+    return FP_ENOMEM;
+  return FP_OK;
+}
+
+void Engine::fillParams(const fp_frame& f, float dt) {
+  SimParams& P = *paramsH_;
+  std::memset(&P, 0, sizeof(P));
+  P.B = B_;
+  P.shift = shift_;
+  P.N = N_;
+  P.W = W_;
+  P.brickLevels = brickLevels_;
+  P.bottom = bottom_;
+  P.h = h_;
+  P.invH = 1.f / h_;
+  P.dt = dt;
+  P.buoyancy = f.simulation.buoyancy;
+  P.cooling = f.simulation.cooling;
+  P.smokeWeight = f.simulation.smoke_weight;
+  P.damping = f.simulation.velocity_damping;
+  P.dissipation = f.simulation.dissipation;
+  P.vorticity = f.simulation.vorticity;
+  P.cutoff = cutoff_;
+  P.time = (float)time_;
+  P.seedF = (float)f.simulation.seed;
+  std::memcpy(&P.seedBits, &P.seedF, 4);
+  P.lifetimeZero = mayHaveFlame_ ? 0 : 1;
+  P.fuelEnabled = f.fuel.enabled ? 1 : 0;
+  P.ignition = f.fuel.ignition_heat;
+  P.burnRate = f.fuel.burn_rate;
+  P.ground = ground_ ? 1 : 0;
+  P.colliderCount = colliderCount_;
+  P.maccormack = maccormack_ ? 1 : 0;
+  P.solidsAll = solidsStale_ ? 1 : 0;
+  P.held = (int)std::max<int64_t>(0, (int64_t)slots_ - (int64_t)slotLimit());
+  P.slots = slots_;
+  P.capacity = capacity_;
+  P.tileRec = (const int4*)tileRecD_.ptr;
+  P.tileNbr = (const int*)tileNbrD_.ptr;
+  P.hash = (const int4*)hashD_.ptr;
+  P.hashMask = (uint32_t)hash_.size() - 1;
+  P.pages = (int*)pages_.ptr;
+  P.entries = (int*)entries_.ptr;
+  P.state = (uint32_t*)state_.ptr;
+  P.activity = (uint32_t*)activity_.ptr;
+  P.records = (int*)records_.ptr;
+  P.blockCounts = (uint32_t*)blockCounts_.ptr;
+  P.active = (uint32_t*)active_.ptr;
+  P.zeroList = (uint32_t*)zeroList_.ptr;
+  P.freeStack = (uint32_t*)freeStack_.ptr;
+  P.counters = (FpCounters*)counters_.ptr;
+  P.vel = (float*)vel_[velIdx_[0]].ptr;
+  P.velP = (float*)vel_[velIdx_[1]].ptr;
+  P.velC = (float*)vel_[velIdx_[2]].ptr;
+  P.velF = (float*)vel_[velIdx_[3]].ptr;
+  P.curl = (float*)curl_.ptr;
+  P.fld = (float*)fld_[fldIdx_[0]].ptr;
+  P.fldP = (float*)fld_[fldIdx_[1]].ptr;
+  P.fldN = (float*)fld_[fldIdx_[2]].ptr;
+  P.expn = (float*)expn_.ptr;
+  P.div = (float*)div_.ptr;
+  P.vmin = (float*)vmin_.ptr;
+  P.vmax = (float*)vmax_.ptr;
+  P.sb = (float*)sb_.ptr;
+  P.donors = (uint16_t*)donors_.ptr;
+  P.solids = (uint32_t*)solids_.ptr;
+  P.p0[0] = (float*)p0_[0].ptr;
+  P.p0[1] = (float*)p0_[1].ptr;
+  P.latest = latest_;
+  for (int l = 0; l <= bottom_; l++) {
+    P.topo[l] = (uint8_t*)topo_[l].ptr;
+    if (l > 0) {
+      P.lp[l][0] = (float*)lp_[l][0].ptr;
+      P.lp[l][1] = (float*)lp_[l][1].ptr;
+      P.lrhs[l] = (float*)lrhs_[l].ptr;
+    }
+  }
+  P.emitters = (const FpEmitter*)emittersD_.ptr;
+  P.colliders = (const FpCollider*)collidersD_.ptr;
+  P.masks = (const uint32_t*)masksD_.ptr;
+  P.forces = (const FpForce*)forcesD_.ptr;
+  P.regions = (const FpRegion*)regionsD_.ptr;
+  P.tileLists = (const uint32_t*)tileListsD_.ptr;
+  P.flame = flame_;
+  P.noise = (const float4*)noise_.ptr;
+}
+
+// readActivity (FluidSimulation.ts:1701-1746), applied before the next step: the
+// measurement lags the step by exactly one.
+int Engine::consumeReadback() {
+  if (!pendingRead_) return FP_OK;
+  int rc = check(cudaEventSynchronize(readEvent_), "step");
+  if (rc) return rc;
+  pendingRead_ = false;
+  const FpCounters* c = (const FpCounters*)readH_;
+  const uint32_t* flags = readH_ + sizeof(FpCounters) / 4;
+  contentTiles_.clear();
+  for (int s = 0; s < capacity_ && s < (int)tileRec_.size(); s++)
+    if (flags[s] && tileRec_[s].w != 0) contentTiles_.push_back({tileRec_[s], flags[s]});
+  activeBricks_ = c->active;
+  usedSlots_ = slots_ - (uint32_t)c->freeCount;
+  lastFailures_ = c->failures;
+  poolLimited_ = c->failures > 0 && slots_ >= slotLimit();
+  return FP_OK;
+}
+
+// One V-cycle of PressureSolver.plan (PressureSolver.ts:276-365); `cur` holds each level's
+// current pressure buffer. The finest level's first iterate was written with the divergence.
+void Engine::vcycle(int level, int cur[]) {
+  SimParams* dP = dParams();
+  if (level == bottom_) {
+    if (capacity_ <= 1024) {
+      fp_launch_bottom(dP, level, 19, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]), capacity_, stream_);
+      cur[level] = 1 - cur[level];
+    } else {
+      for (int i = 0; i < 19; i++) {
+        fp_launch_relax(dP, level, true, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]), capacity_, sms_,
+                        stream_);
+        cur[level] = 1 - cur[level];
+      }
+    }
+    return;
+  }
+  if (level > 0)
+    for (int i = 0; i < 2; i++) {
+      fp_launch_relax(dP, level, level >= brickLevels_, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]),
+                      capacity_, sms_, stream_);
+      cur[level] = 1 - cur[level];
+    }
+  int coarse = level + 1;
+  fp_launch_restrict(dP, level, coarse >= brickLevels_, RHS(level), LP(level, cur[level]), RHS(coarse), LP(coarse, 1),
+                     capacity_, sms_, stream_);
+  cur[coarse] = 1;
+  vcycle(coarse, cur);
+  fp_launch_prolong(dP, level, level >= brickLevels_, LP(level, cur[level]), LP(coarse, cur[coarse]),
+                    LP(level, 1 - cur[level]), capacity_, sms_, stream_);
+  cur[level] = 1 - cur[level];
+  for (int i = 0; i < 3; i++) {
+    fp_launch_relax(dP, level, level >= brickLevels_, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]),
+                    capacity_, sms_, stream_);
+    cur[level] = 1 - cur[level];
+  }
+}
+
+// FluidSimulation.step / substep (FluidSimulation.ts:1367-1531).
+int Engine::step(const fp_frame& f, float dt) {
+  if (!std::isfinite(dt) || dt <= 0 || dt > 1.f / 30.f)
+    return fail(FP_EINVAL, "Simulation step must be in (0, 1/30]. Use fixed substeps.");
+  int rc = packFlame(f.combustion, dt);
+  if (rc) return rc;
+  for (uint32_t i = 0; i < f.collider_count; i++) {
+    const fp_collider& c = f.colliders[i];
+    if (c.shape == FP_SHAPE_MESH) {
+      uint64_t bits = (uint64_t)std::max(0, c.dims[0]) * std::max(0, c.dims[1]) * std::max(0, c.dims[2]);
+      if ((uint64_t)c.mask_offset + (bits + 31) / 32 > f.collider_mask_words)
+        return fail(FP_EINVAL, "Mesh collider occupancy does not match its size.");
+    }
+  }
+  if ((rc = check(cudaSetDevice(device_), "cudaSetDevice"))) return rc;
+  if ((rc = consumeReadback())) return rc;
+  if (dir_.ground != ground_) {
+    dir_.ground = ground_;
+    geometryDirty_ = true;
+  }
+  uint32_t limit = slotLimit();
+  if (limit > slots_ && (rc = growPool(limit))) return rc;
+  updateTiles(f);
+  if (dir_.dirty && (rc = applyTiles())) return rc;
+  if (packScene(f)) {
+    solidsStale_ = true;
+    geometryDirty_ = true;
+  }
+  mayHaveFlame_ = mayHaveFlame_ || f.fuel.enabled;
+  for (uint32_t i = 0; i < f.source_count; i++) mayHaveFlame_ = mayHaveFlame_ || f.sources[i].flame > 0;
+  if ((rc = uploadScene())) return rc;
+  fillParams(f, dt);
+  SimParams* dP = dParams();
+  cudaMemcpyAsync(dP, paramsH_, sizeof(SimParams), cudaMemcpyHostToDevice, stream_);
+
+  fp_launch_allocation(dP, capacity_, colliderCount_ > 0 || solidsStale_, sms_, stream_);
+  solidsStale_ = false;
+  // Topology of the slots granted this step, or of everything after the geometry changed.
+  fp_launch_topology(dP, brickLevels_, bottom_, geometryDirty_, capacity_, sms_, stream_);
+  geometryDirty_ = false;
+  fp_launch_predict(dP, sms_, stream_);
+  fp_launch_correct_evolve(dP, sms_, stream_);
+  if (f.simulation.vorticity != 0.f) fp_launch_curl(dP, sms_, stream_);
+  fp_launch_forces(dP, B_, sms_, stream_);
+  int cur[FP_MAX_LEVELS] = {0};
+  cur[0] = latest_;
+  fp_launch_divergence(dP, P0(1 - cur[0]), sms_, stream_);
+  cur[0] = 1 - cur[0];
+  vcycle(0, cur);
+  latest_ = cur[0];
+  fp_launch_project(dP, P0(latest_), sms_, stream_);
+  std::swap(velIdx_[0], velIdx_[1]);
+  std::swap(fldIdx_[0], fldIdx_[2]);
+
+  // Measurement: counters and the tiles' content flags, then clear failures.
+  size_t words = sizeof(FpCounters) / 4 + capacity_;
+  if (words > readWords_) {
+    if (readH_) cudaFreeHost(readH_);
+    readWords_ = words * 2;
+    if ((rc = check(cudaMallocHost(&readH_, readWords_ * 4), "cudaMallocHost"))) return rc;
+  }
+  cudaMemcpyAsync(readH_, counters_.ptr, sizeof(FpCounters), cudaMemcpyDeviceToHost, stream_);
+  cudaMemcpyAsync(readH_ + sizeof(FpCounters) / 4, (uint32_t*)activity_.ptr + (size_t)capacity_ * 64,
+                  (size_t)capacity_ * 4, cudaMemcpyDeviceToHost, stream_);
+  cudaMemsetAsync(&((FpCounters*)counters_.ptr)->failures, 0, 4, stream_);
+  cudaEventRecord(readEvent_, stream_);
+  pendingRead_ = true;
+  time_ += dt;
+  steps_++;
+  return check(cudaGetLastError(), "step launch");
+}
+
+int Engine::reset() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  return initialize();
+}
+
+int Engine::setRuntime(float cutoff, double budget, int ground) {
+  if (!std::isfinite(cutoff)) return fail(FP_EINVAL, "grid.cutoff must be a finite number from 0 to 1.");
+  cutoff_ = cutoff;
+  if (budget > 0) budget_ = budget;
+  ground_ = ground != 0;
+  return FP_OK;
+}
+
+int Engine::synchronize() { return check(cudaStreamSynchronize(stream_), "synchronize"); }
+
+int Engine::stats(fp_stats* out) {
+  int rc = consumeReadback();
+  if (rc) return rc;
+  std::memset(out, 0, sizeof(*out));
+  out->time = time_;
+  out->steps = (uint64_t)steps_;
+  out->active_bricks = activeBricks_;
+  out->brick_cells = (uint32_t)N_;
+  out->pool_limited = poolLimited_;
+  out->pool_slots = slots_;
+  out->used_slots = usedSlots_;
+  out->tiles = (uint32_t)dir_.count();
+  out->tile_capacity = (uint32_t)capacity_;
+  out->failures = lastFailures_;
+  uint64_t bytes = 0;
+  DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_, &zeroList_,
+                         &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_, &donors_, &solids_,
+                         &tileRecD_, &tileNbrD_, &hashD_, &emittersD_, &collidersD_, &masksD_, &forcesD_,
+                         &regionsD_, &tileListsD_, &noise_, &paramsD_};
+  for (DeviceBuffer* b : all) bytes += b->bytes;
+  for (auto& b : vel_) bytes += b.bytes;
+  for (auto& b : fld_) bytes += b.bytes;
+  for (auto& b : p0_) bytes += b.bytes;
+  for (int l = 0; l < FP_MAX_LEVELS; l++) bytes += topo_[l].bytes + lrhs_[l].bytes + lp_[l][0].bytes + lp_[l][1].bytes;
+  out->memory_bytes = bytes;
+  out->last_vcycles = steps_ > 0 ? 1 : 0;
+  out->last_residual = -1;
+  return FP_OK;
+}
+
+int Engine::readField(int field, float* host, size_t bytes) {
+  const DeviceBuffer* b = nullptr;
+  size_t ch = 0;
+  switch (field) {
+    case FP_FIELD_VELOCITY: b = &vel_[velIdx_[0]]; ch = 3; break;
+    case FP_FIELD_SCALARS: b = &fld_[fldIdx_[0]]; ch = 4; break;
+    case FP_FIELD_EXPANSION: b = &expn_; ch = 1; break;
+    case FP_FIELD_PRESSURE: b = &p0_[latest_]; ch = 1; break;
+    case FP_FIELD_DIVERGENCE: b = &div_; ch = 1; break;
+    case FP_FIELD_CURL: b = &curl_; ch = 4; break;
+    default: return fail(FP_EINVAL, "unknown field");
+  }
+  size_t need = (size_t)slots_ * ch * N_ * 4;
+  if (bytes != need) return fail(FP_EINVAL, "field buffer size mismatch: need " + std::to_string(need) + " bytes");
+  int rc = check(cudaStreamSynchronize(stream_), "read field");
+  if (rc) return rc;
+  return check(cudaMemcpy(host, b->ptr, need, cudaMemcpyDeviceToHost), "read field");
+}
+
+int Engine::readTable(int table, void* host, size_t* bytes) {
+  int rc = consumeReadback();
+  if (rc) return rc;
+  if ((rc = check(cudaStreamSynchronize(stream_), "read table"))) return rc;
+  size_t bricks = (size_t)capacity_ * 64;
+  std::vector<uint32_t> w;
+  auto fetch = [&](const DeviceBuffer& b, size_t words, size_t offsetWords = 0) {
+    size_t old = w.size();
+    w.resize(old + words);
+    cudaMemcpy(w.data() + old, (const uint32_t*)b.ptr + offsetWords, words * 4, cudaMemcpyDeviceToHost);
+  };
+  switch (table) {
+    case FP_TABLE_ENTRIES: fetch(entries_, bricks); break;
+    case FP_TABLE_PAGES: fetch(pages_, bricks); break;
+    case FP_TABLE_STATE: fetch(state_, bricks); break;
+    case FP_TABLE_ACTIVITY: fetch(activity_, bricks + capacity_); break;
+    case FP_TABLE_RECORDS: fetch(records_, bricks * FP_RECORD_WORDS); break;
+    case FP_TABLE_FREE: {
+      FpCounters c;
+      cudaMemcpy(&c, counters_.ptr, sizeof(c), cudaMemcpyDeviceToHost);
+      w.push_back((uint32_t)c.freeCount);
+      w.push_back(lastFailures_);
+      fetch(freeStack_, slots_);
+      break;
+    }
+    case FP_TABLE_ACTIVE: {
+      FpCounters c;
+      cudaMemcpy(&c, counters_.ptr, sizeof(c), cudaMemcpyDeviceToHost);
+      w.push_back(c.active);
+      fetch(active_, c.active);
+      break;
+    }
+    case FP_TABLE_SOLIDS: fetch(solids_, (size_t)slots_ * W_); break;
+    case FP_TABLE_TILES:
+      for (int t = 0; t < capacity_; t++) {
+        int4 r = t < (int)tileRec_.size() ? tileRec_[t] : make_int4(0, 0, 0, 0);
+        w.push_back((uint32_t)r.x);
+        w.push_back((uint32_t)r.y);
+        w.push_back((uint32_t)r.z);
+        w.push_back((uint32_t)r.w);
+      }
+      break;
+    default: return fail(FP_EINVAL, "unknown table");
+  }
+  size_t need = w.size() * 4;
+  if (!host || *bytes < need) {
+    *bytes = need;
+    return fail(FP_ELIMIT, "table buffer too small");
+  }
+  std::memcpy(host, w.data(), need);
+  *bytes = need;
+  return FP_OK;
+}
+
+// readBricks (FluidSimulation.ts:1749-1779): world boxes of the bricks holding a slot.
+int Engine::readBricks(float* boxes, uint32_t* count) {
+  int rc = check(cudaStreamSynchronize(stream_), "read bricks");
+  if (rc) return rc;
+  size_t bricks = (size_t)capacity_ * 64;
+  std::vector<int> pages(bricks);
+  cudaMemcpy(pages.data(), pages_.ptr, bricks * 4, cudaMemcpyDeviceToHost);
+  float size = (float)B_ * h_;
+  uint32_t n = 0;
+  for (size_t id = 0; id < bricks; id++) {
+    const int4& t = tileRec_[id / 64];
+    if (t.w == 0 || pages[id] < 0) continue;
+    if (boxes && n < *count) {
+      int l = (int)(id % 64);
+      float mn[3] = {(float)(t.x * 4 + (l & 3)) * size, (float)(t.y * 4 + ((l >> 2) & 3)) * size,
+                     (float)(t.z * 4 + (l >> 4)) * size};
+      for (int a = 0; a < 3; a++) {
+        boxes[n * 6 + a] = mn[a];
+        boxes[n * 6 + 3 + a] = mn[a] + size;
+      }
+    }
+    n++;
+  }
+  bool fits = boxes && n <= *count;
+  *count = n;
+  return fits ? FP_OK : fail(FP_ELIMIT, "brick buffer too small");
+}
+
+}  // namespace fp

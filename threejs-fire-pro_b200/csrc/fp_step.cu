@@ -1,0 +1,725 @@
+// The step's field kernels over the computing bricks: MacCormack transport of the staggered
+// velocity and of the scalars with their limiters, field evolution and combustion, curl,
+// forces, divergence and projection. One CTA per computing brick, grid-stride over the
+// ascending list the allocation wrote, so no launch depends on a host-side count.
+//
+// Restates src/engine/shaders/fluid-velocity-transport.wgsl, fluid-scalar-transport.wgsl,
+// fluid-field-evolution.wgsl, fluid-forces.wgsl and force-fields.wgsl. Samples read the
+// neighbour bricks' cells through the brick's 27-entry record (shared memory) where the
+// reference reads a texture apron that copies them; bricks without a slot read zero.
+#include "fp_device.cuh"
+#include "fp_launch.h"
+
+namespace {
+
+constexpr int THREADS = 256;
+
+FP_DEV float velComp(const SimParams& P, const Home& H, const float* pool, float px, float py, float pz, int c) {
+  float q[3] = {px, py, pz};
+  q[c] -= 0.5f * P.h;
+  return sampleCells(P, H, pool, 3, c, q[0] / P.h, q[1] / P.h, q[2] / P.h);
+}
+// velocityAt (fluid-advection.wgsl:17-21).
+FP_DEV float3 velocityAt(const SimParams& P, const Home& H, const float* pool, float px, float py, float pz) {
+  return make_float3(velComp(P, H, pool, px, py, pz, 0), velComp(P, H, pool, px, py, pz, 1),
+                     velComp(P, H, pool, px, py, pz, 2));
+}
+FP_DEV float get(const float3& v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
+
+// velocityOnFace (fluid-advection.wgsl:26-44): the face's own component is stored.
+FP_DEV float3 velocityOnFace(const SimParams& P, const Home& H, int x, int y, int z, int c, float3 orig) {
+  float fp[3] = {(float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f};
+  fp[c] += 0.5f;
+  float r[3];
+  for (int k = 0; k < 3; k++) {
+    if (k == c) {
+      r[k] = get(orig, k);
+      continue;
+    }
+    float q[3] = {fp[0], fp[1], fp[2]};
+    q[k] -= 0.5f;
+    r[k] = sampleCells(P, H, P.vel, 3, k, q[0], q[1], q[2]);
+  }
+  return make_float3(r[0], r[1], r[2]);
+}
+
+// packDonor / unpackDonor (fluid-advection.wgsl:79-100), 5 bits an axis.
+FP_DEV uint32_t packDonor(int ox, int oy, int oz) {
+  int bx = ox + 16, by = oy + 16, bz = oz + 16;
+  if (bx < 0 || by < 0 || bz < 0 || bx >= 32 || by >= 32 || bz >= 32) return 1u << 15;
+  return (uint32_t)bx | ((uint32_t)by << 5) | ((uint32_t)bz << 10);
+}
+
+FP_DEV void cellOf(const SimParams& P, const Home& H, int c, int& x, int& y, int& z) {
+  int m = P.B - 1;
+  x = H.bx * P.B + (c & m);
+  y = H.by * P.B + ((c >> P.shift) & m);
+  z = H.bz * P.B + (c >> (2 * P.shift));
+}
+
+// ---------------------------------------------------------------------------------------
+// Predictors: advectVelocityWithBounds (fluid-velocity-transport.wgsl:28-100) and
+// advectScalars (fluid-scalar-transport.wgsl:38-142), fused: both read only the velocity and
+// the scalars at the start of the step.
+__global__ void __launch_bounds__(THREADS) k_predict(const SimParams* __restrict__ Pp) {
+  const SimParams& P = *Pp;
+  __shared__ int nslot[27];
+  uint32_t total = P.counters->active;
+  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+    uint32_t id = P.active[i];
+    Home H = enterBrick(P, id, nslot);
+    size_t slot = (size_t)nslot[13];
+    const size_t N = P.N;
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int x, y, z;
+      cellOf(P, H, c, x, y, z);
+      // Velocity bounds over the forward 2x2x2 block.
+      for (int k = 0; k < 3; k++) {
+        float lo = 1e5f, hi = -1e5f;
+        for (int dz = 0; dz < 2; dz++)
+          for (int dy = 0; dy < 2; dy++)
+            for (int dx = 0; dx < 2; dx++) {
+              float v = cellAt(P, H, P.vel, 3, k, x + dx, y + dy, z + dz);
+              lo = fminf(lo, v);
+              hi = fmaxf(hi, v);
+            }
+        P.vmin[(slot * 3 + k) * N + c] = lo;
+        P.vmax[(slot * 3 + k) * N + c] = hi;
+      }
+      float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+      if (solidAt(P, H, px, py, pz)) {
+        for (int k = 0; k < 3; k++) P.velP[(slot * 3 + k) * N + c] = 0.f;
+      } else {
+        float3 orig = make_float3(P.vel[(slot * 3 + 0) * N + c], P.vel[(slot * 3 + 1) * N + c],
+                                  P.vel[(slot * 3 + 2) * N + c]);
+        for (int comp = 0; comp < 3; comp++) {
+          float face[3] = {px, py, pz};
+          face[comp] += 0.5f * P.h;
+          float3 fv = velocityOnFace(P, H, x, y, z, comp, orig);
+          float3 vm = velocityAt(P, H, P.vel, face[0] - 0.5f * P.dt * fv.x, face[1] - 0.5f * P.dt * fv.y,
+                                 face[2] - 0.5f * P.dt * fv.z);
+          float dep[3] = {face[0] - P.dt * vm.x, face[1] - P.dt * vm.y, face[2] - P.dt * vm.z};
+          float sh[3] = {dep[0], dep[1], dep[2]};
+          sh[comp] -= 0.5f * P.h;
+          int bx = (int)floorf(sh[0] / P.h - 0.5f), by = (int)floorf(sh[1] / P.h - 0.5f),
+              bz = (int)floorf(sh[2] / P.h - 0.5f);
+          P.donors[(slot * 3 + comp) * N + c] = (uint16_t)packDonor(bx - x, by - y, bz - z);
+          P.velP[(slot * 3 + comp) * N + c] = velComp(P, H, P.vel, dep[0], dep[1], dep[2], comp);
+        }
+      }
+      // Scalars: a cell-centred RK2 back trace, the predictor and its donors' range.
+      float3 cv = velocityAt(P, H, P.vel, px, py, pz);
+      float3 vm = velocityAt(P, H, P.vel, px - 0.5f * P.dt * cv.x, py - 0.5f * P.dt * cv.y, pz - 0.5f * P.dt * cv.z);
+      float dx_ = px - P.dt * vm.x, dy_ = py - P.dt * vm.y, dz_ = pz - P.dt * vm.z;
+      float out[4];
+      if (!P.maccormack) {
+        for (int k = 0; k < 4; k++) out[k] = sampleCells(P, H, P.fld, 4, k, dx_ / P.h, dy_ / P.h, dz_ / P.h);
+        out[2] = clamp01(out[2]);
+      } else {
+        float dc[3] = {(float)x + (dx_ - px) / P.h, (float)y + (dy_ - py) / P.h, (float)z + (dz_ - pz) / P.h};
+        int base[3];
+        float fr[3];
+        for (int a = 0; a < 3; a++) {
+          base[a] = (int)floorf(dc[a]);
+          fr[a] = dc[a] - floorf(dc[a]);
+        }
+        float mn0 = 65504.f, mn1 = 65504.f, mn3 = 65504.f, mx0 = -65504.f, mx1 = -65504.f, mx3 = -65504.f;
+        float lmin = 1.f, lmax = 0.f;
+        float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
+        int sh = P.shift;
+        for (int dz = 0; dz < 2; dz++)
+          for (int dy = 0; dy < 2; dy++)
+            for (int dx = 0; dx < 2; dx++) {
+              int cx = base[0] + dx, cy = base[1] + dy, cz = base[2] + dz;
+              int s = brickSlot(P, H, cx >> sh, cy >> sh, cz >> sh);
+              float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+              if (s >= 0) {
+                size_t o = (size_t)s * 4 * N + localCell(P, cx, cy, cz);
+                s0 = P.fld[o];
+                s1 = P.fld[o + N];
+                s2 = P.fld[o + 2 * N];
+                s3 = P.fld[o + 3 * N];
+              }
+              mn0 = fminf(mn0, s0); mn1 = fminf(mn1, s1); mn3 = fminf(mn3, s3);
+              mx0 = fmaxf(mx0, s0); mx1 = fmaxf(mx1, s1); mx3 = fmaxf(mx3, s3);
+              lmin = fminf(lmin, s2);
+              lmax = fmaxf(lmax, s2);
+              float w = (dx ? fr[0] : 1.f - fr[0]) * (dy ? fr[1] : 1.f - fr[1]) * (dz ? fr[2] : 1.f - fr[2]);
+              v0 += s0 * w; v1 += s1 * w; v2 += s2 * w; v3 += s3 * w;
+            }
+        float* b = P.sb + slot * 8 * N;
+        b[0 * N + c] = mn0; b[1 * N + c] = mn1; b[2 * N + c] = mn3; b[3 * N + c] = lmin;
+        b[4 * N + c] = mx0; b[5 * N + c] = mx1; b[6 * N + c] = mx3; b[7 * N + c] = lmax;
+        out[0] = v0;
+        out[1] = v1;
+        out[2] = P.lifetimeZero ? 0.f : v2;
+        out[3] = v3;
+      }
+      for (int k = 0; k < 4; k++) P.fldP[(slot * 4 + k) * N + c] = out[k];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Corrections: correctVelocity (fluid-velocity-transport.wgsl:104-179) and evolveFields
+// (fluid-field-evolution.wgsl:9-84 with fluid-scalar-transport.wgsl:144-199 and
+// fluid-content.wgsl:29-64), fused: both read the predictors and the start-of-step fields.
+__global__ void __launch_bounds__(THREADS) k_correct_evolve(const SimParams* __restrict__ Pp) {
+  const SimParams& P = *Pp;
+  __shared__ int nslot[27];
+  __shared__ uint32_t busyAll, expandsAll;
+  uint32_t total = P.counters->active;
+  uint32_t bricks = (uint32_t)P.capacity * 64u;
+  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+    uint32_t id = P.active[i];
+    if (threadIdx.x == 0) {
+      busyAll = 0;
+      expandsAll = 0;
+    }
+    Home H = enterBrick(P, id, nslot);
+    size_t slot = (size_t)nslot[13];
+    const size_t N = P.N;
+    int tile = (int)(id >> 6);
+    uint32_t busy = 0;
+    bool expands = false;
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int x, y, z;
+      cellOf(P, H, c, x, y, z);
+      float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+      bool solid = solidAt(P, H, px, py, pz);
+      float3 orig = make_float3(P.vel[(slot * 3 + 0) * N + c], P.vel[(slot * 3 + 1) * N + c],
+                                P.vel[(slot * 3 + 2) * N + c]);
+      // --- velocity correction
+      for (int comp = 0; comp < 3; comp++) {
+        float result = 0.f;
+        if (!solid) {
+          float predicted = P.velP[(slot * 3 + comp) * N + c];
+          float face[3] = {px, py, pz};
+          face[comp] += 0.5f * P.h;
+          uint32_t donor = P.donors[(slot * 3 + comp) * N + c];
+          bool retrace = donor == (1u << 15);
+          int base[3] = {x + (int)(donor & 31u) - 16, y + (int)((donor >> 5) & 31u) - 16,
+                         z + (int)((donor >> 10) & 31u) - 16};
+          float3 fv = make_float3(0.f, 0.f, 0.f);
+          if (retrace) {
+            fv = velocityOnFace(P, H, x, y, z, comp, orig);
+            float3 vm = velocityAt(P, H, P.vel, face[0] - 0.5f * P.dt * fv.x, face[1] - 0.5f * P.dt * fv.y,
+                                   face[2] - 0.5f * P.dt * fv.z);
+            float dep[3] = {face[0] - P.dt * vm.x, face[1] - P.dt * vm.y, face[2] - P.dt * vm.z};
+            dep[comp] -= 0.5f * P.h;
+            for (int a = 0; a < 3; a++) base[a] = (int)floorf(dep[a] / P.h - 0.5f);
+          }
+          float lo = 0.f, hi = 0.f;
+          int bs = brickSlot(P, H, base[0] >> P.shift, base[1] >> P.shift, base[2] >> P.shift);
+          if (bs >= 0) {
+            int lc = localCell(P, base[0], base[1], base[2]);
+            lo = P.vmin[((size_t)bs * 3 + comp) * N + lc];
+            hi = P.vmax[((size_t)bs * 3 + comp) * N + lc];
+          }
+          if (lo == hi && predicted == lo) {
+            result = predicted;
+          } else {
+            if (!retrace) fv = velocityOnFace(P, H, x, y, z, comp, orig);
+            float3 vm = velocityAt(P, H, P.vel, face[0] + 0.5f * P.dt * fv.x, face[1] + 0.5f * P.dt * fv.y,
+                                   face[2] + 0.5f * P.dt * fv.z);
+            float fw[3] = {face[0] + P.dt * vm.x, face[1] + P.dt * vm.y, face[2] + P.dt * vm.z};
+            fw[comp] -= 0.5f * P.h;
+            float reversed = sampleCells(P, H, P.velP, 3, comp, fw[0] / P.h, fw[1] / P.h, fw[2] / P.h);
+            float corrected = predicted + 0.5f * (get(orig, comp) - reversed);
+            result = (corrected < lo || corrected > hi) ? predicted : corrected;
+          }
+        }
+        P.velC[(slot * 3 + comp) * N + c] = result;
+      }
+      // --- scalar correction and evolution
+      float value[4] = {0.f, 0.f, 0.f, 0.f};
+      float expansion = 0.f;
+      bool injected = false;
+      bool cvSampled = false;
+      float3 cv = make_float3(0.f, 0.f, 0.f);
+      if (!solid) {
+        float tr[4];
+        const float* adv = P.fldP + slot * 4 * N;
+        if (!P.maccormack) {
+          for (int k = 0; k < 4; k++) tr[k] = adv[k * N + c];
+        } else {
+          const float* b = P.sb + slot * 8 * N;
+          float mn0 = b[0 * N + c], mn1 = b[1 * N + c], mn3 = b[2 * N + c], lmin = b[3 * N + c];
+          float mx0 = b[4 * N + c], mx1 = b[5 * N + c], mx3 = b[6 * N + c], lmax = b[7 * N + c];
+          if (mn0 == mx0 && mn1 == mx1 && mn3 == mx3 && lmin == lmax) {
+            tr[0] = mn0;
+            tr[1] = mn1;
+            tr[2] = clamp01(lmin);
+            tr[3] = mn3;
+          } else {
+            float a0 = adv[0 * N + c], a1 = adv[1 * N + c], a2 = adv[2 * N + c], a3 = adv[3 * N + c];
+            cv = velocityAt(P, H, P.vel, px, py, pz);
+            cvSampled = true;
+            float3 vm = velocityAt(P, H, P.vel, px + 0.5f * P.dt * cv.x, py + 0.5f * P.dt * cv.y, pz + 0.5f * P.dt * cv.z);
+            float fx = px + P.dt * vm.x, fy = py + P.dt * vm.y, fz = pz + P.dt * vm.z;
+            const float* o = P.fld + slot * 4 * N;
+            float o0 = o[0 * N + c], o1 = o[1 * N + c], o2 = o[2 * N + c], o3 = o[3 * N + c];
+            float lifetime = a2;
+            float r0, r1, r3;
+            if (lmin != lmax || a2 != lmin) {
+              float fc[3] = {(float)x + (fx - px) / P.h, (float)y + (fy - py) / P.h, (float)z + (fz - pz) / P.h};
+              int base[3];
+              float fr[3];
+              for (int a = 0; a < 3; a++) {
+                base[a] = (int)floorf(fc[a]);
+                fr[a] = fc[a] - floorf(fc[a]);
+              }
+              float rs0 = 0.f, rs1 = 0.f, rs2 = 0.f, rs3 = 0.f;
+              int sh = P.shift;
+              for (int dz = 0; dz < 2; dz++)
+                for (int dy = 0; dy < 2; dy++)
+                  for (int dx = 0; dx < 2; dx++) {
+                    int cx = base[0] + dx, cy = base[1] + dy, cz = base[2] + dz;
+                    int s = brickSlot(P, H, cx >> sh, cy >> sh, cz >> sh);
+                    float w = (dx ? fr[0] : 1.f - fr[0]) * (dy ? fr[1] : 1.f - fr[1]) * (dz ? fr[2] : 1.f - fr[2]);
+                    if (s >= 0) {
+                      size_t oo = (size_t)s * 4 * N + localCell(P, cx, cy, cz);
+                      rs0 += P.fldP[oo] * w;
+                      rs1 += P.fldP[oo + N] * w;
+                      rs2 += P.fldP[oo + 2 * N] * w;
+                      rs3 += P.fldP[oo + 3 * N] * w;
+                    }
+                  }
+              r0 = rs0;
+              r1 = rs1;
+              r3 = rs3;
+              float cl = a2 + 0.5f * (o2 - rs2);
+              lifetime = (cl < lmin || cl > lmax) ? a2 : cl;
+            } else {
+              r0 = sampleCells(P, H, P.fldP, 4, 0, fx / P.h, fy / P.h, fz / P.h);
+              r1 = sampleCells(P, H, P.fldP, 4, 1, fx / P.h, fy / P.h, fz / P.h);
+              r3 = sampleCells(P, H, P.fldP, 4, 3, fx / P.h, fy / P.h, fz / P.h);
+            }
+            float c0 = a0 + 0.5f * (o0 - r0), c1 = a1 + 0.5f * (o1 - r1), c3 = a3 + 0.5f * (o3 - r3);
+            tr[0] = (c0 < mn0 || c0 > mx0) ? a0 : c0;
+            tr[1] = (c1 < mn1 || c1 > mx1) ? a1 : c1;
+            tr[2] = clamp01(lifetime);
+            tr[3] = (c3 < mn3 || c3 > mx3) ? a3 : c3;
+          }
+        }
+        float lifetime = tr[2];
+        float prodS = 0.f, prodH = 0.f, injectedFuel = 0.f;
+        uint2 list = tileList(P, tile, 0);
+        for (uint32_t j = 0; j < list.y; j++) {
+          const FpEmitter& e = P.emitters[P.tileLists[list.x + j]];
+          float w = emitterWeight(e, px, py, pz);
+          if (w == 0.f) continue;
+          float2 var = burstVariation(e, px, py, pz, P.seedBits);
+          lifetime = fmaxf(lifetime, e.flame * w * var.y);
+          prodS += e.smoke * w * P.dt;
+          prodH += e.heat * var.x * w * P.dt;
+          injectedFuel += e.fuel * w * P.dt;
+        }
+        float remaining = 0.f, burned = 0.f;
+        if (P.fuelEnabled) {
+          remaining = tr[3] + injectedFuel;
+          if (tr[1] + prodH >= P.ignition) {
+            lifetime = fmaxf(lifetime, fminf(remaining, 1.f));
+            float unburned = remaining * expf(-P.burnRate * P.dt);
+            burned = remaining - unburned;
+            remaining = unburned;
+          }
+        }
+        // evaluateFlame (flame-common.wgsl:30-42)
+        float before = clamp01(lifetime);
+        float after = 0.f, f0 = 0.f, f1 = 0.f, f2 = 0.f;
+        if (before > 0.f) {
+          const FpFlame& F = P.flame;
+          after = fmaxf(0.f, before - F.dt / F.lifespan);
+          f0 = F.smoke * F.lifespan * rampIntegral(F, 0, after, before);
+          f1 = F.heat * F.lifespan * rampIntegral(F, 1, after, before);
+          f2 = F.expansion * (F.lifespan * rampIntegral(F, 2, after, before) / F.dt);
+        }
+        expansion = f2 + P.flame.expansion * burned / P.dt;
+        float dS = tr[0] * expf(-P.dissipation * P.dt) + (prodS + f0) * expf(-P.dissipation * P.dt * 0.5f);
+        float dH = tr[1] * expf(-P.cooling * P.dt) + (prodH + f1) * expf(-P.cooling * P.dt * 0.5f);
+        value[0] = fmaxf(dS, 0.f);
+        value[1] = fmaxf(dH, 0.f);
+        value[2] = after;
+        value[3] = remaining;
+        injected = prodS > 0.f || prodH > 0.f || lifetime > tr[2] || injectedFuel > 0.f;
+      }
+      // clearDormant (fluid-common.wgsl:8-13)
+      if (!injected && value[2] == 0.f && value[0] < 0.001f && value[1] < 0.001f && value[3] < 0.001f)
+        value[0] = value[1] = value[2] = value[3] = 0.f;
+      for (int k = 0; k < 4; k++) P.fldN[(slot * 4 + k) * N + c] = value[k];
+      P.expn[slot * N + c] = expansion;
+      if (expansion != 0.f) expands = true;
+      // holdsContent and contentSupport (fluid-content.wgsl:22-39).
+      if (fmaxf(fmaxf(value[0], value[2]), value[3]) > P.cutoff) {
+        if (!cvSampled) cv = velocityAt(P, H, P.vel, px, py, pz);
+        int idc[3] = {x, y, z};
+        float vv[3] = {cv.x, cv.y, cv.z};
+        bool low[3], high[3];
+        for (int a = 0; a < 3; a++) {
+          float side = (float)P.B;
+          float loc = (float)(idc[a] & (P.B - 1)) + 0.5f;
+          float pad = fminf(side, 2.f + fabsf(vv[a]) * P.dt / P.h);
+          low[a] = loc < pad;
+          high[a] = loc + pad >= side;
+        }
+        uint32_t row = 2u | (low[0] ? 1u : 0u) | (high[0] ? 4u : 0u);
+        uint32_t plane = (row << 3u) | (low[1] ? row : 0u) | (high[1] ? (row << 6u) : 0u);
+        busy |= (plane << 9u) | (low[2] ? plane : 0u) | (high[2] ? (plane << 18u) : 0u);
+      }
+    }
+    // recordContent (fluid-content.wgsl:43-64): one update per brick.
+    busy = __reduce_or_sync(0xffffffffu, busy);
+    uint32_t ex = __reduce_or_sync(0xffffffffu, (uint32_t)expands);
+    if ((threadIdx.x & 31) == 0) {
+      if (busy) atomicOr(&busyAll, busy);
+      if (ex) atomicOr(&expandsAll, 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t flags = 0;
+      if (busyAll) {
+        flags = FP_CONTENT | (busyAll << 3);
+        uint32_t l = id & 63u;
+        uint32_t bits = (1u << (l & 3u)) | (16u << ((l >> 2) & 3u)) | (256u << (l >> 4));
+        atomicOr(&P.activity[bricks + (id >> 6)], bits);
+      }
+      if (expandsAll) flags |= FP_EXPANDS;
+      if (flags) P.activity[id] |= flags;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// computeCurl (fluid-forces.wgsl:38-75) of the corrected velocity.
+__global__ void __launch_bounds__(THREADS) k_curl(const SimParams* __restrict__ Pp) {
+  const SimParams& P = *Pp;
+  __shared__ int nslot[27];
+  uint32_t total = P.counters->active;
+  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+    Home H = enterBrick(P, P.active[i], nslot);
+    size_t slot = (size_t)nslot[13];
+    const size_t N = P.N;
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int x, y, z;
+      cellOf(P, H, c, x, y, z);
+      auto cc = [&](int qx, int qy, int qz, int comp) {
+        int r[3] = {qx, qy, qz};
+        r[comp] -= 1;
+        return 0.5f * (cellAt(P, H, P.velC, 3, comp, qx, qy, qz) + cellAt(P, H, P.velC, 3, comp, r[0], r[1], r[2]));
+      };
+      float hh = 0.5f / P.h;
+      float dx0 = (cc(x + 1, y, z, 1) - cc(x - 1, y, z, 1)) * hh, dx1 = (cc(x + 1, y, z, 2) - cc(x - 1, y, z, 2)) * hh;
+      float dy0 = (cc(x, y + 1, z, 0) - cc(x, y - 1, z, 0)) * hh, dy1 = (cc(x, y + 1, z, 2) - cc(x, y - 1, z, 2)) * hh;
+      float dz0 = (cc(x, y, z + 1, 0) - cc(x, y, z - 1, 0)) * hh, dz1 = (cc(x, y, z + 1, 1) - cc(x, y, z - 1, 1)) * hh;
+      float c0 = dy1 - dz1, c1 = dz0 - dx1, c2 = dx0 - dy0;
+      P.curl[(slot * 4 + 0) * N + c] = c0;
+      P.curl[(slot * 4 + 1) * N + c] = c1;
+      P.curl[(slot * 4 + 2) * N + c] = c2;
+      P.curl[(slot * 4 + 3) * N + c] = sqrtf(c0 * c0 + c1 * c1 + c2 * c2);
+    }
+    __syncthreads();
+  }
+}
+
+// externalForces with coverage (force-fields.wgsl:312-365).
+FP_DEV float3 externalForces(const SimParams& P, int tile, float px, float py, float pz) {
+  float3 result = make_float3(0.f, 0.f, 0.f);
+  uint2 list = tileList(P, tile, 1);
+  for (uint32_t j = 0; j < list.y; j++) {
+    const FpForce& f = P.forces[P.tileLists[list.x + j]];
+    float weight = 1.f;
+    if (f.targeted != 0.f) {
+      float covered = 0.f;
+      for (int r = 0; r < (int)f.regionCount; r++) {
+        const FpRegion& g = P.regions[(int)f.regionFirst + r];
+        float dx = fabsf((px - g.center[0]) / fmaxf(g.size[0], 0.03f)),
+              dy = fabsf((py - g.center[1]) / fmaxf(g.size[1], 0.03f)),
+              dz = fabsf((pz - g.center[2]) / fmaxf(g.size[2], 0.03f));
+        float dist = g.box == 3.f ? fmaxf(dx, fmaxf(dy, dz)) : sqrtf(dx * dx + dy * dy + dz * dz);
+        covered = fmaxf(covered, 1.f - smooth(0.5f, 1.f, dist));
+      }
+      weight = covered;
+    }
+    if (weight == 0.f) continue;
+    float3 acc = make_float3(f.axis[0] * f.strength, f.axis[1] * f.strength, f.axis[2] * f.strength);
+    if (f.kind == 1.f) {
+      float qx = px * f.scale * 0.65f + P.seedF, qy = py * f.scale * 0.65f + -P.time * 0.7f,
+            qz = pz * f.scale * 0.65f + P.seedF * 0.25f;
+      float3 n1 = curlNoise(P, qx, qy, qz);
+      float3 n2 = curlNoise(P, qx * 2.03f + 13.7f, qy * 2.03f + 5.3f, qz * 2.03f + 19.1f);
+      acc = make_float3((n1.x + 0.45f * n2.x) * f.strength, (n1.y + 0.45f * n2.y) * f.strength,
+                        (n1.z + 0.45f * n2.z) * f.strength);
+    } else if (f.kind >= 2.f) {
+      float d[3] = {px - f.center[0], py - f.center[1], pz - f.center[2]};
+      float r[3] = {d[0], d[1], d[2]};
+      if (f.kind == 2.f) {
+        float dd = d[0] * f.axis[0] + d[1] * f.axis[1] + d[2] * f.axis[2];
+        for (int a = 0; a < 3; a++) r[a] -= f.axis[a] * dd;
+      }
+      float rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+      float distance = sqrtf(rr);
+      float radius = fmaxf(f.scale, 0.01f);
+      float dir[3];
+      for (int a = 0; a < 3; a++) dir[a] = r[a] / fmaxf(distance, radius * 0.25f);
+      float falloff = 1.f / (1.f + rr / (radius * radius));
+      if (f.kind == 2.f) {
+        float cr[3] = {f.axis[1] * dir[2] - f.axis[2] * dir[1], f.axis[2] * dir[0] - f.axis[0] * dir[2],
+                       f.axis[0] * dir[1] - f.axis[1] * dir[0]};
+        acc = make_float3((cr[0] * f.strength - dir[0] * f.inward + f.axis[0] * f.lift) * falloff,
+                          (cr[1] * f.strength - dir[1] * f.inward + f.axis[1] * f.lift) * falloff,
+                          (cr[2] * f.strength - dir[2] * f.inward + f.axis[2] * f.lift) * falloff);
+      } else {
+        acc = make_float3(dir[0] * f.strength * falloff, dir[1] * f.strength * falloff, dir[2] * f.strength * falloff);
+      }
+    }
+    result.x += acc.x * weight;
+    result.y += acc.y * weight;
+    result.z += acc.z * weight;
+  }
+  return result;
+}
+
+// cellForce / centerForce (fluid-forces.wgsl:79-118).
+FP_DEV float3 cellForce(const SimParams& P, const Home& H, int tile, int x, int y, int z) {
+  if (brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift) < 0) return make_float3(0.f, 0.f, 0.f);
+  float wx = ((float)x + 0.5f) * P.h, wy = ((float)y + 0.5f) * P.h, wz = ((float)z + 0.5f) * P.h;
+  if (solidAt(P, H, wx, wy, wz)) return make_float3(0.f, 0.f, 0.f);
+  // The evolved scalars of this step (the reference swaps field and corrected first).
+  float heat = cellAt(P, H, P.fldN, 4, 1, x, y, z), density = cellAt(P, H, P.fldN, 4, 0, x, y, z);
+  float3 conf = make_float3(0.f, 0.f, 0.f);
+  if (P.vorticity != 0.f) {
+    float c0 = cellAt(P, H, P.curl, 4, 0, x, y, z), c1 = cellAt(P, H, P.curl, 4, 1, x, y, z),
+          c2 = cellAt(P, H, P.curl, 4, 2, x, y, z);
+    float e0 = cellAt(P, H, P.curl, 4, 3, x + 1, y, z) - cellAt(P, H, P.curl, 4, 3, x - 1, y, z);
+    float e1 = cellAt(P, H, P.curl, 4, 3, x, y + 1, z) - cellAt(P, H, P.curl, 4, 3, x, y - 1, z);
+    float e2 = cellAt(P, H, P.curl, 4, 3, x, y, z + 1) - cellAt(P, H, P.curl, 4, 3, x, y, z - 1);
+    float len = sqrtf(e0 * e0 + e1 * e1 + e2 * e2) + 0.0001f;
+    float n0 = e0 / len, n1 = e1 / len, n2 = e2 / len;
+    float s = P.vorticity * P.h;
+    conf = make_float3((n1 * c2 - n2 * c1) * s, (n2 * c0 - n0 * c2) * s, (n0 * c1 - n1 * c0) * s);
+  }
+  float3 ext = externalForces(P, tile, wx, wy, wz);
+  return make_float3(conf.x + ext.x, conf.y + ext.y + (P.buoyancy * heat - P.smokeWeight * density), conf.z + ext.z);
+}
+
+// sourceVelocity (fluid-forces.wgsl:122-149).
+FP_DEV float sourceVelocity(const SimParams& P, int tile, float value, float fx, float fy, float fz, int comp) {
+  float result = value;
+  uint2 list = tileList(P, tile, 0);
+  for (uint32_t j = 0; j < list.y; j++) {
+    const FpEmitter& e = P.emitters[P.tileLists[list.x + j]];
+    if (e.response == 0.f) continue;
+    float w = emitterWeight(e, fx, fy, fz);
+    if (w == 0.f) continue;
+    float radial = 0.f;
+    if (e.outward != 0.f) {
+      float d0 = fx - e.pos[0], d1 = fy - e.pos[1], d2 = fz - e.pos[2];
+      float len = sqrtf(d0 * d0 + d1 * d1 + d2 * d2);
+      float dc = comp == 0 ? d0 : (comp == 1 ? d1 : d2);
+      radial = dc / fmaxf(len, 1e-6f) * e.outward;
+    }
+    result = mixf(result, e.vel[comp] + radial, 1.f - expf(-e.response * w * P.dt));
+  }
+  return result;
+}
+
+// applyForces (fluid-forces.wgsl:151-182): centre forces of the brick and of the cells past
+// it on one axis, staged in shared memory, averaged to the faces.
+__global__ void __launch_bounds__(THREADS) k_forces(const SimParams* __restrict__ Pp) {
+  const SimParams& P = *Pp;
+  __shared__ int nslot[27];
+  extern __shared__ float3 forceTile[];  // (B+1)^3
+  uint32_t total = P.counters->active;
+  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+    uint32_t id = P.active[i];
+    Home H = enterBrick(P, id, nslot);
+    size_t slot = (size_t)nslot[13];
+    const size_t N = P.N;
+    int tile = (int)(id >> 6);
+    int E = P.B + 1;
+    for (int q = threadIdx.x; q < E * E * E; q += blockDim.x) {
+      int lx = q % E, ly = (q / E) % E, lz = q / (E * E);
+      if ((lx == P.B) + (ly == P.B) + (lz == P.B) >= 2) continue;
+      forceTile[q] = cellForce(P, H, tile, H.bx * P.B + lx, H.by * P.B + ly, H.bz * P.B + lz);
+    }
+    __syncthreads();
+    float decay = expf(-P.damping * P.dt);
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int x, y, z;
+      cellOf(P, H, c, x, y, z);
+      int lx = x & (P.B - 1), ly = y & (P.B - 1), lz = z & (P.B - 1);
+      int t = (lz * E + ly) * E + lx;
+      float3 F0 = forceTile[t];
+      float f[3] = {0.5f * (F0.x + forceTile[t + 1].x), 0.5f * (F0.y + forceTile[t + E].y),
+                    0.5f * (F0.z + forceTile[t + E * E].z)};
+      float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+      float out[3];
+      for (int a = 0; a < 3; a++) {
+        float v = P.velC[(slot * 3 + a) * N + c] * decay + P.dt * f[a];
+        float face[3] = {px, py, pz};
+        face[a] += 0.5f * P.h;
+        out[a] = sourceVelocity(P, tile, v, face[0], face[1], face[2], a);
+      }
+      // enforceFaces (fluid-forces.wgsl:15-31)
+      if (solidAt(P, H, px, py, pz)) {
+        out[0] = out[1] = out[2] = 0.f;
+      } else {
+        if (solidAt(P, H, px + P.h, py, pz)) out[0] = 0.f;
+        if (solidAt(P, H, px, py + P.h, pz)) out[1] = 0.f;
+        if (solidAt(P, H, px, py, pz + P.h)) out[2] = 0.f;
+      }
+      for (int a = 0; a < 3; a++) P.velF[(slot * 3 + a) * N + c] = out[a];
+    }
+    __syncthreads();
+  }
+}
+
+// pressureUnknown (fluid-forces.wgsl:210-226): the cell's brick and those of its negative
+// neighbours compute.
+FP_DEV bool pressureUnknown(const SimParams& P, const Home& H, int x, int y, int z) {
+  int sh = P.shift;
+  int lx = (x - 1) >> sh, ly = (y - 1) >> sh, lz = (z - 1) >> sh, hx = x >> sh, hy = y >> sh, hz = z >> sh;
+  if (P.ground) ly = max(ly, 0);
+  for (int bz = lz; bz <= hz; bz++)
+    for (int by = ly; by <= hy; by++)
+      for (int bx = lx; bx <= hx; bx++)
+        if (brickSlot(P, H, bx, by, bz) < 0) return false;
+  return true;
+}
+
+// computeDivergence (fluid-forces.wgsl:184-203) and the finest level's first Jacobi
+// iterate from zero (initializePressure, pressure.wgsl:485-505), fused: the iterate needs
+// only the cell's own right-hand side.
+__global__ void __launch_bounds__(THREADS) k_divergence(const SimParams* __restrict__ Pp, float* __restrict__ pOut) {
+  const SimParams& P = *Pp;
+  __shared__ int nslot[27];
+  uint32_t total = P.counters->active;
+  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+    Home H = enterBrick(P, P.active[i], nslot);
+    size_t slot = (size_t)nslot[13];
+    const size_t N = P.N;
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int x, y, z;
+      cellOf(P, H, c, x, y, z);
+      float d = (P.velF[(slot * 3 + 0) * N + c] - cellAt(P, H, P.velF, 3, 0, x - 1, y, z)) / P.h +
+                (P.velF[(slot * 3 + 1) * N + c] - cellAt(P, H, P.velF, 3, 1, x, y - 1, z)) / P.h +
+                (P.velF[(slot * 3 + 2) * N + c] - cellAt(P, H, P.velF, 3, 2, x, y, z - 1)) / P.h;
+      float rhs = P.h * P.h * (d - P.expn[slot * N + c]);
+      P.div[slot * N + c] = rhs;
+      uint8_t t = P.topo[0][slot * N + c];
+      float first = 0.f;
+      if (!(t & FP_STORED_SOLID) && pressureUnknown(P, H, x, y, z)) {
+        float diag = (float)((t >> 0) & 1) + (float)((t >> 1) & 1) + ((float)((t >> 2) & 1) + (float)((t >> 3) & 1)) +
+                     ((float)((t >> 4) & 1) + (float)((t >> 5) & 1));
+        first = mixf(0.f, (0.f - rhs) / fmaxf(diag, 1e-12f), 0.8f);
+      }
+      pOut[slot * N + c] = first;
+    }
+    __syncthreads();
+  }
+}
+
+// project (fluid-forces.wgsl:228-262) into the velocity pool of the next step.
+__global__ void __launch_bounds__(THREADS) k_project(const SimParams* __restrict__ Pp, const float* __restrict__ p) {
+  const SimParams& P = *Pp;
+  __shared__ int nslot[27];
+  uint32_t total = P.counters->active;
+  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+    Home H = enterBrick(P, P.active[i], nslot);
+    size_t slot = (size_t)nslot[13];
+    const size_t N = P.N;
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int x, y, z;
+      cellOf(P, H, c, x, y, z);
+      float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+      float res[3] = {0.f, 0.f, 0.f};
+      if (!solidAt(P, H, px, py, pz)) {
+        float cp = p[slot * N + c];
+        bool pu = pressureUnknown(P, H, x, y, z);
+        for (int a = 0; a < 3; a++) {
+          int n[3] = {x, y, z};
+          n[a] += 1;
+          float v = P.velF[(slot * 3 + a) * N + c];
+          float nx = ((float)n[0] + 0.5f) * P.h, ny = ((float)n[1] + 0.5f) * P.h, nz = ((float)n[2] + 0.5f) * P.h;
+          if (solidAt(P, H, nx, ny, nz)) {
+            res[a] = 0.f;
+          } else if (!pu && !pressureUnknown(P, H, n[0], n[1], n[2])) {
+            res[a] = 0.f;
+          } else {
+            float pn = cellAt(P, H, p, 1, 0, n[0], n[1], n[2]);
+            res[a] = v - (pn - cp) / P.h;
+          }
+        }
+      }
+      for (int a = 0; a < 3; a++) P.velP[(slot * 3 + a) * N + c] = res[a];
+    }
+    __syncthreads();
+  }
+}
+
+// buildNoise (curl-noise.wgsl:34-45) once: analytic curl of hashed value noise, rounded to
+// half precision as the reference's rgba16float table holds it.
+__device__ float nhash(int px, int py, int pz) {
+  uint32_t v0 = ((uint32_t)px & 15u) * 1664525u + 1013904223u, v1 = ((uint32_t)py & 15u) * 1664525u + 1013904223u,
+           v2 = ((uint32_t)pz & 15u) * 1664525u + 1013904223u;
+  v0 += v1 * v2;
+  v1 += v2 * v0;
+  v2 += v0 * v1;
+  v0 ^= v0 >> 16u;
+  v1 ^= v1 >> 16u;
+  v2 ^= v2 >> 16u;
+  v0 += v1 * v2;
+  v1 += v2 * v0;
+  v2 += v0 * v1;
+  return (float)(v0 >> 8u) / 16777216.f;
+}
+__device__ float3 noiseGradient(float px, float py, float pz) {
+  float p[3] = {px, py, pz}, f[3], s[3], ds[3];
+  int i[3];
+  for (int a = 0; a < 3; a++) {
+    i[a] = (int)floorf(p[a]);
+    f[a] = p[a] - floorf(p[a]);
+    s[a] = f[a] * f[a] * f[a] * (f[a] * (f[a] * 6.f - 15.f) + 10.f);
+    ds[a] = 30.f * f[a] * f[a] * (f[a] - 1.f) * (f[a] - 1.f);
+  }
+  float a = nhash(i[0], i[1], i[2]), b = nhash(i[0] + 1, i[1], i[2]), c = nhash(i[0], i[1] + 1, i[2]),
+        d = nhash(i[0] + 1, i[1] + 1, i[2]), e = nhash(i[0], i[1], i[2] + 1), f1 = nhash(i[0] + 1, i[1], i[2] + 1),
+        g = nhash(i[0], i[1] + 1, i[2] + 1), h = nhash(i[0] + 1, i[1] + 1, i[2] + 1);
+  return make_float3(mixf(mixf(b - a, d - c, s[1]), mixf(f1 - e, h - g, s[1]), s[2]) * ds[0],
+                     mixf(mixf(c - a, d - b, s[0]), mixf(g - e, h - f1, s[0]), s[2]) * ds[1],
+                     mixf(mixf(e - a, f1 - b, s[0]), mixf(g - c, h - d, s[0]), s[1]) * ds[2]);
+}
+__global__ void k_noise(float4* __restrict__ out) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= 64 * 64 * 64) return;
+  int x = idx & 63, y = (idx >> 6) & 63, z = idx >> 12;
+  float px = ((float)x + 0.5f) / 64.f * 16.f, py = ((float)y + 0.5f) / 64.f * 16.f, pz = ((float)z + 0.5f) / 64.f * 16.f;
+  float3 dx = noiseGradient(px, py, pz), dy = noiseGradient(px + 7.1f, py + 3.7f, pz + 11.3f),
+         dz = noiseGradient(px + 5.2f, py + 7.9f, pz + 9.5f);
+  float cx = dz.y - dy.z, cy = dx.z - dz.x, cz = dy.x - dx.y;
+  out[idx] = make_float4(__half2float(__float2half_rn(cx)), __half2float(__float2half_rn(cy)),
+                         __half2float(__float2half_rn(cz)), 0.f);
+}
+
+}  // namespace
+
+void fp_launch_predict(const SimParams* dP, int sms, cudaStream_t st) { k_predict<<<sms * 4, THREADS, 0, st>>>(dP); }
+void fp_launch_correct_evolve(const SimParams* dP, int sms, cudaStream_t st) {
+  k_correct_evolve<<<sms * 4, THREADS, 0, st>>>(dP);
+}
+void fp_launch_curl(const SimParams* dP, int sms, cudaStream_t st) { k_curl<<<sms * 4, THREADS, 0, st>>>(dP); }
+void fp_launch_forces(const SimParams* dP, int B, int sms, cudaStream_t st) {
+  size_t smem = (size_t)(B + 1) * (B + 1) * (B + 1) * sizeof(float3);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_forces, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_forces<<<sms * 4, THREADS, smem, st>>>(dP);
+}
+void fp_launch_divergence(const SimParams* dP, float* pOut, int sms, cudaStream_t st) {
+  k_divergence<<<sms * 4, THREADS, 0, st>>>(dP, pOut);
+}
+void fp_launch_project(const SimParams* dP, const float* p, int sms, cudaStream_t st) {
+  k_project<<<sms * 4, THREADS, 0, st>>>(dP, p);
+}
+void fp_launch_noise(float4* noise, cudaStream_t st) { k_noise<<<64 * 64 * 64 / 256, 256, 0, st>>>(noise); }

@@ -1,0 +1,149 @@
+// Device-visible records of one simulation: the per-step parameters, the packed scene
+// and the addresses of every table and pool. The host engine (fp_engine.cpp) fills a
+// SimParams per simulation per step and copies it to the device; every kernel reads it.
+//
+// HBM layout (per simulation)
+//   per tile slot      tileRec int4 (x,y,z,state), tileNbr int[27]
+//   tile hash          int4 (x,y,z,slot) open addressing, power-of-two size
+//   per brick id       pages, entries, state, activity (+ per tile), records int[28]
+//   per pool slot      [slot][channel][cell] pools, cells x fastest in a brick:
+//                        vel/velA/velB 3ch, curl 4ch, fld/fldA/fldB 4ch, expn, div 1ch,
+//                        vmin/vmax 3ch, scalar bounds 8ch, donors 3 x u16, solids bits
+//   multigrid          level 0: p[2] and topology per slot; brick levels 1.. per slot;
+//                        tile levels per tile slot
+#pragma once
+#include <stdint.h>
+
+#define FP_MAX_LEVELS 8
+#define FP_RECORD_WORDS 28
+#define FP_FRESH_ENTRY 0x2000000
+#define FP_FRESH_SLOT 0x80000000u
+
+// Activity flags (fluid-content.wgsl:11-13) and brick state bits (fluid-allocation.wgsl:38-41).
+#define FP_CONTENT 1u
+#define FP_EXPANDS 2u
+#define FP_MAY_EXPAND 4u
+#define FP_BRICK_FREES 8u
+#define FP_BRICK_REQUESTS 16u
+#define FP_STORED_SOLID 64u
+
+// Emitter (fluid-common.wgsl:34-40), 80 bytes as the reference packs it.
+struct FpEmitter {
+  float pos[3];
+  float enabled;
+  float size[3];
+  float box;
+  float flame, heat, smoke, response;
+  float vel[3];
+  float outward;
+  float period, strength, fuel, pad;
+};
+
+// Collider (fluid-common.wgsl:45-51): kind 0 ellipsoid, 1 box, 2 mesh mask.
+struct FpCollider {
+  float center[3];
+  float kind;
+  float extent[4];
+  float axes[3][4];  // columns
+  int lo[3];
+  int first;
+  int size[4];
+};
+
+// Force rows (force-fields.wgsl:266-272).
+struct FpForce {
+  float axis[3];
+  float strength;
+  float center[3];
+  float kind;
+  float scale, lift, inward, pad0;
+  float regionFirst, regionCount, hasMesh, targeted;
+  float reserved[4];
+};
+struct FpRegion {
+  float center[3];
+  float box;  // 3 box, 1 sphere
+  float size[4];
+};
+
+// FlameParams (flame-common.wgsl:2-6) and its ramps.
+struct FpFlame {
+  float dt, lifespan, smoke, heat;
+  float expansion, pad[3];
+  int counts[4];
+  float knots[3][8][2];
+};
+
+// Work counters the allocation writes and every later kernel reads.
+struct FpCounters {
+  uint32_t active;     // computing bricks this step
+  uint32_t fresh;      // slots granted this step
+  int32_t freeCount;   // free stack height
+  uint32_t failures;   // failed allocations since the last measurement
+  uint32_t frees, requests, granted, pad;
+};
+
+struct SimParams {
+  // lattice
+  int B, shift, N, W;  // cells per brick side, log2, cells per brick, solid words per slot
+  int brickLevels, bottom;
+  float h, invH, dt;
+  // dynamics (Params, fluid-common.wgsl:21-32)
+  float buoyancy, cooling, smokeWeight, damping, dissipation, vorticity;
+  float cutoff, time, seedF;
+  uint32_t seedBits;
+  int lifetimeZero, fuelEnabled;
+  float ignition, burnRate;
+  int ground, colliderCount, maccormack, solidsAll;
+  int held;
+  uint32_t slots;
+  // directory
+  int capacity;  // tile slots; brick ids = capacity * 64
+  const int4* tileRec;
+  const int* tileNbr;
+  const int4* hash;
+  uint32_t hashMask;
+  // per brick id
+  int* pages;
+  int* entries;
+  uint32_t* state;
+  uint32_t* activity;
+  int* records;
+  uint32_t* blockCounts;  // per 256 ids: frees, requests, listedWithPage
+  // lists
+  uint32_t* active;  // ascending brick ids
+  uint32_t* zeroList;  // granted: id, slot
+  uint32_t* freeStack;
+  FpCounters* counters;
+  // pools
+  float* vel;   // velocity at the start of the step
+  float* velP;  // predictor, then the projected velocity
+  float* velC;  // corrected
+  float* velF;  // forced
+  float* curl;
+  float* fld;   // scalars at the start of the step
+  float* fldP;  // predictor
+  float* fldN;  // evolved
+  float* expn;
+  float* div;
+  float* vmin;
+  float* vmax;
+  float* sb;
+  uint16_t* donors;
+  uint32_t* solids;
+  // multigrid
+  float* p0[2];
+  int latest;  // p0 index of the previous solution
+  uint8_t* topo[FP_MAX_LEVELS];
+  float* lp[FP_MAX_LEVELS][2];
+  float* lrhs[FP_MAX_LEVELS];
+  // scene
+  const FpEmitter* emitters;
+  const FpCollider* colliders;
+  const uint32_t* masks;
+  const FpForce* forces;
+  const FpRegion* regions;
+  const uint32_t* tileLists;  // 8-word header per tile slot, then indices
+  FpFlame flame;
+  const float4* noise;  // 64^3 curl noise
+};

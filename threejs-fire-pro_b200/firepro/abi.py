@@ -1,0 +1,216 @@
+"""ctypes mirror of include/firepro.h and the loader of the CUDA library.
+
+The structs follow the C header field for field. `load_library()` opens the in-tree
+`libfirepro.so` built by `build.py`; it raises when the library is missing rather than
+falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+PACKAGE_DIR = Path(__file__).resolve().parent
+LIB_PATH = PACKAGE_DIR.parent / "lib" / "libfirepro.so"
+
+FP_OK = 0
+FP_EINVAL = -1
+FP_ENOMEM = -2
+FP_ELIMIT = -3
+FP_EDEVICE = -4
+FP_ETIMEOUT = -5
+FP_EUNSUPPORTED = -6
+
+FP_PRECISION_FP32 = 0
+FP_PRECISION_MIXED = 1
+
+FP_SHAPE_SPHERE = 0
+FP_SHAPE_BOX = 1
+FP_SHAPE_MESH = 2
+
+FP_FORCE_WIND = 0
+FP_FORCE_TURBULENCE = 1
+FP_FORCE_VORTEX = 2
+FP_FORCE_RADIAL = 3
+
+FP_FIELD_VELOCITY = 0
+FP_FIELD_SCALARS = 1
+FP_FIELD_EXPANSION = 2
+FP_FIELD_PRESSURE = 3
+FP_FIELD_DIVERGENCE = 4
+FP_FIELD_CURL = 5
+FIELD_CHANNELS = {0: 3, 1: 4, 2: 1, 3: 1, 4: 1, 5: 4}
+
+FP_TABLE_ENTRIES = 0
+FP_TABLE_PAGES = 1
+FP_TABLE_STATE = 2
+FP_TABLE_ACTIVITY = 3
+FP_TABLE_RECORDS = 4
+FP_TABLE_FREE = 5
+FP_TABLE_ACTIVE = 6
+FP_TABLE_SOLIDS = 7
+FP_TABLE_TILES = 8
+
+
+class fp_grid(C.Structure):
+    _fields_ = [
+        ("voxel_size", C.c_float),
+        ("velocity_divisor", C.c_int32),
+        ("brick_size", C.c_int32),
+        ("smoke_divisor", C.c_int32),
+        ("scalar_maccormack", C.c_int32),
+        ("precision", C.c_int32),
+        ("voxel_budget", C.c_double),
+    ]
+
+
+class fp_settings(C.Structure):
+    _fields_ = [
+        ("buoyancy", C.c_float),
+        ("smoke_weight", C.c_float),
+        ("velocity_damping", C.c_float),
+        ("cooling", C.c_float),
+        ("dissipation", C.c_float),
+        ("vorticity", C.c_float),
+        ("seed", C.c_uint32),
+    ]
+
+
+class fp_flame_ramp(C.Structure):
+    _fields_ = [("count", C.c_uint32), ("knots", (C.c_float * 2) * 8)]
+
+
+class fp_combustion(C.Structure):
+    _fields_ = [
+        ("lifespan", C.c_float),
+        ("smoke_rate", C.c_float),
+        ("heat_rate", C.c_float),
+        ("expansion_rate", C.c_float),
+        ("ramps", fp_flame_ramp * 3),
+    ]
+
+
+class fp_fuel(C.Structure):
+    _fields_ = [("enabled", C.c_int32), ("ignition_heat", C.c_float), ("burn_rate", C.c_float)]
+
+
+class fp_source(C.Structure):
+    _fields_ = [
+        ("id", C.c_uint64),
+        ("shape", C.c_int32),
+        ("position", C.c_float * 3),
+        ("size", C.c_float * 3),
+        ("flame", C.c_float),
+        ("heat_rate", C.c_float),
+        ("smoke_rate", C.c_float),
+        ("fuel_rate", C.c_float),
+        ("velocity", C.c_float * 3),
+        ("velocity_response", C.c_float),
+        ("outward_speed", C.c_float),
+        ("has_variation", C.c_int32),
+        ("variation_period", C.c_float),
+        ("variation_strength", C.c_float),
+    ]
+
+
+class fp_force(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("vector", C.c_float * 3),
+        ("center", C.c_float * 3),
+        ("strength", C.c_float),
+        ("scale", C.c_float),
+        ("lift", C.c_float),
+        ("inward", C.c_float),
+        ("targeted", C.c_int32),
+        ("first_target", C.c_uint32),
+        ("target_count", C.c_uint32),
+    ]
+
+
+class fp_collider(C.Structure):
+    _fields_ = [
+        ("shape", C.c_int32),
+        ("position", C.c_float * 3),
+        ("size", C.c_float * 3),
+        ("axes", (C.c_float * 3) * 3),
+        ("lo", C.c_int32 * 3),
+        ("dims", C.c_int32 * 3),
+        ("mask_offset", C.c_uint32),
+    ]
+
+
+class fp_frame(C.Structure):
+    _fields_ = [
+        ("simulation", fp_settings),
+        ("combustion", fp_combustion),
+        ("fuel", fp_fuel),
+        ("sources", C.POINTER(fp_source)),
+        ("source_count", C.c_uint32),
+        ("forces", C.POINTER(fp_force)),
+        ("force_count", C.c_uint32),
+        ("force_targets", C.POINTER(fp_source)),
+        ("force_target_count", C.c_uint32),
+        ("colliders", C.POINTER(fp_collider)),
+        ("collider_count", C.c_uint32),
+        ("collider_masks", C.POINTER(C.c_uint32)),
+        ("collider_mask_words", C.c_uint32),
+    ]
+
+
+class fp_stats(C.Structure):
+    _fields_ = [
+        ("time", C.c_double),
+        ("steps", C.c_uint64),
+        ("active_bricks", C.c_uint32),
+        ("brick_cells", C.c_uint32),
+        ("pool_limited", C.c_int32),
+        ("pool_slots", C.c_uint32),
+        ("used_slots", C.c_uint32),
+        ("tiles", C.c_uint32),
+        ("tile_capacity", C.c_uint32),
+        ("failures", C.c_uint32),
+        ("memory_bytes", C.c_uint64),
+        ("last_vcycles", C.c_uint32),
+        ("last_residual", C.c_double),
+    ]
+
+
+# Exported symbols of libfirepro.so (include/firepro.h), with their ctypes signatures.
+SIGNATURES = {
+    "fp_abi_version": (C.c_int, []),
+    "fp_last_error": (C.c_char_p, [C.c_void_p]),
+    "fp_sim_create": (C.c_int, [C.POINTER(fp_grid), C.c_int, C.POINTER(C.c_void_p)]),
+    "fp_sim_destroy": (C.c_int, [C.c_void_p]),
+    "fp_sim_reset": (C.c_int, [C.c_void_p]),
+    "fp_sim_set_runtime": (C.c_int, [C.c_void_p, C.c_float, C.c_double, C.c_int]),
+    "fp_sim_step": (C.c_int, [C.c_void_p, C.POINTER(fp_frame), C.c_float]),
+    "fp_sim_synchronize": (C.c_int, [C.c_void_p]),
+    "fp_sim_stats": (C.c_int, [C.c_void_p, C.POINTER(fp_stats)]),
+    "fp_sim_read_field": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.c_size_t]),
+    "fp_sim_read_table": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_size_t)]),
+    "fp_sim_read_bricks": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint32)]),
+}
+
+_lib = None
+
+
+def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Open libfirepro.so and declare every exported signature. Raises if it is absent."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path is not None else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(
+            f"The CUDA library {p} is missing: build it with "
+            "`python threejs-fire-pro_b200/build.py` (or __graft_entry__.build())."
+        )
+    lib = C.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib

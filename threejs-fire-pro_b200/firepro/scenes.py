@@ -1,0 +1,227 @@
+"""Seeded synthetic scenes that drive the step through the C ABI.
+
+Each scene yields one `fp_frame` per step, built the way `FireSimulation.step` builds its
+`SimulationFrame` (src/library/FireSimulation.ts:455-519): settings, combustion, fuel,
+sources, forces and colliders as they are at that step. No dataset is involved; every
+number derives from the scene's seed.
+
+Scenes
+  single_plume  — one sphere emitter (r = 0.25 m at y = 0.2 m) injecting heat 1.0/s and fuel
+                  0.8/s with a 3-octave value-noise jitter of its rates, over a 6x6x6-brick
+                  block held by a zero-rate box source; buoyancy 1.5, vorticity 0.3,
+                  combustion on; 8^3-cell bricks of 2.5 cm voxels.
+  large_scene   — three seeded sphere/box emitters, a radial burst at step 30 (r = 0.5 m,
+                  outward 20 m/s), 2 m/s turbulence, one sphere and one box collider; grows
+                  to thousands of bricks.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+from . import abi
+
+# DEFAULT_FLAME_SETTINGS ramps (src/engine/flame.ts:16-40).
+DEFAULT_RAMPS = {
+    "smoke": [(0.0, 0.0), (0.2, 1.0), (0.5, 0.0), (1.0, 0.0)],
+    "heat": [(0.0, 0.0), (0.2, 1.0), (1.0, 1.0)],
+    "expansion": [(0.0, 0.0), (0.5, 0.0), (0.75, 1.0), (1.0, 1.0)],
+}
+
+
+def combustion(lifespan=1.2, smoke_rate=2.0, heat_rate=4.0, expansion_rate=1.0, ramps=None) -> abi.fp_combustion:
+    """`FlameSettings` with the reference's default ramps (flame.ts:16-40)."""
+    c = abi.fp_combustion()
+    c.lifespan, c.smoke_rate, c.heat_rate, c.expansion_rate = lifespan, smoke_rate, heat_rate, expansion_rate
+    ramps = ramps or DEFAULT_RAMPS
+    for i, name in enumerate(("smoke", "heat", "expansion")):
+        knots = ramps[name]
+        c.ramps[i].count = len(knots)
+        for k, (x, y) in enumerate(knots):
+            c.ramps[i].knots[k][0] = x
+            c.ramps[i].knots[k][1] = y
+    return c
+
+
+def settings(buoyancy=1.6, smoke_weight=0.12, damping=0.1, cooling=0.62, dissipation=0.35, vorticity=3.2, seed=1):
+    """`SimulationSettings` with the library defaults (src/library/options.ts:324-361)."""
+    s = abi.fp_settings()
+    s.buoyancy, s.smoke_weight, s.velocity_damping = buoyancy, smoke_weight, damping
+    s.cooling, s.dissipation, s.vorticity, s.seed = cooling, dissipation, vorticity, seed
+    return s
+
+
+def source(id, shape="sphere", position=(0, 0, 0), size=(0.3, 0.3, 0.3), flame=0.0, heat=0.0, smoke=0.0, fuel=0.0,
+           velocity=(0, 0, 0), response=0.0, outward=0.0, variation=None) -> abi.fp_source:
+    s = abi.fp_source()
+    s.id = id
+    s.shape = {"sphere": abi.FP_SHAPE_SPHERE, "box": abi.FP_SHAPE_BOX, "mesh": abi.FP_SHAPE_MESH}[shape]
+    s.position[:] = position
+    s.size[:] = size
+    s.flame, s.heat_rate, s.smoke_rate, s.fuel_rate = flame, heat, smoke, fuel
+    s.velocity[:] = velocity
+    s.velocity_response = response
+    s.outward_speed = outward
+    if variation is not None:
+        s.has_variation = 1
+        s.variation_period, s.variation_strength = variation
+    return s
+
+
+def force(kind, vector=(0, 1, 0), center=(0, 0, 0), strength=1.0, scale=1.0, lift=0.0, inward=0.0,
+          targeted=False, first_target=0, target_count=0) -> abi.fp_force:
+    f = abi.fp_force()
+    f.type = {"wind": 0, "turbulence": 1, "vortex": 2, "radial": 3}[kind]
+    f.vector[:] = vector
+    f.center[:] = center
+    f.strength, f.scale, f.lift, f.inward = strength, scale, lift, inward
+    f.targeted = int(targeted)
+    f.first_target, f.target_count = first_target, target_count
+    return f
+
+
+def collider(shape, position=(0, 0, 0), size=(0.2, 0.2, 0.2), axes=((1, 0, 0), (0, 1, 0), (0, 0, 1))):
+    c = abi.fp_collider()
+    c.shape = {"sphere": abi.FP_SHAPE_SPHERE, "box": abi.FP_SHAPE_BOX}[shape]
+    c.position[:] = position
+    c.size[:] = size
+    for a in range(3):
+        c.axes[a][:] = axes[a]
+    return c
+
+
+def _hash01(i: int, seed: int) -> float:
+    h = (i * 374761393 + seed * 668265263) & 0xFFFFFFFF
+    h = ((h ^ (h >> 13)) * 1274126177) & 0xFFFFFFFF
+    h ^= h >> 16
+    return (h & 0xFFFFFF) / float(1 << 24)
+
+
+def value_noise_1d(t: float, seed: int, octaves: int = 3) -> float:
+    """Seeded fractal value noise in [-1, 1]: `octaves` octaves, gain 0.5, lacunarity 2."""
+    total, norm, amp, freq = 0.0, 0.0, 1.0, 1.0
+    for o in range(octaves):
+        x = t * freq
+        i = math.floor(x)
+        f = x - i
+        s = f * f * (3 - 2 * f)
+        a = _hash01(i, seed + 101 * o)
+        b = _hash01(i + 1, seed + 101 * o)
+        total += amp * (2.0 * (a + (b - a) * s) - 1.0)
+        norm += amp
+        amp *= 0.5
+        freq *= 2.0
+    return total / norm
+
+
+@dataclass
+class FrameData:
+    """One step's frame and the ctypes arrays it points into (kept alive with it)."""
+
+    frame: abi.fp_frame
+    keep: list = field(default_factory=list)
+
+
+def make_frame(sim_settings, comb, fuel_enabled, sources, forces=(), targets=(), colliders=(), masks=(),
+               ignition=0.5, burn_rate=4.0) -> FrameData:
+    f = abi.fp_frame()
+    f.simulation = sim_settings
+    f.combustion = comb
+    f.fuel.enabled = int(fuel_enabled)
+    f.fuel.ignition_heat = ignition
+    f.fuel.burn_rate = burn_rate
+    keep = []
+
+    def arr(typ, items):
+        a = (typ * max(1, len(items)))(*items)
+        keep.append(a)
+        return C.cast(a, C.POINTER(typ)), len(items)
+
+    f.sources, f.source_count = arr(abi.fp_source, list(sources))
+    f.forces, f.force_count = arr(abi.fp_force, list(forces))
+    f.force_targets, f.force_target_count = arr(abi.fp_source, list(targets))
+    f.colliders, f.collider_count = arr(abi.fp_collider, list(colliders))
+    f.collider_masks, f.collider_mask_words = arr(C.c_uint32, list(masks))
+    return FrameData(f, keep)
+
+
+class Scene:
+    """A seeded scene: `grid()` for creation, `frame(step)` for every step."""
+
+    name = "scene"
+    voxel_size = 0.025
+    brick_size = 8
+    steps = 120
+
+    def grid(self, precision=abi.FP_PRECISION_FP32, budget=8e6, maccormack=True) -> abi.fp_grid:
+        g = abi.fp_grid()
+        g.voxel_size = self.voxel_size
+        g.velocity_divisor = 1
+        g.brick_size = self.brick_size
+        g.smoke_divisor = 1
+        g.scalar_maccormack = int(maccormack)
+        g.precision = precision
+        g.voxel_budget = budget
+        return g
+
+    def frame(self, step: int) -> FrameData:
+        raise NotImplementedError
+
+
+class SinglePlume(Scene):
+    """The single-simulation plume: 6x6x6-brick starting block around one jittered emitter."""
+
+    name = "single_plume"
+    steps = 120
+
+    def __init__(self, seed: int = 1):
+        self.seed = seed
+        self.settings = settings(buoyancy=1.5, vorticity=0.3, seed=seed)
+        self.comb = combustion()
+
+    def frame(self, step: int) -> FrameData:
+        j = 1.0 + 0.25 * value_noise_1d(step / 12.0, self.seed)
+        plume = source(1, "sphere", (0.0, 0.2, 0.0), (0.25, 0.25, 0.25), flame=0.0, heat=1.0 * j, fuel=0.8 * j)
+        # A zero-rate box whose allocation reach (sourceNear: extent + 2 voxels) covers exactly
+        # bricks -3..2 in x and z and 0..5 in y: the 6x6x6-brick starting block.
+        block = source(2, "box", (0.0, 0.6, 0.0), (0.45, 0.45, 0.45))
+        return make_frame(self.settings, self.comb, True, [plume, block])
+
+
+class LargeScene(Scene):
+    """Three seeded emitters, a burst at step 30, turbulence and two colliders."""
+
+    name = "large_scene"
+    steps = 600
+
+    def __init__(self, seed: int = 1):
+        self.seed = seed
+        self.settings = settings(buoyancy=1.6, vorticity=1.0, seed=seed)
+        self.comb = combustion()
+        rng = [_hash01(k, seed) for k in range(32)]
+        self.emitters = []
+        for e in range(3):
+            x = -1.2 + 1.2 * e + 0.3 * (rng[3 * e] - 0.5)
+            z = 0.4 * (rng[3 * e + 1] - 0.5)
+            r = 0.2 + 0.2 * rng[3 * e + 2]
+            shape = "box" if e == 1 else "sphere"
+            self.emitters.append((shape, (x, 0.25, z), (r, r, r)))
+
+    def frame(self, step: int) -> FrameData:
+        srcs = []
+        for i, (shape, pos, size) in enumerate(self.emitters):
+            j = 1.0 + 0.25 * value_noise_1d(step / 12.0, self.seed + 17 * i)
+            srcs.append(source(10 + i, shape, pos, size, flame=0.8, heat=2.0 * j, smoke=1.5 * j, fuel=0.6 * j,
+                               velocity=(0.0, 1.0, 0.0), response=60.0))
+        if step == 30:
+            # Explosion burst (FireSimulation.ts:471-493): charge / FIXED_DT for one step.
+            srcs.append(source(1000, "sphere", (0.0, 1.0, 0.0), (0.5, 0.5, 0.5), flame=1.0, heat=2.0 * 60,
+                               smoke=0.5 * 60, fuel=0.0, response=60.0, outward=20.0, variation=(0.5, 0.3)))
+        forces = [force("turbulence", strength=2.0, scale=1.0)]
+        cols = [collider("sphere", (0.6, 1.3, 0.0), (0.3, 0.3, 0.3)),
+                collider("box", (-0.6, 1.6, 0.2), (0.35, 0.1, 0.35))]
+        return make_frame(self.settings, self.comb, True, srcs, forces, (), cols)
+
+
+SCENES = {"single_plume": SinglePlume, "large_scene": LargeScene}
