@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark of the sparse-brick simulation step: voxel-steps/s on one B200.
+
+Workload: the large single-simulation scene (three seeded sphere/box emitters, a radial
+burst at step 30, turbulence, a sphere and a box collider; 8^3-cell bricks of 2.5 cm), grown
+until it holds the target brick count, then stepped K times. A "step" is one full
+simulation step: allocation, MacCormack transport, evolution, forces, divergence, one
+multigrid V-cycle and projection over every computing brick.
+
+Legs
+  value     device time of K steps (CUDA events on the simulation's own stream), inputs
+            resident: sum over steps of computing bricks x 512 voxels / time.
+  e2e       the same K-step loop through the public C ABI with host frames: each step copies
+            its scene and parameters host-to-device and reads its measurement back.
+  roofline  per-phase CUDA-event timing (the GpuProfiler analogue) of K more steps; the
+            dominant phase's algorithmic bytes per voxel x voxels / its device time.
+  cpu_baseline  the oracle's FP32 restatement on the host cores (OpenMP), a bounded sample.
+
+`--impl reference` times the reference algorithm's CPU restatement (the reference itself is
+TypeScript/WGSL and cannot run here) on the same scene and metric.
+Multi-GPU (torchrun): independent replicas, one per GPU; the timed region is bracketed by
+barriers and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for p in (ROOT, ROOT / "threejs-fire-pro_b200"):
+    if str(p) not in sys.path:
+        sys.path.insert(0, str(p))
+
+BRICK_VOXELS = 512
+BUDGET = 2 ** 24  # voxels: 32768 slots, ~3.2 GB of pools
+TARGET_BRICKS = 4096
+MAX_GROW_STEPS = 600
+
+# Algorithmic bytes per voxel per phase in FP32: every live field read once and written once
+# per kernel that must touch it (velocity 12 B, scalars 16 B, expansion/divergence/pressure
+# 4 B). Predictor = advect velocity (24) + advect scalars (44); correct_evolve = correct
+# velocity (36) + evolve fields (64); divergence includes the fused first Jacobi iterate's
+# write (4); multigrid = (8/7)(12 B x 3 post-sweeps + 9 B restriction + 8.5 B prolongation).
+BYTES_PER_VOXEL = {
+    "predict": 68.0,
+    "correct_evolve": 100.0,
+    "curl": 28.0,
+    "forces": 56.0,
+    "divergence": 24.0,
+    "multigrid": 8.0 / 7.0 * (12.0 * 3 + 17.5),
+    "project": 28.0,
+}
+STEP_BYTES = sum(BYTES_PER_VOXEL.values())
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi clock and throttle-reason samples every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cpu_sample(scene_cls, max_seconds: float, max_steps: int, threads: int):
+    """The FP32 oracle on the host cores: voxel-steps/s over a bounded run of the scene."""
+    from oracle import fp_oracle
+
+    fp_oracle.set_threads(threads)
+    sc = scene_cls()
+    o = fp_oracle.OracleSim(sc.grid(budget=BUDGET), real=1)
+    o.set_runtime(0.05, BUDGET, True)
+    o.step(sc.frame(0).frame)  # warm-up: allocation of the starting bricks
+    voxels, t0, steps = 0.0, time.perf_counter(), 0
+    step_ms = []
+    while steps < max_steps and time.perf_counter() - t0 < max_seconds:
+        t = time.perf_counter()
+        o.step(sc.frame(steps + 1).frame)
+        step_ms.append((time.perf_counter() - t) * 1e3)
+        voxels += o.active_bricks * BRICK_VOXELS
+        steps += 1
+    elapsed = time.perf_counter() - t0
+    o.close()
+    return voxels / elapsed, steps, voxels / max(steps, 1) / BRICK_VOXELS, step_ms
+
+
+def percentiles(ms):
+    s = sorted(ms)
+    if not s:
+        return None, None
+    return s[len(s) // 2], s[min(len(s) - 1, int(round(0.99 * (len(s) - 1))))]
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from firepro import scenes
+
+    threads = os.cpu_count() or 1
+    value, steps, bricks, step_ms = cpu_sample(scenes.LargeScene, 60.0, args.steps + args.warmup, threads)
+    p50, p99 = percentiles(step_ms)
+    line = {
+        "impl": "reference", "metric": "voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": args.gpus,
+        "steps": steps, "warmup": 1, "ms_per_step": statistics.mean(step_ms) if step_ms else None,
+        "p50_ms": p50, "p99_ms": p99, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": {"workload": "large_scene (seed 1), steps 1.. from the start",
+                                                        "mean_active_bricks": bricks},
+        "cpu_baseline": {"value": value, "unit": "voxel-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"oracle FP32 restatement, {steps} steps of the large scene from step 1 "
+                                   f"(mean {bricks:.0f} bricks), capped at 60 s"},
+        "e2e": {"value": value, "unit": "voxel-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    from firepro import scenes
+    from firepro.engine import FluidSimulation
+
+    torch.cuda.set_device(local)
+    sc = scenes.LargeScene(seed=1)
+    sim = FluidSimulation(sc.grid(budget=BUDGET), device=local)
+    sim.set_runtime(0.05, BUDGET, True)
+    # Grow the scene to the target size (untimed).
+    step = 0
+    while step < MAX_GROW_STEPS:
+        sim.step(sc.frame(step).frame)
+        step += 1
+        if step % 25 == 0 and sim.stats().active_bricks >= TARGET_BRICKS:
+            break
+    for _ in range(args.warmup):
+        sim.step(sc.frame(step).frame)
+        step += 1
+    sim.synchronize()
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    frames = [sc.frame(step + k) for k in range(args.steps)]
+
+    # --- value: device time of K steps on the simulation's stream
+    events = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    launches0 = sim.stats().kernel_launches
+    clocks = Clocks(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    actives = []
+    torch.cuda.profiler.start()  # marks the timed window for `ncu --profile-from-start off`
+    events[0].record(stream)
+    for k, fd in enumerate(frames):
+        sim.step(fd.frame)
+        events[k + 1].record(stream)
+        actives.append(sim.stats().active_bricks)
+    sim.synchronize()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    clock = clocks.stop()
+    barrier(world)
+    step += args.steps
+    launches = sim.stats().kernel_launches - launches0
+    total_ms = events[0].elapsed_time(events[-1])
+    step_ms = [events[k].elapsed_time(events[k + 1]) for k in range(args.steps)]
+    voxels = sum(actives) * BRICK_VOXELS
+    total_ms_max = max_over_ranks(total_ms, world)
+    voxels_all = sum_over_ranks(voxels, world)
+    value = voxels_all / (total_ms_max / 1e3)
+
+    # --- roofline: per-phase device time over K more steps
+    sim.set_profiling(True)
+    for k in range(args.steps):
+        sim.step(sc.frame(step + k).frame)
+    step += args.steps
+    prof = sim.profile()
+    sim.set_profiling(False)
+    peak, peak_kind = measured_peaks()
+    phases = {}
+    for name, (n, ms, vox) in prof.items():
+        if n == 0:
+            continue
+        per = BYTES_PER_VOXEL.get(name)
+        phases[name] = {"launches": int(n), "ms": ms, "share": None,
+                        "gbs": (per * vox / (ms / 1e3) / 1e9) if per and ms > 0 else None}
+    total_prof = sum(p["ms"] for p in phases.values())
+    for p in phases.values():
+        p["share"] = p["ms"] / total_prof if total_prof else None
+    dominant = max(phases, key=lambda k: phases[k]["ms"])
+    dom = phases[dominant]
+    achieved = dom["gbs"]
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "traffic": None,
+                "peak_kind": peak_kind, "bytes_per_voxel": BYTES_PER_VOXEL.get(dominant),
+                "step_gbs": STEP_BYTES * voxels / (total_ms / 1e3) / 1e9, "phases": phases}
+    traffic_file = ROOT / "profiles" / "traffic.json"
+    if traffic_file.exists():
+        t = json.loads(traffic_file.read_text()).get(dominant)
+        if t:
+            # DRAM bytes per voxel from the committed ncu capture, scaled to a launch here.
+            roofline["traffic"] = t["dram_bytes_per_voxel"] * (dom["launches"] and prof[dominant][2] / dom["launches"])
+
+    # --- e2e: the public C ABI with host frames, wall clock, measurement read each step
+    h2d, d2h, e2e_vox = 0, 0, 0.0
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        fd = sc.frame(step + k)  # host buffers built this step
+        sim.step(fd.frame)
+        st = sim.stats()  # device-to-host read of the step's measurement
+        e2e_vox += st.active_bricks * BRICK_VOXELS
+        h2d += st.h2d_bytes
+        d2h += st.d2h_bytes
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_vox = sum_over_ranks(e2e_vox, world)
+    step += args.steps
+    sim.dispose()
+
+    if rank != 0:
+        return
+    p50, p99 = percentiles(step_ms)
+    line = {
+        "metric": "voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "p50_ms": p50, "p99_ms": p99,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "large_scene: 3 seeded sphere/box emitters, burst at step 30, turbulence 2 m/s, "
+                               "sphere+box colliders; 8^3 bricks, 2.5 cm voxels; plain FP32 storage; "
+                               "1 cold-started V-cycle (reference schedule)",
+                   "mean_active_bricks": sum(actives) / len(actives), "grown_steps": step - 3 * args.steps,
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "working set > L2: pools of ~4k bricks x 97 KB"},
+        "roofline": roofline,
+        "e2e": {"value": e2e_vox / e2e_s, "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "gpu_launches": int(launches),
+        "clocks": clock,
+    }
+    if world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        cv, csteps, cbricks, _ = cpu_sample(scenes.LargeScene, 20.0, 400, threads)
+        line["cpu_baseline"] = {"value": cv, "unit": "voxel-steps/s", "cores": threads, "kind": "port",
+                                "sample": f"oracle FP32 restatement, {csteps} steps of the large scene from step 1 "
+                                          f"(mean {cbricks:.0f} bricks), capped at 20 s"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

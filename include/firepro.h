@@ -160,7 +160,19 @@ typedef struct fp_stats {
   uint64_t memory_bytes;    /* device bytes this simulation owns */
   uint32_t last_vcycles;    /* V-cycles the latest pressure solve ran */
   double last_residual;     /* FP64 RMS residual after the latest solve (mixed mode), else -1 */
+  uint64_t kernel_launches; /* kernels this simulation has launched since creation */
+  uint64_t h2d_bytes;       /* host-to-device bytes the latest step copied (scene, parameters) */
+  uint64_t d2h_bytes;       /* device-to-host bytes the latest step read back (its measurement) */
 } fp_stats;
+
+/* Device time of one phase of the step, accumulated while profiling is on: the restatement
+ * of the reference's per-pass GPU timestamps (src/engine/GpuProfiler.ts:21-109). */
+typedef struct fp_phase {
+  char name[32];
+  uint64_t launches;  /* kernels the phase launched */
+  double ms;          /* device milliseconds, CUDA events on the simulation's stream */
+  double voxels;      /* active voxels the phase covered, summed over steps */
+} fp_phase;
 
 /* Per-slot field arrays a test or debug view may copy out (`fp_sim_read_field`). Each
  * is [slot][channel][cell] in FP32, cells x fastest within a brick. */
@@ -213,6 +225,14 @@ int fp_sim_read_table(fp_sim* sim, int table, void* host, size_t* bytes);
  * bricks that hold a slot, six floats each (min xyz, max xyz). `*count` in: capacity in
  * boxes, out: boxes written (or needed, with FP_ELIMIT). */
 int fp_sim_read_bricks(fp_sim* sim, float* boxes, uint32_t* count);
+/* The cudaStream_t the simulation enqueues on, for callers that order their own work after
+ * it or record events against it. No reference counterpart: WebGPU has one queue. */
+int fp_sim_stream(fp_sim* sim, void** stream);
+/* Start (clearing the totals) or stop per-phase device timing: `GpuProfiler` of the
+ * reference (src/engine/GpuProfiler.ts:21-68) with CUDA events. */
+int fp_sim_set_profiling(fp_sim* sim, int enabled);
+/* The per-phase totals since profiling started. `*count` in: capacity, out: phases. */
+int fp_sim_read_profile(fp_sim* sim, fp_phase* phases, uint32_t* count);
 
 #ifdef __cplusplus
 }

@@ -19,6 +19,7 @@
 // Citations are path:line in the reference project.
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -56,8 +57,13 @@ struct Tile {
 struct Directory {
   // Insertion-ordered, like the JS Map of TileDirectory.ts:62.
   std::map<uint64_t, Tile> bySeq;
-  std::map<std::tuple<int, int, int>, uint64_t> byCoord;
+  std::unordered_map<uint64_t, uint64_t> byCoord;  // packed coordinates -> sequence
+  std::unordered_map<uint64_t, int> slotOf;         // packed coordinates -> tile slot
   uint64_t nextSeq = 0;
+  static uint64_t key(int x, int y, int z) {
+    return ((uint64_t)(uint32_t)(x + (1 << 20)) << 42) | ((uint64_t)(uint32_t)(y + (1 << 20)) << 21) |
+           (uint64_t)(uint32_t)(z + (1 << 20));
+  }
   std::vector<int> slotUsed;  // -1 free, else 1 (TileDirectory.ts:63 `slots`)
   std::vector<int> created;
   bool dirty = true;
@@ -66,7 +72,7 @@ struct Directory {
 
   int count() const { return (int)bySeq.size(); }
   Tile* find(int x, int y, int z) {
-    auto it = byCoord.find(std::make_tuple(x, y, z));
+    auto it = byCoord.find(key(x, y, z));
     if (it == byCoord.end()) return nullptr;
     return &bySeq[it->second];
   }
@@ -97,7 +103,8 @@ struct Directory {
           slotUsed[slot] = 1;
           uint64_t seq = nextSeq++;
           bySeq[seq] = Tile{i3(x, y, z), slot, step, false};
-          byCoord[std::make_tuple(x, y, z)] = seq;
+          byCoord[key(x, y, z)] = seq;
+          slotOf[key(x, y, z)] = slot;
           created.push_back(slot);
           dirty = true;
         }
@@ -108,7 +115,8 @@ struct Directory {
       Tile& t = it->second;
       if (t.closing) {
         slotUsed[t.slot] = -1;
-        byCoord.erase(std::make_tuple(t.coord[0], t.coord[1], t.coord[2]));
+        byCoord.erase(key(t.coord[0], t.coord[1], t.coord[2]));
+        slotOf.erase(key(t.coord[0], t.coord[1], t.coord[2]));
         it = bySeq.erase(it);
         dirty = true;
         continue;
@@ -124,13 +132,14 @@ struct Directory {
   void clear() {
     bySeq.clear();
     byCoord.clear();
+    slotOf.clear();
     slotUsed.clear();
     created.clear();
     dirty = true;
   }
-  int slotAt(int x, int y, int z) {
-    Tile* t = find(x, y, z);
-    return t ? t->slot : -1;
+  int slotAt(int x, int y, int z) const {
+    auto it = slotOf.find(key(x, y, z));
+    return it == slotOf.end() ? -1 : it->second;
   }
   std::vector<int> takeCreated() {
     std::vector<int> out;
@@ -414,6 +423,7 @@ struct Sim {
       }
     }
     geometryDirty = true;  // PressureSolver.setBricks -> resetPlans
+    lookupGen = nextGen();
   }
 
   // ---------------------------------------------------------------- addressing (tiles.wgsl)
@@ -425,9 +435,27 @@ struct Sim {
     if (t < 0) return -1;
     return t * 64 + (((bz & 3) * 4 + (by & 3)) * 4 + (bx & 3));
   }
+  // The last brick each thread looked up, valid while `lookupGen` is unchanged: entries and
+  // tiles change only between the step's phases, when the generation moves on.
+  struct LookupCache {
+    const void* sim;
+    uint64_t gen;
+    int bx, by, bz;
+    int32_t entry;
+  };
+  static uint64_t nextGen() {
+    static std::atomic<uint64_t> counter{1};
+    return ++counter;
+  }
+  uint64_t lookupGen = nextGen();
   int32_t brickEntry(int bx, int by, int bz) {
+    static thread_local LookupCache cache = {nullptr, 0, 0, 0, 0, -1};
+    if (cache.sim == this && cache.gen == lookupGen && cache.bx == bx && cache.by == by && cache.bz == bz)
+      return cache.entry;
     int id = brickId(bx, by, bz);
-    return id < 0 ? -1 : entries[id];
+    int32_t e = id < 0 ? -1 : entries[id];
+    cache = LookupCache{this, lookupGen, bx, by, bz, e};
+    return e;
   }
   static int entryPage(int32_t e) { return e < 0 ? -1 : (e & 0xffffff); }
   int brickSlot(int bx, int by, int bz) { return entryPage(brickEntry(bx, by, bz)); }
@@ -871,6 +899,7 @@ struct Sim {
       }
       w[27] = unknowns;
     }
+    lookupGen = nextGen();
     // finishBricks
     int32_t fr = freeCount + (int32_t)frees;
     int32_t granted = std::min((int32_t)requests, std::max(fr - held, 0));
@@ -1938,6 +1967,12 @@ or_sim* or_create(const fp_grid* g, int real, int mode) {
     s->f = new orc::Sim<float>(*g, p);
   return s;
 }
+// The storage-rounding helpers, exported so the tests can pin them to numpy's.
+double or_round_f16(double x) { return orc::round_f16(x); }
+double or_round_bf16(double x) { return orc::round_bf16(x); }
+double or_truncate_half(double x) { return orc::truncate_half(x); }
+double or_noise_hash(int x, int y, int z) { return orc::noise_hash(x, y, z); }
+
 void or_destroy(or_sim* s) {
   if (!s) return;
   delete s->d;

@@ -87,15 +87,19 @@ def force(gpu, orc):
     orc.write_activity(gpu.table(abi.FP_TABLE_ACTIVITY))
 
 
-def lockstep(scene, steps: int, gpu_factory, cutoff=0.05, budget=8e6, ground=True, start=0, log=None):
-    """Run `steps` steps in lockstep; returns per-step (tables, fields) reports."""
-    grid = scene.grid(budget=budget)
+def lockstep(scene, steps: int, gpu_factory, cutoff=0.05, budget=8e6, ground=True, start=0, log=None, grid=None,
+             before_step=None):
+    """Run `steps` steps in lockstep; returns per-step (tables, fields) reports.
+    `before_step(step, gpu, oracle)` may change runtime settings on both."""
+    grid = grid if grid is not None else scene.grid(budget=budget)
     gpu = gpu_factory(grid)
     orc = OracleSim(grid, real=0)
     gpu.set_runtime(cutoff, budget, ground)
     orc.set_runtime(cutoff, budget, ground)
     reports = []
     for s in range(start, start + steps):
+        if before_step:
+            before_step(s, gpu, orc)
         fd = scene.frame(s)
         gpu.step(fd.frame)
         orc.step(fd.frame)

@@ -1,0 +1,143 @@
+"""Parity of the CUDA step with the FP64 oracle, called through the C ABI.
+
+Every test steps the CUDA simulation and the oracle in lockstep from identical state:
+the allocation's integer tables must match bit for bit, and every field within relative
+L2 <= 1e-3 (REL_L2_TOL) per step.
+"""
+import numpy as np
+import pytest
+
+from firepro import abi, scenes
+from firepro.engine import FireProError, FluidSimulation
+import parity
+
+pytestmark = pytest.mark.gpu
+
+TOL = parity.REL_L2_TOL
+
+
+def check(reports, tol=TOL, min_active=1):
+    worst = {}
+    for step, tables, fields, n in reports:
+        for k, v in tables.items():
+            assert v == 0, f"step {step}: table {k} differs in {v} words"
+        for k, v in fields.items():
+            worst[k] = max(worst.get(k, 0.0), v)
+            assert v <= tol, f"step {step}: {k} relative L2 {v:.3e} > {tol}"
+    assert max(r[3] for r in reports) >= min_active
+    return worst
+
+
+def run(scene, steps, **kw):
+    return parity.lockstep(scene, steps, lambda g: FluidSimulation(g), **kw)
+
+
+def test_plume_parity():
+    check(run(scenes.SinglePlume(), 40, budget=2 ** 19), min_active=216)
+
+
+def test_force_scene_parity():
+    """Wind, turbulence, vortex, targeted radial force; rotated box, sphere and mesh-mask
+    colliders; a burst with Perlin variation; an emitter that stops."""
+    check(run(scenes.ForceScene(), 16, budget=2 ** 20))
+
+
+def test_large_scene_through_burst():
+    check(run(scenes.LargeScene(), 34, budget=2 ** 20), min_active=100)
+
+
+def test_pool_exhausted_failures_match():
+    """A budget of 150 bricks: requests past it fail, deterministically in brick order."""
+    reports = run(scenes.SinglePlume(), 8, budget=150 * 512)
+    check(reports)
+
+
+def test_budget_cut_holds_slots():
+    def cut(step, gpu, orc):
+        if step == 3:
+            gpu.set_runtime(0.05, 200 * 512, True)
+            orc.set_runtime(0.05, 200 * 512, True)
+    check(run(scenes.SinglePlume(), 8, budget=2 ** 19, before_step=cut))
+
+
+def test_first_order_scalars():
+    sc = scenes.SinglePlume()
+    check(run(sc, 36, grid=sc.grid(budget=2 ** 19, maccormack=False), budget=2 ** 19))
+
+
+def test_brick16():
+    sc = scenes.SinglePlume()
+    sc.brick_size = 16
+    check(run(sc, 12, budget=2 ** 21))
+
+
+def test_ground_off():
+    check(run(scenes.ForceScene(), 8, budget=2 ** 20, ground=False))
+
+
+def test_cutoff_zero_keeps_tails():
+    check(run(scenes.SinglePlume(), 36, budget=2 ** 19, cutoff=0.0))
+
+
+def test_empty_scene():
+    sim = FluidSimulation(scenes.EmptyScene().grid(budget=2 ** 19))
+    sim.set_runtime(0.05, 2 ** 19, True)
+    for s in range(3):
+        sim.step(scenes.EmptyScene().frame(s).frame)
+    st = sim.stats()
+    assert st.active_bricks == 0 and st.tiles == 0 and st.steps == 3
+    sim.dispose()
+
+
+def test_reset_restarts_exactly():
+    sc = scenes.SinglePlume()
+    a = FluidSimulation(sc.grid(budget=2 ** 19))
+    a.set_runtime(0.05, 2 ** 19, True)
+    for s in range(5):
+        a.step(sc.frame(s).frame)
+    a.reset()
+    b = FluidSimulation(sc.grid(budget=2 ** 19))
+    b.set_runtime(0.05, 2 ** 19, True)
+    for s in range(4):
+        a.step(sc.frame(s).frame)
+        b.step(sc.frame(s).frame)
+    assert a.stats().steps == 4
+    for tid in (abi.FP_TABLE_ENTRIES, abi.FP_TABLE_ACTIVE, abi.FP_TABLE_FREE):
+        assert np.array_equal(a.table(tid), b.table(tid))
+    assert np.array_equal(a.field(abi.FP_FIELD_VELOCITY), b.field(abi.FP_FIELD_VELOCITY))
+    assert np.array_equal(a.field(abi.FP_FIELD_SCALARS), b.field(abi.FP_FIELD_SCALARS))
+
+
+def test_step_validation_leaves_state():
+    sc = scenes.SinglePlume()
+    sim = FluidSimulation(sc.grid(budget=2 ** 19))
+    sim.step(sc.frame(0).frame)
+    for dt in (0.0, 0.05, float("inf")):
+        with pytest.raises(FireProError, match=r"Simulation step must be in \(0, 1/30\]. Use fixed substeps."):
+            sim.step(sc.frame(1).frame, dt)
+    bad = sc.frame(1)
+    bad.frame.combustion.ramps[2].knots[0][0] = 0.1
+    with pytest.raises(FireProError, match="expansion ramp must span lifetime 0–1."):
+        sim.step(bad.frame)
+    assert sim.stats().steps == 1
+
+
+def test_read_bricks_match_entries():
+    sc = scenes.SinglePlume()
+    sim = FluidSimulation(sc.grid(budget=2 ** 19))
+    sim.step(sc.frame(0).frame)
+    boxes = sim.read_bricks()
+    assert boxes.shape == (216, 6)
+    size = 8 * 0.025
+    assert np.allclose(boxes[:, 3:] - boxes[:, :3], size)
+    lo = np.round(boxes[:, :3] / size).astype(int)
+    assert lo[:, 0].min() == -3 and lo[:, 0].max() == 2 and lo[:, 1].min() == 0 and lo[:, 1].max() == 5
+
+
+def test_tile_lifecycle_matches_oracle():
+    class Short(scenes.Scene):
+        def frame(self, step):
+            src = [scenes.source(1, "sphere", (0, 0.4, 0), (0.1, 0.1, 0.1), heat=1.0)] if step < 3 else []
+            return scenes.make_frame(scenes.settings(), scenes.combustion(), False, src)
+
+    check(run(Short(), 66, budget=2 ** 18), tol=TOL)

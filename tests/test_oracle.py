@@ -1,0 +1,201 @@
+"""CPU tests of the oracle: numeric helpers pinned to numpy, allocation invariants, the
+reference's validation messages, tile lifecycle, determinism and projection."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from firepro import abi, scenes
+from oracle.fp_oracle import OracleSim
+
+BUDGET = 2 ** 19
+
+
+def _sim(scene, real=1, budget=BUDGET, cutoff=0.05, ground=True, **grid):
+    o = OracleSim(scene.grid(budget=budget, **grid), real=real)
+    o.set_runtime(cutoff, budget, ground)
+    return o
+
+
+def test_round_f16_matches_numpy(oracle_lib):
+    L = oracle_lib
+    L.or_round_f16.restype = C.c_double
+    L.or_round_f16.argtypes = [C.c_double]
+    rng = np.random.default_rng(0)
+    xs = np.concatenate([rng.normal(0, 10, 2000), rng.normal(0, 1e-5, 500), [0.0, 65504.0, 1e-8, -3.1e-7, 2049.0, 2051.0]])
+    for x in xs.astype(np.float32):
+        assert L.or_round_f16(float(x)) == float(np.float16(x)), x
+
+
+def test_round_bf16_and_truncate(oracle_lib):
+    L = oracle_lib
+    for fn in (L.or_round_bf16, L.or_truncate_half):
+        fn.restype = C.c_double
+        fn.argtypes = [C.c_double]
+    rng = np.random.default_rng(1)
+    for x in rng.normal(0, 5, 500).astype(np.float32):
+        u = np.array([x], np.float32).view(np.uint32)[0]
+        rounded = ((int(u) + 0x7FFF + ((int(u) >> 16) & 1)) & 0xFFFF0000)
+        assert L.or_round_bf16(float(x)) == float(np.array([rounded], np.uint32).view(np.float32)[0])
+        t = L.or_truncate_half(float(x))
+        # Toward zero with ten mantissa bits: |t| <= |x| and within one half ulp.
+        assert abs(t) <= abs(x) and abs(x - t) <= abs(x) * 2 ** -10
+        assert float(np.float16(t)) == t
+
+
+def test_plume_allocation_invariants(oracle_lib):
+    o = _sim(scenes.SinglePlume())
+    sc = scenes.SinglePlume()
+    for s in range(3):
+        o.step(sc.frame(s).frame)
+    entries = o.table(abi.FP_TABLE_ENTRIES).view(np.int32)
+    pages = o.table(abi.FP_TABLE_PAGES).view(np.int32)
+    active = o.table(abi.FP_TABLE_ACTIVE)
+    free = o.table(abi.FP_TABLE_FREE)
+    n = int(active[0])
+    ids = active[1:1 + n]
+    # The starting block is exactly 6x6x6 bricks.
+    assert n == 216
+    assert np.all(np.diff(ids.astype(np.int64)) > 0), "computing bricks are listed in ascending id order"
+    slots = pages[ids]
+    assert np.all(slots >= 0) and len(np.unique(slots)) == n, "each computing brick owns a distinct slot"
+    assert np.all((entries[ids] & 0xFFFFFF) == slots)
+    assert np.all(entries[pages < 0] == -1)
+    # Every slot is either on the free stack or owned.
+    assert int(free[0]) + n == o.slots
+    stack = free[2:2 + int(free[0])]
+    assert len(np.intersect1d(stack, slots)) == 0
+    # Slots are handed out lowest first.
+    assert sorted(slots.tolist()) == list(range(n))
+
+
+def test_plume_first_step_fresh_flags(oracle_lib):
+    o = _sim(scenes.SinglePlume())
+    sc = scenes.SinglePlume()
+    o.step(sc.frame(0).frame)
+    e = o.table(abi.FP_TABLE_ENTRIES).view(np.int32)
+    live = e[e >= 0]
+    assert np.all(live & 0x2000000), "slots granted this step are fresh"
+    o.step(sc.frame(1).frame)
+    e = o.table(abi.FP_TABLE_ENTRIES).view(np.int32)
+    assert not np.any(e[e >= 0] & 0x2000000), "kept slots are not fresh"
+
+
+def test_records_match_entries(oracle_lib):
+    sc = scenes.SinglePlume()
+    o = _sim(sc)
+    for s in range(2):
+        o.step(sc.frame(s).frame)
+    e = o.table(abi.FP_TABLE_ENTRIES).view(np.int32)
+    rec = o.table(abi.FP_TABLE_RECORDS).view(np.int32).reshape(-1, 28)
+    tiles = o.table(abi.FP_TABLE_TILES).view(np.int32).reshape(-1, 4)
+    coord = {}
+    for t, (x, y, z, st) in enumerate(tiles):
+        if st:
+            coord[(x, y, z)] = t
+
+    def brick_id(b):
+        t = coord.get((b[0] >> 2, b[1] >> 2, b[2] >> 2))
+        return -1 if t is None else t * 64 + ((b[2] & 3) * 4 + (b[1] & 3)) * 4 + (b[0] & 3)
+
+    for bid in np.nonzero(e >= 0)[0][:50]:
+        t, l = bid // 64, bid % 64
+        x, y, z, _ = tiles[t]
+        b = (x * 4 + (l & 3), y * 4 + ((l >> 2) & 3), z * 4 + (l >> 4))
+        for k in range(27):
+            d = (k % 3 - 1, (k // 3) % 3 - 1, k // 9 - 1)
+            nb = brick_id((b[0] + d[0], b[1] + d[1], b[2] + d[2]))
+            assert rec[bid, k] == (e[nb] if nb >= 0 else -1)
+
+
+def test_step_validation_messages(oracle_lib):
+    sc = scenes.SinglePlume()
+    o = _sim(sc)
+    fd = sc.frame(0)
+    for dt in (0.0, -1.0, 1 / 29, float("nan")):
+        with pytest.raises(ValueError, match=r"Simulation step must be in \(0, 1/30\]"):
+            o.step(fd.frame, dt)
+    fd.frame.combustion.ramps[0].count = 1
+    with pytest.raises(ValueError, match="smoke ramp needs 2–8 knots"):
+        o.step(fd.frame)
+    fd = sc.frame(0)
+    fd.frame.combustion.ramps[1].knots[1][0] = 1.5
+    with pytest.raises(ValueError, match="heat knots must increase in f32 with coordinates in \\[0,1\\]"):
+        o.step(fd.frame)
+    fd = sc.frame(0)
+    fd.frame.combustion.lifespan = 0.0
+    with pytest.raises(ValueError, match="Flame timestep and lifespan must be positive in f32"):
+        o.step(fd.frame)
+
+
+def test_empty_scene_holds_nothing(oracle_lib):
+    sc = scenes.EmptyScene()
+    o = _sim(sc)
+    for s in range(3):
+        o.step(sc.frame(s).frame)
+    assert o.active_bricks == 0
+    assert o.info(8) == 0, "no tile without a source or content"
+
+
+def test_deterministic(oracle_lib):
+    sc = scenes.SinglePlume()
+    a, b = _sim(sc), _sim(sc)
+    for s in range(4):
+        a.step(sc.frame(s).frame)
+        b.step(sc.frame(s).frame)
+    assert np.array_equal(a.field(abi.FP_FIELD_VELOCITY), b.field(abi.FP_FIELD_VELOCITY))
+    assert np.array_equal(a.field(abi.FP_FIELD_SCALARS), b.field(abi.FP_FIELD_SCALARS))
+
+
+def test_fp32_tracks_fp64(oracle_lib):
+    sc = scenes.SinglePlume()
+    a, b = _sim(sc, real=0), _sim(sc, real=1)
+    for s in range(5):
+        a.step(sc.frame(s).frame)
+        b.step(sc.frame(s).frame)
+    for fid in (abi.FP_FIELD_VELOCITY, abi.FP_FIELD_SCALARS):
+        x, y = a.field(fid, f64=True), b.field(fid)
+        assert np.linalg.norm(x - y) <= 1e-5 * np.linalg.norm(x)
+
+
+def test_tiles_linger_then_close(oracle_lib):
+    """A source that stops leaves its tiles for LINGER_STEPS (60), then they close and go."""
+    class Burst(scenes.Scene):
+        def frame(self, step):
+            src = [scenes.source(1, "sphere", (0, 0.5, 0), (0.1, 0.1, 0.1))] if step == 0 else []
+            return scenes.make_frame(scenes.settings(), scenes.combustion(), False, src)
+
+    sc = Burst()
+    o = _sim(sc)
+    o.step(sc.frame(0).frame)
+    tiles0 = o.info(8)
+    assert tiles0 > 0
+    for s in range(1, 62):
+        o.step(sc.frame(s).frame)
+    assert o.info(8) == tiles0, "tiles linger 60 steps"
+    o.step(sc.frame(62).frame)
+    states = o.table(abi.FP_TABLE_TILES).view(np.int32).reshape(-1, 4)[:, 3]
+    assert np.all(states[states != 0] == 2), "then close"
+    o.step(sc.frame(63).frame)
+    assert o.info(8) == 0, "and are removed a step later"
+
+
+def test_projection_reduces_divergence(oracle_lib):
+    sc = scenes.SinglePlume()
+    o = _sim(sc, real=0)
+    for s in range(40):
+        o.step(sc.frame(s).frame)
+    div = o.field(abi.FP_FIELD_DIVERGENCE, f64=True)  # h^2 (div u - expansion) before projection
+    v = o.field(abi.FP_FIELD_VELOCITY, f64=True)
+    e = o.table(abi.FP_TABLE_ENTRIES).view(np.int32)
+    slots = np.unique(e[e >= 0] & 0xFFFFFF)
+    # Interior divergence of the projected velocity within each brick.
+    B = 8
+    u = v[slots].reshape(len(slots), 3, B, B, B)  # [s, c, z, y, x]
+    d = (u[:, 0, 1:, 1:, 1:] - u[:, 0, 1:, 1:, :-1]) + (u[:, 1, 1:, 1:, 1:] - u[:, 1, 1:, :-1, 1:]) + \
+        (u[:, 2, 1:, 1:, 1:] - u[:, 2, :-1, 1:, 1:])
+    h = 0.025
+    expn = o.field(abi.FP_FIELD_EXPANSION, f64=True)[slots].reshape(len(slots), B, B, B)[:, 1:, 1:, 1:]
+    after = np.linalg.norm(d / h - expn)
+    before = np.linalg.norm(div[slots].reshape(len(slots), B, B, B)[:, 1:, 1:, 1:]) / h ** 2
+    assert after < 0.5 * before, (after, before)

@@ -119,4 +119,20 @@ int fp_sim_read_bricks(fp_sim* sim, float* boxes, uint32_t* count) {
   return sim->engine->readBricks(boxes, count);
 }
 
+int fp_sim_stream(fp_sim* sim, void** stream) {
+  if (!sim || !stream) return failed("fp_sim_stream needs a simulation and an output.", FP_EINVAL);
+  *stream = (void*)sim->engine->stream();
+  return FP_OK;
+}
+
+int fp_sim_set_profiling(fp_sim* sim, int enabled) {
+  if (!sim) return failed("null simulation", FP_EINVAL);
+  return sim->engine->setProfiling(enabled != 0);
+}
+
+int fp_sim_read_profile(fp_sim* sim, fp_phase* phases, uint32_t* count) {
+  if (!sim || !count) return failed("fp_sim_read_profile needs a simulation and a count.", FP_EINVAL);
+  return sim->engine->readProfile(phases, count);
+}
+
 }  // extern "C"

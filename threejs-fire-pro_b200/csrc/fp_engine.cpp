@@ -125,6 +125,7 @@ bool Engine::upload(DeviceBuffer& b, const void* src, size_t bytes) {
     if (!alloc(b, std::max(bytes + bytes / 2, (size_t)256), false)) return false;
   }
   // Synchronous from pageable memory: the source vectors change next step.
+  h2d_ += bytes;
   return cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, stream_) == cudaSuccess;
 }
 
@@ -152,6 +153,10 @@ Engine::~Engine() {
   if (paramsH_) cudaFreeHost(paramsH_);
   if (readH_) cudaFreeHost(readH_);
   if (readEvent_) cudaEventDestroy(readEvent_);
+  for (Phase& ph : phases_) {
+    if (ph.a) cudaEventDestroy(ph.a);
+    if (ph.b) cudaEventDestroy(ph.b);
+  }
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -697,6 +702,66 @@ int Engine::consumeReadback() {
   usedSlots_ = slots_ - (uint32_t)c->freeCount;
   lastFailures_ = c->failures;
   poolLimited_ = c->failures > 0 && slots_ >= slotLimit();
+  if (profilePending_) {
+    for (Phase& ph : phases_) {
+      if (!ph.used) continue;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ph.a, ph.b);
+      ph.ms += ms;
+      ph.launches += ph.stepLaunches;
+      ph.voxels += (double)c->active * N_;
+      ph.used = false;
+    }
+    profilePending_ = false;
+  }
+  return FP_OK;
+}
+
+void Engine::phaseBegin(int id) {
+  if (profiling_) cudaEventRecord(phases_[id].a, stream_);
+}
+void Engine::phaseEnd(int id, int launches) {
+  launches_ += (uint64_t)launches;
+  if (!profiling_) return;
+  Phase& ph = phases_[id];
+  cudaEventRecord(ph.b, stream_);
+  ph.stepLaunches = (uint64_t)launches;
+  ph.used = true;
+  profilePending_ = true;
+}
+
+int Engine::setProfiling(bool on) {
+  int rc = consumeReadback();
+  if (rc) return rc;
+  for (Phase& ph : phases_) {
+    if (!ph.a && (rc = check(cudaEventCreate(&ph.a), "cudaEventCreate"))) return rc;
+    if (!ph.b && (rc = check(cudaEventCreate(&ph.b), "cudaEventCreate"))) return rc;
+    if (on) {
+      ph.launches = 0;
+      ph.ms = 0;
+      ph.voxels = 0;
+    }
+    ph.used = false;
+  }
+  profiling_ = on;
+  return FP_OK;
+}
+
+int Engine::readProfile(fp_phase* out, uint32_t* count) {
+  static const char* names[PH_COUNT] = {"allocation", "topology", "predict", "correct_evolve", "curl",
+                                        "forces", "divergence", "multigrid", "project"};
+  int rc = consumeReadback();
+  if (rc) return rc;
+  uint32_t cap = *count;
+  *count = PH_COUNT;
+  if (!out || cap < PH_COUNT) return fail(FP_ELIMIT, "profile buffer too small");
+  for (int i = 0; i < PH_COUNT; i++) {
+    std::memset(&out[i], 0, sizeof(fp_phase));
+    std::strncpy(out[i].name, names[i], sizeof(out[i].name) - 1);
+    out[i].launches = phases_[i].launches;
+    out[i].ms = phases_[i].ms;
+    out[i].voxels = phases_[i].voxels;
+  }
   return FP_OK;
 }
 
@@ -707,11 +772,13 @@ void Engine::vcycle(int level, int cur[]) {
   if (level == bottom_) {
     if (capacity_ <= 1024) {
       fp_launch_bottom(dP, level, 19, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]), capacity_, stream_);
+      launches_++;
       cur[level] = 1 - cur[level];
     } else {
       for (int i = 0; i < 19; i++) {
         fp_launch_relax(dP, level, true, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]), capacity_, sms_,
                         stream_);
+        launches_++;
         cur[level] = 1 - cur[level];
       }
     }
@@ -721,19 +788,23 @@ void Engine::vcycle(int level, int cur[]) {
     for (int i = 0; i < 2; i++) {
       fp_launch_relax(dP, level, level >= brickLevels_, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]),
                       capacity_, sms_, stream_);
+      launches_++;
       cur[level] = 1 - cur[level];
     }
   int coarse = level + 1;
   fp_launch_restrict(dP, level, coarse >= brickLevels_, RHS(level), LP(level, cur[level]), RHS(coarse), LP(coarse, 1),
                      capacity_, sms_, stream_);
+  launches_++;
   cur[coarse] = 1;
   vcycle(coarse, cur);
   fp_launch_prolong(dP, level, level >= brickLevels_, LP(level, cur[level]), LP(coarse, cur[coarse]),
                     LP(level, 1 - cur[level]), capacity_, sms_, stream_);
+  launches_++;
   cur[level] = 1 - cur[level];
   for (int i = 0; i < 3; i++) {
     fp_launch_relax(dP, level, level >= brickLevels_, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]),
                     capacity_, sms_, stream_);
+    launches_++;
     cur[level] = 1 - cur[level];
   }
 }
@@ -772,23 +843,48 @@ int Engine::step(const fp_frame& f, float dt) {
   fillParams(f, dt);
   SimParams* dP = dParams();
   cudaMemcpyAsync(dP, paramsH_, sizeof(SimParams), cudaMemcpyHostToDevice, stream_);
+  h2d_ += sizeof(SimParams);
 
-  fp_launch_allocation(dP, capacity_, colliderCount_ > 0 || solidsStale_, sms_, stream_);
+  bool solids = colliderCount_ > 0 || solidsStale_;
+  phaseBegin(PH_ALLOC);
+  fp_launch_allocation(dP, capacity_, solids, sms_, stream_);
+  phaseEnd(PH_ALLOC, 7 + (solids ? 1 : 0));
   solidsStale_ = false;
   // Topology of the slots granted this step, or of everything after the geometry changed.
+  phaseBegin(PH_TOPO);
   fp_launch_topology(dP, brickLevels_, bottom_, geometryDirty_, capacity_, sms_, stream_);
+  phaseEnd(PH_TOPO, geometryDirty_ ? 2 : 1);
   geometryDirty_ = false;
+  phaseBegin(PH_PREDICT);
   fp_launch_predict(dP, sms_, stream_);
+  phaseEnd(PH_PREDICT, 1);
+  phaseBegin(PH_CORRECT);
   fp_launch_correct_evolve(dP, sms_, stream_);
-  if (f.simulation.vorticity != 0.f) fp_launch_curl(dP, sms_, stream_);
+  phaseEnd(PH_CORRECT, 1);
+  if (f.simulation.vorticity != 0.f) {
+    phaseBegin(PH_CURL);
+    fp_launch_curl(dP, sms_, stream_);
+    phaseEnd(PH_CURL, 1);
+  }
+  phaseBegin(PH_FORCES);
   fp_launch_forces(dP, B_, sms_, stream_);
+  phaseEnd(PH_FORCES, 1);
   int cur[FP_MAX_LEVELS] = {0};
   cur[0] = latest_;
+  phaseBegin(PH_DIVERGENCE);
   fp_launch_divergence(dP, P0(1 - cur[0]), sms_, stream_);
+  phaseEnd(PH_DIVERGENCE, 1);
   cur[0] = 1 - cur[0];
+  phaseBegin(PH_MULTIGRID);
+  uint64_t before = launches_;
   vcycle(0, cur);
+  int mg = (int)(launches_ - before);
+  launches_ = before;
+  phaseEnd(PH_MULTIGRID, mg);
   latest_ = cur[0];
+  phaseBegin(PH_PROJECT);
   fp_launch_project(dP, P0(latest_), sms_, stream_);
+  phaseEnd(PH_PROJECT, 1);
   std::swap(velIdx_[0], velIdx_[1]);
   std::swap(fldIdx_[0], fldIdx_[2]);
 
@@ -799,6 +895,10 @@ int Engine::step(const fp_frame& f, float dt) {
     readWords_ = words * 2;
     if ((rc = check(cudaMallocHost(&readH_, readWords_ * 4), "cudaMallocHost"))) return rc;
   }
+  d2h_ += sizeof(FpCounters) + (size_t)capacity_ * 4;
+  stepH2d_ = h2d_;
+  stepD2h_ = d2h_;
+  h2d_ = d2h_ = 0;
   cudaMemcpyAsync(readH_, counters_.ptr, sizeof(FpCounters), cudaMemcpyDeviceToHost, stream_);
   cudaMemcpyAsync(readH_ + sizeof(FpCounters) / 4, (uint32_t*)activity_.ptr + (size_t)capacity_ * 64,
                   (size_t)capacity_ * 4, cudaMemcpyDeviceToHost, stream_);
@@ -852,6 +952,9 @@ int Engine::stats(fp_stats* out) {
   out->memory_bytes = bytes;
   out->last_vcycles = steps_ > 0 ? 1 : 0;
   out->last_residual = -1;
+  out->kernel_launches = launches_;
+  out->h2d_bytes = stepH2d_;
+  out->d2h_bytes = stepD2h_;
   return FP_OK;
 }
 

@@ -66,6 +66,9 @@ class Engine {
   int readField(int field, float* host, size_t bytes);
   int readTable(int table, void* host, size_t* bytes);
   int readBricks(float* boxes, uint32_t* count);
+  int setProfiling(bool on);
+  int readProfile(fp_phase* out, uint32_t* count);
+  cudaStream_t stream() const { return stream_; }
   const std::string& error() const { return error_; }
   int fail(int code, const std::string& message) {
     error_ = message;
@@ -125,6 +128,23 @@ class Engine {
   uint32_t* readH_ = nullptr;
   size_t readWords_ = 0;
   cudaEvent_t readEvent_ = nullptr;
+
+  // per-phase device timing (GpuProfiler.ts), and the launch count
+  enum PhaseId { PH_ALLOC, PH_TOPO, PH_PREDICT, PH_CORRECT, PH_CURL, PH_FORCES, PH_DIVERGENCE, PH_MULTIGRID,
+                 PH_PROJECT, PH_COUNT };
+  struct Phase {
+    uint64_t launches = 0, stepLaunches = 0;
+    double ms = 0, voxels = 0;
+    bool used = false;
+    cudaEvent_t a = nullptr, b = nullptr;
+  };
+  Phase phases_[PH_COUNT];
+  bool profiling_ = false;
+  bool profilePending_ = false;
+  uint64_t launches_ = 0;
+  uint64_t h2d_ = 0, d2h_ = 0, stepH2d_ = 0, stepD2h_ = 0;
+  void phaseBegin(int id);
+  void phaseEnd(int id, int launches);
 
   // per-step scene (host)
   std::vector<FpEmitter> emitters_;

@@ -173,7 +173,14 @@ class fp_stats(C.Structure):
         ("memory_bytes", C.c_uint64),
         ("last_vcycles", C.c_uint32),
         ("last_residual", C.c_double),
+        ("kernel_launches", C.c_uint64),
+        ("h2d_bytes", C.c_uint64),
+        ("d2h_bytes", C.c_uint64),
     ]
+
+
+class fp_phase(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_uint64), ("ms", C.c_double), ("voxels", C.c_double)]
 
 
 # Exported symbols of libfirepro.so (include/firepro.h), with their ctypes signatures.
@@ -190,6 +197,9 @@ SIGNATURES = {
     "fp_sim_read_field": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.c_size_t]),
     "fp_sim_read_table": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_size_t)]),
     "fp_sim_read_bricks": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint32)]),
+    "fp_sim_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "fp_sim_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "fp_sim_read_profile": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
 }
 
 _lib = None

@@ -79,6 +79,22 @@ class FluidSimulation:
         self._check(self.lib.fp_sim_read_table(self.h, tid, out.ctypes.data, C.byref(n2)))
         return out[: n2.value // 4]
 
+    def stream(self) -> int:
+        """The cudaStream_t the simulation enqueues on, as an integer handle."""
+        out = C.c_void_p()
+        self._check(self.lib.fp_sim_stream(self.h, C.byref(out)))
+        return out.value or 0
+
+    def set_profiling(self, on: bool):
+        self._check(self.lib.fp_sim_set_profiling(self.h, int(on)))
+
+    def profile(self) -> dict:
+        """Per-phase device time since profiling started: {name: (launches, ms, voxels)}."""
+        arr = (abi.fp_phase * 16)()
+        n = C.c_uint32(16)
+        self._check(self.lib.fp_sim_read_profile(self.h, arr, C.byref(n)))
+        return {arr[i].name.decode(): (arr[i].launches, arr[i].ms, arr[i].voxels) for i in range(n.value)}
+
     def read_bricks(self) -> np.ndarray:
         n = C.c_uint32(0)
         self.lib.fp_sim_read_bricks(self.h, None, C.byref(n))

@@ -224,4 +224,73 @@ class LargeScene(Scene):
         return make_frame(self.settings, self.comb, True, srcs, forces, (), cols)
 
 
-SCENES = {"single_plume": SinglePlume, "large_scene": LargeScene}
+class ForceScene(Scene):
+    """Every force kind (wind, turbulence, vortex, targeted radial), a rotated box and a
+    sphere collider, a mesh-mask collider, smoke and flame emitters with velocity
+    coupling, a one-step burst with Perlin variation at step 6, and an emitter that stops at
+    step 12 so its tiles linger and close."""
+
+    name = "force_scene"
+    steps = 80
+
+    def __init__(self, seed: int = 3):
+        self.seed = seed
+        self.settings = settings(buoyancy=1.6, smoke_weight=0.3, damping=0.2, vorticity=2.0, seed=seed)
+        self.comb = combustion()
+        # A 10x4x10-cell mesh occupancy mask: a slab with a hole.
+        self.mask_lo, self.mask_dims = (-14, 20, -6), (10, 4, 10)
+        bits = []
+        for z in range(10):
+            for y in range(4):
+                for x in range(10):
+                    bits.append(0 if (3 <= x <= 6 and 3 <= z <= 6) else 1)
+        words = [0] * ((len(bits) + 31) // 32)
+        for i, b in enumerate(bits):
+            if b:
+                words[i >> 5] |= 1 << (i & 31)
+        self.mask_words = words
+
+    def frame(self, step: int) -> FrameData:
+        c, s = math.cos(0.4), math.sin(0.4)
+        srcs = [
+            source(1, "sphere", (0.05, 0.25, 0.0), (0.2, 0.2, 0.2), flame=1.0, heat=1.5, smoke=0.5,
+                   velocity=(0.0, 1.4, 0.0), response=60.0),
+            source(2, "box", (-0.5, 0.3, 0.3), (0.12, 0.12, 0.12), flame=0.0, heat=0.85, smoke=4.0,
+                   velocity=(0.3, 1.2, 0.0), response=60.0),
+        ]
+        if step < 12:
+            srcs.append(source(3, "sphere", (0.6, 0.2, -0.4), (0.1, 0.1, 0.1), heat=2.0, fuel=1.0))
+        if step == 6:
+            srcs.append(source(99, "sphere", (0.0, 0.5, 0.0), (0.3, 0.3, 0.3), flame=1.0, heat=2.0 * 60, smoke=0.2 * 60,
+                               response=60.0, outward=8.0, variation=(0.5, 0.6)))
+        targets = [source(1, "sphere", (0.05, 0.25, 0.0), (0.2, 0.2, 0.2))]
+        forces = [force("wind", vector=(1.0, 0.0, 0.0), strength=0.8),
+                  force("turbulence", strength=1.5, scale=2.0),
+                  force("vortex", vector=(0.0, 1.0, 0.0), center=(0.0, 0.5, 0.0), strength=3.0, scale=0.5, lift=1.0,
+                        inward=0.5),
+                  force("radial", center=(0.05, 0.4, 0.0), strength=-2.0, scale=0.4, targeted=True, first_target=0,
+                        target_count=1)]
+        mesh = abi.fp_collider()
+        mesh.shape = abi.FP_SHAPE_MESH
+        mesh.lo[:] = self.mask_lo
+        mesh.dims[:] = self.mask_dims
+        mesh.mask_offset = 0
+        cols = [collider("box", (0.2, 0.9, 0.1), (0.25, 0.05, 0.2), axes=((c, s, 0), (-s, c, 0), (0, 0, 1))),
+                collider("sphere", (-0.4, 0.8, 0.3), (0.12, 0.12, 0.12)), mesh]
+        return make_frame(self.settings, self.comb, True, srcs, forces, targets, cols, self.mask_words)
+
+
+class EmptyScene(Scene):
+    """No sources, forces or colliders: nothing computes."""
+
+    name = "empty"
+
+    def __init__(self, seed: int = 1):
+        self.settings = settings(seed=seed)
+        self.comb = combustion()
+
+    def frame(self, step: int) -> FrameData:
+        return make_frame(self.settings, self.comb, False, [])
+
+
+SCENES = {"single_plume": SinglePlume, "large_scene": LargeScene, "force_scene": ForceScene, "empty": EmptyScene}
