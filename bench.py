@@ -50,7 +50,8 @@ MAX_GROW_STEPS = 600
 # write (4); multigrid = (8/7)(12 B x 3 post-sweeps + 9 B restriction + 8.5 B prolongation).
 BYTES_PER_VOXEL = {
     "predict": 68.0,
-    "correct_evolve": 100.0,
+    "correct": 36.0,
+    "evolve": 64.0,
     "curl": 28.0,
     "forces": 56.0,
     "divergence": 24.0,

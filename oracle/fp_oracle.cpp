@@ -567,9 +567,10 @@ struct Sim {
       flame.counts[ch] = (int)r.count;
     }
   }
-  // Every tile within the world box, or every tile (FluidSimulation.ts:1163-1188).
-  void bin(int kind, int index, bool hasBox, const R* lo, const R* hi) {
-    R tileSize = R(TILE_BRICKS * B) * h;
+  // Every tile within the world box, or every tile (FluidSimulation.ts:1163-1188). The
+  // reference's host arithmetic is JavaScript's: double precision, whatever the oracle's R.
+  void bin(int kind, int index, bool hasBox, const double* lo, const double* hi) {
+    double tileSize = double(TILE_BRICKS * B) * (double)h;
     if (!hasBox) {
       for (int s = 0; s < capacity; s++)
         if (snapshotState[s] != 0) lists[kind][s].push_back(index);
@@ -577,8 +578,8 @@ struct Sim {
     }
     int l[3], u[3];
     for (int a = 0; a < 3; a++) {
-      l[a] = floori((double)(lo[a] / tileSize));
-      u[a] = floori((double)(hi[a] / tileSize));
+      l[a] = floori(lo[a] / tileSize);
+      u[a] = floori(hi[a] / tileSize);
     }
     for (int z = l[2]; z <= u[2]; z++)
       for (int y = l[1]; y <= u[1]; y++)
@@ -589,7 +590,7 @@ struct Sim {
   }
   bool packScene(const fp_frame& f) {
     for (int k = 0; k < 3; k++) lists[k].assign(capacity, {});
-    R brick = R(B) * h;
+    double brick = double(B) * (double)h;
     emitters.clear();
     for (uint32_t i = 0; i < f.source_count; i++) {
       const fp_source& s = f.sources[i];
@@ -609,11 +610,11 @@ struct Sim {
       e.fuel = s.fuel_rate;
       int index = (int)emitters.size();
       emitters.push_back(e);
-      R lo[3], hi[3];
+      double lo[3], hi[3];
       for (int a = 0; a < 3; a++) {
-        R ext = std::max((R)s.size[a], (R)0.03f);
-        lo[a] = e.pos[a] - ext - 2 * brick;
-        hi[a] = e.pos[a] + ext + 2 * brick;
+        double ext = std::max((double)s.size[a], 0.03);
+        lo[a] = (double)s.position[a] - ext - 2 * brick;
+        hi[a] = (double)s.position[a] + ext + 2 * brick;
       }
       bin(0, index, true, lo, hi);
     }
@@ -623,14 +624,14 @@ struct Sim {
     for (uint32_t i = 0; i < f.collider_count; i++) {
       const fp_collider& c = f.colliders[i];
       Collider<R> k{};
-      R lo[3], hi[3];
+      double lo[3], hi[3];
       if (c.shape == FP_SHAPE_MESH) {
         k.kind = 2;
         for (int a = 0; a < 3; a++) {
           k.lo[a] = c.lo[a];
           k.size[a] = c.dims[a];
-          lo[a] = (R)((float)c.lo[a] * (float)h);
-          hi[a] = (R)((float)(c.lo[a] + c.dims[a]) * (float)h);
+          lo[a] = (double)c.lo[a] * (double)h;
+          hi[a] = (double)(c.lo[a] + c.dims[a]) * (double)h;
         }
         k.first = c.mask_offset;
       } else {
@@ -641,12 +642,13 @@ struct Sim {
           for (int b = 0; b < 3; b++) k.axes[a][b] = c.axes[a][b];
         }
         for (int a = 0; a < 3; a++) {
-          R ext = c.size[a];
+          double ext = c.size[a];
           if (k.kind == 1)
-            ext = std::fabs((R)c.axes[0][a]) * (R)c.size[0] + std::fabs((R)c.axes[1][a]) * (R)c.size[1] +
-                  std::fabs((R)c.axes[2][a]) * (R)c.size[2];
-          lo[a] = (R)c.position[a] - ext;
-          hi[a] = (R)c.position[a] + ext;
+            ext = std::fabs((double)c.axes[0][a]) * (double)c.size[0] +
+                  std::fabs((double)c.axes[1][a]) * (double)c.size[1] +
+                  std::fabs((double)c.axes[2][a]) * (double)c.size[2];
+          lo[a] = (double)c.position[a] - ext;
+          hi[a] = (double)c.position[a] + ext;
         }
       }
       colliders.push_back(k);
@@ -675,7 +677,7 @@ struct Sim {
       k.regionFirst = (int)regions.size();
       k.regionCount = 0;
       bool hasReach = false;
-      R lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
+      double lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
       if (k.targeted) {
         for (uint32_t t = 0; t < s.target_count; t++) {
           const fp_source& src = f.force_targets[s.first_target + t];
@@ -689,8 +691,8 @@ struct Sim {
           regions.push_back(r);
           k.regionCount++;
           for (int a = 0; a < 3; a++) {
-            R ext = std::max((R)src.size[a], (R)0.03f);
-            R l = r.center[a] - ext, u = r.center[a] + ext;
+            double ext = std::max((double)src.size[a], 0.03);
+            double l = (double)src.position[a] - ext, u = (double)src.position[a] + ext;
             if (!hasReach) { lo[a] = l; hi[a] = u; } else { lo[a] = std::min(lo[a], l); hi[a] = std::max(hi[a], u); }
           }
           hasReach = true;
@@ -700,7 +702,7 @@ struct Sim {
       if (!k.targeted) {
         bin(1, (int)i, false, nullptr, nullptr);
       } else {
-        R l[3], u[3];
+        double l[3], u[3];
         for (int a = 0; a < 3; a++) {
           l[a] = lo[a] - brick;
           u[a] = hi[a] + brick;
@@ -712,29 +714,29 @@ struct Sim {
   }
 
   // ---------------------------------------------------------------- host step
-  void needBox(const R* lo, const R* hi, R margin) {
-    R size = R(TILE_BRICKS * B) * h;
+  void needBox(const double* lo, const double* hi, double margin) {
+    double size = double(TILE_BRICKS * B) * (double)h;
     I3 l, u;
     for (int a = 0; a < 3; a++) {
-      l[a] = floori((double)((lo[a] - margin) / size));
-      u[a] = floori((double)((hi[a] + margin) / size));
+      l[a] = floori((lo[a] - margin) / size);
+      u[a] = floori((hi[a] + margin) / size);
     }
     dir.need(l, u, steps);
   }
   // FluidSimulation.ts:873-912 updateTiles
   void updateTiles(const fp_frame& f) {
     dir.retire(steps);
-    R reach = R(2 * B) * h;
-    R margin = reach + R(TILE_BRICKS * B) * h;
+    double reach = double(2 * B) * (double)h;
+    double margin = reach + double(TILE_BRICKS * B) * (double)h;
     for (uint32_t i = 0; i < f.source_count; i++) {
       const fp_source& s = f.sources[i];
       if (s.shape == FP_SHAPE_MESH) continue;
-      R ext = std::max(std::max(std::max((R)s.size[0], (R)s.size[1]), (R)s.size[2]), (R)0.03f) +
-              (R)s.outward_speed * R(0.25);
-      R lo[3], hi[3];
+      double ext = std::max(std::max(std::max((double)s.size[0], (double)s.size[1]), (double)s.size[2]), 0.03) +
+                   (double)s.outward_speed * 0.25;
+      double lo[3], hi[3];
       for (int a = 0; a < 3; a++) {
-        lo[a] = (R)s.position[a] - ext;
-        hi[a] = (R)s.position[a] + ext;
+        lo[a] = (double)s.position[a] - ext;
+        hi[a] = (double)s.position[a] + ext;
       }
       needBox(lo, hi, margin);
     }
@@ -794,23 +796,26 @@ struct Sim {
   }
 
   // ---------------------------------------------------------------- allocation
-  // sourceNear (fluid-allocation.wgsl:90-108)
+  // sourceNear (fluid-allocation.wgsl:90-108), in the kernel's f32 arithmetic: its result is
+  // an integer decision that must match the device's bit for bit.
   bool sourceNear(I3 b, int tile) {
-    R size = R(B) * h;
-    R lo[3], hi[3];
+    float hf = (float)h, dtf = (float)dt;
+    float size = (float)B * hf;
+    float lo[3], hi[3];
     for (int a = 0; a < 3; a++) {
-      lo[a] = R(b[a]) * size;
-      hi[a] = (R(b[a]) + R(1)) * size;
+      lo[a] = (float)b[a] * size;
+      hi[a] = ((float)b[a] + 1.f) * size;
     }
     for (int i : lists[0][tile]) {
       const Emitter<R>& e = emitters[i];
       if (!e.enabled) continue;
       bool inside = true;
       for (int a = 0; a < 3; a++) {
-        R motion = std::fabs(e.vel[a]) + std::fabs(e.outward);
-        R pad = std::min(size, R(2) * h + motion * dt);
-        R extent = std::max(e.size[a], (R)0.03f) + pad;
-        if (!(e.pos[a] + extent > lo[a] && e.pos[a] - extent < hi[a])) inside = false;
+        float motion = std::fabs((float)e.vel[a]) + std::fabs((float)e.outward);
+        float pad = std::min(size, 2.f * hf + motion * dtf);
+        float extent = std::max((float)e.size[a], 0.03f) + pad;
+        float pos = (float)e.pos[a];
+        if (!(pos + extent > lo[a] && pos - extent < hi[a])) inside = false;
       }
       if (inside) return true;
     }
@@ -916,16 +921,22 @@ struct Sim {
       uint32_t index = (uint32_t)((q[2] * c.size[1] + q[1]) * c.size[0] + q[0]);
       return ((masks[c.first + (index >> 5)] >> (index & 31u)) & 1u) != 0;
     }
-    R w[3] = {(R(x) + R(0.5)) * h, (R(y) + R(0.5)) * h, (R(z) + R(0.5)) * h};
-    R d[3];
+    // f32, as buildSolids computes it: the bits must match the device's exactly.
+    float hf = (float)h;
+    float w[3] = {((float)x + 0.5f) * hf, ((float)y + 0.5f) * hf, ((float)z + 0.5f) * hf};
+    float d[3];
     for (int a = 0; a < 3; a++) {
       // transpose(axes) * (w - center): row a = column a of axes.
-      R s = 0;
-      for (int k = 0; k < 3; k++) s += c.axes[a][k] * (w[k] - c.center[k]);
-      d[a] = std::fabs(s / c.extent[a]);
+      float s = (float)c.axes[a][0] * (w[0] - (float)c.center[0]);
+      s = s + (float)c.axes[a][1] * (w[1] - (float)c.center[1]);
+      s = s + (float)c.axes[a][2] * (w[2] - (float)c.center[2]);
+      d[a] = std::fabs(s / (float)c.extent[a]);
     }
-    if (c.kind == 1) return d[0] < 1 && d[1] < 1 && d[2] < 1;
-    return d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < R(1);
+    if (c.kind == 1) return d[0] < 1.f && d[1] < 1.f && d[2] < 1.f;
+    float r = d[0] * d[0];
+    r = r + d[1] * d[1];
+    r = r + d[2] * d[2];
+    return r < 1.f;
   }
   void buildSolidsBrick(uint32_t id, int slot) {
     I3 b = brickOf(id);

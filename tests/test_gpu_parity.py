@@ -17,9 +17,17 @@ TOL = parity.REL_L2_TOL
 
 
 def check(reports, tol=TOL, min_active=1):
+    """Allocation tables bit-exact; fields within `tol`. The activity flags come from float
+    threshold tests (content above the cutoff, motion pads) that the CUDA step evaluates in
+    FP32 and the oracle in FP64, so a value within rounding of a threshold may flip: at most
+    one flag word per 500 computing bricks (and 2) may differ. The allocation consumes the
+    CUDA flags on both sides, so its tables stay bit-exact regardless."""
     worst = {}
     for step, tables, fields, n in reports:
         for k, v in tables.items():
+            if k == "activity":
+                assert 0 <= v <= max(2, n // 500), f"step {step}: {v} activity words differ"
+                continue
             assert v == 0, f"step {step}: table {k} differs in {v} words"
         for k, v in fields.items():
             worst[k] = max(worst.get(k, 0.0), v)

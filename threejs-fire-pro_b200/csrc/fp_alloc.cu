@@ -24,8 +24,9 @@ __device__ bool sourceNear(const SimParams& P, int tile, int bx, int by, int bz)
     if (e.enabled < 0.5f) continue;
     bool inside = true;
     for (int a = 0; a < 3; a++) {
+      // Rounded products and sums, never contracted: an integer decision the oracle repeats.
       float motion = fabsf(e.vel[a]) + fabsf(e.outward);
-      float pad = fminf(size, 2.f * P.h + motion * P.dt);
+      float pad = fminf(size, __fadd_rn(__fmul_rn(2.f, P.h), __fmul_rn(motion, P.dt)));
       float extent = fmaxf(e.size[a], 0.03f) + pad;
       if (!(e.pos[a] + extent > lo[a] && e.pos[a] - extent < hi[a])) inside = false;
     }
@@ -283,13 +284,18 @@ __device__ bool insideCollider(const SimParams& P, const FpCollider& c, int x, i
   }
   float w[3] = {((float)x + 0.5f) * P.h, ((float)y + 0.5f) * P.h, ((float)z + 0.5f) * P.h};
   float d[3];
+  // Rounded products and sums, never contracted: the bits are compared with the oracle's.
   for (int a = 0; a < 3; a++) {
-    float s = c.axes[a][0] * (w[0] - c.center[0]) + c.axes[a][1] * (w[1] - c.center[1]) +
-              c.axes[a][2] * (w[2] - c.center[2]);
+    float s = __fmul_rn(c.axes[a][0], w[0] - c.center[0]);
+    s = __fadd_rn(s, __fmul_rn(c.axes[a][1], w[1] - c.center[1]));
+    s = __fadd_rn(s, __fmul_rn(c.axes[a][2], w[2] - c.center[2]));
     d[a] = fabsf(s / c.extent[a]);
   }
   if (kind == 1) return d[0] < 1.f && d[1] < 1.f && d[2] < 1.f;
-  return d[0] * d[0] + d[1] * d[1] + d[2] * d[2] < 1.f;
+  float r = __fmul_rn(d[0], d[0]);
+  r = __fadd_rn(r, __fmul_rn(d[1], d[1]));
+  r = __fadd_rn(r, __fmul_rn(d[2], d[2]));
+  return r < 1.f;
 }
 
 // buildSolids: a CTA per brick, a word of 32 cells per thread.

@@ -358,16 +358,18 @@ int Engine::applyTiles() {
 // updateTiles (FluidSimulation.ts:873-912).
 void Engine::updateTiles(const fp_frame& f) {
   dir_.retire(steps_);
-  float brick = (float)B_ * h_, tile = (float)(TILE_BRICKS * B_) * h_;
-  float margin = 2.f * brick + tile;
+  // Host arithmetic in double precision, as the reference's JavaScript does it.
+  double h = h_, tile = (double)(TILE_BRICKS * B_) * h;
+  double margin = (double)(2 * B_) * h + tile;
   for (uint32_t i = 0; i < f.source_count; i++) {
     const fp_source& s = f.sources[i];
     if (s.shape == FP_SHAPE_MESH) continue;
-    float ext = std::max(std::max(std::max(s.size[0], s.size[1]), s.size[2]), 0.03f) + s.outward_speed * 0.25f;
+    double ext = std::max(std::max(std::max((double)s.size[0], (double)s.size[1]), (double)s.size[2]), 0.03) +
+                 (double)s.outward_speed * 0.25;
     int lo[3], hi[3];
     for (int a = 0; a < 3; a++) {
-      lo[a] = (int)std::floor((s.position[a] - ext - margin) / tile);
-      hi[a] = (int)std::floor((s.position[a] + ext + margin) / tile);
+      lo[a] = (int)std::floor(((double)s.position[a] - ext - margin) / tile);
+      hi[a] = (int)std::floor(((double)s.position[a] + ext + margin) / tile);
     }
     dir_.need(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], steps_);
   }
@@ -418,14 +420,14 @@ int Engine::packFlame(const fp_combustion& c, float dt) {
 }
 
 // Every tile within the world box (FluidSimulation.ts:1163-1188); all tiles without one.
-void Engine::bin(int kind, int index, const float* lo, const float* hi, std::vector<std::vector<uint32_t>>& lists) {
+void Engine::bin(int kind, int index, const double* lo, const double* hi, std::vector<std::vector<uint32_t>>& lists) {
   const auto& slots = dir_.slots();
   if (!lo) {
     for (size_t s = 0; s < slots.size(); s++)
       if (slots[s].alive) lists[(size_t)s * 3 + kind].push_back((uint32_t)index);
     return;
   }
-  float tile = (float)(TILE_BRICKS * B_) * h_;
+  double tile = (double)(TILE_BRICKS * B_) * (double)h_;
   int l[3], u[3];
   for (int a = 0; a < 3; a++) {
     l[a] = (int)std::floor(lo[a] / tile);
@@ -453,7 +455,8 @@ void Engine::bin(int kind, int index, const float* lo, const float* hi, std::vec
 // Returns whether the colliders changed.
 bool Engine::packScene(const fp_frame& f) {
   std::vector<std::vector<uint32_t>> lists((size_t)capacity_ * 3);
-  float brick = (float)B_ * h_;
+  // Reach boxes in double precision, as the reference's JavaScript computes them.
+  double brick = (double)B_ * (double)h_;
   emitters_.clear();
   for (uint32_t i = 0; i < f.source_count; i++) {
     const fp_source& s = f.sources[i];
@@ -476,11 +479,11 @@ bool Engine::packScene(const fp_frame& f) {
     e.fuel = s.fuel_rate;
     int index = (int)emitters_.size();
     emitters_.push_back(e);
-    float lo[3], hi[3];
+    double lo[3], hi[3];
     for (int a = 0; a < 3; a++) {
-      float ext = std::max(s.size[a], 0.03f);
-      lo[a] = s.position[a] - ext - 2.f * brick;
-      hi[a] = s.position[a] + ext + 2.f * brick;
+      double ext = std::max((double)s.size[a], 0.03);
+      lo[a] = (double)s.position[a] - ext - 2 * brick;
+      hi[a] = (double)s.position[a] + ext + 2 * brick;
     }
     bin(0, index, lo, hi, lists);
   }
@@ -489,14 +492,14 @@ bool Engine::packScene(const fp_frame& f) {
   for (uint32_t i = 0; i < f.collider_count; i++) {
     const fp_collider& c = f.colliders[i];
     FpCollider k{};
-    float lo[3], hi[3];
+    double lo[3], hi[3];
     if (c.shape == FP_SHAPE_MESH) {
       k.kind = 2.f;
       for (int a = 0; a < 3; a++) {
         k.lo[a] = c.lo[a];
         k.size[a] = c.dims[a];
-        lo[a] = (float)c.lo[a] * h_;
-        hi[a] = (float)(c.lo[a] + c.dims[a]) * h_;
+        lo[a] = (double)c.lo[a] * (double)h_;
+        hi[a] = (double)(c.lo[a] + c.dims[a]) * (double)h_;
       }
       k.first = (int)c.mask_offset;
     } else {
@@ -507,11 +510,12 @@ bool Engine::packScene(const fp_frame& f) {
         for (int b = 0; b < 3; b++) k.axes[a][b] = c.axes[a][b];
       }
       for (int a = 0; a < 3; a++) {
-        float ext = c.size[a];
+        double ext = c.size[a];
         if (c.shape == FP_SHAPE_BOX)
-          ext = std::fabs(c.axes[0][a]) * c.size[0] + std::fabs(c.axes[1][a]) * c.size[1] + std::fabs(c.axes[2][a]) * c.size[2];
-        lo[a] = c.position[a] - ext;
-        hi[a] = c.position[a] + ext;
+          ext = std::fabs((double)c.axes[0][a]) * (double)c.size[0] + std::fabs((double)c.axes[1][a]) * (double)c.size[1] +
+                std::fabs((double)c.axes[2][a]) * (double)c.size[2];
+        lo[a] = (double)c.position[a] - ext;
+        hi[a] = (double)c.position[a] + ext;
       }
     }
     colliders_.push_back(k);
@@ -540,7 +544,7 @@ bool Engine::packScene(const fp_frame& f) {
     k.targeted = s.targeted ? 1.f : 0.f;
     k.regionFirst = (float)regions_.size();
     bool has = false;
-    float lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
+    double lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
     int count = 0;
     if (s.targeted) {
       for (uint32_t t = 0; t < s.target_count && s.first_target + t < f.force_target_count; t++) {
@@ -555,8 +559,8 @@ bool Engine::packScene(const fp_frame& f) {
         regions_.push_back(r);
         count++;
         for (int a = 0; a < 3; a++) {
-          float ext = std::max(src.size[a], 0.03f);
-          float l = src.position[a] - ext, u = src.position[a] + ext;
+          double ext = std::max((double)src.size[a], 0.03);
+          double l = (double)src.position[a] - ext, u = (double)src.position[a] + ext;
           lo[a] = has ? std::min(lo[a], l) : l;
           hi[a] = has ? std::max(hi[a], u) : u;
         }
@@ -568,7 +572,7 @@ bool Engine::packScene(const fp_frame& f) {
     if (!s.targeted) {
       bin(1, (int)i, nullptr, nullptr, lists);
     } else {
-      float l[3], u[3];
+      double l[3], u[3];
       for (int a = 0; a < 3; a++) {
         l[a] = lo[a] - brick;
         u[a] = hi[a] + brick;
@@ -748,7 +752,7 @@ int Engine::setProfiling(bool on) {
 }
 
 int Engine::readProfile(fp_phase* out, uint32_t* count) {
-  static const char* names[PH_COUNT] = {"allocation", "topology", "predict", "correct_evolve", "curl",
+  static const char* names[PH_COUNT] = {"allocation", "topology", "predict", "correct", "evolve", "curl",
                                         "forces", "divergence", "multigrid", "project"};
   int rc = consumeReadback();
   if (rc) return rc;
@@ -770,7 +774,7 @@ int Engine::readProfile(fp_phase* out, uint32_t* count) {
 void Engine::vcycle(int level, int cur[]) {
   SimParams* dP = dParams();
   if (level == bottom_) {
-    if (capacity_ <= 1024) {
+    if (capacity_ <= fp_bottom_capacity()) {
       fp_launch_bottom(dP, level, 19, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]), capacity_, stream_);
       launches_++;
       cur[level] = 1 - cur[level];
@@ -856,11 +860,14 @@ int Engine::step(const fp_frame& f, float dt) {
   phaseEnd(PH_TOPO, geometryDirty_ ? 2 : 1);
   geometryDirty_ = false;
   phaseBegin(PH_PREDICT);
-  fp_launch_predict(dP, sms_, stream_);
+  fp_launch_predict(dP, B_, sms_, stream_);
   phaseEnd(PH_PREDICT, 1);
   phaseBegin(PH_CORRECT);
-  fp_launch_correct_evolve(dP, sms_, stream_);
+  fp_launch_correct(dP, B_, sms_, stream_);
   phaseEnd(PH_CORRECT, 1);
+  phaseBegin(PH_EVOLVE);
+  fp_launch_evolve(dP, B_, sms_, stream_);
+  phaseEnd(PH_EVOLVE, 1);
   if (f.simulation.vorticity != 0.f) {
     phaseBegin(PH_CURL);
     fp_launch_curl(dP, sms_, stream_);

@@ -130,8 +130,8 @@ class Engine {
   cudaEvent_t readEvent_ = nullptr;
 
   // per-phase device timing (GpuProfiler.ts), and the launch count
-  enum PhaseId { PH_ALLOC, PH_TOPO, PH_PREDICT, PH_CORRECT, PH_CURL, PH_FORCES, PH_DIVERGENCE, PH_MULTIGRID,
-                 PH_PROJECT, PH_COUNT };
+  enum PhaseId { PH_ALLOC, PH_TOPO, PH_PREDICT, PH_CORRECT, PH_EVOLVE, PH_CURL, PH_FORCES, PH_DIVERGENCE,
+                 PH_MULTIGRID, PH_PROJECT, PH_COUNT };
   struct Phase {
     uint64_t launches = 0, stepLaunches = 0;
     double ms = 0, voxels = 0;
@@ -171,7 +171,7 @@ class Engine {
   void updateTiles(const fp_frame& f);
   int packFlame(const fp_combustion& c, float dt);
   bool packScene(const fp_frame& f);
-  void bin(int kind, int index, const float* lo, const float* hi, std::vector<std::vector<uint32_t>>& lists);
+  void bin(int kind, int index, const double* lo, const double* hi, std::vector<std::vector<uint32_t>>& lists);
   int uploadScene();
   void fillParams(const fp_frame& f, float dt);
   int consumeReadback();

@@ -6,8 +6,9 @@
 #include "fp_types.h"
 
 void fp_launch_allocation(const SimParams* dP, int capacity, bool solids, int sms, cudaStream_t st);
-void fp_launch_predict(const SimParams* dP, int sms, cudaStream_t st);
-void fp_launch_correct_evolve(const SimParams* dP, int sms, cudaStream_t st);
+void fp_launch_predict(const SimParams* dP, int B, int sms, cudaStream_t st);
+void fp_launch_correct(const SimParams* dP, int B, int sms, cudaStream_t st);
+void fp_launch_evolve(const SimParams* dP, int B, int sms, cudaStream_t st);
 void fp_launch_curl(const SimParams* dP, int sms, cudaStream_t st);
 void fp_launch_forces(const SimParams* dP, int B, int sms, cudaStream_t st);
 void fp_launch_divergence(const SimParams* dP, float* pOut, int sms, cudaStream_t st);
@@ -26,3 +27,5 @@ void fp_launch_prolong(const SimParams* dP, int level, bool tiles, const float* 
                        int capacity, int sms, cudaStream_t st);
 void fp_launch_bottom(const SimParams* dP, int level, int iterations, const float* rhs, const float* pin, float* pout,
                       int capacity, cudaStream_t st);
+// Most tile slots the one-CTA bottom solve holds in shared memory.
+int fp_bottom_capacity();

@@ -226,54 +226,60 @@ __global__ void __launch_bounds__(64) k_level_tiles(const SimParams* __restrict_
   }
 }
 
-// relaxCoarse (pressure.wgsl:549-599): the bottom level, a tile slot per thread, every
-// iteration in one CTA.
+// relaxCoarse (pressure.wgsl:549-599): the bottom level, one cell per tile slot, every
+// iteration in one CTA. Tile slots stride over the threads; each slot's flags (SOLIDF where
+// it is no unknown) and a ping-pong pair of values live in shared memory, so any number of
+// tiles that fits 12 bytes a slot needs one launch.
 __global__ void __launch_bounds__(1024) k_bottom(const SimParams* __restrict__ Pp, int level, int iterations,
                                                   const float* __restrict__ rhs, const float* __restrict__ pin,
                                                   float* __restrict__ pout) {
   const SimParams& P = *Pp;
-  __shared__ float value[1024];
-  int t = threadIdx.x;
-  bool valid = false;
-  uint32_t f = SOLIDF;
-  float source = 0.f, v = 0.f;
-  int nb[6] = {-1, -1, -1, -1, -1, -1};
-  if (t < P.capacity) {
+  extern __shared__ float bottomSmem[];
+  int cap = P.capacity;
+  float* cur = bottomSmem;
+  float* nxt = bottomSmem + cap;
+  uint32_t* flags = reinterpret_cast<uint32_t*>(bottomSmem + 2 * cap);
+  for (int t = threadIdx.x; t < cap; t += blockDim.x) {
     int4 rec = __ldg(&P.tileRec[t]);
-    valid = rec.w != 0;
-    if (valid) {
+    uint32_t f = SOLIDF | (rec.w != 0 ? 0x80000000u : 0u);  // top bit: a live tile slot
+    float v = 0.f;
+    if (rec.w != 0) {
       Home H = enterTile(P, t, rec);
       if (activeCell(P, H, rec.x, rec.y, rec.z, level)) {
-        f = expandFlags(P.topo[level][t]);
-        source = rhs[t];
+        f = expandFlags(P.topo[level][t]) | 0x80000000u;
         v = pin[t];
       }
-      nb[0] = P.tileNbr[t * 27 + nbrIndex(1, 0, 0)];
-      nb[1] = P.tileNbr[t * 27 + nbrIndex(-1, 0, 0)];
-      nb[2] = P.tileNbr[t * 27 + nbrIndex(0, 1, 0)];
-      nb[3] = P.tileNbr[t * 27 + nbrIndex(0, -1, 0)];
-      nb[4] = P.tileNbr[t * 27 + nbrIndex(0, 0, 1)];
-      nb[5] = P.tileNbr[t * 27 + nbrIndex(0, 0, -1)];
     }
+    flags[t] = f;
+    cur[t] = v;
   }
-  value[t] = v;
   __syncthreads();
-  float diag = diagOf(f);
+  const int nbIndex[6] = {nbrIndex(1, 0, 0), nbrIndex(-1, 0, 0), nbrIndex(0, 1, 0),
+                          nbrIndex(0, -1, 0), nbrIndex(0, 0, 1), nbrIndex(0, 0, -1)};
   for (int it = 0; it < iterations; it++) {
-    float next = 0.f;
-    if (valid && !(f & SOLIDF)) {
-      float w[6];
-      for (int k = 0; k < 6; k++) w[k] = ((f >> k) & 1u) && nb[k] >= 0 ? value[nb[k]] : 0.f;
-      float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
-      float cand = (sum - source) / fmaxf(diag, 1e-12f);
-      next = mixf(v, cand, 0.8f);
+    for (int t = threadIdx.x; t < cap; t += blockDim.x) {
+      uint32_t f = flags[t];
+      float next = 0.f;
+      if ((f & 0x80000000u) && !(f & SOLIDF)) {
+        float w[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+          int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
+          w[k] = n >= 0 ? cur[n] : 0.f;
+        }
+        float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
+        float cand = (sum - rhs[t]) / fmaxf(diagOf(f & 63u), 1e-12f);
+        next = mixf(cur[t], cand, 0.8f);
+      }
+      nxt[t] = next;
     }
     __syncthreads();
-    value[t] = next;
-    v = next;
-    __syncthreads();
+    float* tmp = cur;
+    cur = nxt;
+    nxt = tmp;
   }
-  if (valid) pout[t] = v;
+  for (int t = threadIdx.x; t < cap; t += blockDim.x)
+    if (flags[t] & 0x80000000u) pout[t] = cur[t];
 }
 
 // cellTopology (pressure.wgsl:208-222): solid, or the sides whose neighbours are not solid.
@@ -382,8 +388,15 @@ void fp_launch_prolong(const SimParams* dP, int level, bool tiles, const float* 
     k_level_bricks<PROLONG><<<sms * 4, 256, 0, st>>>(dP, A);
 }
 
+int fp_bottom_capacity() { return (200 * 1024) / 12; }
+
 void fp_launch_bottom(const SimParams* dP, int level, int iterations, const float* rhs, const float* pin, float* pout,
                       int capacity, cudaStream_t st) {
-  (void)capacity;
-  k_bottom<<<1, 1024, 0, st>>>(dP, level, iterations, rhs, pin, pout);
+  size_t smem = (size_t)capacity * 12;
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    configured = true;
+  }
+  k_bottom<<<1, 1024, smem, st>>>(dP, level, iterations, rhs, pin, pout);
 }

@@ -7,30 +7,109 @@
 // fluid-field-evolution.wgsl, fluid-forces.wgsl and force-fields.wgsl. Samples read the
 // neighbour bricks' cells through the brick's 27-entry record (shared memory) where the
 // reference reads a texture apron that copies them; bricks without a slot read zero.
+//
+// Staging: for 8^3 bricks the transport kernels first copy the fields they sample, over the
+// home brick and a HALO-cell rim, into shared memory ([channel][S^3], S = B + 2 HALO), with
+// coalesced loads through the neighbour record. Trilinear taps inside the rim then read
+// shared memory; taps past it (traces longer than the rim) take the directory path. Both
+// paths compute the same sums in the same order.
 #include "fp_device.cuh"
 #include "fp_launch.h"
 
 namespace {
 
 constexpr int THREADS = 256;
+constexpr int HALO = 2;
 
-FP_DEV float velComp(const SimParams& P, const Home& H, const float* pool, float px, float py, float pz, int c) {
+// Where the staged copy sits: its first cell and its side.
+struct Stage {
+  int ox, oy, oz, S, S3;
+};
+
+// A field a kernel reads: the pool and, when staged, its shared copy.
+struct Field {
+  const float* pool;
+  int ch;
+  const float* sm;
+};
+
+FP_DEV float fieldCell(const SimParams& P, const Home& H, const Stage& G, const Field& f, int c, int x, int y, int z) {
+  if (f.sm) {
+    unsigned lx = (unsigned)(x - G.ox), ly = (unsigned)(y - G.oy), lz = (unsigned)(z - G.oz);
+    if (lx < (unsigned)G.S && ly < (unsigned)G.S && lz < (unsigned)G.S)
+      return f.sm[c * G.S3 + ((int)lz * G.S + (int)ly) * G.S + (int)lx];
+  }
+  return cellAt(P, H, f.pool, f.ch, c, x, y, z);
+}
+
+// Trilinear sample at `pos` in cell units (fluid-sampling.wgsl:85-114).
+FP_DEV float fieldSample(const SimParams& P, const Home& H, const Stage& G, const Field& f, int c, float px, float py,
+                         float pz) {
+  if (f.sm) {
+    float qx = px - 0.5f, qy = py - 0.5f, qz = pz - 0.5f;
+    int x0 = (int)floorf(qx), y0 = (int)floorf(qy), z0 = (int)floorf(qz);
+    unsigned lx = (unsigned)(x0 - G.ox), ly = (unsigned)(y0 - G.oy), lz = (unsigned)(z0 - G.oz);
+    if (lx < (unsigned)(G.S - 1) && ly < (unsigned)(G.S - 1) && lz < (unsigned)(G.S - 1)) {
+      float fx = qx - (float)x0, fy = qy - (float)y0, fz = qz - (float)z0;
+      const float* b = f.sm + c * G.S3 + ((int)lz * G.S + (int)ly) * G.S + (int)lx;
+      int S = G.S, S2 = G.S * G.S;
+      float v = 0.f;
+      v += b[0] * ((1.f - fx) * (1.f - fy) * (1.f - fz));
+      v += b[1] * (fx * (1.f - fy) * (1.f - fz));
+      v += b[S] * ((1.f - fx) * fy * (1.f - fz));
+      v += b[S + 1] * (fx * fy * (1.f - fz));
+      v += b[S2] * ((1.f - fx) * (1.f - fy) * fz);
+      v += b[S2 + 1] * (fx * (1.f - fy) * fz);
+      v += b[S2 + S] * ((1.f - fx) * fy * fz);
+      v += b[S2 + S + 1] * (fx * fy * fz);
+      return v;
+    }
+  }
+  return sampleCells(P, H, f.pool, f.ch, c, px, py, pz);
+}
+
+// Copy channels of a pool over the staged box into shared memory; zero where no slot.
+FP_DEV void stageField(const SimParams& P, const Home& H, const Stage& G, float* sm, const float* pool, int ch) {
+  for (int i = threadIdx.x; i < G.S3; i += blockDim.x) {
+    int lx = i % G.S, ly = (i / G.S) % G.S, lz = i / (G.S * G.S);
+    int x = G.ox + lx, y = G.oy + ly, z = G.oz + lz;
+    int s = brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift);
+    size_t base = s < 0 ? 0 : (size_t)s * ch * P.N + localCell(P, x, y, z);
+    for (int c = 0; c < ch; c++) sm[c * G.S3 + i] = s < 0 ? 0.f : pool[base + (size_t)c * P.N];
+  }
+}
+
+FP_DEV Stage stageOf(const SimParams& P, const Home& H, bool staged) {
+  Stage G;
+  G.S = staged ? P.B + 2 * HALO : 0;
+  G.S3 = G.S * G.S * G.S;
+  G.ox = H.bx * P.B - HALO;
+  G.oy = H.by * P.B - HALO;
+  G.oz = H.bz * P.B - HALO;
+  return G;
+}
+
+FP_DEV float velComp(const SimParams& P, const Home& H, const Stage& G, const Field& v, float px, float py, float pz,
+                     int c) {
   float q[3] = {px, py, pz};
   q[c] -= 0.5f * P.h;
-  return sampleCells(P, H, pool, 3, c, q[0] / P.h, q[1] / P.h, q[2] / P.h);
+  return fieldSample(P, H, G, v, c, q[0] / P.h, q[1] / P.h, q[2] / P.h);
 }
 // velocityAt (fluid-advection.wgsl:17-21).
-FP_DEV float3 velocityAt(const SimParams& P, const Home& H, const float* pool, float px, float py, float pz) {
-  return make_float3(velComp(P, H, pool, px, py, pz, 0), velComp(P, H, pool, px, py, pz, 1),
-                     velComp(P, H, pool, px, py, pz, 2));
+FP_DEV float3 velocityAt(const SimParams& P, const Home& H, const Stage& G, const Field& v, float px, float py,
+                         float pz) {
+  return make_float3(velComp(P, H, G, v, px, py, pz, 0), velComp(P, H, G, v, px, py, pz, 1),
+                     velComp(P, H, G, v, px, py, pz, 2));
 }
 FP_DEV float get(const float3& v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
 
 // velocityOnFace (fluid-advection.wgsl:26-44): the face's own component is stored.
-FP_DEV float3 velocityOnFace(const SimParams& P, const Home& H, int x, int y, int z, int c, float3 orig) {
+FP_DEV float3 velocityOnFace(const SimParams& P, const Home& H, const Stage& G, const Field& v, int x, int y, int z,
+                             int c, float3 orig) {
   float fp[3] = {(float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f};
   fp[c] += 0.5f;
   float r[3];
+#pragma unroll
   for (int k = 0; k < 3; k++) {
     if (k == c) {
       r[k] = get(orig, k);
@@ -38,12 +117,12 @@ FP_DEV float3 velocityOnFace(const SimParams& P, const Home& H, int x, int y, in
     }
     float q[3] = {fp[0], fp[1], fp[2]};
     q[k] -= 0.5f;
-    r[k] = sampleCells(P, H, P.vel, 3, k, q[0], q[1], q[2]);
+    r[k] = fieldSample(P, H, G, v, k, q[0], q[1], q[2]);
   }
   return make_float3(r[0], r[1], r[2]);
 }
 
-// packDonor / unpackDonor (fluid-advection.wgsl:79-100), 5 bits an axis.
+// packDonor (fluid-advection.wgsl:79-95), 5 bits an axis; 1 << 15 asks for a retrace.
 FP_DEV uint32_t packDonor(int ox, int oy, int oz) {
   int bx = ox + 16, by = oy + 16, bz = oz + 16;
   if (bx < 0 || by < 0 || bz < 0 || bx >= 32 || by >= 32 || bz >= 32) return 1u << 15;
@@ -61,13 +140,23 @@ FP_DEV void cellOf(const SimParams& P, const Home& H, int c, int& x, int& y, int
 // Predictors: advectVelocityWithBounds (fluid-velocity-transport.wgsl:28-100) and
 // advectScalars (fluid-scalar-transport.wgsl:38-142), fused: both read only the velocity and
 // the scalars at the start of the step.
+template <bool STAGED>
 __global__ void __launch_bounds__(THREADS) k_predict(const SimParams* __restrict__ Pp) {
   const SimParams& P = *Pp;
   __shared__ int nslot[27];
+  extern __shared__ float smem[];
   uint32_t total = P.counters->active;
   for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
     uint32_t id = P.active[i];
     Home H = enterBrick(P, id, nslot);
+    Stage G = stageOf(P, H, STAGED);
+    Field V{P.vel, 3, STAGED ? smem : nullptr};
+    Field F{P.fld, 4, STAGED ? smem + 3 * G.S3 : nullptr};
+    if (STAGED) {
+      stageField(P, H, G, smem, P.vel, 3);
+      stageField(P, H, G, smem + 3 * G.S3, P.fld, 4);
+      __syncthreads();
+    }
     size_t slot = (size_t)nslot[13];
     const size_t N = P.N;
     for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
@@ -79,7 +168,7 @@ __global__ void __launch_bounds__(THREADS) k_predict(const SimParams* __restrict
         for (int dz = 0; dz < 2; dz++)
           for (int dy = 0; dy < 2; dy++)
             for (int dx = 0; dx < 2; dx++) {
-              float v = cellAt(P, H, P.vel, 3, k, x + dx, y + dy, z + dz);
+              float v = fieldCell(P, H, G, V, k, x + dx, y + dy, z + dz);
               lo = fminf(lo, v);
               hi = fmaxf(hi, v);
             }
@@ -90,13 +179,14 @@ __global__ void __launch_bounds__(THREADS) k_predict(const SimParams* __restrict
       if (solidAt(P, H, px, py, pz)) {
         for (int k = 0; k < 3; k++) P.velP[(slot * 3 + k) * N + c] = 0.f;
       } else {
-        float3 orig = make_float3(P.vel[(slot * 3 + 0) * N + c], P.vel[(slot * 3 + 1) * N + c],
-                                  P.vel[(slot * 3 + 2) * N + c]);
+        float3 orig = make_float3(fieldCell(P, H, G, V, 0, x, y, z), fieldCell(P, H, G, V, 1, x, y, z),
+                                  fieldCell(P, H, G, V, 2, x, y, z));
+#pragma unroll
         for (int comp = 0; comp < 3; comp++) {
           float face[3] = {px, py, pz};
           face[comp] += 0.5f * P.h;
-          float3 fv = velocityOnFace(P, H, x, y, z, comp, orig);
-          float3 vm = velocityAt(P, H, P.vel, face[0] - 0.5f * P.dt * fv.x, face[1] - 0.5f * P.dt * fv.y,
+          float3 fv = velocityOnFace(P, H, G, V, x, y, z, comp, orig);
+          float3 vm = velocityAt(P, H, G, V, face[0] - 0.5f * P.dt * fv.x, face[1] - 0.5f * P.dt * fv.y,
                                  face[2] - 0.5f * P.dt * fv.z);
           float dep[3] = {face[0] - P.dt * vm.x, face[1] - P.dt * vm.y, face[2] - P.dt * vm.z};
           float sh[3] = {dep[0], dep[1], dep[2]};
@@ -104,16 +194,16 @@ __global__ void __launch_bounds__(THREADS) k_predict(const SimParams* __restrict
           int bx = (int)floorf(sh[0] / P.h - 0.5f), by = (int)floorf(sh[1] / P.h - 0.5f),
               bz = (int)floorf(sh[2] / P.h - 0.5f);
           P.donors[(slot * 3 + comp) * N + c] = (uint16_t)packDonor(bx - x, by - y, bz - z);
-          P.velP[(slot * 3 + comp) * N + c] = velComp(P, H, P.vel, dep[0], dep[1], dep[2], comp);
+          P.velP[(slot * 3 + comp) * N + c] = velComp(P, H, G, V, dep[0], dep[1], dep[2], comp);
         }
       }
       // Scalars: a cell-centred RK2 back trace, the predictor and its donors' range.
-      float3 cv = velocityAt(P, H, P.vel, px, py, pz);
-      float3 vm = velocityAt(P, H, P.vel, px - 0.5f * P.dt * cv.x, py - 0.5f * P.dt * cv.y, pz - 0.5f * P.dt * cv.z);
+      float3 cv = velocityAt(P, H, G, V, px, py, pz);
+      float3 vm = velocityAt(P, H, G, V, px - 0.5f * P.dt * cv.x, py - 0.5f * P.dt * cv.y, pz - 0.5f * P.dt * cv.z);
       float dx_ = px - P.dt * vm.x, dy_ = py - P.dt * vm.y, dz_ = pz - P.dt * vm.z;
       float out[4];
       if (!P.maccormack) {
-        for (int k = 0; k < 4; k++) out[k] = sampleCells(P, H, P.fld, 4, k, dx_ / P.h, dy_ / P.h, dz_ / P.h);
+        for (int k = 0; k < 4; k++) out[k] = fieldSample(P, H, G, F, k, dx_ / P.h, dy_ / P.h, dz_ / P.h);
         out[2] = clamp01(out[2]);
       } else {
         float dc[3] = {(float)x + (dx_ - px) / P.h, (float)y + (dy_ - py) / P.h, (float)z + (dz_ - pz) / P.h};
@@ -126,20 +216,12 @@ __global__ void __launch_bounds__(THREADS) k_predict(const SimParams* __restrict
         float mn0 = 65504.f, mn1 = 65504.f, mn3 = 65504.f, mx0 = -65504.f, mx1 = -65504.f, mx3 = -65504.f;
         float lmin = 1.f, lmax = 0.f;
         float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
-        int sh = P.shift;
         for (int dz = 0; dz < 2; dz++)
           for (int dy = 0; dy < 2; dy++)
             for (int dx = 0; dx < 2; dx++) {
               int cx = base[0] + dx, cy = base[1] + dy, cz = base[2] + dz;
-              int s = brickSlot(P, H, cx >> sh, cy >> sh, cz >> sh);
-              float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-              if (s >= 0) {
-                size_t o = (size_t)s * 4 * N + localCell(P, cx, cy, cz);
-                s0 = P.fld[o];
-                s1 = P.fld[o + N];
-                s2 = P.fld[o + 2 * N];
-                s3 = P.fld[o + 3 * N];
-              }
+              float s0 = fieldCell(P, H, G, F, 0, cx, cy, cz), s1 = fieldCell(P, H, G, F, 1, cx, cy, cz),
+                    s2 = fieldCell(P, H, G, F, 2, cx, cy, cz), s3 = fieldCell(P, H, G, F, 3, cx, cy, cz);
               mn0 = fminf(mn0, s0); mn1 = fminf(mn1, s1); mn3 = fminf(mn3, s3);
               mx0 = fmaxf(mx0, s0); mx1 = fmaxf(mx1, s1); mx3 = fmaxf(mx3, s3);
               lmin = fminf(lmin, s2);
@@ -162,39 +244,38 @@ __global__ void __launch_bounds__(THREADS) k_predict(const SimParams* __restrict
 }
 
 // ---------------------------------------------------------------------------------------
-// Corrections: correctVelocity (fluid-velocity-transport.wgsl:104-179) and evolveFields
-// (fluid-field-evolution.wgsl:9-84 with fluid-scalar-transport.wgsl:144-199 and
-// fluid-content.wgsl:29-64), fused: both read the predictors and the start-of-step fields.
-__global__ void __launch_bounds__(THREADS) k_correct_evolve(const SimParams* __restrict__ Pp) {
+// correctVelocity (fluid-velocity-transport.wgsl:104-179): bounded MacCormack correction.
+template <bool STAGED>
+__global__ void __launch_bounds__(THREADS) k_correct(const SimParams* __restrict__ Pp) {
   const SimParams& P = *Pp;
   __shared__ int nslot[27];
-  __shared__ uint32_t busyAll, expandsAll;
+  extern __shared__ float smem[];
   uint32_t total = P.counters->active;
-  uint32_t bricks = (uint32_t)P.capacity * 64u;
   for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
     uint32_t id = P.active[i];
-    if (threadIdx.x == 0) {
-      busyAll = 0;
-      expandsAll = 0;
-    }
     Home H = enterBrick(P, id, nslot);
+    Stage G = stageOf(P, H, STAGED);
+    Field V{P.vel, 3, STAGED ? smem : nullptr};
+    Field Vp{P.velP, 3, STAGED ? smem + 3 * G.S3 : nullptr};
+    if (STAGED) {
+      stageField(P, H, G, smem, P.vel, 3);
+      stageField(P, H, G, smem + 3 * G.S3, P.velP, 3);
+      __syncthreads();
+    }
     size_t slot = (size_t)nslot[13];
     const size_t N = P.N;
-    int tile = (int)(id >> 6);
-    uint32_t busy = 0;
-    bool expands = false;
     for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
       int x, y, z;
       cellOf(P, H, c, x, y, z);
       float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
       bool solid = solidAt(P, H, px, py, pz);
-      float3 orig = make_float3(P.vel[(slot * 3 + 0) * N + c], P.vel[(slot * 3 + 1) * N + c],
-                                P.vel[(slot * 3 + 2) * N + c]);
-      // --- velocity correction
+      float3 orig = make_float3(fieldCell(P, H, G, V, 0, x, y, z), fieldCell(P, H, G, V, 1, x, y, z),
+                                fieldCell(P, H, G, V, 2, x, y, z));
+#pragma unroll
       for (int comp = 0; comp < 3; comp++) {
         float result = 0.f;
         if (!solid) {
-          float predicted = P.velP[(slot * 3 + comp) * N + c];
+          float predicted = fieldCell(P, H, G, Vp, comp, x, y, z);
           float face[3] = {px, py, pz};
           face[comp] += 0.5f * P.h;
           uint32_t donor = P.donors[(slot * 3 + comp) * N + c];
@@ -203,8 +284,8 @@ __global__ void __launch_bounds__(THREADS) k_correct_evolve(const SimParams* __r
                          z + (int)((donor >> 10) & 31u) - 16};
           float3 fv = make_float3(0.f, 0.f, 0.f);
           if (retrace) {
-            fv = velocityOnFace(P, H, x, y, z, comp, orig);
-            float3 vm = velocityAt(P, H, P.vel, face[0] - 0.5f * P.dt * fv.x, face[1] - 0.5f * P.dt * fv.y,
+            fv = velocityOnFace(P, H, G, V, x, y, z, comp, orig);
+            float3 vm = velocityAt(P, H, G, V, face[0] - 0.5f * P.dt * fv.x, face[1] - 0.5f * P.dt * fv.y,
                                    face[2] - 0.5f * P.dt * fv.z);
             float dep[3] = {face[0] - P.dt * vm.x, face[1] - P.dt * vm.y, face[2] - P.dt * vm.z};
             dep[comp] -= 0.5f * P.h;
@@ -220,19 +301,59 @@ __global__ void __launch_bounds__(THREADS) k_correct_evolve(const SimParams* __r
           if (lo == hi && predicted == lo) {
             result = predicted;
           } else {
-            if (!retrace) fv = velocityOnFace(P, H, x, y, z, comp, orig);
-            float3 vm = velocityAt(P, H, P.vel, face[0] + 0.5f * P.dt * fv.x, face[1] + 0.5f * P.dt * fv.y,
+            if (!retrace) fv = velocityOnFace(P, H, G, V, x, y, z, comp, orig);
+            float3 vm = velocityAt(P, H, G, V, face[0] + 0.5f * P.dt * fv.x, face[1] + 0.5f * P.dt * fv.y,
                                    face[2] + 0.5f * P.dt * fv.z);
             float fw[3] = {face[0] + P.dt * vm.x, face[1] + P.dt * vm.y, face[2] + P.dt * vm.z};
             fw[comp] -= 0.5f * P.h;
-            float reversed = sampleCells(P, H, P.velP, 3, comp, fw[0] / P.h, fw[1] / P.h, fw[2] / P.h);
+            float reversed = fieldSample(P, H, G, Vp, comp, fw[0] / P.h, fw[1] / P.h, fw[2] / P.h);
             float corrected = predicted + 0.5f * (get(orig, comp) - reversed);
             result = (corrected < lo || corrected > hi) ? predicted : corrected;
           }
         }
         P.velC[(slot * 3 + comp) * N + c] = result;
       }
-      // --- scalar correction and evolution
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// evolveFields (fluid-field-evolution.wgsl:9-84) with correctedScalars
+// (fluid-scalar-transport.wgsl:144-199) and recordContent (fluid-content.wgsl:29-64).
+template <bool STAGED>
+__global__ void __launch_bounds__(THREADS) k_evolve(const SimParams* __restrict__ Pp) {
+  const SimParams& P = *Pp;
+  __shared__ int nslot[27];
+  __shared__ uint32_t busyAll, expandsAll;
+  extern __shared__ float smem[];
+  uint32_t total = P.counters->active;
+  uint32_t bricks = (uint32_t)P.capacity * 64u;
+  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+    uint32_t id = P.active[i];
+    if (threadIdx.x == 0) {
+      busyAll = 0;
+      expandsAll = 0;
+    }
+    Home H = enterBrick(P, id, nslot);
+    Stage G = stageOf(P, H, STAGED);
+    Field V{P.vel, 3, STAGED ? smem : nullptr};
+    Field Fp{P.fldP, 4, STAGED ? smem + 3 * G.S3 : nullptr};
+    if (STAGED) {
+      stageField(P, H, G, smem, P.vel, 3);
+      stageField(P, H, G, smem + 3 * G.S3, P.fldP, 4);
+      __syncthreads();
+    }
+    size_t slot = (size_t)nslot[13];
+    const size_t N = P.N;
+    int tile = (int)(id >> 6);
+    uint32_t busy = 0;
+    bool expands = false;
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int x, y, z;
+      cellOf(P, H, c, x, y, z);
+      float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+      bool solid = solidAt(P, H, px, py, pz);
       float value[4] = {0.f, 0.f, 0.f, 0.f};
       float expansion = 0.f;
       bool injected = false;
@@ -240,9 +361,8 @@ __global__ void __launch_bounds__(THREADS) k_correct_evolve(const SimParams* __r
       float3 cv = make_float3(0.f, 0.f, 0.f);
       if (!solid) {
         float tr[4];
-        const float* adv = P.fldP + slot * 4 * N;
         if (!P.maccormack) {
-          for (int k = 0; k < 4; k++) tr[k] = adv[k * N + c];
+          for (int k = 0; k < 4; k++) tr[k] = fieldCell(P, H, G, Fp, k, x, y, z);
         } else {
           const float* b = P.sb + slot * 8 * N;
           float mn0 = b[0 * N + c], mn1 = b[1 * N + c], mn3 = b[2 * N + c], lmin = b[3 * N + c];
@@ -253,10 +373,11 @@ __global__ void __launch_bounds__(THREADS) k_correct_evolve(const SimParams* __r
             tr[2] = clamp01(lmin);
             tr[3] = mn3;
           } else {
-            float a0 = adv[0 * N + c], a1 = adv[1 * N + c], a2 = adv[2 * N + c], a3 = adv[3 * N + c];
-            cv = velocityAt(P, H, P.vel, px, py, pz);
+            float a0 = fieldCell(P, H, G, Fp, 0, x, y, z), a1 = fieldCell(P, H, G, Fp, 1, x, y, z),
+                  a2 = fieldCell(P, H, G, Fp, 2, x, y, z), a3 = fieldCell(P, H, G, Fp, 3, x, y, z);
+            cv = velocityAt(P, H, G, V, px, py, pz);
             cvSampled = true;
-            float3 vm = velocityAt(P, H, P.vel, px + 0.5f * P.dt * cv.x, py + 0.5f * P.dt * cv.y, pz + 0.5f * P.dt * cv.z);
+            float3 vm = velocityAt(P, H, G, V, px + 0.5f * P.dt * cv.x, py + 0.5f * P.dt * cv.y, pz + 0.5f * P.dt * cv.z);
             float fx = px + P.dt * vm.x, fy = py + P.dt * vm.y, fz = pz + P.dt * vm.z;
             const float* o = P.fld + slot * 4 * N;
             float o0 = o[0 * N + c], o1 = o[1 * N + c], o2 = o[2 * N + c], o3 = o[3 * N + c];
@@ -271,20 +392,15 @@ __global__ void __launch_bounds__(THREADS) k_correct_evolve(const SimParams* __r
                 fr[a] = fc[a] - floorf(fc[a]);
               }
               float rs0 = 0.f, rs1 = 0.f, rs2 = 0.f, rs3 = 0.f;
-              int sh = P.shift;
               for (int dz = 0; dz < 2; dz++)
                 for (int dy = 0; dy < 2; dy++)
                   for (int dx = 0; dx < 2; dx++) {
                     int cx = base[0] + dx, cy = base[1] + dy, cz = base[2] + dz;
-                    int s = brickSlot(P, H, cx >> sh, cy >> sh, cz >> sh);
                     float w = (dx ? fr[0] : 1.f - fr[0]) * (dy ? fr[1] : 1.f - fr[1]) * (dz ? fr[2] : 1.f - fr[2]);
-                    if (s >= 0) {
-                      size_t oo = (size_t)s * 4 * N + localCell(P, cx, cy, cz);
-                      rs0 += P.fldP[oo] * w;
-                      rs1 += P.fldP[oo + N] * w;
-                      rs2 += P.fldP[oo + 2 * N] * w;
-                      rs3 += P.fldP[oo + 3 * N] * w;
-                    }
+                    rs0 += fieldCell(P, H, G, Fp, 0, cx, cy, cz) * w;
+                    rs1 += fieldCell(P, H, G, Fp, 1, cx, cy, cz) * w;
+                    rs2 += fieldCell(P, H, G, Fp, 2, cx, cy, cz) * w;
+                    rs3 += fieldCell(P, H, G, Fp, 3, cx, cy, cz) * w;
                   }
               r0 = rs0;
               r1 = rs1;
@@ -292,9 +408,9 @@ __global__ void __launch_bounds__(THREADS) k_correct_evolve(const SimParams* __r
               float cl = a2 + 0.5f * (o2 - rs2);
               lifetime = (cl < lmin || cl > lmax) ? a2 : cl;
             } else {
-              r0 = sampleCells(P, H, P.fldP, 4, 0, fx / P.h, fy / P.h, fz / P.h);
-              r1 = sampleCells(P, H, P.fldP, 4, 1, fx / P.h, fy / P.h, fz / P.h);
-              r3 = sampleCells(P, H, P.fldP, 4, 3, fx / P.h, fy / P.h, fz / P.h);
+              r0 = fieldSample(P, H, G, Fp, 0, fx / P.h, fy / P.h, fz / P.h);
+              r1 = fieldSample(P, H, G, Fp, 1, fx / P.h, fy / P.h, fz / P.h);
+              r3 = fieldSample(P, H, G, Fp, 3, fx / P.h, fy / P.h, fz / P.h);
             }
             float c0 = a0 + 0.5f * (o0 - r0), c1 = a1 + 0.5f * (o1 - r1), c3 = a3 + 0.5f * (o3 - r3);
             tr[0] = (c0 < mn0 || c0 > mx0) ? a0 : c0;
@@ -353,7 +469,7 @@ __global__ void __launch_bounds__(THREADS) k_correct_evolve(const SimParams* __r
       if (expansion != 0.f) expands = true;
       // holdsContent and contentSupport (fluid-content.wgsl:22-39).
       if (fmaxf(fmaxf(value[0], value[2]), value[3]) > P.cutoff) {
-        if (!cvSampled) cv = velocityAt(P, H, P.vel, px, py, pz);
+        if (!cvSampled) cv = velocityAt(P, H, G, V, px, py, pz);
         int idc[3] = {x, y, z};
         float vv[3] = {cv.x, cv.y, cv.z};
         bool low[3], high[3];
@@ -706,9 +822,36 @@ __global__ void k_noise(float4* __restrict__ out) {
 
 }  // namespace
 
-void fp_launch_predict(const SimParams* dP, int sms, cudaStream_t st) { k_predict<<<sms * 4, THREADS, 0, st>>>(dP); }
-void fp_launch_correct_evolve(const SimParams* dP, int sms, cudaStream_t st) {
-  k_correct_evolve<<<sms * 4, THREADS, 0, st>>>(dP);
+// Staged kernels for 8^3 bricks: `channels` staged fields over (8 + 2 HALO)^3 cells.
+template <typename K>
+static void launchStaged(K kernel, int channels, const SimParams* dP, int sms, cudaStream_t st) {
+  const int S = 8 + 2 * HALO;
+  size_t smem = (size_t)channels * S * S * S * sizeof(float);
+  static bool configured = false;  // per kernel instantiation
+  if (!configured) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    configured = true;
+  }
+  kernel<<<sms * 4, THREADS, smem, st>>>(dP);
+}
+
+void fp_launch_predict(const SimParams* dP, int B, int sms, cudaStream_t st) {
+  if (B == 8)
+    launchStaged(k_predict<true>, 7, dP, sms, st);
+  else
+    k_predict<false><<<sms * 4, THREADS, 0, st>>>(dP);
+}
+void fp_launch_correct(const SimParams* dP, int B, int sms, cudaStream_t st) {
+  if (B == 8)
+    launchStaged(k_correct<true>, 6, dP, sms, st);
+  else
+    k_correct<false><<<sms * 4, THREADS, 0, st>>>(dP);
+}
+void fp_launch_evolve(const SimParams* dP, int B, int sms, cudaStream_t st) {
+  if (B == 8)
+    launchStaged(k_evolve<true>, 7, dP, sms, st);
+  else
+    k_evolve<false><<<sms * 4, THREADS, 0, st>>>(dP);
 }
 void fp_launch_curl(const SimParams* dP, int sms, cudaStream_t st) { k_curl<<<sms * 4, THREADS, 0, st>>>(dP); }
 void fp_launch_forces(const SimParams* dP, int B, int sms, cudaStream_t st) {
