@@ -195,10 +195,12 @@ class LargeScene(Scene):
     name = "large_scene"
     steps = 600
 
-    def __init__(self, seed: int = 1):
+    def __init__(self, seed: int = 1, smoke: float = 1.5, dissipation: float = 0.75, cooling: float = 0.62,
+                 flame_smoke: float = 2.0):
         self.seed = seed
-        self.settings = settings(buoyancy=1.6, vorticity=1.0, seed=seed)
-        self.comb = combustion()
+        self.smoke = smoke
+        self.settings = settings(buoyancy=1.6, vorticity=1.0, seed=seed, dissipation=dissipation, cooling=cooling)
+        self.comb = combustion(smoke_rate=flame_smoke)
         rng = [_hash01(k, seed) for k in range(32)]
         self.emitters = []
         for e in range(3):
@@ -212,7 +214,7 @@ class LargeScene(Scene):
         srcs = []
         for i, (shape, pos, size) in enumerate(self.emitters):
             j = 1.0 + 0.25 * value_noise_1d(step / 12.0, self.seed + 17 * i)
-            srcs.append(source(10 + i, shape, pos, size, flame=0.8, heat=2.0 * j, smoke=1.5 * j, fuel=0.6 * j,
+            srcs.append(source(10 + i, shape, pos, size, flame=0.8, heat=2.0 * j, smoke=self.smoke * j, fuel=0.6 * j,
                                velocity=(0.0, 1.0, 0.0), response=60.0))
         if step == 30:
             # Explosion burst (FireSimulation.ts:471-493): charge / FIXED_DT for one step.
