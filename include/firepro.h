@@ -234,6 +234,26 @@ int fp_sim_set_profiling(fp_sim* sim, int enabled);
 /* The per-phase totals since profiling started. `*count` in: capacity, out: phases. */
 int fp_sim_read_profile(fp_sim* sim, fp_phase* phases, uint32_t* count);
 
+/* Most ids fp_compact_ids_noalloc accepts in one call. */
+#define FP_COMPACT_MAX_IDS (1u << 22)
+
+/* Ordered compaction that allocates nothing. No counterpart in the reference: it is the
+ * step's own ranking of computing bricks (ascending ids of the nonzero flags, as the
+ * allocation lists them) offered to callers that cannot allocate device memory where they
+ * call it, such as a renderer's frame loop that must not stall on cudaMalloc/cudaFree, a host
+ * that owns all device memory through its own allocator or budget, or code inside a stream
+ * capture.
+ *   flags  device array of n words; a nonzero word keeps its index
+ *   ids    device array of at least n words: the kept indices, ascending
+ *   count  device word: how many were kept
+ *   stream a cudaStream_t, or NULL for the default stream; the call only enqueues
+ * n may be at most FP_COMPACT_MAX_IDS; larger n returns FP_ELIMIT and launches nothing.
+ * Scratch is a 64 KB array inside the library that every GPU loading it holds until exit.
+ * The first call on a device looks up that array's address with the device current; make
+ * that first call before any stream capture. All calls share the array, so calls whose
+ * work overlaps on the GPU race; order them on one stream. */
+int fp_compact_ids_noalloc(const uint32_t* flags, uint32_t n, uint32_t* ids, uint32_t* count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,6 +7,7 @@
 
 #include "../../include/firepro.h"
 #include "fp_engine.hpp"
+#include "fp_error.h"
 
 struct fp_sim {
   fp::Engine* engine;
@@ -18,6 +19,8 @@ static int failed(const std::string& message, int code) {
   g_error = message;
   return code;
 }
+
+int fp_set_error(int code, const std::string& message) { return failed(message, code); }
 
 extern "C" {
 

@@ -200,7 +200,9 @@ SIGNATURES = {
     "fp_sim_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "fp_sim_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "fp_sim_read_profile": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
+    "fp_compact_ids_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
+FP_COMPACT_MAX_IDS = 1 << 22
 
 _lib = None
 
