@@ -220,7 +220,7 @@ def run_ours(args, rank, world, local):
     from firepro.engine import FluidSimulation
 
     torch.cuda.set_device(local)
-    sc = scenes.LargeScene(seed=1)
+    sc = scenes.SCENES[args.scene](seed=1)
     sim = FluidSimulation(sc.grid(budget=BUDGET), device=local)
     sim.set_runtime(0.05, BUDGET, True)
     # Grow the scene to the target size (untimed).
@@ -239,7 +239,8 @@ def run_ours(args, rank, world, local):
 
     # --- value: device time of K steps on the simulation's stream
     events = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    launches0 = sim.stats().kernel_launches
+    st0 = sim.stats()
+    launches0 = st0.kernel_launches
     clocks = Clocks(local)
     barrier(world)
     torch.cuda.synchronize()
@@ -258,7 +259,10 @@ def run_ours(args, rank, world, local):
     clock = clocks.stop()
     barrier(world)
     step += args.steps
-    launches = sim.stats().kernel_launches - launches0
+    st1 = sim.stats()
+    launches = st1.kernel_launches - launches0
+    host = {"prepare_ms_per_step": (st1.host_prepare_ms - st0.host_prepare_ms) / args.steps,
+            "wait_ms_per_step": (st1.host_wait_ms - st0.host_wait_ms) / args.steps}
     total_ms = events[0].elapsed_time(events[-1])
     step_ms = [events[k].elapsed_time(events[k + 1]) for k in range(args.steps)]
     voxels = sum(actives) * BRICK_VOXELS
@@ -332,6 +336,7 @@ def run_ours(args, rank, world, local):
         "e2e": {"value": e2e_vox / e2e_s, "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
         "gpu_launches": int(launches),
+        "host": host,
         "clocks": clock,
     }
     if world == 1 and not args.no_cpu:
@@ -350,6 +355,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--scene", default="large_scene", help="workload (default: the large single simulation)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_setup(args)

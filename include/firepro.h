@@ -163,6 +163,8 @@ typedef struct fp_stats {
   uint64_t kernel_launches; /* kernels this simulation has launched since creation */
   uint64_t h2d_bytes;       /* host-to-device bytes the latest step copied (scene, parameters) */
   uint64_t d2h_bytes;       /* device-to-host bytes the latest step read back (its measurement) */
+  double host_prepare_ms;   /* host time in fp_sim_step since creation, waits excluded */
+  double host_wait_ms;      /* host time spent waiting for the previous step's measurement */
 } fp_stats;
 
 /* Device time of one phase of the step, accumulated while profiling is on: the restatement

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <chrono>
 #include <cstring>
 
 #include "fp_launch.h"
@@ -118,15 +119,32 @@ bool Engine::grow(DeviceBuffer& b, size_t bytes, int fill) {
   return true;
 }
 
+// Host-to-device copies go through a pinned arena, so they are truly asynchronous. The arena
+// restarts each step: the previous step's copies ran before its allocation kernels, which
+// precede the measurement the step start waits for.
 bool Engine::upload(DeviceBuffer& b, const void* src, size_t bytes) {
   if (bytes == 0) return true;
   if (bytes > b.bytes) {
-    cudaStreamSynchronize(stream_);
+    cudaStreamSynchronize(stream_);  // the old buffer may still be read: rare growth
     if (!alloc(b, std::max(bytes + bytes / 2, (size_t)256), false)) return false;
   }
-  // Synchronous from pageable memory: the source vectors change next step.
+  size_t off = (stageUsed_ + 255) & ~(size_t)255;
+  if (off + bytes > stageCap_) {
+    cudaStreamSynchronize(stream_);  // copies from the old arena must finish before it goes
+    if (stageH_) cudaFreeHost(stageH_);
+    stageCap_ = std::max(std::max(stageCap_ * 2, off + bytes), (size_t)1 << 20);
+    if (cudaMallocHost(&stageH_, stageCap_) != cudaSuccess) {
+      stageH_ = nullptr;
+      stageCap_ = 0;
+      error_ = "pinned host memory exhausted";
+      return false;
+    }
+    off = 0;
+  }
+  std::memcpy(stageH_ + off, src, bytes);
+  stageUsed_ = off + bytes;
   h2d_ += bytes;
-  return cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, stream_) == cudaSuccess;
+  return cudaMemcpyAsync(b.ptr, stageH_ + off, bytes, cudaMemcpyHostToDevice, stream_) == cudaSuccess;
 }
 
 uint32_t Engine::slotLimit() const {
@@ -151,6 +169,7 @@ Engine::~Engine() {
   if (stream_) cudaStreamSynchronize(stream_);
   freeAll();
   if (paramsH_) cudaFreeHost(paramsH_);
+  if (stageH_) cudaFreeHost(stageH_);
   if (readH_) cudaFreeHost(readH_);
   if (readEvent_) cudaEventDestroy(readEvent_);
   for (Phase& ph : phases_) {
@@ -161,6 +180,7 @@ Engine::~Engine() {
 }
 
 void Engine::freeAll() {
+  clearGraphs();
   DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_, &zeroList_,
                          &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_, &donors_, &solids_,
                          &tileRecD_, &tileNbrD_, &hashD_, &emittersD_, &collidersD_, &masksD_, &forcesD_,
@@ -196,6 +216,8 @@ int Engine::initialize() {
       !alloc(noise_, 64 * 64 * 64 * sizeof(float4)))
     return FP_ENOMEM;
   fp_launch_noise((float4*)noise_.ptr, stream_);
+  fp_mg_configure(B_);
+  fp_step_configure(B_);
   slots_ = 0;
   capacity_ = 0;
   if ((rc = allocatePools(slotLimit()))) return rc;
@@ -251,6 +273,7 @@ int Engine::allocatePools(uint32_t slots) {
 int Engine::growPool(uint32_t target) {
   if (target <= slots_) return FP_OK;
   cudaStreamSynchronize(stream_);
+  clearGraphs();
   size_t s = target, N = N_;
   uint32_t added = target - slots_;
   bool ok = true;
@@ -284,6 +307,8 @@ int Engine::growPool(uint32_t target) {
 // Per-brick and per-tile storage for `capacity` tile slots, keeping every brick's page,
 // state, flags, entry and record (FluidSimulation.ts:633-646).
 int Engine::setCapacity(int capacity) {
+  if (stream_) cudaStreamSynchronize(stream_);
+  clearGraphs();
   size_t bricks = (size_t)capacity * 64;
   size_t oldBricks = (size_t)capacity_ * 64;
   bool ok = grow(pages_, bricks * 4, 0xff) && grow(entries_, bricks * 4, 0xff) && grow(state_, bricks * 4, 0) &&
@@ -351,7 +376,6 @@ int Engine::applyTiles() {
   }
   dir_.dirty = false;
   geometryDirty_ = true;  // PressureSolver.setBricks -> resetPlans
-  cudaStreamSynchronize(stream_);  // the host tables are reused next step
   return FP_OK;
 }
 
@@ -694,7 +718,9 @@ void Engine::fillParams(const fp_frame& f, float dt) {
 // measurement lags the step by exactly one.
 int Engine::consumeReadback() {
   if (!pendingRead_) return FP_OK;
+  auto t0 = std::chrono::steady_clock::now();
   int rc = check(cudaEventSynchronize(readEvent_), "step");
+  hostWaitMs_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (rc) return rc;
   pendingRead_ = false;
   const FpCounters* c = (const FpCounters*)readH_;
@@ -707,6 +733,12 @@ int Engine::consumeReadback() {
   lastFailures_ = c->failures;
   poolLimited_ = c->failures > 0 && slots_ >= slotLimit();
   if (profilePending_) {
+    // The phases after the measurement may still run: wait for the step's last one.
+    for (int k = PH_COUNT - 1; k >= 0; k--)
+      if (phases_[k].used) {
+        cudaEventSynchronize(phases_[k].b);
+        break;
+      }
     for (Phase& ph : phases_) {
       if (!ph.used) continue;
       float ms = 0.f;
@@ -813,8 +845,85 @@ void Engine::vcycle(int level, int cur[]) {
   }
 }
 
+// The step's kernels, readback and measurement event, enqueued on the stream (eagerly, or
+// under capture into a graph). `latest` is the pressure buffer in, then out; `launches` the
+// kernels enqueued.
+void Engine::enqueueKernels(bool solids, bool topoAll, bool curl, int& latest, uint64_t& launches) {
+  SimParams* dP = dParams();
+  uint64_t first = launches_;
+  phaseBegin(PH_ALLOC);
+  fp_launch_allocation(dP, capacity_, solids, sms_, stream_);
+  phaseEnd(PH_ALLOC, 7 + (solids ? 1 : 0));
+  // Topology of the slots granted this step, or of everything after the geometry changed.
+  phaseBegin(PH_TOPO);
+  fp_launch_topology(dP, brickLevels_, bottom_, topoAll, capacity_, sms_, stream_);
+  phaseEnd(PH_TOPO, topoAll ? 2 : 1);
+  phaseBegin(PH_PREDICT);
+  fp_launch_predict(dP, B_, sms_, stream_);
+  phaseEnd(PH_PREDICT, 1);
+  phaseBegin(PH_CORRECT);
+  fp_launch_correct(dP, B_, sms_, stream_);
+  phaseEnd(PH_CORRECT, 1);
+  phaseBegin(PH_EVOLVE);
+  fp_launch_evolve(dP, B_, sms_, stream_);
+  phaseEnd(PH_EVOLVE, 1);
+
+  // Measurement: counters and the tiles' content flags are final once evolution ran, so they
+  // are read back here; the next step waits for this copy only and prepares while the GPU
+  // runs the rest of this step. Failed allocations count from one measurement to the next.
+  cudaMemcpyAsync(readH_, counters_.ptr, sizeof(FpCounters), cudaMemcpyDeviceToHost, stream_);
+  cudaMemcpyAsync(readH_ + sizeof(FpCounters) / 4, (uint32_t*)activity_.ptr + (size_t)capacity_ * 64,
+                  (size_t)capacity_ * 4, cudaMemcpyDeviceToHost, stream_);
+  cudaMemsetAsync(&((FpCounters*)counters_.ptr)->failures, 0, 4, stream_);
+  // Under capture, external: an event-record node the graph replays.
+  if (profiling_)
+    cudaEventRecord(readEvent_, stream_);
+  else
+    cudaEventRecordWithFlags(readEvent_, stream_, cudaEventRecordExternal);
+
+  if (curl) {
+    phaseBegin(PH_CURL);
+    fp_launch_curl(dP, sms_, stream_);
+    phaseEnd(PH_CURL, 1);
+  }
+  phaseBegin(PH_FORCES);
+  fp_launch_forces(dP, B_, sms_, stream_);
+  phaseEnd(PH_FORCES, 1);
+  int cur[FP_MAX_LEVELS] = {0};
+  cur[0] = latest;
+  phaseBegin(PH_DIVERGENCE);
+  fp_launch_divergence(dP, P0(1 - cur[0]), sms_, stream_);
+  phaseEnd(PH_DIVERGENCE, 1);
+  cur[0] = 1 - cur[0];
+  phaseBegin(PH_MULTIGRID);
+  uint64_t before = launches_;
+  vcycle(0, cur);
+  int mg = (int)(launches_ - before);
+  launches_ = before;
+  phaseEnd(PH_MULTIGRID, mg);
+  latest = cur[0];
+  phaseBegin(PH_PROJECT);
+  fp_launch_project(dP, P0(latest), sms_, stream_);
+  phaseEnd(PH_PROJECT, 1);
+  launches = launches_ - first;
+}
+
+void Engine::clearGraphs() {
+  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
+  graphs_.clear();
+}
+
 // FluidSimulation.step / substep (FluidSimulation.ts:1367-1531).
 int Engine::step(const fp_frame& f, float dt) {
+  auto t0 = std::chrono::steady_clock::now();
+  double wait0 = hostWaitMs_;
+  int rc = stepBody(f, dt);
+  double all = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  hostPrepareMs_ += all - (hostWaitMs_ - wait0);
+  return rc;
+}
+
+int Engine::stepBody(const fp_frame& f, float dt) {
   if (!std::isfinite(dt) || dt <= 0 || dt > 1.f / 30.f)
     return fail(FP_EINVAL, "Simulation step must be in (0, 1/30]. Use fixed substeps.");
   int rc = packFlame(f.combustion, dt);
@@ -850,68 +959,59 @@ int Engine::step(const fp_frame& f, float dt) {
   h2d_ += sizeof(SimParams);
 
   bool solids = colliderCount_ > 0 || solidsStale_;
-  phaseBegin(PH_ALLOC);
-  fp_launch_allocation(dP, capacity_, solids, sms_, stream_);
-  phaseEnd(PH_ALLOC, 7 + (solids ? 1 : 0));
-  solidsStale_ = false;
-  // Topology of the slots granted this step, or of everything after the geometry changed.
-  phaseBegin(PH_TOPO);
-  fp_launch_topology(dP, brickLevels_, bottom_, geometryDirty_, capacity_, sms_, stream_);
-  phaseEnd(PH_TOPO, geometryDirty_ ? 2 : 1);
-  geometryDirty_ = false;
-  phaseBegin(PH_PREDICT);
-  fp_launch_predict(dP, B_, sms_, stream_);
-  phaseEnd(PH_PREDICT, 1);
-  phaseBegin(PH_CORRECT);
-  fp_launch_correct(dP, B_, sms_, stream_);
-  phaseEnd(PH_CORRECT, 1);
-  phaseBegin(PH_EVOLVE);
-  fp_launch_evolve(dP, B_, sms_, stream_);
-  phaseEnd(PH_EVOLVE, 1);
-  if (f.simulation.vorticity != 0.f) {
-    phaseBegin(PH_CURL);
-    fp_launch_curl(dP, sms_, stream_);
-    phaseEnd(PH_CURL, 1);
-  }
-  phaseBegin(PH_FORCES);
-  fp_launch_forces(dP, B_, sms_, stream_);
-  phaseEnd(PH_FORCES, 1);
-  int cur[FP_MAX_LEVELS] = {0};
-  cur[0] = latest_;
-  phaseBegin(PH_DIVERGENCE);
-  fp_launch_divergence(dP, P0(1 - cur[0]), sms_, stream_);
-  phaseEnd(PH_DIVERGENCE, 1);
-  cur[0] = 1 - cur[0];
-  phaseBegin(PH_MULTIGRID);
-  uint64_t before = launches_;
-  vcycle(0, cur);
-  int mg = (int)(launches_ - before);
-  launches_ = before;
-  phaseEnd(PH_MULTIGRID, mg);
-  latest_ = cur[0];
-  phaseBegin(PH_PROJECT);
-  fp_launch_project(dP, P0(latest_), sms_, stream_);
-  phaseEnd(PH_PROJECT, 1);
-  std::swap(velIdx_[0], velIdx_[1]);
-  std::swap(fldIdx_[0], fldIdx_[2]);
-
-  // Measurement: counters and the tiles' content flags, then clear failures.
+  bool topoAll = geometryDirty_;
+  bool curl = f.simulation.vorticity != 0.f;
+  // The measurement buffer (a graph captures its address).
   size_t words = sizeof(FpCounters) / 4 + capacity_;
   if (words > readWords_) {
+    cudaStreamSynchronize(stream_);
+    clearGraphs();
     if (readH_) cudaFreeHost(readH_);
     readWords_ = words * 2;
     if ((rc = check(cudaMallocHost(&readH_, readWords_ * 4), "cudaMallocHost"))) return rc;
   }
+  if (profiling_) {
+    // Eager launches with an event pair around each phase.
+    uint64_t n = 0;
+    int latest = latest_;
+    enqueueKernels(solids, topoAll, curl, latest, n);
+    latest_ = latest;
+  } else {
+    // The step's launches as one CUDA graph, captured once per shape and replayed.
+    uint64_t key = (uint64_t)capacity_ | ((uint64_t)solids << 32) | ((uint64_t)topoAll << 33) |
+                   ((uint64_t)curl << 34) | ((uint64_t)latest_ << 35);
+    auto it = graphs_.find(key);
+    if (it == graphs_.end()) {
+      GraphEntry e{};
+      uint64_t saved = launches_;
+      int latest = latest_;
+      if ((rc = check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture")))
+        return rc;
+      enqueueKernels(solids, topoAll, curl, latest, e.launches);
+      cudaGraph_t g = nullptr;
+      rc = check(cudaStreamEndCapture(stream_, &g), "cudaStreamEndCapture");
+      launches_ = saved;
+      if (rc) return rc;
+      rc = check(cudaGraphInstantiate(&e.exec, g, 0), "cudaGraphInstantiate");
+      cudaGraphDestroy(g);
+      if (rc) return rc;
+      e.latest = latest;
+      it = graphs_.emplace(key, e).first;
+    }
+    if ((rc = check(cudaGraphLaunch(it->second.exec, stream_), "cudaGraphLaunch"))) return rc;
+    latest_ = it->second.latest;
+    launches_ += it->second.launches;
+  }
+  solidsStale_ = false;
+  geometryDirty_ = false;
+  pendingRead_ = true;
   d2h_ += sizeof(FpCounters) + (size_t)capacity_ * 4;
+  std::swap(velIdx_[0], velIdx_[1]);
+  std::swap(fldIdx_[0], fldIdx_[2]);
   stepH2d_ = h2d_;
   stepD2h_ = d2h_;
   h2d_ = d2h_ = 0;
-  cudaMemcpyAsync(readH_, counters_.ptr, sizeof(FpCounters), cudaMemcpyDeviceToHost, stream_);
-  cudaMemcpyAsync(readH_ + sizeof(FpCounters) / 4, (uint32_t*)activity_.ptr + (size_t)capacity_ * 64,
-                  (size_t)capacity_ * 4, cudaMemcpyDeviceToHost, stream_);
-  cudaMemsetAsync(&((FpCounters*)counters_.ptr)->failures, 0, 4, stream_);
-  cudaEventRecord(readEvent_, stream_);
-  pendingRead_ = true;
+  stageUsed_ = 0;
   time_ += dt;
   steps_++;
   return check(cudaGetLastError(), "step launch");
@@ -962,6 +1062,8 @@ int Engine::stats(fp_stats* out) {
   out->kernel_launches = launches_;
   out->h2d_bytes = stepH2d_;
   out->d2h_bytes = stepD2h_;
+  out->host_prepare_ms = hostPrepareMs_;
+  out->host_wait_ms = hostWaitMs_;
   return FP_OK;
 }
 

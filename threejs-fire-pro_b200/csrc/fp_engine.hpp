@@ -59,6 +59,7 @@ class Engine {
 
   int initialize();
   int step(const fp_frame& frame, float dt);
+  int stepBody(const fp_frame& frame, float dt);
   int reset();
   int setRuntime(float cutoff, double budget, int ground);
   int synchronize();
@@ -125,6 +126,8 @@ class Engine {
 
   // pinned host staging
   SimParams* paramsH_ = nullptr;
+  uint8_t* stageH_ = nullptr;  // pinned arena of the step's host-to-device copies
+  size_t stageCap_ = 0, stageUsed_ = 0;
   uint32_t* readH_ = nullptr;
   size_t readWords_ = 0;
   cudaEvent_t readEvent_ = nullptr;
@@ -143,8 +146,21 @@ class Engine {
   bool profilePending_ = false;
   uint64_t launches_ = 0;
   uint64_t h2d_ = 0, d2h_ = 0, stepH2d_ = 0, stepD2h_ = 0;
+  double hostPrepareMs_ = 0, hostWaitMs_ = 0;
   void phaseBegin(int id);
   void phaseEnd(int id, int launches);
+
+  // The step's launch sequence as CUDA graphs, one per shape (capacity, solids, topology
+  // rebuild, curl, pressure buffer parity). Kernel arguments hold buffer addresses, so any
+  // reallocation clears the cache.
+  struct GraphEntry {
+    cudaGraphExec_t exec;
+    int latest;
+    uint64_t launches;
+  };
+  std::unordered_map<uint64_t, GraphEntry> graphs_;
+  void enqueueKernels(bool solids, bool topoAll, bool curl, int& latest, uint64_t& launches);
+  void clearGraphs();
 
   // per-step scene (host)
   std::vector<FpEmitter> emitters_;

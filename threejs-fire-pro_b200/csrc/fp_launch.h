@@ -29,3 +29,7 @@ void fp_launch_bottom(const SimParams* dP, int level, int iterations, const floa
                       int capacity, cudaStream_t st);
 // Most tile slots the one-CTA bottom solve holds in shared memory.
 int fp_bottom_capacity();
+// Size the staged brick-level multigrid kernels for bricks of B cells (once per brick size).
+void fp_mg_configure(int B);
+// Set the step kernels' shared-memory limits (before any launch or stream capture).
+void fp_step_configure(int B);

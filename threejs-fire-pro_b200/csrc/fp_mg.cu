@@ -199,6 +199,152 @@ __global__ void __launch_bounds__(256) k_level_bricks(const SimParams* __restric
   }
 }
 
+// Staged brick levels. A CTA copies, for its brick, the values of the level it reads plus a
+// one-cell rim into shared memory, and once per brick whether each negative-octant neighbour
+// brick computes; the cell operations then read no directory. Same arithmetic, same order as
+// relaxCell / restrictCell / prolongCell above.
+//   RELAX     stage A.pin at A.level;           write A.pout at A.level
+//   RESTRICT  stage A.pin at A.level - 1 (fine); write A.pout, A.cfirst at A.level (coarse)
+//   PROLONG   stage A.coarse at A.level + 1;    write A.pout at A.level
+template <int OP>
+__global__ void __launch_bounds__(256) k_level_bricks_staged(const SimParams* __restrict__ Pp, Args A) {
+  const SimParams& P = *Pp;
+  __shared__ int nslot[27];
+  __shared__ int need[8];  // bit k of the index: -1 on axis k
+  extern __shared__ float st[];
+  const int bl = P.brickLevels;
+  const int fineLevel = OP == RESTRICT ? A.level - 1 : A.level;
+  const int stageLevel = OP == PROLONG ? A.level + 1 : fineLevel;
+  const int sb = stageLevel < bl ? 1 << levelShift(P, stageLevel) : 1;  // stage-level cells per brick side
+  // Prolongation stages a two-cell rim and the coarse solid flags: its Neumann ghosts read the
+  // neighbours of the interpolation's coarse cells.
+  const int R = OP == PROLONG ? 2 : 1;
+  const int S = sb + 2 * R, S2 = S * S, S3 = S2 * S;
+  uint8_t* solidSt = reinterpret_cast<uint8_t*>(st + S3);
+  const float* src = OP == PROLONG ? A.coarse : A.pin;
+  const int fs = levelShift(P, fineLevel), fside = 1 << fs, fcells = fside * fside * fside;
+  uint32_t total = P.counters->active;
+  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+    Home H = enterBrick(P, P.active[i], nslot);
+    if (threadIdx.x < 8) {
+      int dx = -(int)(threadIdx.x & 1), dy = -(int)((threadIdx.x >> 1) & 1), dz = -(int)(threadIdx.x >> 2);
+      bool below = P.ground && H.by + dy < 0;
+      need[threadIdx.x] = below || nslot[nbrIndex(dx, dy, dz)] >= 0;
+    }
+    int ox = H.bx * sb - R, oy = H.by * sb - R, oz = H.bz * sb - R;
+    for (int q = threadIdx.x; q < S3; q += blockDim.x) {
+      int lx = q % S, ly = (q / S) % S, lz = q / S2;
+      long a = cellAddress(P, H, ox + lx, oy + ly, oz + lz, stageLevel);
+      st[q] = a < 0 ? 0.f : src[a];
+      if (OP == PROLONG) solidSt[q] = a >= 0 && (P.topo[stageLevel][a] & FP_STORED_SOLID) ? 1 : 0;
+    }
+    __syncthreads();
+    // coarseValue (pressure.wgsl:670-696) from the stage.
+    auto ghost = [&](int cx, int cy, int cz) {
+      int groundY = P.ground ? 0 : -0x7fffffff;
+      int c[3] = {cx, max(cy, groundY), cz};
+      auto at = [&](int x, int y, int z) { return ((z - oz) * S + (y - oy)) * S + (x - ox); };
+      int ci = at(c[0], c[1], c[2]);
+      if (!solidSt[ci]) return st[ci];
+      float sum = 0.f, count = 0.f;
+      for (int axis = 0; axis < 3; axis++)
+        for (int side = -1; side <= 1; side += 2) {
+          int q[3] = {c[0], c[1], c[2]};
+          q[axis] += side;
+          q[1] = max(q[1], groundY);
+          int qi = at(q[0], q[1], q[2]);
+          if (!solidSt[qi]) {
+            sum += st[qi];
+            count += 1.f;
+          }
+        }
+      return sum / fmaxf(count, 1.f);
+    };
+    long slot = nslot[13];
+    // Whether the fine-level cell at local (lx,ly,lz) of this brick is a pressure unknown.
+    auto unknown = [&](int lx, int ly, int lz) {
+      for (int k = 1; k < 8; k++) {
+        if ((k & 1) && lx != 0) continue;
+        if ((k & 2) && ly != 0) continue;
+        if ((k & 4) && lz != 0) continue;
+        if (!need[k]) return false;
+      }
+      return (bool)need[0];
+    };
+    // Stencil sum of the open sides of a fine cell, from the stage (RELAX, RESTRICT).
+    auto sumAt = [&](int lx, int ly, int lz, uint32_t f) {
+      int c = ((lz + 1) * S + (ly + 1)) * S + (lx + 1);
+      float v0 = (f & 1u) ? st[c + 1] : 0.f, v1 = (f & 2u) ? st[c - 1] : 0.f;
+      float v2 = (f & 4u) ? st[c + S] : 0.f, v3 = (f & 8u) ? st[c - S] : 0.f;
+      float v4 = (f & 16u) ? st[c + S2] : 0.f, v5 = (f & 32u) ? st[c - S2] : 0.f;
+      return (v0 + v1) + (v2 + v3) + (v4 + v5);
+    };
+    if (OP == RELAX || OP == PROLONG) {
+      for (int o = threadIdx.x; o < fcells; o += blockDim.x) {
+        int lx = o & (fside - 1), ly = (o >> fs) & (fside - 1), lz = o >> (2 * fs);
+        long a = slot * fcells + o;
+        uint32_t f = expandFlags(P.topo[fineLevel][a]);
+        if ((f & SOLIDF) || !unknown(lx, ly, lz)) {
+          A.pout[a] = 0.f;
+          continue;
+        }
+        if (OP == RELAX) {
+          float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
+          float cand = (sumAt(lx, ly, lz, f) - A.rhs[a]) / fmaxf(diagOf(f), 1e-12f);
+          A.pout[a] = mixf(center, cand, 0.8f);
+        } else {
+          int px = H.bx * fside + lx, py = H.by * fside + ly, pz = H.bz * fside + lz;
+          float qx = ((float)px + 0.5f) * 0.5f - 0.5f, qy = ((float)py + 0.5f) * 0.5f - 0.5f,
+                qz = ((float)pz + 0.5f) * 0.5f - 0.5f;
+          int ix = (int)floorf(qx), iy = (int)floorf(qy), iz = (int)floorf(qz);
+          float fx = qx - floorf(qx), fy = qy - floorf(qy), fz = qz - floorf(qz);
+          bool fast = P.colliderCount == 0 && (!P.ground || iy >= 0);
+          float v[8];
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
+            v[k] = fast ? st[((iz + dz - oz) * S + (iy + dy - oy)) * S + (ix + dx - ox)]
+                        : ghost(ix + dx, iy + dy, iz + dz);
+          }
+          float corr = mixf(mixf(mixf(v[0], v[1], fx), mixf(v[2], v[3], fx), fy),
+                            mixf(mixf(v[4], v[5], fx), mixf(v[6], v[7], fx), fy), fz);
+          A.pout[a] = A.pin[a] + corr;
+        }
+      }
+    } else {  // RESTRICT: coarse cells of this brick at A.level
+      int cs = fs - 1, cside = fside >> 1, ccells = cside * cside * cside;
+      for (int o = threadIdx.x; o < ccells; o += blockDim.x) {
+        int cx = o & (cside - 1), cy = (o >> cs) & (cside - 1), cz = o >> (2 * cs);
+        float residual = 0.f;
+        bool every = true;
+        for (int k = 0; k < 8; k++) {
+          int lx = cx * 2 + (k & 1), ly = cy * 2 + ((k >> 1) & 1), lz = cz * 2 + (k >> 2);
+          bool u = unknown(lx, ly, lz);
+          every = every && u;
+          if (u) {
+            long a = slot * fcells + (((lz << fs) | ly) << fs | lx);
+            uint32_t f = expandFlags(P.topo[fineLevel][a]);
+            if (!(f & SOLIDF)) {
+              float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
+              residual += A.rhs[a] - (sumAt(lx, ly, lz, f) - diagOf(f) * center);
+            }
+          }
+        }
+        float r = residual * 0.5f;
+        long out = slot * ccells + o;
+        A.pout[out] = r;
+        float first = 0.f;
+        if (every) {
+          uint32_t f = expandFlags(P.topo[A.level][out]);
+          if (!(f & SOLIDF)) first = mixf(0.f, (0.f - r) / fmaxf(diagOf(f), 1e-12f), 0.8f);
+        }
+        A.cfirst[out] = first;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 FP_DEV Home enterTile(const SimParams& P, int t, int4 rec) {
   Home H;
   H.tile = t;
@@ -315,12 +461,11 @@ __global__ void __launch_bounds__(128) k_topo_bricks(const SimParams* __restrict
       id = P.zeroList[2 * i];
       slot = (int)P.zeroList[2 * i + 1];
     }
-    if (slot < 0) continue;
-    int tile = (int)(id >> 6);
-    int4 rec = __ldg(&P.tileRec[tile]);
-    Home H = enterTile(P, tile, rec);
-    int l = id & 63;
-    int bx = rec.x * 4 + (l & 3), by = rec.y * 4 + ((l >> 2) & 3), bz = rec.z * 4 + (l >> 4);
+    if (slot < 0) continue;  // uniform across the CTA
+    // The brick's neighbour slots in shared memory: every solid test stays within them.
+    __shared__ int nslot[27];
+    Home H = enterBrick(P, id, nslot);
+    int bx = H.bx, by = H.by, bz = H.bz;
     for (int level = 0; level < P.brickLevels; level++) {
       int s = levelShift(P, level), side = 1 << s, cells = side * side * side;
       for (int o = threadIdx.x; o < cells; o += blockDim.x) {
@@ -328,6 +473,7 @@ __global__ void __launch_bounds__(128) k_topo_bricks(const SimParams* __restrict
         P.topo[level][(size_t)slot * cells + o] = cellTopology(P, H, bx * side + lx, by * side + ly, bz * side + lz, level);
       }
     }
+    __syncthreads();
   }
 }
 
@@ -361,13 +507,27 @@ void fp_launch_topology(const SimParams* dP, int brickLevels, int bottom, bool a
 
 static int tileGrid(int capacity, int sms) { return capacity < sms * 8 ? capacity : sms * 8; }
 
+// Shared memory of the staged brick-level kernels: the largest brick size configured so far.
+static size_t g_stageBytes = 0;
+void fp_mg_configure(int B) {
+  size_t relax = (size_t)(B + 2) * (B + 2) * (B + 2) * sizeof(float);
+  size_t prolong = (size_t)(B / 2 + 4) * (B / 2 + 4) * (B / 2 + 4) * (sizeof(float) + 1);
+  size_t bytes = relax > prolong ? relax : prolong;
+  if (bytes <= g_stageBytes) return;
+  g_stageBytes = bytes;
+  cudaFuncSetAttribute(k_level_bricks_staged<RELAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_level_bricks_staged<RESTRICT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_level_bricks_staged<PROLONG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
 void fp_launch_relax(const SimParams* dP, int level, bool tiles, const float* rhs, const float* pin, float* pout,
                      int capacity, int sms, cudaStream_t st) {
   Args A{level, rhs, pin, nullptr, pout, nullptr};
   if (tiles)
     k_level_tiles<RELAX><<<tileGrid(capacity, sms), 64, 0, st>>>(dP, A);
   else
-    k_level_bricks<RELAX><<<sms * 4, 256, 0, st>>>(dP, A);
+    k_level_bricks_staged<RELAX><<<sms * 4, 256, g_stageBytes, st>>>(dP, A);
 }
 
 void fp_launch_restrict(const SimParams* dP, int fine, bool tiles, const float* rhs, const float* p, float* crhs,
@@ -376,7 +536,7 @@ void fp_launch_restrict(const SimParams* dP, int fine, bool tiles, const float* 
   if (tiles)
     k_level_tiles<RESTRICT><<<tileGrid(capacity, sms), 64, 0, st>>>(dP, A);
   else
-    k_level_bricks<RESTRICT><<<sms * 4, 256, 0, st>>>(dP, A);
+    k_level_bricks_staged<RESTRICT><<<sms * 4, 256, g_stageBytes, st>>>(dP, A);
 }
 
 void fp_launch_prolong(const SimParams* dP, int level, bool tiles, const float* pin, const float* coarse, float* pout,
@@ -385,7 +545,7 @@ void fp_launch_prolong(const SimParams* dP, int level, bool tiles, const float* 
   if (tiles)
     k_level_tiles<PROLONG><<<tileGrid(capacity, sms), 64, 0, st>>>(dP, A);
   else
-    k_level_bricks<PROLONG><<<sms * 4, 256, 0, st>>>(dP, A);
+    k_level_bricks_staged<PROLONG><<<sms * 4, 256, g_stageBytes, st>>>(dP, A);
 }
 
 int fp_bottom_capacity() { return (200 * 1024) / 12; }
@@ -393,10 +553,5 @@ int fp_bottom_capacity() { return (200 * 1024) / 12; }
 void fp_launch_bottom(const SimParams* dP, int level, int iterations, const float* rhs, const float* pin, float* pout,
                       int capacity, cudaStream_t st) {
   size_t smem = (size_t)capacity * 12;
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    configured = true;
-  }
   k_bottom<<<1, 1024, smem, st>>>(dP, level, iterations, rhs, pin, pout);
 }

@@ -68,15 +68,27 @@ FP_DEV float fieldSample(const SimParams& P, const Home& H, const Stage& G, cons
   return sampleCells(P, H, f.pool, f.ch, c, px, py, pz);
 }
 
-// Copy channels of a pool over the staged box into shared memory; zero where no slot.
+// Copy channels of a pool over the staged box into shared memory, zero where no slot, with
+// asynchronous 4-byte copies (cp.async): every thread keeps all its copies in flight and the
+// caller waits once. A brick without a slot reads nothing (source size 0 zero-fills).
 FP_DEV void stageField(const SimParams& P, const Home& H, const Stage& G, float* sm, const float* pool, int ch) {
   for (int i = threadIdx.x; i < G.S3; i += blockDim.x) {
     int lx = i % G.S, ly = (i / G.S) % G.S, lz = i / (G.S * G.S);
     int x = G.ox + lx, y = G.oy + ly, z = G.oz + lz;
     int s = brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift);
-    size_t base = s < 0 ? 0 : (size_t)s * ch * P.N + localCell(P, x, y, z);
-    for (int c = 0; c < ch; c++) sm[c * G.S3 + i] = s < 0 ? 0.f : pool[base + (size_t)c * P.N];
+    const float* src = s < 0 ? pool : pool + (size_t)s * ch * P.N + localCell(P, x, y, z);
+    int bytes = s < 0 ? 0 : 4;
+    for (int c = 0; c < ch; c++) {
+      unsigned dst = (unsigned)__cvta_generic_to_shared(sm + c * G.S3 + i);
+      const float* g = s < 0 ? pool : src + (size_t)c * P.N;
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(g), "r"(bytes) : "memory");
+    }
   }
+}
+// Wait for this thread's staged copies, then for every thread's.
+FP_DEV void stageWait() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
 }
 
 FP_DEV Stage stageOf(const SimParams& P, const Home& H, bool staged) {
@@ -141,7 +153,7 @@ FP_DEV void cellOf(const SimParams& P, const Home& H, int c, int& x, int& y, int
 // advectScalars (fluid-scalar-transport.wgsl:38-142), fused: both read only the velocity and
 // the scalars at the start of the step.
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS) k_predict(const SimParams* __restrict__ Pp) {
+__global__ void __launch_bounds__(THREADS, 3) k_predict(const SimParams* __restrict__ Pp) {
   const SimParams& P = *Pp;
   __shared__ int nslot[27];
   extern __shared__ float smem[];
@@ -155,7 +167,7 @@ __global__ void __launch_bounds__(THREADS) k_predict(const SimParams* __restrict
     if (STAGED) {
       stageField(P, H, G, smem, P.vel, 3);
       stageField(P, H, G, smem + 3 * G.S3, P.fld, 4);
-      __syncthreads();
+      stageWait();
     }
     size_t slot = (size_t)nslot[13];
     const size_t N = P.N;
@@ -246,7 +258,7 @@ __global__ void __launch_bounds__(THREADS) k_predict(const SimParams* __restrict
 // ---------------------------------------------------------------------------------------
 // correctVelocity (fluid-velocity-transport.wgsl:104-179): bounded MacCormack correction.
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS) k_correct(const SimParams* __restrict__ Pp) {
+__global__ void __launch_bounds__(THREADS, 3) k_correct(const SimParams* __restrict__ Pp) {
   const SimParams& P = *Pp;
   __shared__ int nslot[27];
   extern __shared__ float smem[];
@@ -260,7 +272,7 @@ __global__ void __launch_bounds__(THREADS) k_correct(const SimParams* __restrict
     if (STAGED) {
       stageField(P, H, G, smem, P.vel, 3);
       stageField(P, H, G, smem + 3 * G.S3, P.velP, 3);
-      __syncthreads();
+      stageWait();
     }
     size_t slot = (size_t)nslot[13];
     const size_t N = P.N;
@@ -322,7 +334,7 @@ __global__ void __launch_bounds__(THREADS) k_correct(const SimParams* __restrict
 // evolveFields (fluid-field-evolution.wgsl:9-84) with correctedScalars
 // (fluid-scalar-transport.wgsl:144-199) and recordContent (fluid-content.wgsl:29-64).
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS) k_evolve(const SimParams* __restrict__ Pp) {
+__global__ void __launch_bounds__(THREADS, 3) k_evolve(const SimParams* __restrict__ Pp) {
   const SimParams& P = *Pp;
   __shared__ int nslot[27];
   __shared__ uint32_t busyAll, expandsAll;
@@ -342,7 +354,7 @@ __global__ void __launch_bounds__(THREADS) k_evolve(const SimParams* __restrict_
     if (STAGED) {
       stageField(P, H, G, smem, P.vel, 3);
       stageField(P, H, G, smem + 3 * G.S3, P.fldP, 4);
-      __syncthreads();
+      stageWait();
     }
     size_t slot = (size_t)nslot[13];
     const size_t N = P.N;
@@ -823,16 +835,23 @@ __global__ void k_noise(float4* __restrict__ out) {
 }  // namespace
 
 // Staged kernels for 8^3 bricks: `channels` staged fields over (8 + 2 HALO)^3 cells.
+static size_t stagedBytes(int channels) {
+  const int S = 8 + 2 * HALO;
+  return (size_t)channels * S * S * S * sizeof(float);
+}
 template <typename K>
 static void launchStaged(K kernel, int channels, const SimParams* dP, int sms, cudaStream_t st) {
-  const int S = 8 + 2 * HALO;
-  size_t smem = (size_t)channels * S * S * S * sizeof(float);
-  static bool configured = false;  // per kernel instantiation
-  if (!configured) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = true;
-  }
-  kernel<<<sms * 4, THREADS, smem, st>>>(dP);
+  kernel<<<sms * 4, THREADS, stagedBytes(channels), st>>>(dP);
+}
+
+// Shared-memory limits of the step kernels, set once before any launch (and so before any
+// stream capture of one).
+void fp_step_configure(int B) {
+  cudaFuncSetAttribute(k_predict<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
+  cudaFuncSetAttribute(k_correct<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(6));
+  cudaFuncSetAttribute(k_evolve<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
+  size_t smem = (size_t)(B + 1) * (B + 1) * (B + 1) * sizeof(float3);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_forces, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 void fp_launch_predict(const SimParams* dP, int B, int sms, cudaStream_t st) {
@@ -856,7 +875,6 @@ void fp_launch_evolve(const SimParams* dP, int B, int sms, cudaStream_t st) {
 void fp_launch_curl(const SimParams* dP, int sms, cudaStream_t st) { k_curl<<<sms * 4, THREADS, 0, st>>>(dP); }
 void fp_launch_forces(const SimParams* dP, int B, int sms, cudaStream_t st) {
   size_t smem = (size_t)(B + 1) * (B + 1) * (B + 1) * sizeof(float3);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_forces, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_forces<<<sms * 4, THREADS, smem, st>>>(dP);
 }
 void fp_launch_divergence(const SimParams* dP, float* pOut, int sms, cudaStream_t st) {

@@ -176,6 +176,8 @@ class fp_stats(C.Structure):
         ("kernel_launches", C.c_uint64),
         ("h2d_bytes", C.c_uint64),
         ("d2h_bytes", C.c_uint64),
+        ("host_prepare_ms", C.c_double),
+        ("host_wait_ms", C.c_double),
     ]
 
 
