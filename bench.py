@@ -288,7 +288,9 @@ def run_ours(args, rank, world, local):
     total_prof = sum(p["ms"] for p in phases.values())
     for p in phases.values():
         p["share"] = p["ms"] / total_prof if total_prof else None
-    dominant = max(phases, key=lambda k: phases[k]["ms"])
+    # The dominant kernel: the longest phase that is one kernel (the multigrid phase is ~30
+    # launches of several kernels and is reported beside it).
+    dominant = max((k for k in phases if k != "multigrid"), key=lambda k: phases[k]["ms"])
     dom = phases[dominant]
     achieved = dom["gbs"]
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
