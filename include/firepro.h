@@ -236,6 +236,35 @@ int fp_sim_set_profiling(fp_sim* sim, int enabled);
 /* The per-phase totals since profiling started. `*count` in: capacity, out: phases. */
 int fp_sim_read_profile(fp_sim* sim, fp_phase* phases, uint32_t* count);
 
+/* ---- Batches: many independent simulations stepped by one launch.
+ * No reference counterpart: the reference steps one `FluidSimulation` per call. A batch owns
+ * one CUDA stream; its simulations share a brick size and may differ in everything else
+ * (voxel size, budget, scene, dt). `fp_batch_step` steps any subset of them with one upload
+ * and one CUDA graph whose kernels cover every listed simulation's bricks; each simulation's
+ * results are bit-identical to stepping it alone. A simulation is named by the id
+ * `fp_batch_add` returned. Errors of a step name the simulation's position in `ids`. */
+typedef struct fp_batch fp_batch;
+const char* fp_batch_last_error(const fp_batch* batch);
+int fp_batch_create(int device, int brick_size, fp_batch** out);
+int fp_batch_destroy(fp_batch* batch);
+/* Add a simulation of `grid` (validated as by fp_sim_create); `*id` receives its id. */
+int fp_batch_add(fp_batch* batch, const fp_grid* grid, uint32_t* id);
+/* Remove a simulation and free its device memory; its id may be reused. */
+int fp_batch_remove(fp_batch* batch, uint32_t id);
+int fp_batch_reset(fp_batch* batch, uint32_t id);
+int fp_batch_set_runtime(fp_batch* batch, uint32_t id, float cutoff, double voxel_budget, int ground);
+/* Step the `count` simulations `ids` (distinct) with frames[i] and dts[i], in one launch. */
+int fp_batch_step(fp_batch* batch, const uint32_t* ids, const fp_frame* frames, const float* dts, uint32_t count);
+int fp_batch_synchronize(fp_batch* batch);
+int fp_batch_stats(fp_batch* batch, uint32_t id, fp_stats* out);
+int fp_batch_read_field(fp_batch* batch, uint32_t id, int field, float* host, size_t bytes);
+int fp_batch_read_table(fp_batch* batch, uint32_t id, int table, void* host, size_t* bytes);
+int fp_batch_stream(fp_batch* batch, void** stream);
+int fp_batch_set_profiling(fp_batch* batch, int enabled);
+int fp_batch_read_profile(fp_batch* batch, fp_phase* phases, uint32_t* count);
+/* Device bytes a simulation of `grid` holds once created: the admission estimate. */
+int fp_grid_memory_bytes(const fp_grid* grid, uint64_t* bytes);
+
 /* Most ids fp_compact_ids_noalloc accepts in one call. */
 #define FP_COMPACT_MAX_IDS (1u << 22)
 

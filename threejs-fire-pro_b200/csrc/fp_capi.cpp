@@ -1,16 +1,29 @@
 // extern "C" entry points of include/firepro.h. Each validates its arguments, forwards to
 // the host engine and turns any failure into a status code with a message; nothing throws
-// across the ABI.
+// across the ABI. A single simulation is an Engine stepped by a Stepper of its own; a batch
+// shares one Stepper among many Engines.
 #include <cmath>
+#include <memory>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/firepro.h"
 #include "fp_engine.hpp"
 #include "fp_error.h"
 
 struct fp_sim {
+  fp::Stepper* stepper;
   fp::Engine* engine;
+};
+
+struct fp_batch {
+  fp::Stepper* stepper;
+  std::vector<fp::Engine*> sims;  // by id; null where removed
+  std::string error;
+  // per-step scratch
+  std::vector<fp::Engine*> stepSims;
+  std::vector<const fp_frame*> stepFrames;
 };
 
 static thread_local std::string g_error;
@@ -22,19 +35,8 @@ static int failed(const std::string& message, int code) {
 
 int fp_set_error(int code, const std::string& message) { return failed(message, code); }
 
-extern "C" {
-
-int fp_abi_version(void) { return FP_ABI_VERSION; }
-
-const char* fp_last_error(const fp_sim* sim) {
-  if (sim && sim->engine) return sim->engine->error().c_str();
-  return g_error.c_str();
-}
-
 // The grid validation of FluidSimulation's constructor (FluidSimulation.ts:359-379).
-int fp_sim_create(const fp_grid* grid, int device, fp_sim** out) {
-  if (!grid || !out) return failed("fp_sim_create needs a grid and an output handle.", FP_EINVAL);
-  *out = nullptr;
+static int validateGrid(const fp_grid* grid) {
   if (!std::isfinite(grid->voxel_size) || grid->voxel_size < 0.0001f || grid->voxel_size > 16.f)
     return failed("voxelSize must be from 0.0001 to 16 meters.", FP_EINVAL);
   int vd = grid->velocity_divisor;
@@ -54,17 +56,62 @@ int fp_sim_create(const fp_grid* grid, int device, fp_sim** out) {
   if (bs == 32) return failed("brickSize 32 is not implemented by this build.", FP_EUNSUPPORTED);
   if (grid->precision != FP_PRECISION_FP32)
     return failed("FP_PRECISION_MIXED is not implemented by this build.", FP_EUNSUPPORTED);
-  fp::Engine* e = new (std::nothrow) fp::Engine(*grid, device);
-  if (!e) return failed("out of host memory", FP_ENOMEM);
-  int rc = e->initialize();
+  return FP_OK;
+}
+
+static bool frameArraysValid(const fp_frame* f) {
+  return !((f->source_count && !f->sources) || (f->force_count && !f->forces) ||
+           (f->collider_count && !f->colliders) || (f->force_target_count && !f->force_targets) ||
+           (f->collider_mask_words && !f->collider_masks));
+}
+
+static fp::Stepper* newStepper(int device, int brickSize, int& rc) {
+  fp::Stepper* st = new (std::nothrow) fp::Stepper(device, brickSize);
+  if (!st) {
+    rc = failed("out of host memory", FP_ENOMEM);
+    return nullptr;
+  }
+  rc = st->initialize();
+  if (rc) {
+    g_error = st->error();
+    delete st;
+    return nullptr;
+  }
+  return st;
+}
+
+extern "C" {
+
+int fp_abi_version(void) { return FP_ABI_VERSION; }
+
+const char* fp_last_error(const fp_sim* sim) {
+  if (sim && sim->engine) return sim->engine->error().c_str();
+  return g_error.c_str();
+}
+
+int fp_sim_create(const fp_grid* grid, int device, fp_sim** out) {
+  if (!grid || !out) return failed("fp_sim_create needs a grid and an output handle.", FP_EINVAL);
+  *out = nullptr;
+  int rc = validateGrid(grid);
+  if (rc) return rc;
+  fp::Stepper* st = newStepper(device, grid->brick_size, rc);
+  if (!st) return rc;
+  fp::Engine* e = new (std::nothrow) fp::Engine(*grid, st);
+  if (!e) {
+    delete st;
+    return failed("out of host memory", FP_ENOMEM);
+  }
+  rc = e->initialize();
   if (rc) {
     g_error = e->error();
     delete e;
+    delete st;
     return rc;
   }
-  fp_sim* s = new (std::nothrow) fp_sim{e};
+  fp_sim* s = new (std::nothrow) fp_sim{st, e};
   if (!s) {
     delete e;
+    delete st;
     return failed("out of host memory", FP_ENOMEM);
   }
   *out = s;
@@ -74,6 +121,7 @@ int fp_sim_create(const fp_grid* grid, int device, fp_sim** out) {
 int fp_sim_destroy(fp_sim* sim) {
   if (!sim) return FP_OK;
   delete sim->engine;
+  delete sim->stepper;
   delete sim;
   return FP_OK;
 }
@@ -90,16 +138,18 @@ int fp_sim_set_runtime(fp_sim* sim, float cutoff, double voxel_budget, int groun
 
 int fp_sim_step(fp_sim* sim, const fp_frame* frame, float dt) {
   if (!sim || !frame) return failed("fp_sim_step needs a simulation and a frame.", FP_EINVAL);
-  if ((frame->source_count && !frame->sources) || (frame->force_count && !frame->forces) ||
-      (frame->collider_count && !frame->colliders) || (frame->force_target_count && !frame->force_targets) ||
-      (frame->collider_mask_words && !frame->collider_masks))
-    return sim->engine->fail(FP_EINVAL, "frame arrays are null but their counts are not");
-  return sim->engine->step(*frame, dt);
+  if (!frameArraysValid(frame)) return sim->engine->fail(FP_EINVAL, "frame arrays are null but their counts are not");
+  fp::Engine* e = sim->engine;
+  int rc = sim->stepper->step(&e, &frame, &dt, 1);
+  if (rc) e->fail(rc, sim->stepper->error());
+  return rc;
 }
 
 int fp_sim_synchronize(fp_sim* sim) {
   if (!sim) return failed("null simulation", FP_EINVAL);
-  return sim->engine->synchronize();
+  int rc = sim->stepper->synchronize();
+  if (rc) sim->engine->fail(rc, sim->stepper->error());
+  return rc;
 }
 
 int fp_sim_stats(fp_sim* sim, fp_stats* out) {
@@ -124,18 +174,183 @@ int fp_sim_read_bricks(fp_sim* sim, float* boxes, uint32_t* count) {
 
 int fp_sim_stream(fp_sim* sim, void** stream) {
   if (!sim || !stream) return failed("fp_sim_stream needs a simulation and an output.", FP_EINVAL);
-  *stream = (void*)sim->engine->stream();
+  *stream = (void*)sim->stepper->stream();
   return FP_OK;
 }
 
 int fp_sim_set_profiling(fp_sim* sim, int enabled) {
   if (!sim) return failed("null simulation", FP_EINVAL);
-  return sim->engine->setProfiling(enabled != 0);
+  int rc = sim->stepper->setProfiling(enabled != 0);
+  if (rc) sim->engine->fail(rc, sim->stepper->error());
+  return rc;
 }
 
 int fp_sim_read_profile(fp_sim* sim, fp_phase* phases, uint32_t* count) {
   if (!sim || !count) return failed("fp_sim_read_profile needs a simulation and a count.", FP_EINVAL);
-  return sim->engine->readProfile(phases, count);
+  int rc = sim->stepper->readProfile(phases, count);
+  if (rc) sim->engine->fail(rc, sim->stepper->error());
+  return rc;
+}
+
+// ---------------------------------------------------------------------------- batches
+
+const char* fp_batch_last_error(const fp_batch* batch) { return batch ? batch->error.c_str() : g_error.c_str(); }
+
+static int batchFail(fp_batch* b, int code, const std::string& message) {
+  b->error = message;
+  g_error = message;
+  return code;
+}
+
+static fp::Engine* batchSim(fp_batch* b, uint32_t id) { return id < b->sims.size() ? b->sims[id] : nullptr; }
+
+int fp_batch_create(int device, int brick_size, fp_batch** out) {
+  if (!out) return failed("fp_batch_create needs an output handle.", FP_EINVAL);
+  *out = nullptr;
+  if (brick_size != 8 && brick_size != 16) return failed("a batch's brickSize must be 8 or 16.", FP_EINVAL);
+  int rc;
+  fp::Stepper* st = newStepper(device, brick_size, rc);
+  if (!st) return rc;
+  fp_batch* b = new (std::nothrow) fp_batch{};
+  if (!b) {
+    delete st;
+    return failed("out of host memory", FP_ENOMEM);
+  }
+  b->stepper = st;
+  *out = b;
+  return FP_OK;
+}
+
+int fp_batch_destroy(fp_batch* batch) {
+  if (!batch) return FP_OK;
+  for (fp::Engine* e : batch->sims) delete e;
+  delete batch->stepper;
+  delete batch;
+  return FP_OK;
+}
+
+int fp_batch_add(fp_batch* batch, const fp_grid* grid, uint32_t* id) {
+  if (!batch || !grid || !id) return failed("fp_batch_add needs a batch, a grid and an output id.", FP_EINVAL);
+  int rc = validateGrid(grid);
+  if (rc) return batchFail(batch, rc, g_error);
+  if (grid->brick_size != batch->stepper->brickSize())
+    return batchFail(batch, FP_EINVAL, "brickSize differs from the batch's.");
+  fp::Engine* e = new (std::nothrow) fp::Engine(*grid, batch->stepper);
+  if (!e) return batchFail(batch, FP_ENOMEM, "out of host memory");
+  if ((rc = e->initialize())) {
+    std::string m = e->error();
+    delete e;
+    return batchFail(batch, rc, m);
+  }
+  uint32_t slot = 0;
+  while (slot < batch->sims.size() && batch->sims[slot]) slot++;
+  if (slot == batch->sims.size()) batch->sims.push_back(nullptr);
+  batch->sims[slot] = e;
+  *id = slot;
+  return FP_OK;
+}
+
+int fp_batch_remove(fp_batch* batch, uint32_t id) {
+  if (!batch) return failed("null batch", FP_EINVAL);
+  fp::Engine* e = batchSim(batch, id);
+  if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
+  int rc = batch->stepper->consume();
+  if (rc) return batchFail(batch, rc, batch->stepper->error());
+  delete e;
+  batch->sims[id] = nullptr;
+  return FP_OK;
+}
+
+int fp_batch_reset(fp_batch* batch, uint32_t id) {
+  if (!batch) return failed("null batch", FP_EINVAL);
+  fp::Engine* e = batchSim(batch, id);
+  if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
+  int rc = e->reset();
+  return rc ? batchFail(batch, rc, e->error()) : FP_OK;
+}
+
+int fp_batch_set_runtime(fp_batch* batch, uint32_t id, float cutoff, double voxel_budget, int ground) {
+  if (!batch) return failed("null batch", FP_EINVAL);
+  fp::Engine* e = batchSim(batch, id);
+  if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
+  int rc = e->setRuntime(cutoff, voxel_budget, ground);
+  return rc ? batchFail(batch, rc, e->error()) : FP_OK;
+}
+
+int fp_batch_step(fp_batch* batch, const uint32_t* ids, const fp_frame* frames, const float* dts, uint32_t count) {
+  if (!batch) return failed("null batch", FP_EINVAL);
+  if (count && (!ids || !frames || !dts)) return batchFail(batch, FP_EINVAL, "fp_batch_step needs ids, frames and dts.");
+  batch->stepSims.assign(count, nullptr);
+  batch->stepFrames.assign(count, nullptr);
+  for (uint32_t i = 0; i < count; i++) {
+    fp::Engine* e = batchSim(batch, ids[i]);
+    if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(ids[i]));
+    for (uint32_t j = 0; j < i; j++)
+      if (ids[j] == ids[i]) return batchFail(batch, FP_EINVAL, "simulation " + std::to_string(ids[i]) + " listed twice");
+    if (!frameArraysValid(&frames[i]))
+      return batchFail(batch, FP_EINVAL,
+                       "simulation " + std::to_string(i) + ": frame arrays are null but their counts are not");
+    batch->stepSims[i] = e;
+    batch->stepFrames[i] = &frames[i];
+  }
+  int rc = batch->stepper->step(batch->stepSims.data(), batch->stepFrames.data(), dts, (int)count);
+  return rc ? batchFail(batch, rc, batch->stepper->error()) : FP_OK;
+}
+
+int fp_batch_synchronize(fp_batch* batch) {
+  if (!batch) return failed("null batch", FP_EINVAL);
+  int rc = batch->stepper->synchronize();
+  return rc ? batchFail(batch, rc, batch->stepper->error()) : FP_OK;
+}
+
+int fp_batch_stats(fp_batch* batch, uint32_t id, fp_stats* out) {
+  if (!batch || !out) return failed("fp_batch_stats needs a batch and an output.", FP_EINVAL);
+  fp::Engine* e = batchSim(batch, id);
+  if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
+  int rc = e->stats(out);
+  return rc ? batchFail(batch, rc, e->error()) : FP_OK;
+}
+
+int fp_batch_read_field(fp_batch* batch, uint32_t id, int field, float* host, size_t bytes) {
+  if (!batch || !host) return failed("fp_batch_read_field needs a batch and a buffer.", FP_EINVAL);
+  fp::Engine* e = batchSim(batch, id);
+  if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
+  int rc = e->readField(field, host, bytes);
+  return rc ? batchFail(batch, rc, e->error()) : FP_OK;
+}
+
+int fp_batch_read_table(fp_batch* batch, uint32_t id, int table, void* host, size_t* bytes) {
+  if (!batch || !bytes) return failed("fp_batch_read_table needs a batch and a size.", FP_EINVAL);
+  fp::Engine* e = batchSim(batch, id);
+  if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
+  int rc = e->readTable(table, host, bytes);
+  return rc ? batchFail(batch, rc, e->error()) : FP_OK;
+}
+
+int fp_batch_stream(fp_batch* batch, void** stream) {
+  if (!batch || !stream) return failed("fp_batch_stream needs a batch and an output.", FP_EINVAL);
+  *stream = (void*)batch->stepper->stream();
+  return FP_OK;
+}
+
+int fp_batch_set_profiling(fp_batch* batch, int enabled) {
+  if (!batch) return failed("null batch", FP_EINVAL);
+  int rc = batch->stepper->setProfiling(enabled != 0);
+  return rc ? batchFail(batch, rc, batch->stepper->error()) : FP_OK;
+}
+
+int fp_batch_read_profile(fp_batch* batch, fp_phase* phases, uint32_t* count) {
+  if (!batch || !count) return failed("fp_batch_read_profile needs a batch and a count.", FP_EINVAL);
+  int rc = batch->stepper->readProfile(phases, count);
+  return rc ? batchFail(batch, rc, batch->stepper->error()) : FP_OK;
+}
+
+int fp_grid_memory_bytes(const fp_grid* grid, uint64_t* bytes) {
+  if (!grid || !bytes) return failed("fp_grid_memory_bytes needs a grid and an output.", FP_EINVAL);
+  int rc = validateGrid(grid);
+  if (rc) return rc;
+  *bytes = fp::Engine::estimateBytes(*grid);
+  return FP_OK;
 }
 
 }  // extern "C"

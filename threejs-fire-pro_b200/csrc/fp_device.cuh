@@ -10,6 +10,25 @@
 
 #define FP_DEV __device__ __forceinline__
 
+// Work lists of a batch (fp_types.h): the simulations in the launch, a list's total, and the
+// simulation an item belongs to with the item's index in that simulation's own list.
+FP_DEV int batchCount(const FpBatch& b) { return (int)b.work[0]; }
+FP_DEV const uint32_t* workRow(const FpBatch& b, int kind) { return b.work + 1 + kind * b.stride; }
+FP_DEV uint32_t workTotal(const FpBatch& b, int kind) { return workRow(b, kind)[batchCount(b)]; }
+FP_DEV const SimParams& workSim(const FpBatch& b, int kind, uint32_t item, uint32_t& local) {
+  const uint32_t* row = workRow(b, kind);
+  int lo = 0, hi = batchCount(b) - 1;
+  while (lo < hi) {  // the last simulation whose first item is at or before `item`
+    int mid = (lo + hi + 1) >> 1;
+    if (row[mid] <= item)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  local = item - row[lo];
+  return b.sims[lo];
+}
+
 FP_DEV int nbrIndex(int dx, int dy, int dz) { return (dz + 1) * 9 + (dy + 1) * 3 + dx + 1; }
 FP_DEV int entryPage(int e) { return e < 0 ? -1 : (e & 0xffffff); }
 

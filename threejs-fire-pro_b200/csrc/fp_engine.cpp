@@ -97,7 +97,7 @@ bool Engine::alloc(DeviceBuffer& b, size_t bytes, bool zero) {
     return false;
   }
   b.bytes = bytes;
-  if (zero) cudaMemsetAsync(b.ptr, 0, bytes, stream_);
+  if (zero) cudaMemsetAsync(b.ptr, 0, bytes, stream());
   return true;
 }
 
@@ -108,10 +108,10 @@ bool Engine::grow(DeviceBuffer& b, size_t bytes, int fill) {
     error_ = "device memory exhausted";
     return false;
   }
-  cudaMemsetAsync(p, fill, bytes, stream_);
+  cudaMemsetAsync(p, fill, bytes, stream());
   if (b.ptr) {
-    cudaMemcpyAsync(p, b.ptr, b.bytes, cudaMemcpyDeviceToDevice, stream_);
-    cudaStreamSynchronize(stream_);
+    cudaMemcpyAsync(p, b.ptr, b.bytes, cudaMemcpyDeviceToDevice, stream());
+    cudaStreamSynchronize(stream());
     cudaFree(b.ptr);
   }
   b.ptr = p;
@@ -125,12 +125,12 @@ bool Engine::grow(DeviceBuffer& b, size_t bytes, int fill) {
 bool Engine::upload(DeviceBuffer& b, const void* src, size_t bytes) {
   if (bytes == 0) return true;
   if (bytes > b.bytes) {
-    cudaStreamSynchronize(stream_);  // the old buffer may still be read: rare growth
+    cudaStreamSynchronize(stream());  // the old buffer may still be read: rare growth
     if (!alloc(b, std::max(bytes + bytes / 2, (size_t)256), false)) return false;
   }
   size_t off = (stageUsed_ + 255) & ~(size_t)255;
   if (off + bytes > stageCap_) {
-    cudaStreamSynchronize(stream_);  // copies from the old arena must finish before it goes
+    cudaStreamSynchronize(stream());  // copies from the old arena must finish before it goes
     if (stageH_) cudaFreeHost(stageH_);
     stageCap_ = std::max(std::max(stageCap_ * 2, off + bytes), (size_t)1 << 20);
     if (cudaMallocHost(&stageH_, stageCap_) != cudaSuccess) {
@@ -144,7 +144,7 @@ bool Engine::upload(DeviceBuffer& b, const void* src, size_t bytes) {
   std::memcpy(stageH_ + off, src, bytes);
   stageUsed_ = off + bytes;
   h2d_ += bytes;
-  return cudaMemcpyAsync(b.ptr, stageH_ + off, bytes, cudaMemcpyHostToDevice, stream_) == cudaSuccess;
+  return cudaMemcpyAsync(b.ptr, stageH_ + off, bytes, cudaMemcpyHostToDevice, stream()) == cudaSuccess;
 }
 
 uint32_t Engine::slotLimit() const {
@@ -152,7 +152,7 @@ uint32_t Engine::slotLimit() const {
   return (uint32_t)std::max(1.0, v);
 }
 
-Engine::Engine(const fp_grid& g, int device) : device_(device) {
+Engine::Engine(const fp_grid& g, Stepper* owner) : owner_(owner) {
   B_ = g.brick_size;
   shift_ = B_ == 8 ? 3 : 4;
   N_ = B_ * B_ * B_;
@@ -166,25 +166,23 @@ Engine::Engine(const fp_grid& g, int device) : device_(device) {
 }
 
 Engine::~Engine() {
-  if (stream_) cudaStreamSynchronize(stream_);
+  owner_->forget(this);
+  cudaStreamSynchronize(stream());
   freeAll();
-  if (paramsH_) cudaFreeHost(paramsH_);
   if (stageH_) cudaFreeHost(stageH_);
-  if (readH_) cudaFreeHost(readH_);
-  if (readEvent_) cudaEventDestroy(readEvent_);
-  for (Phase& ph : phases_) {
-    if (ph.a) cudaEventDestroy(ph.a);
-    if (ph.b) cudaEventDestroy(ph.b);
-  }
-  if (stream_) cudaStreamDestroy(stream_);
+}
+
+cudaStream_t Engine::stream() const { return owner_->stream(); }
+int Engine::consume() {
+  int rc = owner_->consume();
+  if (rc) error_ = owner_->error();
+  return rc;
 }
 
 void Engine::freeAll() {
-  clearGraphs();
   DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_, &zeroList_,
                          &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_, &donors_, &solids_,
-                         &tileRecD_, &tileNbrD_, &hashD_, &emittersD_, &collidersD_, &masksD_, &forcesD_,
-                         &regionsD_, &tileListsD_, &noise_, &paramsD_};
+                         &tileRecD_, &tileNbrD_, &hashD_};
   for (DeviceBuffer* b : all)
     if (b->ptr) {
       cudaFree(b->ptr);
@@ -204,20 +202,9 @@ void Engine::freeAll() {
 // FluidSimulation.ts:496-549 allocate(): empty pools of the whole voxel budget, no tiles.
 int Engine::initialize() {
   int rc;
-  if ((rc = check(cudaSetDevice(device_), "cudaSetDevice"))) return rc;
-  if (!stream_) {
-    if ((rc = check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
-    cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_);
-    if ((rc = check(cudaMallocHost(&paramsH_, sizeof(SimParams)), "cudaMallocHost"))) return rc;
-    if ((rc = check(cudaEventCreateWithFlags(&readEvent_, cudaEventDisableTiming), "cudaEventCreate"))) return rc;
-  }
+  if ((rc = check(cudaSetDevice(owner_->device()), "cudaSetDevice"))) return rc;
   freeAll();
-  if (!alloc(paramsD_, sizeof(SimParams)) || !alloc(counters_, sizeof(FpCounters)) ||
-      !alloc(noise_, 64 * 64 * 64 * sizeof(float4)))
-    return FP_ENOMEM;
-  fp_launch_noise((float4*)noise_.ptr, stream_);
-  fp_mg_configure(B_);
-  fp_step_configure(B_);
+  if (!alloc(counters_, sizeof(FpCounters))) return FP_ENOMEM;
   slots_ = 0;
   capacity_ = 0;
   if ((rc = allocatePools(slotLimit()))) return rc;
@@ -234,13 +221,29 @@ int Engine::initialize() {
   latest_ = 0;
   activeBricks_ = usedSlots_ = lastFailures_ = 0;
   poolLimited_ = false;
-  pendingRead_ = false;
   colliderCount_ = 0;
   prevColliders_.clear();
   prevMasks_.clear();
   for (int k = 0; k < 4; k++) velIdx_[k] = k;
   for (int k = 0; k < 3; k++) fldIdx_[k] = k;
-  return check(cudaStreamSynchronize(stream_), "initialize");
+  return check(cudaStreamSynchronize(stream()), "initialize");
+}
+
+// Device bytes of a simulation of `g` once its pools exist: per slot the pools and the brick
+// levels, per tile slot (at the minimum capacity) the tables and tile levels.
+uint64_t Engine::estimateBytes(const fp_grid& g) {
+  int B = g.brick_size, shift = B == 8 ? 3 : 4;
+  uint64_t N = (uint64_t)B * B * B;
+  double budget = g.voxel_budget > 0 ? g.voxel_budget : 8e6;
+  uint64_t slots = (uint64_t)std::max(1.0, std::floor(budget / (double)N));
+  uint64_t perSlot = N * 4 * (4 * 3 + 4 + 3 * 4 + 1 + 1 + 3 + 3 + 8 + 2) + N * 3 * 2 + N / 8 + N + 4;
+  for (int l = 1; l < shift; l++) {
+    uint64_t c = (uint64_t)1 << (3 * (shift - l));
+    perSlot += c * 13;
+  }
+  uint64_t tiles = MIN_TILES;
+  uint64_t perTile = 64 * (4 * 5 + FP_RECORD_WORDS * 4 + 8) + 16 + 27 * 4 + 16 + (64 + 8 + 1) * 13;
+  return slots * perSlot + tiles * perTile + 64 * 1024;
 }
 
 // Pools of `slots` slots, all free: the stack pops slot 0 first.
@@ -272,8 +275,7 @@ int Engine::allocatePools(uint32_t slots) {
 // live pools keep their contents.
 int Engine::growPool(uint32_t target) {
   if (target <= slots_) return FP_OK;
-  cudaStreamSynchronize(stream_);
-  clearGraphs();
+  cudaStreamSynchronize(stream());
   size_t s = target, N = N_;
   uint32_t added = target - slots_;
   bool ok = true;
@@ -307,8 +309,7 @@ int Engine::growPool(uint32_t target) {
 // Per-brick and per-tile storage for `capacity` tile slots, keeping every brick's page,
 // state, flags, entry and record (FluidSimulation.ts:633-646).
 int Engine::setCapacity(int capacity) {
-  if (stream_) cudaStreamSynchronize(stream_);
-  clearGraphs();
+  cudaStreamSynchronize(stream());
   size_t bricks = (size_t)capacity * 64;
   size_t oldBricks = (size_t)capacity_ * 64;
   bool ok = grow(pages_, bricks * 4, 0xff) && grow(entries_, bricks * 4, 0xff) && grow(state_, bricks * 4, 0) &&
@@ -320,8 +321,8 @@ int Engine::setCapacity(int capacity) {
     DeviceBuffer next;
     if (!alloc(next, (bricks + capacity) * 4)) return FP_ENOMEM;
     if (activity_.ptr) {
-      cudaMemcpyAsync(next.ptr, activity_.ptr, oldBricks * 4, cudaMemcpyDeviceToDevice, stream_);
-      cudaStreamSynchronize(stream_);
+      cudaMemcpyAsync(next.ptr, activity_.ptr, oldBricks * 4, cudaMemcpyDeviceToDevice, stream());
+      cudaStreamSynchronize(stream());
       cudaFree(activity_.ptr);
     }
     activity_ = next;
@@ -369,10 +370,10 @@ int Engine::applyTiles() {
   // New tiles' bricks start without slots.
   for (int slot : dir_.takeCreated()) {
     size_t off = (size_t)slot * 64 * 4;
-    cudaMemsetAsync((char*)pages_.ptr + off, 0xff, 64 * 4, stream_);
-    cudaMemsetAsync((char*)entries_.ptr + off, 0xff, 64 * 4, stream_);
-    cudaMemsetAsync((char*)state_.ptr + off, 0, 64 * 4, stream_);
-    cudaMemsetAsync((char*)activity_.ptr + off, 0, 64 * 4, stream_);
+    cudaMemsetAsync((char*)pages_.ptr + off, 0xff, 64 * 4, stream());
+    cudaMemsetAsync((char*)entries_.ptr + off, 0xff, 64 * 4, stream());
+    cudaMemsetAsync((char*)state_.ptr + off, 0, 64 * 4, stream());
+    cudaMemsetAsync((char*)activity_.ptr + off, 0, 64 * 4, stream());
   }
   dir_.dirty = false;
   geometryDirty_ = true;  // PressureSolver.setBricks -> resetPlans
@@ -402,7 +403,7 @@ void Engine::updateTiles(const fp_frame& f) {
 }
 
 // packFlameStep (flame.ts:43-87): validate before any state changes.
-int Engine::packFlame(const fp_combustion& c, float dt) {
+int Engine::packFlame(const fp_combustion& c, float dt, FpFlame& out) {
   auto finite = [](float v) { return std::isfinite(v); };
   if (!finite(dt)) return fail(FP_EINVAL, "Flame timestep must be finite in f32.");
   if (!finite(c.lifespan)) return fail(FP_EINVAL, "Flame lifespan must be finite in f32.");
@@ -439,7 +440,7 @@ int Engine::packFlame(const fp_combustion& c, float dt) {
     }
     F.counts[ch] = (int)r.count;
   }
-  flame_ = F;
+  out = F;
   return FP_OK;
 }
 
@@ -620,20 +621,74 @@ bool Engine::packScene(const fp_frame& f) {
   return changed;
 }
 
-int Engine::uploadScene() {
-  if (!upload(emittersD_, emitters_.data(), emitters_.size() * sizeof(FpEmitter)) ||
-      !upload(collidersD_, colliders_.data(), colliders_.size() * sizeof(FpCollider)) ||
-      !upload(masksD_, masks_.data(), masks_.size() * 4) ||
-      !upload(forcesD_, forces_.data(), forces_.size() * sizeof(FpForce)) ||
-      !upload(regionsD_, regions_.data(), regions_.size() * sizeof(FpRegion)) ||
-      !upload(tileListsD_, tileLists_.data(), tileLists_.size() * 4))
-    return FP_ENOMEM;
+// Checks of fp_sim_step before any state changes (FluidSimulation.ts:1367-1369).
+int Engine::validate(const fp_frame& f, float dt) {
+  if (!std::isfinite(dt) || dt <= 0 || dt > 1.f / 30.f)
+    return fail(FP_EINVAL, "Simulation step must be in (0, 1/30]. Use fixed substeps.");
+  FpFlame F;
+  int rc = packFlame(f.combustion, dt, F);
+  if (rc) return rc;
+  for (uint32_t i = 0; i < f.collider_count; i++) {
+    const fp_collider& c = f.colliders[i];
+    if (c.shape == FP_SHAPE_MESH) {
+      uint64_t bits = (uint64_t)std::max(0, c.dims[0]) * std::max(0, c.dims[1]) * std::max(0, c.dims[2]);
+      if ((uint64_t)c.mask_offset + (bits + 31) / 32 > f.collider_mask_words)
+        return fail(FP_EINVAL, "Mesh collider occupancy does not match its size.");
+    }
+  }
   return FP_OK;
 }
 
-void Engine::fillParams(const fp_frame& f, float dt) {
-  SimParams& P = *paramsH_;
+// The host half of substep (FluidSimulation.ts:1367-1440): grow the pool to the budget,
+// update the tiles, pack the scene. The measurement of the previous step was applied.
+int Engine::prepare(const fp_frame& f, float dt) {
+  int rc = packFlame(f.combustion, dt, flame_);
+  if (rc) return rc;
+  if (dir_.ground != ground_) {
+    dir_.ground = ground_;
+    geometryDirty_ = true;
+  }
+  uint32_t limit = slotLimit();
+  if (limit > slots_ && (rc = growPool(limit))) return rc;
+  updateTiles(f);
+  if (dir_.dirty && (rc = applyTiles())) return rc;
+  if (packScene(f)) {
+    solidsStale_ = true;
+    geometryDirty_ = true;
+  }
+  mayHaveFlame_ = mayHaveFlame_ || f.fuel.enabled;
+  for (uint32_t i = 0; i < f.source_count; i++) mayHaveFlame_ = mayHaveFlame_ || f.sources[i].flame > 0;
+  return FP_OK;
+}
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+size_t Engine::sceneBytes() const {
+  return align256(emitters_.size() * sizeof(FpEmitter)) + align256(colliders_.size() * sizeof(FpCollider)) +
+         align256(masks_.size() * 4) + align256(forces_.size() * sizeof(FpForce)) +
+         align256(regions_.size() * sizeof(FpRegion)) + align256(tileLists_.size() * 4);
+}
+
+void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t off, const fp_frame& f, float dt,
+                       uint32_t* readback, const float4* noise) {
+  // The scene blobs, each 256-byte aligned, into the launch's upload.
+  auto put = [&](const void* src, size_t bytes) -> const void* {
+    if (bytes) std::memcpy(hostBase + off, src, bytes);
+    const void* d = devBase + off;
+    off += align256(bytes);
+    return d;
+  };
   std::memset(&P, 0, sizeof(P));
+  P.emitters = (const FpEmitter*)put(emitters_.data(), emitters_.size() * sizeof(FpEmitter));
+  P.colliders = (const FpCollider*)put(colliders_.data(), colliders_.size() * sizeof(FpCollider));
+  P.masks = (const uint32_t*)put(masks_.data(), masks_.size() * 4);
+  P.forces = (const FpForce*)put(forces_.data(), forces_.size() * sizeof(FpForce));
+  P.regions = (const FpRegion*)put(regions_.data(), regions_.size() * sizeof(FpRegion));
+  P.tileLists = (const uint32_t*)put(tileLists_.data(), tileLists_.size() * 4);
+  P.buildSolids = buildSolids() ? 1 : 0;
+  P.topoAll = geometryDirty_ ? 1 : 0;
+  P.curlOn = f.simulation.vorticity != 0.f ? 1 : 0;
+  P.readback = readback;
   P.B = B_;
   P.shift = shift_;
   P.N = N_;
@@ -704,27 +759,29 @@ void Engine::fillParams(const fp_frame& f, float dt) {
       P.lrhs[l] = (float*)lrhs_[l].ptr;
     }
   }
-  P.emitters = (const FpEmitter*)emittersD_.ptr;
-  P.colliders = (const FpCollider*)collidersD_.ptr;
-  P.masks = (const uint32_t*)masksD_.ptr;
-  P.forces = (const FpForce*)forcesD_.ptr;
-  P.regions = (const FpRegion*)regionsD_.ptr;
-  P.tileLists = (const uint32_t*)tileListsD_.ptr;
   P.flame = flame_;
-  P.noise = (const float4*)noise_.ptr;
+  P.noise = noise;
+  stepH2d_ = h2d_ + sizeof(SimParams) + sceneBytes();
+  stepD2h_ = readbackWords() * 4;
+  h2d_ = 0;
+}
+
+void Engine::launched(float dt, int latest) {
+  solidsStale_ = false;
+  geometryDirty_ = false;
+  latest_ = latest;
+  std::swap(velIdx_[0], velIdx_[1]);
+  std::swap(fldIdx_[0], fldIdx_[2]);
+  stageUsed_ = 0;
+  time_ += dt;
+  steps_++;
 }
 
 // readActivity (FluidSimulation.ts:1701-1746), applied before the next step: the
 // measurement lags the step by exactly one.
-int Engine::consumeReadback() {
-  if (!pendingRead_) return FP_OK;
-  auto t0 = std::chrono::steady_clock::now();
-  int rc = check(cudaEventSynchronize(readEvent_), "step");
-  hostWaitMs_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  if (rc) return rc;
-  pendingRead_ = false;
-  const FpCounters* c = (const FpCounters*)readH_;
-  const uint32_t* flags = readH_ + sizeof(FpCounters) / 4;
+void Engine::applyReadback(const uint32_t* words) {
+  const FpCounters* c = (const FpCounters*)words;
+  const uint32_t* flags = words + sizeof(FpCounters) / 4;
   contentTiles_.clear();
   for (int s = 0; s < capacity_ && s < (int)tileRec_.size(); s++)
     if (flags[s] && tileRec_[s].w != 0) contentTiles_.push_back({tileRec_[s], flags[s]});
@@ -732,293 +789,13 @@ int Engine::consumeReadback() {
   usedSlots_ = slots_ - (uint32_t)c->freeCount;
   lastFailures_ = c->failures;
   poolLimited_ = c->failures > 0 && slots_ >= slotLimit();
-  if (profilePending_) {
-    // The phases after the measurement may still run: wait for the step's last one.
-    for (int k = PH_COUNT - 1; k >= 0; k--)
-      if (phases_[k].used) {
-        cudaEventSynchronize(phases_[k].b);
-        break;
-      }
-    for (Phase& ph : phases_) {
-      if (!ph.used) continue;
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, ph.a, ph.b);
-      ph.ms += ms;
-      ph.launches += ph.stepLaunches;
-      ph.voxels += (double)c->active * N_;
-      ph.used = false;
-    }
-    profilePending_ = false;
-  }
-  return FP_OK;
-}
-
-void Engine::phaseBegin(int id) {
-  if (profiling_) cudaEventRecord(phases_[id].a, stream_);
-}
-void Engine::phaseEnd(int id, int launches) {
-  launches_ += (uint64_t)launches;
-  if (!profiling_) return;
-  Phase& ph = phases_[id];
-  cudaEventRecord(ph.b, stream_);
-  ph.stepLaunches = (uint64_t)launches;
-  ph.used = true;
-  profilePending_ = true;
-}
-
-int Engine::setProfiling(bool on) {
-  int rc = consumeReadback();
-  if (rc) return rc;
-  for (Phase& ph : phases_) {
-    if (!ph.a && (rc = check(cudaEventCreate(&ph.a), "cudaEventCreate"))) return rc;
-    if (!ph.b && (rc = check(cudaEventCreate(&ph.b), "cudaEventCreate"))) return rc;
-    if (on) {
-      ph.launches = 0;
-      ph.ms = 0;
-      ph.voxels = 0;
-    }
-    ph.used = false;
-  }
-  profiling_ = on;
-  return FP_OK;
-}
-
-int Engine::readProfile(fp_phase* out, uint32_t* count) {
-  static const char* names[PH_COUNT] = {"allocation", "topology", "predict", "correct", "evolve", "curl",
-                                        "forces", "divergence", "multigrid", "project"};
-  int rc = consumeReadback();
-  if (rc) return rc;
-  uint32_t cap = *count;
-  *count = PH_COUNT;
-  if (!out || cap < PH_COUNT) return fail(FP_ELIMIT, "profile buffer too small");
-  for (int i = 0; i < PH_COUNT; i++) {
-    std::memset(&out[i], 0, sizeof(fp_phase));
-    std::strncpy(out[i].name, names[i], sizeof(out[i].name) - 1);
-    out[i].launches = phases_[i].launches;
-    out[i].ms = phases_[i].ms;
-    out[i].voxels = phases_[i].voxels;
-  }
-  return FP_OK;
-}
-
-// One V-cycle of PressureSolver.plan (PressureSolver.ts:276-365); `cur` holds each level's
-// current pressure buffer. The finest level's first iterate was written with the divergence.
-void Engine::vcycle(int level, int cur[]) {
-  SimParams* dP = dParams();
-  if (level == bottom_) {
-    if (capacity_ <= fp_bottom_capacity()) {
-      fp_launch_bottom(dP, level, 19, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]), capacity_, stream_);
-      launches_++;
-      cur[level] = 1 - cur[level];
-    } else {
-      for (int i = 0; i < 19; i++) {
-        fp_launch_relax(dP, level, true, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]), capacity_, sms_,
-                        stream_);
-        launches_++;
-        cur[level] = 1 - cur[level];
-      }
-    }
-    return;
-  }
-  if (level > 0)
-    for (int i = 0; i < 2; i++) {
-      fp_launch_relax(dP, level, level >= brickLevels_, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]),
-                      capacity_, sms_, stream_);
-      launches_++;
-      cur[level] = 1 - cur[level];
-    }
-  int coarse = level + 1;
-  fp_launch_restrict(dP, level, coarse >= brickLevels_, RHS(level), LP(level, cur[level]), RHS(coarse), LP(coarse, 1),
-                     capacity_, sms_, stream_);
-  launches_++;
-  cur[coarse] = 1;
-  vcycle(coarse, cur);
-  fp_launch_prolong(dP, level, level >= brickLevels_, LP(level, cur[level]), LP(coarse, cur[coarse]),
-                    LP(level, 1 - cur[level]), capacity_, sms_, stream_);
-  launches_++;
-  cur[level] = 1 - cur[level];
-  for (int i = 0; i < 3; i++) {
-    fp_launch_relax(dP, level, level >= brickLevels_, RHS(level), LP(level, cur[level]), LP(level, 1 - cur[level]),
-                    capacity_, sms_, stream_);
-    launches_++;
-    cur[level] = 1 - cur[level];
-  }
-}
-
-// The step's kernels, readback and measurement event, enqueued on the stream (eagerly, or
-// under capture into a graph). `latest` is the pressure buffer in, then out; `launches` the
-// kernels enqueued.
-void Engine::enqueueKernels(bool solids, bool topoAll, bool curl, int& latest, uint64_t& launches) {
-  SimParams* dP = dParams();
-  uint64_t first = launches_;
-  phaseBegin(PH_ALLOC);
-  fp_launch_allocation(dP, capacity_, solids, sms_, stream_);
-  phaseEnd(PH_ALLOC, 7 + (solids ? 1 : 0));
-  // Topology of the slots granted this step, or of everything after the geometry changed.
-  phaseBegin(PH_TOPO);
-  fp_launch_topology(dP, brickLevels_, bottom_, topoAll, capacity_, sms_, stream_);
-  phaseEnd(PH_TOPO, topoAll ? 2 : 1);
-  phaseBegin(PH_PREDICT);
-  fp_launch_predict(dP, B_, sms_, stream_);
-  phaseEnd(PH_PREDICT, 1);
-  phaseBegin(PH_CORRECT);
-  fp_launch_correct(dP, B_, sms_, stream_);
-  phaseEnd(PH_CORRECT, 1);
-  phaseBegin(PH_EVOLVE);
-  fp_launch_evolve(dP, B_, sms_, stream_);
-  phaseEnd(PH_EVOLVE, 1);
-
-  // Measurement: counters and the tiles' content flags are final once evolution ran, so they
-  // are read back here; the next step waits for this copy only and prepares while the GPU
-  // runs the rest of this step. Failed allocations count from one measurement to the next.
-  cudaMemcpyAsync(readH_, counters_.ptr, sizeof(FpCounters), cudaMemcpyDeviceToHost, stream_);
-  cudaMemcpyAsync(readH_ + sizeof(FpCounters) / 4, (uint32_t*)activity_.ptr + (size_t)capacity_ * 64,
-                  (size_t)capacity_ * 4, cudaMemcpyDeviceToHost, stream_);
-  cudaMemsetAsync(&((FpCounters*)counters_.ptr)->failures, 0, 4, stream_);
-  // Under capture, external: an event-record node the graph replays.
-  if (profiling_)
-    cudaEventRecord(readEvent_, stream_);
-  else
-    cudaEventRecordWithFlags(readEvent_, stream_, cudaEventRecordExternal);
-
-  if (curl) {
-    phaseBegin(PH_CURL);
-    fp_launch_curl(dP, sms_, stream_);
-    phaseEnd(PH_CURL, 1);
-  }
-  phaseBegin(PH_FORCES);
-  fp_launch_forces(dP, B_, sms_, stream_);
-  phaseEnd(PH_FORCES, 1);
-  int cur[FP_MAX_LEVELS] = {0};
-  cur[0] = latest;
-  phaseBegin(PH_DIVERGENCE);
-  fp_launch_divergence(dP, P0(1 - cur[0]), sms_, stream_);
-  phaseEnd(PH_DIVERGENCE, 1);
-  cur[0] = 1 - cur[0];
-  phaseBegin(PH_MULTIGRID);
-  uint64_t before = launches_;
-  vcycle(0, cur);
-  int mg = (int)(launches_ - before);
-  launches_ = before;
-  phaseEnd(PH_MULTIGRID, mg);
-  latest = cur[0];
-  phaseBegin(PH_PROJECT);
-  fp_launch_project(dP, P0(latest), sms_, stream_);
-  phaseEnd(PH_PROJECT, 1);
-  launches = launches_ - first;
-}
-
-void Engine::clearGraphs() {
-  for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second.exec);
-  graphs_.clear();
-}
-
-// FluidSimulation.step / substep (FluidSimulation.ts:1367-1531).
-int Engine::step(const fp_frame& f, float dt) {
-  auto t0 = std::chrono::steady_clock::now();
-  double wait0 = hostWaitMs_;
-  int rc = stepBody(f, dt);
-  double all = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  hostPrepareMs_ += all - (hostWaitMs_ - wait0);
-  return rc;
-}
-
-int Engine::stepBody(const fp_frame& f, float dt) {
-  if (!std::isfinite(dt) || dt <= 0 || dt > 1.f / 30.f)
-    return fail(FP_EINVAL, "Simulation step must be in (0, 1/30]. Use fixed substeps.");
-  int rc = packFlame(f.combustion, dt);
-  if (rc) return rc;
-  for (uint32_t i = 0; i < f.collider_count; i++) {
-    const fp_collider& c = f.colliders[i];
-    if (c.shape == FP_SHAPE_MESH) {
-      uint64_t bits = (uint64_t)std::max(0, c.dims[0]) * std::max(0, c.dims[1]) * std::max(0, c.dims[2]);
-      if ((uint64_t)c.mask_offset + (bits + 31) / 32 > f.collider_mask_words)
-        return fail(FP_EINVAL, "Mesh collider occupancy does not match its size.");
-    }
-  }
-  if ((rc = check(cudaSetDevice(device_), "cudaSetDevice"))) return rc;
-  if ((rc = consumeReadback())) return rc;
-  if (dir_.ground != ground_) {
-    dir_.ground = ground_;
-    geometryDirty_ = true;
-  }
-  uint32_t limit = slotLimit();
-  if (limit > slots_ && (rc = growPool(limit))) return rc;
-  updateTiles(f);
-  if (dir_.dirty && (rc = applyTiles())) return rc;
-  if (packScene(f)) {
-    solidsStale_ = true;
-    geometryDirty_ = true;
-  }
-  mayHaveFlame_ = mayHaveFlame_ || f.fuel.enabled;
-  for (uint32_t i = 0; i < f.source_count; i++) mayHaveFlame_ = mayHaveFlame_ || f.sources[i].flame > 0;
-  if ((rc = uploadScene())) return rc;
-  fillParams(f, dt);
-  SimParams* dP = dParams();
-  cudaMemcpyAsync(dP, paramsH_, sizeof(SimParams), cudaMemcpyHostToDevice, stream_);
-  h2d_ += sizeof(SimParams);
-
-  bool solids = colliderCount_ > 0 || solidsStale_;
-  bool topoAll = geometryDirty_;
-  bool curl = f.simulation.vorticity != 0.f;
-  // The measurement buffer (a graph captures its address).
-  size_t words = sizeof(FpCounters) / 4 + capacity_;
-  if (words > readWords_) {
-    cudaStreamSynchronize(stream_);
-    clearGraphs();
-    if (readH_) cudaFreeHost(readH_);
-    readWords_ = words * 2;
-    if ((rc = check(cudaMallocHost(&readH_, readWords_ * 4), "cudaMallocHost"))) return rc;
-  }
-  if (profiling_) {
-    // Eager launches with an event pair around each phase.
-    uint64_t n = 0;
-    int latest = latest_;
-    enqueueKernels(solids, topoAll, curl, latest, n);
-    latest_ = latest;
-  } else {
-    // The step's launches as one CUDA graph, captured once per shape and replayed.
-    uint64_t key = (uint64_t)capacity_ | ((uint64_t)solids << 32) | ((uint64_t)topoAll << 33) |
-                   ((uint64_t)curl << 34) | ((uint64_t)latest_ << 35);
-    auto it = graphs_.find(key);
-    if (it == graphs_.end()) {
-      GraphEntry e{};
-      uint64_t saved = launches_;
-      int latest = latest_;
-      if ((rc = check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture")))
-        return rc;
-      enqueueKernels(solids, topoAll, curl, latest, e.launches);
-      cudaGraph_t g = nullptr;
-      rc = check(cudaStreamEndCapture(stream_, &g), "cudaStreamEndCapture");
-      launches_ = saved;
-      if (rc) return rc;
-      rc = check(cudaGraphInstantiate(&e.exec, g, 0), "cudaGraphInstantiate");
-      cudaGraphDestroy(g);
-      if (rc) return rc;
-      e.latest = latest;
-      it = graphs_.emplace(key, e).first;
-    }
-    if ((rc = check(cudaGraphLaunch(it->second.exec, stream_), "cudaGraphLaunch"))) return rc;
-    latest_ = it->second.latest;
-    launches_ += it->second.launches;
-  }
-  solidsStale_ = false;
-  geometryDirty_ = false;
-  pendingRead_ = true;
-  d2h_ += sizeof(FpCounters) + (size_t)capacity_ * 4;
-  std::swap(velIdx_[0], velIdx_[1]);
-  std::swap(fldIdx_[0], fldIdx_[2]);
-  stepH2d_ = h2d_;
-  stepD2h_ = d2h_;
-  h2d_ = d2h_ = 0;
-  stageUsed_ = 0;
-  time_ += dt;
-  steps_++;
-  return check(cudaGetLastError(), "step launch");
 }
 
 int Engine::reset() {
-  if (stream_) cudaStreamSynchronize(stream_);
+  int rc = consume();
+  if (rc) return rc;
+  owner_->forget(this);
+  cudaStreamSynchronize(stream());
   return initialize();
 }
 
@@ -1030,10 +807,21 @@ int Engine::setRuntime(float cutoff, double budget, int ground) {
   return FP_OK;
 }
 
-int Engine::synchronize() { return check(cudaStreamSynchronize(stream_), "synchronize"); }
+uint64_t Engine::memoryBytes() const {
+  uint64_t bytes = 0;
+  const DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_,
+                               &zeroList_, &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_,
+                               &donors_, &solids_, &tileRecD_, &tileNbrD_, &hashD_};
+  for (const DeviceBuffer* b : all) bytes += b->bytes;
+  for (auto& b : vel_) bytes += b.bytes;
+  for (auto& b : fld_) bytes += b.bytes;
+  for (auto& b : p0_) bytes += b.bytes;
+  for (int l = 0; l < FP_MAX_LEVELS; l++) bytes += topo_[l].bytes + lrhs_[l].bytes + lp_[l][0].bytes + lp_[l][1].bytes;
+  return bytes;
+}
 
 int Engine::stats(fp_stats* out) {
-  int rc = consumeReadback();
+  int rc = consume();
   if (rc) return rc;
   std::memset(out, 0, sizeof(*out));
   out->time = time_;
@@ -1046,24 +834,14 @@ int Engine::stats(fp_stats* out) {
   out->tiles = (uint32_t)dir_.count();
   out->tile_capacity = (uint32_t)capacity_;
   out->failures = lastFailures_;
-  uint64_t bytes = 0;
-  DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_, &zeroList_,
-                         &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_, &donors_, &solids_,
-                         &tileRecD_, &tileNbrD_, &hashD_, &emittersD_, &collidersD_, &masksD_, &forcesD_,
-                         &regionsD_, &tileListsD_, &noise_, &paramsD_};
-  for (DeviceBuffer* b : all) bytes += b->bytes;
-  for (auto& b : vel_) bytes += b.bytes;
-  for (auto& b : fld_) bytes += b.bytes;
-  for (auto& b : p0_) bytes += b.bytes;
-  for (int l = 0; l < FP_MAX_LEVELS; l++) bytes += topo_[l].bytes + lrhs_[l].bytes + lp_[l][0].bytes + lp_[l][1].bytes;
-  out->memory_bytes = bytes;
+  out->memory_bytes = memoryBytes();
   out->last_vcycles = steps_ > 0 ? 1 : 0;
   out->last_residual = -1;
-  out->kernel_launches = launches_;
+  out->kernel_launches = owner_->launches();
   out->h2d_bytes = stepH2d_;
   out->d2h_bytes = stepD2h_;
-  out->host_prepare_ms = hostPrepareMs_;
-  out->host_wait_ms = hostWaitMs_;
+  out->host_prepare_ms = owner_->hostPrepareMs();
+  out->host_wait_ms = owner_->hostWaitMs();
   return FP_OK;
 }
 
@@ -1081,15 +859,16 @@ int Engine::readField(int field, float* host, size_t bytes) {
   }
   size_t need = (size_t)slots_ * ch * N_ * 4;
   if (bytes != need) return fail(FP_EINVAL, "field buffer size mismatch: need " + std::to_string(need) + " bytes");
-  int rc = check(cudaStreamSynchronize(stream_), "read field");
+  int rc = consume();
   if (rc) return rc;
+  if ((rc = check(cudaStreamSynchronize(stream()), "read field"))) return rc;
   return check(cudaMemcpy(host, b->ptr, need, cudaMemcpyDeviceToHost), "read field");
 }
 
 int Engine::readTable(int table, void* host, size_t* bytes) {
-  int rc = consumeReadback();
+  int rc = consume();
   if (rc) return rc;
-  if ((rc = check(cudaStreamSynchronize(stream_), "read table"))) return rc;
+  if ((rc = check(cudaStreamSynchronize(stream()), "read table"))) return rc;
   size_t bricks = (size_t)capacity_ * 64;
   std::vector<uint32_t> w;
   auto fetch = [&](const DeviceBuffer& b, size_t words, size_t offsetWords = 0) {
@@ -1142,8 +921,9 @@ int Engine::readTable(int table, void* host, size_t* bytes) {
 
 // readBricks (FluidSimulation.ts:1749-1779): world boxes of the bricks holding a slot.
 int Engine::readBricks(float* boxes, uint32_t* count) {
-  int rc = check(cudaStreamSynchronize(stream_), "read bricks");
+  int rc = consume();
   if (rc) return rc;
+  if ((rc = check(cudaStreamSynchronize(stream()), "read bricks"))) return rc;
   size_t bricks = (size_t)capacity_ * 64;
   std::vector<int> pages(bricks);
   cudaMemcpy(pages.data(), pages_.ptr, bricks * 4, cudaMemcpyDeviceToHost);

@@ -1,7 +1,14 @@
-// Host engine of one simulation: the C++ counterpart of the reference's `FluidSimulation`
+// Host side of the step.
+//
+// `Engine` is one simulation: the C++ counterpart of the reference's `FluidSimulation`
 // (src/engine/FluidSimulation.ts) and `TileDirectory` (src/engine/TileDirectory.ts). It owns
-// every device buffer, keeps the tile directory, packs each step's scene and enqueues the
-// step's kernels on the simulation's stream.
+// the simulation's device pools and tables, keeps the tile directory and packs each step's
+// scene on the host.
+//
+// `Stepper` launches steps. One step of any number of simulations (all with the same brick
+// size) is one host-to-device copy of their parameters and scenes, then one CUDA graph whose
+// kernels each cover every simulation's bricks (fp_launch.h). A single simulation is a batch
+// of one; the batch and serving front ends step many at once.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -52,33 +59,55 @@ struct DeviceBuffer {
   size_t bytes = 0;
 };
 
+class Stepper;
+
 class Engine {
  public:
-  Engine(const fp_grid& grid, int device);
+  Engine(const fp_grid& grid, Stepper* owner);
   ~Engine();
 
+  // Device pools of the whole voxel budget and an empty directory (FluidSimulation.ts:496-549).
   int initialize();
-  int step(const fp_frame& frame, float dt);
-  int stepBody(const fp_frame& frame, float dt);
   int reset();
   int setRuntime(float cutoff, double budget, int ground);
-  int synchronize();
   int stats(fp_stats* out);
   int readField(int field, float* host, size_t bytes);
   int readTable(int table, void* host, size_t* bytes);
   int readBricks(float* boxes, uint32_t* count);
-  int setProfiling(bool on);
-  int readProfile(fp_phase* out, uint32_t* count);
-  cudaStream_t stream() const { return stream_; }
   const std::string& error() const { return error_; }
   int fail(int code, const std::string& message) {
     error_ = message;
     return code;
   }
+  int brickSize() const { return B_; }
+  // Device bytes a simulation of this grid holds once its pools exist (for admission).
+  static uint64_t estimateBytes(const fp_grid& grid);
+  uint64_t memoryBytes() const;
+
+  // ---- the Stepper's side of a step
+  // Checks the frame and dt without changing any state (FluidSimulation.ts:1367-1369,
+  // flame.ts:43-87).
+  int validate(const fp_frame& frame, float dt);
+  // Host work before the launch: pool growth, tiles, scene packing.
+  int prepare(const fp_frame& frame, float dt);
+  // Bytes the packed scene takes in the launch's upload, 256-byte aligned blobs.
+  size_t sceneBytes() const;
+  // Copy the packed scene into the upload at `off` and fill the step's SimParams.
+  void writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t off, const fp_frame& frame, float dt,
+                 uint32_t* readback, const float4* noise);
+  bool buildSolids() const { return colliderCount_ > 0 || solidsStale_; }
+  bool solidsAll() const { return solidsStale_; }
+  bool topoAll() const { return geometryDirty_; }
+  int capacity() const { return capacity_; }
+  size_t readbackWords() const { return sizeof(FpCounters) / 4 + (size_t)capacity_; }
+  // After the launch: buffers rotate, time advances; the measurement is pending.
+  void launched(float dt, int latest);
+  // The measurement this simulation's last launch wrote (readActivity, FluidSimulation.ts:1701-1746).
+  void applyReadback(const uint32_t* words);
 
  private:
+  Stepper* owner_;
   // configuration
-  int device_;
   int B_, shift_, N_, W_, brickLevels_, bottom_;
   float h_;
   bool maccormack_;
@@ -86,8 +115,6 @@ class Engine {
   double budget_;
   float cutoff_ = 0.f;
   bool ground_ = true;
-  int sms_ = 148;
-  cudaStream_t stream_ = nullptr;
   std::string error_;
 
   // host state
@@ -109,30 +136,103 @@ class Engine {
   bool poolLimited_ = false;
   int latest_ = 0;  // index of the latest pressure solution
   uint32_t slots_ = 0;
-  bool pendingRead_ = false;
-  int64_t readStep_ = -1;
+  uint64_t stepH2d_ = 0, stepD2h_ = 0;
 
   // device memory
-  std::vector<DeviceBuffer*> owned_;
   DeviceBuffer pages_, entries_, state_, activity_, records_, blockCounts_, active_, zeroList_;
   DeviceBuffer freeStack_, counters_;
   DeviceBuffer vel_[4], curl_, fld_[3], expn_, div_, vmin_, vmax_, sb_, donors_, solids_;
   DeviceBuffer p0_[2], topo_[FP_MAX_LEVELS], lp_[FP_MAX_LEVELS][2], lrhs_[FP_MAX_LEVELS];
   DeviceBuffer tileRecD_, tileNbrD_, hashD_;
-  DeviceBuffer emittersD_, collidersD_, masksD_, forcesD_, regionsD_, tileListsD_;
-  DeviceBuffer noise_, paramsD_;
   int velIdx_[4] = {0, 1, 2, 3};  // start, predictor/projected, corrected, forced
   int fldIdx_[3] = {0, 1, 2};     // start, predictor, evolved
 
-  // pinned host staging
-  SimParams* paramsH_ = nullptr;
-  uint8_t* stageH_ = nullptr;  // pinned arena of the step's host-to-device copies
+  // pinned staging of the directory tables' copies
+  uint8_t* stageH_ = nullptr;
   size_t stageCap_ = 0, stageUsed_ = 0;
-  uint32_t* readH_ = nullptr;
-  size_t readWords_ = 0;
-  cudaEvent_t readEvent_ = nullptr;
+  uint64_t h2d_ = 0;
 
-  // per-phase device timing (GpuProfiler.ts), and the launch count
+  // per-step scene (host)
+  std::vector<FpEmitter> emitters_;
+  std::vector<FpCollider> colliders_;
+  std::vector<uint32_t> masks_;
+  std::vector<FpForce> forces_;
+  std::vector<FpRegion> regions_;
+  std::vector<uint32_t> tileLists_;
+  FpFlame flame_;
+
+  cudaStream_t stream() const;
+  bool alloc(DeviceBuffer& b, size_t bytes, bool zero = true);
+  bool grow(DeviceBuffer& b, size_t bytes, int fill);  // keeps contents
+  bool upload(DeviceBuffer& b, const void* src, size_t bytes);
+  void freeAll();
+  int check(cudaError_t e, const char* what);
+  int consume();
+  uint32_t slotLimit() const;
+  int levelShift(int level) const { return level < brickLevels_ ? brickLevels_ - level : brickLevels_ + 2 - level; }
+  int levelCells(int level) const { int s = levelShift(level); return 1 << (3 * s); }
+
+  int allocatePools(uint32_t slots);
+  int growPool(uint32_t target);
+  int setCapacity(int capacity);
+  int applyTiles();
+  void updateTiles(const fp_frame& f);
+  int packFlame(const fp_combustion& c, float dt, FpFlame& out);
+  bool packScene(const fp_frame& f);
+  void bin(int kind, int index, const double* lo, const double* hi, std::vector<std::vector<uint32_t>>& lists);
+};
+
+class Stepper {
+ public:
+  Stepper(int device, int brickSize);
+  ~Stepper();
+  int initialize();
+  cudaStream_t stream() const { return stream_; }
+  int device() const { return device_; }
+  int brickSize() const { return B_; }
+  const std::string& error() const { return error_; }
+
+  // One step of `count` simulations in one launch. Every frame and dt is checked before any
+  // simulation changes; a failure names the simulation's position.
+  int step(Engine* const* sims, const fp_frame* const* frames, const float* dts, int count);
+  // Wait for the last launch's measurement and hand it to its simulations.
+  int consume();
+  // A simulation leaves: its pending measurement is dropped.
+  void forget(const Engine* e);
+  int synchronize();
+  int setProfiling(bool on);
+  int readProfile(fp_phase* out, uint32_t* count);
+  uint64_t launches() const { return launches_; }
+  double hostPrepareMs() const { return hostPrepareMs_; }
+  double hostWaitMs() const { return hostWaitMs_; }
+  uint64_t lastUploadBytes() const { return lastUpload_; }
+  uint64_t lastReadbackBytes() const { return lastReadback_; }
+  const float4* noise() const { return (const float4*)noise_; }
+
+ private:
+  int device_, B_, brickLevels_, bottom_;
+  int sms_ = 148;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t readEvent_ = nullptr;
+  std::string error_;
+  void* noise_ = nullptr;
+
+  // The launch's upload: work rows, then SimParams per simulation, then the scenes.
+  uint8_t* arenaH_ = nullptr;
+  uint8_t* arenaD_ = nullptr;
+  size_t arenaCap_ = 0;
+  int maxSims_ = 0;  // simulations the work rows and parameters have room for
+  // Host-mapped measurement words of every simulation of the launch.
+  uint32_t* readH_ = nullptr;
+  uint32_t* readD_ = nullptr;  // its device alias
+  size_t readCap_ = 0;
+  std::vector<std::pair<Engine*, size_t>> pending_;  // simulation, word offset
+  bool pendingRead_ = false;
+
+  uint64_t launches_ = 0, lastUpload_ = 0, lastReadback_ = 0;
+  double hostPrepareMs_ = 0, hostWaitMs_ = 0;
+
+  // per-phase device timing (GpuProfiler.ts)
   enum PhaseId { PH_ALLOC, PH_TOPO, PH_PREDICT, PH_CORRECT, PH_EVOLVE, PH_CURL, PH_FORCES, PH_DIVERGENCE,
                  PH_MULTIGRID, PH_PROJECT, PH_COUNT };
   struct Phase {
@@ -144,58 +244,22 @@ class Engine {
   Phase phases_[PH_COUNT];
   bool profiling_ = false;
   bool profilePending_ = false;
-  uint64_t launches_ = 0;
-  uint64_t h2d_ = 0, d2h_ = 0, stepH2d_ = 0, stepD2h_ = 0;
-  double hostPrepareMs_ = 0, hostWaitMs_ = 0;
   void phaseBegin(int id);
   void phaseEnd(int id, int launches);
 
-  // The step's launch sequence as CUDA graphs, one per shape (capacity, solids, topology
-  // rebuild, curl, pressure buffer parity). Kernel arguments hold buffer addresses, so any
-  // reallocation clears the cache.
+  // The step's launch sequence as CUDA graphs, one per combination of the optional launches.
   struct GraphEntry {
     cudaGraphExec_t exec;
     int latest;
     uint64_t launches;
   };
   std::unordered_map<uint64_t, GraphEntry> graphs_;
-  void enqueueKernels(bool solids, bool topoAll, bool curl, int& latest, uint64_t& launches);
   void clearGraphs();
-
-  // per-step scene (host)
-  std::vector<FpEmitter> emitters_;
-  std::vector<FpCollider> colliders_;
-  std::vector<uint32_t> masks_;
-  std::vector<FpForce> forces_;
-  std::vector<FpRegion> regions_;
-  std::vector<uint32_t> tileLists_;
-  FpFlame flame_;
-
-  bool alloc(DeviceBuffer& b, size_t bytes, bool zero = true);
-  bool grow(DeviceBuffer& b, size_t bytes, int fill);  // keeps contents
-  bool upload(DeviceBuffer& b, const void* src, size_t bytes);
-  void freeAll();
+  FpBatch batch() const;
+  void enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl, int& latest, uint64_t& launches);
+  void vcycle(int level, int cur[], uint64_t& launches);
   int check(cudaError_t e, const char* what);
-  uint32_t slotLimit() const;
-  int levelShift(int level) const { return level < brickLevels_ ? brickLevels_ - level : brickLevels_ + 2 - level; }
-  int levelCells(int level) const { int s = levelShift(level); return 1 << (3 * s); }
-
-  int allocatePools(uint32_t slots);
-  int growPool(uint32_t target);
-  int setCapacity(int capacity);
-  int applyTiles();
-  void updateTiles(const fp_frame& f);
-  int packFlame(const fp_combustion& c, float dt);
-  bool packScene(const fp_frame& f);
-  void bin(int kind, int index, const double* lo, const double* hi, std::vector<std::vector<uint32_t>>& lists);
-  int uploadScene();
-  void fillParams(const fp_frame& f, float dt);
-  int consumeReadback();
-  void vcycle(int level, int cur[]);
-  float* P0(int k) { return (float*)p0_[k].ptr; }
-  float* LP(int level, int k) { return level == 0 ? P0(k) : (float*)lp_[level][k].ptr; }
-  float* RHS(int level) { return level == 0 ? (float*)div_.ptr : (float*)lrhs_[level].ptr; }
-  SimParams* dParams() { return (SimParams*)paramsD_.ptr; }
+  int reserve(size_t arenaBytes, int sims, size_t readWords);
 };
 
 }  // namespace fp

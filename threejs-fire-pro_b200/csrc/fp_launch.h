@@ -1,34 +1,40 @@
-// Launchers of the step's kernels. Every launcher takes the device copy of the simulation's
-// SimParams and enqueues on `st`; none synchronises.
+// Launchers of the step's kernels. Every launcher covers all simulations of a batch
+// (FpBatch: the device array of their SimParams and the work-list offsets) in one launch of a
+// fixed grid, enqueues on `st` and does not synchronise. Fixed grids and per-simulation
+// buffers read from SimParams keep a captured CUDA graph valid while the simulations grow.
 #pragma once
 #include <cuda_runtime.h>
 
 #include "fp_types.h"
 
-void fp_launch_allocation(const SimParams* dP, int capacity, bool solids, int sms, cudaStream_t st);
-void fp_launch_predict(const SimParams* dP, int B, int sms, cudaStream_t st);
-void fp_launch_correct(const SimParams* dP, int B, int sms, cudaStream_t st);
-void fp_launch_evolve(const SimParams* dP, int B, int sms, cudaStream_t st);
-void fp_launch_curl(const SimParams* dP, int sms, cudaStream_t st);
-void fp_launch_forces(const SimParams* dP, int B, int sms, cudaStream_t st);
-void fp_launch_divergence(const SimParams* dP, float* pOut, int sms, cudaStream_t st);
-void fp_launch_project(const SimParams* dP, const float* p, int sms, cudaStream_t st);
+void fp_launch_allocation(const FpBatch& bt, bool solidsFresh, bool solidsAll, int sms, cudaStream_t st);
+int fp_allocation_launches(bool solidsFresh, bool solidsAll);
+// The measurement of every simulation into its host-mapped readback words.
+void fp_launch_readback(const FpBatch& bt, int sms, cudaStream_t st);
+void fp_launch_predict(const FpBatch& bt, int B, int sms, cudaStream_t st);
+void fp_launch_correct(const FpBatch& bt, int B, int sms, cudaStream_t st);
+void fp_launch_evolve(const FpBatch& bt, int B, int sms, cudaStream_t st);
+void fp_launch_curl(const FpBatch& bt, int sms, cudaStream_t st);
+void fp_launch_forces(const FpBatch& bt, int B, int sms, cudaStream_t st);
+// Divergence with the finest level's first iterate into p0[pSel]; projection with p0[pSel].
+void fp_launch_divergence(const FpBatch& bt, int pSel, int sms, cudaStream_t st);
+void fp_launch_project(const FpBatch& bt, int pSel, int sms, cudaStream_t st);
 void fp_launch_noise(float4* noise, cudaStream_t st);
 
-// Multigrid (pressure.wgsl). Levels below `brickLevels` live in brick slots, the rest in
-// tile slots.
-void fp_launch_topology(const SimParams* dP, int brickLevels, int bottom, bool all, int capacity, int sms,
-                        cudaStream_t st);
-void fp_launch_relax(const SimParams* dP, int level, bool tiles, const float* rhs, const float* pin, float* pout,
-                     int capacity, int sms, cudaStream_t st);
-void fp_launch_restrict(const SimParams* dP, int fine, bool tiles, const float* rhs, const float* p, float* crhs,
-                        float* cfirst, int capacity, int sms, cudaStream_t st);
-void fp_launch_prolong(const SimParams* dP, int level, bool tiles, const float* pin, const float* coarse, float* pout,
-                       int capacity, int sms, cudaStream_t st);
-void fp_launch_bottom(const SimParams* dP, int level, int iterations, const float* rhs, const float* pin, float* pout,
-                      int capacity, cudaStream_t st);
-// Most tile slots the one-CTA bottom solve holds in shared memory.
-int fp_bottom_capacity();
+// Multigrid (pressure.wgsl). Levels below the brick levels live in brick slots, the rest in
+// tile slots. Buffers are named by selector, level * 4 + which: which 0 and 1 are the level's
+// pressure pair, 2 its right-hand side (the divergence at level 0); -1 names none.
+struct MgSel {
+  int level;  // output level
+  int rhs, pin, coarse, pout, cfirst;
+};
+inline int fp_mg_sel(int level, int which) { return level * 4 + which; }
+void fp_launch_topology(const FpBatch& bt, bool anyAll, int sms, cudaStream_t st);
+void fp_launch_relax(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st);
+void fp_launch_restrict(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st);
+void fp_launch_prolong(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st);
+// The bottom level's iterations, a CTA per simulation.
+void fp_launch_bottom(const FpBatch& bt, const MgSel& S, int iterations, int sms, cudaStream_t st);
 // Size the staged brick-level multigrid kernels for bricks of B cells (once per brick size).
 void fp_mg_configure(int B);
 // Set the step kernels' shared-memory limits (before any launch or stream capture).

@@ -112,6 +112,25 @@ struct Args {
   float* cfirst;
 };
 
+// A launch names its buffers by selector, level * 4 + which (0 and 1 the level's pressure
+// pair, 2 its right-hand side; -1 none), and each simulation of the batch resolves them.
+FP_DEV float* mgBuffer(const SimParams& P, int sel) {
+  if (sel < 0) return nullptr;
+  int level = sel >> 2, which = sel & 3;
+  if (which == 2) return level == 0 ? P.div : P.lrhs[level];
+  return level == 0 ? P.p0[which] : P.lp[level][which];
+}
+FP_DEV Args resolve(const SimParams& P, const MgSel& S) {
+  Args A;
+  A.level = S.level;
+  A.rhs = mgBuffer(P, S.rhs);
+  A.pin = mgBuffer(P, S.pin);
+  A.coarse = mgBuffer(P, S.coarse);
+  A.pout = mgBuffer(P, S.pout);
+  A.cfirst = mgBuffer(P, S.cfirst);
+  return A;
+}
+
 FP_DEV void relaxCell(const SimParams& P, const Home& H, const Args& A, long a, int px, int py, int pz) {
   uint32_t f = expandFlags(P.topo[A.level][a]);
   if ((f & SOLIDF) || !activeCell(P, H, px, py, pz, A.level)) {
@@ -181,24 +200,6 @@ FP_DEV void levelCell(const SimParams& P, const Home& H, const Args& A, long a, 
   if (OP == RESTRICT) restrictCell(P, H, A, a, px, py, pz);
 }
 
-// Every cell of `A.level` in every computing brick.
-template <int OP>
-__global__ void __launch_bounds__(256) k_level_bricks(const SimParams* __restrict__ Pp, Args A) {
-  const SimParams& P = *Pp;
-  __shared__ int nslot[27];
-  uint32_t total = P.counters->active;
-  int s = levelShift(P, A.level), side = 1 << s, cells = side * side * side;
-  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
-    Home H = enterBrick(P, P.active[i], nslot);
-    long base = (long)nslot[13] * cells;
-    for (int o = threadIdx.x; o < cells; o += blockDim.x) {
-      int lx = o & (side - 1), ly = (o >> s) & (side - 1), lz = o >> (2 * s);
-      levelCell<OP>(P, H, A, base + o, H.bx * side + lx, H.by * side + ly, H.bz * side + lz);
-    }
-    __syncthreads();
-  }
-}
-
 // Staged brick levels. A CTA copies, for its brick, the values of the level it reads plus a
 // one-cell rim into shared memory, and once per brick whether each negative-octant neighbour
 // brick computes; the cell operations then read no directory. Same arithmetic, same order as
@@ -207,24 +208,26 @@ __global__ void __launch_bounds__(256) k_level_bricks(const SimParams* __restric
 //   RESTRICT  stage A.pin at A.level - 1 (fine); write A.pout, A.cfirst at A.level (coarse)
 //   PROLONG   stage A.coarse at A.level + 1;    write A.pout at A.level
 template <int OP>
-__global__ void __launch_bounds__(256) k_level_bricks_staged(const SimParams* __restrict__ Pp, Args A) {
-  const SimParams& P = *Pp;
+__global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel Sl) {
   __shared__ int nslot[27];
   __shared__ int need[8];  // bit k of the index: -1 on axis k
   extern __shared__ float st[];
-  const int bl = P.brickLevels;
-  const int fineLevel = OP == RESTRICT ? A.level - 1 : A.level;
-  const int stageLevel = OP == PROLONG ? A.level + 1 : fineLevel;
-  const int sb = stageLevel < bl ? 1 << levelShift(P, stageLevel) : 1;  // stage-level cells per brick side
-  // Prolongation stages a two-cell rim and the coarse solid flags: its Neumann ghosts read the
-  // neighbours of the interpolation's coarse cells.
-  const int R = OP == PROLONG ? 2 : 1;
-  const int S = sb + 2 * R, S2 = S * S, S3 = S2 * S;
-  uint8_t* solidSt = reinterpret_cast<uint8_t*>(st + S3);
-  const float* src = OP == PROLONG ? A.coarse : A.pin;
-  const int fs = levelShift(P, fineLevel), fside = 1 << fs, fcells = fside * fside * fside;
-  uint32_t total = P.counters->active;
-  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
+    const Args A = resolve(P, Sl);
+    const int bl = P.brickLevels;
+    const int fineLevel = OP == RESTRICT ? A.level - 1 : A.level;
+    const int stageLevel = OP == PROLONG ? A.level + 1 : fineLevel;
+    const int sb = stageLevel < bl ? 1 << levelShift(P, stageLevel) : 1;  // stage-level cells per brick side
+    // Prolongation stages a two-cell rim and the coarse solid flags: its Neumann ghosts read the
+    // neighbours of the interpolation's coarse cells.
+    const int R = OP == PROLONG ? 2 : 1;
+    const int S = sb + 2 * R, S2 = S * S, S3 = S2 * S;
+    uint8_t* solidSt = reinterpret_cast<uint8_t*>(st + S3);
+    const float* src = OP == PROLONG ? A.coarse : A.pin;
+    const int fs = levelShift(P, fineLevel), fside = 1 << fs, fcells = fside * fside * fside;
     Home H = enterBrick(P, P.active[i], nslot);
     if (threadIdx.x < 8) {
       int dx = -(int)(threadIdx.x & 1), dy = -(int)((threadIdx.x >> 1) & 1), dz = -(int)(threadIdx.x >> 2);
@@ -358,10 +361,14 @@ FP_DEV Home enterTile(const SimParams& P, int t, int4 rec) {
 
 // Every cell of `A.level` (a tile level) in every tile.
 template <int OP>
-__global__ void __launch_bounds__(64) k_level_tiles(const SimParams* __restrict__ Pp, Args A) {
-  const SimParams& P = *Pp;
-  int s = levelShift(P, A.level), side = 1 << s, cells = side * side * side;
-  for (int t = blockIdx.x; t < P.capacity; t += gridDim.x) {
+__global__ void __launch_bounds__(64) k_level_tiles(FpBatch bt, MgSel Sl) {
+  uint32_t total = workTotal(bt, FP_WORK_TILES);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t local;
+    const SimParams& P = workSim(bt, FP_WORK_TILES, item, local);
+    const int t = (int)local;
+    const Args A = resolve(P, Sl);
+    int s = levelShift(P, A.level), side = 1 << s, cells = side * side * side;
     int4 rec = __ldg(&P.tileRec[t]);
     if (rec.w == 0) continue;
     Home H = enterTile(P, t, rec);
@@ -373,59 +380,69 @@ __global__ void __launch_bounds__(64) k_level_tiles(const SimParams* __restrict_
 }
 
 // relaxCoarse (pressure.wgsl:549-599): the bottom level, one cell per tile slot, every
-// iteration in one CTA. Tile slots stride over the threads; each slot's flags (SOLIDF where
-// it is no unknown) and a ping-pong pair of values live in shared memory, so any number of
-// tiles that fits 12 bytes a slot needs one launch.
-__global__ void __launch_bounds__(1024) k_bottom(const SimParams* __restrict__ Pp, int level, int iterations,
-                                                  const float* __restrict__ rhs, const float* __restrict__ pin,
-                                                  float* __restrict__ pout) {
-  const SimParams& P = *Pp;
+// iteration in one CTA; a CTA per simulation. Tile slots stride over the threads; each
+// slot's flags (SOLIDF where it is no unknown) and a ping-pong pair of values live in shared
+// memory when 12 bytes a slot fit `smemBytes`, else the values ping-pong between the level's
+// two pressure buffers in global memory (same arithmetic, same order).
+__global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int iterations, int smemBytes) {
   extern __shared__ float bottomSmem[];
-  int cap = P.capacity;
-  float* cur = bottomSmem;
-  float* nxt = bottomSmem + cap;
-  uint32_t* flags = reinterpret_cast<uint32_t*>(bottomSmem + 2 * cap);
-  for (int t = threadIdx.x; t < cap; t += blockDim.x) {
-    int4 rec = __ldg(&P.tileRec[t]);
-    uint32_t f = SOLIDF | (rec.w != 0 ? 0x80000000u : 0u);  // top bit: a live tile slot
-    float v = 0.f;
-    if (rec.w != 0) {
-      Home H = enterTile(P, t, rec);
-      if (activeCell(P, H, rec.x, rec.y, rec.z, level)) {
-        f = expandFlags(P.topo[level][t]) | 0x80000000u;
-        v = pin[t];
-      }
-    }
-    flags[t] = f;
-    cur[t] = v;
-  }
-  __syncthreads();
   const int nbIndex[6] = {nbrIndex(1, 0, 0), nbrIndex(-1, 0, 0), nbrIndex(0, 1, 0),
                           nbrIndex(0, -1, 0), nbrIndex(0, 0, 1), nbrIndex(0, 0, -1)};
-  for (int it = 0; it < iterations; it++) {
-    for (int t = threadIdx.x; t < cap; t += blockDim.x) {
-      uint32_t f = flags[t];
-      float next = 0.f;
-      if ((f & 0x80000000u) && !(f & SOLIDF)) {
-        float w[6];
-#pragma unroll
-        for (int k = 0; k < 6; k++) {
-          int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
-          w[k] = n >= 0 ? cur[n] : 0.f;
-        }
-        float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
-        float cand = (sum - rhs[t]) / fmaxf(diagOf(f & 63u), 1e-12f);
-        next = mixf(cur[t], cand, 0.8f);
+  int sims = batchCount(bt);
+  for (int sim = blockIdx.x; sim < sims; sim += gridDim.x) {
+    const SimParams& P = bt.sims[sim];
+    const Args A = resolve(P, Sl);
+    const int level = A.level;
+    int cap = P.capacity;
+    bool inShared = (long)cap * 12 <= (long)smemBytes;
+    // In global memory: cur starts in pout (a copy of pin), nxt is pin's buffer.
+    float* cur = inShared ? bottomSmem : A.pout;
+    float* nxt = inShared ? bottomSmem + cap : const_cast<float*>(A.pin);
+    uint32_t* flags = inShared ? reinterpret_cast<uint32_t*>(bottomSmem + 2 * cap) : nullptr;
+    auto flagOf = [&](int t) -> uint32_t {
+      int4 rec = __ldg(&P.tileRec[t]);
+      uint32_t f = SOLIDF | (rec.w != 0 ? 0x80000000u : 0u);  // top bit: a live tile slot
+      if (rec.w != 0) {
+        Home H = enterTile(P, t, rec);
+        if (activeCell(P, H, rec.x, rec.y, rec.z, level)) f = expandFlags(P.topo[level][t]) | 0x80000000u;
       }
-      nxt[t] = next;
+      return f;
+    };
+    for (int t = threadIdx.x; t < cap; t += blockDim.x) {
+      uint32_t f = flagOf(t);
+      // Cells that are no unknown are never read and become zero in the first iteration.
+      if (inShared) flags[t] = f;
+      cur[t] = (f & 0x80000000u) && !(f & SOLIDF) ? A.pin[t] : 0.f;
     }
     __syncthreads();
-    float* tmp = cur;
-    cur = nxt;
-    nxt = tmp;
+    for (int it = 0; it < iterations; it++) {
+      for (int t = threadIdx.x; t < cap; t += blockDim.x) {
+        uint32_t f = inShared ? flags[t] : flagOf(t);
+        float next = 0.f;
+        if ((f & 0x80000000u) && !(f & SOLIDF)) {
+          float w[6];
+#pragma unroll
+          for (int k = 0; k < 6; k++) {
+            int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
+            w[k] = n >= 0 ? cur[n] : 0.f;
+          }
+          float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
+          float cand = (sum - A.rhs[t]) / fmaxf(diagOf(f & 63u), 1e-12f);
+          next = mixf(cur[t], cand, 0.8f);
+        }
+        nxt[t] = next;
+      }
+      __syncthreads();
+      float* tmp = cur;
+      cur = nxt;
+      nxt = tmp;
+    }
+    for (int t = threadIdx.x; t < cap; t += blockDim.x) {
+      uint32_t f = inShared ? flags[t] : flagOf(t);
+      if ((f & 0x80000000u) && cur != A.pout) A.pout[t] = cur[t];
+    }
+    __syncthreads();
   }
-  for (int t = threadIdx.x; t < cap; t += blockDim.x)
-    if (flags[t] & 0x80000000u) pout[t] = cur[t];
 }
 
 // cellTopology (pressure.wgsl:208-222): solid, or the sides whose neighbours are not solid.
@@ -445,15 +462,20 @@ FP_DEV uint8_t cellTopology(const SimParams& P, const Home& H, int px, int py, i
   return flags;
 }
 
-// buildBrickTopology (pressure.wgsl:259-278): the brick levels of every slotted brick, or of
-// the slots granted this step.
-__global__ void __launch_bounds__(128) k_topo_bricks(const SimParams* __restrict__ Pp, int all) {
-  const SimParams& P = *Pp;
-  uint32_t total = all ? (uint32_t)P.capacity * 64u : P.counters->fresh;
-  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+// buildBrickTopology (pressure.wgsl:259-278): the brick levels of the slots granted this
+// step, or (ALL) of every slotted brick of the simulations whose geometry changed.
+template <bool ALL>
+__global__ void __launch_bounds__(128) k_topo_bricks(FpBatch bt) {
+  __shared__ int nslot[27];
+  const int kind = ALL ? FP_WORK_IDS : FP_WORK_FRESH;
+  uint32_t total = workTotal(bt, kind);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, kind, item, i);
+    if ((P.topoAll != 0) != ALL) continue;  // uniform across the CTA
     uint32_t id;
     int slot;
-    if (all) {
+    if (ALL) {
       id = i;
       if (__ldg(&P.tileRec[id >> 6]).w == 0) continue;
       slot = entryPage(P.entries[id]);
@@ -461,9 +483,8 @@ __global__ void __launch_bounds__(128) k_topo_bricks(const SimParams* __restrict
       id = P.zeroList[2 * i];
       slot = (int)P.zeroList[2 * i + 1];
     }
-    if (slot < 0) continue;  // uniform across the CTA
+    if (slot < 0) continue;
     // The brick's neighbour slots in shared memory: every solid test stays within them.
-    __shared__ int nslot[27];
     Home H = enterBrick(P, id, nslot);
     int bx = H.bx, by = H.by, bz = H.bz;
     for (int level = 0; level < P.brickLevels; level++) {
@@ -478,9 +499,13 @@ __global__ void __launch_bounds__(128) k_topo_bricks(const SimParams* __restrict
 }
 
 // buildTileTopology (pressure.wgsl:281-305): every tile's cells at the tile levels.
-__global__ void __launch_bounds__(64) k_topo_tiles(const SimParams* __restrict__ Pp) {
-  const SimParams& P = *Pp;
-  for (int t = blockIdx.x; t < P.capacity; t += gridDim.x) {
+__global__ void __launch_bounds__(64) k_topo_tiles(FpBatch bt) {
+  uint32_t total = workTotal(bt, FP_WORK_TILES);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t local;
+    const SimParams& P = workSim(bt, FP_WORK_TILES, item, local);
+    if (!P.topoAll) continue;
+    int t = (int)local;
     int4 rec = __ldg(&P.tileRec[t]);
     if (rec.w == 0) continue;
     Home H = enterTile(P, t, rec);
@@ -497,18 +522,17 @@ __global__ void __launch_bounds__(64) k_topo_tiles(const SimParams* __restrict__
 
 }  // namespace
 
-void fp_launch_topology(const SimParams* dP, int brickLevels, int bottom, bool all, int capacity, int sms,
-                        cudaStream_t st) {
-  (void)brickLevels;
-  (void)bottom;
-  k_topo_bricks<<<sms * 4, 128, 0, st>>>(dP, all ? 1 : 0);
-  if (all) k_topo_tiles<<<capacity < sms * 8 ? capacity : sms * 8, 64, 0, st>>>(dP);
+void fp_launch_topology(const FpBatch& bt, bool anyAll, int sms, cudaStream_t st) {
+  k_topo_bricks<false><<<sms * 4, 128, 0, st>>>(bt);
+  if (anyAll) {
+    k_topo_bricks<true><<<sms * 4, 128, 0, st>>>(bt);
+    k_topo_tiles<<<sms * 8, 64, 0, st>>>(bt);
+  }
 }
-
-static int tileGrid(int capacity, int sms) { return capacity < sms * 8 ? capacity : sms * 8; }
 
 // Shared memory of the staged brick-level kernels: the largest brick size configured so far.
 static size_t g_stageBytes = 0;
+static const int BOTTOM_SMEM = 200 * 1024;
 void fp_mg_configure(int B) {
   size_t relax = (size_t)(B + 2) * (B + 2) * (B + 2) * sizeof(float);
   size_t prolong = (size_t)(B / 2 + 4) * (B / 2 + 4) * (B / 2 + 4) * (sizeof(float) + 1);
@@ -518,40 +542,25 @@ void fp_mg_configure(int B) {
   cudaFuncSetAttribute(k_level_bricks_staged<RELAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   cudaFuncSetAttribute(k_level_bricks_staged<RESTRICT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   cudaFuncSetAttribute(k_level_bricks_staged<PROLONG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, BOTTOM_SMEM);
 }
 
-void fp_launch_relax(const SimParams* dP, int level, bool tiles, const float* rhs, const float* pin, float* pout,
-                     int capacity, int sms, cudaStream_t st) {
-  Args A{level, rhs, pin, nullptr, pout, nullptr};
+template <int OP>
+static void levelLaunch(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st) {
   if (tiles)
-    k_level_tiles<RELAX><<<tileGrid(capacity, sms), 64, 0, st>>>(dP, A);
+    k_level_tiles<OP><<<sms * 8, 64, 0, st>>>(bt, S);
   else
-    k_level_bricks_staged<RELAX><<<sms * 4, 256, g_stageBytes, st>>>(dP, A);
+    k_level_bricks_staged<OP><<<sms * 4, 256, g_stageBytes, st>>>(bt, S);
 }
-
-void fp_launch_restrict(const SimParams* dP, int fine, bool tiles, const float* rhs, const float* p, float* crhs,
-                        float* cfirst, int capacity, int sms, cudaStream_t st) {
-  Args A{fine + 1, rhs, p, nullptr, crhs, cfirst};
-  if (tiles)
-    k_level_tiles<RESTRICT><<<tileGrid(capacity, sms), 64, 0, st>>>(dP, A);
-  else
-    k_level_bricks_staged<RESTRICT><<<sms * 4, 256, g_stageBytes, st>>>(dP, A);
+void fp_launch_relax(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st) {
+  levelLaunch<RELAX>(bt, S, tiles, sms, st);
 }
-
-void fp_launch_prolong(const SimParams* dP, int level, bool tiles, const float* pin, const float* coarse, float* pout,
-                       int capacity, int sms, cudaStream_t st) {
-  Args A{level, nullptr, pin, coarse, pout, nullptr};
-  if (tiles)
-    k_level_tiles<PROLONG><<<tileGrid(capacity, sms), 64, 0, st>>>(dP, A);
-  else
-    k_level_bricks_staged<PROLONG><<<sms * 4, 256, g_stageBytes, st>>>(dP, A);
+void fp_launch_restrict(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st) {
+  levelLaunch<RESTRICT>(bt, S, tiles, sms, st);
 }
-
-int fp_bottom_capacity() { return (200 * 1024) / 12; }
-
-void fp_launch_bottom(const SimParams* dP, int level, int iterations, const float* rhs, const float* pin, float* pout,
-                      int capacity, cudaStream_t st) {
-  size_t smem = (size_t)capacity * 12;
-  k_bottom<<<1, 1024, smem, st>>>(dP, level, iterations, rhs, pin, pout);
+void fp_launch_prolong(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st) {
+  levelLaunch<PROLONG>(bt, S, tiles, sms, st);
+}
+void fp_launch_bottom(const FpBatch& bt, const MgSel& S, int iterations, int sms, cudaStream_t st) {
+  k_bottom<<<sms, 1024, BOTTOM_SMEM, st>>>(bt, S, iterations, BOTTOM_SMEM);
 }

@@ -153,12 +153,13 @@ FP_DEV void cellOf(const SimParams& P, const Home& H, int c, int& x, int& y, int
 // advectScalars (fluid-scalar-transport.wgsl:38-142), fused: both read only the velocity and
 // the scalars at the start of the step.
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS, 3) k_predict(const SimParams* __restrict__ Pp) {
-  const SimParams& P = *Pp;
+__global__ void __launch_bounds__(THREADS, 3) k_predict(FpBatch bt) {
   __shared__ int nslot[27];
   extern __shared__ float smem[];
-  uint32_t total = P.counters->active;
-  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
     uint32_t id = P.active[i];
     Home H = enterBrick(P, id, nslot);
     Stage G = stageOf(P, H, STAGED);
@@ -258,12 +259,13 @@ __global__ void __launch_bounds__(THREADS, 3) k_predict(const SimParams* __restr
 // ---------------------------------------------------------------------------------------
 // correctVelocity (fluid-velocity-transport.wgsl:104-179): bounded MacCormack correction.
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS, 3) k_correct(const SimParams* __restrict__ Pp) {
-  const SimParams& P = *Pp;
+__global__ void __launch_bounds__(THREADS, 3) k_correct(FpBatch bt) {
   __shared__ int nslot[27];
   extern __shared__ float smem[];
-  uint32_t total = P.counters->active;
-  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
     uint32_t id = P.active[i];
     Home H = enterBrick(P, id, nslot);
     Stage G = stageOf(P, H, STAGED);
@@ -334,14 +336,14 @@ __global__ void __launch_bounds__(THREADS, 3) k_correct(const SimParams* __restr
 // evolveFields (fluid-field-evolution.wgsl:9-84) with correctedScalars
 // (fluid-scalar-transport.wgsl:144-199) and recordContent (fluid-content.wgsl:29-64).
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS, 3) k_evolve(const SimParams* __restrict__ Pp) {
-  const SimParams& P = *Pp;
+__global__ void __launch_bounds__(THREADS, 3) k_evolve(FpBatch bt) {
   __shared__ int nslot[27];
   __shared__ uint32_t busyAll, expandsAll;
   extern __shared__ float smem[];
-  uint32_t total = P.counters->active;
-  uint32_t bricks = (uint32_t)P.capacity * 64u;
-  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
     uint32_t id = P.active[i];
     if (threadIdx.x == 0) {
       busyAll = 0;
@@ -511,7 +513,7 @@ __global__ void __launch_bounds__(THREADS, 3) k_evolve(const SimParams* __restri
         flags = FP_CONTENT | (busyAll << 3);
         uint32_t l = id & 63u;
         uint32_t bits = (1u << (l & 3u)) | (16u << ((l >> 2) & 3u)) | (256u << (l >> 4));
-        atomicOr(&P.activity[bricks + (id >> 6)], bits);
+        atomicOr(&P.activity[(size_t)P.capacity * 64u + (id >> 6)], bits);
       }
       if (expandsAll) flags |= FP_EXPANDS;
       if (flags) P.activity[id] |= flags;
@@ -522,11 +524,13 @@ __global__ void __launch_bounds__(THREADS, 3) k_evolve(const SimParams* __restri
 
 // ---------------------------------------------------------------------------------------
 // computeCurl (fluid-forces.wgsl:38-75) of the corrected velocity.
-__global__ void __launch_bounds__(THREADS) k_curl(const SimParams* __restrict__ Pp) {
-  const SimParams& P = *Pp;
+__global__ void __launch_bounds__(THREADS) k_curl(FpBatch bt) {
   __shared__ int nslot[27];
-  uint32_t total = P.counters->active;
-  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
+    if (!P.curlOn) continue;  // the same for the whole CTA
     Home H = enterBrick(P, P.active[i], nslot);
     size_t slot = (size_t)nslot[13];
     const size_t N = P.N;
@@ -656,12 +660,13 @@ FP_DEV float sourceVelocity(const SimParams& P, int tile, float value, float fx,
 
 // applyForces (fluid-forces.wgsl:151-182): centre forces of the brick and of the cells past
 // it on one axis, staged in shared memory, averaged to the faces.
-__global__ void __launch_bounds__(THREADS) k_forces(const SimParams* __restrict__ Pp) {
-  const SimParams& P = *Pp;
+__global__ void __launch_bounds__(THREADS) k_forces(FpBatch bt) {
   __shared__ int nslot[27];
   extern __shared__ float3 forceTile[];  // (B+1)^3
-  uint32_t total = P.counters->active;
-  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
     uint32_t id = P.active[i];
     Home H = enterBrick(P, id, nslot);
     size_t slot = (size_t)nslot[13];
@@ -721,11 +726,13 @@ FP_DEV bool pressureUnknown(const SimParams& P, const Home& H, int x, int y, int
 // computeDivergence (fluid-forces.wgsl:184-203) and the finest level's first Jacobi
 // iterate from zero (initializePressure, pressure.wgsl:485-505), fused: the iterate needs
 // only the cell's own right-hand side.
-__global__ void __launch_bounds__(THREADS) k_divergence(const SimParams* __restrict__ Pp, float* __restrict__ pOut) {
-  const SimParams& P = *Pp;
+__global__ void __launch_bounds__(THREADS) k_divergence(FpBatch bt, int pSel) {
   __shared__ int nslot[27];
-  uint32_t total = P.counters->active;
-  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
+    float* pOut = P.p0[pSel];
     Home H = enterBrick(P, P.active[i], nslot);
     size_t slot = (size_t)nslot[13];
     const size_t N = P.N;
@@ -751,11 +758,13 @@ __global__ void __launch_bounds__(THREADS) k_divergence(const SimParams* __restr
 }
 
 // project (fluid-forces.wgsl:228-262) into the velocity pool of the next step.
-__global__ void __launch_bounds__(THREADS) k_project(const SimParams* __restrict__ Pp, const float* __restrict__ p) {
-  const SimParams& P = *Pp;
+__global__ void __launch_bounds__(THREADS) k_project(FpBatch bt, int pSel) {
   __shared__ int nslot[27];
-  uint32_t total = P.counters->active;
-  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
+    const float* p = P.p0[pSel];
     Home H = enterBrick(P, P.active[i], nslot);
     size_t slot = (size_t)nslot[13];
     const size_t N = P.N;
@@ -839,10 +848,6 @@ static size_t stagedBytes(int channels) {
   const int S = 8 + 2 * HALO;
   return (size_t)channels * S * S * S * sizeof(float);
 }
-template <typename K>
-static void launchStaged(K kernel, int channels, const SimParams* dP, int sms, cudaStream_t st) {
-  kernel<<<sms * 4, THREADS, stagedBytes(channels), st>>>(dP);
-}
 
 // Shared-memory limits of the step kernels, set once before any launch (and so before any
 // stream capture of one).
@@ -854,33 +859,33 @@ void fp_step_configure(int B) {
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_forces, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-void fp_launch_predict(const SimParams* dP, int B, int sms, cudaStream_t st) {
+void fp_launch_predict(const FpBatch& bt, int B, int sms, cudaStream_t st) {
   if (B == 8)
-    launchStaged(k_predict<true>, 7, dP, sms, st);
+    k_predict<true><<<sms * 4, THREADS, stagedBytes(7), st>>>(bt);
   else
-    k_predict<false><<<sms * 4, THREADS, 0, st>>>(dP);
+    k_predict<false><<<sms * 4, THREADS, 0, st>>>(bt);
 }
-void fp_launch_correct(const SimParams* dP, int B, int sms, cudaStream_t st) {
+void fp_launch_correct(const FpBatch& bt, int B, int sms, cudaStream_t st) {
   if (B == 8)
-    launchStaged(k_correct<true>, 6, dP, sms, st);
+    k_correct<true><<<sms * 4, THREADS, stagedBytes(6), st>>>(bt);
   else
-    k_correct<false><<<sms * 4, THREADS, 0, st>>>(dP);
+    k_correct<false><<<sms * 4, THREADS, 0, st>>>(bt);
 }
-void fp_launch_evolve(const SimParams* dP, int B, int sms, cudaStream_t st) {
+void fp_launch_evolve(const FpBatch& bt, int B, int sms, cudaStream_t st) {
   if (B == 8)
-    launchStaged(k_evolve<true>, 7, dP, sms, st);
+    k_evolve<true><<<sms * 4, THREADS, stagedBytes(7), st>>>(bt);
   else
-    k_evolve<false><<<sms * 4, THREADS, 0, st>>>(dP);
+    k_evolve<false><<<sms * 4, THREADS, 0, st>>>(bt);
 }
-void fp_launch_curl(const SimParams* dP, int sms, cudaStream_t st) { k_curl<<<sms * 4, THREADS, 0, st>>>(dP); }
-void fp_launch_forces(const SimParams* dP, int B, int sms, cudaStream_t st) {
+void fp_launch_curl(const FpBatch& bt, int sms, cudaStream_t st) { k_curl<<<sms * 4, THREADS, 0, st>>>(bt); }
+void fp_launch_forces(const FpBatch& bt, int B, int sms, cudaStream_t st) {
   size_t smem = (size_t)(B + 1) * (B + 1) * (B + 1) * sizeof(float3);
-  k_forces<<<sms * 4, THREADS, smem, st>>>(dP);
+  k_forces<<<sms * 4, THREADS, smem, st>>>(bt);
 }
-void fp_launch_divergence(const SimParams* dP, float* pOut, int sms, cudaStream_t st) {
-  k_divergence<<<sms * 4, THREADS, 0, st>>>(dP, pOut);
+void fp_launch_divergence(const FpBatch& bt, int pSel, int sms, cudaStream_t st) {
+  k_divergence<<<sms * 4, THREADS, 0, st>>>(bt, pSel);
 }
-void fp_launch_project(const SimParams* dP, const float* p, int sms, cudaStream_t st) {
-  k_project<<<sms * 4, THREADS, 0, st>>>(dP, p);
+void fp_launch_project(const FpBatch& bt, int pSel, int sms, cudaStream_t st) {
+  k_project<<<sms * 4, THREADS, 0, st>>>(bt, pSel);
 }
 void fp_launch_noise(float4* noise, cudaStream_t st) { k_noise<<<64 * 64 * 64 / 256, 256, 0, st>>>(noise); }

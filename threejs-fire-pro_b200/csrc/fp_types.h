@@ -84,6 +84,12 @@ struct FpCounters {
 };
 
 struct SimParams {
+  // what this step builds besides the fields (one launch covers many simulations, each
+  // skipping the work its own flags leave out)
+  int buildSolids;  // collider bits of granted slots, or of every slot with solidsAll
+  int topoAll;      // multigrid topology of every slot and tile, not only granted slots
+  int curlOn;       // vorticity confinement is on: the curl is computed
+  uint32_t* readback;  // host-mapped: the counters, then a content word per tile slot
   // lattice
   int B, shift, N, W;  // cells per brick side, log2, cells per brick, solid words per slot
   int brickLevels, bottom;
@@ -146,4 +152,22 @@ struct SimParams {
   const uint32_t* tileLists;  // 8-word header per tile slot, then indices
   FpFlame flame;
   const float4* noise;  // 64^3 curl noise
+};
+
+// Work lists of one launch over a batch of simulations. Each list is the concatenation of
+// the simulations' own lists; a row of prefix offsets (count + 1 entries) maps an item to its
+// simulation. Rows of the host-known lists are written before the launch, the computing
+// bricks and granted slots by the allocation on the device.
+enum FpWork {
+  FP_WORK_IDBLOCKS,  // blocks of 256 brick ids
+  FP_WORK_TILES,     // tile slots
+  FP_WORK_IDS,       // brick ids
+  FP_WORK_ACTIVE,    // computing bricks
+  FP_WORK_FRESH,     // slots granted this step
+  FP_WORK_KINDS
+};
+struct FpBatch {
+  const SimParams* sims;  // one per simulation of the launch
+  uint32_t* work;         // work[0] = simulations; row k at work + 1 + k * stride
+  int stride;             // most simulations + 1
 };

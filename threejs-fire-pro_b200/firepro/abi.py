@@ -203,6 +203,23 @@ SIGNATURES = {
     "fp_sim_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "fp_sim_read_profile": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
     "fp_compact_ids_noalloc": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "fp_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "fp_batch_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "fp_batch_destroy": (C.c_int, [C.c_void_p]),
+    "fp_batch_add": (C.c_int, [C.c_void_p, C.POINTER(fp_grid), C.POINTER(C.c_uint32)]),
+    "fp_batch_remove": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "fp_batch_reset": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "fp_batch_set_runtime": (C.c_int, [C.c_void_p, C.c_uint32, C.c_float, C.c_double, C.c_int]),
+    "fp_batch_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(fp_frame), C.POINTER(C.c_float),
+                                C.c_uint32]),
+    "fp_batch_synchronize": (C.c_int, [C.c_void_p]),
+    "fp_batch_stats": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(fp_stats)]),
+    "fp_batch_read_field": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.POINTER(C.c_float), C.c_size_t]),
+    "fp_batch_read_table": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.POINTER(C.c_size_t)]),
+    "fp_batch_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "fp_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "fp_batch_read_profile": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
+    "fp_grid_memory_bytes": (C.c_int, [C.POINTER(fp_grid), C.POINTER(C.c_uint64)]),
 }
 FP_COMPACT_MAX_IDS = 1 << 22
 

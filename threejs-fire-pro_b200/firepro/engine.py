@@ -102,3 +102,107 @@ class FluidSimulation:
         cnt = C.c_uint32(n.value)
         self._check(self.lib.fp_sim_read_bricks(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), C.byref(cnt)))
         return out[: cnt.value]
+
+
+class SimulationBatch:
+    """Many simulations stepped by one launch (fp_batch_* of the C ABI).
+
+    `add` returns an id; `step` takes a list of (id, frame, dt) and steps them together. Each
+    simulation's results are the same as stepping it alone with `FluidSimulation`.
+    """
+
+    def __init__(self, brick_size: int = 8, device: int = 0):
+        self.lib = abi.load_library()
+        h = C.c_void_p()
+        rc = self.lib.fp_batch_create(device, brick_size, C.byref(h))
+        if rc != abi.FP_OK:
+            raise FireProError(rc, self.lib.fp_last_error(None).decode())
+        self.h = h
+        self.cells = brick_size ** 3
+        self._frames = None
+
+    def _check(self, rc: int):
+        if rc != abi.FP_OK:
+            raise FireProError(rc, self.lib.fp_batch_last_error(self.h).decode())
+
+    def dispose(self):
+        if getattr(self, "h", None):
+            self.lib.fp_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass
+
+    def add(self, grid: abi.fp_grid) -> int:
+        out = C.c_uint32()
+        self._check(self.lib.fp_batch_add(self.h, C.byref(grid), C.byref(out)))
+        return out.value
+
+    def remove(self, sim: int):
+        self._check(self.lib.fp_batch_remove(self.h, sim))
+
+    def reset(self, sim: int):
+        self._check(self.lib.fp_batch_reset(self.h, sim))
+
+    def set_runtime(self, sim: int, cutoff: float, voxel_budget: float, ground: bool):
+        self._check(self.lib.fp_batch_set_runtime(self.h, sim, cutoff, voxel_budget, int(ground)))
+
+    def step(self, items):
+        """Step [(id, fp_frame, dt), ...] in one launch."""
+        n = len(items)
+        ids = (C.c_uint32 * n)(*[i for i, _, _ in items])
+        frames = (abi.fp_frame * n)(*[f for _, f, _ in items])
+        dts = (C.c_float * n)(*[d for _, _, d in items])
+        self._frames = frames  # the frames' arrays stay alive with their owners
+        self._check(self.lib.fp_batch_step(self.h, ids, frames, dts, n))
+
+    def synchronize(self):
+        self._check(self.lib.fp_batch_synchronize(self.h))
+
+    def stats(self, sim: int) -> abi.fp_stats:
+        s = abi.fp_stats()
+        self._check(self.lib.fp_batch_stats(self.h, sim, C.byref(s)))
+        return s
+
+    def field(self, sim: int, fid: int) -> np.ndarray:
+        s = self.stats(sim)
+        ch = abi.FIELD_CHANNELS[fid]
+        out = np.empty((s.pool_slots, ch, self.cells), np.float32)
+        self._check(self.lib.fp_batch_read_field(self.h, sim, fid, out.ctypes.data_as(C.POINTER(C.c_float)),
+                                                 out.nbytes))
+        return out
+
+    def table(self, sim: int, tid: int) -> np.ndarray:
+        n = C.c_size_t(0)
+        self.lib.fp_batch_read_table(self.h, sim, tid, None, C.byref(n))
+        out = np.empty(max(1, n.value // 4), np.uint32)
+        n2 = C.c_size_t(out.nbytes)
+        self._check(self.lib.fp_batch_read_table(self.h, sim, tid, out.ctypes.data, C.byref(n2)))
+        return out[: n2.value // 4]
+
+    def stream(self) -> int:
+        out = C.c_void_p()
+        self._check(self.lib.fp_batch_stream(self.h, C.byref(out)))
+        return out.value or 0
+
+    def set_profiling(self, on: bool):
+        self._check(self.lib.fp_batch_set_profiling(self.h, int(on)))
+
+    def profile(self) -> dict:
+        arr = (abi.fp_phase * 16)()
+        n = C.c_uint32(16)
+        self._check(self.lib.fp_batch_read_profile(self.h, arr, C.byref(n)))
+        return {arr[i].name.decode(): (arr[i].launches, arr[i].ms, arr[i].voxels) for i in range(n.value)}
+
+
+def grid_memory_bytes(grid: abi.fp_grid) -> int:
+    """Device bytes a simulation of `grid` holds once created (the admission estimate)."""
+    lib = abi.load_library()
+    out = C.c_uint64()
+    rc = lib.fp_grid_memory_bytes(C.byref(grid), C.byref(out))
+    if rc != abi.FP_OK:
+        raise FireProError(rc, lib.fp_last_error(None).decode())
+    return out.value
