@@ -213,6 +213,141 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def batched_form(local: int, sims: int = 64, grow: int = 90, steps: int = 60, seed: int = 1) -> dict:
+    """The batched workload: `sims` member scenes (brick budgets log-uniform 16-2048, 1-4
+    emitters of radius 0.1-0.6 m, rates 0.2-2.0 /s), grown `grow` steps, then `steps` timed
+    steps (a) each simulation through its own FluidSimulation, one call after another (the
+    plain drop-in; each has its own stream, so their work may overlap on the GPU) and (b) all
+    of them through one SimulationBatch (one upload, one graph per step). Both evolve the same
+    states bit for bit, so they do the same voxel-steps; wall time of the host loop until the
+    GPU is idle, host frames built inside the loop."""
+    import torch
+
+    from firepro import scenes
+    from firepro.engine import FIXED_DT, FluidSimulation, SimulationBatch
+
+    mem = [scenes.MemberScene(seed, k) for k in range(sims)]
+    batch = SimulationBatch(8, device=local)
+    ids = []
+    for m in mem:
+        i = batch.add(m.grid(budget=m.budget))
+        batch.set_runtime(i, 0.05, m.budget, True)
+        ids.append(i)
+    plain = []
+    for m in mem:
+        s = FluidSimulation(m.grid(budget=m.budget), device=local)
+        s.set_runtime(0.05, m.budget, True)
+        plain.append(s)
+    for st in range(grow):
+        fds = [m.frame(st) for m in mem]
+        batch.step([(i, fd.frame, FIXED_DT) for i, fd in zip(ids, fds)])
+        for s, fd in zip(plain, fds):
+            s.step(fd.frame)
+    batch.synchronize()
+    for s in plain:
+        s.synchronize()
+    # (b) batched: device time on the batch's stream and wall time; actives read each step
+    stream = torch.cuda.ExternalStream(batch.stream(), device=local)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    actives = []
+    t0 = time.perf_counter()
+    ev[0].record(stream)
+    for k in range(steps):
+        fds = [m.frame(grow + k) for m in mem]
+        batch.step([(i, fd.frame, FIXED_DT) for i, fd in zip(ids, fds)])
+        ev[k + 1].record(stream)
+        actives.append(sum(batch.stats(i).active_bricks for i in ids))
+    batch.synchronize()
+    wall_b = time.perf_counter() - t0
+    dev_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+    # (a) plain: one simulation after another
+    t0 = time.perf_counter()
+    for k in range(steps):
+        fds = [m.frame(grow + k) for m in mem]
+        for s, fd in zip(plain, fds):
+            s.step(fd.frame)
+    for s in plain:
+        s.synchronize()
+    wall_p = time.perf_counter() - t0
+    same = [s.stats().active_bricks for s in plain] == [batch.stats(i).active_bricks for i in ids]
+    vox = sum(actives) * BRICK_VOXELS
+    p50, p99 = percentiles(dev_ms)
+    out = {
+        "workload": f"{sims} member scenes, brick budgets log-uniform 16-2048 (seed {seed}), 1-4 emitters r 0.1-0.6 m, "
+                    f"rates 0.2-2.0/s; grown {grow} steps, {steps} timed; plain FP32",
+        "mean_active_bricks": sum(actives) / len(actives),
+        "batched": {"value": vox / wall_b, "device_value": vox / (sum(dev_ms) / 1e3), "ms_per_step": 1e3 * wall_b / steps,
+                    "device_p50_ms": p50, "device_p99_ms": p99},
+        "plain": {"value": vox / wall_p, "ms_per_step": 1e3 * wall_p / steps},
+        "speedup": wall_p / wall_b,
+        "same_final_bricks": same,
+        "unit": "voxel-steps/s",
+    }
+    batch.dispose()
+    for s in plain:
+        s.dispose()
+    return out
+
+
+def served_form(local: int, sessions: int = 64, grow: int = 90, ticks: int = 300, seed: int = 1,
+                min_bricks: int = 16, max_bricks: int = 2048) -> dict:
+    """Serving at `sessions` live sessions: member scenes (brick budgets log-uniform in
+    [min_bricks, max_bricks]) opened on one FireServer, grown `grow` steps submitted as fast as
+    the server takes them, then `ticks` ticks of a 60 Hz wall clock at which every session
+    submits its next step. Latency is submission to completion of the step on the device (the
+    server's clock); throughput is the timed steps' voxel-steps over the span from the first
+    timed submission to the last completion. Frames are built before the timed loop."""
+    from firepro import scenes
+    from firepro.engine import FireServer
+
+    mem = [scenes.MemberScene(seed, k, min_bricks, max_bricks) for k in range(sessions)]
+    srv = FireServer(150 * (1 << 30), max_sessions=256, device=local)
+    ids = [srv.open(m.grid(budget=m.budget)) for m in mem]
+    for s in range(grow):
+        fds = [m.frame(s) for m in mem]
+        for i, fd in zip(ids, fds):
+            srv.submit(i, fd.frame)
+        srv.drain()
+    while srv.poll():
+        pass
+    frames = [[m.frame(grow + t) for m in mem] for t in range(ticks)]
+    first_ticket = None
+    t0 = time.perf_counter()
+    for t in range(ticks):
+        target = t0 + t / 60.0
+        delay = target - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        for i, fd in zip(ids, frames[t]):
+            k = srv.submit(i, fd.frame)
+            if first_ticket is None:
+                first_ticket = k
+    srv.drain(600000)
+    done = []
+    while True:
+        got = srv.poll()
+        if not got:
+            break
+        done += [c for c in got if c.ticket >= first_ticket]
+    st = srv.stats()
+    srv.dispose()
+    lat = sorted(c.done_ms - c.submit_ms for c in done)
+    span_ms = max(c.done_ms for c in done) - min(c.submit_ms for c in done)
+    vox = sum(c.active_bricks for c in done) * BRICK_VOXELS
+    return {
+        "workload": f"{sessions} sessions, member scenes with brick budgets log-uniform {min_bricks}-{max_bricks} "
+                    f"(seed {seed}); grown {grow} steps, then {ticks} ticks at 60 Hz, one step request per session "
+                    f"per tick; plain FP32",
+        "value": vox / (span_ms / 1e3),
+        "unit": "voxel-steps/s",
+        "latency_p50_ms": lat[len(lat) // 2],
+        "latency_p99_ms": lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))],
+        "mean_active_bricks": sum(c.active_bricks for c in done) / ticks,
+        "mean_batch": st.mean_batch,
+        "steps": len(done),
+    }
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -341,6 +476,9 @@ def run_ours(args, rank, world, local):
         "host": host,
         "clocks": clock,
     }
+    if world == 1 and not args.no_forms:
+        line["forms"] = {"batched": batched_form(local, steps=max(10, min(args.steps, 60))),
+                         "served": served_form(local)}
     if world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         cv, csteps, cbricks, _ = cpu_sample(scenes.LargeScene, 20.0, 400, threads)
@@ -357,6 +495,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched and served workloads")
     ap.add_argument("--scene", default="large_scene", help="workload (default: the large single simulation)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

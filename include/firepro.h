@@ -265,6 +265,68 @@ int fp_batch_read_profile(fp_batch* batch, fp_phase* phases, uint32_t* count);
 /* Device bytes a simulation of `grid` holds once created: the admission estimate. */
 int fp_grid_memory_bytes(const fp_grid* grid, uint64_t* bytes);
 
+/* ---- Serving: sessions admitted by device-memory budget, their step requests batched as
+ * they arrive. No reference counterpart. A server owns a batch and a scheduler thread: every
+ * launch steps each live session that has a request queued (the oldest one), so requests
+ * that arrive while a launch runs go into the next; sessions waiting for admission join as
+ * memory and session slots free up. A session's steps run in submission order; a result is
+ * the same alone and among any other sessions (bit for bit). Times are milliseconds on the
+ * server's steady clock since creation. */
+typedef struct fp_server fp_server;
+typedef struct {
+  int device;
+  int brick_size;          /* 8 or 16, the same for every session */
+  uint64_t memory_budget;  /* admission: the sessions' device bytes (fp_grid_memory_bytes) */
+  uint32_t max_sessions;   /* live sessions at most */
+} fp_server_config;
+#define FP_SESSION_WAITING 0 /* queued for admission */
+#define FP_SESSION_LIVE 1
+#define FP_SESSION_CLOSING 2 /* closed by the caller, its queued steps still run */
+#define FP_SESSION_CLOSED 3
+#define FP_SESSION_FAILED 4  /* admission failed (device memory): see fp_server_last_error */
+typedef struct {
+  uint32_t session;
+  int status;             /* FP_OK, or the step's error */
+  uint64_t ticket;        /* fp_server_submit's ticket */
+  uint64_t step;          /* the session's steps after this one */
+  uint32_t active_bricks; /* computing bricks of this step */
+  uint32_t batch_size;    /* sessions in the launch that ran it */
+  double submit_ms, done_ms;
+} fp_completion;
+typedef struct {
+  uint32_t live, waiting, queued_steps;
+  uint64_t memory_bytes;     /* admitted sessions' admission estimate */
+  uint64_t device_bytes;     /* their device memory now */
+  uint64_t steps_done, launches;
+  double voxel_steps;        /* sum over completed steps of computing bricks x cells */
+  double elapsed_ms;         /* since creation */
+  double latency_p50_ms, latency_p99_ms; /* submit to done, over completed steps */
+  double mean_batch;         /* sessions per launch */
+} fp_server_stats;
+const char* fp_server_last_error(const fp_server* server);
+int fp_server_create(const fp_server_config* config, fp_server** out);
+/* Stops the scheduler after the launched steps complete; queued steps are dropped. */
+int fp_server_destroy(fp_server* server);
+/* Open a session of `grid` with the runtime fields of fp_sim_set_runtime; it waits for
+ * admission (FP_SESSION_WAITING) unless memory and a slot are free now. FP_ELIMIT when the
+ * grid alone exceeds the memory budget. */
+int fp_server_open(fp_server* server, const fp_grid* grid, float cutoff, int ground, uint32_t* session);
+/* The session leaves once its queued steps have run; its memory then returns to the budget. */
+int fp_server_close(fp_server* server, uint32_t session);
+int fp_server_session_state(fp_server* server, uint32_t session, int* state);
+/* Queue one step of `session` (frame arrays are copied; dt as fp_sim_step). */
+int fp_server_submit(fp_server* server, uint32_t session, const fp_frame* frame, float dt, uint64_t* ticket);
+/* Completed steps, oldest first: up to `capacity` into `out`, `*count` written. Waits up to
+ * `wait_ms` for the first one when none is ready. */
+int fp_server_poll(fp_server* server, fp_completion* out, uint32_t capacity, uint32_t* count, int wait_ms);
+/* Wait until every queued step has completed (or `wait_ms` passed: FP_ETIMEOUT). */
+int fp_server_drain(fp_server* server, int wait_ms);
+int fp_server_read_stats(fp_server* server, fp_server_stats* out);
+/* A live session's stats (as fp_sim_stats), as of its latest measured step. */
+int fp_server_session_stats(fp_server* server, uint32_t session, fp_stats* out);
+/* A live session's field (as fp_sim_read_field), between its steps. */
+int fp_server_read_field(fp_server* server, uint32_t session, int field, float* host, size_t bytes);
+
 /* Most ids fp_compact_ids_noalloc accepts in one call. */
 #define FP_COMPACT_MAX_IDS (1u << 22)
 

@@ -205,6 +205,10 @@ class Stepper {
   uint64_t launches() const { return launches_; }
   double hostPrepareMs() const { return hostPrepareMs_; }
   double hostWaitMs() const { return hostWaitMs_; }
+  // Host-mapped measurement words of the i-th simulation of the last launch: its counters
+  // (FpCounters), then its tile words. Valid once the launch's measurement completed, until
+  // the next launch.
+  const uint32_t* lastReadback(int i) const { return readH_ + pending_[i].second; }
   uint64_t lastUploadBytes() const { return lastUpload_; }
   uint64_t lastReadbackBytes() const { return lastReadback_; }
   const float4* noise() const { return (const float4*)noise_; }

@@ -185,6 +185,48 @@ class fp_phase(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_uint64), ("ms", C.c_double), ("voxels", C.c_double)]
 
 
+FP_SESSION_WAITING = 0
+FP_SESSION_LIVE = 1
+FP_SESSION_CLOSING = 2
+FP_SESSION_CLOSED = 3
+FP_SESSION_FAILED = 4
+
+
+class fp_server_config(C.Structure):
+    _fields_ = [("device", C.c_int), ("brick_size", C.c_int), ("memory_budget", C.c_uint64),
+                ("max_sessions", C.c_uint32)]
+
+
+class fp_completion(C.Structure):
+    _fields_ = [
+        ("session", C.c_uint32),
+        ("status", C.c_int),
+        ("ticket", C.c_uint64),
+        ("step", C.c_uint64),
+        ("active_bricks", C.c_uint32),
+        ("batch_size", C.c_uint32),
+        ("submit_ms", C.c_double),
+        ("done_ms", C.c_double),
+    ]
+
+
+class fp_server_stats(C.Structure):
+    _fields_ = [
+        ("live", C.c_uint32),
+        ("waiting", C.c_uint32),
+        ("queued_steps", C.c_uint32),
+        ("memory_bytes", C.c_uint64),
+        ("device_bytes", C.c_uint64),
+        ("steps_done", C.c_uint64),
+        ("launches", C.c_uint64),
+        ("voxel_steps", C.c_double),
+        ("elapsed_ms", C.c_double),
+        ("latency_p50_ms", C.c_double),
+        ("latency_p99_ms", C.c_double),
+        ("mean_batch", C.c_double),
+    ]
+
+
 # Exported symbols of libfirepro.so (include/firepro.h), with their ctypes signatures.
 SIGNATURES = {
     "fp_abi_version": (C.c_int, []),
@@ -220,6 +262,18 @@ SIGNATURES = {
     "fp_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "fp_batch_read_profile": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
     "fp_grid_memory_bytes": (C.c_int, [C.POINTER(fp_grid), C.POINTER(C.c_uint64)]),
+    "fp_server_last_error": (C.c_char_p, [C.c_void_p]),
+    "fp_server_create": (C.c_int, [C.POINTER(fp_server_config), C.POINTER(C.c_void_p)]),
+    "fp_server_destroy": (C.c_int, [C.c_void_p]),
+    "fp_server_open": (C.c_int, [C.c_void_p, C.POINTER(fp_grid), C.c_float, C.c_int, C.POINTER(C.c_uint32)]),
+    "fp_server_close": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "fp_server_session_state": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_int)]),
+    "fp_server_submit": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(fp_frame), C.c_float, C.POINTER(C.c_uint64)]),
+    "fp_server_poll": (C.c_int, [C.c_void_p, C.POINTER(fp_completion), C.c_uint32, C.POINTER(C.c_uint32), C.c_int]),
+    "fp_server_drain": (C.c_int, [C.c_void_p, C.c_int]),
+    "fp_server_read_stats": (C.c_int, [C.c_void_p, C.POINTER(fp_server_stats)]),
+    "fp_server_session_stats": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(fp_stats)]),
+    "fp_server_read_field": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.POINTER(C.c_float), C.c_size_t]),
 }
 FP_COMPACT_MAX_IDS = 1 << 22
 

@@ -206,3 +206,77 @@ def grid_memory_bytes(grid: abi.fp_grid) -> int:
     if rc != abi.FP_OK:
         raise FireProError(rc, lib.fp_last_error(None).decode())
     return out.value
+
+
+class FireServer:
+    """Serving front end (fp_server_* of the C ABI): sessions admitted by device-memory
+    budget, their step requests batched by a scheduler thread as they arrive."""
+
+    def __init__(self, memory_budget: int, max_sessions: int = 256, brick_size: int = 8, device: int = 0):
+        self.lib = abi.load_library()
+        cfg = abi.fp_server_config(device, brick_size, int(memory_budget), max_sessions)
+        h = C.c_void_p()
+        rc = self.lib.fp_server_create(C.byref(cfg), C.byref(h))
+        if rc != abi.FP_OK:
+            raise FireProError(rc, self.lib.fp_last_error(None).decode())
+        self.h = h
+        self.cells = brick_size ** 3
+        self._buf = (abi.fp_completion * 1024)()
+
+    def _check(self, rc: int):
+        if rc != abi.FP_OK:
+            raise FireProError(rc, self.lib.fp_server_last_error(self.h).decode())
+
+    def dispose(self):
+        if getattr(self, "h", None):
+            self.lib.fp_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass
+
+    def open(self, grid: abi.fp_grid, cutoff: float = 0.05, ground: bool = True) -> int:
+        out = C.c_uint32()
+        self._check(self.lib.fp_server_open(self.h, C.byref(grid), cutoff, int(ground), C.byref(out)))
+        return out.value
+
+    def close(self, session: int):
+        self._check(self.lib.fp_server_close(self.h, session))
+
+    def state(self, session: int) -> int:
+        out = C.c_int()
+        self._check(self.lib.fp_server_session_state(self.h, session, C.byref(out)))
+        return out.value
+
+    def submit(self, session: int, frame: abi.fp_frame, dt: float = FIXED_DT) -> int:
+        t = C.c_uint64()
+        self._check(self.lib.fp_server_submit(self.h, session, C.byref(frame), dt, C.byref(t)))
+        return t.value
+
+    def poll(self, wait_ms: int = 0) -> list:
+        n = C.c_uint32()
+        self._check(self.lib.fp_server_poll(self.h, self._buf, len(self._buf), C.byref(n), wait_ms))
+        return [abi.fp_completion.from_buffer_copy(self._buf[i]) for i in range(n.value)]
+
+    def drain(self, wait_ms: int = 60000):
+        self._check(self.lib.fp_server_drain(self.h, wait_ms))
+
+    def stats(self) -> abi.fp_server_stats:
+        s = abi.fp_server_stats()
+        self._check(self.lib.fp_server_read_stats(self.h, C.byref(s)))
+        return s
+
+    def session_stats(self, session: int) -> abi.fp_stats:
+        s = abi.fp_stats()
+        self._check(self.lib.fp_server_session_stats(self.h, session, C.byref(s)))
+        return s
+
+    def field(self, session: int, fid: int) -> np.ndarray:
+        ch = abi.FIELD_CHANNELS[fid]
+        out = np.empty((self.session_stats(session).pool_slots, ch, self.cells), np.float32)
+        self._check(self.lib.fp_server_read_field(self.h, session, fid, out.ctypes.data_as(C.POINTER(C.c_float)),
+                                                  out.nbytes))
+        return out

@@ -295,4 +295,41 @@ class EmptyScene(Scene):
         return make_frame(self.settings, self.comb, False, [])
 
 
+class MemberScene(Scene):
+    """One simulation of a batch or a serving session, drawn from `(seed, index)`: 1-4 sphere or
+    box emitters of radius 0.1-0.6 m with heat, smoke and fuel rates 0.2-2.0 /s each, within
+    a metre of the origin, combustion on; its brick budget is drawn log-uniform from
+    [min_bricks, max_bricks] and caps its growth."""
+
+    name = "member"
+
+    def __init__(self, seed: int = 1, index: int = 0, min_bricks: int = 16, max_bricks: int = 2048):
+        self.seed = seed
+        self.index = index
+        r = [_hash01(index * 64 + k, seed) for k in range(64)]
+        self.bricks = int(round(math.exp(math.log(min_bricks) + r[0] * (math.log(max_bricks) - math.log(min_bricks)))))
+        self.settings = settings(buoyancy=1.5, vorticity=0.3 + 1.5 * r[1], seed=seed * 1000 + index)
+        self.comb = combustion()
+        self.emitters = []
+        count = 1 + int(r[2] * 4) if r[2] < 1.0 else 4
+        for e in range(count):
+            q = r[3 + 8 * e: 11 + 8 * e]
+            radius = 0.1 + 0.5 * q[0]
+            pos = (1.6 * (q[1] - 0.5), 0.1 + radius * 0.5 + 0.3 * q[2], 1.6 * (q[3] - 0.5))
+            rates = [0.2 + 1.8 * q[k] for k in (4, 5, 6)]
+            shape = "box" if q[7] < 0.3 else "sphere"
+            self.emitters.append((shape, pos, (radius, radius, radius), rates))
+
+    @property
+    def budget(self) -> float:
+        return float(self.bricks * self.brick_size ** 3)
+
+    def frame(self, step: int) -> FrameData:
+        srcs = []
+        for i, (shape, pos, size, (heat, smoke, fuel)) in enumerate(self.emitters):
+            j = 1.0 + 0.25 * value_noise_1d(step / 12.0, self.seed * 7919 + self.index * 31 + i)
+            srcs.append(source(i + 1, shape, pos, size, flame=0.0, heat=heat * j, smoke=smoke * j, fuel=fuel * j))
+        return make_frame(self.settings, self.comb, True, srcs)
+
+
 SCENES = {"single_plume": SinglePlume, "large_scene": LargeScene, "force_scene": ForceScene, "empty": EmptyScene}
