@@ -224,19 +224,22 @@ def batched_form(local: int, sims: int = 64, grow: int = 90, steps: int = 60, se
     import torch
 
     from firepro import scenes
-    from firepro.engine import FIXED_DT, FluidSimulation, SimulationBatch
+    from firepro.engine import FIXED_DT, FluidSimulation, SimulationBatch, reserved_tiles
 
     mem = [scenes.MemberScene(seed, k) for k in range(sims)]
     batch = SimulationBatch(8, device=local)
     ids = []
+    # Both sides hold tables sized for their budgets, so no step stops to grow them.
     for m in mem:
         i = batch.add(m.grid(budget=m.budget))
         batch.set_runtime(i, 0.05, m.budget, True)
+        batch.reserve_tiles(i, reserved_tiles(m.grid(budget=m.budget)))
         ids.append(i)
     plain = []
     for m in mem:
         s = FluidSimulation(m.grid(budget=m.budget), device=local)
         s.set_runtime(0.05, m.budget, True)
+        s.reserve_tiles(reserved_tiles(m.grid(budget=m.budget)))
         plain.append(s)
     for st in range(grow):
         fds = [m.frame(st) for m in mem]

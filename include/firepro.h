@@ -215,6 +215,10 @@ int fp_sim_set_runtime(fp_sim* sim, float cutoff, double voxel_budget, int groun
 /* `FluidSimulation.step(frame, dt)` (FluidSimulation.ts:1367-1373): dt in (0, 1/30].
  * Enqueues the step on the simulation's CUDA stream; returns before it completes. */
 int fp_sim_step(fp_sim* sim, const fp_frame* frame, float dt);
+/* Hold at least `tiles` tile slots from now on, so that steps never stop to grow the
+ * per-brick tables (the reference doubles them when the tiles outgrow them,
+ * FluidSimulation.ts:629-678). Storage only: results do not change. No reference counterpart. */
+int fp_sim_reserve_tiles(fp_sim* sim, uint32_t tiles);
 /* Wait for the simulation's queued work. */
 int fp_sim_synchronize(fp_sim* sim);
 /* Stats (waits for the latest step's measurement). */
@@ -253,6 +257,8 @@ int fp_batch_add(fp_batch* batch, const fp_grid* grid, uint32_t* id);
 int fp_batch_remove(fp_batch* batch, uint32_t id);
 int fp_batch_reset(fp_batch* batch, uint32_t id);
 int fp_batch_set_runtime(fp_batch* batch, uint32_t id, float cutoff, double voxel_budget, int ground);
+/* As fp_sim_reserve_tiles. */
+int fp_batch_reserve_tiles(fp_batch* batch, uint32_t id, uint32_t tiles);
 /* Step the `count` simulations `ids` (distinct) with frames[i] and dts[i], in one launch. */
 int fp_batch_step(fp_batch* batch, const uint32_t* ids, const fp_frame* frames, const float* dts, uint32_t count);
 int fp_batch_synchronize(fp_batch* batch);
@@ -264,6 +270,9 @@ int fp_batch_set_profiling(fp_batch* batch, int enabled);
 int fp_batch_read_profile(fp_batch* batch, fp_phase* phases, uint32_t* count);
 /* Device bytes a simulation of `grid` holds once created: the admission estimate. */
 int fp_grid_memory_bytes(const fp_grid* grid, uint64_t* bytes);
+/* The tile reservation a server gives a session of `grid`: one tile slot per four bricks of
+ * its budget, a power of two (at least 16). */
+int fp_grid_reserved_tiles(const fp_grid* grid, uint32_t* tiles);
 
 /* ---- Serving: sessions admitted by device-memory budget, their step requests batched as
  * they arrive. No reference counterpart. A server owns a batch and a scheduler thread: every

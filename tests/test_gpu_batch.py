@@ -155,3 +155,31 @@ def _grid16():
     g = scenes.SinglePlume().grid(budget=2 ** 18)
     g.brick_size = 16
     return g
+
+
+def test_reserved_tiles_change_storage_only():
+    """A simulation whose tables are reserved for its budget gives the same fields and the same
+    tables over the tile slots both hold, and no more tile slots in use."""
+    sc = scenes.LargeScene(seed=2)
+    budget = 2 ** 20
+    want, st = run_alone(sc, budget, 20, FIXED_DT)
+    sim = FluidSimulation(sc.grid(budget=budget))
+    sim.set_runtime(0.05, budget, True)
+    sim.reserve_tiles(4096)
+    assert sim.stats().tile_capacity == 4096
+    for s in range(20):
+        fd = sc.frame(s)
+        sim.step(fd.frame)
+    got = snapshot(sim.field, sim.table)
+    for f in FIELDS:
+        assert np.array_equal(got[("f", f)], want[("f", f)])
+    cap = st.tile_capacity
+    per_id = {abi.FP_TABLE_ENTRIES: 1, abi.FP_TABLE_PAGES: 1, abi.FP_TABLE_RECORDS: 28}
+    for t, w in per_id.items():
+        a, b = got[("t", t)], want[("t", t)]
+        assert np.array_equal(a[: cap * 64 * w], b), f"table {t} differs"
+        if t != abi.FP_TABLE_RECORDS:
+            assert np.all(a[cap * 64 * w:].view(np.int32) == -1)
+    assert np.array_equal(got[("t", abi.FP_TABLE_ACTIVE)], want[("t", abi.FP_TABLE_ACTIVE)])
+    assert np.array_equal(got[("t", abi.FP_TABLE_FREE)], want[("t", abi.FP_TABLE_FREE)])
+    sim.dispose()

@@ -145,6 +145,11 @@ int fp_sim_step(fp_sim* sim, const fp_frame* frame, float dt) {
   return rc;
 }
 
+int fp_sim_reserve_tiles(fp_sim* sim, uint32_t tiles) {
+  if (!sim) return failed("null simulation", FP_EINVAL);
+  return sim->engine->reserveTiles(tiles);
+}
+
 int fp_sim_synchronize(fp_sim* sim) {
   if (!sim) return failed("null simulation", FP_EINVAL);
   int rc = sim->stepper->synchronize();
@@ -277,6 +282,14 @@ int fp_batch_set_runtime(fp_batch* batch, uint32_t id, float cutoff, double voxe
   return rc ? batchFail(batch, rc, e->error()) : FP_OK;
 }
 
+int fp_batch_reserve_tiles(fp_batch* batch, uint32_t id, uint32_t tiles) {
+  if (!batch) return failed("null batch", FP_EINVAL);
+  fp::Engine* e = batchSim(batch, id);
+  if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
+  int rc = e->reserveTiles(tiles);
+  return rc ? batchFail(batch, rc, e->error()) : FP_OK;
+}
+
 int fp_batch_step(fp_batch* batch, const uint32_t* ids, const fp_frame* frames, const float* dts, uint32_t count) {
   if (!batch) return failed("null batch", FP_EINVAL);
   if (count && (!ids || !frames || !dts)) return batchFail(batch, FP_EINVAL, "fp_batch_step needs ids, frames and dts.");
@@ -349,7 +362,17 @@ int fp_grid_memory_bytes(const fp_grid* grid, uint64_t* bytes) {
   if (!grid || !bytes) return failed("fp_grid_memory_bytes needs a grid and an output.", FP_EINVAL);
   int rc = validateGrid(grid);
   if (rc) return rc;
-  *bytes = fp::Engine::estimateBytes(*grid);
+  *bytes = fp::Engine::estimateBytes(*grid, fp::Engine::tilesForBudget(grid->voxel_budget, grid->brick_size *
+                                                                                             grid->brick_size *
+                                                                                             grid->brick_size));
+  return FP_OK;
+}
+
+int fp_grid_reserved_tiles(const fp_grid* grid, uint32_t* tiles) {
+  if (!grid || !tiles) return failed("fp_grid_reserved_tiles needs a grid and an output.", FP_EINVAL);
+  int rc = validateGrid(grid);
+  if (rc) return rc;
+  *tiles = fp::Engine::tilesForBudget(grid->voxel_budget, grid->brick_size * grid->brick_size * grid->brick_size);
   return FP_OK;
 }
 

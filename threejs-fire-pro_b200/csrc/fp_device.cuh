@@ -238,6 +238,23 @@ FP_DEV float3 curlNoise(const SimParams& P, float px, float py, float pz) {
 
 // Load a brick's home record (its 27 neighbour entries) into shared memory as slots.
 // Every thread of the block must call this.
+// The home brick and tile of brick `id`; `nslot` is filled by the caller.
+FP_DEV Home homeOf(const SimParams& P, uint32_t id, const int* nslot) {
+  Home H;
+  int tile = (int)(id >> 6);
+  int4 t = __ldg(&P.tileRec[tile]);
+  int l = id & 63;
+  H.tile = tile;
+  H.tx = t.x;
+  H.ty = t.y;
+  H.tz = t.z;
+  H.bx = t.x * 4 + (l & 3);
+  H.by = t.y * 4 + ((l >> 2) & 3);
+  H.bz = t.z * 4 + (l >> 4);
+  H.nslot = nslot;
+  return H;
+}
+
 FP_DEV Home enterBrick(const SimParams& P, uint32_t id, int* nslot) {
   Home H;
   int tile = (int)(id >> 6);

@@ -231,7 +231,7 @@ int Engine::initialize() {
 
 // Device bytes of a simulation of `g` once its pools exist: per slot the pools and the brick
 // levels, per tile slot (at the minimum capacity) the tables and tile levels.
-uint64_t Engine::estimateBytes(const fp_grid& g) {
+uint64_t Engine::estimateBytes(const fp_grid& g, uint32_t tiles) {
   int B = g.brick_size, shift = B == 8 ? 3 : 4;
   uint64_t N = (uint64_t)B * B * B;
   double budget = g.voxel_budget > 0 ? g.voxel_budget : 8e6;
@@ -241,9 +241,33 @@ uint64_t Engine::estimateBytes(const fp_grid& g) {
     uint64_t c = (uint64_t)1 << (3 * (shift - l));
     perSlot += c * 13;
   }
-  uint64_t tiles = MIN_TILES;
   uint64_t perTile = 64 * (4 * 5 + FP_RECORD_WORDS * 4 + 8) + 16 + 27 * 4 + 16 + (64 + 8 + 1) * 13;
-  return slots * perSlot + tiles * perTile + 64 * 1024;
+  return slots * perSlot + (uint64_t)std::max(tiles, (uint32_t)MIN_TILES) * perTile + 64 * 1024;
+}
+
+// Tile slots for a budget of `budget` voxels in bricks of `cells`: one per four bricks the
+// budget holds, a power of two. Sparse tiles (the margins around sources, the ring around
+// content) rarely pass a quarter of the bricks, so a simulation reserved this way does not
+// grow its tables while it runs.
+uint32_t Engine::tilesForBudget(double budget, int cells) {
+  double bricks = std::floor((budget > 0 ? budget : 8e6) / (double)cells);
+  uint32_t want = (uint32_t)std::min(1.0e6, std::ceil(bricks / 4.0));
+  uint32_t tiles = MIN_TILES;
+  while (tiles < want) tiles *= 2;
+  return tiles;
+}
+
+// Tile capacity of at least `tiles` now, so that the steps do not stop to grow it. The
+// capacity only sizes storage: tile slots and brick ids do not depend on it.
+int Engine::reserveTiles(uint32_t tiles) {
+  int rc = consume();
+  if (rc) return rc;
+  if ((int)tiles <= capacity_) return FP_OK;
+  if (tiles > (1u << 24)) return fail(FP_ELIMIT, "tile reservation too large");
+  int cap = capacity_;
+  while (cap < (int)tiles) cap *= 2;
+  if ((rc = setCapacity(cap))) return rc;
+  return applyTiles();
 }
 
 // Pools of `slots` slots, all free: the stack pops slot 0 first.

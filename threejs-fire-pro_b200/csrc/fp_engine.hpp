@@ -80,8 +80,11 @@ class Engine {
     return code;
   }
   int brickSize() const { return B_; }
-  // Device bytes a simulation of this grid holds once its pools exist (for admission).
-  static uint64_t estimateBytes(const fp_grid& grid);
+  // Device bytes a simulation of this grid holds once its pools exist, with `tiles` tile
+  // slots (for admission).
+  static uint64_t estimateBytes(const fp_grid& grid, uint32_t tiles = 0);
+  static uint32_t tilesForBudget(double budget, int cells);
+  int reserveTiles(uint32_t tiles);
   uint64_t memoryBytes() const;
 
   // ---- the Stepper's side of a step

@@ -30,9 +30,9 @@ struct MgSel {
 };
 inline int fp_mg_sel(int level, int which) { return level * 4 + which; }
 void fp_launch_topology(const FpBatch& bt, bool anyAll, int sms, cudaStream_t st);
-void fp_launch_relax(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st);
-void fp_launch_restrict(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st);
-void fp_launch_prolong(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st);
+void fp_launch_relax(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st);
+void fp_launch_restrict(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st);
+void fp_launch_prolong(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st);
 // The bottom level's iterations, a CTA per simulation.
 void fp_launch_bottom(const FpBatch& bt, const MgSel& S, int iterations, int sms, cudaStream_t st);
 // Size the staged brick-level multigrid kernels for bricks of B cells (once per brick size).

@@ -207,15 +207,24 @@ FP_DEV void levelCell(const SimParams& P, const Home& H, const Args& A, long a, 
 //   RELAX     stage A.pin at A.level;           write A.pout at A.level
 //   RESTRICT  stage A.pin at A.level - 1 (fine); write A.pout, A.cfirst at A.level (coarse)
 //   PROLONG   stage A.coarse at A.level + 1;    write A.pout at A.level
-template <int OP>
+template <int OP, int GROUP>
 __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel Sl) {
-  __shared__ int nslot[27];
-  __shared__ int need[8];  // bit k of the index: -1 on axis k
-  extern __shared__ float st[];
+  // GROUP threads per brick, 256 / GROUP bricks per CTA: the coarse brick levels hold 64 or 8
+  // cells a brick, so several bricks share a CTA. Each group has its own neighbour slots,
+  // flags and stage; the CTA's barriers are uniform (groups without a brick skip the work).
+  constexpr int NG = 256 / GROUP;
+  __shared__ int nslotAll[NG][27];
+  __shared__ int needAll[NG][8];  // bit k of the index: -1 on axis k
+  extern __shared__ float stAll[];
+  const int g = threadIdx.x / GROUP, t = threadIdx.x % GROUP;
+  int* nslot = nslotAll[g];
+  int* need = needAll[g];
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
-  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+  for (uint32_t base = blockIdx.x * NG; base < total; base += gridDim.x * NG) {
+    uint32_t item = base + g;
+    const bool has = item < total;
     uint32_t i;
-    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, has ? item : base, i);
     const Args A = resolve(P, Sl);
     const int bl = P.brickLevels;
     const int fineLevel = OP == RESTRICT ? A.level - 1 : A.level;
@@ -225,128 +234,139 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
     // neighbours of the interpolation's coarse cells.
     const int R = OP == PROLONG ? 2 : 1;
     const int S = sb + 2 * R, S2 = S * S, S3 = S2 * S;
+    float* st = stAll + g * (S3 + (S3 + 3) / 4);
     uint8_t* solidSt = reinterpret_cast<uint8_t*>(st + S3);
     const float* src = OP == PROLONG ? A.coarse : A.pin;
     const int fs = levelShift(P, fineLevel), fside = 1 << fs, fcells = fside * fside * fside;
-    Home H = enterBrick(P, P.active[i], nslot);
-    if (threadIdx.x < 8) {
-      int dx = -(int)(threadIdx.x & 1), dy = -(int)((threadIdx.x >> 1) & 1), dz = -(int)(threadIdx.x >> 2);
-      bool below = P.ground && H.by + dy < 0;
-      need[threadIdx.x] = below || nslot[nbrIndex(dx, dy, dz)] >= 0;
-    }
+    const uint32_t id = has ? P.active[i] : 0u;
+    Home H = homeOf(P, id, nslot);
+    if (has && t < 27) nslot[t] = entryPage(P.records[(size_t)id * FP_RECORD_WORDS + t]);
+    __syncthreads();
     int ox = H.bx * sb - R, oy = H.by * sb - R, oz = H.bz * sb - R;
-    for (int q = threadIdx.x; q < S3; q += blockDim.x) {
-      int lx = q % S, ly = (q / S) % S, lz = q / S2;
-      long a = cellAddress(P, H, ox + lx, oy + ly, oz + lz, stageLevel);
-      st[q] = a < 0 ? 0.f : src[a];
-      if (OP == PROLONG) solidSt[q] = a >= 0 && (P.topo[stageLevel][a] & FP_STORED_SOLID) ? 1 : 0;
+    if (has) {
+      if (t < 8) {
+        int dx = -(t & 1), dy = -((t >> 1) & 1), dz = -(t >> 2);
+        bool below = P.ground && H.by + dy < 0;
+        need[t] = below || nslot[nbrIndex(dx, dy, dz)] >= 0;
+      }
+      for (int q = t; q < S3; q += GROUP) {
+        int lx = q % S, ly = (q / S) % S, lz = q / S2;
+        long a = cellAddress(P, H, ox + lx, oy + ly, oz + lz, stageLevel);
+        st[q] = a < 0 ? 0.f : src[a];
+        if (OP == PROLONG) solidSt[q] = a >= 0 && (P.topo[stageLevel][a] & FP_STORED_SOLID) ? 1 : 0;
+      }
     }
     __syncthreads();
-    // coarseValue (pressure.wgsl:670-696) from the stage.
-    auto ghost = [&](int cx, int cy, int cz) {
-      int groundY = P.ground ? 0 : -0x7fffffff;
-      int c[3] = {cx, max(cy, groundY), cz};
-      auto at = [&](int x, int y, int z) { return ((z - oz) * S + (y - oy)) * S + (x - ox); };
-      int ci = at(c[0], c[1], c[2]);
-      if (!solidSt[ci]) return st[ci];
-      float sum = 0.f, count = 0.f;
-      for (int axis = 0; axis < 3; axis++)
-        for (int side = -1; side <= 1; side += 2) {
-          int q[3] = {c[0], c[1], c[2]};
-          q[axis] += side;
-          q[1] = max(q[1], groundY);
-          int qi = at(q[0], q[1], q[2]);
-          if (!solidSt[qi]) {
-            sum += st[qi];
-            count += 1.f;
-          }
-        }
-      return sum / fmaxf(count, 1.f);
-    };
-    long slot = nslot[13];
-    // Whether the fine-level cell at local (lx,ly,lz) of this brick is a pressure unknown.
-    auto unknown = [&](int lx, int ly, int lz) {
-      for (int k = 1; k < 8; k++) {
-        if ((k & 1) && lx != 0) continue;
-        if ((k & 2) && ly != 0) continue;
-        if ((k & 4) && lz != 0) continue;
-        if (!need[k]) return false;
-      }
-      return (bool)need[0];
-    };
-    // Stencil sum of the open sides of a fine cell, from the stage (RELAX, RESTRICT).
-    auto sumAt = [&](int lx, int ly, int lz, uint32_t f) {
-      int c = ((lz + 1) * S + (ly + 1)) * S + (lx + 1);
-      float v0 = (f & 1u) ? st[c + 1] : 0.f, v1 = (f & 2u) ? st[c - 1] : 0.f;
-      float v2 = (f & 4u) ? st[c + S] : 0.f, v3 = (f & 8u) ? st[c - S] : 0.f;
-      float v4 = (f & 16u) ? st[c + S2] : 0.f, v5 = (f & 32u) ? st[c - S2] : 0.f;
-      return (v0 + v1) + (v2 + v3) + (v4 + v5);
-    };
-    if (OP == RELAX || OP == PROLONG) {
-      for (int o = threadIdx.x; o < fcells; o += blockDim.x) {
-        int lx = o & (fside - 1), ly = (o >> fs) & (fside - 1), lz = o >> (2 * fs);
-        long a = slot * fcells + o;
-        uint32_t f = expandFlags(P.topo[fineLevel][a]);
-        if ((f & SOLIDF) || !unknown(lx, ly, lz)) {
-          A.pout[a] = 0.f;
-          continue;
-        }
-        if (OP == RELAX) {
-          float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
-          float cand = (sumAt(lx, ly, lz, f) - A.rhs[a]) / fmaxf(diagOf(f), 1e-12f);
-          A.pout[a] = mixf(center, cand, 0.8f);
-        } else {
-          int px = H.bx * fside + lx, py = H.by * fside + ly, pz = H.bz * fside + lz;
-          float qx = ((float)px + 0.5f) * 0.5f - 0.5f, qy = ((float)py + 0.5f) * 0.5f - 0.5f,
-                qz = ((float)pz + 0.5f) * 0.5f - 0.5f;
-          int ix = (int)floorf(qx), iy = (int)floorf(qy), iz = (int)floorf(qz);
-          float fx = qx - floorf(qx), fy = qy - floorf(qy), fz = qz - floorf(qz);
-          bool fast = P.colliderCount == 0 && (!P.ground || iy >= 0);
-          float v[8];
-#pragma unroll
-          for (int k = 0; k < 8; k++) {
-            int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
-            v[k] = fast ? st[((iz + dz - oz) * S + (iy + dy - oy)) * S + (ix + dx - ox)]
-                        : ghost(ix + dx, iy + dy, iz + dz);
-          }
-          float corr = mixf(mixf(mixf(v[0], v[1], fx), mixf(v[2], v[3], fx), fy),
-                            mixf(mixf(v[4], v[5], fx), mixf(v[6], v[7], fx), fy), fz);
-          A.pout[a] = A.pin[a] + corr;
-        }
-      }
-    } else {  // RESTRICT: coarse cells of this brick at A.level
-      int cs = fs - 1, cside = fside >> 1, ccells = cside * cside * cside;
-      for (int o = threadIdx.x; o < ccells; o += blockDim.x) {
-        int cx = o & (cside - 1), cy = (o >> cs) & (cside - 1), cz = o >> (2 * cs);
-        float residual = 0.f;
-        bool every = true;
-        for (int k = 0; k < 8; k++) {
-          int lx = cx * 2 + (k & 1), ly = cy * 2 + ((k >> 1) & 1), lz = cz * 2 + (k >> 2);
-          bool u = unknown(lx, ly, lz);
-          every = every && u;
-          if (u) {
-            long a = slot * fcells + (((lz << fs) | ly) << fs | lx);
-            uint32_t f = expandFlags(P.topo[fineLevel][a]);
-            if (!(f & SOLIDF)) {
-              float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
-              residual += A.rhs[a] - (sumAt(lx, ly, lz, f) - diagOf(f) * center);
+    if (has) {
+      // coarseValue (pressure.wgsl:670-696) from the stage.
+      auto ghost = [&](int cx, int cy, int cz) {
+        int groundY = P.ground ? 0 : -0x7fffffff;
+        int c[3] = {cx, max(cy, groundY), cz};
+        auto at = [&](int x, int y, int z) { return ((z - oz) * S + (y - oy)) * S + (x - ox); };
+        int ci = at(c[0], c[1], c[2]);
+        if (!solidSt[ci]) return st[ci];
+        float sum = 0.f, count = 0.f;
+        for (int axis = 0; axis < 3; axis++)
+          for (int side = -1; side <= 1; side += 2) {
+            int q[3] = {c[0], c[1], c[2]};
+            q[axis] += side;
+            q[1] = max(q[1], groundY);
+            int qi = at(q[0], q[1], q[2]);
+            if (!solidSt[qi]) {
+              sum += st[qi];
+              count += 1.f;
             }
           }
+        return sum / fmaxf(count, 1.f);
+      };
+      long slot = nslot[13];
+      // Whether the fine-level cell at local (lx,ly,lz) of this brick is a pressure unknown.
+      auto unknown = [&](int lx, int ly, int lz) {
+        for (int k = 1; k < 8; k++) {
+          if ((k & 1) && lx != 0) continue;
+          if ((k & 2) && ly != 0) continue;
+          if ((k & 4) && lz != 0) continue;
+          if (!need[k]) return false;
         }
-        float r = residual * 0.5f;
-        long out = slot * ccells + o;
-        A.pout[out] = r;
-        float first = 0.f;
-        if (every) {
-          uint32_t f = expandFlags(P.topo[A.level][out]);
-          if (!(f & SOLIDF)) first = mixf(0.f, (0.f - r) / fmaxf(diagOf(f), 1e-12f), 0.8f);
+        return (bool)need[0];
+      };
+      // Stencil sum of the open sides of a fine cell, from the stage (RELAX, RESTRICT).
+      auto sumAt = [&](int lx, int ly, int lz, uint32_t f) {
+        int c = ((lz + 1) * S + (ly + 1)) * S + (lx + 1);
+        float v0 = (f & 1u) ? st[c + 1] : 0.f, v1 = (f & 2u) ? st[c - 1] : 0.f;
+        float v2 = (f & 4u) ? st[c + S] : 0.f, v3 = (f & 8u) ? st[c - S] : 0.f;
+        float v4 = (f & 16u) ? st[c + S2] : 0.f, v5 = (f & 32u) ? st[c - S2] : 0.f;
+        return (v0 + v1) + (v2 + v3) + (v4 + v5);
+      };
+      if (OP == RELAX || OP == PROLONG) {
+        for (int o = t; o < fcells; o += GROUP) {
+          int lx = o & (fside - 1), ly = (o >> fs) & (fside - 1), lz = o >> (2 * fs);
+          long a = slot * fcells + o;
+          uint32_t f = expandFlags(P.topo[fineLevel][a]);
+          if ((f & SOLIDF) || !unknown(lx, ly, lz)) {
+            A.pout[a] = 0.f;
+            continue;
+          }
+          if (OP == RELAX) {
+            float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
+            float cand = (sumAt(lx, ly, lz, f) - A.rhs[a]) / fmaxf(diagOf(f), 1e-12f);
+            A.pout[a] = mixf(center, cand, 0.8f);
+          } else {
+            int px = H.bx * fside + lx, py = H.by * fside + ly, pz = H.bz * fside + lz;
+            float qx = ((float)px + 0.5f) * 0.5f - 0.5f, qy = ((float)py + 0.5f) * 0.5f - 0.5f,
+                  qz = ((float)pz + 0.5f) * 0.5f - 0.5f;
+            int ix = (int)floorf(qx), iy = (int)floorf(qy), iz = (int)floorf(qz);
+            float fx = qx - floorf(qx), fy = qy - floorf(qy), fz = qz - floorf(qz);
+            bool fast = P.colliderCount == 0 && (!P.ground || iy >= 0);
+            float v[8];
+  #pragma unroll
+            for (int k = 0; k < 8; k++) {
+              int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
+              v[k] = fast ? st[((iz + dz - oz) * S + (iy + dy - oy)) * S + (ix + dx - ox)]
+                          : ghost(ix + dx, iy + dy, iz + dz);
+            }
+            float corr = mixf(mixf(mixf(v[0], v[1], fx), mixf(v[2], v[3], fx), fy),
+                              mixf(mixf(v[4], v[5], fx), mixf(v[6], v[7], fx), fy), fz);
+            A.pout[a] = A.pin[a] + corr;
+          }
         }
-        A.cfirst[out] = first;
+      } else {  // RESTRICT: coarse cells of this brick at A.level
+        int cs = fs - 1, cside = fside >> 1, ccells = cside * cside * cside;
+        for (int o = t; o < ccells; o += GROUP) {
+          int cx = o & (cside - 1), cy = (o >> cs) & (cside - 1), cz = o >> (2 * cs);
+          float residual = 0.f;
+          bool every = true;
+          for (int k = 0; k < 8; k++) {
+            int lx = cx * 2 + (k & 1), ly = cy * 2 + ((k >> 1) & 1), lz = cz * 2 + (k >> 2);
+            bool u = unknown(lx, ly, lz);
+            every = every && u;
+            if (u) {
+              long a = slot * fcells + (((lz << fs) | ly) << fs | lx);
+              uint32_t f = expandFlags(P.topo[fineLevel][a]);
+              if (!(f & SOLIDF)) {
+                float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
+                residual += A.rhs[a] - (sumAt(lx, ly, lz, f) - diagOf(f) * center);
+              }
+            }
+          }
+          float r = residual * 0.5f;
+          long out = slot * ccells + o;
+          A.pout[out] = r;
+          float first = 0.f;
+          if (every) {
+            uint32_t f = expandFlags(P.topo[A.level][out]);
+            if (!(f & SOLIDF)) first = mixf(0.f, (0.f - r) / fmaxf(diagOf(f), 1e-12f), 0.8f);
+          }
+          A.cfirst[out] = first;
+        }
       }
     }
     __syncthreads();
   }
 }
+
+// Threads per brick of the staged kernels for a level of `cells` cells per brick.
+static int groupFor(int cells) { return cells >= 256 ? 256 : (cells >= 64 ? 64 : 32); }
 
 FP_DEV Home enterTile(const SimParams& P, int t, int4 rec) {
   Home H;
@@ -487,6 +507,25 @@ __global__ void __launch_bounds__(128) k_topo_bricks(FpBatch bt) {
     // The brick's neighbour slots in shared memory: every solid test stays within them.
     Home H = enterBrick(P, id, nslot);
     int bx = H.bx, by = H.by, bz = H.bz;
+    // Away from the ground, a brick whose neighbourhood holds no solid cell has every side of
+    // every cell open at every brick level: cellTopology would return 63 throughout.
+    bool solidNear = P.ground && by == 0;
+    if (!solidNear && P.colliderCount > 0) {
+      bool any = false;
+      for (int q = threadIdx.x; q < 27 * P.W; q += blockDim.x) {
+        int s = nslot[q / P.W];
+        if (s >= 0 && P.solids[(size_t)s * P.W + q % P.W] != 0u) any = true;
+      }
+      solidNear = __syncthreads_or(any) != 0;
+    }
+    if (!solidNear) {
+      for (int level = 0; level < P.brickLevels; level++) {
+        int s = levelShift(P, level), cells = 1 << (3 * s);
+        for (int o = threadIdx.x; o < cells; o += blockDim.x) P.topo[level][(size_t)slot * cells + o] = 63;
+      }
+      __syncthreads();
+      continue;
+    }
     for (int level = 0; level < P.brickLevels; level++) {
       int s = levelShift(P, level), side = 1 << s, cells = side * side * side;
       for (int o = threadIdx.x; o < cells; o += blockDim.x) {
@@ -530,36 +569,61 @@ void fp_launch_topology(const FpBatch& bt, bool anyAll, int sms, cudaStream_t st
   }
 }
 
-// Shared memory of the staged brick-level kernels: the largest brick size configured so far.
-static size_t g_stageBytes = 0;
 static const int BOTTOM_SMEM = 200 * 1024;
+static const int STAGE_SMEM_MAX = 64 * 1024;
+
+template <int OP>
+static void allowStage() {
+  cudaFuncSetAttribute(k_level_bricks_staged<OP, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM_MAX);
+  cudaFuncSetAttribute(k_level_bricks_staged<OP, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM_MAX);
+  cudaFuncSetAttribute(k_level_bricks_staged<OP, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM_MAX);
+}
 void fp_mg_configure(int B) {
-  size_t relax = (size_t)(B + 2) * (B + 2) * (B + 2) * sizeof(float);
-  size_t prolong = (size_t)(B / 2 + 4) * (B / 2 + 4) * (B / 2 + 4) * (sizeof(float) + 1);
-  size_t bytes = relax > prolong ? relax : prolong;
-  if (bytes <= g_stageBytes) return;
-  g_stageBytes = bytes;
-  cudaFuncSetAttribute(k_level_bricks_staged<RELAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  cudaFuncSetAttribute(k_level_bricks_staged<RESTRICT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  cudaFuncSetAttribute(k_level_bricks_staged<PROLONG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  (void)B;
+  allowStage<RELAX>();
+  allowStage<RESTRICT>();
+  allowStage<PROLONG>();
   cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, BOTTOM_SMEM);
 }
 
+// The staged kernel's group size and shared memory for an operation whose output level is
+// `level`, in bricks of B cells: the same arithmetic as the kernel's.
 template <int OP>
-static void levelLaunch(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st) {
-  if (tiles)
+static size_t stageLayout(int level, int B, int& group) {
+  int bl = B == 8 ? 3 : 4;
+  auto shift = [&](int l) { return l < bl ? bl - l : bl + 2 - l; };
+  int fine = OP == RESTRICT ? level - 1 : level;
+  int stage = OP == PROLONG ? level + 1 : fine;
+  int sb = stage < bl ? 1 << shift(stage) : 1;
+  int R = OP == PROLONG ? 2 : 1;
+  int S = sb + 2 * R, S3 = S * S * S;
+  group = groupFor(1 << (3 * shift(fine)));
+  return (size_t)(256 / group) * (size_t)(S3 + (S3 + 3) / 4) * sizeof(float);
+}
+
+template <int OP>
+static void levelLaunch(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st) {
+  if (tiles) {
     k_level_tiles<OP><<<sms * 8, 64, 0, st>>>(bt, S);
+    return;
+  }
+  int group;
+  size_t smem = stageLayout<OP>(S.level, B, group);
+  if (group == 256)
+    k_level_bricks_staged<OP, 256><<<sms * 4, 256, smem, st>>>(bt, S);
+  else if (group == 64)
+    k_level_bricks_staged<OP, 64><<<sms * 4, 256, smem, st>>>(bt, S);
   else
-    k_level_bricks_staged<OP><<<sms * 4, 256, g_stageBytes, st>>>(bt, S);
+    k_level_bricks_staged<OP, 32><<<sms * 4, 256, smem, st>>>(bt, S);
 }
-void fp_launch_relax(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st) {
-  levelLaunch<RELAX>(bt, S, tiles, sms, st);
+void fp_launch_relax(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st) {
+  levelLaunch<RELAX>(bt, S, tiles, B, sms, st);
 }
-void fp_launch_restrict(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st) {
-  levelLaunch<RESTRICT>(bt, S, tiles, sms, st);
+void fp_launch_restrict(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st) {
+  levelLaunch<RESTRICT>(bt, S, tiles, B, sms, st);
 }
-void fp_launch_prolong(const FpBatch& bt, const MgSel& S, bool tiles, int sms, cudaStream_t st) {
-  levelLaunch<PROLONG>(bt, S, tiles, sms, st);
+void fp_launch_prolong(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st) {
+  levelLaunch<PROLONG>(bt, S, tiles, B, sms, st);
 }
 void fp_launch_bottom(const FpBatch& bt, const MgSel& S, int iterations, int sms, cudaStream_t st) {
   k_bottom<<<sms, 1024, BOTTOM_SMEM, st>>>(bt, S, iterations, BOTTOM_SMEM);

@@ -216,6 +216,9 @@ void schedule(fp_server* S) {
       fp::Engine* e = new (std::nothrow) fp::Engine(s->grid, S->stepper);
       int rc = e ? e->initialize() : FP_ENOMEM;
       if (!rc) rc = e->setRuntime(s->cutoff, s->grid.voxel_budget, s->ground);
+      // Tables sized for the budget up front: no step of the batch stops to grow them.
+      int cells = s->grid.brick_size * s->grid.brick_size * s->grid.brick_size;
+      if (!rc) rc = e->reserveTiles(fp::Engine::tilesForBudget(s->grid.voxel_budget, cells));
       std::lock_guard<std::mutex> lk(S->mu);
       if (rc) {
         S->error = e ? e->error() : "out of host memory";

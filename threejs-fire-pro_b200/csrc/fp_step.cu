@@ -153,182 +153,194 @@ FP_DEV void cellOf(const SimParams& P, const Home& H, int c, int& x, int& y, int
 // advectScalars (fluid-scalar-transport.wgsl:38-142), fused: both read only the velocity and
 // the scalars at the start of the step.
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS, 3) k_predict(FpBatch bt) {
+FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
   extern __shared__ float smem[];
+  const SimParams& P = *Pp;
+  uint32_t id = P.active[i];
+  Home H = enterBrick(P, id, nslot);
+  Stage G = stageOf(P, H, STAGED);
+  Field V{P.vel, 3, STAGED ? smem : nullptr};
+  Field F{P.fld, 4, STAGED ? smem + 3 * G.S3 : nullptr};
+  if (STAGED) {
+    stageField(P, H, G, smem, P.vel, 3);
+    stageField(P, H, G, smem + 3 * G.S3, P.fld, 4);
+    stageWait();
+  }
+  size_t slot = (size_t)nslot[13];
+  const size_t N = P.N;
+  for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+    int x, y, z;
+    cellOf(P, H, c, x, y, z);
+    // Velocity bounds over the forward 2x2x2 block.
+    for (int k = 0; k < 3; k++) {
+      float lo = 1e5f, hi = -1e5f;
+      for (int dz = 0; dz < 2; dz++)
+        for (int dy = 0; dy < 2; dy++)
+          for (int dx = 0; dx < 2; dx++) {
+            float v = fieldCell(P, H, G, V, k, x + dx, y + dy, z + dz);
+            lo = fminf(lo, v);
+            hi = fmaxf(hi, v);
+          }
+      P.vmin[(slot * 3 + k) * N + c] = lo;
+      P.vmax[(slot * 3 + k) * N + c] = hi;
+    }
+    float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+    if (solidAt(P, H, px, py, pz)) {
+      for (int k = 0; k < 3; k++) P.velP[(slot * 3 + k) * N + c] = 0.f;
+    } else {
+      float3 orig = make_float3(fieldCell(P, H, G, V, 0, x, y, z), fieldCell(P, H, G, V, 1, x, y, z),
+                                fieldCell(P, H, G, V, 2, x, y, z));
+#pragma unroll
+      for (int comp = 0; comp < 3; comp++) {
+        float face[3] = {px, py, pz};
+        face[comp] += 0.5f * P.h;
+        float3 fv = velocityOnFace(P, H, G, V, x, y, z, comp, orig);
+        float3 vm = velocityAt(P, H, G, V, face[0] - 0.5f * P.dt * fv.x, face[1] - 0.5f * P.dt * fv.y,
+                               face[2] - 0.5f * P.dt * fv.z);
+        float dep[3] = {face[0] - P.dt * vm.x, face[1] - P.dt * vm.y, face[2] - P.dt * vm.z};
+        float sh[3] = {dep[0], dep[1], dep[2]};
+        sh[comp] -= 0.5f * P.h;
+        // Divided, not multiplied by 1/h: still air lands exactly on a cell boundary here and
+        // the donor cell is an integer decision the oracle repeats.
+        int bx = (int)floorf(sh[0] / P.h - 0.5f), by = (int)floorf(sh[1] / P.h - 0.5f),
+            bz = (int)floorf(sh[2] / P.h - 0.5f);
+        P.donors[(slot * 3 + comp) * N + c] = (uint16_t)packDonor(bx - x, by - y, bz - z);
+        P.velP[(slot * 3 + comp) * N + c] = velComp(P, H, G, V, dep[0], dep[1], dep[2], comp);
+      }
+    }
+    // Scalars: a cell-centred RK2 back trace, the predictor and its donors' range.
+    float3 cv = velocityAt(P, H, G, V, px, py, pz);
+    float3 vm = velocityAt(P, H, G, V, px - 0.5f * P.dt * cv.x, py - 0.5f * P.dt * cv.y, pz - 0.5f * P.dt * cv.z);
+    float dx_ = px - P.dt * vm.x, dy_ = py - P.dt * vm.y, dz_ = pz - P.dt * vm.z;
+    float out[4];
+    if (!P.maccormack) {
+      for (int k = 0; k < 4; k++) out[k] = fieldSample(P, H, G, F, k, dx_ / P.h, dy_ / P.h, dz_ / P.h);
+      out[2] = clamp01(out[2]);
+    } else {
+      float dc[3] = {(float)x + (dx_ - px) / P.h, (float)y + (dy_ - py) / P.h, (float)z + (dz_ - pz) / P.h};
+      int base[3];
+      float fr[3];
+      for (int a = 0; a < 3; a++) {
+        base[a] = (int)floorf(dc[a]);
+        fr[a] = dc[a] - floorf(dc[a]);
+      }
+      float mn0 = 65504.f, mn1 = 65504.f, mn3 = 65504.f, mx0 = -65504.f, mx1 = -65504.f, mx3 = -65504.f;
+      float lmin = 1.f, lmax = 0.f;
+      float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
+      for (int dz = 0; dz < 2; dz++)
+        for (int dy = 0; dy < 2; dy++)
+          for (int dx = 0; dx < 2; dx++) {
+            int cx = base[0] + dx, cy = base[1] + dy, cz = base[2] + dz;
+            float s0 = fieldCell(P, H, G, F, 0, cx, cy, cz), s1 = fieldCell(P, H, G, F, 1, cx, cy, cz),
+                  s2 = fieldCell(P, H, G, F, 2, cx, cy, cz), s3 = fieldCell(P, H, G, F, 3, cx, cy, cz);
+            mn0 = fminf(mn0, s0); mn1 = fminf(mn1, s1); mn3 = fminf(mn3, s3);
+            mx0 = fmaxf(mx0, s0); mx1 = fmaxf(mx1, s1); mx3 = fmaxf(mx3, s3);
+            lmin = fminf(lmin, s2);
+            lmax = fmaxf(lmax, s2);
+            float w = (dx ? fr[0] : 1.f - fr[0]) * (dy ? fr[1] : 1.f - fr[1]) * (dz ? fr[2] : 1.f - fr[2]);
+            v0 += s0 * w; v1 += s1 * w; v2 += s2 * w; v3 += s3 * w;
+          }
+      float* b = P.sb + slot * 8 * N;
+      b[0 * N + c] = mn0; b[1 * N + c] = mn1; b[2 * N + c] = mn3; b[3 * N + c] = lmin;
+      b[4 * N + c] = mx0; b[5 * N + c] = mx1; b[6 * N + c] = mx3; b[7 * N + c] = lmax;
+      out[0] = v0;
+      out[1] = v1;
+      out[2] = P.lifetimeZero ? 0.f : v2;
+      out[3] = v3;
+    }
+    for (int k = 0; k < 4; k++) P.fldP[(slot * 4 + k) * N + c] = out[k];
+  }
+  __syncthreads();
+}
+template <bool STAGED>
+__global__ void __launch_bounds__(THREADS, 3) k_predict(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    uint32_t id = P.active[i];
-    Home H = enterBrick(P, id, nslot);
-    Stage G = stageOf(P, H, STAGED);
-    Field V{P.vel, 3, STAGED ? smem : nullptr};
-    Field F{P.fld, 4, STAGED ? smem + 3 * G.S3 : nullptr};
-    if (STAGED) {
-      stageField(P, H, G, smem, P.vel, 3);
-      stageField(P, H, G, smem + 3 * G.S3, P.fld, 4);
-      stageWait();
-    }
-    size_t slot = (size_t)nslot[13];
-    const size_t N = P.N;
-    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
-      int x, y, z;
-      cellOf(P, H, c, x, y, z);
-      // Velocity bounds over the forward 2x2x2 block.
-      for (int k = 0; k < 3; k++) {
-        float lo = 1e5f, hi = -1e5f;
-        for (int dz = 0; dz < 2; dz++)
-          for (int dy = 0; dy < 2; dy++)
-            for (int dx = 0; dx < 2; dx++) {
-              float v = fieldCell(P, H, G, V, k, x + dx, y + dy, z + dz);
-              lo = fminf(lo, v);
-              hi = fmaxf(hi, v);
-            }
-        P.vmin[(slot * 3 + k) * N + c] = lo;
-        P.vmax[(slot * 3 + k) * N + c] = hi;
-      }
-      float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-      if (solidAt(P, H, px, py, pz)) {
-        for (int k = 0; k < 3; k++) P.velP[(slot * 3 + k) * N + c] = 0.f;
-      } else {
-        float3 orig = make_float3(fieldCell(P, H, G, V, 0, x, y, z), fieldCell(P, H, G, V, 1, x, y, z),
-                                  fieldCell(P, H, G, V, 2, x, y, z));
-#pragma unroll
-        for (int comp = 0; comp < 3; comp++) {
-          float face[3] = {px, py, pz};
-          face[comp] += 0.5f * P.h;
-          float3 fv = velocityOnFace(P, H, G, V, x, y, z, comp, orig);
-          float3 vm = velocityAt(P, H, G, V, face[0] - 0.5f * P.dt * fv.x, face[1] - 0.5f * P.dt * fv.y,
-                                 face[2] - 0.5f * P.dt * fv.z);
-          float dep[3] = {face[0] - P.dt * vm.x, face[1] - P.dt * vm.y, face[2] - P.dt * vm.z};
-          float sh[3] = {dep[0], dep[1], dep[2]};
-          sh[comp] -= 0.5f * P.h;
-          int bx = (int)floorf(sh[0] / P.h - 0.5f), by = (int)floorf(sh[1] / P.h - 0.5f),
-              bz = (int)floorf(sh[2] / P.h - 0.5f);
-          P.donors[(slot * 3 + comp) * N + c] = (uint16_t)packDonor(bx - x, by - y, bz - z);
-          P.velP[(slot * 3 + comp) * N + c] = velComp(P, H, G, V, dep[0], dep[1], dep[2], comp);
-        }
-      }
-      // Scalars: a cell-centred RK2 back trace, the predictor and its donors' range.
-      float3 cv = velocityAt(P, H, G, V, px, py, pz);
-      float3 vm = velocityAt(P, H, G, V, px - 0.5f * P.dt * cv.x, py - 0.5f * P.dt * cv.y, pz - 0.5f * P.dt * cv.z);
-      float dx_ = px - P.dt * vm.x, dy_ = py - P.dt * vm.y, dz_ = pz - P.dt * vm.z;
-      float out[4];
-      if (!P.maccormack) {
-        for (int k = 0; k < 4; k++) out[k] = fieldSample(P, H, G, F, k, dx_ / P.h, dy_ / P.h, dz_ / P.h);
-        out[2] = clamp01(out[2]);
-      } else {
-        float dc[3] = {(float)x + (dx_ - px) / P.h, (float)y + (dy_ - py) / P.h, (float)z + (dz_ - pz) / P.h};
-        int base[3];
-        float fr[3];
-        for (int a = 0; a < 3; a++) {
-          base[a] = (int)floorf(dc[a]);
-          fr[a] = dc[a] - floorf(dc[a]);
-        }
-        float mn0 = 65504.f, mn1 = 65504.f, mn3 = 65504.f, mx0 = -65504.f, mx1 = -65504.f, mx3 = -65504.f;
-        float lmin = 1.f, lmax = 0.f;
-        float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
-        for (int dz = 0; dz < 2; dz++)
-          for (int dy = 0; dy < 2; dy++)
-            for (int dx = 0; dx < 2; dx++) {
-              int cx = base[0] + dx, cy = base[1] + dy, cz = base[2] + dz;
-              float s0 = fieldCell(P, H, G, F, 0, cx, cy, cz), s1 = fieldCell(P, H, G, F, 1, cx, cy, cz),
-                    s2 = fieldCell(P, H, G, F, 2, cx, cy, cz), s3 = fieldCell(P, H, G, F, 3, cx, cy, cz);
-              mn0 = fminf(mn0, s0); mn1 = fminf(mn1, s1); mn3 = fminf(mn3, s3);
-              mx0 = fmaxf(mx0, s0); mx1 = fmaxf(mx1, s1); mx3 = fmaxf(mx3, s3);
-              lmin = fminf(lmin, s2);
-              lmax = fmaxf(lmax, s2);
-              float w = (dx ? fr[0] : 1.f - fr[0]) * (dy ? fr[1] : 1.f - fr[1]) * (dz ? fr[2] : 1.f - fr[2]);
-              v0 += s0 * w; v1 += s1 * w; v2 += s2 * w; v3 += s3 * w;
-            }
-        float* b = P.sb + slot * 8 * N;
-        b[0 * N + c] = mn0; b[1 * N + c] = mn1; b[2 * N + c] = mn3; b[3 * N + c] = lmin;
-        b[4 * N + c] = mx0; b[5 * N + c] = mx1; b[6 * N + c] = mx3; b[7 * N + c] = lmax;
-        out[0] = v0;
-        out[1] = v1;
-        out[2] = P.lifetimeZero ? 0.f : v2;
-        out[3] = v3;
-      }
-      for (int k = 0; k < 4; k++) P.fldP[(slot * 4 + k) * N + c] = out[k];
-    }
-    __syncthreads();
+    brick_predict<STAGED>(&P, i);
   }
 }
 
 // ---------------------------------------------------------------------------------------
 // correctVelocity (fluid-velocity-transport.wgsl:104-179): bounded MacCormack correction.
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS, 3) k_correct(FpBatch bt) {
+FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
   extern __shared__ float smem[];
+  const SimParams& P = *Pp;
+  uint32_t id = P.active[i];
+  Home H = enterBrick(P, id, nslot);
+  Stage G = stageOf(P, H, STAGED);
+  Field V{P.vel, 3, STAGED ? smem : nullptr};
+  Field Vp{P.velP, 3, STAGED ? smem + 3 * G.S3 : nullptr};
+  if (STAGED) {
+    stageField(P, H, G, smem, P.vel, 3);
+    stageField(P, H, G, smem + 3 * G.S3, P.velP, 3);
+    stageWait();
+  }
+  size_t slot = (size_t)nslot[13];
+  const size_t N = P.N;
+  for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+    int x, y, z;
+    cellOf(P, H, c, x, y, z);
+    float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+    bool solid = solidAt(P, H, px, py, pz);
+    float3 orig = make_float3(fieldCell(P, H, G, V, 0, x, y, z), fieldCell(P, H, G, V, 1, x, y, z),
+                              fieldCell(P, H, G, V, 2, x, y, z));
+#pragma unroll
+    for (int comp = 0; comp < 3; comp++) {
+      float result = 0.f;
+      if (!solid) {
+        float predicted = fieldCell(P, H, G, Vp, comp, x, y, z);
+        float face[3] = {px, py, pz};
+        face[comp] += 0.5f * P.h;
+        uint32_t donor = P.donors[(slot * 3 + comp) * N + c];
+        bool retrace = donor == (1u << 15);
+        int base[3] = {x + (int)(donor & 31u) - 16, y + (int)((donor >> 5) & 31u) - 16,
+                       z + (int)((donor >> 10) & 31u) - 16};
+        float3 fv = make_float3(0.f, 0.f, 0.f);
+        if (retrace) {
+          fv = velocityOnFace(P, H, G, V, x, y, z, comp, orig);
+          float3 vm = velocityAt(P, H, G, V, face[0] - 0.5f * P.dt * fv.x, face[1] - 0.5f * P.dt * fv.y,
+                                 face[2] - 0.5f * P.dt * fv.z);
+          float dep[3] = {face[0] - P.dt * vm.x, face[1] - P.dt * vm.y, face[2] - P.dt * vm.z};
+          dep[comp] -= 0.5f * P.h;
+          for (int a = 0; a < 3; a++) base[a] = (int)floorf(dep[a] / P.h - 0.5f);  // as in the predictor
+        }
+        float lo = 0.f, hi = 0.f;
+        int bs = brickSlot(P, H, base[0] >> P.shift, base[1] >> P.shift, base[2] >> P.shift);
+        if (bs >= 0) {
+          int lc = localCell(P, base[0], base[1], base[2]);
+          lo = P.vmin[((size_t)bs * 3 + comp) * N + lc];
+          hi = P.vmax[((size_t)bs * 3 + comp) * N + lc];
+        }
+        if (lo == hi && predicted == lo) {
+          result = predicted;
+        } else {
+          if (!retrace) fv = velocityOnFace(P, H, G, V, x, y, z, comp, orig);
+          float3 vm = velocityAt(P, H, G, V, face[0] + 0.5f * P.dt * fv.x, face[1] + 0.5f * P.dt * fv.y,
+                                 face[2] + 0.5f * P.dt * fv.z);
+          float fw[3] = {face[0] + P.dt * vm.x, face[1] + P.dt * vm.y, face[2] + P.dt * vm.z};
+          fw[comp] -= 0.5f * P.h;
+          float reversed = fieldSample(P, H, G, Vp, comp, fw[0] / P.h, fw[1] / P.h, fw[2] / P.h);
+          float corrected = predicted + 0.5f * (get(orig, comp) - reversed);
+          result = (corrected < lo || corrected > hi) ? predicted : corrected;
+        }
+      }
+      P.velC[(slot * 3 + comp) * N + c] = result;
+    }
+  }
+  __syncthreads();
+}
+template <bool STAGED>
+__global__ void __launch_bounds__(THREADS, 3) k_correct(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    uint32_t id = P.active[i];
-    Home H = enterBrick(P, id, nslot);
-    Stage G = stageOf(P, H, STAGED);
-    Field V{P.vel, 3, STAGED ? smem : nullptr};
-    Field Vp{P.velP, 3, STAGED ? smem + 3 * G.S3 : nullptr};
-    if (STAGED) {
-      stageField(P, H, G, smem, P.vel, 3);
-      stageField(P, H, G, smem + 3 * G.S3, P.velP, 3);
-      stageWait();
-    }
-    size_t slot = (size_t)nslot[13];
-    const size_t N = P.N;
-    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
-      int x, y, z;
-      cellOf(P, H, c, x, y, z);
-      float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-      bool solid = solidAt(P, H, px, py, pz);
-      float3 orig = make_float3(fieldCell(P, H, G, V, 0, x, y, z), fieldCell(P, H, G, V, 1, x, y, z),
-                                fieldCell(P, H, G, V, 2, x, y, z));
-#pragma unroll
-      for (int comp = 0; comp < 3; comp++) {
-        float result = 0.f;
-        if (!solid) {
-          float predicted = fieldCell(P, H, G, Vp, comp, x, y, z);
-          float face[3] = {px, py, pz};
-          face[comp] += 0.5f * P.h;
-          uint32_t donor = P.donors[(slot * 3 + comp) * N + c];
-          bool retrace = donor == (1u << 15);
-          int base[3] = {x + (int)(donor & 31u) - 16, y + (int)((donor >> 5) & 31u) - 16,
-                         z + (int)((donor >> 10) & 31u) - 16};
-          float3 fv = make_float3(0.f, 0.f, 0.f);
-          if (retrace) {
-            fv = velocityOnFace(P, H, G, V, x, y, z, comp, orig);
-            float3 vm = velocityAt(P, H, G, V, face[0] - 0.5f * P.dt * fv.x, face[1] - 0.5f * P.dt * fv.y,
-                                   face[2] - 0.5f * P.dt * fv.z);
-            float dep[3] = {face[0] - P.dt * vm.x, face[1] - P.dt * vm.y, face[2] - P.dt * vm.z};
-            dep[comp] -= 0.5f * P.h;
-            for (int a = 0; a < 3; a++) base[a] = (int)floorf(dep[a] / P.h - 0.5f);
-          }
-          float lo = 0.f, hi = 0.f;
-          int bs = brickSlot(P, H, base[0] >> P.shift, base[1] >> P.shift, base[2] >> P.shift);
-          if (bs >= 0) {
-            int lc = localCell(P, base[0], base[1], base[2]);
-            lo = P.vmin[((size_t)bs * 3 + comp) * N + lc];
-            hi = P.vmax[((size_t)bs * 3 + comp) * N + lc];
-          }
-          if (lo == hi && predicted == lo) {
-            result = predicted;
-          } else {
-            if (!retrace) fv = velocityOnFace(P, H, G, V, x, y, z, comp, orig);
-            float3 vm = velocityAt(P, H, G, V, face[0] + 0.5f * P.dt * fv.x, face[1] + 0.5f * P.dt * fv.y,
-                                   face[2] + 0.5f * P.dt * fv.z);
-            float fw[3] = {face[0] + P.dt * vm.x, face[1] + P.dt * vm.y, face[2] + P.dt * vm.z};
-            fw[comp] -= 0.5f * P.h;
-            float reversed = fieldSample(P, H, G, Vp, comp, fw[0] / P.h, fw[1] / P.h, fw[2] / P.h);
-            float corrected = predicted + 0.5f * (get(orig, comp) - reversed);
-            result = (corrected < lo || corrected > hi) ? predicted : corrected;
-          }
-        }
-        P.velC[(slot * 3 + comp) * N + c] = result;
-      }
-    }
-    __syncthreads();
+    brick_correct<STAGED>(&P, i);
   }
 }
 
@@ -336,223 +348,232 @@ __global__ void __launch_bounds__(THREADS, 3) k_correct(FpBatch bt) {
 // evolveFields (fluid-field-evolution.wgsl:9-84) with correctedScalars
 // (fluid-scalar-transport.wgsl:144-199) and recordContent (fluid-content.wgsl:29-64).
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS, 3) k_evolve(FpBatch bt) {
+FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
   __shared__ uint32_t busyAll, expandsAll;
   extern __shared__ float smem[];
+  const SimParams& P = *Pp;
+  uint32_t id = P.active[i];
+  if (threadIdx.x == 0) {
+    busyAll = 0;
+    expandsAll = 0;
+  }
+  Home H = enterBrick(P, id, nslot);
+  Stage G = stageOf(P, H, STAGED);
+  Field V{P.vel, 3, STAGED ? smem : nullptr};
+  Field Fp{P.fldP, 4, STAGED ? smem + 3 * G.S3 : nullptr};
+  if (STAGED) {
+    stageField(P, H, G, smem, P.vel, 3);
+    stageField(P, H, G, smem + 3 * G.S3, P.fldP, 4);
+    stageWait();
+  }
+  size_t slot = (size_t)nslot[13];
+  const size_t N = P.N;
+  int tile = (int)(id >> 6);
+  uint32_t busy = 0;
+  bool expands = false;
+  for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+    int x, y, z;
+    cellOf(P, H, c, x, y, z);
+    float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+    bool solid = solidAt(P, H, px, py, pz);
+    float value[4] = {0.f, 0.f, 0.f, 0.f};
+    float expansion = 0.f;
+    bool injected = false;
+    bool cvSampled = false;
+    float3 cv = make_float3(0.f, 0.f, 0.f);
+    if (!solid) {
+      float tr[4];
+      if (!P.maccormack) {
+        for (int k = 0; k < 4; k++) tr[k] = fieldCell(P, H, G, Fp, k, x, y, z);
+      } else {
+        const float* b = P.sb + slot * 8 * N;
+        float mn0 = b[0 * N + c], mn1 = b[1 * N + c], mn3 = b[2 * N + c], lmin = b[3 * N + c];
+        float mx0 = b[4 * N + c], mx1 = b[5 * N + c], mx3 = b[6 * N + c], lmax = b[7 * N + c];
+        if (mn0 == mx0 && mn1 == mx1 && mn3 == mx3 && lmin == lmax) {
+          tr[0] = mn0;
+          tr[1] = mn1;
+          tr[2] = clamp01(lmin);
+          tr[3] = mn3;
+        } else {
+          float a0 = fieldCell(P, H, G, Fp, 0, x, y, z), a1 = fieldCell(P, H, G, Fp, 1, x, y, z),
+                a2 = fieldCell(P, H, G, Fp, 2, x, y, z), a3 = fieldCell(P, H, G, Fp, 3, x, y, z);
+          cv = velocityAt(P, H, G, V, px, py, pz);
+          cvSampled = true;
+          float3 vm = velocityAt(P, H, G, V, px + 0.5f * P.dt * cv.x, py + 0.5f * P.dt * cv.y, pz + 0.5f * P.dt * cv.z);
+          float fx = px + P.dt * vm.x, fy = py + P.dt * vm.y, fz = pz + P.dt * vm.z;
+          const float* o = P.fld + slot * 4 * N;
+          float o0 = o[0 * N + c], o1 = o[1 * N + c], o2 = o[2 * N + c], o3 = o[3 * N + c];
+          float lifetime = a2;
+          float r0, r1, r3;
+          if (lmin != lmax || a2 != lmin) {
+            float fc[3] = {(float)x + (fx - px) / P.h, (float)y + (fy - py) / P.h, (float)z + (fz - pz) / P.h};
+            int base[3];
+            float fr[3];
+            for (int a = 0; a < 3; a++) {
+              base[a] = (int)floorf(fc[a]);
+              fr[a] = fc[a] - floorf(fc[a]);
+            }
+            float rs0 = 0.f, rs1 = 0.f, rs2 = 0.f, rs3 = 0.f;
+            for (int dz = 0; dz < 2; dz++)
+              for (int dy = 0; dy < 2; dy++)
+                for (int dx = 0; dx < 2; dx++) {
+                  int cx = base[0] + dx, cy = base[1] + dy, cz = base[2] + dz;
+                  float w = (dx ? fr[0] : 1.f - fr[0]) * (dy ? fr[1] : 1.f - fr[1]) * (dz ? fr[2] : 1.f - fr[2]);
+                  rs0 += fieldCell(P, H, G, Fp, 0, cx, cy, cz) * w;
+                  rs1 += fieldCell(P, H, G, Fp, 1, cx, cy, cz) * w;
+                  rs2 += fieldCell(P, H, G, Fp, 2, cx, cy, cz) * w;
+                  rs3 += fieldCell(P, H, G, Fp, 3, cx, cy, cz) * w;
+                }
+            r0 = rs0;
+            r1 = rs1;
+            r3 = rs3;
+            float cl = a2 + 0.5f * (o2 - rs2);
+            lifetime = (cl < lmin || cl > lmax) ? a2 : cl;
+          } else {
+            r0 = fieldSample(P, H, G, Fp, 0, fx / P.h, fy / P.h, fz / P.h);
+            r1 = fieldSample(P, H, G, Fp, 1, fx / P.h, fy / P.h, fz / P.h);
+            r3 = fieldSample(P, H, G, Fp, 3, fx / P.h, fy / P.h, fz / P.h);
+          }
+          float c0 = a0 + 0.5f * (o0 - r0), c1 = a1 + 0.5f * (o1 - r1), c3 = a3 + 0.5f * (o3 - r3);
+          tr[0] = (c0 < mn0 || c0 > mx0) ? a0 : c0;
+          tr[1] = (c1 < mn1 || c1 > mx1) ? a1 : c1;
+          tr[2] = clamp01(lifetime);
+          tr[3] = (c3 < mn3 || c3 > mx3) ? a3 : c3;
+        }
+      }
+      float lifetime = tr[2];
+      float prodS = 0.f, prodH = 0.f, injectedFuel = 0.f;
+      uint2 list = tileList(P, tile, 0);
+      for (uint32_t j = 0; j < list.y; j++) {
+        const FpEmitter& e = P.emitters[P.tileLists[list.x + j]];
+        float w = emitterWeight(e, px, py, pz);
+        if (w == 0.f) continue;
+        float2 var = burstVariation(e, px, py, pz, P.seedBits);
+        lifetime = fmaxf(lifetime, e.flame * w * var.y);
+        prodS += e.smoke * w * P.dt;
+        prodH += e.heat * var.x * w * P.dt;
+        injectedFuel += e.fuel * w * P.dt;
+      }
+      float remaining = 0.f, burned = 0.f;
+      if (P.fuelEnabled) {
+        remaining = tr[3] + injectedFuel;
+        if (tr[1] + prodH >= P.ignition) {
+          lifetime = fmaxf(lifetime, fminf(remaining, 1.f));
+          float unburned = remaining * expf(-P.burnRate * P.dt);
+          burned = remaining - unburned;
+          remaining = unburned;
+        }
+      }
+      // evaluateFlame (flame-common.wgsl:30-42)
+      float before = clamp01(lifetime);
+      float after = 0.f, f0 = 0.f, f1 = 0.f, f2 = 0.f;
+      if (before > 0.f) {
+        const FpFlame& F = P.flame;
+        after = fmaxf(0.f, before - F.dt / F.lifespan);
+        f0 = F.smoke * F.lifespan * rampIntegral(F, 0, after, before);
+        f1 = F.heat * F.lifespan * rampIntegral(F, 1, after, before);
+        f2 = F.expansion * (F.lifespan * rampIntegral(F, 2, after, before) / F.dt);
+      }
+      expansion = f2 + P.flame.expansion * burned / P.dt;
+      float dS = tr[0] * expf(-P.dissipation * P.dt) + (prodS + f0) * expf(-P.dissipation * P.dt * 0.5f);
+      float dH = tr[1] * expf(-P.cooling * P.dt) + (prodH + f1) * expf(-P.cooling * P.dt * 0.5f);
+      value[0] = fmaxf(dS, 0.f);
+      value[1] = fmaxf(dH, 0.f);
+      value[2] = after;
+      value[3] = remaining;
+      injected = prodS > 0.f || prodH > 0.f || lifetime > tr[2] || injectedFuel > 0.f;
+    }
+    // clearDormant (fluid-common.wgsl:8-13)
+    if (!injected && value[2] == 0.f && value[0] < 0.001f && value[1] < 0.001f && value[3] < 0.001f)
+      value[0] = value[1] = value[2] = value[3] = 0.f;
+    for (int k = 0; k < 4; k++) P.fldN[(slot * 4 + k) * N + c] = value[k];
+    P.expn[slot * N + c] = expansion;
+    if (expansion != 0.f) expands = true;
+    // holdsContent and contentSupport (fluid-content.wgsl:22-39).
+    if (fmaxf(fmaxf(value[0], value[2]), value[3]) > P.cutoff) {
+      if (!cvSampled) cv = velocityAt(P, H, G, V, px, py, pz);
+      int idc[3] = {x, y, z};
+      float vv[3] = {cv.x, cv.y, cv.z};
+      bool low[3], high[3];
+      for (int a = 0; a < 3; a++) {
+        float side = (float)P.B;
+        float loc = (float)(idc[a] & (P.B - 1)) + 0.5f;
+        float pad = fminf(side, 2.f + fabsf(vv[a]) * P.dt / P.h);
+        low[a] = loc < pad;
+        high[a] = loc + pad >= side;
+      }
+      uint32_t row = 2u | (low[0] ? 1u : 0u) | (high[0] ? 4u : 0u);
+      uint32_t plane = (row << 3u) | (low[1] ? row : 0u) | (high[1] ? (row << 6u) : 0u);
+      busy |= (plane << 9u) | (low[2] ? plane : 0u) | (high[2] ? (plane << 18u) : 0u);
+    }
+  }
+  // recordContent (fluid-content.wgsl:43-64): one update per brick.
+  busy = __reduce_or_sync(0xffffffffu, busy);
+  uint32_t ex = __reduce_or_sync(0xffffffffu, (uint32_t)expands);
+  if ((threadIdx.x & 31) == 0) {
+    if (busy) atomicOr(&busyAll, busy);
+    if (ex) atomicOr(&expandsAll, 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t flags = 0;
+    if (busyAll) {
+      flags = FP_CONTENT | (busyAll << 3);
+      uint32_t l = id & 63u;
+      uint32_t bits = (1u << (l & 3u)) | (16u << ((l >> 2) & 3u)) | (256u << (l >> 4));
+      atomicOr(&P.activity[(size_t)P.capacity * 64u + (id >> 6)], bits);
+    }
+    if (expandsAll) flags |= FP_EXPANDS;
+    if (flags) P.activity[id] |= flags;
+  }
+  __syncthreads();
+}
+template <bool STAGED>
+__global__ void __launch_bounds__(THREADS, 3) k_evolve(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    uint32_t id = P.active[i];
-    if (threadIdx.x == 0) {
-      busyAll = 0;
-      expandsAll = 0;
-    }
-    Home H = enterBrick(P, id, nslot);
-    Stage G = stageOf(P, H, STAGED);
-    Field V{P.vel, 3, STAGED ? smem : nullptr};
-    Field Fp{P.fldP, 4, STAGED ? smem + 3 * G.S3 : nullptr};
-    if (STAGED) {
-      stageField(P, H, G, smem, P.vel, 3);
-      stageField(P, H, G, smem + 3 * G.S3, P.fldP, 4);
-      stageWait();
-    }
-    size_t slot = (size_t)nslot[13];
-    const size_t N = P.N;
-    int tile = (int)(id >> 6);
-    uint32_t busy = 0;
-    bool expands = false;
-    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
-      int x, y, z;
-      cellOf(P, H, c, x, y, z);
-      float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-      bool solid = solidAt(P, H, px, py, pz);
-      float value[4] = {0.f, 0.f, 0.f, 0.f};
-      float expansion = 0.f;
-      bool injected = false;
-      bool cvSampled = false;
-      float3 cv = make_float3(0.f, 0.f, 0.f);
-      if (!solid) {
-        float tr[4];
-        if (!P.maccormack) {
-          for (int k = 0; k < 4; k++) tr[k] = fieldCell(P, H, G, Fp, k, x, y, z);
-        } else {
-          const float* b = P.sb + slot * 8 * N;
-          float mn0 = b[0 * N + c], mn1 = b[1 * N + c], mn3 = b[2 * N + c], lmin = b[3 * N + c];
-          float mx0 = b[4 * N + c], mx1 = b[5 * N + c], mx3 = b[6 * N + c], lmax = b[7 * N + c];
-          if (mn0 == mx0 && mn1 == mx1 && mn3 == mx3 && lmin == lmax) {
-            tr[0] = mn0;
-            tr[1] = mn1;
-            tr[2] = clamp01(lmin);
-            tr[3] = mn3;
-          } else {
-            float a0 = fieldCell(P, H, G, Fp, 0, x, y, z), a1 = fieldCell(P, H, G, Fp, 1, x, y, z),
-                  a2 = fieldCell(P, H, G, Fp, 2, x, y, z), a3 = fieldCell(P, H, G, Fp, 3, x, y, z);
-            cv = velocityAt(P, H, G, V, px, py, pz);
-            cvSampled = true;
-            float3 vm = velocityAt(P, H, G, V, px + 0.5f * P.dt * cv.x, py + 0.5f * P.dt * cv.y, pz + 0.5f * P.dt * cv.z);
-            float fx = px + P.dt * vm.x, fy = py + P.dt * vm.y, fz = pz + P.dt * vm.z;
-            const float* o = P.fld + slot * 4 * N;
-            float o0 = o[0 * N + c], o1 = o[1 * N + c], o2 = o[2 * N + c], o3 = o[3 * N + c];
-            float lifetime = a2;
-            float r0, r1, r3;
-            if (lmin != lmax || a2 != lmin) {
-              float fc[3] = {(float)x + (fx - px) / P.h, (float)y + (fy - py) / P.h, (float)z + (fz - pz) / P.h};
-              int base[3];
-              float fr[3];
-              for (int a = 0; a < 3; a++) {
-                base[a] = (int)floorf(fc[a]);
-                fr[a] = fc[a] - floorf(fc[a]);
-              }
-              float rs0 = 0.f, rs1 = 0.f, rs2 = 0.f, rs3 = 0.f;
-              for (int dz = 0; dz < 2; dz++)
-                for (int dy = 0; dy < 2; dy++)
-                  for (int dx = 0; dx < 2; dx++) {
-                    int cx = base[0] + dx, cy = base[1] + dy, cz = base[2] + dz;
-                    float w = (dx ? fr[0] : 1.f - fr[0]) * (dy ? fr[1] : 1.f - fr[1]) * (dz ? fr[2] : 1.f - fr[2]);
-                    rs0 += fieldCell(P, H, G, Fp, 0, cx, cy, cz) * w;
-                    rs1 += fieldCell(P, H, G, Fp, 1, cx, cy, cz) * w;
-                    rs2 += fieldCell(P, H, G, Fp, 2, cx, cy, cz) * w;
-                    rs3 += fieldCell(P, H, G, Fp, 3, cx, cy, cz) * w;
-                  }
-              r0 = rs0;
-              r1 = rs1;
-              r3 = rs3;
-              float cl = a2 + 0.5f * (o2 - rs2);
-              lifetime = (cl < lmin || cl > lmax) ? a2 : cl;
-            } else {
-              r0 = fieldSample(P, H, G, Fp, 0, fx / P.h, fy / P.h, fz / P.h);
-              r1 = fieldSample(P, H, G, Fp, 1, fx / P.h, fy / P.h, fz / P.h);
-              r3 = fieldSample(P, H, G, Fp, 3, fx / P.h, fy / P.h, fz / P.h);
-            }
-            float c0 = a0 + 0.5f * (o0 - r0), c1 = a1 + 0.5f * (o1 - r1), c3 = a3 + 0.5f * (o3 - r3);
-            tr[0] = (c0 < mn0 || c0 > mx0) ? a0 : c0;
-            tr[1] = (c1 < mn1 || c1 > mx1) ? a1 : c1;
-            tr[2] = clamp01(lifetime);
-            tr[3] = (c3 < mn3 || c3 > mx3) ? a3 : c3;
-          }
-        }
-        float lifetime = tr[2];
-        float prodS = 0.f, prodH = 0.f, injectedFuel = 0.f;
-        uint2 list = tileList(P, tile, 0);
-        for (uint32_t j = 0; j < list.y; j++) {
-          const FpEmitter& e = P.emitters[P.tileLists[list.x + j]];
-          float w = emitterWeight(e, px, py, pz);
-          if (w == 0.f) continue;
-          float2 var = burstVariation(e, px, py, pz, P.seedBits);
-          lifetime = fmaxf(lifetime, e.flame * w * var.y);
-          prodS += e.smoke * w * P.dt;
-          prodH += e.heat * var.x * w * P.dt;
-          injectedFuel += e.fuel * w * P.dt;
-        }
-        float remaining = 0.f, burned = 0.f;
-        if (P.fuelEnabled) {
-          remaining = tr[3] + injectedFuel;
-          if (tr[1] + prodH >= P.ignition) {
-            lifetime = fmaxf(lifetime, fminf(remaining, 1.f));
-            float unburned = remaining * expf(-P.burnRate * P.dt);
-            burned = remaining - unburned;
-            remaining = unburned;
-          }
-        }
-        // evaluateFlame (flame-common.wgsl:30-42)
-        float before = clamp01(lifetime);
-        float after = 0.f, f0 = 0.f, f1 = 0.f, f2 = 0.f;
-        if (before > 0.f) {
-          const FpFlame& F = P.flame;
-          after = fmaxf(0.f, before - F.dt / F.lifespan);
-          f0 = F.smoke * F.lifespan * rampIntegral(F, 0, after, before);
-          f1 = F.heat * F.lifespan * rampIntegral(F, 1, after, before);
-          f2 = F.expansion * (F.lifespan * rampIntegral(F, 2, after, before) / F.dt);
-        }
-        expansion = f2 + P.flame.expansion * burned / P.dt;
-        float dS = tr[0] * expf(-P.dissipation * P.dt) + (prodS + f0) * expf(-P.dissipation * P.dt * 0.5f);
-        float dH = tr[1] * expf(-P.cooling * P.dt) + (prodH + f1) * expf(-P.cooling * P.dt * 0.5f);
-        value[0] = fmaxf(dS, 0.f);
-        value[1] = fmaxf(dH, 0.f);
-        value[2] = after;
-        value[3] = remaining;
-        injected = prodS > 0.f || prodH > 0.f || lifetime > tr[2] || injectedFuel > 0.f;
-      }
-      // clearDormant (fluid-common.wgsl:8-13)
-      if (!injected && value[2] == 0.f && value[0] < 0.001f && value[1] < 0.001f && value[3] < 0.001f)
-        value[0] = value[1] = value[2] = value[3] = 0.f;
-      for (int k = 0; k < 4; k++) P.fldN[(slot * 4 + k) * N + c] = value[k];
-      P.expn[slot * N + c] = expansion;
-      if (expansion != 0.f) expands = true;
-      // holdsContent and contentSupport (fluid-content.wgsl:22-39).
-      if (fmaxf(fmaxf(value[0], value[2]), value[3]) > P.cutoff) {
-        if (!cvSampled) cv = velocityAt(P, H, G, V, px, py, pz);
-        int idc[3] = {x, y, z};
-        float vv[3] = {cv.x, cv.y, cv.z};
-        bool low[3], high[3];
-        for (int a = 0; a < 3; a++) {
-          float side = (float)P.B;
-          float loc = (float)(idc[a] & (P.B - 1)) + 0.5f;
-          float pad = fminf(side, 2.f + fabsf(vv[a]) * P.dt / P.h);
-          low[a] = loc < pad;
-          high[a] = loc + pad >= side;
-        }
-        uint32_t row = 2u | (low[0] ? 1u : 0u) | (high[0] ? 4u : 0u);
-        uint32_t plane = (row << 3u) | (low[1] ? row : 0u) | (high[1] ? (row << 6u) : 0u);
-        busy |= (plane << 9u) | (low[2] ? plane : 0u) | (high[2] ? (plane << 18u) : 0u);
-      }
-    }
-    // recordContent (fluid-content.wgsl:43-64): one update per brick.
-    busy = __reduce_or_sync(0xffffffffu, busy);
-    uint32_t ex = __reduce_or_sync(0xffffffffu, (uint32_t)expands);
-    if ((threadIdx.x & 31) == 0) {
-      if (busy) atomicOr(&busyAll, busy);
-      if (ex) atomicOr(&expandsAll, 1u);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t flags = 0;
-      if (busyAll) {
-        flags = FP_CONTENT | (busyAll << 3);
-        uint32_t l = id & 63u;
-        uint32_t bits = (1u << (l & 3u)) | (16u << ((l >> 2) & 3u)) | (256u << (l >> 4));
-        atomicOr(&P.activity[(size_t)P.capacity * 64u + (id >> 6)], bits);
-      }
-      if (expandsAll) flags |= FP_EXPANDS;
-      if (flags) P.activity[id] |= flags;
-    }
-    __syncthreads();
+    brick_evolve<STAGED>(&P, i);
   }
 }
 
 // ---------------------------------------------------------------------------------------
 // computeCurl (fluid-forces.wgsl:38-75) of the corrected velocity.
-__global__ void __launch_bounds__(THREADS) k_curl(FpBatch bt) {
+FP_DEV void brick_curl(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
+  const SimParams& P = *Pp;
+  if (!P.curlOn) return;  // the same for the whole CTA
+  Home H = enterBrick(P, P.active[i], nslot);
+  size_t slot = (size_t)nslot[13];
+  const size_t N = P.N;
+  for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+    int x, y, z;
+    cellOf(P, H, c, x, y, z);
+    auto cc = [&](int qx, int qy, int qz, int comp) {
+      int r[3] = {qx, qy, qz};
+      r[comp] -= 1;
+      return 0.5f * (cellAt(P, H, P.velC, 3, comp, qx, qy, qz) + cellAt(P, H, P.velC, 3, comp, r[0], r[1], r[2]));
+    };
+    float hh = 0.5f / P.h;
+    float dx0 = (cc(x + 1, y, z, 1) - cc(x - 1, y, z, 1)) * hh, dx1 = (cc(x + 1, y, z, 2) - cc(x - 1, y, z, 2)) * hh;
+    float dy0 = (cc(x, y + 1, z, 0) - cc(x, y - 1, z, 0)) * hh, dy1 = (cc(x, y + 1, z, 2) - cc(x, y - 1, z, 2)) * hh;
+    float dz0 = (cc(x, y, z + 1, 0) - cc(x, y, z - 1, 0)) * hh, dz1 = (cc(x, y, z + 1, 1) - cc(x, y, z - 1, 1)) * hh;
+    float c0 = dy1 - dz1, c1 = dz0 - dx1, c2 = dx0 - dy0;
+    P.curl[(slot * 4 + 0) * N + c] = c0;
+    P.curl[(slot * 4 + 1) * N + c] = c1;
+    P.curl[(slot * 4 + 2) * N + c] = c2;
+    P.curl[(slot * 4 + 3) * N + c] = sqrtf(c0 * c0 + c1 * c1 + c2 * c2);
+  }
+  __syncthreads();
+}
+__global__ void __launch_bounds__(THREADS) k_curl(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    if (!P.curlOn) continue;  // the same for the whole CTA
-    Home H = enterBrick(P, P.active[i], nslot);
-    size_t slot = (size_t)nslot[13];
-    const size_t N = P.N;
-    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
-      int x, y, z;
-      cellOf(P, H, c, x, y, z);
-      auto cc = [&](int qx, int qy, int qz, int comp) {
-        int r[3] = {qx, qy, qz};
-        r[comp] -= 1;
-        return 0.5f * (cellAt(P, H, P.velC, 3, comp, qx, qy, qz) + cellAt(P, H, P.velC, 3, comp, r[0], r[1], r[2]));
-      };
-      float hh = 0.5f / P.h;
-      float dx0 = (cc(x + 1, y, z, 1) - cc(x - 1, y, z, 1)) * hh, dx1 = (cc(x + 1, y, z, 2) - cc(x - 1, y, z, 2)) * hh;
-      float dy0 = (cc(x, y + 1, z, 0) - cc(x, y - 1, z, 0)) * hh, dy1 = (cc(x, y + 1, z, 2) - cc(x, y - 1, z, 2)) * hh;
-      float dz0 = (cc(x, y, z + 1, 0) - cc(x, y, z - 1, 0)) * hh, dz1 = (cc(x, y, z + 1, 1) - cc(x, y, z - 1, 1)) * hh;
-      float c0 = dy1 - dz1, c1 = dz0 - dx1, c2 = dx0 - dy0;
-      P.curl[(slot * 4 + 0) * N + c] = c0;
-      P.curl[(slot * 4 + 1) * N + c] = c1;
-      P.curl[(slot * 4 + 2) * N + c] = c2;
-      P.curl[(slot * 4 + 3) * N + c] = sqrtf(c0 * c0 + c1 * c1 + c2 * c2);
-    }
-    __syncthreads();
+    brick_curl(&P, i);
   }
 }
 
@@ -660,53 +681,57 @@ FP_DEV float sourceVelocity(const SimParams& P, int tile, float value, float fx,
 
 // applyForces (fluid-forces.wgsl:151-182): centre forces of the brick and of the cells past
 // it on one axis, staged in shared memory, averaged to the faces.
-__global__ void __launch_bounds__(THREADS) k_forces(FpBatch bt) {
+FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
   extern __shared__ float3 forceTile[];  // (B+1)^3
+  const SimParams& P = *Pp;
+  uint32_t id = P.active[i];
+  Home H = enterBrick(P, id, nslot);
+  size_t slot = (size_t)nslot[13];
+  const size_t N = P.N;
+  int tile = (int)(id >> 6);
+  int E = P.B + 1;
+  for (int q = threadIdx.x; q < E * E * E; q += blockDim.x) {
+    int lx = q % E, ly = (q / E) % E, lz = q / (E * E);
+    if ((lx == P.B) + (ly == P.B) + (lz == P.B) >= 2) continue;
+    forceTile[q] = cellForce(P, H, tile, H.bx * P.B + lx, H.by * P.B + ly, H.bz * P.B + lz);
+  }
+  __syncthreads();
+  float decay = expf(-P.damping * P.dt);
+  for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+    int x, y, z;
+    cellOf(P, H, c, x, y, z);
+    int lx = x & (P.B - 1), ly = y & (P.B - 1), lz = z & (P.B - 1);
+    int t = (lz * E + ly) * E + lx;
+    float3 F0 = forceTile[t];
+    float f[3] = {0.5f * (F0.x + forceTile[t + 1].x), 0.5f * (F0.y + forceTile[t + E].y),
+                  0.5f * (F0.z + forceTile[t + E * E].z)};
+    float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+    float out[3];
+    for (int a = 0; a < 3; a++) {
+      float v = P.velC[(slot * 3 + a) * N + c] * decay + P.dt * f[a];
+      float face[3] = {px, py, pz};
+      face[a] += 0.5f * P.h;
+      out[a] = sourceVelocity(P, tile, v, face[0], face[1], face[2], a);
+    }
+    // enforceFaces (fluid-forces.wgsl:15-31)
+    if (solidAt(P, H, px, py, pz)) {
+      out[0] = out[1] = out[2] = 0.f;
+    } else {
+      if (solidAt(P, H, px + P.h, py, pz)) out[0] = 0.f;
+      if (solidAt(P, H, px, py + P.h, pz)) out[1] = 0.f;
+      if (solidAt(P, H, px, py, pz + P.h)) out[2] = 0.f;
+    }
+    for (int a = 0; a < 3; a++) P.velF[(slot * 3 + a) * N + c] = out[a];
+  }
+  __syncthreads();
+}
+__global__ void __launch_bounds__(THREADS) k_forces(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    uint32_t id = P.active[i];
-    Home H = enterBrick(P, id, nslot);
-    size_t slot = (size_t)nslot[13];
-    const size_t N = P.N;
-    int tile = (int)(id >> 6);
-    int E = P.B + 1;
-    for (int q = threadIdx.x; q < E * E * E; q += blockDim.x) {
-      int lx = q % E, ly = (q / E) % E, lz = q / (E * E);
-      if ((lx == P.B) + (ly == P.B) + (lz == P.B) >= 2) continue;
-      forceTile[q] = cellForce(P, H, tile, H.bx * P.B + lx, H.by * P.B + ly, H.bz * P.B + lz);
-    }
-    __syncthreads();
-    float decay = expf(-P.damping * P.dt);
-    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
-      int x, y, z;
-      cellOf(P, H, c, x, y, z);
-      int lx = x & (P.B - 1), ly = y & (P.B - 1), lz = z & (P.B - 1);
-      int t = (lz * E + ly) * E + lx;
-      float3 F0 = forceTile[t];
-      float f[3] = {0.5f * (F0.x + forceTile[t + 1].x), 0.5f * (F0.y + forceTile[t + E].y),
-                    0.5f * (F0.z + forceTile[t + E * E].z)};
-      float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-      float out[3];
-      for (int a = 0; a < 3; a++) {
-        float v = P.velC[(slot * 3 + a) * N + c] * decay + P.dt * f[a];
-        float face[3] = {px, py, pz};
-        face[a] += 0.5f * P.h;
-        out[a] = sourceVelocity(P, tile, v, face[0], face[1], face[2], a);
-      }
-      // enforceFaces (fluid-forces.wgsl:15-31)
-      if (solidAt(P, H, px, py, pz)) {
-        out[0] = out[1] = out[2] = 0.f;
-      } else {
-        if (solidAt(P, H, px + P.h, py, pz)) out[0] = 0.f;
-        if (solidAt(P, H, px, py + P.h, pz)) out[1] = 0.f;
-        if (solidAt(P, H, px, py, pz + P.h)) out[2] = 0.f;
-      }
-      for (int a = 0; a < 3; a++) P.velF[(slot * 3 + a) * N + c] = out[a];
-    }
-    __syncthreads();
+    brick_forces(&P, i);
   }
 }
 
@@ -726,74 +751,82 @@ FP_DEV bool pressureUnknown(const SimParams& P, const Home& H, int x, int y, int
 // computeDivergence (fluid-forces.wgsl:184-203) and the finest level's first Jacobi
 // iterate from zero (initializePressure, pressure.wgsl:485-505), fused: the iterate needs
 // only the cell's own right-hand side.
-__global__ void __launch_bounds__(THREADS) k_divergence(FpBatch bt, int pSel) {
+FP_DEV void brick_divergence(const SimParams* __restrict__ Pp, uint32_t i, int pSel) {
   __shared__ int nslot[27];
+  const SimParams& P = *Pp;
+  float* pOut = P.p0[pSel];
+  Home H = enterBrick(P, P.active[i], nslot);
+  size_t slot = (size_t)nslot[13];
+  const size_t N = P.N;
+  for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+    int x, y, z;
+    cellOf(P, H, c, x, y, z);
+    float d = (P.velF[(slot * 3 + 0) * N + c] - cellAt(P, H, P.velF, 3, 0, x - 1, y, z)) / P.h +
+              (P.velF[(slot * 3 + 1) * N + c] - cellAt(P, H, P.velF, 3, 1, x, y - 1, z)) / P.h +
+              (P.velF[(slot * 3 + 2) * N + c] - cellAt(P, H, P.velF, 3, 2, x, y, z - 1)) / P.h;
+    float rhs = P.h * P.h * (d - P.expn[slot * N + c]);
+    P.div[slot * N + c] = rhs;
+    uint8_t t = P.topo[0][slot * N + c];
+    float first = 0.f;
+    if (!(t & FP_STORED_SOLID) && pressureUnknown(P, H, x, y, z)) {
+      float diag = (float)((t >> 0) & 1) + (float)((t >> 1) & 1) + ((float)((t >> 2) & 1) + (float)((t >> 3) & 1)) +
+                   ((float)((t >> 4) & 1) + (float)((t >> 5) & 1));
+      first = mixf(0.f, (0.f - rhs) / fmaxf(diag, 1e-12f), 0.8f);
+    }
+    pOut[slot * N + c] = first;
+  }
+  __syncthreads();
+}
+__global__ void __launch_bounds__(THREADS) k_divergence(FpBatch bt, int pSel) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    float* pOut = P.p0[pSel];
-    Home H = enterBrick(P, P.active[i], nslot);
-    size_t slot = (size_t)nslot[13];
-    const size_t N = P.N;
-    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
-      int x, y, z;
-      cellOf(P, H, c, x, y, z);
-      float d = (P.velF[(slot * 3 + 0) * N + c] - cellAt(P, H, P.velF, 3, 0, x - 1, y, z)) / P.h +
-                (P.velF[(slot * 3 + 1) * N + c] - cellAt(P, H, P.velF, 3, 1, x, y - 1, z)) / P.h +
-                (P.velF[(slot * 3 + 2) * N + c] - cellAt(P, H, P.velF, 3, 2, x, y, z - 1)) / P.h;
-      float rhs = P.h * P.h * (d - P.expn[slot * N + c]);
-      P.div[slot * N + c] = rhs;
-      uint8_t t = P.topo[0][slot * N + c];
-      float first = 0.f;
-      if (!(t & FP_STORED_SOLID) && pressureUnknown(P, H, x, y, z)) {
-        float diag = (float)((t >> 0) & 1) + (float)((t >> 1) & 1) + ((float)((t >> 2) & 1) + (float)((t >> 3) & 1)) +
-                     ((float)((t >> 4) & 1) + (float)((t >> 5) & 1));
-        first = mixf(0.f, (0.f - rhs) / fmaxf(diag, 1e-12f), 0.8f);
-      }
-      pOut[slot * N + c] = first;
-    }
-    __syncthreads();
+    brick_divergence(&P, i, pSel);
   }
 }
 
 // project (fluid-forces.wgsl:228-262) into the velocity pool of the next step.
-__global__ void __launch_bounds__(THREADS) k_project(FpBatch bt, int pSel) {
+FP_DEV void brick_project(const SimParams* __restrict__ Pp, uint32_t i, int pSel) {
   __shared__ int nslot[27];
+  const SimParams& P = *Pp;
+  const float* p = P.p0[pSel];
+  Home H = enterBrick(P, P.active[i], nslot);
+  size_t slot = (size_t)nslot[13];
+  const size_t N = P.N;
+  for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+    int x, y, z;
+    cellOf(P, H, c, x, y, z);
+    float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+    float res[3] = {0.f, 0.f, 0.f};
+    if (!solidAt(P, H, px, py, pz)) {
+      float cp = p[slot * N + c];
+      bool pu = pressureUnknown(P, H, x, y, z);
+      for (int a = 0; a < 3; a++) {
+        int n[3] = {x, y, z};
+        n[a] += 1;
+        float v = P.velF[(slot * 3 + a) * N + c];
+        float nx = ((float)n[0] + 0.5f) * P.h, ny = ((float)n[1] + 0.5f) * P.h, nz = ((float)n[2] + 0.5f) * P.h;
+        if (solidAt(P, H, nx, ny, nz)) {
+          res[a] = 0.f;
+        } else if (!pu && !pressureUnknown(P, H, n[0], n[1], n[2])) {
+          res[a] = 0.f;
+        } else {
+          float pn = cellAt(P, H, p, 1, 0, n[0], n[1], n[2]);
+          res[a] = v - (pn - cp) / P.h;
+        }
+      }
+    }
+    for (int a = 0; a < 3; a++) P.velP[(slot * 3 + a) * N + c] = res[a];
+  }
+  __syncthreads();
+}
+__global__ void __launch_bounds__(THREADS) k_project(FpBatch bt, int pSel) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    const float* p = P.p0[pSel];
-    Home H = enterBrick(P, P.active[i], nslot);
-    size_t slot = (size_t)nslot[13];
-    const size_t N = P.N;
-    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
-      int x, y, z;
-      cellOf(P, H, c, x, y, z);
-      float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-      float res[3] = {0.f, 0.f, 0.f};
-      if (!solidAt(P, H, px, py, pz)) {
-        float cp = p[slot * N + c];
-        bool pu = pressureUnknown(P, H, x, y, z);
-        for (int a = 0; a < 3; a++) {
-          int n[3] = {x, y, z};
-          n[a] += 1;
-          float v = P.velF[(slot * 3 + a) * N + c];
-          float nx = ((float)n[0] + 0.5f) * P.h, ny = ((float)n[1] + 0.5f) * P.h, nz = ((float)n[2] + 0.5f) * P.h;
-          if (solidAt(P, H, nx, ny, nz)) {
-            res[a] = 0.f;
-          } else if (!pu && !pressureUnknown(P, H, n[0], n[1], n[2])) {
-            res[a] = 0.f;
-          } else {
-            float pn = cellAt(P, H, p, 1, 0, n[0], n[1], n[2]);
-            res[a] = v - (pn - cp) / P.h;
-          }
-        }
-      }
-      for (int a = 0; a < 3; a++) P.velP[(slot * 3 + a) * N + c] = res[a];
-    }
-    __syncthreads();
+    brick_project(&P, i, pSel);
   }
 }
 

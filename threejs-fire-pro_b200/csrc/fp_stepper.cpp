@@ -56,7 +56,9 @@ int Stepper::initialize() {
   // Shared-memory limits before any capture.
   fp_mg_configure(B_);
   fp_step_configure(B_);
-  if ((rc = reserve(1 << 16, 16, 1 << 12))) return rc;
+  // Room for a few hundred simulations' parameters and scenes from the start: growing the
+  // upload later waits for the stream and captures the graphs again.
+  if ((rc = reserve(4 << 20, 256, 1 << 16))) return rc;
   return check(cudaStreamSynchronize(stream_), "initialize");
 }
 
@@ -326,7 +328,7 @@ void Stepper::vcycle(int level, int cur[], uint64_t& launches) {
   auto relax = [&](int n) {
     for (int i = 0; i < n; i++) {
       MgSel S{level, sel(level, 2), sel(level, cur[level]), -1, sel(level, 1 - cur[level]), -1};
-      fp_launch_relax(batch(), S, tiles, sms_, stream_);
+      fp_launch_relax(batch(), S, tiles, B_, sms_, stream_);
       launches++;
       cur[level] = 1 - cur[level];
     }
@@ -334,12 +336,12 @@ void Stepper::vcycle(int level, int cur[], uint64_t& launches) {
   if (level > 0) relax(2);
   int coarse = level + 1;
   MgSel R{coarse, sel(level, 2), sel(level, cur[level]), -1, sel(coarse, 2), sel(coarse, 1)};
-  fp_launch_restrict(batch(), R, coarse >= brickLevels_, sms_, stream_);
+  fp_launch_restrict(batch(), R, coarse >= brickLevels_, B_, sms_, stream_);
   launches++;
   cur[coarse] = 1;
   vcycle(coarse, cur, launches);
   MgSel Pr{level, -1, sel(level, cur[level]), sel(coarse, cur[coarse]), sel(level, 1 - cur[level]), -1};
-  fp_launch_prolong(batch(), Pr, tiles, sms_, stream_);
+  fp_launch_prolong(batch(), Pr, tiles, B_, sms_, stream_);
   launches++;
   cur[level] = 1 - cur[level];
   relax(3);

@@ -262,6 +262,9 @@ SIGNATURES = {
     "fp_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "fp_batch_read_profile": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
     "fp_grid_memory_bytes": (C.c_int, [C.POINTER(fp_grid), C.POINTER(C.c_uint64)]),
+    "fp_grid_reserved_tiles": (C.c_int, [C.POINTER(fp_grid), C.POINTER(C.c_uint32)]),
+    "fp_sim_reserve_tiles": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "fp_batch_reserve_tiles": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "fp_server_last_error": (C.c_char_p, [C.c_void_p]),
     "fp_server_create": (C.c_int, [C.POINTER(fp_server_config), C.POINTER(C.c_void_p)]),
     "fp_server_destroy": (C.c_int, [C.c_void_p]),

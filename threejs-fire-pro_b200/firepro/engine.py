@@ -53,6 +53,9 @@ class FluidSimulation:
     def step(self, frame: abi.fp_frame, dt: float = FIXED_DT):
         self._check(self.lib.fp_sim_step(self.h, C.byref(frame), dt))
 
+    def reserve_tiles(self, tiles: int):
+        self._check(self.lib.fp_sim_reserve_tiles(self.h, tiles))
+
     def reset(self):
         self._check(self.lib.fp_sim_reset(self.h))
 
@@ -150,6 +153,9 @@ class SimulationBatch:
     def set_runtime(self, sim: int, cutoff: float, voxel_budget: float, ground: bool):
         self._check(self.lib.fp_batch_set_runtime(self.h, sim, cutoff, voxel_budget, int(ground)))
 
+    def reserve_tiles(self, sim: int, tiles: int):
+        self._check(self.lib.fp_batch_reserve_tiles(self.h, sim, tiles))
+
     def step(self, items):
         """Step [(id, fp_frame, dt), ...] in one launch."""
         n = len(items)
@@ -196,6 +202,16 @@ class SimulationBatch:
         n = C.c_uint32(16)
         self._check(self.lib.fp_batch_read_profile(self.h, arr, C.byref(n)))
         return {arr[i].name.decode(): (arr[i].launches, arr[i].ms, arr[i].voxels) for i in range(n.value)}
+
+
+def reserved_tiles(grid: abi.fp_grid) -> int:
+    """The tile reservation a server gives a session of `grid`."""
+    lib = abi.load_library()
+    out = C.c_uint32()
+    rc = lib.fp_grid_reserved_tiles(C.byref(grid), C.byref(out))
+    if rc != abi.FP_OK:
+        raise FireProError(rc, lib.fp_last_error(None).decode())
+    return out.value
 
 
 def grid_memory_bytes(grid: abi.fp_grid) -> int:
