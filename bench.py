@@ -351,6 +351,56 @@ def served_form(local: int, sessions: int = 64, grow: int = 90, ticks: int = 300
     }
 
 
+def precision_form(local: int, steps: int = 30, vcycles: int = 8, tolerance: float = 1e-4) -> dict:
+    """The large scene in plain FP32 and in FP_PRECISION_MIXED (FP16 scalar state, BF16 coarse
+    multigrid, FP32 defect correction), both solving the pressure to the same FP64-measured
+    relative residual (at most `vcycles` V-cycles): device time per step on the simulation's
+    stream, the V-cycles run and the projected velocity's divergence, from the same grown
+    state size."""
+    import torch
+
+    from firepro import abi, scenes
+    from firepro.engine import FluidSimulation
+
+    out = {"solver": {"vcycles": vcycles, "tolerance": tolerance}}
+    for name, precision in (("fp32", abi.FP_PRECISION_FP32), ("mixed", abi.FP_PRECISION_MIXED)):
+        sc = scenes.LargeScene(seed=1)
+        sim = FluidSimulation(sc.grid(budget=BUDGET, precision=precision), device=local)
+        sim.set_runtime(0.05, BUDGET, True)
+        sim.set_solver(vcycles, tolerance)
+        step = 0
+        while step < MAX_GROW_STEPS:
+            sim.step(sc.frame(step).frame)
+            step += 1
+            if step % 25 == 0 and sim.stats().active_bricks >= TARGET_BRICKS:
+                break
+        for _ in range(3):
+            sim.step(sc.frame(step).frame)
+            step += 1
+        sim.synchronize()
+        stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        actives, cycles, div = [], [], []
+        ev[0].record(stream)
+        for k in range(steps):
+            sim.step(sc.frame(step).frame)
+            step += 1
+            actives.append(sim.stats().active_bricks)
+        ev[1].record(stream)
+        sim.synchronize()
+        ms = ev[0].elapsed_time(ev[1])
+        sol = sim.read_solver()
+        st = sim.stats()
+        out[name] = {"value": sum(actives) * BRICK_VOXELS / (ms / 1e3), "ms_per_step": ms / steps,
+                     "mean_active_bricks": sum(actives) / len(actives), "vcycles_last": sol.vcycles,
+                     "residual_last": sol.residual[max(0, sol.vcycles - 1)], "divergence_last": sol.divergence,
+                     "memory_bytes": st.memory_bytes}
+        sim.dispose()
+    out["speedup"] = out["mixed"]["value"] / out["fp32"]["value"]
+    out["unit"] = "voxel-steps/s"
+    return out
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -481,7 +531,8 @@ def run_ours(args, rank, world, local):
     }
     if world == 1 and not args.no_forms:
         line["forms"] = {"batched": batched_form(local, steps=max(10, min(args.steps, 60))),
-                         "served": served_form(local)}
+                         "served": served_form(local),
+                         "precision": precision_form(local)}
     if world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         cv, csteps, cbricks, _ = cpu_sample(scenes.LargeScene, 20.0, 400, threads)

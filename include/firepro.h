@@ -38,7 +38,9 @@ extern "C" {
 
 /* Storage precision of the pools. Arithmetic is FP32 in every mode. */
 #define FP_PRECISION_FP32 0  /* plain FP32 storage everywhere (the drop-in) */
-#define FP_PRECISION_MIXED 1 /* FP16 scalar pools, BF16 coarse multigrid, FP32 velocity */
+#define FP_PRECISION_MIXED 1 /* FP16 scalar pools (smoke, heat, lifetime, fuel), BF16 multigrid
+                                levels above the finest; velocity, the finest pressure level,
+                                divergence and expansion FP32; measured every step */
 
 /* Source shapes (types.ts:248 SimulationSource.shape). */
 #define FP_SHAPE_SPHERE 0
@@ -165,7 +167,21 @@ typedef struct fp_stats {
   uint64_t d2h_bytes;       /* device-to-host bytes the latest step read back (its measurement) */
   double host_prepare_ms;   /* host time in fp_sim_step since creation, waits excluded */
   double host_wait_ms;      /* host time spent waiting for the previous step's measurement */
+  double last_divergence;   /* post-projection RMS(h div u) / RMS(u) of that solve when measured, else -1 */
 } fp_stats;
+
+/* The latest step's pressure solve (`fp_sim_read_solver`). No reference counterpart: the
+ * reference runs one V-cycle and measures nothing. Norms are FP64 sums on the GPU over the
+ * finest level's pressure unknowns. */
+#define FP_MAX_VCYCLES 16
+typedef struct fp_solver_stats {
+  uint32_t vcycles;                  /* V-cycles the solve ran */
+  int32_t measured;                  /* the post-projection divergence was measured */
+  double unknowns;                   /* unknown cells */
+  double rhs_rms;                    /* RMS of the right-hand side h^2 (div u* - expansion) */
+  double residual[FP_MAX_VCYCLES];   /* RMS residual / RMS right-hand side after each V-cycle */
+  double divergence;                 /* RMS(h div u) / RMS(u) of the projected velocity, or -1 */
+} fp_solver_stats;
 
 /* Device time of one phase of the step, accumulated while profiling is on: the restatement
  * of the reference's per-pass GPU timestamps (src/engine/GpuProfiler.ts:21-109). */
@@ -219,6 +235,14 @@ int fp_sim_step(fp_sim* sim, const fp_frame* frame, float dt);
  * per-brick tables (the reference doubles them when the tiles outgrow them,
  * FluidSimulation.ts:629-678). Storage only: results do not change. No reference counterpart. */
 int fp_sim_reserve_tiles(fp_sim* sim, uint32_t tiles);
+/* The pressure solve: up to `vcycles` (1..FP_MAX_VCYCLES) V-cycles a step; after each, the
+ * FP64 residual decides, and the solve stops once RMS residual <= tolerance x RMS right-hand
+ * side (tolerance 0: run all of them). Every V-cycle after the first is a defect correction:
+ * the finest level stays FP32 and the coarse correction comes from the residual of the current
+ * iterate. The default (1, 0) is the reference's schedule (PressureSolver.ts:276-365). */
+int fp_sim_set_solver(fp_sim* sim, int vcycles, float tolerance);
+/* The latest step's solve (waits for the step's work). */
+int fp_sim_read_solver(fp_sim* sim, fp_solver_stats* out);
 /* Wait for the simulation's queued work. */
 int fp_sim_synchronize(fp_sim* sim);
 /* Stats (waits for the latest step's measurement). */
@@ -259,6 +283,10 @@ int fp_batch_reset(fp_batch* batch, uint32_t id);
 int fp_batch_set_runtime(fp_batch* batch, uint32_t id, float cutoff, double voxel_budget, int ground);
 /* As fp_sim_reserve_tiles. */
 int fp_batch_reserve_tiles(fp_batch* batch, uint32_t id, uint32_t tiles);
+/* As fp_sim_set_solver and fp_sim_read_solver. A launch runs as many V-cycles as its most
+ * demanding simulation asks for; each simulation stops at its own limit or tolerance. */
+int fp_batch_set_solver(fp_batch* batch, uint32_t id, int vcycles, float tolerance);
+int fp_batch_read_solver(fp_batch* batch, uint32_t id, fp_solver_stats* out);
 /* Step the `count` simulations `ids` (distinct) with frames[i] and dts[i], in one launch. */
 int fp_batch_step(fp_batch* batch, const uint32_t* ids, const fp_frame* frames, const float* dts, uint32_t count);
 int fp_batch_synchronize(fp_batch* batch);

@@ -269,6 +269,7 @@ struct Sim {
   std::vector<Level> levels;
   std::vector<R> pres[2];  // level 0 pressures
   int latest = 0;
+  int vcycles = 1;  // V-cycles a step; later ones are defect corrections of the finest level
 
   // --- per step scene
   std::vector<Emitter<R>> emitters;
@@ -1854,7 +1855,9 @@ struct Sim {
       }
       return;
     }
-    smooth(index, index > 0 ? 2 : 1, initialize);
+    // The finest level's only pre-smoothing is the first iterate from zero; a later V-cycle
+    // restricts the residual of the current iterate directly.
+    smooth(index, index > 0 ? 2 : (initialize ? 1 : 0), initialize);
     Level& L = levels[index];
     Level& C = levels[index + 1];
     restrictLevel(index, RHS(index), P(index, L.current), RHS(index + 1), P(index + 1, 1));
@@ -1870,7 +1873,7 @@ struct Sim {
     buildTopology();
     levels[0].current = latest;
     bool initialize = true;
-    cycle(0, initialize);
+    for (int c = 0; c < vcycles; c++) cycle(0, initialize);
     latest = levels[0].current;
   }
 
@@ -2005,6 +2008,14 @@ void or_set_runtime(or_sim* s, float cutoff, double budget, int ground) {
     return 0;
   };
   if (s->d) fn(*s->d); else fn(*s->f);
+}
+// The number of V-cycles of each later step's pressure solve (the CUDA step's solver setting
+// with tolerance 0).
+void or_set_solver(or_sim* s, int vcycles) {
+  if (s->d)
+    s->d->vcycles = vcycles;
+  else
+    s->f->vcycles = vcycles;
 }
 int or_step(or_sim* s, const fp_frame* f, float dt) {
   std::string e = s->d ? s->d->step(*f, dt) : s->f->step(*f, dt);

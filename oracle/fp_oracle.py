@@ -35,6 +35,7 @@ def lib():
         L.or_destroy.argtypes = [C.c_void_p]
         L.or_set_threads.argtypes = [C.c_int]
         L.or_set_runtime.argtypes = [C.c_void_p, C.c_float, C.c_double, C.c_int]
+        L.or_set_solver.argtypes = [C.c_void_p, C.c_int]
         L.or_step.restype = C.c_int
         L.or_step.argtypes = [C.c_void_p, C.c_void_p, C.c_float]
         L.or_error.restype = C.c_char_p
@@ -79,6 +80,10 @@ class OracleSim:
 
     def set_runtime(self, cutoff: float, budget: float, ground: bool):
         self.L.or_set_runtime(self.h, cutoff, budget, int(ground))
+
+    def set_solver(self, vcycles: int):
+        """V-cycles of each later step's pressure solve (defect corrections after the first)."""
+        self.L.or_set_solver(self.h, vcycles)
 
     def step(self, frame, dt: float = 1.0 / 60.0):
         if self.L.or_step(self.h, C.byref(frame), dt) != 0:

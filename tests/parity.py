@@ -88,14 +88,18 @@ def force(gpu, orc):
 
 
 def lockstep(scene, steps: int, gpu_factory, cutoff=0.05, budget=8e6, ground=True, start=0, log=None, grid=None,
-             before_step=None):
+             before_step=None, vcycles=1):
     """Run `steps` steps in lockstep; returns per-step (tables, fields) reports.
-    `before_step(step, gpu, oracle)` may change runtime settings on both."""
+    `before_step(step, gpu, oracle)` may change runtime settings on both. `vcycles` V-cycles
+    a step on both sides (tolerance 0: all of them run)."""
     grid = grid if grid is not None else scene.grid(budget=budget)
     gpu = gpu_factory(grid)
     orc = OracleSim(grid, real=0)
     gpu.set_runtime(cutoff, budget, ground)
     orc.set_runtime(cutoff, budget, ground)
+    if vcycles != 1:
+        gpu.set_solver(vcycles, 0.0)
+        orc.set_solver(vcycles)
     reports = []
     for s in range(start, start + steps):
         if before_step:

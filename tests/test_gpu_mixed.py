@@ -1,0 +1,115 @@
+"""Mixed precision and the defect-corrected pressure solve, through the C ABI.
+
+FP_PRECISION_MIXED stores the advected scalars' state in FP16 and the multigrid levels above
+the finest in BF16, with FP32 arithmetic; later V-cycles correct the finest FP32 level from its
+residual. Parity is against the FP64 oracle running the same number of V-cycles: tables bit
+for bit; velocity and pressure within relative L2 1e-3 per step (teacher forced, as the FP32
+parity tests). The FP16 scalars and what derives from them (the expansion and the divergence
+right-hand side) are held to MIXED_SCALAR_TOL: rounding the state to FP16 costs up to 2.8e-4
+relative per store, and quantised values sit exactly on the MacCormack limiter's bounds far
+more often, where FP32 and FP64 keep or revert the correction differently.
+"""
+import numpy as np
+import pytest
+
+from firepro import abi, scenes
+from firepro.engine import FIXED_DT, FluidSimulation
+import parity
+from test_gpu_parity import TOL, check
+
+pytestmark = pytest.mark.gpu
+
+MIXED_SCALAR_TOL = 5e-3
+FP16_DERIVED = ("smoke", "heat", "lifetime", "fuel", "expansion", "divergence")
+
+
+def run(scene, steps, vcycles, precision=abi.FP_PRECISION_FP32, budget=2 ** 19, **kw):
+    grid = scene.grid(budget=budget, precision=precision)
+    return parity.lockstep(scene, steps, lambda g: FluidSimulation(g), budget=budget, grid=grid, vcycles=vcycles, **kw)
+
+
+def check_mixed(reports, min_active=1):
+    """Tables as check(); velocity and pressure within TOL, the FP16-derived fields within
+    MIXED_SCALAR_TOL."""
+    worst = {}
+    for step, tables, fields, n in reports:
+        for k, v in tables.items():
+            if k == "activity":
+                assert 0 <= v <= max(2, n // 500), f"step {step}: {v} activity words differ"
+                continue
+            assert v == 0, f"step {step}: table {k} differs in {v} words"
+        for k, v in fields.items():
+            worst[k] = max(worst.get(k, 0.0), v)
+            tol = MIXED_SCALAR_TOL if k in FP16_DERIVED else TOL
+            assert v <= tol, f"step {step}: {k} relative L2 {v:.3e} > {tol}"
+    assert max(r[3] for r in reports) >= min_active
+    print("worst relative L2:", {k: f"{v:.2e}" for k, v in worst.items()})
+    return worst
+
+
+def test_fp32_defect_correction_parity():
+    """Three V-cycles a step in FP32 against the oracle's three."""
+    check(run(scenes.SinglePlume(), 16, 3), min_active=216)
+
+
+def test_mixed_plume_parity():
+    check_mixed(run(scenes.SinglePlume(), 24, 4, precision=abi.FP_PRECISION_MIXED), min_active=216)
+
+
+def test_mixed_large_scene_parity():
+    """Through the burst at step 30, colliders and turbulence, FP16 scalars, BF16 coarse levels."""
+    check_mixed(run(scenes.LargeScene(), 34, 4, precision=abi.FP_PRECISION_MIXED, budget=2 ** 20), min_active=100)
+
+
+def test_mixed_force_scene_parity():
+    check_mixed(run(scenes.ForceScene(), 16, 4, precision=abi.FP_PRECISION_MIXED, budget=2 ** 20))
+
+
+def solve_history(precision, vcycles, tolerance, steps=20):
+    sc = scenes.SinglePlume()
+    sim = FluidSimulation(sc.grid(budget=2 ** 19, precision=precision))
+    sim.set_runtime(0.05, 2 ** 19, True)
+    sim.set_solver(vcycles, tolerance)
+    out = []
+    for s in range(steps):
+        fd = sc.frame(s)
+        sim.step(fd.frame)
+        out.append(sim.read_solver())
+    sim.dispose()
+    return out
+
+
+@pytest.mark.parametrize("precision", [abi.FP_PRECISION_FP32, abi.FP_PRECISION_MIXED])
+def test_defect_correction_converges(precision):
+    """Residuals fall cycle by cycle; the solve stops at the tolerance and then the projected
+    velocity's divergence is small."""
+    hist = solve_history(precision, 16, 1e-5)
+    for st in hist[2:]:
+        r = [st.residual[c] for c in range(st.vcycles)]
+        assert st.vcycles >= 2 and st.unknowns > 0 and st.rhs_rms > 0
+        assert all(b < a for a, b in zip(r, r[1:])), f"residuals do not fall: {r}"
+        assert r[-1] <= 1e-5 or st.vcycles == 16, f"stopped early at {r[-1]:.2e}"
+        assert st.measured and 0 <= st.divergence <= 1e-4, f"post-projection divergence {st.divergence:.2e}"
+    print("cycles", [h.vcycles for h in hist], "last residual", hist[-1].residual[hist[-1].vcycles - 1],
+          "divergence", hist[-1].divergence)
+
+
+def test_mixed_matches_fp32_within_tolerance():
+    """The same plume in both precisions, solved to 1e-5: the fields agree within 1e-3."""
+    sc = scenes.SinglePlume()
+    fields = {}
+    for precision in (abi.FP_PRECISION_FP32, abi.FP_PRECISION_MIXED):
+        sim = FluidSimulation(sc.grid(budget=2 ** 19, precision=precision))
+        sim.set_runtime(0.05, 2 ** 19, True)
+        sim.set_solver(16, 1e-5)
+        for s in range(12):
+            fd = sc.frame(s)
+            sim.step(fd.frame)
+        fields[precision] = (sim.field(abi.FP_FIELD_VELOCITY), sim.field(abi.FP_FIELD_SCALARS),
+                             sim.table(abi.FP_TABLE_ENTRIES))
+        sim.dispose()
+    a, b = fields[abi.FP_PRECISION_FP32], fields[abi.FP_PRECISION_MIXED]
+    slots = parity.active_slots(a[2])
+    assert np.array_equal(parity.active_slots(b[2]), slots)
+    assert parity.rel_l2(b[0][slots], a[0][slots].astype(np.float64)) <= MIXED_SCALAR_TOL
+    assert parity.rel_l2(b[1][slots], a[1][slots].astype(np.float64)) <= MIXED_SCALAR_TOL

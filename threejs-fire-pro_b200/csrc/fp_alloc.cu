@@ -413,29 +413,36 @@ __global__ void __launch_bounds__(256) k_zero_fresh(FpBatch bt) {
     const SimParams& P = workSim(bt, FP_WORK_FRESH, item, i);
     size_t slot = P.zeroList[2 * i + 1];
     float4* v = reinterpret_cast<float4*>(P.vel + slot * 3 * P.N);
-    float4* f = reinterpret_cast<float4*>(P.fld + slot * 4 * P.N);
+    // The scalar pool holds 4 channels of 4 bytes (FP32) or 2 bytes (FP16) a cell.
+    const int scalarBytes = P.scalarHalf ? 2 : 4;
+    float4* f = reinterpret_cast<float4*>(reinterpret_cast<char*>(P.fld) + slot * 4 * P.N * scalarBytes);
     float4* e = reinterpret_cast<float4*>(P.expn + slot * P.N);
     float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int k = threadIdx.x; k < 3 * P.N / 4; k += blockDim.x) v[k] = z;
-    for (int k = threadIdx.x; k < 4 * P.N / 4; k += blockDim.x) f[k] = z;
+    for (int k = threadIdx.x; k < P.N * scalarBytes / 4; k += blockDim.x) f[k] = z;
     for (int k = threadIdx.x; k < P.N / 4; k += blockDim.x) e[k] = z;
   }
 }
 
 // The measurement of each simulation (readActivity, FluidSimulation.ts:1701-1746): its
-// counters and a content word per tile slot, into host-mapped memory; then failed
-// allocations count afresh. A CTA per simulation.
+// counters, the previous step's pressure-solve measurements and a content word per tile slot,
+// into host-mapped memory; then failed allocations count afresh and the solve's
+// measurements start over. A CTA per simulation.
 __global__ void __launch_bounds__(256) k_readback(FpBatch bt) {
   int sims = batchCount(bt);
-  const int cw = (int)(sizeof(FpCounters) / 4);
+  const int cw = (int)(sizeof(FpCounters) / 4), sw = (int)(sizeof(FpSolver) / 4);
   for (int sim = blockIdx.x; sim < sims; sim += gridDim.x) {
     const SimParams& P = bt.sims[sim];
     const uint32_t* counters = reinterpret_cast<const uint32_t*>(P.counters);
+    const uint32_t* solver = reinterpret_cast<const uint32_t*>(P.solver);
     const uint32_t* tiles = P.activity + (size_t)P.capacity * 64;
-    for (int k = threadIdx.x; k < cw + P.capacity; k += blockDim.x)
-      P.readback[k] = k < cw ? counters[k] : tiles[k - cw];
+    for (int k = threadIdx.x; k < cw + sw + P.capacity; k += blockDim.x)
+      P.readback[k] = k < cw ? counters[k] : (k < cw + sw ? solver[k - cw] : tiles[k - cw - sw]);
     __syncthreads();
     if (threadIdx.x == 0) P.counters->failures = 0;
+    uint32_t* clear = reinterpret_cast<uint32_t*>(P.solver);
+    for (int k = threadIdx.x; k < sw; k += blockDim.x) clear[k] = 0u;
+    __syncthreads();
   }
 }
 

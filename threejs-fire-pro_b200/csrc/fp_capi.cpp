@@ -54,8 +54,6 @@ static int validateGrid(const fp_grid* grid) {
   if (vd != 1) return failed("velocityDivisor 2 and 4 are not implemented by this build.", FP_EUNSUPPORTED);
   if (sd != 1) return failed("smokeDivisor 2 and 4 are not implemented by this build.", FP_EUNSUPPORTED);
   if (bs == 32) return failed("brickSize 32 is not implemented by this build.", FP_EUNSUPPORTED);
-  if (grid->precision != FP_PRECISION_FP32)
-    return failed("FP_PRECISION_MIXED is not implemented by this build.", FP_EUNSUPPORTED);
   return FP_OK;
 }
 
@@ -148,6 +146,16 @@ int fp_sim_step(fp_sim* sim, const fp_frame* frame, float dt) {
 int fp_sim_reserve_tiles(fp_sim* sim, uint32_t tiles) {
   if (!sim) return failed("null simulation", FP_EINVAL);
   return sim->engine->reserveTiles(tiles);
+}
+
+int fp_sim_set_solver(fp_sim* sim, int vcycles, float tolerance) {
+  if (!sim) return failed("null simulation", FP_EINVAL);
+  return sim->engine->setSolver(vcycles, tolerance);
+}
+
+int fp_sim_read_solver(fp_sim* sim, fp_solver_stats* out) {
+  if (!sim || !out) return failed("fp_sim_read_solver needs a simulation and an output.", FP_EINVAL);
+  return sim->engine->readSolver(out);
 }
 
 int fp_sim_synchronize(fp_sim* sim) {
@@ -287,6 +295,22 @@ int fp_batch_reserve_tiles(fp_batch* batch, uint32_t id, uint32_t tiles) {
   fp::Engine* e = batchSim(batch, id);
   if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
   int rc = e->reserveTiles(tiles);
+  return rc ? batchFail(batch, rc, e->error()) : FP_OK;
+}
+
+int fp_batch_set_solver(fp_batch* batch, uint32_t id, int vcycles, float tolerance) {
+  if (!batch) return failed("null batch", FP_EINVAL);
+  fp::Engine* e = batchSim(batch, id);
+  if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
+  int rc = e->setSolver(vcycles, tolerance);
+  return rc ? batchFail(batch, rc, e->error()) : FP_OK;
+}
+
+int fp_batch_read_solver(fp_batch* batch, uint32_t id, fp_solver_stats* out) {
+  if (!batch || !out) return failed("fp_batch_read_solver needs a batch and an output.", FP_EINVAL);
+  fp::Engine* e = batchSim(batch, id);
+  if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
+  int rc = e->readSolver(out);
   return rc ? batchFail(batch, rc, e->error()) : FP_OK;
 }
 

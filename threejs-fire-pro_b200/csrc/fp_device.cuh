@@ -2,6 +2,7 @@
 // and each brick's 27-neighbour record, trilinear sampling with exact weights, solid tests,
 // the emitter, flame and noise functions. Reference semantics are cited per function.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -27,6 +28,41 @@ FP_DEV const SimParams& workSim(const FpBatch& b, int kind, uint32_t item, uint3
   }
   local = item - row[lo];
   return b.sims[lo];
+}
+
+// Storage of the scalar pools (FP16 in FP_PRECISION_MIXED) and of the coarse multigrid levels
+// (BF16): loads widen to FP32, stores round to nearest even. `narrow` is uniform per launch.
+FP_DEV float ldHalf(const float* pool, size_t i, bool narrow) {
+  return narrow ? __half2float(reinterpret_cast<const __half*>(pool)[i]) : pool[i];
+}
+FP_DEV void stHalf(float* pool, size_t i, float v, bool narrow) {
+  if (narrow)
+    reinterpret_cast<__half*>(pool)[i] = __float2half_rn(v);
+  else
+    pool[i] = v;
+}
+FP_DEV float ldBf(const float* p, long i, bool narrow) {
+  return narrow ? __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(p)[i]) : p[i];
+}
+FP_DEV void stBf(float* p, long i, float v, bool narrow) {
+  if (narrow)
+    reinterpret_cast<__nv_bfloat16*>(p)[i] = __float2bfloat16_rn(v);
+  else
+    p[i] = v;
+}
+
+// Sum of a double over the CTA (blockDim a multiple of 32, at most 1024), in a fixed order;
+// thread 0 holds it. Every thread of the CTA must call it.
+FP_DEV double blockSum(double v, double* scratch) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += scratch[w];
+  __syncthreads();
+  return s;
 }
 
 FP_DEV int nbrIndex(int dx, int dy, int dz) { return (dz + 1) * 9 + (dy + 1) * 3 + dx + 1; }
@@ -88,16 +124,17 @@ FP_DEV int localCell(const SimParams& P, int x, int y, int z) {
 }
 // Cell (x,y,z) of a pool of `ch` channels: zero in a brick without a slot
 // (fluid-sampling.wgsl:68-75).
-FP_DEV float cellAt(const SimParams& P, const Home& H, const float* pool, int ch, int c, int x, int y, int z) {
+FP_DEV float cellAt(const SimParams& P, const Home& H, const float* pool, int ch, int c, int x, int y, int z,
+                    bool half = false) {
   int s = brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift);
   if (s < 0) return 0.f;
-  return pool[((size_t)s * ch + c) * P.N + localCell(P, x, y, z)];
+  return ldHalf(pool, ((size_t)s * ch + c) * P.N + localCell(P, x, y, z), half);
 }
 
 // Trilinear sample of one channel at `pos` in cell units, centres at .5
 // (fluid-sampling.wgsl:85-114): bricks without a slot read zero.
 FP_DEV float sampleCells(const SimParams& P, const Home& H, const float* pool, int ch, int c, float px, float py,
-                         float pz) {
+                         float pz, bool half = false) {
   float qx = px - 0.5f, qy = py - 0.5f, qz = pz - 0.5f;
   int x0 = (int)floorf(qx), y0 = (int)floorf(qy), z0 = (int)floorf(qz);
   float fx = qx - (float)x0, fy = qy - (float)y0, fz = qz - (float)z0;
@@ -113,7 +150,7 @@ FP_DEV float sampleCells(const SimParams& P, const Home& H, const float* pool, i
       for (int dx = 0; dx < 2; dx++) {
         int s = brickSlot(P, H, dx ? bx1 : bx0, dy ? by1 : by0, dz ? bz1 : bz0);
         float w = (dx ? fx : 1.f - fx) * (dy ? fy : 1.f - fy) * (dz ? fz : 1.f - fz);
-        float val = s < 0 ? 0.f : pool[((size_t)s * ch + c) * P.N + localCell(P, x0 + dx, y0 + dy, z0 + dz)];
+        float val = s < 0 ? 0.f : ldHalf(pool, ((size_t)s * ch + c) * P.N + localCell(P, x0 + dx, y0 + dy, z0 + dz), half);
         v += val * w;
       }
   return v;

@@ -1,6 +1,8 @@
 // Host engine: see fp_engine.hpp. Citations are path:line in the reference project.
 #include "fp_engine.hpp"
 
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <chrono>
@@ -163,6 +165,7 @@ Engine::Engine(const fp_grid& g, Stepper* owner) : owner_(owner) {
   maccormack_ = g.scalar_maccormack != 0;
   precision_ = g.precision;
   budget_ = g.voxel_budget > 0 ? g.voxel_budget : 8e6;
+  measure_ = precision_ == FP_PRECISION_MIXED;  // mixed storage reports its accuracy every step
 }
 
 Engine::~Engine() {
@@ -182,7 +185,7 @@ int Engine::consume() {
 void Engine::freeAll() {
   DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_, &zeroList_,
                          &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_, &donors_, &solids_,
-                         &tileRecD_, &tileNbrD_, &hashD_};
+                         &tileRecD_, &tileNbrD_, &hashD_, &solver_};
   for (DeviceBuffer* b : all)
     if (b->ptr) {
       cudaFree(b->ptr);
@@ -204,7 +207,8 @@ int Engine::initialize() {
   int rc;
   if ((rc = check(cudaSetDevice(owner_->device()), "cudaSetDevice"))) return rc;
   freeAll();
-  if (!alloc(counters_, sizeof(FpCounters))) return FP_ENOMEM;
+  if (!alloc(counters_, sizeof(FpCounters)) || !alloc(solver_, sizeof(FpSolver))) return FP_ENOMEM;
+  lastSolver_ = FpSolver{};
   slots_ = 0;
   capacity_ = 0;
   if ((rc = allocatePools(slotLimit()))) return rc;
@@ -236,12 +240,16 @@ uint64_t Engine::estimateBytes(const fp_grid& g, uint32_t tiles) {
   uint64_t N = (uint64_t)B * B * B;
   double budget = g.voxel_budget > 0 ? g.voxel_budget : 8e6;
   uint64_t slots = (uint64_t)std::max(1.0, std::floor(budget / (double)N));
-  uint64_t perSlot = N * 4 * (4 * 3 + 4 + 3 * 4 + 1 + 1 + 3 + 3 + 8 + 2) + N * 3 * 2 + N / 8 + N + 4;
+  // FP32: velocity x4 (3 channels), curl, expansion, divergence, bounds (3+3+8), pressure x2,
+  // the scalar predictor (4); the two scalar state pools (4 channels) and the coarse levels in
+  // the precision's width.
+  const uint64_t narrow = g.precision == FP_PRECISION_MIXED ? 2 : 4;
+  uint64_t perSlot = N * 4 * (4 * 3 + 4 + 1 + 1 + 3 + 3 + 8 + 2 + 4) + N * 2 * 4 * narrow + N * 3 * 2 + N / 8 + N + 4;
   for (int l = 1; l < shift; l++) {
     uint64_t c = (uint64_t)1 << (3 * (shift - l));
-    perSlot += c * 13;
+    perSlot += c * (3 * narrow + 1);
   }
-  uint64_t perTile = 64 * (4 * 5 + FP_RECORD_WORDS * 4 + 8) + 16 + 27 * 4 + 16 + (64 + 8 + 1) * 13;
+  uint64_t perTile = 64 * (4 * 5 + FP_RECORD_WORDS * 4 + 8) + 16 + 27 * 4 + 16 + (64 + 8 + 1) * (3 * narrow + 1);
   return slots * perSlot + (uint64_t)std::max(tiles, (uint32_t)MIN_TILES) * perTile + 64 * 1024;
 }
 
@@ -275,14 +283,16 @@ int Engine::allocatePools(uint32_t slots) {
   size_t s = slots, N = N_;
   bool ok = true;
   for (auto& b : vel_) ok = ok && alloc(b, s * 3 * N * 4);
-  for (auto& b : fld_) ok = ok && alloc(b, s * 4 * N * 4);
+  // fld_[1] is the predictor within a step (FP32); fld_[0] and fld_[2] trade the state.
+  for (int k = 0; k < 3; k++) ok = ok && alloc(fld_[k], s * 4 * N * (k == 1 ? 4 : scalarBytes()));
   ok = ok && alloc(curl_, s * 4 * N * 4) && alloc(expn_, s * N * 4) && alloc(div_, s * N * 4) &&
        alloc(vmin_, s * 3 * N * 4) && alloc(vmax_, s * 3 * N * 4) && alloc(sb_, s * 8 * N * 4) &&
        alloc(donors_, s * 3 * N * 2) && alloc(solids_, s * W_ * 4) && alloc(p0_[0], s * N * 4) &&
        alloc(p0_[1], s * N * 4) && alloc(topo_[0], s * N) && alloc(freeStack_, s * 4);
   for (int l = 1; l < brickLevels_ && ok; l++) {
     size_t c = s * levelCells(l);
-    ok = alloc(lp_[l][0], c * 4) && alloc(lp_[l][1], c * 4) && alloc(lrhs_[l], c * 4) && alloc(topo_[l], c);
+    ok = alloc(lp_[l][0], c * coarseBytes()) && alloc(lp_[l][1], c * coarseBytes()) &&
+         alloc(lrhs_[l], c * coarseBytes()) && alloc(topo_[l], c);
   }
   if (!ok) return FP_ENOMEM;
   std::vector<uint32_t> stack(slots);
@@ -304,14 +314,15 @@ int Engine::growPool(uint32_t target) {
   uint32_t added = target - slots_;
   bool ok = true;
   for (auto& b : vel_) ok = ok && grow(b, s * 3 * N * 4, 0);
-  for (auto& b : fld_) ok = ok && grow(b, s * 4 * N * 4, 0);
+  for (int k = 0; k < 3; k++) ok = ok && grow(fld_[k], s * 4 * N * (k == 1 ? 4 : scalarBytes()), 0);
   ok = ok && grow(curl_, s * 4 * N * 4, 0) && grow(expn_, s * N * 4, 0) && grow(div_, s * N * 4, 0) &&
        grow(vmin_, s * 3 * N * 4, 0) && grow(vmax_, s * 3 * N * 4, 0) && grow(sb_, s * 8 * N * 4, 0) &&
        grow(donors_, s * 3 * N * 2, 0) && grow(solids_, s * W_ * 4, 0) && grow(p0_[0], s * N * 4, 0) &&
        grow(p0_[1], s * N * 4, 0) && grow(topo_[0], s * N, 0);
   for (int l = 1; l < brickLevels_ && ok; l++) {
     size_t c = s * levelCells(l);
-    ok = grow(lp_[l][0], c * 4, 0) && grow(lp_[l][1], c * 4, 0) && grow(lrhs_[l], c * 4, 0) && grow(topo_[l], c, 0);
+    ok = grow(lp_[l][0], c * coarseBytes(), 0) && grow(lp_[l][1], c * coarseBytes(), 0) &&
+         grow(lrhs_[l], c * coarseBytes(), 0) && grow(topo_[l], c, 0);
   }
   if (!ok) return FP_ENOMEM;
   std::vector<uint32_t> old(slots_);
@@ -353,8 +364,8 @@ int Engine::setCapacity(int capacity) {
   }
   for (int l = brickLevels_; l <= bottom_; l++) {
     size_t c = (size_t)capacity * levelCells(l);
-    ok = ok && grow(lp_[l][0], c * 4, 0) && grow(lp_[l][1], c * 4, 0) && grow(lrhs_[l], c * 4, 0) &&
-         grow(topo_[l], c, 0);
+    ok = ok && grow(lp_[l][0], c * coarseBytes(), 0) && grow(lp_[l][1], c * coarseBytes(), 0) &&
+         grow(lrhs_[l], c * coarseBytes(), 0) && grow(topo_[l], c, 0);
   }
   if (!ok) return FP_ENOMEM;
   capacity_ = capacity;
@@ -775,6 +786,11 @@ void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t
   P.p0[0] = (float*)p0_[0].ptr;
   P.p0[1] = (float*)p0_[1].ptr;
   P.latest = latest_;
+  P.scalarHalf = precision_ == FP_PRECISION_MIXED ? 1 : 0;
+  P.coarseBf16 = precision_ == FP_PRECISION_MIXED ? 1 : 0;
+  P.vcycles = vcycles_;
+  P.tolerance = tolerance_;
+  P.solver = (FpSolver*)solver_.ptr;
   for (int l = 0; l <= bottom_; l++) {
     P.topo[l] = (uint8_t*)topo_[l].ptr;
     if (l > 0) {
@@ -805,7 +821,8 @@ void Engine::launched(float dt, int latest) {
 // measurement lags the step by exactly one.
 void Engine::applyReadback(const uint32_t* words) {
   const FpCounters* c = (const FpCounters*)words;
-  const uint32_t* flags = words + sizeof(FpCounters) / 4;
+  std::memcpy(&lastSolver_, words + sizeof(FpCounters) / 4, sizeof(FpSolver));
+  const uint32_t* flags = words + (sizeof(FpCounters) + sizeof(FpSolver)) / 4;
   contentTiles_.clear();
   for (int s = 0; s < capacity_ && s < (int)tileRec_.size(); s++)
     if (flags[s] && tileRec_[s].w != 0) contentTiles_.push_back({tileRec_[s], flags[s]});
@@ -823,6 +840,33 @@ int Engine::reset() {
   return initialize();
 }
 
+// The latest step's pressure solve, once the step's work is done.
+int Engine::readSolver(fp_solver_stats* out) {
+  int rc = consume();
+  if (rc) return rc;
+  if ((rc = check(cudaStreamSynchronize(stream()), "read solver"))) return rc;
+  FpSolver S{};
+  if ((rc = check(cudaMemcpy(&S, solver_.ptr, sizeof(FpSolver), cudaMemcpyDeviceToHost), "read solver"))) return rc;
+  std::memset(out, 0, sizeof(*out));
+  out->vcycles = (uint32_t)S.cycles;
+  out->unknowns = S.unknowns;
+  out->rhs_rms = S.unknowns > 0 ? std::sqrt(S.rhs2 / S.unknowns) : 0.0;
+  for (int c = 0; c < S.cycles && c < FP_MAX_VCYCLES; c++)
+    out->residual[c] = S.rhs2 > 0 ? std::sqrt(S.res2[c] / S.rhs2) : 0.0;
+  out->divergence = S.measured && S.vel2 > 0 ? std::sqrt(S.div2 / S.vel2) : -1.0;
+  out->measured = S.measured;
+  return FP_OK;
+}
+
+int Engine::setSolver(int vcycles, float tolerance) {
+  if (vcycles < 1 || vcycles > FP_MAX_VCYCLES)
+    return fail(FP_EINVAL, "vcycles must be from 1 to " + std::to_string(FP_MAX_VCYCLES) + ".");
+  if (!std::isfinite(tolerance) || tolerance < 0.f) return fail(FP_EINVAL, "tolerance must be finite and nonnegative.");
+  vcycles_ = vcycles;
+  tolerance_ = tolerance;
+  return FP_OK;
+}
+
 int Engine::setRuntime(float cutoff, double budget, int ground) {
   if (!std::isfinite(cutoff)) return fail(FP_EINVAL, "grid.cutoff must be a finite number from 0 to 1.");
   cutoff_ = cutoff;
@@ -835,7 +879,7 @@ uint64_t Engine::memoryBytes() const {
   uint64_t bytes = 0;
   const DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_,
                                &zeroList_, &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_,
-                               &donors_, &solids_, &tileRecD_, &tileNbrD_, &hashD_};
+                               &donors_, &solids_, &tileRecD_, &tileNbrD_, &hashD_, &solver_};
   for (const DeviceBuffer* b : all) bytes += b->bytes;
   for (auto& b : vel_) bytes += b.bytes;
   for (auto& b : fld_) bytes += b.bytes;
@@ -859,8 +903,12 @@ int Engine::stats(fp_stats* out) {
   out->tile_capacity = (uint32_t)capacity_;
   out->failures = lastFailures_;
   out->memory_bytes = memoryBytes();
-  out->last_vcycles = steps_ > 0 ? 1 : 0;
-  out->last_residual = -1;
+  // The pressure solve's measurements travel with the next step's measurement: these are the
+  // step before the latest one's (readSolver gives the latest step's).
+  const FpSolver& S = lastSolver_;
+  out->last_vcycles = S.cycles > 0 ? (uint32_t)S.cycles : (steps_ > 1 ? 1u : 0u);
+  out->last_residual = S.cycles > 0 && S.rhs2 > 0 ? std::sqrt(S.res2[S.cycles - 1] / S.rhs2) : -1.0;
+  out->last_divergence = S.measured && S.vel2 > 0 ? std::sqrt(S.div2 / S.vel2) : -1.0;
   out->kernel_launches = owner_->launches();
   out->h2d_bytes = stepH2d_;
   out->d2h_bytes = stepD2h_;
@@ -886,6 +934,13 @@ int Engine::readField(int field, float* host, size_t bytes) {
   int rc = consume();
   if (rc) return rc;
   if ((rc = check(cudaStreamSynchronize(stream()), "read field"))) return rc;
+  if (field == FP_FIELD_SCALARS && scalarBytes() == 2) {
+    // FP16 storage: widened to FP32 for the caller.
+    std::vector<__half> raw(need / 4);
+    if ((rc = check(cudaMemcpy(raw.data(), b->ptr, raw.size() * 2, cudaMemcpyDeviceToHost), "read field"))) return rc;
+    for (size_t i = 0; i < raw.size(); i++) host[i] = __half2float(raw[i]);
+    return FP_OK;
+  }
   return check(cudaMemcpy(host, b->ptr, need, cudaMemcpyDeviceToHost), "read field");
 }
 

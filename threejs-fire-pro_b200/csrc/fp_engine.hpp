@@ -102,7 +102,14 @@ class Engine {
   bool solidsAll() const { return solidsStale_; }
   bool topoAll() const { return geometryDirty_; }
   int capacity() const { return capacity_; }
-  size_t readbackWords() const { return sizeof(FpCounters) / 4 + (size_t)capacity_; }
+  size_t readbackWords() const { return (sizeof(FpCounters) + sizeof(FpSolver)) / 4 + (size_t)capacity_; }
+  // Pressure solve (no reference counterpart; the reference runs one V-cycle): up to
+  // `vcycles` V-cycles a step, stopping at a relative FP64 residual of `tolerance` (0: all).
+  int setSolver(int vcycles, float tolerance);
+  int readSolver(fp_solver_stats* out);
+  int vcycles() const { return vcycles_; }
+  // Whether the step measures the residual and the post-projection divergence.
+  bool measures() const { return vcycles_ > 1 || tolerance_ > 0.f || measure_; }
   // After the launch: buffers rotate, time advances; the measurement is pending.
   void launched(float dt, int latest);
   // The measurement this simulation's last launch wrote (readActivity, FluidSimulation.ts:1701-1746).
@@ -138,6 +145,10 @@ class Engine {
   uint32_t activeBricks_ = 0, usedSlots_ = 0, lastFailures_ = 0;
   bool poolLimited_ = false;
   int latest_ = 0;  // index of the latest pressure solution
+  int vcycles_ = 1;
+  float tolerance_ = 0.f;
+  bool measure_ = false;
+  FpSolver lastSolver_{};
   uint32_t slots_ = 0;
   uint64_t stepH2d_ = 0, stepD2h_ = 0;
 
@@ -146,7 +157,7 @@ class Engine {
   DeviceBuffer freeStack_, counters_;
   DeviceBuffer vel_[4], curl_, fld_[3], expn_, div_, vmin_, vmax_, sb_, donors_, solids_;
   DeviceBuffer p0_[2], topo_[FP_MAX_LEVELS], lp_[FP_MAX_LEVELS][2], lrhs_[FP_MAX_LEVELS];
-  DeviceBuffer tileRecD_, tileNbrD_, hashD_;
+  DeviceBuffer tileRecD_, tileNbrD_, hashD_, solver_;
   int velIdx_[4] = {0, 1, 2, 3};  // start, predictor/projected, corrected, forced
   int fldIdx_[3] = {0, 1, 2};     // start, predictor, evolved
 
@@ -165,6 +176,9 @@ class Engine {
   FpFlame flame_;
 
   cudaStream_t stream() const;
+  // Bytes a value of the scalar pools and of the coarse multigrid levels takes.
+  size_t scalarBytes() const { return precision_ == FP_PRECISION_MIXED ? 2 : 4; }
+  size_t coarseBytes() const { return precision_ == FP_PRECISION_MIXED ? 2 : 4; }
   bool alloc(DeviceBuffer& b, size_t bytes, bool zero = true);
   bool grow(DeviceBuffer& b, size_t bytes, int fill);  // keeps contents
   bool upload(DeviceBuffer& b, const void* src, size_t bytes);
@@ -263,7 +277,9 @@ class Stepper {
   std::unordered_map<uint64_t, GraphEntry> graphs_;
   void clearGraphs();
   FpBatch batch() const;
-  void enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl, int& latest, uint64_t& launches);
+  void enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl, int vcycles, bool measure, int& latest,
+               uint64_t& launches);
+  int cycle_ = 0;  // the V-cycle being enqueued
   void vcycle(int level, int cur[], uint64_t& launches);
   int check(cudaError_t e, const char* what);
   int reserve(size_t arenaBytes, int sims, size_t readWords);

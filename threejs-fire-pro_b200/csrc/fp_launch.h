@@ -27,6 +27,7 @@ void fp_launch_noise(float4* noise, cudaStream_t st);
 struct MgSel {
   int level;  // output level
   int rhs, pin, coarse, pout, cfirst;
+  int cycle;  // V-cycle of the step: from the second on, simulations that converged skip
 };
 inline int fp_mg_sel(int level, int which) { return level * 4 + which; }
 void fp_launch_topology(const FpBatch& bt, bool anyAll, int sms, cudaStream_t st);
@@ -35,6 +36,13 @@ void fp_launch_restrict(const FpBatch& bt, const MgSel& S, bool tiles, int B, in
 void fp_launch_prolong(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st);
 // The bottom level's iterations, a CTA per simulation.
 void fp_launch_bottom(const FpBatch& bt, const MgSel& S, int iterations, int sms, cudaStream_t st);
+// After V-cycle `cycle`: the FP64 sums of squares of the finest level's residual (and, after
+// the first, of its right-hand side) over the unknowns, then each simulation's convergence
+// decision. A simulation that converged skips the later cycles.
+void fp_launch_residual(const FpBatch& bt, int pSel, int cycle, int sms, cudaStream_t st);
+// After the projection: FP64 sums of squares of h x divergence and of the face velocities over
+// the interior unknowns.
+void fp_launch_post_divergence(const FpBatch& bt, int sms, cudaStream_t st);
 // Size the staged brick-level multigrid kernels for bricks of B cells (once per brick size).
 void fp_mg_configure(int B);
 // Set the step kernels' shared-memory limits (before any launch or stream capture).

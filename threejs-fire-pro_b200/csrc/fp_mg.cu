@@ -60,9 +60,11 @@ FP_DEV float diagOf(uint32_t f) {
   return (float)((f >> 0) & 1u) + (float)((f >> 1) & 1u) + ((float)((f >> 2) & 1u) + (float)((f >> 3) & 1u)) +
          ((float)((f >> 4) & 1u) + (float)((f >> 5) & 1u));
 }
+// Levels above the finest hold BF16 values in FP_PRECISION_MIXED.
+FP_DEV bool narrowLevel(const SimParams& P, int level) { return level > 0 && P.coarseBf16 != 0; }
 FP_DEV float readAt(const SimParams& P, const Home& H, const float* arr, int px, int py, int pz, int level) {
   long a = cellAddress(P, H, px, py, pz, level);
-  return a < 0 ? 0.f : arr[a];
+  return a < 0 ? 0.f : ldBf(arr, a, narrowLevel(P, level));
 }
 // stencil (pressure.wgsl:360-402): open neighbours' sum; cubic cells weigh 1 on every axis.
 FP_DEV float stencilSum(const SimParams& P, const Home& H, const float* p, int px, int py, int pz, uint32_t f,
@@ -110,6 +112,8 @@ struct Args {
   const float* coarse;
   float* pout;
   float* cfirst;
+  bool rhsN, pinN, coarseN, poutN, cfirstN;  // the buffer holds BF16
+  bool skip;                                 // a later V-cycle of a converged solve: no work
 };
 
 // A launch names its buffers by selector, level * 4 + which (0 and 1 the level's pressure
@@ -128,24 +132,30 @@ FP_DEV Args resolve(const SimParams& P, const MgSel& S) {
   A.coarse = mgBuffer(P, S.coarse);
   A.pout = mgBuffer(P, S.pout);
   A.cfirst = mgBuffer(P, S.cfirst);
+  A.rhsN = S.rhs >= 0 && narrowLevel(P, S.rhs >> 2);
+  A.pinN = S.pin >= 0 && narrowLevel(P, S.pin >> 2);
+  A.coarseN = S.coarse >= 0 && narrowLevel(P, S.coarse >> 2);
+  A.poutN = S.pout >= 0 && narrowLevel(P, S.pout >> 2);
+  A.cfirstN = S.cfirst >= 0 && narrowLevel(P, S.cfirst >> 2);
+  A.skip = S.cycle > 0 && P.solver->converged != 0;
   return A;
 }
 
 FP_DEV void relaxCell(const SimParams& P, const Home& H, const Args& A, long a, int px, int py, int pz) {
   uint32_t f = expandFlags(P.topo[A.level][a]);
   if ((f & SOLIDF) || !activeCell(P, H, px, py, pz, A.level)) {
-    A.pout[a] = 0.f;
+    stBf(A.pout, a, 0.f, A.poutN);
     return;
   }
   float sum = stencilSum(P, H, A.pin, px, py, pz, f, A.level);
-  float cand = (sum - A.rhs[a]) / fmaxf(diagOf(f), 1e-12f);
-  A.pout[a] = mixf(A.pin[a], cand, 0.8f);
+  float cand = (sum - ldBf(A.rhs, a, A.rhsN)) / fmaxf(diagOf(f), 1e-12f);
+  stBf(A.pout, a, mixf(ldBf(A.pin, a, A.pinN), cand, 0.8f), A.poutN);
 }
 
 FP_DEV void prolongCell(const SimParams& P, const Home& H, const Args& A, long a, int px, int py, int pz) {
   uint32_t f = expandFlags(P.topo[A.level][a]);
   if ((f & SOLIDF) || !activeCell(P, H, px, py, pz, A.level)) {
-    A.pout[a] = 0.f;
+    stBf(A.pout, a, 0.f, A.poutN);
     return;
   }
   int cl = A.level + 1;
@@ -162,7 +172,7 @@ FP_DEV void prolongCell(const SimParams& P, const Home& H, const Args& A, long a
   }
   float corr = mixf(mixf(mixf(v[0], v[1], fx), mixf(v[2], v[3], fx), fy), mixf(mixf(v[4], v[5], fx), mixf(v[6], v[7], fx), fy),
                     fz);
-  A.pout[a] = A.pin[a] + corr;
+  stBf(A.pout, a, ldBf(A.pin, a, A.pinN) + corr, A.poutN);
 }
 
 // restrictCell (pressure.wgsl:601-647): (cx,cy,cz) is a cell of the coarse (output) level.
@@ -179,18 +189,18 @@ FP_DEV void restrictCell(const SimParams& P, const Home& H, const Args& A, long 
       uint32_t f = expandFlags(P.topo[fine][a]);
       if (!(f & SOLIDF)) {
         float sum = stencilSum(P, H, A.pin, px, py, pz, f, fine);
-        residual += A.rhs[a] - (sum - diagOf(f) * A.pin[a]);
+        residual += ldBf(A.rhs, a, A.rhsN) - (sum - diagOf(f) * ldBf(A.pin, a, A.pinN));
       }
     }
   }
   float r = residual * 0.5f;
-  A.pout[out] = r;  // the coarse right-hand side
+  stBf(A.pout, out, r, A.poutN);  // the coarse right-hand side
   float first = 0.f;
   if (every) {
     uint32_t f = expandFlags(P.topo[A.level][out]);
     if (!(f & SOLIDF)) first = mixf(0.f, (0.f - r) / fmaxf(diagOf(f), 1e-12f), 0.8f);
   }
-  A.cfirst[out] = first;
+  stBf(A.cfirst, out, first, A.cfirstN);
 }
 
 template <int OP>
@@ -222,10 +232,10 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t base = blockIdx.x * NG; base < total; base += gridDim.x * NG) {
     uint32_t item = base + g;
-    const bool has = item < total;
     uint32_t i;
-    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, has ? item : base, i);
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item < total ? item : base, i);
     const Args A = resolve(P, Sl);
+    const bool has = item < total && !A.skip;
     const int bl = P.brickLevels;
     const int fineLevel = OP == RESTRICT ? A.level - 1 : A.level;
     const int stageLevel = OP == PROLONG ? A.level + 1 : fineLevel;
@@ -237,6 +247,7 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
     float* st = stAll + g * (S3 + (S3 + 3) / 4);
     uint8_t* solidSt = reinterpret_cast<uint8_t*>(st + S3);
     const float* src = OP == PROLONG ? A.coarse : A.pin;
+    const bool srcN = OP == PROLONG ? A.coarseN : A.pinN;
     const int fs = levelShift(P, fineLevel), fside = 1 << fs, fcells = fside * fside * fside;
     const uint32_t id = has ? P.active[i] : 0u;
     Home H = homeOf(P, id, nslot);
@@ -252,7 +263,7 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
       for (int q = t; q < S3; q += GROUP) {
         int lx = q % S, ly = (q / S) % S, lz = q / S2;
         long a = cellAddress(P, H, ox + lx, oy + ly, oz + lz, stageLevel);
-        st[q] = a < 0 ? 0.f : src[a];
+        st[q] = a < 0 ? 0.f : ldBf(src, a, srcN);
         if (OP == PROLONG) solidSt[q] = a >= 0 && (P.topo[stageLevel][a] & FP_STORED_SOLID) ? 1 : 0;
       }
     }
@@ -304,13 +315,13 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
           long a = slot * fcells + o;
           uint32_t f = expandFlags(P.topo[fineLevel][a]);
           if ((f & SOLIDF) || !unknown(lx, ly, lz)) {
-            A.pout[a] = 0.f;
+            stBf(A.pout, a, 0.f, A.poutN);
             continue;
           }
           if (OP == RELAX) {
             float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
-            float cand = (sumAt(lx, ly, lz, f) - A.rhs[a]) / fmaxf(diagOf(f), 1e-12f);
-            A.pout[a] = mixf(center, cand, 0.8f);
+            float cand = (sumAt(lx, ly, lz, f) - ldBf(A.rhs, a, A.rhsN)) / fmaxf(diagOf(f), 1e-12f);
+            stBf(A.pout, a, mixf(center, cand, 0.8f), A.poutN);
           } else {
             int px = H.bx * fside + lx, py = H.by * fside + ly, pz = H.bz * fside + lz;
             float qx = ((float)px + 0.5f) * 0.5f - 0.5f, qy = ((float)py + 0.5f) * 0.5f - 0.5f,
@@ -327,7 +338,7 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
             }
             float corr = mixf(mixf(mixf(v[0], v[1], fx), mixf(v[2], v[3], fx), fy),
                               mixf(mixf(v[4], v[5], fx), mixf(v[6], v[7], fx), fy), fz);
-            A.pout[a] = A.pin[a] + corr;
+            stBf(A.pout, a, ldBf(A.pin, a, A.pinN) + corr, A.poutN);
           }
         }
       } else {  // RESTRICT: coarse cells of this brick at A.level
@@ -345,19 +356,19 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
               uint32_t f = expandFlags(P.topo[fineLevel][a]);
               if (!(f & SOLIDF)) {
                 float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
-                residual += A.rhs[a] - (sumAt(lx, ly, lz, f) - diagOf(f) * center);
+                residual += ldBf(A.rhs, a, A.rhsN) - (sumAt(lx, ly, lz, f) - diagOf(f) * center);
               }
             }
           }
           float r = residual * 0.5f;
           long out = slot * ccells + o;
-          A.pout[out] = r;
+          stBf(A.pout, out, r, A.poutN);
           float first = 0.f;
           if (every) {
             uint32_t f = expandFlags(P.topo[A.level][out]);
             if (!(f & SOLIDF)) first = mixf(0.f, (0.f - r) / fmaxf(diagOf(f), 1e-12f), 0.8f);
           }
-          A.cfirst[out] = first;
+          stBf(A.cfirst, out, first, A.cfirstN);
         }
       }
     }
@@ -388,6 +399,7 @@ __global__ void __launch_bounds__(64) k_level_tiles(FpBatch bt, MgSel Sl) {
     const SimParams& P = workSim(bt, FP_WORK_TILES, item, local);
     const int t = (int)local;
     const Args A = resolve(P, Sl);
+    if (A.skip) continue;  // the same for the whole CTA
     int s = levelShift(P, A.level), side = 1 << s, cells = side * side * side;
     int4 rec = __ldg(&P.tileRec[t]);
     if (rec.w == 0) continue;
@@ -412,12 +424,15 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
   for (int sim = blockIdx.x; sim < sims; sim += gridDim.x) {
     const SimParams& P = bt.sims[sim];
     const Args A = resolve(P, Sl);
+    if (A.skip) continue;  // the same for the whole CTA
     const int level = A.level;
     int cap = P.capacity;
     bool inShared = (long)cap * 12 <= (long)smemBytes;
-    // In global memory: cur starts in pout (a copy of pin), nxt is pin's buffer.
+    // In global memory: cur starts in pout (a copy of pin), nxt is pin's buffer; both hold the
+    // level's storage type (gN). Shared memory holds FP32.
     float* cur = inShared ? bottomSmem : A.pout;
     float* nxt = inShared ? bottomSmem + cap : const_cast<float*>(A.pin);
+    const bool gN = !inShared && A.poutN;
     uint32_t* flags = inShared ? reinterpret_cast<uint32_t*>(bottomSmem + 2 * cap) : nullptr;
     auto flagOf = [&](int t) -> uint32_t {
       int4 rec = __ldg(&P.tileRec[t]);
@@ -432,7 +447,8 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
       uint32_t f = flagOf(t);
       // Cells that are no unknown are never read and become zero in the first iteration.
       if (inShared) flags[t] = f;
-      cur[t] = (f & 0x80000000u) && !(f & SOLIDF) ? A.pin[t] : 0.f;
+      // pin and pout are the level's two buffers: the copy into pout reads no value it wrote.
+      stBf(cur, t, (f & 0x80000000u) && !(f & SOLIDF) ? ldBf(A.pin, t, A.pinN) : 0.f, gN);
     }
     __syncthreads();
     for (int it = 0; it < iterations; it++) {
@@ -444,13 +460,13 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
 #pragma unroll
           for (int k = 0; k < 6; k++) {
             int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
-            w[k] = n >= 0 ? cur[n] : 0.f;
+            w[k] = n >= 0 ? ldBf(cur, n, gN) : 0.f;
           }
           float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
-          float cand = (sum - A.rhs[t]) / fmaxf(diagOf(f & 63u), 1e-12f);
-          next = mixf(cur[t], cand, 0.8f);
+          float cand = (sum - ldBf(A.rhs, t, A.rhsN)) / fmaxf(diagOf(f & 63u), 1e-12f);
+          next = mixf(ldBf(cur, t, gN), cand, 0.8f);
         }
-        nxt[t] = next;
+        stBf(nxt, t, next, gN);
       }
       __syncthreads();
       float* tmp = cur;
@@ -459,9 +475,64 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
     }
     for (int t = threadIdx.x; t < cap; t += blockDim.x) {
       uint32_t f = inShared ? flags[t] : flagOf(t);
-      if ((f & 0x80000000u) && cur != A.pout) A.pout[t] = cur[t];
+      if ((f & 0x80000000u) && cur != A.pout) stBf(A.pout, t, ldBf(cur, t, gN), A.poutN);
     }
     __syncthreads();
+  }
+}
+
+// The finest level's residual rhs - (sum - diag p) over its unknowns, as restrictCell forms
+// it, squared and summed in FP64 per simulation.
+__global__ void __launch_bounds__(256) k_residual(FpBatch bt, int pSel, int cycle) {
+  __shared__ int nslot[27];
+  __shared__ double scratch[32];
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
+    if (cycle > 0 && P.solver->converged) continue;  // the same for the whole CTA
+    Home H = enterBrick(P, P.active[i], nslot);
+    const float* p = P.p0[pSel];
+    const long slot = nslot[13];
+    const int m = P.B - 1;
+    double r2 = 0.0, b2 = 0.0, n = 0.0;
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int x = H.bx * P.B + (c & m), y = H.by * P.B + ((c >> P.shift) & m), z = H.bz * P.B + (c >> (2 * P.shift));
+      long a = slot * P.N + c;
+      uint32_t f = expandFlags(P.topo[0][a]);
+      if ((f & SOLIDF) || !activeCell(P, H, x, y, z, 0)) continue;
+      float rhs = P.div[a];
+      float r = rhs - (stencilSum(P, H, p, x, y, z, f, 0) - diagOf(f) * p[a]);
+      r2 += (double)r * (double)r;
+      b2 += (double)rhs * (double)rhs;
+      n += 1.0;
+    }
+    r2 = blockSum(r2, scratch);
+    b2 = blockSum(b2, scratch);
+    n = blockSum(n, scratch);
+    if (threadIdx.x == 0) {
+      atomicAdd(&P.solver->res2[cycle], r2);
+      if (cycle == 0) {
+        atomicAdd(&P.solver->rhs2, b2);
+        atomicAdd(&P.solver->unknowns, n);
+      }
+    }
+  }
+}
+
+// Each simulation's decision after V-cycle `cycle`: converged once the residual's RMS is at
+// most the tolerance times the right-hand side's. One CTA.
+__global__ void k_converge(FpBatch bt, int cycle) {
+  int sims = batchCount(bt);
+  for (int sim = threadIdx.x; sim < sims; sim += blockDim.x) {
+    const SimParams& P = bt.sims[sim];
+    FpSolver* S = P.solver;
+    if (cycle > 0 && S->converged) continue;
+    S->cycles = cycle + 1;
+    double tol = (double)P.tolerance;
+    // Done: the residual met the tolerance, or this simulation's own cycle limit is reached
+    // (the launch runs as many cycles as its most demanding simulation).
+    if ((tol > 0.0 && S->res2[cycle] <= tol * tol * S->rhs2) || cycle + 1 >= P.vcycles) S->converged = 1;
   }
 }
 
@@ -627,4 +698,9 @@ void fp_launch_prolong(const FpBatch& bt, const MgSel& S, bool tiles, int B, int
 }
 void fp_launch_bottom(const FpBatch& bt, const MgSel& S, int iterations, int sms, cudaStream_t st) {
   k_bottom<<<sms, 1024, BOTTOM_SMEM, st>>>(bt, S, iterations, BOTTOM_SMEM);
+}
+
+void fp_launch_residual(const FpBatch& bt, int pSel, int cycle, int sms, cudaStream_t st) {
+  k_residual<<<sms * 4, 256, 0, st>>>(bt, pSel, cycle);
+  k_converge<<<1, 256, 0, st>>>(bt, cycle);
 }

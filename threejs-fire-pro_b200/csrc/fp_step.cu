@@ -31,6 +31,7 @@ struct Field {
   const float* pool;
   int ch;
   const float* sm;
+  bool half;  // the pool holds __half (the scalar pools in FP_PRECISION_MIXED)
 };
 
 FP_DEV float fieldCell(const SimParams& P, const Home& H, const Stage& G, const Field& f, int c, int x, int y, int z) {
@@ -39,7 +40,7 @@ FP_DEV float fieldCell(const SimParams& P, const Home& H, const Stage& G, const 
     if (lx < (unsigned)G.S && ly < (unsigned)G.S && lz < (unsigned)G.S)
       return f.sm[c * G.S3 + ((int)lz * G.S + (int)ly) * G.S + (int)lx];
   }
-  return cellAt(P, H, f.pool, f.ch, c, x, y, z);
+  return cellAt(P, H, f.pool, f.ch, c, x, y, z, f.half);
 }
 
 // Trilinear sample at `pos` in cell units (fluid-sampling.wgsl:85-114).
@@ -65,13 +66,25 @@ FP_DEV float fieldSample(const SimParams& P, const Home& H, const Stage& G, cons
       return v;
     }
   }
-  return sampleCells(P, H, f.pool, f.ch, c, px, py, pz);
+  return sampleCells(P, H, f.pool, f.ch, c, px, py, pz, f.half);
 }
 
 // Copy channels of a pool over the staged box into shared memory, zero where no slot, with
 // asynchronous 4-byte copies (cp.async): every thread keeps all its copies in flight and the
-// caller waits once. A brick without a slot reads nothing (source size 0 zero-fills).
-FP_DEV void stageField(const SimParams& P, const Home& H, const Stage& G, float* sm, const float* pool, int ch) {
+// caller waits once. A brick without a slot reads nothing (source size 0 zero-fills). A half
+// pool is widened to FP32 on the way (plain loads: cp.async moves at least 4 bytes).
+FP_DEV void stageField(const SimParams& P, const Home& H, const Stage& G, float* sm, const float* pool, int ch,
+                       bool half = false) {
+  if (half) {
+    for (int i = threadIdx.x; i < G.S3; i += blockDim.x) {
+      int lx = i % G.S, ly = (i / G.S) % G.S, lz = i / (G.S * G.S);
+      int x = G.ox + lx, y = G.oy + ly, z = G.oz + lz;
+      int s = brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift);
+      size_t base = s < 0 ? 0 : (size_t)s * ch * P.N + localCell(P, x, y, z);
+      for (int c = 0; c < ch; c++) sm[c * G.S3 + i] = s < 0 ? 0.f : ldHalf(pool, base + (size_t)c * P.N, true);
+    }
+    return;
+  }
   for (int i = threadIdx.x; i < G.S3; i += blockDim.x) {
     int lx = i % G.S, ly = (i / G.S) % G.S, lz = i / (G.S * G.S);
     int x = G.ox + lx, y = G.oy + ly, z = G.oz + lz;
@@ -161,10 +174,10 @@ FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
   Home H = enterBrick(P, id, nslot);
   Stage G = stageOf(P, H, STAGED);
   Field V{P.vel, 3, STAGED ? smem : nullptr};
-  Field F{P.fld, 4, STAGED ? smem + 3 * G.S3 : nullptr};
+  Field F{P.fld, 4, STAGED ? smem + 3 * G.S3 : nullptr, P.scalarHalf != 0};
   if (STAGED) {
     stageField(P, H, G, smem, P.vel, 3);
-    stageField(P, H, G, smem + 3 * G.S3, P.fld, 4);
+    stageField(P, H, G, smem + 3 * G.S3, P.fld, 4, F.half);
     stageWait();
   }
   size_t slot = (size_t)nslot[13];
@@ -249,6 +262,8 @@ FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
       out[2] = P.lifetimeZero ? 0.f : v2;
       out[3] = v3;
     }
+    // The predictor lives within the step: FP32 in every precision, so the limiter compares
+    // the corrected value with unrounded predictions.
     for (int k = 0; k < 4; k++) P.fldP[(slot * 4 + k) * N + c] = out[k];
   }
   __syncthreads();
@@ -361,7 +376,8 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
   Home H = enterBrick(P, id, nslot);
   Stage G = stageOf(P, H, STAGED);
   Field V{P.vel, 3, STAGED ? smem : nullptr};
-  Field Fp{P.fldP, 4, STAGED ? smem + 3 * G.S3 : nullptr};
+  Field Fp{P.fldP, 4, STAGED ? smem + 3 * G.S3 : nullptr, false};  // the predictor: FP32
+  const bool half = P.scalarHalf != 0;                             // the state pools
   if (STAGED) {
     stageField(P, H, G, smem, P.vel, 3);
     stageField(P, H, G, smem + 3 * G.S3, P.fldP, 4);
@@ -402,8 +418,9 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
           cvSampled = true;
           float3 vm = velocityAt(P, H, G, V, px + 0.5f * P.dt * cv.x, py + 0.5f * P.dt * cv.y, pz + 0.5f * P.dt * cv.z);
           float fx = px + P.dt * vm.x, fy = py + P.dt * vm.y, fz = pz + P.dt * vm.z;
-          const float* o = P.fld + slot * 4 * N;
-          float o0 = o[0 * N + c], o1 = o[1 * N + c], o2 = o[2 * N + c], o3 = o[3 * N + c];
+          const size_t o = slot * 4 * N + c;
+          float o0 = ldHalf(P.fld, o, half), o1 = ldHalf(P.fld, o + N, half), o2 = ldHalf(P.fld, o + 2 * N, half),
+                o3 = ldHalf(P.fld, o + 3 * N, half);
           float lifetime = a2;
           float r0, r1, r3;
           if (lmin != lmax || a2 != lmin) {
@@ -487,7 +504,7 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
     // clearDormant (fluid-common.wgsl:8-13)
     if (!injected && value[2] == 0.f && value[0] < 0.001f && value[1] < 0.001f && value[3] < 0.001f)
       value[0] = value[1] = value[2] = value[3] = 0.f;
-    for (int k = 0; k < 4; k++) P.fldN[(slot * 4 + k) * N + c] = value[k];
+    for (int k = 0; k < 4; k++) stHalf(P.fldN, (slot * 4 + k) * N + c, value[k], half);
     P.expn[slot * N + c] = expansion;
     if (expansion != 0.f) expands = true;
     // holdsContent and contentSupport (fluid-content.wgsl:22-39).
@@ -641,7 +658,8 @@ FP_DEV float3 cellForce(const SimParams& P, const Home& H, int tile, int x, int 
   float wx = ((float)x + 0.5f) * P.h, wy = ((float)y + 0.5f) * P.h, wz = ((float)z + 0.5f) * P.h;
   if (solidAt(P, H, wx, wy, wz)) return make_float3(0.f, 0.f, 0.f);
   // The evolved scalars of this step (the reference swaps field and corrected first).
-  float heat = cellAt(P, H, P.fldN, 4, 1, x, y, z), density = cellAt(P, H, P.fldN, 4, 0, x, y, z);
+  const bool half = P.scalarHalf != 0;
+  float heat = cellAt(P, H, P.fldN, 4, 1, x, y, z, half), density = cellAt(P, H, P.fldN, 4, 0, x, y, z, half);
   float3 conf = make_float3(0.f, 0.f, 0.f);
   if (P.vorticity != 0.f) {
     float c0 = cellAt(P, H, P.curl, 4, 0, x, y, z), c1 = cellAt(P, H, P.curl, 4, 1, x, y, z),
@@ -874,6 +892,50 @@ __global__ void k_noise(float4* __restrict__ out) {
                          __half2float(__float2half_rn(cz)), 0.f);
 }
 
+// The projected velocity's divergence: over the cells that are pressure unknowns, not solid,
+// with every neighbour an unknown or solid, the sum of squares of h x div u = sum over axes of
+// the face differences, and of the cell's three face velocities. FP64 sums per simulation.
+__global__ void __launch_bounds__(THREADS) k_post_divergence(FpBatch bt) {
+  __shared__ int nslot[27];
+  __shared__ double scratch[32];
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
+    Home H = enterBrick(P, P.active[i], nslot);
+    const size_t slot = (size_t)nslot[13], N = P.N;
+    double d2 = 0.0, v2 = 0.0;
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int x, y, z;
+      cellOf(P, H, c, x, y, z);
+      auto solid = [&](int qx, int qy, int qz) {
+        return solidAt(P, H, ((float)qx + 0.5f) * P.h, ((float)qy + 0.5f) * P.h, ((float)qz + 0.5f) * P.h);
+      };
+      if (solid(x, y, z) || !pressureUnknown(P, H, x, y, z)) continue;
+      bool interior = true;
+      const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+      for (int k = 0; k < 6 && interior; k++) {
+        int qx = x + off[k][0], qy = y + off[k][1], qz = z + off[k][2];
+        interior = solid(qx, qy, qz) || pressureUnknown(P, H, qx, qy, qz);
+      }
+      if (!interior) continue;
+      float u0 = P.velP[(slot * 3 + 0) * N + c], u1 = P.velP[(slot * 3 + 1) * N + c],
+            u2 = P.velP[(slot * 3 + 2) * N + c];
+      float d = (u0 - cellAt(P, H, P.velP, 3, 0, x - 1, y, z)) + (u1 - cellAt(P, H, P.velP, 3, 1, x, y - 1, z)) +
+                (u2 - cellAt(P, H, P.velP, 3, 2, x, y, z - 1));
+      d2 += (double)d * (double)d;
+      v2 += (double)u0 * u0 + (double)u1 * u1 + (double)u2 * u2;
+    }
+    d2 = blockSum(d2, scratch);
+    v2 = blockSum(v2, scratch);
+    if (threadIdx.x == 0) {
+      atomicAdd(&P.solver->div2, d2);
+      atomicAdd(&P.solver->vel2, v2);
+      P.solver->measured = 1;
+    }
+  }
+}
+
 }  // namespace
 
 // Staged kernels for 8^3 bricks: `channels` staged fields over (8 + 2 HALO)^3 cells.
@@ -922,3 +984,6 @@ void fp_launch_project(const FpBatch& bt, int pSel, int sms, cudaStream_t st) {
   k_project<<<sms * 4, THREADS, 0, st>>>(bt, pSel);
 }
 void fp_launch_noise(float4* noise, cudaStream_t st) { k_noise<<<64 * 64 * 64 / 256, 256, 0, st>>>(noise); }
+void fp_launch_post_divergence(const FpBatch& bt, int sms, cudaStream_t st) {
+  k_post_divergence<<<sms * 4, THREADS, 0, st>>>(bt);
+}

@@ -204,7 +204,8 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
   uint32_t* rowIds = work + 1 + FP_WORK_IDS * bt.stride;
   uint32_t blocks = 0, tiles = 0, ids = 0;
   size_t word = 0;
-  bool solidsFresh = false, solidsAll = false, topoAll = false, curl = false;
+  bool solidsFresh = false, solidsAll = false, topoAll = false, curl = false, measure = false;
+  int vcycles = 1;
   pending_.clear();
   for (int i = 0; i < count; i++) {
     Engine* e = sims[i];
@@ -224,6 +225,8 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
     solidsAll = solidsAll || e->solidsAll();
     topoAll = topoAll || e->topoAll();
     curl = curl || frames[i]->simulation.vorticity != 0.f;
+    vcycles = std::max(vcycles, e->vcycles());
+    measure = measure || e->measures();
   }
   rowBlocks[count] = blocks;
   rowTiles[count] = tiles;
@@ -236,16 +239,17 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
   if (profiling_) {
     // Eager launches with an event pair around each phase.
     uint64_t n = 0;
-    enqueue(solidsFresh, solidsAll, topoAll, curl, latest, n);
+    enqueue(solidsFresh, solidsAll, topoAll, curl, vcycles, measure, latest, n);
     launches_ += n;
   } else {
-    uint64_t key = (uint64_t)solidsFresh | ((uint64_t)solidsAll << 1) | ((uint64_t)topoAll << 2) | ((uint64_t)curl << 3);
+    uint64_t key = (uint64_t)solidsFresh | ((uint64_t)solidsAll << 1) | ((uint64_t)topoAll << 2) | ((uint64_t)curl << 3) |
+                   ((uint64_t)measure << 4) | ((uint64_t)vcycles << 5);
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
       GraphEntry ge{};
       if ((rc = check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture")))
         return done(rc);
-      enqueue(solidsFresh, solidsAll, topoAll, curl, ge.latest, ge.launches);
+      enqueue(solidsFresh, solidsAll, topoAll, curl, vcycles, measure, ge.latest, ge.launches);
       cudaGraph_t g = nullptr;
       rc = check(cudaStreamEndCapture(stream_, &g), "cudaStreamEndCapture");
       if (rc) return done(rc);
@@ -319,7 +323,7 @@ void Stepper::vcycle(int level, int cur[], uint64_t& launches) {
   auto sel = [](int l, int which) { return fp_mg_sel(l, which); };
   bool tiles = level >= brickLevels_;
   if (level == bottom_) {
-    MgSel S{level, sel(level, 2), sel(level, cur[level]), -1, sel(level, 1 - cur[level]), -1};
+    MgSel S{level, sel(level, 2), sel(level, cur[level]), -1, sel(level, 1 - cur[level]), -1, cycle_};
     fp_launch_bottom(batch(), S, 19, sms_, stream_);
     launches++;
     cur[level] = 1 - cur[level];
@@ -327,7 +331,7 @@ void Stepper::vcycle(int level, int cur[], uint64_t& launches) {
   }
   auto relax = [&](int n) {
     for (int i = 0; i < n; i++) {
-      MgSel S{level, sel(level, 2), sel(level, cur[level]), -1, sel(level, 1 - cur[level]), -1};
+      MgSel S{level, sel(level, 2), sel(level, cur[level]), -1, sel(level, 1 - cur[level]), -1, cycle_};
       fp_launch_relax(batch(), S, tiles, B_, sms_, stream_);
       launches++;
       cur[level] = 1 - cur[level];
@@ -335,12 +339,12 @@ void Stepper::vcycle(int level, int cur[], uint64_t& launches) {
   };
   if (level > 0) relax(2);
   int coarse = level + 1;
-  MgSel R{coarse, sel(level, 2), sel(level, cur[level]), -1, sel(coarse, 2), sel(coarse, 1)};
+  MgSel R{coarse, sel(level, 2), sel(level, cur[level]), -1, sel(coarse, 2), sel(coarse, 1), cycle_};
   fp_launch_restrict(batch(), R, coarse >= brickLevels_, B_, sms_, stream_);
   launches++;
   cur[coarse] = 1;
   vcycle(coarse, cur, launches);
-  MgSel Pr{level, -1, sel(level, cur[level]), sel(coarse, cur[coarse]), sel(level, 1 - cur[level]), -1};
+  MgSel Pr{level, -1, sel(level, cur[level]), sel(coarse, cur[coarse]), sel(level, 1 - cur[level]), -1, cycle_};
   fp_launch_prolong(batch(), Pr, tiles, B_, sms_, stream_);
   launches++;
   cur[level] = 1 - cur[level];
@@ -349,7 +353,8 @@ void Stepper::vcycle(int level, int cur[], uint64_t& launches) {
 
 // The step's kernels, measurement and its event, enqueued on the stream (eagerly, or under
 // capture into a graph). `latest` receives the finest level's buffer holding the solution.
-void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl, int& latest, uint64_t& launches) {
+void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl, int vcycles, bool measure, int& latest,
+                      uint64_t& launches) {
   FpBatch bt = batch();
   launches = 0;
   phaseBegin(PH_ALLOC);
@@ -403,14 +408,30 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   cur[0] = 1;
   phaseBegin(PH_MULTIGRID);
   uint64_t mg = 0;
-  vcycle(0, cur, mg);
+  // Up to `vcycles` V-cycles. Each leaves the finest level's result in the buffer it started
+  // from (four flips: prolongation and three sweeps), so a simulation that converged and skips
+  // the later cycles ends in the same buffer. After each cycle, when measured, the FP64
+  // residual decides convergence.
+  for (int c = 0; c < vcycles; c++) {
+    cycle_ = c;
+    vcycle(0, cur, mg);
+    if (vcycles > 1 || measure) {
+      fp_launch_residual(bt, cur[0], c, sms_, stream_);
+      mg += 2;
+    }
+  }
+  cycle_ = 0;
   launches += mg;
   phaseEnd(PH_MULTIGRID, (int)mg);
   latest = cur[0];
   phaseBegin(PH_PROJECT);
   fp_launch_project(bt, latest, sms_, stream_);
   launches++;
-  phaseEnd(PH_PROJECT, 1);
+  if (measure) {
+    fp_launch_post_divergence(bt, sms_, stream_);
+    launches++;
+  }
+  phaseEnd(PH_PROJECT, measure ? 2 : 1);
 }
 
 }  // namespace fp

@@ -83,6 +83,20 @@ struct FpCounters {
   uint32_t frees, requests, granted, pad;
 };
 
+// The pressure solve's measurements of one step (device). Sums are FP64: the norms decide
+// convergence. The post-projection divergence is measured over the same unknowns.
+#define FP_MAX_VCYCLES 16
+struct FpSolver {
+  double rhs2;                  // sum of squares of the right-hand side over the unknowns
+  double res2[FP_MAX_VCYCLES];  // sum of squares of the residual after each V-cycle
+  double div2, vel2;            // post-projection divergence x h, and face velocity: sums of squares
+  double unknowns;              // unknown cells counted
+  int cycles;                   // V-cycles run
+  int converged;                // the latest norm met the tolerance: later cycles skip
+  int measured;                 // the post-projection divergence was measured
+  int pad;
+};
+
 struct SimParams {
   // what this step builds besides the fields (one launch covers many simulations, each
   // skipping the work its own flags leave out)
@@ -140,6 +154,14 @@ struct SimParams {
   // multigrid
   float* p0[2];
   int latest;  // p0 index of the previous solution
+  // storage precision (FP_PRECISION_MIXED): the scalar pools fld/fldP/fldN hold __half, the
+  // multigrid levels above 0 (lp, lrhs) __nv_bfloat16; everything else FP32
+  int scalarHalf, coarseBf16;
+  // pressure solve: up to `vcycles` V-cycles, stopping once the FP64 RMS residual of the
+  // finest level is at most `tolerance` x its RMS right-hand side (0: run them all)
+  int vcycles;
+  float tolerance;
+  FpSolver* solver;  // device: this step's norms and state
   uint8_t* topo[FP_MAX_LEVELS];
   float* lp[FP_MAX_LEVELS][2];
   float* lrhs[FP_MAX_LEVELS];

@@ -178,6 +178,21 @@ class fp_stats(C.Structure):
         ("d2h_bytes", C.c_uint64),
         ("host_prepare_ms", C.c_double),
         ("host_wait_ms", C.c_double),
+        ("last_divergence", C.c_double),
+    ]
+
+
+FP_MAX_VCYCLES = 16
+
+
+class fp_solver_stats(C.Structure):
+    _fields_ = [
+        ("vcycles", C.c_uint32),
+        ("measured", C.c_int32),
+        ("unknowns", C.c_double),
+        ("rhs_rms", C.c_double),
+        ("residual", C.c_double * FP_MAX_VCYCLES),
+        ("divergence", C.c_double),
     ]
 
 
@@ -264,6 +279,10 @@ SIGNATURES = {
     "fp_grid_memory_bytes": (C.c_int, [C.POINTER(fp_grid), C.POINTER(C.c_uint64)]),
     "fp_grid_reserved_tiles": (C.c_int, [C.POINTER(fp_grid), C.POINTER(C.c_uint32)]),
     "fp_sim_reserve_tiles": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "fp_sim_set_solver": (C.c_int, [C.c_void_p, C.c_int, C.c_float]),
+    "fp_sim_read_solver": (C.c_int, [C.c_void_p, C.POINTER(fp_solver_stats)]),
+    "fp_batch_set_solver": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_float]),
+    "fp_batch_read_solver": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(fp_solver_stats)]),
     "fp_batch_reserve_tiles": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "fp_server_last_error": (C.c_char_p, [C.c_void_p]),
     "fp_server_create": (C.c_int, [C.POINTER(fp_server_config), C.POINTER(C.c_void_p)]),

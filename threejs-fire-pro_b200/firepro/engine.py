@@ -56,6 +56,16 @@ class FluidSimulation:
     def reserve_tiles(self, tiles: int):
         self._check(self.lib.fp_sim_reserve_tiles(self.h, tiles))
 
+    def set_solver(self, vcycles: int, tolerance: float = 0.0):
+        """Up to `vcycles` V-cycles a step, stopping at relative residual `tolerance` (0: all)."""
+        self._check(self.lib.fp_sim_set_solver(self.h, vcycles, tolerance))
+
+    def read_solver(self) -> abi.fp_solver_stats:
+        """The latest step's pressure solve (waits for the step)."""
+        s = abi.fp_solver_stats()
+        self._check(self.lib.fp_sim_read_solver(self.h, C.byref(s)))
+        return s
+
     def reset(self):
         self._check(self.lib.fp_sim_reset(self.h))
 
@@ -155,6 +165,14 @@ class SimulationBatch:
 
     def reserve_tiles(self, sim: int, tiles: int):
         self._check(self.lib.fp_batch_reserve_tiles(self.h, sim, tiles))
+
+    def set_solver(self, sim: int, vcycles: int, tolerance: float = 0.0):
+        self._check(self.lib.fp_batch_set_solver(self.h, sim, vcycles, tolerance))
+
+    def read_solver(self, sim: int) -> abi.fp_solver_stats:
+        s = abi.fp_solver_stats()
+        self._check(self.lib.fp_batch_read_solver(self.h, sim, C.byref(s)))
+        return s
 
     def step(self, items):
         """Step [(id, fp_frame, dt), ...] in one launch."""
