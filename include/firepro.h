@@ -243,6 +243,34 @@ int fp_sim_reserve_tiles(fp_sim* sim, uint32_t tiles);
 int fp_sim_set_solver(fp_sim* sim, int vcycles, float tolerance);
 /* The latest step's solve (waits for the step's work). */
 int fp_sim_read_solver(fp_sim* sim, fp_solver_stats* out);
+/* ---- Volume rendering: a headless restatement of the renderer's compute passes and camera
+ * march (lighting.wgsl smoothSmoke/buildOccupancy/buildLighting, volume-march.wgsl
+ * fireProMarch, scene-volume.wgsl fireProSceneVolume with no scene depth and half resolution
+ * off, fire-emission.wgsl, volume-reconstruction.wgsl, blackbody.ts). The image is linear
+ * radiance and opacity, row-major from the top-left pixel, four floats a pixel. */
+typedef struct fp_camera {
+  float inverse_view_projection[16]; /* clip to world, column-major (the WGSL mat4x4f's columns) */
+  uint32_t width, height;            /* pixels */
+  float time;                        /* seconds: the jitter's frame is floor(time x 60) */
+} fp_camera;
+typedef struct fp_render_settings {
+  float optical[4];       /* smoke extinction, fire brightness, shadow extinction, anisotropy g */
+  float light[4];         /* directional light direction (towards the light), intensity */
+  float smoke[4];         /* smoke albedo RGB, hot-soot glow */
+  float fire[4];          /* fire tint RGB, temperature in kelvin */
+  float scene_light[3];   /* the scene's light colour on the sun term */
+  float ambient_light[3]; /* ambient light on the smoke */
+  float flame_opacity;
+  uint32_t shadow_samples;   /* samples towards the sun per lighting texel (the reference: 32) */
+  uint32_t ray_steps;        /* the march's step count over the ray's length in the box (256) */
+  int32_t filter;            /* 0 trilinear, 1 quadratic B-spline, 2 cubic B-spline (flame only) */
+  uint32_t lighting_divisor; /* fine cells per lighting texel side: 1, 2 or 4 (4) */
+} fp_render_settings;
+/* Render the simulation's latest state into `rgba` (host, width x height x 4 floats). */
+int fp_sim_render(fp_sim* sim, const fp_camera* camera, const fp_render_settings* settings, float* rgba);
+/* The same into device memory of this simulation's GPU (width x height x 4 floats); enqueued
+ * on the simulation's stream. */
+int fp_sim_render_device(fp_sim* sim, const fp_camera* camera, const fp_render_settings* settings, float* rgba);
 /* Wait for the simulation's queued work. */
 int fp_sim_synchronize(fp_sim* sim);
 /* Stats (waits for the latest step's measurement). */

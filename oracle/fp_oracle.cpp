@@ -19,6 +19,7 @@
 // Citations are path:line in the reference project.
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -745,6 +746,446 @@ struct Sim {
       dir.need(i3(ct.first[0] - 1, ct.first[1] - 1, ct.first[2] - 1),
                i3(ct.first[0] + 1, ct.first[1] + 1, ct.first[2] + 1), steps);
     if (dir.dirty) applyTiles();
+    // The sources' bricks (bricksOver, FluidSimulation.ts:862-868) and the render box.
+    sourceBoxes.clear();
+    double brick = double(B) * (double)h;
+    for (uint32_t i = 0; i < f.source_count; i++) {
+      const fp_source& s = f.sources[i];
+      if (s.shape == FP_SHAPE_MESH) continue;
+      double ext = std::max(std::max(std::max((double)s.size[0], (double)s.size[1]), (double)s.size[2]), 0.03) +
+                   (double)s.outward_speed * 0.25;
+      for (int a = 0; a < 3; a++) sourceBoxes.push_back((int)std::floor(((double)s.position[a] - ext) / brick));
+      for (int a = 0; a < 3; a++) sourceBoxes.push_back((int)std::floor(((double)s.position[a] + ext) / brick));
+    }
+    updateRenderBox();
+  }
+
+  // ---------------------------------------------------------------- rendering (test oracle)
+  // updateBoxes (FluidSimulation.ts:916-957) for one cluster: content bricks and source
+  // bricks whose centre lies in a tile, two bricks of margin, within the tiles.
+  int renderLo[3] = {0, 0, 0}, renderHi[3] = {-1, -1, -1};
+  bool renderBox = false;
+  std::vector<int> sourceBoxes;
+  void updateRenderBox() {
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    bool any = false;
+    auto include = [&](const int* l, const int* u) {
+      int c[3];
+      for (int a = 0; a < 3; a++) c[a] = (int)std::floor(((double)l[a] + (double)u[a]) / 2.0);
+      if (ground) c[1] = std::max(0, c[1]);
+      if (dir.slotAt((int)std::floor(c[0] / 4.0), (int)std::floor(c[1] / 4.0), (int)std::floor(c[2] / 4.0)) < 0) return;
+      for (int a = 0; a < 3; a++) {
+        lo[a] = any ? std::min(lo[a], l[a]) : l[a];
+        hi[a] = any ? std::max(hi[a], u[a]) : u[a];
+      }
+      any = true;
+    };
+    for (auto& ct : contentTiles) {
+      int l[3], u[3];
+      bool ok = true;
+      for (int a = 0; a < 3 && ok; a++) {
+        uint32_t used = (ct.second >> (a * 4)) & 15u;
+        if (!used) {
+          ok = false;
+          break;
+        }
+        int low = 0, high = 0;
+        while (!((used >> low) & 1u)) low++;
+        for (int b = 0; b < 4; b++)
+          if ((used >> b) & 1u) high = b;
+        l[a] = ct.first[a] * 4 + low;
+        u[a] = ct.first[a] * 4 + high;
+      }
+      if (ok) include(l, u);
+    }
+    for (size_t s = 0; s + 6 <= sourceBoxes.size(); s += 6) include(&sourceBoxes[s], &sourceBoxes[s + 3]);
+    renderBox = any;
+    if (!any) return;
+    int tlo[3] = {0, 0, 0}, thi[3] = {0, 0, 0};
+    bool first = true;
+    for (const auto& kv : dir.bySeq) {
+      const I3& t = kv.second.coord;
+      for (int a = 0; a < 3; a++) {
+        tlo[a] = first ? t[a] : std::min(tlo[a], t[a]);
+        thi[a] = first ? t[a] : std::max(thi[a], t[a]);
+      }
+      first = false;
+    }
+    for (int a = 0; a < 3; a++) {
+      renderLo[a] = std::max(lo[a] - 2, tlo[a] * 4);
+      renderHi[a] = std::min(hi[a] + 2, (thi[a] + 1) * 4 - 1);
+    }
+  }
+
+  // The render (lighting.wgsl, volume-march.wgsl, fire-emission.wgsl,
+  // volume-reconstruction.wgsl) in R, cell by cell: the render field, occupancy and lighting
+  // of every boxed brick with a slot, then a march per pixel.
+  struct Render {
+    const fp_camera* cam;
+    const fp_render_settings* rs;
+    std::vector<float> lut;
+    int lightShift;
+    std::unordered_map<uint64_t, int> index;  // boxed slotted brick -> row
+    std::vector<R> field;                     // [row][4][N]
+    std::vector<uint8_t> occupancy;           // [row][blocks]
+    std::vector<R> light;                     // [row][4][L^3]
+  };
+  static uint64_t brickKey(int x, int y, int z) {
+    return ((uint64_t)(uint32_t)(x + (1 << 20)) << 42) | ((uint64_t)(uint32_t)(y + (1 << 20)) << 21) |
+           (uint64_t)(uint32_t)(z + (1 << 20));
+  }
+  bool boxed(int bx, int by, int bz) const {
+    return bx >= renderLo[0] && bx <= renderHi[0] && by >= renderLo[1] && by <= renderHi[1] && bz >= renderLo[2] &&
+           bz <= renderHi[2];
+  }
+  int boxSlot(int bx, int by, int bz) { return boxed(bx, by, bz) ? brickSlot(bx, by, bz) : -1; }
+  static R glowOf(R life) { return std::min(std::max(life * R(5), R(0)), R(1)); }
+  R rawSmoke(int x, int y, int z) {
+    int s = boxSlot(x >> shift, y >> shift, z >> shift);
+    return s < 0 ? R(0) : fld[(size_t)s * 4 * N + local(x, y, z)];
+  }
+  void clampBox(R q[3], int per) {
+    for (int a = 0; a < 3; a++)
+      q[a] = std::min(std::max(q[a], R(renderLo[a]) * R(per) + R(.5)), R(renderHi[a] + 1) * R(per) - R(.5));
+  }
+  R smokeSample(R qx, R qy, R qz) {
+    R q[3] = {qx, qy, qz};
+    clampBox(q, B);
+    R g[3], fr[3];
+    int b[3];
+    for (int a = 0; a < 3; a++) {
+      g[a] = q[a] - R(.5);
+      b[a] = (int)std::floor(g[a]);
+      fr[a] = g[a] - R(b[a]);
+    }
+    R v = 0;
+    for (int k = 0; k < 8; k++) {
+      int d[3] = {k & 1, (k >> 1) & 1, k >> 2};
+      R w = (d[0] ? fr[0] : 1 - fr[0]) * (d[1] ? fr[1] : 1 - fr[1]) * (d[2] ? fr[2] : 1 - fr[2]);
+      v += rawSmoke(b[0] + d[0], b[1] + d[1], b[2] + d[2]) * w;
+    }
+    return v;
+  }
+  R smoothedSmoke(int x, int y, int z) {
+    R d = 0;
+    for (int k = 0; k < 8; k++) d += smokeSample(R(x + (k & 1)), R(y + ((k >> 1) & 1)), R(z + (k >> 2)));
+    return std::max(R(0), d * R(.125));
+  }
+  std::array<R, 4> renderCell(Render& G, int x, int y, int z, bool apron) {
+    auto it = G.index.find(brickKey(x >> shift, y >> shift, z >> shift));
+    if (it != G.index.end()) {
+      size_t o = (size_t)it->second * 4 * N + local(x, y, z);
+      return {G.field[o], G.field[o + N], G.field[o + 2 * N], G.field[o + 3 * N]};
+    }
+    if (!apron) return {0, 0, 0, 0};
+    return {smoothedSmoke(x, y, z), 0, 0, 0};
+  }
+  std::array<R, 4> renderSample(Render& G, R qx, R qy, R qz) {
+    R q[3] = {qx, qy, qz};
+    clampBox(q, B);
+    R g[3], fr[3];
+    int b[3];
+    for (int a = 0; a < 3; a++) {
+      g[a] = q[a] - R(.5);
+      b[a] = (int)std::floor(g[a]);
+      fr[a] = g[a] - R(b[a]);
+    }
+    bool based = G.index.count(brickKey(b[0] >> shift, b[1] >> shift, b[2] >> shift)) > 0;
+    std::array<R, 4> v = {0, 0, 0, 0};
+    for (int k = 0; k < 8; k++) {
+      int d[3] = {k & 1, (k >> 1) & 1, k >> 2};
+      R w = (d[0] ? fr[0] : 1 - fr[0]) * (d[1] ? fr[1] : 1 - fr[1]) * (d[2] ? fr[2] : 1 - fr[2]);
+      auto c = renderCell(G, b[0] + d[0], b[1] + d[1], b[2] + d[2], based);
+      for (int ch = 0; ch < 4; ch++) v[ch] += c[ch] * w;
+    }
+    return v;
+  }
+  std::array<R, 4> reconstruct(Render& G, R px, R py, R pz, int mode) {
+    if (mode == 0) return renderSample(G, px, py, pz);
+    R pos[2][3], wt[2][3], p[3] = {px, py, pz};
+    for (int a = 0; a < 3; a++) {
+      R g = p[a] - R(.5);
+      if (mode == 1) {
+        R center = std::floor(g + R(.5)), delta = g - center;
+        R w0 = R(.5) * (R(.5) - delta) * (R(.5) - delta), w1 = R(.75) - delta * delta,
+          w2 = R(.5) * (R(.5) + delta) * (R(.5) + delta);
+        wt[0][a] = w0 + w1;
+        wt[1][a] = w2;
+        pos[0][a] = center - R(.5) + w1 / wt[0][a];
+        pos[1][a] = center + R(1.5);
+      } else {
+        R base = std::floor(g), q = g - base, inv = 1 - q;
+        R w0 = inv * inv * inv / 6, w1 = (3 * q * q * q - 6 * q * q + 4) / 6, w2 = (-3 * q * q * q + 3 * q * q + 3 * q + 1) / 6,
+          w3 = q * q * q / 6;
+        wt[0][a] = w0 + w1;
+        wt[1][a] = w2 + w3;
+        pos[0][a] = base - R(.5) + w1 / wt[0][a];
+        pos[1][a] = base + R(1.5) + w3 / wt[1][a];
+      }
+    }
+    std::array<R, 4> v = {0, 0, 0, 0};
+    for (int i = 0; i < 8; i++) {
+      int ix = (i >> 2) & 1, iy = (i >> 1) & 1, iz = i & 1;
+      auto s = renderSample(G, pos[ix][0], pos[iy][1], pos[iz][2]);
+      R w = wt[ix][0] * wt[iy][1] * wt[iz][2];
+      for (int ch = 0; ch < 4; ch++) v[ch] += w * s[ch];
+    }
+    for (int ch = 0; ch < 4; ch++) v[ch] = std::max(v[ch], R(0));
+    return v;
+  }
+  R extinctionOf(Render& G, const std::array<R, 4>& f) {
+    return std::max(R(0), f[0]) * R(G.rs->optical[0]) + glowOf(f[2]) * R(G.rs->flame_opacity);
+  }
+  std::array<R, 3> emissionOf(Render& G, const std::array<R, 4>& f) {
+    const fp_render_settings& S = *G.rs;
+    if (S.optical[1] <= 0) return {0, 0, 0};
+    R s = std::max(R(0), f[0]) * R(S.optical[0]), flame = glowOf(f[2]) * R(S.flame_opacity);
+    R source[3];
+    for (int c = 0; c < 3; c++) source[c] = (1 - R(S.smoke[c])) * s * R(S.smoke[3]) + flame;
+    if (source[0] == 0 && source[1] == 0 && source[2] == 0) return {0, 0, 0};
+    R heat = std::max(R(0), f[1]);
+    R kelvin = R(800) + heat / (heat + 2) * (R(S.fire[3]) - 800);
+    R u = std::min(std::max((kelvin - 500) / 9500, R(0)), R(1)) * R(511);
+    int i0 = (int)std::floor(u), i1 = std::min(i0 + 1, 511);
+    R fr = u - R(i0), spec[4];
+    for (int c = 0; c < 4; c++) spec[c] = R(G.lut[i0 * 4 + c]) * (1 - fr) + R(G.lut[i1 * 4 + c]) * fr;
+    R scale = std::exp2(std::min(std::max(spec[3], R(-24)), R(10)));
+    R thermal[3] = {spec[0] * scale, spec[1] * scale, spec[2] * scale};
+    R tintPeak = std::max(R(S.fire[0]), std::max(R(S.fire[1]), R(S.fire[2])));
+    R sat = 1 - std::min(R(S.fire[0]), std::min(R(S.fire[1]), R(S.fire[2]))) / std::max(tintPeak, R(1e-6));
+    R peak = std::max(thermal[0], std::max(thermal[1], thermal[2]));
+    std::array<R, 3> out;
+    for (int c = 0; c < 3; c++)
+      out[c] = (thermal[c] * tintPeak * (1 - sat) + R(S.fire[c]) * peak * sat) * source[c] * R(S.optical[1]);
+    return out;
+  }
+  std::array<R, 4> sampleWorld(Render& G, R px, R py, R pz) {
+    R size = R(B) * h, p[3] = {px, py, pz};
+    for (int a = 0; a < 3; a++)
+      if (p[a] < R(renderLo[a]) * size || p[a] > R(renderHi[a] + 1) * size) return {0, 0, 0, 0};
+    return renderSample(G, px / h, py / h, pz / h);
+  }
+  std::array<R, 4> incidentLight(Render& G, R px, R py, R pz) {
+    const fp_render_settings& S = *G.rs;
+    auto lf = sampleWorld(G, px, py, pz);
+    if (lf[0] + glowOf(lf[2]) < R(1e-5)) return {0, 0, 0, 1};
+    R ln = std::sqrt(R(S.light[0]) * S.light[0] + R(S.light[1]) * S.light[1] + R(S.light[2]) * S.light[2]);
+    R sun[3] = {R(S.light[0]) / ln, R(S.light[1]) / ln, R(S.light[2]) / ln}, p[3] = {px, py, pz};
+    R size = R(B) * h, exit = R(1e30);
+    for (int a = 0; a < 3; a++) {
+      if (!(std::fabs(sun[a]) > R(1e-6))) continue;
+      R edge = (sun[a] > 0 ? R(renderHi[a] + 1) : R(renderLo[a])) * size;
+      exit = std::min(exit, (edge - p[a]) / sun[a]);
+    }
+    exit = std::max(R(0), exit);
+    int count = (int)S.shadow_samples;
+    R ds = exit / R(count), depth = 0;
+    if (S.light[3] > 0)
+      for (int i = 0; i < count; i++) {
+        R t = (R(i) + R(.5)) * ds;
+        auto f = sampleWorld(G, px + sun[0] * t, py + sun[1] * t, pz + sun[2] * t);
+        depth += (std::max(R(0), f[0]) * R(S.optical[2]) + glowOf(f[2]) * R(S.flame_opacity)) * ds;
+        if (depth > 9) break;
+      }
+    const R dirs[6][3] = {{.36, .48, -.8}, {-.36, -.48, .8}, {-.8, .6, 0}, {.8, -.6, 0}, {.48, .64, .6}, {-.48, -.64, -.6}};
+    R glow[3] = {0, 0, 0};
+    if (S.optical[1] > 0 && lf[0] > R(1e-5))
+      for (int d = 0; d < 6; d++) {
+        R t = 0, interval = R(.075), transmission = 1;
+        for (int s = 0; s < 6; s++) {
+          R q = t + interval * R(.5);
+          auto f = sampleWorld(G, px + dirs[d][0] * q, py + dirs[d][1] * q, pz + dirs[d][2] * q);
+          R ext = extinctionOf(G, f), att = std::exp(-ext * interval), depth2 = ext * interval;
+          R integ = depth2 < R(.001) ? interval * (1 - R(.5) * depth2 + depth2 * depth2 / 6) : (1 - att) / ext;
+          auto e = emissionOf(G, f);
+          for (int c = 0; c < 3; c++) glow[c] += transmission * e[c] * integ / 6;
+          transmission *= att;
+          t += interval;
+          interval *= R(1.65);
+        }
+      }
+    return {glow[0], glow[1], glow[2], std::exp(-depth)};
+  }
+  std::array<R, 4> lightSample(Render& G, R qx, R qy, R qz) {
+    const int L = 1 << G.lightShift, L3 = L * L * L;
+    R texel = h * R(B >> G.lightShift), q[3] = {qx, qy, qz};
+    clampBox(q, L);
+    R g[3], fr[3];
+    int b[3];
+    for (int a = 0; a < 3; a++) {
+      g[a] = q[a] - R(.5);
+      b[a] = (int)std::floor(g[a]);
+      fr[a] = g[a] - R(b[a]);
+    }
+    if (!G.index.count(brickKey(b[0] >> G.lightShift, b[1] >> G.lightShift, b[2] >> G.lightShift))) return {0, 0, 0, 1};
+    std::array<R, 4> v = {0, 0, 0, 0};
+    for (int k = 0; k < 8; k++) {
+      int d[3] = {k & 1, (k >> 1) & 1, k >> 2};
+      int x = b[0] + d[0], y = b[1] + d[1], z = b[2] + d[2];
+      R w = (d[0] ? fr[0] : 1 - fr[0]) * (d[1] ? fr[1] : 1 - fr[1]) * (d[2] ? fr[2] : 1 - fr[2]);
+      auto it = G.index.find(brickKey(x >> G.lightShift, y >> G.lightShift, z >> G.lightShift));
+      std::array<R, 4> t;
+      if (it != G.index.end()) {
+        int m = L - 1;
+        size_t o = (size_t)it->second * 4 * L3 + (((z & m) * L + (y & m)) * L + (x & m));
+        t = {G.light[o], G.light[o + L3], G.light[o + 2 * L3], G.light[o + 3 * L3]};
+      } else {
+        t = incidentLight(G, (R(x) + R(.5)) * texel, (R(y) + R(.5)) * texel, (R(z) + R(.5)) * texel);
+      }
+      for (int c = 0; c < 4; c++) v[c] += t[c] * w;
+    }
+    return v;
+  }
+  static R jitterOf(uint32_t px, uint32_t py, float time) {
+    uint32_t s0 = px * 1664525u + 1013904223u, s1 = py * 1664525u + 1013904223u,
+             s2 = (uint32_t)(time * 60.f) * 1664525u + 1013904223u;
+    s0 += s1 * s2;
+    s1 += s2 * s0;
+    s2 += s0 * s1;
+    s0 ^= s0 >> 16u;
+    s1 ^= s1 >> 16u;
+    s2 ^= s2 >> 16u;
+    s0 += s1 * s2;
+    return R((float)(s0 >> 8u) / 16777216.f);
+  }
+  void render(const fp_camera& cam, const fp_render_settings& rs, const float* lut, float* image) {
+    Render G;
+    G.cam = &cam;
+    G.rs = &rs;
+    G.lut.assign(lut, lut + 512 * 4);
+    int divShift = rs.lighting_divisor == 1 ? 0 : (rs.lighting_divisor == 2 ? 1 : 2);
+    G.lightShift = shift - divShift;
+    const int L = 1 << G.lightShift, L3 = L * L * L, per = B / 8, blocks = per * per * per;
+    std::vector<I3> bricks;
+    for (uint32_t id : active) {
+      I3 b = brickOf(id);
+      if (boxSlot(b[0], b[1], b[2]) < 0) continue;
+      G.index[brickKey(b[0], b[1], b[2])] = (int)bricks.size();
+      bricks.push_back(b);
+    }
+    size_t nb = bricks.size();
+    G.field.assign(nb * 4 * N, 0);
+    G.occupancy.assign(nb * blocks, 0);
+    G.light.assign(nb * 4 * L3, 0);
+#pragma omp parallel for schedule(dynamic)
+    for (long r = 0; r < (long)nb; r++) {
+      const I3& b = bricks[r];
+      int s = boxSlot(b[0], b[1], b[2]);
+      for (int k = 0; k < N; k++) {
+        int x = b[0] * B + (k & (B - 1)), y = b[1] * B + ((k >> shift) & (B - 1)), z = b[2] * B + (k >> (2 * shift));
+        size_t o = (size_t)r * 4 * N + k;
+        G.field[o] = smoothedSmoke(x, y, z);
+        for (int c = 1; c < 4; c++) G.field[o + c * N] = fld[((size_t)s * 4 + c) * N + k];
+      }
+    }
+#pragma omp parallel for schedule(dynamic)
+    for (long r = 0; r < (long)nb; r++) {
+      const I3& b = bricks[r];
+      for (int blk = 0; blk < blocks; blk++) {
+        int o[3] = {b[0] * B + (blk % per) * 8 - 2, b[1] * B + ((blk / per) % per) * 8 - 2,
+                    b[2] * B + (blk / (per * per)) * 8 - 2};
+        int flags = 0;
+        for (int u = 0; u < 216; u++) {
+          int ux = o[0] + (u % 6) * 2, uy = o[1] + ((u / 6) % 6) * 2, uz = o[2] + (u / 36) * 2;
+          if (!G.index.count(brickKey(ux >> shift, uy >> shift, uz >> shift))) continue;
+          for (int k = 0; k < 8; k++) {
+            auto f = renderCell(G, ux + (k & 1), uy + ((k >> 1) & 1), uz + (k >> 2), true);
+            R g = glowOf(f[2]);
+            flags |= (g > R(.002) ? 1 : 0) | (f[0] + g > R(.002) ? 2 : 0);
+          }
+        }
+        G.occupancy[(size_t)r * blocks + blk] = (uint8_t)flags;
+      }
+      R texel = h * R(B >> G.lightShift);
+      for (int k = 0; k < L3; k++) {
+        int lx = k % L, ly = (k / L) % L, lz = k / (L * L);
+        auto li = incidentLight(G, (R(b[0] * L + lx) + R(.5)) * texel, (R(b[1] * L + ly) + R(.5)) * texel,
+                                (R(b[2] * L + lz) + R(.5)) * texel);
+        for (int c = 0; c < 4; c++) G.light[(size_t)r * 4 * L3 + c * L3 + k] = li[c];
+      }
+    }
+    const int W = (int)cam.width, Hh = (int)cam.height;
+#pragma omp parallel for schedule(dynamic)
+    for (long pix = 0; pix < (long)W * Hh; pix++) {
+      int px = (int)(pix % W), py = (int)(pix / W);
+      float* out = image + pix * 4;
+      out[0] = out[1] = out[2] = out[3] = 0.f;
+      if (!renderBox || steps == 0) continue;
+      R cx = (R(px) + R(.5)) / R(W) * 2 - 1, cy = 1 - (R(py) + R(.5)) / R(Hh) * 2;
+      const float* M = cam.inverse_view_projection;
+      R nh[4], fh[4];
+      for (int r = 0; r < 4; r++) {
+        nh[r] = R(M[r]) * cx + R(M[4 + r]) * cy + R(M[12 + r]);
+        fh[r] = R(M[r]) * cx + R(M[4 + r]) * cy + R(M[8 + r]) * R(.99999f) + R(M[12 + r]);
+      }
+      R ro[3], rd[3];
+      for (int a = 0; a < 3; a++) {
+        ro[a] = nh[a] / nh[3];
+        rd[a] = fh[a] / fh[3] - ro[a];
+      }
+      R rl = std::sqrt(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2]);
+      for (int a = 0; a < 3; a++) rd[a] /= rl;
+      R brickSize = h * R(B), safe[3], exitSide[3], lo = 0, hi = R(1e30);
+      for (int a = 0; a < 3; a++) {
+        safe[a] = std::fabs(rd[a]) > R(1e-6) ? rd[a] : R(1e-6);
+        exitSide[a] = rd[a] > 0 ? 1 : 0;
+        R ta = (R(renderLo[a]) * brickSize - ro[a]) / safe[a], tb = (R(renderHi[a] + 1) * brickSize - ro[a]) / safe[a];
+        lo = std::max(lo, std::min(ta, tb));
+        hi = std::min(hi, std::max(ta, tb));
+      }
+      if (!(hi > lo)) continue;
+      R end = hi, stepSize = std::max(h * R(.5), (hi - lo) / R(rs.ray_steps));
+      R jitter = jitterOf((uint32_t)px, (uint32_t)py, cam.time);
+      R ln = std::sqrt(R(rs.light[0]) * rs.light[0] + R(rs.light[1]) * rs.light[1] + R(rs.light[2]) * rs.light[2]);
+      R g = rs.optical[3];
+      R mu = (rd[0] * rs.light[0] + rd[1] * rs.light[1] + rd[2] * rs.light[2]) / ln;
+      R phase = (1 - g * g) / std::pow(std::max(R(.05), 1 + g * g - 2 * g * mu), R(1.5));
+      R dk = R(rs.light[3]) * (R(.35) + phase * R(.3));
+      R lightRatio = R(B >> G.lightShift);
+      R t = lo, trans = 1, rad[3] = {0, 0, 0};
+      while (t < end && trans >= R(.008)) {
+        R ds = std::min(stepSize, end - t), tt = t + jitter * ds;
+        R p[3] = {ro[0] + rd[0] * tt, ro[1] + rd[1] * tt, ro[2] + rd[2] * tt};
+        R cell[3] = {p[0] / h, p[1] / h, p[2] / h};
+        int ci[3] = {(int)std::floor(cell[0]), (int)std::floor(cell[1]), (int)std::floor(cell[2])};
+        auto it = G.index.find(brickKey(ci[0] >> shift, ci[1] >> shift, ci[2] >> shift));
+        R size = brickSize;
+        int flags = 0;
+        if (it != G.index.end()) {
+          int m = B - 1;
+          int block = ((((ci[2] & m) >> 3) * per) + ((ci[1] & m) >> 3)) * per + ((ci[0] & m) >> 3);
+          flags = G.occupancy[(size_t)it->second * blocks + block];
+          size = h * 8;
+        }
+        if (!(flags & 2)) {
+          R dist = R(1e30);
+          for (int a = 0; a < 3; a++) dist = std::min(dist, ((std::floor(p[a] / size) + exitSide[a]) * size - p[a]) / safe[a]);
+          t = std::min(t + std::max(R(1), std::floor(dist / stepSize) + 1) * stepSize, end);
+          continue;
+        }
+        auto f = reconstruct(G, cell[0], cell[1], cell[2], (flags & 1) ? rs.filter : 0);
+        if (f[0] + glowOf(f[2]) > R(.002)) {
+          auto glow = emissionOf(G, f);
+          R density = std::max(R(0), f[0]) * R(rs.optical[0]), sc[3] = {0, 0, 0};
+          if (density > 0) {
+            auto inc = lightSample(G, cell[0] / lightRatio, cell[1] / lightRatio, cell[2] / lightRatio);
+            for (int c = 0; c < 3; c++)
+              sc[c] = R(rs.smoke[c]) * (R(rs.ambient_light[c]) + R(rs.scene_light[c]) * dk * inc[3] + inc[c] * R(.65)) *
+                      density;
+          }
+          R ext = extinctionOf(G, f), tau = ext * ds;
+          R integral = ds * (1 - R(.5) * tau + tau * tau / 6);
+          if (tau >= R(.001)) integral = (1 - std::exp(-tau)) / ext;
+          for (int c = 0; c < 3; c++) rad[c] += trans * (sc[c] + glow[c]) * integral;
+          trans *= 1 - std::min(R(1), ext * integral);
+        }
+        t += ds;
+      }
+      out[0] = (float)rad[0];
+      out[1] = (float)rad[1];
+      out[2] = (float)rad[2];
+      out[3] = (float)(1 - trans);
+    }
   }
 
   std::string step(const fp_frame& f, float dtf) {
@@ -2008,6 +2449,55 @@ void or_set_runtime(or_sim* s, float cutoff, double budget, int ground) {
     return 0;
   };
   if (s->d) fn(*s->d); else fn(*s->f);
+}
+// blackbodyTable (src/engine/blackbody.ts:1-97), restated for the oracle: Planck radiance
+// against the multi-lobe CIE observer fit (Wyman, Sloan and Shirley, JCGT 2013), linear sRGB,
+// peak-normalised, log2 radiance relative to 1800 K, 512 entries from 500 K to 10000 K.
+static void or_blackbody(double kelvin, double rgb[3]) {
+  static const double lobes[7][5] = {{0, 0.362, 442, 0.0624, 0.0374},  {0, 1.056, 599.8, 0.0264, 0.0323},
+                                     {0, -0.065, 501.1, 0.049, 0.0382}, {1, 0.821, 568.8, 0.0213, 0.0247},
+                                     {1, 0.286, 530.9, 0.0613, 0.0322}, {2, 1.217, 437, 0.0845, 0.0278},
+                                     {2, 0.681, 459, 0.0385, 0.0725}};
+  const double hp = 6.62607015e-34, c = 299792458.0, kb = 1.380649e-23;
+  double xyz[3] = {0, 0, 0};
+  for (int i = 0; i < 95; i++) {
+    double wl = 360.0 + 5.0 * i, w = wl * 1e-9;
+    double radiance = 2 * hp * c * c / (std::pow(w, 5) * std::expm1(hp * c / (w * kb * kelvin))) * 5e-9;
+    for (const auto& L : lobes) {
+      double d = (wl - L[2]) * (wl < L[2] ? L[3] : L[4]);
+      xyz[(int)L[0]] += L[1] * std::exp(-0.5 * d * d) * radiance;
+    }
+  }
+  rgb[0] = std::max(0.0, 3.2406 * xyz[0] - 1.5372 * xyz[1] - 0.4986 * xyz[2]);
+  rgb[1] = std::max(0.0, -0.9689 * xyz[0] + 1.8758 * xyz[1] + 0.0415 * xyz[2]);
+  rgb[2] = std::max(0.0, 0.0557 * xyz[0] - 0.204 * xyz[1] + 1.057 * xyz[2]);
+}
+void or_blackbody_table(float* out) {
+  double ref[3];
+  or_blackbody(1800.0, ref);
+  double refPeak = std::max(ref[0], std::max(ref[1], ref[2]));
+  for (int i = 0; i < 512; i++) {
+    double rgb[3];
+    or_blackbody(500.0 + 9500.0 * i / 511.0, rgb);
+    double peak = std::max(rgb[0], std::max(rgb[1], rgb[2]));
+    if (peak <= 0) {
+      out[i * 4] = out[i * 4 + 1] = out[i * 4 + 2] = 0.f;
+      out[i * 4 + 3] = -32.f;
+      continue;
+    }
+    for (int c = 0; c < 3; c++) out[i * 4 + c] = (float)(rgb[c] / peak);
+    out[i * 4 + 3] = (float)std::max(-32.0, std::log2(peak / refPeak));
+  }
+}
+// The render of the current state (the CUDA render's restatement), into `image` (w x h x 4).
+int or_render(or_sim* s, const fp_camera* cam, const fp_render_settings* rs, float* image) {
+  std::vector<float> lut(512 * 4);
+  or_blackbody_table(lut.data());
+  if (s->d)
+    s->d->render(*cam, *rs, lut.data(), image);
+  else
+    s->f->render(*cam, *rs, lut.data(), image);
+  return 0;
 }
 // The number of V-cycles of each later step's pressure solve (the CUDA step's solver setting
 // with tolerance 0).

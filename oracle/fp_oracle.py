@@ -38,6 +38,8 @@ def lib():
         L.or_set_solver.argtypes = [C.c_void_p, C.c_int]
         L.or_step.restype = C.c_int
         L.or_step.argtypes = [C.c_void_p, C.c_void_p, C.c_float]
+        L.or_render.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.or_blackbody_table.argtypes = [C.c_void_p]
         L.or_error.restype = C.c_char_p
         L.or_error.argtypes = [C.c_void_p]
         L.or_info.restype = C.c_int64
@@ -69,6 +71,12 @@ class OracleSim:
         if not self.h:
             raise ValueError("oracle rejected the grid")
         self.real = real
+
+    def render(self, camera, settings) -> np.ndarray:
+        """The render of the current state: (height, width, 4) linear radiance and opacity."""
+        out = np.zeros((camera.height, camera.width, 4), np.float32)
+        self.L.or_render(self.h, C.byref(camera), C.byref(settings), out.ctypes.data)
+        return out
 
     def close(self):
         if self.h:
@@ -131,6 +139,13 @@ class OracleSim:
     def write_activity(self, arr: np.ndarray):
         a = np.ascontiguousarray(arr, np.uint32)
         assert self.L.or_write_activity(self.h, a.ctypes.data, a.size) == 0
+
+
+def blackbody_table() -> np.ndarray:
+    """The oracle's blackbody table: (512, 4) RGB peak-normalised and log2 radiance, 500-10000 K."""
+    out = np.zeros((512, 4), np.float32)
+    lib().or_blackbody_table(out.ctypes.data)
+    return out
 
 
 def set_threads(n: int):

@@ -88,7 +88,7 @@ def force(gpu, orc):
 
 
 def lockstep(scene, steps: int, gpu_factory, cutoff=0.05, budget=8e6, ground=True, start=0, log=None, grid=None,
-             before_step=None, vcycles=1):
+             before_step=None, vcycles=1, after=None):
     """Run `steps` steps in lockstep; returns per-step (tables, fields) reports.
     `before_step(step, gpu, oracle)` may change runtime settings on both. `vcycles` V-cycles
     a step on both sides (tolerance 0: all of them run)."""
@@ -114,6 +114,8 @@ def lockstep(scene, steps: int, gpu_factory, cutoff=0.05, budget=8e6, ground=Tru
         if log:
             log(s, tables, fields, len(slots))
         force(gpu, orc)
+    if after:
+        after(gpu, orc)  # both hold the same state here
     gpu.dispose()
     orc.close()
     return reports

@@ -148,6 +148,18 @@ int fp_sim_reserve_tiles(fp_sim* sim, uint32_t tiles) {
   return sim->engine->reserveTiles(tiles);
 }
 
+int fp_sim_render(fp_sim* sim, const fp_camera* camera, const fp_render_settings* settings, float* rgba) {
+  if (!sim || !camera || !settings || !rgba)
+    return failed("fp_sim_render needs a simulation, a camera, settings and an image.", FP_EINVAL);
+  return sim->engine->render(*camera, *settings, nullptr, rgba);
+}
+
+int fp_sim_render_device(fp_sim* sim, const fp_camera* camera, const fp_render_settings* settings, float* rgba) {
+  if (!sim || !camera || !settings || !rgba)
+    return failed("fp_sim_render_device needs a simulation, a camera, settings and an image.", FP_EINVAL);
+  return sim->engine->render(*camera, *settings, rgba, nullptr);
+}
+
 int fp_sim_set_solver(fp_sim* sim, int vcycles, float tolerance) {
   if (!sim) return failed("null simulation", FP_EINVAL);
   return sim->engine->setSolver(vcycles, tolerance);

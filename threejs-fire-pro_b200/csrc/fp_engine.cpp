@@ -172,6 +172,10 @@ Engine::~Engine() {
   owner_->forget(this);
   cudaStreamSynchronize(stream());
   freeAll();
+  DeviceBuffer* render[] = {&renderField_, &lighting_, &occupancy_, &lut_, &renderParams_, &image_};
+  for (DeviceBuffer* b : render)
+    if (b->ptr) cudaFree(b->ptr);
+  if (renderParamsH_) cudaFreeHost(renderParamsH_);
   if (stageH_) cudaFreeHost(stageH_);
 }
 
@@ -421,6 +425,8 @@ void Engine::updateTiles(const fp_frame& f) {
   // Host arithmetic in double precision, as the reference's JavaScript does it.
   double h = h_, tile = (double)(TILE_BRICKS * B_) * h;
   double margin = (double)(2 * B_) * h + tile;
+  double brick = (double)B_ * h;
+  sourceBoxes_.clear();
   for (uint32_t i = 0; i < f.source_count; i++) {
     const fp_source& s = f.sources[i];
     if (s.shape == FP_SHAPE_MESH) continue;
@@ -432,6 +438,9 @@ void Engine::updateTiles(const fp_frame& f) {
       hi[a] = (int)std::floor(((double)s.position[a] + ext + margin) / tile);
     }
     dir_.need(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], steps_);
+    // bricksOver (FluidSimulation.ts:862-868): the source's bricks, for the render box.
+    for (int a = 0; a < 3; a++) sourceBoxes_.push_back((int)std::floor(((double)s.position[a] - ext) / brick));
+    for (int a = 0; a < 3; a++) sourceBoxes_.push_back((int)std::floor(((double)s.position[a] + ext) / brick));
   }
   for (auto& ct : contentTiles_)
     dir_.need(ct.first.x - 1, ct.first.y - 1, ct.first.z - 1, ct.first.x + 1, ct.first.y + 1, ct.first.z + 1, steps_);
@@ -687,6 +696,7 @@ int Engine::prepare(const fp_frame& f, float dt) {
   if (limit > slots_ && (rc = growPool(limit))) return rc;
   updateTiles(f);
   if (dir_.dirty && (rc = applyTiles())) return rc;
+  updateRenderBox();
   if (packScene(f)) {
     solidsStale_ = true;
     geometryDirty_ = true;

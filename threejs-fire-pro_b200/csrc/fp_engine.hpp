@@ -107,6 +107,9 @@ class Engine {
   // `vcycles` V-cycles a step, stopping at a relative FP64 residual of `tolerance` (0: all).
   int setSolver(int vcycles, float tolerance);
   int readSolver(fp_solver_stats* out);
+  // Volume rendering of the latest state (fp_render.cu) into device memory `image` (enqueued),
+  // or into host memory `host` (waits).
+  int render(const fp_camera& camera, const fp_render_settings& settings, float* image, float* host);
   int vcycles() const { return vcycles_; }
   // Whether the step measures the residual and the post-projection divergence.
   bool measures() const { return vcycles_ > 1 || tolerance_ > 0.f || measure_; }
@@ -160,6 +163,15 @@ class Engine {
   DeviceBuffer tileRecD_, tileNbrD_, hashD_, solver_;
   int velIdx_[4] = {0, 1, 2, 3};  // start, predictor/projected, corrected, forced
   int fldIdx_[3] = {0, 1, 2};     // start, predictor, evolved
+
+  // rendering: the box in bricks (inclusive) from the latest step's content and sources, the
+  // render pools and the parameters of a render
+  int renderLo_[3] = {0, 0, 0}, renderHi_[3] = {-1, -1, -1};
+  bool renderBox_ = false;
+  std::vector<int> sourceBoxes_;  // lo xyz, hi xyz per source
+  DeviceBuffer renderField_, lighting_, occupancy_, lut_, renderParams_, image_;
+  SimParams* renderParamsH_ = nullptr;
+  void updateRenderBox();
 
   // pinned staging of the directory tables' copies
   uint8_t* stageH_ = nullptr;

@@ -1,0 +1,481 @@
+// Volume rendering of a simulation's state, headless: restates the renderer's compute passes
+// (src/engine/shaders/lighting.wgsl smoothSmoke 69-99, buildOccupancy 149-244, incidentLight
+// 257-310, lightSlot 312-347) and the camera march (volume-march.wgsl fireProRay 18-24,
+// fireProHit 28-35, fireProStep 77-79, fireProJitter 94-102, fireProShade 106-138,
+// fireProDirect 141-146, fireProMarch 178-268; scene-volume.wgsl 39-44 and 160-167 with no
+// scene depth and half resolution off), the optical model (fire-emission.wgsl) and the
+// reconstruction filters (volume-reconstruction.wgsl).
+//
+// Where the reference reads a pool slot's apron (a copy of the +1 neighbours), these kernels
+// read the neighbour's slot; a neighbour without a slot reads what the apron would hold: the
+// smoothed density computed on the spot for the render field, the incident light computed on
+// the spot for the lighting pool. The render uses one box: the bricks with content and the
+// sources' bricks, with a margin of two bricks, within the tiles (FluidSimulation.ts:916-957
+// for a scene of one cluster).
+#include "fp_device.cuh"
+#include "fp_render.h"
+
+namespace {
+
+constexpr int RTHREADS = 128;
+
+// A thread's last brick lookup.
+struct SlotCache {
+  int bx, by, bz, slot;
+};
+
+FP_DEV bool inBox(const FpRender& R, int bx, int by, int bz) {
+  return bx >= R.boxLo[0] && bx <= R.boxHi[0] && by >= R.boxLo[1] && by <= R.boxHi[1] && bz >= R.boxLo[2] &&
+         bz <= R.boxHi[2];
+}
+// fireProPage: the slot of world brick b inside the box, or -1.
+FP_DEV int slotAt(const SimParams& P, const FpRender& R, SlotCache& c, int bx, int by, int bz) {
+  if (bx == c.bx && by == c.by && bz == c.bz) return c.slot;
+  int s = -1;
+  if (inBox(R, bx, by, bz)) {
+    int t = hashFind(P, bx >> 2, by >> 2, bz >> 2);
+    if (t >= 0) s = entryPage(P.entries[t * 64 + (((bz & 3) * 4 + (by & 3)) * 4 + (bx & 3))]);
+  }
+  c = SlotCache{bx, by, bz, s};
+  return s;
+}
+
+FP_DEV float glowOf(float life) { return fminf(fmaxf(life * 5.f, 0.f), 1.f); }  // fireProGlow
+
+// The simulation's smoke at a world cell: zero outside the box or without a slot.
+FP_DEV float rawSmoke(const SimParams& P, const FpRender& R, SlotCache& c, int x, int y, int z) {
+  int s = slotAt(P, R, c, x >> P.shift, y >> P.shift, z >> P.shift);
+  if (s < 0) return 0.f;
+  return ldHalf(P.fld, (size_t)s * 4 * P.N + localCell(P, x, y, z), P.scalarHalf != 0);
+}
+// fireProField of the smoke at `q` in cells: clamped to the box, trilinear.
+FP_DEV float smokeSample(const SimParams& P, const FpRender& R, SlotCache& c, float qx, float qy, float qz) {
+  float B = (float)P.B;
+  qx = fminf(fmaxf(qx, (float)R.boxLo[0] * B + .5f), (float)(R.boxHi[0] + 1) * B - .5f);
+  qy = fminf(fmaxf(qy, (float)R.boxLo[1] * B + .5f), (float)(R.boxHi[1] + 1) * B - .5f);
+  qz = fminf(fmaxf(qz, (float)R.boxLo[2] * B + .5f), (float)(R.boxHi[2] + 1) * B - .5f);
+  float gx = qx - .5f, gy = qy - .5f, gz = qz - .5f;
+  int x0 = (int)floorf(gx), y0 = (int)floorf(gy), z0 = (int)floorf(gz);
+  float fx = gx - (float)x0, fy = gy - (float)y0, fz = gz - (float)z0;
+  float v = 0.f;
+  for (int k = 0; k < 8; k++) {
+    int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
+    float w = (dx ? fx : 1.f - fx) * (dy ? fy : 1.f - fy) * (dz ? fz : 1.f - fz);
+    v += rawSmoke(P, R, c, x0 + dx, y0 + dy, z0 + dz) * w;
+  }
+  return v;
+}
+// smoothSmoke's [1,2,1]/4 density at a world cell: eight half-offset samples.
+FP_DEV float smoothedSmoke(const SimParams& P, const FpRender& R, SlotCache& c, int x, int y, int z) {
+  float d = 0.f;
+  for (int k = 0; k < 8; k++)
+    d += smokeSample(P, R, c, (float)(x + (k & 1)), (float)(y + ((k >> 1) & 1)), (float)(z + (k >> 2)));
+  return fmaxf(0.f, d * .125f);
+}
+
+// The render field at a world cell. A cell of a brick with a slot reads the pool. A cell in a
+// brick without one reads as the apron of a sample based in a slotted brick would hold it
+// (`apron`: the smoothed density, no heat, flame or fuel), else zero.
+FP_DEV float4 renderCell(const SimParams& P, const FpRender& R, SlotCache& c, int x, int y, int z, bool apron) {
+  int s = slotAt(P, R, c, x >> P.shift, y >> P.shift, z >> P.shift);
+  if (s >= 0) {
+    size_t i = (size_t)s * 4 * P.N + localCell(P, x, y, z);
+    return make_float4(R.renderField[i], R.renderField[i + P.N], R.renderField[i + 2 * P.N], R.renderField[i + 3 * P.N]);
+  }
+  if (!apron) return make_float4(0.f, 0.f, 0.f, 0.f);
+  return make_float4(smoothedSmoke(P, R, c, x, y, z), 0.f, 0.f, 0.f);
+}
+FP_DEV void add4(float4& a, const float4& b, float w) {
+  a.x += b.x * w;
+  a.y += b.y * w;
+  a.z += b.z * w;
+  a.w += b.w * w;
+}
+// fireProField of the render field at `q` in cells (fireProSample, volume-bricks.wgsl).
+FP_DEV float4 renderSample(const SimParams& P, const FpRender& R, SlotCache& c, float qx, float qy, float qz) {
+  float B = (float)P.B;
+  qx = fminf(fmaxf(qx, (float)R.boxLo[0] * B + .5f), (float)(R.boxHi[0] + 1) * B - .5f);
+  qy = fminf(fmaxf(qy, (float)R.boxLo[1] * B + .5f), (float)(R.boxHi[1] + 1) * B - .5f);
+  qz = fminf(fmaxf(qz, (float)R.boxLo[2] * B + .5f), (float)(R.boxHi[2] + 1) * B - .5f);
+  float gx = qx - .5f, gy = qy - .5f, gz = qz - .5f;
+  int x0 = (int)floorf(gx), y0 = (int)floorf(gy), z0 = (int)floorf(gz);
+  float fx = gx - (float)x0, fy = gy - (float)y0, fz = gz - (float)z0;
+  bool based = slotAt(P, R, c, x0 >> P.shift, y0 >> P.shift, z0 >> P.shift) >= 0;
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int k = 0; k < 8; k++) {
+    int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
+    float w = (dx ? fx : 1.f - fx) * (dy ? fy : 1.f - fy) * (dz ? fz : 1.f - fz);
+    add4(v, renderCell(P, R, c, x0 + dx, y0 + dy, z0 + dz, based), w);
+  }
+  return v;
+}
+
+// fireProReconstruct (volume-reconstruction.wgsl:5-95): 0 trilinear; 1 quadratic and 2 cubic
+// B-splines from eight trilinear samples.
+FP_DEV float4 reconstruct(const SimParams& P, const FpRender& R, SlotCache& c, float px, float py, float pz, int mode) {
+  if (mode == 0) return renderSample(P, R, c, px, py, pz);
+  float pos[2][3], wt[2][3];
+  float p[3] = {px, py, pz};
+  for (int a = 0; a < 3; a++) {
+    float g = p[a] - .5f;
+    if (mode == 1) {
+      float center = floorf(g + .5f), delta = g - center;
+      float w0 = .5f * (.5f - delta) * (.5f - delta), w1 = .75f - delta * delta, w2 = .5f * (.5f + delta) * (.5f + delta);
+      wt[0][a] = w0 + w1;
+      wt[1][a] = w2;
+      pos[0][a] = center - .5f + w1 / wt[0][a];
+      pos[1][a] = center + 1.5f;
+    } else {
+      float base = floorf(g), q = g - floorf(g), inv = 1.f - q;
+      float w0 = inv * inv * inv / 6.f, w1 = (3.f * q * q * q - 6.f * q * q + 4.f) / 6.f;
+      float w2 = (-3.f * q * q * q + 3.f * q * q + 3.f * q + 1.f) / 6.f, w3 = q * q * q / 6.f;
+      wt[0][a] = w0 + w1;
+      wt[1][a] = w2 + w3;
+      pos[0][a] = base - .5f + w1 / wt[0][a];
+      pos[1][a] = base + 1.5f + w3 / wt[1][a];
+    }
+  }
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  // The reference's order: x outermost, then y, then z.
+  for (int i = 0; i < 8; i++) {
+    int ix = (i >> 2) & 1, iy = (i >> 1) & 1, iz = i & 1;
+    add4(v, renderSample(P, R, c, pos[ix][0], pos[iy][1], pos[iz][2]), wt[ix][0] * wt[iy][1] * wt[iz][2]);
+  }
+  return make_float4(fmaxf(v.x, 0.f), fmaxf(v.y, 0.f), fmaxf(v.z, 0.f), fmaxf(v.w, 0.f));
+}
+
+// fireProExtinction and fireProEmission (fire-emission.wgsl:18-56).
+FP_DEV float extinctionOf(const FpRender& R, const float4& f) {
+  return fmaxf(0.f, f.x) * R.optical[0] + glowOf(f.z) * R.flameOpacity;
+}
+FP_DEV float3 emissionOf(const FpRender& R, const float4& f) {
+  if (R.optical[1] <= 0.f) return make_float3(0.f, 0.f, 0.f);
+  float s = fmaxf(0.f, f.x) * R.optical[0], flame = glowOf(f.z) * R.flameOpacity;
+  float3 source = make_float3((1.f - R.smoke[0]) * s * R.smoke[3] + flame, (1.f - R.smoke[1]) * s * R.smoke[3] + flame,
+                              (1.f - R.smoke[2]) * s * R.smoke[3] + flame);
+  if (source.x == 0.f && source.y == 0.f && source.z == 0.f) return make_float3(0.f, 0.f, 0.f);
+  float heat = fmaxf(0.f, f.y);
+  float kelvin = 800.f + heat / (heat + 2.f) * (R.fire[3] - 800.f);
+  float u = fminf(fmaxf((kelvin - 500.f) / 9500.f, 0.f), 1.f) * (float)(FP_BLACKBODY_SIZE - 1);
+  int i0 = (int)floorf(u);
+  int i1 = min(i0 + 1, FP_BLACKBODY_SIZE - 1);
+  float fr = u - (float)i0;
+  float4 a = __ldg(&R.lut[i0]), b = __ldg(&R.lut[i1]);
+  float4 spec = make_float4(mixf(a.x, b.x, fr), mixf(a.y, b.y, fr), mixf(a.z, b.z, fr), mixf(a.w, b.w, fr));
+  float scale = exp2f(fminf(fmaxf(spec.w, -24.f), 10.f));
+  float3 thermal = make_float3(spec.x * scale, spec.y * scale, spec.z * scale);
+  float tintPeak = fmaxf(R.fire[0], fmaxf(R.fire[1], R.fire[2]));
+  float saturation = 1.f - fminf(R.fire[0], fminf(R.fire[1], R.fire[2])) / fmaxf(tintPeak, 1e-6f);
+  float peak = fmaxf(thermal.x, fmaxf(thermal.y, thermal.z));
+  float k = R.optical[1];
+  return make_float3(mixf(thermal.x * tintPeak, R.fire[0] * peak, saturation) * source.x * k,
+                     mixf(thermal.y * tintPeak, R.fire[1] * peak, saturation) * source.y * k,
+                     mixf(thermal.z * tintPeak, R.fire[2] * peak, saturation) * source.z * k);
+}
+
+// sampleWorld (volume-common.wgsl:33-43): the render field at world point p, zero outside
+// the box.
+FP_DEV float4 sampleWorld(const SimParams& P, const FpRender& R, SlotCache& c, float px, float py, float pz) {
+  float size = (float)P.B * P.h;
+  if (px < (float)R.boxLo[0] * size || py < (float)R.boxLo[1] * size || pz < (float)R.boxLo[2] * size ||
+      px > (float)(R.boxHi[0] + 1) * size || py > (float)(R.boxHi[1] + 1) * size || pz > (float)(R.boxHi[2] + 1) * size)
+    return make_float4(0.f, 0.f, 0.f, 0.f);
+  return renderSample(P, R, c, px / P.h, py / P.h, pz / P.h);
+}
+
+// exitDistance (lighting.wgsl:248-255).
+FP_DEV float exitDistance(const SimParams& P, const FpRender& R, float px, float py, float pz, float dx, float dy,
+                          float dz) {
+  float size = (float)P.B * P.h;
+  float p[3] = {px, py, pz}, d[3] = {dx, dy, dz}, m = 1e30f;
+  for (int a = 0; a < 3; a++) {
+    if (!(fabsf(d[a]) > 1e-6f)) continue;
+    float edge = (d[a] > 0.f ? (float)(R.boxHi[a] + 1) : (float)R.boxLo[a]) * size;
+    m = fminf(m, (edge - p[a]) / d[a]);
+  }
+  return fmaxf(0.f, m);
+}
+
+// integratedTransmission (volume-common.wgsl:47-53).
+FP_DEV float integratedTransmission(float extinction, float distance, float attenuation) {
+  float depth = extinction * distance;
+  if (depth < .001f) return distance * (1.f - .5f * depth + depth * depth / 6.f);
+  return (1.f - attenuation) / extinction;
+}
+
+// incidentLight (lighting.wgsl:257-310): glow RGB and the sun's transmittance at p.
+FP_DEV float4 incidentLight(const SimParams& P, const FpRender& R, SlotCache& c, float px, float py, float pz) {
+  float4 local = sampleWorld(P, R, c, px, py, pz);
+  if (local.x + glowOf(local.z) < 1e-5f) return make_float4(0.f, 0.f, 0.f, 1.f);
+  float ln = sqrtf(R.light[0] * R.light[0] + R.light[1] * R.light[1] + R.light[2] * R.light[2]);
+  float sx = R.light[0] / ln, sy = R.light[1] / ln, sz = R.light[2] / ln;
+  int count = R.shadowSamples;
+  float ds = exitDistance(P, R, px, py, pz, sx, sy, sz) / (float)count;
+  float depth = 0.f;
+  if (R.light[3] > 0.f) {
+    for (int i = 0; i < count; i++) {
+      float t = ((float)i + .5f) * ds;
+      float4 f = sampleWorld(P, R, c, px + sx * t, py + sy * t, pz + sz * t);
+      depth += (fmaxf(0.f, f.x) * R.optical[2] + glowOf(f.z) * R.flameOpacity) * ds;
+      if (depth > 9.f) break;
+    }
+  }
+  const float dirs[6][3] = {{.36f, .48f, -.8f}, {-.36f, -.48f, .8f}, {-.8f, .6f, 0.f},
+                            {.8f, -.6f, 0.f},   {.48f, .64f, .6f},   {-.48f, -.64f, -.6f}};
+  float3 glow = make_float3(0.f, 0.f, 0.f);
+  if (R.optical[1] > 0.f && local.x > 1e-5f) {
+    for (int d = 0; d < 6; d++) {
+      float t = 0.f, interval = .075f, transmission = 1.f;
+      for (int s = 0; s < 6; s++) {
+        float q = t + interval * .5f;
+        float4 f = sampleWorld(P, R, c, px + dirs[d][0] * q, py + dirs[d][1] * q, pz + dirs[d][2] * q);
+        float ext = extinctionOf(R, f);
+        float att = expf(-ext * interval);
+        float3 e = emissionOf(R, f);
+        float w = transmission * integratedTransmission(ext, interval, att) / 6.f;
+        glow.x += e.x * w;
+        glow.y += e.y * w;
+        glow.z += e.z * w;
+        transmission *= att;
+        t += interval;
+        interval *= 1.65f;
+      }
+    }
+  }
+  return make_float4(glow.x, glow.y, glow.z, expf(-depth));
+}
+
+// The brick of computing brick `i` inside the box, with its slot; false otherwise.
+FP_DEV bool boxBrick(const SimParams& P, const FpRender& R, SlotCache& c, uint32_t i, int& bx, int& by, int& bz,
+                     int& slot) {
+  uint32_t id = P.active[i];
+  int4 t = __ldg(&P.tileRec[id >> 6]);
+  int l = id & 63;
+  bx = t.x * 4 + (l & 3);
+  by = t.y * 4 + ((l >> 2) & 3);
+  bz = t.z * 4 + (l >> 4);
+  if (!inBox(R, bx, by, bz)) return false;
+  slot = slotAt(P, R, c, bx, by, bz);
+  return slot >= 0;
+}
+
+// smoothSmoke: each boxed brick's render field, the smoothed density with heat, lifetime and
+// fuel as they are.
+__global__ void __launch_bounds__(RTHREADS) k_render_field(const SimParams* __restrict__ Pp, FpRender R) {
+  const SimParams& P = *Pp;
+  uint32_t total = P.counters->active;
+  const bool half = P.scalarHalf != 0;
+  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+    SlotCache c{1 << 30, 0, 0, -1};
+    int bx, by, bz, slot;
+    if (!boxBrick(P, R, c, i, bx, by, bz, slot)) continue;
+    for (int k = threadIdx.x; k < P.N; k += blockDim.x) {
+      int x = bx * P.B + (k & (P.B - 1)), y = by * P.B + ((k >> P.shift) & (P.B - 1)), z = bz * P.B + (k >> (2 * P.shift));
+      size_t o = (size_t)slot * 4 * P.N + k;
+      R.renderField[o] = smoothedSmoke(P, R, c, x, y, z);
+      R.renderField[o + P.N] = ldHalf(P.fld, o + P.N, half);
+      R.renderField[o + 2 * P.N] = ldHalf(P.fld, o + 2 * P.N, half);
+      R.renderField[o + 3 * P.N] = ldHalf(P.fld, o + 3 * P.N, half);
+    }
+  }
+}
+
+// buildOccupancy and buildLighting of each boxed brick, from the render field.
+__global__ void __launch_bounds__(RTHREADS) k_render_light(const SimParams* __restrict__ Pp, FpRender R) {
+  const SimParams& P = *Pp;
+  __shared__ int flags;
+  uint32_t total = P.counters->active;
+  const int L = 1 << R.lightShift, L3 = L * L * L;
+  const float texel = P.h * (float)(P.B >> R.lightShift);
+  const int per = P.B / 8, blocks = per * per * per;
+  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+    SlotCache c{1 << 30, 0, 0, -1};
+    int bx, by, bz, slot;
+    if (!boxBrick(P, R, c, i, bx, by, bz, slot)) continue;  // the same for the whole CTA
+    // Each 8-cell block with a halo of two cells, in units of 2x2x2 cells: a unit in a
+    // slotted brick looks at its corner cells of the render field.
+    for (int b = 0; b < blocks; b++) {
+      if (threadIdx.x == 0) flags = 0;
+      __syncthreads();
+      int ox = bx * P.B + (b % per) * 8 - 2, oy = by * P.B + ((b / per) % per) * 8 - 2, oz = bz * P.B + (b / (per * per)) * 8 - 2;
+      int mine = 0;
+      for (int u = threadIdx.x; u < 216; u += blockDim.x) {
+        int ux = ox + (u % 6) * 2, uy = oy + ((u / 6) % 6) * 2, uz = oz + (u / 36) * 2;
+        if (slotAt(P, R, c, ux >> P.shift, uy >> P.shift, uz >> P.shift) < 0) continue;
+        for (int k = 0; k < 8; k++) {
+          float4 f = renderCell(P, R, c, ux + (k & 1), uy + ((k >> 1) & 1), uz + (k >> 2), true);
+          float g = glowOf(f.z);
+          mine |= (g > .002f ? 1 : 0) | (f.x + g > .002f ? 2 : 0);
+        }
+      }
+      if (mine) atomicOr(&flags, mine);
+      __syncthreads();
+      if (threadIdx.x == 0) R.occupancy[(size_t)slot * blocks + b] = (uint8_t)flags;
+      __syncthreads();
+    }
+    // The brick's texels of the lighting lattice.
+    for (int k = threadIdx.x; k < L3; k += blockDim.x) {
+      int lx = k % L, ly = (k / L) % L, lz = k / (L * L);
+      float4 light = incidentLight(P, R, c, ((float)(bx * L + lx) + .5f) * texel, ((float)(by * L + ly) + .5f) * texel,
+                                   ((float)(bz * L + lz) + .5f) * texel);
+      size_t o = (size_t)slot * 4 * L3 + k;
+      R.lighting[o] = light.x;
+      R.lighting[o + L3] = light.y;
+      R.lighting[o + 2 * L3] = light.z;
+      R.lighting[o + 3 * L3] = light.w;
+    }
+  }
+}
+
+// fireProLight (volume-bricks.wgsl:158-178) at `q` in lighting texels.
+FP_DEV float4 lightSample(const SimParams& P, const FpRender& R, SlotCache& c, float qx, float qy, float qz) {
+  const int L = 1 << R.lightShift, L3 = L * L * L;
+  const float texel = P.h * (float)(P.B >> R.lightShift);
+  qx = fminf(fmaxf(qx, (float)R.boxLo[0] * L + .5f), (float)(R.boxHi[0] + 1) * L - .5f);
+  qy = fminf(fmaxf(qy, (float)R.boxLo[1] * L + .5f), (float)(R.boxHi[1] + 1) * L - .5f);
+  qz = fminf(fmaxf(qz, (float)R.boxLo[2] * L + .5f), (float)(R.boxHi[2] + 1) * L - .5f);
+  float gx = qx - .5f, gy = qy - .5f, gz = qz - .5f;
+  int x0 = (int)floorf(gx), y0 = (int)floorf(gy), z0 = (int)floorf(gz);
+  if (slotAt(P, R, c, x0 >> R.lightShift, y0 >> R.lightShift, z0 >> R.lightShift) < 0)
+    return make_float4(0.f, 0.f, 0.f, 1.f);
+  float fx = gx - (float)x0, fy = gy - (float)y0, fz = gz - (float)z0;
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int k = 0; k < 8; k++) {
+    int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
+    int x = x0 + dx, y = y0 + dy, z = z0 + dz;
+    float w = (dx ? fx : 1.f - fx) * (dy ? fy : 1.f - fy) * (dz ? fz : 1.f - fz);
+    int s = slotAt(P, R, c, x >> R.lightShift, y >> R.lightShift, z >> R.lightShift);
+    float4 t;
+    if (s >= 0) {
+      int m = L - 1;
+      size_t o = (size_t)s * 4 * L3 + (((z & m) * L + (y & m)) * L + (x & m));
+      t = make_float4(R.lighting[o], R.lighting[o + L3], R.lighting[o + 2 * L3], R.lighting[o + 3 * L3]);
+    } else {  // the apron of a neighbour without a slot: lit where it stands
+      t = incidentLight(P, R, c, ((float)x + .5f) * texel, ((float)y + .5f) * texel, ((float)z + .5f) * texel);
+    }
+    add4(v, t, w);
+  }
+  return v;
+}
+
+// fireProJitter (volume-march.wgsl:94-102).
+FP_DEV float jitterOf(uint32_t px, uint32_t py, float time) {
+  uint32_t s0 = px * 1664525u + 1013904223u, s1 = py * 1664525u + 1013904223u,
+           s2 = (uint32_t)(time * 60.f) * 1664525u + 1013904223u;
+  s0 += s1 * s2;
+  s1 += s2 * s0;
+  s2 += s0 * s1;
+  s0 ^= s0 >> 16u;
+  s1 ^= s1 >> 16u;
+  s2 ^= s2 >> 16u;
+  s0 += s1 * s2;
+  return (float)(s0 >> 8u) / 16777216.f;
+}
+
+// A pixel's march (fireProSceneVolume with fireProMarch), a thread a pixel.
+__global__ void __launch_bounds__(RTHREADS) k_march(const SimParams* __restrict__ Pp, FpRender R) {
+  const SimParams& P = *Pp;
+  int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= R.width * R.height) return;
+  int px = pix % R.width, py = pix / R.width;
+  float4* out = reinterpret_cast<float4*>(R.image) + pix;
+  *out = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (!R.hasBox) return;
+  // fireProRay
+  float ux = ((float)px + .5f) / (float)R.width, uy = ((float)py + .5f) / (float)R.height;
+  float cx = ux * 2.f - 1.f, cy = 1.f - uy * 2.f;
+  const float* M = R.ivp;
+  auto apply = [&](float z, float* o) {
+    for (int r = 0; r < 4; r++) o[r] = M[r] * cx + M[4 + r] * cy + M[8 + r] * z + M[12 + r];
+  };
+  float nh[4], fh[4];
+  apply(0.f, nh);
+  apply(.99999f, fh);
+  float ro[3] = {nh[0] / nh[3], nh[1] / nh[3], nh[2] / nh[3]};
+  float rd[3] = {fh[0] / fh[3] - ro[0], fh[1] / fh[3] - ro[1], fh[2] / fh[3] - ro[2]};
+  float rl = sqrtf(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2]);
+  for (int a = 0; a < 3; a++) rd[a] /= rl;
+  // fireProHit / fireProSpan over the box
+  const float brickSize = P.h * (float)P.B;
+  float safe[3], exitSide[3], lo = 0.f, hi = 1e30f;
+  for (int a = 0; a < 3; a++) {
+    safe[a] = fabsf(rd[a]) > 1e-6f ? rd[a] : 1e-6f;
+    exitSide[a] = rd[a] > 0.f ? 1.f : 0.f;
+    float ta = ((float)R.boxLo[a] * brickSize - ro[a]) / safe[a];
+    float tb = ((float)(R.boxHi[a] + 1) * brickSize - ro[a]) / safe[a];
+    lo = fmaxf(lo, fminf(ta, tb));
+    hi = fminf(hi, fmaxf(ta, tb));
+  }
+  if (!(hi > lo)) return;
+  const float end = hi, exitT = hi;
+  const float stepSize = fmaxf(P.h * .5f, (hi - lo) / (float)R.raySteps);
+  const float jitter = jitterOf((uint32_t)px, (uint32_t)py, R.time);
+  // fireProDirect
+  float ln = sqrtf(R.light[0] * R.light[0] + R.light[1] * R.light[1] + R.light[2] * R.light[2]);
+  float g = R.optical[3];
+  float mu = (rd[0] * R.light[0] + rd[1] * R.light[1] + rd[2] * R.light[2]) / ln;
+  float phase = (1.f - g * g) / powf(fmaxf(.05f, 1.f + g * g - 2.f * g * mu), 1.5f);
+  float dk = R.light[3] * (.35f + phase * .3f);
+  float direct[3] = {R.sceneLight[0] * dk, R.sceneLight[1] * dk, R.sceneLight[2] * dk};
+  const float lightRatio = (float)(P.B >> R.lightShift);
+  SlotCache c{0, 0, 0, -1};
+  c.bx = 1 << 30;
+  float t = lo, trans = 1.f;
+  float rad[3] = {0.f, 0.f, 0.f};
+  while (t < end && trans >= .008f) {
+    if (t >= exitT) break;
+    float ds = fminf(stepSize, fminf(end, exitT) - t);
+    float tt = t + jitter * ds;
+    float p[3] = {ro[0] + rd[0] * tt, ro[1] + rd[1] * tt, ro[2] + rd[2] * tt};
+    float cell[3] = {p[0] / P.h, p[1] / P.h, p[2] / P.h};
+    int ci[3] = {(int)floorf(cell[0]), (int)floorf(cell[1]), (int)floorf(cell[2])};
+    int slot = slotAt(P, R, c, ci[0] >> P.shift, ci[1] >> P.shift, ci[2] >> P.shift);
+    float size = brickSize;
+    int flags = 0;
+    if (slot >= 0) {  // fireProOccupancy: the sample's 8-cell block of the brick
+      const int per = P.B / 8, m = P.B - 1;
+      int block = ((((ci[2] & m) >> 3) * per) + ((ci[1] & m) >> 3)) * per + ((ci[0] & m) >> 3);
+      flags = R.occupancy[(size_t)slot * per * per * per + block];
+      size = P.h * 8.f;
+    }
+    if (!(flags & 2)) {
+      // Skip whole steps past the empty block, keeping the lattice.
+      float dist = 1e30f;
+      for (int a = 0; a < 3; a++) dist = fminf(dist, ((floorf(p[a] / size) + exitSide[a]) * size - p[a]) / safe[a]);
+      t = fminf(t + fmaxf(1.f, floorf(dist / stepSize) + 1.f) * stepSize, exitT);
+      continue;
+    }
+    float4 f = reconstruct(P, R, c, cell[0], cell[1], cell[2], (flags & 1) ? R.filter : 0);
+    if (f.x + glowOf(f.z) > .002f) {
+      // fireProShade
+      float3 glow = emissionOf(R, f);
+      float density = fmaxf(0.f, f.x) * R.optical[0];
+      float sc[3] = {0.f, 0.f, 0.f};
+      if (density > 0.f) {
+        float4 inc = lightSample(P, R, c, cell[0] / lightRatio, cell[1] / lightRatio, cell[2] / lightRatio);
+        sc[0] = R.smoke[0] * (R.ambient[0] + direct[0] * inc.w + inc.x * .65f) * density;
+        sc[1] = R.smoke[1] * (R.ambient[1] + direct[1] * inc.w + inc.y * .65f) * density;
+        sc[2] = R.smoke[2] * (R.ambient[2] + direct[2] * inc.w + inc.z * .65f) * density;
+      }
+      float ext = extinctionOf(R, f);
+      float tau = ext * ds;
+      float integral = ds * (1.f - .5f * tau + tau * tau / 6.f);
+      if (tau >= .001f) integral = (1.f - expf(-tau)) / ext;
+      rad[0] += trans * (sc[0] + glow.x) * integral;
+      rad[1] += trans * (sc[1] + glow.y) * integral;
+      rad[2] += trans * (sc[2] + glow.z) * integral;
+      trans *= 1.f - fminf(1.f, ext * integral);
+    }
+    t += ds;
+  }
+  *out = make_float4(rad[0], rad[1], rad[2], 1.f - trans);
+}
+
+}  // namespace
+
+void fp_launch_render(const SimParams* dP, const FpRender& R, int sms, cudaStream_t st) {
+  k_render_field<<<sms * 8, RTHREADS, 0, st>>>(dP, R);
+  k_render_light<<<sms * 8, RTHREADS, 0, st>>>(dP, R);
+  int pixels = R.width * R.height;
+  k_march<<<(pixels + RTHREADS - 1) / RTHREADS, RTHREADS, 0, st>>>(dP, R);
+}

@@ -1,0 +1,33 @@
+// Device-side description of one render of a simulation (fp_sim_render): the camera, the
+// render settings as the reference's RenderParams uniform holds them (volume-common.wgsl:4-10),
+// the render box and the render pools.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fp_types.h"
+
+#define FP_BLACKBODY_SIZE 512
+
+struct FpRender {
+  float ivp[16];  // clip to world, column-major
+  int width, height;
+  float time;
+  float optical[4], light[4], smoke[4], fire[4];
+  float sceneLight[3], ambient[3];
+  float flameOpacity;
+  int shadowSamples, raySteps, filter;
+  int lightShift;       // lighting texels per brick side = 1 << lightShift
+  int boxLo[3], boxHi[3];  // the render box in bricks, inclusive
+  int hasBox;
+  float* renderField;   // [slot][4][cells]: smoothed smoke, heat, lifetime, fuel
+  float* lighting;      // [slot][4][texels]: glow RGB, sun transmittance
+  uint8_t* occupancy;   // [slot]: bit 0 flame glow, bit 1 anything visible, in the block and halo
+  const float4* lut;    // blackbody: peak-normalised linear RGB, log2 radiance
+  float* image;         // width x height x 4
+};
+
+// Launchers (fp_render.cu): the render pools of every active brick in the box, then the march.
+void fp_launch_render(const SimParams* dP, const FpRender& R, int sms, cudaStream_t st);
+// The blackbody table (blackbody.ts:85-97) computed on the host, FP_BLACKBODY_SIZE entries.
+void fp_blackbody_table(float* out4);

@@ -1,0 +1,209 @@
+// Host side of the volume render (fp_render.cu): the blackbody table, the render box and
+// Engine::render.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fp_engine.hpp"
+#include "fp_render.h"
+
+// blackbodyTable (src/engine/blackbody.ts:1-97): Planck radiance integrated against the
+// multi-lobe CIE 1931 observer fit of Wyman, Sloan and Shirley (JCGT 2013, Table 1) at 5 nm
+// from 360 nm, converted to linear sRGB, each entry peak-normalised with its log2 radiance
+// relative to 1800 K; 500 K to 10000 K.
+static const double kLobes[3][3][4] = {
+    {{0.362, 442, 0.0624, 0.0374}, {1.056, 599.8, 0.0264, 0.0323}, {-0.065, 501.1, 0.049, 0.0382}},
+    {{0.821, 568.8, 0.0213, 0.0247}, {0.286, 530.9, 0.0613, 0.0322}, {0, 0, 0, 0}},
+    {{1.217, 437, 0.0845, 0.0278}, {0.681, 459, 0.0385, 0.0725}, {0, 0, 0, 0}}};
+static const int kLobeCount[3] = {3, 2, 2};
+
+static void blackbodyRGB(double kelvin, double rgb[3]) {
+  const double h = 6.62607015e-34, c = 299792458.0, k = 1.380649e-23;
+  double xyz[3] = {0, 0, 0};
+  for (int i = 0; i < 95; i++) {
+    double wavelength = 360.0 + i * 5.0;
+    double w = wavelength * 1e-9;
+    double radiance = 2.0 * h * c * c / (std::pow(w, 5) * std::expm1(h * c / (w * k * kelvin))) * 5e-9;
+    for (int ch = 0; ch < 3; ch++) {
+      double s = 0.0;
+      for (int l = 0; l < kLobeCount[ch]; l++) {
+        const double* L = kLobes[ch][l];
+        double d = (wavelength - L[1]) * (wavelength < L[1] ? L[2] : L[3]);
+        s += L[0] * std::exp(-0.5 * d * d);
+      }
+      xyz[ch] += s * radiance;
+    }
+  }
+  rgb[0] = std::max(0.0, 3.2406 * xyz[0] - 1.5372 * xyz[1] - 0.4986 * xyz[2]);
+  rgb[1] = std::max(0.0, -0.9689 * xyz[0] + 1.8758 * xyz[1] + 0.0415 * xyz[2]);
+  rgb[2] = std::max(0.0, 0.0557 * xyz[0] - 0.204 * xyz[1] + 1.057 * xyz[2]);
+}
+
+void fp_blackbody_table(float* out4) {
+  double ref[3];
+  blackbodyRGB(1800.0, ref);
+  double refPeak = std::max(ref[0], std::max(ref[1], ref[2]));
+  for (int i = 0; i < FP_BLACKBODY_SIZE; i++) {
+    double kelvin = 500.0 + (10000.0 - 500.0) * i / (FP_BLACKBODY_SIZE - 1);
+    double rgb[3];
+    blackbodyRGB(kelvin, rgb);
+    double peak = std::max(rgb[0], std::max(rgb[1], rgb[2]));
+    if (peak <= 0) {
+      out4[i * 4 + 0] = out4[i * 4 + 1] = out4[i * 4 + 2] = 0.f;
+      out4[i * 4 + 3] = -32.f;
+      continue;
+    }
+    for (int ch = 0; ch < 3; ch++) out4[i * 4 + ch] = (float)(rgb[ch] / peak);
+    out4[i * 4 + 3] = (float)std::max(-32.0, std::log2(peak / refPeak));
+  }
+}
+
+namespace fp {
+
+// updateBoxes (FluidSimulation.ts:916-957) for a scene of one cluster: the bricks with content
+// at the latest measurement and the sources' bricks, whose centre lies in a tile, grown by two
+// bricks and kept within the tiles.
+void Engine::updateRenderBox() {
+  const int TB = 4, MARGIN = 2;
+  int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  bool any = false;
+  auto include = [&](const int* l, const int* u) {
+    int c[3];
+    for (int a = 0; a < 3; a++) c[a] = (int)std::floor(((double)l[a] + (double)u[a]) / 2.0);
+    if (ground_) c[1] = std::max(0, c[1]);
+    auto div = [](int n) { return (int)std::floor((double)n / 4.0); };
+    if (dir_.slotAt(div(c[0]), div(c[1]), div(c[2])) < 0) return;
+    for (int a = 0; a < 3; a++) {
+      lo[a] = any ? std::min(lo[a], l[a]) : l[a];
+      hi[a] = any ? std::max(hi[a], u[a]) : u[a];
+    }
+    any = true;
+  };
+  for (auto& ct : contentTiles_) {
+    int t[3] = {ct.first.x, ct.first.y, ct.first.z}, l[3], u[3];
+    bool ok = true;
+    for (int a = 0; a < 3; a++) {
+      uint32_t used = (ct.second >> (a * 4)) & 15u;
+      if (!used) ok = false;
+      if (!used) break;
+      l[a] = t[a] * TB + __builtin_ctz(used);
+      u[a] = t[a] * TB + (31 - __builtin_clz(used));
+    }
+    if (ok) include(l, u);
+  }
+  for (size_t s = 0; s + 6 <= sourceBoxes_.size(); s += 6) include(&sourceBoxes_[s], &sourceBoxes_[s + 3]);
+  renderBox_ = any;
+  if (!any) return;
+  // The tiles' extent in bricks.
+  int tlo[3] = {0, 0, 0}, thi[3] = {0, 0, 0};
+  bool first = true;
+  for (const auto& t : dir_.slots()) {
+    if (!t.alive) continue;
+    int v[3] = {t.x, t.y, t.z};
+    for (int a = 0; a < 3; a++) {
+      tlo[a] = first ? v[a] : std::min(tlo[a], v[a]);
+      thi[a] = first ? v[a] : std::max(thi[a], v[a]);
+    }
+    first = false;
+  }
+  for (int a = 0; a < 3; a++) {
+    renderLo_[a] = std::max(lo[a] - MARGIN, tlo[a] * TB);
+    renderHi_[a] = std::min(hi[a] + MARGIN, (thi[a] + 1) * TB - 1);
+  }
+}
+
+int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* image, float* host) {
+  if (cam.width == 0 || cam.height == 0 || cam.width > 16384 || cam.height > 16384)
+    return fail(FP_EINVAL, "render: width and height must be from 1 to 16384.");
+  if (rs.lighting_divisor != 1 && rs.lighting_divisor != 2 && rs.lighting_divisor != 4)
+    return fail(FP_EINVAL, "rendering.lightingDivisor must be 1, 2 or 4.");
+  if (rs.ray_steps < 8 || rs.ray_steps > 1024) return fail(FP_EINVAL, "rendering.raySteps must be from 8 to 1024.");
+  if (rs.shadow_samples < 1 || rs.shadow_samples > 256) return fail(FP_EINVAL, "shadow samples must be from 1 to 256.");
+  if (rs.filter < 0 || rs.filter > 2) return fail(FP_EINVAL, "rendering.filter must be 0, 1 or 2.");
+  int rc = consume();
+  if (rc) return rc;
+  const int divShift = rs.lighting_divisor == 1 ? 0 : (rs.lighting_divisor == 2 ? 1 : 2);
+  const int lightShift = shift_ - divShift, L = 1 << lightShift, blocks = (B_ / 8) * (B_ / 8) * (B_ / 8);
+  size_t pixels = (size_t)cam.width * cam.height;
+  // Pools sized for every slot; the table and the parameters once.
+  bool ok = (renderField_.bytes >= (size_t)slots_ * 4 * N_ * 4 || grow(renderField_, (size_t)slots_ * 4 * N_ * 4, 0)) &&
+            (lighting_.bytes >= (size_t)slots_ * 4 * L * L * L * 4 ||
+             grow(lighting_, (size_t)slots_ * 4 * L * L * L * 4, 0)) &&
+            (occupancy_.bytes >= (size_t)slots_ * blocks || grow(occupancy_, (size_t)slots_ * blocks, 0)) &&
+            (renderParams_.ptr || alloc(renderParams_, sizeof(SimParams), false));
+  if (!ok) return FP_ENOMEM;
+  if (!lut_.ptr) {
+    std::vector<float> table(FP_BLACKBODY_SIZE * 4);
+    fp_blackbody_table(table.data());
+    if (!alloc(lut_, table.size() * 4, false)) return FP_ENOMEM;
+    if ((rc = check(cudaMemcpy(lut_.ptr, table.data(), table.size() * 4, cudaMemcpyHostToDevice), "render"))) return rc;
+  }
+  if (!renderParamsH_ && (rc = check(cudaMallocHost(&renderParamsH_, sizeof(SimParams)), "cudaMallocHost"))) return rc;
+  float* out = image;
+  if (host) {
+    if (image_.bytes < pixels * 16 && !alloc(image_, pixels * 16, false)) return FP_ENOMEM;
+    out = (float*)image_.ptr;
+  }
+  // The parameters the render reads: the latest state and the directory.
+  cudaStreamSynchronize(stream());  // the previous render's parameters were read
+  SimParams& P = *renderParamsH_;
+  std::memset(&P, 0, sizeof(P));
+  P.B = B_;
+  P.shift = shift_;
+  P.N = N_;
+  P.W = W_;
+  P.h = h_;
+  P.invH = 1.f / h_;
+  P.capacity = capacity_;
+  P.tileRec = (const int4*)tileRecD_.ptr;
+  P.tileNbr = (const int*)tileNbrD_.ptr;
+  P.hash = (const int4*)hashD_.ptr;
+  P.hashMask = (uint32_t)hash_.size() - 1;
+  P.entries = (int*)entries_.ptr;
+  P.records = (int*)records_.ptr;
+  P.active = (uint32_t*)active_.ptr;
+  P.counters = (FpCounters*)counters_.ptr;
+  P.fld = (float*)fld_[fldIdx_[0]].ptr;
+  P.scalarHalf = precision_ == FP_PRECISION_MIXED ? 1 : 0;
+  if ((rc = check(cudaMemcpyAsync(renderParams_.ptr, &P, sizeof(P), cudaMemcpyHostToDevice, stream()), "render")))
+    return rc;
+  FpRender R;
+  std::memset(&R, 0, sizeof(R));
+  std::memcpy(R.ivp, cam.inverse_view_projection, sizeof(R.ivp));
+  R.width = (int)cam.width;
+  R.height = (int)cam.height;
+  R.time = cam.time;
+  std::memcpy(R.optical, rs.optical, sizeof(R.optical));
+  std::memcpy(R.light, rs.light, sizeof(R.light));
+  std::memcpy(R.smoke, rs.smoke, sizeof(R.smoke));
+  std::memcpy(R.fire, rs.fire, sizeof(R.fire));
+  std::memcpy(R.sceneLight, rs.scene_light, sizeof(R.sceneLight));
+  std::memcpy(R.ambient, rs.ambient_light, sizeof(R.ambient));
+  R.flameOpacity = rs.flame_opacity;
+  R.shadowSamples = (int)rs.shadow_samples;
+  R.raySteps = (int)rs.ray_steps;
+  R.filter = rs.filter;
+  R.lightShift = lightShift;
+  for (int a = 0; a < 3; a++) {
+    R.boxLo[a] = renderLo_[a];
+    R.boxHi[a] = renderHi_[a];
+  }
+  R.hasBox = renderBox_ && steps_ > 0 ? 1 : 0;
+  R.renderField = (float*)renderField_.ptr;
+  R.lighting = (float*)lighting_.ptr;
+  R.occupancy = (uint8_t*)occupancy_.ptr;
+  R.lut = (const float4*)lut_.ptr;
+  R.image = out;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, owner_->device());
+  fp_launch_render((const SimParams*)renderParams_.ptr, R, sms, stream());
+  if ((rc = check(cudaGetLastError(), "render launch"))) return rc;
+  if (host) {
+    if ((rc = check(cudaMemcpyAsync(host, out, pixels * 16, cudaMemcpyDeviceToHost, stream()), "render"))) return rc;
+    return check(cudaStreamSynchronize(stream()), "render");
+  }
+  return FP_OK;
+}
+
+}  // namespace fp

@@ -182,6 +182,27 @@ class fp_stats(C.Structure):
     ]
 
 
+class fp_camera(C.Structure):
+    _fields_ = [("inverse_view_projection", C.c_float * 16), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("time", C.c_float)]
+
+
+class fp_render_settings(C.Structure):
+    _fields_ = [
+        ("optical", C.c_float * 4),
+        ("light", C.c_float * 4),
+        ("smoke", C.c_float * 4),
+        ("fire", C.c_float * 4),
+        ("scene_light", C.c_float * 3),
+        ("ambient_light", C.c_float * 3),
+        ("flame_opacity", C.c_float),
+        ("shadow_samples", C.c_uint32),
+        ("ray_steps", C.c_uint32),
+        ("filter", C.c_int32),
+        ("lighting_divisor", C.c_uint32),
+    ]
+
+
 FP_MAX_VCYCLES = 16
 
 
@@ -280,6 +301,8 @@ SIGNATURES = {
     "fp_grid_reserved_tiles": (C.c_int, [C.POINTER(fp_grid), C.POINTER(C.c_uint32)]),
     "fp_sim_reserve_tiles": (C.c_int, [C.c_void_p, C.c_uint32]),
     "fp_sim_set_solver": (C.c_int, [C.c_void_p, C.c_int, C.c_float]),
+    "fp_sim_render": (C.c_int, [C.c_void_p, C.POINTER(fp_camera), C.POINTER(fp_render_settings), C.c_void_p]),
+    "fp_sim_render_device": (C.c_int, [C.c_void_p, C.POINTER(fp_camera), C.POINTER(fp_render_settings), C.c_void_p]),
     "fp_sim_read_solver": (C.c_int, [C.c_void_p, C.POINTER(fp_solver_stats)]),
     "fp_batch_set_solver": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_float]),
     "fp_batch_read_solver": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(fp_solver_stats)]),

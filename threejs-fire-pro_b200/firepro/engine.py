@@ -60,6 +60,16 @@ class FluidSimulation:
         """Up to `vcycles` V-cycles a step, stopping at relative residual `tolerance` (0: all)."""
         self._check(self.lib.fp_sim_set_solver(self.h, vcycles, tolerance))
 
+    def render(self, camera: abi.fp_camera, settings: abi.fp_render_settings) -> np.ndarray:
+        """The latest state rendered: (height, width, 4) linear radiance and opacity."""
+        out = np.zeros((camera.height, camera.width, 4), np.float32)
+        self._check(self.lib.fp_sim_render(self.h, C.byref(camera), C.byref(settings), out.ctypes.data))
+        return out
+
+    def render_device(self, camera: abi.fp_camera, settings: abi.fp_render_settings, image_ptr: int):
+        """Render into device memory at `image_ptr` (width x height x 4 floats), enqueued."""
+        self._check(self.lib.fp_sim_render_device(self.h, C.byref(camera), C.byref(settings), image_ptr))
+
     def read_solver(self) -> abi.fp_solver_stats:
         """The latest step's pressure solve (waits for the step)."""
         s = abi.fp_solver_stats()
