@@ -131,6 +131,14 @@ FP_DEV float cellAt(const SimParams& P, const Home& H, const float* pool, int ch
   return ldHalf(pool, ((size_t)s * ch + c) * P.N + localCell(P, x, y, z), half);
 }
 
+// a + t (b - a): exact at t = 0 and wherever a == b, so a constant field samples exactly.
+FP_DEV float lerpf(float a, float b, float t) { return fmaf(t, b - a, a); }
+// Trilinear blend of the 2x2x2 corner values t (x fastest, then y, then z).
+FP_DEV float blend8(const float* t, float fx, float fy, float fz) {
+  return lerpf(lerpf(lerpf(t[0], t[1], fx), lerpf(t[2], t[3], fx), fy),
+               lerpf(lerpf(t[4], t[5], fx), lerpf(t[6], t[7], fx), fy), fz);
+}
+
 // Trilinear sample of one channel at `pos` in cell units, centres at .5
 // (fluid-sampling.wgsl:85-114): bricks without a slot read zero.
 FP_DEV float sampleCells(const SimParams& P, const Home& H, const float* pool, int ch, int c, float px, float py,
@@ -141,19 +149,14 @@ FP_DEV float sampleCells(const SimParams& P, const Home& H, const float* pool, i
   int sh = P.shift;
   int bx0 = x0 >> sh, bx1 = (x0 + 1) >> sh, by0 = y0 >> sh, by1 = (y0 + 1) >> sh, bz0 = z0 >> sh,
       bz1 = (z0 + 1) >> sh;
-  float v = 0.f;
+  float t[8];
 #pragma unroll
-  for (int dz = 0; dz < 2; dz++)
-#pragma unroll
-    for (int dy = 0; dy < 2; dy++)
-#pragma unroll
-      for (int dx = 0; dx < 2; dx++) {
-        int s = brickSlot(P, H, dx ? bx1 : bx0, dy ? by1 : by0, dz ? bz1 : bz0);
-        float w = (dx ? fx : 1.f - fx) * (dy ? fy : 1.f - fy) * (dz ? fz : 1.f - fz);
-        float val = s < 0 ? 0.f : ldHalf(pool, ((size_t)s * ch + c) * P.N + localCell(P, x0 + dx, y0 + dy, z0 + dz), half);
-        v += val * w;
-      }
-  return v;
+  for (int j = 0; j < 8; j++) {
+    int dx = j & 1, dy = (j >> 1) & 1, dz = j >> 2;
+    int s = brickSlot(P, H, dx ? bx1 : bx0, dy ? by1 : by0, dz ? bz1 : bz0);
+    t[j] = s < 0 ? 0.f : ldHalf(pool, ((size_t)s * ch + c) * P.N + localCell(P, x0 + dx, y0 + dy, z0 + dz), half);
+  }
+  return blend8(t, fx, fy, fz);
 }
 
 // solidCell (solids.wgsl:15-31): the ground, then colliders drawn into each slot's bits.

@@ -20,6 +20,10 @@ namespace {
 
 constexpr int THREADS = 256;
 constexpr int HALO = 2;
+// Resident CTAs per SM the transport kernels are compiled for (register cap 65536 / (256 n)).
+#ifndef FP_TRANSPORT_CTAS
+#define FP_TRANSPORT_CTAS 4
+#endif
 
 // Where the staged copy sits: its first cell and its side.
 struct Stage {
@@ -34,13 +38,36 @@ struct Field {
   bool half;  // the pool holds __half (the scalar pools in FP_PRECISION_MIXED)
 };
 
-FP_DEV float fieldCell(const SimParams& P, const Home& H, const Stage& G, const Field& f, int c, int x, int y, int z) {
-  if (f.sm) {
-    unsigned lx = (unsigned)(x - G.ox), ly = (unsigned)(y - G.oy), lz = (unsigned)(z - G.oz);
-    if (lx < (unsigned)G.S && ly < (unsigned)G.S && lz < (unsigned)G.S)
-      return f.sm[c * G.S3 + ((int)lz * G.S + (int)ly) * G.S + (int)lx];
-  }
+// The staged offset of cell (x,y,z), which the caller knows lies inside the staged box.
+FP_DEV int stagedAt(const Stage& G, int x, int y, int z) { return ((z - G.oz) * G.S + (y - G.oy)) * G.S + (x - G.ox); }
+
+// A cell within HALO cells of the home brick: the staged box always holds it, so no check.
+FP_DEV float nearCell(const SimParams& P, const Home& H, const Stage& G, const Field& f, int c, int x, int y, int z) {
+  if (f.sm) return f.sm[c * G.S3 + stagedAt(G, x, y, z)];
   return cellAt(P, H, f.pool, f.ch, c, x, y, z, f.half);
+}
+
+// The 2x2x2 block from corner (x0,y0,z0) of channel c into t (x fastest): from shared memory
+// when `b` (the corner's staged address, channel 0) is set, else through the directory.
+FP_DEV void blockCells(const SimParams& P, const Home& H, const Stage& G, const Field& f, int c, const float* b, int x0,
+                       int y0, int z0, float* t) {
+  if (b) {
+    const float* q = b + c * G.S3;
+    int S = G.S, S2 = G.S * G.S;
+    t[0] = q[0]; t[1] = q[1]; t[2] = q[S]; t[3] = q[S + 1];
+    t[4] = q[S2]; t[5] = q[S2 + 1]; t[6] = q[S2 + S]; t[7] = q[S2 + S + 1];
+    return;
+  }
+#pragma unroll
+  for (int j = 0; j < 8; j++) t[j] = cellAt(P, H, f.pool, f.ch, c, x0 + (j & 1), y0 + ((j >> 1) & 1), z0 + (j >> 2), f.half);
+}
+// The staged address of the block from corner (x0,y0,z0) when the whole block is staged.
+FP_DEV const float* stagedBlock(const Stage& G, const Field& f, int x0, int y0, int z0) {
+  if (!f.sm) return nullptr;
+  unsigned lx = (unsigned)(x0 - G.ox), ly = (unsigned)(y0 - G.oy), lz = (unsigned)(z0 - G.oz);
+  unsigned lim = (unsigned)(G.S - 1);
+  if (lx < lim && ly < lim && lz < lim) return f.sm + ((int)lz * G.S + (int)ly) * G.S + (int)lx;
+  return nullptr;
 }
 
 // Trilinear sample at `pos` in cell units (fluid-sampling.wgsl:85-114).
@@ -48,22 +75,12 @@ FP_DEV float fieldSample(const SimParams& P, const Home& H, const Stage& G, cons
                          float pz) {
   if (f.sm) {
     float qx = px - 0.5f, qy = py - 0.5f, qz = pz - 0.5f;
-    int x0 = (int)floorf(qx), y0 = (int)floorf(qy), z0 = (int)floorf(qz);
-    unsigned lx = (unsigned)(x0 - G.ox), ly = (unsigned)(y0 - G.oy), lz = (unsigned)(z0 - G.oz);
-    if (lx < (unsigned)(G.S - 1) && ly < (unsigned)(G.S - 1) && lz < (unsigned)(G.S - 1)) {
-      float fx = qx - (float)x0, fy = qy - (float)y0, fz = qz - (float)z0;
-      const float* b = f.sm + c * G.S3 + ((int)lz * G.S + (int)ly) * G.S + (int)lx;
-      int S = G.S, S2 = G.S * G.S;
-      float v = 0.f;
-      v += b[0] * ((1.f - fx) * (1.f - fy) * (1.f - fz));
-      v += b[1] * (fx * (1.f - fy) * (1.f - fz));
-      v += b[S] * ((1.f - fx) * fy * (1.f - fz));
-      v += b[S + 1] * (fx * fy * (1.f - fz));
-      v += b[S2] * ((1.f - fx) * (1.f - fy) * fz);
-      v += b[S2 + 1] * (fx * (1.f - fy) * fz);
-      v += b[S2 + S] * ((1.f - fx) * fy * fz);
-      v += b[S2 + S + 1] * (fx * fy * fz);
-      return v;
+    float gx = floorf(qx), gy = floorf(qy), gz = floorf(qz);
+    const float* b = stagedBlock(G, f, (int)gx, (int)gy, (int)gz);
+    if (b) {
+      float t[8];
+      blockCells(P, H, G, f, c, b, 0, 0, 0, t);
+      return blend8(t, qx - gx, qy - gy, qz - gz);
     }
   }
   return sampleCells(P, H, f.pool, f.ch, c, px, py, pz, f.half);
@@ -114,25 +131,57 @@ FP_DEV Stage stageOf(const SimParams& P, const Home& H, bool staged) {
   return G;
 }
 
+// Component c of the staggered velocity at world position p: stored half a cell back along c.
 FP_DEV float velComp(const SimParams& P, const Home& H, const Stage& G, const Field& v, float px, float py, float pz,
                      int c) {
-  float q[3] = {px, py, pz};
-  q[c] -= 0.5f * P.h;
-  return fieldSample(P, H, G, v, c, q[0] / P.h, q[1] / P.h, q[2] / P.h);
+  float qx = px * P.invH, qy = py * P.invH, qz = pz * P.invH;
+  return fieldSample(P, H, G, v, c, c == 0 ? qx - 0.5f : qx, c == 1 ? qy - 0.5f : qy, c == 2 ? qz - 0.5f : qz);
 }
-// velocityAt (fluid-advection.wgsl:17-21).
+// velocityAt (fluid-advection.wgsl:17-21): the three staggered samples share their floors
+// (per axis: unshifted, and shifted half a cell for the component stored along it) and one
+// check that all three blocks are staged.
 FP_DEV float3 velocityAt(const SimParams& P, const Home& H, const Stage& G, const Field& v, float px, float py,
                          float pz) {
-  return make_float3(velComp(P, H, G, v, px, py, pz, 0), velComp(P, H, G, v, px, py, pz, 1),
-                     velComp(P, H, G, v, px, py, pz, 2));
+  const float q[3] = {px * P.invH, py * P.invH, pz * P.invH};
+  if (v.sm) {
+    const int o[3] = {G.ox, G.oy, G.oz};
+    int i0[3], i1[3];
+    float f0[3], f1[3];
+    bool in = true;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      float u0 = q[a] - 0.5f, u1 = q[a] - 1.f;
+      float g0 = floorf(u0), g1 = floorf(u1);
+      i0[a] = (int)g0 - o[a];
+      i1[a] = (int)g1 - o[a];
+      f0[a] = u0 - g0;
+      f1[a] = u1 - g1;
+      in = in && i1[a] >= 0 && i0[a] < G.S - 1;  // i1 <= i0 <= i1 + 1
+    }
+    if (in) {
+      const int S = G.S, S2 = G.S * G.S;
+      float t[8];
+      float3 r;
+      blockCells(P, H, G, v, 0, v.sm + i0[2] * S2 + i0[1] * S + i1[0], 0, 0, 0, t);
+      r.x = blend8(t, f1[0], f0[1], f0[2]);
+      blockCells(P, H, G, v, 1, v.sm + i0[2] * S2 + i1[1] * S + i0[0], 0, 0, 0, t);
+      r.y = blend8(t, f0[0], f1[1], f0[2]);
+      blockCells(P, H, G, v, 2, v.sm + i1[2] * S2 + i0[1] * S + i0[0], 0, 0, 0, t);
+      r.z = blend8(t, f0[0], f0[1], f1[2]);
+      return r;
+    }
+  }
+  return make_float3(sampleCells(P, H, v.pool, v.ch, 0, q[0] - 0.5f, q[1], q[2], v.half),
+                     sampleCells(P, H, v.pool, v.ch, 1, q[0], q[1] - 0.5f, q[2], v.half),
+                     sampleCells(P, H, v.pool, v.ch, 2, q[0], q[1], q[2] - 0.5f, v.half));
 }
 FP_DEV float get(const float3& v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
 
-// velocityOnFace (fluid-advection.wgsl:26-44): the face's own component is stored.
+// velocityOnFace (fluid-advection.wgsl:26-44): the face's own component is stored; each other
+// component k is the trilinear sample at the face centre, which falls midway between two
+// cells along c and along k and on the cell plane of the third axis: the mean of four cells.
 FP_DEV float3 velocityOnFace(const SimParams& P, const Home& H, const Stage& G, const Field& v, int x, int y, int z,
                              int c, float3 orig) {
-  float fp[3] = {(float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f};
-  fp[c] += 0.5f;
   float r[3];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
@@ -140,11 +189,19 @@ FP_DEV float3 velocityOnFace(const SimParams& P, const Home& H, const Stage& G, 
       r[k] = get(orig, k);
       continue;
     }
-    float q[3] = {fp[0], fp[1], fp[2]};
-    q[k] -= 0.5f;
-    r[k] = fieldSample(P, H, G, v, k, q[0], q[1], q[2]);
+    const int cx = c == 0, cy = c == 1, cz = c == 2, kx = k == 0, ky = k == 1, kz = k == 2;
+    float a = nearCell(P, H, G, v, k, x, y, z), b = nearCell(P, H, G, v, k, x + cx, y + cy, z + cz);
+    float d = nearCell(P, H, G, v, k, x - kx, y - ky, z - kz),
+          e = nearCell(P, H, G, v, k, x + cx - kx, y + cy - ky, z + cz - kz);
+    r[k] = 0.25f * ((a + b) + (d + e));
   }
   return make_float3(r[0], r[1], r[2]);
+}
+// velocityAt at the centre of cell (x,y,z): each component midway between its two faces.
+FP_DEV float3 centreVelocity(const SimParams& P, const Home& H, const Stage& G, const Field& v, int x, int y, int z) {
+  return make_float3(0.5f * (nearCell(P, H, G, v, 0, x - 1, y, z) + nearCell(P, H, G, v, 0, x, y, z)),
+                     0.5f * (nearCell(P, H, G, v, 1, x, y - 1, z) + nearCell(P, H, G, v, 1, x, y, z)),
+                     0.5f * (nearCell(P, H, G, v, 2, x, y, z - 1) + nearCell(P, H, G, v, 2, x, y, z)));
 }
 
 // packDonor (fluid-advection.wgsl:79-95), 5 bits an axis; 1 << 15 asks for a retrace.
@@ -185,25 +242,28 @@ FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
   for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
     int x, y, z;
     cellOf(P, H, c, x, y, z);
-    // Velocity bounds over the forward 2x2x2 block.
+    // Velocity bounds over the forward 2x2x2 block (staged: HALO >= 1).
+    const float* home = V.sm ? V.sm + stagedAt(G, x, y, z) : nullptr;
+#pragma unroll
     for (int k = 0; k < 3; k++) {
+      float t[8];
+      blockCells(P, H, G, V, k, home, x, y, z, t);
       float lo = 1e5f, hi = -1e5f;
-      for (int dz = 0; dz < 2; dz++)
-        for (int dy = 0; dy < 2; dy++)
-          for (int dx = 0; dx < 2; dx++) {
-            float v = fieldCell(P, H, G, V, k, x + dx, y + dy, z + dz);
-            lo = fminf(lo, v);
-            hi = fmaxf(hi, v);
-          }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        lo = fminf(lo, t[j]);
+        hi = fmaxf(hi, t[j]);
+      }
       P.vmin[(slot * 3 + k) * N + c] = lo;
       P.vmax[(slot * 3 + k) * N + c] = hi;
     }
     float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-    if (solidAt(P, H, px, py, pz)) {
+    // solidAt at a cell centre is solidCell of that cell: centre / h + 0.25 floors to it.
+    if (solidCell(P, H, x, y, z)) {
       for (int k = 0; k < 3; k++) P.velP[(slot * 3 + k) * N + c] = 0.f;
     } else {
-      float3 orig = make_float3(fieldCell(P, H, G, V, 0, x, y, z), fieldCell(P, H, G, V, 1, x, y, z),
-                                fieldCell(P, H, G, V, 2, x, y, z));
+      float3 orig = make_float3(nearCell(P, H, G, V, 0, x, y, z), nearCell(P, H, G, V, 1, x, y, z),
+                                nearCell(P, H, G, V, 2, x, y, z));
 #pragma unroll
       for (int comp = 0; comp < 3; comp++) {
         float face[3] = {px, py, pz};
@@ -223,45 +283,43 @@ FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
       }
     }
     // Scalars: a cell-centred RK2 back trace, the predictor and its donors' range.
-    float3 cv = velocityAt(P, H, G, V, px, py, pz);
+    float3 cv = centreVelocity(P, H, G, V, x, y, z);
     float3 vm = velocityAt(P, H, G, V, px - 0.5f * P.dt * cv.x, py - 0.5f * P.dt * cv.y, pz - 0.5f * P.dt * cv.z);
     float dx_ = px - P.dt * vm.x, dy_ = py - P.dt * vm.y, dz_ = pz - P.dt * vm.z;
-    float out[4];
-    if (!P.maccormack) {
-      for (int k = 0; k < 4; k++) out[k] = fieldSample(P, H, G, F, k, dx_ / P.h, dy_ / P.h, dz_ / P.h);
-      out[2] = clamp01(out[2]);
-    } else {
-      float dc[3] = {(float)x + (dx_ - px) / P.h, (float)y + (dy_ - py) / P.h, (float)z + (dz_ - pz) / P.h};
-      int base[3];
-      float fr[3];
-      for (int a = 0; a < 3; a++) {
-        base[a] = (int)floorf(dc[a]);
-        fr[a] = dc[a] - floorf(dc[a]);
-      }
-      float mn0 = 65504.f, mn1 = 65504.f, mn3 = 65504.f, mx0 = -65504.f, mx1 = -65504.f, mx3 = -65504.f;
-      float lmin = 1.f, lmax = 0.f;
-      float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
-      for (int dz = 0; dz < 2; dz++)
-        for (int dy = 0; dy < 2; dy++)
-          for (int dx = 0; dx < 2; dx++) {
-            int cx = base[0] + dx, cy = base[1] + dy, cz = base[2] + dz;
-            float s0 = fieldCell(P, H, G, F, 0, cx, cy, cz), s1 = fieldCell(P, H, G, F, 1, cx, cy, cz),
-                  s2 = fieldCell(P, H, G, F, 2, cx, cy, cz), s3 = fieldCell(P, H, G, F, 3, cx, cy, cz);
-            mn0 = fminf(mn0, s0); mn1 = fminf(mn1, s1); mn3 = fminf(mn3, s3);
-            mx0 = fmaxf(mx0, s0); mx1 = fmaxf(mx1, s1); mx3 = fmaxf(mx3, s3);
-            lmin = fminf(lmin, s2);
-            lmax = fmaxf(lmax, s2);
-            float w = (dx ? fr[0] : 1.f - fr[0]) * (dy ? fr[1] : 1.f - fr[1]) * (dz ? fr[2] : 1.f - fr[2]);
-            v0 += s0 * w; v1 += s1 * w; v2 += s2 * w; v3 += s3 * w;
-          }
-      float* b = P.sb + slot * 8 * N;
-      b[0 * N + c] = mn0; b[1 * N + c] = mn1; b[2 * N + c] = mn3; b[3 * N + c] = lmin;
-      b[4 * N + c] = mx0; b[5 * N + c] = mx1; b[6 * N + c] = mx3; b[7 * N + c] = lmax;
-      out[0] = v0;
-      out[1] = v1;
-      out[2] = P.lifetimeZero ? 0.f : v2;
-      out[3] = v3;
+    // The departure's trilinear block in cell units: corner `base`, fractions `fr`.
+    const float dc[3] = {(float)x + (dx_ - px) * P.invH, (float)y + (dy_ - py) * P.invH,
+                         (float)z + (dz_ - pz) * P.invH};
+    int base[3];
+    float fr[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      float g = floorf(dc[a]);
+      base[a] = (int)g;
+      fr[a] = dc[a] - g;
     }
+    const float* blk = stagedBlock(G, F, base[0], base[1], base[2]);
+    float out[4];
+    float* sb = P.sb + slot * 8 * N;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      float t[8];
+      blockCells(P, H, G, F, k, blk, base[0], base[1], base[2], t);
+      out[k] = blend8(t, fr[0], fr[1], fr[2]);
+      if (P.maccormack) {
+        // The donors' range; FP16-finite for smoke, heat and fuel, [0,1]-anchored for lifetime.
+        float lo = k == 2 ? 1.f : 65504.f, hi = k == 2 ? 0.f : -65504.f;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          lo = fminf(lo, t[j]);
+          hi = fmaxf(hi, t[j]);
+        }
+        const int row = k < 2 ? k : 5 - k;  // rows: smoke, heat, fuel, lifetime
+        sb[row * N + c] = lo;
+        sb[(4 + row) * N + c] = hi;
+      }
+    }
+    if (!P.maccormack) out[2] = clamp01(out[2]);
+    else if (P.lifetimeZero) out[2] = 0.f;
     // The predictor lives within the step: FP32 in every precision, so the limiter compares
     // the corrected value with unrounded predictions.
     for (int k = 0; k < 4; k++) P.fldP[(slot * 4 + k) * N + c] = out[k];
@@ -269,7 +327,7 @@ FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
   __syncthreads();
 }
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS, 3) k_predict(FpBatch bt) {
+__global__ void __launch_bounds__(THREADS, FP_TRANSPORT_CTAS) k_predict(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
@@ -301,14 +359,14 @@ FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
     int x, y, z;
     cellOf(P, H, c, x, y, z);
     float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-    bool solid = solidAt(P, H, px, py, pz);
-    float3 orig = make_float3(fieldCell(P, H, G, V, 0, x, y, z), fieldCell(P, H, G, V, 1, x, y, z),
-                              fieldCell(P, H, G, V, 2, x, y, z));
+    bool solid = solidCell(P, H, x, y, z);  // solidAt at the cell centre
+    float3 orig = make_float3(nearCell(P, H, G, V, 0, x, y, z), nearCell(P, H, G, V, 1, x, y, z),
+                              nearCell(P, H, G, V, 2, x, y, z));
 #pragma unroll
     for (int comp = 0; comp < 3; comp++) {
       float result = 0.f;
       if (!solid) {
-        float predicted = fieldCell(P, H, G, Vp, comp, x, y, z);
+        float predicted = nearCell(P, H, G, Vp, comp, x, y, z);
         float face[3] = {px, py, pz};
         face[comp] += 0.5f * P.h;
         uint32_t donor = P.donors[(slot * 3 + comp) * N + c];
@@ -339,7 +397,7 @@ FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
                                  face[2] + 0.5f * P.dt * fv.z);
           float fw[3] = {face[0] + P.dt * vm.x, face[1] + P.dt * vm.y, face[2] + P.dt * vm.z};
           fw[comp] -= 0.5f * P.h;
-          float reversed = fieldSample(P, H, G, Vp, comp, fw[0] / P.h, fw[1] / P.h, fw[2] / P.h);
+          float reversed = fieldSample(P, H, G, Vp, comp, fw[0] * P.invH, fw[1] * P.invH, fw[2] * P.invH);
           float corrected = predicted + 0.5f * (get(orig, comp) - reversed);
           result = (corrected < lo || corrected > hi) ? predicted : corrected;
         }
@@ -350,7 +408,7 @@ FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
   __syncthreads();
 }
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS, 3) k_correct(FpBatch bt) {
+__global__ void __launch_bounds__(THREADS, FP_TRANSPORT_CTAS) k_correct(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
@@ -392,7 +450,7 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
     int x, y, z;
     cellOf(P, H, c, x, y, z);
     float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-    bool solid = solidAt(P, H, px, py, pz);
+    bool solid = solidCell(P, H, x, y, z);  // solidAt at the cell centre
     float value[4] = {0.f, 0.f, 0.f, 0.f};
     float expansion = 0.f;
     bool injected = false;
@@ -401,7 +459,7 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
     if (!solid) {
       float tr[4];
       if (!P.maccormack) {
-        for (int k = 0; k < 4; k++) tr[k] = fieldCell(P, H, G, Fp, k, x, y, z);
+        for (int k = 0; k < 4; k++) tr[k] = nearCell(P, H, G, Fp, k, x, y, z);
       } else {
         const float* b = P.sb + slot * 8 * N;
         float mn0 = b[0 * N + c], mn1 = b[1 * N + c], mn3 = b[2 * N + c], lmin = b[3 * N + c];
@@ -412,45 +470,39 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
           tr[2] = clamp01(lmin);
           tr[3] = mn3;
         } else {
-          float a0 = fieldCell(P, H, G, Fp, 0, x, y, z), a1 = fieldCell(P, H, G, Fp, 1, x, y, z),
-                a2 = fieldCell(P, H, G, Fp, 2, x, y, z), a3 = fieldCell(P, H, G, Fp, 3, x, y, z);
-          cv = velocityAt(P, H, G, V, px, py, pz);
+          float a0 = nearCell(P, H, G, Fp, 0, x, y, z), a1 = nearCell(P, H, G, Fp, 1, x, y, z),
+                a2 = nearCell(P, H, G, Fp, 2, x, y, z), a3 = nearCell(P, H, G, Fp, 3, x, y, z);
+          cv = centreVelocity(P, H, G, V, x, y, z);
           cvSampled = true;
           float3 vm = velocityAt(P, H, G, V, px + 0.5f * P.dt * cv.x, py + 0.5f * P.dt * cv.y, pz + 0.5f * P.dt * cv.z);
           float fx = px + P.dt * vm.x, fy = py + P.dt * vm.y, fz = pz + P.dt * vm.z;
           const size_t o = slot * 4 * N + c;
           float o0 = ldHalf(P.fld, o, half), o1 = ldHalf(P.fld, o + N, half), o2 = ldHalf(P.fld, o + 2 * N, half),
                 o3 = ldHalf(P.fld, o + 3 * N, half);
+          // The forward trace's trilinear block of the predictor, in cell units.
+          const float fc[3] = {(float)x + (fx - px) * P.invH, (float)y + (fy - py) * P.invH,
+                               (float)z + (fz - pz) * P.invH};
+          int base[3];
+          float fr[3];
+#pragma unroll
+          for (int a = 0; a < 3; a++) {
+            float g = floorf(fc[a]);
+            base[a] = (int)g;
+            fr[a] = fc[a] - g;
+          }
+          const float* blk = stagedBlock(G, Fp, base[0], base[1], base[2]);
+          float rs[4];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            float t[8];
+            blockCells(P, H, G, Fp, k, blk, base[0], base[1], base[2], t);
+            rs[k] = blend8(t, fr[0], fr[1], fr[2]);
+          }
+          float r0 = rs[0], r1 = rs[1], r3 = rs[3];
           float lifetime = a2;
-          float r0, r1, r3;
           if (lmin != lmax || a2 != lmin) {
-            float fc[3] = {(float)x + (fx - px) / P.h, (float)y + (fy - py) / P.h, (float)z + (fz - pz) / P.h};
-            int base[3];
-            float fr[3];
-            for (int a = 0; a < 3; a++) {
-              base[a] = (int)floorf(fc[a]);
-              fr[a] = fc[a] - floorf(fc[a]);
-            }
-            float rs0 = 0.f, rs1 = 0.f, rs2 = 0.f, rs3 = 0.f;
-            for (int dz = 0; dz < 2; dz++)
-              for (int dy = 0; dy < 2; dy++)
-                for (int dx = 0; dx < 2; dx++) {
-                  int cx = base[0] + dx, cy = base[1] + dy, cz = base[2] + dz;
-                  float w = (dx ? fr[0] : 1.f - fr[0]) * (dy ? fr[1] : 1.f - fr[1]) * (dz ? fr[2] : 1.f - fr[2]);
-                  rs0 += fieldCell(P, H, G, Fp, 0, cx, cy, cz) * w;
-                  rs1 += fieldCell(P, H, G, Fp, 1, cx, cy, cz) * w;
-                  rs2 += fieldCell(P, H, G, Fp, 2, cx, cy, cz) * w;
-                  rs3 += fieldCell(P, H, G, Fp, 3, cx, cy, cz) * w;
-                }
-            r0 = rs0;
-            r1 = rs1;
-            r3 = rs3;
-            float cl = a2 + 0.5f * (o2 - rs2);
+            float cl = a2 + 0.5f * (o2 - rs[2]);
             lifetime = (cl < lmin || cl > lmax) ? a2 : cl;
-          } else {
-            r0 = fieldSample(P, H, G, Fp, 0, fx / P.h, fy / P.h, fz / P.h);
-            r1 = fieldSample(P, H, G, Fp, 1, fx / P.h, fy / P.h, fz / P.h);
-            r3 = fieldSample(P, H, G, Fp, 3, fx / P.h, fy / P.h, fz / P.h);
           }
           float c0 = a0 + 0.5f * (o0 - r0), c1 = a1 + 0.5f * (o1 - r1), c3 = a3 + 0.5f * (o3 - r3);
           tr[0] = (c0 < mn0 || c0 > mx0) ? a0 : c0;
@@ -509,7 +561,7 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
     if (expansion != 0.f) expands = true;
     // holdsContent and contentSupport (fluid-content.wgsl:22-39).
     if (fmaxf(fmaxf(value[0], value[2]), value[3]) > P.cutoff) {
-      if (!cvSampled) cv = velocityAt(P, H, G, V, px, py, pz);
+      if (!cvSampled) cv = centreVelocity(P, H, G, V, x, y, z);
       int idc[3] = {x, y, z};
       float vv[3] = {cv.x, cv.y, cv.z};
       bool low[3], high[3];
@@ -547,7 +599,7 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
   __syncthreads();
 }
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS, 3) k_evolve(FpBatch bt) {
+__global__ void __launch_bounds__(THREADS, FP_TRANSPORT_CTAS) k_evolve(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
@@ -656,7 +708,7 @@ FP_DEV float3 externalForces(const SimParams& P, int tile, float px, float py, f
 FP_DEV float3 cellForce(const SimParams& P, const Home& H, int tile, int x, int y, int z) {
   if (brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift) < 0) return make_float3(0.f, 0.f, 0.f);
   float wx = ((float)x + 0.5f) * P.h, wy = ((float)y + 0.5f) * P.h, wz = ((float)z + 0.5f) * P.h;
-  if (solidAt(P, H, wx, wy, wz)) return make_float3(0.f, 0.f, 0.f);
+  if (solidCell(P, H, x, y, z)) return make_float3(0.f, 0.f, 0.f);  // solidAt at the centre
   // The evolved scalars of this step (the reference swaps field and corrected first).
   const bool half = P.scalarHalf != 0;
   float heat = cellAt(P, H, P.fldN, 4, 1, x, y, z, half), density = cellAt(P, H, P.fldN, 4, 0, x, y, z, half);
@@ -733,18 +785,19 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
       out[a] = sourceVelocity(P, tile, v, face[0], face[1], face[2], a);
     }
     // enforceFaces (fluid-forces.wgsl:15-31)
-    if (solidAt(P, H, px, py, pz)) {
+    // solidAt at a cell centre is solidCell of that cell: centre / h + 0.25 floors to it.
+    if (solidCell(P, H, x, y, z)) {
       out[0] = out[1] = out[2] = 0.f;
     } else {
-      if (solidAt(P, H, px + P.h, py, pz)) out[0] = 0.f;
-      if (solidAt(P, H, px, py + P.h, pz)) out[1] = 0.f;
-      if (solidAt(P, H, px, py, pz + P.h)) out[2] = 0.f;
+      if (solidCell(P, H, x + 1, y, z)) out[0] = 0.f;
+      if (solidCell(P, H, x, y + 1, z)) out[1] = 0.f;
+      if (solidCell(P, H, x, y, z + 1)) out[2] = 0.f;
     }
     for (int a = 0; a < 3; a++) P.velF[(slot * 3 + a) * N + c] = out[a];
   }
   __syncthreads();
 }
-__global__ void __launch_bounds__(THREADS) k_forces(FpBatch bt) {
+__global__ void __launch_bounds__(THREADS, 4) k_forces(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
@@ -815,17 +868,15 @@ FP_DEV void brick_project(const SimParams* __restrict__ Pp, uint32_t i, int pSel
   for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
     int x, y, z;
     cellOf(P, H, c, x, y, z);
-    float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
     float res[3] = {0.f, 0.f, 0.f};
-    if (!solidAt(P, H, px, py, pz)) {
+    if (!solidCell(P, H, x, y, z)) {  // solidAt at the cell centre
       float cp = p[slot * N + c];
       bool pu = pressureUnknown(P, H, x, y, z);
       for (int a = 0; a < 3; a++) {
         int n[3] = {x, y, z};
         n[a] += 1;
         float v = P.velF[(slot * 3 + a) * N + c];
-        float nx = ((float)n[0] + 0.5f) * P.h, ny = ((float)n[1] + 0.5f) * P.h, nz = ((float)n[2] + 0.5f) * P.h;
-        if (solidAt(P, H, nx, ny, nz)) {
+        if (solidCell(P, H, n[0], n[1], n[2])) {
           res[a] = 0.f;
         } else if (!pu && !pressureUnknown(P, H, n[0], n[1], n[2])) {
           res[a] = 0.f;
@@ -909,7 +960,7 @@ __global__ void __launch_bounds__(THREADS) k_post_divergence(FpBatch bt) {
       int x, y, z;
       cellOf(P, H, c, x, y, z);
       auto solid = [&](int qx, int qy, int qz) {
-        return solidAt(P, H, ((float)qx + 0.5f) * P.h, ((float)qy + 0.5f) * P.h, ((float)qz + 0.5f) * P.h);
+        return solidCell(P, H, qx, qy, qz);  // solidAt at the cell centre
       };
       if (solid(x, y, z) || !pressureUnknown(P, H, x, y, z)) continue;
       bool interior = true;
