@@ -520,6 +520,7 @@ def run_ours(args, rank, world, local):
                                "sphere+box colliders; 8^3 bricks, 2.5 cm voxels; plain FP32 storage; "
                                "1 cold-started V-cycle (reference schedule)",
                    "mean_active_bricks": sum(actives) / len(actives), "grown_steps": step - 3 * args.steps,
+                   "live_tiles": int(st.tiles), "tile_capacity": int(st.tile_capacity),
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "working set > L2: pools of ~4k bricks x 97 KB"},
         "roofline": roofline,

@@ -67,17 +67,53 @@ def gpu_slots(gpu) -> int:
     return int(gpu.stats().pool_slots)
 
 
+# A MacCormack limiter test whose corrected value lies within FP32 rounding of the donors'
+# bound may go the other way in the FP64 oracle; that face then keeps the predicted instead of
+# the corrected value (or the reverse), which moves the face and the divergence of its two
+# cells by up to the correction. Like the activity flags, a few such isolated flips are
+# allowed per step: without the FLIP_CELLS(n) largest pointwise differences a field must be
+# within the tolerance, and with them within FLIP_BOUND times it.
+FLIP_BOUND = 10.0
+
+
+def flip_cells(bricks: int) -> int:
+    return 2 * max(2, bricks // 500)
+
+
+def trimmed_rel_l2(a: np.ndarray, b: np.ndarray, k: int) -> float:
+    """rel_l2 without the k largest pointwise differences (the denominator keeps them)."""
+    d = np.abs(a.astype(np.float64) - b).ravel()
+    if 0 < k < d.size:
+        d = np.partition(d, d.size - k)[: d.size - k]
+    den = float(np.linalg.norm(b.ravel()))
+    num = float(np.linalg.norm(d))
+    if den == 0.0:
+        return 0.0 if num == 0.0 else float("inf")
+    return num / den
+
+
 def compare_fields(gpu, orc, slots: np.ndarray) -> dict:
+    """Per field (scalars per channel): relative L2, and under name + "@trim" the same without
+    the flip_cells(len(slots)) largest pointwise differences."""
     out = {}
+    k = flip_cells(len(slots))
     for name, fid in CHECK_FIELDS.items():
         a = gpu.field(fid)[slots]
         b = orc.field(fid, f64=orc.real == 0)[slots]
         if fid == abi.FP_FIELD_SCALARS:
-            for k, ch in enumerate(("smoke", "heat", "lifetime", "fuel")):
-                out[ch] = rel_l2(a[:, k], b[:, k])
+            for c, ch in enumerate(("smoke", "heat", "lifetime", "fuel")):
+                out[ch] = rel_l2(a[:, c], b[:, c])
+                out[ch + "@trim"] = trimmed_rel_l2(a[:, c], b[:, c], k)
         else:
             out[name] = rel_l2(a, b)
+            out[name + "@trim"] = trimmed_rel_l2(a, b, k)
     return out
+
+
+def field_within(fields: dict, name: str, tol: float) -> bool:
+    """The acceptance rule above for one field of a compare_fields report."""
+    v = fields[name]
+    return v <= tol or (fields[name + "@trim"] <= tol and v <= FLIP_BOUND * tol)
 
 
 def force(gpu, orc):

@@ -21,7 +21,9 @@ def check(reports, tol=TOL, min_active=1):
     threshold tests (content above the cutoff, motion pads) that the CUDA step evaluates in
     FP32 and the oracle in FP64, so a value within rounding of a threshold may flip: at most
     one flag word per 500 computing bricks (and 2) may differ. The allocation consumes the
-    CUDA flags on both sides, so its tables stay bit-exact regardless."""
+    CUDA flags on both sides, so its tables stay bit-exact regardless. The limiter's tests
+    may flip the same way (parity.field_within): a field may exceed `tol` only through a few
+    isolated cells, and then by at most FLIP_BOUND times."""
     worst = {}
     for step, tables, fields, n in reports:
         for k, v in tables.items():
@@ -31,7 +33,11 @@ def check(reports, tol=TOL, min_active=1):
             assert v == 0, f"step {step}: table {k} differs in {v} words"
         for k, v in fields.items():
             worst[k] = max(worst.get(k, 0.0), v)
-            assert v <= tol, f"step {step}: {k} relative L2 {v:.3e} > {tol}"
+            if k.endswith("@trim"):
+                continue
+            assert parity.field_within(fields, k, tol), (
+                f"step {step}: {k} relative L2 {v:.3e} ({fields[k + '@trim']:.3e} without "
+                f"{parity.flip_cells(n)} flip cells) > {tol}")
     assert max(r[3] for r in reports) >= min_active
     return worst
 

@@ -19,6 +19,11 @@ INCLUDE = HERE.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-ccbin", "g++"]
+# The multigrid runs the same cell operations in several kernels (per brick, per tile, the
+# fused coarse cycle, chosen by a simulation's tile capacity). Without multiply-add
+# contraction each operation rounds the same in all of them, so the pressure of a simulation
+# does not depend on which kernels ran it.
+FILE_FLAGS = {"fp_mg.cu": ["-fmad=false"]}
 
 
 def _sources():
@@ -39,7 +44,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
         objects.append(obj)
         if obj.exists() and obj.stat().st_mtime > max(src.stat().st_mtime, newest_header) and not ptxas_info:
             continue
-        cmd = [NVCC, *ARCH, *FLAGS, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+        cmd = [NVCC, *ARCH, *FLAGS, *FILE_FLAGS.get(src.name, []), "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
         if ptxas_info and src.suffix == ".cu":
             cmd.insert(1, "-Xptxas=-v")
         if verbose:

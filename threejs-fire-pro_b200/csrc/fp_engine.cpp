@@ -189,7 +189,7 @@ int Engine::consume() {
 void Engine::freeAll() {
   DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_, &zeroList_,
                          &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_, &donors_, &solids_,
-                         &tileRecD_, &tileNbrD_, &hashD_, &solver_};
+                         &tileRecD_, &tileNbrD_, &hashD_, &solver_, &tileMask_};
   for (DeviceBuffer* b : all)
     if (b->ptr) {
       cudaFree(b->ptr);
@@ -253,7 +253,7 @@ uint64_t Engine::estimateBytes(const fp_grid& g, uint32_t tiles) {
     uint64_t c = (uint64_t)1 << (3 * (shift - l));
     perSlot += c * (3 * narrow + 1);
   }
-  uint64_t perTile = 64 * (4 * 5 + FP_RECORD_WORDS * 4 + 8) + 16 + 27 * 4 + 16 + (64 + 8 + 1) * (3 * narrow + 1);
+  uint64_t perTile = 64 * (4 * 5 + FP_RECORD_WORDS * 4 + 8) + 16 + 27 * 4 + 16 + 8 + (64 + 8 + 1) * (3 * narrow + 1);
   return slots * perSlot + (uint64_t)std::max(tiles, (uint32_t)MIN_TILES) * perTile + 64 * 1024;
 }
 
@@ -353,7 +353,8 @@ int Engine::setCapacity(int capacity) {
   size_t oldBricks = (size_t)capacity_ * 64;
   bool ok = grow(pages_, bricks * 4, 0xff) && grow(entries_, bricks * 4, 0xff) && grow(state_, bricks * 4, 0) &&
             grow(records_, bricks * FP_RECORD_WORDS * 4, 0xff) && alloc(active_, bricks * 4) &&
-            alloc(zeroList_, bricks * 8) && alloc(blockCounts_, (bricks / 256 + 1) * 16);
+            alloc(zeroList_, bricks * 8) && alloc(blockCounts_, (bricks / 256 + 1) * 16) &&
+            alloc(tileMask_, (size_t)capacity * 8);
   if (!ok) return FP_ENOMEM;
   // activity: bricks, then a word per tile slot.
   {
@@ -766,6 +767,7 @@ void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t
   P.capacity = capacity_;
   P.tileRec = (const int4*)tileRecD_.ptr;
   P.tileNbr = (const int*)tileNbrD_.ptr;
+  P.tileMask = (uint64_t*)tileMask_.ptr;
   P.hash = (const int4*)hashD_.ptr;
   P.hashMask = (uint32_t)hash_.size() - 1;
   P.pages = (int*)pages_.ptr;
@@ -889,7 +891,7 @@ uint64_t Engine::memoryBytes() const {
   uint64_t bytes = 0;
   const DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_,
                                &zeroList_, &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_,
-                               &donors_, &solids_, &tileRecD_, &tileNbrD_, &hashD_, &solver_};
+                               &donors_, &solids_, &tileRecD_, &tileNbrD_, &hashD_, &solver_, &tileMask_};
   for (const DeviceBuffer* b : all) bytes += b->bytes;
   for (auto& b : vel_) bytes += b.bytes;
   for (auto& b : fld_) bytes += b.bytes;

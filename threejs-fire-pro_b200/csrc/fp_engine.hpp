@@ -160,7 +160,7 @@ class Engine {
   DeviceBuffer freeStack_, counters_;
   DeviceBuffer vel_[4], curl_, fld_[3], expn_, div_, vmin_, vmax_, sb_, donors_, solids_;
   DeviceBuffer p0_[2], topo_[FP_MAX_LEVELS], lp_[FP_MAX_LEVELS][2], lrhs_[FP_MAX_LEVELS];
-  DeviceBuffer tileRecD_, tileNbrD_, hashD_, solver_;
+  DeviceBuffer tileRecD_, tileNbrD_, hashD_, solver_, tileMask_;
   int velIdx_[4] = {0, 1, 2, 3};  // start, predictor/projected, corrected, forced
   int fldIdx_[3] = {0, 1, 2};     // start, predictor, evolved
 
@@ -291,7 +291,8 @@ class Stepper {
   FpBatch batch() const;
   void enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl, int vcycles, bool measure, int& latest,
                uint64_t& launches);
-  int cycle_ = 0;  // the V-cycle being enqueued
+  int cycle_ = 0;             // the V-cycle being enqueued
+  bool fusedCoarse_ = false;  // the V-cycle below the first tile level runs as k_coarse
   void vcycle(int level, int cur[], uint64_t& launches);
   int check(cudaError_t e, const char* what);
   int reserve(size_t arenaBytes, int sims, size_t readWords);

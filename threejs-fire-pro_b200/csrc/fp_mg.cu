@@ -24,26 +24,36 @@ FP_DEV long cellAddress(const SimParams& P, const Home& H, int px, int py, int p
     if (slot < 0) return -1;
     owner = slot;
   } else {
-    int t = tileAt(P, H, px >> s, py >> s, pz >> s);
+    // Multigrid homes are live tiles, and a live tile is its own centre neighbour.
+    int tx = px >> s, ty = py >> s, tz = pz >> s;
+    int t = (tx == H.tx && ty == H.ty && tz == H.tz && H.tile >= 0) ? H.tile : tileAt(P, H, tx, ty, tz);
     if (t < 0) return -1;
     owner = t;
   }
   return owner * side * side * side + ((pz & m) * side + (py & m)) * side + (px & m);
 }
 
+// Whether cell (px,py,pz) of tile level `level` is a pressure unknown: every brick it covers
+// computes, from the tile's mask of computing bricks (k_tile_masks, this step).
+FP_DEV bool tileCellActive(const SimParams& P, const Home& H, int px, int py, int pz, int level) {
+  int s = levelShift(P, level), side = 1 << s;
+  int tx = px >> s, ty = py >> s, tz = pz >> s;
+  int t = (tx == H.tx && ty == H.ty && tz == H.tz && H.tile >= 0) ? H.tile : tileAt(P, H, tx, ty, tz);
+  if (t < 0) return false;
+  uint64_t m = P.tileMask[t];
+  int lx = px & (side - 1), ly = py & (side - 1), lz = pz & (side - 1);
+  if (side == 4) return (m >> ((lz * 4 + ly) * 4 + lx)) & 1ull;  // a cell per brick
+  if (side == 2) {                                                   // 2^3 bricks a cell
+    uint64_t c = 0x0000000000330033ull << (2 * lx + 8 * ly + 32 * lz);
+    return (m & c) == c;
+  }
+  return m == ~0ull;  // the whole tile
+}
+
 // activeCell (pressure.wgsl:100-136): whether a level's cell is a pressure unknown.
 FP_DEV bool activeCell(const SimParams& P, const Home& H, int px, int py, int pz, int level) {
   int bl = P.brickLevels;
-  if (level >= bl) {
-    int n = 1 << (level - bl);
-    for (int z = 0; z < n; z++)
-      for (int y = 0; y < n; y++)
-        for (int x = 0; x < n; x++) {
-          int id = brickIdAt(P, H, px * n + x, py * n + y, pz * n + z);
-          if (id < 0 || P.entries[id] < 0 || P.records[(size_t)id * FP_RECORD_WORDS + 27] == 0) return false;
-        }
-    return true;
-  }
+  if (level >= bl) return tileCellActive(P, H, px, py, pz, level);  // every covered brick computes
   int span = 1 << level;
   int lx = (px * span - 1) >> bl, ly = (py * span - 1) >> bl, lz = (pz * span - 1) >> bl;
   int hx = (px * span + span - 1) >> bl, hy = (py * span + span - 1) >> bl, hz = (pz * span + span - 1) >> bl;
@@ -180,6 +190,7 @@ FP_DEV void restrictCell(const SimParams& P, const Home& H, const Args& A, long 
   int fine = A.level - 1;
   float residual = 0.f;
   bool every = true;
+#pragma unroll
   for (int k = 0; k < 8; k++) {
     int px = cx * 2 + (k & 1), py = cy * 2 + ((k >> 1) & 1), pz = cz * 2 + (k >> 2);
     bool unknown = activeCell(P, H, px, py, pz, fine);
@@ -210,25 +221,42 @@ FP_DEV void levelCell(const SimParams& P, const Home& H, const Args& A, long a, 
   if (OP == RESTRICT) restrictCell(P, H, A, a, px, py, pz);
 }
 
-// Staged brick levels. A CTA copies, for its brick, the values of the level it reads plus a
-// one-cell rim into shared memory, and once per brick whether each negative-octant neighbour
-// brick computes; the cell operations then read no directory. Same arithmetic, same order as
+// Staged brick levels. A CTA copies, for its bricks, the values of the level it reads plus a
+// rim into shared memory, and once per brick whether each negative-octant neighbour brick
+// computes; the cell operations then read no directory. Same arithmetic, same order as
 // relaxCell / restrictCell / prolongCell above.
 //   RELAX     stage A.pin at A.level;           write A.pout at A.level
 //   RESTRICT  stage A.pin at A.level - 1 (fine); write A.pout, A.cfirst at A.level (coarse)
 //   PROLONG   stage A.coarse at A.level + 1;    write A.pout at A.level
-template <int OP, int GROUP>
+// SB, the staged level's cells per brick side, fixes every shape at compile time; SB = 1 is
+// the first tile level (one cell per brick), which prolongation stages through the tiles.
+template <int OP, int SB>
+struct Staged {
+  static constexpr int R = OP == PROLONG ? 2 : 1;  // rim: prolongation's Neumann ghosts reach two
+  static constexpr int S = SB + 2 * R, S2 = S * S, S3 = S2 * S;
+  static constexpr int FS = OP == PROLONG ? 2 * SB : SB;  // the fine level's side
+  static constexpr int OS = OP == RESTRICT ? SB / 2 : FS;  // the output level's side
+  static constexpr int OUT = OS * OS * OS;
+  static constexpr int GROUP = OUT >= 256 ? 256 : (OUT >= 64 ? 64 : 32);  // threads per brick
+  static constexpr int NG = 256 / GROUP;                                  // bricks per CTA
+  static constexpr int WORDS = S3 + (OP == PROLONG ? (S3 + 3) / 4 : 0);   // values + solid bytes
+  static constexpr size_t SMEM = (size_t)NG * WORDS * sizeof(float);
+};
+constexpr int log2c(int v) { return v <= 1 ? 0 : 1 + log2c(v / 2); }
+
+template <int OP, int SB>
 __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel Sl) {
-  // GROUP threads per brick, 256 / GROUP bricks per CTA: the coarse brick levels hold 64 or 8
-  // cells a brick, so several bricks share a CTA. Each group has its own neighbour slots,
-  // flags and stage; the CTA's barriers are uniform (groups without a brick skip the work).
-  constexpr int NG = 256 / GROUP;
+  using K = Staged<OP, SB>;
+  constexpr int S = K::S, S2 = K::S2, S3 = K::S3, R = K::R, GROUP = K::GROUP, NG = K::NG;
+  constexpr int FS = K::FS, fs = log2c(FS), FCELLS = FS * FS * FS;
   __shared__ int nslotAll[NG][27];
   __shared__ int needAll[NG][8];  // bit k of the index: -1 on axis k
   extern __shared__ float stAll[];
   const int g = threadIdx.x / GROUP, t = threadIdx.x % GROUP;
   int* nslot = nslotAll[g];
   int* need = needAll[g];
+  float* st = stAll + g * K::WORDS;
+  uint8_t* solidSt = reinterpret_cast<uint8_t*>(st + S3);
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t base = blockIdx.x * NG; base < total; base += gridDim.x * NG) {
     uint32_t item = base + g;
@@ -236,24 +264,15 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item < total ? item : base, i);
     const Args A = resolve(P, Sl);
     const bool has = item < total && !A.skip;
-    const int bl = P.brickLevels;
     const int fineLevel = OP == RESTRICT ? A.level - 1 : A.level;
     const int stageLevel = OP == PROLONG ? A.level + 1 : fineLevel;
-    const int sb = stageLevel < bl ? 1 << levelShift(P, stageLevel) : 1;  // stage-level cells per brick side
-    // Prolongation stages a two-cell rim and the coarse solid flags: its Neumann ghosts read the
-    // neighbours of the interpolation's coarse cells.
-    const int R = OP == PROLONG ? 2 : 1;
-    const int S = sb + 2 * R, S2 = S * S, S3 = S2 * S;
-    float* st = stAll + g * (S3 + (S3 + 3) / 4);
-    uint8_t* solidSt = reinterpret_cast<uint8_t*>(st + S3);
     const float* src = OP == PROLONG ? A.coarse : A.pin;
     const bool srcN = OP == PROLONG ? A.coarseN : A.pinN;
-    const int fs = levelShift(P, fineLevel), fside = 1 << fs, fcells = fside * fside * fside;
     const uint32_t id = has ? P.active[i] : 0u;
     Home H = homeOf(P, id, nslot);
     if (has && t < 27) nslot[t] = entryPage(P.records[(size_t)id * FP_RECORD_WORDS + t]);
     __syncthreads();
-    int ox = H.bx * sb - R, oy = H.by * sb - R, oz = H.bz * sb - R;
+    const int ox = H.bx * SB - R, oy = H.by * SB - R, oz = H.bz * SB - R;
     if (has) {
       if (t < 8) {
         int dx = -(t & 1), dy = -((t >> 1) & 1), dz = -(t >> 2);
@@ -261,14 +280,36 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
         need[t] = below || nslot[nbrIndex(dx, dy, dz)] >= 0;
       }
       for (int q = t; q < S3; q += GROUP) {
-        int lx = q % S, ly = (q / S) % S, lz = q / S2;
-        long a = cellAddress(P, H, ox + lx, oy + ly, oz + lz, stageLevel);
+        const int lx = q % S, ly = (q / S) % S, lz = q / S2;
+        long a;
+        if (SB > 1) {
+          // Brick levels: the neighbour brick from the record, the cell within it.
+          const int dx = lx < R ? -1 : (lx >= R + SB ? 1 : 0), dy = ly < R ? -1 : (ly >= R + SB ? 1 : 0),
+                    dz = lz < R ? -1 : (lz >= R + SB ? 1 : 0);
+          const int s = nslot[nbrIndex(dx, dy, dz)];
+          const int cx = (lx - R) & (SB - 1), cy = (ly - R) & (SB - 1), cz = (lz - R) & (SB - 1);
+          a = s < 0 ? -1 : (long)s * (SB * SB * SB) + (cz * SB + cy) * SB + cx;
+        } else {
+          a = cellAddress(P, H, ox + lx, oy + ly, oz + lz, stageLevel);
+        }
         st[q] = a < 0 ? 0.f : ldBf(src, a, srcN);
         if (OP == PROLONG) solidSt[q] = a >= 0 && (P.topo[stageLevel][a] & FP_STORED_SOLID) ? 1 : 0;
       }
     }
     __syncthreads();
     if (has) {
+      // The negative-octant neighbours that compute, as bits; a fine cell on the brick's low
+      // faces is an unknown when every neighbour its faces touch computes (activeCell).
+      uint32_t needBits = 0;
+#pragma unroll
+      for (int k = 0; k < 8; k++) needBits |= need[k] ? 1u << k : 0u;
+      auto unknown = [&](int lx, int ly, int lz) {
+        uint32_t sub = 1u;  // the octants k whose set axes are all on a low face here
+        if (lx == 0) sub |= sub << 1;
+        if (ly == 0) sub |= sub << 2;
+        if (lz == 0) sub |= sub << 4;
+        return (~needBits & sub) == 0u;
+      };
       // coarseValue (pressure.wgsl:670-696) from the stage.
       auto ghost = [&](int cx, int cy, int cz) {
         int groundY = P.ground ? 0 : -0x7fffffff;
@@ -290,17 +331,7 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
           }
         return sum / fmaxf(count, 1.f);
       };
-      long slot = nslot[13];
-      // Whether the fine-level cell at local (lx,ly,lz) of this brick is a pressure unknown.
-      auto unknown = [&](int lx, int ly, int lz) {
-        for (int k = 1; k < 8; k++) {
-          if ((k & 1) && lx != 0) continue;
-          if ((k & 2) && ly != 0) continue;
-          if ((k & 4) && lz != 0) continue;
-          if (!need[k]) return false;
-        }
-        return (bool)need[0];
-      };
+      const long slot = nslot[13];
       // Stencil sum of the open sides of a fine cell, from the stage (RELAX, RESTRICT).
       auto sumAt = [&](int lx, int ly, int lz, uint32_t f) {
         int c = ((lz + 1) * S + (ly + 1)) * S + (lx + 1);
@@ -310,9 +341,9 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
         return (v0 + v1) + (v2 + v3) + (v4 + v5);
       };
       if (OP == RELAX || OP == PROLONG) {
-        for (int o = t; o < fcells; o += GROUP) {
-          int lx = o & (fside - 1), ly = (o >> fs) & (fside - 1), lz = o >> (2 * fs);
-          long a = slot * fcells + o;
+        for (int o = t; o < FCELLS; o += GROUP) {
+          const int lx = o & (FS - 1), ly = (o >> fs) & (FS - 1), lz = o >> (2 * fs);
+          const long a = slot * FCELLS + o;
           uint32_t f = expandFlags(P.topo[fineLevel][a]);
           if ((f & SOLIDF) || !unknown(lx, ly, lz)) {
             stBf(A.pout, a, 0.f, A.poutN);
@@ -323,18 +354,22 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
             float cand = (sumAt(lx, ly, lz, f) - ldBf(A.rhs, a, A.rhsN)) / fmaxf(diagOf(f), 1e-12f);
             stBf(A.pout, a, mixf(center, cand, 0.8f), A.poutN);
           } else {
-            int px = H.bx * fside + lx, py = H.by * fside + ly, pz = H.bz * fside + lz;
+            int px = H.bx * FS + lx, py = H.by * FS + ly, pz = H.bz * FS + lz;
             float qx = ((float)px + 0.5f) * 0.5f - 0.5f, qy = ((float)py + 0.5f) * 0.5f - 0.5f,
                   qz = ((float)pz + 0.5f) * 0.5f - 0.5f;
             int ix = (int)floorf(qx), iy = (int)floorf(qy), iz = (int)floorf(qz);
             float fx = qx - floorf(qx), fy = qy - floorf(qy), fz = qz - floorf(qz);
             bool fast = P.colliderCount == 0 && (!P.ground || iy >= 0);
+            // Below the ground the mirrored ghosts read the row above it, which a brick under
+            // y = 0 does not stage: those read through the directory.
+            bool staged = !(P.ground && H.by < 0);
             float v[8];
-  #pragma unroll
+#pragma unroll
             for (int k = 0; k < 8; k++) {
               int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
-              v[k] = fast ? st[((iz + dz - oz) * S + (iy + dy - oy)) * S + (ix + dx - ox)]
-                          : ghost(ix + dx, iy + dy, iz + dz);
+              v[k] = fast     ? st[((iz + dz - oz) * S + (iy + dy - oy)) * S + (ix + dx - ox)]
+                     : staged ? ghost(ix + dx, iy + dy, iz + dz)
+                              : coarseValue(P, H, A.coarse, A.level + 1, ix + dx, iy + dy, iz + dz);
             }
             float corr = mixf(mixf(mixf(v[0], v[1], fx), mixf(v[2], v[3], fx), fy),
                               mixf(mixf(v[4], v[5], fx), mixf(v[6], v[7], fx), fy), fz);
@@ -342,17 +377,18 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
           }
         }
       } else {  // RESTRICT: coarse cells of this brick at A.level
-        int cs = fs - 1, cside = fside >> 1, ccells = cside * cside * cside;
+        constexpr int cside = FS / 2, cs = fs - 1, ccells = cside * cside * cside;
         for (int o = t; o < ccells; o += GROUP) {
-          int cx = o & (cside - 1), cy = (o >> cs) & (cside - 1), cz = o >> (2 * cs);
+          const int cx = o & (cside - 1), cy = (o >> cs) & (cside - 1), cz = o >> (2 * cs);
           float residual = 0.f;
           bool every = true;
+#pragma unroll
           for (int k = 0; k < 8; k++) {
             int lx = cx * 2 + (k & 1), ly = cy * 2 + ((k >> 1) & 1), lz = cz * 2 + (k >> 2);
             bool u = unknown(lx, ly, lz);
             every = every && u;
             if (u) {
-              long a = slot * fcells + (((lz << fs) | ly) << fs | lx);
+              long a = slot * FCELLS + (((lz << fs) | ly) << fs | lx);
               uint32_t f = expandFlags(P.topo[fineLevel][a]);
               if (!(f & SOLIDF)) {
                 float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
@@ -376,8 +412,6 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
   }
 }
 
-// Threads per brick of the staged kernels for a level of `cells` cells per brick.
-static int groupFor(int cells) { return cells >= 256 ? 256 : (cells >= 64 ? 64 : 32); }
 
 FP_DEV Home enterTile(const SimParams& P, int t, int4 rec) {
   Home H;
@@ -390,32 +424,33 @@ FP_DEV Home enterTile(const SimParams& P, int t, int4 rec) {
   return H;
 }
 
-// Every cell of `A.level` (a tile level) in every tile.
-template <int OP>
+// Every cell of `A.level` (a tile level of CELLS cells a tile) in every tile: a thread per
+// cell, 64 / CELLS tiles per CTA; no barriers, so threads of dead tiles just move on.
+template <int OP, int CELLS>
 __global__ void __launch_bounds__(64) k_level_tiles(FpBatch bt, MgSel Sl) {
+  constexpr int NT = 64 / CELLS, s = CELLS == 64 ? 2 : (CELLS == 8 ? 1 : 0), side = 1 << s;
+  const int g = threadIdx.x / CELLS, o = threadIdx.x % CELLS;
   uint32_t total = workTotal(bt, FP_WORK_TILES);
-  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+  for (uint32_t item = blockIdx.x * NT + g; item < total; item += gridDim.x * NT) {
     uint32_t local;
     const SimParams& P = workSim(bt, FP_WORK_TILES, item, local);
     const int t = (int)local;
     const Args A = resolve(P, Sl);
-    if (A.skip) continue;  // the same for the whole CTA
-    int s = levelShift(P, A.level), side = 1 << s, cells = side * side * side;
+    if (A.skip) continue;
     int4 rec = __ldg(&P.tileRec[t]);
     if (rec.w == 0) continue;
     Home H = enterTile(P, t, rec);
-    for (int o = threadIdx.x; o < cells; o += blockDim.x) {
-      int lx = o & (side - 1), ly = (o >> s) & (side - 1), lz = o >> (2 * s);
-      levelCell<OP>(P, H, A, (long)t * cells + o, rec.x * side + lx, rec.y * side + ly, rec.z * side + lz);
-    }
+    int lx = o & (side - 1), ly = (o >> s) & (side - 1), lz = o >> (2 * s);
+    levelCell<OP>(P, H, A, (long)t * CELLS + o, rec.x * side + lx, rec.y * side + ly, rec.z * side + lz);
   }
 }
 
 // relaxCoarse (pressure.wgsl:549-599): the bottom level, one cell per tile slot, every
-// iteration in one CTA; a CTA per simulation. Tile slots stride over the threads; each
-// slot's flags (SOLIDF where it is no unknown) and a ping-pong pair of values live in shared
-// memory when 12 bytes a slot fit `smemBytes`, else the values ping-pong between the level's
-// two pressure buffers in global memory (same arithmetic, same order).
+// iteration in one CTA; a CTA per simulation. Tile slots stride over the threads. When 28
+// bytes a slot fit `smemBytes`, each slot's flags (SOLIDF where it is no unknown), right-hand
+// side, face neighbours and a ping-pong pair of values live in shared memory; else the values
+// ping-pong between the level's two pressure buffers in global memory (same arithmetic, same
+// order).
 __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int iterations, int smemBytes) {
   extern __shared__ float bottomSmem[];
   const int nbIndex[6] = {nbrIndex(1, 0, 0), nbrIndex(-1, 0, 0), nbrIndex(0, 1, 0),
@@ -427,13 +462,15 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
     if (A.skip) continue;  // the same for the whole CTA
     const int level = A.level;
     int cap = P.capacity;
-    bool inShared = (long)cap * 12 <= (long)smemBytes;
+    bool inShared = (long)cap * 28 <= (long)smemBytes;
     // In global memory: cur starts in pout (a copy of pin), nxt is pin's buffer; both hold the
     // level's storage type (gN). Shared memory holds FP32.
     float* cur = inShared ? bottomSmem : A.pout;
     float* nxt = inShared ? bottomSmem + cap : const_cast<float*>(A.pin);
     const bool gN = !inShared && A.poutN;
-    uint32_t* flags = inShared ? reinterpret_cast<uint32_t*>(bottomSmem + 2 * cap) : nullptr;
+    float* rhsSm = bottomSmem + 2 * cap;
+    uint32_t* flags = inShared ? reinterpret_cast<uint32_t*>(bottomSmem + 3 * cap) : nullptr;
+    int16_t* nbSm = reinterpret_cast<int16_t*>(bottomSmem + 4 * cap);  // 6 a slot
     auto flagOf = [&](int t) -> uint32_t {
       int4 rec = __ldg(&P.tileRec[t]);
       uint32_t f = SOLIDF | (rec.w != 0 ? 0x80000000u : 0u);  // top bit: a live tile slot
@@ -446,7 +483,12 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
     for (int t = threadIdx.x; t < cap; t += blockDim.x) {
       uint32_t f = flagOf(t);
       // Cells that are no unknown are never read and become zero in the first iteration.
-      if (inShared) flags[t] = f;
+      if (inShared) {
+        flags[t] = f;
+        rhsSm[t] = ldBf(A.rhs, t, A.rhsN);
+        for (int k = 0; k < 6; k++)
+          nbSm[t * 6 + k] = (int16_t)(((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1);
+      }
       // pin and pout are the level's two buffers: the copy into pout reads no value it wrote.
       stBf(cur, t, (f & 0x80000000u) && !(f & SOLIDF) ? ldBf(A.pin, t, A.pinN) : 0.f, gN);
     }
@@ -459,11 +501,13 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
           float w[6];
 #pragma unroll
           for (int k = 0; k < 6; k++) {
-            int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
+            int n = inShared ? (int)nbSm[t * 6 + k]
+                             : (((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1);
             w[k] = n >= 0 ? ldBf(cur, n, gN) : 0.f;
           }
           float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
-          float cand = (sum - ldBf(A.rhs, t, A.rhsN)) / fmaxf(diagOf(f & 63u), 1e-12f);
+          float rhs = inShared ? rhsSm[t] : ldBf(A.rhs, t, A.rhsN);
+          float cand = (sum - rhs) / fmaxf(diagOf(f & 63u), 1e-12f);
           next = mixf(ldBf(cur, t, gN), cand, 0.8f);
         }
         stBf(nxt, t, next, gN);
@@ -477,6 +521,187 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
       uint32_t f = inShared ? flags[t] : flagOf(t);
       if ((f & 0x80000000u) && cur != A.pout) stBf(A.pout, t, ldBf(cur, t, gN), A.poutN);
     }
+    __syncthreads();
+  }
+}
+
+// A value as the storage of a level rounds it.
+FP_DEV float bfRound(float v, bool narrow) { return narrow ? __bfloat162float(__float2bfloat16_rn(v)) : v; }
+
+// The second tile level (2^3 cells a tile) and the bottom (one cell a tile) in one CTA per
+// simulation: the V-cycle from level bl + 1 down (two relaxations, restriction to the bottom,
+// the bottom's iterations, prolongation, three relaxations), with both levels' iterates,
+// right-hand sides and flags in shared memory by tile slot, __syncthreads between sweeps.
+// The arithmetic and its order are those of k_level_tiles (relaxCell, restrictCell,
+// prolongCell) and k_bottom; every value a level stores is rounded as its storage rounds it.
+//   A.level: level bl + 1; A.rhs its right-hand side; A.pin its first iterate; A.pout where
+//   its result goes; A.cfirst: the bottom's result (read back by the prolongation).
+constexpr int COARSE_SLOT_BYTES = 8 * 3 * 4 + 8 + 3 * 4 + 4;  // per tile slot
+constexpr int COARSE_SMEM = 224 * 1024;
+constexpr uint32_t LIVE = 0x80000000u;
+constexpr uint8_t UNKNOWN = 0x80;  // level bl + 1 flag byte: activeCell; bit 6 solid; 0-5 open
+
+// The level bl + 1 cell next to cell o of tile t on side k (+x, -x, +y, -y, +z, -z), as an
+// index of the level's tile-slot arrays; -1 without a tile there.
+FP_DEV int coarseNbr(const SimParams& P, int t, int o, int k) {
+  int l[3] = {o & 1, (o >> 1) & 1, o >> 2}, d[3] = {0, 0, 0};
+  const int ax = k >> 1, step = (k & 1) ? -1 : 1;
+  int v = l[ax] + step;
+  if (v < 0 || v > 1) d[ax] = step;
+  l[ax] = v & 1;
+  int nt = d[ax] == 0 ? t : __ldg(&P.tileNbr[t * 27 + nbrIndex(d[0], d[1], d[2])]);
+  return nt < 0 ? -1 : nt * 8 + ((l[2] * 2 + l[1]) * 2 + l[0]);
+}
+
+__global__ void __launch_bounds__(1024) k_coarse(FpBatch bt, MgSel Sl, int iterations) {
+  extern __shared__ float coarseSmem[];
+  const int nbIndex[6] = {nbrIndex(1, 0, 0), nbrIndex(-1, 0, 0), nbrIndex(0, 1, 0),
+                          nbrIndex(0, -1, 0), nbrIndex(0, 0, 1), nbrIndex(0, 0, -1)};
+  const int sims = batchCount(bt);
+  for (int sim = blockIdx.x; sim < sims; sim += gridDim.x) {
+    const SimParams& P = bt.sims[sim];
+    const Args A = resolve(P, Sl);
+    if (A.skip) continue;  // the same for the whole CTA
+    const int L = A.level, BL = L + 1, cap = P.capacity, n4 = cap * 8;
+    if ((long)cap * COARSE_SLOT_BYTES > COARSE_SMEM) continue;  // the host sizes batches to fit
+    const bool nL = narrowLevel(P, L), nB = narrowLevel(P, BL);
+    float* pa = coarseSmem;  // level L: iterates, right-hand side
+    float* pb = pa + n4;
+    float* rh = pb + n4;
+    float* ca = rh + n4;  // bottom: iterates, right-hand side
+    float* cb = ca + cap;
+    float* cr = cb + cap;
+    uint32_t* fb = reinterpret_cast<uint32_t*>(cr + cap);
+    uint8_t* fl = reinterpret_cast<uint8_t*>(fb + cap);
+    for (int c = threadIdx.x; c < n4; c += blockDim.x) {
+      const int t = c >> 3, o = c & 7;
+      int4 rec = __ldg(&P.tileRec[t]);
+      uint8_t f = 0;
+      float p = 0.f, r = 0.f;
+      if (rec.w != 0) {
+        Home H = enterTile(P, t, rec);
+        int px = rec.x * 2 + (o & 1), py = rec.y * 2 + ((o >> 1) & 1), pz = rec.z * 2 + (o >> 2);
+        f = (uint8_t)(P.topo[L][c] | (activeCell(P, H, px, py, pz, L) ? UNKNOWN : 0));
+        p = ldBf(A.pin, c, nL);
+        r = ldBf(A.rhs, c, nL);
+      }
+      fl[c] = f;
+      pa[c] = p;
+      rh[c] = r;
+    }
+    __syncthreads();
+    // stencil (pressure.wgsl:360-402) of level L from `src`.
+    auto sumL = [&](const float* src, int t, int o, uint32_t f) {
+      float w[6];
+#pragma unroll
+      for (int k = 0; k < 6; k++) {
+        int n = ((f >> k) & 1u) ? coarseNbr(P, t, o, k) : -1;
+        w[k] = n >= 0 ? src[n] : 0.f;
+      }
+      return (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
+    };
+    // relaxCell at level L, src -> dst.
+    auto relax = [&](const float* src, float* dst) {
+      for (int c = threadIdx.x; c < n4; c += blockDim.x) {
+        const uint8_t f = fl[c];
+        float v = 0.f;
+        if ((f & UNKNOWN) && !(f & FP_STORED_SOLID)) {
+          float cand = (sumL(src, c >> 3, c & 7, f & 63u) - rh[c]) / fmaxf(diagOf(f & 63u), 1e-12f);
+          v = bfRound(mixf(src[c], cand, 0.8f), nL);
+        }
+        dst[c] = v;
+      }
+      __syncthreads();
+    };
+    relax(pa, pb);
+    relax(pb, pa);
+    // restrictCell into the bottom (one cell a tile), its first iterate and k_bottom's flags.
+    for (int t = threadIdx.x; t < cap; t += blockDim.x) {
+      int4 rec = __ldg(&P.tileRec[t]);
+      float r = 0.f, first = 0.f;
+      uint32_t f = SOLIDF;
+      if (rec.w != 0) {
+        float residual = 0.f;
+        bool every = true;
+        for (int k = 0; k < 8; k++) {
+          const int c = t * 8 + k;
+          const uint8_t fk = fl[c];
+          every = every && (fk & UNKNOWN);
+          if ((fk & UNKNOWN) && !(fk & FP_STORED_SOLID))
+            residual += rh[c] - (sumL(pa, t, k, fk & 63u) - diagOf(fk & 63u) * pa[c]);
+        }
+        r = residual * 0.5f;
+        const uint8_t tb = P.topo[BL][t];
+        if (every && !(tb & FP_STORED_SOLID)) first = mixf(0.f, (0.f - r) / fmaxf(diagOf(tb & 63u), 1e-12f), 0.8f);
+        // activeCell at the bottom covers the tile's 64 bricks: every cell above is an unknown.
+        f = (every ? expandFlags(tb) : SOLIDF) | LIVE;
+      }
+      cr[t] = bfRound(r, nB);
+      ca[t] = (f & LIVE) && !(f & SOLIDF) ? bfRound(first, nB) : 0.f;
+      fb[t] = f;
+    }
+    __syncthreads();
+    // relaxCoarse (pressure.wgsl:549-599): FP32 iterates in shared memory.
+    float* cur = ca;
+    float* nxt = cb;
+    for (int it = 0; it < iterations; it++) {
+      for (int t = threadIdx.x; t < cap; t += blockDim.x) {
+        const uint32_t f = fb[t];
+        float next = 0.f;
+        if ((f & LIVE) && !(f & SOLIDF)) {
+          float w[6];
+#pragma unroll
+          for (int k = 0; k < 6; k++) {
+            int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
+            w[k] = n >= 0 ? cur[n] : 0.f;
+          }
+          float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
+          float cand = (sum - cr[t]) / fmaxf(diagOf(f & 63u), 1e-12f);
+          next = mixf(cur[t], cand, 0.8f);
+        }
+        nxt[t] = next;
+      }
+      __syncthreads();
+      float* tmp = cur;
+      cur = nxt;
+      nxt = tmp;
+    }
+    for (int t = threadIdx.x; t < cap; t += blockDim.x)
+      if (fb[t] & LIVE) stBf(A.cfirst, t, cur[t], nB);
+    __syncthreads();
+    // prolongCell at level L from the bottom's stored result, pa -> pb.
+    for (int c = threadIdx.x; c < n4; c += blockDim.x) {
+      const int t = c >> 3, o = c & 7;
+      const uint8_t f = fl[c];
+      float out = 0.f;
+      if ((f & UNKNOWN) && !(f & FP_STORED_SOLID)) {
+        int4 rec = __ldg(&P.tileRec[t]);
+        Home H = enterTile(P, t, rec);
+        int px = rec.x * 2 + (o & 1), py = rec.y * 2 + ((o >> 1) & 1), pz = rec.z * 2 + (o >> 2);
+        float qx = ((float)px + 0.5f) * 0.5f - 0.5f, qy = ((float)py + 0.5f) * 0.5f - 0.5f,
+              qz = ((float)pz + 0.5f) * 0.5f - 0.5f;
+        int ix = (int)floorf(qx), iy = (int)floorf(qy), iz = (int)floorf(qz);
+        float fx = qx - floorf(qx), fy = qy - floorf(qy), fz = qz - floorf(qz);
+        bool fast = P.colliderCount == 0 && (!P.ground || iy >= 0);
+        float v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
+          v[k] = fast ? readAt(P, H, A.cfirst, ix + dx, iy + dy, iz + dz, BL)
+                      : coarseValue(P, H, A.cfirst, BL, ix + dx, iy + dy, iz + dz);
+        }
+        float corr = mixf(mixf(mixf(v[0], v[1], fx), mixf(v[2], v[3], fx), fy),
+                          mixf(mixf(v[4], v[5], fx), mixf(v[6], v[7], fx), fy), fz);
+        out = bfRound(pa[c] + corr, nL);
+      }
+      pb[c] = out;
+    }
+    __syncthreads();
+    relax(pb, pa);
+    relax(pa, pb);
+    relax(pb, pa);
+    for (int c = threadIdx.x; c < n4; c += blockDim.x)
+      if (__ldg(&P.tileRec[c >> 3]).w != 0) stBf(A.pout, c, pa[c], nL);
     __syncthreads();
   }
 }
@@ -538,10 +763,10 @@ __global__ void k_converge(FpBatch bt, int cycle) {
 
 // cellTopology (pressure.wgsl:208-222): solid, or the sides whose neighbours are not solid.
 FP_DEV uint8_t cellTopology(const SimParams& P, const Home& H, int px, int py, int pz, int level) {
-  float s = P.h * (float)(1 << level);
-  auto blocked = [&](int x, int y, int z) {
-    return solidAt(P, H, ((float)x + 0.5f) * s, ((float)y + 0.5f) * s, ((float)z + 0.5f) * s);
-  };
+  // solidAt at the centre of a level's cell, ((x + .5) 2^level h) / h + .25, floors to the
+  // level-0 cell x 2^level + 2^(level-1) (x itself at level 0): solidCell of that cell.
+  const int span = 1 << level, half = span >> 1;
+  auto blocked = [&](int x, int y, int z) { return solidCell(P, H, x * span + half, y * span + half, z * span + half); };
   if (blocked(px, py, pz)) return FP_STORED_SOLID;
   uint8_t flags = 0;
   if (!blocked(px + 1, py, pz)) flags |= 1;
@@ -608,6 +833,22 @@ __global__ void __launch_bounds__(128) k_topo_bricks(FpBatch bt) {
   }
 }
 
+// Each tile slot's mask of computing bricks this step (activeCell at the tile levels,
+// pressure.wgsl:100-136, asks whether every brick a cell covers has an entry and computes):
+// a CTA of 64 threads per tile, a thread per brick.
+__global__ void __launch_bounds__(64) k_tile_masks(FpBatch bt) {
+  uint32_t total = workTotal(bt, FP_WORK_TILES);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t local;
+    const SimParams& P = workSim(bt, FP_WORK_TILES, item, local);
+    const int t = (int)local;
+    const size_t id = (size_t)t * 64 + threadIdx.x;
+    bool on = __ldg(&P.tileRec[t]).w != 0 && P.entries[id] >= 0 && P.records[id * FP_RECORD_WORDS + 27] != 0;
+    uint32_t half = __ballot_sync(0xffffffffu, on);
+    if ((threadIdx.x & 31) == 0) reinterpret_cast<uint32_t*>(P.tileMask)[2 * t + (threadIdx.x >> 5)] = half;
+  }
+}
+
 // buildTileTopology (pressure.wgsl:281-305): every tile's cells at the tile levels.
 __global__ void __launch_bounds__(64) k_topo_tiles(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_TILES);
@@ -633,6 +874,7 @@ __global__ void __launch_bounds__(64) k_topo_tiles(FpBatch bt) {
 }  // namespace
 
 void fp_launch_topology(const FpBatch& bt, bool anyAll, int sms, cudaStream_t st) {
+  k_tile_masks<<<sms * 16, 64, 0, st>>>(bt);
   k_topo_bricks<false><<<sms * 4, 128, 0, st>>>(bt);
   if (anyAll) {
     k_topo_bricks<true><<<sms * 4, 128, 0, st>>>(bt);
@@ -641,51 +883,82 @@ void fp_launch_topology(const FpBatch& bt, bool anyAll, int sms, cudaStream_t st
 }
 
 static const int BOTTOM_SMEM = 200 * 1024;
-static const int STAGE_SMEM_MAX = 64 * 1024;
-
-template <int OP>
-static void allowStage() {
-  cudaFuncSetAttribute(k_level_bricks_staged<OP, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM_MAX);
-  cudaFuncSetAttribute(k_level_bricks_staged<OP, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM_MAX);
-  cudaFuncSetAttribute(k_level_bricks_staged<OP, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, STAGE_SMEM_MAX);
+// Resident CTAs per SM of each staged instantiation, from the occupancy calculator.
+template <int OP, int SB>
+static int& stagedCtas() {
+  static int n = 4;
+  return n;
+}
+template <int OP, int SB>
+static void configureStaged() {
+  using K = Staged<OP, SB>;
+  cudaFuncSetAttribute(k_level_bricks_staged<OP, SB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_level_bricks_staged<OP, SB>, 256, K::SMEM) != cudaSuccess)
+    n = 4;
+  stagedCtas<OP, SB>() = n > 0 ? n : 1;
 }
 void fp_mg_configure(int B) {
   (void)B;
-  allowStage<RELAX>();
-  allowStage<RESTRICT>();
-  allowStage<PROLONG>();
+  configureStaged<RELAX, 16>();
+  configureStaged<RELAX, 8>();
+  configureStaged<RELAX, 4>();
+  configureStaged<RELAX, 2>();
+  configureStaged<RESTRICT, 16>();
+  configureStaged<RESTRICT, 8>();
+  configureStaged<RESTRICT, 4>();
+  configureStaged<PROLONG, 8>();
+  configureStaged<PROLONG, 4>();
+  configureStaged<PROLONG, 2>();
+  configureStaged<PROLONG, 1>();
   cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, BOTTOM_SMEM);
+  cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, COARSE_SMEM);
 }
 
-// The staged kernel's group size and shared memory for an operation whose output level is
-// `level`, in bricks of B cells: the same arithmetic as the kernel's.
+template <int OP, int SB>
+static void stagedLaunch(const FpBatch& bt, const MgSel& S, int sms, cudaStream_t st) {
+  k_level_bricks_staged<OP, SB><<<sms * stagedCtas<OP, SB>(), 256, Staged<OP, SB>::SMEM, st>>>(bt, S);
+}
+
+// The staged level's cells per brick side for an operation whose output level is `level`,
+// in bricks of B cells (1: the first tile level).
 template <int OP>
-static size_t stageLayout(int level, int B, int& group) {
+static int stagedSide(int level, int B) {
   int bl = B == 8 ? 3 : 4;
-  auto shift = [&](int l) { return l < bl ? bl - l : bl + 2 - l; };
-  int fine = OP == RESTRICT ? level - 1 : level;
-  int stage = OP == PROLONG ? level + 1 : fine;
-  int sb = stage < bl ? 1 << shift(stage) : 1;
-  int R = OP == PROLONG ? 2 : 1;
-  int S = sb + 2 * R, S3 = S * S * S;
-  group = groupFor(1 << (3 * shift(fine)));
-  return (size_t)(256 / group) * (size_t)(S3 + (S3 + 3) / 4) * sizeof(float);
+  int stage = OP == PROLONG ? level + 1 : (OP == RESTRICT ? level - 1 : level);
+  return stage < bl ? 1 << (bl - stage) : 1;
 }
 
 template <int OP>
 static void levelLaunch(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st) {
   if (tiles) {
-    k_level_tiles<OP><<<sms * 8, 64, 0, st>>>(bt, S);
+    // The tile levels hold 4^3, 2^3 and one cell a tile.
+    const int below = S.level - (B == 8 ? 3 : 4);
+    if (below == 0)
+      k_level_tiles<OP, 64><<<sms * 16, 64, 0, st>>>(bt, S);
+    else if (below == 1)
+      k_level_tiles<OP, 8><<<sms * 16, 64, 0, st>>>(bt, S);
+    else
+      k_level_tiles<OP, 1><<<sms * 16, 64, 0, st>>>(bt, S);
     return;
   }
-  int group;
-  size_t smem = stageLayout<OP>(S.level, B, group);
-  if (group == 256)
-    k_level_bricks_staged<OP, 256><<<sms * 4, 256, smem, st>>>(bt, S);
-  else if (group == 64)
-    k_level_bricks_staged<OP, 64><<<sms * 4, 256, smem, st>>>(bt, S);
-  else
-    k_level_bricks_staged<OP, 32><<<sms * 4, 256, smem, st>>>(bt, S);
+  // Relaxation stages sides 16..2, restriction its fine sides 16..4, prolongation 8..1.
+  const int sb = stagedSide<OP>(S.level, B);
+  if constexpr (OP == RELAX) {
+    if (sb == 16) stagedLaunch<OP, 16>(bt, S, sms, st);
+    else if (sb == 8) stagedLaunch<OP, 8>(bt, S, sms, st);
+    else if (sb == 4) stagedLaunch<OP, 4>(bt, S, sms, st);
+    else stagedLaunch<OP, 2>(bt, S, sms, st);
+  } else if constexpr (OP == RESTRICT) {
+    if (sb == 16) stagedLaunch<OP, 16>(bt, S, sms, st);
+    else if (sb == 8) stagedLaunch<OP, 8>(bt, S, sms, st);
+    else stagedLaunch<OP, 4>(bt, S, sms, st);
+  } else {
+    if (sb == 8) stagedLaunch<OP, 8>(bt, S, sms, st);
+    else if (sb == 4) stagedLaunch<OP, 4>(bt, S, sms, st);
+    else if (sb == 2) stagedLaunch<OP, 2>(bt, S, sms, st);
+    else stagedLaunch<OP, 1>(bt, S, sms, st);
+  }
 }
 void fp_launch_relax(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st) {
   levelLaunch<RELAX>(bt, S, tiles, B, sms, st);
@@ -698,6 +971,10 @@ void fp_launch_prolong(const FpBatch& bt, const MgSel& S, bool tiles, int B, int
 }
 void fp_launch_bottom(const FpBatch& bt, const MgSel& S, int iterations, int sms, cudaStream_t st) {
   k_bottom<<<sms, 1024, BOTTOM_SMEM, st>>>(bt, S, iterations, BOTTOM_SMEM);
+}
+bool fp_coarse_fits(int capacity) { return (long)capacity * COARSE_SLOT_BYTES <= COARSE_SMEM; }
+void fp_launch_coarse(const FpBatch& bt, const MgSel& S, int iterations, int sms, cudaStream_t st) {
+  k_coarse<<<sms, 1024, COARSE_SMEM, st>>>(bt, S, iterations);
 }
 
 void fp_launch_residual(const FpBatch& bt, int pSel, int cycle, int sms, cudaStream_t st) {

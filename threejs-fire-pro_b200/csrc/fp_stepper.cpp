@@ -206,10 +206,12 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
   size_t word = 0;
   bool solidsFresh = false, solidsAll = false, topoAll = false, curl = false, measure = false;
   int vcycles = 1;
+  fusedCoarse_ = true;
   pending_.clear();
   for (int i = 0; i < count; i++) {
     Engine* e = sims[i];
     uint32_t cap = (uint32_t)e->capacity();
+    fusedCoarse_ = fusedCoarse_ && fp_coarse_fits((int)cap);
     rowBlocks[i] = blocks;
     rowTiles[i] = tiles;
     rowIds[i] = ids;
@@ -243,7 +245,7 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
     launches_ += n;
   } else {
     uint64_t key = (uint64_t)solidsFresh | ((uint64_t)solidsAll << 1) | ((uint64_t)topoAll << 2) | ((uint64_t)curl << 3) |
-                   ((uint64_t)measure << 4) | ((uint64_t)vcycles << 5);
+                   ((uint64_t)measure << 4) | ((uint64_t)vcycles << 5) | ((uint64_t)fusedCoarse_ << 16);
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
       GraphEntry ge{};
@@ -322,6 +324,15 @@ int Stepper::readProfile(fp_phase* out, uint32_t* count) {
 void Stepper::vcycle(int level, int cur[], uint64_t& launches) {
   auto sel = [](int l, int which) { return fp_mg_sel(l, which); };
   bool tiles = level >= brickLevels_;
+  if (fusedCoarse_ && level == brickLevels_ + 1) {
+    // Two relaxations, restriction, the bottom, prolongation, three relaxations: an even
+    // number of flips leaves the result in the buffer of the first iterate.
+    MgSel S{level, sel(level, 2), sel(level, cur[level]), -1, sel(level, cur[level]), sel(bottom_, 0), cycle_};
+    fp_launch_coarse(batch(), S, 19, sms_, stream_);
+    launches++;
+    cur[bottom_] = 0;
+    return;
+  }
   if (level == bottom_) {
     MgSel S{level, sel(level, 2), sel(level, cur[level]), -1, sel(level, 1 - cur[level]), -1, cycle_};
     fp_launch_bottom(batch(), S, 19, sms_, stream_);
@@ -365,8 +376,8 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   // Topology of the slots granted this step, or of everything after the geometry changed.
   phaseBegin(PH_TOPO);
   fp_launch_topology(bt, topoAll, sms_, stream_);
-  launches += topoAll ? 3 : 1;
-  phaseEnd(PH_TOPO, topoAll ? 3 : 1);
+  launches += topoAll ? 4 : 2;
+  phaseEnd(PH_TOPO, topoAll ? 4 : 2);
   phaseBegin(PH_PREDICT);
   fp_launch_predict(bt, B_, sms_, stream_);
   phaseEnd(PH_PREDICT, 1);

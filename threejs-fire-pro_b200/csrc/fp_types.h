@@ -121,6 +121,7 @@ struct SimParams {
   int capacity;  // tile slots; brick ids = capacity * 64
   const int4* tileRec;
   const int* tileNbr;
+  uint64_t* tileMask;  // per tile slot, each step: bit l when brick l of the tile computes
   const int4* hash;
   uint32_t hashMask;
   // per brick id
