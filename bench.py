@@ -249,39 +249,43 @@ def batched_form(local: int, sims: int = 64, grow: int = 90, steps: int = 60, se
     batch.synchronize()
     for s in plain:
         s.synchronize()
-    # (b) batched: device time on the batch's stream and wall time; actives read each step
+    # The frames are the workload's input, built before the timed loops; the voxel-steps come
+    # from each simulation's count of bricks stepped, read once before and once after.
+    frames = [[m.frame(grow + k) for m in mem] for k in range(steps)]
+    stepped_b = lambda: sum(batch.stats(i).bricks_stepped for i in ids)
+    stepped_p = lambda: sum(s.stats().bricks_stepped for s in plain)
+    # (b) batched: device time on the batch's stream and wall time
     stream = torch.cuda.ExternalStream(batch.stream(), device=local)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
-    actives = []
+    b0 = stepped_b()
     t0 = time.perf_counter()
     ev[0].record(stream)
     for k in range(steps):
-        fds = [m.frame(grow + k) for m in mem]
-        batch.step([(i, fd.frame, FIXED_DT) for i, fd in zip(ids, fds)])
+        batch.step([(i, fd.frame, FIXED_DT) for i, fd in zip(ids, frames[k])])
         ev[k + 1].record(stream)
-        actives.append(sum(batch.stats(i).active_bricks for i in ids))
     batch.synchronize()
     wall_b = time.perf_counter() - t0
+    vox_b = (stepped_b() - b0) * BRICK_VOXELS
     dev_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
     # (a) plain: one simulation after another
+    p0 = stepped_p()
     t0 = time.perf_counter()
     for k in range(steps):
-        fds = [m.frame(grow + k) for m in mem]
-        for s, fd in zip(plain, fds):
+        for s, fd in zip(plain, frames[k]):
             s.step(fd.frame)
     for s in plain:
         s.synchronize()
     wall_p = time.perf_counter() - t0
-    same = [s.stats().active_bricks for s in plain] == [batch.stats(i).active_bricks for i in ids]
-    vox = sum(actives) * BRICK_VOXELS
+    vox_p = (stepped_p() - p0) * BRICK_VOXELS
+    same = [s.stats().active_bricks for s in plain] == [batch.stats(i).active_bricks for i in ids] and vox_b == vox_p
     p50, p99 = percentiles(dev_ms)
     out = {
         "workload": f"{sims} member scenes, brick budgets log-uniform 16-2048 (seed {seed}), 1-4 emitters r 0.1-0.6 m, "
-                    f"rates 0.2-2.0/s; grown {grow} steps, {steps} timed; plain FP32",
-        "mean_active_bricks": sum(actives) / len(actives),
-        "batched": {"value": vox / wall_b, "device_value": vox / (sum(dev_ms) / 1e3), "ms_per_step": 1e3 * wall_b / steps,
+                    f"rates 0.2-2.0/s; grown {grow} steps, {steps} timed, frames built before; plain FP32",
+        "mean_active_bricks": vox_b / BRICK_VOXELS / steps,
+        "batched": {"value": vox_b / wall_b, "device_value": vox_b / (sum(dev_ms) / 1e3), "ms_per_step": 1e3 * wall_b / steps,
                     "device_p50_ms": p50, "device_p99_ms": p99},
-        "plain": {"value": vox / wall_p, "ms_per_step": 1e3 * wall_p / steps},
+        "plain": {"value": vox_p / wall_p, "ms_per_step": 1e3 * wall_p / steps},
         "speedup": wall_p / wall_b,
         "same_final_bricks": same,
         "unit": "voxel-steps/s",

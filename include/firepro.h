@@ -168,6 +168,7 @@ typedef struct fp_stats {
   double host_prepare_ms;   /* host time in fp_sim_step since creation, waits excluded */
   double host_wait_ms;      /* host time spent waiting for the previous step's measurement */
   double last_divergence;   /* post-projection RMS(h div u) / RMS(u) of that solve when measured, else -1 */
+  uint64_t bricks_stepped;  /* computing bricks summed over the measured steps since creation or reset */
 } fp_stats;
 
 /* The latest step's pressure solve (`fp_sim_read_solver`). No reference counterpart: the

@@ -228,6 +228,7 @@ int Engine::initialize() {
   steps_ = 0;
   latest_ = 0;
   activeBricks_ = usedSlots_ = lastFailures_ = 0;
+  bricksStepped_ = 0;
   poolLimited_ = false;
   colliderCount_ = 0;
   prevColliders_.clear();
@@ -839,6 +840,7 @@ void Engine::applyReadback(const uint32_t* words) {
   for (int s = 0; s < capacity_ && s < (int)tileRec_.size(); s++)
     if (flags[s] && tileRec_[s].w != 0) contentTiles_.push_back({tileRec_[s], flags[s]});
   activeBricks_ = c->active;
+  bricksStepped_ += c->active;
   usedSlots_ = slots_ - (uint32_t)c->freeCount;
   lastFailures_ = c->failures;
   poolLimited_ = c->failures > 0 && slots_ >= slotLimit();
@@ -907,6 +909,7 @@ int Engine::stats(fp_stats* out) {
   out->time = time_;
   out->steps = (uint64_t)steps_;
   out->active_bricks = activeBricks_;
+  out->bricks_stepped = bricksStepped_;
   out->brick_cells = (uint32_t)N_;
   out->pool_limited = poolLimited_;
   out->pool_slots = slots_;

@@ -146,6 +146,7 @@ class Engine {
   std::vector<uint32_t> prevMasks_;
   std::vector<std::pair<int4, uint32_t>> contentTiles_;
   uint32_t activeBricks_ = 0, usedSlots_ = 0, lastFailures_ = 0;
+  uint64_t bricksStepped_ = 0;  // computing bricks summed over the measured steps
   bool poolLimited_ = false;
   int latest_ = 0;  // index of the latest pressure solution
   int vcycles_ = 1;

@@ -179,6 +179,7 @@ class fp_stats(C.Structure):
         ("host_prepare_ms", C.c_double),
         ("host_wait_ms", C.c_double),
         ("last_divergence", C.c_double),
+        ("bricks_stepped", C.c_uint64),
     ]
 
 
