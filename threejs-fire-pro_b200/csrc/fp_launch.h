@@ -14,7 +14,7 @@ void fp_launch_readback(const FpBatch& bt, int sms, cudaStream_t st);
 void fp_launch_predict(const FpBatch& bt, int B, int sms, cudaStream_t st);
 void fp_launch_correct(const FpBatch& bt, int B, int sms, cudaStream_t st);
 void fp_launch_evolve(const FpBatch& bt, int B, int sms, cudaStream_t st);
-void fp_launch_curl(const FpBatch& bt, int sms, cudaStream_t st);
+void fp_launch_curl(const FpBatch& bt, int B, int sms, cudaStream_t st);
 void fp_launch_forces(const FpBatch& bt, int B, int sms, cudaStream_t st);
 // Divergence with the finest level's first iterate into p0[pSel]; projection with p0[pSel].
 void fp_launch_divergence(const FpBatch& bt, int pSel, int sms, cudaStream_t st);

@@ -783,7 +783,8 @@ FP_DEV uint8_t cellTopology(const SimParams& P, const Home& H, int px, int py, i
 template <bool ALL>
 __global__ void __launch_bounds__(128) k_topo_bricks(FpBatch bt) {
   __shared__ int nslot[27];
-  const int kind = ALL ? FP_WORK_IDS : FP_WORK_FRESH;
+  // Every slotted brick is on the ascending list of computing bricks.
+  const int kind = ALL ? FP_WORK_ACTIVE : FP_WORK_FRESH;
   uint32_t total = workTotal(bt, kind);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
@@ -792,7 +793,7 @@ __global__ void __launch_bounds__(128) k_topo_bricks(FpBatch bt) {
     uint32_t id;
     int slot;
     if (ALL) {
-      id = i;
+      id = P.active[i];
       if (__ldg(&P.tileRec[id >> 6]).w == 0) continue;
       slot = entryPage(P.entries[id]);
     } else {

@@ -20,6 +20,7 @@ namespace {
 
 constexpr int THREADS = 256;
 constexpr int HALO = 2;
+constexpr int STAGE_SIDE = 8 + 2 * HALO;  // the staged kernels run for 8^3 bricks only
 // Resident CTAs per SM the transport kernels are compiled for (register cap 65536 / (256 n)).
 #ifndef FP_TRANSPORT_CTAS
 #define FP_TRANSPORT_CTAS 4
@@ -86,30 +87,29 @@ FP_DEV float fieldSample(const SimParams& P, const Home& H, const Stage& G, cons
   return sampleCells(P, H, f.pool, f.ch, c, px, py, pz, f.half);
 }
 
-// Copy channels of a pool over the staged box into shared memory, zero where no slot, with
-// asynchronous 4-byte copies (cp.async): every thread keeps all its copies in flight and the
-// caller waits once. A brick without a slot reads nothing (source size 0 zero-fills). A half
-// pool is widened to FP32 on the way (plain loads: cp.async moves at least 4 bytes).
+// Copy channels [0, nch) of a pool of `ch` channels over the staged box into shared memory,
+// zero where no slot, with asynchronous 4-byte copies (cp.async): every thread keeps all its
+// copies in flight and the caller waits once. A brick without a slot reads nothing (source
+// size 0 zero-fills). A half pool is widened to FP32 on the way (plain loads: cp.async moves
+// at least 4 bytes). SIDE, when not 0, is the box's side G.S known at compile time.
+template <int SIDE = 0>
 FP_DEV void stageField(const SimParams& P, const Home& H, const Stage& G, float* sm, const float* pool, int ch,
-                       bool half = false) {
-  if (half) {
-    for (int i = threadIdx.x; i < G.S3; i += blockDim.x) {
-      int lx = i % G.S, ly = (i / G.S) % G.S, lz = i / (G.S * G.S);
-      int x = G.ox + lx, y = G.oy + ly, z = G.oz + lz;
-      int s = brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift);
-      size_t base = s < 0 ? 0 : (size_t)s * ch * P.N + localCell(P, x, y, z);
-      for (int c = 0; c < ch; c++) sm[c * G.S3 + i] = s < 0 ? 0.f : ldHalf(pool, base + (size_t)c * P.N, true);
-    }
-    return;
-  }
-  for (int i = threadIdx.x; i < G.S3; i += blockDim.x) {
-    int lx = i % G.S, ly = (i / G.S) % G.S, lz = i / (G.S * G.S);
+                       bool half = false, int nch = 0) {
+  const int S = SIDE ? SIDE : G.S, S3 = S * S * S;
+  if (nch <= 0) nch = ch;
+  for (int i = threadIdx.x; i < S3; i += blockDim.x) {
+    int lx = i % S, ly = (i / S) % S, lz = i / (S * S);
     int x = G.ox + lx, y = G.oy + ly, z = G.oz + lz;
     int s = brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift);
+    if (half) {
+      size_t base = s < 0 ? 0 : (size_t)s * ch * P.N + localCell(P, x, y, z);
+      for (int c = 0; c < nch; c++) sm[c * S3 + i] = s < 0 ? 0.f : ldHalf(pool, base + (size_t)c * P.N, true);
+      continue;
+    }
     const float* src = s < 0 ? pool : pool + (size_t)s * ch * P.N + localCell(P, x, y, z);
     int bytes = s < 0 ? 0 : 4;
-    for (int c = 0; c < ch; c++) {
-      unsigned dst = (unsigned)__cvta_generic_to_shared(sm + c * G.S3 + i);
+    for (int c = 0; c < nch; c++) {
+      unsigned dst = (unsigned)__cvta_generic_to_shared(sm + c * S3 + i);
       const float* g = s < 0 ? pool : src + (size_t)c * P.N;
       asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(g), "r"(bytes) : "memory");
     }
@@ -233,8 +233,8 @@ FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
   Field V{P.vel, 3, STAGED ? smem : nullptr};
   Field F{P.fld, 4, STAGED ? smem + 3 * G.S3 : nullptr, P.scalarHalf != 0};
   if (STAGED) {
-    stageField(P, H, G, smem, P.vel, 3);
-    stageField(P, H, G, smem + 3 * G.S3, P.fld, 4, F.half);
+    stageField<STAGE_SIDE>(P, H, G, smem, P.vel, 3);
+    stageField<STAGE_SIDE>(P, H, G, smem + 3 * G.S3, P.fld, 4, F.half);
     stageWait();
   }
   size_t slot = (size_t)nslot[13];
@@ -349,8 +349,8 @@ FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
   Field V{P.vel, 3, STAGED ? smem : nullptr};
   Field Vp{P.velP, 3, STAGED ? smem + 3 * G.S3 : nullptr};
   if (STAGED) {
-    stageField(P, H, G, smem, P.vel, 3);
-    stageField(P, H, G, smem + 3 * G.S3, P.velP, 3);
+    stageField<STAGE_SIDE>(P, H, G, smem, P.vel, 3);
+    stageField<STAGE_SIDE>(P, H, G, smem + 3 * G.S3, P.velP, 3);
     stageWait();
   }
   size_t slot = (size_t)nslot[13];
@@ -437,8 +437,8 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
   Field Fp{P.fldP, 4, STAGED ? smem + 3 * G.S3 : nullptr, false};  // the predictor: FP32
   const bool half = P.scalarHalf != 0;                             // the state pools
   if (STAGED) {
-    stageField(P, H, G, smem, P.vel, 3);
-    stageField(P, H, G, smem + 3 * G.S3, P.fldP, 4);
+    stageField<STAGE_SIDE>(P, H, G, smem, P.vel, 3);
+    stageField<STAGE_SIDE>(P, H, G, smem + 3 * G.S3, P.fldP, 4);
     stageWait();
   }
   size_t slot = (size_t)nslot[13];
@@ -609,12 +609,26 @@ __global__ void __launch_bounds__(THREADS, FP_TRANSPORT_CTAS) k_evolve(FpBatch b
 }
 
 // ---------------------------------------------------------------------------------------
-// computeCurl (fluid-forces.wgsl:38-75) of the corrected velocity.
+// computeCurl (fluid-forces.wgsl:38-75) of the corrected velocity. Staged (8^3 bricks): the
+// corrected velocity over the brick and a one-cell rim, every read from shared memory.
+template <bool STAGED>
 FP_DEV void brick_curl(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
+  extern __shared__ float smem[];
   const SimParams& P = *Pp;
   if (!P.curlOn) return;  // the same for the whole CTA
   Home H = enterBrick(P, P.active[i], nslot);
+  Stage G;
+  G.S = STAGED ? P.B + 2 : 0;
+  G.S3 = G.S * G.S * G.S;
+  G.ox = H.bx * P.B - 1;
+  G.oy = H.by * P.B - 1;
+  G.oz = H.bz * P.B - 1;
+  Field V{P.velC, 3, STAGED ? smem : nullptr};
+  if (STAGED) {
+    stageField<8 + 2>(P, H, G, smem, P.velC, 3);
+    stageWait();
+  }
   size_t slot = (size_t)nslot[13];
   const size_t N = P.N;
   for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
@@ -623,7 +637,7 @@ FP_DEV void brick_curl(const SimParams* __restrict__ Pp, uint32_t i) {
     auto cc = [&](int qx, int qy, int qz, int comp) {
       int r[3] = {qx, qy, qz};
       r[comp] -= 1;
-      return 0.5f * (cellAt(P, H, P.velC, 3, comp, qx, qy, qz) + cellAt(P, H, P.velC, 3, comp, r[0], r[1], r[2]));
+      return 0.5f * (nearCell(P, H, G, V, comp, qx, qy, qz) + nearCell(P, H, G, V, comp, r[0], r[1], r[2]));
     };
     float hh = 0.5f / P.h;
     float dx0 = (cc(x + 1, y, z, 1) - cc(x - 1, y, z, 1)) * hh, dx1 = (cc(x + 1, y, z, 2) - cc(x - 1, y, z, 2)) * hh;
@@ -637,12 +651,13 @@ FP_DEV void brick_curl(const SimParams* __restrict__ Pp, uint32_t i) {
   }
   __syncthreads();
 }
+template <bool STAGED>
 __global__ void __launch_bounds__(THREADS) k_curl(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_curl(&P, i);
+    brick_curl<STAGED>(&P, i);
   }
 }
 
@@ -705,20 +720,22 @@ FP_DEV float3 externalForces(const SimParams& P, int tile, float px, float py, f
 }
 
 // cellForce / centerForce (fluid-forces.wgsl:79-118).
-FP_DEV float3 cellForce(const SimParams& P, const Home& H, int tile, int x, int y, int z) {
+// The curl is read over the force region and a one-cell rim (Gc, Fc), the evolved scalars
+// over the force region (Gs, Fs): staged or through the directory.
+FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage& Gc, const Field& Fc, const Stage& Gs,
+                        const Field& Fs, int tile, int x, int y, int z) {
   if (brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift) < 0) return make_float3(0.f, 0.f, 0.f);
   float wx = ((float)x + 0.5f) * P.h, wy = ((float)y + 0.5f) * P.h, wz = ((float)z + 0.5f) * P.h;
   if (solidCell(P, H, x, y, z)) return make_float3(0.f, 0.f, 0.f);  // solidAt at the centre
   // The evolved scalars of this step (the reference swaps field and corrected first).
-  const bool half = P.scalarHalf != 0;
-  float heat = cellAt(P, H, P.fldN, 4, 1, x, y, z, half), density = cellAt(P, H, P.fldN, 4, 0, x, y, z, half);
+  float heat = nearCell(P, H, Gs, Fs, 1, x, y, z), density = nearCell(P, H, Gs, Fs, 0, x, y, z);
   float3 conf = make_float3(0.f, 0.f, 0.f);
   if (P.vorticity != 0.f) {
-    float c0 = cellAt(P, H, P.curl, 4, 0, x, y, z), c1 = cellAt(P, H, P.curl, 4, 1, x, y, z),
-          c2 = cellAt(P, H, P.curl, 4, 2, x, y, z);
-    float e0 = cellAt(P, H, P.curl, 4, 3, x + 1, y, z) - cellAt(P, H, P.curl, 4, 3, x - 1, y, z);
-    float e1 = cellAt(P, H, P.curl, 4, 3, x, y + 1, z) - cellAt(P, H, P.curl, 4, 3, x, y - 1, z);
-    float e2 = cellAt(P, H, P.curl, 4, 3, x, y, z + 1) - cellAt(P, H, P.curl, 4, 3, x, y, z - 1);
+    float c0 = nearCell(P, H, Gc, Fc, 0, x, y, z), c1 = nearCell(P, H, Gc, Fc, 1, x, y, z),
+          c2 = nearCell(P, H, Gc, Fc, 2, x, y, z);
+    float e0 = nearCell(P, H, Gc, Fc, 3, x + 1, y, z) - nearCell(P, H, Gc, Fc, 3, x - 1, y, z);
+    float e1 = nearCell(P, H, Gc, Fc, 3, x, y + 1, z) - nearCell(P, H, Gc, Fc, 3, x, y - 1, z);
+    float e2 = nearCell(P, H, Gc, Fc, 3, x, y, z + 1) - nearCell(P, H, Gc, Fc, 3, x, y, z - 1);
     float len = sqrtf(e0 * e0 + e1 * e1 + e2 * e2) + 0.0001f;
     float n0 = e0 / len, n1 = e1 / len, n2 = e2 / len;
     float s = P.vorticity * P.h;
@@ -750,21 +767,44 @@ FP_DEV float sourceVelocity(const SimParams& P, int tile, float value, float fx,
 }
 
 // applyForces (fluid-forces.wgsl:151-182): centre forces of the brick and of the cells past
-// it on one axis, staged in shared memory, averaged to the faces.
+// it on one axis, staged in shared memory, averaged to the faces. Staged (8^3 bricks): the
+// curl over that region and a one-cell rim and the evolved smoke and heat over the region are
+// copied to shared memory first.
+template <bool STAGED>
 FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
-  extern __shared__ float3 forceTile[];  // (B+1)^3
+  extern __shared__ float3 forceTile[];  // (B+1)^3, then the staged curl and scalars
   const SimParams& P = *Pp;
   uint32_t id = P.active[i];
   Home H = enterBrick(P, id, nslot);
   size_t slot = (size_t)nslot[13];
   const size_t N = P.N;
   int tile = (int)(id >> 6);
-  int E = P.B + 1;
-  for (int q = threadIdx.x; q < E * E * E; q += blockDim.x) {
+  const int E = STAGED ? 9 : P.B + 1, E3 = E * E * E;
+  float* stage = reinterpret_cast<float*>(forceTile + E3);
+  Stage Gc, Gs;
+  Gc.S = STAGED ? E + 2 : 0;
+  Gc.S3 = Gc.S * Gc.S * Gc.S;
+  Gc.ox = H.bx * P.B - 1;
+  Gc.oy = H.by * P.B - 1;
+  Gc.oz = H.bz * P.B - 1;
+  Gs.S = STAGED ? E : 0;
+  Gs.S3 = Gs.S * Gs.S * Gs.S;
+  Gs.ox = H.bx * P.B;
+  Gs.oy = H.by * P.B;
+  Gs.oz = H.bz * P.B;
+  const bool half = P.scalarHalf != 0;
+  Field Fc{P.curl, 4, STAGED ? stage : nullptr};
+  Field Fs{P.fldN, 4, STAGED ? stage + 4 * Gc.S3 : nullptr, half};
+  if (STAGED) {
+    if (P.vorticity != 0.f) stageField<11>(P, H, Gc, stage, P.curl, 4);
+    stageField<9>(P, H, Gs, stage + 4 * Gc.S3, P.fldN, 4, half, 2);  // smoke, heat
+    stageWait();
+  }
+  for (int q = threadIdx.x; q < E3; q += blockDim.x) {
     int lx = q % E, ly = (q / E) % E, lz = q / (E * E);
     if ((lx == P.B) + (ly == P.B) + (lz == P.B) >= 2) continue;
-    forceTile[q] = cellForce(P, H, tile, H.bx * P.B + lx, H.by * P.B + ly, H.bz * P.B + lz);
+    forceTile[q] = cellForce(P, H, Gc, Fc, Gs, Fs, tile, H.bx * P.B + lx, H.by * P.B + ly, H.bz * P.B + lz);
   }
   __syncthreads();
   float decay = expf(-P.damping * P.dt);
@@ -797,14 +837,18 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   }
   __syncthreads();
 }
+template <bool STAGED>
 __global__ void __launch_bounds__(THREADS, 4) k_forces(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_forces(&P, i);
+    brick_forces<STAGED>(&P, i);
   }
 }
+// Shared memory of the staged force kernel: the (B+1)^3 force tile, the curl over (B+3)^3,
+// two scalar channels over (B+1)^3.
+constexpr size_t FORCE_STAGED_BYTES = 729 * sizeof(float3) + (4 * 1331 + 2 * 729) * sizeof(float);
 
 // pressureUnknown (fluid-forces.wgsl:210-226): the cell's brick and those of its negative
 // neighbours compute.
@@ -1002,7 +1046,7 @@ void fp_step_configure(int B) {
   cudaFuncSetAttribute(k_correct<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(6));
   cudaFuncSetAttribute(k_evolve<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
   size_t smem = (size_t)(B + 1) * (B + 1) * (B + 1) * sizeof(float3);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_forces, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_forces<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 void fp_launch_predict(const FpBatch& bt, int B, int sms, cudaStream_t st) {
@@ -1023,10 +1067,19 @@ void fp_launch_evolve(const FpBatch& bt, int B, int sms, cudaStream_t st) {
   else
     k_evolve<false><<<sms * 4, THREADS, 0, st>>>(bt);
 }
-void fp_launch_curl(const FpBatch& bt, int sms, cudaStream_t st) { k_curl<<<sms * 4, THREADS, 0, st>>>(bt); }
+void fp_launch_curl(const FpBatch& bt, int B, int sms, cudaStream_t st) {
+  if (B == 8)
+    k_curl<true><<<sms * 4, THREADS, 3 * 10 * 10 * 10 * sizeof(float), st>>>(bt);
+  else
+    k_curl<false><<<sms * 4, THREADS, 0, st>>>(bt);
+}
 void fp_launch_forces(const FpBatch& bt, int B, int sms, cudaStream_t st) {
+  if (B == 8) {
+    k_forces<true><<<sms * 4, THREADS, FORCE_STAGED_BYTES, st>>>(bt);
+    return;
+  }
   size_t smem = (size_t)(B + 1) * (B + 1) * (B + 1) * sizeof(float3);
-  k_forces<<<sms * 4, THREADS, smem, st>>>(bt);
+  k_forces<false><<<sms * 4, THREADS, smem, st>>>(bt);
 }
 void fp_launch_divergence(const FpBatch& bt, int pSel, int sms, cudaStream_t st) {
   k_divergence<<<sms * 4, THREADS, 0, st>>>(bt, pSel);

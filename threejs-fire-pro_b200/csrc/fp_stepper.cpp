@@ -402,7 +402,7 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
 
   if (curl) {
     phaseBegin(PH_CURL);
-    fp_launch_curl(bt, sms_, stream_);
+    fp_launch_curl(bt, B_, sms_, stream_);
     launches++;
     phaseEnd(PH_CURL, 1);
   }
