@@ -273,6 +273,24 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
     if (has && t < 27) nslot[t] = entryPage(P.records[(size_t)id * FP_RECORD_WORDS + t]);
     __syncthreads();
     const int ox = H.bx * SB - R, oy = H.by * SB - R, oz = H.bz * SB - R;
+    // Relaxation and prolongation: this thread's own cells' flags and right-hand side or
+    // current value, loaded before the stage so that both sets of loads are in flight together.
+    constexpr int K = OP == RESTRICT ? 1 : (FCELLS + GROUP - 1) / GROUP;
+    uint8_t ownTopo[K];
+    float ownValue[K];
+    if (OP != RESTRICT && has) {
+      const long slot0 = nslot[13];
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        const int o = t + k * GROUP;
+        if (o < FCELLS) {
+          const long a = slot0 * FCELLS + o;
+          ownTopo[k] = P.topo[fineLevel][a];
+          ownValue[k] = OP == RELAX ? ldBf(A.rhs, a, A.rhsN) : ldBf(A.pin, a, A.pinN);
+        }
+      }
+    }
+    bool solidStaged = false;  // prolongation: a solid coarse cell in this thread's stage cells
     if (has) {
       if (t < 8) {
         int dx = -(t & 1), dy = -((t >> 1) & 1), dz = -(t >> 2);
@@ -293,10 +311,20 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
           a = cellAddress(P, H, ox + lx, oy + ly, oz + lz, stageLevel);
         }
         st[q] = a < 0 ? 0.f : ldBf(src, a, srcN);
-        if (OP == PROLONG) solidSt[q] = a >= 0 && (P.topo[stageLevel][a] & FP_STORED_SOLID) ? 1 : 0;
+        if (OP == PROLONG) {
+          const bool solid = a >= 0 && (P.topo[stageLevel][a] & FP_STORED_SOLID);
+          solidSt[q] = solid ? 1 : 0;
+          solidStaged = solidStaged || solid;
+        }
       }
     }
-    __syncthreads();
+    // Without a solid coarse cell anywhere in the CTA's stages a Neumann ghost is the staged
+    // value itself (coarseValue's first test), so prolongation may read the stage directly.
+    bool anySolid = false;
+    if (OP == PROLONG)
+      anySolid = __syncthreads_or(solidStaged) != 0;
+    else
+      __syncthreads();
     if (has) {
       // The negative-octant neighbours that compute, as bits; a fine cell on the brick's low
       // faces is an unknown when every neighbour its faces touch computes (activeCell).
@@ -341,17 +369,20 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
         return (v0 + v1) + (v2 + v3) + (v4 + v5);
       };
       if (OP == RELAX || OP == PROLONG) {
-        for (int o = t; o < FCELLS; o += GROUP) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          const int o = t + k * GROUP;
+          if (o >= FCELLS) break;
           const int lx = o & (FS - 1), ly = (o >> fs) & (FS - 1), lz = o >> (2 * fs);
           const long a = slot * FCELLS + o;
-          uint32_t f = expandFlags(P.topo[fineLevel][a]);
+          uint32_t f = expandFlags(ownTopo[k]);
           if ((f & SOLIDF) || !unknown(lx, ly, lz)) {
             stBf(A.pout, a, 0.f, A.poutN);
             continue;
           }
           if (OP == RELAX) {
             float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
-            float cand = (sumAt(lx, ly, lz, f) - ldBf(A.rhs, a, A.rhsN)) / fmaxf(diagOf(f), 1e-12f);
+            float cand = (sumAt(lx, ly, lz, f) - ownValue[k]) / fmaxf(diagOf(f), 1e-12f);
             stBf(A.pout, a, mixf(center, cand, 0.8f), A.poutN);
           } else {
             int px = H.bx * FS + lx, py = H.by * FS + ly, pz = H.bz * FS + lz;
@@ -359,7 +390,7 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
                   qz = ((float)pz + 0.5f) * 0.5f - 0.5f;
             int ix = (int)floorf(qx), iy = (int)floorf(qy), iz = (int)floorf(qz);
             float fx = qx - floorf(qx), fy = qy - floorf(qy), fz = qz - floorf(qz);
-            bool fast = P.colliderCount == 0 && (!P.ground || iy >= 0);
+            bool fast = (P.colliderCount == 0 || !anySolid) && (!P.ground || iy >= 0);
             // Below the ground the mirrored ghosts read the row above it, which a brick under
             // y = 0 does not stage: those read through the directory.
             bool staged = !(P.ground && H.by < 0);
@@ -373,7 +404,7 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
             }
             float corr = mixf(mixf(mixf(v[0], v[1], fx), mixf(v[2], v[3], fx), fy),
                               mixf(mixf(v[4], v[5], fx), mixf(v[6], v[7], fx), fy), fz);
-            stBf(A.pout, a, ldBf(A.pin, a, A.pinN) + corr, A.poutN);
+            stBf(A.pout, a, ownValue[k] + corr, A.poutN);
           }
         }
       } else {  // RESTRICT: coarse cells of this brick at A.level
