@@ -189,7 +189,7 @@ int Engine::consume() {
 void Engine::freeAll() {
   DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_, &zeroList_,
                          &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_, &donors_, &solids_,
-                         &tileRecD_, &tileNbrD_, &hashD_, &solver_, &tileMask_};
+                         &tileRecD_, &tileNbrD_, &hashD_, &solver_, &tileMask_, &liveTilesD_, &tileIndexD_};
   for (DeviceBuffer* b : all)
     if (b->ptr) {
       cudaFree(b->ptr);
@@ -254,7 +254,7 @@ uint64_t Engine::estimateBytes(const fp_grid& g, uint32_t tiles) {
     uint64_t c = (uint64_t)1 << (3 * (shift - l));
     perSlot += c * (3 * narrow + 1);
   }
-  uint64_t perTile = 64 * (4 * 5 + FP_RECORD_WORDS * 4 + 8) + 16 + 27 * 4 + 16 + 8 + (64 + 8 + 1) * (3 * narrow + 1);
+  uint64_t perTile = 64 * (4 * 5 + FP_RECORD_WORDS * 4 + 8) + 16 + 27 * 4 + 16 + 8 + 8 + (64 + 8 + 1) * (3 * narrow + 1);
   return slots * perSlot + (uint64_t)std::max(tiles, (uint32_t)MIN_TILES) * perTile + 64 * 1024;
 }
 
@@ -405,8 +405,19 @@ int Engine::applyTiles() {
         for (int dx = -1; dx <= 1; dx++)
           tileNbr_[s * 27 + (dz + 1) * 9 + (dy + 1) * 3 + dx + 1] = dir_.slotAt(t.x + dx, t.y + dy, t.z + dz);
   }
+  // The live slots in ascending order and each slot's position among them: the tile levels of
+  // the multigrid walk only these.
+  liveTiles_.clear();
+  tileIndex_.assign(capacity_, -1);
+  for (int s = 0; s < capacity_; s++)
+    if (tileRec_[s].w != 0) {
+      tileIndex_[s] = (int)liveTiles_.size();
+      liveTiles_.push_back(s);
+    }
   if (!upload(tileRecD_, tileRec_.data(), tileRec_.size() * sizeof(int4)) ||
-      !upload(tileNbrD_, tileNbr_.data(), tileNbr_.size() * 4) || !upload(hashD_, hash_.data(), hash_.size() * sizeof(int4)))
+      !upload(tileNbrD_, tileNbr_.data(), tileNbr_.size() * 4) || !upload(hashD_, hash_.data(), hash_.size() * sizeof(int4)) ||
+      !upload(liveTilesD_, liveTiles_.data(), liveTiles_.size() * 4) ||
+      !upload(tileIndexD_, tileIndex_.data(), tileIndex_.size() * 4))
     return FP_ENOMEM;
   // New tiles' bricks start without slots.
   for (int slot : dir_.takeCreated()) {
@@ -769,6 +780,9 @@ void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t
   P.tileRec = (const int4*)tileRecD_.ptr;
   P.tileNbr = (const int*)tileNbrD_.ptr;
   P.tileMask = (uint64_t*)tileMask_.ptr;
+  P.liveTiles = (const int*)liveTilesD_.ptr;
+  P.tileIndex = (const int*)tileIndexD_.ptr;
+  P.liveCount = (int)liveTiles_.size();
   P.hash = (const int4*)hashD_.ptr;
   P.hashMask = (uint32_t)hash_.size() - 1;
   P.pages = (int*)pages_.ptr;
@@ -893,7 +907,8 @@ uint64_t Engine::memoryBytes() const {
   uint64_t bytes = 0;
   const DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_,
                                &zeroList_, &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_,
-                               &donors_, &solids_, &tileRecD_, &tileNbrD_, &hashD_, &solver_, &tileMask_};
+                               &donors_, &solids_, &tileRecD_, &tileNbrD_, &hashD_, &solver_, &tileMask_,
+                               &liveTilesD_, &tileIndexD_};
   for (const DeviceBuffer* b : all) bytes += b->bytes;
   for (auto& b : vel_) bytes += b.bytes;
   for (auto& b : fld_) bytes += b.bytes;

@@ -102,6 +102,7 @@ class Engine {
   bool solidsAll() const { return solidsStale_; }
   bool topoAll() const { return geometryDirty_; }
   int capacity() const { return capacity_; }
+  int liveTiles() const { return (int)liveTiles_.size(); }
   size_t readbackWords() const { return (sizeof(FpCounters) + sizeof(FpSolver)) / 4 + (size_t)capacity_; }
   // Pressure solve (no reference counterpart; the reference runs one V-cycle): up to
   // `vcycles` V-cycles a step, stopping at a relative FP64 residual of `tolerance` (0: all).
@@ -161,7 +162,8 @@ class Engine {
   DeviceBuffer freeStack_, counters_;
   DeviceBuffer vel_[4], curl_, fld_[3], expn_, div_, vmin_, vmax_, sb_, donors_, solids_;
   DeviceBuffer p0_[2], topo_[FP_MAX_LEVELS], lp_[FP_MAX_LEVELS][2], lrhs_[FP_MAX_LEVELS];
-  DeviceBuffer tileRecD_, tileNbrD_, hashD_, solver_, tileMask_;
+  DeviceBuffer tileRecD_, tileNbrD_, hashD_, solver_, tileMask_, liveTilesD_, tileIndexD_;
+  std::vector<int> liveTiles_, tileIndex_;  // live tile slots ascending; slot -> position or -1
   int velIdx_[4] = {0, 1, 2, 3};  // start, predictor/projected, corrected, forced
   int fldIdx_[3] = {0, 1, 2};     // start, predictor, evolved
 

@@ -38,8 +38,8 @@ void fp_launch_prolong(const FpBatch& bt, const MgSel& S, bool tiles, int B, int
 void fp_launch_bottom(const FpBatch& bt, const MgSel& S, int iterations, int sms, cudaStream_t st);
 // The V-cycle from the second tile level down in one CTA per simulation (k_coarse): S.level is
 // that level, S.rhs its right-hand side, S.pin its first iterate, S.pout its result, S.cfirst
-// the bottom's result. Usable when every simulation's tile capacity fits (fp_coarse_fits).
-bool fp_coarse_fits(int capacity);
+// the bottom's result. Usable when every simulation's live tiles fit (fp_coarse_fits).
+bool fp_coarse_fits(int liveTiles);
 void fp_launch_coarse(const FpBatch& bt, const MgSel& S, int iterations, int sms, cudaStream_t st);
 // After V-cycle `cycle`: the FP64 sums of squares of the finest level's residual (and, after
 // the first, of its right-hand side) over the unknowns, then each simulation's convergence

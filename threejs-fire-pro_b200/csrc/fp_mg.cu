@@ -396,9 +396,9 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
             bool staged = !(P.ground && H.by < 0);
             float v[8];
 #pragma unroll
-            for (int k = 0; k < 8; k++) {
-              int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
-              v[k] = fast     ? st[((iz + dz - oz) * S + (iy + dy - oy)) * S + (ix + dx - ox)]
+            for (int q = 0; q < 8; q++) {
+              int dx = q & 1, dy = (q >> 1) & 1, dz = q >> 2;
+              v[q] = fast     ? st[((iz + dz - oz) * S + (iy + dy - oy)) * S + (ix + dx - ox)]
                      : staged ? ghost(ix + dx, iy + dy, iz + dz)
                               : coarseValue(P, H, A.coarse, A.level + 1, ix + dx, iy + dy, iz + dz);
             }
@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(64) k_level_tiles(FpBatch bt, MgSel Sl) {
   for (uint32_t item = blockIdx.x * NT + g; item < total; item += gridDim.x * NT) {
     uint32_t local;
     const SimParams& P = workSim(bt, FP_WORK_TILES, item, local);
-    const int t = (int)local;
+    const int t = P.liveTiles[local];
     const Args A = resolve(P, Sl);
     if (A.skip) continue;
     int4 rec = __ldg(&P.tileRec[t]);
@@ -477,11 +477,11 @@ __global__ void __launch_bounds__(64) k_level_tiles(FpBatch bt, MgSel Sl) {
 }
 
 // relaxCoarse (pressure.wgsl:549-599): the bottom level, one cell per tile slot, every
-// iteration in one CTA; a CTA per simulation. Tile slots stride over the threads. When 28
-// bytes a slot fit `smemBytes`, each slot's flags (SOLIDF where it is no unknown), right-hand
-// side, face neighbours and a ping-pong pair of values live in shared memory; else the values
-// ping-pong between the level's two pressure buffers in global memory (same arithmetic, same
-// order).
+// iteration in one CTA; a CTA per simulation. The live tiles stride over the threads. When 28
+// bytes a live tile fit `smemBytes`, each one's flags (SOLIDF where it is no unknown),
+// right-hand side, face neighbours (as live positions) and a ping-pong pair of values live in
+// shared memory; else the values ping-pong between the level's two pressure buffers in global
+// memory by slot (same arithmetic, same order).
 __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int iterations, int smemBytes) {
   extern __shared__ float bottomSmem[];
   const int nbIndex[6] = {nbrIndex(1, 0, 0), nbrIndex(-1, 0, 0), nbrIndex(0, 1, 0),
@@ -491,54 +491,83 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
     const SimParams& P = bt.sims[sim];
     const Args A = resolve(P, Sl);
     if (A.skip) continue;  // the same for the whole CTA
-    const int level = A.level;
-    int cap = P.capacity;
-    bool inShared = (long)cap * 28 <= (long)smemBytes;
-    // In global memory: cur starts in pout (a copy of pin), nxt is pin's buffer; both hold the
-    // level's storage type (gN). Shared memory holds FP32.
-    float* cur = inShared ? bottomSmem : A.pout;
-    float* nxt = inShared ? bottomSmem + cap : const_cast<float*>(A.pin);
-    const bool gN = !inShared && A.poutN;
-    float* rhsSm = bottomSmem + 2 * cap;
-    uint32_t* flags = inShared ? reinterpret_cast<uint32_t*>(bottomSmem + 3 * cap) : nullptr;
-    int16_t* nbSm = reinterpret_cast<int16_t*>(bottomSmem + 4 * cap);  // 6 a slot
-    auto flagOf = [&](int t) -> uint32_t {
+    const int level = A.level, L = P.liveCount;
+    auto flagOf = [&](int t) -> uint32_t {  // t is live
       int4 rec = __ldg(&P.tileRec[t]);
-      uint32_t f = SOLIDF | (rec.w != 0 ? 0x80000000u : 0u);  // top bit: a live tile slot
-      if (rec.w != 0) {
-        Home H = enterTile(P, t, rec);
-        if (activeCell(P, H, rec.x, rec.y, rec.z, level)) f = expandFlags(P.topo[level][t]) | 0x80000000u;
-      }
-      return f;
+      Home H = enterTile(P, t, rec);
+      return (activeCell(P, H, rec.x, rec.y, rec.z, level) ? expandFlags(P.topo[level][t]) : SOLIDF) | 0x80000000u;
     };
-    for (int t = threadIdx.x; t < cap; t += blockDim.x) {
-      uint32_t f = flagOf(t);
-      // Cells that are no unknown are never read and become zero in the first iteration.
-      if (inShared) {
-        flags[t] = f;
-        rhsSm[t] = ldBf(A.rhs, t, A.rhsN);
-        for (int k = 0; k < 6; k++)
-          nbSm[t * 6 + k] = (int16_t)(((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1);
+    if ((long)L * 28 <= (long)smemBytes) {
+      float* cur = bottomSmem;
+      float* nxt = cur + L;
+      float* rhs = nxt + L;
+      uint32_t* flags = reinterpret_cast<uint32_t*>(rhs + L);
+      int16_t* nb = reinterpret_cast<int16_t*>(flags + L);  // 6 a tile
+      for (int j = threadIdx.x; j < L; j += blockDim.x) {
+        const int t = P.liveTiles[j];
+        const uint32_t f = flagOf(t);
+        flags[j] = f;
+        rhs[j] = ldBf(A.rhs, t, A.rhsN);
+        for (int k = 0; k < 6; k++) {
+          int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
+          nb[j * 6 + k] = (int16_t)(n >= 0 ? P.tileIndex[n] : -1);
+        }
+        // Cells that are no unknown are never read and become zero in the first iteration.
+        cur[j] = !(f & SOLIDF) ? ldBf(A.pin, t, A.pinN) : 0.f;
       }
+      __syncthreads();
+      for (int it = 0; it < iterations; it++) {
+        for (int j = threadIdx.x; j < L; j += blockDim.x) {
+          const uint32_t f = flags[j];
+          float next = 0.f;
+          if (!(f & SOLIDF)) {
+            float w[6];
+#pragma unroll
+            for (int k = 0; k < 6; k++) {
+              const int n = nb[j * 6 + k];
+              w[k] = n >= 0 ? cur[n] : 0.f;
+            }
+            float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
+            float cand = (sum - rhs[j]) / fmaxf(diagOf(f & 63u), 1e-12f);
+            next = mixf(cur[j], cand, 0.8f);
+          }
+          nxt[j] = next;
+        }
+        __syncthreads();
+        float* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+      }
+      for (int j = threadIdx.x; j < L; j += blockDim.x) stBf(A.pout, P.liveTiles[j], cur[j], A.poutN);
+      __syncthreads();
+      continue;
+    }
+    // In global memory: cur starts in pout (a copy of pin), nxt is pin's buffer; both hold the
+    // level's storage type.
+    float* cur = A.pout;
+    float* nxt = const_cast<float*>(A.pin);
+    const bool gN = A.poutN;
+    for (int j = threadIdx.x; j < L; j += blockDim.x) {
+      const int t = P.liveTiles[j];
+      const uint32_t f = flagOf(t);
       // pin and pout are the level's two buffers: the copy into pout reads no value it wrote.
-      stBf(cur, t, (f & 0x80000000u) && !(f & SOLIDF) ? ldBf(A.pin, t, A.pinN) : 0.f, gN);
+      stBf(cur, t, !(f & SOLIDF) ? ldBf(A.pin, t, A.pinN) : 0.f, gN);
     }
     __syncthreads();
     for (int it = 0; it < iterations; it++) {
-      for (int t = threadIdx.x; t < cap; t += blockDim.x) {
-        uint32_t f = inShared ? flags[t] : flagOf(t);
+      for (int j = threadIdx.x; j < L; j += blockDim.x) {
+        const int t = P.liveTiles[j];
+        const uint32_t f = flagOf(t);
         float next = 0.f;
-        if ((f & 0x80000000u) && !(f & SOLIDF)) {
+        if (!(f & SOLIDF)) {
           float w[6];
 #pragma unroll
           for (int k = 0; k < 6; k++) {
-            int n = inShared ? (int)nbSm[t * 6 + k]
-                             : (((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1);
+            int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
             w[k] = n >= 0 ? ldBf(cur, n, gN) : 0.f;
           }
           float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
-          float rhs = inShared ? rhsSm[t] : ldBf(A.rhs, t, A.rhsN);
-          float cand = (sum - rhs) / fmaxf(diagOf(f & 63u), 1e-12f);
+          float cand = (sum - ldBf(A.rhs, t, A.rhsN)) / fmaxf(diagOf(f & 63u), 1e-12f);
           next = mixf(ldBf(cur, t, gN), cand, 0.8f);
         }
         stBf(nxt, t, next, gN);
@@ -548,10 +577,11 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
       cur = nxt;
       nxt = tmp;
     }
-    for (int t = threadIdx.x; t < cap; t += blockDim.x) {
-      uint32_t f = inShared ? flags[t] : flagOf(t);
-      if ((f & 0x80000000u) && cur != A.pout) stBf(A.pout, t, ldBf(cur, t, gN), A.poutN);
-    }
+    if (cur != A.pout)
+      for (int j = threadIdx.x; j < L; j += blockDim.x) {
+        const int t = P.liveTiles[j];
+        stBf(A.pout, t, ldBf(cur, t, gN), A.poutN);
+      }
     __syncthreads();
   }
 }
@@ -562,26 +592,26 @@ FP_DEV float bfRound(float v, bool narrow) { return narrow ? __bfloat162float(__
 // The second tile level (2^3 cells a tile) and the bottom (one cell a tile) in one CTA per
 // simulation: the V-cycle from level bl + 1 down (two relaxations, restriction to the bottom,
 // the bottom's iterations, prolongation, three relaxations), with both levels' iterates,
-// right-hand sides and flags in shared memory by tile slot, __syncthreads between sweeps.
+// right-hand sides and flags in shared memory by live tile, __syncthreads between sweeps.
 // The arithmetic and its order are those of k_level_tiles (relaxCell, restrictCell,
 // prolongCell) and k_bottom; every value a level stores is rounded as its storage rounds it.
 //   A.level: level bl + 1; A.rhs its right-hand side; A.pin its first iterate; A.pout where
 //   its result goes; A.cfirst: the bottom's result (read back by the prolongation).
-constexpr int COARSE_SLOT_BYTES = 8 * 3 * 4 + 8 + 3 * 4 + 4;  // per tile slot
+constexpr int COARSE_SLOT_BYTES = 8 * 3 * 4 + 8 + 3 * 4 + 4 + 6 * 2;  // per live tile
 constexpr int COARSE_SMEM = 224 * 1024;
 constexpr uint32_t LIVE = 0x80000000u;
 constexpr uint8_t UNKNOWN = 0x80;  // level bl + 1 flag byte: activeCell; bit 6 solid; 0-5 open
 
 // The level bl + 1 cell next to cell o of tile t on side k (+x, -x, +y, -y, +z, -z), as an
 // index of the level's tile-slot arrays; -1 without a tile there.
-FP_DEV int coarseNbr(const SimParams& P, int t, int o, int k) {
-  int l[3] = {o & 1, (o >> 1) & 1, o >> 2}, d[3] = {0, 0, 0};
+// `faces` holds each live tile's six face neighbours as live positions (-1 without one).
+FP_DEV int coarseNbr(const int16_t* faces, int j, int o, int k) {
+  int l[3] = {o & 1, (o >> 1) & 1, o >> 2};
   const int ax = k >> 1, step = (k & 1) ? -1 : 1;
   int v = l[ax] + step;
-  if (v < 0 || v > 1) d[ax] = step;
   l[ax] = v & 1;
-  int nt = d[ax] == 0 ? t : __ldg(&P.tileNbr[t * 27 + nbrIndex(d[0], d[1], d[2])]);
-  return nt < 0 ? -1 : nt * 8 + ((l[2] * 2 + l[1]) * 2 + l[0]);
+  const int nj = (v < 0 || v > 1) ? faces[j * 6 + k] : j;
+  return nj < 0 ? -1 : nj * 8 + ((l[2] * 2 + l[1]) * 2 + l[0]);
 }
 
 __global__ void __launch_bounds__(1024) k_coarse(FpBatch bt, MgSel Sl, int iterations) {
@@ -593,40 +623,41 @@ __global__ void __launch_bounds__(1024) k_coarse(FpBatch bt, MgSel Sl, int itera
     const SimParams& P = bt.sims[sim];
     const Args A = resolve(P, Sl);
     if (A.skip) continue;  // the same for the whole CTA
-    const int L = A.level, BL = L + 1, cap = P.capacity, n4 = cap * 8;
-    if ((long)cap * COARSE_SLOT_BYTES > COARSE_SMEM) continue;  // the host sizes batches to fit
+    // Shared arrays by live position j (tile slot P.liveTiles[j]); level L cells at j * 8 + o.
+    const int L = A.level, BL = L + 1, nt = P.liveCount, n4 = nt * 8;
+    if ((long)nt * COARSE_SLOT_BYTES > COARSE_SMEM) continue;  // the host sizes batches to fit
     const bool nL = narrowLevel(P, L), nB = narrowLevel(P, BL);
     float* pa = coarseSmem;  // level L: iterates, right-hand side
     float* pb = pa + n4;
     float* rh = pb + n4;
     float* ca = rh + n4;  // bottom: iterates, right-hand side
-    float* cb = ca + cap;
-    float* cr = cb + cap;
-    uint32_t* fb = reinterpret_cast<uint32_t*>(cr + cap);
-    uint8_t* fl = reinterpret_cast<uint8_t*>(fb + cap);
+    float* cb = ca + nt;
+    float* cr = cb + nt;
+    uint32_t* fb = reinterpret_cast<uint32_t*>(cr + nt);
+    uint8_t* fl = reinterpret_cast<uint8_t*>(fb + nt);
+    int16_t* faces = reinterpret_cast<int16_t*>(fl + n4);  // six a live tile
+    for (int q = threadIdx.x; q < nt * 6; q += blockDim.x) {
+      const int j = q / 6, k = q % 6;
+      const int n = __ldg(&P.tileNbr[P.liveTiles[j] * 27 + nbIndex[k]]);
+      faces[q] = (int16_t)(n >= 0 ? P.tileIndex[n] : -1);
+    }
     for (int c = threadIdx.x; c < n4; c += blockDim.x) {
-      const int t = c >> 3, o = c & 7;
+      const int t = P.liveTiles[c >> 3], o = c & 7;
+      const long a = (long)t * 8 + o;  // the cell's storage
       int4 rec = __ldg(&P.tileRec[t]);
-      uint8_t f = 0;
-      float p = 0.f, r = 0.f;
-      if (rec.w != 0) {
-        Home H = enterTile(P, t, rec);
-        int px = rec.x * 2 + (o & 1), py = rec.y * 2 + ((o >> 1) & 1), pz = rec.z * 2 + (o >> 2);
-        f = (uint8_t)(P.topo[L][c] | (activeCell(P, H, px, py, pz, L) ? UNKNOWN : 0));
-        p = ldBf(A.pin, c, nL);
-        r = ldBf(A.rhs, c, nL);
-      }
-      fl[c] = f;
-      pa[c] = p;
-      rh[c] = r;
+      Home H = enterTile(P, t, rec);
+      int px = rec.x * 2 + (o & 1), py = rec.y * 2 + ((o >> 1) & 1), pz = rec.z * 2 + (o >> 2);
+      fl[c] = (uint8_t)(P.topo[L][a] | (activeCell(P, H, px, py, pz, L) ? UNKNOWN : 0));
+      pa[c] = ldBf(A.pin, a, nL);
+      rh[c] = ldBf(A.rhs, a, nL);
     }
     __syncthreads();
-    // stencil (pressure.wgsl:360-402) of level L from `src`.
-    auto sumL = [&](const float* src, int t, int o, uint32_t f) {
+    // stencil (pressure.wgsl:360-402) of level L from `src`, cell o of live position j.
+    auto sumL = [&](const float* src, int j, int o, uint32_t f) {
       float w[6];
 #pragma unroll
       for (int k = 0; k < 6; k++) {
-        int n = ((f >> k) & 1u) ? coarseNbr(P, t, o, k) : -1;
+        int n = ((f >> k) & 1u) ? coarseNbr(faces, j, o, k) : -1;
         w[k] = n >= 0 ? src[n] : 0.f;
       }
       return (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
@@ -647,19 +678,19 @@ __global__ void __launch_bounds__(1024) k_coarse(FpBatch bt, MgSel Sl, int itera
     relax(pa, pb);
     relax(pb, pa);
     // restrictCell into the bottom (one cell a tile), its first iterate and k_bottom's flags.
-    for (int t = threadIdx.x; t < cap; t += blockDim.x) {
-      int4 rec = __ldg(&P.tileRec[t]);
+    for (int j = threadIdx.x; j < nt; j += blockDim.x) {
+      const int t = P.liveTiles[j];
       float r = 0.f, first = 0.f;
       uint32_t f = SOLIDF;
-      if (rec.w != 0) {
+      {
         float residual = 0.f;
         bool every = true;
         for (int k = 0; k < 8; k++) {
-          const int c = t * 8 + k;
+          const int c = j * 8 + k;
           const uint8_t fk = fl[c];
           every = every && (fk & UNKNOWN);
           if ((fk & UNKNOWN) && !(fk & FP_STORED_SOLID))
-            residual += rh[c] - (sumL(pa, t, k, fk & 63u) - diagOf(fk & 63u) * pa[c]);
+            residual += rh[c] - (sumL(pa, j, k, fk & 63u) - diagOf(fk & 63u) * pa[c]);
         }
         r = residual * 0.5f;
         const uint8_t tb = P.topo[BL][t];
@@ -667,42 +698,41 @@ __global__ void __launch_bounds__(1024) k_coarse(FpBatch bt, MgSel Sl, int itera
         // activeCell at the bottom covers the tile's 64 bricks: every cell above is an unknown.
         f = (every ? expandFlags(tb) : SOLIDF) | LIVE;
       }
-      cr[t] = bfRound(r, nB);
-      ca[t] = (f & LIVE) && !(f & SOLIDF) ? bfRound(first, nB) : 0.f;
-      fb[t] = f;
+      cr[j] = bfRound(r, nB);
+      ca[j] = !(f & SOLIDF) ? bfRound(first, nB) : 0.f;
+      fb[j] = f;
     }
     __syncthreads();
     // relaxCoarse (pressure.wgsl:549-599): FP32 iterates in shared memory.
     float* cur = ca;
     float* nxt = cb;
     for (int it = 0; it < iterations; it++) {
-      for (int t = threadIdx.x; t < cap; t += blockDim.x) {
-        const uint32_t f = fb[t];
+      for (int j = threadIdx.x; j < nt; j += blockDim.x) {
+        const uint32_t f = fb[j];
         float next = 0.f;
-        if ((f & LIVE) && !(f & SOLIDF)) {
+        if (!(f & SOLIDF)) {
           float w[6];
 #pragma unroll
           for (int k = 0; k < 6; k++) {
-            int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
+            const int n = ((f >> k) & 1u) ? faces[j * 6 + k] : -1;
             w[k] = n >= 0 ? cur[n] : 0.f;
           }
           float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
-          float cand = (sum - cr[t]) / fmaxf(diagOf(f & 63u), 1e-12f);
-          next = mixf(cur[t], cand, 0.8f);
+          float cand = (sum - cr[j]) / fmaxf(diagOf(f & 63u), 1e-12f);
+          next = mixf(cur[j], cand, 0.8f);
         }
-        nxt[t] = next;
+        nxt[j] = next;
       }
       __syncthreads();
       float* tmp = cur;
       cur = nxt;
       nxt = tmp;
     }
-    for (int t = threadIdx.x; t < cap; t += blockDim.x)
-      if (fb[t] & LIVE) stBf(A.cfirst, t, cur[t], nB);
+    for (int j = threadIdx.x; j < nt; j += blockDim.x) stBf(A.cfirst, P.liveTiles[j], cur[j], nB);
     __syncthreads();
     // prolongCell at level L from the bottom's stored result, pa -> pb.
     for (int c = threadIdx.x; c < n4; c += blockDim.x) {
-      const int t = c >> 3, o = c & 7;
+      const int t = P.liveTiles[c >> 3], o = c & 7;
       const uint8_t f = fl[c];
       float out = 0.f;
       if ((f & UNKNOWN) && !(f & FP_STORED_SOLID)) {
@@ -731,8 +761,7 @@ __global__ void __launch_bounds__(1024) k_coarse(FpBatch bt, MgSel Sl, int itera
     relax(pb, pa);
     relax(pa, pb);
     relax(pb, pa);
-    for (int c = threadIdx.x; c < n4; c += blockDim.x)
-      if (__ldg(&P.tileRec[c >> 3]).w != 0) stBf(A.pout, c, pa[c], nL);
+    for (int c = threadIdx.x; c < n4; c += blockDim.x) stBf(A.pout, (long)P.liveTiles[c >> 3] * 8 + (c & 7), pa[c], nL);
     __syncthreads();
   }
 }
@@ -873,7 +902,7 @@ __global__ void __launch_bounds__(64) k_tile_masks(FpBatch bt) {
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t local;
     const SimParams& P = workSim(bt, FP_WORK_TILES, item, local);
-    const int t = (int)local;
+    const int t = P.liveTiles[local];
     const size_t id = (size_t)t * 64 + threadIdx.x;
     bool on = __ldg(&P.tileRec[t]).w != 0 && P.entries[id] >= 0 && P.records[id * FP_RECORD_WORDS + 27] != 0;
     uint32_t half = __ballot_sync(0xffffffffu, on);
@@ -888,7 +917,7 @@ __global__ void __launch_bounds__(64) k_topo_tiles(FpBatch bt) {
     uint32_t local;
     const SimParams& P = workSim(bt, FP_WORK_TILES, item, local);
     if (!P.topoAll) continue;
-    int t = (int)local;
+    int t = P.liveTiles[local];
     int4 rec = __ldg(&P.tileRec[t]);
     if (rec.w == 0) continue;
     Home H = enterTile(P, t, rec);
@@ -1004,7 +1033,7 @@ void fp_launch_prolong(const FpBatch& bt, const MgSel& S, bool tiles, int B, int
 void fp_launch_bottom(const FpBatch& bt, const MgSel& S, int iterations, int sms, cudaStream_t st) {
   k_bottom<<<sms, 1024, BOTTOM_SMEM, st>>>(bt, S, iterations, BOTTOM_SMEM);
 }
-bool fp_coarse_fits(int capacity) { return (long)capacity * COARSE_SLOT_BYTES <= COARSE_SMEM; }
+bool fp_coarse_fits(int liveTiles) { return (long)liveTiles * COARSE_SLOT_BYTES <= COARSE_SMEM; }
 void fp_launch_coarse(const FpBatch& bt, const MgSel& S, int iterations, int sms, cudaStream_t st) {
   k_coarse<<<sms, 1024, COARSE_SMEM, st>>>(bt, S, iterations);
 }

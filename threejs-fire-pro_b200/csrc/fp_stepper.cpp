@@ -211,12 +211,12 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
   for (int i = 0; i < count; i++) {
     Engine* e = sims[i];
     uint32_t cap = (uint32_t)e->capacity();
-    fusedCoarse_ = fusedCoarse_ && fp_coarse_fits((int)cap);
+    fusedCoarse_ = fusedCoarse_ && fp_coarse_fits(e->liveTiles());
     rowBlocks[i] = blocks;
     rowTiles[i] = tiles;
     rowIds[i] = ids;
     blocks += (cap * 64 + 255) / 256;
-    tiles += cap;
+    tiles += (uint32_t)e->liveTiles();  // the tile-level kernels walk the live tiles
     ids += cap * 64;
     SimParams* P = reinterpret_cast<SimParams*>(arenaH_ + paramsOff) + i;
     e->writeStep(*P, arenaH_, arenaD_, off, *frames[i], dts[i], readD_ + word, noise());

@@ -122,6 +122,9 @@ struct SimParams {
   const int4* tileRec;
   const int* tileNbr;
   uint64_t* tileMask;  // per tile slot, each step: bit l when brick l of the tile computes
+  const int* liveTiles;  // the live tile slots, ascending (liveCount of them)
+  const int* tileIndex;  // per tile slot: its position in liveTiles, -1 when not live
+  int liveCount;
   const int4* hash;
   uint32_t hashMask;
   // per brick id
@@ -183,7 +186,7 @@ struct SimParams {
 // bricks and granted slots by the allocation on the device.
 enum FpWork {
   FP_WORK_IDBLOCKS,  // blocks of 256 brick ids
-  FP_WORK_TILES,     // tile slots
+  FP_WORK_TILES,     // live tile slots (through SimParams::liveTiles)
   FP_WORK_IDS,       // brick ids
   FP_WORK_ACTIVE,    // computing bricks
   FP_WORK_FRESH,     // slots granted this step
