@@ -59,7 +59,7 @@ typedef struct fp_grid {
   float voxel_size;        /* meters, [0.0001, 16] */
   int32_t velocity_divisor;/* 1 (the reference also allows 2 and 4) */
   int32_t brick_size;      /* fine cells per brick side: 8 or 16 */
-  int32_t smoke_divisor;   /* 1 (the reference also allows 2 and 4) */
+  int32_t smoke_divisor;   /* 1, 2 or 4: smoke density on a grid that many times coarser */
   int32_t scalar_maccormack; /* bounded MacCormack scalar transport: 0 or 1 */
   int32_t precision;       /* FP_PRECISION_* */
   double voxel_budget;     /* grid.maxVoxels; 0 means the reference default 8,000,000 */
@@ -201,6 +201,9 @@ typedef struct fp_phase {
 #define FP_FIELD_PRESSURE 3   /* 1 channel: the latest solution */
 #define FP_FIELD_DIVERGENCE 4 /* 1 channel: the Poisson right-hand side */
 #define FP_FIELD_CURL 5       /* 4 channels: curl xyz and magnitude */
+#define FP_FIELD_SMOKE 6      /* 1 channel on the coarse smoke grid (smoke_divisor d > 1): (B/d)^3
+                                 cells a slot; with coarse smoke the smoke channel of
+                                 FP_FIELD_SCALARS holds only the step's source production */
 
 /* Integer tables a test may copy out (`fp_sim_read_table`), bit-exact against the oracle. */
 #define FP_TABLE_ENTRIES 0     /* int32 per brick id: slot | FRESH (0x2000000), or -1 */

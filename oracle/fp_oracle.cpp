@@ -261,6 +261,12 @@ struct Sim {
   std::vector<R> sb;                           // scalar bounds [slot][8][N]
   std::vector<int32_t> vdonor;                 // velocity donor bases [slot][3][N][3]
   std::vector<uint32_t> solids;                // [slot][W]
+  // Coarse smoke (smokeDivisor d > 1, smoke.wgsl): density on its own grid of SB = B/d cells
+  // a brick side at spacing sp = h d; smk the state, smkP the predictor, smkN the evolved,
+  // smkBnd the donors' min and max [slot][2][SN].
+  int smokeDiv = 1, SB = 0, sshift = 0, SN = 0;
+  R sp = 0;
+  std::vector<R> smk, smkP, smkN, smkBnd;
   // multigrid: per level p (ping-pong), rhs, topology
   struct Level {
     std::vector<R> p[2], rhs;
@@ -304,6 +310,12 @@ struct Sim {
     h = (R)(float)g.voxel_size;
     maccormack = g.scalar_maccormack != 0;
     prec = p;
+    smokeDiv = g.smoke_divisor > 1 ? g.smoke_divisor : 1;
+    SB = B / smokeDiv;
+    sshift = 0;
+    while ((1 << sshift) < SB) sshift++;
+    SN = SB * SB * SB;
+    sp = h * (R)smokeDiv;  // voxelSize x smokeDivisor: a power of two, exact
     brickLevels = shift;
     bottom = brickLevels + 2;
     if (g.voxel_budget > 0) voxelBudget = g.voxel_budget;
@@ -348,6 +360,10 @@ struct Sim {
     sb.resize(s * 8 * N, 0);
     vdonor.resize(s * 3 * N * 3, 0);
     solids.resize(s * W, 0);
+    if (smokeDiv > 1) {
+      smk.resize(s * SN, 0); smkP.resize(s * SN, 0); smkN.resize(s * SN, 0);
+      smkBnd.resize(s * 2 * SN, 0);
+    }
     pres[0].resize(s * N, 0); pres[1].resize(s * N, 0);
     levels.resize(bottom + 1);
     levels[0].topo.resize(s * N, 0);
@@ -488,6 +504,32 @@ struct Sim {
         for (int x = 0; x < 2; x++) {
           R w = (x ? f[0] : R(1) - f[0]) * (y ? f[1] : R(1) - f[1]) * (z ? f[2] : R(1) - f[2]);
           value += cellAt(pool, ch, c, b[0] + x, b[1] + y, b[2] + z) * w;
+        }
+    return value;
+  }
+  // The coarse smoke grid (fluid-sampling.wgsl:4-20: each grid shares the brick footprint,
+  // with its own cells per side): cell (x,y,z) of a [slot][SN] pool, zero without a slot, and
+  // the trilinear sample at `q` in its cell units, centres at .5.
+  R coarseCell(const std::vector<R>& pool, int x, int y, int z) {
+    int slot = brickSlot(x >> sshift, y >> sshift, z >> sshift);
+    if (slot < 0) return 0;
+    int m = SB - 1;
+    return pool[(size_t)slot * SN + ((z & m) * SB + (y & m)) * SB + (x & m)];
+  }
+  R coarseSample(const std::vector<R>& pool, R px, R py, R pz) {
+    R q[3] = {px - R(0.5), py - R(0.5), pz - R(0.5)};
+    int b[3];
+    R f[3];
+    for (int a = 0; a < 3; a++) {
+      b[a] = floori((double)q[a]);
+      f[a] = q[a] - (R)b[a];
+    }
+    R value = 0;
+    for (int z = 0; z < 2; z++)
+      for (int y = 0; y < 2; y++)
+        for (int x = 0; x < 2; x++) {
+          R w = (x ? f[0] : R(1) - f[0]) * (y ? f[1] : R(1) - f[1]) * (z ? f[2] : R(1) - f[2]);
+          value += coarseCell(pool, b[0] + x, b[1] + y, b[2] + z) * w;
         }
     return value;
   }
@@ -1417,6 +1459,8 @@ struct Sim {
       std::fill(vel.begin() + s * 3 * N, vel.begin() + (s + 1) * 3 * N, R(0));
       std::fill(fld.begin() + s * 4 * N, fld.begin() + (s + 1) * 4 * N, R(0));
       std::fill(expn.begin() + s * N, expn.begin() + (s + 1) * N, R(0));
+      if (smokeDiv > 1)  // zeroSmokeBricks (smoke.wgsl:188-223): all three smoke pools
+        for (auto* pool : {&smk, &smkP, &smkN}) std::fill(pool->begin() + s * SN, pool->begin() + (s + 1) * SN, R(0));
     }
   }
 
@@ -1571,6 +1615,8 @@ struct Sim {
         out[2] = lifetimeZero ? R(0) : value[2];
         out[3] = value[3];
       }
+      // With coarse smoke the fine X channel carries no density (fluid-scalar-transport.wgsl:127, :137).
+      if (smokeDiv > 1) out[0] = 0;
       for (int k = 0; k < 4; k++) fldP[((size_t)slot * 4 + k) * N + c] = ss(out[k]);
     });
   }
@@ -1698,6 +1744,9 @@ struct Sim {
               tr[0] = bd[0]; tr[1] = bd[1]; tr[2] = clampr(lifetime, R(0), R(1)); tr[3] = bd[2];
             }
           }
+          // With coarse smoke the fine X channel stages only this step's source production
+          // (fluid-scalar-transport.wgsl:190-199).
+          if (smokeDiv > 1) tr[0] = 0;
           // The corrected scalars as the half-float field held them.
           for (int k = 0; k < 4; k++) tr[k] = prec.truncate ? (R)truncate_half((double)tr[k]) : ss(tr[k]);
           R lifetime = tr[2];
@@ -1740,8 +1789,9 @@ struct Sim {
         for (int k = 0; k < 4; k++) fldN[((size_t)slot * 4 + k) * N + c] = ss(value[k]);
         expn[(size_t)slot * N + c] = store_round(expansion, prec.expn);
         if (expansion != 0) expands = true;
-        // holdsContent (fluid-content.wgsl:22-24) tests the value before its store rounds.
-        if (std::max(std::max(value[0], value[2]), value[3]) > (R)cutoff) {
+        // holdsContent (fluid-content.wgsl:22-24) tests the value before its store rounds; the
+        // fine X channel counts only without coarse smoke.
+        if (std::max(std::max(smokeDiv > 1 ? R(0) : value[0], value[2]), value[3]) > (R)cutoff) {
           V3<R> v = traceVel();
           busy |= contentSupport(x, y, z, v);
         }
@@ -1777,12 +1827,137 @@ struct Sim {
     uint32_t plane = (row << 3u) | (low[1] ? row : 0u) | (high[1] ? (row << 6u) : 0u);
     return (plane << 9u) | (low[2] ? plane : 0u) | (high[2] ? (plane << 18u) : 0u);
   }
+  // ---------------------------------------------------------------- coarse smoke
+  // Cell `c` of the coarse grid in brick id `b`; its centre in world units.
+  I3 coarseCellOf(I3 b, int c) const {
+    return I3{b[0] * SB + (c & (SB - 1)), b[1] * SB + ((c >> sshift) & (SB - 1)), b[2] * SB + (c >> (2 * sshift))};
+  }
+  V3<R> coarseCenter(I3 q) const {
+    return v3<R>((R(q[0]) + R(0.5)) * sp, (R(q[1]) + R(0.5)) * sp, (R(q[2]) + R(0.5)) * sp);
+  }
+  // advectSmoke (smoke.wgsl:101-124): the RK2 back trace of each coarse cell's centre through
+  // the start-of-step velocity, the predictor sampled there and (MacCormack) the donors' range,
+  // smokeDonorBounds (:63-77): min from 1e30 and max from 0 over the 2x2x2 block.
+  void advectSmoke() {
+    long n = (long)active.size();
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long i = 0; i < n; i++) {
+      uint32_t id = active[i];
+      size_t slot = (size_t)entryPage(entries[id]);
+      I3 b = brickOf(id);
+      for (int c = 0; c < SN; c++) {
+        I3 q = coarseCellOf(b, c);
+        V3<R> pos = coarseCenter(q);
+        R density = 0;
+        if (!solidAt(pos[0], pos[1], pos[2])) {
+          V3<R> dep = trace(pos, velocityAt(pos), R(-1));
+          density = coarseSample(smk, dep[0] / sp, dep[1] / sp, dep[2] / sp);
+          if (maccormack) {
+            int base[3];
+            for (int a = 0; a < 3; a++) base[a] = floori((double)(dep[a] / sp - R(0.5)));
+            R lo = R(1e30), hi = 0;
+            for (int k = 0; k < 8; k++) {
+              R v = coarseCell(smk, base[0] + (k & 1), base[1] + ((k >> 1) & 1), base[2] + (k >> 2));
+              lo = std::min(lo, v);
+              hi = std::max(hi, v);
+            }
+            smkBnd[(slot * 2 + 0) * SN + c] = store_round(lo, prec.scal);
+            smkBnd[(slot * 2 + 1) * SN + c] = store_round(hi, prec.scal);
+          }
+        }
+        smkP[slot * SN + c] = ss(density);
+      }
+    }
+  }
+  // contentSupport (fluid-content.wgsl:29-39) on the smoke grid: SB cells a side, the pad in
+  // smoke cells (two at least).
+  uint32_t smokeSupport(I3 q, V3<R> v) {
+    bool low[3], high[3];
+    for (int a = 0; a < 3; a++) {
+      R side = R(SB);
+      R loc = R(q[a] & (SB - 1)) + R(0.5);
+      R pad = std::min(side, std::max(R(2), R(2) * (h / sp)) + std::fabs(v[a]) * dt / sp);
+      low[a] = loc < pad;
+      high[a] = loc + pad >= side;
+    }
+    uint32_t row = 2u | (low[0] ? 1u : 0u) | (high[0] ? 4u : 0u);
+    uint32_t plane = (row << 3u) | (low[1] ? row : 0u) | (high[1] ? (row << 6u) : 0u);
+    return (plane << 9u) | (low[2] ? plane : 0u) | (high[2] ? (plane << 18u) : 0u);
+  }
+  // evolveSmoke (smoke.wgsl:126-178): bounded MacCormack correction of the predictor, decay,
+  // the volume average of the fine cells' source production (smokeProduction :23-38, the mean
+  // of each 2x2x2 block of evolved fine fields), dormant clearing, content flags per brick.
+  void evolveSmoke() {
+    long n = (long)active.size();
+    std::vector<uint32_t> busyOut(n, 0);
+    const int blocks = smokeDiv / 2;
+    const R volume = R(smokeDiv * smokeDiv * smokeDiv / 8);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long i = 0; i < n; i++) {
+      uint32_t id = active[i];
+      size_t slot = (size_t)entryPage(entries[id]);
+      I3 b = brickOf(id);
+      uint32_t busy = 0;
+      for (int c = 0; c < SN; c++) {
+        I3 q = coarseCellOf(b, c);
+        V3<R> pos = coarseCenter(q);
+        R density = 0;
+        if (!solidAt(pos[0], pos[1], pos[2])) {
+          V3<R> cv = velocityAt(pos);
+          R predictor = smkP[slot * SN + c];
+          R bounded = predictor;
+          if (maccormack) {
+            R lo = smkBnd[(slot * 2 + 0) * SN + c], hi = smkBnd[(slot * 2 + 1) * SN + c];
+            if (lo != hi || predictor != lo) {
+              R original = smk[slot * SN + c];
+              V3<R> fwd = trace(pos, cv, R(1));
+              R reversed = coarseSample(smkP, fwd[0] / sp, fwd[1] / sp, fwd[2] / sp);
+              R corrected = predictor + R(0.5) * (original - reversed);
+              bounded = (corrected < lo || corrected > hi) ? predictor : corrected;
+            }
+          }
+          R transported = prec.truncate ? (R)truncate_half((double)bounded) : bounded;
+          R produced[4] = {0, 0, 0, 0};
+          for (int bz = 0; bz < blocks; bz++)
+            for (int by = 0; by < blocks; by++)
+              for (int bx = 0; bx < blocks; bx++) {
+                // The shared corner of a 2x2x2 block of fine cells: a trilinear sample there
+                // is the block's mean.
+                R fx = R(q[0] * smokeDiv + 2 * bx + 1), fy = R(q[1] * smokeDiv + 2 * by + 1),
+                  fz = R(q[2] * smokeDiv + 2 * bz + 1);
+                for (int k = 0; k < 4; k++) produced[k] += sampleCells(fld, 4, k, fx, fy, fz);
+              }
+          for (int k = 0; k < 4; k++) produced[k] /= volume;
+          density = std::max(R(0), transported * std::exp(-dissipation * dt) + produced[0]);
+          if (produced[0] == 0 && produced[2] == 0 && std::max(density, std::max(produced[1], produced[3])) < R(0.001))
+            density = 0;
+          if (density > (R)cutoff) busy |= smokeSupport(q, cv);
+        }
+        smkN[slot * SN + c] = ss(density);
+      }
+      busyOut[i] = busy;
+    }
+    // recordContent (fluid-content.wgsl:43-64)
+    for (long i = 0; i < n; i++) {
+      if (!busyOut[i]) continue;
+      uint32_t id = active[i];
+      uint32_t l = id & 63u;
+      uint32_t bits = (1u << (l & 3u)) | (16u << ((l >> 2) & 3u)) | (256u << (l >> 4));
+      activity[(size_t)capacity * 64 + (id >> 6)] |= bits;
+      activity[id] |= CONTENT | (busyOut[i] << 3);
+    }
+  }
   void transport() {
     advectVelocity();
     correctVelocity();
     advectScalars();
     evolveFields();
     fld.swap(fldN);
+    if (smokeDiv > 1) {
+      advectSmoke();
+      evolveSmoke();
+      smk.swap(smkN);
+    }
   }
 
   // ---------------------------------------------------------------- forces
@@ -1902,6 +2077,9 @@ struct Sim {
     V3<R> F = v3<R>(0, 0, 0);
     if (!solidAt(w[0], w[1], w[2])) {
       R heat = cellAt(fld, 4, 1, x, y, z), density = cellAt(fld, 4, 0, x, y, z);
+      // smokeVelocityAverage (smoke.wgsl:4-21) at one velocity cell per smoke spacing or less:
+      // the coarse density sampled at the cell centre.
+      if (smokeDiv > 1) density = coarseSample(smk, w[0] / sp, w[1] / sp, w[2] / sp);
       V3<R> conf = v3<R>(0, 0, 0);
       if (vorticity != 0) {
         R c[3] = {cellAt(curl, 4, 0, x, y, z), cellAt(curl, 4, 1, x, y, z), cellAt(curl, 4, 2, x, y, z)};
@@ -2528,6 +2706,7 @@ int64_t or_info(or_sim* s, int what) {
       case 6: return sim.poolLimited;
       case 7: return sim.lastFailures;
       case 8: return sim.dir.count();
+      case 9: return sim.SN;  // coarse smoke cells a brick (smokeDivisor > 1)
     }
     return -1;
   };
@@ -2546,6 +2725,7 @@ static int field_io(or_sim* s, int field, float* buf, size_t count, int write) {
       case FP_FIELD_PRESSURE: v = &sim.pres[sim.latest]; break;
       case FP_FIELD_DIVERGENCE: v = &sim.div; break;
       case FP_FIELD_CURL: v = &sim.curl; break;
+      case FP_FIELD_SMOKE: v = &sim.smk; break;
       default: return -1;
     }
     if (count != v->size()) return -2;
@@ -2573,6 +2753,7 @@ int or_read_field64(or_sim* s, int field, double* out, size_t count) {
     case FP_FIELD_PRESSURE: v = &sim.pres[sim.latest]; break;
     case FP_FIELD_DIVERGENCE: v = &sim.div; break;
     case FP_FIELD_CURL: v = &sim.curl; break;
+    case FP_FIELD_SMOKE: v = &sim.smk; break;
     default: return -1;
   }
   if (count != v->size()) return -2;

@@ -58,7 +58,8 @@ def lib():
     return _lib
 
 
-CHANNELS = {0: 3, 1: 4, 2: 1, 3: 1, 4: 1, 5: 4}
+CHANNELS = {0: 3, 1: 4, 2: 1, 3: 1, 4: 1, 5: 4, 6: 1}
+SMOKE_FIELD = 6  # the coarse smoke grid: (B / smoke_divisor)^3 cells a slot
 
 
 class OracleSim:
@@ -117,14 +118,15 @@ class OracleSim:
         return self.info(3)
 
     def field(self, fid: int, f64: bool = False) -> np.ndarray:
-        n = self.slots * CHANNELS[fid] * self.cells
+        cells = self.info(9) if fid == SMOKE_FIELD else self.cells
+        n = self.slots * CHANNELS[fid] * cells
         if f64:
             out = np.empty(n, np.float64)
             assert self.L.or_read_field64(self.h, fid, out.ctypes.data, n) == 0
         else:
             out = np.empty(n, np.float32)
             assert self.L.or_read_field(self.h, fid, out.ctypes.data, n) == 0
-        return out.reshape(self.slots, CHANNELS[fid], self.cells)
+        return out.reshape(self.slots, CHANNELS[fid], cells)
 
     def write_field(self, fid: int, arr: np.ndarray):
         a = np.ascontiguousarray(arr, np.float32).ravel()

@@ -107,6 +107,11 @@ def compare_fields(gpu, orc, slots: np.ndarray) -> dict:
         else:
             out[name] = rel_l2(a, b)
             out[name + "@trim"] = trimmed_rel_l2(a, b, k)
+    if getattr(gpu, "smoke_cells", 0):  # the coarse smoke grid (smoke_divisor > 1)
+        a = gpu.field(abi.FP_FIELD_SMOKE)[slots]
+        b = orc.field(abi.FP_FIELD_SMOKE, f64=orc.real == 0)[slots]
+        out["coarse_smoke"] = rel_l2(a, b)
+        out["coarse_smoke@trim"] = trimmed_rel_l2(a, b, k)
     return out
 
 
@@ -120,6 +125,8 @@ def force(gpu, orc):
     """Copy the CUDA state that carries into the next step into the oracle."""
     for fid in (abi.FP_FIELD_VELOCITY, abi.FP_FIELD_SCALARS, abi.FP_FIELD_EXPANSION):
         orc.write_field(fid, gpu.field(fid))
+    if getattr(gpu, "smoke_cells", 0):
+        orc.write_field(abi.FP_FIELD_SMOKE, gpu.field(abi.FP_FIELD_SMOKE))
     orc.write_activity(gpu.table(abi.FP_TABLE_ACTIVITY))
 
 

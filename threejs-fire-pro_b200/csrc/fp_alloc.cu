@@ -421,6 +421,12 @@ __global__ void __launch_bounds__(256) k_zero_fresh(FpBatch bt) {
     for (int k = threadIdx.x; k < 3 * P.N / 4; k += blockDim.x) v[k] = z;
     for (int k = threadIdx.x; k < P.N * scalarBytes / 4; k += blockDim.x) f[k] = z;
     for (int k = threadIdx.x; k < P.N / 4; k += blockDim.x) e[k] = z;
+    // Coarse smoke's state in the scalars' width (zeroSmokeBricks, smoke.wgsl:188-223); a
+    // slot's cells are a multiple of 16 bytes (at least 8 cells).
+    if (P.smokeDiv > 1) {
+      float4* s = reinterpret_cast<float4*>(reinterpret_cast<char*>(P.smk) + slot * P.smokeCells * scalarBytes);
+      for (int k = threadIdx.x; k < P.smokeCells * scalarBytes / 16; k += blockDim.x) s[k] = z;
+    }
   }
 }
 

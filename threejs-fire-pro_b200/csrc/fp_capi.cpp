@@ -52,7 +52,6 @@ static int validateGrid(const fp_grid* grid) {
   if (!(grid->voxel_budget >= 0) || !std::isfinite(grid->voxel_budget))
     return failed("voxel_budget must be a finite, nonnegative voxel count.", FP_EINVAL);
   if (vd != 1) return failed("velocityDivisor 2 and 4 are not implemented by this build.", FP_EUNSUPPORTED);
-  if (sd != 1) return failed("smokeDivisor 2 and 4 are not implemented by this build.", FP_EUNSUPPORTED);
   if (bs == 32) return failed("brickSize 32 is not implemented by this build.", FP_EUNSUPPORTED);
   return FP_OK;
 }

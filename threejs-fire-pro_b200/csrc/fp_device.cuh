@@ -159,6 +159,26 @@ FP_DEV float sampleCells(const SimParams& P, const Home& H, const float* pool, i
   return blend8(t, fx, fy, fz);
 }
 
+// The coarse smoke grid (fluid-sampling.wgsl:4-20: every grid shares the brick footprint with
+// its own cells a side, here 2^P.smokeShift): cell (x,y,z) of a [slot][smokeCells] pool, zero
+// in a brick without a slot, and the trilinear sample at `q` in its cells, centres at .5.
+FP_DEV float smokeCell(const SimParams& P, const Home& H, const float* pool, int x, int y, int z, bool half) {
+  const int sh = P.smokeShift, m = (1 << sh) - 1;
+  int s = brickSlot(P, H, x >> sh, y >> sh, z >> sh);
+  if (s < 0) return 0.f;
+  return ldHalf(pool, (size_t)s * P.smokeCells + ((((z & m) << sh) | (y & m)) << sh | (x & m)), half);
+}
+FP_DEV float smokeSample(const SimParams& P, const Home& H, const float* pool, float px, float py, float pz,
+                         bool half) {
+  float qx = px - 0.5f, qy = py - 0.5f, qz = pz - 0.5f;
+  float gx = floorf(qx), gy = floorf(qy), gz = floorf(qz);
+  int x0 = (int)gx, y0 = (int)gy, z0 = (int)gz;
+  float t[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) t[j] = smokeCell(P, H, pool, x0 + (j & 1), y0 + ((j >> 1) & 1), z0 + (j >> 2), half);
+  return blend8(t, qx - gx, qy - gy, qz - gz);
+}
+
 // solidCell (solids.wgsl:15-31): the ground, then colliders drawn into each slot's bits.
 FP_DEV bool solidCell(const SimParams& P, const Home& H, int x, int y, int z) {
   if (P.ground && y < 0) return true;

@@ -164,6 +164,11 @@ Engine::Engine(const fp_grid& g, Stepper* owner) : owner_(owner) {
   h_ = g.voxel_size;
   maccormack_ = g.scalar_maccormack != 0;
   precision_ = g.precision;
+  smokeDiv_ = g.smoke_divisor > 1 ? g.smoke_divisor : 1;
+  SB_ = B_ / smokeDiv_;
+  sshift_ = 0;
+  while ((1 << sshift_) < SB_) sshift_++;
+  SN_ = SB_ * SB_ * SB_;
   budget_ = g.voxel_budget > 0 ? g.voxel_budget : 8e6;
   measure_ = precision_ == FP_PRECISION_MIXED;  // mixed storage reports its accuracy every step
 }
@@ -198,6 +203,8 @@ void Engine::freeAll() {
     }
   for (auto& b : vel_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
   for (auto& b : fld_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
+  for (auto& b : smoke_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
+  if (smokeBnd_.ptr) { cudaFree(smokeBnd_.ptr); smokeBnd_ = DeviceBuffer{}; }
   for (auto& b : p0_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
   for (int l = 0; l < FP_MAX_LEVELS; l++) {
     if (topo_[l].ptr) { cudaFree(topo_[l].ptr); topo_[l] = DeviceBuffer{}; }
@@ -235,6 +242,7 @@ int Engine::initialize() {
   prevMasks_.clear();
   for (int k = 0; k < 4; k++) velIdx_[k] = k;
   for (int k = 0; k < 3; k++) fldIdx_[k] = k;
+  for (int k = 0; k < 3; k++) smokeIdx_[k] = k;
   return check(cudaStreamSynchronize(stream()), "initialize");
 }
 
@@ -253,6 +261,10 @@ uint64_t Engine::estimateBytes(const fp_grid& g, uint32_t tiles) {
   for (int l = 1; l < shift; l++) {
     uint64_t c = (uint64_t)1 << (3 * (shift - l));
     perSlot += c * (3 * narrow + 1);
+  }
+  if (g.smoke_divisor > 1) {  // coarse smoke: state pair, FP32 predictor, donor range
+    uint64_t d = (uint64_t)g.smoke_divisor;
+    perSlot += N / (d * d * d) * (2 * narrow + 4 + 8);
   }
   uint64_t perTile = 64 * (4 * 5 + FP_RECORD_WORDS * 4 + 8) + 16 + 27 * 4 + 16 + 8 + 8 + (64 + 8 + 1) * (3 * narrow + 1);
   return slots * perSlot + (uint64_t)std::max(tiles, (uint32_t)MIN_TILES) * perTile + 64 * 1024;
@@ -299,6 +311,10 @@ int Engine::allocatePools(uint32_t slots) {
     ok = alloc(lp_[l][0], c * coarseBytes()) && alloc(lp_[l][1], c * coarseBytes()) &&
          alloc(lrhs_[l], c * coarseBytes()) && alloc(topo_[l], c);
   }
+  // Coarse smoke: the state pair in the scalars' width, the FP32 predictor and donor range.
+  if (ok && smokeDiv_ > 1)
+    ok = alloc(smoke_[0], s * SN_ * scalarBytes()) && alloc(smoke_[1], s * SN_ * 4) &&
+         alloc(smoke_[2], s * SN_ * scalarBytes()) && alloc(smokeBnd_, s * 2 * SN_ * 4);
   if (!ok) return FP_ENOMEM;
   std::vector<uint32_t> stack(slots);
   for (uint32_t i = 0; i < slots; i++) stack[i] = slots - 1 - i;
@@ -329,6 +345,9 @@ int Engine::growPool(uint32_t target) {
     ok = grow(lp_[l][0], c * coarseBytes(), 0) && grow(lp_[l][1], c * coarseBytes(), 0) &&
          grow(lrhs_[l], c * coarseBytes(), 0) && grow(topo_[l], c, 0);
   }
+  if (ok && smokeDiv_ > 1)
+    for (int k = 0; k < 3; k++) ok = ok && grow(smoke_[k], s * SN_ * (k == 1 ? 4 : scalarBytes()), 0);
+  if (ok && smokeDiv_ > 1) ok = grow(smokeBnd_, s * 2 * SN_ * 4, 0);
   if (!ok) return FP_ENOMEM;
   std::vector<uint32_t> old(slots_);
   cudaMemcpy(old.data(), freeStack_.ptr, (size_t)slots_ * 4, cudaMemcpyDeviceToHost);
@@ -808,6 +827,13 @@ void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t
   P.vmin = (float*)vmin_.ptr;
   P.vmax = (float*)vmax_.ptr;
   P.sb = (float*)sb_.ptr;
+  P.smokeDiv = smokeDiv_;
+  P.smokeShift = sshift_;
+  P.smokeCells = SN_;
+  P.smk = (float*)smoke_[smokeIdx_[0]].ptr;
+  P.smkP = (float*)smoke_[smokeIdx_[1]].ptr;
+  P.smkN = (float*)smoke_[smokeIdx_[2]].ptr;
+  P.smkB = (float*)smokeBnd_.ptr;
   P.donors = (uint16_t*)donors_.ptr;
   P.solids = (uint32_t*)solids_.ptr;
   P.p0[0] = (float*)p0_[0].ptr;
@@ -839,6 +865,7 @@ void Engine::launched(float dt, int latest) {
   latest_ = latest;
   std::swap(velIdx_[0], velIdx_[1]);
   std::swap(fldIdx_[0], fldIdx_[2]);
+  std::swap(smokeIdx_[0], smokeIdx_[2]);
   stageUsed_ = 0;
   time_ += dt;
   steps_++;
@@ -912,6 +939,8 @@ uint64_t Engine::memoryBytes() const {
   for (const DeviceBuffer* b : all) bytes += b->bytes;
   for (auto& b : vel_) bytes += b.bytes;
   for (auto& b : fld_) bytes += b.bytes;
+  for (auto& b : smoke_) bytes += b.bytes;
+  bytes += smokeBnd_.bytes;
   for (auto& b : p0_) bytes += b.bytes;
   for (int l = 0; l < FP_MAX_LEVELS; l++) bytes += topo_[l].bytes + lrhs_[l].bytes + lp_[l][0].bytes + lp_[l][1].bytes;
   return bytes;
@@ -957,14 +986,20 @@ int Engine::readField(int field, float* host, size_t bytes) {
     case FP_FIELD_PRESSURE: b = &p0_[latest_]; ch = 1; break;
     case FP_FIELD_DIVERGENCE: b = &div_; ch = 1; break;
     case FP_FIELD_CURL: b = &curl_; ch = 4; break;
+    case FP_FIELD_SMOKE:
+      if (smokeDiv_ == 1) return fail(FP_EINVAL, "the smoke field exists with smokeDivisor 2 or 4 only");
+      b = &smoke_[smokeIdx_[0]];
+      ch = 1;
+      break;
     default: return fail(FP_EINVAL, "unknown field");
   }
-  size_t need = (size_t)slots_ * ch * N_ * 4;
+  const size_t cells = field == FP_FIELD_SMOKE ? (size_t)SN_ : (size_t)N_;
+  size_t need = (size_t)slots_ * ch * cells * 4;
   if (bytes != need) return fail(FP_EINVAL, "field buffer size mismatch: need " + std::to_string(need) + " bytes");
   int rc = consume();
   if (rc) return rc;
   if ((rc = check(cudaStreamSynchronize(stream()), "read field"))) return rc;
-  if (field == FP_FIELD_SCALARS && scalarBytes() == 2) {
+  if ((field == FP_FIELD_SCALARS || field == FP_FIELD_SMOKE) && scalarBytes() == 2) {
     // FP16 storage: widened to FP32 for the caller.
     std::vector<__half> raw(need / 4);
     if ((rc = check(cudaMemcpy(raw.data(), b->ptr, raw.size() * 2, cudaMemcpyDeviceToHost), "read field"))) return rc;

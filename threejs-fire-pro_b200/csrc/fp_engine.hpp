@@ -103,6 +103,7 @@ class Engine {
   bool topoAll() const { return geometryDirty_; }
   int capacity() const { return capacity_; }
   int liveTiles() const { return (int)liveTiles_.size(); }
+  int smokeDivisor() const { return smokeDiv_; }
   size_t readbackWords() const { return (sizeof(FpCounters) + sizeof(FpSolver)) / 4 + (size_t)capacity_; }
   // Pressure solve (no reference counterpart; the reference runs one V-cycle): up to
   // `vcycles` V-cycles a step, stopping at a relative FP64 residual of `tolerance` (0: all).
@@ -166,6 +167,11 @@ class Engine {
   std::vector<int> liveTiles_, tileIndex_;  // live tile slots ascending; slot -> position or -1
   int velIdx_[4] = {0, 1, 2, 3};  // start, predictor/projected, corrected, forced
   int fldIdx_[3] = {0, 1, 2};     // start, predictor, evolved
+  // Coarse smoke (smoke_divisor d > 1): SB_ = B/d cells a side (2^sshift_), SN_ a slot; the
+  // pools trade like the scalars' (start, predictor, evolved), the donor range beside them.
+  int smokeDiv_ = 1, SB_ = 0, sshift_ = 0, SN_ = 0;
+  DeviceBuffer smoke_[3], smokeBnd_;
+  int smokeIdx_[3] = {0, 1, 2};
 
   // rendering: the box in bricks (inclusive) from the latest step's content and sources, the
   // render pools and the parameters of a render
@@ -296,6 +302,7 @@ class Stepper {
                uint64_t& launches);
   int cycle_ = 0;             // the V-cycle being enqueued
   bool fusedCoarse_ = false;  // the V-cycle below the first tile level runs as k_coarse
+  bool anySmoke_ = false;     // a simulation of the launch keeps coarse smoke
   void vcycle(int level, int cur[], uint64_t& launches);
   int check(cudaError_t e, const char* what);
   int reserve(size_t arenaBytes, int sims, size_t readWords);

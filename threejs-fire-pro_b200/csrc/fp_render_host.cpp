@@ -121,6 +121,7 @@ int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* im
   if (rs.ray_steps < 8 || rs.ray_steps > 1024) return fail(FP_EINVAL, "rendering.raySteps must be from 8 to 1024.");
   if (rs.shadow_samples < 1 || rs.shadow_samples > 256) return fail(FP_EINVAL, "shadow samples must be from 1 to 256.");
   if (rs.filter < 0 || rs.filter > 2) return fail(FP_EINVAL, "rendering.filter must be 0, 1 or 2.");
+  if (smokeDiv_ > 1) return fail(FP_EUNSUPPORTED, "render: smoke on a coarse grid is not rendered by this build.");
   int rc = consume();
   if (rc) return rc;
   const int divShift = rs.lighting_divisor == 1 ? 0 : (rs.lighting_divisor == 2 ? 1 : 2);

@@ -320,6 +320,9 @@ FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
     }
     if (!P.maccormack) out[2] = clamp01(out[2]);
     else if (P.lifetimeZero) out[2] = 0.f;
+    // With coarse smoke the fine smoke channel carries no density
+    // (fluid-scalar-transport.wgsl:127, :137).
+    if (P.smokeDiv > 1) out[0] = 0.f;
     // The predictor lives within the step: FP32 in every precision, so the limiter compares
     // the corrected value with unrounded predictions.
     for (int k = 0; k < 4; k++) P.fldP[(slot * 4 + k) * N + c] = out[k];
@@ -511,6 +514,9 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
           tr[3] = (c3 < mn3 || c3 > mx3) ? a3 : c3;
         }
       }
+      // With coarse smoke the fine smoke channel stages only this step's source production
+      // (fluid-scalar-transport.wgsl:190-199).
+      if (P.smokeDiv > 1) tr[0] = 0.f;
       float lifetime = tr[2];
       float prodS = 0.f, prodH = 0.f, injectedFuel = 0.f;
       uint2 list = tileList(P, tile, 0);
@@ -560,7 +566,7 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
     P.expn[slot * N + c] = expansion;
     if (expansion != 0.f) expands = true;
     // holdsContent and contentSupport (fluid-content.wgsl:22-39).
-    if (fmaxf(fmaxf(value[0], value[2]), value[3]) > P.cutoff) {
+    if (fmaxf(fmaxf(P.smokeDiv > 1 ? 0.f : value[0], value[2]), value[3]) > P.cutoff) {
       if (!cvSampled) cv = centreVelocity(P, H, G, V, x, y, z);
       int idc[3] = {x, y, z};
       float vv[3] = {cv.x, cv.y, cv.z};
@@ -729,6 +735,13 @@ FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage& Gc, cons
   if (solidCell(P, H, x, y, z)) return make_float3(0.f, 0.f, 0.f);  // solidAt at the centre
   // The evolved scalars of this step (the reference swaps field and corrected first).
   float heat = nearCell(P, H, Gs, Fs, 1, x, y, z), density = nearCell(P, H, Gs, Fs, 0, x, y, z);
+  // smokeVelocityAverage (smoke.wgsl:4-21) at one velocity cell per smoke spacing or less: the
+  // evolved coarse density sampled at the cell centre ((x + .5) / d in smoke cells, exact).
+  if (P.smokeDiv > 1) {
+    const float inv = 1.f / (float)P.smokeDiv;
+    density = smokeSample(P, H, P.smkN, ((float)x + 0.5f) * inv, ((float)y + 0.5f) * inv, ((float)z + 0.5f) * inv,
+                          P.scalarHalf != 0);
+  }
   float3 conf = make_float3(0.f, 0.f, 0.f);
   if (P.vorticity != 0.f) {
     float c0 = nearCell(P, H, Gc, Fc, 0, x, y, z), c1 = nearCell(P, H, Gc, Fc, 1, x, y, z),
@@ -1031,7 +1044,171 @@ __global__ void __launch_bounds__(THREADS) k_post_divergence(FpBatch bt) {
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// Coarse smoke (smoke_divisor d > 1, smoke.wgsl): a CTA of 64 threads per computing brick,
+// a thread per coarse cell. Positions are world positions of coarse cell centres; velocities
+// are the start-of-step velocity, sampled through the directory.
+constexpr int SMOKE_THREADS = 64;
+
+struct SmokeCell {
+  int q[3];
+  float p[3];
+};
+FP_DEV SmokeCell smokeCellOf(const SimParams& P, const Home& H, int c) {
+  const int sh = P.smokeShift, SB = 1 << sh;
+  const float sp = P.h * (float)P.smokeDiv;  // voxelSize x d: a power of two, exact
+  SmokeCell s;
+  s.q[0] = H.bx * SB + (c & (SB - 1));
+  s.q[1] = H.by * SB + ((c >> sh) & (SB - 1));
+  s.q[2] = H.bz * SB + (c >> (2 * sh));
+  for (int a = 0; a < 3; a++) s.p[a] = ((float)s.q[a] + 0.5f) * sp;
+  return s;
+}
+// traceBack / traceForward (fluid-advection.wgsl:67-75) from `p` with centre velocity `cv`.
+FP_DEV float3 smokeTrace(const SimParams& P, const Home& H, const float* p, float3 cv, float sign) {
+  Stage G{};
+  Field V{P.vel, 3, nullptr};
+  float3 vm = velocityAt(P, H, G, V, p[0] + sign * 0.5f * P.dt * cv.x, p[1] + sign * 0.5f * P.dt * cv.y,
+                         p[2] + sign * 0.5f * P.dt * cv.z);
+  return make_float3(p[0] + sign * P.dt * vm.x, p[1] + sign * P.dt * vm.y, p[2] + sign * P.dt * vm.z);
+}
+
+// advectSmoke (smoke.wgsl:101-124): the predictor at the back-traced departure and, for
+// MacCormack, the donors' range (smokeDonorBounds :63-77: min from 1e30, max from 0).
+__global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_advect(FpBatch bt) {
+  __shared__ int nslot[27];
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
+    if (P.smokeDiv == 1) continue;  // the same for the whole CTA
+    Home H = enterBrick(P, P.active[i], nslot);
+    const size_t slot = (size_t)nslot[13], SN = (size_t)P.smokeCells;
+    const float sp = P.h * (float)P.smokeDiv, invSp = 1.f / sp;
+    const bool half = P.scalarHalf != 0;
+    Stage G{};
+    Field V{P.vel, 3, nullptr};
+    for (int c = threadIdx.x; c < P.smokeCells; c += blockDim.x) {
+      SmokeCell s = smokeCellOf(P, H, c);
+      float density = 0.f;
+      if (!solidAt(P, H, s.p[0], s.p[1], s.p[2])) {
+        float3 cv = velocityAt(P, H, G, V, s.p[0], s.p[1], s.p[2]);
+        float3 dep = smokeTrace(P, H, s.p, cv, -1.f);
+        density = smokeSample(P, H, P.smk, dep.x * invSp, dep.y * invSp, dep.z * invSp, half);
+        if (P.maccormack) {
+          // The donor block is an integer decision: divided, as the oracle does.
+          int bx = (int)floorf(dep.x / sp - 0.5f), by = (int)floorf(dep.y / sp - 0.5f), bz = (int)floorf(dep.z / sp - 0.5f);
+          float lo = 1e30f, hi = 0.f;
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            float v = smokeCell(P, H, P.smk, bx + (k & 1), by + ((k >> 1) & 1), bz + (k >> 2), half);
+            lo = fminf(lo, v);
+            hi = fmaxf(hi, v);
+          }
+          P.smkB[(slot * 2 + 0) * SN + c] = lo;
+          P.smkB[(slot * 2 + 1) * SN + c] = hi;
+        }
+      }
+      P.smkP[slot * SN + c] = density;
+    }
+    __syncthreads();
+  }
+}
+
+// contentSupport (fluid-content.wgsl:29-39) on the smoke grid: pads in smoke cells, two at least.
+FP_DEV uint32_t smokeSupport(const SimParams& P, const int* q, float3 v) {
+  const int SB = 1 << P.smokeShift;
+  const float sp = P.h * (float)P.smokeDiv, side = (float)SB;
+  const float vv[3] = {v.x, v.y, v.z};
+  bool low[3], high[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    float loc = (float)(q[a] & (SB - 1)) + 0.5f;
+    float pad = fminf(side, fmaxf(2.f, 2.f * (P.h / sp)) + fabsf(vv[a]) * P.dt / sp);
+    low[a] = loc < pad;
+    high[a] = loc + pad >= side;
+  }
+  uint32_t row = 2u | (low[0] ? 1u : 0u) | (high[0] ? 4u : 0u);
+  uint32_t plane = (row << 3u) | (low[1] ? row : 0u) | (high[1] ? (row << 6u) : 0u);
+  return (plane << 9u) | (low[2] ? plane : 0u) | (high[2] ? (plane << 18u) : 0u);
+}
+
+// evolveSmoke (smoke.wgsl:126-178): the bounded MacCormack correction, decay, the volume
+// average of the evolved fine cells' source production (smokeProduction :23-38: the mean of
+// each 2x2x2 block, a trilinear sample at its shared corner), dormant clearing, content flags.
+__global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_evolve(FpBatch bt) {
+  __shared__ int nslot[27];
+  __shared__ uint32_t busyAll;
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
+    if (P.smokeDiv == 1) continue;  // the same for the whole CTA
+    const uint32_t id = P.active[i];
+    if (threadIdx.x == 0) busyAll = 0;
+    Home H = enterBrick(P, id, nslot);
+    const size_t slot = (size_t)nslot[13], SN = (size_t)P.smokeCells;
+    const int d = P.smokeDiv, blocks = d / 2;
+    const float sp = P.h * (float)d, invSp = 1.f / sp, volume = (float)(d * d * d / 8);
+    const bool half = P.scalarHalf != 0;
+    Stage G{};
+    Field V{P.vel, 3, nullptr};
+    uint32_t busy = 0;
+    for (int c = threadIdx.x; c < P.smokeCells; c += blockDim.x) {
+      SmokeCell s = smokeCellOf(P, H, c);
+      float density = 0.f;
+      if (!solidAt(P, H, s.p[0], s.p[1], s.p[2])) {
+        float3 cv = velocityAt(P, H, G, V, s.p[0], s.p[1], s.p[2]);
+        const float predictor = P.smkP[slot * SN + c];
+        float bounded = predictor;
+        if (P.maccormack) {
+          const float lo = P.smkB[(slot * 2 + 0) * SN + c], hi = P.smkB[(slot * 2 + 1) * SN + c];
+          if (lo != hi || predictor != lo) {
+            const float original = ldHalf(P.smk, slot * SN + c, half);
+            float3 fwd = smokeTrace(P, H, s.p, cv, 1.f);
+            float reversed = smokeSample(P, H, P.smkP, fwd.x * invSp, fwd.y * invSp, fwd.z * invSp, false);
+            float corrected = predictor + 0.5f * (original - reversed);
+            bounded = (corrected < lo || corrected > hi) ? predictor : corrected;
+          }
+        }
+        float produced[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int bz = 0; bz < blocks; bz++)
+          for (int by = 0; by < blocks; by++)
+            for (int bx = 0; bx < blocks; bx++) {
+              const float fx = (float)(s.q[0] * d + 2 * bx + 1), fy = (float)(s.q[1] * d + 2 * by + 1),
+                          fz = (float)(s.q[2] * d + 2 * bz + 1);
+#pragma unroll
+              for (int k = 0; k < 4; k++) produced[k] += sampleCells(P, H, P.fldN, 4, k, fx, fy, fz, half);
+            }
+#pragma unroll
+        for (int k = 0; k < 4; k++) produced[k] /= volume;
+        density = fmaxf(0.f, bounded * expf(-P.dissipation * P.dt) + produced[0]);
+        if (produced[0] == 0.f && produced[2] == 0.f && fmaxf(density, fmaxf(produced[1], produced[3])) < 0.001f)
+          density = 0.f;
+        if (density > P.cutoff) busy |= smokeSupport(P, s.q, cv);
+      }
+      stHalf(P.smkN, slot * SN + c, density, half);
+    }
+    // recordContent (fluid-content.wgsl:43-64)
+    busy = __reduce_or_sync(0xffffffffu, busy);
+    if ((threadIdx.x & 31) == 0 && busy) atomicOr(&busyAll, busy);
+    __syncthreads();
+    if (threadIdx.x == 0 && busyAll) {
+      uint32_t l = id & 63u;
+      uint32_t bits = (1u << (l & 3u)) | (16u << ((l >> 2) & 3u)) | (256u << (l >> 4));
+      atomicOr(&P.activity[(size_t)P.capacity * 64u + (id >> 6)], bits);
+      P.activity[id] |= FP_CONTENT | (busyAll << 3);
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace
+
+void fp_launch_smoke(const FpBatch& bt, int sms, cudaStream_t st) {
+  k_smoke_advect<<<sms * 16, SMOKE_THREADS, 0, st>>>(bt);
+  k_smoke_evolve<<<sms * 16, SMOKE_THREADS, 0, st>>>(bt);
+}
 
 // Staged kernels for 8^3 bricks: `channels` staged fields over (8 + 2 HALO)^3 cells.
 static size_t stagedBytes(int channels) {

@@ -207,11 +207,13 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
   bool solidsFresh = false, solidsAll = false, topoAll = false, curl = false, measure = false;
   int vcycles = 1;
   fusedCoarse_ = true;
+  anySmoke_ = false;
   pending_.clear();
   for (int i = 0; i < count; i++) {
     Engine* e = sims[i];
     uint32_t cap = (uint32_t)e->capacity();
     fusedCoarse_ = fusedCoarse_ && fp_coarse_fits(e->liveTiles());
+    anySmoke_ = anySmoke_ || e->smokeDivisor() > 1;
     rowBlocks[i] = blocks;
     rowTiles[i] = tiles;
     rowIds[i] = ids;
@@ -245,7 +247,8 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
     launches_ += n;
   } else {
     uint64_t key = (uint64_t)solidsFresh | ((uint64_t)solidsAll << 1) | ((uint64_t)topoAll << 2) | ((uint64_t)curl << 3) |
-                   ((uint64_t)measure << 4) | ((uint64_t)vcycles << 5) | ((uint64_t)fusedCoarse_ << 16);
+                   ((uint64_t)measure << 4) | ((uint64_t)vcycles << 5) | ((uint64_t)fusedCoarse_ << 16) |
+                   ((uint64_t)anySmoke_ << 17);
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
       GraphEntry ge{};
@@ -386,8 +389,11 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   phaseEnd(PH_CORRECT, 1);
   phaseBegin(PH_EVOLVE);
   fp_launch_evolve(bt, B_, sms_, stream_);
-  phaseEnd(PH_EVOLVE, 1);
-  launches += 3;
+  // Coarse smoke evolves after the fine fields, whose source production it averages, and
+  // records content before the measurement.
+  if (anySmoke_) fp_launch_smoke(bt, sms_, stream_);
+  phaseEnd(PH_EVOLVE, anySmoke_ ? 3 : 1);
+  launches += anySmoke_ ? 5 : 3;
 
   // Measurement: counters and the tiles' content flags are final once evolution ran, so they
   // are read here; the next step waits for this event only and prepares while the GPU runs

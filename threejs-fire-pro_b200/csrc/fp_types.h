@@ -154,6 +154,14 @@ struct SimParams {
   float* vmax;
   float* sb;
   uint16_t* donors;
+  // coarse smoke (smoke_divisor d > 1, smoke.wgsl): density on 2^smokeShift cells a brick side
+  // (smokeCells a slot) at spacing h d; smk the start of the step and smkN the evolved (the
+  // scalars' storage width), smkP the FP32 predictor, smkB its donors' min and max [slot][2][cells]
+  int smokeDiv, smokeShift, smokeCells;
+  float* smk;
+  float* smkP;
+  float* smkN;
+  float* smkB;
   uint32_t* solids;
   // multigrid
   float* p0[2];

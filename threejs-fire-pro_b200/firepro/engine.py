@@ -31,6 +31,8 @@ class FluidSimulation:
             raise FireProError(rc, self.lib.fp_last_error(None).decode())
         self.h = h
         self.cells = grid.brick_size ** 3
+        # cells a slot of the coarse smoke grid (FP_FIELD_SMOKE), smoke_divisor > 1 only
+        self.smoke_cells = self.cells // grid.smoke_divisor ** 3 if grid.smoke_divisor > 1 else 0
 
     def _check(self, rc: int):
         if rc != abi.FP_OK:
@@ -90,7 +92,8 @@ class FluidSimulation:
     def field(self, fid: int) -> np.ndarray:
         s = self.stats()
         ch = abi.FIELD_CHANNELS[fid]
-        out = np.empty((s.pool_slots, ch, self.cells), np.float32)
+        cells = self.smoke_cells if fid == abi.FP_FIELD_SMOKE else self.cells
+        out = np.empty((s.pool_slots, ch, cells), np.float32)
         self._check(self.lib.fp_sim_read_field(self.h, fid, out.ctypes.data_as(C.POINTER(C.c_float)), out.nbytes))
         return out
 
