@@ -130,6 +130,18 @@ typedef struct fp_collider {
 } fp_collider;
 
 /* `SimulationFrame` (types.ts:295-302). */
+/* Mesh emission (a `SimulationSource` with `samples`, types.ts): the reference's
+ * MeshSourceRasterizer (MeshSourceRasterizer.ts:64-167) splats the surface samples to lattice
+ * cells on the host side of this boundary; each record is one field cell, 48 bytes as the
+ * reference packs them (MeshSource, fluid-common.wgsl:53-57). A mesh source itself is an
+ * fp_source of shape FP_SHAPE_MESH whose `position` is its samples' lower bound and `size`
+ * their upper bound (the tiles around it, FluidSimulation.ts:879-893). */
+typedef struct fp_mesh_source {
+  int32_t cell[4];  /* lattice cell x, y, z; w unused */
+  float scalar[4];  /* flame lifetime, heat rate, smoke rate, fuel rate */
+  float motion[4];  /* velocity x response per axis, then the response (0: no coupling) */
+} fp_mesh_source;
+
 typedef struct fp_frame {
   fp_settings simulation;
   fp_combustion combustion;
@@ -144,6 +156,8 @@ typedef struct fp_frame {
   uint32_t collider_count;
   const uint32_t* collider_masks;
   uint32_t collider_mask_words;
+  const fp_mesh_source* mesh_sources; /* the step's mesh emission records (records 1..count) */
+  uint32_t mesh_source_count;
 } fp_frame;
 
 /* What `FireSimulation.stats` and `FluidSimulation`'s getters report

@@ -758,6 +758,41 @@ struct Sim {
   }
 
   // ---------------------------------------------------------------- host step
+  // Mesh emission (FluidSimulation.ts:1318-1351): records from 1 (record 0 is none); per
+  // brick id its table, numbered in the records' order, and per table a record a cell.
+  std::vector<fp_mesh_source> meshRecords;
+  std::vector<int> meshTables;
+  void buildMeshTables(const fp_frame& f) {
+    meshRecords.assign(1, fp_mesh_source{});
+    meshRecords.insert(meshRecords.end(), f.mesh_sources, f.mesh_sources + f.mesh_source_count);
+    meshTables.clear();
+    if (f.mesh_source_count == 0) return;
+    const size_t bricks = (size_t)capacity * 64;
+    std::map<int, int> tables;
+    std::vector<std::pair<size_t, int>> placed;
+    for (int r = 1; r < (int)meshRecords.size(); r++) {
+      const int* cell = meshRecords[r].cell;
+      int id = brickId(cell[0] >> shift, cell[1] >> shift, cell[2] >> shift);
+      if (id < 0) continue;
+      auto it = tables.find(id);
+      if (it == tables.end()) it = tables.emplace(id, (int)tables.size()).first;
+      size_t index = ((((size_t)it->second * B + (cell[2] & (B - 1))) * B + (cell[1] & (B - 1))) * B) + (cell[0] & (B - 1));
+      placed.push_back({index, r});
+    }
+    meshTables.assign(bricks + tables.size() * (size_t)N, 0);
+    std::fill(meshTables.begin(), meshTables.begin() + bricks, -1);
+    for (auto& t : tables) meshTables[t.first] = t.second;
+    for (auto& p : placed) meshTables[bricks + p.first] = p.second;
+  }
+  int meshTable(int id) const { return meshTables.empty() || id < 0 ? -1 : meshTables[id]; }
+  // meshSourceAt (fluid-sources.wgsl:9-22) for field cell (x,y,z): its record (0: none).
+  const fp_mesh_source& meshSourceAt(int x, int y, int z) {
+    if (meshTables.empty()) return meshRecords[0];
+    int table = meshTable(brickId(x >> shift, y >> shift, z >> shift));
+    if (table < 0) return meshRecords[0];
+    size_t index = (((size_t)table * B + (z & (B - 1))) * B + (y & (B - 1))) * B + (x & (B - 1));
+    return meshRecords[meshTables[(size_t)capacity * 64 + index]];
+  }
   void needBox(const double* lo, const double* hi, double margin) {
     double size = double(TILE_BRICKS * B) * (double)h;
     I3 l, u;
@@ -774,7 +809,13 @@ struct Sim {
     double margin = reach + double(TILE_BRICKS * B) * (double)h;
     for (uint32_t i = 0; i < f.source_count; i++) {
       const fp_source& s = f.sources[i];
-      if (s.shape == FP_SHAPE_MESH) continue;
+      if (s.shape == FP_SHAPE_MESH) {
+        // The samples' bounds, a voxel more margin (FluidSimulation.ts:879-893).
+        double lo[3] = {(double)s.position[0], (double)s.position[1], (double)s.position[2]};
+        double hi[3] = {(double)s.size[0], (double)s.size[1], (double)s.size[2]};
+        needBox(lo, hi, margin + (double)h);
+        continue;
+      }
       double ext = std::max(std::max(std::max((double)s.size[0], (double)s.size[1]), (double)s.size[2]), 0.03) +
                    (double)s.outward_speed * 0.25;
       double lo[3], hi[3];
@@ -793,7 +834,11 @@ struct Sim {
     double brick = double(B) * (double)h;
     for (uint32_t i = 0; i < f.source_count; i++) {
       const fp_source& s = f.sources[i];
-      if (s.shape == FP_SHAPE_MESH) continue;
+      if (s.shape == FP_SHAPE_MESH) {
+        for (int a = 0; a < 3; a++) sourceBoxes.push_back((int)std::floor((double)s.position[a] / brick));
+        for (int a = 0; a < 3; a++) sourceBoxes.push_back((int)std::floor((double)s.size[a] / brick));
+        continue;
+      }
       double ext = std::max(std::max(std::max((double)s.size[0], (double)s.size[1]), (double)s.size[2]), 0.03) +
                    (double)s.outward_speed * 0.25;
       for (int a = 0; a < 3; a++) sourceBoxes.push_back((int)std::floor(((double)s.position[a] - ext) / brick));
@@ -1249,6 +1294,7 @@ struct Sim {
       solidsStale = true;
       geometryDirty = true;
     }
+    buildMeshTables(f);
     mayHaveFlame = mayHaveFlame || f.fuel.enabled;
     for (uint32_t i = 0; i < f.source_count; i++) mayHaveFlame = mayHaveFlame || f.sources[i].flame > 0;
     dt = (R)dtf;
@@ -1325,7 +1371,7 @@ struct Sim {
               int nb = brickId(b[0] + x, b[1] + y, b[2] + z);
               if (nb < 0) continue;
               int toward = neighborIndex(-x, -y, -z);
-              listed = ((activity[nb] >> 3u) & (1u << toward)) != 0u;
+              listed = ((activity[nb] >> 3u) & (1u << toward)) != 0u || meshTable(nb) >= 0;
             }
         if (open && !listed) listed = sourceNear(b, tile);
         int32_t page = pages[index];
@@ -1762,6 +1808,13 @@ struct Sim {
             prodH += e.heat * var[0] * w * dt;
             injectedFuel += e.fuel * w * dt;
           }
+          {  // mesh emission at this cell (fluid-field-evolution.wgsl:33-36)
+            const fp_mesh_source& ms = meshSourceAt(x, y, z);
+            lifetime = std::max(lifetime, (R)ms.scalar[0]);
+            prodS += (R)ms.scalar[2] * dt;
+            prodH += (R)ms.scalar[1] * dt;
+            injectedFuel += (R)ms.scalar[3] * dt;
+          }
           R remaining = 0, burned = 0;
           if (fuelEnabled) {
             remaining = tr[3] + injectedFuel;
@@ -2114,6 +2167,12 @@ struct Sim {
       }
       result = mixr(result, e.vel[comp] + radial[comp], R(1) - std::exp(-e.response * w * dt));
     }
+    // Mesh emission's velocity coupling (fluid-forces.wgsl:143-147) at the face's field cell.
+    I3 fc = {floori((double)(face[0] / h + R(0.25))), floori((double)(face[1] / h + R(0.25))),
+             floori((double)(face[2] / h + R(0.25)))};
+    const fp_mesh_source& ms = meshSourceAt(fc[0], fc[1], fc[2]);
+    if (ms.motion[3] > 0)
+      result = mixr(result, (R)ms.motion[comp] / (R)ms.motion[3], R(1) - std::exp(-(R)ms.motion[3] * dt));
     return result;
   }
   // applyForces (fluid-forces.wgsl:151-182), then computeDivergence (:184-203).

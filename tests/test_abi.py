@@ -33,7 +33,7 @@ def test_abi_version(cuda_lib_path):
 
 def test_struct_layouts_match_c():
     structs = ["fp_grid", "fp_settings", "fp_flame_ramp", "fp_combustion", "fp_fuel", "fp_source", "fp_force",
-               "fp_collider", "fp_frame", "fp_stats", "fp_phase", "fp_server_config", "fp_completion",
+               "fp_collider", "fp_mesh_source", "fp_frame", "fp_stats", "fp_phase", "fp_server_config", "fp_completion",
                "fp_server_stats", "fp_solver_stats", "fp_camera", "fp_render_settings"]
     src = "#include <stdio.h>\n#include <stddef.h>\n#include \"firepro.h\"\nint main(void){\n"
     for s in structs:

@@ -112,6 +112,17 @@ def test_coarse_smoke(divisor, brick):
     assert seen["coarse"] * divisor ** 3 > 5.0 * seen["fine"] > 0.0
 
 
+@pytest.mark.parametrize("brick", [8, 16])
+def test_mesh_emission(brick):
+    """Mesh emission (fluid-sources.wgsl:9-22): records of the cells a mesh source reaches,
+    tables per brick rebuilt as the records move, flame, heat, smoke and fuel injection, the
+    velocity coupling at faces, and bricks listed for holding mesh emission."""
+    sc = scenes.MeshEmitterScene()
+    sc.brick_size = brick
+    reports = run(sc, 24, budget=2 ** 20)
+    check(reports, min_active=8 if brick == 16 else 30)
+
+
 def test_coarse_smoke_render_unsupported():
     sc = scenes.ForceScene()
     g = sc.grid(budget=2 ** 20)

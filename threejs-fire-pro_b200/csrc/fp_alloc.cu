@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(RANK_BLOCK) k_build_bricks(FpBatch bt) {
               int nb = brickIdAt(P, H, bx + x, by + y, bz + z);
               if (nb < 0) continue;
               int toward = nbrIndex(-x, -y, -z);
-              listed = ((P.activity[nb] >> 3u) & (1u << toward)) != 0u;
+              listed = ((P.activity[nb] >> 3u) & (1u << toward)) != 0u || (P.meshCount > 0 && P.meshTables[nb] >= 0);
             }
         if (open && !listed) listed = sourceNear(P, tile, bx, by, bz);
         int page = P.pages[index];

@@ -179,6 +179,20 @@ FP_DEV float smokeSample(const SimParams& P, const Home& H, const float* pool, f
   return blend8(t, qx - gx, qy - gy, qz - gz);
 }
 
+// meshSourceAt (fluid-sources.wgsl:9-22) for field cell (x,y,z): its mesh emission record,
+// or null where none (record 0, all zero, changes nothing).
+FP_DEV const FpMeshSource* meshSourceAt(const SimParams& P, const Home& H, int x, int y, int z) {
+  if (P.meshCount == 0) return nullptr;
+  int id = brickIdAt(P, H, x >> P.shift, y >> P.shift, z >> P.shift);
+  if (id < 0) return nullptr;
+  int table = P.meshTables[id];
+  if (table < 0) return nullptr;
+  const int m = P.B - 1, sh = P.shift;
+  size_t index = (((((size_t)table << sh) | (size_t)(z & m)) << sh | (size_t)(y & m)) << sh) | (size_t)(x & m);
+  int r = P.meshTables[(size_t)P.capacity * 64 + index];
+  return r > 0 ? &P.meshSources[r] : nullptr;
+}
+
 // solidCell (solids.wgsl:15-31): the ground, then colliders drawn into each slot's bits.
 FP_DEV bool solidCell(const SimParams& P, const Home& H, int x, int y, int z) {
   if (P.ground && y < 0) return true;

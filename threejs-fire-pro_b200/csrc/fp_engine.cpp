@@ -204,7 +204,9 @@ void Engine::freeAll() {
   for (auto& b : vel_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
   for (auto& b : fld_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
   for (auto& b : smoke_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
-  if (smokeBnd_.ptr) { cudaFree(smokeBnd_.ptr); smokeBnd_ = DeviceBuffer{}; }
+  for (DeviceBuffer* b : {&smokeBnd_, &meshTablesD_, &meshSourcesD_})
+    if (b->ptr) { cudaFree(b->ptr); *b = DeviceBuffer{}; }
+  meshVersion_ = ~0ull;
   for (auto& b : p0_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
   for (int l = 0; l < FP_MAX_LEVELS; l++) {
     if (topo_[l].ptr) { cudaFree(topo_[l].ptr); topo_[l] = DeviceBuffer{}; }
@@ -399,6 +401,7 @@ int Engine::setCapacity(int capacity) {
 
 // applyTiles (FluidSimulation.ts:629-678) with TileDirectory.tables (TileDirectory.ts:151-186).
 int Engine::applyTiles() {
+  tileVersion_++;
   int needed = std::max(MIN_TILES, dir_.slotsUsed());
   if (needed > capacity_) {
     int cap = capacity_;
@@ -461,7 +464,20 @@ void Engine::updateTiles(const fp_frame& f) {
   sourceBoxes_.clear();
   for (uint32_t i = 0; i < f.source_count; i++) {
     const fp_source& s = f.sources[i];
-    if (s.shape == FP_SHAPE_MESH) continue;
+    if (s.shape == FP_SHAPE_MESH) {
+      // A mesh source's samples span [position, size]; a voxel more margin
+      // (FluidSimulation.ts:879-893).
+      double m = margin + h;
+      int lo[3], hi[3];
+      for (int a = 0; a < 3; a++) {
+        lo[a] = (int)std::floor(((double)s.position[a] - m) / tile);
+        hi[a] = (int)std::floor(((double)s.size[a] + m) / tile);
+      }
+      dir_.need(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], steps_);
+      for (int a = 0; a < 3; a++) sourceBoxes_.push_back((int)std::floor((double)s.position[a] / brick));
+      for (int a = 0; a < 3; a++) sourceBoxes_.push_back((int)std::floor((double)s.size[a] / brick));
+      continue;
+    }
     double ext = std::max(std::max(std::max((double)s.size[0], (double)s.size[1]), (double)s.size[2]), 0.03) +
                  (double)s.outward_speed * 0.25;
     int lo[3], hi[3];
@@ -694,6 +710,43 @@ bool Engine::packScene(const fp_frame& f) {
       std::copy(l.begin(), l.end(), tileLists_.begin() + next);
       next += l.size();
     }
+  // Mesh emission (FluidSimulation.ts:1318-1351): the records, record 0 being none, and each
+  // brick's table of them (its cells' record indices), rebuilt when the records or the tiles
+  // change.
+  meshCount_ = (int)f.mesh_source_count;
+  if (meshCount_ > 0) {
+    static_assert(sizeof(FpMeshSource) == sizeof(fp_mesh_source), "mesh record layout");
+    bool same = meshVersion_ == tileVersion_ && meshRecords_.size() == (size_t)meshCount_ + 1 &&
+                std::memcmp(meshRecords_.data() + 1, f.mesh_sources, (size_t)meshCount_ * sizeof(FpMeshSource)) == 0;
+    if (!same) {
+      meshRecords_.assign(1, FpMeshSource{});
+      const FpMeshSource* in = reinterpret_cast<const FpMeshSource*>(f.mesh_sources);
+      meshRecords_.insert(meshRecords_.end(), in, in + meshCount_);
+      const size_t bricks = (size_t)capacity_ * 64;
+      const int mask = B_ - 1;
+      std::unordered_map<int, int> tables;
+      std::vector<std::pair<size_t, int>> placed;
+      for (int r = 1; r <= meshCount_; r++) {
+        const int* cell = meshRecords_[r].cell;
+        int b[3] = {cell[0] >> shift_, cell[1] >> shift_, cell[2] >> shift_};
+        int slot = dir_.slotAt(b[0] >> 2, b[1] >> 2, b[2] >> 2);
+        if (slot < 0) continue;
+        int id = slot * 64 + (((b[2] & 3) * 4 + (b[1] & 3)) * 4 + (b[0] & 3));
+        int table = tables.emplace(id, (int)tables.size()).first->second;
+        size_t index = (((((size_t)table << shift_) | (size_t)(cell[2] & mask)) << shift_ | (size_t)(cell[1] & mask))
+                        << shift_) | (size_t)(cell[0] & mask);
+        placed.push_back({index, r});
+      }
+      meshTables_.assign(bricks + tables.size() * (size_t)N_, 0);
+      std::fill(meshTables_.begin(), meshTables_.begin() + bricks, -1);
+      for (auto& t : tables) meshTables_[t.first] = t.second;
+      for (auto& p : placed) meshTables_[bricks + p.first] = p.second;
+      meshVersion_ = tileVersion_;
+      if (!upload(meshTablesD_, meshTables_.data(), meshTables_.size() * 4) ||
+          !upload(meshSourcesD_, meshRecords_.data(), meshRecords_.size() * sizeof(FpMeshSource)))
+        meshCount_ = 0;  // out of memory: the step runs without mesh emission, the error stays set
+    }
+  }
   return changed;
 }
 
@@ -733,6 +786,7 @@ int Engine::prepare(const fp_frame& f, float dt) {
     solidsStale_ = true;
     geometryDirty_ = true;
   }
+  if (meshCount_ != (int)f.mesh_source_count) return fail(FP_ENOMEM, "device memory exhausted (mesh emission tables)");
   mayHaveFlame_ = mayHaveFlame_ || f.fuel.enabled;
   for (uint32_t i = 0; i < f.source_count; i++) mayHaveFlame_ = mayHaveFlame_ || f.sources[i].flame > 0;
   return FP_OK;
@@ -834,6 +888,9 @@ void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t
   P.smkP = (float*)smoke_[smokeIdx_[1]].ptr;
   P.smkN = (float*)smoke_[smokeIdx_[2]].ptr;
   P.smkB = (float*)smokeBnd_.ptr;
+  P.meshCount = meshCount_;
+  P.meshTables = (const int*)meshTablesD_.ptr;
+  P.meshSources = (const FpMeshSource*)meshSourcesD_.ptr;
   P.donors = (uint16_t*)donors_.ptr;
   P.solids = (uint32_t*)solids_.ptr;
   P.p0[0] = (float*)p0_[0].ptr;
@@ -940,7 +997,7 @@ uint64_t Engine::memoryBytes() const {
   for (auto& b : vel_) bytes += b.bytes;
   for (auto& b : fld_) bytes += b.bytes;
   for (auto& b : smoke_) bytes += b.bytes;
-  bytes += smokeBnd_.bytes;
+  bytes += smokeBnd_.bytes + meshTablesD_.bytes + meshSourcesD_.bytes;
   for (auto& b : p0_) bytes += b.bytes;
   for (int l = 0; l < FP_MAX_LEVELS; l++) bytes += topo_[l].bytes + lrhs_[l].bytes + lp_[l][0].bytes + lp_[l][1].bytes;
   return bytes;

@@ -172,6 +172,13 @@ class Engine {
   int smokeDiv_ = 1, SB_ = 0, sshift_ = 0, SN_ = 0;
   DeviceBuffer smoke_[3], smokeBnd_;
   int smokeIdx_[3] = {0, 1, 2};
+  // Mesh emission: the records (0: none), per brick id its table (-1 none) then the tables'
+  // record indices; rebuilt when the records or the tiles (tileVersion_) change.
+  std::vector<FpMeshSource> meshRecords_;
+  std::vector<int> meshTables_;
+  DeviceBuffer meshTablesD_, meshSourcesD_;
+  int meshCount_ = 0;
+  uint64_t tileVersion_ = 0, meshVersion_ = ~0ull;
 
   // rendering: the box in bricks (inclusive) from the latest step's content and sources, the
   // render pools and the parameters of a render

@@ -530,6 +530,13 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
         prodH += e.heat * var.x * w * P.dt;
         injectedFuel += e.fuel * w * P.dt;
       }
+      // Mesh emission at this cell (fluid-field-evolution.wgsl:33-36).
+      if (const FpMeshSource* ms = meshSourceAt(P, H, x, y, z)) {
+        lifetime = fmaxf(lifetime, ms->scalar[0]);
+        prodS += ms->scalar[2] * P.dt;
+        prodH += ms->scalar[1] * P.dt;
+        injectedFuel += ms->scalar[3] * P.dt;
+      }
       float remaining = 0.f, burned = 0.f;
       if (P.fuelEnabled) {
         remaining = tr[3] + injectedFuel;
@@ -759,7 +766,9 @@ FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage& Gc, cons
 }
 
 // sourceVelocity (fluid-forces.wgsl:122-149).
-FP_DEV float sourceVelocity(const SimParams& P, int tile, float value, float fx, float fy, float fz, int comp) {
+// (cx,cy,cz) is the field cell of the face position, the cell after the face on its axis.
+FP_DEV float sourceVelocity(const SimParams& P, const Home& H, int tile, float value, float fx, float fy, float fz,
+                            int comp, int cx, int cy, int cz) {
   float result = value;
   uint2 list = tileList(P, tile, 0);
   for (uint32_t j = 0; j < list.y; j++) {
@@ -776,6 +785,10 @@ FP_DEV float sourceVelocity(const SimParams& P, int tile, float value, float fx,
     }
     result = mixf(result, e.vel[comp] + radial, 1.f - expf(-e.response * w * P.dt));
   }
+  // Mesh emission's velocity coupling (fluid-forces.wgsl:143-147).
+  const FpMeshSource* ms = meshSourceAt(P, H, cx, cy, cz);
+  if (ms && ms->motion[3] > 0.f)
+    result = mixf(result, ms->motion[comp] / ms->motion[3], 1.f - expf(-ms->motion[3] * P.dt));
   return result;
 }
 
@@ -835,7 +848,7 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
       float v = P.velC[(slot * 3 + a) * N + c] * decay + P.dt * f[a];
       float face[3] = {px, py, pz};
       face[a] += 0.5f * P.h;
-      out[a] = sourceVelocity(P, tile, v, face[0], face[1], face[2], a);
+      out[a] = sourceVelocity(P, H, tile, v, face[0], face[1], face[2], a, x + (a == 0), y + (a == 1), z + (a == 2));
     }
     // enforceFaces (fluid-forces.wgsl:15-31)
     // solidAt at a cell centre is solidCell of that cell: centre / h + 0.25 floors to it.

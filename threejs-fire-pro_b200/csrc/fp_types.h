@@ -66,6 +66,13 @@ struct FpRegion {
   float size[4];
 };
 
+// MeshSource (fluid-common.wgsl:53-57): one field cell a mesh source's samples reach.
+struct FpMeshSource {
+  int cell[4];
+  float scalar[4];  // flame lifetime, heat, smoke, fuel rates
+  float motion[4];  // velocity x response, response
+};
+
 // FlameParams (flame-common.wgsl:2-6) and its ramps.
 struct FpFlame {
   float dt, lifespan, smoke, heat;
@@ -184,6 +191,11 @@ struct SimParams {
   const FpForce* forces;
   const FpRegion* regions;
   const uint32_t* tileLists;  // 8-word header per tile slot, then indices
+  // mesh emission (fluid-sources.wgsl:3-22): per brick id its table (-1 none), then per table
+  // a record index per cell (0: none); meshCount records from 1 (0: no mesh emission)
+  const int* meshTables;
+  const FpMeshSource* meshSources;
+  int meshCount;
   FpFlame flame;
   const float4* noise;  // 64^3 curl noise
 };

@@ -141,6 +141,10 @@ class fp_collider(C.Structure):
     ]
 
 
+class fp_mesh_source(C.Structure):
+    _fields_ = [("cell", C.c_int32 * 4), ("scalar", C.c_float * 4), ("motion", C.c_float * 4)]
+
+
 class fp_frame(C.Structure):
     _fields_ = [
         ("simulation", fp_settings),
@@ -156,6 +160,8 @@ class fp_frame(C.Structure):
         ("collider_count", C.c_uint32),
         ("collider_masks", C.POINTER(C.c_uint32)),
         ("collider_mask_words", C.c_uint32),
+        ("mesh_sources", C.POINTER(fp_mesh_source)),
+        ("mesh_source_count", C.c_uint32),
     ]
 
 

@@ -124,7 +124,7 @@ class FrameData:
 
 
 def make_frame(sim_settings, comb, fuel_enabled, sources, forces=(), targets=(), colliders=(), masks=(),
-               ignition=0.5, burn_rate=4.0) -> FrameData:
+               ignition=0.5, burn_rate=4.0, mesh_sources=()) -> FrameData:
     f = abi.fp_frame()
     f.simulation = sim_settings
     f.combustion = comb
@@ -143,6 +143,7 @@ def make_frame(sim_settings, comb, fuel_enabled, sources, forces=(), targets=(),
     f.force_targets, f.force_target_count = arr(abi.fp_source, list(targets))
     f.colliders, f.collider_count = arr(abi.fp_collider, list(colliders))
     f.collider_masks, f.collider_mask_words = arr(C.c_uint32, list(masks))
+    f.mesh_sources, f.mesh_source_count = arr(abi.fp_mesh_source, list(mesh_sources))
     return FrameData(f, keep)
 
 
@@ -280,6 +281,46 @@ class ForceScene(Scene):
         cols = [collider("box", (0.2, 0.9, 0.1), (0.25, 0.05, 0.2), axes=((c, s, 0), (-s, c, 0), (0, 0, 1))),
                 collider("sphere", (-0.4, 0.8, 0.3), (0.12, 0.12, 0.12)), mesh]
         return make_frame(self.settings, self.comb, True, srcs, forces, targets, cols, self.mask_words)
+
+
+class MeshEmitterScene(Scene):
+    """Mesh emission: a disc of lattice cells (the records a mesh source's surface samples
+    splat to, MeshSourceRasterizer's output) burning with upward velocity coupling, stepping one
+    cell in x every 5 steps so the tables are rebuilt; one sphere emitter beside it."""
+
+    name = "mesh_emitter"
+    steps = 40
+
+    def __init__(self, seed: int = 1, radius_cells: int = 6):
+        self.seed = seed
+        self.radius = radius_cells
+        self.settings = settings(buoyancy=1.5, vorticity=0.3, seed=seed)
+        self.comb = combustion()
+
+    def records(self, step: int):
+        shift = step // 5
+        out = []
+        r = self.radius
+        for dz in range(-r, r + 1):
+            for dx in range(-r, r + 1):
+                if dx * dx + dz * dz > r * r:
+                    continue
+                m = abi.fp_mesh_source()
+                m.cell[:] = (dx + shift, 4, dz, 0)
+                w = 1.0 - (dx * dx + dz * dz) / float((r + 1) * (r + 1))
+                m.scalar[:] = (0.9 * w, 2.0 * w, 1.2 * w, 0.5 * w)  # flame, heat, smoke, fuel
+                m.motion[:] = (0.0, 1.5 * 4.0 * w, 0.0, 4.0 * w)     # velocity x response, response
+                out.append(m)
+        return out
+
+    def frame(self, step: int) -> FrameData:
+        recs = self.records(step)
+        h = self.voxel_size
+        lo = [min(m.cell[a] for m in recs) * h + 0.5 * h for a in range(3)]
+        hi = [max(m.cell[a] for m in recs) * h + 0.5 * h for a in range(3)]
+        mesh = source(3, "mesh", lo, hi, flame=0.9, heat=2.0, smoke=1.2, fuel=0.5)
+        ball = source(4, "sphere", (0.6, 0.2, 0.0), (0.15, 0.15, 0.15), heat=1.0, smoke=0.8)
+        return make_frame(self.settings, self.comb, True, [mesh, ball], mesh_sources=recs)
 
 
 class EmptyScene(Scene):
