@@ -158,6 +158,13 @@ typedef struct fp_frame {
   uint32_t collider_mask_words;
   const fp_mesh_source* mesh_sources; /* the step's mesh emission records (records 1..count) */
   uint32_t mesh_source_count;
+  /* Mesh force targets (ForceFields.ts:115-179): a force target of FP_SHAPE_MESH (its
+   * `position` the samples' lower bound, `size` the upper) covers the lattice cells
+   * target_cells[3k .. 3k+2] for k in [first, first + count), with (first, count) =
+   * target_cell_ranges[2t], [2t + 1] for target t of force_targets. */
+  const int32_t* target_cells;
+  uint32_t target_cell_count;         /* cells, three words each */
+  const uint32_t* target_cell_ranges; /* two words per force target (force_target_count) */
 } fp_frame;
 
 /* What `FireSimulation.stats` and `FluidSimulation`'s getters report

@@ -26,6 +26,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <set>
 #include <string>
 #include <tuple>
 #include <unordered_map>
@@ -186,6 +187,7 @@ struct Force {
   R scale, lift, inward;
   int regionFirst, regionCount;
   bool targeted;
+  bool hasMesh;
 };
 template <class R>
 struct Region {
@@ -284,6 +286,7 @@ struct Sim {
   std::vector<uint32_t> masks;
   std::vector<Force<R>> forces;
   std::vector<Region<R>> regions;
+  std::set<std::array<int, 4>> coverage;  // (force, x, y, z) of the velocity cells mesh targets cover
   std::vector<std::vector<int>> lists[3];  // per kind, per tile slot
   FlameP<R> flame;
   std::vector<V3<float>> noiseTable;  // 64^3 curl noise (built once)
@@ -707,6 +710,7 @@ struct Sim {
     // Forces (ForceFields.ts:41-114).
     forces.clear();
     regions.clear();
+    coverage.clear();
     for (uint32_t i = 0; i < f.force_count; i++) {
       const fp_force& s = f.forces[i];
       Force<R> k{};
@@ -725,7 +729,24 @@ struct Sim {
       if (k.targeted) {
         for (uint32_t t = 0; t < s.target_count; t++) {
           const fp_source& src = f.force_targets[s.first_target + t];
-          if (src.shape == FP_SHAPE_MESH) continue;
+          if (src.shape == FP_SHAPE_MESH) {
+            // A mesh target covers the cells its samples reach; the reach grows by the
+            // samples' bounds (position lo, size hi) and a velocity cell (ForceFields.ts:97-107).
+            k.hasMesh = true;
+            uint32_t ti = s.first_target + t;
+            if (!f.target_cell_ranges || f.target_cell_ranges[2 * ti + 1] == 0) continue;
+            for (int a = 0; a < 3; a++) {
+              double l = (double)src.position[a] - (double)h, u = (double)src.size[a] + (double)h;
+              if (!hasReach) { lo[a] = l; hi[a] = u; } else { lo[a] = std::min(lo[a], l); hi[a] = std::max(hi[a], u); }
+            }
+            hasReach = true;
+            uint32_t first = f.target_cell_ranges[2 * ti], n = f.target_cell_ranges[2 * ti + 1];
+            for (uint32_t c = 0; c < n; c++) {
+              const int32_t* cell = f.target_cells + 3 * ((size_t)first + c);
+              coverage.insert({(int)i, cell[0], cell[1], cell[2]});
+            }
+            continue;
+          }
           Region<R> r;
           for (int a = 0; a < 3; a++) {
             r.center[a] = src.position[a];
@@ -2053,13 +2074,19 @@ struct Sim {
     for (int a = 0; a < 3; a++) out[a] = rot[a][0] * s[0] + rot[a][1] * s[1] + rot[a][2] * s[2];
     return out;
   }
-  // externalForces + coverage (force-fields.wgsl:312-365)
-  V3<R> externalForces(int tile, V3<R> p) {
+  // meshCovers (force-fields.wgsl:27-47): a mesh target of force `index` covers velocity cell
+  // (x,y,z) while the cell's brick has an id.
+  bool meshCovers(int index, int x, int y, int z) {
+    if (brickId(x >> shift, y >> shift, z >> shift) < 0) return false;
+    return coverage.count({index, x, y, z}) != 0;
+  }
+  // externalForces + coverage (force-fields.wgsl:49-103) at velocity cell (x,y,z), centre p.
+  V3<R> externalForces(int tile, int x, int y, int z, V3<R> p) {
     V3<R> result = v3<R>(0, 0, 0);
     for (int index : lists[1][tile]) {
       const Force<R>& f = forces[index];
       R weight = 1;
-      if (f.targeted) {
+      if (f.targeted && !(f.hasMesh && meshCovers(index, x, y, z))) {
         R covered = 0;
         for (int r = 0; r < f.regionCount; r++) {
           const Region<R>& g = regions[f.regionFirst + r];
@@ -2144,7 +2171,7 @@ struct Sim {
         R s = vorticity * h;
         conf = v3<R>((n[1] * c[2] - n[2] * c[1]) * s, (n[2] * c[0] - n[0] * c[2]) * s, (n[0] * c[1] - n[1] * c[0]) * s);
       }
-      V3<R> ext = externalForces(tile, w);
+      V3<R> ext = externalForces(tile, x, y, z, w);
       for (int a = 0; a < 3; a++) F[a] = conf[a] + ext[a];
       F[1] += buoyancy * heat - smokeWeight * density;
     }

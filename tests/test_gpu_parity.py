@@ -123,6 +123,17 @@ def test_mesh_emission(brick):
     check(reports, min_active=8 if brick == 16 else 30)
 
 
+@pytest.mark.parametrize("brick", [8, 16])
+def test_mesh_force_targets(brick):
+    """Mesh force targets (force-fields.wgsl:13-65, ForceFields.ts:97-179): a targeted force
+    covers the velocity cells of its mesh target through the per-brick coverage table, rebuilt
+    as the cells move, and elsewhere the smooth analytic region of its other target."""
+    sc = scenes.MeshTargetScene()
+    sc.brick_size = brick
+    reports = run(sc, 24, budget=2 ** 20)
+    check(reports, min_active=8 if brick == 16 else 30)
+
+
 def test_coarse_smoke_render_unsupported():
     sc = scenes.ForceScene()
     g = sc.grid(budget=2 ** 20)

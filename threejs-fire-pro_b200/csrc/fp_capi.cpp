@@ -59,7 +59,8 @@ static int validateGrid(const fp_grid* grid) {
 static bool frameArraysValid(const fp_frame* f) {
   return !((f->source_count && !f->sources) || (f->force_count && !f->forces) ||
            (f->collider_count && !f->colliders) || (f->force_target_count && !f->force_targets) ||
-           (f->collider_mask_words && !f->collider_masks) || (f->mesh_source_count && !f->mesh_sources));
+           (f->collider_mask_words && !f->collider_masks) || (f->mesh_source_count && !f->mesh_sources) ||
+           (f->target_cell_count && (!f->target_cells || !f->target_cell_ranges)));
 }
 
 static fp::Stepper* newStepper(int device, int brickSize, int& rc) {

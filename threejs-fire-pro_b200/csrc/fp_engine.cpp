@@ -7,6 +7,7 @@
 #include <cmath>
 #include <chrono>
 #include <cstring>
+#include <map>
 
 #include "fp_launch.h"
 
@@ -204,9 +205,9 @@ void Engine::freeAll() {
   for (auto& b : vel_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
   for (auto& b : fld_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
   for (auto& b : smoke_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
-  for (DeviceBuffer* b : {&smokeBnd_, &meshTablesD_, &meshSourcesD_})
+  for (DeviceBuffer* b : {&smokeBnd_, &meshTablesD_, &meshSourcesD_, &coverageD_})
     if (b->ptr) { cudaFree(b->ptr); *b = DeviceBuffer{}; }
-  meshVersion_ = ~0ull;
+  meshVersion_ = coverageVersion_ = ~0ull;
   for (auto& b : p0_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
   for (int l = 0; l < FP_MAX_LEVELS; l++) {
     if (topo_[l].ptr) { cudaFree(topo_[l].ptr); topo_[l] = DeviceBuffer{}; }
@@ -666,7 +667,19 @@ bool Engine::packScene(const fp_frame& f) {
     if (s.targeted) {
       for (uint32_t t = 0; t < s.target_count && s.first_target + t < f.force_target_count; t++) {
         const fp_source& src = f.force_targets[s.first_target + t];
-        if (src.shape == FP_SHAPE_MESH) continue;
+        if (src.shape == FP_SHAPE_MESH) {
+          // Mesh targets cover the cells their samples reach (coverage below); the reach
+          // grows by their samples' bounds, a velocity cell more (ForceFields.ts:97-107).
+          k.hasMesh = 1.f;
+          if (!f.target_cell_ranges || f.target_cell_ranges[2 * (s.first_target + t) + 1] == 0) continue;
+          for (int a = 0; a < 3; a++) {
+            double l = (double)src.position[a] - (double)h_, u = (double)src.size[a] + (double)h_;
+            lo[a] = has ? std::min(lo[a], l) : l;
+            hi[a] = has ? std::max(hi[a], u) : u;
+          }
+          has = true;
+          continue;
+        }
         FpRegion r{};
         for (int a = 0; a < 3; a++) {
           r.center[a] = src.position[a];
@@ -696,6 +709,59 @@ bool Engine::packScene(const fp_frame& f) {
       }
       bin(1, (int)i, l, u, lists);
     }
+  }
+  // Mesh targets' coverage (ForceFields.ts:115-179): per brick id its first entry (or none),
+  // then per covered brick a count and, per force covering it, the force's index and a bit
+  // per velocity cell; rebuilt when the targets or the tiles change.
+  std::vector<int32_t> targets;  // force index, cell count, cells, ... of the mesh targets
+  for (uint32_t i = 0; i < f.force_count; i++) {
+    const fp_force& s = f.forces[i];
+    if (!s.targeted || !f.target_cell_ranges) continue;
+    for (uint32_t t = 0; t < s.target_count && s.first_target + t < f.force_target_count; t++) {
+      uint32_t ti = s.first_target + t;
+      if (f.force_targets[ti].shape != FP_SHAPE_MESH || f.target_cell_ranges[2 * ti + 1] == 0) continue;
+      uint32_t first = f.target_cell_ranges[2 * ti], n = f.target_cell_ranges[2 * ti + 1];
+      targets.push_back((int32_t)i);
+      targets.push_back((int32_t)n);
+      targets.insert(targets.end(), f.target_cells + 3 * (size_t)first, f.target_cells + 3 * ((size_t)first + n));
+    }
+  }
+  coverageOn_ = !targets.empty();
+  if (coverageOn_ && (targets != coverageTargets_ || coverageVersion_ != tileVersion_)) {
+    coverageTargets_ = targets;
+    coverageVersion_ = tileVersion_;
+    const size_t bricks = (size_t)capacity_ * 64, words = 1 + (size_t)(N_ + 31) / 32;
+    const int mask = B_ - 1;
+    std::map<int, std::map<int, std::vector<uint32_t>>> entries;  // brick id -> force -> bits
+    std::vector<int> order;                                        // brick ids, first seen first
+    for (size_t p = 0; p < targets.size();) {
+      int index = targets[p], n = targets[p + 1];
+      const int32_t* cells = &targets[p + 2];
+      for (int c = 0; c < n; c++) {
+        const int32_t* cell = cells + 3 * c;
+        int b[3] = {cell[0] >> shift_, cell[1] >> shift_, cell[2] >> shift_};
+        int slot = dir_.slotAt(b[0] >> 2, b[1] >> 2, b[2] >> 2);
+        if (slot < 0) continue;
+        int id = slot * 64 + (((b[2] & 3) * 4 + (b[1] & 3)) * 4 + (b[0] & 3));
+        auto& forcesOf = entries[id];
+        if (forcesOf.empty()) order.push_back(id);
+        auto& bits = forcesOf[index];
+        if (bits.empty()) bits.assign(words - 1, 0u);
+        int bit = (((cell[2] & mask) * B_) + (cell[1] & mask)) * B_ + (cell[0] & mask);
+        bits[bit >> 5] |= 1u << (bit & 31);
+      }
+      p += 2 + 3 * (size_t)n;
+    }
+    coverage_.assign(bricks, 0xffffffffu);
+    for (int id : order) {
+      coverage_[id] = (uint32_t)coverage_.size();
+      coverage_.push_back((uint32_t)entries[id].size());
+      for (auto& fb : entries[id]) {
+        coverage_.push_back((uint32_t)fb.first);
+        coverage_.insert(coverage_.end(), fb.second.begin(), fb.second.end());
+      }
+    }
+    if (!upload(coverageD_, coverage_.data(), coverage_.size() * 4)) sceneUploadFailed_ = true;
   }
   // What reaches each tile: an 8-word header per tile slot, then the indices.
   size_t length = (size_t)capacity_ * 8;
@@ -743,8 +809,10 @@ bool Engine::packScene(const fp_frame& f) {
       for (auto& p : placed) meshTables_[bricks + p.first] = p.second;
       meshVersion_ = tileVersion_;
       if (!upload(meshTablesD_, meshTables_.data(), meshTables_.size() * 4) ||
-          !upload(meshSourcesD_, meshRecords_.data(), meshRecords_.size() * sizeof(FpMeshSource)))
-        meshCount_ = 0;  // out of memory: the step runs without mesh emission, the error stays set
+          !upload(meshSourcesD_, meshRecords_.data(), meshRecords_.size() * sizeof(FpMeshSource))) {
+        sceneUploadFailed_ = true;
+        meshVersion_ = ~0ull;
+      }
     }
   }
   return changed;
@@ -765,6 +833,11 @@ int Engine::validate(const fp_frame& f, float dt) {
         return fail(FP_EINVAL, "Mesh collider occupancy does not match its size.");
     }
   }
+  if (f.target_cell_ranges)
+    for (uint32_t t = 0; t < f.force_target_count; t++)
+      if (f.force_targets[t].shape == FP_SHAPE_MESH &&
+          (uint64_t)f.target_cell_ranges[2 * t] + f.target_cell_ranges[2 * t + 1] > f.target_cell_count)
+        return fail(FP_EINVAL, "Mesh force target cells lie outside target_cells.");
   return FP_OK;
 }
 
@@ -782,11 +855,15 @@ int Engine::prepare(const fp_frame& f, float dt) {
   updateTiles(f);
   if (dir_.dirty && (rc = applyTiles())) return rc;
   updateRenderBox();
+  sceneUploadFailed_ = false;
   if (packScene(f)) {
     solidsStale_ = true;
     geometryDirty_ = true;
   }
-  if (meshCount_ != (int)f.mesh_source_count) return fail(FP_ENOMEM, "device memory exhausted (mesh emission tables)");
+  if (sceneUploadFailed_) {
+    coverageVersion_ = ~0ull;  // built again by the next step
+    return fail(FP_ENOMEM, "device memory exhausted (mesh emission or force coverage tables)");
+  }
   mayHaveFlame_ = mayHaveFlame_ || f.fuel.enabled;
   for (uint32_t i = 0; i < f.source_count; i++) mayHaveFlame_ = mayHaveFlame_ || f.sources[i].flame > 0;
   return FP_OK;
@@ -891,6 +968,7 @@ void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t
   P.meshCount = meshCount_;
   P.meshTables = (const int*)meshTablesD_.ptr;
   P.meshSources = (const FpMeshSource*)meshSourcesD_.ptr;
+  P.forceCoverage = coverageOn_ ? (const uint32_t*)coverageD_.ptr : nullptr;
   P.donors = (uint16_t*)donors_.ptr;
   P.solids = (uint32_t*)solids_.ptr;
   P.p0[0] = (float*)p0_[0].ptr;
@@ -997,7 +1075,7 @@ uint64_t Engine::memoryBytes() const {
   for (auto& b : vel_) bytes += b.bytes;
   for (auto& b : fld_) bytes += b.bytes;
   for (auto& b : smoke_) bytes += b.bytes;
-  bytes += smokeBnd_.bytes + meshTablesD_.bytes + meshSourcesD_.bytes;
+  bytes += smokeBnd_.bytes + meshTablesD_.bytes + meshSourcesD_.bytes + coverageD_.bytes;
   for (auto& b : p0_) bytes += b.bytes;
   for (int l = 0; l < FP_MAX_LEVELS; l++) bytes += topo_[l].bytes + lrhs_[l].bytes + lp_[l][0].bytes + lp_[l][1].bytes;
   return bytes;

@@ -179,6 +179,14 @@ class Engine {
   DeviceBuffer meshTablesD_, meshSourcesD_;
   int meshCount_ = 0;
   uint64_t tileVersion_ = 0, meshVersion_ = ~0ull;
+  // Mesh force targets' coverage of velocity cells by brick (force-fields.wgsl:13-47): the
+  // table, and the targets (force index, cell count, cells) it was built from.
+  std::vector<uint32_t> coverage_;
+  std::vector<int32_t> coverageTargets_;
+  DeviceBuffer coverageD_;
+  bool coverageOn_ = false;
+  uint64_t coverageVersion_ = ~0ull;
+  bool sceneUploadFailed_ = false;
 
   // rendering: the box in bricks (inclusive) from the latest step's content and sources, the
   // render pools and the parameters of a render

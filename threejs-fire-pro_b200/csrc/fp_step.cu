@@ -675,13 +675,33 @@ __global__ void __launch_bounds__(THREADS) k_curl(FpBatch bt) {
 }
 
 // externalForces with coverage (force-fields.wgsl:312-365).
-FP_DEV float3 externalForces(const SimParams& P, int tile, float px, float py, float pz) {
+// meshCovers (force-fields.wgsl:27-47): whether mesh targets of force `index` cover velocity
+// cell (x,y,z), from the coverage table.
+FP_DEV bool meshCovers(const SimParams& P, const Home& H, uint32_t index, int x, int y, int z) {
+  if (!P.forceCoverage) return false;
+  int id = brickIdAt(P, H, x >> P.shift, y >> P.shift, z >> P.shift);
+  if (id < 0) return false;
+  uint32_t first = P.forceCoverage[id];
+  if (first == 0xffffffffu) return false;
+  const uint32_t bit = (uint32_t)localCell(P, x, y, z), words = 1u + (uint32_t)(P.N + 31) / 32u;
+  const uint32_t n = P.forceCoverage[first];
+  for (uint32_t e = 0; e < n; e++) {
+    const uint32_t row = first + 1u + e * words;
+    if (P.forceCoverage[row] == index) return ((P.forceCoverage[row + 1u + (bit >> 5)] >> (bit & 31u)) & 1u) != 0u;
+  }
+  return false;
+}
+
+// externalForces and coverage (force-fields.wgsl:49-103) at velocity cell (x,y,z), centre p.
+FP_DEV float3 externalForces(const SimParams& P, const Home& H, int tile, int x, int y, int z, float px, float py,
+                             float pz) {
   float3 result = make_float3(0.f, 0.f, 0.f);
   uint2 list = tileList(P, tile, 1);
   for (uint32_t j = 0; j < list.y; j++) {
-    const FpForce& f = P.forces[P.tileLists[list.x + j]];
+    const uint32_t index = P.tileLists[list.x + j];
+    const FpForce& f = P.forces[index];
     float weight = 1.f;
-    if (f.targeted != 0.f) {
+    if (f.targeted != 0.f && !(f.hasMesh == 1.f && meshCovers(P, H, index, x, y, z))) {
       float covered = 0.f;
       for (int r = 0; r < (int)f.regionCount; r++) {
         const FpRegion& g = P.regions[(int)f.regionFirst + r];
@@ -761,7 +781,7 @@ FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage& Gc, cons
     float s = P.vorticity * P.h;
     conf = make_float3((n1 * c2 - n2 * c1) * s, (n2 * c0 - n0 * c2) * s, (n0 * c1 - n1 * c0) * s);
   }
-  float3 ext = externalForces(P, tile, wx, wy, wz);
+  float3 ext = externalForces(P, H, tile, x, y, z, wx, wy, wz);
   return make_float3(conf.x + ext.x, conf.y + ext.y + (P.buoyancy * heat - P.smokeWeight * density), conf.z + ext.z);
 }
 

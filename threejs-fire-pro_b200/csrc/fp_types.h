@@ -196,6 +196,9 @@ struct SimParams {
   const int* meshTables;
   const FpMeshSource* meshSources;
   int meshCount;
+  // mesh force targets (force-fields.wgsl:13-47): per brick id its first entry (~0u none), then
+  // per covered brick a count and per force its index and a bit per velocity cell; null: none
+  const uint32_t* forceCoverage;
   FpFlame flame;
   const float4* noise;  // 64^3 curl noise
 };

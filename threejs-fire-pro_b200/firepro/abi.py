@@ -162,6 +162,9 @@ class fp_frame(C.Structure):
         ("collider_mask_words", C.c_uint32),
         ("mesh_sources", C.POINTER(fp_mesh_source)),
         ("mesh_source_count", C.c_uint32),
+        ("target_cells", C.POINTER(C.c_int32)),
+        ("target_cell_count", C.c_uint32),
+        ("target_cell_ranges", C.POINTER(C.c_uint32)),
     ]
 
 

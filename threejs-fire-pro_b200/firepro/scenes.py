@@ -124,7 +124,9 @@ class FrameData:
 
 
 def make_frame(sim_settings, comb, fuel_enabled, sources, forces=(), targets=(), colliders=(), masks=(),
-               ignition=0.5, burn_rate=4.0, mesh_sources=()) -> FrameData:
+               ignition=0.5, burn_rate=4.0, mesh_sources=(), target_cells=()) -> FrameData:
+    """`target_cells`: per force target, the lattice cells a mesh target covers (empty for the
+    analytic ones)."""
     f = abi.fp_frame()
     f.simulation = sim_settings
     f.combustion = comb
@@ -144,6 +146,15 @@ def make_frame(sim_settings, comb, fuel_enabled, sources, forces=(), targets=(),
     f.colliders, f.collider_count = arr(abi.fp_collider, list(colliders))
     f.collider_masks, f.collider_mask_words = arr(C.c_uint32, list(masks))
     f.mesh_sources, f.mesh_source_count = arr(abi.fp_mesh_source, list(mesh_sources))
+    words, ranges = [], []
+    for t in range(len(targets)):
+        cells = list(target_cells[t]) if t < len(target_cells) else []
+        ranges += [len(words) // 3, len(cells)]
+        for c in cells:
+            words += list(c)
+    f.target_cells, _ = arr(C.c_int32, words)
+    f.target_cell_count = len(words) // 3
+    f.target_cell_ranges, _ = arr(C.c_uint32, ranges)
     return FrameData(f, keep)
 
 
@@ -321,6 +332,36 @@ class MeshEmitterScene(Scene):
         mesh = source(3, "mesh", lo, hi, flame=0.9, heat=2.0, smoke=1.2, fuel=0.5)
         ball = source(4, "sphere", (0.6, 0.2, 0.0), (0.15, 0.15, 0.15), heat=1.0, smoke=0.8)
         return make_frame(self.settings, self.comb, True, [mesh, ball], mesh_sources=recs)
+
+
+class MeshTargetScene(MeshEmitterScene):
+    """Mesh force targets: the burning disc plus a targeted wind whose targets are a mesh (a
+    column of cells above the disc, the velocity cells its samples reach, following the disc)
+    and a sphere around the side emitter, so coverage comes from the cell bits in one place and
+    the analytic region in the other; an untargeted vortex beside them."""
+
+    name = "mesh_target"
+
+    def target_cells(self, step: int):
+        shift = step // 5
+        return [(dx + shift, y, dz) for y in range(5, 14) for dz in range(-3, 4) for dx in range(-3, 4)]
+
+    def frame(self, step: int) -> FrameData:
+        recs = self.records(step)
+        h = self.voxel_size
+        lo = [min(m.cell[a] for m in recs) * h + 0.5 * h for a in range(3)]
+        hi = [max(m.cell[a] for m in recs) * h + 0.5 * h for a in range(3)]
+        mesh = source(3, "mesh", lo, hi, flame=0.9, heat=2.0, smoke=1.2, fuel=0.5)
+        ball = source(4, "sphere", (0.6, 0.2, 0.0), (0.15, 0.15, 0.15), heat=1.0, smoke=0.8)
+        cells = self.target_cells(step)
+        tlo = [min(c[a] for c in cells) * h + 0.5 * h for a in range(3)]
+        thi = [max(c[a] for c in cells) * h + 0.5 * h for a in range(3)]
+        targets = [source(5, "mesh", tlo, thi), source(4, "sphere", (0.6, 0.2, 0.0), (0.15, 0.15, 0.15))]
+        forces = [force("wind", vector=(1.0, 0.0, 0.4), strength=2.5, targeted=True, first_target=0, target_count=2),
+                  force("vortex", vector=(0.0, 1.0, 0.0), center=(0.0, 0.5, 0.0), strength=1.5, scale=0.5,
+                        lift=0.5, inward=0.3)]
+        return make_frame(self.settings, self.comb, True, [mesh, ball], forces, targets, mesh_sources=recs,
+                          target_cells=[cells, []])
 
 
 class EmptyScene(Scene):
