@@ -296,6 +296,16 @@ int fp_sim_render(fp_sim* sim, const fp_camera* camera, const fp_render_settings
 /* The same into device memory of this simulation's GPU (width x height x 4 floats); enqueued
  * on the simulation's stream. */
 int fp_sim_render_device(fp_sim* sim, const fp_camera* camera, const fp_render_settings* settings, float* rgba);
+/* Scene lights (collectLights, scene-lights.wgsl:37-106; replaces SceneLights.sample's GPU
+ * pass, SceneLights.ts:150-214): every brick that computed in the latest step samples its
+ * cells on a 4^3 lattice and adds, to the anchor nearest the brick's centre (height above an
+ * anchor counts a quarter; ties go to the first), the luminance of their emission, its
+ * luminance-weighted offset from the anchor and its RGB. `anchors` holds `anchor_count`
+ * world positions (3 floats each); `sums` receives 8 floats per anchor (luminance, offset
+ * xyz, RGB, 0), the totals SceneLights.apply turns into lights. Synchronous. Coarse smoke
+ * (smoke_divisor > 1) is FP_EUNSUPPORTED, as for the render. */
+int fp_sim_collect_lights(fp_sim* sim, const fp_render_settings* settings, const float* anchors,
+                          uint32_t anchor_count, float* sums);
 /* Wait for the simulation's queued work. */
 int fp_sim_synchronize(fp_sim* sim);
 /* Stats (waits for the latest step's measurement). */

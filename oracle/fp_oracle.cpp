@@ -1156,6 +1156,51 @@ struct Sim {
     s0 += s1 * s2;
     return R((float)(s0 >> 8u) / 16777216.f);
   }
+  // collectLights (scene-lights.wgsl:37-106): every computing brick samples its cells on a 4^3
+  // lattice (stride B/4, at the stride's middle), and adds to the anchor nearest its centre
+  // (height above an anchor counting a quarter; ties to the first) the luminance of their
+  // emission, its luminance-weighted offset from the anchor and its RGB: 8 floats an anchor.
+  void collectLights(const fp_render_settings& rs, const float* lut, const float* anchors, int count, double* sums) {
+    Render G;
+    G.rs = &rs;
+    G.lut.assign(lut, lut + 512 * 4);
+    const int stride = B / 4;
+    const double side = (double)B * (double)h;
+    for (int i = 0; i < count * 8; i++) sums[i] = 0;
+    if (count == 0) return;
+    for (uint32_t id : active) {
+      int slot = entryPage(entries[id]);
+      if (slot < 0) continue;
+      I3 b = brickOf(id);
+      double c[3] = {((double)b[0] + .5) * side, ((double)b[1] + .5) * side, ((double)b[2] + .5) * side};
+      int best = 0;
+      double bestD = 1e300;
+      for (int k = 0; k < count; k++) {
+        double d[3] = {c[0] - anchors[3 * k], c[1] - anchors[3 * k + 1], c[2] - anchors[3 * k + 2]};
+        double rise = d[1] > 0 ? d[1] * .25 : d[1];
+        double dist = d[0] * d[0] + d[2] * d[2] + rise * rise;
+        if (dist < bestD) {
+          bestD = dist;
+          best = k;
+        }
+      }
+      double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+      for (int lane = 0; lane < 64; lane++) {
+        int l[3] = {(lane & 3) * stride + stride / 2, ((lane >> 2) & 3) * stride + stride / 2, (lane >> 4) * stride + stride / 2};
+        size_t o = (size_t)slot * 4 * N + (size_t)((l[2] * B + l[1]) * B + l[0]);
+        std::array<R, 4> f = {fld[o], fld[o + N], fld[o + 2 * N], fld[o + 3 * N]};
+        std::array<R, 3> rgb = emissionOf(G, f);
+        double lum = .2126 * (double)rgb[0] + .7152 * (double)rgb[1] + .0722 * (double)rgb[2];
+        acc[0] += lum;
+        for (int a = 0; a < 3; a++) {
+          double p = ((double)(b[a] * B + l[a]) + .5) * (double)h;
+          acc[1 + a] += (p - (double)anchors[3 * best + a]) * lum;
+          acc[4 + a] += (double)rgb[a];
+        }
+      }
+      for (int k = 0; k < 7; k++) sums[best * 8 + k] += acc[k];
+    }
+  }
   void render(const fp_camera& cam, const fp_render_settings& rs, const float* lut, float* image) {
     Render G;
     G.cam = &cam;
@@ -2761,6 +2806,16 @@ int or_render(or_sim* s, const fp_camera* cam, const fp_render_settings* rs, flo
     s->d->render(*cam, *rs, lut.data(), image);
   else
     s->f->render(*cam, *rs, lut.data(), image);
+  return 0;
+}
+// The scene-light sums of the current state (FP64), 8 per anchor.
+int or_collect_lights(or_sim* s, const fp_render_settings* rs, const float* anchors, int count, double* sums) {
+  std::vector<float> lut(512 * 4);
+  or_blackbody_table(lut.data());
+  if (s->d)
+    s->d->collectLights(*rs, lut.data(), anchors, count, sums);
+  else
+    s->f->collectLights(*rs, lut.data(), anchors, count, sums);
   return 0;
 }
 // The number of V-cycles of each later step's pressure solve (the CUDA step's solver setting

@@ -39,6 +39,7 @@ def lib():
         L.or_step.restype = C.c_int
         L.or_step.argtypes = [C.c_void_p, C.c_void_p, C.c_float]
         L.or_render.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.or_collect_lights.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         L.or_blackbody_table.argtypes = [C.c_void_p]
         L.or_error.restype = C.c_char_p
         L.or_error.argtypes = [C.c_void_p]
@@ -77,6 +78,13 @@ class OracleSim:
         """The render of the current state: (height, width, 4) linear radiance and opacity."""
         out = np.zeros((camera.height, camera.width, 4), np.float32)
         self.L.or_render(self.h, C.byref(camera), C.byref(settings), out.ctypes.data)
+        return out
+
+    def collect_lights(self, settings, anchors) -> np.ndarray:
+        """The scene-light sums (count, 8) of the current state, FP64."""
+        a = np.ascontiguousarray(np.asarray(anchors, np.float32).reshape(-1, 3))
+        out = np.zeros((len(a), 8), np.float64)
+        self.L.or_collect_lights(self.h, C.byref(settings), a.ctypes.data, len(a), out.ctypes.data)
         return out
 
     def close(self):

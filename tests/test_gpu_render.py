@@ -72,3 +72,40 @@ def test_render_validation():
     with pytest.raises(FireProError):
         sim.render(render.look_at((1, 1, 1), (0, 0, 0), 8, 8), st)
     sim.dispose()
+
+
+def test_scene_lights_parity():
+    """collectLights (scene-lights.wgsl:37-106) against the oracle on the same state: each
+    anchor's luminance, luminance-weighted offset and RGB sums; the totals over anchors do not
+    depend on where the anchors are; `measure_lights` places each light inside the flames."""
+    st = render.default_settings()
+    sc = scenes.ForceScene()
+    anchors = np.array([[0.05, 0.25, 0.0], [-0.5, 0.3, 0.3], [0.6, 0.2, -0.4], [0.0, 0.5, 0.0]], np.float32)
+    moved = np.array([[3.0, 0.0, 3.0], [-0.1, 0.9, 0.2]], np.float32)
+    out = {}
+
+    def after(gpu, orc):
+        out["gpu"], out["orc"] = gpu.collect_lights(st, anchors), orc.collect_lights(st, anchors)
+        out["gpu_moved"], out["orc_moved"] = gpu.collect_lights(st, moved), orc.collect_lights(st, moved)
+        out["none"] = gpu.collect_lights(st, np.zeros((0, 3), np.float32))
+
+    parity.lockstep(sc, 10, lambda g: FluidSimulation(g), budget=2 ** 20, after=after)
+    gpu, orc = out["gpu"].astype(np.float64), out["orc"]
+    assert orc[:, 0].sum() > 0, "the flames should emit"
+    assert out["none"].shape == (0, 8)
+    for name, g, o in (("anchors", gpu, orc), ("moved", out["gpu_moved"].astype(np.float64), out["orc_moved"])):
+        scale = o[:, 0].sum()
+        for k in range(7):
+            # the offsets cancel: their tolerance is the mass times a brick's width
+            tol = 1e-4 * (np.abs(o[:, k]) + (scale * 0.2 if 1 <= k <= 3 else 0.0)) + 1e-9
+            assert np.all(np.abs(g[:, k] - o[:, k]) <= tol), (name, k, g[:, k], o[:, k])
+        assert np.all(g[:, 7] == 0)
+    for k in (0, 4, 5, 6):
+        assert abs(gpu[:, k].sum() - out["gpu_moved"][:, k].astype(np.float64).sum()) <= 1e-5 * gpu[:, k].sum()
+    lights = render.measure_lights(gpu, anchors, 8, sc.voxel_size)
+    for (position, rgb, intensity), row in zip(lights, gpu):
+        if row[0] > 0:
+            assert 0 < intensity <= 400 and rgb.max() <= 1.0 + 1e-6
+            if row[4:7].max() >= 1e-8:  # dimmer colours are divided by 1e-8, as the reference does
+                assert rgb.max() == pytest.approx(1.0)
+            assert position[1] >= 0.0

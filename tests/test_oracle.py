@@ -199,3 +199,25 @@ def test_projection_reduces_divergence(oracle_lib):
     after = np.linalg.norm(d / h - expn)
     before = np.linalg.norm(div[slots].reshape(len(slots), B, B, B)[:, 1:, 1:, 1:]) / h ** 2
     assert after < 0.5 * before, (after, before)
+
+
+def test_scene_light_sums(oracle_lib):
+    """collectLights in the oracle: every computing brick's emission goes to exactly one
+    anchor, so the luminance and RGB totals over anchors do not depend on the anchors; a single
+    anchor gathers them all, and its offset sum is the luminance-weighted centroid's."""
+    from firepro import render
+    sc = scenes.ForceScene()
+    o = _sim(sc, real=1, budget=2 ** 20)
+    for s in range(4):
+        o.step(sc.frame(s).frame)
+    st = render.default_settings()
+    one = o.collect_lights(st, [[0.0, 0.0, 0.0]])
+    three = o.collect_lights(st, [[0.0, 0.2, 0.0], [1.0, 0.2, 0.0], [-1.0, 0.5, 0.3]])
+    assert one[0, 0] > 0
+    for k in (0, 4, 5, 6):
+        assert three[:, k].sum() == pytest.approx(one[0, k], rel=1e-12)
+    centroid = one[0, 1:4] / one[0, 0]
+    assert 0.0 < centroid[1] < 1.5 and abs(centroid[0]) < 0.5 and abs(centroid[2]) < 0.5
+    far = o.collect_lights(st, [[0.0, 0.0, 0.0], [50.0, 0.0, 0.0]])
+    assert far[1, 0] == 0 and far[0, 0] == pytest.approx(one[0, 0], rel=1e-12)
+    o.close()

@@ -160,6 +160,13 @@ int fp_sim_render_device(fp_sim* sim, const fp_camera* camera, const fp_render_s
   return sim->engine->render(*camera, *settings, rgba, nullptr);
 }
 
+int fp_sim_collect_lights(fp_sim* sim, const fp_render_settings* settings, const float* anchors,
+                          uint32_t anchor_count, float* sums) {
+  if (!sim || !settings || (anchor_count && (!anchors || !sums)))
+    return failed("fp_sim_collect_lights needs a simulation, settings, anchors and sums.", FP_EINVAL);
+  return sim->engine->collectLights(*settings, anchors, anchor_count, sums);
+}
+
 int fp_sim_set_solver(fp_sim* sim, int vcycles, float tolerance) {
   if (!sim) return failed("null simulation", FP_EINVAL);
   return sim->engine->setSolver(vcycles, tolerance);

@@ -112,6 +112,8 @@ class Engine {
   // Volume rendering of the latest state (fp_render.cu) into device memory `image` (enqueued),
   // or into host memory `host` (waits).
   int render(const fp_camera& camera, const fp_render_settings& settings, float* image, float* host);
+  // Scene-light sums of the latest state (fp_sim_collect_lights), into host `sums`.
+  int collectLights(const fp_render_settings& settings, const float* anchors, uint32_t count, float* sums);
   int vcycles() const { return vcycles_; }
   // Whether the step measures the residual and the post-projection divergence.
   bool measures() const { return vcycles_ > 1 || tolerance_ > 0.f || measure_; }
@@ -193,8 +195,10 @@ class Engine {
   int renderLo_[3] = {0, 0, 0}, renderHi_[3] = {-1, -1, -1};
   bool renderBox_ = false;
   std::vector<int> sourceBoxes_;  // lo xyz, hi xyz per source
-  DeviceBuffer renderField_, lighting_, occupancy_, lut_, renderParams_, image_;
+  DeviceBuffer renderField_, lighting_, occupancy_, lut_, renderParams_, image_, anchors_, lightSums_;
   SimParams* renderParamsH_ = nullptr;
+  // The blackbody table and the render parameters of the latest state (device).
+  int renderInputs();
   void updateRenderBox();
 
   // pinned staging of the directory tables' copies

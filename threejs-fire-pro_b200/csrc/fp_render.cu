@@ -471,7 +471,83 @@ __global__ void __launch_bounds__(RTHREADS) k_march(const SimParams* __restrict_
   *out = make_float4(rad[0], rad[1], rad[2], 1.f - trans);
 }
 
+// collectLights (scene-lights.wgsl:37-106): a CTA of 64 lanes per computing brick, a lane per
+// cell of the brick's 4^3 sample lattice (stride B/4, at the stride's middle). The brick's
+// anchor is the nearest to its centre (height above an anchor counting a quarter; ties to the
+// lower index); the lanes' luminance, luminance-weighted offsets and RGB are summed in shared
+// memory and seven lanes add the totals to the anchor's floats.
+__global__ void __launch_bounds__(64) k_collect_lights(const SimParams* __restrict__ Pp, FpRender R,
+                                                       const float* __restrict__ anchors, int count, float* sums) {
+  const SimParams& P = *Pp;
+  __shared__ float2 nearest[64];
+  __shared__ float4 positions[64];
+  __shared__ float4 colors[64];
+  const uint32_t total = P.counters->active;
+  const int lane = threadIdx.x, stride = P.B >> 2;
+  const bool half = P.scalarHalf != 0;
+  const float side = (float)P.B * P.h;
+  for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
+    const uint32_t id = P.active[i];
+    const int e = P.entries[id];
+    if (e < 0) continue;  // the same for the whole CTA
+    const int slot = entryPage(e);
+    const int4 t = __ldg(&P.tileRec[id >> 6]);
+    const int l = id & 63;
+    const int b[3] = {t.x * 4 + (l & 3), t.y * 4 + ((l >> 2) & 3), t.z * 4 + (l >> 4)};
+    const int lx = (lane & 3) * stride + stride / 2, ly = ((lane >> 2) & 3) * stride + stride / 2,
+              lz = (lane >> 4) * stride + stride / 2;
+    const size_t o = (size_t)slot * 4 * P.N + (size_t)((lz * P.B + ly) * P.B + lx);
+    const float4 f = make_float4(ldHalf(P.fld, o, half), ldHalf(P.fld, o + P.N, half), ldHalf(P.fld, o + 2 * P.N, half),
+                                 ldHalf(P.fld, o + 3 * P.N, half));
+    const float3 rgb = emissionOf(R, f);
+    const float luminance = rgb.x * .2126f + rgb.y * .7152f + rgb.z * .0722f;
+    const float cx = ((float)b[0] + .5f) * side, cy = ((float)b[1] + .5f) * side, cz = ((float)b[2] + .5f) * side;
+    float2 best = make_float2(1e38f, 0.f);
+    for (int k = lane; k < count; k += 64) {
+      float dx = cx - anchors[3 * k], dy = cy - anchors[3 * k + 1], dz = cz - anchors[3 * k + 2];
+      float rise = dy > 0.f ? dy * .25f : dy;
+      float d = dx * dx + dz * dz + rise * rise;
+      if (d < best.x) best = make_float2(d, (float)k);
+    }
+    nearest[lane] = best;
+    __syncthreads();
+    for (int reach = 32; reach > 0; reach >>= 1) {
+      if (lane < reach) {
+        float2 other = nearest[lane + reach], mine = nearest[lane];
+        if (other.x < mine.x || (other.x == mine.x && other.y < mine.y)) nearest[lane] = other;
+      }
+      __syncthreads();
+    }
+    const int anchor = (int)nearest[0].y;
+    const float px = ((float)(b[0] * P.B + lx) + .5f) * P.h, py = ((float)(b[1] * P.B + ly) + .5f) * P.h,
+                pz = ((float)(b[2] * P.B + lz) + .5f) * P.h;
+    positions[lane] = make_float4(luminance, (px - anchors[3 * anchor]) * luminance,
+                                  (py - anchors[3 * anchor + 1]) * luminance, (pz - anchors[3 * anchor + 2]) * luminance);
+    colors[lane] = make_float4(rgb.x, rgb.y, rgb.z, 0.f);
+    __syncthreads();
+    for (int reach = 32; reach > 0; reach >>= 1) {
+      if (lane < reach) {
+        float4 a = positions[lane], c = positions[lane + reach], u = colors[lane], v = colors[lane + reach];
+        positions[lane] = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, a.w + c.w);
+        colors[lane] = make_float4(u.x + v.x, u.y + v.y, u.z + v.z, 0.f);
+      }
+      __syncthreads();
+    }
+    if (lane < 7) {
+      const float totals[7] = {positions[0].x, positions[0].y, positions[0].z, positions[0].w,
+                               colors[0].x, colors[0].y, colors[0].z};
+      atomicAdd(&sums[anchor * 8 + lane], totals[lane]);
+    }
+    __syncthreads();  // the shared sums are read before the next brick's lanes write them
+  }
+}
+
 }  // namespace
+
+void fp_launch_collect_lights(const SimParams* dP, const FpRender& R, const float* anchors, int count, float* sums,
+                              int sms, cudaStream_t st) {
+  k_collect_lights<<<sms * 16, 64, 0, st>>>(dP, R, anchors, count, sums);
+}
 
 void fp_launch_render(const SimParams* dP, const FpRender& R, int sms, cudaStream_t st) {
   k_render_field<<<sms * 8, RTHREADS, 0, st>>>(dP, R);

@@ -29,5 +29,8 @@ struct FpRender {
 
 // Launchers (fp_render.cu): the render pools of every active brick in the box, then the march.
 void fp_launch_render(const SimParams* dP, const FpRender& R, int sms, cudaStream_t st);
+// Scene-light sums (scene-lights.wgsl): 8 floats per anchor added into `sums` (zeroed).
+void fp_launch_collect_lights(const SimParams* dP, const FpRender& R, const float* anchors, int count, float* sums,
+                              int sms, cudaStream_t st);
 // The blackbody table (blackbody.ts:85-97) computed on the host, FP_BLACKBODY_SIZE entries.
 void fp_blackbody_table(float* out4);

@@ -113,39 +113,18 @@ void Engine::updateRenderBox() {
   }
 }
 
-int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* image, float* host) {
-  if (cam.width == 0 || cam.height == 0 || cam.width > 16384 || cam.height > 16384)
-    return fail(FP_EINVAL, "render: width and height must be from 1 to 16384.");
-  if (rs.lighting_divisor != 1 && rs.lighting_divisor != 2 && rs.lighting_divisor != 4)
-    return fail(FP_EINVAL, "rendering.lightingDivisor must be 1, 2 or 4.");
-  if (rs.ray_steps < 8 || rs.ray_steps > 1024) return fail(FP_EINVAL, "rendering.raySteps must be from 8 to 1024.");
-  if (rs.shadow_samples < 1 || rs.shadow_samples > 256) return fail(FP_EINVAL, "shadow samples must be from 1 to 256.");
-  if (rs.filter < 0 || rs.filter > 2) return fail(FP_EINVAL, "rendering.filter must be 0, 1 or 2.");
-  if (smokeDiv_ > 1) return fail(FP_EUNSUPPORTED, "render: smoke on a coarse grid is not rendered by this build.");
-  int rc = consume();
-  if (rc) return rc;
-  const int divShift = rs.lighting_divisor == 1 ? 0 : (rs.lighting_divisor == 2 ? 1 : 2);
-  const int lightShift = shift_ - divShift, L = 1 << lightShift, blocks = (B_ / 8) * (B_ / 8) * (B_ / 8);
-  size_t pixels = (size_t)cam.width * cam.height;
-  // Pools sized for every slot; the table and the parameters once.
-  bool ok = (renderField_.bytes >= (size_t)slots_ * 4 * N_ * 4 || grow(renderField_, (size_t)slots_ * 4 * N_ * 4, 0)) &&
-            (lighting_.bytes >= (size_t)slots_ * 4 * L * L * L * 4 ||
-             grow(lighting_, (size_t)slots_ * 4 * L * L * L * 4, 0)) &&
-            (occupancy_.bytes >= (size_t)slots_ * blocks || grow(occupancy_, (size_t)slots_ * blocks, 0)) &&
-            (renderParams_.ptr || alloc(renderParams_, sizeof(SimParams), false));
-  if (!ok) return FP_ENOMEM;
+// The blackbody table and the parameters a render pass reads: the latest state and the
+// directory (device, on the simulation's stream).
+int Engine::renderInputs() {
+  int rc;
   if (!lut_.ptr) {
     std::vector<float> table(FP_BLACKBODY_SIZE * 4);
     fp_blackbody_table(table.data());
     if (!alloc(lut_, table.size() * 4, false)) return FP_ENOMEM;
     if ((rc = check(cudaMemcpy(lut_.ptr, table.data(), table.size() * 4, cudaMemcpyHostToDevice), "render"))) return rc;
   }
+  if (!renderParams_.ptr && !alloc(renderParams_, sizeof(SimParams), false)) return FP_ENOMEM;
   if (!renderParamsH_ && (rc = check(cudaMallocHost(&renderParamsH_, sizeof(SimParams)), "cudaMallocHost"))) return rc;
-  float* out = image;
-  if (host) {
-    if (image_.bytes < pixels * 16 && !alloc(image_, pixels * 16, false)) return FP_ENOMEM;
-    out = (float*)image_.ptr;
-  }
   // The parameters the render reads: the latest state and the directory.
   cudaStreamSynchronize(stream());  // the previous render's parameters were read
   SimParams& P = *renderParamsH_;
@@ -169,12 +148,11 @@ int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* im
   P.scalarHalf = precision_ == FP_PRECISION_MIXED ? 1 : 0;
   if ((rc = check(cudaMemcpyAsync(renderParams_.ptr, &P, sizeof(P), cudaMemcpyHostToDevice, stream()), "render")))
     return rc;
-  FpRender R;
-  std::memset(&R, 0, sizeof(R));
-  std::memcpy(R.ivp, cam.inverse_view_projection, sizeof(R.ivp));
-  R.width = (int)cam.width;
-  R.height = (int)cam.height;
-  R.time = cam.time;
+  return FP_OK;
+}
+
+// The optical model's settings (fire-emission.wgsl's uniforms).
+static void optics(FpRender& R, const fp_render_settings& rs) {
   std::memcpy(R.optical, rs.optical, sizeof(R.optical));
   std::memcpy(R.light, rs.light, sizeof(R.light));
   std::memcpy(R.smoke, rs.smoke, sizeof(R.smoke));
@@ -182,6 +160,42 @@ int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* im
   std::memcpy(R.sceneLight, rs.scene_light, sizeof(R.sceneLight));
   std::memcpy(R.ambient, rs.ambient_light, sizeof(R.ambient));
   R.flameOpacity = rs.flame_opacity;
+}
+
+int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* image, float* host) {
+  if (cam.width == 0 || cam.height == 0 || cam.width > 16384 || cam.height > 16384)
+    return fail(FP_EINVAL, "render: width and height must be from 1 to 16384.");
+  if (rs.lighting_divisor != 1 && rs.lighting_divisor != 2 && rs.lighting_divisor != 4)
+    return fail(FP_EINVAL, "rendering.lightingDivisor must be 1, 2 or 4.");
+  if (rs.ray_steps < 8 || rs.ray_steps > 1024) return fail(FP_EINVAL, "rendering.raySteps must be from 8 to 1024.");
+  if (rs.shadow_samples < 1 || rs.shadow_samples > 256) return fail(FP_EINVAL, "shadow samples must be from 1 to 256.");
+  if (rs.filter < 0 || rs.filter > 2) return fail(FP_EINVAL, "rendering.filter must be 0, 1 or 2.");
+  if (smokeDiv_ > 1) return fail(FP_EUNSUPPORTED, "render: smoke on a coarse grid is not rendered by this build.");
+  int rc = consume();
+  if (rc) return rc;
+  const int divShift = rs.lighting_divisor == 1 ? 0 : (rs.lighting_divisor == 2 ? 1 : 2);
+  const int lightShift = shift_ - divShift, L = 1 << lightShift, blocks = (B_ / 8) * (B_ / 8) * (B_ / 8);
+  size_t pixels = (size_t)cam.width * cam.height;
+  // Pools sized for every slot; the table and the parameters once.
+  bool ok = (renderField_.bytes >= (size_t)slots_ * 4 * N_ * 4 || grow(renderField_, (size_t)slots_ * 4 * N_ * 4, 0)) &&
+            (lighting_.bytes >= (size_t)slots_ * 4 * L * L * L * 4 ||
+             grow(lighting_, (size_t)slots_ * 4 * L * L * L * 4, 0)) &&
+            (occupancy_.bytes >= (size_t)slots_ * blocks || grow(occupancy_, (size_t)slots_ * blocks, 0)) &&
+            (renderParams_.ptr || alloc(renderParams_, sizeof(SimParams), false));
+  if (!ok) return FP_ENOMEM;
+  float* out = image;
+  if (host) {
+    if (image_.bytes < pixels * 16 && !alloc(image_, pixels * 16, false)) return FP_ENOMEM;
+    out = (float*)image_.ptr;
+  }
+  if ((rc = renderInputs())) return rc;
+  FpRender R;
+  std::memset(&R, 0, sizeof(R));
+  std::memcpy(R.ivp, cam.inverse_view_projection, sizeof(R.ivp));
+  R.width = (int)cam.width;
+  R.height = (int)cam.height;
+  R.time = cam.time;
+  optics(R, rs);
   R.shadowSamples = (int)rs.shadow_samples;
   R.raySteps = (int)rs.ray_steps;
   R.filter = rs.filter;
@@ -205,6 +219,33 @@ int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* im
     return check(cudaStreamSynchronize(stream()), "render");
   }
   return FP_OK;
+}
+
+int Engine::collectLights(const fp_render_settings& rs, const float* anchors, uint32_t count, float* sums) {
+  if (count > 65536) return fail(FP_EINVAL, "scene lights: at most 65536 anchors.");
+  if (smokeDiv_ > 1) return fail(FP_EUNSUPPORTED, "scene lights: smoke on a coarse grid is not read by this build.");
+  int rc = consume();
+  if (rc) return rc;
+  if (count == 0) return FP_OK;
+  if ((rc = renderInputs())) return rc;
+  const size_t abytes = (size_t)count * 3 * 4, sbytes = (size_t)count * 8 * 4;
+  if ((anchors_.bytes < abytes && !grow(anchors_, abytes, 0)) || (lightSums_.bytes < sbytes && !grow(lightSums_, sbytes, 0)))
+    return FP_ENOMEM;
+  if ((rc = check(cudaMemcpyAsync(anchors_.ptr, anchors, abytes, cudaMemcpyHostToDevice, stream()), "scene lights")) ||
+      (rc = check(cudaMemsetAsync(lightSums_.ptr, 0, sbytes, stream()), "scene lights")))
+    return rc;
+  FpRender R;
+  std::memset(&R, 0, sizeof(R));
+  optics(R, rs);
+  R.lut = (const float4*)lut_.ptr;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, owner_->device());
+  fp_launch_collect_lights((const SimParams*)renderParams_.ptr, R, (const float*)anchors_.ptr, (int)count,
+                           (float*)lightSums_.ptr, sms, stream());
+  if ((rc = check(cudaGetLastError(), "scene lights launch"))) return rc;
+  if ((rc = check(cudaMemcpyAsync(sums, lightSums_.ptr, sbytes, cudaMemcpyDeviceToHost, stream()), "scene lights")))
+    return rc;
+  return check(cudaStreamSynchronize(stream()), "scene lights");
 }
 
 }  // namespace fp

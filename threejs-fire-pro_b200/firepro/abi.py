@@ -314,6 +314,7 @@ SIGNATURES = {
     "fp_sim_set_solver": (C.c_int, [C.c_void_p, C.c_int, C.c_float]),
     "fp_sim_render": (C.c_int, [C.c_void_p, C.POINTER(fp_camera), C.POINTER(fp_render_settings), C.c_void_p]),
     "fp_sim_render_device": (C.c_int, [C.c_void_p, C.POINTER(fp_camera), C.POINTER(fp_render_settings), C.c_void_p]),
+    "fp_sim_collect_lights": (C.c_int, [C.c_void_p, C.POINTER(fp_render_settings), C.c_void_p, C.c_uint32, C.c_void_p]),
     "fp_sim_read_solver": (C.c_int, [C.c_void_p, C.POINTER(fp_solver_stats)]),
     "fp_batch_set_solver": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_float]),
     "fp_batch_read_solver": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(fp_solver_stats)]),

@@ -72,6 +72,15 @@ class FluidSimulation:
         """Render into device memory at `image_ptr` (width x height x 4 floats), enqueued."""
         self._check(self.lib.fp_sim_render_device(self.h, C.byref(camera), C.byref(settings), image_ptr))
 
+    def collect_lights(self, settings: abi.fp_render_settings, anchors) -> np.ndarray:
+        """Scene-light sums of the latest state (SceneLights.sample's GPU pass): (anchors, 8)
+        floats, the luminance, its weighted offset from the anchor and the RGB of the flames
+        nearest each anchor."""
+        a = np.ascontiguousarray(np.asarray(anchors, np.float32).reshape(-1, 3))
+        out = np.zeros((len(a), 8), np.float32)
+        self._check(self.lib.fp_sim_collect_lights(self.h, C.byref(settings), a.ctypes.data, len(a), out.ctypes.data))
+        return out
+
     def read_solver(self) -> abi.fp_solver_stats:
         """The latest step's pressure solve (waits for the step)."""
         s = abi.fp_solver_stats()

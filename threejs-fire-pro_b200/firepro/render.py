@@ -56,3 +56,20 @@ def default_settings(filter_mode: int = 2, ray_steps: int = 256, lighting_diviso
     s.filter = filter_mode
     s.lighting_divisor = lighting_divisor
     return s
+
+
+def measure_lights(sums: np.ndarray, anchors, brick_size: int, voxel_size: float, intensity: float = 1.0):
+    """Each anchor's light from its scene-light sums (SceneLights.apply, SceneLights.ts:216-248):
+    the anchor moved to the centroid of its emission, the colour normalised to its peak
+    channel (no less than 1e-8), and an intensity of twice the emitted energy (each sample
+    stands for a cube a quarter of a brick wide) times `intensity`, capped at 400. Returns
+    (position, rgb, intensity) per anchor."""
+    sample = (brick_size / 4) * voxel_size
+    lights = []
+    for row, anchor in zip(np.asarray(sums, np.float64), np.asarray(anchors, np.float64).reshape(-1, 3)):
+        mass, offset, rgb = row[0], row[1:4], row[4:7]
+        energy = max(0.0, mass) * sample ** 3
+        position = anchor + (offset / mass if mass > 0 else 0.0)
+        peak = max(float(rgb.max()), 1e-8)
+        lights.append((position, rgb / peak, min(400.0, energy * 2 * intensity)))
+    return lights
