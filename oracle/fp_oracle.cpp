@@ -307,7 +307,7 @@ struct Sim {
   // ================================================================================
   Sim(const fp_grid& g, Prec p) {
     B = g.brick_size;
-    shift = B == 8 ? 3 : 4;
+    shift = B == 8 ? 3 : (B == 16 ? 4 : 5);
     N = B * B * B;
     W = N / 32;
     h = (R)(float)g.voxel_size;
@@ -2722,7 +2722,7 @@ or_sim* or_create(const fp_grid* g, int real, int mode) {
     p.scal = orc::STORE_F16;
     p.pc = orc::STORE_BF16;
   }
-  if (g->brick_size != 8 && g->brick_size != 16) return nullptr;
+  if (g->brick_size != 8 && g->brick_size != 16 && g->brick_size != 32) return nullptr;
   or_sim* s = new or_sim();
   s->real = real;
   if (real == 0)

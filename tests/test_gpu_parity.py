@@ -85,6 +85,20 @@ def test_brick16():
     check(run(sc, 12, budget=2 ** 21))
 
 
+def test_brick32():
+    """32^3 bricks (brickSize 32): five brick levels, 32^3 staged multigrid relaxation and
+    restriction, forces in 16^3 cubes."""
+    sc = scenes.SinglePlume()
+    sc.brick_size = 32
+    check(run(sc, 10, budget=2 ** 22), min_active=8)
+
+
+def test_brick32_forces():
+    sc = scenes.ForceScene()
+    sc.brick_size = 32
+    check(run(sc, 8, budget=2 ** 22), min_active=8)
+
+
 def test_ground_off():
     check(run(scenes.ForceScene(), 8, budget=2 ** 20, ground=False))
 

@@ -52,7 +52,6 @@ static int validateGrid(const fp_grid* grid) {
   if (!(grid->voxel_budget >= 0) || !std::isfinite(grid->voxel_budget))
     return failed("voxel_budget must be a finite, nonnegative voxel count.", FP_EINVAL);
   if (vd != 1) return failed("velocityDivisor 2 and 4 are not implemented by this build.", FP_EUNSUPPORTED);
-  if (bs == 32) return failed("brickSize 32 is not implemented by this build.", FP_EUNSUPPORTED);
   return FP_OK;
 }
 
@@ -239,7 +238,8 @@ static fp::Engine* batchSim(fp_batch* b, uint32_t id) { return id < b->sims.size
 int fp_batch_create(int device, int brick_size, fp_batch** out) {
   if (!out) return failed("fp_batch_create needs an output handle.", FP_EINVAL);
   *out = nullptr;
-  if (brick_size != 8 && brick_size != 16) return failed("a batch's brickSize must be 8 or 16.", FP_EINVAL);
+  if (brick_size != 8 && brick_size != 16 && brick_size != 32)
+    return failed("a batch's brickSize must be 8, 16 or 32.", FP_EINVAL);
   int rc;
   fp::Stepper* st = newStepper(device, brick_size, rc);
   if (!st) return rc;

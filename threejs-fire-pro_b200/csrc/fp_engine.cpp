@@ -157,7 +157,7 @@ uint32_t Engine::slotLimit() const {
 
 Engine::Engine(const fp_grid& g, Stepper* owner) : owner_(owner) {
   B_ = g.brick_size;
-  shift_ = B_ == 8 ? 3 : 4;
+  shift_ = B_ == 8 ? 3 : (B_ == 16 ? 4 : 5);
   N_ = B_ * B_ * B_;
   W_ = N_ / 32;
   brickLevels_ = shift_;
@@ -252,7 +252,7 @@ int Engine::initialize() {
 // Device bytes of a simulation of `g` once its pools exist: per slot the pools and the brick
 // levels, per tile slot (at the minimum capacity) the tables and tile levels.
 uint64_t Engine::estimateBytes(const fp_grid& g, uint32_t tiles) {
-  int B = g.brick_size, shift = B == 8 ? 3 : 4;
+  int B = g.brick_size, shift = B == 8 ? 3 : (B == 16 ? 4 : 5);
   uint64_t N = (uint64_t)B * B * B;
   double budget = g.voxel_budget > 0 ? g.voxel_budget : 8e6;
   uint64_t slots = (uint64_t)std::max(1.0, std::floor(budget / (double)N));

@@ -961,13 +961,16 @@ static void configureStaged() {
 }
 void fp_mg_configure(int B) {
   (void)B;
+  configureStaged<RELAX, 32>();
   configureStaged<RELAX, 16>();
   configureStaged<RELAX, 8>();
   configureStaged<RELAX, 4>();
   configureStaged<RELAX, 2>();
+  configureStaged<RESTRICT, 32>();
   configureStaged<RESTRICT, 16>();
   configureStaged<RESTRICT, 8>();
   configureStaged<RESTRICT, 4>();
+  configureStaged<PROLONG, 16>();
   configureStaged<PROLONG, 8>();
   configureStaged<PROLONG, 4>();
   configureStaged<PROLONG, 2>();
@@ -985,7 +988,7 @@ static void stagedLaunch(const FpBatch& bt, const MgSel& S, int sms, cudaStream_
 // in bricks of B cells (1: the first tile level).
 template <int OP>
 static int stagedSide(int level, int B) {
-  int bl = B == 8 ? 3 : 4;
+  int bl = B == 8 ? 3 : (B == 16 ? 4 : 5);
   int stage = OP == PROLONG ? level + 1 : (OP == RESTRICT ? level - 1 : level);
   return stage < bl ? 1 << (bl - stage) : 1;
 }
@@ -994,7 +997,7 @@ template <int OP>
 static void levelLaunch(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st) {
   if (tiles) {
     // The tile levels hold 4^3, 2^3 and one cell a tile.
-    const int below = S.level - (B == 8 ? 3 : 4);
+    const int below = S.level - (B == 8 ? 3 : (B == 16 ? 4 : 5));
     if (below == 0)
       k_level_tiles<OP, 64><<<sms * 16, 64, 0, st>>>(bt, S);
     else if (below == 1)
@@ -1003,19 +1006,22 @@ static void levelLaunch(const FpBatch& bt, const MgSel& S, bool tiles, int B, in
       k_level_tiles<OP, 1><<<sms * 16, 64, 0, st>>>(bt, S);
     return;
   }
-  // Relaxation stages sides 16..2, restriction its fine sides 16..4, prolongation 8..1.
+  // Relaxation stages sides 32..2, restriction its fine sides 32..4, prolongation 16..1.
   const int sb = stagedSide<OP>(S.level, B);
   if constexpr (OP == RELAX) {
-    if (sb == 16) stagedLaunch<OP, 16>(bt, S, sms, st);
+    if (sb == 32) stagedLaunch<OP, 32>(bt, S, sms, st);
+    else if (sb == 16) stagedLaunch<OP, 16>(bt, S, sms, st);
     else if (sb == 8) stagedLaunch<OP, 8>(bt, S, sms, st);
     else if (sb == 4) stagedLaunch<OP, 4>(bt, S, sms, st);
     else stagedLaunch<OP, 2>(bt, S, sms, st);
   } else if constexpr (OP == RESTRICT) {
-    if (sb == 16) stagedLaunch<OP, 16>(bt, S, sms, st);
+    if (sb == 32) stagedLaunch<OP, 32>(bt, S, sms, st);
+    else if (sb == 16) stagedLaunch<OP, 16>(bt, S, sms, st);
     else if (sb == 8) stagedLaunch<OP, 8>(bt, S, sms, st);
     else stagedLaunch<OP, 4>(bt, S, sms, st);
   } else {
-    if (sb == 8) stagedLaunch<OP, 8>(bt, S, sms, st);
+    if (sb == 16) stagedLaunch<OP, 16>(bt, S, sms, st);
+    else if (sb == 8) stagedLaunch<OP, 8>(bt, S, sms, st);
     else if (sb == 4) stagedLaunch<OP, 4>(bt, S, sms, st);
     else if (sb == 2) stagedLaunch<OP, 2>(bt, S, sms, st);
     else stagedLaunch<OP, 1>(bt, S, sms, st);

@@ -299,8 +299,8 @@ const char* fp_server_last_error(const fp_server* server) {
 int fp_server_create(const fp_server_config* config, fp_server** out) {
   if (!config || !out) return fp_set_error(FP_EINVAL, "fp_server_create needs a configuration and an output.");
   *out = nullptr;
-  if (config->brick_size != 8 && config->brick_size != 16)
-    return fp_set_error(FP_EINVAL, "a server's brickSize must be 8 or 16.");
+  if (config->brick_size != 8 && config->brick_size != 16 && config->brick_size != 32)
+    return fp_set_error(FP_EINVAL, "a server's brickSize must be 8, 16 or 32.");
   if (config->max_sessions == 0) return fp_set_error(FP_EINVAL, "max_sessions must be positive.");
   fp_server* S = new (std::nothrow) fp_server{};
   if (!S) return fp_set_error(FP_ENOMEM, "out of host memory");

@@ -816,17 +816,22 @@ FP_DEV float sourceVelocity(const SimParams& P, const Home& H, int tile, float v
 // it on one axis, staged in shared memory, averaged to the faces. Staged (8^3 bricks): the
 // curl over that region and a one-cell rim and the evolved smoke and heat over the region are
 // copied to shared memory first.
+// The side of the cubes the force kernel walks a brick in: their force tiles fit shared memory.
+constexpr int FORCE_SUB = 16;
+
 template <bool STAGED>
 FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
-  extern __shared__ float3 forceTile[];  // (B+1)^3, then the staged curl and scalars
+  extern __shared__ float3 forceTile[];  // (SUB+1)^3, then the staged curl and scalars
   const SimParams& P = *Pp;
   uint32_t id = P.active[i];
   Home H = enterBrick(P, id, nslot);
   size_t slot = (size_t)nslot[13];
   const size_t N = P.N;
   int tile = (int)(id >> 6);
-  const int E = STAGED ? 9 : P.B + 1, E3 = E * E * E;
+  // The brick in cubes of SUB cells a side (one cube up to 16^3 bricks, 8 of them in a 32^3
+  // brick), each with its centre forces on the cube and one cell beyond its upper faces.
+  const int SUB = STAGED ? 8 : min(P.B, FORCE_SUB), E = SUB + 1, E3 = E * E * E, per = P.B / SUB;
   float* stage = reinterpret_cast<float*>(forceTile + E3);
   Stage Gc, Gs;
   Gc.S = STAGED ? E + 2 : 0;
@@ -847,41 +852,45 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
     stageField<9>(P, H, Gs, stage + 4 * Gc.S3, P.fldN, 4, half, 2);  // smoke, heat
     stageWait();
   }
-  for (int q = threadIdx.x; q < E3; q += blockDim.x) {
-    int lx = q % E, ly = (q / E) % E, lz = q / (E * E);
-    if ((lx == P.B) + (ly == P.B) + (lz == P.B) >= 2) continue;
-    forceTile[q] = cellForce(P, H, Gc, Fc, Gs, Fs, tile, H.bx * P.B + lx, H.by * P.B + ly, H.bz * P.B + lz);
-  }
-  __syncthreads();
-  float decay = expf(-P.damping * P.dt);
-  for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
-    int x, y, z;
-    cellOf(P, H, c, x, y, z);
-    int lx = x & (P.B - 1), ly = y & (P.B - 1), lz = z & (P.B - 1);
-    int t = (lz * E + ly) * E + lx;
-    float3 F0 = forceTile[t];
-    float f[3] = {0.5f * (F0.x + forceTile[t + 1].x), 0.5f * (F0.y + forceTile[t + E].y),
-                  0.5f * (F0.z + forceTile[t + E * E].z)};
-    float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-    float out[3];
-    for (int a = 0; a < 3; a++) {
-      float v = P.velC[(slot * 3 + a) * N + c] * decay + P.dt * f[a];
-      float face[3] = {px, py, pz};
-      face[a] += 0.5f * P.h;
-      out[a] = sourceVelocity(P, H, tile, v, face[0], face[1], face[2], a, x + (a == 0), y + (a == 1), z + (a == 2));
+  const float decay = expf(-P.damping * P.dt);
+  for (int cube = 0; cube < per * per * per; cube++) {
+    const int ox = H.bx * P.B + (cube % per) * SUB, oy = H.by * P.B + ((cube / per) % per) * SUB,
+              oz = H.bz * P.B + (cube / (per * per)) * SUB;
+    for (int q = threadIdx.x; q < E3; q += blockDim.x) {
+      int lx = q % E, ly = (q / E) % E, lz = q / (E * E);
+      if ((lx == SUB) + (ly == SUB) + (lz == SUB) >= 2) continue;
+      forceTile[q] = cellForce(P, H, Gc, Fc, Gs, Fs, tile, ox + lx, oy + ly, oz + lz);
     }
-    // enforceFaces (fluid-forces.wgsl:15-31)
-    // solidAt at a cell centre is solidCell of that cell: centre / h + 0.25 floors to it.
-    if (solidCell(P, H, x, y, z)) {
-      out[0] = out[1] = out[2] = 0.f;
-    } else {
-      if (solidCell(P, H, x + 1, y, z)) out[0] = 0.f;
-      if (solidCell(P, H, x, y + 1, z)) out[1] = 0.f;
-      if (solidCell(P, H, x, y, z + 1)) out[2] = 0.f;
+    __syncthreads();
+    for (int k = threadIdx.x; k < SUB * SUB * SUB; k += blockDim.x) {
+      const int lx = k % SUB, ly = (k / SUB) % SUB, lz = k / (SUB * SUB);
+      const int x = ox + lx, y = oy + ly, z = oz + lz;
+      const int c = (((z & (P.B - 1)) * P.B) + (y & (P.B - 1))) * P.B + (x & (P.B - 1));
+      int t = (lz * E + ly) * E + lx;
+      float3 F0 = forceTile[t];
+      float f[3] = {0.5f * (F0.x + forceTile[t + 1].x), 0.5f * (F0.y + forceTile[t + E].y),
+                    0.5f * (F0.z + forceTile[t + E * E].z)};
+      float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+      float out[3];
+      for (int a = 0; a < 3; a++) {
+        float v = P.velC[(slot * 3 + a) * N + c] * decay + P.dt * f[a];
+        float face[3] = {px, py, pz};
+        face[a] += 0.5f * P.h;
+        out[a] = sourceVelocity(P, H, tile, v, face[0], face[1], face[2], a, x + (a == 0), y + (a == 1), z + (a == 2));
+      }
+      // enforceFaces (fluid-forces.wgsl:15-31)
+      // solidAt at a cell centre is solidCell of that cell: centre / h + 0.25 floors to it.
+      if (solidCell(P, H, x, y, z)) {
+        out[0] = out[1] = out[2] = 0.f;
+      } else {
+        if (solidCell(P, H, x + 1, y, z)) out[0] = 0.f;
+        if (solidCell(P, H, x, y + 1, z)) out[1] = 0.f;
+        if (solidCell(P, H, x, y, z + 1)) out[2] = 0.f;
+      }
+      for (int a = 0; a < 3; a++) P.velF[(slot * 3 + a) * N + c] = out[a];
     }
-    for (int a = 0; a < 3; a++) P.velF[(slot * 3 + a) * N + c] = out[a];
+    __syncthreads();  // the tile is read before the next cube's forces overwrite it
   }
-  __syncthreads();
 }
 template <bool STAGED>
 __global__ void __launch_bounds__(THREADS, 4) k_forces(FpBatch bt) {
@@ -1255,7 +1264,7 @@ void fp_step_configure(int B) {
   cudaFuncSetAttribute(k_predict<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
   cudaFuncSetAttribute(k_correct<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(6));
   cudaFuncSetAttribute(k_evolve<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
-  size_t smem = (size_t)(B + 1) * (B + 1) * (B + 1) * sizeof(float3);
+  const size_t side = (size_t)(B < FORCE_SUB ? B : FORCE_SUB) + 1, smem = side * side * side * sizeof(float3);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_forces<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
@@ -1288,7 +1297,7 @@ void fp_launch_forces(const FpBatch& bt, int B, int sms, cudaStream_t st) {
     k_forces<true><<<sms * 4, THREADS, FORCE_STAGED_BYTES, st>>>(bt);
     return;
   }
-  size_t smem = (size_t)(B + 1) * (B + 1) * (B + 1) * sizeof(float3);
+  const size_t side = (size_t)(B < FORCE_SUB ? B : FORCE_SUB) + 1, smem = side * side * side * sizeof(float3);
   k_forces<false><<<sms * 4, THREADS, smem, st>>>(bt);
 }
 void fp_launch_divergence(const FpBatch& bt, int pSel, int sms, cudaStream_t st) {

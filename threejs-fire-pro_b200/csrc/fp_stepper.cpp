@@ -19,7 +19,7 @@ namespace fp {
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
 Stepper::Stepper(int device, int brickSize) : device_(device), B_(brickSize) {
-  brickLevels_ = B_ == 8 ? 3 : 4;
+  brickLevels_ = B_ == 8 ? 3 : (B_ == 16 ? 4 : 5);
   bottom_ = brickLevels_ + 2;
 }
 
