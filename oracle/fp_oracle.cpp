@@ -221,6 +221,10 @@ template <class R>
 struct Sim {
   // --- configuration
   int B, shift, N, W;  // brick cells per side, log2, cells per brick, solid words per slot
+  // The velocity and pressure lattice (velocityDivisor d, FluidSimulation.ts:365-373): B/d
+  // cells a brick side at spacing h d, the brick footprint shared with the field lattice.
+  int vd = 1, VB, vshift, VN;
+  R vh;
   R h;                 // voxel size (float value)
   bool maccormack;
   Prec prec;
@@ -319,7 +323,13 @@ struct Sim {
     while ((1 << sshift) < SB) sshift++;
     SN = SB * SB * SB;
     sp = h * (R)smokeDiv;  // voxelSize x smokeDivisor: a power of two, exact
-    brickLevels = shift;
+    vd = g.velocity_divisor > 1 ? g.velocity_divisor : 1;
+    VB = B / vd;
+    vshift = 0;
+    while ((1 << vshift) < VB) vshift++;
+    VN = VB * VB * VB;
+    vh = h * (R)vd;  // velocityGrid = voxelSize x velocityDivisor: a power of two, exact
+    brickLevels = vshift;  // the pressure lives on the velocity lattice
     bottom = brickLevels + 2;
     if (g.voxel_budget > 0) voxelBudget = g.voxel_budget;
     buildNoise();
@@ -355,21 +365,21 @@ struct Sim {
   }
   void resizePools(uint32_t n) {
     size_t s = n;
-    vel.resize(s * 3 * N, 0); velP.resize(s * 3 * N, 0); velC.resize(s * 3 * N, 0); velF.resize(s * 3 * N, 0);
-    curl.resize(s * 4 * N, 0);
+    vel.resize(s * 3 * VN, 0); velP.resize(s * 3 * VN, 0); velC.resize(s * 3 * VN, 0); velF.resize(s * 3 * VN, 0);
+    curl.resize(s * 4 * VN, 0);
     fld.resize(s * 4 * N, 0); fldP.resize(s * 4 * N, 0); fldN.resize(s * 4 * N, 0);
-    expn.resize(s * N, 0); div.resize(s * N, 0);
-    vmin.resize(s * 3 * N, 0); vmax.resize(s * 3 * N, 0);
+    expn.resize(s * N, 0); div.resize(s * VN, 0);
+    vmin.resize(s * 3 * VN, 0); vmax.resize(s * 3 * VN, 0);
     sb.resize(s * 8 * N, 0);
-    vdonor.resize(s * 3 * N * 3, 0);
+    vdonor.resize(s * 3 * VN * 3, 0);
     solids.resize(s * W, 0);
     if (smokeDiv > 1) {
       smk.resize(s * SN, 0); smkP.resize(s * SN, 0); smkN.resize(s * SN, 0);
       smkBnd.resize(s * 2 * SN, 0);
     }
-    pres[0].resize(s * N, 0); pres[1].resize(s * N, 0);
+    pres[0].resize(s * VN, 0); pres[1].resize(s * VN, 0);
     levels.resize(bottom + 1);
-    levels[0].topo.resize(s * N, 0);
+    levels[0].topo.resize(s * VN, 0);
     for (int l = 1; l < brickLevels; l++) {
       size_t c = s * levelCells(l);
       levels[l].p[0].resize(c, 0); levels[l].p[1].resize(c, 0); levels[l].rhs.resize(c, 0);
@@ -553,11 +563,50 @@ struct Sim {
   V3<R> center(int x, int y, int z) { return v3<R>((R(x) + R(0.5)) * h, (R(y) + R(0.5)) * h, (R(z) + R(0.5)) * h); }
 
   // ---------------------------------------------------------------- velocity sampling
-  // fluid-advection.wgsl:17-21: the MAC component at world position `p`.
+  // The velocity lattice (fluid-sampling.wgsl:4-13: each grid shares the brick footprint with
+  // its own cells per side): cell offset, cell of a [slot][ch][VN] pool, trilinear sample in its
+  // cell units, a cell's centre.
+  int vlocal(int x, int y, int z) const { return ((z & (VB - 1)) * VB + (y & (VB - 1))) * VB + (x & (VB - 1)); }
+  R vcell(const std::vector<R>& pool, int ch, int c, int x, int y, int z) {
+    int s = brickSlot(x >> vshift, y >> vshift, z >> vshift);
+    if (s < 0) return 0;
+    return pool[((size_t)s * ch + c) * VN + vlocal(x, y, z)];
+  }
+  R vsample(const std::vector<R>& pool, int ch, int c, R px, R py, R pz) {
+    R q[3] = {px - R(0.5), py - R(0.5), pz - R(0.5)};
+    int b[3];
+    R f[3];
+    for (int a = 0; a < 3; a++) {
+      b[a] = floori((double)q[a]);
+      f[a] = q[a] - (R)b[a];
+    }
+    R value = 0;
+    for (int z = 0; z < 2; z++)
+      for (int y = 0; y < 2; y++)
+        for (int x = 0; x < 2; x++) {
+          R w = (x ? f[0] : R(1) - f[0]) * (y ? f[1] : R(1) - f[1]) * (z ? f[2] : R(1) - f[2]);
+          value += vcell(pool, ch, c, b[0] + x, b[1] + y, b[2] + z) * w;
+        }
+    return value;
+  }
+  V3<R> vcenter(int x, int y, int z) { return v3<R>((R(x) + R(0.5)) * vh, (R(y) + R(0.5)) * vh, (R(z) + R(0.5)) * vh); }
+  // velocityCellAverage (fluid-sampling.wgsl:268-285): the box average of the field cells under
+  // velocity cell (x,y,z), each linear sample on the shared corner of a 2x2x2 block.
+  R fieldAverage(const std::vector<R>& pool, int ch, int c, int x, int y, int z) {
+    if (vd == 1) return cellAt(pool, ch, c, x, y, z);
+    int blocks = vd / 2;
+    R sum = 0;
+    for (int k = 0; k < blocks; k++)
+      for (int j = 0; j < blocks; j++)
+        for (int i = 0; i < blocks; i++)
+          sum += sampleCells(pool, ch, c, R(x * vd + 1 + 2 * i), R(y * vd + 1 + 2 * j), R(z * vd + 1 + 2 * k));
+    return sum / R(blocks * blocks * blocks);
+  }
+  // fluid-advection.wgsl:9-15: the MAC component at world position `p`.
   R velComp(const std::vector<R>& pool, V3<R> p, int c) {
     V3<R> q = p;
-    q[c] -= R(0.5) * h;
-    return sampleCells(pool, 3, c, q[0] / h, q[1] / h, q[2] / h);
+    q[c] -= R(0.5) * vh;
+    return vsample(pool, 3, c, q[0] / vh, q[1] / vh, q[2] / vh);
   }
   V3<R> velocityAt(V3<R> p) { return v3<R>(velComp(vel, p, 0), velComp(vel, p, 1), velComp(vel, p, 2)); }
   // fluid-advection.wgsl:26-44
@@ -572,7 +621,7 @@ struct Sim {
       }
       R q[3] = {fp[0], fp[1], fp[2]};
       q[k] -= R(0.5);
-      r[k] = sampleCells(vel, 3, k, q[0], q[1], q[2]);
+      r[k] = vsample(vel, 3, k, q[0], q[1], q[2]);
     }
     return r;
   }
@@ -736,7 +785,7 @@ struct Sim {
             uint32_t ti = s.first_target + t;
             if (!f.target_cell_ranges || f.target_cell_ranges[2 * ti + 1] == 0) continue;
             for (int a = 0; a < 3; a++) {
-              double l = (double)src.position[a] - (double)h, u = (double)src.size[a] + (double)h;
+              double l = (double)src.position[a] - (double)vh, u = (double)src.size[a] + (double)vh;
               if (!hasReach) { lo[a] = l; hi[a] = u; } else { lo[a] = std::min(lo[a], l); hi[a] = std::max(hi[a], u); }
             }
             hasReach = true;
@@ -1408,7 +1457,7 @@ struct Sim {
       bool inside = true;
       for (int a = 0; a < 3; a++) {
         float motion = std::fabs((float)e.vel[a]) + std::fabs((float)e.outward);
-        float pad = std::min(size, 2.f * hf + motion * dtf);
+        float pad = std::min(size, 2.f * (float)vh + motion * dtf);
         float extent = std::max((float)e.size[a], 0.03f) + pad;
         float pos = (float)e.pos[a];
         if (!(pos + extent > lo[a] && pos - extent < hi[a])) inside = false;
@@ -1568,7 +1617,7 @@ struct Sim {
     for (auto& z : zeroed) {
       if (!(z.second & 0x80000000u)) continue;
       size_t s = z.second & 0xffffffu;
-      std::fill(vel.begin() + s * 3 * N, vel.begin() + (s + 1) * 3 * N, R(0));
+      std::fill(vel.begin() + s * 3 * VN, vel.begin() + (s + 1) * 3 * VN, R(0));
       std::fill(fld.begin() + s * 4 * N, fld.begin() + (s + 1) * 4 * N, R(0));
       std::fill(expn.begin() + s * N, expn.begin() + (s + 1) * N, R(0));
       if (smokeDiv > 1)  // zeroSmokeBricks (smoke.wgsl:188-223): all three smoke pools
@@ -1591,85 +1640,100 @@ struct Sim {
       }
     }
   }
+  // The same over the velocity lattice's cells.
+  template <class F>
+  void forActiveVCells(F fn) {
+    long n = (long)active.size();
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long i = 0; i < n; i++) {
+      uint32_t id = active[i];
+      int slot = entryPage(entries[id]);
+      I3 b = brickOf(id);
+      for (int c = 0; c < VN; c++) {
+        int x = b[0] * VB + (c & (VB - 1)), y = b[1] * VB + ((c >> vshift) & (VB - 1)), z = b[2] * VB + (c >> (2 * vshift));
+        fn(id, slot, c, x, y, z);
+      }
+    }
+  }
   R sv(R x) { return store_round(x, prec.vel); }
   R ss(R x) { return store_round(x, prec.scal); }
 
   // advectVelocityWithBounds (fluid-velocity-transport.wgsl:28-100)
   void advectVelocity() {
-    forActiveCells([&](uint32_t, int slot, int c, int x, int y, int z) {
+    forActiveVCells([&](uint32_t, int slot, int c, int x, int y, int z) {
       // Bounds over the 2x2x2 forward block of the velocity.
       for (int k = 0; k < 3; k++) {
         R lo = R(1e5), hi = R(-1e5);
         for (int dz = 0; dz < 2; dz++)
           for (int dy = 0; dy < 2; dy++)
             for (int dx = 0; dx < 2; dx++) {
-              R v = cellAt(vel, 3, k, x + dx, y + dy, z + dz);
+              R v = vcell(vel, 3, k, x + dx, y + dy, z + dz);
               lo = std::min(lo, v);
               hi = std::max(hi, v);
             }
-        vmin[((size_t)slot * 3 + k) * N + c] = store_round(lo, prec.bounds);
-        vmax[((size_t)slot * 3 + k) * N + c] = store_round(hi, prec.bounds);
+        vmin[((size_t)slot * 3 + k) * VN + c] = store_round(lo, prec.bounds);
+        vmax[((size_t)slot * 3 + k) * VN + c] = store_round(hi, prec.bounds);
       }
-      V3<R> pos = center(x, y, z);
+      V3<R> pos = vcenter(x, y, z);
       if (solidAt(pos[0], pos[1], pos[2])) {
-        for (int k = 0; k < 3; k++) velP[((size_t)slot * 3 + k) * N + c] = 0;
+        for (int k = 0; k < 3; k++) velP[((size_t)slot * 3 + k) * VN + c] = 0;
         return;
       }
-      V3<R> orig = v3<R>(vel[((size_t)slot * 3 + 0) * N + c], vel[((size_t)slot * 3 + 1) * N + c],
-                         vel[((size_t)slot * 3 + 2) * N + c]);
+      V3<R> orig = v3<R>(vel[((size_t)slot * 3 + 0) * VN + c], vel[((size_t)slot * 3 + 1) * VN + c],
+                         vel[((size_t)slot * 3 + 2) * VN + c]);
       for (int comp = 0; comp < 3; comp++) {
         V3<R> face = pos;
-        face[comp] += R(0.5) * h;
+        face[comp] += R(0.5) * vh;
         V3<R> fv = velocityOnFace(x, y, z, comp, orig);
         V3<R> mid, dep;
         for (int a = 0; a < 3; a++) mid[a] = face[a] - R(0.5) * dt * fv[a];
         V3<R> vm = velocityAt(mid);
         for (int a = 0; a < 3; a++) dep[a] = face[a] - dt * vm[a];
-        int32_t* d = &vdonor[(((size_t)slot * 3 + comp) * N + c) * 3];
+        int32_t* d = &vdonor[(((size_t)slot * 3 + comp) * VN + c) * 3];
         V3<R> shifted = dep;
-        shifted[comp] -= R(0.5) * h;
-        for (int a = 0; a < 3; a++) d[a] = floori((double)(shifted[a] / h - R(0.5)));
-        velP[((size_t)slot * 3 + comp) * N + c] = sv(velComp(vel, dep, comp));
+        shifted[comp] -= R(0.5) * vh;
+        for (int a = 0; a < 3; a++) d[a] = floori((double)(shifted[a] / vh - R(0.5)));
+        velP[((size_t)slot * 3 + comp) * VN + c] = sv(velComp(vel, dep, comp));
       }
     });
   }
   // correctVelocity (fluid-velocity-transport.wgsl:104-179)
   void correctVelocity() {
-    forActiveCells([&](uint32_t, int slot, int c, int x, int y, int z) {
-      V3<R> pos = center(x, y, z);
+    forActiveVCells([&](uint32_t, int slot, int c, int x, int y, int z) {
+      V3<R> pos = vcenter(x, y, z);
       if (solidAt(pos[0], pos[1], pos[2])) {
-        for (int k = 0; k < 3; k++) velC[((size_t)slot * 3 + k) * N + c] = 0;
+        for (int k = 0; k < 3; k++) velC[((size_t)slot * 3 + k) * VN + c] = 0;
         return;
       }
       V3<R> orig;
-      for (int k = 0; k < 3; k++) orig[k] = vel[((size_t)slot * 3 + k) * N + c];
+      for (int k = 0; k < 3; k++) orig[k] = vel[((size_t)slot * 3 + k) * VN + c];
       for (int comp = 0; comp < 3; comp++) {
-        R predicted = velP[((size_t)slot * 3 + comp) * N + c];
-        const int32_t* d = &vdonor[(((size_t)slot * 3 + comp) * N + c) * 3];
-        int bs = brickSlot(d[0] >> shift, d[1] >> shift, d[2] >> shift);
+        R predicted = velP[((size_t)slot * 3 + comp) * VN + c];
+        const int32_t* d = &vdonor[(((size_t)slot * 3 + comp) * VN + c) * 3];
+        int bs = brickSlot(d[0] >> vshift, d[1] >> vshift, d[2] >> vshift);
         R lo = 0, hi = 0;
         if (bs >= 0) {
-          int lc = local(d[0], d[1], d[2]);
-          lo = vmin[((size_t)bs * 3 + comp) * N + lc];
-          hi = vmax[((size_t)bs * 3 + comp) * N + lc];
+          int lc = vlocal(d[0], d[1], d[2]);
+          lo = vmin[((size_t)bs * 3 + comp) * VN + lc];
+          hi = vmax[((size_t)bs * 3 + comp) * VN + lc];
         }
         R result;
         if (lo == hi && predicted == lo) {
           result = predicted;
         } else {
           V3<R> face = pos;
-          face[comp] += R(0.5) * h;
+          face[comp] += R(0.5) * vh;
           V3<R> fv = velocityOnFace(x, y, z, comp, orig);
           V3<R> mid, fwd;
           for (int a = 0; a < 3; a++) mid[a] = face[a] + R(0.5) * dt * fv[a];
           V3<R> vm = velocityAt(mid);
           for (int a = 0; a < 3; a++) fwd[a] = face[a] + dt * vm[a];
-          fwd[comp] -= R(0.5) * h;
-          R reversed = sampleCells(velP, 3, comp, fwd[0] / h, fwd[1] / h, fwd[2] / h);
+          fwd[comp] -= R(0.5) * vh;
+          R reversed = vsample(velP, 3, comp, fwd[0] / vh, fwd[1] / vh, fwd[2] / vh);
           R corrected = predicted + R(0.5) * (orig[comp] - reversed);
           result = (corrected < lo || corrected > hi) ? predicted : corrected;
         }
-        velC[((size_t)slot * 3 + comp) * N + c] = sv(result);
+        velC[((size_t)slot * 3 + comp) * VN + c] = sv(result);
       }
     });
   }
@@ -1938,7 +2002,7 @@ struct Sim {
     for (int a = 0; a < 3; a++) {
       R side = R(B);
       R loc = R(id[a] & (B - 1)) + R(0.5);
-      R pad = std::min(side, std::max(R(2), R(2)) + std::fabs(v[a]) * dt / h);
+      R pad = std::min(side, std::max(R(2), R(2) * R(vd)) + std::fabs(v[a]) * dt / h);
       low[a] = loc < pad;
       high[a] = loc + pad >= side;
     }
@@ -1995,7 +2059,7 @@ struct Sim {
     for (int a = 0; a < 3; a++) {
       R side = R(SB);
       R loc = R(q[a] & (SB - 1)) + R(0.5);
-      R pad = std::min(side, std::max(R(2), R(2) * (h / sp)) + std::fabs(v[a]) * dt / sp);
+      R pad = std::min(side, std::max(R(2), R(2) * (vh / sp)) + std::fabs(v[a]) * dt / sp);
       low[a] = loc < pad;
       high[a] = loc + pad >= side;
     }
@@ -2122,7 +2186,7 @@ struct Sim {
   // meshCovers (force-fields.wgsl:27-47): a mesh target of force `index` covers velocity cell
   // (x,y,z) while the cell's brick has an id.
   bool meshCovers(int index, int x, int y, int z) {
-    if (brickId(x >> shift, y >> shift, z >> shift) < 0) return false;
+    if (brickId(x >> vshift, y >> vshift, z >> vshift) < 0) return false;
     return coverage.count({index, x, y, z}) != 0;
   }
   // externalForces + coverage (force-fields.wgsl:49-103) at velocity cell (x,y,z), centre p.
@@ -2179,41 +2243,53 @@ struct Sim {
   }
   // computeCurl (fluid-forces.wgsl:38-75) over the corrected velocity.
   void computeCurl() {
-    forActiveCells([&](uint32_t, int slot, int c, int x, int y, int z) {
+    forActiveVCells([&](uint32_t, int slot, int c, int x, int y, int z) {
       auto cc = [&](int px, int py, int pz, int comp) {
         int q[3] = {px, py, pz};
         q[comp] -= 1;
-        return R(0.5) * (cellAt(velC, 3, comp, px, py, pz) + cellAt(velC, 3, comp, q[0], q[1], q[2]));
+        return R(0.5) * (vcell(velC, 3, comp, px, py, pz) + vcell(velC, 3, comp, q[0], q[1], q[2]));
       };
-      R hh = R(0.5) / h;
+      R hh = R(0.5) / vh;
       R dx0 = (cc(x + 1, y, z, 1) - cc(x - 1, y, z, 1)) * hh, dx1 = (cc(x + 1, y, z, 2) - cc(x - 1, y, z, 2)) * hh;
       R dy0 = (cc(x, y + 1, z, 0) - cc(x, y - 1, z, 0)) * hh, dy1 = (cc(x, y + 1, z, 2) - cc(x, y - 1, z, 2)) * hh;
       R dz0 = (cc(x, y, z + 1, 0) - cc(x, y, z - 1, 0)) * hh, dz1 = (cc(x, y, z + 1, 1) - cc(x, y, z - 1, 1)) * hh;
       R cv[3] = {dy1 - dz1, dz0 - dx1, dx0 - dy0};
       R mag = std::sqrt(cv[0] * cv[0] + cv[1] * cv[1] + cv[2] * cv[2]);
-      for (int k = 0; k < 3; k++) curl[((size_t)slot * 4 + k) * N + c] = store_round(cv[k], prec.curl);
-      curl[((size_t)slot * 4 + 3) * N + c] = store_round(mag, prec.curl);
+      for (int k = 0; k < 3; k++) curl[((size_t)slot * 4 + k) * VN + c] = store_round(cv[k], prec.curl);
+      curl[((size_t)slot * 4 + 3) * VN + c] = store_round(mag, prec.curl);
     });
   }
   // centerForce (fluid-forces.wgsl:79-104), cellForce (:113-118)
   V3<R> cellForce(int tile, int x, int y, int z) {
-    if (brickSlot(x >> shift, y >> shift, z >> shift) < 0) return v3<R>(0, 0, 0);
-    V3<R> w = center(x, y, z);
+    if (brickSlot(x >> vshift, y >> vshift, z >> vshift) < 0) return v3<R>(0, 0, 0);
+    V3<R> w = vcenter(x, y, z);
     V3<R> F = v3<R>(0, 0, 0);
     if (!solidAt(w[0], w[1], w[2])) {
-      R heat = cellAt(fld, 4, 1, x, y, z), density = cellAt(fld, 4, 0, x, y, z);
-      // smokeVelocityAverage (smoke.wgsl:4-21) at one velocity cell per smoke spacing or less:
-      // the coarse density sampled at the cell centre.
-      if (smokeDiv > 1) density = coarseSample(smk, w[0] / sp, w[1] / sp, w[2] / sp);
+      R heat = fieldAverage(fld, 4, 1, x, y, z), density = fieldAverage(fld, 4, 0, x, y, z);
+      // smokeVelocityAverage (smoke.wgsl:4-21): at one velocity cell per smoke spacing or less
+      // the coarse density sampled at the cell centre, else the mean of its 2x2x2 blocks.
+      if (smokeDiv > 1) {
+        int ratio = std::max(1, vd / smokeDiv);
+        if (ratio == 1) {
+          density = coarseSample(smk, w[0] / sp, w[1] / sp, w[2] / sp);
+        } else {
+          density = 0;
+          for (int k = 0; k < ratio; k += 2)
+            for (int j = 0; j < ratio; j += 2)
+              for (int i = 0; i < ratio; i += 2)
+                density += coarseSample(smk, R(x * ratio + i + 1), R(y * ratio + j + 1), R(z * ratio + k + 1));
+          density /= R(ratio * ratio * ratio / 8);
+        }
+      }
       V3<R> conf = v3<R>(0, 0, 0);
       if (vorticity != 0) {
-        R c[3] = {cellAt(curl, 4, 0, x, y, z), cellAt(curl, 4, 1, x, y, z), cellAt(curl, 4, 2, x, y, z)};
-        R eta[3] = {cellAt(curl, 4, 3, x + 1, y, z) - cellAt(curl, 4, 3, x - 1, y, z),
-                    cellAt(curl, 4, 3, x, y + 1, z) - cellAt(curl, 4, 3, x, y - 1, z),
-                    cellAt(curl, 4, 3, x, y, z + 1) - cellAt(curl, 4, 3, x, y, z - 1)};
+        R c[3] = {vcell(curl, 4, 0, x, y, z), vcell(curl, 4, 1, x, y, z), vcell(curl, 4, 2, x, y, z)};
+        R eta[3] = {vcell(curl, 4, 3, x + 1, y, z) - vcell(curl, 4, 3, x - 1, y, z),
+                    vcell(curl, 4, 3, x, y + 1, z) - vcell(curl, 4, 3, x, y - 1, z),
+                    vcell(curl, 4, 3, x, y, z + 1) - vcell(curl, 4, 3, x, y, z - 1)};
         R len = std::sqrt(eta[0] * eta[0] + eta[1] * eta[1] + eta[2] * eta[2]) + R(0.0001);
         R n[3] = {eta[0] / len, eta[1] / len, eta[2] / len};
-        R s = vorticity * h;
+        R s = vorticity * vh;
         conf = v3<R>((n[1] * c[2] - n[2] * c[1]) * s, (n[2] * c[0] - n[0] * c[2]) * s, (n[0] * c[1] - n[1] * c[0]) * s);
       }
       V3<R> ext = externalForces(tile, x, y, z, w);
@@ -2250,36 +2326,36 @@ struct Sim {
   // applyForces (fluid-forces.wgsl:151-182), then computeDivergence (:184-203).
   void forcesStep() {
     if (vorticity != 0) computeCurl();
-    forActiveCells([&](uint32_t id, int slot, int c, int x, int y, int z) {
+    forActiveVCells([&](uint32_t id, int slot, int c, int x, int y, int z) {
       int tile = (int)(id >> 6);
       V3<R> F0 = cellForce(tile, x, y, z);
       V3<R> Fx = cellForce(tile, x + 1, y, z), Fy = cellForce(tile, x, y + 1, z), Fz = cellForce(tile, x, y, z + 1);
       R force[3] = {R(0.5) * (F0[0] + Fx[0]), R(0.5) * (F0[1] + Fy[1]), R(0.5) * (F0[2] + Fz[2])};
-      V3<R> pos = center(x, y, z);
+      V3<R> pos = vcenter(x, y, z);
       R decay = std::exp(-damping * dt);
       R v[3];
-      for (int a = 0; a < 3; a++) v[a] = velC[((size_t)slot * 3 + a) * N + c] * decay + dt * force[a];
+      for (int a = 0; a < 3; a++) v[a] = velC[((size_t)slot * 3 + a) * VN + c] * decay + dt * force[a];
       R out[3];
       for (int a = 0; a < 3; a++) {
         V3<R> face = pos;
-        face[a] += R(0.5) * h;
+        face[a] += R(0.5) * vh;
         out[a] = sourceVelocity(tile, v[a], face, a);
       }
       // enforceFaces (fluid-forces.wgsl:15-31)
       if (solidAt(pos[0], pos[1], pos[2])) {
         out[0] = out[1] = out[2] = 0;
       } else {
-        if (solidAt(pos[0] + h, pos[1], pos[2])) out[0] = 0;
-        if (solidAt(pos[0], pos[1] + h, pos[2])) out[1] = 0;
-        if (solidAt(pos[0], pos[1], pos[2] + h)) out[2] = 0;
+        if (solidAt(pos[0] + vh, pos[1], pos[2])) out[0] = 0;
+        if (solidAt(pos[0], pos[1] + vh, pos[2])) out[1] = 0;
+        if (solidAt(pos[0], pos[1], pos[2] + vh)) out[2] = 0;
       }
-      for (int a = 0; a < 3; a++) velF[((size_t)slot * 3 + a) * N + c] = sv(out[a]);
+      for (int a = 0; a < 3; a++) velF[((size_t)slot * 3 + a) * VN + c] = sv(out[a]);
     });
-    forActiveCells([&](uint32_t, int slot, int c, int x, int y, int z) {
-      R d = (velF[((size_t)slot * 3 + 0) * N + c] - cellAt(velF, 3, 0, x - 1, y, z)) / h +
-            (velF[((size_t)slot * 3 + 1) * N + c] - cellAt(velF, 3, 1, x, y - 1, z)) / h +
-            (velF[((size_t)slot * 3 + 2) * N + c] - cellAt(velF, 3, 2, x, y, z - 1)) / h;
-      div[(size_t)slot * N + c] = store_round(h * h * (d - expn[(size_t)slot * N + c]), prec.p0);
+    forActiveVCells([&](uint32_t, int slot, int c, int x, int y, int z) {
+      R d = (velF[((size_t)slot * 3 + 0) * VN + c] - vcell(velF, 3, 0, x - 1, y, z)) / vh +
+            (velF[((size_t)slot * 3 + 1) * VN + c] - vcell(velF, 3, 1, x, y - 1, z)) / vh +
+            (velF[((size_t)slot * 3 + 2) * VN + c] - vcell(velF, 3, 2, x, y, z - 1)) / vh;
+      div[(size_t)slot * VN + c] = store_round(vh * vh * (d - fieldAverage(expn, 1, 0, x, y, z)), prec.p0);
     });
   }
 
@@ -2329,7 +2405,7 @@ struct Sim {
     return true;
   }
   bool blockedAt(int px, int py, int pz, int level) {
-    R s = h * R(1 << level);
+    R s = vh * R(1 << level);
     return solidAt((R(px) + R(0.5)) * s, (R(py) + R(0.5)) * s, (R(pz) + R(0.5)) * s);
   }
   uint8_t cellTopology(int px, int py, int pz, int level) {
@@ -2631,8 +2707,8 @@ struct Sim {
   bool pressureUnknown(int px, int py, int pz) {
     int p[3] = {px, py, pz}, lo[3], hi[3];
     for (int a = 0; a < 3; a++) {
-      lo[a] = (p[a] - 1) >> shift;
-      hi[a] = p[a] >> shift;
+      lo[a] = (p[a] - 1) >> vshift;
+      hi[a] = p[a] >> vshift;
     }
     if (ground) lo[1] = std::max(lo[1], 0);
     for (int z = lo[2]; z <= hi[2]; z++)
@@ -2642,34 +2718,34 @@ struct Sim {
     return true;
   }
   R cellPressure(int x, int y, int z) {
-    int s = brickSlot(x >> shift, y >> shift, z >> shift);
+    int s = brickSlot(x >> vshift, y >> vshift, z >> vshift);
     if (s < 0) return 0;
-    return pres[latest][(size_t)s * N + local(x, y, z)];
+    return pres[latest][(size_t)s * VN + vlocal(x, y, z)];
   }
   // project (fluid-forces.wgsl:205-262) into the velocity pool of the next step.
   void projectStep() {
     std::vector<R> out(vel.size(), 0);
-    forActiveCells([&](uint32_t, int slot, int c, int x, int y, int z) {
-      V3<R> pos = center(x, y, z);
+    forActiveVCells([&](uint32_t, int slot, int c, int x, int y, int z) {
+      V3<R> pos = vcenter(x, y, z);
       R res[3] = {0, 0, 0};
       if (!solidAt(pos[0], pos[1], pos[2])) {
-        R cp = pres[latest][(size_t)slot * N + c];
+        R cp = pres[latest][(size_t)slot * VN + c];
         bool pu = pressureUnknown(x, y, z);
         for (int a = 0; a < 3; a++) {
           int n[3] = {x, y, z};
           n[a] += 1;
-          R v = velF[((size_t)slot * 3 + a) * N + c];
-          V3<R> nc = center(n[0], n[1], n[2]);
+          R v = velF[((size_t)slot * 3 + a) * VN + c];
+          V3<R> nc = vcenter(n[0], n[1], n[2]);
           if (solidAt(nc[0], nc[1], nc[2])) {
             res[a] = 0;
           } else if (!pu && !pressureUnknown(n[0], n[1], n[2])) {
             res[a] = 0;
           } else {
-            res[a] = v - (cellPressure(n[0], n[1], n[2]) - cp) / h;
+            res[a] = v - (cellPressure(n[0], n[1], n[2]) - cp) / vh;
           }
         }
       }
-      for (int a = 0; a < 3; a++) out[((size_t)slot * 3 + a) * N + c] = sv(res[a]);
+      for (int a = 0; a < 3; a++) out[((size_t)slot * 3 + a) * VN + c] = sv(res[a]);
     });
     vel.swap(out);
   }
@@ -2848,6 +2924,7 @@ int64_t or_info(or_sim* s, int what) {
       case 7: return sim.lastFailures;
       case 8: return sim.dir.count();
       case 9: return sim.SN;  // coarse smoke cells a brick (smokeDivisor > 1)
+      case 10: return sim.VN;  // velocity and pressure cells a brick
     }
     return -1;
   };

@@ -61,6 +61,7 @@ def lib():
 
 CHANNELS = {0: 3, 1: 4, 2: 1, 3: 1, 4: 1, 5: 4, 6: 1}
 SMOKE_FIELD = 6  # the coarse smoke grid: (B / smoke_divisor)^3 cells a slot
+VELOCITY_FIELDS = (0, 3, 4, 5)  # the velocity lattice: (B / velocity_divisor)^3 cells a slot
 
 
 class OracleSim:
@@ -126,7 +127,7 @@ class OracleSim:
         return self.info(3)
 
     def field(self, fid: int, f64: bool = False) -> np.ndarray:
-        cells = self.info(9) if fid == SMOKE_FIELD else self.cells
+        cells = self.info(9) if fid == SMOKE_FIELD else (self.info(10) if fid in VELOCITY_FIELDS else self.cells)
         n = self.slots * CHANNELS[fid] * cells
         if f64:
             out = np.empty(n, np.float64)

@@ -85,6 +85,42 @@ def test_brick16():
     check(run(sc, 12, budget=2 ** 21))
 
 
+@pytest.mark.parametrize("vd,brick", [(2, 8), (4, 8), (2, 16), (4, 32)])
+def test_velocity_divisor(vd, brick):
+    """velocityDivisor 2 and 4 (FluidSimulation.ts:365-373): velocity, curl, divergence and
+    pressure on a lattice of B/d cells a brick side at spacing h d, the scalars on the field
+    lattice; traces sample the coarse velocity, forces read the field cells' means
+    (velocityCellAverage), the divergence the expansion's mean; solids at the coarse cells'
+    centres; every force kind and collider of the force scene."""
+    sc = scenes.ForceScene()
+    sc.brick_size = brick
+    sc.velocity_divisor = vd
+    check(run(sc, 12, budget=2 ** 22 if brick == 32 else 2 ** 20), min_active=8)
+
+
+def test_velocity_divisor_plume():
+    sc = scenes.SinglePlume()
+    sc.velocity_divisor = 2
+    check(run(sc, 24, budget=2 ** 19), min_active=216)
+
+
+@pytest.mark.parametrize("form", ["mesh_target", "coarse_smoke_2", "coarse_smoke_4"])
+def test_velocity_divisor_forms(form):
+    """The velocity lattice with mesh emission and mesh force targets (the face's field cell,
+    coverage of velocity cells), and with coarse smoke at a spacing below, equal to and above
+    the velocity cell (smokeVelocityAverage)."""
+    if form == "mesh_target":
+        sc = scenes.MeshTargetScene()
+        sc.velocity_divisor = 2
+        grid = sc.grid(budget=2 ** 20)
+    else:
+        sc = scenes.ForceScene()
+        sc.velocity_divisor = 4 if form == "coarse_smoke_2" else 2
+        grid = sc.grid(budget=2 ** 20)
+        grid.smoke_divisor = 2 if form == "coarse_smoke_2" else 4
+    check(run(sc, 12, grid=grid, budget=2 ** 20), min_active=8)
+
+
 def test_brick32():
     """32^3 bricks (brickSize 32): five brick levels, 32^3 staged multigrid relaxation and
     restriction, forces in 16^3 cubes."""

@@ -27,7 +27,8 @@ __device__ bool sourceNear(const SimParams& P, int tile, int bx, int by, int bz)
     for (int a = 0; a < 3; a++) {
       // Rounded products and sums, never contracted: an integer decision the oracle repeats.
       float motion = fabsf(e.vel[a]) + fabsf(e.outward);
-      float pad = fminf(size, __fadd_rn(__fmul_rn(2.f, P.h), __fmul_rn(motion, P.dt)));
+      // two velocity cells (spacing h d, exact) and a step of motion
+      float pad = fminf(size, __fadd_rn(__fmul_rn(2.f, P.h * (float)P.velDiv), __fmul_rn(motion, P.dt)));
       float extent = fmaxf(e.size[a], 0.03f) + pad;
       if (!(e.pos[a] + extent > lo[a] && e.pos[a] - extent < hi[a])) inside = false;
     }
@@ -412,13 +413,14 @@ __global__ void __launch_bounds__(256) k_zero_fresh(FpBatch bt) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_FRESH, item, i);
     size_t slot = P.zeroList[2 * i + 1];
-    float4* v = reinterpret_cast<float4*>(P.vel + slot * 3 * P.N);
+    const int VN = P.vview->N;  // the velocity lattice's cells a slot
+    float4* v = reinterpret_cast<float4*>(P.vel + slot * 3 * VN);
     // The scalar pool holds 4 channels of 4 bytes (FP32) or 2 bytes (FP16) a cell.
     const int scalarBytes = P.scalarHalf ? 2 : 4;
     float4* f = reinterpret_cast<float4*>(reinterpret_cast<char*>(P.fld) + slot * 4 * P.N * scalarBytes);
     float4* e = reinterpret_cast<float4*>(P.expn + slot * P.N);
     float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int k = threadIdx.x; k < 3 * P.N / 4; k += blockDim.x) v[k] = z;
+    for (int k = threadIdx.x; k < 3 * VN / 4; k += blockDim.x) v[k] = z;
     for (int k = threadIdx.x; k < P.N * scalarBytes / 4; k += blockDim.x) f[k] = z;
     for (int k = threadIdx.x; k < P.N / 4; k += blockDim.x) e[k] = z;
     // Coarse smoke's state in the scalars' width (zeroSmokeBricks, smoke.wgsl:188-223); a

@@ -51,7 +51,6 @@ static int validateGrid(const fp_grid* grid) {
     return failed("precision must be FP_PRECISION_FP32 or FP_PRECISION_MIXED.", FP_EINVAL);
   if (!(grid->voxel_budget >= 0) || !std::isfinite(grid->voxel_budget))
     return failed("voxel_budget must be a finite, nonnegative voxel count.", FP_EINVAL);
-  if (vd != 1) return failed("velocityDivisor 2 and 4 are not implemented by this build.", FP_EUNSUPPORTED);
   return FP_OK;
 }
 

@@ -159,6 +159,21 @@ FP_DEV float sampleCells(const SimParams& P, const Home& H, const float* pool, i
   return blend8(t, fx, fy, fz);
 }
 
+// velocityCellAverage (fluid-sampling.wgsl:268-285): the mean of the field cells under velocity
+// cell (x,y,z) when the velocity divisor d is above 1, through the field view F: a trilinear
+// sample on the shared corner of a 2x2x2 block of field cells is that block's mean.
+FP_DEV float fieldAverage(const SimParams& F, const Home& H, const float* pool, int ch, int c, int x, int y, int z,
+                          bool half) {
+  const int d = F.velDiv, blocks = d >> 1;
+  float sum = 0.f;
+  for (int k = 0; k < blocks; k++)
+    for (int j = 0; j < blocks; j++)
+      for (int i = 0; i < blocks; i++)
+        sum += sampleCells(F, H, pool, ch, c, (float)(x * d + 1 + 2 * i), (float)(y * d + 1 + 2 * j),
+                           (float)(z * d + 1 + 2 * k), half);
+  return sum / (float)(blocks * blocks * blocks);
+}
+
 // The coarse smoke grid (fluid-sampling.wgsl:4-20: every grid shares the brick footprint with
 // its own cells a side, here 2^P.smokeShift): cell (x,y,z) of a [slot][smokeCells] pool, zero
 // in a brick without a slot, and the trilinear sample at `q` in its cells, centres at .5.
@@ -193,18 +208,30 @@ FP_DEV const FpMeshSource* meshSourceAt(const SimParams& P, const Home& H, int x
   return r > 0 ? &P.meshSources[r] : nullptr;
 }
 
-// solidCell (solids.wgsl:15-31): the ground, then colliders drawn into each slot's bits.
-FP_DEV bool solidCell(const SimParams& P, const Home& H, int x, int y, int z) {
+// solidCell (solids.wgsl:15-31) of field cell (x,y,z): the ground, then colliders drawn into
+// each slot's bits.
+FP_DEV bool solidFine(const SimParams& P, const Home& H, int x, int y, int z) {
   if (P.ground && y < 0) return true;
   if (P.colliderCount == 0) return false;
-  int s = brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift);
+  const int fs = P.fshift, m = (1 << fs) - 1;
+  int s = brickSlot(P, H, x >> fs, y >> fs, z >> fs);
   if (s < 0) return false;
-  int bit = localCell(P, x, y, z);
+  int bit = (((z & m) << fs | (y & m)) << fs) | (x & m);
   return ((P.solids[(size_t)s * P.W + (bit >> 5)] >> (bit & 31)) & 1u) != 0u;
+}
+// solidAt at the centre of cell (x,y,z) of this lattice: ((x + .5) s h) / h + .25 floors to
+// field cell x s + s/2 (s = solidSpan; x itself on the field lattice).
+FP_DEV bool solidCell(const SimParams& P, const Home& H, int x, int y, int z) {
+  if (P.solidSpan > 1) {
+    const int s = P.solidSpan, o = s >> 1;
+    return solidFine(P, H, x * s + o, y * s + o, z * s + o);
+  }
+  return solidFine(P, H, x, y, z);
 }
 // fieldCell (solids.wgsl:7-9) and solidAt (:33-35).
 FP_DEV bool solidAt(const SimParams& P, const Home& H, float wx, float wy, float wz) {
-  return solidCell(P, H, (int)floorf(wx / P.h + 0.25f), (int)floorf(wy / P.h + 0.25f), (int)floorf(wz / P.h + 0.25f));
+  return solidFine(P, H, (int)floorf(wx / P.fineH + 0.25f), (int)floorf(wy / P.fineH + 0.25f),
+                   (int)floorf(wz / P.fineH + 0.25f));
 }
 
 FP_DEV float mixf(float a, float b, float t) { return a * (1.f - t) + b * t; }

@@ -160,7 +160,12 @@ Engine::Engine(const fp_grid& g, Stepper* owner) : owner_(owner) {
   shift_ = B_ == 8 ? 3 : (B_ == 16 ? 4 : 5);
   N_ = B_ * B_ * B_;
   W_ = N_ / 32;
-  brickLevels_ = shift_;
+  vd_ = g.velocity_divisor > 1 ? g.velocity_divisor : 1;
+  VB_ = B_ / vd_;
+  vshift_ = 0;
+  while ((1 << vshift_) < VB_) vshift_++;
+  VN_ = VB_ * VB_ * VB_;
+  brickLevels_ = vshift_;  // the pressure lives on the velocity lattice
   bottom_ = brickLevels_ + 2;
   h_ = g.voxel_size;
   maccormack_ = g.scalar_maccormack != 0;
@@ -252,17 +257,20 @@ int Engine::initialize() {
 // Device bytes of a simulation of `g` once its pools exist: per slot the pools and the brick
 // levels, per tile slot (at the minimum capacity) the tables and tile levels.
 uint64_t Engine::estimateBytes(const fp_grid& g, uint32_t tiles) {
-  int B = g.brick_size, shift = B == 8 ? 3 : (B == 16 ? 4 : 5);
-  uint64_t N = (uint64_t)B * B * B;
+  int B = g.brick_size, vd = g.velocity_divisor > 1 ? g.velocity_divisor : 1, vshift = 0;
+  while ((1 << vshift) < B / vd) vshift++;
+  uint64_t N = (uint64_t)B * B * B, VN = N / ((uint64_t)vd * vd * vd);
   double budget = g.voxel_budget > 0 ? g.voxel_budget : 8e6;
   uint64_t slots = (uint64_t)std::max(1.0, std::floor(budget / (double)N));
-  // FP32: velocity x4 (3 channels), curl, expansion, divergence, bounds (3+3+8), pressure x2,
-  // the scalar predictor (4); the two scalar state pools (4 channels) and the coarse levels in
+  // FP32 on the velocity lattice: velocity x4 (3 channels), curl, divergence, bounds (3+3),
+  // pressure x2, donors, topology; on the field lattice: expansion, scalar bounds (8), the scalar
+  // predictor (4), solid bits; the two scalar state pools (4 channels) and the coarse levels in
   // the precision's width.
   const uint64_t narrow = g.precision == FP_PRECISION_MIXED ? 2 : 4;
-  uint64_t perSlot = N * 4 * (4 * 3 + 4 + 1 + 1 + 3 + 3 + 8 + 2 + 4) + N * 2 * 4 * narrow + N * 3 * 2 + N / 8 + N + 4;
-  for (int l = 1; l < shift; l++) {
-    uint64_t c = (uint64_t)1 << (3 * (shift - l));
+  uint64_t perSlot = VN * 4 * (4 * 3 + 4 + 1 + 3 + 3 + 2) + VN * 3 * 2 + VN + N * 4 * (1 + 8 + 4) +
+                     N * 2 * 4 * narrow + N / 8 + 4;
+  for (int l = 1; l < vshift; l++) {
+    uint64_t c = (uint64_t)1 << (3 * (vshift - l));
     perSlot += c * (3 * narrow + 1);
   }
   if (g.smoke_divisor > 1) {  // coarse smoke: state pair, FP32 predictor, donor range
@@ -300,15 +308,15 @@ int Engine::reserveTiles(uint32_t tiles) {
 
 // Pools of `slots` slots, all free: the stack pops slot 0 first.
 int Engine::allocatePools(uint32_t slots) {
-  size_t s = slots, N = N_;
+  size_t s = slots, N = N_, VN = VN_;  // field and velocity lattice cells a slot
   bool ok = true;
-  for (auto& b : vel_) ok = ok && alloc(b, s * 3 * N * 4);
+  for (auto& b : vel_) ok = ok && alloc(b, s * 3 * VN * 4);
   // fld_[1] is the predictor within a step (FP32); fld_[0] and fld_[2] trade the state.
   for (int k = 0; k < 3; k++) ok = ok && alloc(fld_[k], s * 4 * N * (k == 1 ? 4 : scalarBytes()));
-  ok = ok && alloc(curl_, s * 4 * N * 4) && alloc(expn_, s * N * 4) && alloc(div_, s * N * 4) &&
-       alloc(vmin_, s * 3 * N * 4) && alloc(vmax_, s * 3 * N * 4) && alloc(sb_, s * 8 * N * 4) &&
-       alloc(donors_, s * 3 * N * 2) && alloc(solids_, s * W_ * 4) && alloc(p0_[0], s * N * 4) &&
-       alloc(p0_[1], s * N * 4) && alloc(topo_[0], s * N) && alloc(freeStack_, s * 4);
+  ok = ok && alloc(curl_, s * 4 * VN * 4) && alloc(expn_, s * N * 4) && alloc(div_, s * VN * 4) &&
+       alloc(vmin_, s * 3 * VN * 4) && alloc(vmax_, s * 3 * VN * 4) && alloc(sb_, s * 8 * N * 4) &&
+       alloc(donors_, s * 3 * VN * 2) && alloc(solids_, s * W_ * 4) && alloc(p0_[0], s * VN * 4) &&
+       alloc(p0_[1], s * VN * 4) && alloc(topo_[0], s * VN) && alloc(freeStack_, s * 4);
   for (int l = 1; l < brickLevels_ && ok; l++) {
     size_t c = s * levelCells(l);
     ok = alloc(lp_[l][0], c * coarseBytes()) && alloc(lp_[l][1], c * coarseBytes()) &&
@@ -334,15 +342,15 @@ int Engine::allocatePools(uint32_t slots) {
 int Engine::growPool(uint32_t target) {
   if (target <= slots_) return FP_OK;
   cudaStreamSynchronize(stream());
-  size_t s = target, N = N_;
+  size_t s = target, N = N_, VN = VN_;
   uint32_t added = target - slots_;
   bool ok = true;
-  for (auto& b : vel_) ok = ok && grow(b, s * 3 * N * 4, 0);
+  for (auto& b : vel_) ok = ok && grow(b, s * 3 * VN * 4, 0);
   for (int k = 0; k < 3; k++) ok = ok && grow(fld_[k], s * 4 * N * (k == 1 ? 4 : scalarBytes()), 0);
-  ok = ok && grow(curl_, s * 4 * N * 4, 0) && grow(expn_, s * N * 4, 0) && grow(div_, s * N * 4, 0) &&
-       grow(vmin_, s * 3 * N * 4, 0) && grow(vmax_, s * 3 * N * 4, 0) && grow(sb_, s * 8 * N * 4, 0) &&
-       grow(donors_, s * 3 * N * 2, 0) && grow(solids_, s * W_ * 4, 0) && grow(p0_[0], s * N * 4, 0) &&
-       grow(p0_[1], s * N * 4, 0) && grow(topo_[0], s * N, 0);
+  ok = ok && grow(curl_, s * 4 * VN * 4, 0) && grow(expn_, s * N * 4, 0) && grow(div_, s * VN * 4, 0) &&
+       grow(vmin_, s * 3 * VN * 4, 0) && grow(vmax_, s * 3 * VN * 4, 0) && grow(sb_, s * 8 * N * 4, 0) &&
+       grow(donors_, s * 3 * VN * 2, 0) && grow(solids_, s * W_ * 4, 0) && grow(p0_[0], s * VN * 4, 0) &&
+       grow(p0_[1], s * VN * 4, 0) && grow(topo_[0], s * VN, 0);
   for (int l = 1; l < brickLevels_ && ok; l++) {
     size_t c = s * levelCells(l);
     ok = grow(lp_[l][0], c * coarseBytes(), 0) && grow(lp_[l][1], c * coarseBytes(), 0) &&
@@ -673,7 +681,8 @@ bool Engine::packScene(const fp_frame& f) {
           k.hasMesh = 1.f;
           if (!f.target_cell_ranges || f.target_cell_ranges[2 * (s.first_target + t) + 1] == 0) continue;
           for (int a = 0; a < 3; a++) {
-            double l = (double)src.position[a] - (double)h_, u = (double)src.size[a] + (double)h_;
+            const double vh = (double)h_ * vd_;  // a velocity cell
+            double l = (double)src.position[a] - vh, u = (double)src.size[a] + vh;
             lo[a] = has ? std::min(lo[a], l) : l;
             hi[a] = has ? std::max(hi[a], u) : u;
           }
@@ -730,8 +739,9 @@ bool Engine::packScene(const fp_frame& f) {
   if (coverageOn_ && (targets != coverageTargets_ || coverageVersion_ != tileVersion_)) {
     coverageTargets_ = targets;
     coverageVersion_ = tileVersion_;
-    const size_t bricks = (size_t)capacity_ * 64, words = 1 + (size_t)(N_ + 31) / 32;
-    const int mask = B_ - 1;
+    // Velocity cells: the coverage lives on the velocity lattice (force-fields.wgsl:27-47).
+    const size_t bricks = (size_t)capacity_ * 64, words = 1 + (size_t)(VN_ + 31) / 32;
+    const int mask = VB_ - 1;
     std::map<int, std::map<int, std::vector<uint32_t>>> entries;  // brick id -> force -> bits
     std::vector<int> order;                                        // brick ids, first seen first
     for (size_t p = 0; p < targets.size();) {
@@ -739,7 +749,7 @@ bool Engine::packScene(const fp_frame& f) {
       const int32_t* cells = &targets[p + 2];
       for (int c = 0; c < n; c++) {
         const int32_t* cell = cells + 3 * c;
-        int b[3] = {cell[0] >> shift_, cell[1] >> shift_, cell[2] >> shift_};
+        int b[3] = {cell[0] >> vshift_, cell[1] >> vshift_, cell[2] >> vshift_};
         int slot = dir_.slotAt(b[0] >> 2, b[1] >> 2, b[2] >> 2);
         if (slot < 0) continue;
         int id = slot * 64 + (((b[2] & 3) * 4 + (b[1] & 3)) * 4 + (b[0] & 3));
@@ -747,7 +757,7 @@ bool Engine::packScene(const fp_frame& f) {
         if (forcesOf.empty()) order.push_back(id);
         auto& bits = forcesOf[index];
         if (bits.empty()) bits.assign(words - 1, 0u);
-        int bit = (((cell[2] & mask) * B_) + (cell[1] & mask)) * B_ + (cell[0] & mask);
+        int bit = (((cell[2] & mask) * VB_) + (cell[1] & mask)) * VB_ + (cell[0] & mask);
         bits[bit >> 5] |= 1u << (bit & 31);
       }
       p += 2 + 3 * (size_t)n;
@@ -874,7 +884,8 @@ static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 size_t Engine::sceneBytes() const {
   return align256(emitters_.size() * sizeof(FpEmitter)) + align256(colliders_.size() * sizeof(FpCollider)) +
          align256(masks_.size() * 4) + align256(forces_.size() * sizeof(FpForce)) +
-         align256(regions_.size() * sizeof(FpRegion)) + align256(tileLists_.size() * 4);
+         align256(regions_.size() * sizeof(FpRegion)) + align256(tileLists_.size() * 4) +
+         (vd_ > 1 ? align256(sizeof(SimParams)) : 0);  // the velocity view
 }
 
 void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t off, const fp_frame& f, float dt,
@@ -989,6 +1000,27 @@ void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t
   }
   P.flame = flame_;
   P.noise = noise;
+  // The lattice views: this SimParams is the field view, and the velocity view too when d = 1;
+  // with d > 1 the velocity view follows the scene, alike but for its lattice.
+  P.velDiv = vd_;
+  P.solidSpan = 1;
+  P.fshift = shift_;
+  P.fineH = h_;
+  const SimParams* self = reinterpret_cast<const SimParams*>(devBase + (reinterpret_cast<uint8_t*>(&P) - hostBase));
+  P.fview = self;
+  P.vview = self;
+  if (vd_ > 1) {
+    SimParams* V = reinterpret_cast<SimParams*>(hostBase + off);
+    P.vview = reinterpret_cast<const SimParams*>(devBase + off);
+    off += align256(sizeof(SimParams));
+    *V = P;
+    V->B = VB_;
+    V->shift = vshift_;
+    V->N = VN_;
+    V->h = h_ * (float)vd_;
+    V->invH = 1.f / V->h;
+    V->solidSpan = vd_;
+  }
   stepH2d_ = h2d_ + sizeof(SimParams) + sceneBytes();
   stepD2h_ = readbackWords() * 4;
   h2d_ = 0;
@@ -1128,7 +1160,9 @@ int Engine::readField(int field, float* host, size_t bytes) {
       break;
     default: return fail(FP_EINVAL, "unknown field");
   }
-  const size_t cells = field == FP_FIELD_SMOKE ? (size_t)SN_ : (size_t)N_;
+  const bool velocityLattice =
+      field == FP_FIELD_VELOCITY || field == FP_FIELD_PRESSURE || field == FP_FIELD_DIVERGENCE || field == FP_FIELD_CURL;
+  const size_t cells = field == FP_FIELD_SMOKE ? (size_t)SN_ : (velocityLattice ? (size_t)VN_ : (size_t)N_);
   size_t need = (size_t)slots_ * ch * cells * 4;
   if (bytes != need) return fail(FP_EINVAL, "field buffer size mismatch: need " + std::to_string(need) + " bytes");
   int rc = consume();

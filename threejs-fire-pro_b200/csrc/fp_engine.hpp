@@ -104,6 +104,7 @@ class Engine {
   int capacity() const { return capacity_; }
   int liveTiles() const { return (int)liveTiles_.size(); }
   int smokeDivisor() const { return smokeDiv_; }
+  int velocityDivisor() const { return vd_; }
   size_t readbackWords() const { return (sizeof(FpCounters) + sizeof(FpSolver)) / 4 + (size_t)capacity_; }
   // Pressure solve (no reference counterpart; the reference runs one V-cycle): up to
   // `vcycles` V-cycles a step, stopping at a relative FP64 residual of `tolerance` (0: all).
@@ -126,6 +127,7 @@ class Engine {
   Stepper* owner_;
   // configuration
   int B_, shift_, N_, W_, brickLevels_, bottom_;
+  int vd_, VB_, vshift_, VN_;  // the velocity lattice: velocityDivisor d, B/d cells a side
   float h_;
   bool maccormack_;
   int precision_;
@@ -272,6 +274,7 @@ class Stepper {
 
  private:
   int device_, B_, brickLevels_, bottom_;
+  int vd_ = 0;  // the simulations' velocity divisor, from the first step
   int sms_ = 148;
   cudaStream_t stream_ = nullptr;
   cudaEvent_t readEvent_ = nullptr;

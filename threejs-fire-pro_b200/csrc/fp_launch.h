@@ -11,14 +11,14 @@ void fp_launch_allocation(const FpBatch& bt, bool solidsFresh, bool solidsAll, i
 int fp_allocation_launches(bool solidsFresh, bool solidsAll);
 // The measurement of every simulation into its host-mapped readback words.
 void fp_launch_readback(const FpBatch& bt, int sms, cudaStream_t st);
-void fp_launch_predict(const FpBatch& bt, int B, int sms, cudaStream_t st);
-void fp_launch_correct(const FpBatch& bt, int B, int sms, cudaStream_t st);
-void fp_launch_evolve(const FpBatch& bt, int B, int sms, cudaStream_t st);
+void fp_launch_predict(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st);
+void fp_launch_correct(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st);
+void fp_launch_evolve(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st);
 // Coarse smoke (smoke_divisor > 1): advection with the donors' range, then evolution with
 // source production and content flags; simulations without coarse smoke skip both.
 void fp_launch_smoke(const FpBatch& bt, int sms, cudaStream_t st);
-void fp_launch_curl(const FpBatch& bt, int B, int sms, cudaStream_t st);
-void fp_launch_forces(const FpBatch& bt, int B, int sms, cudaStream_t st);
+void fp_launch_curl(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st);
+void fp_launch_forces(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st);
 // Divergence with the finest level's first iterate into p0[pSel]; projection with p0[pSel].
 void fp_launch_divergence(const FpBatch& bt, int pSel, int sms, cudaStream_t st);
 void fp_launch_project(const FpBatch& bt, int pSel, int sms, cudaStream_t st);

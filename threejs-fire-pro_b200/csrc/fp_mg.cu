@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
   for (uint32_t base = blockIdx.x * NG; base < total; base += gridDim.x * NG) {
     uint32_t item = base + g;
     uint32_t i;
-    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item < total ? item : base, i);
+    const SimParams& P = *workSim(bt, FP_WORK_ACTIVE, item < total ? item : base, i).vview;
     const Args A = resolve(P, Sl);
     const bool has = item < total && !A.skip;
     const int fineLevel = OP == RESTRICT ? A.level - 1 : A.level;
@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(64) k_level_tiles(FpBatch bt, MgSel Sl) {
   uint32_t total = workTotal(bt, FP_WORK_TILES);
   for (uint32_t item = blockIdx.x * NT + g; item < total; item += gridDim.x * NT) {
     uint32_t local;
-    const SimParams& P = workSim(bt, FP_WORK_TILES, item, local);
+    const SimParams& P = *workSim(bt, FP_WORK_TILES, item, local).vview;
     const int t = P.liveTiles[local];
     const Args A = resolve(P, Sl);
     if (A.skip) continue;
@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
                           nbrIndex(0, -1, 0), nbrIndex(0, 0, 1), nbrIndex(0, 0, -1)};
   int sims = batchCount(bt);
   for (int sim = blockIdx.x; sim < sims; sim += gridDim.x) {
-    const SimParams& P = bt.sims[sim];
+    const SimParams& P = *bt.sims[sim].vview;
     const Args A = resolve(P, Sl);
     if (A.skip) continue;  // the same for the whole CTA
     const int level = A.level, L = P.liveCount;
@@ -620,7 +620,7 @@ __global__ void __launch_bounds__(1024) k_coarse(FpBatch bt, MgSel Sl, int itera
                           nbrIndex(0, -1, 0), nbrIndex(0, 0, 1), nbrIndex(0, 0, -1)};
   const int sims = batchCount(bt);
   for (int sim = blockIdx.x; sim < sims; sim += gridDim.x) {
-    const SimParams& P = bt.sims[sim];
+    const SimParams& P = *bt.sims[sim].vview;
     const Args A = resolve(P, Sl);
     if (A.skip) continue;  // the same for the whole CTA
     // Shared arrays by live position j (tile slot P.liveTiles[j]); level L cells at j * 8 + o.
@@ -774,7 +774,7 @@ __global__ void __launch_bounds__(256) k_residual(FpBatch bt, int pSel, int cycl
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
-    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
+    const SimParams& P = *workSim(bt, FP_WORK_ACTIVE, item, i).vview;
     if (cycle > 0 && P.solver->converged) continue;  // the same for the whole CTA
     Home H = enterBrick(P, P.active[i], nslot);
     const float* p = P.p0[pSel];
@@ -810,7 +810,7 @@ __global__ void __launch_bounds__(256) k_residual(FpBatch bt, int pSel, int cycl
 __global__ void k_converge(FpBatch bt, int cycle) {
   int sims = batchCount(bt);
   for (int sim = threadIdx.x; sim < sims; sim += blockDim.x) {
-    const SimParams& P = bt.sims[sim];
+    const SimParams& P = *bt.sims[sim].vview;
     FpSolver* S = P.solver;
     if (cycle > 0 && S->converged) continue;
     S->cycles = cycle + 1;
@@ -823,10 +823,10 @@ __global__ void k_converge(FpBatch bt, int cycle) {
 
 // cellTopology (pressure.wgsl:208-222): solid, or the sides whose neighbours are not solid.
 FP_DEV uint8_t cellTopology(const SimParams& P, const Home& H, int px, int py, int pz, int level) {
-  // solidAt at the centre of a level's cell, ((x + .5) 2^level h) / h + .25, floors to the
-  // level-0 cell x 2^level + 2^(level-1) (x itself at level 0): solidCell of that cell.
-  const int span = 1 << level, half = span >> 1;
-  auto blocked = [&](int x, int y, int z) { return solidCell(P, H, x * span + half, y * span + half, z * span + half); };
+  // solidAt at the centre of a level's cell, ((x + .5) s h) / h + .25 with s = 2^level field
+  // cells a level-0 cell side (solidSpan), floors to field cell x s + s/2 (x itself for s = 1).
+  const int span = (1 << level) * P.solidSpan, half = span >> 1;
+  auto blocked = [&](int x, int y, int z) { return solidFine(P, H, x * span + half, y * span + half, z * span + half); };
   if (blocked(px, py, pz)) return FP_STORED_SOLID;
   uint8_t flags = 0;
   if (!blocked(px + 1, py, pz)) flags |= 1;
@@ -848,7 +848,7 @@ __global__ void __launch_bounds__(128) k_topo_bricks(FpBatch bt) {
   uint32_t total = workTotal(bt, kind);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
-    const SimParams& P = workSim(bt, kind, item, i);
+    const SimParams& P = *workSim(bt, kind, item, i).vview;
     if ((P.topoAll != 0) != ALL) continue;  // uniform across the CTA
     uint32_t id;
     int slot;
@@ -901,7 +901,7 @@ __global__ void __launch_bounds__(64) k_tile_masks(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_TILES);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t local;
-    const SimParams& P = workSim(bt, FP_WORK_TILES, item, local);
+    const SimParams& P = *workSim(bt, FP_WORK_TILES, item, local).vview;
     const int t = P.liveTiles[local];
     const size_t id = (size_t)t * 64 + threadIdx.x;
     bool on = __ldg(&P.tileRec[t]).w != 0 && P.entries[id] >= 0 && P.records[id * FP_RECORD_WORDS + 27] != 0;
@@ -915,7 +915,7 @@ __global__ void __launch_bounds__(64) k_topo_tiles(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_TILES);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t local;
-    const SimParams& P = workSim(bt, FP_WORK_TILES, item, local);
+    const SimParams& P = *workSim(bt, FP_WORK_TILES, item, local).vview;
     if (!P.topoAll) continue;
     int t = P.liveTiles[local];
     int4 rec = __ldg(&P.tileRec[t]);
@@ -985,10 +985,15 @@ static void stagedLaunch(const FpBatch& bt, const MgSel& S, int sms, cudaStream_
 }
 
 // The staged level's cells per brick side for an operation whose output level is `level`,
-// in bricks of B cells (1: the first tile level).
+// in bricks of B velocity cells a side (1: the first tile level).
+static int log2i(int v) {
+  int s = 0;
+  while ((1 << s) < v) s++;
+  return s;
+}
 template <int OP>
 static int stagedSide(int level, int B) {
-  int bl = B == 8 ? 3 : (B == 16 ? 4 : 5);
+  int bl = log2i(B);
   int stage = OP == PROLONG ? level + 1 : (OP == RESTRICT ? level - 1 : level);
   return stage < bl ? 1 << (bl - stage) : 1;
 }
@@ -997,7 +1002,7 @@ template <int OP>
 static void levelLaunch(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st) {
   if (tiles) {
     // The tile levels hold 4^3, 2^3 and one cell a tile.
-    const int below = S.level - (B == 8 ? 3 : (B == 16 ? 4 : 5));
+    const int below = S.level - log2i(B);
     if (below == 0)
       k_level_tiles<OP, 64><<<sms * 16, 64, 0, st>>>(bt, S);
     else if (below == 1)

@@ -146,6 +146,11 @@ int Engine::renderInputs() {
   P.counters = (FpCounters*)counters_.ptr;
   P.fld = (float*)fld_[fldIdx_[0]].ptr;
   P.scalarHalf = precision_ == FP_PRECISION_MIXED ? 1 : 0;
+  P.velDiv = vd_;  // the field lattice's view only: the render reads no velocity
+  P.solidSpan = 1;
+  P.fshift = shift_;
+  P.fineH = h_;
+  P.fview = P.vview = (const SimParams*)renderParams_.ptr;
   if ((rc = check(cudaMemcpyAsync(renderParams_.ptr, &P, sizeof(P), cudaMemcpyHostToDevice, stream()), "render")))
     return rc;
   return FP_OK;

@@ -222,6 +222,104 @@ FP_DEV void cellOf(const SimParams& P, const Home& H, int c, int& x, int& y, int
 // Predictors: advectVelocityWithBounds (fluid-velocity-transport.wgsl:28-100) and
 // advectScalars (fluid-scalar-transport.wgsl:38-142), fused: both read only the velocity and
 // the scalars at the start of the step.
+// advectVelocityWithBounds (fluid-velocity-transport.wgsl:28-100) at velocity cell (x,y,z),
+// offset c of its brick's slot, on the velocity lattice P.
+FP_DEV void predictVelocity(const SimParams& P, const Home& H, const Stage& G, const Field& V, size_t slot, int c, int x,
+                            int y, int z) {
+  const size_t N = P.N;
+  // Velocity bounds over the forward 2x2x2 block (staged: HALO >= 1).
+  const float* home = V.sm ? V.sm + stagedAt(G, x, y, z) : nullptr;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    float t[8];
+    blockCells(P, H, G, V, k, home, x, y, z, t);
+    float lo = 1e5f, hi = -1e5f;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      lo = fminf(lo, t[j]);
+      hi = fmaxf(hi, t[j]);
+    }
+    P.vmin[(slot * 3 + k) * N + c] = lo;
+    P.vmax[(slot * 3 + k) * N + c] = hi;
+  }
+  const float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+  // solidAt at a cell centre is solidCell of that cell: centre / h + 0.25 floors to it.
+  if (solidCell(P, H, x, y, z)) {
+    for (int k = 0; k < 3; k++) P.velP[(slot * 3 + k) * N + c] = 0.f;
+  } else {
+    float3 orig = make_float3(nearCell(P, H, G, V, 0, x, y, z), nearCell(P, H, G, V, 1, x, y, z),
+                              nearCell(P, H, G, V, 2, x, y, z));
+#pragma unroll
+    for (int comp = 0; comp < 3; comp++) {
+      float face[3] = {px, py, pz};
+      face[comp] += 0.5f * P.h;
+      float3 fv = velocityOnFace(P, H, G, V, x, y, z, comp, orig);
+      float3 vm = velocityAt(P, H, G, V, face[0] - 0.5f * P.dt * fv.x, face[1] - 0.5f * P.dt * fv.y,
+                             face[2] - 0.5f * P.dt * fv.z);
+      float dep[3] = {face[0] - P.dt * vm.x, face[1] - P.dt * vm.y, face[2] - P.dt * vm.z};
+      float sh[3] = {dep[0], dep[1], dep[2]};
+      sh[comp] -= 0.5f * P.h;
+      // Divided, not multiplied by 1/h: still air lands exactly on a cell boundary here and
+      // the donor cell is an integer decision the oracle repeats.
+      int bx = (int)floorf(sh[0] / P.h - 0.5f), by = (int)floorf(sh[1] / P.h - 0.5f),
+          bz = (int)floorf(sh[2] / P.h - 0.5f);
+      P.donors[(slot * 3 + comp) * N + c] = (uint16_t)packDonor(bx - x, by - y, bz - z);
+      P.velP[(slot * 3 + comp) * N + c] = velComp(P, H, G, V, dep[0], dep[1], dep[2], comp);
+    }
+  }
+}
+// advectScalars (fluid-scalar-transport.wgsl:38-142) at field cell (x,y,z), offset c of its
+// brick's slot: P the field lattice, VP the velocity lattice the trace samples.
+FP_DEV void predictScalars(const SimParams& P, const SimParams& VP, const Home& H, const Stage& G, const Field& V,
+                           const Field& F, size_t slot, int c, int x, int y, int z) {
+  const size_t N = P.N;
+  // Scalars: a cell-centred RK2 back trace, the predictor and its donors' range.
+  const float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+  float3 cv = VP.velDiv == 1 ? centreVelocity(VP, H, G, V, x, y, z) : velocityAt(VP, H, G, V, px, py, pz);
+  float3 vm = velocityAt(VP, H, G, V, px - 0.5f * P.dt * cv.x, py - 0.5f * P.dt * cv.y, pz - 0.5f * P.dt * cv.z);
+  float dx_ = px - P.dt * vm.x, dy_ = py - P.dt * vm.y, dz_ = pz - P.dt * vm.z;
+  // The departure's trilinear block in cell units: corner `base`, fractions `fr`.
+  const float dc[3] = {(float)x + (dx_ - px) * P.invH, (float)y + (dy_ - py) * P.invH,
+                       (float)z + (dz_ - pz) * P.invH};
+  int base[3];
+  float fr[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    float g = floorf(dc[a]);
+    base[a] = (int)g;
+    fr[a] = dc[a] - g;
+  }
+  const float* blk = stagedBlock(G, F, base[0], base[1], base[2]);
+  float out[4];
+  float* sb = P.sb + slot * 8 * N;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    float t[8];
+    blockCells(P, H, G, F, k, blk, base[0], base[1], base[2], t);
+    out[k] = blend8(t, fr[0], fr[1], fr[2]);
+    if (P.maccormack) {
+      // The donors' range; FP16-finite for smoke, heat and fuel, [0,1]-anchored for lifetime.
+      float lo = k == 2 ? 1.f : 65504.f, hi = k == 2 ? 0.f : -65504.f;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        lo = fminf(lo, t[j]);
+        hi = fmaxf(hi, t[j]);
+      }
+      const int row = k < 2 ? k : 5 - k;  // rows: smoke, heat, fuel, lifetime
+      sb[row * N + c] = lo;
+      sb[(4 + row) * N + c] = hi;
+    }
+  }
+  if (!P.maccormack) out[2] = clamp01(out[2]);
+  else if (P.lifetimeZero) out[2] = 0.f;
+  // With coarse smoke the fine smoke channel carries no density
+  // (fluid-scalar-transport.wgsl:127, :137).
+  if (P.smokeDiv > 1) out[0] = 0.f;
+  // The predictor lives within the step: FP32 in every precision, so the limiter compares
+  // the corrected value with unrounded predictions.
+  for (int k = 0; k < 4; k++) P.fldP[(slot * 4 + k) * N + c] = out[k];
+}
+
 template <bool STAGED>
 FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
@@ -238,94 +336,26 @@ FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
     stageWait();
   }
   size_t slot = (size_t)nslot[13];
-  const size_t N = P.N;
-  for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
-    int x, y, z;
-    cellOf(P, H, c, x, y, z);
-    // Velocity bounds over the forward 2x2x2 block (staged: HALO >= 1).
-    const float* home = V.sm ? V.sm + stagedAt(G, x, y, z) : nullptr;
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      float t[8];
-      blockCells(P, H, G, V, k, home, x, y, z, t);
-      float lo = 1e5f, hi = -1e5f;
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        lo = fminf(lo, t[j]);
-        hi = fmaxf(hi, t[j]);
-      }
-      P.vmin[(slot * 3 + k) * N + c] = lo;
-      P.vmax[(slot * 3 + k) * N + c] = hi;
+  if (STAGED || P.velDiv == 1) {
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int x, y, z;
+      cellOf(P, H, c, x, y, z);
+      predictVelocity(P, H, G, V, slot, c, x, y, z);
+      predictScalars(P, P, H, G, V, F, slot, c, x, y, z);
     }
-    float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-    // solidAt at a cell centre is solidCell of that cell: centre / h + 0.25 floors to it.
-    if (solidCell(P, H, x, y, z)) {
-      for (int k = 0; k < 3; k++) P.velP[(slot * 3 + k) * N + c] = 0.f;
-    } else {
-      float3 orig = make_float3(nearCell(P, H, G, V, 0, x, y, z), nearCell(P, H, G, V, 1, x, y, z),
-                                nearCell(P, H, G, V, 2, x, y, z));
-#pragma unroll
-      for (int comp = 0; comp < 3; comp++) {
-        float face[3] = {px, py, pz};
-        face[comp] += 0.5f * P.h;
-        float3 fv = velocityOnFace(P, H, G, V, x, y, z, comp, orig);
-        float3 vm = velocityAt(P, H, G, V, face[0] - 0.5f * P.dt * fv.x, face[1] - 0.5f * P.dt * fv.y,
-                               face[2] - 0.5f * P.dt * fv.z);
-        float dep[3] = {face[0] - P.dt * vm.x, face[1] - P.dt * vm.y, face[2] - P.dt * vm.z};
-        float sh[3] = {dep[0], dep[1], dep[2]};
-        sh[comp] -= 0.5f * P.h;
-        // Divided, not multiplied by 1/h: still air lands exactly on a cell boundary here and
-        // the donor cell is an integer decision the oracle repeats.
-        int bx = (int)floorf(sh[0] / P.h - 0.5f), by = (int)floorf(sh[1] / P.h - 0.5f),
-            bz = (int)floorf(sh[2] / P.h - 0.5f);
-        P.donors[(slot * 3 + comp) * N + c] = (uint16_t)packDonor(bx - x, by - y, bz - z);
-        P.velP[(slot * 3 + comp) * N + c] = velComp(P, H, G, V, dep[0], dep[1], dep[2], comp);
-      }
+  } else {
+    // The velocity lattice's cells, then the field lattice's.
+    const SimParams& VP = *P.vview;
+    for (int c = threadIdx.x; c < VP.N; c += blockDim.x) {
+      int x, y, z;
+      cellOf(VP, H, c, x, y, z);
+      predictVelocity(VP, H, G, V, slot, c, x, y, z);
     }
-    // Scalars: a cell-centred RK2 back trace, the predictor and its donors' range.
-    float3 cv = centreVelocity(P, H, G, V, x, y, z);
-    float3 vm = velocityAt(P, H, G, V, px - 0.5f * P.dt * cv.x, py - 0.5f * P.dt * cv.y, pz - 0.5f * P.dt * cv.z);
-    float dx_ = px - P.dt * vm.x, dy_ = py - P.dt * vm.y, dz_ = pz - P.dt * vm.z;
-    // The departure's trilinear block in cell units: corner `base`, fractions `fr`.
-    const float dc[3] = {(float)x + (dx_ - px) * P.invH, (float)y + (dy_ - py) * P.invH,
-                         (float)z + (dz_ - pz) * P.invH};
-    int base[3];
-    float fr[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      float g = floorf(dc[a]);
-      base[a] = (int)g;
-      fr[a] = dc[a] - g;
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int x, y, z;
+      cellOf(P, H, c, x, y, z);
+      predictScalars(P, VP, H, G, V, F, slot, c, x, y, z);
     }
-    const float* blk = stagedBlock(G, F, base[0], base[1], base[2]);
-    float out[4];
-    float* sb = P.sb + slot * 8 * N;
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      float t[8];
-      blockCells(P, H, G, F, k, blk, base[0], base[1], base[2], t);
-      out[k] = blend8(t, fr[0], fr[1], fr[2]);
-      if (P.maccormack) {
-        // The donors' range; FP16-finite for smoke, heat and fuel, [0,1]-anchored for lifetime.
-        float lo = k == 2 ? 1.f : 65504.f, hi = k == 2 ? 0.f : -65504.f;
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-          lo = fminf(lo, t[j]);
-          hi = fmaxf(hi, t[j]);
-        }
-        const int row = k < 2 ? k : 5 - k;  // rows: smoke, heat, fuel, lifetime
-        sb[row * N + c] = lo;
-        sb[(4 + row) * N + c] = hi;
-      }
-    }
-    if (!P.maccormack) out[2] = clamp01(out[2]);
-    else if (P.lifetimeZero) out[2] = 0.f;
-    // With coarse smoke the fine smoke channel carries no density
-    // (fluid-scalar-transport.wgsl:127, :137).
-    if (P.smokeDiv > 1) out[0] = 0.f;
-    // The predictor lives within the step: FP32 in every precision, so the limiter compares
-    // the corrected value with unrounded predictions.
-    for (int k = 0; k < 4; k++) P.fldP[(slot * 4 + k) * N + c] = out[k];
   }
   __syncthreads();
 }
@@ -416,7 +446,7 @@ __global__ void __launch_bounds__(THREADS, FP_TRANSPORT_CTAS) k_correct(FpBatch 
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_correct<STAGED>(&P, i);
+    brick_correct<STAGED>(P.vview, i);  // the velocity lattice
   }
 }
 
@@ -436,6 +466,7 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
   }
   Home H = enterBrick(P, id, nslot);
   Stage G = stageOf(P, H, STAGED);
+  const SimParams& VP = STAGED ? P : *P.vview;  // the velocity lattice the traces sample
   Field V{P.vel, 3, STAGED ? smem : nullptr};
   Field Fp{P.fldP, 4, STAGED ? smem + 3 * G.S3 : nullptr, false};  // the predictor: FP32
   const bool half = P.scalarHalf != 0;                             // the state pools
@@ -475,9 +506,9 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
         } else {
           float a0 = nearCell(P, H, G, Fp, 0, x, y, z), a1 = nearCell(P, H, G, Fp, 1, x, y, z),
                 a2 = nearCell(P, H, G, Fp, 2, x, y, z), a3 = nearCell(P, H, G, Fp, 3, x, y, z);
-          cv = centreVelocity(P, H, G, V, x, y, z);
+          cv = VP.velDiv == 1 ? centreVelocity(VP, H, G, V, x, y, z) : velocityAt(VP, H, G, V, px, py, pz);
           cvSampled = true;
-          float3 vm = velocityAt(P, H, G, V, px + 0.5f * P.dt * cv.x, py + 0.5f * P.dt * cv.y, pz + 0.5f * P.dt * cv.z);
+          float3 vm = velocityAt(VP, H, G, V, px + 0.5f * P.dt * cv.x, py + 0.5f * P.dt * cv.y, pz + 0.5f * P.dt * cv.z);
           float fx = px + P.dt * vm.x, fy = py + P.dt * vm.y, fz = pz + P.dt * vm.z;
           const size_t o = slot * 4 * N + c;
           float o0 = ldHalf(P.fld, o, half), o1 = ldHalf(P.fld, o + N, half), o2 = ldHalf(P.fld, o + 2 * N, half),
@@ -574,14 +605,15 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
     if (expansion != 0.f) expands = true;
     // holdsContent and contentSupport (fluid-content.wgsl:22-39).
     if (fmaxf(fmaxf(P.smokeDiv > 1 ? 0.f : value[0], value[2]), value[3]) > P.cutoff) {
-      if (!cvSampled) cv = centreVelocity(P, H, G, V, x, y, z);
+      if (!cvSampled) cv = VP.velDiv == 1 ? centreVelocity(VP, H, G, V, x, y, z) : velocityAt(VP, H, G, V, px, py, pz);
       int idc[3] = {x, y, z};
       float vv[3] = {cv.x, cv.y, cv.z};
       bool low[3], high[3];
       for (int a = 0; a < 3; a++) {
         float side = (float)P.B;
         float loc = (float)(idc[a] & (P.B - 1)) + 0.5f;
-        float pad = fminf(side, 2.f + fabsf(vv[a]) * P.dt / P.h);
+        // two velocity cells of stencil (2 d field cells), and a step of motion
+        float pad = fminf(side, fmaxf(2.f, 2.f * (float)P.velDiv) + fabsf(vv[a]) * P.dt / P.h);
         low[a] = loc < pad;
         high[a] = loc + pad >= side;
       }
@@ -670,7 +702,7 @@ __global__ void __launch_bounds__(THREADS) k_curl(FpBatch bt) {
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_curl<STAGED>(&P, i);
+    brick_curl<STAGED>(P.vview, i);  // the velocity lattice
   }
 }
 
@@ -760,14 +792,34 @@ FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage& Gc, cons
   if (brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift) < 0) return make_float3(0.f, 0.f, 0.f);
   float wx = ((float)x + 0.5f) * P.h, wy = ((float)y + 0.5f) * P.h, wz = ((float)z + 0.5f) * P.h;
   if (solidCell(P, H, x, y, z)) return make_float3(0.f, 0.f, 0.f);  // solidAt at the centre
-  // The evolved scalars of this step (the reference swaps field and corrected first).
-  float heat = nearCell(P, H, Gs, Fs, 1, x, y, z), density = nearCell(P, H, Gs, Fs, 0, x, y, z);
-  // smokeVelocityAverage (smoke.wgsl:4-21) at one velocity cell per smoke spacing or less: the
-  // evolved coarse density sampled at the cell centre ((x + .5) / d in smoke cells, exact).
+  // The evolved scalars of this step (the reference swaps field and corrected first); with a
+  // velocity divisor d > 1 their mean over the velocity cell (velocityCellAverage).
+  float heat, density;
+  if (P.velDiv == 1) {
+    heat = nearCell(P, H, Gs, Fs, 1, x, y, z);
+    density = nearCell(P, H, Gs, Fs, 0, x, y, z);
+  } else {
+    heat = fieldAverage(*P.fview, H, Fs.pool, 4, 1, x, y, z, Fs.half);
+    density = fieldAverage(*P.fview, H, Fs.pool, 4, 0, x, y, z, Fs.half);
+  }
+  // smokeVelocityAverage (smoke.wgsl:4-21): at one velocity cell per smoke spacing or less the
+  // evolved coarse density sampled at the cell centre ((x + .5) d_v / d_s in smoke cells, exact),
+  // else the mean of its 2x2x2 blocks of smoke cells.
   if (P.smokeDiv > 1) {
-    const float inv = 1.f / (float)P.smokeDiv;
-    density = smokeSample(P, H, P.smkN, ((float)x + 0.5f) * inv, ((float)y + 0.5f) * inv, ((float)z + 0.5f) * inv,
-                          P.scalarHalf != 0);
+    const bool sh = P.scalarHalf != 0;
+    const int ratio = P.velDiv > P.smokeDiv ? P.velDiv / P.smokeDiv : 1;
+    if (ratio == 1) {
+      const float f = (float)P.velDiv / (float)P.smokeDiv;
+      density = smokeSample(P, H, P.smkN, ((float)x + 0.5f) * f, ((float)y + 0.5f) * f, ((float)z + 0.5f) * f, sh);
+    } else {
+      density = 0.f;
+      for (int k = 0; k < ratio; k += 2)
+        for (int j = 0; j < ratio; j += 2)
+          for (int q = 0; q < ratio; q += 2)
+            density += smokeSample(P, H, P.smkN, (float)(x * ratio + q + 1), (float)(y * ratio + j + 1),
+                                   (float)(z * ratio + k + 1), sh);
+      density /= (float)(ratio * ratio * ratio / 8);
+    }
   }
   float3 conf = make_float3(0.f, 0.f, 0.f);
   if (P.vorticity != 0.f) {
@@ -805,8 +857,8 @@ FP_DEV float sourceVelocity(const SimParams& P, const Home& H, int tile, float v
     }
     result = mixf(result, e.vel[comp] + radial, 1.f - expf(-e.response * w * P.dt));
   }
-  // Mesh emission's velocity coupling (fluid-forces.wgsl:143-147).
-  const FpMeshSource* ms = meshSourceAt(P, H, cx, cy, cz);
+  // Mesh emission's velocity coupling (fluid-forces.wgsl:143-147), on the field lattice.
+  const FpMeshSource* ms = meshSourceAt(P.velDiv == 1 ? P : *P.fview, H, cx, cy, cz);
   if (ms && ms->motion[3] > 0.f)
     result = mixf(result, ms->motion[comp] / ms->motion[3], 1.f - expf(-ms->motion[3] * P.dt));
   return result;
@@ -876,7 +928,10 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
         float v = P.velC[(slot * 3 + a) * N + c] * decay + P.dt * f[a];
         float face[3] = {px, py, pz};
         face[a] += 0.5f * P.h;
-        out[a] = sourceVelocity(P, H, tile, v, face[0], face[1], face[2], a, x + (a == 0), y + (a == 1), z + (a == 2));
+        // the face's field cell: (x + 1) d on its axis, x d + d/2 on the others (x + 1, x for d = 1)
+      const int d = P.velDiv, o = d >> 1;
+      out[a] = sourceVelocity(P, H, tile, v, face[0], face[1], face[2], a, a == 0 ? (x + 1) * d : x * d + o,
+                              a == 1 ? (y + 1) * d : y * d + o, a == 2 ? (z + 1) * d : z * d + o);
       }
       // enforceFaces (fluid-forces.wgsl:15-31)
       // solidAt at a cell centre is solidCell of that cell: centre / h + 0.25 floors to it.
@@ -898,7 +953,7 @@ __global__ void __launch_bounds__(THREADS, 4) k_forces(FpBatch bt) {
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_forces<STAGED>(&P, i);
+    brick_forces<STAGED>(P.vview, i);  // the velocity lattice
   }
 }
 // Shared memory of the staged force kernel: the (B+1)^3 force tile, the curl over (B+3)^3,
@@ -934,7 +989,10 @@ FP_DEV void brick_divergence(const SimParams* __restrict__ Pp, uint32_t i, int p
     float d = (P.velF[(slot * 3 + 0) * N + c] - cellAt(P, H, P.velF, 3, 0, x - 1, y, z)) / P.h +
               (P.velF[(slot * 3 + 1) * N + c] - cellAt(P, H, P.velF, 3, 1, x, y - 1, z)) / P.h +
               (P.velF[(slot * 3 + 2) * N + c] - cellAt(P, H, P.velF, 3, 2, x, y, z - 1)) / P.h;
-    float rhs = P.h * P.h * (d - P.expn[slot * N + c]);
+    // The expansion rate is on the field lattice: its mean over the velocity cell
+    // (velocityCellAverage, fluid-forces.wgsl:202).
+    const float ex = P.velDiv == 1 ? P.expn[slot * N + c] : fieldAverage(*P.fview, H, P.expn, 1, 0, x, y, z, false);
+    float rhs = P.h * P.h * (d - ex);
     P.div[slot * N + c] = rhs;
     uint8_t t = P.topo[0][slot * N + c];
     float first = 0.f;
@@ -952,7 +1010,7 @@ __global__ void __launch_bounds__(THREADS) k_divergence(FpBatch bt, int pSel) {
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_divergence(&P, i, pSel);
+    brick_divergence(P.vview, i, pSel);  // the velocity lattice
   }
 }
 
@@ -994,7 +1052,7 @@ __global__ void __launch_bounds__(THREADS) k_project(FpBatch bt, int pSel) {
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_project(&P, i, pSel);
+    brick_project(P.vview, i, pSel);  // the velocity lattice
   }
 }
 
@@ -1051,7 +1109,7 @@ __global__ void __launch_bounds__(THREADS) k_post_divergence(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
-    const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
+    const SimParams& P = *workSim(bt, FP_WORK_ACTIVE, item, i).vview;  // the velocity lattice
     Home H = enterBrick(P, P.active[i], nslot);
     const size_t slot = (size_t)nslot[13], N = P.N;
     double d2 = 0.0, v2 = 0.0;
@@ -1110,7 +1168,7 @@ FP_DEV SmokeCell smokeCellOf(const SimParams& P, const Home& H, int c) {
 FP_DEV float3 smokeTrace(const SimParams& P, const Home& H, const float* p, float3 cv, float sign) {
   Stage G{};
   Field V{P.vel, 3, nullptr};
-  float3 vm = velocityAt(P, H, G, V, p[0] + sign * 0.5f * P.dt * cv.x, p[1] + sign * 0.5f * P.dt * cv.y,
+  float3 vm = velocityAt(*P.vview, H, G, V, p[0] + sign * 0.5f * P.dt * cv.x, p[1] + sign * 0.5f * P.dt * cv.y,
                          p[2] + sign * 0.5f * P.dt * cv.z);
   return make_float3(p[0] + sign * P.dt * vm.x, p[1] + sign * P.dt * vm.y, p[2] + sign * P.dt * vm.z);
 }
@@ -1134,7 +1192,7 @@ __global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_advect(FpBatch bt) {
       SmokeCell s = smokeCellOf(P, H, c);
       float density = 0.f;
       if (!solidAt(P, H, s.p[0], s.p[1], s.p[2])) {
-        float3 cv = velocityAt(P, H, G, V, s.p[0], s.p[1], s.p[2]);
+        float3 cv = velocityAt(*P.vview, H, G, V, s.p[0], s.p[1], s.p[2]);
         float3 dep = smokeTrace(P, H, s.p, cv, -1.f);
         density = smokeSample(P, H, P.smk, dep.x * invSp, dep.y * invSp, dep.z * invSp, half);
         if (P.maccormack) {
@@ -1166,7 +1224,7 @@ FP_DEV uint32_t smokeSupport(const SimParams& P, const int* q, float3 v) {
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     float loc = (float)(q[a] & (SB - 1)) + 0.5f;
-    float pad = fminf(side, fmaxf(2.f, 2.f * (P.h / sp)) + fabsf(vv[a]) * P.dt / sp);
+    float pad = fminf(side, fmaxf(2.f, 2.f * ((P.h * (float)P.velDiv) / sp)) + fabsf(vv[a]) * P.dt / sp);
     low[a] = loc < pad;
     high[a] = loc + pad >= side;
   }
@@ -1200,7 +1258,7 @@ __global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_evolve(FpBatch bt) {
       SmokeCell s = smokeCellOf(P, H, c);
       float density = 0.f;
       if (!solidAt(P, H, s.p[0], s.p[1], s.p[2])) {
-        float3 cv = velocityAt(P, H, G, V, s.p[0], s.p[1], s.p[2]);
+        float3 cv = velocityAt(*P.vview, H, G, V, s.p[0], s.p[1], s.p[2]);
         const float predictor = P.smkP[slot * SN + c];
         float bounded = predictor;
         if (P.maccormack) {
@@ -1268,32 +1326,32 @@ void fp_step_configure(int B) {
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_forces<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-void fp_launch_predict(const FpBatch& bt, int B, int sms, cudaStream_t st) {
-  if (B == 8)
+void fp_launch_predict(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
+  if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
     k_predict<true><<<sms * 4, THREADS, stagedBytes(7), st>>>(bt);
   else
     k_predict<false><<<sms * 4, THREADS, 0, st>>>(bt);
 }
-void fp_launch_correct(const FpBatch& bt, int B, int sms, cudaStream_t st) {
-  if (B == 8)
+void fp_launch_correct(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
+  if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
     k_correct<true><<<sms * 4, THREADS, stagedBytes(6), st>>>(bt);
   else
     k_correct<false><<<sms * 4, THREADS, 0, st>>>(bt);
 }
-void fp_launch_evolve(const FpBatch& bt, int B, int sms, cudaStream_t st) {
-  if (B == 8)
+void fp_launch_evolve(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
+  if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
     k_evolve<true><<<sms * 4, THREADS, stagedBytes(7), st>>>(bt);
   else
     k_evolve<false><<<sms * 4, THREADS, 0, st>>>(bt);
 }
-void fp_launch_curl(const FpBatch& bt, int B, int sms, cudaStream_t st) {
-  if (B == 8)
+void fp_launch_curl(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
+  if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
     k_curl<true><<<sms * 4, THREADS, 3 * 10 * 10 * 10 * sizeof(float), st>>>(bt);
   else
     k_curl<false><<<sms * 4, THREADS, 0, st>>>(bt);
 }
-void fp_launch_forces(const FpBatch& bt, int B, int sms, cudaStream_t st) {
-  if (B == 8) {
+void fp_launch_forces(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
+  if (B == 8 && vd == 1) {  // staged: 8^3 bricks, one lattice
     k_forces<true><<<sms * 4, THREADS, FORCE_STAGED_BYTES, st>>>(bt);
     return;
   }

@@ -173,6 +173,18 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
       error_ = who(i) + "brick size differs from the batch's";
       return done(FP_EINVAL);
     }
+  // The velocity lattice's brick levels are the launch's: one velocity divisor a stepper.
+  if (vd_ == 0) {
+    vd_ = sims[0]->velocityDivisor();
+    brickLevels_ = 0;
+    while ((1 << brickLevels_) < B_ / vd_) brickLevels_++;
+    bottom_ = brickLevels_ + 2;
+  }
+  for (int i = 0; i < count; i++)
+    if (sims[i]->velocityDivisor() != vd_) {
+      error_ = who(i) + "velocity divisor differs from the batch's";
+      return done(FP_EINVAL);
+    }
   for (int i = 0; i < count; i++)
     if ((rc = sims[i]->validate(*frames[i], dts[i]))) {
       error_ = who(i) + sims[i]->error();
@@ -346,7 +358,7 @@ void Stepper::vcycle(int level, int cur[], uint64_t& launches) {
   auto relax = [&](int n) {
     for (int i = 0; i < n; i++) {
       MgSel S{level, sel(level, 2), sel(level, cur[level]), -1, sel(level, 1 - cur[level]), -1, cycle_};
-      fp_launch_relax(batch(), S, tiles, B_, sms_, stream_);
+      fp_launch_relax(batch(), S, tiles, B_ / vd_, sms_, stream_);
       launches++;
       cur[level] = 1 - cur[level];
     }
@@ -354,12 +366,12 @@ void Stepper::vcycle(int level, int cur[], uint64_t& launches) {
   if (level > 0) relax(2);
   int coarse = level + 1;
   MgSel R{coarse, sel(level, 2), sel(level, cur[level]), -1, sel(coarse, 2), sel(coarse, 1), cycle_};
-  fp_launch_restrict(batch(), R, coarse >= brickLevels_, B_, sms_, stream_);
+  fp_launch_restrict(batch(), R, coarse >= brickLevels_, B_ / vd_, sms_, stream_);
   launches++;
   cur[coarse] = 1;
   vcycle(coarse, cur, launches);
   MgSel Pr{level, -1, sel(level, cur[level]), sel(coarse, cur[coarse]), sel(level, 1 - cur[level]), -1, cycle_};
-  fp_launch_prolong(batch(), Pr, tiles, B_, sms_, stream_);
+  fp_launch_prolong(batch(), Pr, tiles, B_ / vd_, sms_, stream_);
   launches++;
   cur[level] = 1 - cur[level];
   relax(3);
@@ -382,13 +394,13 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   launches += topoAll ? 4 : 2;
   phaseEnd(PH_TOPO, topoAll ? 4 : 2);
   phaseBegin(PH_PREDICT);
-  fp_launch_predict(bt, B_, sms_, stream_);
+  fp_launch_predict(bt, B_, vd_, sms_, stream_);
   phaseEnd(PH_PREDICT, 1);
   phaseBegin(PH_CORRECT);
-  fp_launch_correct(bt, B_, sms_, stream_);
+  fp_launch_correct(bt, B_, vd_, sms_, stream_);
   phaseEnd(PH_CORRECT, 1);
   phaseBegin(PH_EVOLVE);
-  fp_launch_evolve(bt, B_, sms_, stream_);
+  fp_launch_evolve(bt, B_, vd_, sms_, stream_);
   // Coarse smoke evolves after the fine fields, whose source production it averages, and
   // records content before the measurement.
   if (anySmoke_) fp_launch_smoke(bt, sms_, stream_);
@@ -408,12 +420,12 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
 
   if (curl) {
     phaseBegin(PH_CURL);
-    fp_launch_curl(bt, B_, sms_, stream_);
+    fp_launch_curl(bt, B_, vd_, sms_, stream_);
     launches++;
     phaseEnd(PH_CURL, 1);
   }
   phaseBegin(PH_FORCES);
-  fp_launch_forces(bt, B_, sms_, stream_);
+  fp_launch_forces(bt, B_, vd_, sms_, stream_);
   launches++;
   phaseEnd(PH_FORCES, 1);
   // Cold start every step: the divergence writes the first iterate into p0[1].

@@ -115,6 +115,18 @@ struct SimParams {
   int B, shift, N, W;  // cells per brick side, log2, cells per brick, solid words per slot
   int brickLevels, bottom;
   float h, invH, dt;
+  // The two lattices of a simulation (velocityDivisor d, FluidSimulation.ts:365-373): the field
+  // lattice (scalars, expansion, solids, mesh tables) and the velocity lattice (velocity, curl,
+  // divergence, pressure and its levels) of B/d cells a brick side at spacing h d. A simulation
+  // has a SimParams per lattice, alike but for the lattice fields above (`brickLevels` and
+  // `bottom` are the velocity lattice's in both); `fview` and `vview` point at the two (at
+  // itself when d = 1). Velocity kernels run on `vview`, field kernels on `fview`.
+  const SimParams* fview;
+  const SimParams* vview;
+  int velDiv;     // d
+  int solidSpan;  // field cells a side per cell of this lattice: d in the velocity view, else 1
+  int fshift;     // the field lattice's log2 cells a brick side
+  float fineH;    // the field lattice's spacing
   // dynamics (Params, fluid-common.wgsl:21-32)
   float buoyancy, cooling, smokeWeight, damping, dissipation, vorticity;
   float cutoff, time, seedF;

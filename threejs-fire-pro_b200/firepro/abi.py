@@ -41,6 +41,8 @@ FP_FIELD_DIVERGENCE = 4
 FP_FIELD_CURL = 5
 FP_FIELD_SMOKE = 6  # the coarse smoke grid, (B / smoke_divisor)^3 cells a slot
 FIELD_CHANNELS = {0: 3, 1: 4, 2: 1, 3: 1, 4: 1, 5: 4, 6: 1}
+# fields on the velocity lattice: (brick_size / velocity_divisor)^3 cells a slot
+VELOCITY_FIELDS = (FP_FIELD_VELOCITY, FP_FIELD_PRESSURE, FP_FIELD_DIVERGENCE, FP_FIELD_CURL)
 
 FP_TABLE_ENTRIES = 0
 FP_TABLE_PAGES = 1

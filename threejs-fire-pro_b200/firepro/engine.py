@@ -31,6 +31,8 @@ class FluidSimulation:
             raise FireProError(rc, self.lib.fp_last_error(None).decode())
         self.h = h
         self.cells = grid.brick_size ** 3
+        # cells a slot of the velocity lattice (velocity, pressure, divergence, curl)
+        self.velocity_cells = self.cells // max(1, grid.velocity_divisor) ** 3
         # cells a slot of the coarse smoke grid (FP_FIELD_SMOKE), smoke_divisor > 1 only
         self.smoke_cells = self.cells // grid.smoke_divisor ** 3 if grid.smoke_divisor > 1 else 0
 
@@ -101,7 +103,8 @@ class FluidSimulation:
     def field(self, fid: int) -> np.ndarray:
         s = self.stats()
         ch = abi.FIELD_CHANNELS[fid]
-        cells = self.smoke_cells if fid == abi.FP_FIELD_SMOKE else self.cells
+        cells = self.smoke_cells if fid == abi.FP_FIELD_SMOKE else (
+            self.velocity_cells if fid in abi.VELOCITY_FIELDS else self.cells)
         out = np.empty((s.pool_slots, ch, cells), np.float32)
         self._check(self.lib.fp_sim_read_field(self.h, fid, out.ctypes.data_as(C.POINTER(C.c_float)), out.nbytes))
         return out

@@ -164,12 +164,13 @@ class Scene:
     name = "scene"
     voxel_size = 0.025
     brick_size = 8
+    velocity_divisor = 1
     steps = 120
 
     def grid(self, precision=abi.FP_PRECISION_FP32, budget=8e6, maccormack=True) -> abi.fp_grid:
         g = abi.fp_grid()
         g.voxel_size = self.voxel_size
-        g.velocity_divisor = 1
+        g.velocity_divisor = self.velocity_divisor
         g.brick_size = self.brick_size
         g.smoke_divisor = 1
         g.scalar_maccormack = int(maccormack)
