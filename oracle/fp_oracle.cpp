@@ -984,6 +984,7 @@ struct Sim {
     int lightShift;
     std::unordered_map<uint64_t, int> index;  // boxed slotted brick -> row
     std::vector<R> field;                     // [row][4][N]
+    std::vector<R> smoke;                     // coarse smoke: [row][SN], smoothed
     std::vector<uint8_t> occupancy;           // [row][blocks]
     std::vector<R> light;                     // [row][4][L^3]
   };
@@ -1028,13 +1029,82 @@ struct Sim {
     for (int k = 0; k < 8; k++) d += smokeSample(R(x + (k & 1)), R(y + ((k >> 1) & 1)), R(z + (k >> 2)));
     return std::max(R(0), d * R(.125));
   }
+  // The coarse smoke grid (lighting.wgsl smoothCoarseSmoke :104-129, cachedSmokeCell :133-156,
+  // volume-common.wgsl renderSmokeAt :74-78), SB cells a brick side.
+  R rawCoarse(int x, int y, int z) {
+    int s = boxSlot(x >> sshift, y >> sshift, z >> sshift);
+    if (s < 0) return R(0);
+    int m = SB - 1;
+    return smk[(size_t)s * SN + ((z & m) * SB + (y & m)) * SB + (x & m)];
+  }
+  R coarseRenderSample(R qx, R qy, R qz) {
+    R q[3] = {qx, qy, qz};
+    clampBox(q, SB);
+    R g[3], fr[3];
+    int b[3];
+    for (int a = 0; a < 3; a++) {
+      g[a] = q[a] - R(.5);
+      b[a] = (int)std::floor(g[a]);
+      fr[a] = g[a] - R(b[a]);
+    }
+    R v = 0;
+    for (int k = 0; k < 8; k++) {
+      int d[3] = {k & 1, (k >> 1) & 1, k >> 2};
+      R w = (d[0] ? fr[0] : 1 - fr[0]) * (d[1] ? fr[1] : 1 - fr[1]) * (d[2] ? fr[2] : 1 - fr[2]);
+      v += rawCoarse(b[0] + d[0], b[1] + d[1], b[2] + d[2]) * w;
+    }
+    return v;
+  }
+  R smoothedCoarse(int x, int y, int z) {
+    R d = 0;
+    for (int k = 0; k < 8; k++) d += coarseRenderSample(R(x + (k & 1)), R(y + ((k >> 1) & 1)), R(z + (k >> 2)));
+    return std::max(R(0), d * R(.125));
+  }
+  R renderSmokeCell(Render& G, int x, int y, int z, bool apron) {
+    auto it = G.index.find(brickKey(x >> sshift, y >> sshift, z >> sshift));
+    int m = SB - 1;
+    if (it != G.index.end()) return G.smoke[(size_t)it->second * SN + ((z & m) * SB + (y & m)) * SB + (x & m)];
+    return apron ? smoothedCoarse(x, y, z) : R(0);
+  }
+  R renderSmokeAt(Render& G, R qx, R qy, R qz) {
+    R q[3] = {qx, qy, qz};
+    clampBox(q, SB);
+    R g[3], fr[3];
+    int b[3];
+    for (int a = 0; a < 3; a++) {
+      g[a] = q[a] - R(.5);
+      b[a] = (int)std::floor(g[a]);
+      fr[a] = g[a] - R(b[a]);
+    }
+    bool based = G.index.count(brickKey(b[0] >> sshift, b[1] >> sshift, b[2] >> sshift)) > 0;
+    R v = 0;
+    for (int k = 0; k < 8; k++) {
+      int d[3] = {k & 1, (k >> 1) & 1, k >> 2};
+      R w = (d[0] ? fr[0] : 1 - fr[0]) * (d[1] ? fr[1] : 1 - fr[1]) * (d[2] ? fr[2] : 1 - fr[2]);
+      v += renderSmokeCell(G, b[0] + d[0], b[1] + d[1], b[2] + d[2], based) * w;
+    }
+    return v;
+  }
+  R cachedSmokeCell(Render& G, int x, int y, int z) {
+    int m = SB - 1, b[3] = {x >> sshift, y >> sshift, z >> sshift}, l[3] = {x & m, y & m, z & m};
+    auto it = G.index.find(brickKey(b[0], b[1], b[2]));
+    if (it != G.index.end()) return G.smoke[(size_t)it->second * SN + (l[2] * SB + l[1]) * SB + l[0]];
+    for (int k = 1; k < 8; k++) {
+      if (((k & 1) && l[0] != 0) || ((k & 2) && l[1] != 0) || ((k & 4) && l[2] != 0)) continue;
+      if (G.index.count(brickKey(b[0] - (k & 1), b[1] - ((k >> 1) & 1), b[2] - ((k >> 2) & 1))))
+        return smoothedCoarse(x, y, z);
+    }
+    return R(0);
+  }
   std::array<R, 4> renderCell(Render& G, int x, int y, int z, bool apron) {
     auto it = G.index.find(brickKey(x >> shift, y >> shift, z >> shift));
     if (it != G.index.end()) {
       size_t o = (size_t)it->second * 4 * N + local(x, y, z);
       return {G.field[o], G.field[o + N], G.field[o + 2 * N], G.field[o + 3 * N]};
     }
-    if (!apron) return {0, 0, 0, 0};
+    // With coarse smoke the render reads the simulation's fields, whose apron holds zero where
+    // no neighbour slot is.
+    if (!apron || smokeDiv > 1) return {0, 0, 0, 0};
     return {smoothedSmoke(x, y, z), 0, 0, 0};
   }
   std::array<R, 4> renderSample(Render& G, R qx, R qy, R qz) {
@@ -1120,7 +1190,9 @@ struct Sim {
     R size = R(B) * h, p[3] = {px, py, pz};
     for (int a = 0; a < 3; a++)
       if (p[a] < R(renderLo[a]) * size || p[a] > R(renderHi[a] + 1) * size) return {0, 0, 0, 0};
-    return renderSample(G, px / h, py / h, pz / h);
+    auto f = renderSample(G, px / h, py / h, pz / h);
+    if (smokeDiv > 1) f[0] = renderSmokeAt(G, px / h / R(smokeDiv), py / h / R(smokeDiv), pz / h / R(smokeDiv));
+    return f;
   }
   std::array<R, 4> incidentLight(Render& G, R px, R py, R pz) {
     const fp_render_settings& S = *G.rs;
@@ -1267,6 +1339,7 @@ struct Sim {
     }
     size_t nb = bricks.size();
     G.field.assign(nb * 4 * N, 0);
+    if (smokeDiv > 1) G.smoke.assign(nb * SN, 0);
     G.occupancy.assign(nb * blocks, 0);
     G.light.assign(nb * 4 * L3, 0);
 #pragma omp parallel for schedule(dynamic)
@@ -1276,9 +1349,14 @@ struct Sim {
       for (int k = 0; k < N; k++) {
         int x = b[0] * B + (k & (B - 1)), y = b[1] * B + ((k >> shift) & (B - 1)), z = b[2] * B + (k >> (2 * shift));
         size_t o = (size_t)r * 4 * N + k;
-        G.field[o] = smoothedSmoke(x, y, z);
+        G.field[o] = smokeDiv > 1 ? fld[(size_t)s * 4 * N + k] : smoothedSmoke(x, y, z);
         for (int c = 1; c < 4; c++) G.field[o + c * N] = fld[((size_t)s * 4 + c) * N + k];
       }
+      if (smokeDiv > 1)
+        for (int k = 0; k < SN; k++) {
+          int x = b[0] * SB + (k & (SB - 1)), y = b[1] * SB + ((k >> sshift) & (SB - 1)), z = b[2] * SB + (k >> (2 * sshift));
+          G.smoke[(size_t)r * SN + k] = smoothedCoarse(x, y, z);
+        }
     }
 #pragma omp parallel for schedule(dynamic)
     for (long r = 0; r < (long)nb; r++) {
@@ -1287,14 +1365,33 @@ struct Sim {
         int o[3] = {b[0] * B + (blk % per) * 8 - 2, b[1] * B + ((blk / per) % per) * 8 - 2,
                     b[2] * B + (blk / (per * per)) * 8 - 2};
         int flags = 0;
+        const bool coarse = smokeDiv > 1;
+        R glowMax = 0, smokeMax = 0;
         for (int u = 0; u < 216; u++) {
           int ux = o[0] + (u % 6) * 2, uy = o[1] + ((u / 6) % 6) * 2, uz = o[2] + (u / 36) * 2;
           if (!G.index.count(brickKey(ux >> shift, uy >> shift, uz >> shift))) continue;
           for (int k = 0; k < 8; k++) {
             auto f = renderCell(G, ux + (k & 1), uy + ((k >> 1) & 1), uz + (k >> 2), true);
             R g = glowOf(f[2]);
-            flags |= (g > R(.002) ? 1 : 0) | (f[0] + g > R(.002) ? 2 : 0);
+            flags |= (g > R(.002) ? 1 : 0) | ((coarse ? R(0) : f[0]) + g > R(.002) ? 2 : 0);
+            glowMax = std::max(glowMax, g);
           }
+        }
+        if (coarse) {  // every trilinear donor of coarse density in the block and halo
+          R ratio = R(smokeDiv);
+          int lo[3], hi[3];
+          for (int a = 0; a < 3; a++) {
+            lo[a] = (int)std::floor(R(o[a]) / ratio - R(.5));
+            hi[a] = (int)std::floor(R(o[a] + 12) / ratio - R(.5)) + 1;
+          }
+          for (int z = lo[2]; z <= hi[2]; z++)
+            for (int y = lo[1]; y <= hi[1]; y++)
+              for (int x = lo[0]; x <= hi[0]; x++) {
+                int q[3] = {x, y, z};
+                for (int a = 0; a < 3; a++) q[a] = std::min(std::max(q[a], renderLo[a] * SB), (renderHi[a] + 1) * SB - 1);
+                smokeMax = std::max(smokeMax, cachedSmokeCell(G, q[0], q[1], q[2]));
+              }
+          if (smokeMax + glowMax > R(.002)) flags |= 2;
         }
         G.occupancy[(size_t)r * blocks + blk] = (uint8_t)flags;
       }
@@ -1366,6 +1463,7 @@ struct Sim {
           continue;
         }
         auto f = reconstruct(G, cell[0], cell[1], cell[2], (flags & 1) ? rs.filter : 0);
+        if (smokeDiv > 1) f[0] = renderSmokeAt(G, cell[0] / R(smokeDiv), cell[1] / R(smokeDiv), cell[2] / R(smokeDiv));
         if (f[0] + glowOf(f[2]) > R(.002)) {
           auto glow = emissionOf(G, f);
           R density = std::max(R(0), f[0]) * R(rs.optical[0]), sc[3] = {0, 0, 0};

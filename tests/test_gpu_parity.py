@@ -184,7 +184,7 @@ def test_mesh_force_targets(brick):
     check(reports, min_active=8 if brick == 16 else 30)
 
 
-def test_coarse_smoke_render_unsupported():
+def test_coarse_smoke_lights_unsupported():
     sc = scenes.ForceScene()
     g = sc.grid(budget=2 ** 20)
     g.smoke_divisor = 2
@@ -192,7 +192,7 @@ def test_coarse_smoke_render_unsupported():
     sim.step(sc.frame(0).frame)
     from firepro import render
     with pytest.raises(FireProError):
-        sim.render(render.look_at((1, 1, 1), (0, 0, 0), 8, 8), render.default_settings())
+        sim.collect_lights(render.default_settings(), [[0.0, 0.3, 0.0]])
     sim.dispose()
 
 

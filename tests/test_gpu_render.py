@@ -41,6 +41,33 @@ def test_flame_render_parity(filter_mode):
     assert err <= RENDER_TOL
 
 
+@pytest.mark.parametrize("divisor,velocity", [(2, 1), (4, 2)])
+def test_coarse_smoke_render_parity(divisor, velocity):
+    """Coarse smoke (smokeDivisor 2 and 4): the smoke smoothed on its own lattice
+    (smoothCoarseSmoke), sampled once per march step and light sample (renderSmokeAt), the
+    fields as the simulation holds them, and the occupancy's conservative bound over coarse
+    donors (cachedSmokeCell); with a velocity divisor too."""
+    cam = render.look_at((1.4, 1.0, 2.0), (0.0, 0.45, 0.0), 64, 48, time=0.5)
+    st = render.default_settings(ray_steps=128)
+    sc = scenes.ForceScene()
+    sc.velocity_divisor = velocity
+    g = sc.grid(budget=2 ** 20)
+    g.smoke_divisor = divisor
+    out = {}
+
+    def after(gpu, orc):
+        out["gpu"] = gpu.render(cam, st)
+        out["orc"] = orc.render(cam, st)
+
+    parity.lockstep(sc, 12, lambda gr: FluidSimulation(gr), budget=2 ** 20, grid=g, after=after)
+    gpu, orc = out["gpu"], out["orc"]
+    assert np.isfinite(gpu).all()
+    assert orc[..., 3].max() > 0.05, "the smoke should be visible"
+    err = parity.rel_l2(gpu, orc.astype(np.float64))
+    print(f"coarse smoke /{divisor}: relative L2 {err:.2e}, opacity max {orc[..., 3].max():.3f}")
+    assert err <= RENDER_TOL
+
+
 def test_large_scene_render_parity():
     """Colliders, turbulence, three emitters; lighting at divisor 2."""
     cam = render.look_at((2.5, 1.6, 3.2), (0.0, 0.8, 0.0), 64, 40, time=1.0)

@@ -73,16 +73,93 @@ FP_DEV float smoothedSmoke(const SimParams& P, const FpRender& R, SlotCache& c, 
   return fmaxf(0.f, d * .125f);
 }
 
+// The coarse smoke grid (smoke_divisor d > 1): 2^P.smokeShift cells a brick side.
+// The simulation's coarse density at a coarse cell: zero outside the box or without a slot.
+FP_DEV float rawCoarse(const SimParams& P, const FpRender& R, SlotCache& c, int x, int y, int z) {
+  const int sh = P.smokeShift, m = (1 << sh) - 1;
+  int s = slotAt(P, R, c, x >> sh, y >> sh, z >> sh);
+  if (s < 0) return 0.f;
+  return ldHalf(P.smk, (size_t)s * P.smokeCells + (((z & m) << sh | (y & m)) << sh | (x & m)), P.scalarHalf != 0);
+}
+// fireProField of the coarse density at `q` in coarse cells: clamped to the box, trilinear.
+FP_DEV float coarseSample(const SimParams& P, const FpRender& R, SlotCache& c, float qx, float qy, float qz) {
+  float S = (float)(1 << P.smokeShift);
+  qx = fminf(fmaxf(qx, (float)R.boxLo[0] * S + .5f), (float)(R.boxHi[0] + 1) * S - .5f);
+  qy = fminf(fmaxf(qy, (float)R.boxLo[1] * S + .5f), (float)(R.boxHi[1] + 1) * S - .5f);
+  qz = fminf(fmaxf(qz, (float)R.boxLo[2] * S + .5f), (float)(R.boxHi[2] + 1) * S - .5f);
+  float gx = qx - .5f, gy = qy - .5f, gz = qz - .5f;
+  int x0 = (int)floorf(gx), y0 = (int)floorf(gy), z0 = (int)floorf(gz);
+  float fx = gx - (float)x0, fy = gy - (float)y0, fz = gz - (float)z0;
+  float v = 0.f;
+  for (int k = 0; k < 8; k++) {
+    int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
+    float w = (dx ? fx : 1.f - fx) * (dy ? fy : 1.f - fy) * (dz ? fz : 1.f - fz);
+    v += rawCoarse(P, R, c, x0 + dx, y0 + dy, z0 + dz) * w;
+  }
+  return v;
+}
+// smoothCoarseSmoke (lighting.wgsl:104-129): the [1,2,1]/4 density at a coarse cell.
+FP_DEV float smoothedCoarse(const SimParams& P, const FpRender& R, SlotCache& c, int x, int y, int z) {
+  float d = 0.f;
+  for (int k = 0; k < 8; k++)
+    d += coarseSample(P, R, c, (float)(x + (k & 1)), (float)(y + ((k >> 1) & 1)), (float)(z + (k >> 2)));
+  return fmaxf(0.f, d * .125f);
+}
+// The smoothed coarse density at a coarse cell: the pool in a brick with a slot, else what a
+// sample based in a slotted brick reads from its apron (`apron`), else zero.
+FP_DEV float renderSmokeCell(const SimParams& P, const FpRender& R, SlotCache& c, int x, int y, int z, bool apron) {
+  const int sh = P.smokeShift, m = (1 << sh) - 1;
+  int s = slotAt(P, R, c, x >> sh, y >> sh, z >> sh);
+  if (s >= 0) return R.renderSmoke[(size_t)s * P.smokeCells + (((z & m) << sh | (y & m)) << sh | (x & m))];
+  return apron ? smoothedCoarse(P, R, c, x, y, z) : 0.f;
+}
+// renderSmokeAt (volume-common.wgsl:74-78): fireProField of the smoothed coarse density at `q`
+// in coarse cells.
+FP_DEV float renderSmokeAt(const SimParams& P, const FpRender& R, SlotCache& c, float qx, float qy, float qz) {
+  const int sh = P.smokeShift;
+  float S = (float)(1 << sh);
+  qx = fminf(fmaxf(qx, (float)R.boxLo[0] * S + .5f), (float)(R.boxHi[0] + 1) * S - .5f);
+  qy = fminf(fmaxf(qy, (float)R.boxLo[1] * S + .5f), (float)(R.boxHi[1] + 1) * S - .5f);
+  qz = fminf(fmaxf(qz, (float)R.boxLo[2] * S + .5f), (float)(R.boxHi[2] + 1) * S - .5f);
+  float gx = qx - .5f, gy = qy - .5f, gz = qz - .5f;
+  int x0 = (int)floorf(gx), y0 = (int)floorf(gy), z0 = (int)floorf(gz);
+  float fx = gx - (float)x0, fy = gy - (float)y0, fz = gz - (float)z0;
+  bool based = slotAt(P, R, c, x0 >> sh, y0 >> sh, z0 >> sh) >= 0;
+  float v = 0.f;
+  for (int k = 0; k < 8; k++) {
+    int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
+    float w = (dx ? fx : 1.f - fx) * (dy ? fy : 1.f - fy) * (dz ? fz : 1.f - fz);
+    v += renderSmokeCell(P, R, c, x0 + dx, y0 + dy, z0 + dz, based) * w;
+  }
+  return v;
+}
+// cachedSmokeCell (lighting.wgsl:133-156): the smoothed coarse density a conservative bound
+// reads at coarse cell (x,y,z): the pool, else the apron a previous neighbour holds.
+FP_DEV float cachedSmokeCell(const SimParams& P, const FpRender& R, SlotCache& c, int x, int y, int z) {
+  const int sh = P.smokeShift, m = (1 << sh) - 1;
+  int bx = x >> sh, by = y >> sh, bz = z >> sh;
+  int s = slotAt(P, R, c, bx, by, bz);
+  if (s >= 0) return R.renderSmoke[(size_t)s * P.smokeCells + (((z & m) << sh | (y & m)) << sh | (x & m))];
+  const int l[3] = {x & m, y & m, z & m};
+  for (int k = 1; k < 8; k++) {
+    if (((k & 1) && l[0] != 0) || ((k & 2) && l[1] != 0) || ((k & 4) && l[2] != 0)) continue;
+    if (slotAt(P, R, c, bx - (k & 1), by - ((k >> 1) & 1), bz - ((k >> 2) & 1)) >= 0)
+      return smoothedCoarse(P, R, c, x, y, z);
+  }
+  return 0.f;
+}
+
 // The render field at a world cell. A cell of a brick with a slot reads the pool. A cell in a
 // brick without one reads as the apron of a sample based in a slotted brick would hold it
-// (`apron`: the smoothed density, no heat, flame or fuel), else zero.
+// (`apron`: the smoothed density, no heat, flame or fuel; all zero with coarse smoke, whose
+// field apron holds no neighbour), else zero.
 FP_DEV float4 renderCell(const SimParams& P, const FpRender& R, SlotCache& c, int x, int y, int z, bool apron) {
   int s = slotAt(P, R, c, x >> P.shift, y >> P.shift, z >> P.shift);
   if (s >= 0) {
     size_t i = (size_t)s * 4 * P.N + localCell(P, x, y, z);
     return make_float4(R.renderField[i], R.renderField[i + P.N], R.renderField[i + 2 * P.N], R.renderField[i + 3 * P.N]);
   }
-  if (!apron) return make_float4(0.f, 0.f, 0.f, 0.f);
+  if (!apron || P.smokeDiv > 1) return make_float4(0.f, 0.f, 0.f, 0.f);
   return make_float4(smoothedSmoke(P, R, c, x, y, z), 0.f, 0.f, 0.f);
 }
 FP_DEV void add4(float4& a, const float4& b, float w) {
@@ -180,7 +257,12 @@ FP_DEV float4 sampleWorld(const SimParams& P, const FpRender& R, SlotCache& c, f
   if (px < (float)R.boxLo[0] * size || py < (float)R.boxLo[1] * size || pz < (float)R.boxLo[2] * size ||
       px > (float)(R.boxHi[0] + 1) * size || py > (float)(R.boxHi[1] + 1) * size || pz > (float)(R.boxHi[2] + 1) * size)
     return make_float4(0.f, 0.f, 0.f, 0.f);
-  return renderSample(P, R, c, px / P.h, py / P.h, pz / P.h);
+  float4 f = renderSample(P, R, c, px / P.h, py / P.h, pz / P.h);
+  if (P.smokeDiv > 1) {
+    const float r = 1.f / (float)P.smokeDiv;  // fine cells to coarse: a power of two, exact
+    f.x = renderSmokeAt(P, R, c, px / P.h * r, py / P.h * r, pz / P.h * r);
+  }
+  return f;
 }
 
 // exitDistance (lighting.wgsl:248-255).
@@ -272,10 +354,17 @@ __global__ void __launch_bounds__(RTHREADS) k_render_field(const SimParams* __re
     for (int k = threadIdx.x; k < P.N; k += blockDim.x) {
       int x = bx * P.B + (k & (P.B - 1)), y = by * P.B + ((k >> P.shift) & (P.B - 1)), z = bz * P.B + (k >> (2 * P.shift));
       size_t o = (size_t)slot * 4 * P.N + k;
-      R.renderField[o] = smoothedSmoke(P, R, c, x, y, z);
+      R.renderField[o] = P.smokeDiv > 1 ? ldHalf(P.fld, o, half) : smoothedSmoke(P, R, c, x, y, z);
       R.renderField[o + P.N] = ldHalf(P.fld, o + P.N, half);
       R.renderField[o + 2 * P.N] = ldHalf(P.fld, o + 2 * P.N, half);
       R.renderField[o + 3 * P.N] = ldHalf(P.fld, o + 3 * P.N, half);
+    }
+    if (P.smokeDiv > 1) {  // smoothCoarseSmoke on the brick's coarse cells
+      const int sh = P.smokeShift, S = 1 << sh;
+      for (int k = threadIdx.x; k < P.smokeCells; k += blockDim.x) {
+        int x = bx * S + (k & (S - 1)), y = by * S + ((k >> sh) & (S - 1)), z = bz * S + (k >> (2 * sh));
+        R.renderSmoke[(size_t)slot * P.smokeCells + k] = smoothedCoarse(P, R, c, x, y, z);
+      }
     }
   }
 }
@@ -284,6 +373,8 @@ __global__ void __launch_bounds__(RTHREADS) k_render_field(const SimParams* __re
 __global__ void __launch_bounds__(RTHREADS) k_render_light(const SimParams* __restrict__ Pp, FpRender R) {
   const SimParams& P = *Pp;
   __shared__ int flags;
+  __shared__ int glowBits, smokeBits;  // the coarse bound's maxima (nonnegative floats' bits)
+  if (threadIdx.x == 0) glowBits = smokeBits = 0;
   uint32_t total = P.counters->active;
   const int L = 1 << R.lightShift, L3 = L * L * L;
   const float texel = P.h * (float)(P.B >> R.lightShift);
@@ -299,18 +390,52 @@ __global__ void __launch_bounds__(RTHREADS) k_render_light(const SimParams* __re
       __syncthreads();
       int ox = bx * P.B + (b % per) * 8 - 2, oy = by * P.B + ((b / per) % per) * 8 - 2, oz = bz * P.B + (b / (per * per)) * 8 - 2;
       int mine = 0;
+      const bool coarse = P.smokeDiv > 1;
+      float glowMax = 0.f, smokeMax = 0.f;
       for (int u = threadIdx.x; u < 216; u += blockDim.x) {
         int ux = ox + (u % 6) * 2, uy = oy + ((u / 6) % 6) * 2, uz = oz + (u / 36) * 2;
         if (slotAt(P, R, c, ux >> P.shift, uy >> P.shift, uz >> P.shift) < 0) continue;
         for (int k = 0; k < 8; k++) {
           float4 f = renderCell(P, R, c, ux + (k & 1), uy + ((k >> 1) & 1), uz + (k >> 2), true);
           float g = glowOf(f.z);
-          mine |= (g > .002f ? 1 : 0) | (f.x + g > .002f ? 2 : 0);
+          mine |= (g > .002f ? 1 : 0) | ((coarse ? 0.f : f.x) + g > .002f ? 2 : 0);
+          glowMax = fmaxf(glowMax, g);
+        }
+      }
+      if (coarse) {
+        // Every trilinear donor of coarse density in the block and halo (lighting.wgsl:222-238).
+        const int d = P.smokeDiv, S = 1 << P.smokeShift;
+        const float ratio = (float)d;
+        int lo[3], hi[3], size[3], boxLo[3], boxHi[3];
+        const int o[3] = {ox, oy, oz};
+        for (int a = 0; a < 3; a++) {
+          lo[a] = (int)floorf((float)o[a] / ratio - .5f);
+          hi[a] = (int)floorf((float)(o[a] + 12) / ratio - .5f) + 1;
+          size[a] = hi[a] - lo[a] + 1;
+          boxLo[a] = R.boxLo[a] * S;
+          boxHi[a] = (R.boxHi[a] + 1) * S - 1;
+        }
+        for (int q = threadIdx.x; q < size[0] * size[1] * size[2]; q += blockDim.x) {
+          int cq[3] = {lo[0] + q % size[0], lo[1] + (q / size[0]) % size[1], lo[2] + q / (size[0] * size[1])};
+          for (int a = 0; a < 3; a++) cq[a] = min(max(cq[a], boxLo[a]), boxHi[a]);
+          smokeMax = fmaxf(smokeMax, cachedSmokeCell(P, R, c, cq[0], cq[1], cq[2]));
+        }
+        glowMax = fmaxf(glowMax, __shfl_xor_sync(0xffffffffu, glowMax, 16));
+        for (int w = 8; w > 0; w >>= 1) glowMax = fmaxf(glowMax, __shfl_xor_sync(0xffffffffu, glowMax, w));
+        for (int w = 16; w > 0; w >>= 1) smokeMax = fmaxf(smokeMax, __shfl_xor_sync(0xffffffffu, smokeMax, w));
+        if ((threadIdx.x & 31) == 0) {
+          atomicMax(&glowBits, __float_as_int(glowMax));
+          atomicMax(&smokeBits, __float_as_int(smokeMax));
         }
       }
       if (mine) atomicOr(&flags, mine);
       __syncthreads();
-      if (threadIdx.x == 0) R.occupancy[(size_t)slot * blocks + b] = (uint8_t)flags;
+      if (coarse && threadIdx.x == 0 && __int_as_float(smokeBits) + __int_as_float(glowBits) > .002f) flags |= 2;
+      if (threadIdx.x == 0) {
+        R.occupancy[(size_t)slot * blocks + b] = (uint8_t)flags;
+        glowBits = 0;
+        smokeBits = 0;
+      }
       __syncthreads();
     }
     // The brick's texels of the lighting lattice.
@@ -446,6 +571,10 @@ __global__ void __launch_bounds__(RTHREADS) k_march(const SimParams* __restrict_
       continue;
     }
     float4 f = reconstruct(P, R, c, cell[0], cell[1], cell[2], (flags & 1) ? R.filter : 0);
+    if (P.smokeDiv > 1) {  // fireProRenderField: the smoothed coarse density, trilinear
+      const float r = 1.f / (float)P.smokeDiv;
+      f.x = renderSmokeAt(P, R, c, cell[0] * r, cell[1] * r, cell[2] * r);
+    }
     if (f.x + glowOf(f.z) > .002f) {
       // fireProShade
       float3 glow = emissionOf(R, f);

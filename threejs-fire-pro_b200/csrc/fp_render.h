@@ -20,7 +20,9 @@ struct FpRender {
   int lightShift;       // lighting texels per brick side = 1 << lightShift
   int boxLo[3], boxHi[3];  // the render box in bricks, inclusive
   int hasBox;
-  float* renderField;   // [slot][4][cells]: smoothed smoke, heat, lifetime, fuel
+  float* renderField;   // [slot][4][cells]: smoothed smoke, heat, lifetime, fuel (coarse smoke:
+                        // the simulation's fields as they are)
+  float* renderSmoke;   // coarse smoke (smokeDiv > 1): [slot][smoke cells], the smoothed density
   float* lighting;      // [slot][4][texels]: glow RGB, sun transmittance
   uint8_t* occupancy;   // [slot]: bit 0 flame glow, bit 1 anything visible, in the block and halo
   const float4* lut;    // blackbody: peak-normalised linear RGB, log2 radiance

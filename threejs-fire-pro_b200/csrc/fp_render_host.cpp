@@ -146,6 +146,10 @@ int Engine::renderInputs() {
   P.counters = (FpCounters*)counters_.ptr;
   P.fld = (float*)fld_[fldIdx_[0]].ptr;
   P.scalarHalf = precision_ == FP_PRECISION_MIXED ? 1 : 0;
+  P.smokeDiv = smokeDiv_;  // the coarse smoke grid, when there is one
+  P.smokeShift = sshift_;
+  P.smokeCells = SN_;
+  P.smk = (float*)smoke_[smokeIdx_[0]].ptr;
   P.velDiv = vd_;  // the field lattice's view only: the render reads no velocity
   P.solidSpan = 1;
   P.fshift = shift_;
@@ -175,7 +179,6 @@ int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* im
   if (rs.ray_steps < 8 || rs.ray_steps > 1024) return fail(FP_EINVAL, "rendering.raySteps must be from 8 to 1024.");
   if (rs.shadow_samples < 1 || rs.shadow_samples > 256) return fail(FP_EINVAL, "shadow samples must be from 1 to 256.");
   if (rs.filter < 0 || rs.filter > 2) return fail(FP_EINVAL, "rendering.filter must be 0, 1 or 2.");
-  if (smokeDiv_ > 1) return fail(FP_EUNSUPPORTED, "render: smoke on a coarse grid is not rendered by this build.");
   int rc = consume();
   if (rc) return rc;
   const int divShift = rs.lighting_divisor == 1 ? 0 : (rs.lighting_divisor == 2 ? 1 : 2);
@@ -186,6 +189,8 @@ int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* im
             (lighting_.bytes >= (size_t)slots_ * 4 * L * L * L * 4 ||
              grow(lighting_, (size_t)slots_ * 4 * L * L * L * 4, 0)) &&
             (occupancy_.bytes >= (size_t)slots_ * blocks || grow(occupancy_, (size_t)slots_ * blocks, 0)) &&
+            (smokeDiv_ == 1 || renderSmoke_.bytes >= (size_t)slots_ * SN_ * 4 ||
+             grow(renderSmoke_, (size_t)slots_ * SN_ * 4, 0)) &&
             (renderParams_.ptr || alloc(renderParams_, sizeof(SimParams), false));
   if (!ok) return FP_ENOMEM;
   float* out = image;
@@ -211,6 +216,7 @@ int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* im
   }
   R.hasBox = renderBox_ && steps_ > 0 ? 1 : 0;
   R.renderField = (float*)renderField_.ptr;
+  R.renderSmoke = (float*)renderSmoke_.ptr;
   R.lighting = (float*)lighting_.ptr;
   R.occupancy = (uint8_t*)occupancy_.ptr;
   R.lut = (const float4*)lut_.ptr;
