@@ -277,6 +277,13 @@ typedef struct fp_camera {
   float inverse_view_projection[16]; /* clip to world, column-major (the WGSL mat4x4f's columns) */
   uint32_t width, height;            /* pixels */
   float time;                        /* seconds: the jitter's frame is floor(time x 60) */
+  /* The scene's depth buffer, host memory (width x height floats, clip-space z from 0 near to 1
+   * far, rows from the top): a ray ends where the scene's geometry is (fireProSceneDistance,
+   * volume-march.wgsl:76-89). Null: nothing in front of the volume. */
+  const float* scene_depth;
+  /* 1: a half-resolution pass first records the march at 8 depths, and each pixel resumes from
+   * the last one in front of the scene (scene-volume.wgsl:146-160, volume-slices.wgsl). */
+  uint32_t half_resolution;
 } fp_camera;
 typedef struct fp_render_settings {
   float optical[4];       /* smoke extinction, fire brightness, shadow extinction, anisotropy g */

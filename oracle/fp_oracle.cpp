@@ -1404,82 +1404,161 @@ struct Sim {
       }
     }
     const int W = (int)cam.width, Hh = (int)cam.height;
+    // A ray of viewport point (ux, uy) (fireProRay, fireProSpan) and what its march keeps.
+    struct Ray {
+      R ro[3], rd[3], safe[3], exitSide[3], lo, hi, stepSize, jitter, direct[3];
+    };
+    const R brickSize = h * R(B), lightRatio = R(B >> G.lightShift);
+    auto rayOf = [&](R ux, R uy, Ray& r) -> bool {
+      R cx = ux * 2 - 1, cy = 1 - uy * 2;
+      const float* M = cam.inverse_view_projection;
+      R nh[4], fh[4];
+      for (int k = 0; k < 4; k++) {
+        nh[k] = R(M[k]) * cx + R(M[4 + k]) * cy + R(M[12 + k]);
+        fh[k] = R(M[k]) * cx + R(M[4 + k]) * cy + R(M[8 + k]) * R(.99999f) + R(M[12 + k]);
+      }
+      for (int a = 0; a < 3; a++) {
+        r.ro[a] = nh[a] / nh[3];
+        r.rd[a] = fh[a] / fh[3] - r.ro[a];
+      }
+      R rl = std::sqrt(r.rd[0] * r.rd[0] + r.rd[1] * r.rd[1] + r.rd[2] * r.rd[2]);
+      for (int a = 0; a < 3; a++) r.rd[a] /= rl;
+      r.lo = 0;
+      r.hi = R(1e30);
+      for (int a = 0; a < 3; a++) {
+        r.safe[a] = std::fabs(r.rd[a]) > R(1e-6) ? r.rd[a] : R(1e-6);
+        r.exitSide[a] = r.rd[a] > 0 ? 1 : 0;
+        R ta = (R(renderLo[a]) * brickSize - r.ro[a]) / r.safe[a], tb = (R(renderHi[a] + 1) * brickSize - r.ro[a]) / r.safe[a];
+        r.lo = std::max(r.lo, std::min(ta, tb));
+        r.hi = std::min(r.hi, std::max(ta, tb));
+      }
+      if (!(r.hi > r.lo)) return false;
+      r.stepSize = std::max(h * R(.5), (r.hi - r.lo) / R(rs.ray_steps));
+      R ln = std::sqrt(R(rs.light[0]) * rs.light[0] + R(rs.light[1]) * rs.light[1] + R(rs.light[2]) * rs.light[2]);
+      R g = rs.optical[3];
+      R mu = (r.rd[0] * rs.light[0] + r.rd[1] * rs.light[1] + r.rd[2] * rs.light[2]) / ln;
+      R phase = (1 - g * g) / std::pow(std::max(R(.05), 1 + g * g - 2 * g * mu), R(1.5));
+      R dk = R(rs.light[3]) * (R(.35) + phase * R(.3));
+      for (int c = 0; c < 3; c++) r.direct[c] = R(rs.scene_light[c]) * dk;
+      return true;
+    };
+    // One step of fireProMarch at t, ds long; returns the next t.
+    auto marchStep = [&](const Ray& r, R t, R ds, R& trans, R* rad) -> R {
+      R tt = t + r.jitter * ds;
+      R p[3] = {r.ro[0] + r.rd[0] * tt, r.ro[1] + r.rd[1] * tt, r.ro[2] + r.rd[2] * tt};
+      R cell[3] = {p[0] / h, p[1] / h, p[2] / h};
+      int ci[3] = {(int)std::floor(cell[0]), (int)std::floor(cell[1]), (int)std::floor(cell[2])};
+      auto it = G.index.find(brickKey(ci[0] >> shift, ci[1] >> shift, ci[2] >> shift));
+      R size = brickSize;
+      int flags = 0;
+      if (it != G.index.end()) {
+        int m = B - 1;
+        int block = ((((ci[2] & m) >> 3) * per) + ((ci[1] & m) >> 3)) * per + ((ci[0] & m) >> 3);
+        flags = G.occupancy[(size_t)it->second * blocks + block];
+        size = h * 8;
+      }
+      if (!(flags & 2)) {
+        R dist = R(1e30);
+        for (int a = 0; a < 3; a++) dist = std::min(dist, ((std::floor(p[a] / size) + r.exitSide[a]) * size - p[a]) / r.safe[a]);
+        return std::min(t + std::max(R(1), std::floor(dist / r.stepSize) + 1) * r.stepSize, r.hi);
+      }
+      auto f = reconstruct(G, cell[0], cell[1], cell[2], (flags & 1) ? rs.filter : 0);
+      if (smokeDiv > 1) f[0] = renderSmokeAt(G, cell[0] / R(smokeDiv), cell[1] / R(smokeDiv), cell[2] / R(smokeDiv));
+      if (f[0] + glowOf(f[2]) > R(.002)) {
+        auto glow = emissionOf(G, f);
+        R density = std::max(R(0), f[0]) * R(rs.optical[0]), sc[3] = {0, 0, 0};
+        if (density > 0) {
+          auto inc = lightSample(G, cell[0] / lightRatio, cell[1] / lightRatio, cell[2] / lightRatio);
+          for (int c = 0; c < 3; c++)
+            sc[c] = R(rs.smoke[c]) * (R(rs.ambient_light[c]) + r.direct[c] * inc[3] + inc[c] * R(.65)) * density;
+        }
+        R ext = extinctionOf(G, f), tau = ext * ds;
+        R integral = ds * (1 - R(.5) * tau + tau * tau / 6);
+        if (tau >= R(.001)) integral = (1 - std::exp(-tau)) / ext;
+        for (int c = 0; c < 3; c++) rad[c] += trans * (sc[c] + glow[c]) * integral;
+        trans *= 1 - std::min(R(1), ext * integral);
+      }
+      return t + ds;
+    };
+    // buildSlices (volume-slices.wgsl:28-122) at half resolution.
+    const int SW = std::max(1, (W + 1) / 2), SH = std::max(1, (Hh + 1) / 2), NS = 8;
+    std::vector<R> slices;
+    const bool half = cam.half_resolution != 0 && renderBox && steps > 0;
+    if (half) {
+      slices.assign((size_t)SW * SH * NS * 4, 0);
+#pragma omp parallel for schedule(dynamic)
+      for (long pix = 0; pix < (long)SW * SH; pix++) {
+        int px = (int)(pix % SW), py = (int)(pix / SW);
+        R* out = &slices[(size_t)pix * NS * 4];
+        R trans = 1, rad[3] = {0, 0, 0};
+        int recorded = 0;
+        Ray r;
+        if (rayOf((R(px) + R(.5)) / R(SW), (R(py) + R(.5)) / R(SH), r)) {
+          r.jitter = jitterOf((uint32_t)px, (uint32_t)py, cam.time);
+          R spacing = std::max(r.hi - r.lo, R(0)) / R(NS), t = r.lo, depth = r.lo + spacing;
+          while (recorded < NS && t < r.hi && trans >= R(.008)) {
+            R ds = std::min(r.stepSize, std::min(depth, r.hi) - t);
+            t = marchStep(r, t, ds, trans, rad);
+            while (recorded < NS && t >= depth) {
+              R v[4] = {rad[0], rad[1], rad[2], 1 - trans};
+              for (int c = 0; c < 4; c++) out[recorded * 4 + c] = v[c];
+              recorded++;
+              depth = r.lo + spacing * R(recorded + 1);
+            }
+          }
+        }
+        for (; recorded < NS; recorded++) {
+          R v[4] = {rad[0], rad[1], rad[2], 1 - trans};
+          for (int c = 0; c < 4; c++) out[recorded * 4 + c] = v[c];
+        }
+      }
+    }
 #pragma omp parallel for schedule(dynamic)
     for (long pix = 0; pix < (long)W * Hh; pix++) {
       int px = (int)(pix % W), py = (int)(pix / W);
       float* out = image + pix * 4;
       out[0] = out[1] = out[2] = out[3] = 0.f;
       if (!renderBox || steps == 0) continue;
-      R cx = (R(px) + R(.5)) / R(W) * 2 - 1, cy = 1 - (R(py) + R(.5)) / R(Hh) * 2;
-      const float* M = cam.inverse_view_projection;
-      R nh[4], fh[4];
-      for (int r = 0; r < 4; r++) {
-        nh[r] = R(M[r]) * cx + R(M[4 + r]) * cy + R(M[12 + r]);
-        fh[r] = R(M[r]) * cx + R(M[4 + r]) * cy + R(M[8 + r]) * R(.99999f) + R(M[12 + r]);
+      R ux = (R(px) + R(.5)) / R(W), uy = (R(py) + R(.5)) / R(Hh);
+      Ray r;
+      if (!rayOf(ux, uy, r)) continue;
+      // fireProSceneDistance (volume-march.wgsl:76-89)
+      R end = r.hi;
+      if (cam.scene_depth && cam.scene_depth[pix] < .999999f) {
+        const float* M = cam.inverse_view_projection;
+        R cx = ux * 2 - 1, cy = 1 - uy * 2, d = cam.scene_depth[pix], hit[4], dist = 0;
+        for (int k = 0; k < 4; k++) hit[k] = R(M[k]) * cx + R(M[4 + k]) * cy + R(M[8 + k]) * d + R(M[12 + k]);
+        for (int a = 0; a < 3; a++) dist += (hit[a] / hit[3] - r.ro[a]) * r.rd[a];
+        end = std::min(end, dist);
       }
-      R ro[3], rd[3];
-      for (int a = 0; a < 3; a++) {
-        ro[a] = nh[a] / nh[3];
-        rd[a] = fh[a] / fh[3] - ro[a];
-      }
-      R rl = std::sqrt(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2]);
-      for (int a = 0; a < 3; a++) rd[a] /= rl;
-      R brickSize = h * R(B), safe[3], exitSide[3], lo = 0, hi = R(1e30);
-      for (int a = 0; a < 3; a++) {
-        safe[a] = std::fabs(rd[a]) > R(1e-6) ? rd[a] : R(1e-6);
-        exitSide[a] = rd[a] > 0 ? 1 : 0;
-        R ta = (R(renderLo[a]) * brickSize - ro[a]) / safe[a], tb = (R(renderHi[a] + 1) * brickSize - ro[a]) / safe[a];
-        lo = std::max(lo, std::min(ta, tb));
-        hi = std::min(hi, std::max(ta, tb));
-      }
-      if (!(hi > lo)) continue;
-      R end = hi, stepSize = std::max(h * R(.5), (hi - lo) / R(rs.ray_steps));
-      R jitter = jitterOf((uint32_t)px, (uint32_t)py, cam.time);
-      R ln = std::sqrt(R(rs.light[0]) * rs.light[0] + R(rs.light[1]) * rs.light[1] + R(rs.light[2]) * rs.light[2]);
-      R g = rs.optical[3];
-      R mu = (rd[0] * rs.light[0] + rd[1] * rs.light[1] + rd[2] * rs.light[2]) / ln;
-      R phase = (1 - g * g) / std::pow(std::max(R(.05), 1 + g * g - 2 * g * mu), R(1.5));
-      R dk = R(rs.light[3]) * (R(.35) + phase * R(.3));
-      R lightRatio = R(B >> G.lightShift);
-      R t = lo, trans = 1, rad[3] = {0, 0, 0};
-      while (t < end && trans >= R(.008)) {
-        R ds = std::min(stepSize, end - t), tt = t + jitter * ds;
-        R p[3] = {ro[0] + rd[0] * tt, ro[1] + rd[1] * tt, ro[2] + rd[2] * tt};
-        R cell[3] = {p[0] / h, p[1] / h, p[2] / h};
-        int ci[3] = {(int)std::floor(cell[0]), (int)std::floor(cell[1]), (int)std::floor(cell[2])};
-        auto it = G.index.find(brickKey(ci[0] >> shift, ci[1] >> shift, ci[2] >> shift));
-        R size = brickSize;
-        int flags = 0;
-        if (it != G.index.end()) {
-          int m = B - 1;
-          int block = ((((ci[2] & m) >> 3) * per) + ((ci[1] & m) >> 3)) * per + ((ci[0] & m) >> 3);
-          flags = G.occupancy[(size_t)it->second * blocks + block];
-          size = h * 8;
-        }
-        if (!(flags & 2)) {
-          R dist = R(1e30);
-          for (int a = 0; a < 3; a++) dist = std::min(dist, ((std::floor(p[a] / size) + exitSide[a]) * size - p[a]) / safe[a]);
-          t = std::min(t + std::max(R(1), std::floor(dist / stepSize) + 1) * stepSize, end);
-          continue;
-        }
-        auto f = reconstruct(G, cell[0], cell[1], cell[2], (flags & 1) ? rs.filter : 0);
-        if (smokeDiv > 1) f[0] = renderSmokeAt(G, cell[0] / R(smokeDiv), cell[1] / R(smokeDiv), cell[2] / R(smokeDiv));
-        if (f[0] + glowOf(f[2]) > R(.002)) {
-          auto glow = emissionOf(G, f);
-          R density = std::max(R(0), f[0]) * R(rs.optical[0]), sc[3] = {0, 0, 0};
-          if (density > 0) {
-            auto inc = lightSample(G, cell[0] / lightRatio, cell[1] / lightRatio, cell[2] / lightRatio);
-            for (int c = 0; c < 3; c++)
-              sc[c] = R(rs.smoke[c]) * (R(rs.ambient_light[c]) + R(rs.scene_light[c]) * dk * inc[3] + inc[c] * R(.65)) *
-                      density;
+      if (end <= r.lo) continue;
+      r.jitter = jitterOf((uint32_t)px, (uint32_t)py, cam.time);
+      R t = r.lo, trans = 1, rad[3] = {0, 0, 0};
+      if (half) {  // resume from the last slice in front of the scene (scene-volume.wgsl:146-160)
+        R slice = std::floor((end - r.lo) / (r.hi - r.lo) * R(NS));
+        if (slice >= 1) {
+          int layer = (int)std::min(slice, R(NS)) - 1;
+          R gx = ux * R(SW) - R(.5), gy = uy * R(SH) - R(.5);
+          R fx0 = std::floor(gx), fy0 = std::floor(gy), wx = gx - fx0, wy = gy - fy0;
+          int x0 = (int)fx0, y0 = (int)fy0;
+          int xs[2] = {std::min(std::max(x0, 0), SW - 1), std::min(std::max(x0 + 1, 0), SW - 1)};
+          int ys[2] = {std::min(std::max(y0, 0), SH - 1), std::min(std::max(y0 + 1, 0), SH - 1)};
+          R v[4] = {0, 0, 0, 0};
+          for (int k = 0; k < 4; k++) {
+            int ix = k & 1, iy = k >> 1;
+            R w = (ix ? wx : 1 - wx) * (iy ? wy : 1 - wy);
+            const R* sv4 = &slices[(((size_t)ys[iy] * SW + xs[ix]) * NS + layer) * 4];
+            for (int c = 0; c < 4; c++) v[c] += sv4[c] * w;
           }
-          R ext = extinctionOf(G, f), tau = ext * ds;
-          R integral = ds * (1 - R(.5) * tau + tau * tau / 6);
-          if (tau >= R(.001)) integral = (1 - std::exp(-tau)) / ext;
-          for (int c = 0; c < 3; c++) rad[c] += trans * (sc[c] + glow[c]) * integral;
-          trans *= 1 - std::min(R(1), ext * integral);
+          t = r.lo + (r.hi - r.lo) * std::min(slice, R(NS)) / R(NS);
+          trans = 1 - v[3];
+          for (int c = 0; c < 3; c++) rad[c] = v[c];
         }
-        t += ds;
+      }
+      while (t < end && trans >= R(.008)) {
+        if (t >= r.hi) break;
+        R ds = std::min(r.stepSize, std::min(end, r.hi) - t);
+        t = marchStep(r, t, ds, trans, rad);
       }
       out[0] = (float)rad[0];
       out[1] = (float)rad[1];

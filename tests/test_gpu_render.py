@@ -5,6 +5,8 @@ each step, so after the last step they hold identical fields and directories. Th
 (linear radiance and opacity) must agree within relative L2 RENDER_TOL: the march is the
 same arithmetic in FP32 and FP64, with the same jitter, occupancy skips and thresholds.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -136,3 +138,40 @@ def test_scene_lights_parity():
             if row[4:7].max() >= 1e-8:  # dimmer colours are divided by 1e-8, as the reference does
                 assert rgb.max() == pytest.approx(1.0)
             assert position[1] >= 0.0
+
+
+@pytest.mark.parametrize("half", [0, 1])
+def test_scene_depth_and_half_resolution(half):
+    """fireProSceneDistance (volume-march.wgsl:76-89): a depth buffer ends the rays at a tilted
+    plane through the flames; with `half_resolution` the half-resolution pass records eight
+    depths (buildSlices) and each pixel resumes from the last one in front of the scene."""
+    w, hgt = 64, 48
+    cam = render.look_at((1.4, 1.0, 2.0), (0.0, 0.45, 0.0), w, hgt, time=0.5)
+    # clip z of a plane 2.35 m + 0.4 (u - .5) m from the eye along each pixel's ray: from the
+    # projection's depth mapping, z_clip = (far (d - near)) / (d (far - near)) for eye depth d
+    near, far = 0.05, 50.0
+    u = (np.arange(w) + 0.5) / w
+    d = 2.35 + 0.4 * (u[None, :] - 0.5) + np.zeros((hgt, 1))
+    depth = np.ascontiguousarray((far * (d - near) / (d * (far - near))).astype(np.float32))
+    depth[:, : w // 8] = 1.0  # a band with nothing in front
+    cam.scene_depth = depth.ctypes.data_as(C.POINTER(C.c_float))
+    cam.half_resolution = half
+    st = render.default_settings(ray_steps=128)
+    out = {}
+
+    def after(gpu, orc):
+        out["gpu"] = gpu.render(cam, st)
+        out["orc"] = orc.render(cam, st)
+        cam.scene_depth = None
+        out["open"] = orc.render(cam, st)
+
+    parity.lockstep(scenes.ForceScene(), 12, lambda g: FluidSimulation(g), budget=2 ** 20, after=after)
+    gpu, orc = out["gpu"], out["orc"]
+    assert np.isfinite(gpu).all()
+    assert orc[..., 3].max() > 0.05
+    err = parity.rel_l2(gpu, orc.astype(np.float64))
+    print(f"depth, half {half}: relative L2 {err:.2e}")
+    assert err <= RENDER_TOL
+    # the depth clipped something, and nothing where the band is open
+    assert np.abs(out["open"] - orc).max() > 1e-3
+    assert np.allclose(out["open"][:, : w // 8], orc[:, : w // 8], atol=1e-5) or half

@@ -183,7 +183,7 @@ Engine::~Engine() {
   owner_->forget(this);
   cudaStreamSynchronize(stream());
   freeAll();
-  DeviceBuffer* render[] = {&renderField_, &renderSmoke_, &lighting_, &occupancy_, &lut_, &renderParams_, &image_, &anchors_, &lightSums_};
+  DeviceBuffer* render[] = {&renderField_, &renderSmoke_, &sceneDepth_, &slices_, &lighting_, &occupancy_, &lut_, &renderParams_, &image_, &anchors_, &lightSums_};
   for (DeviceBuffer* b : render)
     if (b->ptr) cudaFree(b->ptr);
   if (renderParamsH_) cudaFreeHost(renderParamsH_);

@@ -197,7 +197,7 @@ class Engine {
   int renderLo_[3] = {0, 0, 0}, renderHi_[3] = {-1, -1, -1};
   bool renderBox_ = false;
   std::vector<int> sourceBoxes_;  // lo xyz, hi xyz per source
-  DeviceBuffer renderField_, renderSmoke_, lighting_, occupancy_, lut_, renderParams_, image_, anchors_, lightSums_;
+  DeviceBuffer renderField_, renderSmoke_, sceneDepth_, slices_, lighting_, occupancy_, lut_, renderParams_, image_, anchors_, lightSums_;
   SimParams* renderParamsH_ = nullptr;
   // The blackbody table and the render parameters of the latest state (device).
   int renderInputs();

@@ -498,6 +498,134 @@ FP_DEV float jitterOf(uint32_t px, uint32_t py, float time) {
 }
 
 // A pixel's march (fireProSceneVolume with fireProMarch), a thread a pixel.
+// A camera ray through the box (fireProRay, fireProSpan) and what its march keeps fixed.
+struct Ray {
+  float ro[3], rd[3], safe[3], exitSide[3];
+  float lo, hi;  // box entry and exit distances
+  float stepSize, jitter, direct[3];
+};
+// The ray of viewport point (ux, uy) in [0,1]^2; false when it misses the box.
+FP_DEV bool rayOf(const SimParams& P, const FpRender& R, float ux, float uy, Ray& r) {
+  float cx = ux * 2.f - 1.f, cy = 1.f - uy * 2.f;
+  const float* M = R.ivp;
+  float nh[4], fh[4];
+  for (int k = 0; k < 4; k++) {
+    nh[k] = M[k] * cx + M[4 + k] * cy + M[8 + k] * 0.f + M[12 + k];
+    fh[k] = M[k] * cx + M[4 + k] * cy + M[8 + k] * .99999f + M[12 + k];
+  }
+  for (int a = 0; a < 3; a++) {
+    r.ro[a] = nh[a] / nh[3];
+    r.rd[a] = fh[a] / fh[3] - r.ro[a];
+  }
+  float rl = sqrtf(r.rd[0] * r.rd[0] + r.rd[1] * r.rd[1] + r.rd[2] * r.rd[2]);
+  for (int a = 0; a < 3; a++) r.rd[a] /= rl;
+  const float brickSize = P.h * (float)P.B;
+  r.lo = 0.f;
+  r.hi = 1e30f;
+  for (int a = 0; a < 3; a++) {
+    r.safe[a] = fabsf(r.rd[a]) > 1e-6f ? r.rd[a] : 1e-6f;
+    r.exitSide[a] = r.rd[a] > 0.f ? 1.f : 0.f;
+    float ta = ((float)R.boxLo[a] * brickSize - r.ro[a]) / r.safe[a];
+    float tb = ((float)(R.boxHi[a] + 1) * brickSize - r.ro[a]) / r.safe[a];
+    r.lo = fmaxf(r.lo, fminf(ta, tb));
+    r.hi = fminf(r.hi, fmaxf(ta, tb));
+  }
+  if (!(r.hi > r.lo)) return false;
+  r.stepSize = fmaxf(P.h * .5f, (r.hi - r.lo) / (float)R.raySteps);
+  // fireProDirect
+  float ln = sqrtf(R.light[0] * R.light[0] + R.light[1] * R.light[1] + R.light[2] * R.light[2]);
+  float g = R.optical[3];
+  float mu = (r.rd[0] * R.light[0] + r.rd[1] * R.light[1] + r.rd[2] * R.light[2]) / ln;
+  float phase = (1.f - g * g) / powf(fmaxf(.05f, 1.f + g * g - 2.f * g * mu), 1.5f);
+  float dk = R.light[3] * (.35f + phase * .3f);
+  for (int a = 0; a < 3; a++) r.direct[a] = R.sceneLight[a] * dk;
+  return true;
+}
+
+// One step of fireProMarch (volume-march.wgsl:178-268) at t, ds long: past an empty block a
+// skip of whole steps up to the exit, else the shaded sample. Returns the next t.
+FP_DEV float marchStep(const SimParams& P, const FpRender& R, SlotCache& c, const Ray& r, float t, float ds, float& trans,
+                       float* rad) {
+  const float brickSize = P.h * (float)P.B, lightRatio = (float)(P.B >> R.lightShift);
+  float tt = t + r.jitter * ds;
+  float p[3] = {r.ro[0] + r.rd[0] * tt, r.ro[1] + r.rd[1] * tt, r.ro[2] + r.rd[2] * tt};
+  float cell[3] = {p[0] / P.h, p[1] / P.h, p[2] / P.h};
+  int ci[3] = {(int)floorf(cell[0]), (int)floorf(cell[1]), (int)floorf(cell[2])};
+  int slot = slotAt(P, R, c, ci[0] >> P.shift, ci[1] >> P.shift, ci[2] >> P.shift);
+  float size = brickSize;
+  int flags = 0;
+  if (slot >= 0) {  // fireProOccupancy: the sample's 8-cell block of the brick
+    const int per = P.B / 8, m = P.B - 1;
+    int block = ((((ci[2] & m) >> 3) * per) + ((ci[1] & m) >> 3)) * per + ((ci[0] & m) >> 3);
+    flags = R.occupancy[(size_t)slot * per * per * per + block];
+    size = P.h * 8.f;
+  }
+  if (!(flags & 2)) {
+    // Skip whole steps past the empty block, keeping the lattice.
+    float dist = 1e30f;
+    for (int a = 0; a < 3; a++) dist = fminf(dist, ((floorf(p[a] / size) + r.exitSide[a]) * size - p[a]) / r.safe[a]);
+    return fminf(t + fmaxf(1.f, floorf(dist / r.stepSize) + 1.f) * r.stepSize, r.hi);
+  }
+  float4 f = reconstruct(P, R, c, cell[0], cell[1], cell[2], (flags & 1) ? R.filter : 0);
+  if (P.smokeDiv > 1) {  // fireProRenderField: the smoothed coarse density, trilinear
+    const float q = 1.f / (float)P.smokeDiv;
+    f.x = renderSmokeAt(P, R, c, cell[0] * q, cell[1] * q, cell[2] * q);
+  }
+  if (f.x + glowOf(f.z) > .002f) {
+    // fireProShade
+    float3 glow = emissionOf(R, f);
+    float density = fmaxf(0.f, f.x) * R.optical[0];
+    float sc[3] = {0.f, 0.f, 0.f};
+    if (density > 0.f) {
+      float4 inc = lightSample(P, R, c, cell[0] / lightRatio, cell[1] / lightRatio, cell[2] / lightRatio);
+      sc[0] = R.smoke[0] * (R.ambient[0] + r.direct[0] * inc.w + inc.x * .65f) * density;
+      sc[1] = R.smoke[1] * (R.ambient[1] + r.direct[1] * inc.w + inc.y * .65f) * density;
+      sc[2] = R.smoke[2] * (R.ambient[2] + r.direct[2] * inc.w + inc.z * .65f) * density;
+    }
+    float ext = extinctionOf(R, f);
+    float tau = ext * ds;
+    float integral = ds * (1.f - .5f * tau + tau * tau / 6.f);
+    if (tau >= .001f) integral = (1.f - expf(-tau)) / ext;
+    rad[0] += trans * (sc[0] + glow.x) * integral;
+    rad[1] += trans * (sc[1] + glow.y) * integral;
+    rad[2] += trans * (sc[2] + glow.z) * integral;
+    trans *= 1.f - fminf(1.f, ext * integral);
+  }
+  return t + ds;
+}
+
+// buildSlices (volume-slices.wgsl:28-122): a ray per half-resolution pixel marches the whole
+// span, recording radiance and opacity at FP_SLICES evenly spaced depths; depths passed by a
+// skip keep the values of the moment, those past the exit or an opaque ray the final ones.
+__global__ void __launch_bounds__(RTHREADS) k_slices(const SimParams* __restrict__ Pp, FpRender R) {
+  const SimParams& P = *Pp;
+  int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= R.sliceW * R.sliceH) return;
+  int px = pix % R.sliceW, py = pix / R.sliceW;
+  float4* out = reinterpret_cast<float4*>(R.slices) + (size_t)pix * FP_SLICES;
+  float trans = 1.f, rad[3] = {0.f, 0.f, 0.f};
+  int recorded = 0;
+  Ray r;
+  if (R.hasBox && rayOf(P, R, ((float)px + .5f) / (float)R.sliceW, ((float)py + .5f) / (float)R.sliceH, r)) {
+    r.jitter = jitterOf((uint32_t)px, (uint32_t)py, R.time);
+    const float spacing = fmaxf(r.hi - r.lo, 0.f) / (float)FP_SLICES;
+    SlotCache c{1 << 30, 0, 0, -1};
+    float t = r.lo, depth = r.lo + spacing;
+    while (recorded < FP_SLICES && t < r.hi && trans >= .008f) {
+      float ds = fminf(r.stepSize, fminf(depth, r.hi) - t);
+      t = marchStep(P, R, c, r, t, ds, trans, rad);
+      while (recorded < FP_SLICES && t >= depth) {
+        out[recorded] = make_float4(rad[0], rad[1], rad[2], 1.f - trans);
+        recorded++;
+        depth = r.lo + spacing * (float)(recorded + 1);
+      }
+    }
+  }
+  for (; recorded < FP_SLICES; recorded++) out[recorded] = make_float4(rad[0], rad[1], rad[2], 1.f - trans);
+}
+
+// fireProSceneVolume (scene-volume.wgsl:39-44, 146-167): the march of each pixel's ray up to
+// the scene's depth, from the last half-resolution slice in front of it when slices exist.
 __global__ void __launch_bounds__(RTHREADS) k_march(const SimParams* __restrict__ Pp, FpRender R) {
   const SimParams& P = *Pp;
   int pix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -506,96 +634,58 @@ __global__ void __launch_bounds__(RTHREADS) k_march(const SimParams* __restrict_
   float4* out = reinterpret_cast<float4*>(R.image) + pix;
   *out = make_float4(0.f, 0.f, 0.f, 0.f);
   if (!R.hasBox) return;
-  // fireProRay
-  float ux = ((float)px + .5f) / (float)R.width, uy = ((float)py + .5f) / (float)R.height;
-  float cx = ux * 2.f - 1.f, cy = 1.f - uy * 2.f;
-  const float* M = R.ivp;
-  auto apply = [&](float z, float* o) {
-    for (int r = 0; r < 4; r++) o[r] = M[r] * cx + M[4 + r] * cy + M[8 + r] * z + M[12 + r];
-  };
-  float nh[4], fh[4];
-  apply(0.f, nh);
-  apply(.99999f, fh);
-  float ro[3] = {nh[0] / nh[3], nh[1] / nh[3], nh[2] / nh[3]};
-  float rd[3] = {fh[0] / fh[3] - ro[0], fh[1] / fh[3] - ro[1], fh[2] / fh[3] - ro[2]};
-  float rl = sqrtf(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2]);
-  for (int a = 0; a < 3; a++) rd[a] /= rl;
-  // fireProHit / fireProSpan over the box
-  const float brickSize = P.h * (float)P.B;
-  float safe[3], exitSide[3], lo = 0.f, hi = 1e30f;
-  for (int a = 0; a < 3; a++) {
-    safe[a] = fabsf(rd[a]) > 1e-6f ? rd[a] : 1e-6f;
-    exitSide[a] = rd[a] > 0.f ? 1.f : 0.f;
-    float ta = ((float)R.boxLo[a] * brickSize - ro[a]) / safe[a];
-    float tb = ((float)(R.boxHi[a] + 1) * brickSize - ro[a]) / safe[a];
-    lo = fmaxf(lo, fminf(ta, tb));
-    hi = fminf(hi, fmaxf(ta, tb));
+  const float ux = ((float)px + .5f) / (float)R.width, uy = ((float)py + .5f) / (float)R.height;
+  Ray r;
+  if (!rayOf(P, R, ux, uy, r)) return;
+  // fireProSceneDistance (volume-march.wgsl:76-89): the scene's depth ends the ray.
+  float end = r.hi;
+  if (R.depth) {
+    const float d = R.depth[pix];
+    if (d < .999999f) {
+      const float cx = ux * 2.f - 1.f, cy = 1.f - uy * 2.f;
+      const float* M = R.ivp;
+      float hit[4];
+      for (int k = 0; k < 4; k++) hit[k] = M[k] * cx + M[4 + k] * cy + M[8 + k] * d + M[12 + k];
+      float dist = 0.f;
+      for (int a = 0; a < 3; a++) dist += (hit[a] / hit[3] - r.ro[a]) * r.rd[a];
+      end = fminf(end, dist);
+    }
   }
-  if (!(hi > lo)) return;
-  const float end = hi, exitT = hi;
-  const float stepSize = fmaxf(P.h * .5f, (hi - lo) / (float)R.raySteps);
-  const float jitter = jitterOf((uint32_t)px, (uint32_t)py, R.time);
-  // fireProDirect
-  float ln = sqrtf(R.light[0] * R.light[0] + R.light[1] * R.light[1] + R.light[2] * R.light[2]);
-  float g = R.optical[3];
-  float mu = (rd[0] * R.light[0] + rd[1] * R.light[1] + rd[2] * R.light[2]) / ln;
-  float phase = (1.f - g * g) / powf(fmaxf(.05f, 1.f + g * g - 2.f * g * mu), 1.5f);
-  float dk = R.light[3] * (.35f + phase * .3f);
-  float direct[3] = {R.sceneLight[0] * dk, R.sceneLight[1] * dk, R.sceneLight[2] * dk};
-  const float lightRatio = (float)(P.B >> R.lightShift);
-  SlotCache c{0, 0, 0, -1};
-  c.bx = 1 << 30;
-  float t = lo, trans = 1.f;
+  if (end <= r.lo) return;
+  r.jitter = jitterOf((uint32_t)px, (uint32_t)py, R.time);
+  float t = r.lo, trans = 1.f;
   float rad[3] = {0.f, 0.f, 0.f};
-  while (t < end && trans >= .008f) {
-    if (t >= exitT) break;
-    float ds = fminf(stepSize, fminf(end, exitT) - t);
-    float tt = t + jitter * ds;
-    float p[3] = {ro[0] + rd[0] * tt, ro[1] + rd[1] * tt, ro[2] + rd[2] * tt};
-    float cell[3] = {p[0] / P.h, p[1] / P.h, p[2] / P.h};
-    int ci[3] = {(int)floorf(cell[0]), (int)floorf(cell[1]), (int)floorf(cell[2])};
-    int slot = slotAt(P, R, c, ci[0] >> P.shift, ci[1] >> P.shift, ci[2] >> P.shift);
-    float size = brickSize;
-    int flags = 0;
-    if (slot >= 0) {  // fireProOccupancy: the sample's 8-cell block of the brick
-      const int per = P.B / 8, m = P.B - 1;
-      int block = ((((ci[2] & m) >> 3) * per) + ((ci[1] & m) >> 3)) * per + ((ci[0] & m) >> 3);
-      flags = R.occupancy[(size_t)slot * per * per * per + block];
-      size = P.h * 8.f;
-    }
-    if (!(flags & 2)) {
-      // Skip whole steps past the empty block, keeping the lattice.
-      float dist = 1e30f;
-      for (int a = 0; a < 3; a++) dist = fminf(dist, ((floorf(p[a] / size) + exitSide[a]) * size - p[a]) / safe[a]);
-      t = fminf(t + fmaxf(1.f, floorf(dist / stepSize) + 1.f) * stepSize, exitT);
-      continue;
-    }
-    float4 f = reconstruct(P, R, c, cell[0], cell[1], cell[2], (flags & 1) ? R.filter : 0);
-    if (P.smokeDiv > 1) {  // fireProRenderField: the smoothed coarse density, trilinear
-      const float r = 1.f / (float)P.smokeDiv;
-      f.x = renderSmokeAt(P, R, c, cell[0] * r, cell[1] * r, cell[2] * r);
-    }
-    if (f.x + glowOf(f.z) > .002f) {
-      // fireProShade
-      float3 glow = emissionOf(R, f);
-      float density = fmaxf(0.f, f.x) * R.optical[0];
-      float sc[3] = {0.f, 0.f, 0.f};
-      if (density > 0.f) {
-        float4 inc = lightSample(P, R, c, cell[0] / lightRatio, cell[1] / lightRatio, cell[2] / lightRatio);
-        sc[0] = R.smoke[0] * (R.ambient[0] + direct[0] * inc.w + inc.x * .65f) * density;
-        sc[1] = R.smoke[1] * (R.ambient[1] + direct[1] * inc.w + inc.y * .65f) * density;
-        sc[2] = R.smoke[2] * (R.ambient[2] + direct[2] * inc.w + inc.z * .65f) * density;
+  if (R.slices) {
+    // Resume from the last slice in front of the scene: the half-resolution texels
+    // interpolated bilinearly (clamped at the edges) on that slice.
+    const float count = (float)FP_SLICES;
+    const float slice = floorf((end - r.lo) / (r.hi - r.lo) * count);
+    if (slice >= 1.f) {
+      const int layer = (int)fminf(slice, count) - 1;
+      float gx = ux * (float)R.sliceW - .5f, gy = uy * (float)R.sliceH - .5f;
+      float fx0 = floorf(gx), fy0 = floorf(gy);
+      float wx = gx - fx0, wy = gy - fy0;
+      int x0 = (int)fx0, y0 = (int)fy0;
+      int xs[2] = {min(max(x0, 0), R.sliceW - 1), min(max(x0 + 1, 0), R.sliceW - 1)};
+      int ys[2] = {min(max(y0, 0), R.sliceH - 1), min(max(y0 + 1, 0), R.sliceH - 1)};
+      const float4* S = reinterpret_cast<const float4*>(R.slices);
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int k = 0; k < 4; k++) {
+        int ix = k & 1, iy = k >> 1;
+        add4(v, S[((size_t)ys[iy] * R.sliceW + xs[ix]) * FP_SLICES + layer], (ix ? wx : 1.f - wx) * (iy ? wy : 1.f - wy));
       }
-      float ext = extinctionOf(R, f);
-      float tau = ext * ds;
-      float integral = ds * (1.f - .5f * tau + tau * tau / 6.f);
-      if (tau >= .001f) integral = (1.f - expf(-tau)) / ext;
-      rad[0] += trans * (sc[0] + glow.x) * integral;
-      rad[1] += trans * (sc[1] + glow.y) * integral;
-      rad[2] += trans * (sc[2] + glow.z) * integral;
-      trans *= 1.f - fminf(1.f, ext * integral);
+      t = r.lo + (r.hi - r.lo) * fminf(slice, count) / count;
+      trans = 1.f - v.w;
+      rad[0] = v.x;
+      rad[1] = v.y;
+      rad[2] = v.z;
     }
-    t += ds;
+  }
+  SlotCache c{1 << 30, 0, 0, -1};
+  while (t < end && trans >= .008f) {
+    if (t >= r.hi) break;
+    float ds = fminf(r.stepSize, fminf(end, r.hi) - t);
+    t = marchStep(P, R, c, r, t, ds, trans, rad);
   }
   *out = make_float4(rad[0], rad[1], rad[2], 1.f - trans);
 }
@@ -681,6 +771,10 @@ void fp_launch_collect_lights(const SimParams* dP, const FpRender& R, const floa
 void fp_launch_render(const SimParams* dP, const FpRender& R, int sms, cudaStream_t st) {
   k_render_field<<<sms * 8, RTHREADS, 0, st>>>(dP, R);
   k_render_light<<<sms * 8, RTHREADS, 0, st>>>(dP, R);
+  if (R.slices) {
+    int half = R.sliceW * R.sliceH;
+    k_slices<<<(half + RTHREADS - 1) / RTHREADS, RTHREADS, 0, st>>>(dP, R);
+  }
   int pixels = R.width * R.height;
   k_march<<<(pixels + RTHREADS - 1) / RTHREADS, RTHREADS, 0, st>>>(dP, R);
 }

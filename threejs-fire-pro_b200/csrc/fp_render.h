@@ -9,6 +9,9 @@
 
 #define FP_BLACKBODY_SIZE 512
 
+// Depths a half-resolution pass records (VolumeSlices.ts DEPTH_SLICES).
+#define FP_SLICES 8
+
 struct FpRender {
   float ivp[16];  // clip to world, column-major
   int width, height;
@@ -27,6 +30,9 @@ struct FpRender {
   uint8_t* occupancy;   // [slot]: bit 0 flame glow, bit 1 anything visible, in the block and halo
   const float4* lut;    // blackbody: peak-normalised linear RGB, log2 radiance
   float* image;         // width x height x 4
+  const float* depth;   // the scene's depth buffer (width x height, clip z 0..1), or null
+  float* slices;        // half resolution: sliceW x sliceH x FP_SLICES x 4, or null (full resolution)
+  int sliceW, sliceH;
 };
 
 // Launchers (fp_render.cu): the render pools of every active brick in the box, then the march.

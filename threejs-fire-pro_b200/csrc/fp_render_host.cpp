@@ -179,6 +179,7 @@ int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* im
   if (rs.ray_steps < 8 || rs.ray_steps > 1024) return fail(FP_EINVAL, "rendering.raySteps must be from 8 to 1024.");
   if (rs.shadow_samples < 1 || rs.shadow_samples > 256) return fail(FP_EINVAL, "shadow samples must be from 1 to 256.");
   if (rs.filter < 0 || rs.filter > 2) return fail(FP_EINVAL, "rendering.filter must be 0, 1 or 2.");
+  if (cam.half_resolution > 1) return fail(FP_EINVAL, "render: half_resolution must be 0 or 1.");
   int rc = consume();
   if (rc) return rc;
   const int divShift = rs.lighting_divisor == 1 ? 0 : (rs.lighting_divisor == 2 ? 1 : 2);
@@ -199,6 +200,18 @@ int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* im
     out = (float*)image_.ptr;
   }
   if ((rc = renderInputs())) return rc;
+  // The scene's depth and the half-resolution slices.
+  const float* depth = nullptr;
+  if (cam.scene_depth) {
+    if (sceneDepth_.bytes < pixels * 4 && !alloc(sceneDepth_, pixels * 4, false)) return FP_ENOMEM;
+    if ((rc = check(cudaMemcpyAsync(sceneDepth_.ptr, cam.scene_depth, pixels * 4, cudaMemcpyHostToDevice, stream()),
+                    "render")))
+      return rc;
+    depth = (const float*)sceneDepth_.ptr;
+  }
+  const int sliceW = std::max(1, (int)((cam.width + 1) / 2)), sliceH = std::max(1, (int)((cam.height + 1) / 2));
+  const size_t sliceBytes = (size_t)sliceW * sliceH * FP_SLICES * 16;
+  if (cam.half_resolution && slices_.bytes < sliceBytes && !alloc(slices_, sliceBytes, false)) return FP_ENOMEM;
   FpRender R;
   std::memset(&R, 0, sizeof(R));
   std::memcpy(R.ivp, cam.inverse_view_projection, sizeof(R.ivp));
@@ -215,6 +228,10 @@ int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* im
     R.boxHi[a] = renderHi_[a];
   }
   R.hasBox = renderBox_ && steps_ > 0 ? 1 : 0;
+  R.depth = depth;
+  R.slices = cam.half_resolution ? (float*)slices_.ptr : nullptr;
+  R.sliceW = sliceW;
+  R.sliceH = sliceH;
   R.renderField = (float*)renderField_.ptr;
   R.renderSmoke = (float*)renderSmoke_.ptr;
   R.lighting = (float*)lighting_.ptr;

@@ -197,7 +197,7 @@ class fp_stats(C.Structure):
 
 class fp_camera(C.Structure):
     _fields_ = [("inverse_view_projection", C.c_float * 16), ("width", C.c_uint32), ("height", C.c_uint32),
-                ("time", C.c_float)]
+                ("time", C.c_float), ("scene_depth", C.POINTER(C.c_float)), ("half_resolution", C.c_uint32)]
 
 
 class fp_render_settings(C.Structure):

@@ -157,6 +157,7 @@ class SimulationBatch:
             raise FireProError(rc, self.lib.fp_last_error(None).decode())
         self.h = h
         self.cells = brick_size ** 3
+        self._divisors = {}  # per simulation: its velocity divisor (velocity-lattice field sizes)
         self._frames = None
 
     def _check(self, rc: int):
@@ -177,6 +178,7 @@ class SimulationBatch:
     def add(self, grid: abi.fp_grid) -> int:
         out = C.c_uint32()
         self._check(self.lib.fp_batch_add(self.h, C.byref(grid), C.byref(out)))
+        self._divisors[out.value] = max(1, grid.velocity_divisor)
         return out.value
 
     def remove(self, sim: int):
@@ -219,7 +221,8 @@ class SimulationBatch:
     def field(self, sim: int, fid: int) -> np.ndarray:
         s = self.stats(sim)
         ch = abi.FIELD_CHANNELS[fid]
-        out = np.empty((s.pool_slots, ch, self.cells), np.float32)
+        cells = self.cells // self._divisors.get(sim, 1) ** 3 if fid in abi.VELOCITY_FIELDS else self.cells
+        out = np.empty((s.pool_slots, ch, cells), np.float32)
         self._check(self.lib.fp_batch_read_field(self.h, sim, fid, out.ctypes.data_as(C.POINTER(C.c_float)),
                                                  out.nbytes))
         return out
