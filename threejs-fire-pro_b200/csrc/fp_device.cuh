@@ -162,8 +162,8 @@ FP_DEV float sampleCells(const SimParams& P, const Home& H, const float* pool, i
 // velocityCellAverage (fluid-sampling.wgsl:268-285): the mean of the field cells under velocity
 // cell (x,y,z) when the velocity divisor d is above 1, through the field view F: a trilinear
 // sample on the shared corner of a 2x2x2 block of field cells is that block's mean.
-FP_DEV float fieldAverage(const SimParams& F, const Home& H, const float* pool, int ch, int c, int x, int y, int z,
-                          bool half) {
+static __device__ __noinline__ float fieldAverage(const SimParams& F, const Home& H, const float* pool, int ch, int c, int x,
+                                           int y, int z, bool half) {
   const int d = F.velDiv, blocks = d >> 1;
   float sum = 0.f;
   for (int k = 0; k < blocks; k++)
@@ -219,14 +219,23 @@ FP_DEV bool solidFine(const SimParams& P, const Home& H, int x, int y, int z) {
   int bit = (((z & m) << fs | (y & m)) << fs) | (x & m);
   return ((P.solids[(size_t)s * P.W + (bit >> 5)] >> (bit & 31)) & 1u) != 0u;
 }
+// The same on a coarser lattice of s field cells a side (solidSpan): the field cell under its
+// centre. Out of line: only the velocity view of a divided lattice calls it.
+static __device__ __noinline__ bool solidScaled(const SimParams& P, const Home& H, int x, int y, int z) {
+  const int s = P.solidSpan, o = s >> 1;
+  return solidFine(P, H, x * s + o, y * s + o, z * s + o);
+}
 // solidAt at the centre of cell (x,y,z) of this lattice: ((x + .5) s h) / h + .25 floors to
 // field cell x s + s/2 (s = solidSpan; x itself on the field lattice).
 FP_DEV bool solidCell(const SimParams& P, const Home& H, int x, int y, int z) {
-  if (P.solidSpan > 1) {
-    const int s = P.solidSpan, o = s >> 1;
-    return solidFine(P, H, x * s + o, y * s + o, z * s + o);
-  }
-  return solidFine(P, H, x, y, z);
+  if (P.solidSpan > 1) return solidScaled(P, H, x, y, z);
+  // this view is the field lattice
+  if (P.ground && y < 0) return true;
+  if (P.colliderCount == 0) return false;
+  int s = brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift);
+  if (s < 0) return false;
+  int bit = localCell(P, x, y, z);
+  return ((P.solids[(size_t)s * P.W + (bit >> 5)] >> (bit & 31)) & 1u) != 0u;
 }
 // fieldCell (solids.wgsl:7-9) and solidAt (:33-35).
 FP_DEV bool solidAt(const SimParams& P, const Home& H, float wx, float wy, float wz) {

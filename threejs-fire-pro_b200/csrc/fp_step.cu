@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(THREADS, FP_TRANSPORT_CTAS) k_correct(FpBatch 
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_correct<STAGED>(P.vview, i);  // the velocity lattice
+    brick_correct<STAGED>(STAGED ? &P : P.vview, i);  // the velocity lattice (staged: the only one)
   }
 }
 
@@ -702,7 +702,7 @@ __global__ void __launch_bounds__(THREADS) k_curl(FpBatch bt) {
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_curl<STAGED>(P.vview, i);  // the velocity lattice
+    brick_curl<STAGED>(STAGED ? &P : P.vview, i);  // the velocity lattice (staged: the only one)
   }
 }
 
@@ -787,6 +787,7 @@ FP_DEV float3 externalForces(const SimParams& P, const Home& H, int tile, int x,
 // cellForce / centerForce (fluid-forces.wgsl:79-118).
 // The curl is read over the force region and a one-cell rim (Gc, Fc), the evolved scalars
 // over the force region (Gs, Fs): staged or through the directory.
+template <bool ONE>
 FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage& Gc, const Field& Fc, const Stage& Gs,
                         const Field& Fs, int tile, int x, int y, int z) {
   if (brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift) < 0) return make_float3(0.f, 0.f, 0.f);
@@ -795,7 +796,7 @@ FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage& Gc, cons
   // The evolved scalars of this step (the reference swaps field and corrected first); with a
   // velocity divisor d > 1 their mean over the velocity cell (velocityCellAverage).
   float heat, density;
-  if (P.velDiv == 1) {
+  if (ONE || P.velDiv == 1) {
     heat = nearCell(P, H, Gs, Fs, 1, x, y, z);
     density = nearCell(P, H, Gs, Fs, 0, x, y, z);
   } else {
@@ -807,9 +808,9 @@ FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage& Gc, cons
   // else the mean of its 2x2x2 blocks of smoke cells.
   if (P.smokeDiv > 1) {
     const bool sh = P.scalarHalf != 0;
-    const int ratio = P.velDiv > P.smokeDiv ? P.velDiv / P.smokeDiv : 1;
+    const int ratio = (!ONE && P.velDiv > P.smokeDiv) ? P.velDiv / P.smokeDiv : 1;
     if (ratio == 1) {
-      const float f = (float)P.velDiv / (float)P.smokeDiv;
+      const float f = (ONE ? 1.f : (float)P.velDiv) / (float)P.smokeDiv;
       density = smokeSample(P, H, P.smkN, ((float)x + 0.5f) * f, ((float)y + 0.5f) * f, ((float)z + 0.5f) * f, sh);
     } else {
       density = 0.f;
@@ -818,7 +819,7 @@ FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage& Gc, cons
           for (int q = 0; q < ratio; q += 2)
             density += smokeSample(P, H, P.smkN, (float)(x * ratio + q + 1), (float)(y * ratio + j + 1),
                                    (float)(z * ratio + k + 1), sh);
-      density /= (float)(ratio * ratio * ratio / 8);
+      density /= (float)max(1, (ratio / 2) * (ratio / 2) * (ratio / 2));  // ratio^3 / 8 blocks
     }
   }
   float3 conf = make_float3(0.f, 0.f, 0.f);
@@ -839,6 +840,7 @@ FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage& Gc, cons
 
 // sourceVelocity (fluid-forces.wgsl:122-149).
 // (cx,cy,cz) is the field cell of the face position, the cell after the face on its axis.
+template <bool ONE>
 FP_DEV float sourceVelocity(const SimParams& P, const Home& H, int tile, float value, float fx, float fy, float fz,
                             int comp, int cx, int cy, int cz) {
   float result = value;
@@ -858,7 +860,7 @@ FP_DEV float sourceVelocity(const SimParams& P, const Home& H, int tile, float v
     result = mixf(result, e.vel[comp] + radial, 1.f - expf(-e.response * w * P.dt));
   }
   // Mesh emission's velocity coupling (fluid-forces.wgsl:143-147), on the field lattice.
-  const FpMeshSource* ms = meshSourceAt(P.velDiv == 1 ? P : *P.fview, H, cx, cy, cz);
+  const FpMeshSource* ms = meshSourceAt((ONE || P.velDiv == 1) ? P : *P.fview, H, cx, cy, cz);
   if (ms && ms->motion[3] > 0.f)
     result = mixf(result, ms->motion[comp] / ms->motion[3], 1.f - expf(-ms->motion[3] * P.dt));
   return result;
@@ -883,7 +885,7 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   int tile = (int)(id >> 6);
   // The brick in cubes of SUB cells a side (one cube up to 16^3 bricks, 8 of them in a 32^3
   // brick), each with its centre forces on the cube and one cell beyond its upper faces.
-  const int SUB = STAGED ? 8 : min(P.B, FORCE_SUB), E = SUB + 1, E3 = E * E * E, per = P.B / SUB;
+  const int SUB = STAGED ? 8 : min(P.B, FORCE_SUB), E = SUB + 1, E3 = E * E * E, per = STAGED ? 1 : P.B / SUB;
   float* stage = reinterpret_cast<float*>(forceTile + E3);
   Stage Gc, Gs;
   Gc.S = STAGED ? E + 2 : 0;
@@ -911,7 +913,7 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
     for (int q = threadIdx.x; q < E3; q += blockDim.x) {
       int lx = q % E, ly = (q / E) % E, lz = q / (E * E);
       if ((lx == SUB) + (ly == SUB) + (lz == SUB) >= 2) continue;
-      forceTile[q] = cellForce(P, H, Gc, Fc, Gs, Fs, tile, ox + lx, oy + ly, oz + lz);
+      forceTile[q] = cellForce<STAGED>(P, H, Gc, Fc, Gs, Fs, tile, ox + lx, oy + ly, oz + lz);
     }
     __syncthreads();
     for (int k = threadIdx.x; k < SUB * SUB * SUB; k += blockDim.x) {
@@ -929,9 +931,9 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
         float face[3] = {px, py, pz};
         face[a] += 0.5f * P.h;
         // the face's field cell: (x + 1) d on its axis, x d + d/2 on the others (x + 1, x for d = 1)
-      const int d = P.velDiv, o = d >> 1;
-      out[a] = sourceVelocity(P, H, tile, v, face[0], face[1], face[2], a, a == 0 ? (x + 1) * d : x * d + o,
-                              a == 1 ? (y + 1) * d : y * d + o, a == 2 ? (z + 1) * d : z * d + o);
+        const int d = STAGED ? 1 : P.velDiv, o = d >> 1;
+        out[a] = sourceVelocity<STAGED>(P, H, tile, v, face[0], face[1], face[2], a, a == 0 ? (x + 1) * d : x * d + o,
+                                        a == 1 ? (y + 1) * d : y * d + o, a == 2 ? (z + 1) * d : z * d + o);
       }
       // enforceFaces (fluid-forces.wgsl:15-31)
       // solidAt at a cell centre is solidCell of that cell: centre / h + 0.25 floors to it.
@@ -953,7 +955,7 @@ __global__ void __launch_bounds__(THREADS, 4) k_forces(FpBatch bt) {
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_forces<STAGED>(P.vview, i);  // the velocity lattice
+    brick_forces<STAGED>(STAGED ? &P : P.vview, i);  // the velocity lattice (staged: the only one)
   }
 }
 // Shared memory of the staged force kernel: the (B+1)^3 force tile, the curl over (B+3)^3,
@@ -976,6 +978,8 @@ FP_DEV bool pressureUnknown(const SimParams& P, const Home& H, int x, int y, int
 // computeDivergence (fluid-forces.wgsl:184-203) and the finest level's first Jacobi
 // iterate from zero (initializePressure, pressure.wgsl:485-505), fused: the iterate needs
 // only the cell's own right-hand side.
+// ONE: one lattice (velocity divisor 1) known at compile time.
+template <bool ONE>
 FP_DEV void brick_divergence(const SimParams* __restrict__ Pp, uint32_t i, int pSel) {
   __shared__ int nslot[27];
   const SimParams& P = *Pp;
@@ -991,7 +995,8 @@ FP_DEV void brick_divergence(const SimParams* __restrict__ Pp, uint32_t i, int p
               (P.velF[(slot * 3 + 2) * N + c] - cellAt(P, H, P.velF, 3, 2, x, y, z - 1)) / P.h;
     // The expansion rate is on the field lattice: its mean over the velocity cell
     // (velocityCellAverage, fluid-forces.wgsl:202).
-    const float ex = P.velDiv == 1 ? P.expn[slot * N + c] : fieldAverage(*P.fview, H, P.expn, 1, 0, x, y, z, false);
+    const float ex =
+        (ONE || P.velDiv == 1) ? P.expn[slot * N + c] : fieldAverage(*P.fview, H, P.expn, 1, 0, x, y, z, false);
     float rhs = P.h * P.h * (d - ex);
     P.div[slot * N + c] = rhs;
     uint8_t t = P.topo[0][slot * N + c];
@@ -1005,12 +1010,13 @@ FP_DEV void brick_divergence(const SimParams* __restrict__ Pp, uint32_t i, int p
   }
   __syncthreads();
 }
+template <bool ONE>
 __global__ void __launch_bounds__(THREADS) k_divergence(FpBatch bt, int pSel) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_divergence(P.vview, i, pSel);  // the velocity lattice
+    brick_divergence<ONE>(ONE ? &P : P.vview, i, pSel);  // the velocity lattice
   }
 }
 
@@ -1358,8 +1364,11 @@ void fp_launch_forces(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st
   const size_t side = (size_t)(B < FORCE_SUB ? B : FORCE_SUB) + 1, smem = side * side * side * sizeof(float3);
   k_forces<false><<<sms * 4, THREADS, smem, st>>>(bt);
 }
-void fp_launch_divergence(const FpBatch& bt, int pSel, int sms, cudaStream_t st) {
-  k_divergence<<<sms * 4, THREADS, 0, st>>>(bt, pSel);
+void fp_launch_divergence(const FpBatch& bt, int pSel, int vd, int sms, cudaStream_t st) {
+  if (vd == 1)
+    k_divergence<true><<<sms * 4, THREADS, 0, st>>>(bt, pSel);
+  else
+    k_divergence<false><<<sms * 4, THREADS, 0, st>>>(bt, pSel);
 }
 void fp_launch_project(const FpBatch& bt, int pSel, int sms, cudaStream_t st) {
   k_project<<<sms * 4, THREADS, 0, st>>>(bt, pSel);

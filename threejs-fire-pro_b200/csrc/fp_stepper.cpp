@@ -431,7 +431,7 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   // Cold start every step: the divergence writes the first iterate into p0[1].
   int cur[FP_MAX_LEVELS] = {0};
   phaseBegin(PH_DIVERGENCE);
-  fp_launch_divergence(bt, 1, sms_, stream_);
+  fp_launch_divergence(bt, 1, vd_, sms_, stream_);
   launches++;
   phaseEnd(PH_DIVERGENCE, 1);
   cur[0] = 1;
