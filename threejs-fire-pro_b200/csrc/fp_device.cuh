@@ -227,8 +227,10 @@ static __device__ __noinline__ bool solidScaled(const SimParams& P, const Home& 
 }
 // solidAt at the centre of cell (x,y,z) of this lattice: ((x + .5) s h) / h + .25 floors to
 // field cell x s + s/2 (s = solidSpan; x itself on the field lattice).
+// ONE: this view is known at compile time to be the field lattice (velocity divisor 1).
+template <bool ONE = false>
 FP_DEV bool solidCell(const SimParams& P, const Home& H, int x, int y, int z) {
-  if (P.solidSpan > 1) return solidScaled(P, H, x, y, z);
+  if (!ONE && P.solidSpan > 1) return solidScaled(P, H, x, y, z);
   // this view is the field lattice
   if (P.ground && y < 0) return true;
   if (P.colliderCount == 0) return false;

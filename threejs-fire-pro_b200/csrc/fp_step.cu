@@ -392,7 +392,7 @@ FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
     int x, y, z;
     cellOf(P, H, c, x, y, z);
     float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-    bool solid = solidCell(P, H, x, y, z);  // solidAt at the cell centre
+    bool solid = solidCell<STAGED>(P, H, x, y, z);  // solidAt at the cell centre
     float3 orig = make_float3(nearCell(P, H, G, V, 0, x, y, z), nearCell(P, H, G, V, 1, x, y, z),
                               nearCell(P, H, G, V, 2, x, y, z));
 #pragma unroll
@@ -484,7 +484,7 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
     int x, y, z;
     cellOf(P, H, c, x, y, z);
     float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-    bool solid = solidCell(P, H, x, y, z);  // solidAt at the cell centre
+    bool solid = solidCell<STAGED>(P, H, x, y, z);  // solidAt at the cell centre
     float value[4] = {0.f, 0.f, 0.f, 0.f};
     float expansion = 0.f;
     bool injected = false;
@@ -792,7 +792,7 @@ FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage& Gc, cons
                         const Field& Fs, int tile, int x, int y, int z) {
   if (brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift) < 0) return make_float3(0.f, 0.f, 0.f);
   float wx = ((float)x + 0.5f) * P.h, wy = ((float)y + 0.5f) * P.h, wz = ((float)z + 0.5f) * P.h;
-  if (solidCell(P, H, x, y, z)) return make_float3(0.f, 0.f, 0.f);  // solidAt at the centre
+  if (solidCell<ONE>(P, H, x, y, z)) return make_float3(0.f, 0.f, 0.f);  // solidAt at the centre
   // The evolved scalars of this step (the reference swaps field and corrected first); with a
   // velocity divisor d > 1 their mean over the velocity cell (velocityCellAverage).
   float heat, density;
@@ -937,12 +937,12 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
       }
       // enforceFaces (fluid-forces.wgsl:15-31)
       // solidAt at a cell centre is solidCell of that cell: centre / h + 0.25 floors to it.
-      if (solidCell(P, H, x, y, z)) {
+      if (solidCell<STAGED>(P, H, x, y, z)) {
         out[0] = out[1] = out[2] = 0.f;
       } else {
-        if (solidCell(P, H, x + 1, y, z)) out[0] = 0.f;
-        if (solidCell(P, H, x, y + 1, z)) out[1] = 0.f;
-        if (solidCell(P, H, x, y, z + 1)) out[2] = 0.f;
+        if (solidCell<STAGED>(P, H, x + 1, y, z)) out[0] = 0.f;
+        if (solidCell<STAGED>(P, H, x, y + 1, z)) out[1] = 0.f;
+        if (solidCell<STAGED>(P, H, x, y, z + 1)) out[2] = 0.f;
       }
       for (int a = 0; a < 3; a++) P.velF[(slot * 3 + a) * N + c] = out[a];
     }
@@ -1021,6 +1021,7 @@ __global__ void __launch_bounds__(THREADS) k_divergence(FpBatch bt, int pSel) {
 }
 
 // project (fluid-forces.wgsl:228-262) into the velocity pool of the next step.
+template <bool ONE>
 FP_DEV void brick_project(const SimParams* __restrict__ Pp, uint32_t i, int pSel) {
   __shared__ int nslot[27];
   const SimParams& P = *Pp;
@@ -1032,14 +1033,14 @@ FP_DEV void brick_project(const SimParams* __restrict__ Pp, uint32_t i, int pSel
     int x, y, z;
     cellOf(P, H, c, x, y, z);
     float res[3] = {0.f, 0.f, 0.f};
-    if (!solidCell(P, H, x, y, z)) {  // solidAt at the cell centre
+    if (!solidCell<ONE>(P, H, x, y, z)) {  // solidAt at the cell centre
       float cp = p[slot * N + c];
       bool pu = pressureUnknown(P, H, x, y, z);
       for (int a = 0; a < 3; a++) {
         int n[3] = {x, y, z};
         n[a] += 1;
         float v = P.velF[(slot * 3 + a) * N + c];
-        if (solidCell(P, H, n[0], n[1], n[2])) {
+        if (solidCell<ONE>(P, H, n[0], n[1], n[2])) {
           res[a] = 0.f;
         } else if (!pu && !pressureUnknown(P, H, n[0], n[1], n[2])) {
           res[a] = 0.f;
@@ -1053,12 +1054,13 @@ FP_DEV void brick_project(const SimParams* __restrict__ Pp, uint32_t i, int pSel
   }
   __syncthreads();
 }
+template <bool ONE>
 __global__ void __launch_bounds__(THREADS) k_project(FpBatch bt, int pSel) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_project(P.vview, i, pSel);  // the velocity lattice
+    brick_project<ONE>(ONE ? &P : P.vview, i, pSel);  // the velocity lattice
   }
 }
 
@@ -1370,8 +1372,11 @@ void fp_launch_divergence(const FpBatch& bt, int pSel, int vd, int sms, cudaStre
   else
     k_divergence<false><<<sms * 4, THREADS, 0, st>>>(bt, pSel);
 }
-void fp_launch_project(const FpBatch& bt, int pSel, int sms, cudaStream_t st) {
-  k_project<<<sms * 4, THREADS, 0, st>>>(bt, pSel);
+void fp_launch_project(const FpBatch& bt, int pSel, int vd, int sms, cudaStream_t st) {
+  if (vd == 1)
+    k_project<true><<<sms * 4, THREADS, 0, st>>>(bt, pSel);
+  else
+    k_project<false><<<sms * 4, THREADS, 0, st>>>(bt, pSel);
 }
 void fp_launch_noise(float4* noise, cudaStream_t st) { k_noise<<<64 * 64 * 64 / 256, 256, 0, st>>>(noise); }
 void fp_launch_post_divergence(const FpBatch& bt, int sms, cudaStream_t st) {

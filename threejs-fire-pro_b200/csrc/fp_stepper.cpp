@@ -454,7 +454,7 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   phaseEnd(PH_MULTIGRID, (int)mg);
   latest = cur[0];
   phaseBegin(PH_PROJECT);
-  fp_launch_project(bt, latest, sms_, stream_);
+  fp_launch_project(bt, latest, vd_, sms_, stream_);
   launches++;
   if (measure) {
     fp_launch_post_divergence(bt, sms_, stream_);
