@@ -309,8 +309,8 @@ int fp_sim_render_device(fp_sim* sim, const fp_camera* camera, const fp_render_s
  * anchor counts a quarter; ties go to the first), the luminance of their emission, its
  * luminance-weighted offset from the anchor and its RGB. `anchors` holds `anchor_count`
  * world positions (3 floats each); `sums` receives 8 floats per anchor (luminance, offset
- * xyz, RGB, 0), the totals SceneLights.apply turns into lights. Synchronous. Coarse smoke
- * (smoke_divisor > 1) is FP_EUNSUPPORTED, as for the render. */
+ * xyz, RGB, 0), the totals SceneLights.apply turns into lights. Synchronous. With coarse smoke a
+ * sample's density is the coarse grid's, trilinear at the cell's centre. */
 int fp_sim_collect_lights(fp_sim* sim, const fp_render_settings* settings, const float* anchors,
                           uint32_t anchor_count, float* sums);
 /* Wait for the simulation's queued work. */

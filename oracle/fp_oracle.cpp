@@ -1310,6 +1310,25 @@ struct Sim {
         int l[3] = {(lane & 3) * stride + stride / 2, ((lane >> 2) & 3) * stride + stride / 2, (lane >> 4) * stride + stride / 2};
         size_t o = (size_t)slot * 4 * N + (size_t)((l[2] * B + l[1]) * B + l[0]);
         std::array<R, 4> f = {fld[o], fld[o + N], fld[o + 2 * N], fld[o + 3 * N]};
+        if (smokeDiv > 1) {  // the coarse density at the cell's centre; taps before the brick read zero
+          R q[3], fr[3], v = 0;
+          int c0[3];
+          for (int a = 0; a < 3; a++) {
+            q[a] = (R(l[a]) + R(.5)) / R(smokeDiv) - R(.5);
+            c0[a] = (int)std::floor(q[a]);
+            fr[a] = q[a] - R(c0[a]);
+          }
+          for (int k = 0; k < 8; k++) {
+            int d[3] = {k & 1, (k >> 1) & 1, k >> 2}, cl[3] = {c0[0] + d[0], c0[1] + d[1], c0[2] + d[2]};
+            if (cl[0] < 0 || cl[1] < 0 || cl[2] < 0) continue;
+            int s = brickSlot(b[0] + (cl[0] >> sshift), b[1] + (cl[1] >> sshift), b[2] + (cl[2] >> sshift));
+            if (s < 0) continue;
+            int m = SB - 1;
+            R w = (d[0] ? fr[0] : 1 - fr[0]) * (d[1] ? fr[1] : 1 - fr[1]) * (d[2] ? fr[2] : 1 - fr[2]);
+            v += smk[(size_t)s * SN + ((cl[2] & m) * SB + (cl[1] & m)) * SB + (cl[0] & m)] * w;
+          }
+          f[0] = v;
+        }
         std::array<R, 3> rgb = emissionOf(G, f);
         double lum = .2126 * (double)rgb[0] + .7152 * (double)rgb[1] + .0722 * (double)rgb[2];
         acc[0] += lum;

@@ -184,18 +184,6 @@ def test_mesh_force_targets(brick):
     check(reports, min_active=8 if brick == 16 else 30)
 
 
-def test_coarse_smoke_lights_unsupported():
-    sc = scenes.ForceScene()
-    g = sc.grid(budget=2 ** 20)
-    g.smoke_divisor = 2
-    sim = FluidSimulation(g)
-    sim.step(sc.frame(0).frame)
-    from firepro import render
-    with pytest.raises(FireProError):
-        sim.collect_lights(render.default_settings(), [[0.0, 0.3, 0.0]])
-    sim.dispose()
-
-
 def test_cutoff_zero_keeps_tails():
     check(run(scenes.SinglePlume(), 36, budget=2 ** 19, cutoff=0.0))
 

@@ -103,12 +103,16 @@ def test_render_validation():
     sim.dispose()
 
 
-def test_scene_lights_parity():
+@pytest.mark.parametrize("smoke_divisor", [1, 2])
+def test_scene_lights_parity(smoke_divisor):
     """collectLights (scene-lights.wgsl:37-106) against the oracle on the same state: each
     anchor's luminance, luminance-weighted offset and RGB sums; the totals over anchors do not
-    depend on where the anchors are; `measure_lights` places each light inside the flames."""
+    depend on where the anchors are; `measure_lights` places each light inside the flames. With
+    coarse smoke each sample's density comes from the coarse grid."""
     st = render.default_settings()
     sc = scenes.ForceScene()
+    grid = sc.grid(budget=2 ** 20)
+    grid.smoke_divisor = smoke_divisor
     anchors = np.array([[0.05, 0.25, 0.0], [-0.5, 0.3, 0.3], [0.6, 0.2, -0.4], [0.0, 0.5, 0.0]], np.float32)
     moved = np.array([[3.0, 0.0, 3.0], [-0.1, 0.9, 0.2]], np.float32)
     out = {}
@@ -118,7 +122,7 @@ def test_scene_lights_parity():
         out["gpu_moved"], out["orc_moved"] = gpu.collect_lights(st, moved), orc.collect_lights(st, moved)
         out["none"] = gpu.collect_lights(st, np.zeros((0, 3), np.float32))
 
-    parity.lockstep(sc, 10, lambda g: FluidSimulation(g), budget=2 ** 20, after=after)
+    parity.lockstep(sc, 10, lambda g: FluidSimulation(g), budget=2 ** 20, grid=grid, after=after)
     gpu, orc = out["gpu"].astype(np.float64), out["orc"]
     assert orc[:, 0].sum() > 0, "the flames should emit"
     assert out["none"].shape == (0, 8)

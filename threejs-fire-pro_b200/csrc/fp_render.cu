@@ -716,8 +716,36 @@ __global__ void __launch_bounds__(64) k_collect_lights(const SimParams* __restri
     const int lx = (lane & 3) * stride + stride / 2, ly = ((lane >> 2) & 3) * stride + stride / 2,
               lz = (lane >> 4) * stride + stride / 2;
     const size_t o = (size_t)slot * 4 * P.N + (size_t)((lz * P.B + ly) * P.B + lx);
-    const float4 f = make_float4(ldHalf(P.fld, o, half), ldHalf(P.fld, o + P.N, half), ldHalf(P.fld, o + 2 * P.N, half),
-                                 ldHalf(P.fld, o + 3 * P.N, half));
+    float4 f = make_float4(ldHalf(P.fld, o, half), ldHalf(P.fld, o + P.N, half), ldHalf(P.fld, o + 2 * P.N, half),
+                           ldHalf(P.fld, o + 3 * P.N, half));
+    if (P.smokeDiv > 1) {
+      // The coarse density sampled trilinearly at the cell's centre on the smoke lattice
+      // (scene-lights.wgsl:59-65): a tap past the brick reads the +1 neighbour (the slot's
+      // apron), zero without a slot; taps before the brick read zero.
+      const int sh = P.smokeShift, S = 1 << sh, m = S - 1;
+      const float r = 1.f / (float)P.smokeDiv;
+      const float q[3] = {((float)lx + .5f) * r - .5f, ((float)ly + .5f) * r - .5f, ((float)lz + .5f) * r - .5f};
+      int c0[3];
+      float fr[3];
+      for (int a = 0; a < 3; a++) {
+        float g = floorf(q[a]);
+        c0[a] = (int)g;
+        fr[a] = q[a] - g;
+      }
+      float v = 0.f;
+      for (int k = 0; k < 8; k++) {
+        int d[3] = {k & 1, (k >> 1) & 1, k >> 2};
+        int cl[3] = {c0[0] + d[0], c0[1] + d[1], c0[2] + d[2]};
+        if (cl[0] < 0 || cl[1] < 0 || cl[2] < 0) continue;
+        int nb[3] = {b[0] + (cl[0] >> sh), b[1] + (cl[1] >> sh), b[2] + (cl[2] >> sh)};
+        int t = hashFind(P, nb[0] >> 2, nb[1] >> 2, nb[2] >> 2);
+        int s = t < 0 ? -1 : entryPage(P.entries[t * 64 + (((nb[2] & 3) * 4 + (nb[1] & 3)) * 4 + (nb[0] & 3))]);
+        if (s < 0) continue;
+        float w = (d[0] ? fr[0] : 1.f - fr[0]) * (d[1] ? fr[1] : 1.f - fr[1]) * (d[2] ? fr[2] : 1.f - fr[2]);
+        v += ldHalf(P.smk, (size_t)s * P.smokeCells + ((((cl[2] & m) << sh) | (cl[1] & m)) << sh | (cl[0] & m)), half) * w;
+      }
+      f.x = v;
+    }
     const float3 rgb = emissionOf(R, f);
     const float luminance = rgb.x * .2126f + rgb.y * .7152f + rgb.z * .0722f;
     const float cx = ((float)b[0] + .5f) * side, cy = ((float)b[1] + .5f) * side, cz = ((float)b[2] + .5f) * side;

@@ -251,7 +251,6 @@ int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* im
 
 int Engine::collectLights(const fp_render_settings& rs, const float* anchors, uint32_t count, float* sums) {
   if (count > 65536) return fail(FP_EINVAL, "scene lights: at most 65536 anchors.");
-  if (smokeDiv_ > 1) return fail(FP_EUNSUPPORTED, "scene lights: smoke on a coarse grid is not read by this build.");
   int rc = consume();
   if (rc) return rc;
   if (count == 0) return FP_OK;
