@@ -42,6 +42,9 @@ BRICK_VOXELS = 512
 BUDGET = 2 ** 24  # voxels: 32768 slots, ~3.2 GB of pools
 TARGET_BRICKS = 4096
 MAX_GROW_STEPS = 600
+# Steps the large scene grows (untimed) before the warm-up and the timed steps, in every arm:
+# past the burst, to about 4.1k computing bricks, then ~4.9k over the timed steps.
+GROW_STEPS = 180
 
 # Algorithmic bytes per voxel per phase in FP32: every live field read once and written once
 # per kernel that must touch it (velocity 12 B, scalars 16 B, expansion/divergence/pressure
@@ -59,6 +62,11 @@ BYTES_PER_VOXEL = {
     "project": 28.0,
 }
 STEP_BYTES = sum(BYTES_PER_VOXEL.values())
+
+
+WORKLOAD = ("large_scene (seed 1): 3 seeded sphere/box emitters, burst at step 30, turbulence 2 m/s, sphere+box "
+            "colliders; 8^3 bricks, 2.5 cm voxels, budget 2^24 voxels; grown 180 steps + W warm-up, then K timed; "
+            "plain FP32 storage; 1 cold-started V-cycle (reference schedule)")
 
 
 def measured_peaks():
@@ -164,11 +172,11 @@ def sum_over_ranks(x: float, world: int) -> float:
 
 def cpu_sample(scene_cls, max_seconds: float, max_steps: int, threads: int, warmup: int = 1):
     """The FP32 oracle on the host cores: voxel-steps/s over a bounded run of the scene, after
-    `warmup` untimed steps (the first allocates the starting bricks)."""
+    `warmup` untimed steps (the GPU arm's growth and warm-up, so both time the same state)."""
     from oracle import fp_oracle
 
     fp_oracle.set_threads(threads)
-    sc = scene_cls()
+    sc = scene_cls(seed=1)
     o = fp_oracle.OracleSim(sc.grid(budget=BUDGET), real=1)
     o.set_runtime(0.05, BUDGET, True)
     warmup = max(1, warmup)
@@ -200,17 +208,21 @@ def run_reference(args, rank, world):
     from firepro import scenes
 
     threads = os.cpu_count() or 1
-    value, steps, bricks, step_ms = cpu_sample(scenes.LargeScene, 60.0, args.steps, threads, warmup=args.warmup)
+    # The GPU arm's workload: the same scene grown the same GROW_STEPS steps and W warm-up
+    # steps untimed, then K timed steps (capped at 120 s of CPU time).
+    untimed = GROW_STEPS + args.warmup
+    value, steps, bricks, step_ms = cpu_sample(scenes.LargeScene, 120.0, args.steps, threads, warmup=untimed)
     p50, p99 = percentiles(step_ms)
     line = {
         "impl": "reference", "metric": "voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": args.gpus,
-        "steps": steps, "warmup": max(1, args.warmup), "ms_per_step": statistics.mean(step_ms) if step_ms else None,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": statistics.mean(step_ms) if step_ms else None,
         "p50_ms": p50, "p99_ms": p99, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic", "config": {"workload": "large_scene (seed 1), steps 1.. from the start",
-                                                        "mean_active_bricks": bricks},
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grown_steps": GROW_STEPS, "mean_active_bricks": bricks},
         "cpu_baseline": {"value": value, "unit": "voxel-steps/s", "cores": threads, "kind": "port",
-                         "sample": f"oracle FP32 restatement, {steps} timed steps of the large scene after "
-                                   f"{max(1, args.warmup)} untimed (mean {bricks:.0f} bricks), capped at 60 s"},
+                         "sample": f"oracle FP32 restatement of the step on {threads} threads: the large scene grown "
+                                   f"{GROW_STEPS} + {args.warmup} steps untimed, then {steps} timed steps "
+                                   f"(mean {bricks:.0f} bricks), capped at 120 s"},
         "e2e": {"value": value, "unit": "voxel-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -418,13 +430,11 @@ def run_ours(args, rank, world, local):
     sc = scenes.SCENES[args.scene](seed=1)
     sim = FluidSimulation(sc.grid(budget=BUDGET), device=local)
     sim.set_runtime(0.05, BUDGET, True)
-    # Grow the scene to the target size (untimed).
+    # Grow the scene (untimed): GROW_STEPS steps, as the reference arm does.
     step = 0
-    while step < MAX_GROW_STEPS:
+    while step < GROW_STEPS:
         sim.step(sc.frame(step).frame)
         step += 1
-        if step % 25 == 0 and sim.stats().active_bricks >= TARGET_BRICKS:
-            break
     for _ in range(args.warmup):
         sim.step(sc.frame(step).frame)
         step += 1
@@ -523,10 +533,8 @@ def run_ours(args, rank, world, local):
         "metric": "voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "p50_ms": p50, "p99_ms": p99,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "large_scene: 3 seeded sphere/box emitters, burst at step 30, turbulence 2 m/s, "
-                               "sphere+box colliders; 8^3 bricks, 2.5 cm voxels; plain FP32 storage; "
-                               "1 cold-started V-cycle (reference schedule)",
-                   "mean_active_bricks": sum(actives) / len(actives), "grown_steps": step - 3 * args.steps,
+        "config": {"workload": WORKLOAD,
+                   "mean_active_bricks": sum(actives) / len(actives), "grown_steps": GROW_STEPS,
                    "live_tiles": int(st.tiles), "tile_capacity": int(st.tile_capacity),
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "working set > L2: pools of ~4k bricks x 97 KB"},
@@ -543,10 +551,12 @@ def run_ours(args, rank, world, local):
                          "precision": precision_form(local)}
     if world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        cv, csteps, cbricks, _ = cpu_sample(scenes.LargeScene, 20.0, 400, threads)
+        untimed = GROW_STEPS + args.warmup
+        cv, csteps, cbricks, _ = cpu_sample(scenes.LargeScene, 20.0, args.steps, threads, warmup=untimed)
         line["cpu_baseline"] = {"value": cv, "unit": "voxel-steps/s", "cores": threads, "kind": "port",
-                                "sample": f"oracle FP32 restatement, {csteps} steps of the large scene from step 1 "
-                                          f"(mean {cbricks:.0f} bricks), capped at 20 s"}
+                                "sample": f"oracle FP32 restatement on {threads} threads: the large scene grown "
+                                          f"{GROW_STEPS} + {args.warmup} steps untimed (as this arm), then {csteps} "
+                                          f"timed steps (mean {cbricks:.0f} bricks), capped at 20 s"}
     print(json.dumps(line), flush=True)
 
 

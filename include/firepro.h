@@ -3,8 +3,8 @@
  *
  * This is the drop-in boundary for Fire Pro's engine layer: one call per method of the
  * reference's `FluidSimulation` class (src/engine/FluidSimulation.ts), with plain structs
- * and pointers in place of WebGPU resources and JS objects. A Node-API addon (see
- * INTEGRATION.md) or Python ctypes binds these symbols one to one.
+ * and pointers in place of WebGPU resources and JS objects. A Node-API addon or Python
+ * ctypes binds these symbols one to one.
  *
  * Conventions
  *  - Every function returns an `int` status (FP_OK or a negative FP_E* code) and never
@@ -57,8 +57,8 @@ extern "C" {
  * as `FluidSimulation`'s constructor does (FluidSimulation.ts:359-379). */
 typedef struct fp_grid {
   float voxel_size;        /* meters, [0.0001, 16] */
-  int32_t velocity_divisor;/* 1 (the reference also allows 2 and 4) */
-  int32_t brick_size;      /* fine cells per brick side: 8 or 16 */
+  int32_t velocity_divisor;/* 1, 2 or 4: velocity cells are that many fine cells a side */
+  int32_t brick_size;      /* fine cells per brick side: 8, 16 or 32 */
   int32_t smoke_divisor;   /* 1, 2 or 4: smoke density on a grid that many times coarser */
   int32_t scalar_maccormack; /* bounded MacCormack scalar transport: 0 or 1 */
   int32_t precision;       /* FP_PRECISION_* */
@@ -90,7 +90,8 @@ typedef struct fp_fuel {
 } fp_fuel;
 
 /* `SimulationSource` (types.ts:246-268). `id` replaces the string id: a source whose id
- * was absent last step is new. Mesh sources carry no samples in this ABI version. */
+ * was absent last step is new. A mesh source's surface samples arrive already splatted to
+ * lattice cells, as the frame's `mesh_sources` records. */
 typedef struct fp_source {
   uint64_t id;
   int32_t shape;            /* FP_SHAPE_* */
@@ -269,10 +270,11 @@ int fp_sim_set_solver(fp_sim* sim, int vcycles, float tolerance);
 /* The latest step's solve (waits for the step's work). */
 int fp_sim_read_solver(fp_sim* sim, fp_solver_stats* out);
 /* ---- Volume rendering: a headless restatement of the renderer's compute passes and camera
- * march (lighting.wgsl smoothSmoke/buildOccupancy/buildLighting, volume-march.wgsl
- * fireProMarch, scene-volume.wgsl fireProSceneVolume with no scene depth and half resolution
- * off, fire-emission.wgsl, volume-reconstruction.wgsl, blackbody.ts). The image is linear
- * radiance and opacity, row-major from the top-left pixel, four floats a pixel. */
+ * march (lighting.wgsl smoothSmoke/buildOccupancy/buildLighting, volume-slices.wgsl
+ * buildSlices, volume-march.wgsl fireProMarch, scene-volume.wgsl fireProSceneVolume with an
+ * optional scene depth buffer and half-resolution slices, fire-emission.wgsl,
+ * volume-reconstruction.wgsl, blackbody.ts). The image is linear radiance and opacity,
+ * row-major from the top-left pixel, four floats a pixel. */
 typedef struct fp_camera {
   float inverse_view_projection[16]; /* clip to world, column-major (the WGSL mat4x4f's columns) */
   uint32_t width, height;            /* pixels */
@@ -382,7 +384,7 @@ int fp_grid_reserved_tiles(const fp_grid* grid, uint32_t* tiles);
 typedef struct fp_server fp_server;
 typedef struct {
   int device;
-  int brick_size;          /* 8 or 16, the same for every session */
+  int brick_size;          /* 8, 16 or 32, the same for every session */
   uint64_t memory_budget;  /* admission: the sessions' device bytes (fp_grid_memory_bytes) */
   uint32_t max_sessions;   /* live sessions at most */
 } fp_server_config;
@@ -416,12 +418,16 @@ int fp_server_create(const fp_server_config* config, fp_server** out);
 int fp_server_destroy(fp_server* server);
 /* Open a session of `grid` with the runtime fields of fp_sim_set_runtime; it waits for
  * admission (FP_SESSION_WAITING) unless memory and a slot are free now. FP_ELIMIT when the
- * grid alone exceeds the memory budget. */
+ * grid alone exceeds the memory budget. Every session of a server shares the velocity
+ * divisor of the first one opened: another divisor is FP_EINVAL. */
 int fp_server_open(fp_server* server, const fp_grid* grid, float cutoff, int ground, uint32_t* session);
 /* The session leaves once its queued steps have run; its memory then returns to the budget. */
 int fp_server_close(fp_server* server, uint32_t session);
 int fp_server_session_state(fp_server* server, uint32_t session, int* state);
-/* Queue one step of `session` (frame arrays are copied; dt as fp_sim_step). */
+/* Queue one step of `session` (the frame and every array it points into are copied; dt as
+ * fp_sim_step). The frame's full check (flame ramps, mesh arrays) runs when its launch is
+ * built: a frame that fails it completes with that status alone, the other sessions' steps of
+ * the launch run. */
 int fp_server_submit(fp_server* server, uint32_t session, const fp_frame* frame, float dt, uint64_t* ticket);
 /* Completed steps, oldest first: up to `capacity` into `out`, `*count` written. Waits up to
  * `wait_ms` for the first one when none is ready. */
@@ -450,7 +456,9 @@ int fp_server_read_field(fp_server* server, uint32_t session, int field, float* 
  * n may be at most FP_COMPACT_MAX_IDS; larger n returns FP_ELIMIT and launches nothing.
  * Scratch is a 64 KB array inside the library that every GPU loading it holds until exit.
  * The first call on a device looks up that array's address with the device current; make
- * that first call before any stream capture. All calls share the array, so calls whose
+ * that first call before any stream capture. The address is kept for the process: after a
+ * cudaDeviceReset (or any teardown of the device's primary context) it is stale, so do not
+ * call this entry point again in that process. All calls share the array, so calls whose
  * work overlaps on the GPU race; order them on one stream. */
 int fp_compact_ids_noalloc(const uint32_t* flags, uint32_t n, uint32_t* ids, uint32_t* count, void* stream);
 

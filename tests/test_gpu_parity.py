@@ -25,6 +25,7 @@ def check(reports, tol=TOL, min_active=1):
     may flip the same way (parity.field_within): a field may exceed `tol` only through a few
     isolated cells, and then by at most FLIP_BOUND times."""
     worst = {}
+    trimmed = {}  # field -> steps that passed only through the flip-cell trim
     for step, tables, fields, n in reports:
         for k, v in tables.items():
             if k == "activity":
@@ -38,7 +39,17 @@ def check(reports, tol=TOL, min_active=1):
             assert parity.field_within(fields, k, tol), (
                 f"step {step}: {k} relative L2 {v:.3e} ({fields[k + '@trim']:.3e} without "
                 f"{parity.flip_cells(n)} flip cells) > {tol}")
+            if v > tol:
+                trimmed.setdefault(k, []).append(step)
     assert max(r[3] for r in reports) >= min_active
+    # How often the trim was needed, per field: printed with the test's output, and bounded so
+    # that a slow drift cannot pass through it step after step.
+    steps = len(reports)
+    print(f"parity: {steps} steps, up to {max(r[3] for r in reports)} bricks; steps passing only without "
+          f"flip cells: " + (", ".join(f"{k} {len(v)} ({v[:6]})" for k, v in sorted(trimmed.items())) or "none"))
+    for k, v in trimmed.items():
+        assert len(v) <= max(2, steps // 10), f"{k} needed the flip-cell trim in {len(v)} of {steps} steps: {v}"
+    worst["trimmed_steps"] = {k: len(v) for k, v in trimmed.items()}
     return worst
 
 
@@ -47,7 +58,16 @@ def run(scene, steps, **kw):
 
 
 def test_plume_parity():
-    check(run(scenes.SinglePlume(), 40, budget=2 ** 19), min_active=216)
+    """The single plume's 120 steps, every one in lockstep."""
+    check(run(scenes.SinglePlume(), 120, budget=2 ** 19), min_active=216)
+
+
+def test_large_scene_at_bench_state():
+    """The large scene where the benchmark times it: the bench's budget (2^24 voxels, 32768
+    slots), stepped in lockstep from the start through the burst and the growth to more than
+    4096 computing bricks (the bench grows 180 steps, then times the steps after)."""
+    reports = run(scenes.LargeScene(), 186, budget=2 ** 24)
+    check(reports, min_active=4096)
 
 
 def test_force_scene_parity():

@@ -132,3 +132,93 @@ def test_session_limit_and_statistics():
     srv.close(ids[0])
     wait_state(srv, ids[2], abi.FP_SESSION_LIVE)
     srv.dispose()
+
+
+def _plain_fields(scene, grid, frames):
+    sim = FluidSimulation(grid)
+    sim.set_runtime(0.05, grid.voxel_budget, True)
+    for fd in frames:
+        sim.step(fd.frame)
+    out = {f: sim.field(f) for f in FIELDS}
+    sim.dispose()
+    return out
+
+
+def test_server_copies_mesh_frames():
+    """Mesh emission records, mesh target cells and their ranges are copied at submission: the
+    caller's arrays are overwritten right after each submit, and the served fields still equal
+    fp_sim_step's on the intact frames."""
+    import ctypes as C
+
+    scs = [scenes.MeshEmitterScene(), scenes.MeshTargetScene()]
+    steps = 8
+    srv = FireServer(8 * GB)
+    ids = [srv.open(sc.grid(budget=2 ** 20)) for sc in scs]
+    for s in range(steps):
+        for i, sc in zip(ids, scs):
+            fd = sc.frame(s)
+            srv.submit(i, fd.frame)
+            for a in fd.keep:  # the caller reuses its memory
+                C.memset(C.addressof(a), 0xFF, C.sizeof(a))
+    srv.drain()
+    done = []
+    while True:
+        got = srv.poll()
+        if not got:
+            break
+        done += got
+    assert len(done) == 2 * steps and all(c.status == abi.FP_OK for c in done)
+    served = [{f: srv.field(i, f) for f in FIELDS} for i in ids]
+    srv.dispose()
+    for sc, got in zip(scs, served):
+        plain = _plain_fields(sc, sc.grid(budget=2 ** 20), [sc.frame(s) for s in range(steps)])
+        for f in FIELDS:
+            assert np.array_equal(got[f], plain[f]), f"{sc.name} field {f}: served and plain differ"
+
+
+def test_server_isolates_an_invalid_frame():
+    """One session among eight submits a frame whose flame ramp is invalid: that step alone
+    fails, with the reference's message, and the other sessions' fields are bit-identical to
+    stepping each alone (a session that raises mid-batch harms no other)."""
+    ms = [scenes.MemberScene(3, k, max_bricks=256) for k in range(8)]
+    steps, bad_session, bad_step = 6, 3, 2
+    srv = FireServer(16 * GB)
+    ids = [srv.open(m.grid(budget=m.budget)) for m in ms]
+    keep = []
+    for s in range(steps):
+        for k, (i, m) in enumerate(zip(ids, ms)):
+            fd = m.frame(s)
+            if k == bad_session and s == bad_step:
+                fd.frame.combustion.ramps[2].knots[0][0] = 0.1
+            keep.append(fd)
+            srv.submit(i, fd.frame)
+    srv.drain()
+    done = []
+    while True:
+        got = srv.poll()
+        if not got:
+            break
+        done += got
+    failed = [c for c in done if c.status != abi.FP_OK]
+    assert len(failed) == 1 and failed[0].session == ids[bad_session]
+    assert failed[0].status == abi.FP_EINVAL
+    assert "expansion ramp must span lifetime 0–1." in srv.lib.fp_server_last_error(srv.h).decode()
+    assert sum(1 for c in done if c.status == abi.FP_OK) == 8 * steps - 1
+    served = {i: {f: srv.field(i, f) for f in FIELDS} for i in ids}
+    srv.dispose()
+    for k, (i, m) in enumerate(zip(ids, ms)):
+        frames = [m.frame(s) for s in range(steps) if not (k == bad_session and s == bad_step)]
+        plain = _plain_fields(m, m.grid(budget=m.budget), frames)
+        for f in FIELDS:
+            assert np.array_equal(served[i][f], plain[f]), f"session {k} field {f}: served and alone differ"
+
+
+def test_server_refuses_another_velocity_divisor():
+    srv = FireServer(8 * GB)
+    a = scenes.SinglePlume()
+    srv.open(a.grid(budget=2 ** 19))
+    g = a.grid(budget=2 ** 19)
+    g.velocity_divisor = 2
+    with pytest.raises(FireProError, match="velocityDivisor 2 differs"):
+        srv.open(g)
+    srv.dispose()

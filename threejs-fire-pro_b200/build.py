@@ -8,6 +8,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
@@ -38,7 +39,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     LIB.parent.mkdir(exist_ok=True)
     newest_header = max((h.stat().st_mtime for h in _headers()), default=0)
-    objects = []
+    objects, commands = [], []
     for src in _sources():
         obj = BUILD / (src.name + ".o")
         objects.append(obj)
@@ -49,7 +50,11 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
             cmd.insert(1, "-Xptxas=-v")
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        commands.append(cmd)
+    # The sources compile independently: one nvcc per source at a time, as many as there are cores.
+    with ThreadPoolExecutor(max_workers=max(1, min(len(commands), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(subprocess.run, cmd, check=True) for cmd in commands]:
+            f.result()
     if not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objects):
         cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objects), "-lcudart"]
         if verbose:

@@ -27,25 +27,38 @@
 
 namespace {
 
-// A frame and the arrays it points into, owned by the request.
+// A frame and every array it points into, owned by the request: the scheduler reads them
+// after fp_server_submit has returned, when the caller's arrays may be gone.
 struct FrameCopy {
   fp_frame frame;
   std::vector<fp_source> sources, targets;
   std::vector<fp_force> forces;
   std::vector<fp_collider> colliders;
   std::vector<uint32_t> masks;
+  std::vector<fp_mesh_source> meshSources;
+  std::vector<int32_t> targetCells;
+  std::vector<uint32_t> targetRanges;
+  template <class T>
+  static const T* own(std::vector<T>& v, const T* src, size_t n) {
+    if (!src || !n) {
+      v.clear();
+      return src && !n ? nullptr : src;
+    }
+    v.assign(src, src + n);
+    return v.data();
+  }
   void assign(const fp_frame& f) {
     frame = f;
-    sources.assign(f.sources, f.sources + f.source_count);
-    targets.assign(f.force_targets, f.force_targets + f.force_target_count);
-    forces.assign(f.forces, f.forces + f.force_count);
-    colliders.assign(f.colliders, f.colliders + f.collider_count);
-    masks.assign(f.collider_masks, f.collider_masks + f.collider_mask_words);
-    frame.sources = sources.data();
-    frame.force_targets = targets.data();
-    frame.forces = forces.data();
-    frame.colliders = colliders.data();
-    frame.collider_masks = masks.data();
+    frame.sources = own(sources, f.sources, f.source_count);
+    frame.force_targets = own(targets, f.force_targets, f.force_target_count);
+    frame.forces = own(forces, f.forces, f.force_count);
+    frame.colliders = own(colliders, f.colliders, f.collider_count);
+    frame.collider_masks = own(masks, f.collider_masks, f.collider_mask_words);
+    frame.mesh_sources = own(meshSources, f.mesh_sources, f.mesh_source_count);
+    frame.target_cells = own(targetCells, f.target_cells, (size_t)f.target_cell_count * 3);
+    // Two words per force target; present only with target cells.
+    frame.target_cell_ranges =
+        f.target_cell_ranges ? own(targetRanges, f.target_cell_ranges, (size_t)f.force_target_count * 2) : nullptr;
   }
 };
 
@@ -83,6 +96,7 @@ struct fp_server {
   std::deque<uint32_t> waiting;
   uint64_t memory = 0;
   uint32_t live = 0;
+  int velocityDivisor = 0;  // the sessions' velocity divisor, from the first one opened
   uint64_t nextTicket = 1;
   uint64_t queued = 0, inFlight = 0;
   std::deque<fp_completion> completed;
@@ -241,6 +255,42 @@ void schedule(fp_server* S) {
     dts.clear();
     stepsAfter.clear();
     {
+      // Each request is checked on its own (flame ramps, dt, mesh arrays) before the launch is
+      // built: one session's invalid frame fails only its own step, with its message, and the
+      // others run (the reference validates before any state changes, flame.ts:47-85,
+      // FluidSimulation.ts:1368-1369).
+      std::vector<Request*> bad;
+      std::vector<std::string> why;
+      std::vector<int> codes;
+      std::vector<Request*> good;
+      for (Request* r : reqs) {
+        fp::Engine* e;
+        {
+          std::lock_guard<std::mutex> lk(S->mu);
+          e = S->sessions[r->session]->engine;
+        }
+        int vrc = e->validate(r->frame.frame, r->dt);
+        if (vrc) {
+          bad.push_back(r);
+          codes.push_back(vrc);
+          why.push_back("session " + std::to_string(r->session) + ": " + e->error());
+        } else {
+          good.push_back(r);
+        }
+      }
+      for (size_t k = 0; k < bad.size(); k++) {
+        std::vector<Request*> one{bad[k]};
+        {
+          std::lock_guard<std::mutex> lk(S->mu);
+          S->error = why[k];
+        }
+        failRequests(S, one, codes[k]);
+      }
+      reqs.swap(good);
+      if (reqs.empty()) {
+        S->done.notify_all();
+        continue;
+      }
       std::lock_guard<std::mutex> lk(S->mu);
       for (Request* r : reqs) {
         Session* s = S->sessions[r->session];
@@ -344,6 +394,19 @@ int fp_server_open(fp_server* S, const fp_grid* grid, float cutoff, int ground, 
   int rc = fp_grid_memory_bytes(grid, &bytes);
   if (rc) return serverFail(S, rc, fp_last_error(nullptr));
   if (grid->brick_size != S->cfg.brick_size) return serverFail(S, FP_EINVAL, "brickSize differs from the server's.");
+  {
+    // One launch steps every live session on one velocity lattice: the server takes the
+    // velocity divisor of its first session, and a grid with another one is refused here
+    // rather than failing every launch it would join.
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->velocityDivisor == 0) S->velocityDivisor = grid->velocity_divisor;
+    if (grid->velocity_divisor != S->velocityDivisor) {
+      S->error = "velocityDivisor " + std::to_string(grid->velocity_divisor) + " differs from the server's (" +
+                 std::to_string(S->velocityDivisor) + ").";
+      fp_set_error(FP_EINVAL, S->error);
+      return FP_EINVAL;
+    }
+  }
   if (!std::isfinite(cutoff)) return serverFail(S, FP_EINVAL, "grid.cutoff must be a finite number from 0 to 1.");
   if (bytes > S->cfg.memory_budget)
     return serverFail(S, FP_ELIMIT, "the session needs " + std::to_string(bytes) + " device bytes, more than the budget");
@@ -404,7 +467,8 @@ int fp_server_submit(fp_server* S, uint32_t session, const fp_frame* frame, floa
   if (!S || !frame) return fp_set_error(FP_EINVAL, "fp_server_submit needs a server and a frame.");
   if ((frame->source_count && !frame->sources) || (frame->force_count && !frame->forces) ||
       (frame->collider_count && !frame->colliders) || (frame->force_target_count && !frame->force_targets) ||
-      (frame->collider_mask_words && !frame->collider_masks))
+      (frame->collider_mask_words && !frame->collider_masks) || (frame->mesh_source_count && !frame->mesh_sources) ||
+      (frame->target_cell_count && (!frame->target_cells || !frame->target_cell_ranges)))
     return serverFail(S, FP_EINVAL, "frame arrays are null but their counts are not");
   if (!std::isfinite(dt) || dt <= 0 || dt > 1.f / 30.f)
     return serverFail(S, FP_EINVAL, "Simulation step must be in (0, 1/30]. Use fixed substeps.");
@@ -491,16 +555,22 @@ int fp_server_read_stats(fp_server* S, fp_server_stats* out) {
   return FP_OK;
 }
 
+// A live session's Engine, looked up with the GPU lock held (the scheduler deletes the Engines
+// of closed sessions under it, and takes the GPU lock before the session lock, as here).
+static fp::Engine* liveEngine(fp_server* S, uint32_t session) {
+  std::lock_guard<std::mutex> lk(S->mu);
+  Session* s = sessionOf(S, session);
+  return s && (s->state == FP_SESSION_LIVE || s->state == FP_SESSION_CLOSING) ? s->engine : nullptr;
+}
+
 int fp_server_session_stats(fp_server* S, uint32_t session, fp_stats* out) {
   if (!S || !out) return fp_set_error(FP_EINVAL, "fp_server_session_stats needs a server and an output.");
-  fp::Engine* e = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(S->mu);
-    Session* s = sessionOf(S, session);
-    if (s) e = s->engine;
+  std::unique_lock<std::mutex> g(S->gpu);
+  fp::Engine* e = liveEngine(S, session);
+  if (!e) {
+    g.unlock();
+    return serverFail(S, FP_EINVAL, "session " + std::to_string(session) + " is not live");
   }
-  if (!e) return serverFail(S, FP_EINVAL, "session " + std::to_string(session) + " is not live");
-  std::lock_guard<std::mutex> g(S->gpu);
   int rc = e->stats(out);
   if (rc) return serverFail(S, rc, e->error());
   return FP_OK;
@@ -508,14 +578,12 @@ int fp_server_session_stats(fp_server* S, uint32_t session, fp_stats* out) {
 
 int fp_server_read_field(fp_server* S, uint32_t session, int field, float* host, size_t bytes) {
   if (!S || !host) return fp_set_error(FP_EINVAL, "fp_server_read_field needs a server and a buffer.");
-  fp::Engine* e = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(S->mu);
-    Session* s = sessionOf(S, session);
-    if (s) e = s->engine;
+  std::unique_lock<std::mutex> g(S->gpu);
+  fp::Engine* e = liveEngine(S, session);
+  if (!e) {
+    g.unlock();
+    return serverFail(S, FP_EINVAL, "session " + std::to_string(session) + " is not live");
   }
-  if (!e) return serverFail(S, FP_EINVAL, "session " + std::to_string(session) + " is not live");
-  std::lock_guard<std::mutex> g(S->gpu);
   int rc = e->readField(field, host, bytes);
   if (rc) return serverFail(S, rc, e->error());
   return FP_OK;
