@@ -189,7 +189,7 @@ typedef struct fp_stats {
   uint64_t d2h_bytes;       /* device-to-host bytes the latest step read back (its measurement) */
   double host_prepare_ms;   /* host time in fp_sim_step since creation, waits excluded */
   double host_wait_ms;      /* host time spent waiting for the previous step's measurement */
-  double last_divergence;   /* post-projection RMS(h div u) / RMS(u) of that solve when measured, else -1 */
+  double last_divergence;   /* post-projection RMS(h (div u - e)) / RMS(u) of that solve when measured, else -1 */
   uint64_t bricks_stepped;  /* computing bricks summed over the measured steps since creation or reset */
 } fp_stats;
 
@@ -203,7 +203,9 @@ typedef struct fp_solver_stats {
   double unknowns;                   /* unknown cells */
   double rhs_rms;                    /* RMS of the right-hand side h^2 (div u* - expansion) */
   double residual[FP_MAX_VCYCLES];   /* RMS residual / RMS right-hand side after each V-cycle */
-  double divergence;                 /* RMS(h div u) / RMS(u) of the projected velocity, or -1 */
+  double divergence;                 /* RMS(h (div u - e)) / RMS(u) of the projected velocity over
+                                        the interior unknowns, e the expansion rate the projection
+                                        keeps (computeDivergence's source), or -1 */
 } fp_solver_stats;
 
 /* Device time of one phase of the step, accumulated while profiling is on: the restatement
@@ -269,6 +271,35 @@ int fp_sim_reserve_tiles(fp_sim* sim, uint32_t tiles);
 int fp_sim_set_solver(fp_sim* sim, int vcycles, float tolerance);
 /* The latest step's solve (waits for the step's work). */
 int fp_sim_read_solver(fp_sim* sim, fp_solver_stats* out);
+
+/* The pressure solve's schedule. The default (all fields zero) is the reference's V-cycle
+ * (PressureSolver.ts:276-365): weighted Jacobi (omega 0.8), every level down to one cell a
+ * tile, the first iterate from zero and 2 more sweeps before each restriction below the finest
+ * level, 3 after each prolongation, 19 bottom iterations; the red-black fields are then
+ * ignored. No reference counterpart for the rest:
+ *  - FP_SMOOTHER_REDBLACK: red-black Gauss-Seidel, in place (the cells of a level with x + y + z
+ *    even, then the odd ones; after a prolongation the odd ones first), on the `levels` finest
+ *    levels: `pre_sweeps` before each restriction, `post_sweeps` after each prolongation and
+ *    `bottom_sweeps` on the coarsest of them; every level starts from zero.
+ *  - FP_KRYLOV_FCG: flexible conjugate gradients on the finest level with one V-cycle of the
+ *    smoother as the preconditioner (either smoother): the first V-cycle gives the start, each
+ *    later one a search direction made A-orthogonal to the previous one; the dot products and
+ *    the residual norm are FP64 sums on the GPU. fp_sim_set_solver's `vcycles` then counts the
+ *    V-cycles of the whole solve and its tolerance applies to the CG residual.
+ * One launch steps simulations of one schedule: a batch step of simulations that differ fails. */
+#define FP_SMOOTHER_JACOBI 0
+#define FP_SMOOTHER_REDBLACK 1
+#define FP_KRYLOV_NONE 0
+#define FP_KRYLOV_FCG 1
+typedef struct fp_solver_schedule {
+  int32_t smoother;       /* FP_SMOOTHER_* */
+  int32_t levels;         /* red-black: levels from the finest, 2 up to all of them; 0 = all */
+  int32_t pre_sweeps;     /* red-black: 1..8 */
+  int32_t post_sweeps;    /* red-black: 0..8 */
+  int32_t bottom_sweeps;  /* red-black: 1..64 */
+  int32_t krylov;         /* FP_KRYLOV_* */
+} fp_solver_schedule;
+int fp_sim_set_schedule(fp_sim* sim, const fp_solver_schedule* schedule);
 /* ---- Volume rendering: a headless restatement of the renderer's compute passes and camera
  * march (lighting.wgsl smoothSmoke/buildOccupancy/buildLighting, volume-slices.wgsl
  * buildSlices, volume-march.wgsl fireProMarch, scene-volume.wgsl fireProSceneVolume with an
@@ -359,6 +390,8 @@ int fp_batch_reserve_tiles(fp_batch* batch, uint32_t id, uint32_t tiles);
  * demanding simulation asks for; each simulation stops at its own limit or tolerance. */
 int fp_batch_set_solver(fp_batch* batch, uint32_t id, int vcycles, float tolerance);
 int fp_batch_read_solver(fp_batch* batch, uint32_t id, fp_solver_stats* out);
+/* As fp_sim_set_schedule; the simulations of one fp_batch_step must share a schedule. */
+int fp_batch_set_schedule(fp_batch* batch, uint32_t id, const fp_solver_schedule* schedule);
 /* Step the `count` simulations `ids` (distinct) with frames[i] and dts[i], in one launch. */
 int fp_batch_step(fp_batch* batch, const uint32_t* ids, const fp_frame* frames, const float* dts, uint32_t count);
 int fp_batch_synchronize(fp_batch* batch);

@@ -283,6 +283,14 @@ struct Sim {
   std::vector<R> pres[2];  // level 0 pressures
   int latest = 0;
   int vcycles = 1;  // V-cycles a step; later ones are defect corrections of the finest level
+  // The solve's schedule (fp_solver_schedule): the reference's Jacobi V-cycle, or red-black
+  // Gauss-Seidel on the `mgLevels` finest levels; optionally flexible CG around either.
+  int smoother = FP_SMOOTHER_JACOBI, mgLevels = 0, preSweeps = 2, postSweeps = 2, bottomSweeps = 8;
+  int krylov = FP_KRYLOV_NONE;
+  float tolerance = 0;  // CG: stop once RMS residual <= tolerance x RMS right-hand side
+  std::vector<R>* rhs0 = nullptr;  // the finest level's right-hand side: the divergence, or the CG residual
+  std::vector<R> kx, ks, kd, kq;   // CG: iterate, residual (rhs + A x), direction, A direction
+  std::vector<double> cgRes2;      // CG: the residual's sum of squares after each V-cycle
 
   // --- per step scene
   std::vector<Emitter<R>> emitters;
@@ -2811,7 +2819,7 @@ struct Sim {
   }
   // The level's pressure pair and right-hand side.
   std::vector<R>& P(int level, int k) { return level == 0 ? pres[k] : levels[level].p[k]; }
-  std::vector<R>& RHS(int level) { return level == 0 ? div : levels[level].rhs; }
+  std::vector<R>& RHS(int level) { return level == 0 ? (rhs0 ? *rhs0 : div) : levels[level].rhs; }
   void smooth(int level, int n, bool& initialize) {
     Level& L = levels[level];
     for (int i = 0; i < n; i++) {
@@ -2889,13 +2897,182 @@ struct Sim {
     L.current = 1 - L.current;
     smooth(index, 3, initialize);
   }
-  // PressureSolver.solve (PressureSolver.ts:371-402) with PRESSURE_CYCLES = 1.
+  // ---- red-black Gauss-Seidel (no reference counterpart; the reference smooths with Jacobi)
+  // The coarsest level of the red-black V-cycle.
+  int coarsestLevel() const { return mgLevels > 0 ? std::min(mgLevels - 1, bottom) : bottom; }
+  // One colour of a level in place: the cells with x + y + z of parity `colour` take
+  // (sum of open neighbours - rhs) / diag, the others keep their value. From `zero`, every
+  // neighbour reads zero and the other colour's cells become zero.
+  void relaxColour(int level, std::vector<R>& p, int colour, bool zero) {
+    const std::vector<R>& rhs = RHS(level);
+    forLevelCells(level, [&](int px, int py, int pz) {
+      long a = cellAddress(px, py, pz, level);
+      if (((px + py + pz) & 1) != colour) {
+        if (zero) p[a] = 0;
+        return;
+      }
+      uint32_t flags = flagsOf(level, a);
+      if ((flags & SOLID) || !activeCell(px, py, pz, level)) {
+        p[a] = 0;
+        return;
+      }
+      R sum = 0, diag = axisDiag(flags);
+      if (!zero) stencil(px, py, pz, flags, level, p, sum, diag);
+      p[a] = store_round((sum - rhs[a]) / std::max(diag, R(1e-12)), storeMode(level));
+    });
+  }
+  // `n` sweeps: red then black, or after a prolongation black then red.
+  void sweepsRB(int level, std::vector<R>& p, int n, bool zero, bool post) {
+    for (int i = 0; i < n; i++) {
+      int first = post ? 1 : 0;
+      relaxColour(level, p, first, zero && i == 0);
+      relaxColour(level, p, 1 - first, false);
+    }
+  }
+  void cycleRB(int index, bool zero) {
+    std::vector<R>& p = P(index, 0);
+    if (index == coarsestLevel()) {
+      sweepsRB(index, p, bottomSweeps, zero, false);
+      return;
+    }
+    sweepsRB(index, p, preSweeps, zero, false);
+    // The restriction's first iterate of the coarse level goes to the level's other buffer,
+    // unused: the coarse level starts from zero.
+    restrictLevel(index, RHS(index), p, RHS(index + 1), P(index + 1, 1));
+    cycleRB(index + 1, true);
+    prolongate(index, p, P(index + 1, 0), p);
+    sweepsRB(index, p, postSweeps, false, true);
+  }
+  // One V-cycle of the schedule's smoother on the finest level, from zero (`zero`) or from its
+  // current iterate; returns the finest level's buffer that holds the result.
+  std::vector<R>& vcycleOnce(bool zero, bool& initialize) {
+    if (smoother == FP_SMOOTHER_REDBLACK) {
+      cycleRB(0, zero);
+      return P(0, 0);
+    }
+    if (zero) initialize = true;
+    cycle(0, initialize);
+    return P(0, levels[0].current);
+  }
+
+  // ---- flexible conjugate gradients on the finest level (no reference counterpart)
+  // Finest-level unknowns, and A v = diag v - (sum of open neighbours) there.
+  bool unknown0(int px, int py, int pz, long a) {
+    uint32_t flags = flagsOf(0, a);
+    return !(flags & SOLID) && activeCell(px, py, pz, 0);
+  }
+  // Over the finest level's unknown cells: fn(a, flags, px, py, pz) -> a contribution to a sum.
+  template <class F>
+  double sumUnknowns(F fn) {
+    int side = levelSide(0), cells = side * side * side;
+    long n = (long)active.size();
+    double total = 0;
+#pragma omp parallel for schedule(dynamic, 8) reduction(+ : total)
+    for (long i = 0; i < n; i++) {
+      I3 b = brickOf(active[i]);
+      for (int o = 0; o < cells; o++) {
+        int px = b[0] * side + o % side, py = b[1] * side + (o / side) % side, pz = b[2] * side + o / (side * side);
+        long a = cellAddress(px, py, pz, 0);
+        if (a < 0 || !unknown0(px, py, pz, a)) continue;
+        total += fn(a, flagsOf(0, a), px, py, pz);
+      }
+    }
+    return total;
+  }
+  R applyAt(const std::vector<R>& v, long a, uint32_t flags, int px, int py, int pz) {
+    R sum, diag;
+    stencil(px, py, pz, flags, 0, v, sum, diag);
+    return diag * v[a] - sum;
+  }
+  void solveFCG() {
+    size_t n = pres[0].size();
+    kx.assign(n, 0);
+    ks.assign(n, 0);
+    kd.assign(n, 0);
+    kq.assign(n, 0);
+    cgRes2.assign(vcycles, 0.0);
+    bool initialize = true;
+    rhs0 = nullptr;
+    // The start: one V-cycle from zero on the divergence; s = rhs + A x.
+    kx = vcycleOnce(true, initialize);
+    double rhs2 = 0;
+    double r2 = sumUnknowns([&](long a, uint32_t f, int px, int py, int pz) {
+      R v = div[a] + applyAt(kx, a, f, px, py, pz);
+      ks[a] = v;
+      return (double)v * (double)v;
+    });
+    rhs2 = sumUnknowns([&](long a, uint32_t, int, int, int) { return (double)div[a] * (double)div[a]; });
+    cgRes2[0] = r2;
+    double dqPrev = 0;
+    for (int c = 1; c < vcycles; c++) {
+      if (tolerance > 0 && cgRes2[c - 1] <= (double)tolerance * (double)tolerance * rhs2) break;
+      // z = V(s): one V-cycle from zero with the residual as its right-hand side.
+      rhs0 = &ks;
+      std::vector<R> z = vcycleOnce(true, initialize);
+      rhs0 = nullptr;
+      double beta = 0;
+      if (c > 1) {
+        double zq = sumUnknowns([&](long a, uint32_t, int, int, int) { return (double)z[a] * (double)kq[a]; });
+        beta = dqPrev != 0 ? -zq / dqPrev : 0.0;
+      }
+      // d = z + beta d; q = A z + beta q (= A d); then d.q and d.s.
+      std::vector<R> az(n, 0);
+      sumUnknowns([&](long a, uint32_t f, int px, int py, int pz) {
+        az[a] = applyAt(z, a, f, px, py, pz);
+        return 0.0;
+      });
+      double dq = sumUnknowns([&](long a, uint32_t, int, int, int) {
+        R d = z[a] + (R)beta * kd[a];
+        R q = az[a] + (R)beta * kq[a];
+        kd[a] = d;
+        kq[a] = q;
+        return (double)d * (double)q;
+      });
+      double ds = sumUnknowns([&](long a, uint32_t, int, int, int) { return (double)kd[a] * (double)ks[a]; });
+      double alpha = dq != 0 ? -ds / dq : 0.0;
+      dqPrev = dq;
+      cgRes2[c] = sumUnknowns([&](long a, uint32_t, int, int, int) {
+        kx[a] += (R)alpha * kd[a];
+        R v = ks[a] + (R)alpha * kq[a];
+        ks[a] = v;
+        return (double)v * (double)v;
+      });
+    }
+    pres[latest] = kx;
+  }
+  // PressureSolver.solve (PressureSolver.ts:371-402) with PRESSURE_CYCLES = 1, or the
+  // schedule's solve.
   void solvePressure() {
     buildZeroedTopology();
     buildTopology();
+    if (krylov == FP_KRYLOV_FCG) {
+      levels[0].current = latest;
+      solveFCG();
+      return;
+    }
+    cgRes2.assign(vcycles, 0.0);
+    // The residual rhs + A p of the finest level's iterate, as a sum of squares.
+    auto residual2 = [&](const std::vector<R>& p) {
+      return sumUnknowns([&](long a, uint32_t f, int px, int py, int pz) {
+        double v = (double)(div[a] + applyAt(p, a, f, px, py, pz));
+        return v * v;
+      });
+    };
+    if (smoother == FP_SMOOTHER_REDBLACK) {
+      // In place on the finest level's first buffer; later V-cycles correct the current iterate.
+      for (int c = 0; c < vcycles; c++) {
+        cycleRB(0, c == 0);
+        cgRes2[c] = residual2(P(0, 0));
+      }
+      latest = 0;
+      return;
+    }
     levels[0].current = latest;
     bool initialize = true;
-    for (int c = 0; c < vcycles; c++) cycle(0, initialize);
+    for (int c = 0; c < vcycles; c++) {
+      cycle(0, initialize);
+      if (vcycles > 1) cgRes2[c] = residual2(P(0, levels[0].current));
+    }
     latest = levels[0].current;
   }
 
@@ -3097,6 +3274,31 @@ void or_set_solver(or_sim* s, int vcycles) {
     s->d->vcycles = vcycles;
   else
     s->f->vcycles = vcycles;
+}
+// The pressure solve's schedule (fp_solver_schedule) and the CG tolerance, for later steps.
+void or_set_schedule(or_sim* s, const fp_solver_schedule* sc, float tolerance) {
+  auto fn = [&](auto& sim) {
+    sim.smoother = sc->smoother;
+    sim.mgLevels = sc->levels;
+    sim.preSweeps = sc->pre_sweeps;
+    sim.postSweeps = sc->post_sweeps;
+    sim.bottomSweeps = sc->bottom_sweeps;
+    sim.krylov = sc->krylov;
+    sim.tolerance = tolerance;
+  };
+  if (s->d)
+    fn(*s->d);
+  else
+    fn(*s->f);
+}
+// The finest level's CG residual sums of squares of the latest solve, one per V-cycle run.
+int or_read_cg(or_sim* s, double* out, int capacity) {
+  auto fn = [&](auto& sim) -> int {
+    int n = std::min(capacity, (int)sim.cgRes2.size());
+    for (int i = 0; i < n; i++) out[i] = sim.cgRes2[i];
+    return n;
+  };
+  return s->d ? fn(*s->d) : fn(*s->f);
 }
 int or_step(or_sim* s, const fp_frame* f, float dt) {
   std::string e = s->d ? s->d->step(*f, dt) : s->f->step(*f, dt);

@@ -36,6 +36,9 @@ def lib():
         L.or_set_threads.argtypes = [C.c_int]
         L.or_set_runtime.argtypes = [C.c_void_p, C.c_float, C.c_double, C.c_int]
         L.or_set_solver.argtypes = [C.c_void_p, C.c_int]
+        L.or_set_schedule.argtypes = [C.c_void_p, C.c_void_p, C.c_float]
+        L.or_read_cg.restype = C.c_int
+        L.or_read_cg.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.or_step.restype = C.c_int
         L.or_step.argtypes = [C.c_void_p, C.c_void_p, C.c_float]
         L.or_render.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -102,6 +105,16 @@ class OracleSim:
     def set_solver(self, vcycles: int):
         """V-cycles of each later step's pressure solve (defect corrections after the first)."""
         self.L.or_set_solver(self.h, vcycles)
+
+    def set_schedule(self, schedule, tolerance: float = 0.0):
+        """The pressure solve's schedule (an abi.fp_solver_schedule) for later steps."""
+        self.L.or_set_schedule(self.h, C.byref(schedule), tolerance)
+
+    def cg_residuals(self) -> np.ndarray:
+        """The latest CG solve's residual sums of squares, one per V-cycle it ran."""
+        out = np.zeros(16, np.float64)
+        n = self.L.or_read_cg(self.h, out.ctypes.data, 16)
+        return out[:n]
 
     def step(self, frame, dt: float = 1.0 / 60.0):
         if self.L.or_step(self.h, C.byref(frame), dt) != 0:

@@ -131,10 +131,11 @@ def force(gpu, orc):
 
 
 def lockstep(scene, steps: int, gpu_factory, cutoff=0.05, budget=8e6, ground=True, start=0, log=None, grid=None,
-             before_step=None, vcycles=1, after=None):
+             before_step=None, vcycles=1, after=None, schedule=None):
     """Run `steps` steps in lockstep; returns per-step (tables, fields) reports.
     `before_step(step, gpu, oracle)` may change runtime settings on both. `vcycles` V-cycles
-    a step on both sides (tolerance 0: all of them run)."""
+    a step on both sides (tolerance 0: all of them run), with the pressure-solve `schedule`
+    (an abi.fp_solver_schedule; None: the reference's)."""
     grid = grid if grid is not None else scene.grid(budget=budget)
     gpu = gpu_factory(grid)
     orc = OracleSim(grid, real=0)
@@ -143,6 +144,9 @@ def lockstep(scene, steps: int, gpu_factory, cutoff=0.05, budget=8e6, ground=Tru
     if vcycles != 1:
         gpu.set_solver(vcycles, 0.0)
         orc.set_solver(vcycles)
+    if schedule is not None:
+        gpu.set_schedule(schedule)
+        orc.set_schedule(schedule)
     reports = []
     for s in range(start, start + steps):
         if before_step:

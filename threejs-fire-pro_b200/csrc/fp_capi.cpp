@@ -170,6 +170,11 @@ int fp_sim_set_solver(fp_sim* sim, int vcycles, float tolerance) {
   return sim->engine->setSolver(vcycles, tolerance);
 }
 
+int fp_sim_set_schedule(fp_sim* sim, const fp_solver_schedule* schedule) {
+  if (!sim || !schedule) return failed("fp_sim_set_schedule needs a simulation and a schedule.", FP_EINVAL);
+  return sim->engine->setSchedule(*schedule);
+}
+
 int fp_sim_read_solver(fp_sim* sim, fp_solver_stats* out) {
   if (!sim || !out) return failed("fp_sim_read_solver needs a simulation and an output.", FP_EINVAL);
   return sim->engine->readSolver(out);
@@ -321,6 +326,14 @@ int fp_batch_set_solver(fp_batch* batch, uint32_t id, int vcycles, float toleran
   fp::Engine* e = batchSim(batch, id);
   if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
   int rc = e->setSolver(vcycles, tolerance);
+  return rc ? batchFail(batch, rc, e->error()) : FP_OK;
+}
+
+int fp_batch_set_schedule(fp_batch* batch, uint32_t id, const fp_solver_schedule* schedule) {
+  if (!batch || !schedule) return failed("fp_batch_set_schedule needs a batch and a schedule.", FP_EINVAL);
+  fp::Engine* e = batchSim(batch, id);
+  if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
+  int rc = e->setSchedule(*schedule);
   return rc ? batchFail(batch, rc, e->error()) : FP_OK;
 }
 

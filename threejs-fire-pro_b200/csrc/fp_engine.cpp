@@ -214,6 +214,7 @@ void Engine::freeAll() {
     if (b->ptr) { cudaFree(b->ptr); *b = DeviceBuffer{}; }
   meshVersion_ = coverageVersion_ = ~0ull;
   for (auto& b : p0_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
+  for (auto& b : kry_) if (b.ptr) { cudaFree(b.ptr); b = DeviceBuffer{}; }
   for (int l = 0; l < FP_MAX_LEVELS; l++) {
     if (topo_[l].ptr) { cudaFree(topo_[l].ptr); topo_[l] = DeviceBuffer{}; }
     if (lrhs_[l].ptr) { cudaFree(lrhs_[l].ptr); lrhs_[l] = DeviceBuffer{}; }
@@ -327,6 +328,10 @@ int Engine::allocatePools(uint32_t slots) {
     ok = alloc(smoke_[0], s * SN_ * scalarBytes()) && alloc(smoke_[1], s * SN_ * 4) &&
          alloc(smoke_[2], s * SN_ * scalarBytes()) && alloc(smokeBnd_, s * 2 * SN_ * 4);
   if (!ok) return FP_ENOMEM;
+  if (schedule_.krylov) {
+    int rc = krylovPools(slots);
+    if (rc) return rc;
+  }
   std::vector<uint32_t> stack(slots);
   for (uint32_t i = 0; i < slots; i++) stack[i] = slots - 1 - i;
   cudaMemcpy(freeStack_.ptr, stack.data(), s * 4, cudaMemcpyHostToDevice);
@@ -360,6 +365,10 @@ int Engine::growPool(uint32_t target) {
     for (int k = 0; k < 3; k++) ok = ok && grow(smoke_[k], s * SN_ * (k == 1 ? 4 : scalarBytes()), 0);
   if (ok && smokeDiv_ > 1) ok = grow(smokeBnd_, s * 2 * SN_ * 4, 0);
   if (!ok) return FP_ENOMEM;
+  if (schedule_.krylov) {
+    int rc = krylovPools(target);
+    if (rc) return rc;
+  }
   std::vector<uint32_t> old(slots_);
   cudaMemcpy(old.data(), freeStack_.ptr, (size_t)slots_ * 4, cudaMemcpyDeviceToHost);
   std::vector<uint32_t> next(target);
@@ -984,6 +993,8 @@ void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t
   P.solids = (uint32_t*)solids_.ptr;
   P.p0[0] = (float*)p0_[0].ptr;
   P.p0[1] = (float*)p0_[1].ptr;
+  P.p0[2] = (float*)p0_[2].ptr;
+  for (int k = 0; k < 3; k++) P.kry[k] = (float*)kry_[k].ptr;
   P.latest = latest_;
   P.scalarHalf = precision_ == FP_PRECISION_MIXED ? 1 : 0;
   P.coarseBf16 = precision_ == FP_PRECISION_MIXED ? 1 : 0;
@@ -1089,6 +1100,35 @@ int Engine::setSolver(int vcycles, float tolerance) {
   return FP_OK;
 }
 
+int Engine::krylovPools(uint32_t slots) {
+  size_t bytes = (size_t)slots * VN_ * 4;
+  bool ok = grow(p0_[2], bytes, 0);
+  for (auto& b : kry_) ok = ok && grow(b, bytes, 0);
+  return ok ? FP_OK : fail(FP_ENOMEM, "out of device memory for the CG buffers");
+}
+
+int Engine::setSchedule(const fp_solver_schedule& sc) {
+  if (sc.smoother != FP_SMOOTHER_JACOBI && sc.smoother != FP_SMOOTHER_REDBLACK)
+    return fail(FP_EINVAL, "smoother must be FP_SMOOTHER_JACOBI or FP_SMOOTHER_REDBLACK.");
+  if (sc.krylov != FP_KRYLOV_NONE && sc.krylov != FP_KRYLOV_FCG)
+    return fail(FP_EINVAL, "krylov must be FP_KRYLOV_NONE or FP_KRYLOV_FCG.");
+  fp_solver_schedule next = sc;
+  if (sc.smoother == FP_SMOOTHER_REDBLACK) {
+    if (sc.levels != 0 && (sc.levels < 2 || sc.levels > bottom_ + 1))
+      return fail(FP_EINVAL, "levels must be 0 or from 2 to " + std::to_string(bottom_ + 1) + ".");
+    if (sc.pre_sweeps < 1 || sc.pre_sweeps > 8) return fail(FP_EINVAL, "pre_sweeps must be from 1 to 8.");
+    if (sc.post_sweeps < 0 || sc.post_sweeps > 8) return fail(FP_EINVAL, "post_sweeps must be from 0 to 8.");
+    if (sc.bottom_sweeps < 1 || sc.bottom_sweeps > 64) return fail(FP_EINVAL, "bottom_sweeps must be from 1 to 64.");
+  } else {
+    next.levels = next.pre_sweeps = next.post_sweeps = next.bottom_sweeps = 0;  // the reference's plan
+  }
+  int rc = consume();
+  if (rc) return rc;
+  if (next.krylov && (rc = krylovPools(slots_))) return rc;
+  schedule_ = next;
+  return FP_OK;
+}
+
 int Engine::setRuntime(float cutoff, double budget, int ground) {
   if (!std::isfinite(cutoff)) return fail(FP_EINVAL, "grid.cutoff must be a finite number from 0 to 1.");
   cutoff_ = cutoff;
@@ -1109,6 +1149,7 @@ uint64_t Engine::memoryBytes() const {
   for (auto& b : smoke_) bytes += b.bytes;
   bytes += smokeBnd_.bytes + meshTablesD_.bytes + meshSourcesD_.bytes + coverageD_.bytes;
   for (auto& b : p0_) bytes += b.bytes;
+  for (auto& b : kry_) bytes += b.bytes;
   for (int l = 0; l < FP_MAX_LEVELS; l++) bytes += topo_[l].bytes + lrhs_[l].bytes + lp_[l][0].bytes + lp_[l][1].bytes;
   return bytes;
 }

@@ -110,6 +110,9 @@ class Engine {
   // `vcycles` V-cycles a step, stopping at a relative FP64 residual of `tolerance` (0: all).
   int setSolver(int vcycles, float tolerance);
   int readSolver(fp_solver_stats* out);
+  // The solve's smoother, levels, sweeps and Krylov wrapper (fp_sim_set_schedule).
+  int setSchedule(const fp_solver_schedule& schedule);
+  const fp_solver_schedule& schedule() const { return schedule_; }
   // Volume rendering of the latest state (fp_render.cu) into device memory `image` (enqueued),
   // or into host memory `host` (waits).
   int render(const fp_camera& camera, const fp_render_settings& settings, float* image, float* host);
@@ -157,6 +160,9 @@ class Engine {
   int latest_ = 0;  // index of the latest pressure solution
   int vcycles_ = 1;
   float tolerance_ = 0.f;
+  fp_solver_schedule schedule_{};  // zeroed: the reference's Jacobi V-cycle
+  // The CG buffers (p0_[2], kry_) for `slots` slots when the schedule wraps the V-cycle in CG.
+  int krylovPools(uint32_t slots);
   bool measure_ = false;
   FpSolver lastSolver_{};
   uint32_t slots_ = 0;
@@ -166,7 +172,8 @@ class Engine {
   DeviceBuffer pages_, entries_, state_, activity_, records_, blockCounts_, active_, zeroList_;
   DeviceBuffer freeStack_, counters_;
   DeviceBuffer vel_[4], curl_, fld_[3], expn_, div_, vmin_, vmax_, sb_, donors_, solids_;
-  DeviceBuffer p0_[2], topo_[FP_MAX_LEVELS], lp_[FP_MAX_LEVELS][2], lrhs_[FP_MAX_LEVELS];
+  DeviceBuffer p0_[3], topo_[FP_MAX_LEVELS], lp_[FP_MAX_LEVELS][2], lrhs_[FP_MAX_LEVELS];
+  DeviceBuffer kry_[3];  // flexible CG: residual, direction, A direction (p0_[2] its iterate)
   DeviceBuffer tileRecD_, tileNbrD_, hashD_, solver_, tileMask_, liveTilesD_, tileIndexD_;
   std::vector<int> liveTiles_, tileIndex_;  // live tile slots ascending; slot -> position or -1
   int velIdx_[4] = {0, 1, 2, 3};  // start, predictor/projected, corrected, forced
@@ -325,7 +332,11 @@ class Stepper {
   int cycle_ = 0;             // the V-cycle being enqueued
   bool fusedCoarse_ = false;  // the V-cycle below the first tile level runs as k_coarse
   bool anySmoke_ = false;     // a simulation of the launch keeps coarse smoke
+  fp_solver_schedule schedule_{};  // the launch's pressure-solve schedule (its simulations')
+  int rhs0Sel_ = 2;           // the finest level's right-hand side: the divergence, or the CG residual
   void vcycle(int level, int cur[], uint64_t& launches);
+  // One red-black V-cycle from `level` down, in place; from zero when `zero`.
+  void vcycleRB(int level, bool zero, uint64_t& launches);
   int check(cudaError_t e, const char* what);
   int reserve(size_t arenaBytes, int sims, size_t readWords);
 };

@@ -73,6 +73,7 @@ FP_DEV float diagOf(uint32_t f) {
 // Levels above the finest hold BF16 values in FP_PRECISION_MIXED.
 FP_DEV bool narrowLevel(const SimParams& P, int level) { return level > 0 && P.coarseBf16 != 0; }
 FP_DEV float readAt(const SimParams& P, const Home& H, const float* arr, int px, int py, int pz, int level) {
+  if (!arr) return 0.f;  // a relaxation from zero
   long a = cellAddress(P, H, px, py, pz, level);
   return a < 0 ? 0.f : ldBf(arr, a, narrowLevel(P, level));
 }
@@ -124,6 +125,7 @@ struct Args {
   float* cfirst;
   bool rhsN, pinN, coarseN, poutN, cfirstN;  // the buffer holds BF16
   bool skip;                                 // a later V-cycle of a converged solve: no work
+  int colour;                                // MgSel::colour
 };
 
 // A launch names its buffers by selector, level * 4 + which (0 and 1 the level's pressure
@@ -132,6 +134,7 @@ FP_DEV float* mgBuffer(const SimParams& P, int sel) {
   if (sel < 0) return nullptr;
   int level = sel >> 2, which = sel & 3;
   if (which == 2) return level == 0 ? P.div : P.lrhs[level];
+  if (which == 3) return level == 0 ? P.kry[0] : nullptr;
   return level == 0 ? P.p0[which] : P.lp[level][which];
 }
 FP_DEV Args resolve(const SimParams& P, const MgSel& S) {
@@ -148,18 +151,30 @@ FP_DEV Args resolve(const SimParams& P, const MgSel& S) {
   A.poutN = S.pout >= 0 && narrowLevel(P, S.pout >> 2);
   A.cfirstN = S.cfirst >= 0 && narrowLevel(P, S.cfirst >> 2);
   A.skip = S.cycle > 0 && P.solver->converged != 0;
+  A.colour = S.colour;
   return A;
 }
 
+// Red-black: the cell's colour, 0 for x + y + z even.
+FP_DEV int parityOf(int px, int py, int pz) { return (px + py + pz) & 1; }
+
 FP_DEV void relaxCell(const SimParams& P, const Home& H, const Args& A, long a, int px, int py, int pz) {
+  if (A.colour != 0 && parityOf(px, py, pz) != A.colour - 1) {
+    // Red-black, the other colour: kept, or zero when the level starts from zero.
+    if (!A.pin) stBf(A.pout, a, 0.f, A.poutN);
+    return;
+  }
   uint32_t f = expandFlags(P.topo[A.level][a]);
   if ((f & SOLIDF) || !activeCell(P, H, px, py, pz, A.level)) {
     stBf(A.pout, a, 0.f, A.poutN);
     return;
   }
-  float sum = stencilSum(P, H, A.pin, px, py, pz, f, A.level);
+  float sum = A.pin ? stencilSum(P, H, A.pin, px, py, pz, f, A.level) : 0.f;
   float cand = (sum - ldBf(A.rhs, a, A.rhsN)) / fmaxf(diagOf(f), 1e-12f);
-  stBf(A.pout, a, mixf(ldBf(A.pin, a, A.pinN), cand, 0.8f), A.poutN);
+  if (A.colour != 0)
+    stBf(A.pout, a, cand, A.poutN);  // Gauss-Seidel in place
+  else
+    stBf(A.pout, a, mixf(A.pin ? ldBf(A.pin, a, A.pinN) : 0.f, cand, 0.8f), A.poutN);
 }
 
 FP_DEV void prolongCell(const SimParams& P, const Home& H, const Args& A, long a, int px, int py, int pz) {
@@ -310,7 +325,10 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
         } else {
           a = cellAddress(P, H, ox + lx, oy + ly, oz + lz, stageLevel);
         }
-        st[q] = a < 0 ? 0.f : ldBf(src, a, srcN);
+        // A relaxation from zero stages nothing; a red-black half-sweep stages only the other
+        // colour (a cell of the colour it writes reads none of its own colour).
+        const bool skipLoad = OP == RELAX && (!src || (A.colour != 0 && ((ox + oy + oz + lx + ly + lz) & 1) == A.colour - 1));
+        st[q] = (a < 0 || skipLoad) ? 0.f : ldBf(src, a, srcN);
         if (OP == PROLONG) {
           const bool solid = a >= 0 && (P.topo[stageLevel][a] & FP_STORED_SOLID);
           solidSt[q] = solid ? 1 : 0;
@@ -375,15 +393,25 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
           if (o >= FCELLS) break;
           const int lx = o & (FS - 1), ly = (o >> fs) & (FS - 1), lz = o >> (2 * fs);
           const long a = slot * FCELLS + o;
+          if (OP == RELAX && A.colour != 0 &&
+              ((H.bx * FS + lx + H.by * FS + ly + H.bz * FS + lz) & 1) != A.colour - 1) {
+            // Red-black, the other colour: kept, or zero when the level starts from zero.
+            if (!src) stBf(A.pout, a, 0.f, A.poutN);
+            continue;
+          }
           uint32_t f = expandFlags(ownTopo[k]);
           if ((f & SOLIDF) || !unknown(lx, ly, lz)) {
             stBf(A.pout, a, 0.f, A.poutN);
             continue;
           }
           if (OP == RELAX) {
-            float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
             float cand = (sumAt(lx, ly, lz, f) - ownValue[k]) / fmaxf(diagOf(f), 1e-12f);
-            stBf(A.pout, a, mixf(center, cand, 0.8f), A.poutN);
+            if (A.colour != 0) {
+              stBf(A.pout, a, cand, A.poutN);  // Gauss-Seidel in place
+            } else {
+              float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
+              stBf(A.pout, a, mixf(center, cand, 0.8f), A.poutN);
+            }
           } else {
             int px = H.bx * FS + lx, py = H.by * FS + ly, pz = H.bz * FS + lz;
             float qx = ((float)px + 0.5f) * 0.5f - 0.5f, qy = ((float)py + 0.5f) * 0.5f - 0.5f,
@@ -805,6 +833,190 @@ __global__ void __launch_bounds__(256) k_residual(FpBatch bt, int pSel, int cycl
   }
 }
 
+// The red-black bottom (no reference counterpart): `sweeps` red-black Gauss-Seidel sweeps of
+// the bottom level (one cell a tile) in place, every sweep the even tiles (x + y + z) then the
+// odd ones, in one CTA per simulation. Same cell arithmetic as relaxCell's red-black branch;
+// each value is rounded as the level's storage rounds it. With S.pin -1 the level starts from
+// zero. Shared memory by live tile when 20 bytes a tile fit, else in place in global memory.
+__global__ void __launch_bounds__(1024) k_bottom_rb(FpBatch bt, MgSel Sl, int sweeps, int smemBytes) {
+  extern __shared__ float bottomSmem[];
+  const int nbIndex[6] = {nbrIndex(1, 0, 0), nbrIndex(-1, 0, 0), nbrIndex(0, 1, 0),
+                          nbrIndex(0, -1, 0), nbrIndex(0, 0, 1), nbrIndex(0, 0, -1)};
+  constexpr uint32_t ODD = 0x40000000u;
+  int sims = batchCount(bt);
+  for (int sim = blockIdx.x; sim < sims; sim += gridDim.x) {
+    const SimParams& P = *bt.sims[sim].vview;
+    const Args A = resolve(P, Sl);
+    if (A.skip) continue;  // the same for the whole CTA
+    const int level = A.level, L = P.liveCount;
+    const bool nB = A.poutN;
+    auto flagOf = [&](int t) -> uint32_t {  // t is live
+      int4 rec = __ldg(&P.tileRec[t]);
+      Home H = enterTile(P, t, rec);
+      uint32_t f = activeCell(P, H, rec.x, rec.y, rec.z, level) ? expandFlags(P.topo[level][t]) : SOLIDF;
+      return f | (((rec.x + rec.y + rec.z) & 1) ? ODD : 0u);
+    };
+    if ((long)L * 20 <= (long)smemBytes) {
+      float* cur = bottomSmem;
+      float* rhs = cur + L;
+      uint32_t* flags = reinterpret_cast<uint32_t*>(rhs + L);
+      int16_t* nb = reinterpret_cast<int16_t*>(flags + L);  // 6 a tile
+      for (int j = threadIdx.x; j < L; j += blockDim.x) {
+        const int t = P.liveTiles[j];
+        const uint32_t f = flagOf(t);
+        flags[j] = f;
+        rhs[j] = ldBf(A.rhs, t, A.rhsN);
+        for (int k = 0; k < 6; k++) {
+          int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
+          nb[j * 6 + k] = (int16_t)(n >= 0 ? P.tileIndex[n] : -1);
+        }
+        cur[j] = (A.pin && !(f & SOLIDF)) ? ldBf(A.pin, t, A.pinN) : 0.f;
+      }
+      __syncthreads();
+      for (int it = 0; it < sweeps; it++)
+        for (int colour = 0; colour < 2; colour++) {
+          for (int j = threadIdx.x; j < L; j += blockDim.x) {
+            const uint32_t f = flags[j];
+            if ((int)((f & ODD) != 0) != colour) continue;
+            float next = 0.f;
+            if (!(f & SOLIDF)) {
+              float w[6];
+#pragma unroll
+              for (int k = 0; k < 6; k++) {
+                const int n = nb[j * 6 + k];
+                w[k] = n >= 0 ? cur[n] : 0.f;
+              }
+              float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
+              next = bfRound((sum - rhs[j]) / fmaxf(diagOf(f & 63u), 1e-12f), nB);
+            }
+            cur[j] = next;
+          }
+          __syncthreads();
+        }
+      for (int j = threadIdx.x; j < L; j += blockDim.x) stBf(A.pout, P.liveTiles[j], cur[j], nB);
+      __syncthreads();
+      continue;
+    }
+    // In place in global memory (A.pout, the level's storage type).
+    for (int j = threadIdx.x; j < L; j += blockDim.x) {
+      const int t = P.liveTiles[j];
+      const uint32_t f = flagOf(t);
+      if (!A.pin || (f & SOLIDF)) stBf(A.pout, t, 0.f, nB);
+    }
+    __syncthreads();
+    for (int it = 0; it < sweeps; it++)
+      for (int colour = 0; colour < 2; colour++) {
+        for (int j = threadIdx.x; j < L; j += blockDim.x) {
+          const int t = P.liveTiles[j];
+          const uint32_t f = flagOf(t);
+          if ((int)((f & ODD) != 0) != colour || (f & SOLIDF)) continue;
+          float w[6];
+#pragma unroll
+          for (int k = 0; k < 6; k++) {
+            int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
+            w[k] = n >= 0 ? ldBf(A.pout, n, nB) : 0.f;
+          }
+          float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
+          stBf(A.pout, t, (sum - ldBf(A.rhs, t, A.rhsN)) / fmaxf(diagOf(f & 63u), 1e-12f), nB);
+        }
+        __syncthreads();
+      }
+  }
+}
+
+// ---- Flexible conjugate gradients on the finest level (FP_KRYLOV_FCG; no reference
+// counterpart). A v = diag v - (sum of the open neighbours), the operator the relaxation
+// inverts; the residual s = rhs + A x has the sign restrictCell's residual has. A CTA per
+// computing brick, a thread per cell; FP64 sums per CTA, one double atomic each.
+//   begin:     x = p, s = rhs + A p; |s|^2 -> res2[0], |rhs|^2 -> rhs2, unknowns
+//   dot:       z.q (the new preconditioned residual against the old A d) -> zq[c]
+//   direction: beta = -zq[c] / dq[c-1] (0 at c = 1); d = z + beta d, q = A z + beta q (= A d);
+//              d.q -> dq[c], d.s -> ds[c]
+//   update:    alpha = -ds[c] / dq[c]; x += alpha d, s += alpha q; |s|^2 -> res2[c]
+enum FcgOp { FCG_BEGIN = 0, FCG_DOT = 1, FCG_DIRECTION = 2, FCG_UPDATE = 3 };
+
+template <int OP>
+__global__ void __launch_bounds__(256) k_fcg(FpBatch bt, int vSel, int cycle) {
+  __shared__ int nslot[27];
+  __shared__ double scratch[32];
+  uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
+  for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+    uint32_t i;
+    const SimParams& P = *workSim(bt, FP_WORK_ACTIVE, item, i).vview;
+    FpSolver* S = P.solver;
+    if (cycle > 0 && S->converged) continue;  // the same for the whole CTA
+    Home H = enterBrick(P, P.active[i], nslot);
+    const long slot = nslot[13];
+    const int m = P.B - 1;
+    const float* v = vSel >= 0 ? P.p0[vSel] : nullptr;  // BEGIN: p; DOT, DIRECTION: z
+    float* x = P.p0[2];
+    float* sres = P.kry[0];
+    float* d = P.kry[1];
+    float* q = P.kry[2];
+    const bool first = cycle <= 1;
+    const float beta = (OP == FCG_DIRECTION && !first && S->dq[cycle - 1] != 0.0) ? (float)(-S->zq[cycle] / S->dq[cycle - 1]) : 0.f;
+    const float alpha = (OP == FCG_UPDATE && S->dq[cycle] != 0.0) ? (float)(-S->ds[cycle] / S->dq[cycle]) : 0.f;
+    double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int px = H.bx * P.B + (c & m), py = H.by * P.B + ((c >> P.shift) & m), pz = H.bz * P.B + (c >> (2 * P.shift));
+      long a = slot * P.N + c;
+      uint32_t f = expandFlags(P.topo[0][a]);
+      bool unknown = !(f & SOLIDF) && activeCell(P, H, px, py, pz, 0);
+      if (OP == FCG_BEGIN) {
+        float p = v[a];
+        x[a] = p;
+        float r = 0.f;
+        if (unknown) {
+          float rhs = P.div[a];
+          r = rhs - (stencilSum(P, H, v, px, py, pz, f, 0) - diagOf(f) * p);
+          s1 += (double)r * (double)r;
+          s2 += (double)rhs * (double)rhs;
+          s3 += 1.0;
+        }
+        sres[a] = r;
+      } else if (OP == FCG_DOT) {
+        if (unknown) s1 += (double)v[a] * (double)q[a];
+      } else if (OP == FCG_DIRECTION) {
+        float dn = 0.f, qn = 0.f;
+        if (unknown) {
+          float z = v[a];
+          float az = diagOf(f) * z - stencilSum(P, H, v, px, py, pz, f, 0);
+          dn = first ? z : z + beta * d[a];
+          qn = first ? az : az + beta * q[a];
+          s1 += (double)dn * (double)qn;
+          s2 += (double)dn * (double)sres[a];
+        }
+        d[a] = dn;
+        q[a] = qn;
+      } else {
+        if (unknown) {
+          x[a] = x[a] + alpha * d[a];
+          float r = sres[a] + alpha * q[a];
+          sres[a] = r;
+          s1 += (double)r * (double)r;
+        }
+      }
+    }
+    s1 = blockSum(s1, scratch);
+    if (OP == FCG_BEGIN || OP == FCG_DIRECTION) s2 = blockSum(s2, scratch);
+    if (OP == FCG_BEGIN) s3 = blockSum(s3, scratch);
+    if (threadIdx.x == 0) {
+      if (OP == FCG_BEGIN) {
+        atomicAdd(&S->res2[0], s1);
+        atomicAdd(&S->rhs2, s2);
+        atomicAdd(&S->unknowns, s3);
+      } else if (OP == FCG_DOT) {
+        atomicAdd(&S->zq[cycle], s1);
+      } else if (OP == FCG_DIRECTION) {
+        atomicAdd(&S->dq[cycle], s1);
+        atomicAdd(&S->ds[cycle], s2);
+      } else {
+        atomicAdd(&S->res2[cycle], s1);
+      }
+    }
+  }
+}
+
 // Each simulation's decision after V-cycle `cycle`: converged once the residual's RMS is at
 // most the tolerance times the right-hand side's. One CTA.
 __global__ void k_converge(FpBatch bt, int cycle) {
@@ -976,6 +1188,7 @@ void fp_mg_configure(int B) {
   configureStaged<PROLONG, 2>();
   configureStaged<PROLONG, 1>();
   cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, BOTTOM_SMEM);
+  cudaFuncSetAttribute(k_bottom_rb, cudaFuncAttributeMaxDynamicSharedMemorySize, BOTTOM_SMEM);
   cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, COARSE_SMEM);
 }
 
@@ -1051,5 +1264,21 @@ void fp_launch_coarse(const FpBatch& bt, const MgSel& S, int iterations, int sms
 
 void fp_launch_residual(const FpBatch& bt, int pSel, int cycle, int sms, cudaStream_t st) {
   k_residual<<<sms * 4, 256, 0, st>>>(bt, pSel, cycle);
+  k_converge<<<1, 256, 0, st>>>(bt, cycle);
+}
+
+void fp_launch_bottom_rb(const FpBatch& bt, const MgSel& S, int sweeps, int sms, cudaStream_t st) {
+  k_bottom_rb<<<sms, 1024, BOTTOM_SMEM, st>>>(bt, S, sweeps, BOTTOM_SMEM);
+}
+
+void fp_launch_fcg_begin(const FpBatch& bt, int pSel, int sms, cudaStream_t st) {
+  k_fcg<FCG_BEGIN><<<sms * 4, 256, 0, st>>>(bt, pSel, 0);
+  k_converge<<<1, 256, 0, st>>>(bt, 0);
+}
+int fp_fcg_iterate_launches(int cycle) { return cycle > 1 ? 4 : 3; }
+void fp_launch_fcg_iterate(const FpBatch& bt, int zSel, int cycle, int sms, cudaStream_t st) {
+  if (cycle > 1) k_fcg<FCG_DOT><<<sms * 4, 256, 0, st>>>(bt, zSel, cycle);
+  k_fcg<FCG_DIRECTION><<<sms * 4, 256, 0, st>>>(bt, zSel, cycle);
+  k_fcg<FCG_UPDATE><<<sms * 4, 256, 0, st>>>(bt, -1, cycle);
   k_converge<<<1, 256, 0, st>>>(bt, cycle);
 }

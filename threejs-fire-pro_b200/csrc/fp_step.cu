@@ -1137,8 +1137,11 @@ __global__ void __launch_bounds__(THREADS) k_post_divergence(FpBatch bt) {
       if (!interior) continue;
       float u0 = P.velP[(slot * 3 + 0) * N + c], u1 = P.velP[(slot * 3 + 1) * N + c],
             u2 = P.velP[(slot * 3 + 2) * N + c];
+      // What the projection drives to zero: h (div u - expansion), the expansion rate the cell's
+      // mean on the field lattice as computeDivergence subtracts it (fluid-forces.wgsl:184-203).
+      const float ex = P.velDiv == 1 ? P.expn[slot * N + c] : fieldAverage(*P.fview, H, P.expn, 1, 0, x, y, z, false);
       float d = (u0 - cellAt(P, H, P.velP, 3, 0, x - 1, y, z)) + (u1 - cellAt(P, H, P.velP, 3, 1, x, y - 1, z)) +
-                (u2 - cellAt(P, H, P.velP, 3, 2, x, y, z - 1));
+                (u2 - cellAt(P, H, P.velP, 3, 2, x, y, z - 1)) - P.h * ex;
       d2 += (double)d * (double)d;
       v2 += (double)u0 * u0 + (double)u1 * u1 + (double)u2 * u2;
     }

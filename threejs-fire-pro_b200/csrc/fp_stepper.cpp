@@ -185,6 +185,12 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
       error_ = who(i) + "velocity divisor differs from the batch's";
       return done(FP_EINVAL);
     }
+  // One launch runs one pressure-solve schedule.
+  for (int i = 1; i < count; i++)
+    if (std::memcmp(&sims[i]->schedule(), &sims[0]->schedule(), sizeof(fp_solver_schedule)) != 0) {
+      error_ = who(i) + "solver schedule differs from the batch's";
+      return done(FP_EINVAL);
+    }
   for (int i = 0; i < count; i++)
     if ((rc = sims[i]->validate(*frames[i], dts[i]))) {
       error_ = who(i) + sims[i]->error();
@@ -217,6 +223,7 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
   uint32_t blocks = 0, tiles = 0, ids = 0;
   size_t word = 0;
   bool solidsFresh = false, solidsAll = false, topoAll = false, curl = false, measure = false;
+  schedule_ = sims[0]->schedule();
   int vcycles = 1;
   fusedCoarse_ = true;
   anySmoke_ = false;
@@ -260,7 +267,10 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
   } else {
     uint64_t key = (uint64_t)solidsFresh | ((uint64_t)solidsAll << 1) | ((uint64_t)topoAll << 2) | ((uint64_t)curl << 3) |
                    ((uint64_t)measure << 4) | ((uint64_t)vcycles << 5) | ((uint64_t)fusedCoarse_ << 16) |
-                   ((uint64_t)anySmoke_ << 17);
+                   ((uint64_t)anySmoke_ << 17) | ((uint64_t)schedule_.smoother << 18) |
+                   ((uint64_t)schedule_.krylov << 19) | ((uint64_t)schedule_.levels << 20) |
+                   ((uint64_t)schedule_.pre_sweeps << 24) | ((uint64_t)schedule_.post_sweeps << 28) |
+                   ((uint64_t)schedule_.bottom_sweeps << 32);
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
       GraphEntry ge{};
@@ -357,7 +367,7 @@ void Stepper::vcycle(int level, int cur[], uint64_t& launches) {
   }
   auto relax = [&](int n) {
     for (int i = 0; i < n; i++) {
-      MgSel S{level, sel(level, 2), sel(level, cur[level]), -1, sel(level, 1 - cur[level]), -1, cycle_};
+      MgSel S{level, level == 0 ? rhs0Sel_ : sel(level, 2), sel(level, cur[level]), -1, sel(level, 1 - cur[level]), -1, cycle_};
       fp_launch_relax(batch(), S, tiles, B_ / vd_, sms_, stream_);
       launches++;
       cur[level] = 1 - cur[level];
@@ -365,7 +375,7 @@ void Stepper::vcycle(int level, int cur[], uint64_t& launches) {
   };
   if (level > 0) relax(2);
   int coarse = level + 1;
-  MgSel R{coarse, sel(level, 2), sel(level, cur[level]), -1, sel(coarse, 2), sel(coarse, 1), cycle_};
+  MgSel R{coarse, level == 0 ? rhs0Sel_ : sel(level, 2), sel(level, cur[level]), -1, sel(coarse, 2), sel(coarse, 1), cycle_};
   fp_launch_restrict(batch(), R, coarse >= brickLevels_, B_ / vd_, sms_, stream_);
   launches++;
   cur[coarse] = 1;
@@ -375,6 +385,51 @@ void Stepper::vcycle(int level, int cur[], uint64_t& launches) {
   launches++;
   cur[level] = 1 - cur[level];
   relax(3);
+}
+
+// One V-cycle of the red-black schedule (fp_solver_schedule) from `level` down: every level in
+// place in its first buffer, `pre_sweeps` before each restriction, the coarse level from zero,
+// prolongation in place, `post_sweeps` (odd cells first) after it; the coarsest of the
+// schedule's levels takes `bottom_sweeps` (the bottom level in one CTA per simulation). The
+// restriction's first iterate of the coarse level goes to its second buffer, unused.
+void Stepper::vcycleRB(int level, bool zero, uint64_t& launches) {
+  auto sel = [](int l, int which) { return fp_mg_sel(l, which); };
+  const fp_solver_schedule& sc = schedule_;
+  const int coarsest = sc.levels > 0 ? std::min(sc.levels - 1, bottom_) : bottom_;
+  const bool tiles = level >= brickLevels_;
+  const int rhs = level == 0 ? rhs0Sel_ : sel(level, 2), buf = sel(level, 0);
+  auto half = [&](int parity, bool fromZero) {
+    MgSel S{level, rhs, fromZero ? -1 : buf, -1, buf, -1, cycle_, parity + 1};
+    fp_launch_relax(batch(), S, tiles, B_ / vd_, sms_, stream_);
+    launches++;
+  };
+  auto sweeps = [&](int n, bool fromZero, bool post) {
+    for (int i = 0; i < n; i++) {
+      const int first = post ? 1 : 0;
+      half(first, fromZero && i == 0);
+      half(1 - first, false);
+    }
+  };
+  if (level == coarsest) {
+    if (level == bottom_) {
+      MgSel S{level, rhs, zero ? -1 : buf, -1, buf, -1, cycle_, 1};
+      fp_launch_bottom_rb(batch(), S, sc.bottom_sweeps, sms_, stream_);
+      launches++;
+    } else {
+      sweeps(sc.bottom_sweeps, zero, false);
+    }
+    return;
+  }
+  sweeps(sc.pre_sweeps, zero, false);
+  const int coarse = level + 1;
+  MgSel R{coarse, rhs, buf, -1, sel(coarse, 2), sel(coarse, 1), cycle_, 0};
+  fp_launch_restrict(batch(), R, coarse >= brickLevels_, B_ / vd_, sms_, stream_);
+  launches++;
+  vcycleRB(coarse, true, launches);
+  MgSel Pr{level, -1, buf, sel(coarse, 0), buf, -1, cycle_, 0};
+  fp_launch_prolong(batch(), Pr, tiles, B_ / vd_, sms_, stream_);
+  launches++;
+  sweeps(sc.post_sweeps, false, true);
 }
 
 // The step's kernels, measurement and its event, enqueued on the stream (eagerly, or under
@@ -437,22 +492,72 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   cur[0] = 1;
   phaseBegin(PH_MULTIGRID);
   uint64_t mg = 0;
-  // Up to `vcycles` V-cycles. Each leaves the finest level's result in the buffer it started
-  // from (four flips: prolongation and three sweeps), so a simulation that converged and skips
-  // the later cycles ends in the same buffer. After each cycle, when measured, the FP64
-  // residual decides convergence.
-  for (int c = 0; c < vcycles; c++) {
-    cycle_ = c;
-    vcycle(0, cur, mg);
-    if (vcycles > 1 || measure) {
-      fp_launch_residual(bt, cur[0], c, sms_, stream_);
-      mg += 2;
+  rhs0Sel_ = fp_mg_sel(0, 2);
+  const bool redBlack = schedule_.smoother == FP_SMOOTHER_REDBLACK;
+  if (schedule_.krylov == FP_KRYLOV_FCG) {
+    // Flexible CG: V-cycle 0 from the divergence gives the start x (the CG iterate, p0[2]);
+    // each later V-cycle, from zero on the residual s (level 0's selector 3), gives z, the next
+    // direction and step. Simulations that converged skip the later cycles' work.
+    cycle_ = 0;
+    int x0 = 0;
+    if (redBlack) {
+      vcycleRB(0, true, mg);
+    } else {
+      vcycle(0, cur, mg);
+      x0 = cur[0];
     }
+    fp_launch_fcg_begin(bt, x0, sms_, stream_);
+    mg += 2;
+    rhs0Sel_ = fp_mg_sel(0, 3);
+    for (int c = 1; c < vcycles; c++) {
+      cycle_ = c;
+      int z = 0;
+      if (redBlack) {
+        vcycleRB(0, true, mg);
+      } else {
+        // The first iterate from zero (as the divergence kernel writes it for V-cycle 0).
+        MgSel S{0, rhs0Sel_, -1, -1, fp_mg_sel(0, 1), -1, cycle_, 0};
+        fp_launch_relax(bt, S, false, B_ / vd_, sms_, stream_);
+        mg++;
+        cur[0] = 1;
+        vcycle(0, cur, mg);
+        z = cur[0];
+      }
+      fp_launch_fcg_iterate(bt, z, c, sms_, stream_);
+      mg += fp_fcg_iterate_launches(c);
+    }
+    rhs0Sel_ = fp_mg_sel(0, 2);
+    latest = 2;
+  } else if (redBlack) {
+    // In place in p0[0]; a later V-cycle corrects the current iterate (a converged simulation
+    // skips it and keeps its result in the same buffer).
+    for (int c = 0; c < vcycles; c++) {
+      cycle_ = c;
+      vcycleRB(0, c == 0, mg);
+      if (vcycles > 1 || measure) {
+        fp_launch_residual(bt, 0, c, sms_, stream_);
+        mg += 2;
+      }
+    }
+    latest = 0;
+  } else {
+    // Up to `vcycles` V-cycles. Each leaves the finest level's result in the buffer it started
+    // from (four flips: prolongation and three sweeps), so a simulation that converged and
+    // skips the later cycles ends in the same buffer. After each cycle, when measured, the
+    // FP64 residual decides convergence.
+    for (int c = 0; c < vcycles; c++) {
+      cycle_ = c;
+      vcycle(0, cur, mg);
+      if (vcycles > 1 || measure) {
+        fp_launch_residual(bt, cur[0], c, sms_, stream_);
+        mg += 2;
+      }
+    }
+    latest = cur[0];
   }
   cycle_ = 0;
   launches += mg;
   phaseEnd(PH_MULTIGRID, (int)mg);
-  latest = cur[0];
   phaseBegin(PH_PROJECT);
   fp_launch_project(bt, latest, vd_, sms_, stream_);
   launches++;

@@ -102,6 +102,8 @@ struct FpSolver {
   int converged;                // the latest norm met the tolerance: later cycles skip
   int measured;                 // the post-projection divergence was measured
   int pad;
+  // flexible CG, per V-cycle: z.q (new preconditioned residual against the old A d), d.q, d.s
+  double zq[FP_MAX_VCYCLES], dq[FP_MAX_VCYCLES], ds[FP_MAX_VCYCLES];
 };
 
 struct SimParams {
@@ -183,8 +185,11 @@ struct SimParams {
   float* smkB;
   uint32_t* solids;
   // multigrid
-  float* p0[2];
+  float* p0[3];  // the finest level's pair, then the CG iterate (null without CG)
   int latest;  // p0 index of the previous solution
+  // flexible CG on the finest level (FP_KRYLOV_FCG, null without): the residual rhs + A x, the
+  // search direction d and A d
+  float* kry[3];
   // storage precision (FP_PRECISION_MIXED): the scalar pools fld/fldP/fldN hold __half, the
   // multigrid levels above 0 (lp, lrhs) __nv_bfloat16; everything else FP32
   int scalarHalf, coarseBf16;

@@ -230,6 +230,22 @@ class fp_solver_stats(C.Structure):
     ]
 
 
+FP_SMOOTHER_JACOBI = 0
+FP_SMOOTHER_REDBLACK = 1
+FP_KRYLOV_NONE = 0
+FP_KRYLOV_FCG = 1
+
+
+class fp_solver_schedule(C.Structure):
+    _fields_ = [("smoother", C.c_int32), ("levels", C.c_int32), ("pre_sweeps", C.c_int32),
+                ("post_sweeps", C.c_int32), ("bottom_sweeps", C.c_int32), ("krylov", C.c_int32)]
+
+
+def schedule(smoother=FP_SMOOTHER_JACOBI, levels=0, pre=2, post=2, bottom=8, krylov=FP_KRYLOV_NONE):
+    """An fp_solver_schedule; the default is the reference's Jacobi V-cycle."""
+    return fp_solver_schedule(smoother, levels, pre, post, bottom, krylov)
+
+
 class fp_phase(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_uint64), ("ms", C.c_double), ("voxels", C.c_double)]
 
@@ -314,11 +330,13 @@ SIGNATURES = {
     "fp_grid_reserved_tiles": (C.c_int, [C.POINTER(fp_grid), C.POINTER(C.c_uint32)]),
     "fp_sim_reserve_tiles": (C.c_int, [C.c_void_p, C.c_uint32]),
     "fp_sim_set_solver": (C.c_int, [C.c_void_p, C.c_int, C.c_float]),
+    "fp_sim_set_schedule": (C.c_int, [C.c_void_p, C.c_void_p]),
     "fp_sim_render": (C.c_int, [C.c_void_p, C.POINTER(fp_camera), C.POINTER(fp_render_settings), C.c_void_p]),
     "fp_sim_render_device": (C.c_int, [C.c_void_p, C.POINTER(fp_camera), C.POINTER(fp_render_settings), C.c_void_p]),
     "fp_sim_collect_lights": (C.c_int, [C.c_void_p, C.POINTER(fp_render_settings), C.c_void_p, C.c_uint32, C.c_void_p]),
     "fp_sim_read_solver": (C.c_int, [C.c_void_p, C.POINTER(fp_solver_stats)]),
     "fp_batch_set_solver": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_float]),
+    "fp_batch_set_schedule": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
     "fp_batch_read_solver": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(fp_solver_stats)]),
     "fp_batch_reserve_tiles": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "fp_server_last_error": (C.c_char_p, [C.c_void_p]),

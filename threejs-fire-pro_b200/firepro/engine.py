@@ -64,6 +64,10 @@ class FluidSimulation:
         """Up to `vcycles` V-cycles a step, stopping at relative residual `tolerance` (0: all)."""
         self._check(self.lib.fp_sim_set_solver(self.h, vcycles, tolerance))
 
+    def set_schedule(self, schedule: abi.fp_solver_schedule):
+        """The pressure solve's smoother, levels, sweeps and Krylov wrapper (fp_sim_set_schedule)."""
+        self._check(self.lib.fp_sim_set_schedule(self.h, C.byref(schedule)))
+
     def render(self, camera: abi.fp_camera, settings: abi.fp_render_settings) -> np.ndarray:
         """The latest state rendered: (height, width, 4) linear radiance and opacity."""
         out = np.zeros((camera.height, camera.width, 4), np.float32)
@@ -195,6 +199,9 @@ class SimulationBatch:
 
     def set_solver(self, sim: int, vcycles: int, tolerance: float = 0.0):
         self._check(self.lib.fp_batch_set_solver(self.h, sim, vcycles, tolerance))
+
+    def set_schedule(self, sim: int, schedule: abi.fp_solver_schedule):
+        self._check(self.lib.fp_batch_set_schedule(self.h, sim, C.byref(schedule)))
 
     def read_solver(self, sim: int) -> abi.fp_solver_stats:
         s = abi.fp_solver_stats()
