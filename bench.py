@@ -370,29 +370,47 @@ def served_form(local: int, sessions: int = 64, grow: int = 90, ticks: int = 300
     }
 
 
-def precision_form(local: int, steps: int = 30, vcycles: int = 8, tolerance: float = 1e-4) -> dict:
-    """The large scene in plain FP32 and in FP_PRECISION_MIXED (FP16 scalar state, BF16 coarse
-    multigrid, FP32 defect correction), both solving the pressure to the same FP64-measured
-    relative residual (at most `vcycles` V-cycles): device time per step on the simulation's
-    stream, the V-cycles run and the projected velocity's divergence, from the same grown
-    state size."""
+# The accurate solve every form that compares at equal accuracy uses: flexible CG around a
+# red-black V-cycle on every level (2 + 2 sweeps, 8 at the bottom), to a relative residual of
+# 1e-6 in at most 16 V-cycles, which holds post-projection divergence under 1e-4 of the velocity
+# on the large scene at the benchmark's size.
+ACCURATE = {"smoother": 1, "levels": 0, "pre": 2, "post": 2, "bottom": 8, "krylov": 1, "vcycles": 16, "tolerance": 1e-6}
+
+
+def accurate_schedule():
+    from firepro import abi
+
+    a = ACCURATE
+    return abi.schedule(a["smoother"], a["levels"], a["pre"], a["post"], a["bottom"], a["krylov"])
+
+
+def precision_form(local: int, steps: int = 30) -> dict:
+    """The large scene grown GROW_STEPS steps, then timed `steps` steps: plain FP32 storage and
+    FP_PRECISION_MIXED (FP16 scalar state, BF16 coarse multigrid, FP32 finest level and CG), both
+    with the accurate solve; and the reference's single V-cycle in FP32 for comparison. Device
+    time per step on the simulation's stream, V-cycles, the worst post-projection divergence
+    (h (div u - e) / u, RMS) over the timed steps."""
     import torch
 
     from firepro import abi, scenes
     from firepro.engine import FluidSimulation
 
-    out = {"solver": {"vcycles": vcycles, "tolerance": tolerance}}
-    for name, precision in (("fp32", abi.FP_PRECISION_FP32), ("mixed", abi.FP_PRECISION_MIXED)):
+    out = {"solver": dict(ACCURATE, name="FCG(red-black V-cycle)")}
+    runs = (("fp32", abi.FP_PRECISION_FP32, True), ("mixed", abi.FP_PRECISION_MIXED, True),
+            ("fp32_reference_vcycle", abi.FP_PRECISION_FP32, False))
+    for name, precision, accurate in runs:
         sc = scenes.LargeScene(seed=1)
         sim = FluidSimulation(sc.grid(budget=BUDGET, precision=precision), device=local)
         sim.set_runtime(0.05, BUDGET, True)
-        sim.set_solver(vcycles, tolerance)
         step = 0
-        while step < MAX_GROW_STEPS:
+        while step < GROW_STEPS:
             sim.step(sc.frame(step).frame)
             step += 1
-            if step % 25 == 0 and sim.stats().active_bricks >= TARGET_BRICKS:
-                break
+        if accurate:
+            sim.set_schedule(accurate_schedule())
+            sim.set_solver(ACCURATE["vcycles"], ACCURATE["tolerance"])
+        else:
+            sim.set_solver(1, 1e-30)  # one V-cycle, measured
         for _ in range(3):
             sim.step(sc.frame(step).frame)
             step += 1
@@ -408,15 +426,61 @@ def precision_form(local: int, steps: int = 30, vcycles: int = 8, tolerance: flo
         ev[1].record(stream)
         sim.synchronize()
         ms = ev[0].elapsed_time(ev[1])
-        sol = sim.read_solver()
+        # The solve's accuracy over more steps, each read back (untimed).
+        for k in range(10):
+            sim.step(sc.frame(step).frame)
+            step += 1
+            sol = sim.read_solver()
+            cycles.append(int(sol.vcycles))
+            div.append(sol.divergence)
         st = sim.stats()
         out[name] = {"value": sum(actives) * BRICK_VOXELS / (ms / 1e3), "ms_per_step": ms / steps,
-                     "mean_active_bricks": sum(actives) / len(actives), "vcycles_last": sol.vcycles,
-                     "residual_last": sol.residual[max(0, sol.vcycles - 1)], "divergence_last": sol.divergence,
+                     "mean_active_bricks": sum(actives) / len(actives), "vcycles": cycles,
+                     "residual_last": sol.residual[max(0, sol.vcycles - 1)], "divergence_max": max(div),
                      "memory_bytes": st.memory_bytes}
         sim.dispose()
-    out["speedup"] = out["mixed"]["value"] / out["fp32"]["value"]
+    out["speedup_mixed_vs_fp32"] = out["mixed"]["value"] / out["fp32"]["value"]
     out["unit"] = "voxel-steps/s"
+    return out
+
+
+def serving_forms(local: int, wall: float = 20.0) -> dict:
+    """The serving workload (Poisson arrivals at 20 sessions/s, budgets log-uniform 32-8192
+    bricks, lifetimes 5-60 s of simulated time, 60 Hz step requests, at most 256 live sessions,
+    150 GB admission cap), every arm with the accurate solve: served + mixed precision, served +
+    FP32, and the plain FP32 drop-in (one FluidSimulation per session, one fp_sim_step call
+    each). Voxel-steps/s and latency over the second half of `wall` seconds. Then the served +
+    mixed capacity sweep: N sessions open from the start (budgets 32-8192), 60 Hz each, until
+    p99 passes 16 ms, and the p99 at 64 live sessions."""
+    from firepro import abi, scenes, workloads
+
+    sched, vc, tol = accurate_schedule(), ACCURATE["vcycles"], ACCURATE["tolerance"]
+    trace = workloads.serving_trace(seed=1, rate=20.0, duration=wall)
+    out = {"workload": f"Poisson arrivals 20/s over {wall:.0f} s ({len(trace)} sessions), budgets log-uniform "
+                       f"32-8192 bricks, lifetimes 5-60 s simulated, 60 Hz requests (each after the previous "
+                       f"completed), <= 256 live, 150 GB cap; solve FCG(red-black) to 1e-6; window: second half",
+           "unit": "voxel-steps/s"}
+    arms = (("served_mixed", lambda: workloads.ServerBackend(abi.FP_PRECISION_MIXED, sched, vc, tol, device=local)),
+            ("served_fp32", lambda: workloads.ServerBackend(abi.FP_PRECISION_FP32, sched, vc, tol, device=local)),
+            ("plain_fp32", lambda: workloads.PlainBackend(abi.FP_PRECISION_FP32, sched, vc, tol, device=local)))
+    for name, make in arms:
+        be = make()
+        out[name] = workloads.run_trace(be, trace, wall)
+        be.dispose()
+    out["ratio_served_mixed_vs_plain_fp32"] = out["served_mixed"]["value"] / max(1.0, out["plain_fp32"]["value"])
+    sweep = []
+    for n in (32, 64, 128, 256):
+        be = workloads.ServerBackend(abi.FP_PRECISION_MIXED, sched, vc, tol, device=local)
+        members = [scenes.MemberScene(2, k, 32, 8192) for k in range(n)]
+        r = workloads.run_fixed(be, members, wall=6.0, grow=30)
+        be.dispose()
+        r["sessions"] = n
+        sweep.append(r)
+        if r["latency_p99_ms"] is not None and r["latency_p99_ms"] > 16.0:
+            break
+    ok = [r for r in sweep if r["latency_p99_ms"] is not None and r["latency_p99_ms"] <= 16.0]
+    out["capacity_sweep"] = {"runs": sweep, "capacity_value": max((r["value"] for r in ok), default=None),
+                             "p99_at_64_ms": next((r["latency_p99_ms"] for r in sweep if r["sessions"] == 64), None)}
     return out
 
 
@@ -547,8 +611,9 @@ def run_ours(args, rank, world, local):
     }
     if world == 1 and not args.no_forms:
         line["forms"] = {"batched": batched_form(local, steps=max(10, min(args.steps, 60))),
-                         "served": served_form(local),
-                         "precision": precision_form(local)}
+                         "served_64": served_form(local),
+                         "precision": precision_form(local),
+                         "serving": serving_forms(local)}
     if world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         untimed = GROW_STEPS + args.warmup

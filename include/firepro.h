@@ -470,6 +470,10 @@ int fp_server_drain(fp_server* server, int wait_ms);
 int fp_server_read_stats(fp_server* server, fp_server_stats* out);
 /* A live session's stats (as fp_sim_stats), as of its latest measured step. */
 int fp_server_session_stats(fp_server* server, uint32_t session, fp_stats* out);
+/* The pressure solve of every session admitted from now on (as fp_sim_set_schedule and
+ * fp_sim_set_solver; by default the reference's single V-cycle). One launch runs one schedule,
+ * so set it before opening the sessions it should apply to. */
+int fp_server_set_solver(fp_server* server, const fp_solver_schedule* schedule, int vcycles, float tolerance);
 /* A live session's field (as fp_sim_read_field), between its steps. */
 int fp_server_read_field(fp_server* server, uint32_t session, int field, float* host, size_t bytes);
 

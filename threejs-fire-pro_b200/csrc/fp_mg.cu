@@ -837,7 +837,7 @@ __global__ void __launch_bounds__(256) k_residual(FpBatch bt, int pSel, int cycl
 // the bottom level (one cell a tile) in place, every sweep the even tiles (x + y + z) then the
 // odd ones, in one CTA per simulation. Same cell arithmetic as relaxCell's red-black branch;
 // each value is rounded as the level's storage rounds it. With S.pin -1 the level starts from
-// zero. Shared memory by live tile when 20 bytes a tile fit, else in place in global memory.
+// zero. Shared memory by live tile when 24 bytes a tile fit, else in place in global memory.
 __global__ void __launch_bounds__(1024) k_bottom_rb(FpBatch bt, MgSel Sl, int sweeps, int smemBytes) {
   extern __shared__ float bottomSmem[];
   const int nbIndex[6] = {nbrIndex(1, 0, 0), nbrIndex(-1, 0, 0), nbrIndex(0, 1, 0),
@@ -856,7 +856,7 @@ __global__ void __launch_bounds__(1024) k_bottom_rb(FpBatch bt, MgSel Sl, int sw
       uint32_t f = activeCell(P, H, rec.x, rec.y, rec.z, level) ? expandFlags(P.topo[level][t]) : SOLIDF;
       return f | (((rec.x + rec.y + rec.z) & 1) ? ODD : 0u);
     };
-    if ((long)L * 20 <= (long)smemBytes) {
+    if ((long)L * 24 <= (long)smemBytes) {
       float* cur = bottomSmem;
       float* rhs = cur + L;
       uint32_t* flags = reinterpret_cast<uint32_t*>(rhs + L);

@@ -74,6 +74,9 @@ struct Session {
   fp_grid grid;
   float cutoff;
   int ground;
+  fp_solver_schedule schedule;  // the server's solve when the session opened
+  int vcycles;
+  float tolerance;
   int state = FP_SESSION_WAITING;
   fp::Engine* engine = nullptr;
   uint64_t bytes = 0;
@@ -97,6 +100,9 @@ struct fp_server {
   uint64_t memory = 0;
   uint32_t live = 0;
   int velocityDivisor = 0;  // the sessions' velocity divisor, from the first one opened
+  fp_solver_schedule schedule{};  // the pressure solve of sessions admitted from now on
+  int vcycles = 1;
+  float tolerance = 0.f;
   uint64_t nextTicket = 1;
   uint64_t queued = 0, inFlight = 0;
   std::deque<fp_completion> completed;
@@ -233,6 +239,8 @@ void schedule(fp_server* S) {
       // Tables sized for the budget up front: no step of the batch stops to grow them.
       int cells = s->grid.brick_size * s->grid.brick_size * s->grid.brick_size;
       if (!rc) rc = e->reserveTiles(fp::Engine::tilesForBudget(s->grid.voxel_budget, cells));
+      if (!rc) rc = e->setSchedule(s->schedule);
+      if (!rc) rc = e->setSolver(s->vcycles, s->tolerance);
       std::lock_guard<std::mutex> lk(S->mu);
       if (rc) {
         S->error = e ? e->error() : "out of host memory";
@@ -418,6 +426,9 @@ int fp_server_open(fp_server* S, const fp_grid* grid, float cutoff, int ground, 
   s->bytes = bytes;
   {
     std::lock_guard<std::mutex> lk(S->mu);
+    s->schedule = S->schedule;
+    s->vcycles = S->vcycles;
+    s->tolerance = S->tolerance;
     uint32_t id = 0;
     while (id < S->sessions.size() && S->sessions[id]) id++;
     if (id == S->sessions.size()) S->sessions.push_back(nullptr);
@@ -426,6 +437,26 @@ int fp_server_open(fp_server* S, const fp_grid* grid, float cutoff, int ground, 
     *session = id;
   }
   S->work.notify_all();
+  return FP_OK;
+}
+
+int fp_server_set_solver(fp_server* S, const fp_solver_schedule* schedule, int vcycles, float tolerance) {
+  if (!S || !schedule) return fp_set_error(FP_EINVAL, "fp_server_set_solver needs a server and a schedule.");
+  if (schedule->smoother != FP_SMOOTHER_JACOBI && schedule->smoother != FP_SMOOTHER_REDBLACK)
+    return serverFail(S, FP_EINVAL, "smoother must be FP_SMOOTHER_JACOBI or FP_SMOOTHER_REDBLACK.");
+  if (schedule->krylov != FP_KRYLOV_NONE && schedule->krylov != FP_KRYLOV_FCG)
+    return serverFail(S, FP_EINVAL, "krylov must be FP_KRYLOV_NONE or FP_KRYLOV_FCG.");
+  if (vcycles < 1 || vcycles > FP_MAX_VCYCLES)
+    return serverFail(S, FP_EINVAL, "vcycles must be from 1 to " + std::to_string(FP_MAX_VCYCLES) + ".");
+  if (!std::isfinite(tolerance) || tolerance < 0.f)
+    return serverFail(S, FP_EINVAL, "tolerance must be finite and nonnegative.");
+  // The red-black limits are checked per session at admission (they depend on its levels).
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->schedule = *schedule;
+  if (schedule->smoother == FP_SMOOTHER_JACOBI)
+    S->schedule.levels = S->schedule.pre_sweeps = S->schedule.post_sweeps = S->schedule.bottom_sweeps = 0;
+  S->vcycles = vcycles;
+  S->tolerance = tolerance;
   return FP_OK;
 }
 

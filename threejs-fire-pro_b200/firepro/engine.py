@@ -312,6 +312,10 @@ class FireServer:
         self._check(self.lib.fp_server_open(self.h, C.byref(grid), cutoff, int(ground), C.byref(out)))
         return out.value
 
+    def set_solver(self, schedule: abi.fp_solver_schedule, vcycles: int = 1, tolerance: float = 0.0):
+        """The pressure solve of the sessions opened from now on (fp_server_set_solver)."""
+        self._check(self.lib.fp_server_set_solver(self.h, C.byref(schedule), vcycles, tolerance))
+
     def close(self, session: int):
         self._check(self.lib.fp_server_close(self.h, session))
 
