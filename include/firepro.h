@@ -358,6 +358,18 @@ int fp_sim_read_table(fp_sim* sim, int table, void* host, size_t* bytes);
  * bricks that hold a slot, six floats each (min xyz, max xyz). `*count` in: capacity in
  * boxes, out: boxes written (or needed, with FP_ELIMIT). */
 int fp_sim_read_bricks(fp_sim* sim, float* boxes, uint32_t* count);
+/* Session snapshot and restore (no reference counterpart: the reference's document,
+ * editor/document.ts:60-61, saves settings, not state). `fp_sim_snapshot` waits for the
+ * simulation's work and copies its whole state between steps (host tables, device pools,
+ * tables and multigrid levels) into one blob the library allocates in host memory:
+ * `*blob` and `*bytes` receive it; release it with fp_snapshot_free. `fp_sim_restore` puts
+ * a blob back into a simulation of the same grid (another simulation, another device, or the
+ * same one rewound); the restored simulation then steps bit for bit as the original would
+ * have. A blob of another grid, truncated or inconsistent is FP_EINVAL and changes nothing.
+ * The blob is for this library build on this host architecture only. */
+int fp_sim_snapshot(fp_sim* sim, void** blob, size_t* bytes);
+int fp_sim_restore(fp_sim* sim, const void* blob, size_t bytes);
+void fp_snapshot_free(void* blob);
 /* The cudaStream_t the simulation enqueues on, for callers that order their own work after
  * it or record events against it. No reference counterpart: WebGPU has one queue. */
 int fp_sim_stream(fp_sim* sim, void** stream);
@@ -470,6 +482,12 @@ int fp_server_drain(fp_server* server, int wait_ms);
 int fp_server_read_stats(fp_server* server, fp_server_stats* out);
 /* A live session's stats (as fp_sim_stats), as of its latest measured step. */
 int fp_server_session_stats(fp_server* server, uint32_t session, fp_stats* out);
+/* A live session's snapshot (as fp_sim_snapshot) once its queued steps have run (FP_EINVAL
+ * while any is queued or running), and a snapshot restored into a live session of the same
+ * grid with no steps queued: a server evicts a session to host memory by snapshot and close,
+ * and brings it back by open and restore. */
+int fp_server_snapshot(fp_server* server, uint32_t session, void** blob, size_t* bytes);
+int fp_server_restore(fp_server* server, uint32_t session, const void* blob, size_t bytes);
 /* The pressure solve of every session admitted from now on (as fp_sim_set_schedule and
  * fp_sim_set_solver; by default the reference's single V-cycle). One launch runs one schedule,
  * so set it before opening the sessions it should apply to. */

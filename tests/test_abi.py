@@ -14,7 +14,7 @@ HEADER = ROOT / "include" / "firepro.h"
 
 def declared_functions():
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(fp_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|void|const char\*)\s+(fp_\w+)\s*\(", text, re.M)))
 
 
 def test_library_exports_every_declared_function(cuda_lib_path):

@@ -3,6 +3,8 @@
 // across the ABI. A single simulation is an Engine stepped by a Stepper of its own; a batch
 // shares one Stepper among many Engines.
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <memory>
 #include <new>
 #include <string>
@@ -201,6 +203,30 @@ int fp_sim_read_table(fp_sim* sim, int table, void* host, size_t* bytes) {
   if (!sim || !bytes) return failed("fp_sim_read_table needs a simulation and a size.", FP_EINVAL);
   return sim->engine->readTable(table, host, bytes);
 }
+
+// A snapshot blob in malloc'd host memory for the caller (fp_snapshot_free releases it).
+static int handOut(std::vector<uint8_t>& v, void** blob, size_t* bytes) {
+  void* p = std::malloc(v.size() ? v.size() : 1);
+  if (!p) return failed("out of host memory for the snapshot", FP_ENOMEM);
+  std::memcpy(p, v.data(), v.size());
+  *blob = p;
+  *bytes = v.size();
+  return FP_OK;
+}
+
+int fp_sim_snapshot(fp_sim* sim, void** blob, size_t* bytes) {
+  if (!sim || !blob || !bytes) return failed("fp_sim_snapshot needs a simulation and outputs.", FP_EINVAL);
+  std::vector<uint8_t> v;
+  int rc = sim->engine->snapshot(v);
+  return rc ? rc : handOut(v, blob, bytes);
+}
+
+int fp_sim_restore(fp_sim* sim, const void* blob, size_t bytes) {
+  if (!sim || !blob) return failed("fp_sim_restore needs a simulation and a snapshot.", FP_EINVAL);
+  return sim->engine->restore(static_cast<const uint8_t*>(blob), bytes);
+}
+
+void fp_snapshot_free(void* blob) { std::free(blob); }
 
 int fp_sim_read_bricks(fp_sim* sim, float* boxes, uint32_t* count) {
   if (!sim || !count) return failed("fp_sim_read_bricks needs a simulation and a count.", FP_EINVAL);

@@ -24,7 +24,11 @@ namespace fp {
 
 // The directory of tiles (TileDirectory.ts:61-186): 4x4x4 bricks each, created around
 // sources and content, lingering 60 steps after nothing needs them, slots reused lowest first.
+class Engine;
+
 class TileDirectory {
+  friend class Engine;  // a snapshot saves and restores the directory whole
+
  public:
   struct Tile {
     int x, y, z;
@@ -110,6 +114,10 @@ class Engine {
   // `vcycles` V-cycles a step, stopping at a relative FP64 residual of `tolerance` (0: all).
   int setSolver(int vcycles, float tolerance);
   int readSolver(fp_solver_stats* out);
+  // The whole state between steps, host and device, as one blob (fp_sim_snapshot), and back
+  // into a simulation of the same grid (fp_sim_restore).
+  int snapshot(std::vector<uint8_t>& out);
+  int restore(const uint8_t* data, size_t bytes);
   // The solve's smoother, levels, sweeps and Krylov wrapper (fp_sim_set_schedule).
   int setSchedule(const fp_solver_schedule& schedule);
   const fp_solver_schedule& schedule() const { return schedule_; }

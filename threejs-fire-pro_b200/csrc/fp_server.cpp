@@ -13,6 +13,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <mutex>
@@ -81,6 +82,7 @@ struct Session {
   fp::Engine* engine = nullptr;
   uint64_t bytes = 0;
   uint64_t steps = 0;
+  int inflight = 0;  // steps launched and not yet completed
   std::deque<Request*> queue;
 };
 
@@ -151,6 +153,7 @@ void CUDART_CB onLaunchDone(void* p) {
       S->voxelSteps += (double)c->active * L->cells;
       S->stepsDone++;
       S->inFlight--;
+      S->sessions[r->session]->inflight--;
       delete r;
     }
   }
@@ -170,6 +173,7 @@ void failRequests(fp_server* S, std::vector<Request*>& reqs, int status) {
     out.done_ms = t;
     S->completed.push_back(out);
     S->inFlight--;
+    S->sessions[r->session]->inflight--;
     delete r;
   }
   reqs.clear();
@@ -217,6 +221,7 @@ void schedule(fp_server* S) {
       for (Session* s : S->sessions)
         if (s && s->state == FP_SESSION_LIVE && !s->queue.empty()) {
           reqs.push_back(s->queue.front());
+          s->inflight++;
           s->queue.pop_front();
           S->queued--;
           S->inFlight++;
@@ -586,6 +591,22 @@ int fp_server_read_stats(fp_server* S, fp_server_stats* out) {
   return FP_OK;
 }
 
+// A live session with no step queued or in flight: its Engine, with the GPU lock held by the
+// caller (the scheduler only touches an Engine under that lock).
+static fp::Engine* idleEngine(fp_server* S, uint32_t session, std::string& why) {
+  std::lock_guard<std::mutex> lk(S->mu);
+  Session* s = sessionOf(S, session);
+  if (!s || s->state != FP_SESSION_LIVE || !s->engine) {
+    why = "session " + std::to_string(session) + " is not live";
+    return nullptr;
+  }
+  if (!s->queue.empty() || s->inflight) {
+    why = "session " + std::to_string(session) + " has steps queued or running";
+    return nullptr;
+  }
+  return s->engine;
+}
+
 // A live session's Engine, looked up with the GPU lock held (the scheduler deletes the Engines
 // of closed sessions under it, and takes the GPU lock before the session lock, as here).
 static fp::Engine* liveEngine(fp_server* S, uint32_t session) {
@@ -603,6 +624,40 @@ int fp_server_session_stats(fp_server* S, uint32_t session, fp_stats* out) {
     return serverFail(S, FP_EINVAL, "session " + std::to_string(session) + " is not live");
   }
   int rc = e->stats(out);
+  if (rc) return serverFail(S, rc, e->error());
+  return FP_OK;
+}
+
+int fp_server_snapshot(fp_server* S, uint32_t session, void** blob, size_t* bytes) {
+  if (!S || !blob || !bytes) return fp_set_error(FP_EINVAL, "fp_server_snapshot needs a server and outputs.");
+  std::unique_lock<std::mutex> g(S->gpu);
+  std::string why;
+  fp::Engine* e = idleEngine(S, session, why);
+  if (!e) {
+    g.unlock();
+    return serverFail(S, FP_EINVAL, why);
+  }
+  std::vector<uint8_t> v;
+  int rc = e->snapshot(v);
+  if (rc) return serverFail(S, rc, e->error());
+  void* p = std::malloc(v.size() ? v.size() : 1);
+  if (!p) return serverFail(S, FP_ENOMEM, "out of host memory for the snapshot");
+  std::memcpy(p, v.data(), v.size());
+  *blob = p;
+  *bytes = v.size();
+  return FP_OK;
+}
+
+int fp_server_restore(fp_server* S, uint32_t session, const void* blob, size_t bytes) {
+  if (!S || !blob) return fp_set_error(FP_EINVAL, "fp_server_restore needs a server and a snapshot.");
+  std::unique_lock<std::mutex> g(S->gpu);
+  std::string why;
+  fp::Engine* e = idleEngine(S, session, why);
+  if (!e) {
+    g.unlock();
+    return serverFail(S, FP_EINVAL, why);
+  }
+  int rc = e->restore(static_cast<const uint8_t*>(blob), bytes);
   if (rc) return serverFail(S, rc, e->error());
   return FP_OK;
 }

@@ -338,6 +338,11 @@ SIGNATURES = {
     "fp_batch_set_solver": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_float]),
     "fp_batch_set_schedule": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
     "fp_server_set_solver": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_float]),
+    "fp_sim_snapshot": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "fp_sim_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "fp_snapshot_free": (None, [C.c_void_p]),
+    "fp_server_snapshot": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "fp_server_restore": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t]),
     "fp_batch_read_solver": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(fp_solver_stats)]),
     "fp_batch_reserve_tiles": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "fp_server_last_error": (C.c_char_p, [C.c_void_p]),

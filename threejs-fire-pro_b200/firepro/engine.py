@@ -68,6 +68,19 @@ class FluidSimulation:
         """The pressure solve's smoother, levels, sweeps and Krylov wrapper (fp_sim_set_schedule)."""
         self._check(self.lib.fp_sim_set_schedule(self.h, C.byref(schedule)))
 
+    def snapshot(self) -> bytes:
+        """The whole state between steps as bytes (fp_sim_snapshot)."""
+        p, n = C.c_void_p(), C.c_size_t()
+        self._check(self.lib.fp_sim_snapshot(self.h, C.byref(p), C.byref(n)))
+        try:
+            return C.string_at(p, n.value)
+        finally:
+            self.lib.fp_snapshot_free(p)
+
+    def restore(self, blob: bytes):
+        """Put a snapshot of a simulation of the same grid back (fp_sim_restore)."""
+        self._check(self.lib.fp_sim_restore(self.h, blob, len(blob)))
+
     def render(self, camera: abi.fp_camera, settings: abi.fp_render_settings) -> np.ndarray:
         """The latest state rendered: (height, width, 4) linear radiance and opacity."""
         out = np.zeros((camera.height, camera.width, 4), np.float32)
@@ -311,6 +324,18 @@ class FireServer:
         out = C.c_uint32()
         self._check(self.lib.fp_server_open(self.h, C.byref(grid), cutoff, int(ground), C.byref(out)))
         return out.value
+
+    def snapshot(self, session: int) -> bytes:
+        """A live, idle session's state (fp_server_snapshot)."""
+        p, n = C.c_void_p(), C.c_size_t()
+        self._check(self.lib.fp_server_snapshot(self.h, session, C.byref(p), C.byref(n)))
+        try:
+            return C.string_at(p, n.value)
+        finally:
+            self.lib.fp_snapshot_free(p)
+
+    def restore(self, session: int, blob: bytes):
+        self._check(self.lib.fp_server_restore(self.h, session, blob, len(blob)))
 
     def set_solver(self, schedule: abi.fp_solver_schedule, vcycles: int = 1, tolerance: float = 0.0):
         """The pressure solve of the sessions opened from now on (fp_server_set_solver)."""
