@@ -495,6 +495,47 @@ int fp_server_set_solver(fp_server* server, const fp_solver_schedule* schedule, 
 /* A live session's field (as fp_sim_read_field), between its steps. */
 int fp_server_read_field(fp_server* server, uint32_t session, int field, float* host, size_t bytes);
 
+/* ---- Mesh colliders and mesh emitters on the GPU: the reference's host-side passes that turn
+ * a triangle mesh into what fp_frame takes (a collider's occupancy bits, an emitter's records).
+ * Arithmetic is FP64 as the reference's JavaScript numbers are. */
+typedef struct fp_mesh {
+  const float* positions;   /* vertex_count x 3: the geometry's local vertex positions */
+  uint32_t vertex_count;
+  const uint32_t* indices;  /* index_count indices, three a triangle; NULL: the vertices in threes */
+  uint32_t index_count;
+} fp_mesh;
+/* Collider.meshMask (handles.ts:299-325) with MeshCollider.voxelize (MeshCollider.ts:85-167):
+ * the occupancy of the lattice cells of `spacing` meters from the world origin whose centres the
+ * closed mesh, placed by `world` (4x4 column-major, Matrix4.elements), encloses: a box one cell
+ * beyond the mesh's transformed bounds, each column a ray along +z whose crossings' winding
+ * decides. Writes the box's first cell `lo` and `dims`; `*word_count` receives the words its
+ * bits take (one bit a cell, x fastest, fp_collider's mask layout) and, when `words` is not NULL
+ * and `*word_count` held at least that many on entry, the bits. The caller has checked the mesh
+ * as MeshCollider's constructor does (closed, consistently wound). */
+int fp_mesh_voxelize(int device, const fp_mesh* mesh, const double world[16], double spacing, int32_t lo[3],
+                     int32_t dims[3], uint32_t* words, uint32_t* word_count);
+/* A mesh emitter's surface samples as `Emitter.source` gives them (handles.ts:143-184): world
+ * positions and weights (MeshSurface, MeshSurface.ts:15-103), the mesh's surface area, the
+ * source's rates and velocity. */
+typedef struct fp_mesh_emitter {
+  const double* samples;   /* sample_count x 3 world positions */
+  const double* weights;   /* sample_count */
+  uint32_t sample_count;
+  double surface_area;
+  double flame, heat_rate, smoke_rate, fuel_rate;
+  double velocity[3];
+  double velocity_response;
+} fp_mesh_emitter;
+/* MeshSourceRasterizer.prepare (MeshSourceRasterizer.ts:64-167): every sample splats its weight
+ * x the surface area over the 8 lattice cells around it (trilinear, cells of `spacing`, divided
+ * by the mean face area); per emitter a cell's coverage is capped at 1 and scales its rates;
+ * emitters sum (the flame takes the maximum). `records` receives one fp_mesh_source per covered
+ * cell, ascending by (x, y, z) (fp_frame.mesh_sources takes them as they are); `*count` in:
+ * capacity, out: records (FP_ELIMIT and the number needed when they do not fit). The reference's
+ * limit of two million cell visits and its errors apply. */
+int fp_mesh_splat(int device, const fp_mesh_emitter* emitters, uint32_t emitter_count, double spacing,
+                  fp_mesh_source* records, uint32_t* count);
+
 /* Most ids fp_compact_ids_noalloc accepts in one call. */
 #define FP_COMPACT_MAX_IDS (1u << 22)
 

@@ -37,6 +37,11 @@ def lib():
         L.or_set_runtime.argtypes = [C.c_void_p, C.c_float, C.c_double, C.c_int]
         L.or_set_solver.argtypes = [C.c_void_p, C.c_int]
         L.or_set_schedule.argtypes = [C.c_void_p, C.c_void_p, C.c_float]
+        L.or_mesh_voxelize.restype = C.c_int64
+        L.or_mesh_voxelize.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_double,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64]
+        L.or_mesh_splat.restype = C.c_int64
+        L.or_mesh_splat.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_void_p, C.c_uint64]
         L.or_read_cg.restype = C.c_int
         L.or_read_cg.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.or_step.restype = C.c_int
@@ -174,3 +179,35 @@ def blackbody_table() -> np.ndarray:
 
 def set_threads(n: int):
     lib().or_set_threads(n)
+
+
+def mesh_voxelize(positions, indices, world, spacing: float):
+    """The oracle's Collider.meshMask + MeshCollider.voxelize: (lo, dims, words)."""
+    L = lib()
+    pos = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+    idx = None if indices is None else np.ascontiguousarray(indices, dtype=np.uint32).ravel()
+    w = np.ascontiguousarray(np.asarray(world, dtype=np.float64).ravel(order="F"))
+    lo, dims = np.zeros(3, np.int32), np.zeros(3, np.int32)
+    L.or_mesh_voxelize(pos.ctypes.data, len(pos), None if idx is None else idx.ctypes.data,
+                       0 if idx is None else len(idx), w.ctypes.data, spacing, lo.ctypes.data, dims.ctypes.data, None, 0)
+    words = np.zeros((int(np.prod(dims.astype(np.int64))) + 31) // 32, np.uint32)
+    n = L.or_mesh_voxelize(pos.ctypes.data, len(pos), None if idx is None else idx.ctypes.data,
+                           0 if idx is None else len(idx), w.ctypes.data, spacing, lo.ctypes.data, dims.ctypes.data,
+                           words.ctypes.data, len(words))
+    assert n == len(words)
+    return lo, dims, words
+
+
+def mesh_splat(emitters, spacing: float) -> np.ndarray:
+    """The oracle's MeshSourceRasterizer.prepare: records (n, 12) as int32/float32 words in a
+    structured view (cell xyzw int32, then 8 float32), ascending by cell."""
+    from firepro import abi
+
+    L = lib()
+    arr = (abi.fp_mesh_emitter * max(1, len(emitters)))(*[e.struct() for e in emitters])
+    n = L.or_mesh_splat(C.addressof(arr), len(emitters), spacing, None, 0)
+    if n < 0:
+        n = 1 << 22
+    out = (abi.fp_mesh_source * max(1, n))()
+    got = L.or_mesh_splat(C.addressof(arr), len(emitters), spacing, C.addressof(out), n)
+    return list(out[:got])

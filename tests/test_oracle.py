@@ -250,3 +250,51 @@ def test_solver_schedules_converge():
     # CG never lets the residual grow much, step to step.
     for name in ("fcg", "fcg_redblack"):
         assert np.all(out[name][1:] <= 1.5 * out[name][:-1]), out[name]
+
+
+def _cube(half):
+    v = np.array([[x, y, z] for z in (-half, half) for y in (-half, half) for x in (-half, half)], np.float32)
+    # outward-wound faces of the cube (corner index = x + 2y + 4z)
+    quads = [(0, 2, 3, 1), (4, 5, 7, 6), (0, 1, 5, 4), (2, 6, 7, 3), (0, 4, 6, 2), (1, 3, 7, 5)]
+    tris = []
+    for a, b, c, d in quads:
+        tris += [(a, b, c), (a, c, d)]
+    return v, np.array(tris, np.uint32)
+
+
+def test_mesh_voxelize_cube_is_cell_centre_inclusion():
+    """The oracle's MeshCollider.voxelize on a box: a cell is solid exactly when its centre lies
+    inside the box (faces placed off the cell centres)."""
+    from oracle import fp_oracle
+
+    pos, idx = _cube(0.113)
+    M = np.eye(4)
+    M[:3, 3] = [0.31, 0.52, -0.07]
+    h = 0.025
+    lo, dims, words = fp_oracle.mesh_voxelize(pos, idx, M, h)
+    bits = np.unpackbits(words.view(np.uint8), bitorder="little")[: int(np.prod(dims))].reshape(dims[2], dims[1], dims[0])
+    z, y, x = np.meshgrid(*[(np.arange(dims[a]) + lo[a] + 0.5) * h for a in (2, 1, 0)], indexing="ij")
+    inside = (np.abs(x - 0.31) < 0.113) & (np.abs(y - 0.52) < 0.113) & (np.abs(z + 0.07) < 0.113)
+    assert inside.sum() > 500 and np.array_equal(bits.astype(bool), inside)
+
+
+def test_mesh_splat_single_sample():
+    """The oracle's MeshSourceRasterizer: one sample splats weight x area / mean face area over
+    its 8 cells trilinearly; coverage caps at 1 and scales the rates."""
+    from firepro.mesh import MeshEmitter
+    from oracle import fp_oracle
+
+    h = 0.1
+    e = MeshEmitter([[0.125, 0.26, 0.375]], [1.0], 0.01 * 3, flame=0.5, heat=2.0, smoke=1.0, fuel=0.25,
+                    velocity=(0, 1, 0), response=60.0)
+    recs = fp_oracle.mesh_splat([e], h)
+    assert len(recs) == 8
+    g = np.array([0.125, 0.26, 0.375]) / h - 0.5
+    base, f = np.floor(g), g - np.floor(g)
+    for r in recs:
+        off = np.array(r.cell[:3]) - base
+        w = np.prod(np.where(off == 1, f, 1 - f))
+        cover = min(1.0, w * 0.03 / (h * h))
+        assert r.scalar[1] == pytest.approx(2.0 * cover, rel=1e-6)
+        assert r.scalar[0] == pytest.approx(0.5 * cover, rel=1e-6)
+        assert r.motion[1] == pytest.approx(60.0 * cover, rel=1e-6) and r.motion[3] == pytest.approx(60.0 * cover, rel=1e-6)

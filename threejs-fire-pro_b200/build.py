@@ -24,7 +24,10 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxe
 # fused coarse cycle, chosen by a simulation's tile capacity). Without multiply-add
 # contraction each operation rounds the same in all of them, so the pressure of a simulation
 # does not depend on which kernels ran it.
-FILE_FLAGS = {"fp_mg.cu": ["-fmad=false"]}
+FILE_FLAGS = {"fp_mg.cu": ["-fmad=false"],
+              # The mesh voxelizer decides bits with FP64 edge tests as the reference's JavaScript
+              # does: no contraction on the device or the host.
+              "fp_mesh.cu": ["-fmad=false", "-Xcompiler", "-ffp-contract=off"]}
 
 
 def _sources():

@@ -230,6 +230,18 @@ class fp_solver_stats(C.Structure):
     ]
 
 
+class fp_mesh(C.Structure):
+    _fields_ = [("positions", C.POINTER(C.c_float)), ("vertex_count", C.c_uint32),
+                ("indices", C.POINTER(C.c_uint32)), ("index_count", C.c_uint32)]
+
+
+class fp_mesh_emitter(C.Structure):
+    _fields_ = [("samples", C.POINTER(C.c_double)), ("weights", C.POINTER(C.c_double)), ("sample_count", C.c_uint32),
+                ("surface_area", C.c_double), ("flame", C.c_double), ("heat_rate", C.c_double),
+                ("smoke_rate", C.c_double), ("fuel_rate", C.c_double), ("velocity", C.c_double * 3),
+                ("velocity_response", C.c_double)]
+
+
 FP_SMOOTHER_JACOBI = 0
 FP_SMOOTHER_REDBLACK = 1
 FP_KRYLOV_NONE = 0
@@ -339,6 +351,9 @@ SIGNATURES = {
     "fp_batch_set_schedule": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
     "fp_server_set_solver": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_float]),
     "fp_sim_snapshot": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "fp_mesh_voxelize": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.POINTER(C.c_uint32)]),
+    "fp_mesh_splat": (C.c_int, [C.c_int, C.c_void_p, C.c_uint32, C.c_double, C.c_void_p, C.POINTER(C.c_uint32)]),
     "fp_sim_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "fp_snapshot_free": (None, [C.c_void_p]),
     "fp_server_snapshot": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
