@@ -444,6 +444,61 @@ def precision_form(local: int, steps: int = 30) -> dict:
     return out
 
 
+def stress_form(local: int, grow: int = 600, steps: int = 20, renders: int = 5) -> dict:
+    """The stress workload: the 25 m/s jet scene grown `grow` steps (untimed) at the
+    benchmark's budget, its step timed (plain FP32, the 6-level reference V-cycle), and the
+    half-resolution camera render at 960x540 with 128 ray steps and 16 shadow samples timed on
+    the simulation's stream: ms per render, march samples per second (pixels x ray steps /
+    time, an upper bound on the samples the march takes) and the render passes' pool bytes."""
+    import numpy as np
+    import torch
+
+    from firepro import render, scenes
+    from firepro.engine import FluidSimulation
+
+    sc = scenes.StressScene(seed=1)
+    sim = FluidSimulation(sc.grid(budget=BUDGET), device=local)
+    sim.set_runtime(0.05, BUDGET, True)
+    step = 0
+    while step < grow:
+        sim.step(sc.frame(step).frame)
+        step += 1
+    sim.synchronize()
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    actives = []
+    ev[0].record(stream)
+    for _ in range(steps):
+        sim.step(sc.frame(step).frame)
+        step += 1
+        actives.append(sim.stats().active_bricks)
+    ev[1].record(stream)
+    sim.synchronize()
+    step_ms = ev[0].elapsed_time(ev[1]) / steps
+    cam = render.look_at((-0.5, 1.2, 3.2), (-0.2, 0.6, 0.0), 960, 540)
+    cam.half_resolution = 1
+    rs = render.default_settings(ray_steps=128, shadow_samples=16)
+    image = torch.empty((540, 960, 4), dtype=torch.float32, device=f"cuda:{local}")
+    sim.render_device(cam, rs, image.data_ptr())  # warm-up: pools, table
+    sim.synchronize()
+    ev[0].record(stream)
+    for _ in range(renders):
+        sim.render_device(cam, rs, image.data_ptr())
+    ev[1].record(stream)
+    sim.synchronize()
+    render_ms = ev[0].elapsed_time(ev[1]) / renders
+    lit = float((image[..., 3] > 0.01).float().mean().item())
+    out = {"workload": f"25 m/s jet (box emitter 0.05 m on a wandering path, fuel 1.0, 3 m/s crosswise wind), "
+                       f"grown {grow} steps, budget 2^24 voxels; render 960x540 half resolution, 128 ray steps, "
+                       f"16 shadow samples, cubic filter",
+           "mean_active_bricks": sum(actives) / len(actives), "step_ms": step_ms,
+           "value": sum(actives) * BRICK_VOXELS / (step_ms * steps / 1e3), "unit": "voxel-steps/s",
+           "render_ms": render_ms, "render_samples_per_s": 960 * 540 * 128 / (render_ms / 1e3),
+           "covered_pixel_fraction": lit}
+    sim.dispose()
+    return out
+
+
 def serving_forms(local: int, wall: float = 20.0) -> dict:
     """The serving workload (Poisson arrivals at 20 sessions/s, budgets log-uniform 32-8192
     bricks, lifetimes 5-60 s of simulated time, 60 Hz step requests, at most 256 live sessions,
@@ -613,6 +668,7 @@ def run_ours(args, rank, world, local):
         line["forms"] = {"batched": batched_form(local, steps=max(10, min(args.steps, 60))),
                          "served_64": served_form(local),
                          "precision": precision_form(local),
+                         "stress": stress_form(local),
                          "serving": serving_forms(local)}
     if world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1

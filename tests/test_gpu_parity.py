@@ -80,6 +80,12 @@ def test_large_scene_through_burst():
     check(run(scenes.LargeScene(), 34, budget=2 ** 20), min_active=100)
 
 
+def test_stress_jet_parity():
+    """The 25 m/s jet: back-traces up to four cells long leave the transport kernels' staged
+    rim and take the directory path; a crosswise wind; combustion with fuel."""
+    check(run(scenes.StressScene(), 30, budget=2 ** 21), min_active=30)
+
+
 def test_pool_exhausted_failures_match():
     """A budget of 150 bricks: requests past it fail, deterministically in brick order."""
     reports = run(scenes.SinglePlume(), 8, budget=150 * 512)

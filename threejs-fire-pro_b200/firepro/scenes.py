@@ -365,6 +365,34 @@ class MeshTargetScene(MeshEmitterScene):
                           target_cells=[cells, []])
 
 
+class StressScene(Scene):
+    """A flamethrower-like jet: a 5 cm box emitter wandering on a smooth path (the editor's
+    wanderPosition-style motion, editor/scenes/motion.ts), pushing 25 m/s of fuel-rich flame
+    along +x (CFL up to 4 in 2.5 cm voxels at 60 Hz), combustion with fuel 1.0, a 3 m/s
+    crosswise wind; grows to thousands of bricks."""
+
+    name = "stress"
+    steps = 300
+
+    def __init__(self, seed: int = 1, speed: float = 25.0):
+        self.seed = seed
+        self.speed = speed
+        self.settings = settings(buoyancy=1.6, vorticity=1.5, seed=seed, dissipation=0.02, cooling=0.2, damping=0.02)
+        self.comb = combustion(smoke_rate=1.5)
+
+    def position(self, step: int):
+        t = step / 60.0
+        return (-1.5 + 0.15 * math.sin(1.3 * t + self.seed), 0.4 + 0.1 * math.sin(0.9 * t),
+                0.2 * math.sin(0.7 * t + 2.0 * self.seed))
+
+    def frame(self, step: int) -> FrameData:
+        j = 1.0 + 0.2 * value_noise_1d(step / 12.0, self.seed)
+        jet = source(1, "box", self.position(step), (0.05, 0.05, 0.05), flame=1.0, heat=30.0 * j, smoke=40.0 * j,
+                     fuel=1.0 * j, velocity=(self.speed, 2.0, 0.0), response=60.0)
+        wind = force("wind", vector=(0.0, 0.0, 1.0), strength=3.0)
+        return make_frame(self.settings, self.comb, True, [jet], [wind])
+
+
 class EmptyScene(Scene):
     """No sources, forces or colliders: nothing computes."""
 
@@ -415,4 +443,5 @@ class MemberScene(Scene):
         return make_frame(self.settings, self.comb, True, srcs)
 
 
-SCENES = {"single_plume": SinglePlume, "large_scene": LargeScene, "force_scene": ForceScene, "empty": EmptyScene}
+SCENES = {"single_plume": SinglePlume, "large_scene": LargeScene, "force_scene": ForceScene, "stress": StressScene,
+          "empty": EmptyScene}
