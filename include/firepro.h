@@ -402,6 +402,9 @@ int fp_batch_reserve_tiles(fp_batch* batch, uint32_t id, uint32_t tiles);
  * demanding simulation asks for; each simulation stops at its own limit or tolerance. */
 int fp_batch_set_solver(fp_batch* batch, uint32_t id, int vcycles, float tolerance);
 int fp_batch_read_solver(fp_batch* batch, uint32_t id, fp_solver_stats* out);
+/* As fp_sim_snapshot and fp_sim_restore, for a simulation of the batch. */
+int fp_batch_snapshot(fp_batch* batch, uint32_t id, void** blob, size_t* bytes);
+int fp_batch_restore(fp_batch* batch, uint32_t id, const void* blob, size_t bytes);
 /* As fp_sim_set_schedule; the simulations of one fp_batch_step must share a schedule. */
 int fp_batch_set_schedule(fp_batch* batch, uint32_t id, const fp_solver_schedule* schedule);
 /* Step the `count` simulations `ids` (distinct) with frames[i] and dts[i], in one launch. */

@@ -355,6 +355,24 @@ int fp_batch_set_solver(fp_batch* batch, uint32_t id, int vcycles, float toleran
   return rc ? batchFail(batch, rc, e->error()) : FP_OK;
 }
 
+int fp_batch_snapshot(fp_batch* batch, uint32_t id, void** blob, size_t* bytes) {
+  if (!batch || !blob || !bytes) return failed("fp_batch_snapshot needs a batch and outputs.", FP_EINVAL);
+  fp::Engine* e = batchSim(batch, id);
+  if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
+  std::vector<uint8_t> v;
+  int rc = e->snapshot(v);
+  if (rc) return batchFail(batch, rc, e->error());
+  return handOut(v, blob, bytes);
+}
+
+int fp_batch_restore(fp_batch* batch, uint32_t id, const void* blob, size_t bytes) {
+  if (!batch || !blob) return failed("fp_batch_restore needs a batch and a snapshot.", FP_EINVAL);
+  fp::Engine* e = batchSim(batch, id);
+  if (!e) return batchFail(batch, FP_EINVAL, "no simulation with id " + std::to_string(id));
+  int rc = e->restore(static_cast<const uint8_t*>(blob), bytes);
+  return rc ? batchFail(batch, rc, e->error()) : FP_OK;
+}
+
 int fp_batch_set_schedule(fp_batch* batch, uint32_t id, const fp_solver_schedule* schedule) {
   if (!batch || !schedule) return failed("fp_batch_set_schedule needs a batch and a schedule.", FP_EINVAL);
   fp::Engine* e = batchSim(batch, id);

@@ -355,6 +355,8 @@ SIGNATURES = {
                                    C.POINTER(C.c_uint32)]),
     "fp_mesh_splat": (C.c_int, [C.c_int, C.c_void_p, C.c_uint32, C.c_double, C.c_void_p, C.POINTER(C.c_uint32)]),
     "fp_sim_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "fp_batch_snapshot": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "fp_batch_restore": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t]),
     "fp_snapshot_free": (None, [C.c_void_p]),
     "fp_server_snapshot": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
     "fp_server_restore": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t]),

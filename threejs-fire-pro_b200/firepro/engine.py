@@ -216,6 +216,17 @@ class SimulationBatch:
     def set_schedule(self, sim: int, schedule: abi.fp_solver_schedule):
         self._check(self.lib.fp_batch_set_schedule(self.h, sim, C.byref(schedule)))
 
+    def snapshot(self, sim: int) -> bytes:
+        p, n = C.c_void_p(), C.c_size_t()
+        self._check(self.lib.fp_batch_snapshot(self.h, sim, C.byref(p), C.byref(n)))
+        try:
+            return C.string_at(p, n.value)
+        finally:
+            self.lib.fp_snapshot_free(p)
+
+    def restore(self, sim: int, blob: bytes):
+        self._check(self.lib.fp_batch_restore(self.h, sim, blob, len(blob)))
+
     def read_solver(self, sim: int) -> abi.fp_solver_stats:
         s = abi.fp_solver_stats()
         self._check(self.lib.fp_batch_read_solver(self.h, sim, C.byref(s)))
