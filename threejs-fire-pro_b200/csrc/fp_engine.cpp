@@ -199,7 +199,7 @@ int Engine::consume() {
 
 void Engine::freeAll() {
   DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_, &zeroList_,
-                         &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_, &donors_, &solids_,
+                         &freeStack_, &counters_, &curl_, &expn_, &div_, &sb_, &donors_, &solids_,
                          &tileRecD_, &tileNbrD_, &hashD_, &solver_, &tileMask_, &liveTilesD_, &tileIndexD_};
   for (DeviceBuffer* b : all)
     if (b->ptr) {
@@ -263,12 +263,12 @@ uint64_t Engine::estimateBytes(const fp_grid& g, uint32_t tiles) {
   uint64_t N = (uint64_t)B * B * B, VN = N / ((uint64_t)vd * vd * vd);
   double budget = g.voxel_budget > 0 ? g.voxel_budget : 8e6;
   uint64_t slots = (uint64_t)std::max(1.0, std::floor(budget / (double)N));
-  // FP32 on the velocity lattice: velocity x4 (3 channels), curl, divergence, bounds (3+3),
-  // pressure x2, donors, topology; on the field lattice: expansion, scalar bounds (8), the scalar
+  // FP32 on the velocity lattice: velocity x4 (3 channels), curl, divergence, pressure x2,
+  // donors, topology; on the field lattice: expansion, scalar bounds (8), the scalar
   // predictor (4), solid bits; the two scalar state pools (4 channels) and the coarse levels in
   // the precision's width.
   const uint64_t narrow = g.precision == FP_PRECISION_MIXED ? 2 : 4;
-  uint64_t perSlot = VN * 4 * (4 * 3 + 4 + 1 + 3 + 3 + 2) + VN * 3 * 2 + VN + N * 4 * (1 + 8 + 4) +
+  uint64_t perSlot = VN * 4 * (4 * 3 + 4 + 1 + 2) + VN * 3 * 2 + VN + N * 4 * (1 + 8 + 4) +
                      N * 2 * 4 * narrow + N / 8 + 4;
   for (int l = 1; l < vshift; l++) {
     uint64_t c = (uint64_t)1 << (3 * (vshift - l));
@@ -315,7 +315,7 @@ int Engine::allocatePools(uint32_t slots) {
   // fld_[1] is the predictor within a step (FP32); fld_[0] and fld_[2] trade the state.
   for (int k = 0; k < 3; k++) ok = ok && alloc(fld_[k], s * 4 * N * (k == 1 ? 4 : scalarBytes()));
   ok = ok && alloc(curl_, s * 4 * VN * 4) && alloc(expn_, s * N * 4) && alloc(div_, s * VN * 4) &&
-       alloc(vmin_, s * 3 * VN * 4) && alloc(vmax_, s * 3 * VN * 4) && alloc(sb_, s * 8 * N * 4) &&
+       alloc(sb_, s * 8 * N * 4) &&
        alloc(donors_, s * 3 * VN * 2) && alloc(solids_, s * W_ * 4) && alloc(p0_[0], s * VN * 4) &&
        alloc(p0_[1], s * VN * 4) && alloc(topo_[0], s * VN) && alloc(freeStack_, s * 4);
   for (int l = 1; l < brickLevels_ && ok; l++) {
@@ -353,7 +353,7 @@ int Engine::growPool(uint32_t target) {
   for (auto& b : vel_) ok = ok && grow(b, s * 3 * VN * 4, 0);
   for (int k = 0; k < 3; k++) ok = ok && grow(fld_[k], s * 4 * N * (k == 1 ? 4 : scalarBytes()), 0);
   ok = ok && grow(curl_, s * 4 * VN * 4, 0) && grow(expn_, s * N * 4, 0) && grow(div_, s * VN * 4, 0) &&
-       grow(vmin_, s * 3 * VN * 4, 0) && grow(vmax_, s * 3 * VN * 4, 0) && grow(sb_, s * 8 * N * 4, 0) &&
+       grow(sb_, s * 8 * N * 4, 0) &&
        grow(donors_, s * 3 * VN * 2, 0) && grow(solids_, s * W_ * 4, 0) && grow(p0_[0], s * VN * 4, 0) &&
        grow(p0_[1], s * VN * 4, 0) && grow(topo_[0], s * VN, 0);
   for (int l = 1; l < brickLevels_ && ok; l++) {
@@ -975,8 +975,6 @@ void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t
   P.fldN = (float*)fld_[fldIdx_[2]].ptr;
   P.expn = (float*)expn_.ptr;
   P.div = (float*)div_.ptr;
-  P.vmin = (float*)vmin_.ptr;
-  P.vmax = (float*)vmax_.ptr;
   P.sb = (float*)sb_.ptr;
   P.smokeDiv = smokeDiv_;
   P.smokeShift = sshift_;
@@ -1140,7 +1138,7 @@ int Engine::setRuntime(float cutoff, double budget, int ground) {
 uint64_t Engine::memoryBytes() const {
   uint64_t bytes = 0;
   const DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_,
-                               &zeroList_, &freeStack_, &counters_, &curl_, &expn_, &div_, &vmin_, &vmax_, &sb_,
+                               &zeroList_, &freeStack_, &counters_, &curl_, &expn_, &div_, &sb_,
                                &donors_, &solids_, &tileRecD_, &tileNbrD_, &hashD_, &solver_, &tileMask_,
                                &liveTilesD_, &tileIndexD_};
   for (const DeviceBuffer* b : all) bytes += b->bytes;

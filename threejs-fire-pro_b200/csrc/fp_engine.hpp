@@ -179,7 +179,7 @@ class Engine {
   // device memory
   DeviceBuffer pages_, entries_, state_, activity_, records_, blockCounts_, active_, zeroList_;
   DeviceBuffer freeStack_, counters_;
-  DeviceBuffer vel_[4], curl_, fld_[3], expn_, div_, vmin_, vmax_, sb_, donors_, solids_;
+  DeviceBuffer vel_[4], curl_, fld_[3], expn_, div_, sb_, donors_, solids_;
   DeviceBuffer p0_[3], topo_[FP_MAX_LEVELS], lp_[FP_MAX_LEVELS][2], lrhs_[FP_MAX_LEVELS];
   DeviceBuffer kry_[3];  // flexible CG: residual, direction, A direction (p0_[2] its iterate)
   DeviceBuffer tileRecD_, tileNbrD_, hashD_, solver_, tileMask_, liveTilesD_, tileIndexD_;

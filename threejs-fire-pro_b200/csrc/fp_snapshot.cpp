@@ -19,7 +19,7 @@ namespace fp {
 namespace {
 
 constexpr uint32_t MAGIC = 0x4e535046u;  // "FPSN"
-constexpr uint32_t VERSION = 1;
+constexpr uint32_t VERSION = 2;
 
 struct Writer {
   std::vector<uint8_t>& out;
@@ -74,7 +74,7 @@ struct Reader {
 #define FP_SNAPSHOT_BUFFERS(X)                                                                            \
   X(pages_) X(entries_) X(state_) X(activity_) X(records_) X(blockCounts_) X(active_) X(zeroList_)        \
   X(freeStack_) X(counters_) X(vel_[0]) X(vel_[1]) X(vel_[2]) X(vel_[3]) X(curl_) X(fld_[0]) X(fld_[1])   \
-  X(fld_[2]) X(expn_) X(div_) X(vmin_) X(vmax_) X(sb_) X(donors_) X(solids_) X(p0_[0]) X(p0_[1])           \
+  X(fld_[2]) X(expn_) X(div_) X(sb_) X(donors_) X(solids_) X(p0_[0]) X(p0_[1])           \
   X(p0_[2]) X(kry_[0]) X(kry_[1]) X(kry_[2]) X(tileRecD_) X(tileNbrD_) X(hashD_) X(solver_) X(tileMask_) \
   X(liveTilesD_) X(tileIndexD_) X(smoke_[0]) X(smoke_[1]) X(smoke_[2]) X(smokeBnd_) X(meshTablesD_)      \
   X(meshSourcesD_) X(coverageD_)
@@ -281,7 +281,7 @@ int Engine::restore(const uint8_t* data, size_t bytes) {
     bool sane = capacity > 0 && sizes[0] >= ids * 4 && sizes[1] >= ids * 4 && sizes[2] >= ids * 4 &&
                 sizes[3] >= (ids + capacity) * 4 && sizes[4] >= ids * FP_RECORD_WORDS * 4 && sizes[8] >= (uint64_t)slots * 4;
     for (int k = 10; k < 14; k++) sane = sane && sizes[k] >= vpool;  // vel_
-    sane = sane && sizes[25] >= (uint64_t)slots * VN_ * 4 && sizes[26] >= (uint64_t)slots * VN_ * 4;  // p0_[0..1]
+    sane = sane && sizes[23] >= (uint64_t)slots * VN_ * 4 && sizes[24] >= (uint64_t)slots * VN_ * 4;  // p0_[0..1]
     sane = sane && tileRec.size() == (size_t)capacity && tileNbr.size() == (size_t)capacity * 27;
     if (!sane) return fail(FP_EINVAL, "the snapshot's tables do not match its sizes");
   }

@@ -227,21 +227,8 @@ FP_DEV void cellOf(const SimParams& P, const Home& H, int c, int& x, int& y, int
 FP_DEV void predictVelocity(const SimParams& P, const Home& H, const Stage& G, const Field& V, size_t slot, int c, int x,
                             int y, int z) {
   const size_t N = P.N;
-  // Velocity bounds over the forward 2x2x2 block (staged: HALO >= 1).
-  const float* home = V.sm ? V.sm + stagedAt(G, x, y, z) : nullptr;
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    float t[8];
-    blockCells(P, H, G, V, k, home, x, y, z, t);
-    float lo = 1e5f, hi = -1e5f;
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      lo = fminf(lo, t[j]);
-      hi = fmaxf(hi, t[j]);
-    }
-    P.vmin[(slot * 3 + k) * N + c] = lo;
-    P.vmax[(slot * 3 + k) * N + c] = hi;
-  }
+  // The limiter's bounds (the forward 2x2x2 block of each donor cell) are taken where the
+  // correction needs them, at the donor, from the same start-of-step velocity.
   const float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
   // solidAt at a cell centre is solidCell of that cell: centre / h + 0.25 floors to it.
   if (solidCell(P, H, x, y, z)) {
@@ -415,12 +402,21 @@ FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
           dep[comp] -= 0.5f * P.h;
           for (int a = 0; a < 3; a++) base[a] = (int)floorf(dep[a] / P.h - 0.5f);  // as in the predictor
         }
+        // The bounds of the donor: the start-of-step component over the 2x2x2 block forward of
+        // the donor cell (advectVelocityWithBounds' shared-tile min/max,
+        // fluid-velocity-transport.wgsl:66-100), zero for a donor brick without a slot.
         float lo = 0.f, hi = 0.f;
         int bs = brickSlot(P, H, base[0] >> P.shift, base[1] >> P.shift, base[2] >> P.shift);
         if (bs >= 0) {
-          int lc = localCell(P, base[0], base[1], base[2]);
-          lo = P.vmin[((size_t)bs * 3 + comp) * N + lc];
-          hi = P.vmax[((size_t)bs * 3 + comp) * N + lc];
+          float t[8];
+          blockCells(P, H, G, V, comp, stagedBlock(G, V, base[0], base[1], base[2]), base[0], base[1], base[2], t);
+          lo = 1e5f;
+          hi = -1e5f;
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            lo = fminf(lo, t[j]);
+            hi = fmaxf(hi, t[j]);
+          }
         }
         if (lo == hi && predicted == lo) {
           result = predicted;

@@ -7,9 +7,10 @@
 //   tile hash          int4 (x,y,z,slot) open addressing, power-of-two size
 //   per brick id       pages, entries, state, activity (+ per tile), records int[28]
 //   per pool slot      [slot][channel][cell] pools, cells x fastest in a brick:
-//                        vel/velA/velB 3ch, curl 4ch, fld/fldA/fldB 4ch, expn, div 1ch,
-//                        vmin/vmax 3ch, scalar bounds 8ch, donors 3 x u16, solids bits
-//   multigrid          level 0: p[2] and topology per slot; brick levels 1.. per slot;
+//                        velocity x4 3ch, curl 4ch, scalars x3 4ch, expn, div 1ch,
+//                        scalar bounds 8ch, velocity donors 3 x u16, solids bits
+//   multigrid          level 0: p[2] (+ the CG iterate, residual, direction and A direction
+//                        with FP_KRYLOV_FCG) and topology per slot; brick levels 1.. per slot;
 //                        tile levels per tile slot
 #pragma once
 #include <stdint.h>
@@ -171,8 +172,6 @@ struct SimParams {
   float* fldN;  // evolved
   float* expn;
   float* div;
-  float* vmin;
-  float* vmax;
   float* sb;
   uint16_t* donors;
   // coarse smoke (smoke_divisor d > 1, smoke.wgsl): density on 2^smokeShift cells a brick side
