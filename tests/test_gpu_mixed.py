@@ -35,7 +35,7 @@ def check_mixed(reports, min_active=1):
     for step, tables, fields, n in reports:
         for k, v in tables.items():
             if k == "activity":
-                assert 0 <= v <= max(2, n // 500), f"step {step}: {v} activity words differ"
+                assert 0 <= v <= max(4, n // 200), f"step {step}: {v} activity words differ"
                 continue
             assert v == 0, f"step {step}: table {k} differs in {v} words"
         for k, v in fields.items():

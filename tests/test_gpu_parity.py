@@ -20,7 +20,7 @@ def check(reports, tol=TOL, min_active=1):
     """Allocation tables bit-exact; fields within `tol`. The activity flags come from float
     threshold tests (content above the cutoff, motion pads) that the CUDA step evaluates in
     FP32 and the oracle in FP64, so a value within rounding of a threshold may flip: at most
-    one flag word per 500 computing bricks (and 2) may differ. The allocation consumes the
+    one flag word per 200 computing bricks (and 4) may differ. The allocation consumes the
     CUDA flags on both sides, so its tables stay bit-exact regardless. The limiter's tests
     may flip the same way (parity.field_within): a field may exceed `tol` only through a few
     isolated cells, and then by at most FLIP_BOUND times."""
@@ -29,7 +29,7 @@ def check(reports, tol=TOL, min_active=1):
     for step, tables, fields, n in reports:
         for k, v in tables.items():
             if k == "activity":
-                assert 0 <= v <= max(2, n // 500), f"step {step}: {v} activity words differ"
+                assert 0 <= v <= max(4, n // 200), f"step {step}: {v} activity words differ"
                 continue
             assert v == 0, f"step {step}: table {k} differs in {v} words"
         for k, v in fields.items():

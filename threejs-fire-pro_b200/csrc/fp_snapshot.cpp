@@ -19,7 +19,7 @@ namespace fp {
 namespace {
 
 constexpr uint32_t MAGIC = 0x4e535046u;  // "FPSN"
-constexpr uint32_t VERSION = 2;
+constexpr uint32_t VERSION = 3;
 
 struct Writer {
   std::vector<uint8_t>& out;
@@ -77,7 +77,12 @@ struct Reader {
   X(fld_[2]) X(expn_) X(div_) X(sb_) X(donors_) X(solids_) X(p0_[0]) X(p0_[1])           \
   X(p0_[2]) X(kry_[0]) X(kry_[1]) X(kry_[2]) X(tileRecD_) X(tileNbrD_) X(hashD_) X(solver_) X(tileMask_) \
   X(liveTilesD_) X(tileIndexD_) X(smoke_[0]) X(smoke_[1]) X(smoke_[2]) X(smokeBnd_) X(meshTablesD_)      \
-  X(meshSourcesD_) X(coverageD_)
+  X(meshSourcesD_) X(coverageD_) \
+  FP_SNAPSHOT_LEVEL(X, 0) FP_SNAPSHOT_LEVEL(X, 1) FP_SNAPSHOT_LEVEL(X, 2) FP_SNAPSHOT_LEVEL(X, 3)     \
+  FP_SNAPSHOT_LEVEL(X, 4) FP_SNAPSHOT_LEVEL(X, 5) FP_SNAPSHOT_LEVEL(X, 6) FP_SNAPSHOT_LEVEL(X, 7)
+// The multigrid levels: topology, pressure pair, right-hand side (index 43 + 4 level on).
+#define FP_SNAPSHOT_LEVEL(X, l) X(topo_[l]) X(lp_[l][0]) X(lp_[l][1]) X(lrhs_[l])
+static_assert(FP_MAX_LEVELS == 8, "the snapshot lists eight multigrid levels");
 
 int Engine::snapshot(std::vector<uint8_t>& out) {
   int rc = consume();
@@ -283,6 +288,14 @@ int Engine::restore(const uint8_t* data, size_t bytes) {
     for (int k = 10; k < 14; k++) sane = sane && sizes[k] >= vpool;  // vel_
     sane = sane && sizes[23] >= (uint64_t)slots * VN_ * 4 && sizes[24] >= (uint64_t)slots * VN_ * 4;  // p0_[0..1]
     sane = sane && tileRec.size() == (size_t)capacity && tileNbr.size() == (size_t)capacity * 27;
+    // Every level's topology and values: per slot on the brick levels, per tile slot on the
+    // tile levels.
+    for (int l = 0; l <= bottom_ && sane; l++) {
+      const uint64_t cells = (uint64_t)levelCells(l) * (l < brickLevels_ ? slots : (uint64_t)capacity);
+      sane = sizes[43 + 4 * l] >= cells;
+      if (l > 0) sane = sane && sizes[44 + 4 * l] >= cells * coarseBytes() && sizes[45 + 4 * l] >= cells * coarseBytes() &&
+                        sizes[46 + 4 * l] >= cells * coarseBytes();
+    }
     if (!sane) return fail(FP_EINVAL, "the snapshot's tables do not match its sizes");
   }
 #define FP_LOAD(b)                                                                                      \
