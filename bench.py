@@ -411,73 +411,104 @@ def served_form(local: int, sessions: int = 64, grow: int = 90, ticks: int = 300
 
 
 # The accurate solve every form that compares at equal accuracy uses: flexible CG around a
-# red-black V-cycle on every level (2 + 2 sweeps, 8 at the bottom), to a relative residual of
-# 1e-6 in at most 16 V-cycles, which holds post-projection divergence under 1e-4 of the velocity
-# on the large scene at the benchmark's size.
-ACCURATE = {"smoother": 1, "levels": 0, "pre": 2, "post": 2, "bottom": 8, "krylov": 1, "vcycles": 16, "tolerance": 1e-6}
+# red-black V-cycle on every level (2 + 2 sweeps, 8 at the bottom) with every brick's topology
+# rebuilt each step, a fixed number of V-cycles a step: the fewest that hold post-projection
+# divergence under 1e-4 of the velocity on the large scene at the benchmark's size, chosen by
+# precision_form (which runs first) from CANDIDATE_VCYCLES.
+ACCURATE = {"smoother": 1, "levels": 0, "pre": 2, "post": 2, "bottom": 8, "krylov": 1, "topology": 1,
+            "vcycles": 6, "tolerance": 0.0}
+CANDIDATE_VCYCLES = (4, 5, 6, 8, 10)
+DIVERGENCE_GATE = 1e-4
 
 
 def accurate_schedule():
     from firepro import abi
 
     a = ACCURATE
-    return abi.schedule(a["smoother"], a["levels"], a["pre"], a["post"], a["bottom"], a["krylov"])
+    return abi.schedule(a["smoother"], a["levels"], a["pre"], a["post"], a["bottom"], a["krylov"], a["topology"])
+
+
+def _timed_steps(sim, sc, step, steps, local):
+    """Device time of `steps` steps on the simulation's stream, then 10 more read back for the
+    solve's accuracy: (ms per step, mean bricks, V-cycles, worst divergence, last residual)."""
+    import torch
+
+    sim.synchronize()
+    stream = torch.cuda.ExternalStream(sim.stream(), device=local)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    actives = []
+    ev[0].record(stream)
+    for k in range(steps):
+        sim.step(sc.frame(step + k).frame)
+        actives.append(sim.stats().active_bricks)
+    ev[1].record(stream)
+    sim.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / steps
+    cycles, div = [], []
+    for k in range(10):
+        sim.step(sc.frame(step + steps + k).frame)
+        sol = sim.read_solver()
+        cycles.append(int(sol.vcycles))
+        div.append(sol.divergence)
+    return ms, sum(actives) / len(actives), cycles, max(div), sol.residual[max(0, sol.vcycles - 1)]
 
 
 def precision_form(local: int, steps: int = 30) -> dict:
-    """The large scene grown GROW_STEPS steps, then timed `steps` steps: plain FP32 storage and
-    FP_PRECISION_MIXED (FP16 scalar state, BF16 coarse multigrid, FP32 finest level and CG), both
-    with the accurate solve; and the reference's single V-cycle in FP32 for comparison. Device
-    time per step on the simulation's stream, V-cycles, the worst post-projection divergence
-    (h (div u - e) / u, RMS) over the timed steps."""
-    import torch
-
+    """The large scene grown GROW_STEPS steps in plain FP32 and saved; from that state each
+    candidate V-cycle count of the accurate solve runs 3 + 10 steps and reports its worst
+    post-projection divergence (RMS of h (div u - e) / u); the fewest that meet 1e-4 becomes the
+    accurate solve of this run. Then, each from the same kind of grown state: FP32 storage and
+    FP_PRECISION_MIXED (FP16 scalar state, BF16 coarse multigrid, FP32 finest level and CG) with
+    the accurate solve, and the reference's single V-cycle, timed `steps` steps on the
+    simulation's stream."""
     from firepro import abi, scenes
     from firepro.engine import FluidSimulation
 
-    out = {"solver": dict(ACCURATE, name="FCG(red-black V-cycle)")}
-    runs = (("fp32", abi.FP_PRECISION_FP32, True), ("mixed", abi.FP_PRECISION_MIXED, True),
-            ("fp32_reference_vcycle", abi.FP_PRECISION_FP32, False))
-    for name, precision, accurate in runs:
+    out = {"solver": dict(ACCURATE, name="FCG(red-black V-cycle), topology each step")}
+    grown = {}
+    for name, precision in (("fp32", abi.FP_PRECISION_FP32), ("mixed", abi.FP_PRECISION_MIXED)):
         sc = scenes.LargeScene(seed=1)
         sim = FluidSimulation(sc.grid(budget=BUDGET, precision=precision), device=local)
         sim.set_runtime(0.05, BUDGET, True)
-        step = 0
-        while step < GROW_STEPS:
+        for step in range(GROW_STEPS):
             sim.step(sc.frame(step).frame)
-            step += 1
+        grown[name] = (sim, sc, sim.snapshot())
+    sim, sc, blob = grown["fp32"]
+    calibration = []
+    for vc in CANDIDATE_VCYCLES:
+        sim.restore(blob)
+        sim.set_schedule(accurate_schedule())
+        sim.set_solver(vc, 0.0)
+        for k in range(3):
+            sim.step(sc.frame(GROW_STEPS + k).frame)
+        worst = 0.0
+        for k in range(10):
+            sim.step(sc.frame(GROW_STEPS + 3 + k).frame)
+            worst = max(worst, sim.read_solver().divergence)
+        calibration.append({"vcycles": vc, "divergence_max": worst})
+    ok = [c["vcycles"] for c in calibration if c["divergence_max"] <= DIVERGENCE_GATE]
+    ACCURATE["vcycles"] = ok[0] if ok else CANDIDATE_VCYCLES[-1]
+    out["solver"]["vcycles"] = ACCURATE["vcycles"]
+    out["calibration"] = calibration
+    runs = (("fp32", "fp32", True), ("mixed", "mixed", True), ("fp32_reference_vcycle", "fp32", False))
+    for name, which, accurate in runs:
+        sim, sc, blob = grown[which]
+        sim.restore(blob)
         if accurate:
             sim.set_schedule(accurate_schedule())
             sim.set_solver(ACCURATE["vcycles"], ACCURATE["tolerance"])
         else:
+            sim.set_schedule(abi.schedule())
             sim.set_solver(1, 1e-30)  # one V-cycle, measured
+        step = GROW_STEPS
         for _ in range(3):
             sim.step(sc.frame(step).frame)
             step += 1
-        sim.synchronize()
-        stream = torch.cuda.ExternalStream(sim.stream(), device=local)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        actives, cycles, div = [], [], []
-        ev[0].record(stream)
-        for k in range(steps):
-            sim.step(sc.frame(step).frame)
-            step += 1
-            actives.append(sim.stats().active_bricks)
-        ev[1].record(stream)
-        sim.synchronize()
-        ms = ev[0].elapsed_time(ev[1])
-        # The solve's accuracy over more steps, each read back (untimed).
-        for k in range(10):
-            sim.step(sc.frame(step).frame)
-            step += 1
-            sol = sim.read_solver()
-            cycles.append(int(sol.vcycles))
-            div.append(sol.divergence)
-        st = sim.stats()
-        out[name] = {"value": sum(actives) * BRICK_VOXELS / (ms / 1e3), "ms_per_step": ms / steps,
-                     "mean_active_bricks": sum(actives) / len(actives), "vcycles": cycles,
-                     "residual_last": sol.residual[max(0, sol.vcycles - 1)], "divergence_max": max(div),
-                     "memory_bytes": st.memory_bytes}
+        ms, bricks, cycles, worst, residual = _timed_steps(sim, sc, step, steps, local)
+        out[name] = {"value": bricks * BRICK_VOXELS / (ms / 1e3), "ms_per_step": ms, "mean_active_bricks": bricks,
+                     "vcycles": cycles, "residual_last": residual, "divergence_max": worst,
+                     "memory_bytes": sim.stats().memory_bytes}
+    for sim, _, _ in grown.values():
         sim.dispose()
     out["speedup_mixed_vs_fp32"] = out["mixed"]["value"] / out["fp32"]["value"]
     out["unit"] = "voxel-steps/s"

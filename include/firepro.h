@@ -298,6 +298,12 @@ typedef struct fp_solver_schedule {
   int32_t post_sweeps;    /* red-black: 0..8 */
   int32_t bottom_sweeps;  /* red-black: 1..64 */
   int32_t krylov;         /* FP_KRYLOV_* */
+  /* 0: the reference's multigrid topology, rebuilt for fresh bricks each step (a brick's cells
+   * keep the open sides they had when a neighbour brick without a slot was granted one, so near
+   * a collider the solve and the projection may disagree on which faces are solid);
+   * 1: every brick's topology rebuilt each step, so the solve's operator always sees the solids
+   * the projection sees (what the accuracy gate needs near colliders). */
+  int32_t topology;
 } fp_solver_schedule;
 int fp_sim_set_schedule(fp_sim* sim, const fp_solver_schedule* schedule);
 /* ---- Volume rendering: a headless restatement of the renderer's compute passes and camera

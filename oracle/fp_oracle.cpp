@@ -287,6 +287,7 @@ struct Sim {
   // Gauss-Seidel on the `mgLevels` finest levels; optionally flexible CG around either.
   int smoother = FP_SMOOTHER_JACOBI, mgLevels = 0, preSweeps = 2, postSweeps = 2, bottomSweeps = 8;
   int krylov = FP_KRYLOV_NONE;
+  int topologyEachStep = 0;  // the schedule's topology 1: every brick's topology rebuilt each step
   float tolerance = 0;  // CG: stop once RMS residual <= tolerance x RMS right-hand side
   std::vector<R>* rhs0 = nullptr;  // the finest level's right-hand side: the divergence, or the CG residual
   std::vector<R> kx, ks, kd, kq;   // CG: iterate, residual (rhs + A x), direction, A direction
@@ -2630,7 +2631,7 @@ struct Sim {
     }
   }
   void buildTopology() {
-    if (geometryDirty) {
+    if (geometryDirty || topologyEachStep) {
       for (size_t id = 0; id < (size_t)capacity * 64; id++) {
         if (snapshotState[id >> 6] == 0) continue;
         int slot = entryPage(entries[id]);
@@ -3123,6 +3124,45 @@ struct Sim {
     vel.swap(out);
   }
 
+  // The projected velocity's divergence less the expansion it keeps, over the interior
+  // unknowns (every neighbour solid or an unknown), as the CUDA measurement takes it:
+  // out[0] sum of (h div u - h e)^2, out[1] sum of the face velocities' squares, out[2] cells,
+  // then the `top` largest cells as (x, y, z, value, solid neighbours, expansion) in out[3..].
+  void postDivergence(double* out, int top) {
+    std::vector<std::array<double, 6>> cells;
+    double d2 = 0, v2 = 0;
+    forActiveVCells([&](uint32_t, int slot, int c, int x, int y, int z) {
+      (void)slot;
+      auto solid = [&](int qx, int qy, int qz) { V3<R> p = vcenter(qx, qy, qz); return solidAt(p[0], p[1], p[2]); };
+      if (solid(x, y, z) || !pressureUnknown(x, y, z)) return;
+      const int off[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+      int solids = 0;
+      for (int k = 0; k < 6; k++) {
+        const bool sk = solid(x + off[k][0], y + off[k][1], z + off[k][2]);
+        solids += sk ? 1 : 0;
+        if (!sk && !pressureUnknown(x + off[k][0], y + off[k][1], z + off[k][2])) return;
+      }
+      R u0 = vcell(vel, 3, 0, x, y, z), u1 = vcell(vel, 3, 1, x, y, z), u2 = vcell(vel, 3, 2, x, y, z);
+      R e = vd == 1 ? expn[(size_t)brickSlot(x >> shift, y >> shift, z >> shift) * N + local(x, y, z)] : R(0);
+      double d = (double)((u0 - vcell(vel, 3, 0, x - 1, y, z)) + (u1 - vcell(vel, 3, 1, x, y - 1, z)) +
+                          (u2 - vcell(vel, 3, 2, x, y, z - 1)) - vh * e);
+#pragma omp critical
+      {
+        d2 += d * d;
+        v2 += (double)u0 * u0 + (double)u1 * u1 + (double)u2 * u2;
+        cells.push_back({(double)x, (double)y, (double)z, d, (double)solids, (double)e});
+      }
+    });
+    std::sort(cells.begin(), cells.end(), [](const std::array<double, 6>& a, const std::array<double, 6>& b) {
+      return std::fabs(a[3]) > std::fabs(b[3]);
+    });
+    out[0] = d2;
+    out[1] = v2;
+    out[2] = (double)cells.size();
+    for (int k = 0; k < top && k < (int)cells.size(); k++)
+      for (int j = 0; j < 6; j++) out[3 + 6 * k + j] = cells[k][j];
+  }
+
   // ---------------------------------------------------------------- measurement
   // readActivity (FluidSimulation.ts:1701-1746), applied before the next step.
   void readActivity() {
@@ -3284,12 +3324,20 @@ void or_set_schedule(or_sim* s, const fp_solver_schedule* sc, float tolerance) {
     sim.postSweeps = sc->post_sweeps;
     sim.bottomSweeps = sc->bottom_sweeps;
     sim.krylov = sc->krylov;
+    sim.topologyEachStep = sc->topology;
     sim.tolerance = tolerance;
   };
   if (s->d)
     fn(*s->d);
   else
     fn(*s->f);
+}
+// The latest state's post-projection divergence (Sim::postDivergence).
+void or_post_divergence(or_sim* s, double* out, int top) {
+  if (s->d)
+    s->d->postDivergence(out, top);
+  else
+    s->f->postDivergence(out, top);
 }
 // The finest level's CG residual sums of squares of the latest solve, one per V-cycle run.
 int or_read_cg(or_sim* s, double* out, int capacity) {

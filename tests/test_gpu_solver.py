@@ -38,6 +38,14 @@ def test_redblack_all_levels_with_colliders_parity():
     check(run(sc, 10, budget=2 ** 20, schedule=abi.schedule(RB, levels=4, pre=1, post=1, bottom=4)))
 
 
+def test_topology_each_step_parity():
+    """Every brick's topology rebuilt each step (schedule topology 1) around the colliders of the
+    force scene and the large scene, with flexible CG: lockstep with the oracle."""
+    sched = abi.schedule(RB, levels=0, pre=2, post=2, bottom=8, krylov=FCG, topology=1)
+    check(run(scenes.ForceScene(), 10, budget=2 ** 20, vcycles=6, schedule=sched))
+    check(run(scenes.LargeScene(), 40, budget=2 ** 20, vcycles=6, schedule=sched), min_active=100)
+
+
 @pytest.mark.parametrize("smoother", [abi.FP_SMOOTHER_JACOBI, RB])
 def test_fcg_parity(smoother):
     """Flexible CG with the reference V-cycle or a red-black one as preconditioner: 5 V-cycles
@@ -49,14 +57,15 @@ def test_fcg_parity(smoother):
 
 def test_fcg_meets_the_divergence_gate_at_bench_size():
     """The large scene at the benchmark's budget, grown 180 steps (past 4096 computing bricks):
-    flexible CG around the red-black V-cycle, to a relative residual of 1e-6, leaves the
+    flexible CG around the red-black V-cycle, to a relative residual of 1e-6, with every brick's
+    topology rebuilt each step (so the solve sees the solids the projection sees), leaves the
     projected velocity's divergence (less the expansion it keeps) at most 1e-4 of the velocity
     every step; the reference's single V-cycle does not."""
     sc = scenes.LargeScene()
     budget = 2 ** 24
     sim = FluidSimulation(sc.grid(budget=budget))
     sim.set_runtime(0.05, budget, True)
-    sim.set_schedule(abi.schedule(RB, levels=0, pre=2, post=2, bottom=8, krylov=FCG))
+    sim.set_schedule(abi.schedule(RB, levels=0, pre=2, post=2, bottom=8, krylov=FCG, topology=1))
     sim.set_solver(16, 1e-6)
     worst, cycles = 0.0, []
     for s in range(190):
@@ -84,7 +93,8 @@ def test_schedule_validation():
     sim = FluidSimulation(scenes.SinglePlume().grid(budget=2 ** 19))
     for bad, msg in [(abi.schedule(RB, levels=1), "levels must be"), (abi.schedule(RB, pre=0), "pre_sweeps"),
                      (abi.schedule(RB, post=9), "post_sweeps"), (abi.schedule(RB, bottom=0), "bottom_sweeps"),
-                     (abi.schedule(smoother=7), "smoother"), (abi.schedule(krylov=3), "krylov")]:
+                     (abi.schedule(smoother=7), "smoother"), (abi.schedule(krylov=3), "krylov"),
+                     (abi.schedule(topology=2), "topology")]:
         with pytest.raises(FireProError, match=msg):
             sim.set_schedule(bad)
     sim.dispose()

@@ -914,7 +914,7 @@ void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t
   P.regions = (const FpRegion*)put(regions_.data(), regions_.size() * sizeof(FpRegion));
   P.tileLists = (const uint32_t*)put(tileLists_.data(), tileLists_.size() * 4);
   P.buildSolids = buildSolids() ? 1 : 0;
-  P.topoAll = geometryDirty_ ? 1 : 0;
+  P.topoAll = topoAll() ? 1 : 0;
   P.curlOn = f.simulation.vorticity != 0.f ? 1 : 0;
   P.readback = readback;
   P.B = B_;
@@ -1110,6 +1110,7 @@ int Engine::setSchedule(const fp_solver_schedule& sc) {
     return fail(FP_EINVAL, "smoother must be FP_SMOOTHER_JACOBI or FP_SMOOTHER_REDBLACK.");
   if (sc.krylov != FP_KRYLOV_NONE && sc.krylov != FP_KRYLOV_FCG)
     return fail(FP_EINVAL, "krylov must be FP_KRYLOV_NONE or FP_KRYLOV_FCG.");
+  if (sc.topology != 0 && sc.topology != 1) return fail(FP_EINVAL, "topology must be 0 or 1.");
   fp_solver_schedule next = sc;
   if (sc.smoother == FP_SMOOTHER_REDBLACK) {
     if (sc.levels != 0 && (sc.levels < 2 || sc.levels > bottom_ + 1))

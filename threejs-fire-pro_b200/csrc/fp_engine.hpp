@@ -104,7 +104,7 @@ class Engine {
                  uint32_t* readback, const float4* noise);
   bool buildSolids() const { return colliderCount_ > 0 || solidsStale_; }
   bool solidsAll() const { return solidsStale_; }
-  bool topoAll() const { return geometryDirty_; }
+  bool topoAll() const { return geometryDirty_ || schedule_.topology != 0; }
   int capacity() const { return capacity_; }
   int liveTiles() const { return (int)liveTiles_.size(); }
   int smokeDivisor() const { return smokeDiv_; }

@@ -451,6 +451,7 @@ int fp_server_set_solver(fp_server* S, const fp_solver_schedule* schedule, int v
     return serverFail(S, FP_EINVAL, "smoother must be FP_SMOOTHER_JACOBI or FP_SMOOTHER_REDBLACK.");
   if (schedule->krylov != FP_KRYLOV_NONE && schedule->krylov != FP_KRYLOV_FCG)
     return serverFail(S, FP_EINVAL, "krylov must be FP_KRYLOV_NONE or FP_KRYLOV_FCG.");
+  if (schedule->topology != 0 && schedule->topology != 1) return serverFail(S, FP_EINVAL, "topology must be 0 or 1.");
   if (vcycles < 1 || vcycles > FP_MAX_VCYCLES)
     return serverFail(S, FP_EINVAL, "vcycles must be from 1 to " + std::to_string(FP_MAX_VCYCLES) + ".");
   if (!std::isfinite(tolerance) || tolerance < 0.f)

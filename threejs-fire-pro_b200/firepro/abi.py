@@ -250,12 +250,13 @@ FP_KRYLOV_FCG = 1
 
 class fp_solver_schedule(C.Structure):
     _fields_ = [("smoother", C.c_int32), ("levels", C.c_int32), ("pre_sweeps", C.c_int32),
-                ("post_sweeps", C.c_int32), ("bottom_sweeps", C.c_int32), ("krylov", C.c_int32)]
+                ("post_sweeps", C.c_int32), ("bottom_sweeps", C.c_int32), ("krylov", C.c_int32),
+                ("topology", C.c_int32)]
 
 
-def schedule(smoother=FP_SMOOTHER_JACOBI, levels=0, pre=2, post=2, bottom=8, krylov=FP_KRYLOV_NONE):
+def schedule(smoother=FP_SMOOTHER_JACOBI, levels=0, pre=2, post=2, bottom=8, krylov=FP_KRYLOV_NONE, topology=0):
     """An fp_solver_schedule; the default is the reference's Jacobi V-cycle."""
-    return fp_solver_schedule(smoother, levels, pre, post, bottom, krylov)
+    return fp_solver_schedule(smoother, levels, pre, post, bottom, krylov, topology)
 
 
 class fp_phase(C.Structure):

@@ -32,15 +32,18 @@ class Candidate:
     tolerance: float
 
 
-def default_candidates(tolerance: float = 1e-6) -> list:
+def default_candidates() -> list:
+    """CG around Jacobi or red-black V-cycles with every brick's topology rebuilt each step (the
+    solve then sees the solids the projection sees), fixed V-cycle counts."""
     RB, J, FCG = abi.FP_SMOOTHER_REDBLACK, abi.FP_SMOOTHER_JACOBI, abi.FP_KRYLOV_FCG
-    return [
-        Candidate("fcg(jacobi)", abi.schedule(J, krylov=FCG), 16, tolerance),
-        Candidate("fcg(rb 2/2/8)", abi.schedule(RB, 0, 2, 2, 8, FCG), 16, tolerance),
-        Candidate("fcg(rb 1/1/4)", abi.schedule(RB, 0, 1, 1, 4, FCG), 16, tolerance),
-        Candidate("fcg(rb 4 levels 2/2/16)", abi.schedule(RB, 4, 2, 2, 16, FCG), 16, tolerance),
-        Candidate("rb 2/2/8 defect correction", abi.schedule(RB, 0, 2, 2, 8), 16, tolerance),
-    ]
+    out = []
+    for vc in (4, 5, 6, 8):
+        out.append(Candidate(f"fcg(rb 2/2/8) x{vc}", abi.schedule(RB, 0, 2, 2, 8, FCG, 1), vc, 0.0))
+    for vc in (6, 8):
+        out.append(Candidate(f"fcg(jacobi) x{vc}", abi.schedule(J, krylov=FCG, topology=1), vc, 0.0))
+    out.append(Candidate("fcg(rb 1/1/4) x8", abi.schedule(RB, 0, 1, 1, 4, FCG, 1), 8, 0.0))
+    out.append(Candidate("fcg(rb 4 levels 2/2/16) x6", abi.schedule(RB, 4, 2, 2, 16, FCG, 1), 6, 0.0))
+    return out
 
 
 @dataclass
