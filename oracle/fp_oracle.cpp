@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <array>
+#include <functional>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -927,24 +928,91 @@ struct Sim {
   }
 
   // ---------------------------------------------------------------- rendering (test oracle)
-  // updateBoxes (FluidSimulation.ts:916-957) for one cluster: content bricks and source
-  // bricks whose centre lies in a tile, two bricks of margin, within the tiles.
-  int renderLo[3] = {0, 0, 0}, renderHi[3] = {-1, -1, -1};
-  bool renderBox = false;
+  // TileDirectory.clusters (TileDirectory.ts:189-237) and updateBoxes (FluidSimulation.ts:
+  // 916-957): tiles grouped by touch in insertion order, groups boxed, overlapping boxes merged
+  // until none overlap; then per cluster the content and source bricks whose centre's tile lies
+  // in it, two bricks of margin, within the cluster's tiles. Boxes in cluster order, six ints
+  // each (lo xyz, hi xyz in bricks, inclusive).
+  std::vector<int> renderBoxes;
   std::vector<int> sourceBoxes;
   void updateRenderBox() {
-    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    bool any = false;
+    std::map<uint64_t, int> group;  // tile key -> group
+    std::vector<std::array<int, 6>> boxes;
+    for (auto& kv : dir.bySeq) {
+      const Tile& first = kv.second;
+      uint64_t fk = Directory::key(first.coord[0], first.coord[1], first.coord[2]);
+      if (group.count(fk)) continue;
+      int index = (int)boxes.size();
+      std::array<int, 6> box = {first.coord[0], first.coord[1], first.coord[2], first.coord[0], first.coord[1], first.coord[2]};
+      group[fk] = index;
+      std::vector<I3> stack = {first.coord};
+      while (!stack.empty()) {
+        I3 c = stack.back();
+        stack.pop_back();
+        for (int a = 0; a < 3; a++) {
+          box[a] = std::min(box[a], c[a]);
+          box[3 + a] = std::max(box[3 + a], c[a]);
+        }
+        for (int dz = -1; dz <= 1; dz++)
+          for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+              Tile* n = dir.find(c[0] + dx, c[1] + dy, c[2] + dz);
+              if (!n) continue;
+              uint64_t nk = Directory::key(n->coord[0], n->coord[1], n->coord[2]);
+              if (group.count(nk)) continue;
+              group[nk] = index;
+              stack.push_back(n->coord);
+            }
+      }
+      boxes.push_back(box);
+    }
+    std::vector<int> into(boxes.size());
+    for (size_t i = 0; i < into.size(); i++) into[i] = (int)i;
+    std::function<int(int)> root = [&](int i) { return into[i] == i ? i : (into[i] = root(into[i])); };
+    auto overlaps = [](const std::array<int, 6>& a, const std::array<int, 6>& b) {
+      for (int k = 0; k < 3; k++)
+        if (!(a[k] <= b[3 + k] && b[k] <= a[3 + k])) return false;
+      return true;
+    };
+    for (bool merged = true; merged;) {
+      merged = false;
+      for (size_t i = 0; i < boxes.size(); i++)
+        for (size_t j = i + 1; j < boxes.size(); j++) {
+          int a = root((int)i), b = root((int)j);
+          if (a == b || !overlaps(boxes[a], boxes[b])) continue;
+          for (int k = 0; k < 3; k++) {
+            boxes[a][k] = std::min(boxes[a][k], boxes[b][k]);
+            boxes[a][3 + k] = std::max(boxes[a][3 + k], boxes[b][3 + k]);
+          }
+          into[b] = a;
+          merged = true;
+        }
+    }
+    std::vector<int> renumbered(boxes.size(), -1);
+    std::vector<std::array<int, 6>> clusters;
+    for (size_t i = 0; i < boxes.size(); i++)
+      if (root((int)i) == (int)i) {
+        renumbered[i] = (int)clusters.size();
+        clusters.push_back(boxes[i]);
+      }
+    std::map<int, std::array<int, 6>> found;
     auto include = [&](const int* l, const int* u) {
       int c[3];
       for (int a = 0; a < 3; a++) c[a] = (int)std::floor(((double)l[a] + (double)u[a]) / 2.0);
       if (ground) c[1] = std::max(0, c[1]);
-      if (dir.slotAt((int)std::floor(c[0] / 4.0), (int)std::floor(c[1] / 4.0), (int)std::floor(c[2] / 4.0)) < 0) return;
-      for (int a = 0; a < 3; a++) {
-        lo[a] = any ? std::min(lo[a], l[a]) : l[a];
-        hi[a] = any ? std::max(hi[a], u[a]) : u[a];
+      int t[3] = {(int)std::floor(c[0] / 4.0), (int)std::floor(c[1] / 4.0), (int)std::floor(c[2] / 4.0)};
+      auto g = group.find(Directory::key(t[0], t[1], t[2]));
+      if (g == group.end()) return;
+      int cluster = renumbered[root(g->second)];
+      auto it = found.find(cluster);
+      if (it == found.end()) {
+        found[cluster] = {l[0], l[1], l[2], u[0], u[1], u[2]};
+        return;
       }
-      any = true;
+      for (int a = 0; a < 3; a++) {
+        it->second[a] = std::min(it->second[a], l[a]);
+        it->second[3 + a] = std::max(it->second[3 + a], u[a]);
+      }
     };
     for (auto& ct : contentTiles) {
       int l[3], u[3];
@@ -964,23 +1032,28 @@ struct Sim {
       }
       if (ok) include(l, u);
     }
-    for (size_t s = 0; s + 6 <= sourceBoxes.size(); s += 6) include(&sourceBoxes[s], &sourceBoxes[s + 3]);
-    renderBox = any;
-    if (!any) return;
-    int tlo[3] = {0, 0, 0}, thi[3] = {0, 0, 0};
-    bool first = true;
-    for (const auto& kv : dir.bySeq) {
-      const I3& t = kv.second.coord;
-      for (int a = 0; a < 3; a++) {
-        tlo[a] = first ? t[a] : std::min(tlo[a], t[a]);
-        thi[a] = first ? t[a] : std::max(thi[a], t[a]);
-      }
-      first = false;
+    for (size_t k = 0; k + 6 <= sourceBoxes.size(); k += 6) include(&sourceBoxes[k], &sourceBoxes[k + 3]);
+    renderBoxes.clear();
+    for (auto& kv : found) {
+      const std::array<int, 6>& tiles = clusters[kv.first];
+      for (int a = 0; a < 3; a++) renderBoxes.push_back(std::max(kv.second[a] - 2, tiles[a] * 4));
+      for (int a = 0; a < 3; a++) renderBoxes.push_back(std::min(kv.second[3 + a] + 2, (tiles[3 + a] + 1) * 4 - 1));
     }
-    for (int a = 0; a < 3; a++) {
-      renderLo[a] = std::max(lo[a] - 2, tlo[a] * 4);
-      renderHi[a] = std::min(hi[a] + 2, (thi[a] + 1) * 4 - 1);
+  }
+  // The box a render thread samples in (its pages and clamps): per thread.
+  static int* curBox() {
+    static thread_local int b[6] = {0, 0, 0, -1, -1, -1};
+    return b;
+  }
+  void useBox(int k) {
+    for (int a = 0; a < 6; a++) curBox()[a] = renderBoxes[(size_t)6 * k + a];
+  }
+  int boxOf(int bx, int by, int bz) const {
+    for (size_t k = 0; k + 6 <= renderBoxes.size(); k += 6) {
+      const int* b = &renderBoxes[k];
+      if (bx >= b[0] && bx <= b[3] && by >= b[1] && by <= b[4] && bz >= b[2] && bz <= b[5]) return (int)(k / 6);
     }
+    return -1;
   }
 
   // The render (lighting.wgsl, volume-march.wgsl, fire-emission.wgsl,
@@ -1002,8 +1075,15 @@ struct Sim {
            (uint64_t)(uint32_t)(z + (1 << 20));
   }
   bool boxed(int bx, int by, int bz) const {
-    return bx >= renderLo[0] && bx <= renderHi[0] && by >= renderLo[1] && by <= renderHi[1] && bz >= renderLo[2] &&
-           bz <= renderHi[2];
+    const int* b = curBox();
+    return bx >= b[0] && bx <= b[3] && by >= b[1] && by <= b[4] && bz >= b[2] && bz <= b[5];
+  }
+  // The render row of brick b when it lies in the current box.
+  template <class G_>
+  int rowOf(G_& G, int bx, int by, int bz) {
+    if (!boxed(bx, by, bz)) return -1;
+    auto it = G.index.find(brickKey(bx, by, bz));
+    return it == G.index.end() ? -1 : it->second;
   }
   int boxSlot(int bx, int by, int bz) { return boxed(bx, by, bz) ? brickSlot(bx, by, bz) : -1; }
   static R glowOf(R life) { return std::min(std::max(life * R(5), R(0)), R(1)); }
@@ -1013,7 +1093,7 @@ struct Sim {
   }
   void clampBox(R q[3], int per) {
     for (int a = 0; a < 3; a++)
-      q[a] = std::min(std::max(q[a], R(renderLo[a]) * R(per) + R(.5)), R(renderHi[a] + 1) * R(per) - R(.5));
+      q[a] = std::min(std::max(q[a], R(curBox()[a]) * R(per) + R(.5)), R(curBox()[3 + a] + 1) * R(per) - R(.5));
   }
   R smokeSample(R qx, R qy, R qz) {
     R q[3] = {qx, qy, qz};
@@ -1070,9 +1150,9 @@ struct Sim {
     return std::max(R(0), d * R(.125));
   }
   R renderSmokeCell(Render& G, int x, int y, int z, bool apron) {
-    auto it = G.index.find(brickKey(x >> sshift, y >> sshift, z >> sshift));
+    int row = rowOf(G, x >> sshift, y >> sshift, z >> sshift);
     int m = SB - 1;
-    if (it != G.index.end()) return G.smoke[(size_t)it->second * SN + ((z & m) * SB + (y & m)) * SB + (x & m)];
+    if (row >= 0) return G.smoke[(size_t)row * SN + ((z & m) * SB + (y & m)) * SB + (x & m)];
     return apron ? smoothedCoarse(x, y, z) : R(0);
   }
   R renderSmokeAt(Render& G, R qx, R qy, R qz) {
@@ -1085,7 +1165,7 @@ struct Sim {
       b[a] = (int)std::floor(g[a]);
       fr[a] = g[a] - R(b[a]);
     }
-    bool based = G.index.count(brickKey(b[0] >> sshift, b[1] >> sshift, b[2] >> sshift)) > 0;
+    bool based = rowOf(G, b[0] >> sshift, b[1] >> sshift, b[2] >> sshift) >= 0;
     R v = 0;
     for (int k = 0; k < 8; k++) {
       int d[3] = {k & 1, (k >> 1) & 1, k >> 2};
@@ -1096,19 +1176,19 @@ struct Sim {
   }
   R cachedSmokeCell(Render& G, int x, int y, int z) {
     int m = SB - 1, b[3] = {x >> sshift, y >> sshift, z >> sshift}, l[3] = {x & m, y & m, z & m};
-    auto it = G.index.find(brickKey(b[0], b[1], b[2]));
-    if (it != G.index.end()) return G.smoke[(size_t)it->second * SN + (l[2] * SB + l[1]) * SB + l[0]];
+    int row = rowOf(G, b[0], b[1], b[2]);
+    if (row >= 0) return G.smoke[(size_t)row * SN + (l[2] * SB + l[1]) * SB + l[0]];
     for (int k = 1; k < 8; k++) {
       if (((k & 1) && l[0] != 0) || ((k & 2) && l[1] != 0) || ((k & 4) && l[2] != 0)) continue;
-      if (G.index.count(brickKey(b[0] - (k & 1), b[1] - ((k >> 1) & 1), b[2] - ((k >> 2) & 1))))
+      if (rowOf(G, b[0] - (k & 1), b[1] - ((k >> 1) & 1), b[2] - ((k >> 2) & 1)) >= 0)
         return smoothedCoarse(x, y, z);
     }
     return R(0);
   }
   std::array<R, 4> renderCell(Render& G, int x, int y, int z, bool apron) {
-    auto it = G.index.find(brickKey(x >> shift, y >> shift, z >> shift));
-    if (it != G.index.end()) {
-      size_t o = (size_t)it->second * 4 * N + local(x, y, z);
+    int row = rowOf(G, x >> shift, y >> shift, z >> shift);
+    if (row >= 0) {
+      size_t o = (size_t)row * 4 * N + local(x, y, z);
       return {G.field[o], G.field[o + N], G.field[o + 2 * N], G.field[o + 3 * N]};
     }
     // With coarse smoke the render reads the simulation's fields, whose apron holds zero where
@@ -1126,7 +1206,7 @@ struct Sim {
       b[a] = (int)std::floor(g[a]);
       fr[a] = g[a] - R(b[a]);
     }
-    bool based = G.index.count(brickKey(b[0] >> shift, b[1] >> shift, b[2] >> shift)) > 0;
+    bool based = rowOf(G, b[0] >> shift, b[1] >> shift, b[2] >> shift) >= 0;
     std::array<R, 4> v = {0, 0, 0, 0};
     for (int k = 0; k < 8; k++) {
       int d[3] = {k & 1, (k >> 1) & 1, k >> 2};
@@ -1198,7 +1278,7 @@ struct Sim {
   std::array<R, 4> sampleWorld(Render& G, R px, R py, R pz) {
     R size = R(B) * h, p[3] = {px, py, pz};
     for (int a = 0; a < 3; a++)
-      if (p[a] < R(renderLo[a]) * size || p[a] > R(renderHi[a] + 1) * size) return {0, 0, 0, 0};
+      if (p[a] < R(curBox()[a]) * size || p[a] > R(curBox()[3 + a] + 1) * size) return {0, 0, 0, 0};
     auto f = renderSample(G, px / h, py / h, pz / h);
     if (smokeDiv > 1) f[0] = renderSmokeAt(G, px / h / R(smokeDiv), py / h / R(smokeDiv), pz / h / R(smokeDiv));
     return f;
@@ -1212,7 +1292,7 @@ struct Sim {
     R size = R(B) * h, exit = R(1e30);
     for (int a = 0; a < 3; a++) {
       if (!(std::fabs(sun[a]) > R(1e-6))) continue;
-      R edge = (sun[a] > 0 ? R(renderHi[a] + 1) : R(renderLo[a])) * size;
+      R edge = (sun[a] > 0 ? R(curBox()[3 + a] + 1) : R(curBox()[a])) * size;
       exit = std::min(exit, (edge - p[a]) / sun[a]);
     }
     exit = std::max(R(0), exit);
@@ -1255,17 +1335,17 @@ struct Sim {
       b[a] = (int)std::floor(g[a]);
       fr[a] = g[a] - R(b[a]);
     }
-    if (!G.index.count(brickKey(b[0] >> G.lightShift, b[1] >> G.lightShift, b[2] >> G.lightShift))) return {0, 0, 0, 1};
+    if (rowOf(G, b[0] >> G.lightShift, b[1] >> G.lightShift, b[2] >> G.lightShift) < 0) return {0, 0, 0, 1};
     std::array<R, 4> v = {0, 0, 0, 0};
     for (int k = 0; k < 8; k++) {
       int d[3] = {k & 1, (k >> 1) & 1, k >> 2};
       int x = b[0] + d[0], y = b[1] + d[1], z = b[2] + d[2];
       R w = (d[0] ? fr[0] : 1 - fr[0]) * (d[1] ? fr[1] : 1 - fr[1]) * (d[2] ? fr[2] : 1 - fr[2]);
-      auto it = G.index.find(brickKey(x >> G.lightShift, y >> G.lightShift, z >> G.lightShift));
+      int row = rowOf(G, x >> G.lightShift, y >> G.lightShift, z >> G.lightShift);
       std::array<R, 4> t;
-      if (it != G.index.end()) {
+      if (row >= 0) {
         int m = L - 1;
-        size_t o = (size_t)it->second * 4 * L3 + (((z & m) * L + (y & m)) * L + (x & m));
+        size_t o = (size_t)row * 4 * L3 + (((z & m) * L + (y & m)) * L + (x & m));
         t = {G.light[o], G.light[o + L3], G.light[o + 2 * L3], G.light[o + 3 * L3]};
       } else {
         t = incidentLight(G, (R(x) + R(.5)) * texel, (R(y) + R(.5)) * texel, (R(z) + R(.5)) * texel);
@@ -1358,13 +1438,18 @@ struct Sim {
     int divShift = rs.lighting_divisor == 1 ? 0 : (rs.lighting_divisor == 2 ? 1 : 2);
     G.lightShift = shift - divShift;
     const int L = 1 << G.lightShift, L3 = L * L * L, per = B / 8, blocks = per * per * per;
+    // Every slotted computing brick inside a box (boxes never overlap), with its box.
     std::vector<I3> bricks;
-    for (uint32_t id : active) {
-      I3 b = brickOf(id);
-      if (boxSlot(b[0], b[1], b[2]) < 0) continue;
-      G.index[brickKey(b[0], b[1], b[2])] = (int)bricks.size();
-      bricks.push_back(b);
-    }
+    std::vector<int> boxOfRow;
+    if (steps > 0)
+      for (uint32_t id : active) {
+        I3 b = brickOf(id);
+        int k = boxOf(b[0], b[1], b[2]);
+        if (k < 0 || brickSlot(b[0], b[1], b[2]) < 0) continue;
+        G.index[brickKey(b[0], b[1], b[2])] = (int)bricks.size();
+        bricks.push_back(b);
+        boxOfRow.push_back(k);
+      }
     size_t nb = bricks.size();
     G.field.assign(nb * 4 * N, 0);
     if (smokeDiv > 1) G.smoke.assign(nb * SN, 0);
@@ -1373,6 +1458,7 @@ struct Sim {
 #pragma omp parallel for schedule(dynamic)
     for (long r = 0; r < (long)nb; r++) {
       const I3& b = bricks[r];
+      useBox(boxOfRow[r]);
       int s = boxSlot(b[0], b[1], b[2]);
       for (int k = 0; k < N; k++) {
         int x = b[0] * B + (k & (B - 1)), y = b[1] * B + ((k >> shift) & (B - 1)), z = b[2] * B + (k >> (2 * shift));
@@ -1389,6 +1475,7 @@ struct Sim {
 #pragma omp parallel for schedule(dynamic)
     for (long r = 0; r < (long)nb; r++) {
       const I3& b = bricks[r];
+      useBox(boxOfRow[r]);
       for (int blk = 0; blk < blocks; blk++) {
         int o[3] = {b[0] * B + (blk % per) * 8 - 2, b[1] * B + ((blk / per) % per) * 8 - 2,
                     b[2] * B + (blk / (per * per)) * 8 - 2};
@@ -1397,7 +1484,7 @@ struct Sim {
         R glowMax = 0, smokeMax = 0;
         for (int u = 0; u < 216; u++) {
           int ux = o[0] + (u % 6) * 2, uy = o[1] + ((u / 6) % 6) * 2, uz = o[2] + (u / 36) * 2;
-          if (!G.index.count(brickKey(ux >> shift, uy >> shift, uz >> shift))) continue;
+          if (rowOf(G, ux >> shift, uy >> shift, uz >> shift) < 0) continue;
           for (int k = 0; k < 8; k++) {
             auto f = renderCell(G, ux + (k & 1), uy + ((k >> 1) & 1), uz + (k >> 2), true);
             R g = glowOf(f[2]);
@@ -1416,7 +1503,7 @@ struct Sim {
             for (int y = lo[1]; y <= hi[1]; y++)
               for (int x = lo[0]; x <= hi[0]; x++) {
                 int q[3] = {x, y, z};
-                for (int a = 0; a < 3; a++) q[a] = std::min(std::max(q[a], renderLo[a] * SB), (renderHi[a] + 1) * SB - 1);
+                for (int a = 0; a < 3; a++) q[a] = std::min(std::max(q[a], curBox()[a] * SB), (curBox()[3 + a] + 1) * SB - 1);
                 smokeMax = std::max(smokeMax, cachedSmokeCell(G, q[0], q[1], q[2]));
               }
           if (smokeMax + glowMax > R(.002)) flags |= 2;
@@ -1437,6 +1524,38 @@ struct Sim {
       R ro[3], rd[3], safe[3], exitSide[3], lo, hi, stepSize, jitter, direct[3];
     };
     const R brickSize = h * R(B), lightRatio = R(B >> G.lightShift);
+    const int boxCount = steps > 0 ? (int)(renderBoxes.size() / 6) : 0;
+    // fireProHit: entry and exit of box k (the exit first when it misses).
+    auto boxHit = [&](const Ray& r, int k, R* hit) {
+      const int* bx = &renderBoxes[(size_t)6 * k];
+      R lo = 0, hi = R(1e30);
+      for (int a = 0; a < 3; a++) {
+        R ta = (R(bx[a]) * brickSize - r.ro[a]) / r.safe[a], tb = (R(bx[3 + a] + 1) * brickSize - r.ro[a]) / r.safe[a];
+        lo = std::max(lo, std::min(ta, tb));
+        hi = std::min(hi, std::max(ta, tb));
+      }
+      hit[0] = lo;
+      hit[1] = hi;
+    };
+    // fireProEnter: the box the ray is in at t, or enters next, becomes the current one.
+    auto enterBox = [&](const Ray& r, R& t, R& exit) -> bool {
+      R entry = R(1e30), out = 0;
+      int best = -1;
+      for (int k = 0; k < boxCount; k++) {
+        R hit[2];
+        boxHit(r, k, hit);
+        if (hit[1] > hit[0] && hit[1] > t && hit[0] < entry) {
+          entry = hit[0];
+          out = hit[1];
+          best = k;
+        }
+      }
+      if (best < 0) return false;
+      useBox(best);
+      exit = out;
+      t = std::max(t, entry);
+      return true;
+    };
     auto rayOf = [&](R ux, R uy, Ray& r) -> bool {
       R cx = ux * 2 - 1, cy = 1 - uy * 2;
       const float* M = cam.inverse_view_projection;
@@ -1451,17 +1570,25 @@ struct Sim {
       }
       R rl = std::sqrt(r.rd[0] * r.rd[0] + r.rd[1] * r.rd[1] + r.rd[2] * r.rd[2]);
       for (int a = 0; a < 3; a++) r.rd[a] /= rl;
-      r.lo = 0;
-      r.hi = R(1e30);
       for (int a = 0; a < 3; a++) {
         r.safe[a] = std::fabs(r.rd[a]) > R(1e-6) ? r.rd[a] : R(1e-6);
         r.exitSide[a] = r.rd[a] > 0 ? 1 : 0;
-        R ta = (R(renderLo[a]) * brickSize - r.ro[a]) / r.safe[a], tb = (R(renderHi[a] + 1) * brickSize - r.ro[a]) / r.safe[a];
-        r.lo = std::max(r.lo, std::min(ta, tb));
-        r.hi = std::min(r.hi, std::max(ta, tb));
+      }
+      // fireProSpan: first entry, last exit, length inside every box.
+      r.lo = R(1e30);
+      r.hi = 0;
+      R length = 0;
+      for (int k = 0; k < boxCount; k++) {
+        R hit[2];
+        boxHit(r, k, hit);
+        if (hit[1] > hit[0]) {
+          r.lo = std::min(r.lo, hit[0]);
+          r.hi = std::max(r.hi, hit[1]);
+          length += hit[1] - hit[0];
+        }
       }
       if (!(r.hi > r.lo)) return false;
-      r.stepSize = std::max(h * R(.5), (r.hi - r.lo) / R(rs.ray_steps));
+      r.stepSize = std::max(h * R(.5), length / R(rs.ray_steps));
       R ln = std::sqrt(R(rs.light[0]) * rs.light[0] + R(rs.light[1]) * rs.light[1] + R(rs.light[2]) * rs.light[2]);
       R g = rs.optical[3];
       R mu = (r.rd[0] * rs.light[0] + r.rd[1] * rs.light[1] + r.rd[2] * rs.light[2]) / ln;
@@ -1471,24 +1598,24 @@ struct Sim {
       return true;
     };
     // One step of fireProMarch at t, ds long; returns the next t.
-    auto marchStep = [&](const Ray& r, R t, R ds, R& trans, R* rad) -> R {
+    auto marchStep = [&](const Ray& r, R t, R ds, R exit, R& trans, R* rad) -> R {
       R tt = t + r.jitter * ds;
       R p[3] = {r.ro[0] + r.rd[0] * tt, r.ro[1] + r.rd[1] * tt, r.ro[2] + r.rd[2] * tt};
       R cell[3] = {p[0] / h, p[1] / h, p[2] / h};
       int ci[3] = {(int)std::floor(cell[0]), (int)std::floor(cell[1]), (int)std::floor(cell[2])};
-      auto it = G.index.find(brickKey(ci[0] >> shift, ci[1] >> shift, ci[2] >> shift));
+      int row = rowOf(G, ci[0] >> shift, ci[1] >> shift, ci[2] >> shift);
       R size = brickSize;
       int flags = 0;
-      if (it != G.index.end()) {
+      if (row >= 0) {
         int m = B - 1;
         int block = ((((ci[2] & m) >> 3) * per) + ((ci[1] & m) >> 3)) * per + ((ci[0] & m) >> 3);
-        flags = G.occupancy[(size_t)it->second * blocks + block];
+        flags = G.occupancy[(size_t)row * blocks + block];
         size = h * 8;
       }
       if (!(flags & 2)) {
         R dist = R(1e30);
         for (int a = 0; a < 3; a++) dist = std::min(dist, ((std::floor(p[a] / size) + r.exitSide[a]) * size - p[a]) / r.safe[a]);
-        return std::min(t + std::max(R(1), std::floor(dist / r.stepSize) + 1) * r.stepSize, r.hi);
+        return std::min(t + std::max(R(1), std::floor(dist / r.stepSize) + 1) * r.stepSize, exit);
       }
       auto f = reconstruct(G, cell[0], cell[1], cell[2], (flags & 1) ? rs.filter : 0);
       if (smokeDiv > 1) f[0] = renderSmokeAt(G, cell[0] / R(smokeDiv), cell[1] / R(smokeDiv), cell[2] / R(smokeDiv));
@@ -1511,7 +1638,7 @@ struct Sim {
     // buildSlices (volume-slices.wgsl:28-122) at half resolution.
     const int SW = std::max(1, (W + 1) / 2), SH = std::max(1, (Hh + 1) / 2), NS = 8;
     std::vector<R> slices;
-    const bool half = cam.half_resolution != 0 && renderBox && steps > 0;
+    const bool half = cam.half_resolution != 0 && boxCount > 0;
     if (half) {
       slices.assign((size_t)SW * SH * NS * 4, 0);
 #pragma omp parallel for schedule(dynamic)
@@ -1523,10 +1650,14 @@ struct Sim {
         Ray r;
         if (rayOf((R(px) + R(.5)) / R(SW), (R(py) + R(.5)) / R(SH), r)) {
           r.jitter = jitterOf((uint32_t)px, (uint32_t)py, cam.time);
-          R spacing = std::max(r.hi - r.lo, R(0)) / R(NS), t = r.lo, depth = r.lo + spacing;
+          R spacing = std::max(r.hi - r.lo, R(0)) / R(NS), t = r.lo, depth = r.lo + spacing, exit = t;
           while (recorded < NS && t < r.hi && trans >= R(.008)) {
-            R ds = std::min(r.stepSize, std::min(depth, r.hi) - t);
-            t = marchStep(r, t, ds, trans, rad);
+            if (t >= exit) {
+              if (!enterBox(r, t, exit)) break;
+            } else {
+              R ds = std::min(r.stepSize, std::min(depth, exit) - t);
+              t = marchStep(r, t, ds, exit, trans, rad);
+            }
             while (recorded < NS && t >= depth) {
               R v[4] = {rad[0], rad[1], rad[2], 1 - trans};
               for (int c = 0; c < 4; c++) out[recorded * 4 + c] = v[c];
@@ -1546,7 +1677,7 @@ struct Sim {
       int px = (int)(pix % W), py = (int)(pix / W);
       float* out = image + pix * 4;
       out[0] = out[1] = out[2] = out[3] = 0.f;
-      if (!renderBox || steps == 0) continue;
+      if (boxCount == 0) continue;
       R ux = (R(px) + R(.5)) / R(W), uy = (R(py) + R(.5)) / R(Hh);
       Ray r;
       if (!rayOf(ux, uy, r)) continue;
@@ -1583,10 +1714,14 @@ struct Sim {
           for (int c = 0; c < 3; c++) rad[c] = v[c];
         }
       }
+      R exit = t;  // fireProMarch's cursor starts exited: the first pass enters the box at t
       while (t < end && trans >= R(.008)) {
-        if (t >= r.hi) break;
-        R ds = std::min(r.stepSize, std::min(end, r.hi) - t);
-        t = marchStep(r, t, ds, trans, rad);
+        if (t >= exit) {
+          if (!enterBox(r, t, exit)) break;
+          continue;
+        }
+        R ds = std::min(r.stepSize, std::min(end, exit) - t);
+        t = marchStep(r, t, ds, exit, trans, rad);
       }
       out[0] = (float)rad[0];
       out[1] = (float)rad[1];

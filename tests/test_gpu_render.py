@@ -179,3 +179,36 @@ def test_scene_depth_and_half_resolution(half):
     # the depth clipped something, and nothing where the band is open
     assert np.abs(out["open"] - orc).max() > 1e-3
     assert np.allclose(out["open"][:, : w // 8], orc[:, : w // 8], atol=1e-5) or half
+
+
+class TwoFires(scenes.Scene):
+    """Two burning emitters 4.4 m apart: their tiles form two clusters, so the render marches two
+    boxes (TileDirectory.clusters, FluidSimulation.updateBoxes) and a ray between them crosses
+    empty space that no box holds."""
+
+    name = "two_fires"
+
+    def __init__(self):
+        self.settings = scenes.settings(buoyancy=1.5, vorticity=0.5, seed=9)
+        self.comb = scenes.combustion()
+
+    def frame(self, step):
+        srcs = [scenes.source(1, "sphere", (-2.2, 0.25, 0.0), (0.2, 0.2, 0.2), flame=0.9, heat=2.0, smoke=1.5, fuel=0.6),
+                scenes.source(2, "box", (2.2, 0.25, 0.1), (0.15, 0.15, 0.15), flame=0.7, heat=1.5, smoke=2.0, fuel=0.4)]
+        return scenes.make_frame(self.settings, self.comb, True, srcs)
+
+
+@pytest.mark.parametrize("half", [0, 1])
+def test_two_cluster_render_parity(half):
+    """One render box per cluster of tiles: the passes clamp and page within each brick's own
+    box, the march crosses the boxes in order (span, step and slices over all of them)."""
+    cam = render.look_at((0.0, 1.2, 6.5), (0.0, 0.5, 0.0), 96, 48, time=0.25)
+    cam.half_resolution = half
+    st = render.default_settings(ray_steps=128)
+    gpu, orc = render_pair(TwoFires(), 14, 2 ** 21, cam, st)
+    assert np.isfinite(gpu).all()
+    left, right = orc[:, :48, 3].max(), orc[:, 48:, 3].max()
+    assert left > 0.02 and right > 0.02, (left, right)
+    err = parity.rel_l2(gpu, orc.astype(np.float64))
+    print(f"two clusters (half {half}): relative L2 {err:.2e}")
+    assert err <= RENDER_TOL

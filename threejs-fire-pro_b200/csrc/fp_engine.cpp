@@ -43,7 +43,7 @@ void TileDirectory::need(int lx, int ly, int lz, int hx, int hy, int hz, int64_t
           slot = (int)slots_.size();
           slots_.push_back(Tile{});
         }
-        slots_[slot] = Tile{x, y, z, step, false, true};
+        slots_[slot] = Tile{x, y, z, step, false, true, nextSeq_++};
         index_[key(x, y, z)] = slot;
         created_.push_back(slot);
         dirty = true;
@@ -183,7 +183,7 @@ Engine::~Engine() {
   owner_->forget(this);
   cudaStreamSynchronize(stream());
   freeAll();
-  DeviceBuffer* render[] = {&renderField_, &renderSmoke_, &sceneDepth_, &slices_, &lighting_, &occupancy_, &lut_, &renderParams_, &image_, &anchors_, &lightSums_};
+  DeviceBuffer* render[] = {&renderField_, &renderSmoke_, &sceneDepth_, &slices_, &lighting_, &occupancy_, &lut_, &renderParams_, &image_, &anchors_, &lightSums_, &renderBoxesD_};
   for (DeviceBuffer* b : render)
     if (b->ptr) cudaFree(b->ptr);
   if (renderParamsH_) cudaFreeHost(renderParamsH_);
@@ -467,6 +467,7 @@ int Engine::applyTiles() {
     cudaMemsetAsync((char*)state_.ptr + off, 0, 64 * 4, stream());
     cudaMemsetAsync((char*)activity_.ptr + off, 0, 64 * 4, stream());
   }
+  buildClusters();
   dir_.dirty = false;
   geometryDirty_ = true;  // PressureSolver.setBricks -> resetPlans
   return FP_OK;

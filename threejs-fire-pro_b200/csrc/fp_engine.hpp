@@ -35,6 +35,7 @@ class TileDirectory {
     int64_t needed;
     bool closing;
     bool alive;
+    uint64_t seq;  // creation order (the reference's Map keeps tiles in insertion order)
   };
   bool ground = true;
   bool dirty = true;
@@ -56,6 +57,7 @@ class TileDirectory {
   std::vector<Tile> slots_;
   std::unordered_map<uint64_t, int> index_;
   std::vector<int> created_;
+  uint64_t nextSeq_ = 0;
 };
 
 struct DeviceBuffer {
@@ -209,10 +211,13 @@ class Engine {
 
   // rendering: the box in bricks (inclusive) from the latest step's content and sources, the
   // render pools and the parameters of a render
-  int renderLo_[3] = {0, 0, 0}, renderHi_[3] = {-1, -1, -1};
-  bool renderBox_ = false;
+  // TileDirectory.clusters (TileDirectory.ts:189-237), built with the tables: each tile slot's
+  // cluster (-1 none) and each cluster's box of tiles (lo xyz, hi xyz); the render boxes of the
+  // latest step in bricks (lo xyz, hi xyz inclusive), one per cluster with content or sources.
+  std::vector<int> clusterOf_, clusterBoxes_, renderBoxes_;
+  void buildClusters();
   std::vector<int> sourceBoxes_;  // lo xyz, hi xyz per source
-  DeviceBuffer renderField_, renderSmoke_, sceneDepth_, slices_, lighting_, occupancy_, lut_, renderParams_, image_, anchors_, lightSums_;
+  DeviceBuffer renderField_, renderSmoke_, sceneDepth_, slices_, lighting_, occupancy_, lut_, renderParams_, image_, anchors_, lightSums_, renderBoxesD_;
   SimParams* renderParamsH_ = nullptr;
   // The blackbody table and the render parameters of the latest state (device).
   int renderInputs();

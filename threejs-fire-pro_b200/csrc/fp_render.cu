@@ -9,9 +9,10 @@
 // Where the reference reads a pool slot's apron (a copy of the +1 neighbours), these kernels
 // read the neighbour's slot; a neighbour without a slot reads what the apron would hold: the
 // smoothed density computed on the spot for the render field, the incident light computed on
-// the spot for the lighting pool. The render uses one box: the bricks with content and the
-// sources' bricks, with a margin of two bricks, within the tiles (FluidSimulation.ts:916-957
-// for a scene of one cluster).
+// the spot for the lighting pool. The render marches one box per cluster of tiles that holds
+// content or sources (FluidSimulation.ts:916-957, TileDirectory.ts:189-245): a sample reads the
+// pages of the box it lies in only, clamped to that box, and a ray crosses the boxes in order
+// (volume-march.wgsl fireProSpan, fireProNext, fireProEnter).
 #include "fp_device.cuh"
 #include "fp_render.h"
 
@@ -19,24 +20,45 @@ namespace {
 
 constexpr int RTHREADS = 128;
 
-// A thread's last brick lookup.
+// A thread's current box (the pages its samples read) and its last brick lookup.
 struct SlotCache {
   int bx, by, bz, slot;
+  int lo[3], hi[3];  // the current box in bricks, inclusive
 };
-
-FP_DEV bool inBox(const FpRender& R, int bx, int by, int bz) {
-  return bx >= R.boxLo[0] && bx <= R.boxHi[0] && by >= R.boxLo[1] && by <= R.boxHi[1] && bz >= R.boxLo[2] &&
-         bz <= R.boxHi[2];
+FP_DEV SlotCache noBox() {
+  SlotCache c;
+  c.bx = 1 << 30;
+  c.by = c.bz = 0;
+  c.slot = -1;
+  for (int a = 0; a < 3; a++) {
+    c.lo[a] = 0;
+    c.hi[a] = -1;
+  }
+  return c;
 }
-// fireProPage: the slot of world brick b inside the box, or -1.
+// Box k becomes the current one; the lookup cache starts over (pages are per box).
+FP_DEV void useBox(const FpRender& R, SlotCache& c, int k) {
+  for (int a = 0; a < 3; a++) {
+    c.lo[a] = R.boxes[6 * k + a];
+    c.hi[a] = R.boxes[6 * k + 3 + a];
+  }
+  c.bx = 1 << 30;
+}
+FP_DEV bool inBox(const SlotCache& c, int bx, int by, int bz) {
+  return bx >= c.lo[0] && bx <= c.hi[0] && by >= c.lo[1] && by <= c.hi[1] && bz >= c.lo[2] && bz <= c.hi[2];
+}
+// fireProPage: the slot of world brick b inside the current box, or -1.
 FP_DEV int slotAt(const SimParams& P, const FpRender& R, SlotCache& c, int bx, int by, int bz) {
   if (bx == c.bx && by == c.by && bz == c.bz) return c.slot;
   int s = -1;
-  if (inBox(R, bx, by, bz)) {
+  if (inBox(c, bx, by, bz)) {
     int t = hashFind(P, bx >> 2, by >> 2, bz >> 2);
     if (t >= 0) s = entryPage(P.entries[t * 64 + (((bz & 3) * 4 + (by & 3)) * 4 + (bx & 3))]);
   }
-  c = SlotCache{bx, by, bz, s};
+  c.bx = bx;
+  c.by = by;
+  c.bz = bz;
+  c.slot = s;
   return s;
 }
 
@@ -51,9 +73,9 @@ FP_DEV float rawSmoke(const SimParams& P, const FpRender& R, SlotCache& c, int x
 // fireProField of the smoke at `q` in cells: clamped to the box, trilinear.
 FP_DEV float smokeSample(const SimParams& P, const FpRender& R, SlotCache& c, float qx, float qy, float qz) {
   float B = (float)P.B;
-  qx = fminf(fmaxf(qx, (float)R.boxLo[0] * B + .5f), (float)(R.boxHi[0] + 1) * B - .5f);
-  qy = fminf(fmaxf(qy, (float)R.boxLo[1] * B + .5f), (float)(R.boxHi[1] + 1) * B - .5f);
-  qz = fminf(fmaxf(qz, (float)R.boxLo[2] * B + .5f), (float)(R.boxHi[2] + 1) * B - .5f);
+  qx = fminf(fmaxf(qx, (float)c.lo[0] * B + .5f), (float)(c.hi[0] + 1) * B - .5f);
+  qy = fminf(fmaxf(qy, (float)c.lo[1] * B + .5f), (float)(c.hi[1] + 1) * B - .5f);
+  qz = fminf(fmaxf(qz, (float)c.lo[2] * B + .5f), (float)(c.hi[2] + 1) * B - .5f);
   float gx = qx - .5f, gy = qy - .5f, gz = qz - .5f;
   int x0 = (int)floorf(gx), y0 = (int)floorf(gy), z0 = (int)floorf(gz);
   float fx = gx - (float)x0, fy = gy - (float)y0, fz = gz - (float)z0;
@@ -84,9 +106,9 @@ FP_DEV float rawCoarse(const SimParams& P, const FpRender& R, SlotCache& c, int 
 // fireProField of the coarse density at `q` in coarse cells: clamped to the box, trilinear.
 FP_DEV float coarseSample(const SimParams& P, const FpRender& R, SlotCache& c, float qx, float qy, float qz) {
   float S = (float)(1 << P.smokeShift);
-  qx = fminf(fmaxf(qx, (float)R.boxLo[0] * S + .5f), (float)(R.boxHi[0] + 1) * S - .5f);
-  qy = fminf(fmaxf(qy, (float)R.boxLo[1] * S + .5f), (float)(R.boxHi[1] + 1) * S - .5f);
-  qz = fminf(fmaxf(qz, (float)R.boxLo[2] * S + .5f), (float)(R.boxHi[2] + 1) * S - .5f);
+  qx = fminf(fmaxf(qx, (float)c.lo[0] * S + .5f), (float)(c.hi[0] + 1) * S - .5f);
+  qy = fminf(fmaxf(qy, (float)c.lo[1] * S + .5f), (float)(c.hi[1] + 1) * S - .5f);
+  qz = fminf(fmaxf(qz, (float)c.lo[2] * S + .5f), (float)(c.hi[2] + 1) * S - .5f);
   float gx = qx - .5f, gy = qy - .5f, gz = qz - .5f;
   int x0 = (int)floorf(gx), y0 = (int)floorf(gy), z0 = (int)floorf(gz);
   float fx = gx - (float)x0, fy = gy - (float)y0, fz = gz - (float)z0;
@@ -118,9 +140,9 @@ FP_DEV float renderSmokeCell(const SimParams& P, const FpRender& R, SlotCache& c
 FP_DEV float renderSmokeAt(const SimParams& P, const FpRender& R, SlotCache& c, float qx, float qy, float qz) {
   const int sh = P.smokeShift;
   float S = (float)(1 << sh);
-  qx = fminf(fmaxf(qx, (float)R.boxLo[0] * S + .5f), (float)(R.boxHi[0] + 1) * S - .5f);
-  qy = fminf(fmaxf(qy, (float)R.boxLo[1] * S + .5f), (float)(R.boxHi[1] + 1) * S - .5f);
-  qz = fminf(fmaxf(qz, (float)R.boxLo[2] * S + .5f), (float)(R.boxHi[2] + 1) * S - .5f);
+  qx = fminf(fmaxf(qx, (float)c.lo[0] * S + .5f), (float)(c.hi[0] + 1) * S - .5f);
+  qy = fminf(fmaxf(qy, (float)c.lo[1] * S + .5f), (float)(c.hi[1] + 1) * S - .5f);
+  qz = fminf(fmaxf(qz, (float)c.lo[2] * S + .5f), (float)(c.hi[2] + 1) * S - .5f);
   float gx = qx - .5f, gy = qy - .5f, gz = qz - .5f;
   int x0 = (int)floorf(gx), y0 = (int)floorf(gy), z0 = (int)floorf(gz);
   float fx = gx - (float)x0, fy = gy - (float)y0, fz = gz - (float)z0;
@@ -171,9 +193,9 @@ FP_DEV void add4(float4& a, const float4& b, float w) {
 // fireProField of the render field at `q` in cells (fireProSample, volume-bricks.wgsl).
 FP_DEV float4 renderSample(const SimParams& P, const FpRender& R, SlotCache& c, float qx, float qy, float qz) {
   float B = (float)P.B;
-  qx = fminf(fmaxf(qx, (float)R.boxLo[0] * B + .5f), (float)(R.boxHi[0] + 1) * B - .5f);
-  qy = fminf(fmaxf(qy, (float)R.boxLo[1] * B + .5f), (float)(R.boxHi[1] + 1) * B - .5f);
-  qz = fminf(fmaxf(qz, (float)R.boxLo[2] * B + .5f), (float)(R.boxHi[2] + 1) * B - .5f);
+  qx = fminf(fmaxf(qx, (float)c.lo[0] * B + .5f), (float)(c.hi[0] + 1) * B - .5f);
+  qy = fminf(fmaxf(qy, (float)c.lo[1] * B + .5f), (float)(c.hi[1] + 1) * B - .5f);
+  qz = fminf(fmaxf(qz, (float)c.lo[2] * B + .5f), (float)(c.hi[2] + 1) * B - .5f);
   float gx = qx - .5f, gy = qy - .5f, gz = qz - .5f;
   int x0 = (int)floorf(gx), y0 = (int)floorf(gy), z0 = (int)floorf(gz);
   float fx = gx - (float)x0, fy = gy - (float)y0, fz = gz - (float)z0;
@@ -254,8 +276,8 @@ FP_DEV float3 emissionOf(const FpRender& R, const float4& f) {
 // the box.
 FP_DEV float4 sampleWorld(const SimParams& P, const FpRender& R, SlotCache& c, float px, float py, float pz) {
   float size = (float)P.B * P.h;
-  if (px < (float)R.boxLo[0] * size || py < (float)R.boxLo[1] * size || pz < (float)R.boxLo[2] * size ||
-      px > (float)(R.boxHi[0] + 1) * size || py > (float)(R.boxHi[1] + 1) * size || pz > (float)(R.boxHi[2] + 1) * size)
+  if (px < (float)c.lo[0] * size || py < (float)c.lo[1] * size || pz < (float)c.lo[2] * size ||
+      px > (float)(c.hi[0] + 1) * size || py > (float)(c.hi[1] + 1) * size || pz > (float)(c.hi[2] + 1) * size)
     return make_float4(0.f, 0.f, 0.f, 0.f);
   float4 f = renderSample(P, R, c, px / P.h, py / P.h, pz / P.h);
   if (P.smokeDiv > 1) {
@@ -266,13 +288,13 @@ FP_DEV float4 sampleWorld(const SimParams& P, const FpRender& R, SlotCache& c, f
 }
 
 // exitDistance (lighting.wgsl:248-255).
-FP_DEV float exitDistance(const SimParams& P, const FpRender& R, float px, float py, float pz, float dx, float dy,
+FP_DEV float exitDistance(const SimParams& P, const SlotCache& c, float px, float py, float pz, float dx, float dy,
                           float dz) {
   float size = (float)P.B * P.h;
   float p[3] = {px, py, pz}, d[3] = {dx, dy, dz}, m = 1e30f;
   for (int a = 0; a < 3; a++) {
     if (!(fabsf(d[a]) > 1e-6f)) continue;
-    float edge = (d[a] > 0.f ? (float)(R.boxHi[a] + 1) : (float)R.boxLo[a]) * size;
+    float edge = (d[a] > 0.f ? (float)(c.hi[a] + 1) : (float)c.lo[a]) * size;
     m = fminf(m, (edge - p[a]) / d[a]);
   }
   return fmaxf(0.f, m);
@@ -292,7 +314,7 @@ FP_DEV float4 incidentLight(const SimParams& P, const FpRender& R, SlotCache& c,
   float ln = sqrtf(R.light[0] * R.light[0] + R.light[1] * R.light[1] + R.light[2] * R.light[2]);
   float sx = R.light[0] / ln, sy = R.light[1] / ln, sz = R.light[2] / ln;
   int count = R.shadowSamples;
-  float ds = exitDistance(P, R, px, py, pz, sx, sy, sz) / (float)count;
+  float ds = exitDistance(P, c, px, py, pz, sx, sy, sz) / (float)count;
   float depth = 0.f;
   if (R.light[3] > 0.f) {
     for (int i = 0; i < count; i++) {
@@ -327,7 +349,8 @@ FP_DEV float4 incidentLight(const SimParams& P, const FpRender& R, SlotCache& c,
   return make_float4(glow.x, glow.y, glow.z, expf(-depth));
 }
 
-// The brick of computing brick `i` inside the box, with its slot; false otherwise.
+// The brick of computing brick `i` inside a box, that box made the current one, with its
+// slot; false when no box holds it.
 FP_DEV bool boxBrick(const SimParams& P, const FpRender& R, SlotCache& c, uint32_t i, int& bx, int& by, int& bz,
                      int& slot) {
   uint32_t id = P.active[i];
@@ -336,7 +359,13 @@ FP_DEV bool boxBrick(const SimParams& P, const FpRender& R, SlotCache& c, uint32
   bx = t.x * 4 + (l & 3);
   by = t.y * 4 + ((l >> 2) & 3);
   bz = t.z * 4 + (l >> 4);
-  if (!inBox(R, bx, by, bz)) return false;
+  int k = 0;
+  for (; k < R.boxCount; k++) {
+    const int* b = R.boxes + 6 * k;
+    if (bx >= b[0] && bx <= b[3] && by >= b[1] && by <= b[4] && bz >= b[2] && bz <= b[5]) break;
+  }
+  if (k == R.boxCount) return false;
+  useBox(R, c, k);
   slot = slotAt(P, R, c, bx, by, bz);
   return slot >= 0;
 }
@@ -348,7 +377,7 @@ __global__ void __launch_bounds__(RTHREADS) k_render_field(const SimParams* __re
   uint32_t total = P.counters->active;
   const bool half = P.scalarHalf != 0;
   for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
-    SlotCache c{1 << 30, 0, 0, -1};
+    SlotCache c = noBox();
     int bx, by, bz, slot;
     if (!boxBrick(P, R, c, i, bx, by, bz, slot)) continue;
     for (int k = threadIdx.x; k < P.N; k += blockDim.x) {
@@ -380,7 +409,7 @@ __global__ void __launch_bounds__(RTHREADS) k_render_light(const SimParams* __re
   const float texel = P.h * (float)(P.B >> R.lightShift);
   const int per = P.B / 8, blocks = per * per * per;
   for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
-    SlotCache c{1 << 30, 0, 0, -1};
+    SlotCache c = noBox();
     int bx, by, bz, slot;
     if (!boxBrick(P, R, c, i, bx, by, bz, slot)) continue;  // the same for the whole CTA
     // Each 8-cell block with a halo of two cells, in units of 2x2x2 cells: a unit in a
@@ -412,8 +441,8 @@ __global__ void __launch_bounds__(RTHREADS) k_render_light(const SimParams* __re
           lo[a] = (int)floorf((float)o[a] / ratio - .5f);
           hi[a] = (int)floorf((float)(o[a] + 12) / ratio - .5f) + 1;
           size[a] = hi[a] - lo[a] + 1;
-          boxLo[a] = R.boxLo[a] * S;
-          boxHi[a] = (R.boxHi[a] + 1) * S - 1;
+          boxLo[a] = c.lo[a] * S;
+          boxHi[a] = (c.hi[a] + 1) * S - 1;
         }
         for (int q = threadIdx.x; q < size[0] * size[1] * size[2]; q += blockDim.x) {
           int cq[3] = {lo[0] + q % size[0], lo[1] + (q / size[0]) % size[1], lo[2] + q / (size[0] * size[1])};
@@ -456,9 +485,9 @@ __global__ void __launch_bounds__(RTHREADS) k_render_light(const SimParams* __re
 FP_DEV float4 lightSample(const SimParams& P, const FpRender& R, SlotCache& c, float qx, float qy, float qz) {
   const int L = 1 << R.lightShift, L3 = L * L * L;
   const float texel = P.h * (float)(P.B >> R.lightShift);
-  qx = fminf(fmaxf(qx, (float)R.boxLo[0] * L + .5f), (float)(R.boxHi[0] + 1) * L - .5f);
-  qy = fminf(fmaxf(qy, (float)R.boxLo[1] * L + .5f), (float)(R.boxHi[1] + 1) * L - .5f);
-  qz = fminf(fmaxf(qz, (float)R.boxLo[2] * L + .5f), (float)(R.boxHi[2] + 1) * L - .5f);
+  qx = fminf(fmaxf(qx, (float)c.lo[0] * L + .5f), (float)(c.hi[0] + 1) * L - .5f);
+  qy = fminf(fmaxf(qy, (float)c.lo[1] * L + .5f), (float)(c.hi[1] + 1) * L - .5f);
+  qz = fminf(fmaxf(qz, (float)c.lo[2] * L + .5f), (float)(c.hi[2] + 1) * L - .5f);
   float gx = qx - .5f, gy = qy - .5f, gz = qz - .5f;
   int x0 = (int)floorf(gx), y0 = (int)floorf(gy), z0 = (int)floorf(gz);
   if (slotAt(P, R, c, x0 >> R.lightShift, y0 >> R.lightShift, z0 >> R.lightShift) < 0)
@@ -498,13 +527,26 @@ FP_DEV float jitterOf(uint32_t px, uint32_t py, float time) {
 }
 
 // A pixel's march (fireProSceneVolume with fireProMarch), a thread a pixel.
-// A camera ray through the box (fireProRay, fireProSpan) and what its march keeps fixed.
+// A camera ray through the boxes (fireProRay, fireProSpan) and what its march keeps fixed.
 struct Ray {
   float ro[3], rd[3], safe[3], exitSide[3];
-  float lo, hi;  // box entry and exit distances
+  float lo, hi;  // the first box entry and the last exit
   float stepSize, jitter, direct[3];
 };
-// The ray of viewport point (ux, uy) in [0,1]^2; false when it misses the box.
+// fireProHit: where the ray enters and leaves box k (entry after exit when it misses).
+FP_DEV float2 boxHit(const FpRender& R, const Ray& r, int k, float brickSize) {
+  const int* b = R.boxes + 6 * k;
+  float lo = 0.f, hi = 1e30f;
+  for (int a = 0; a < 3; a++) {
+    float ta = ((float)b[a] * brickSize - r.ro[a]) / r.safe[a];
+    float tb = ((float)(b[3 + a] + 1) * brickSize - r.ro[a]) / r.safe[a];
+    lo = fmaxf(lo, fminf(ta, tb));
+    hi = fminf(hi, fmaxf(ta, tb));
+  }
+  return make_float2(lo, hi);
+}
+// The ray of viewport point (ux, uy) in [0,1]^2, its span through the boxes and step; false
+// when it misses them all.
 FP_DEV bool rayOf(const SimParams& P, const FpRender& R, float ux, float uy, Ray& r) {
   float cx = ux * 2.f - 1.f, cy = 1.f - uy * 2.f;
   const float* M = R.ivp;
@@ -520,18 +562,24 @@ FP_DEV bool rayOf(const SimParams& P, const FpRender& R, float ux, float uy, Ray
   float rl = sqrtf(r.rd[0] * r.rd[0] + r.rd[1] * r.rd[1] + r.rd[2] * r.rd[2]);
   for (int a = 0; a < 3; a++) r.rd[a] /= rl;
   const float brickSize = P.h * (float)P.B;
-  r.lo = 0.f;
-  r.hi = 1e30f;
   for (int a = 0; a < 3; a++) {
     r.safe[a] = fabsf(r.rd[a]) > 1e-6f ? r.rd[a] : 1e-6f;
     r.exitSide[a] = r.rd[a] > 0.f ? 1.f : 0.f;
-    float ta = ((float)R.boxLo[a] * brickSize - r.ro[a]) / r.safe[a];
-    float tb = ((float)(R.boxHi[a] + 1) * brickSize - r.ro[a]) / r.safe[a];
-    r.lo = fmaxf(r.lo, fminf(ta, tb));
-    r.hi = fminf(r.hi, fmaxf(ta, tb));
+  }
+  // fireProSpan: the first entry, the last exit and the length inside every box.
+  r.lo = 1e30f;
+  r.hi = 0.f;
+  float length = 0.f;
+  for (int k = 0; k < R.boxCount; k++) {
+    float2 hit = boxHit(R, r, k, brickSize);
+    if (hit.y > hit.x) {
+      r.lo = fminf(r.lo, hit.x);
+      r.hi = fmaxf(r.hi, hit.y);
+      length += hit.y - hit.x;
+    }
   }
   if (!(r.hi > r.lo)) return false;
-  r.stepSize = fmaxf(P.h * .5f, (r.hi - r.lo) / (float)R.raySteps);
+  r.stepSize = fmaxf(P.h * .5f, length / (float)R.raySteps);
   // fireProDirect
   float ln = sqrtf(R.light[0] * R.light[0] + R.light[1] * R.light[1] + R.light[2] * R.light[2]);
   float g = R.optical[3];
@@ -542,10 +590,33 @@ FP_DEV bool rayOf(const SimParams& P, const FpRender& R, float ux, float uy, Ray
   return true;
 }
 
-// One step of fireProMarch (volume-march.wgsl:178-268) at t, ds long: past an empty block a
-// skip of whole steps up to the exit, else the shaded sample. Returns the next t.
-FP_DEV float marchStep(const SimParams& P, const FpRender& R, SlotCache& c, const Ray& r, float t, float ds, float& trans,
-                       float* rad) {
+// fireProEnter (fireProNext): the box the ray is in at t, or the next one it enters, becomes the
+// current one with its exit, and t moves to its entry; false past the last box. Boxes never
+// overlap, so of the boxes the ray has not left, the one it enters first is the one.
+FP_DEV bool enterBox(const SimParams& P, const FpRender& R, const Ray& r, float& t, float& exit, SlotCache& c) {
+  const float brickSize = P.h * (float)P.B;
+  float entry = 1e30f, out = 0.f;
+  int best = -1;
+  for (int k = 0; k < R.boxCount; k++) {
+    float2 hit = boxHit(R, r, k, brickSize);
+    if (hit.y > hit.x && hit.y > t && hit.x < entry) {
+      entry = hit.x;
+      out = hit.y;
+      best = k;
+    }
+  }
+  if (best < 0) return false;
+  useBox(R, c, best);
+  exit = out;
+  t = fmaxf(t, entry);
+  return true;
+}
+
+// One step of fireProMarch (volume-march.wgsl:178-268) at t, ds long, in the current box (which
+// the ray leaves at `exit`): past an empty block a skip of whole steps up to the exit, else the
+// shaded sample. Returns the next t.
+FP_DEV float marchStep(const SimParams& P, const FpRender& R, SlotCache& c, const Ray& r, float t, float ds, float exit,
+                       float& trans, float* rad) {
   const float brickSize = P.h * (float)P.B, lightRatio = (float)(P.B >> R.lightShift);
   float tt = t + r.jitter * ds;
   float p[3] = {r.ro[0] + r.rd[0] * tt, r.ro[1] + r.rd[1] * tt, r.ro[2] + r.rd[2] * tt};
@@ -564,7 +635,7 @@ FP_DEV float marchStep(const SimParams& P, const FpRender& R, SlotCache& c, cons
     // Skip whole steps past the empty block, keeping the lattice.
     float dist = 1e30f;
     for (int a = 0; a < 3; a++) dist = fminf(dist, ((floorf(p[a] / size) + r.exitSide[a]) * size - p[a]) / r.safe[a]);
-    return fminf(t + fmaxf(1.f, floorf(dist / r.stepSize) + 1.f) * r.stepSize, r.hi);
+    return fminf(t + fmaxf(1.f, floorf(dist / r.stepSize) + 1.f) * r.stepSize, exit);
   }
   float4 f = reconstruct(P, R, c, cell[0], cell[1], cell[2], (flags & 1) ? R.filter : 0);
   if (P.smokeDiv > 1) {  // fireProRenderField: the smoothed coarse density, trilinear
@@ -594,9 +665,10 @@ FP_DEV float marchStep(const SimParams& P, const FpRender& R, SlotCache& c, cons
   return t + ds;
 }
 
-// buildSlices (volume-slices.wgsl:28-122): a ray per half-resolution pixel marches the whole
-// span, recording radiance and opacity at FP_SLICES evenly spaced depths; depths passed by a
-// skip keep the values of the moment, those past the exit or an opaque ray the final ones.
+// buildSlices (volume-slices.wgsl:28-122): a ray per half-resolution pixel marches from the
+// first box entry to the last exit, box by box, recording radiance and opacity at FP_SLICES
+// evenly spaced depths; depths passed by a skip or a jump between boxes keep the values of the
+// moment, those past the exit or an opaque ray the final ones.
 __global__ void __launch_bounds__(RTHREADS) k_slices(const SimParams* __restrict__ Pp, FpRender R) {
   const SimParams& P = *Pp;
   int pix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -606,14 +678,18 @@ __global__ void __launch_bounds__(RTHREADS) k_slices(const SimParams* __restrict
   float trans = 1.f, rad[3] = {0.f, 0.f, 0.f};
   int recorded = 0;
   Ray r;
-  if (R.hasBox && rayOf(P, R, ((float)px + .5f) / (float)R.sliceW, ((float)py + .5f) / (float)R.sliceH, r)) {
+  if (R.boxCount > 0 && rayOf(P, R, ((float)px + .5f) / (float)R.sliceW, ((float)py + .5f) / (float)R.sliceH, r)) {
     r.jitter = jitterOf((uint32_t)px, (uint32_t)py, R.time);
     const float spacing = fmaxf(r.hi - r.lo, 0.f) / (float)FP_SLICES;
-    SlotCache c{1 << 30, 0, 0, -1};
-    float t = r.lo, depth = r.lo + spacing;
+    SlotCache c = noBox();
+    float t = r.lo, depth = r.lo + spacing, exit = t;
     while (recorded < FP_SLICES && t < r.hi && trans >= .008f) {
-      float ds = fminf(r.stepSize, fminf(depth, r.hi) - t);
-      t = marchStep(P, R, c, r, t, ds, trans, rad);
+      if (t >= exit) {
+        if (!enterBox(P, R, r, t, exit, c)) break;
+      } else {
+        float ds = fminf(r.stepSize, fminf(depth, exit) - t);
+        t = marchStep(P, R, c, r, t, ds, exit, trans, rad);
+      }
       while (recorded < FP_SLICES && t >= depth) {
         out[recorded] = make_float4(rad[0], rad[1], rad[2], 1.f - trans);
         recorded++;
@@ -625,7 +701,8 @@ __global__ void __launch_bounds__(RTHREADS) k_slices(const SimParams* __restrict
 }
 
 // fireProSceneVolume (scene-volume.wgsl:39-44, 146-167): the march of each pixel's ray up to
-// the scene's depth, from the last half-resolution slice in front of it when slices exist.
+// the scene's depth through the boxes, from the last half-resolution slice in front of it when
+// slices exist.
 __global__ void __launch_bounds__(RTHREADS) k_march(const SimParams* __restrict__ Pp, FpRender R) {
   const SimParams& P = *Pp;
   int pix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -633,7 +710,7 @@ __global__ void __launch_bounds__(RTHREADS) k_march(const SimParams* __restrict_
   int px = pix % R.width, py = pix / R.width;
   float4* out = reinterpret_cast<float4*>(R.image) + pix;
   *out = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (!R.hasBox) return;
+  if (R.boxCount == 0) return;
   const float ux = ((float)px + .5f) / (float)R.width, uy = ((float)py + .5f) / (float)R.height;
   Ray r;
   if (!rayOf(P, R, ux, uy, r)) return;
@@ -681,11 +758,16 @@ __global__ void __launch_bounds__(RTHREADS) k_march(const SimParams* __restrict_
       rad[2] = v.z;
     }
   }
-  SlotCache c{1 << 30, 0, 0, -1};
+  // fireProMarch: the cursor starts exited, so the first pass enters the box at t.
+  SlotCache c = noBox();
+  float exit = t;
   while (t < end && trans >= .008f) {
-    if (t >= r.hi) break;
-    float ds = fminf(r.stepSize, fminf(end, r.hi) - t);
-    t = marchStep(P, R, c, r, t, ds, trans, rad);
+    if (t >= exit) {
+      if (!enterBox(P, R, r, t, exit, c)) break;
+      continue;
+    }
+    float ds = fminf(r.stepSize, fminf(end, exit) - t);
+    t = marchStep(P, R, c, r, t, ds, exit, trans, rad);
   }
   *out = make_float4(rad[0], rad[1], rad[2], 1.f - trans);
 }

@@ -21,8 +21,9 @@ struct FpRender {
   float flameOpacity;
   int shadowSamples, raySteps, filter;
   int lightShift;       // lighting texels per brick side = 1 << lightShift
-  int boxLo[3], boxHi[3];  // the render box in bricks, inclusive
-  int hasBox;
+  const int* boxes;     // the render boxes: lo xyz, hi xyz in bricks (inclusive), six ints each;
+                        // boxes never overlap, each lies in one cluster of tiles
+  int boxCount;
   float* renderField;   // [slot][4][cells]: smoothed smoke, heat, lifetime, fuel (coarse smoke:
                         // the simulation's fields as they are)
   float* renderSmoke;   // coarse smoke (smokeDiv > 1): [slot][smoke cells], the smoothed density

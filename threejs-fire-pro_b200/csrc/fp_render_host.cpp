@@ -1,6 +1,8 @@
 // Host side of the volume render (fp_render.cu): the blackbody table, the render box and
 // Engine::render.
 #include <algorithm>
+#include <array>
+#include <map>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -61,24 +63,105 @@ void fp_blackbody_table(float* out4) {
 
 namespace fp {
 
-// updateBoxes (FluidSimulation.ts:916-957) for a scene of one cluster: the bricks with content
-// at the latest measurement and the sources' bricks, whose centre lies in a tile, grown by two
-// bricks and kept within the tiles.
+// TileDirectory.clusters (TileDirectory.ts:189-237): the tiles grouped by touch (faces, edges or
+// corners), in creation order, each group boxed; boxes that overlap merge until none do, and
+// the surviving boxes are numbered in the order of their first group.
+void Engine::buildClusters() {
+  const auto& slots = dir_.slots();
+  std::vector<int> order;
+  for (size_t s = 0; s < slots.size(); s++)
+    if (slots[s].alive) order.push_back((int)s);
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return slots[a].seq < slots[b].seq; });
+  std::vector<int> group(slots.size(), -1);
+  std::vector<std::array<int, 6>> boxes;
+  std::vector<int> stack;
+  for (int first : order) {
+    if (group[first] >= 0) continue;
+    const int index = (int)boxes.size();
+    const TileDirectory::Tile& f = slots[first];
+    std::array<int, 6> box = {f.x, f.y, f.z, f.x, f.y, f.z};
+    group[first] = index;
+    stack.assign(1, first);
+    while (!stack.empty()) {
+      const TileDirectory::Tile& t = slots[stack.back()];
+      stack.pop_back();
+      const int c[3] = {t.x, t.y, t.z};
+      for (int a = 0; a < 3; a++) {
+        box[a] = std::min(box[a], c[a]);
+        box[3 + a] = std::max(box[3 + a], c[a]);
+      }
+      for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+          for (int dx = -1; dx <= 1; dx++) {
+            int n = dir_.slotAt(t.x + dx, t.y + dy, t.z + dz);
+            if (n >= 0 && group[n] < 0) {
+              group[n] = index;
+              stack.push_back(n);
+            }
+          }
+    }
+    boxes.push_back(box);
+  }
+  std::vector<int> into(boxes.size());
+  for (size_t i = 0; i < into.size(); i++) into[i] = (int)i;
+  auto root = [&](int i) {
+    while (into[i] != i) i = into[i] = into[into[i]];
+    return i;
+  };
+  auto overlaps = [](const std::array<int, 6>& a, const std::array<int, 6>& b) {
+    for (int k = 0; k < 3; k++)
+      if (!(a[k] <= b[3 + k] && b[k] <= a[3 + k])) return false;
+    return true;
+  };
+  for (bool merged = true; merged;) {
+    merged = false;
+    for (size_t i = 0; i < boxes.size(); i++)
+      for (size_t j = i + 1; j < boxes.size(); j++) {
+        int a = root((int)i), b = root((int)j);
+        if (a == b || !overlaps(boxes[a], boxes[b])) continue;
+        for (int k = 0; k < 3; k++) {
+          boxes[a][k] = std::min(boxes[a][k], boxes[b][k]);
+          boxes[a][3 + k] = std::max(boxes[a][3 + k], boxes[b][3 + k]);
+        }
+        into[b] = a;
+        merged = true;
+      }
+  }
+  std::vector<int> renumbered(boxes.size(), -1);
+  clusterBoxes_.clear();
+  for (size_t i = 0; i < boxes.size(); i++)
+    if (root((int)i) == (int)i) {
+      renumbered[i] = (int)(clusterBoxes_.size() / 6);
+      clusterBoxes_.insert(clusterBoxes_.end(), boxes[i].begin(), boxes[i].end());
+    }
+  clusterOf_.assign(slots.size(), -1);
+  for (size_t s = 0; s < slots.size(); s++)
+    if (group[s] >= 0) clusterOf_[s] = renumbered[root(group[s])];
+}
+
+// updateBoxes (FluidSimulation.ts:916-957): what the render draws in each cluster of tiles, the
+// bricks with content at the latest measurement and the sources' bricks (each in the cluster of
+// its centre's tile), grown by two bricks and kept within the cluster's tiles; clusters with none
+// of these get no box. Boxes in cluster order.
 void Engine::updateRenderBox() {
   const int TB = 4, MARGIN = 2;
-  int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-  bool any = false;
+  std::map<int, std::array<int, 6>> found;
   auto include = [&](const int* l, const int* u) {
     int c[3];
     for (int a = 0; a < 3; a++) c[a] = (int)std::floor(((double)l[a] + (double)u[a]) / 2.0);
     if (ground_) c[1] = std::max(0, c[1]);
     auto div = [](int n) { return (int)std::floor((double)n / 4.0); };
-    if (dir_.slotAt(div(c[0]), div(c[1]), div(c[2])) < 0) return;
-    for (int a = 0; a < 3; a++) {
-      lo[a] = any ? std::min(lo[a], l[a]) : l[a];
-      hi[a] = any ? std::max(hi[a], u[a]) : u[a];
+    int slot = dir_.slotAt(div(c[0]), div(c[1]), div(c[2]));
+    if (slot < 0 || slot >= (int)clusterOf_.size() || clusterOf_[slot] < 0) return;
+    auto it = found.find(clusterOf_[slot]);
+    if (it == found.end()) {
+      found[clusterOf_[slot]] = {l[0], l[1], l[2], u[0], u[1], u[2]};
+      return;
     }
-    any = true;
+    for (int a = 0; a < 3; a++) {
+      it->second[a] = std::min(it->second[a], l[a]);
+      it->second[3 + a] = std::max(it->second[3 + a], u[a]);
+    }
   };
   for (auto& ct : contentTiles_) {
     int t[3] = {ct.first.x, ct.first.y, ct.first.z}, l[3], u[3];
@@ -93,23 +176,11 @@ void Engine::updateRenderBox() {
     if (ok) include(l, u);
   }
   for (size_t s = 0; s + 6 <= sourceBoxes_.size(); s += 6) include(&sourceBoxes_[s], &sourceBoxes_[s + 3]);
-  renderBox_ = any;
-  if (!any) return;
-  // The tiles' extent in bricks.
-  int tlo[3] = {0, 0, 0}, thi[3] = {0, 0, 0};
-  bool first = true;
-  for (const auto& t : dir_.slots()) {
-    if (!t.alive) continue;
-    int v[3] = {t.x, t.y, t.z};
-    for (int a = 0; a < 3; a++) {
-      tlo[a] = first ? v[a] : std::min(tlo[a], v[a]);
-      thi[a] = first ? v[a] : std::max(thi[a], v[a]);
-    }
-    first = false;
-  }
-  for (int a = 0; a < 3; a++) {
-    renderLo_[a] = std::max(lo[a] - MARGIN, tlo[a] * TB);
-    renderHi_[a] = std::min(hi[a] + MARGIN, (thi[a] + 1) * TB - 1);
+  renderBoxes_.clear();
+  for (auto& kv : found) {
+    const int* tiles = &clusterBoxes_[(size_t)kv.first * 6];
+    for (int a = 0; a < 3; a++) renderBoxes_.push_back(std::max(kv.second[a] - MARGIN, tiles[a] * TB));
+    for (int a = 0; a < 3; a++) renderBoxes_.push_back(std::min(kv.second[3 + a] + MARGIN, (tiles[3 + a] + 1) * TB - 1));
   }
 }
 
@@ -223,11 +294,16 @@ int Engine::render(const fp_camera& cam, const fp_render_settings& rs, float* im
   R.raySteps = (int)rs.ray_steps;
   R.filter = rs.filter;
   R.lightShift = lightShift;
-  for (int a = 0; a < 3; a++) {
-    R.boxLo[a] = renderLo_[a];
-    R.boxHi[a] = renderHi_[a];
+  // The boxes of the latest step (none before the first).
+  R.boxCount = steps_ > 0 ? (int)(renderBoxes_.size() / 6) : 0;
+  if (R.boxCount > 0) {
+    const size_t bytes = renderBoxes_.size() * 4;
+    if (renderBoxesD_.bytes < bytes && !alloc(renderBoxesD_, std::max<size_t>(bytes, 64 * 24), false)) return FP_ENOMEM;
+    if ((rc = check(cudaMemcpyAsync(renderBoxesD_.ptr, renderBoxes_.data(), bytes, cudaMemcpyHostToDevice, stream()),
+                    "render")))
+      return rc;
   }
-  R.hasBox = renderBox_ && steps_ > 0 ? 1 : 0;
+  R.boxes = (const int*)renderBoxesD_.ptr;
   R.depth = depth;
   R.slices = cam.half_resolution ? (float*)slices_.ptr : nullptr;
   R.sliceW = sliceW;

@@ -19,7 +19,7 @@ namespace fp {
 namespace {
 
 constexpr uint32_t MAGIC = 0x4e535046u;  // "FPSN"
-constexpr uint32_t VERSION = 3;
+constexpr uint32_t VERSION = 4;
 
 struct Writer {
   std::vector<uint8_t>& out;
@@ -144,9 +144,10 @@ int Engine::snapshot(std::vector<uint8_t>& out) {
   w.pod(coverageVersion_);
   w.vec(liveTiles_);
   w.vec(tileIndex_);
-  w.raw(renderLo_, sizeof(renderLo_));
-  w.raw(renderHi_, sizeof(renderHi_));
-  w.pod(renderBox_);
+  w.vec(renderBoxes_);
+  w.vec(clusterOf_);
+  w.vec(clusterBoxes_);
+  w.pod(dir_.nextSeq_);
   w.vec(sourceBoxes_);
   // device buffers: size, then contents
   std::vector<uint8_t> host;
@@ -224,12 +225,12 @@ int Engine::restore(const uint8_t* data, size_t bytes) {
   r.vec(contentTiles);
   uint32_t activeBricks, usedSlots, lastFailures, slots;
   uint64_t bricksStepped, tileVersion, meshVersion, coverageVersion;
-  bool poolLimited, measure, coverageOn, renderBox;
+  bool poolLimited, measure, coverageOn;
   int latest, vcycles, meshCount;
   float tolerance;
   fp_solver_schedule schedule;
   FpSolver lastSolver;
-  int velIdx[4], fldIdx[3], smokeIdx[3], renderLo[3], renderHi[3];
+  int velIdx[4], fldIdx[3], smokeIdx[3];
   std::vector<FpMeshSource> meshRecords;
   std::vector<int> meshTables, liveTiles, tileIndex, sourceBoxes;
   std::vector<uint32_t> coverage;
@@ -260,9 +261,12 @@ int Engine::restore(const uint8_t* data, size_t bytes) {
   r.pod(coverageVersion);
   r.vec(liveTiles);
   r.vec(tileIndex);
-  r.raw(renderLo, sizeof(renderLo));
-  r.raw(renderHi, sizeof(renderHi));
-  r.pod(renderBox);
+  std::vector<int> renderBoxes, clusterOf, clusterBoxes;
+  uint64_t nextSeq = 0;
+  r.vec(renderBoxes);
+  r.vec(clusterOf);
+  r.vec(clusterBoxes);
+  r.pod(nextSeq);
   r.vec(sourceBoxes);
   if (!r.ok) return fail(FP_EINVAL, "the snapshot is truncated");
   // Device buffers: each resized to its saved size and filled. First every size is read and
@@ -356,9 +360,10 @@ int Engine::restore(const uint8_t* data, size_t bytes) {
   coverageVersion_ = coverageVersion;
   liveTiles_ = liveTiles;
   tileIndex_ = tileIndex;
-  std::memcpy(renderLo_, renderLo, sizeof(renderLo));
-  std::memcpy(renderHi_, renderHi, sizeof(renderHi));
-  renderBox_ = renderBox;
+  renderBoxes_ = renderBoxes;
+  clusterOf_ = clusterOf;
+  clusterBoxes_ = clusterBoxes;
+  dir_.nextSeq_ = nextSeq;
   sourceBoxes_ = sourceBoxes;
   return FP_OK;
 }
