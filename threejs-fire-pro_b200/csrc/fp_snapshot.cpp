@@ -89,6 +89,16 @@ int Engine::snapshot(std::vector<uint8_t>& out) {
   if (rc) return rc;
   if ((rc = check(cudaStreamSynchronize(stream()), "snapshot"))) return rc;
   out.clear();
+  {
+    // Room for every buffer at once: the pools of a large budget take gigabytes.
+    size_t bytes = 1 << 20;
+#define FP_SIZE(b) bytes += (b.ptr ? b.bytes : 0) + 8;
+    FP_SNAPSHOT_BUFFERS(FP_SIZE)
+#undef FP_SIZE
+    bytes += (tileRec_.size() + hash_.size()) * sizeof(int4) + tileNbr_.size() * 4 + coverage_.size() * 4 +
+             meshTables_.size() * 4 + meshRecords_.size() * sizeof(FpMeshSource);
+    out.reserve(bytes);
+  }
   Writer w{out};
   w.pod(MAGIC);
   w.pod(VERSION);

@@ -27,9 +27,14 @@ constexpr int STAGE_SIDE = 8 + 2 * HALO;  // the staged kernels run for 8^3 bric
 #endif
 
 // Where the staged copy sits: its first cell and its side.
+// SS, the box's side, is a compile-time constant, so staged addresses fold into immediate
+// offsets of the shared-memory loads.
+template <int SS>
 struct Stage {
-  int ox, oy, oz, S, S3;
+  int ox, oy, oz;
+  static constexpr int S = SS, S3 = SS * SS * SS;
 };
+using TransportStage = Stage<8 + 2 * HALO>;
 
 // A field a kernel reads: the pool and, when staged, its shared copy.
 struct Field {
@@ -40,17 +45,20 @@ struct Field {
 };
 
 // The staged offset of cell (x,y,z), which the caller knows lies inside the staged box.
-FP_DEV int stagedAt(const Stage& G, int x, int y, int z) { return ((z - G.oz) * G.S + (y - G.oy)) * G.S + (x - G.ox); }
+template <int SS>
+FP_DEV int stagedAt(const Stage<SS>& G, int x, int y, int z) { return ((z - G.oz) * G.S + (y - G.oy)) * G.S + (x - G.ox); }
 
 // A cell within HALO cells of the home brick: the staged box always holds it, so no check.
-FP_DEV float nearCell(const SimParams& P, const Home& H, const Stage& G, const Field& f, int c, int x, int y, int z) {
+template <int SS>
+FP_DEV float nearCell(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& f, int c, int x, int y, int z) {
   if (f.sm) return f.sm[c * G.S3 + stagedAt(G, x, y, z)];
   return cellAt(P, H, f.pool, f.ch, c, x, y, z, f.half);
 }
 
 // The 2x2x2 block from corner (x0,y0,z0) of channel c into t (x fastest): from shared memory
 // when `b` (the corner's staged address, channel 0) is set, else through the directory.
-FP_DEV void blockCells(const SimParams& P, const Home& H, const Stage& G, const Field& f, int c, const float* b, int x0,
+template <int SS>
+FP_DEV void blockCells(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& f, int c, const float* b, int x0,
                        int y0, int z0, float* t) {
   if (b) {
     const float* q = b + c * G.S3;
@@ -63,7 +71,8 @@ FP_DEV void blockCells(const SimParams& P, const Home& H, const Stage& G, const 
   for (int j = 0; j < 8; j++) t[j] = cellAt(P, H, f.pool, f.ch, c, x0 + (j & 1), y0 + ((j >> 1) & 1), z0 + (j >> 2), f.half);
 }
 // The staged address of the block from corner (x0,y0,z0) when the whole block is staged.
-FP_DEV const float* stagedBlock(const Stage& G, const Field& f, int x0, int y0, int z0) {
+template <int SS>
+FP_DEV const float* stagedBlock(const Stage<SS>& G, const Field& f, int x0, int y0, int z0) {
   if (!f.sm) return nullptr;
   unsigned lx = (unsigned)(x0 - G.ox), ly = (unsigned)(y0 - G.oy), lz = (unsigned)(z0 - G.oz);
   unsigned lim = (unsigned)(G.S - 1);
@@ -72,7 +81,8 @@ FP_DEV const float* stagedBlock(const Stage& G, const Field& f, int x0, int y0, 
 }
 
 // Trilinear sample at `pos` in cell units (fluid-sampling.wgsl:85-114).
-FP_DEV float fieldSample(const SimParams& P, const Home& H, const Stage& G, const Field& f, int c, float px, float py,
+template <int SS>
+FP_DEV float fieldSample(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& f, int c, float px, float py,
                          float pz) {
   if (f.sm) {
     float qx = px - 0.5f, qy = py - 0.5f, qz = pz - 0.5f;
@@ -91,11 +101,11 @@ FP_DEV float fieldSample(const SimParams& P, const Home& H, const Stage& G, cons
 // zero where no slot, with asynchronous 4-byte copies (cp.async): every thread keeps all its
 // copies in flight and the caller waits once. A brick without a slot reads nothing (source
 // size 0 zero-fills). A half pool is widened to FP32 on the way (plain loads: cp.async moves
-// at least 4 bytes). SIDE, when not 0, is the box's side G.S known at compile time.
-template <int SIDE = 0>
-FP_DEV void stageField(const SimParams& P, const Home& H, const Stage& G, float* sm, const float* pool, int ch,
+// at least 4 bytes).
+template <int SS>
+FP_DEV void stageField(const SimParams& P, const Home& H, const Stage<SS>& G, float* sm, const float* pool, int ch,
                        bool half = false, int nch = 0) {
-  const int S = SIDE ? SIDE : G.S, S3 = S * S * S;
+  constexpr int S = SS, S3 = S * S * S;
   if (nch <= 0) nch = ch;
   for (int i = threadIdx.x; i < S3; i += blockDim.x) {
     int lx = i % S, ly = (i / S) % S, lz = i / (S * S);
@@ -121,10 +131,8 @@ FP_DEV void stageWait() {
   __syncthreads();
 }
 
-FP_DEV Stage stageOf(const SimParams& P, const Home& H, bool staged) {
-  Stage G;
-  G.S = staged ? P.B + 2 * HALO : 0;
-  G.S3 = G.S * G.S * G.S;
+FP_DEV TransportStage stageOf(const SimParams& P, const Home& H) {
+  TransportStage G;
   G.ox = H.bx * P.B - HALO;
   G.oy = H.by * P.B - HALO;
   G.oz = H.bz * P.B - HALO;
@@ -132,7 +140,8 @@ FP_DEV Stage stageOf(const SimParams& P, const Home& H, bool staged) {
 }
 
 // Component c of the staggered velocity at world position p: stored half a cell back along c.
-FP_DEV float velComp(const SimParams& P, const Home& H, const Stage& G, const Field& v, float px, float py, float pz,
+template <int SS>
+FP_DEV float velComp(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& v, float px, float py, float pz,
                      int c) {
   float qx = px * P.invH, qy = py * P.invH, qz = pz * P.invH;
   return fieldSample(P, H, G, v, c, c == 0 ? qx - 0.5f : qx, c == 1 ? qy - 0.5f : qy, c == 2 ? qz - 0.5f : qz);
@@ -140,7 +149,8 @@ FP_DEV float velComp(const SimParams& P, const Home& H, const Stage& G, const Fi
 // velocityAt (fluid-advection.wgsl:17-21): the three staggered samples share their floors
 // (per axis: unshifted, and shifted half a cell for the component stored along it) and one
 // check that all three blocks are staged.
-FP_DEV float3 velocityAt(const SimParams& P, const Home& H, const Stage& G, const Field& v, float px, float py,
+template <int SS>
+FP_DEV float3 velocityAt(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& v, float px, float py,
                          float pz) {
   const float q[3] = {px * P.invH, py * P.invH, pz * P.invH};
   if (v.sm) {
@@ -180,7 +190,8 @@ FP_DEV float get(const float3& v, int c) { return c == 0 ? v.x : (c == 1 ? v.y :
 // velocityOnFace (fluid-advection.wgsl:26-44): the face's own component is stored; each other
 // component k is the trilinear sample at the face centre, which falls midway between two
 // cells along c and along k and on the cell plane of the third axis: the mean of four cells.
-FP_DEV float3 velocityOnFace(const SimParams& P, const Home& H, const Stage& G, const Field& v, int x, int y, int z,
+template <int SS>
+FP_DEV float3 velocityOnFace(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& v, int x, int y, int z,
                              int c, float3 orig) {
   float r[3];
 #pragma unroll
@@ -198,7 +209,8 @@ FP_DEV float3 velocityOnFace(const SimParams& P, const Home& H, const Stage& G, 
   return make_float3(r[0], r[1], r[2]);
 }
 // velocityAt at the centre of cell (x,y,z): each component midway between its two faces.
-FP_DEV float3 centreVelocity(const SimParams& P, const Home& H, const Stage& G, const Field& v, int x, int y, int z) {
+template <int SS>
+FP_DEV float3 centreVelocity(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& v, int x, int y, int z) {
   return make_float3(0.5f * (nearCell(P, H, G, v, 0, x - 1, y, z) + nearCell(P, H, G, v, 0, x, y, z)),
                      0.5f * (nearCell(P, H, G, v, 1, x, y - 1, z) + nearCell(P, H, G, v, 1, x, y, z)),
                      0.5f * (nearCell(P, H, G, v, 2, x, y, z - 1) + nearCell(P, H, G, v, 2, x, y, z)));
@@ -224,7 +236,8 @@ FP_DEV void cellOf(const SimParams& P, const Home& H, int c, int& x, int& y, int
 // the scalars at the start of the step.
 // advectVelocityWithBounds (fluid-velocity-transport.wgsl:28-100) at velocity cell (x,y,z),
 // offset c of its brick's slot, on the velocity lattice P.
-FP_DEV void predictVelocity(const SimParams& P, const Home& H, const Stage& G, const Field& V, size_t slot, int c, int x,
+template <int SS>
+FP_DEV void predictVelocity(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& V, size_t slot, int c, int x,
                             int y, int z) {
   const size_t N = P.N;
   // The limiter's bounds (the forward 2x2x2 block of each donor cell) are taken where the
@@ -257,7 +270,8 @@ FP_DEV void predictVelocity(const SimParams& P, const Home& H, const Stage& G, c
 }
 // advectScalars (fluid-scalar-transport.wgsl:38-142) at field cell (x,y,z), offset c of its
 // brick's slot: P the field lattice, VP the velocity lattice the trace samples.
-FP_DEV void predictScalars(const SimParams& P, const SimParams& VP, const Home& H, const Stage& G, const Field& V,
+template <int SS>
+FP_DEV void predictScalars(const SimParams& P, const SimParams& VP, const Home& H, const Stage<SS>& G, const Field& V,
                            const Field& F, size_t slot, int c, int x, int y, int z) {
   const size_t N = P.N;
   // Scalars: a cell-centred RK2 back trace, the predictor and its donors' range.
@@ -314,12 +328,12 @@ FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
   const SimParams& P = *Pp;
   uint32_t id = P.active[i];
   Home H = enterBrick(P, id, nslot);
-  Stage G = stageOf(P, H, STAGED);
+  TransportStage G = stageOf(P, H);
   Field V{P.vel, 3, STAGED ? smem : nullptr};
   Field F{P.fld, 4, STAGED ? smem + 3 * G.S3 : nullptr, P.scalarHalf != 0};
   if (STAGED) {
-    stageField<STAGE_SIDE>(P, H, G, smem, P.vel, 3);
-    stageField<STAGE_SIDE>(P, H, G, smem + 3 * G.S3, P.fld, 4, F.half);
+    stageField(P, H, G, smem, P.vel, 3);
+    stageField(P, H, G, smem + 3 * G.S3, P.fld, 4, F.half);
     stageWait();
   }
   size_t slot = (size_t)nslot[13];
@@ -365,12 +379,12 @@ FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
   const SimParams& P = *Pp;
   uint32_t id = P.active[i];
   Home H = enterBrick(P, id, nslot);
-  Stage G = stageOf(P, H, STAGED);
+  TransportStage G = stageOf(P, H);
   Field V{P.vel, 3, STAGED ? smem : nullptr};
   Field Vp{P.velP, 3, STAGED ? smem + 3 * G.S3 : nullptr};
   if (STAGED) {
-    stageField<STAGE_SIDE>(P, H, G, smem, P.vel, 3);
-    stageField<STAGE_SIDE>(P, H, G, smem + 3 * G.S3, P.velP, 3);
+    stageField(P, H, G, smem, P.vel, 3);
+    stageField(P, H, G, smem + 3 * G.S3, P.velP, 3);
     stageWait();
   }
   size_t slot = (size_t)nslot[13];
@@ -461,14 +475,14 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
     expandsAll = 0;
   }
   Home H = enterBrick(P, id, nslot);
-  Stage G = stageOf(P, H, STAGED);
+  TransportStage G = stageOf(P, H);
   const SimParams& VP = STAGED ? P : *P.vview;  // the velocity lattice the traces sample
   Field V{P.vel, 3, STAGED ? smem : nullptr};
   Field Fp{P.fldP, 4, STAGED ? smem + 3 * G.S3 : nullptr, false};  // the predictor: FP32
   const bool half = P.scalarHalf != 0;                             // the state pools
   if (STAGED) {
-    stageField<STAGE_SIDE>(P, H, G, smem, P.vel, 3);
-    stageField<STAGE_SIDE>(P, H, G, smem + 3 * G.S3, P.fldP, 4);
+    stageField(P, H, G, smem, P.vel, 3);
+    stageField(P, H, G, smem + 3 * G.S3, P.fldP, 4);
     stageWait();
   }
   size_t slot = (size_t)nslot[13];
@@ -659,15 +673,13 @@ FP_DEV void brick_curl(const SimParams* __restrict__ Pp, uint32_t i) {
   const SimParams& P = *Pp;
   if (!P.curlOn) return;  // the same for the whole CTA
   Home H = enterBrick(P, P.active[i], nslot);
-  Stage G;
-  G.S = STAGED ? P.B + 2 : 0;
-  G.S3 = G.S * G.S * G.S;
+  Stage<8 + 2> G;  // staged: 8^3 bricks and a one-cell rim
   G.ox = H.bx * P.B - 1;
   G.oy = H.by * P.B - 1;
   G.oz = H.bz * P.B - 1;
   Field V{P.velC, 3, STAGED ? smem : nullptr};
   if (STAGED) {
-    stageField<8 + 2>(P, H, G, smem, P.velC, 3);
+    stageField(P, H, G, smem, P.velC, 3);
     stageWait();
   }
   size_t slot = (size_t)nslot[13];
@@ -783,8 +795,8 @@ FP_DEV float3 externalForces(const SimParams& P, const Home& H, int tile, int x,
 // cellForce / centerForce (fluid-forces.wgsl:79-118).
 // The curl is read over the force region and a one-cell rim (Gc, Fc), the evolved scalars
 // over the force region (Gs, Fs): staged or through the directory.
-template <bool ONE>
-FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage& Gc, const Field& Fc, const Stage& Gs,
+template <bool ONE, int SC, int SS>
+FP_DEV float3 cellForce(const SimParams& P, const Home& H, const Stage<SC>& Gc, const Field& Fc, const Stage<SS>& Gs,
                         const Field& Fs, int tile, int x, int y, int z) {
   if (brickSlot(P, H, x >> P.shift, y >> P.shift, z >> P.shift) < 0) return make_float3(0.f, 0.f, 0.f);
   float wx = ((float)x + 0.5f) * P.h, wy = ((float)y + 0.5f) * P.h, wz = ((float)z + 0.5f) * P.h;
@@ -883,14 +895,12 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   // brick), each with its centre forces on the cube and one cell beyond its upper faces.
   const int SUB = STAGED ? 8 : min(P.B, FORCE_SUB), E = SUB + 1, E3 = E * E * E, per = STAGED ? 1 : P.B / SUB;
   float* stage = reinterpret_cast<float*>(forceTile + E3);
-  Stage Gc, Gs;
-  Gc.S = STAGED ? E + 2 : 0;
-  Gc.S3 = Gc.S * Gc.S * Gc.S;
+  // Staged (8^3 bricks: E = 9): the curl over E + 2 cells a side, two scalars over E.
+  Stage<11> Gc;
+  Stage<9> Gs;
   Gc.ox = H.bx * P.B - 1;
   Gc.oy = H.by * P.B - 1;
   Gc.oz = H.bz * P.B - 1;
-  Gs.S = STAGED ? E : 0;
-  Gs.S3 = Gs.S * Gs.S * Gs.S;
   Gs.ox = H.bx * P.B;
   Gs.oy = H.by * P.B;
   Gs.oz = H.bz * P.B;
@@ -898,8 +908,8 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   Field Fc{P.curl, 4, STAGED ? stage : nullptr};
   Field Fs{P.fldN, 4, STAGED ? stage + 4 * Gc.S3 : nullptr, half};
   if (STAGED) {
-    if (P.vorticity != 0.f) stageField<11>(P, H, Gc, stage, P.curl, 4);
-    stageField<9>(P, H, Gs, stage + 4 * Gc.S3, P.fldN, 4, half, 2);  // smoke, heat
+    if (P.vorticity != 0.f) stageField(P, H, Gc, stage, P.curl, 4);
+    stageField(P, H, Gs, stage + 4 * Gc.S3, P.fldN, 4, half, 2);  // smoke, heat
     stageWait();
   }
   const float decay = expf(-P.damping * P.dt);
@@ -1173,7 +1183,7 @@ FP_DEV SmokeCell smokeCellOf(const SimParams& P, const Home& H, int c) {
 }
 // traceBack / traceForward (fluid-advection.wgsl:67-75) from `p` with centre velocity `cv`.
 FP_DEV float3 smokeTrace(const SimParams& P, const Home& H, const float* p, float3 cv, float sign) {
-  Stage G{};
+  TransportStage G{};
   Field V{P.vel, 3, nullptr};
   float3 vm = velocityAt(*P.vview, H, G, V, p[0] + sign * 0.5f * P.dt * cv.x, p[1] + sign * 0.5f * P.dt * cv.y,
                          p[2] + sign * 0.5f * P.dt * cv.z);
@@ -1193,7 +1203,7 @@ __global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_advect(FpBatch bt) {
     const size_t slot = (size_t)nslot[13], SN = (size_t)P.smokeCells;
     const float sp = P.h * (float)P.smokeDiv, invSp = 1.f / sp;
     const bool half = P.scalarHalf != 0;
-    Stage G{};
+    TransportStage G{};
     Field V{P.vel, 3, nullptr};
     for (int c = threadIdx.x; c < P.smokeCells; c += blockDim.x) {
       SmokeCell s = smokeCellOf(P, H, c);
@@ -1258,7 +1268,7 @@ __global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_evolve(FpBatch bt) {
     const int d = P.smokeDiv, blocks = d / 2;
     const float sp = P.h * (float)d, invSp = 1.f / sp, volume = (float)(d * d * d / 8);
     const bool half = P.scalarHalf != 0;
-    Stage G{};
+    TransportStage G{};
     Field V{P.vel, 3, nullptr};
     uint32_t busy = 0;
     for (int c = threadIdx.x; c < P.smokeCells; c += blockDim.x) {

@@ -12,6 +12,38 @@ import numpy as np
 from . import abi
 
 
+class Snapshot:
+    """A state blob the library allocated (fp_*_snapshot), kept in host memory without a copy
+    (states of large budgets take gigabytes) and released with fp_snapshot_free. `bytes(blob)`
+    copies it; restore() takes either."""
+
+    def __init__(self, lib, ptr: C.c_void_p, size: int):
+        self.lib, self.ptr, self.size = lib, ptr, size
+
+    def __len__(self) -> int:
+        return self.size
+
+    def __bytes__(self) -> bytes:
+        out = bytearray(self.size)
+        C.memmove((C.c_char * self.size).from_buffer(out), self.ptr, self.size)
+        return bytes(out)
+
+    def __getitem__(self, key):
+        return bytes(self)[key]
+
+    def __del__(self):
+        if getattr(self, "ptr", None):
+            self.lib.fp_snapshot_free(self.ptr)
+            self.ptr = None
+
+
+def _blob(blob):
+    """(pointer, size) of a Snapshot or a bytes-like blob."""
+    if isinstance(blob, Snapshot):
+        return blob.ptr, blob.size
+    return blob, len(blob)
+
+
 class FireProError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(message)
@@ -68,18 +100,15 @@ class FluidSimulation:
         """The pressure solve's smoother, levels, sweeps and Krylov wrapper (fp_sim_set_schedule)."""
         self._check(self.lib.fp_sim_set_schedule(self.h, C.byref(schedule)))
 
-    def snapshot(self) -> bytes:
-        """The whole state between steps as bytes (fp_sim_snapshot)."""
+    def snapshot(self) -> Snapshot:
+        """The whole state between steps (fp_sim_snapshot)."""
         p, n = C.c_void_p(), C.c_size_t()
         self._check(self.lib.fp_sim_snapshot(self.h, C.byref(p), C.byref(n)))
-        try:
-            return C.string_at(p, n.value)
-        finally:
-            self.lib.fp_snapshot_free(p)
+        return Snapshot(self.lib, p, n.value)
 
-    def restore(self, blob: bytes):
+    def restore(self, blob):
         """Put a snapshot of a simulation of the same grid back (fp_sim_restore)."""
-        self._check(self.lib.fp_sim_restore(self.h, blob, len(blob)))
+        self._check(self.lib.fp_sim_restore(self.h, *_blob(blob)))
 
     def render(self, camera: abi.fp_camera, settings: abi.fp_render_settings) -> np.ndarray:
         """The latest state rendered: (height, width, 4) linear radiance and opacity."""
@@ -216,16 +245,13 @@ class SimulationBatch:
     def set_schedule(self, sim: int, schedule: abi.fp_solver_schedule):
         self._check(self.lib.fp_batch_set_schedule(self.h, sim, C.byref(schedule)))
 
-    def snapshot(self, sim: int) -> bytes:
+    def snapshot(self, sim: int) -> Snapshot:
         p, n = C.c_void_p(), C.c_size_t()
         self._check(self.lib.fp_batch_snapshot(self.h, sim, C.byref(p), C.byref(n)))
-        try:
-            return C.string_at(p, n.value)
-        finally:
-            self.lib.fp_snapshot_free(p)
+        return Snapshot(self.lib, p, n.value)
 
-    def restore(self, sim: int, blob: bytes):
-        self._check(self.lib.fp_batch_restore(self.h, sim, blob, len(blob)))
+    def restore(self, sim: int, blob):
+        self._check(self.lib.fp_batch_restore(self.h, sim, *_blob(blob)))
 
     def read_solver(self, sim: int) -> abi.fp_solver_stats:
         s = abi.fp_solver_stats()
@@ -336,17 +362,14 @@ class FireServer:
         self._check(self.lib.fp_server_open(self.h, C.byref(grid), cutoff, int(ground), C.byref(out)))
         return out.value
 
-    def snapshot(self, session: int) -> bytes:
+    def snapshot(self, session: int) -> Snapshot:
         """A live, idle session's state (fp_server_snapshot)."""
         p, n = C.c_void_p(), C.c_size_t()
         self._check(self.lib.fp_server_snapshot(self.h, session, C.byref(p), C.byref(n)))
-        try:
-            return C.string_at(p, n.value)
-        finally:
-            self.lib.fp_snapshot_free(p)
+        return Snapshot(self.lib, p, n.value)
 
-    def restore(self, session: int, blob: bytes):
-        self._check(self.lib.fp_server_restore(self.h, session, blob, len(blob)))
+    def restore(self, session: int, blob):
+        self._check(self.lib.fp_server_restore(self.h, session, *_blob(blob)))
 
     def set_solver(self, schedule: abi.fp_solver_schedule, vcycles: int = 1, tolerance: float = 0.0):
         """The pressure solve of the sessions opened from now on (fp_server_set_solver)."""
