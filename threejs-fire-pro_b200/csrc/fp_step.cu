@@ -28,15 +28,20 @@ constexpr int STAGE_SIDE = 8 + 2 * HALO;  // the staged kernels run for 8^3 bric
 
 // Where the staged copy sits: its first cell and its side.
 // SS, the box's side, is a compile-time constant, so staged addresses fold into immediate
-// offsets of the shared-memory loads.
+// offsets of the shared-memory loads. SS = 0: nothing is staged (every read goes through the
+// directory), known at compile time, so a staged kernel carries no code for the unstaged form
+// and the reverse.
 template <int SS>
 struct Stage {
   int ox, oy, oz;
   static constexpr int S = SS, S3 = SS * SS * SS;
 };
-using TransportStage = Stage<8 + 2 * HALO>;
+// The transport kernels' box: the brick and a HALO-cell rim when staged, else nothing.
+template <bool STAGED>
+using TransportStage = Stage<STAGED ? 8 + 2 * HALO : 0>;
 
-// A field a kernel reads: the pool and, when staged, its shared copy.
+// A field a kernel reads: the pool and, when staged, its shared copy (set exactly when the
+// kernel's Stage has a side).
 struct Field {
   const float* pool;
   int ch;
@@ -51,8 +56,26 @@ FP_DEV int stagedAt(const Stage<SS>& G, int x, int y, int z) { return ((z - G.oz
 // A cell within HALO cells of the home brick: the staged box always holds it, so no check.
 template <int SS>
 FP_DEV float nearCell(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& f, int c, int x, int y, int z) {
-  if (f.sm) return f.sm[c * G.S3 + stagedAt(G, x, y, z)];
-  return cellAt(P, H, f.pool, f.ch, c, x, y, z, f.half);
+  if constexpr (SS > 0) return f.sm[c * G.S3 + stagedAt(G, x, y, z)];
+  else return cellAt(P, H, f.pool, f.ch, c, x, y, z, f.half);
+}
+
+// The staged kernels' taps past the staged box (traces longer than the rim): out of line, so
+// the rare path costs the kernels no instruction-cache space.
+// Returned by value, so the callers' blocks stay in registers.
+struct Cells8 {
+  float v[8];
+};
+static __device__ __noinline__ Cells8 blockCellsFar(const SimParams& P, const Home& H, const Field& f, int c, int x0,
+                                                    int y0, int z0) {
+  Cells8 r;
+#pragma unroll
+  for (int j = 0; j < 8; j++) r.v[j] = cellAt(P, H, f.pool, f.ch, c, x0 + (j & 1), y0 + ((j >> 1) & 1), z0 + (j >> 2), f.half);
+  return r;
+}
+static __device__ __noinline__ float sampleFar(const SimParams& P, const Home& H, const Field& f, int c, float px,
+                                               float py, float pz) {
+  return sampleCells(P, H, f.pool, f.ch, c, px, py, pz, f.half);
 }
 
 // The 2x2x2 block from corner (x0,y0,z0) of channel c into t (x fastest): from shared memory
@@ -60,20 +83,27 @@ FP_DEV float nearCell(const SimParams& P, const Home& H, const Stage<SS>& G, con
 template <int SS>
 FP_DEV void blockCells(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& f, int c, const float* b, int x0,
                        int y0, int z0, float* t) {
-  if (b) {
-    const float* q = b + c * G.S3;
-    int S = G.S, S2 = G.S * G.S;
-    t[0] = q[0]; t[1] = q[1]; t[2] = q[S]; t[3] = q[S + 1];
-    t[4] = q[S2]; t[5] = q[S2 + 1]; t[6] = q[S2 + S]; t[7] = q[S2 + S + 1];
-    return;
-  }
+  if constexpr (SS > 0) {
+    if (b) {
+      const float* q = b + c * G.S3;
+      constexpr int S = SS, S2 = SS * SS;
+      t[0] = q[0]; t[1] = q[1]; t[2] = q[S]; t[3] = q[S + 1];
+      t[4] = q[S2]; t[5] = q[S2 + 1]; t[6] = q[S2 + S]; t[7] = q[S2 + S + 1];
+    } else {
+      Cells8 r = blockCellsFar(P, H, f, c, x0, y0, z0);
 #pragma unroll
-  for (int j = 0; j < 8; j++) t[j] = cellAt(P, H, f.pool, f.ch, c, x0 + (j & 1), y0 + ((j >> 1) & 1), z0 + (j >> 2), f.half);
+      for (int j = 0; j < 8; j++) t[j] = r.v[j];
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+      t[j] = cellAt(P, H, f.pool, f.ch, c, x0 + (j & 1), y0 + ((j >> 1) & 1), z0 + (j >> 2), f.half);
+  }
 }
 // The staged address of the block from corner (x0,y0,z0) when the whole block is staged.
 template <int SS>
 FP_DEV const float* stagedBlock(const Stage<SS>& G, const Field& f, int x0, int y0, int z0) {
-  if (!f.sm) return nullptr;
+  if constexpr (SS == 0) return nullptr;
   unsigned lx = (unsigned)(x0 - G.ox), ly = (unsigned)(y0 - G.oy), lz = (unsigned)(z0 - G.oz);
   unsigned lim = (unsigned)(G.S - 1);
   if (lx < lim && ly < lim && lz < lim) return f.sm + ((int)lz * G.S + (int)ly) * G.S + (int)lx;
@@ -84,7 +114,7 @@ FP_DEV const float* stagedBlock(const Stage<SS>& G, const Field& f, int x0, int 
 template <int SS>
 FP_DEV float fieldSample(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& f, int c, float px, float py,
                          float pz) {
-  if (f.sm) {
+  if constexpr (SS > 0) {
     float qx = px - 0.5f, qy = py - 0.5f, qz = pz - 0.5f;
     float gx = floorf(qx), gy = floorf(qy), gz = floorf(qz);
     const float* b = stagedBlock(G, f, (int)gx, (int)gy, (int)gz);
@@ -93,8 +123,10 @@ FP_DEV float fieldSample(const SimParams& P, const Home& H, const Stage<SS>& G, 
       blockCells(P, H, G, f, c, b, 0, 0, 0, t);
       return blend8(t, qx - gx, qy - gy, qz - gz);
     }
+    return sampleFar(P, H, f, c, px, py, pz);
+  } else {
+    return sampleCells(P, H, f.pool, f.ch, c, px, py, pz, f.half);
   }
-  return sampleCells(P, H, f.pool, f.ch, c, px, py, pz, f.half);
 }
 
 // Copy channels [0, nch) of a pool of `ch` channels over the staged box into shared memory,
@@ -105,7 +137,8 @@ FP_DEV float fieldSample(const SimParams& P, const Home& H, const Stage<SS>& G, 
 template <int SS>
 FP_DEV void stageField(const SimParams& P, const Home& H, const Stage<SS>& G, float* sm, const float* pool, int ch,
                        bool half = false, int nch = 0) {
-  constexpr int S = SS, S3 = S * S * S;
+  constexpr int S = SS > 0 ? SS : 1, S3 = SS * SS * SS;
+  if constexpr (SS == 0) return;
   if (nch <= 0) nch = ch;
   for (int i = threadIdx.x; i < S3; i += blockDim.x) {
     int lx = i % S, ly = (i / S) % S, lz = i / (S * S);
@@ -131,8 +164,9 @@ FP_DEV void stageWait() {
   __syncthreads();
 }
 
-FP_DEV TransportStage stageOf(const SimParams& P, const Home& H) {
-  TransportStage G;
+template <bool STAGED>
+FP_DEV TransportStage<STAGED> stageOf(const SimParams& P, const Home& H) {
+  TransportStage<STAGED> G;
   G.ox = H.bx * P.B - HALO;
   G.oy = H.by * P.B - HALO;
   G.oz = H.bz * P.B - HALO;
@@ -146,6 +180,17 @@ FP_DEV float velComp(const SimParams& P, const Home& H, const Stage<SS>& G, cons
   float qx = px * P.invH, qy = py * P.invH, qz = pz * P.invH;
   return fieldSample(P, H, G, v, c, c == 0 ? qx - 0.5f : qx, c == 1 ? qy - 0.5f : qy, c == 2 ? qz - 0.5f : qz);
 }
+// velocityAt through the directory, q in cell units.
+FP_DEV float3 velocityCells(const SimParams& P, const Home& H, const Field& v, const float* q) {
+  return make_float3(sampleCells(P, H, v.pool, v.ch, 0, q[0] - 0.5f, q[1], q[2], v.half),
+                     sampleCells(P, H, v.pool, v.ch, 1, q[0], q[1] - 0.5f, q[2], v.half),
+                     sampleCells(P, H, v.pool, v.ch, 2, q[0], q[1], q[2] - 0.5f, v.half));
+}
+static __device__ __noinline__ float3 velocityFar(const SimParams& P, const Home& H, const Field& v, float qx, float qy,
+                                                  float qz) {
+  const float q[3] = {qx, qy, qz};
+  return velocityCells(P, H, v, q);
+}
 // velocityAt (fluid-advection.wgsl:17-21): the three staggered samples share their floors
 // (per axis: unshifted, and shifted half a cell for the component stored along it) and one
 // check that all three blocks are staged.
@@ -153,7 +198,7 @@ template <int SS>
 FP_DEV float3 velocityAt(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& v, float px, float py,
                          float pz) {
   const float q[3] = {px * P.invH, py * P.invH, pz * P.invH};
-  if (v.sm) {
+  if constexpr (SS > 0) {
     const int o[3] = {G.ox, G.oy, G.oz};
     int i0[3], i1[3];
     float f0[3], f1[3];
@@ -169,7 +214,7 @@ FP_DEV float3 velocityAt(const SimParams& P, const Home& H, const Stage<SS>& G, 
       in = in && i1[a] >= 0 && i0[a] < G.S - 1;  // i1 <= i0 <= i1 + 1
     }
     if (in) {
-      const int S = G.S, S2 = G.S * G.S;
+      constexpr int S = SS, S2 = SS * SS;
       float t[8];
       float3 r;
       blockCells(P, H, G, v, 0, v.sm + i0[2] * S2 + i0[1] * S + i1[0], 0, 0, 0, t);
@@ -180,10 +225,10 @@ FP_DEV float3 velocityAt(const SimParams& P, const Home& H, const Stage<SS>& G, 
       r.z = blend8(t, f0[0], f0[1], f1[2]);
       return r;
     }
+    return velocityFar(P, H, v, q[0], q[1], q[2]);
+  } else {
+    return velocityCells(P, H, v, q);
   }
-  return make_float3(sampleCells(P, H, v.pool, v.ch, 0, q[0] - 0.5f, q[1], q[2], v.half),
-                     sampleCells(P, H, v.pool, v.ch, 1, q[0], q[1] - 0.5f, q[2], v.half),
-                     sampleCells(P, H, v.pool, v.ch, 2, q[0], q[1], q[2] - 0.5f, v.half));
 }
 FP_DEV float get(const float3& v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
 
@@ -328,7 +373,7 @@ FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
   const SimParams& P = *Pp;
   uint32_t id = P.active[i];
   Home H = enterBrick(P, id, nslot);
-  TransportStage G = stageOf(P, H);
+  TransportStage<STAGED> G = stageOf<STAGED>(P, H);
   Field V{P.vel, 3, STAGED ? smem : nullptr};
   Field F{P.fld, 4, STAGED ? smem + 3 * G.S3 : nullptr, P.scalarHalf != 0};
   if (STAGED) {
@@ -379,7 +424,7 @@ FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
   const SimParams& P = *Pp;
   uint32_t id = P.active[i];
   Home H = enterBrick(P, id, nslot);
-  TransportStage G = stageOf(P, H);
+  TransportStage<STAGED> G = stageOf<STAGED>(P, H);
   Field V{P.vel, 3, STAGED ? smem : nullptr};
   Field Vp{P.velP, 3, STAGED ? smem + 3 * G.S3 : nullptr};
   if (STAGED) {
@@ -475,7 +520,7 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
     expandsAll = 0;
   }
   Home H = enterBrick(P, id, nslot);
-  TransportStage G = stageOf(P, H);
+  TransportStage<STAGED> G = stageOf<STAGED>(P, H);
   const SimParams& VP = STAGED ? P : *P.vview;  // the velocity lattice the traces sample
   Field V{P.vel, 3, STAGED ? smem : nullptr};
   Field Fp{P.fldP, 4, STAGED ? smem + 3 * G.S3 : nullptr, false};  // the predictor: FP32
@@ -673,7 +718,7 @@ FP_DEV void brick_curl(const SimParams* __restrict__ Pp, uint32_t i) {
   const SimParams& P = *Pp;
   if (!P.curlOn) return;  // the same for the whole CTA
   Home H = enterBrick(P, P.active[i], nslot);
-  Stage<8 + 2> G;  // staged: 8^3 bricks and a one-cell rim
+  Stage<STAGED ? 8 + 2 : 0> G;  // staged: 8^3 bricks and a one-cell rim
   G.ox = H.bx * P.B - 1;
   G.oy = H.by * P.B - 1;
   G.oz = H.bz * P.B - 1;
@@ -896,8 +941,8 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   const int SUB = STAGED ? 8 : min(P.B, FORCE_SUB), E = SUB + 1, E3 = E * E * E, per = STAGED ? 1 : P.B / SUB;
   float* stage = reinterpret_cast<float*>(forceTile + E3);
   // Staged (8^3 bricks: E = 9): the curl over E + 2 cells a side, two scalars over E.
-  Stage<11> Gc;
-  Stage<9> Gs;
+  Stage<STAGED ? 11 : 0> Gc;
+  Stage<STAGED ? 9 : 0> Gs;
   Gc.ox = H.bx * P.B - 1;
   Gc.oy = H.by * P.B - 1;
   Gc.oz = H.bz * P.B - 1;
@@ -1183,7 +1228,7 @@ FP_DEV SmokeCell smokeCellOf(const SimParams& P, const Home& H, int c) {
 }
 // traceBack / traceForward (fluid-advection.wgsl:67-75) from `p` with centre velocity `cv`.
 FP_DEV float3 smokeTrace(const SimParams& P, const Home& H, const float* p, float3 cv, float sign) {
-  TransportStage G{};
+  Stage<0> G{};
   Field V{P.vel, 3, nullptr};
   float3 vm = velocityAt(*P.vview, H, G, V, p[0] + sign * 0.5f * P.dt * cv.x, p[1] + sign * 0.5f * P.dt * cv.y,
                          p[2] + sign * 0.5f * P.dt * cv.z);
@@ -1203,7 +1248,7 @@ __global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_advect(FpBatch bt) {
     const size_t slot = (size_t)nslot[13], SN = (size_t)P.smokeCells;
     const float sp = P.h * (float)P.smokeDiv, invSp = 1.f / sp;
     const bool half = P.scalarHalf != 0;
-    TransportStage G{};
+    Stage<0> G{};
     Field V{P.vel, 3, nullptr};
     for (int c = threadIdx.x; c < P.smokeCells; c += blockDim.x) {
       SmokeCell s = smokeCellOf(P, H, c);
@@ -1268,7 +1313,7 @@ __global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_evolve(FpBatch bt) {
     const int d = P.smokeDiv, blocks = d / 2;
     const float sp = P.h * (float)d, invSp = 1.f / sp, volume = (float)(d * d * d / 8);
     const bool half = P.scalarHalf != 0;
-    TransportStage G{};
+    Stage<0> G{};
     Field V{P.vel, 3, nullptr};
     uint32_t busy = 0;
     for (int c = threadIdx.x; c < P.smokeCells; c += blockDim.x) {
