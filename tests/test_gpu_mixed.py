@@ -4,10 +4,15 @@ FP_PRECISION_MIXED stores the advected scalars' state in FP16 and the multigrid 
 the finest in BF16, with FP32 arithmetic; later V-cycles correct the finest FP32 level from its
 residual. Parity is against the FP64 oracle running the same number of V-cycles: tables bit
 for bit; velocity and pressure within relative L2 1e-3 per step (teacher forced, as the FP32
-parity tests). The FP16 scalars and what derives from them (the expansion and the divergence
-right-hand side) are held to MIXED_SCALAR_TOL: rounding the state to FP16 costs up to 2.8e-4
-relative per store, and quantised values sit exactly on the MacCormack limiter's bounds far
-more often, where FP32 and FP64 keep or revert the correction differently.
+parity tests). The FP16 scalars (smoke, heat, lifetime, fuel) are held to the same 1e-3 with
+the same flip-cell rule: rounding the state to FP16 costs up to 2.8e-4 relative per store.
+Two derived fields cannot meet 1e-3 and are held to MIXED_FLAME_TOL: the expansion and the
+divergence right-hand side that subtracts it. The expansion is the flame ramp's integral over
+[lifetime after, lifetime before] plus the burned fuel; it lives only where the flame burns, so
+a lifetime or fuel value that the limiter keeps on one side and reverts on the other (quantised
+FP16 values sit exactly on the limiter's bounds far more often than FP32 ones) moves a large
+share of the field's norm. Observed worst per step (large scene, 34 steps): expansion 4.8e-3
+(2.8e-3 without the flip cells), divergence 1.0e-3; every other field within 1e-3.
 """
 import numpy as np
 import pytest
@@ -19,8 +24,9 @@ from test_gpu_parity import TOL, check
 
 pytestmark = pytest.mark.gpu
 
-MIXED_SCALAR_TOL = 5e-3
-FP16_DERIVED = ("smoke", "heat", "lifetime", "fuel", "expansion", "divergence")
+MIXED_SCALAR_TOL = 5e-3  # free-running comparison of the two precisions (below)
+MIXED_FLAME_TOL = 5e-3
+FLAME_DERIVED = ("expansion", "divergence")
 
 
 def run(scene, steps, vcycles, precision=abi.FP_PRECISION_FP32, budget=2 ** 19, **kw):
@@ -29,9 +35,12 @@ def run(scene, steps, vcycles, precision=abi.FP_PRECISION_FP32, budget=2 ** 19, 
 
 
 def check_mixed(reports, min_active=1):
-    """Tables as check(); velocity and pressure within TOL, the FP16-derived fields within
-    MIXED_SCALAR_TOL."""
+    """Tables as check(); every field within TOL (the flip-cell rule of parity.field_within)
+    except the expansion and divergence, within MIXED_FLAME_TOL; the flip-cell rule needed in at
+    most half the steps per field (quantised FP16 values meet the limiter's bounds exactly far
+    more often than FP32 ones, so isolated flips come in more steps)."""
     worst = {}
+    trimmed = {}
     for step, tables, fields, n in reports:
         for k, v in tables.items():
             if k == "activity":
@@ -42,10 +51,14 @@ def check_mixed(reports, min_active=1):
             worst[k] = max(worst.get(k, 0.0), v)
             if k.endswith("@trim"):
                 continue
-            tol = MIXED_SCALAR_TOL if k in FP16_DERIVED else TOL
+            tol = MIXED_FLAME_TOL if k in FLAME_DERIVED else TOL
             assert parity.field_within(fields, k, tol), f"step {step}: {k} relative L2 {v:.3e} > {tol}"
+            if v > tol:
+                trimmed.setdefault(k, []).append(step)
     assert max(r[3] for r in reports) >= min_active
     print("worst relative L2:", {k: f"{v:.2e}" for k, v in worst.items()})
+    for k, v in trimmed.items():
+        assert len(v) <= max(2, len(reports) // 2), f"{k} needed the flip-cell trim in {len(v)} of {len(reports)} steps"
     return worst
 
 

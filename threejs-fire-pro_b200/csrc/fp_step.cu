@@ -21,9 +21,10 @@ namespace {
 constexpr int THREADS = 256;
 constexpr int HALO = 2;
 constexpr int STAGE_SIDE = 8 + 2 * HALO;  // the staged kernels run for 8^3 bricks only
-// Resident CTAs per SM the transport kernels are compiled for (register cap 65536 / (256 n)).
+// Resident CTAs per SM the transport and force kernels are compiled and launched for (register
+// cap 65536 / (256 n)): three (85 registers) beat four (64, with spills) on the B200.
 #ifndef FP_TRANSPORT_CTAS
-#define FP_TRANSPORT_CTAS 4
+#define FP_TRANSPORT_CTAS 3
 #endif
 
 // Where the staged copy sits: its first cell and its side.
@@ -1001,7 +1002,7 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   }
 }
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS, 4) k_forces(FpBatch bt) {
+__global__ void __launch_bounds__(THREADS, FP_TRANSPORT_CTAS) k_forces(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
@@ -1390,21 +1391,21 @@ void fp_step_configure(int B) {
 
 void fp_launch_predict(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
   if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
-    k_predict<true><<<sms * 4, THREADS, stagedBytes(7), st>>>(bt);
+    k_predict<true><<<sms * FP_TRANSPORT_CTAS, THREADS, stagedBytes(7), st>>>(bt);
   else
-    k_predict<false><<<sms * 4, THREADS, 0, st>>>(bt);
+    k_predict<false><<<sms * FP_TRANSPORT_CTAS, THREADS, 0, st>>>(bt);
 }
 void fp_launch_correct(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
   if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
-    k_correct<true><<<sms * 4, THREADS, stagedBytes(6), st>>>(bt);
+    k_correct<true><<<sms * FP_TRANSPORT_CTAS, THREADS, stagedBytes(6), st>>>(bt);
   else
-    k_correct<false><<<sms * 4, THREADS, 0, st>>>(bt);
+    k_correct<false><<<sms * FP_TRANSPORT_CTAS, THREADS, 0, st>>>(bt);
 }
 void fp_launch_evolve(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
   if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
-    k_evolve<true><<<sms * 4, THREADS, stagedBytes(7), st>>>(bt);
+    k_evolve<true><<<sms * FP_TRANSPORT_CTAS, THREADS, stagedBytes(7), st>>>(bt);
   else
-    k_evolve<false><<<sms * 4, THREADS, 0, st>>>(bt);
+    k_evolve<false><<<sms * FP_TRANSPORT_CTAS, THREADS, 0, st>>>(bt);
 }
 void fp_launch_curl(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
   if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
@@ -1414,11 +1415,11 @@ void fp_launch_curl(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) 
 }
 void fp_launch_forces(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
   if (B == 8 && vd == 1) {  // staged: 8^3 bricks, one lattice
-    k_forces<true><<<sms * 4, THREADS, FORCE_STAGED_BYTES, st>>>(bt);
+    k_forces<true><<<sms * FP_TRANSPORT_CTAS, THREADS, FORCE_STAGED_BYTES, st>>>(bt);
     return;
   }
   const size_t side = (size_t)(B < FORCE_SUB ? B : FORCE_SUB) + 1, smem = side * side * side * sizeof(float3);
-  k_forces<false><<<sms * 4, THREADS, smem, st>>>(bt);
+  k_forces<false><<<sms * FP_TRANSPORT_CTAS, THREADS, smem, st>>>(bt);
 }
 void fp_launch_divergence(const FpBatch& bt, int pSel, int vd, int sms, cudaStream_t st) {
   if (vd == 1)
