@@ -276,3 +276,15 @@ def test_tile_lifecycle_matches_oracle():
             return scenes.make_frame(scenes.settings(), scenes.combustion(), False, src)
 
     check(run(Short(), 66, budget=2 ** 18), tol=TOL)
+
+
+def test_default_grid_large_scene():
+    """The reference's default grid (options.ts:460-462: 16^3 bricks, velocityDivisor 2,
+    smokeDivisor 2) on the large scene through the burst at step 30: colliders, turbulence,
+    three emitters, coarse smoke."""
+    sc = scenes.LargeScene()
+    sc.brick_size = 16
+    sc.velocity_divisor = 2
+    grid = sc.grid(budget=2 ** 22)
+    grid.smoke_divisor = 2
+    check(run(sc, 34, grid=grid, budget=2 ** 22), min_active=16)
