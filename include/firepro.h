@@ -208,6 +208,22 @@ typedef struct fp_solver_stats {
                                         keeps (computeDivergence's source), or -1 */
 } fp_solver_stats;
 
+/* The bounds-checked build (`fp_sim_read_bounds`): the library built with `build.py --debug`
+ * (lib/libfirepro_debug.so) checks every index its kernels read out of a table (a slot from a
+ * brick entry or a neighbour record, a tile from the directory or its hash, a brick id from a
+ * work list) against the table's size before using it. A bad index is counted, the first is
+ * kept, and its access is skipped (it reads as "no slot"): no kernel traps or faults. No
+ * reference counterpart (SURVEY's debug aid: WebGPU validation of the reference's bindings). */
+typedef struct fp_bounds {
+  int32_t checked; /* 1: this library checks (the debug build); 0: the release build, nothing below */
+  uint32_t count;  /* bad indices seen since the simulation was created or reset */
+  int32_t site;    /* where the first was read: 1 neighbour record, 2 brick entry, 3 tile neighbour,
+                      4 tile hash, 5 brick id of a work list */
+  int32_t pad;
+  int64_t index;   /* the first bad index */
+  int64_t limit;   /* the size of its table */
+} fp_bounds;
+
 /* Device time of one phase of the step, accumulated while profiling is on: the restatement
  * of the reference's per-pass GPU timestamps (src/engine/GpuProfiler.ts:21-109). */
 typedef struct fp_phase {
@@ -271,6 +287,9 @@ int fp_sim_reserve_tiles(fp_sim* sim, uint32_t tiles);
 int fp_sim_set_solver(fp_sim* sim, int vcycles, float tolerance);
 /* The latest step's solve (waits for the step's work). */
 int fp_sim_read_solver(fp_sim* sim, fp_solver_stats* out);
+/* The bounds-checked build's record of this simulation (waits for its work); `checked` 0 in
+ * the release build. */
+int fp_sim_read_bounds(fp_sim* sim, fp_bounds* out);
 
 /* The pressure solve's schedule. The default (all fields zero) is the reference's V-cycle
  * (PressureSolver.ts:276-365): weighted Jacobi (omega 0.8), every level down to one cell a

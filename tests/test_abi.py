@@ -6,6 +6,8 @@ import subprocess
 import tempfile
 from pathlib import Path
 
+import pytest
+
 from firepro import abi
 
 ROOT = Path(__file__).resolve().parent.parent
@@ -26,6 +28,15 @@ def test_library_exports_every_declared_function(cuda_lib_path):
     assert set(names) == set(abi.SIGNATURES), "the ctypes mirror declares exactly the header's functions"
 
 
+def test_debug_library_exports_every_declared_function():
+    """The bounds-checked build (build.py --debug) exports the same functions."""
+    if not abi.DEBUG_LIB_PATH.exists():
+        pytest.skip("the bounds-checked build is not built here")
+    lib = C.CDLL(str(abi.DEBUG_LIB_PATH))
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
 def test_abi_version(cuda_lib_path):
     lib = abi.load_library(cuda_lib_path)
     assert lib.fp_abi_version() == 1
@@ -34,7 +45,7 @@ def test_abi_version(cuda_lib_path):
 def test_struct_layouts_match_c():
     structs = ["fp_grid", "fp_settings", "fp_flame_ramp", "fp_combustion", "fp_fuel", "fp_source", "fp_force",
                "fp_collider", "fp_mesh_source", "fp_frame", "fp_stats", "fp_phase", "fp_server_config", "fp_completion",
-               "fp_server_stats", "fp_solver_stats", "fp_camera", "fp_render_settings"]
+               "fp_server_stats", "fp_solver_stats", "fp_camera", "fp_render_settings", "fp_bounds"]
     src = "#include <stdio.h>\n#include <stddef.h>\n#include \"firepro.h\"\nint main(void){\n"
     for s in structs:
         src += f'  printf("{s} %zu\\n", sizeof({s}));\n'

@@ -2,6 +2,9 @@
 
 Each source compiles to an object under `_build/` when it (or a header) is newer than its
 object; the shared library links them. nvcc cross-compiles: no GPU is needed to build.
+`--debug` (build(debug=True)) builds the bounds-checked library `lib/libfirepro_debug.so`
+instead (FP_BOUNDS, objects under `_build/debug/`): its kernels check every index they read out
+of a table and record the first bad one (fp_sim_read_bounds).
 """
 from __future__ import annotations
 
@@ -15,6 +18,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 BUILD = HERE / "_build"
 LIB = HERE / "lib" / "libfirepro.so"
+DEBUG_LIB = HERE / "lib" / "libfirepro_debug.so"
 INCLUDE = HERE.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -38,17 +42,19 @@ def _headers():
     return list(CSRC.glob("*.h")) + list(CSRC.glob("*.hpp")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
 
 
-def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
-    LIB.parent.mkdir(exist_ok=True)
+def build(verbose: bool = False, ptxas_info: bool = False, debug: bool = False) -> Path:
+    out_dir, lib, defines = (BUILD / "debug", DEBUG_LIB, ["-DFP_BOUNDS"]) if debug else (BUILD, LIB, [])
+    out_dir.mkdir(parents=True, exist_ok=True)
+    lib.parent.mkdir(exist_ok=True)
     newest_header = max((h.stat().st_mtime for h in _headers()), default=0)
     objects, commands = [], []
     for src in _sources():
-        obj = BUILD / (src.name + ".o")
+        obj = out_dir / (src.name + ".o")
         objects.append(obj)
         if obj.exists() and obj.stat().st_mtime > max(src.stat().st_mtime, newest_header) and not ptxas_info:
             continue
-        cmd = [NVCC, *ARCH, *FLAGS, *FILE_FLAGS.get(src.name, []), "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+        cmd = [NVCC, *ARCH, *FLAGS, *defines, *FILE_FLAGS.get(src.name, []), "-I", str(INCLUDE), "-c", str(src), "-o",
+               str(obj)]
         if ptxas_info and src.suffix == ".cu":
             cmd.insert(1, "-Xptxas=-v")
         if verbose:
@@ -58,13 +64,13 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
     with ThreadPoolExecutor(max_workers=max(1, min(len(commands), os.cpu_count() or 1))) as pool:
         for f in [pool.submit(subprocess.run, cmd, check=True) for cmd in commands]:
             f.result()
-    if not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objects):
-        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objects), "-lcudart"]
+    if not lib.exists() or any(o.stat().st_mtime > lib.stat().st_mtime for o in objects):
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(lib), *map(str, objects), "-lcudart"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    build(verbose=True, ptxas_info="--ptxas" in sys.argv)
+    build(verbose=True, ptxas_info="--ptxas" in sys.argv, debug="--debug" in sys.argv)

@@ -182,6 +182,11 @@ int fp_sim_read_solver(fp_sim* sim, fp_solver_stats* out) {
   return sim->engine->readSolver(out);
 }
 
+int fp_sim_read_bounds(fp_sim* sim, fp_bounds* out) {
+  if (!sim || !out) return failed("fp_sim_read_bounds needs a simulation and an output.", FP_EINVAL);
+  return sim->engine->readBounds(out);
+}
+
 int fp_sim_synchronize(fp_sim* sim) {
   if (!sim) return failed("null simulation", FP_EINVAL);
   int rc = sim->stepper->synchronize();

@@ -68,6 +68,46 @@ FP_DEV double blockSum(double v, double* scratch) {
 FP_DEV int nbrIndex(int dx, int dy, int dz) { return (dz + 1) * 9 + (dy + 1) * 3 + dx + 1; }
 FP_DEV int entryPage(int e) { return e < 0 ? -1 : (e & 0xffffff); }
 
+// The bounds-checked build (FP_BOUNDS, FpBounds in fp_types.h). checkSlot / checkTile pass an
+// index read out of a table through when it is -1 (none) or within the table, and otherwise
+// record it and return -1, so the access it would have made is skipped. homeOk tells a CTA
+// whether its brick id and the brick's own slot are usable; a CTA whose home is not returns
+// before any work. Without FP_BOUNDS every check compiles to nothing.
+#ifdef FP_BOUNDS
+static __device__ __noinline__ void boundsFail(FpBounds* b, int site, long long index, long long limit) {
+  if (!b) return;
+  if (atomicAdd(&b->count, 1u) == 0u) {
+    b->site = site;
+    b->index = index;
+    b->limit = limit;
+  }
+}
+FP_DEV int checkIndex(const SimParams& P, int site, int v, long long limit) {
+  if (v < -1 || (long long)v >= limit) {
+    boundsFail(P.bounds, site, v, limit);
+    return -1;
+  }
+  return v;
+}
+#else
+FP_DEV int checkIndex(const SimParams&, int, int v, long long) { return v; }
+#endif
+FP_DEV int checkSlot(const SimParams& P, int site, int slot) { return checkIndex(P, site, slot, (long long)P.slots); }
+FP_DEV int checkTile(const SimParams& P, int site, int tile) { return checkIndex(P, site, tile, (long long)P.capacity); }
+FP_DEV bool homeOk(const SimParams& P, uint32_t id) {
+#ifdef FP_BOUNDS
+  if ((long long)id >= (long long)P.capacity * 64) {
+    boundsFail(P.bounds, FP_SITE_BRICK_ID, id, (long long)P.capacity * 64);
+    return false;
+  }
+  return checkSlot(P, FP_SITE_ENTRY, entryPage(P.entries[id])) >= 0;
+#else
+  (void)P;
+  (void)id;
+  return true;
+#endif
+}
+
 // tileHash (tiles.wgsl:166-169).
 FP_DEV uint32_t tileHash(int x, int y, int z) {
   return ((uint32_t)x * 73856093u) ^ ((uint32_t)y * 19349663u) ^ ((uint32_t)z * 83492791u);
@@ -79,7 +119,7 @@ FP_DEV int hashFind(const SimParams& P, int x, int y, int z) {
   for (uint32_t probe = 0; probe <= mask; probe++) {
     int4 e = __ldg(&P.hash[h]);
     if (e.w < 0) break;
-    if (e.x == x && e.y == y && e.z == z) return e.w;
+    if (e.x == x && e.y == y && e.z == z) return checkTile(P, FP_SITE_HASH, e.w);
     h = (h + 1) & mask;
   }
   return -1;
@@ -98,7 +138,7 @@ FP_DEV int tileAt(const SimParams& P, const Home& H, int x, int y, int z) {
   if (H.tile >= 0) {
     int dx = x - H.tx, dy = y - H.ty, dz = z - H.tz;
     if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1)
-      return __ldg(&P.tileNbr[H.tile * 27 + nbrIndex(dx, dy, dz)]);
+      return checkTile(P, FP_SITE_TILE_NBR, __ldg(&P.tileNbr[H.tile * 27 + nbrIndex(dx, dy, dz)]));
   }
   return hashFind(P, x, y, z);
 }
@@ -116,7 +156,7 @@ FP_DEV int brickEntryG(const SimParams& P, const Home& H, int bx, int by, int bz
 FP_DEV int brickSlot(const SimParams& P, const Home& H, int bx, int by, int bz) {
   int dx = bx - H.bx, dy = by - H.by, dz = bz - H.bz;
   if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1) return H.nslot[nbrIndex(dx, dy, dz)];
-  return entryPage(brickEntryG(P, H, bx, by, bz));
+  return checkSlot(P, FP_SITE_ENTRY, entryPage(brickEntryG(P, H, bx, by, bz)));
 }
 FP_DEV int localCell(const SimParams& P, int x, int y, int z) {
   int m = P.B - 1;
@@ -380,7 +420,8 @@ FP_DEV Home enterBrick(const SimParams& P, uint32_t id, int* nslot) {
   H.by = t.y * 4 + ((l >> 2) & 3);
   H.bz = t.z * 4 + (l >> 4);
   H.nslot = nslot;
-  if (threadIdx.x < 27) nslot[threadIdx.x] = entryPage(P.records[(size_t)id * FP_RECORD_WORDS + threadIdx.x]);
+  if (threadIdx.x < 27)
+    nslot[threadIdx.x] = checkSlot(P, FP_SITE_RECORD, entryPage(P.records[(size_t)id * FP_RECORD_WORDS + threadIdx.x]));
   __syncthreads();
   return H;
 }

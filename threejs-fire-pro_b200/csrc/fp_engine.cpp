@@ -200,7 +200,8 @@ int Engine::consume() {
 void Engine::freeAll() {
   DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_, &zeroList_,
                          &freeStack_, &counters_, &curl_, &expn_, &div_, &sb_, &donors_, &solids_,
-                         &tileRecD_, &tileNbrD_, &hashD_, &solver_, &tileMask_, &liveTilesD_, &tileIndexD_};
+                         &tileRecD_, &tileNbrD_, &hashD_, &solver_, &tileMask_, &liveTilesD_, &tileIndexD_,
+                         &bounds_};
   for (DeviceBuffer* b : all)
     if (b->ptr) {
       cudaFree(b->ptr);
@@ -227,7 +228,8 @@ int Engine::initialize() {
   int rc;
   if ((rc = check(cudaSetDevice(owner_->device()), "cudaSetDevice"))) return rc;
   freeAll();
-  if (!alloc(counters_, sizeof(FpCounters)) || !alloc(solver_, sizeof(FpSolver))) return FP_ENOMEM;
+  if (!alloc(counters_, sizeof(FpCounters)) || !alloc(solver_, sizeof(FpSolver)) || !alloc(bounds_, sizeof(FpBounds)))
+    return FP_ENOMEM;
   lastSolver_ = FpSolver{};
   slots_ = 0;
   capacity_ = 0;
@@ -1000,6 +1002,7 @@ void Engine::writeStep(SimParams& P, uint8_t* hostBase, uint8_t* devBase, size_t
   P.vcycles = vcycles_;
   P.tolerance = tolerance_;
   P.solver = (FpSolver*)solver_.ptr;
+  P.bounds = (FpBounds*)bounds_.ptr;
   for (int l = 0; l <= bottom_; l++) {
     P.topo[l] = (uint8_t*)topo_[l].ptr;
     if (l > 0) {
@@ -1090,6 +1093,23 @@ int Engine::readSolver(fp_solver_stats* out) {
   return FP_OK;
 }
 
+int Engine::readBounds(fp_bounds* out) {
+  std::memset(out, 0, sizeof(*out));
+#ifdef FP_BOUNDS
+  int rc = consume();
+  if (rc) return rc;
+  if ((rc = check(cudaStreamSynchronize(stream()), "read bounds"))) return rc;
+  FpBounds b{};
+  if ((rc = check(cudaMemcpy(&b, bounds_.ptr, sizeof(b), cudaMemcpyDeviceToHost), "read bounds"))) return rc;
+  out->checked = 1;
+  out->count = b.count;
+  out->site = b.site;
+  out->index = b.index;
+  out->limit = b.limit;
+#endif
+  return FP_OK;
+}
+
 int Engine::setSolver(int vcycles, float tolerance) {
   if (vcycles < 1 || vcycles > FP_MAX_VCYCLES)
     return fail(FP_EINVAL, "vcycles must be from 1 to " + std::to_string(FP_MAX_VCYCLES) + ".");
@@ -1142,7 +1162,7 @@ uint64_t Engine::memoryBytes() const {
   const DeviceBuffer* all[] = {&pages_, &entries_, &state_, &activity_, &records_, &blockCounts_, &active_,
                                &zeroList_, &freeStack_, &counters_, &curl_, &expn_, &div_, &sb_,
                                &donors_, &solids_, &tileRecD_, &tileNbrD_, &hashD_, &solver_, &tileMask_,
-                               &liveTilesD_, &tileIndexD_};
+                               &liveTilesD_, &tileIndexD_, &bounds_};
   for (const DeviceBuffer* b : all) bytes += b->bytes;
   for (auto& b : vel_) bytes += b.bytes;
   for (auto& b : fld_) bytes += b.bytes;

@@ -116,6 +116,7 @@ class Engine {
   // `vcycles` V-cycles a step, stopping at a relative FP64 residual of `tolerance` (0: all).
   int setSolver(int vcycles, float tolerance);
   int readSolver(fp_solver_stats* out);
+  int readBounds(fp_bounds* out);
   // The whole state between steps, host and device, as one blob (fp_sim_snapshot), and back
   // into a simulation of the same grid (fp_sim_restore).
   int snapshot(std::vector<uint8_t>& out);
@@ -185,6 +186,7 @@ class Engine {
   DeviceBuffer p0_[3], topo_[FP_MAX_LEVELS], lp_[FP_MAX_LEVELS][2], lrhs_[FP_MAX_LEVELS];
   DeviceBuffer kry_[3];  // flexible CG: residual, direction, A direction (p0_[2] its iterate)
   DeviceBuffer tileRecD_, tileNbrD_, hashD_, solver_, tileMask_, liveTilesD_, tileIndexD_;
+  DeviceBuffer bounds_;  // FpBounds: the bounds-checked build's record
   std::vector<int> liveTiles_, tileIndex_;  // live tile slots ascending; slot -> position or -1
   int velIdx_[4] = {0, 1, 2, 3};  // start, predictor/projected, corrected, forced
   int fldIdx_[3] = {0, 1, 2};     // start, predictor, evolved

@@ -278,14 +278,14 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
     uint32_t i;
     const SimParams& P = *workSim(bt, FP_WORK_ACTIVE, item < total ? item : base, i).vview;
     const Args A = resolve(P, Sl);
-    const bool has = item < total && !A.skip;
+    const bool has = item < total && !A.skip && homeOk(P, P.active[i]);  // homeOk: the bounds-checked build
     const int fineLevel = OP == RESTRICT ? A.level - 1 : A.level;
     const int stageLevel = OP == PROLONG ? A.level + 1 : fineLevel;
     const float* src = OP == PROLONG ? A.coarse : A.pin;
     const bool srcN = OP == PROLONG ? A.coarseN : A.pinN;
     const uint32_t id = has ? P.active[i] : 0u;
     Home H = homeOf(P, id, nslot);
-    if (has && t < 27) nslot[t] = entryPage(P.records[(size_t)id * FP_RECORD_WORDS + t]);
+    if (has && t < 27) nslot[t] = checkSlot(P, FP_SITE_RECORD, entryPage(P.records[(size_t)id * FP_RECORD_WORDS + t]));
     __syncthreads();
     const int ox = H.bx * SB - R, oy = H.by * SB - R, oz = H.bz * SB - R;
     // Relaxation and prolongation: this thread's own cells' flags and right-hand side or
@@ -537,7 +537,7 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
         flags[j] = f;
         rhs[j] = ldBf(A.rhs, t, A.rhsN);
         for (int k = 0; k < 6; k++) {
-          int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
+          int n = ((f >> k) & 1u) ? checkTile(P, FP_SITE_TILE_NBR, __ldg(&P.tileNbr[t * 27 + nbIndex[k]])) : -1;
           nb[j * 6 + k] = (int16_t)(n >= 0 ? P.tileIndex[n] : -1);
         }
         // Cells that are no unknown are never read and become zero in the first iteration.
@@ -591,7 +591,7 @@ __global__ void __launch_bounds__(1024) k_bottom(FpBatch bt, MgSel Sl, int itera
           float w[6];
 #pragma unroll
           for (int k = 0; k < 6; k++) {
-            int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
+            int n = ((f >> k) & 1u) ? checkTile(P, FP_SITE_TILE_NBR, __ldg(&P.tileNbr[t * 27 + nbIndex[k]])) : -1;
             w[k] = n >= 0 ? ldBf(cur, n, gN) : 0.f;
           }
           float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
@@ -666,7 +666,7 @@ __global__ void __launch_bounds__(1024) k_coarse(FpBatch bt, MgSel Sl, int itera
     int16_t* faces = reinterpret_cast<int16_t*>(fl + n4);  // six a live tile
     for (int q = threadIdx.x; q < nt * 6; q += blockDim.x) {
       const int j = q / 6, k = q % 6;
-      const int n = __ldg(&P.tileNbr[P.liveTiles[j] * 27 + nbIndex[k]]);
+      const int n = checkTile(P, FP_SITE_TILE_NBR, __ldg(&P.tileNbr[P.liveTiles[j] * 27 + nbIndex[k]]));
       faces[q] = (int16_t)(n >= 0 ? P.tileIndex[n] : -1);
     }
     for (int c = threadIdx.x; c < n4; c += blockDim.x) {
@@ -804,6 +804,7 @@ __global__ void __launch_bounds__(256) k_residual(FpBatch bt, int pSel, int cycl
     uint32_t i;
     const SimParams& P = *workSim(bt, FP_WORK_ACTIVE, item, i).vview;
     if (cycle > 0 && P.solver->converged) continue;  // the same for the whole CTA
+    if (!homeOk(P, P.active[i])) continue;  // the bounds-checked build only
     Home H = enterBrick(P, P.active[i], nslot);
     const float* p = P.p0[pSel];
     const long slot = nslot[13];
@@ -867,7 +868,7 @@ __global__ void __launch_bounds__(1024) k_bottom_rb(FpBatch bt, MgSel Sl, int sw
         flags[j] = f;
         rhs[j] = ldBf(A.rhs, t, A.rhsN);
         for (int k = 0; k < 6; k++) {
-          int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
+          int n = ((f >> k) & 1u) ? checkTile(P, FP_SITE_TILE_NBR, __ldg(&P.tileNbr[t * 27 + nbIndex[k]])) : -1;
           nb[j * 6 + k] = (int16_t)(n >= 0 ? P.tileIndex[n] : -1);
         }
         cur[j] = (A.pin && !(f & SOLIDF)) ? ldBf(A.pin, t, A.pinN) : 0.f;
@@ -913,7 +914,7 @@ __global__ void __launch_bounds__(1024) k_bottom_rb(FpBatch bt, MgSel Sl, int sw
           float w[6];
 #pragma unroll
           for (int k = 0; k < 6; k++) {
-            int n = ((f >> k) & 1u) ? __ldg(&P.tileNbr[t * 27 + nbIndex[k]]) : -1;
+            int n = ((f >> k) & 1u) ? checkTile(P, FP_SITE_TILE_NBR, __ldg(&P.tileNbr[t * 27 + nbIndex[k]])) : -1;
             w[k] = n >= 0 ? ldBf(A.pout, n, nB) : 0.f;
           }
           float sum = (w[0] + w[1]) + (w[2] + w[3]) + (w[4] + w[5]);
@@ -945,6 +946,7 @@ __global__ void __launch_bounds__(256) k_fcg(FpBatch bt, int vSel, int cycle) {
     const SimParams& P = *workSim(bt, FP_WORK_ACTIVE, item, i).vview;
     FpSolver* S = P.solver;
     if (cycle > 0 && S->converged) continue;  // the same for the whole CTA
+    if (!homeOk(P, P.active[i])) continue;  // the bounds-checked build only
     Home H = enterBrick(P, P.active[i], nslot);
     const long slot = nslot[13];
     const int m = P.B - 1;
@@ -1074,6 +1076,7 @@ __global__ void __launch_bounds__(128) k_topo_bricks(FpBatch bt) {
     }
     if (slot < 0) continue;
     // The brick's neighbour slots in shared memory: every solid test stays within them.
+    if (!homeOk(P, id)) continue;  // the bounds-checked build only
     Home H = enterBrick(P, id, nslot);
     int bx = H.bx, by = H.by, bz = H.bz;
     // Away from the ground, a brick whose neighbourhood holds no solid cell has every side of

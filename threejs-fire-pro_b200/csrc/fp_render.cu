@@ -53,7 +53,7 @@ FP_DEV int slotAt(const SimParams& P, const FpRender& R, SlotCache& c, int bx, i
   int s = -1;
   if (inBox(c, bx, by, bz)) {
     int t = hashFind(P, bx >> 2, by >> 2, bz >> 2);
-    if (t >= 0) s = entryPage(P.entries[t * 64 + (((bz & 3) * 4 + (by & 3)) * 4 + (bx & 3))]);
+    if (t >= 0) s = checkSlot(P, FP_SITE_ENTRY, entryPage(P.entries[t * 64 + (((bz & 3) * 4 + (by & 3)) * 4 + (bx & 3))]));
   }
   c.bx = bx;
   c.by = by;
@@ -354,6 +354,7 @@ FP_DEV float4 incidentLight(const SimParams& P, const FpRender& R, SlotCache& c,
 FP_DEV bool boxBrick(const SimParams& P, const FpRender& R, SlotCache& c, uint32_t i, int& bx, int& by, int& bz,
                      int& slot) {
   uint32_t id = P.active[i];
+  if (!homeOk(P, id)) return false;  // the bounds-checked build only
   int4 t = __ldg(&P.tileRec[id >> 6]);
   int l = id & 63;
   bx = t.x * 4 + (l & 3);
@@ -789,6 +790,7 @@ __global__ void __launch_bounds__(64) k_collect_lights(const SimParams* __restri
   const float side = (float)P.B * P.h;
   for (uint32_t i = blockIdx.x; i < total; i += gridDim.x) {
     const uint32_t id = P.active[i];
+    if (!homeOk(P, id)) continue;  // the bounds-checked build only
     const int e = P.entries[id];
     if (e < 0) continue;  // the same for the whole CTA
     const int slot = entryPage(e);
@@ -821,7 +823,7 @@ __global__ void __launch_bounds__(64) k_collect_lights(const SimParams* __restri
         if (cl[0] < 0 || cl[1] < 0 || cl[2] < 0) continue;
         int nb[3] = {b[0] + (cl[0] >> sh), b[1] + (cl[1] >> sh), b[2] + (cl[2] >> sh)};
         int t = hashFind(P, nb[0] >> 2, nb[1] >> 2, nb[2] >> 2);
-        int s = t < 0 ? -1 : entryPage(P.entries[t * 64 + (((nb[2] & 3) * 4 + (nb[1] & 3)) * 4 + (nb[0] & 3))]);
+        int s = t < 0 ? -1 : checkSlot(P, FP_SITE_ENTRY, entryPage(P.entries[t * 64 + (((nb[2] & 3) * 4 + (nb[1] & 3)) * 4 + (nb[0] & 3))]));
         if (s < 0) continue;
         float w = (d[0] ? fr[0] : 1.f - fr[0]) * (d[1] ? fr[1] : 1.f - fr[1]) * (d[2] ? fr[2] : 1.f - fr[2]);
         v += ldHalf(P.smk, (size_t)s * P.smokeCells + ((((cl[2] & m) << sh) | (cl[1] & m)) << sh | (cl[0] & m)), half) * w;

@@ -207,6 +207,8 @@ int Engine::renderInputs() {
   P.h = h_;
   P.invH = 1.f / h_;
   P.capacity = capacity_;
+  P.slots = slots_;
+  P.bounds = (FpBounds*)bounds_.ptr;
   P.tileRec = (const int4*)tileRecD_.ptr;
   P.tileNbr = (const int*)tileNbrD_.ptr;
   P.hash = (const int4*)hashD_.ptr;

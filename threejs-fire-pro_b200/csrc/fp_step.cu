@@ -20,7 +20,6 @@ namespace {
 
 constexpr int THREADS = 256;
 constexpr int HALO = 2;
-constexpr int STAGE_SIDE = 8 + 2 * HALO;  // the staged kernels run for 8^3 bricks only
 // Resident CTAs per SM the transport and force kernels are compiled and launched for (register
 // cap 65536 / (256 n)): three (85 registers) beat four (64, with spills) on the B200.
 #ifndef FP_TRANSPORT_CTAS
@@ -373,6 +372,7 @@ FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
   extern __shared__ float smem[];
   const SimParams& P = *Pp;
   uint32_t id = P.active[i];
+  if (!homeOk(P, id)) return;  // the bounds-checked build only
   Home H = enterBrick(P, id, nslot);
   TransportStage<STAGED> G = stageOf<STAGED>(P, H);
   Field V{P.vel, 3, STAGED ? smem : nullptr};
@@ -424,6 +424,7 @@ FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
   extern __shared__ float smem[];
   const SimParams& P = *Pp;
   uint32_t id = P.active[i];
+  if (!homeOk(P, id)) return;  // the bounds-checked build only
   Home H = enterBrick(P, id, nslot);
   TransportStage<STAGED> G = stageOf<STAGED>(P, H);
   Field V{P.vel, 3, STAGED ? smem : nullptr};
@@ -520,6 +521,7 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
     busyAll = 0;
     expandsAll = 0;
   }
+  if (!homeOk(P, id)) return;  // the bounds-checked build only
   Home H = enterBrick(P, id, nslot);
   TransportStage<STAGED> G = stageOf<STAGED>(P, H);
   const SimParams& VP = STAGED ? P : *P.vview;  // the velocity lattice the traces sample
@@ -718,6 +720,7 @@ FP_DEV void brick_curl(const SimParams* __restrict__ Pp, uint32_t i) {
   extern __shared__ float smem[];
   const SimParams& P = *Pp;
   if (!P.curlOn) return;  // the same for the whole CTA
+  if (!homeOk(P, P.active[i])) return;  // the bounds-checked build only
   Home H = enterBrick(P, P.active[i], nslot);
   Stage<STAGED ? 8 + 2 : 0> G;  // staged: 8^3 bricks and a one-cell rim
   G.ox = H.bx * P.B - 1;
@@ -933,6 +936,7 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   extern __shared__ float3 forceTile[];  // (SUB+1)^3, then the staged curl and scalars
   const SimParams& P = *Pp;
   uint32_t id = P.active[i];
+  if (!homeOk(P, id)) return;  // the bounds-checked build only
   Home H = enterBrick(P, id, nslot);
   size_t slot = (size_t)nslot[13];
   const size_t N = P.N;
@@ -1036,6 +1040,7 @@ FP_DEV void brick_divergence(const SimParams* __restrict__ Pp, uint32_t i, int p
   __shared__ int nslot[27];
   const SimParams& P = *Pp;
   float* pOut = P.p0[pSel];
+  if (!homeOk(P, P.active[i])) return;  // the bounds-checked build only
   Home H = enterBrick(P, P.active[i], nslot);
   size_t slot = (size_t)nslot[13];
   const size_t N = P.N;
@@ -1078,6 +1083,7 @@ FP_DEV void brick_project(const SimParams* __restrict__ Pp, uint32_t i, int pSel
   __shared__ int nslot[27];
   const SimParams& P = *Pp;
   const float* p = P.p0[pSel];
+  if (!homeOk(P, P.active[i])) return;  // the bounds-checked build only
   Home H = enterBrick(P, P.active[i], nslot);
   size_t slot = (size_t)nslot[13];
   const size_t N = P.N;
@@ -1170,6 +1176,7 @@ __global__ void __launch_bounds__(THREADS) k_post_divergence(FpBatch bt) {
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = *workSim(bt, FP_WORK_ACTIVE, item, i).vview;  // the velocity lattice
+    if (!homeOk(P, P.active[i])) continue;  // the bounds-checked build only
     Home H = enterBrick(P, P.active[i], nslot);
     const size_t slot = (size_t)nslot[13], N = P.N;
     double d2 = 0.0, v2 = 0.0;
@@ -1245,6 +1252,7 @@ __global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_advect(FpBatch bt) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
     if (P.smokeDiv == 1) continue;  // the same for the whole CTA
+    if (!homeOk(P, P.active[i])) continue;  // the bounds-checked build only
     Home H = enterBrick(P, P.active[i], nslot);
     const size_t slot = (size_t)nslot[13], SN = (size_t)P.smokeCells;
     const float sp = P.h * (float)P.smokeDiv, invSp = 1.f / sp;
@@ -1309,6 +1317,7 @@ __global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_evolve(FpBatch bt) {
     if (P.smokeDiv == 1) continue;  // the same for the whole CTA
     const uint32_t id = P.active[i];
     if (threadIdx.x == 0) busyAll = 0;
+    if (!homeOk(P, id)) continue;  // the bounds-checked build only
     Home H = enterBrick(P, id, nslot);
     const size_t slot = (size_t)nslot[13], SN = (size_t)P.smokeCells;
     const int d = P.smokeDiv, blocks = d / 2;

@@ -107,6 +107,26 @@ struct FpSolver {
   double zq[FP_MAX_VCYCLES], dq[FP_MAX_VCYCLES], ds[FP_MAX_VCYCLES];
 };
 
+// The bounds-checked build (compiled with FP_BOUNDS): every index a kernel reads out of a table
+// (a slot from an entry or a neighbour record, a tile from the directory or its hash, a brick id
+// from a list) is checked against its table before use. A bad one is counted, the first one is
+// kept (its site, value and limit), and the access is skipped: it reads as "no slot" or "no
+// tile", so the kernel goes on and returns normally.
+enum FpBoundsSite {
+  FP_SITE_RECORD = 1,  // a neighbour record's slot (enterBrick)
+  FP_SITE_ENTRY = 2,   // a brick entry's slot (brickSlot beyond the neighbours)
+  FP_SITE_TILE_NBR = 3,  // a tile neighbour slot (tileAt)
+  FP_SITE_HASH = 4,    // a tile slot from the hash (hashFind)
+  FP_SITE_BRICK_ID = 5,  // a brick id from a work list (enterBrick)
+  FP_SITE_LEVEL = 6,   // a multigrid cell's owner slot (cellAddress)
+};
+struct FpBounds {
+  unsigned int count;  // violations seen
+  int site;            // FpBoundsSite of the first
+  long long index;     // the first bad index
+  long long limit;     // the size of its table
+};
+
 struct SimParams {
   // what this step builds besides the fields (one launch covers many simulations, each
   // skipping the work its own flags leave out)
@@ -197,6 +217,7 @@ struct SimParams {
   int vcycles;
   float tolerance;
   FpSolver* solver;  // device: this step's norms and state
+  FpBounds* bounds;  // device: the bounds-checked build's record (unused otherwise)
   uint8_t* topo[FP_MAX_LEVELS];
   float* lp[FP_MAX_LEVELS][2];
   float* lrhs[FP_MAX_LEVELS];

@@ -12,6 +12,9 @@ from pathlib import Path
 
 PACKAGE_DIR = Path(__file__).resolve().parent
 LIB_PATH = PACKAGE_DIR.parent / "lib" / "libfirepro.so"
+# The bounds-checked build (`build.py --debug`); FIREPRO_LIBRARY names the library to open instead
+# of LIB_PATH (set it to this path to run a program on the checked build).
+DEBUG_LIB_PATH = PACKAGE_DIR.parent / "lib" / "libfirepro_debug.so"
 
 FP_OK = 0
 FP_EINVAL = -1
@@ -230,6 +233,11 @@ class fp_solver_stats(C.Structure):
     ]
 
 
+class fp_bounds(C.Structure):
+    _fields_ = [("checked", C.c_int32), ("count", C.c_uint32), ("site", C.c_int32), ("pad", C.c_int32),
+                ("index", C.c_int64), ("limit", C.c_int64)]
+
+
 class fp_mesh(C.Structure):
     _fields_ = [("positions", C.POINTER(C.c_float)), ("vertex_count", C.c_uint32),
                 ("indices", C.POINTER(C.c_uint32)), ("index_count", C.c_uint32)]
@@ -348,6 +356,7 @@ SIGNATURES = {
     "fp_sim_render_device": (C.c_int, [C.c_void_p, C.POINTER(fp_camera), C.POINTER(fp_render_settings), C.c_void_p]),
     "fp_sim_collect_lights": (C.c_int, [C.c_void_p, C.POINTER(fp_render_settings), C.c_void_p, C.c_uint32, C.c_void_p]),
     "fp_sim_read_solver": (C.c_int, [C.c_void_p, C.POINTER(fp_solver_stats)]),
+    "fp_sim_read_bounds": (C.c_int, [C.c_void_p, C.POINTER(fp_bounds)]),
     "fp_batch_set_solver": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, C.c_float]),
     "fp_batch_set_schedule": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
     "fp_server_set_solver": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_float]),
@@ -386,7 +395,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = Path(path) if path is not None else LIB_PATH
+    p = Path(path) if path is not None else Path(os.environ.get("FIREPRO_LIBRARY") or LIB_PATH)
     if not p.exists():
         raise RuntimeError(
             f"The CUDA library {p} is missing: build it with "

@@ -135,6 +135,12 @@ class FluidSimulation:
         self._check(self.lib.fp_sim_read_solver(self.h, C.byref(s)))
         return s
 
+    def read_bounds(self) -> abi.fp_bounds:
+        """The bounds-checked build's record (checked 0 in the release build)."""
+        b = abi.fp_bounds()
+        self._check(self.lib.fp_sim_read_bounds(self.h, C.byref(b)))
+        return b
+
     def reset(self):
         self._check(self.lib.fp_sim_reset(self.h))
 
