@@ -31,17 +31,15 @@ import parity
 from test_gpu_parity import check
 
 sc = getattr(scenes, {scene!r})()
-sims = []
-def factory(g):
-    sims.append(FluidSimulation(g))
-    return sims[-1]
-reports = parity.lockstep(sc, {steps}, factory, budget={budget})
+out = {{}}
+def after(sim, orc):  # the last step's state, before the simulation is disposed
+    cam = render.look_at((0.0, 1.0, 3.0), (0.0, 0.5, 0.0), 160, 90)
+    sim.render(cam, render.default_settings(ray_steps=48, shadow_samples=8))
+    b = sim.read_bounds()
+    out.update(checked=b.checked, count=b.count, site=b.site, index=b.index, limit=b.limit)
+reports = parity.lockstep(sc, {steps}, lambda g: FluidSimulation(g), budget={budget}, after=after)
 check(reports, min_active={min_active})
-sim = sims[-1]
-cam = render.look_at((0.0, 1.0, 3.0), (0.0, 0.5, 0.0), 160, 90)
-sim.render(cam, render.default_settings(ray_steps=48, shadow_samples=8))
-b = sim.read_bounds()
-print("BOUNDS " + json.dumps(dict(checked=b.checked, count=b.count, site=b.site, index=b.index, limit=b.limit)))
+print("BOUNDS " + json.dumps(out))
 """
 
 

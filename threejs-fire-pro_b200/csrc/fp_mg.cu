@@ -456,7 +456,9 @@ __global__ void __launch_bounds__(256) k_level_bricks_staged(FpBatch bt, MgSel S
             }
           }
           float r = residual * 0.5f;
-          long out = slot * ccells + o;
+          // From the last brick level (2^3 a brick) the coarse level is the first tile level,
+          // one cell a brick at the brick's own id (tile slot x 64 + its place in the tile).
+          const long out = SB == 2 ? (long)id : slot * ccells + o;
           stBf(A.pout, out, r, A.poutN);
           float first = 0.f;
           if (every) {
@@ -501,6 +503,198 @@ __global__ void __launch_bounds__(64) k_level_tiles(FpBatch bt, MgSel Sl) {
     Home H = enterTile(P, t, rec);
     int lx = o & (side - 1), ly = (o >> s) & (side - 1), lz = o >> (2 * s);
     levelCell<OP>(P, H, A, (long)t * CELLS + o, rec.x * side + lx, rec.y * side + ly, rec.z * side + lz);
+  }
+}
+
+// Staged tile levels: k_level_bricks_staged with a live tile in place of a brick. A group of 64
+// threads copies, for its tile, the values of the level it reads over the tile and a rim from
+// the tile's 27 neighbour tiles (tileNbr) into shared memory; a cell is an unknown when its
+// brick computes (the tile's mask, tileCellActive). Same arithmetic, same order as relaxCell /
+// restrictCell / prolongCell.
+//   RELAX     stage A.pin at A.level (TS = 4: the first tile level, a cell a brick)
+//   RESTRICT  stage A.pin at A.level - 1 (TS = 4); write A.pout, A.cfirst at A.level (2^3 a tile)
+//   PROLONG   stage A.coarse at A.level + 1 (TS = 2); write A.pout at A.level (4^3 a tile)
+template <int OP, int TS>
+struct TileStaged {
+  static constexpr int R = OP == PROLONG ? 2 : 1;  // prolongation's Neumann ghosts reach two
+  static constexpr int S = TS + 2 * R, S2 = S * S, S3 = S2 * S;
+  static constexpr int FS = OP == PROLONG ? 2 * TS : TS;  // the fine level's side (4: a cell a brick)
+  static constexpr int FCELLS = FS * FS * FS;
+  static constexpr int GROUP = 64, NG = 4;  // threads per tile, tiles per CTA
+  static constexpr int WORDS = S3 + (OP == PROLONG ? (S3 + 3) / 4 : 0);  // values + solid bytes
+  static constexpr size_t SMEM = (size_t)NG * WORDS * sizeof(float);
+  static_assert(FS == 4 && FCELLS == GROUP, "the fine level is the first tile level, a thread a cell");
+};
+
+template <int OP, int TS>
+__global__ void __launch_bounds__(256) k_level_tiles_staged(FpBatch bt, MgSel Sl) {
+  using K = TileStaged<OP, TS>;
+  constexpr int S = K::S, S2 = K::S2, S3 = K::S3, R = K::R, GROUP = K::GROUP, NG = K::NG, FCELLS = K::FCELLS;
+  constexpr int TS3 = TS * TS * TS;
+  __shared__ int nbrAll[NG][27];
+  extern __shared__ float stAll[];
+  const int g = threadIdx.x / GROUP, t = threadIdx.x % GROUP;
+  int* nbr = nbrAll[g];
+  float* st = stAll + g * K::WORDS;
+  uint8_t* solidSt = reinterpret_cast<uint8_t*>(st + S3);
+  const uint32_t total = workTotal(bt, FP_WORK_TILES);
+  for (uint32_t base = blockIdx.x * NG; base < total; base += gridDim.x * NG) {
+    const uint32_t item = base + g;
+    uint32_t local;
+    const SimParams& P = *workSim(bt, FP_WORK_TILES, item < total ? item : base, local).vview;
+    const Args A = resolve(P, Sl);
+    const int tile = item < total ? P.liveTiles[local] : 0;
+    const int4 rec = item < total ? __ldg(&P.tileRec[tile]) : make_int4(0, 0, 0, 0);
+    const bool has = item < total && !A.skip && rec.w != 0;
+    const int fineLevel = OP == RESTRICT ? A.level - 1 : A.level;
+    const int stageLevel = OP == PROLONG ? A.level + 1 : fineLevel;
+    const float* src = OP == PROLONG ? A.coarse : A.pin;
+    const bool srcN = OP == PROLONG ? A.coarseN : A.pinN;
+    if (has && t < 27) nbr[t] = checkTile(P, FP_SITE_TILE_NBR, __ldg(&P.tileNbr[(size_t)tile * 27 + t]));
+    __syncthreads();
+    // The stage's first cell, in cells of the staged level.
+    const int ox = rec.x * TS - R, oy = rec.y * TS - R, oz = rec.z * TS - R;
+    // This thread's fine cell (RELAX, PROLONG): its flags and right-hand side or value, loaded
+    // before the stage so that both sets of loads are in flight together.
+    const long own = (long)tile * FCELLS + t;
+    uint8_t ownTopo = 0;
+    float ownValue = 0.f;
+    if (OP != RESTRICT && has) {
+      ownTopo = P.topo[fineLevel][own];
+      ownValue = OP == RELAX ? ldBf(A.rhs, own, A.rhsN) : ldBf(A.pin, own, A.pinN);
+    }
+    bool solidStaged = false;
+    if (has) {
+      for (int q = t; q < S3; q += GROUP) {
+        const int lx = q % S, ly = (q / S) % S, lz = q / S2;
+        const int dx = lx < R ? -1 : (lx >= R + TS ? 1 : 0), dy = ly < R ? -1 : (ly >= R + TS ? 1 : 0),
+                  dz = lz < R ? -1 : (lz >= R + TS ? 1 : 0);
+        const int n = nbr[nbrIndex(dx, dy, dz)];
+        const int cx = (lx - R) & (TS - 1), cy = (ly - R) & (TS - 1), cz = (lz - R) & (TS - 1);
+        const long a = n < 0 ? -1 : (long)n * TS3 + (cz * TS + cy) * TS + cx;
+        const bool skipLoad = OP == RELAX && (!src || (A.colour != 0 && ((ox + oy + oz + lx + ly + lz) & 1) == A.colour - 1));
+        st[q] = (a < 0 || skipLoad) ? 0.f : ldBf(src, a, srcN);
+        if (OP == PROLONG) {
+          const bool solid = a >= 0 && (P.topo[stageLevel][a] & FP_STORED_SOLID);
+          solidSt[q] = solid ? 1 : 0;
+          solidStaged = solidStaged || solid;
+        }
+      }
+    }
+    bool anySolid = false;
+    if (OP == PROLONG)
+      anySolid = __syncthreads_or(solidStaged) != 0;
+    else
+      __syncthreads();
+    if (has) {
+      const uint64_t mask = P.tileMask[tile];
+      auto unknown = [&](int lx, int ly, int lz) { return ((mask >> ((lz * 4 + ly) * 4 + lx)) & 1ull) != 0ull; };
+      auto sumAt = [&](int lx, int ly, int lz, uint32_t f) {
+        int c = ((lz + 1) * S + (ly + 1)) * S + (lx + 1);
+        float v0 = (f & 1u) ? st[c + 1] : 0.f, v1 = (f & 2u) ? st[c - 1] : 0.f;
+        float v2 = (f & 4u) ? st[c + S] : 0.f, v3 = (f & 8u) ? st[c - S] : 0.f;
+        float v4 = (f & 16u) ? st[c + S2] : 0.f, v5 = (f & 32u) ? st[c - S2] : 0.f;
+        return (v0 + v1) + (v2 + v3) + (v4 + v5);
+      };
+      const int lx = t & 3, ly = (t >> 2) & 3, lz = t >> 4;
+      const int px = rec.x * 4 + lx, py = rec.y * 4 + ly, pz = rec.z * 4 + lz;
+      if (OP == RELAX) {
+        if (A.colour != 0 && parityOf(px, py, pz) != A.colour - 1) {
+          if (!src) stBf(A.pout, own, 0.f, A.poutN);  // the other colour: kept, or zero from zero
+        } else {
+          const uint32_t f = expandFlags(ownTopo);
+          if ((f & SOLIDF) || !unknown(lx, ly, lz)) {
+            stBf(A.pout, own, 0.f, A.poutN);
+          } else {
+            float cand = (sumAt(lx, ly, lz, f) - ownValue) / fmaxf(diagOf(f), 1e-12f);
+            if (A.colour != 0) {
+              stBf(A.pout, own, cand, A.poutN);  // Gauss-Seidel in place
+            } else {
+              float center = st[((lz + 1) * S + (ly + 1)) * S + (lx + 1)];
+              stBf(A.pout, own, mixf(center, cand, 0.8f), A.poutN);
+            }
+          }
+        }
+      } else if (OP == PROLONG) {
+        const uint32_t f = expandFlags(ownTopo);
+        if ((f & SOLIDF) || !unknown(lx, ly, lz)) {
+          stBf(A.pout, own, 0.f, A.poutN);
+        } else {
+          float qx = ((float)px + 0.5f) * 0.5f - 0.5f, qy = ((float)py + 0.5f) * 0.5f - 0.5f,
+                qz = ((float)pz + 0.5f) * 0.5f - 0.5f;
+          int ix = (int)floorf(qx), iy = (int)floorf(qy), iz = (int)floorf(qz);
+          float fx = qx - floorf(qx), fy = qy - floorf(qy), fz = qz - floorf(qz);
+          bool fast = (P.colliderCount == 0 || !anySolid) && (!P.ground || iy >= 0);
+          // Below the ground the mirrored ghosts read the row above it, which a tile under y = 0
+          // does not stage: those read through the directory.
+          const bool staged = !(P.ground && rec.y < 0);
+          auto at = [&](int x, int y, int z) { return ((z - oz) * S + (y - oy)) * S + (x - ox); };
+          auto ghost = [&](int cx, int cy, int cz) {
+            int groundY = P.ground ? 0 : -0x7fffffff;
+            int c[3] = {cx, max(cy, groundY), cz};
+            int ci = at(c[0], c[1], c[2]);
+            if (!solidSt[ci]) return st[ci];
+            float sum = 0.f, count = 0.f;
+            for (int axis = 0; axis < 3; axis++)
+              for (int side = -1; side <= 1; side += 2) {
+                int q[3] = {c[0], c[1], c[2]};
+                q[axis] += side;
+                q[1] = max(q[1], groundY);
+                int qi = at(q[0], q[1], q[2]);
+                if (!solidSt[qi]) {
+                  sum += st[qi];
+                  count += 1.f;
+                }
+              }
+            return sum / fmaxf(count, 1.f);
+          };
+          float v[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            int dx = q & 1, dy = (q >> 1) & 1, dz = q >> 2;
+            if (fast) {
+              v[q] = st[at(ix + dx, iy + dy, iz + dz)];
+            } else if (staged) {
+              v[q] = ghost(ix + dx, iy + dy, iz + dz);
+            } else {
+              Home H = enterTile(P, tile, rec);
+              v[q] = coarseValue(P, H, A.coarse, A.level + 1, ix + dx, iy + dy, iz + dz);
+            }
+          }
+          float corr = mixf(mixf(mixf(v[0], v[1], fx), mixf(v[2], v[3], fx), fy),
+                            mixf(mixf(v[4], v[5], fx), mixf(v[6], v[7], fx), fy), fz);
+          stBf(A.pout, own, ownValue + corr, A.poutN);
+        }
+      } else if (t < 8) {  // RESTRICT: the tile's 2^3 coarse cells at A.level
+        const int cx = t & 1, cy = (t >> 1) & 1, cz = t >> 2;
+        float residual = 0.f;
+        bool every = true;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          int fx = cx * 2 + (k & 1), fy = cy * 2 + ((k >> 1) & 1), fz = cz * 2 + (k >> 2);
+          bool u = unknown(fx, fy, fz);
+          every = every && u;
+          if (u) {
+            long a = (long)tile * FCELLS + ((fz * 4 + fy) * 4 + fx);
+            uint32_t f = expandFlags(P.topo[fineLevel][a]);
+            if (!(f & SOLIDF)) {
+              float center = st[((fz + 1) * S + (fy + 1)) * S + (fx + 1)];
+              residual += ldBf(A.rhs, a, A.rhsN) - (sumAt(fx, fy, fz, f) - diagOf(f) * center);
+            }
+          }
+        }
+        float r = residual * 0.5f;
+        const long out = (long)tile * 8 + t;
+        stBf(A.pout, out, r, A.poutN);
+        float first = 0.f;
+        if (every) {
+          uint32_t f = expandFlags(P.topo[A.level][out]);
+          if (!(f & SOLIDF)) first = mixf(0.f, (0.f - r) / fmaxf(diagOf(f), 1e-12f), 0.8f);
+        }
+        stBf(A.cfirst, out, first, A.cfirstN);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -1119,9 +1313,19 @@ __global__ void __launch_bounds__(64) k_tile_masks(FpBatch bt) {
     const SimParams& P = *workSim(bt, FP_WORK_TILES, item, local).vview;
     const int t = P.liveTiles[local];
     const size_t id = (size_t)t * 64 + threadIdx.x;
-    bool on = __ldg(&P.tileRec[t]).w != 0 && P.entries[id] >= 0 && P.records[id * FP_RECORD_WORDS + 27] != 0;
+    const bool slotted = __ldg(&P.tileRec[t]).w != 0 && P.entries[id] >= 0;
+    bool on = slotted && P.records[id * FP_RECORD_WORDS + 27] != 0;
     uint32_t half = __ballot_sync(0xffffffffu, on);
     if ((threadIdx.x & 31) == 0) reinterpret_cast<uint32_t*>(P.tileMask)[2 * t + (threadIdx.x >> 5)] = half;
+    // The first tile level's right-hand side and first iterate at a brick without a slot: the
+    // restriction into that level writes only slotted bricks' cells (no other has an unknown
+    // child, so restrictCell would write zero there).
+    if (!slotted) {
+      const int L = P.brickLevels;
+      const bool narrow = narrowLevel(P, L);
+      stBf(P.lrhs[L], (long)id, 0.f, narrow);
+      stBf(P.lp[L][1], (long)id, 0.f, narrow);
+    }
   }
 }
 
@@ -1159,6 +1363,24 @@ void fp_launch_topology(const FpBatch& bt, bool anyAll, int sms, cudaStream_t st
 }
 
 static const int BOTTOM_SMEM = 200 * 1024;
+// Resident CTAs per SM of each staged tile-level instantiation, from the occupancy calculator.
+template <int OP, int TS>
+static int& tileStagedCtas() {
+  static int n = 4;
+  return n;
+}
+template <int OP, int TS>
+static void configureTileStaged() {
+  using K = TileStaged<OP, TS>;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_level_tiles_staged<OP, TS>, 256, K::SMEM) != cudaSuccess) n = 4;
+  tileStagedCtas<OP, TS>() = n > 0 ? n : 1;
+}
+template <int OP, int TS>
+static void tileStagedLaunch(const FpBatch& bt, const MgSel& S, int sms, cudaStream_t st) {
+  k_level_tiles_staged<OP, TS><<<sms * tileStagedCtas<OP, TS>(), 256, TileStaged<OP, TS>::SMEM, st>>>(bt, S);
+}
+
 // Resident CTAs per SM of each staged instantiation, from the occupancy calculator.
 template <int OP, int SB>
 static int& stagedCtas() {
@@ -1185,11 +1407,15 @@ void fp_mg_configure(int B) {
   configureStaged<RESTRICT, 16>();
   configureStaged<RESTRICT, 8>();
   configureStaged<RESTRICT, 4>();
+  configureStaged<RESTRICT, 2>();
   configureStaged<PROLONG, 16>();
   configureStaged<PROLONG, 8>();
   configureStaged<PROLONG, 4>();
   configureStaged<PROLONG, 2>();
   configureStaged<PROLONG, 1>();
+  configureTileStaged<RELAX, 4>();
+  configureTileStaged<RESTRICT, 4>();
+  configureTileStaged<PROLONG, 2>();
   cudaFuncSetAttribute(k_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, BOTTOM_SMEM);
   cudaFuncSetAttribute(k_bottom_rb, cudaFuncAttributeMaxDynamicSharedMemorySize, BOTTOM_SMEM);
   cudaFuncSetAttribute(k_coarse, cudaFuncAttributeMaxDynamicSharedMemorySize, COARSE_SMEM);
@@ -1216,9 +1442,31 @@ static int stagedSide(int level, int B) {
 
 template <int OP>
 static void levelLaunch(const FpBatch& bt, const MgSel& S, bool tiles, int B, int sms, cudaStream_t st) {
+  if constexpr (OP == RESTRICT) {
+    // Into the first tile level: a brick's cell there restricts the brick's own 2^3 cells, staged
+    // per brick like the brick levels. Cells of bricks without a slot have no unknown child and
+    // stay zero (k_tile_masks clears them each step).
+    if (tiles && S.level == log2i(B)) {
+      stagedLaunch<OP, 2>(bt, S, sms, st);
+      return;
+    }
+  }
   if (tiles) {
-    // The tile levels hold 4^3, 2^3 and one cell a tile.
+    // The tile levels hold 4^3, 2^3 and one cell a tile. Those that read or write the first
+    // (a cell a brick) are staged per tile.
     const int below = S.level - log2i(B);
+    if (OP == RELAX && below == 0) {
+      tileStagedLaunch<RELAX, 4>(bt, S, sms, st);
+      return;
+    }
+    if (OP == RESTRICT && below == 1) {
+      tileStagedLaunch<RESTRICT, 4>(bt, S, sms, st);
+      return;
+    }
+    if (OP == PROLONG && below == 0) {
+      tileStagedLaunch<PROLONG, 2>(bt, S, sms, st);
+      return;
+    }
     if (below == 0)
       k_level_tiles<OP, 64><<<sms * 16, 64, 0, st>>>(bt, S);
     else if (below == 1)
@@ -1239,7 +1487,8 @@ static void levelLaunch(const FpBatch& bt, const MgSel& S, bool tiles, int B, in
     if (sb == 32) stagedLaunch<OP, 32>(bt, S, sms, st);
     else if (sb == 16) stagedLaunch<OP, 16>(bt, S, sms, st);
     else if (sb == 8) stagedLaunch<OP, 8>(bt, S, sms, st);
-    else stagedLaunch<OP, 4>(bt, S, sms, st);
+    else if (sb == 4) stagedLaunch<OP, 4>(bt, S, sms, st);
+    else stagedLaunch<OP, 2>(bt, S, sms, st);
   } else {
     if (sb == 16) stagedLaunch<OP, 16>(bt, S, sms, st);
     else if (sb == 8) stagedLaunch<OP, 8>(bt, S, sms, st);

@@ -754,7 +754,7 @@ FP_DEV void brick_curl(const SimParams* __restrict__ Pp, uint32_t i) {
   __syncthreads();
 }
 template <bool STAGED>
-__global__ void __launch_bounds__(THREADS) k_curl(FpBatch bt) {
+__global__ void __launch_bounds__(THREADS, 6) k_curl(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
@@ -1068,7 +1068,7 @@ FP_DEV void brick_divergence(const SimParams* __restrict__ Pp, uint32_t i, int p
   __syncthreads();
 }
 template <bool ONE>
-__global__ void __launch_bounds__(THREADS) k_divergence(FpBatch bt, int pSel) {
+__global__ void __launch_bounds__(THREADS, 6) k_divergence(FpBatch bt, int pSel) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
@@ -1418,9 +1418,9 @@ void fp_launch_evolve(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st
 }
 void fp_launch_curl(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
   if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
-    k_curl<true><<<sms * 4, THREADS, 3 * 10 * 10 * 10 * sizeof(float), st>>>(bt);
+    k_curl<true><<<sms * 6, THREADS, 3 * 10 * 10 * 10 * sizeof(float), st>>>(bt);
   else
-    k_curl<false><<<sms * 4, THREADS, 0, st>>>(bt);
+    k_curl<false><<<sms * 6, THREADS, 0, st>>>(bt);
 }
 void fp_launch_forces(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
   if (B == 8 && vd == 1) {  // staged: 8^3 bricks, one lattice
@@ -1432,9 +1432,9 @@ void fp_launch_forces(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st
 }
 void fp_launch_divergence(const FpBatch& bt, int pSel, int vd, int sms, cudaStream_t st) {
   if (vd == 1)
-    k_divergence<true><<<sms * 4, THREADS, 0, st>>>(bt, pSel);
+    k_divergence<true><<<sms * 6, THREADS, 0, st>>>(bt, pSel);
   else
-    k_divergence<false><<<sms * 4, THREADS, 0, st>>>(bt, pSel);
+    k_divergence<false><<<sms * 6, THREADS, 0, st>>>(bt, pSel);
 }
 void fp_launch_project(const FpBatch& bt, int pSel, int vd, int sms, cudaStream_t st) {
   if (vd == 1)
