@@ -819,7 +819,7 @@ FP_DEV float bfRound(float v, bool narrow) { return narrow ? __bfloat162float(__
 // prolongCell) and k_bottom; every value a level stores is rounded as its storage rounds it.
 //   A.level: level bl + 1; A.rhs its right-hand side; A.pin its first iterate; A.pout where
 //   its result goes; A.cfirst: the bottom's result (read back by the prolongation).
-constexpr int COARSE_SLOT_BYTES = 8 * 3 * 4 + 8 + 3 * 4 + 4 + 6 * 2;  // per live tile
+constexpr int COARSE_SLOT_BYTES = 8 * 3 * 4 + 8 + 3 * 4 + 4 + 6 * 2 + 27 * 2;  // per live tile
 constexpr int COARSE_SMEM = 224 * 1024;
 constexpr uint32_t LIVE = 0x80000000u;
 constexpr uint8_t UNKNOWN = 0x80;  // level bl + 1 flag byte: activeCell; bit 6 solid; 0-5 open
@@ -858,10 +858,21 @@ __global__ void __launch_bounds__(1024) k_coarse(FpBatch bt, MgSel Sl, int itera
     uint32_t* fb = reinterpret_cast<uint32_t*>(cr + nt);
     uint8_t* fl = reinterpret_cast<uint8_t*>(fb + nt);
     int16_t* faces = reinterpret_cast<int16_t*>(fl + n4);  // six a live tile
-    for (int q = threadIdx.x; q < nt * 6; q += blockDim.x) {
-      const int j = q / 6, k = q % 6;
-      const int n = checkTile(P, FP_SITE_TILE_NBR, __ldg(&P.tileNbr[P.liveTiles[j] * 27 + nbIndex[k]]));
-      faces[q] = (int16_t)(n >= 0 ? P.tileIndex[n] : -1);
+    // All 27 neighbour tiles of each live tile: the live position, -2 for a tile that is not
+    // live (its stored values are read from global memory), -1 for none.
+    int16_t* nb27 = faces + nt * 6;
+    bool solidNear = false;  // a bottom cell of a neighbour tile is solid
+    for (int q = threadIdx.x; q < nt * 27; q += blockDim.x) {
+      const int j = q / 27, k = q % 27;
+      const int n = checkTile(P, FP_SITE_TILE_NBR, __ldg(&P.tileNbr[P.liveTiles[j] * 27 + k]));
+      const int pos = n >= 0 ? P.tileIndex[n] : -1;
+      nb27[q] = (int16_t)(n < 0 ? -1 : (pos >= 0 ? pos : -2));
+      solidNear = solidNear || (n >= 0 && (P.topo[BL][n] & FP_STORED_SOLID));
+      const int dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = k / 9 - 1;
+      if ((dx != 0) + (dy != 0) + (dz != 0) == 1) {  // a face: +x, -x, +y, -y, +z, -z
+        const int f = dx != 0 ? (dx > 0 ? 0 : 1) : (dy != 0 ? (dy > 0 ? 2 : 3) : (dz > 0 ? 4 : 5));
+        faces[j * 6 + f] = (int16_t)pos;
+      }
     }
     for (int c = threadIdx.x; c < n4; c += blockDim.x) {
       const int t = P.liveTiles[c >> 3], o = c & 7;
@@ -873,7 +884,9 @@ __global__ void __launch_bounds__(1024) k_coarse(FpBatch bt, MgSel Sl, int itera
       pa[c] = ldBf(A.pin, a, nL);
       rh[c] = ldBf(A.rhs, a, nL);
     }
-    __syncthreads();
+    // Without a solid bottom cell next to any live tile every Neumann ghost of the prolongation
+    // is the bottom value itself (coarseValue's first test), read from shared memory.
+    const bool anySolid = __syncthreads_or(solidNear) != 0;
     // stencil (pressure.wgsl:360-402) of level L from `src`, cell o of live position j.
     auto sumL = [&](const float* src, int j, int o, uint32_t f) {
       float w[6];
@@ -952,6 +965,14 @@ __global__ void __launch_bounds__(1024) k_coarse(FpBatch bt, MgSel Sl, int itera
     }
     for (int j = threadIdx.x; j < nt; j += blockDim.x) stBf(A.cfirst, P.liveTiles[j], cur[j], nB);
     __syncthreads();
+    // The bottom's stored result at the bottom cell (tile) (dx,dy,dz) from live tile j (slot t):
+    // from shared memory as its storage rounds it, from global memory for a tile not live.
+    auto bottomNear = [&](int j, int t, int dx, int dy, int dz) {
+      const int k = nbrIndex(dx, dy, dz), pos = nb27[j * 27 + k];
+      if (pos >= 0) return bfRound(cur[pos], nB);
+      if (pos == -1) return 0.f;
+      return ldBf(A.cfirst, __ldg(&P.tileNbr[t * 27 + k]), nB);
+    };
     // prolongCell at level L from the bottom's stored result, pa -> pb.
     for (int c = threadIdx.x; c < n4; c += blockDim.x) {
       const int t = P.liveTiles[c >> 3], o = c & 7;
@@ -966,12 +987,18 @@ __global__ void __launch_bounds__(1024) k_coarse(FpBatch bt, MgSel Sl, int itera
         int ix = (int)floorf(qx), iy = (int)floorf(qy), iz = (int)floorf(qz);
         float fx = qx - floorf(qx), fy = qy - floorf(qy), fz = qz - floorf(qz);
         bool fast = P.colliderCount == 0 && (!P.ground || iy >= 0);
+        const int groundY = P.ground ? 0 : -0x7fffffff;
         float v[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) {
           int dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
-          v[k] = fast ? readAt(P, H, A.cfirst, ix + dx, iy + dy, iz + dz, BL)
-                      : coarseValue(P, H, A.cfirst, BL, ix + dx, iy + dy, iz + dz);
+          // The ghost's cell (coarseValue mirrors the ground), next to this tile: no solid cell
+          // there, so the ghost and the plain sample are both its value.
+          const int ox = ix + dx - rec.x, oy = max(iy + dy, groundY) - rec.y, oz = iz + dz - rec.z;
+          const bool near = ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1 && oz >= -1 && oz <= 1;
+          v[k] = (!anySolid && near) ? bottomNear(c >> 3, t, ox, oy, oz)
+                 : fast              ? readAt(P, H, A.cfirst, ix + dx, iy + dy, iz + dz, BL)
+                                     : coarseValue(P, H, A.cfirst, BL, ix + dx, iy + dy, iz + dz);
         }
         float corr = mixf(mixf(mixf(v[0], v[1], fx), mixf(v[2], v[3], fx), fy),
                           mixf(mixf(v[4], v[5], fx), mixf(v[6], v[7], fx), fy), fz);
