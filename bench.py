@@ -69,6 +69,14 @@ WORKLOAD = ("large_scene (seed 1): 3 seeded sphere/box emitters, burst at step 3
             "plain FP32 storage; 1 cold-started V-cycle (reference schedule)")
 
 
+def workload_config(gpus: int) -> dict:
+    """The `config` of both arms: what the workload is, nothing measured (the state it reached
+    is reported beside it, under `state`)."""
+    return {"workload": WORKLOAD, "grown_steps": GROW_STEPS, "budget_voxels": BUDGET, "brick_size": 8,
+            "parallelism": "replicas" if gpus > 1 else "single",
+            "l2": "working set > L2: pools of ~4k bricks x 97 KB"}
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -218,7 +226,8 @@ def run_reference(args, rank, world):
         "steps": steps, "warmup": args.warmup, "ms_per_step": statistics.mean(step_ms) if step_ms else None,
         "p50_ms": p50, "p99_ms": p99, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grown_steps": GROW_STEPS, "mean_active_bricks": bricks},
+        "config": workload_config(args.gpus),
+        "state": {"mean_active_bricks": bricks},
         "cpu_baseline": {"value": value, "unit": "voxel-steps/s", "cores": threads, "kind": "port",
                          "sample": f"oracle FP32 restatement of the step on {threads} threads: the large scene grown "
                                    f"{GROW_STEPS} + {args.warmup} steps untimed, then {steps} timed steps "
@@ -603,10 +612,18 @@ def default_grid_form(local: int, steps: int = 20) -> dict:
     ev[1].record(stream)
     sim.synchronize()
     ms = ev[0].elapsed_time(ev[1]) / steps
+    # per-phase device time of 10 more steps (fp_sim_set_profiling)
+    sim.set_profiling(True)
+    for _ in range(10):
+        sim.step(sc.frame(step).frame)
+        step += 1
+    prof = sim.profile()
+    sim.set_profiling(False)
     out = {"workload": f"large_scene (seed 1) on 16^3 bricks, velocity divisor 2, smoke divisor 2, 2.5 cm voxels, "
                        f"budget 2^24 voxels; grown {GROW_STEPS} steps, {steps} timed; plain FP32, reference V-cycle",
            "mean_active_bricks": sum(actives) / len(actives), "ms_per_step": ms,
-           "value": sum(actives) * 16 ** 3 / (ms * steps / 1e3), "unit": "voxel-steps/s"}
+           "value": sum(actives) * 16 ** 3 / (ms * steps / 1e3), "unit": "voxel-steps/s",
+           "phases_ms_per_step": {name: t / 10 for name, (n, t, _) in prof.items() if n}}
     sim.dispose()
     return out
 
@@ -765,11 +782,9 @@ def run_ours(args, rank, world, local):
         "metric": "voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "p50_ms": p50, "p99_ms": p99,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD,
-                   "mean_active_bricks": sum(actives) / len(actives), "grown_steps": GROW_STEPS,
-                   "live_tiles": int(st.tiles), "tile_capacity": int(st.tile_capacity),
-                   "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "working set > L2: pools of ~4k bricks x 97 KB"},
+        "config": workload_config(world),
+        "state": {"mean_active_bricks": sum(actives) / len(actives), "live_tiles": int(st.tiles),
+                  "tile_capacity": int(st.tile_capacity)},
         "roofline": roofline,
         "e2e": {"value": e2e_vox / e2e_s, "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
