@@ -362,9 +362,9 @@ __device__ bool insideCollider(const SimParams& P, const FpCollider& c, int x, i
   return r < 1.f;
 }
 
-// buildSolids: a CTA per brick, a word of 32 cells per thread. ALL: every slotted brick of
-// the simulations whose colliders changed; otherwise the slots granted this step in the
-// simulations that have colliders.
+// buildSolids: a CTA per brick, a warp per word of 32 cells, a lane per cell (the word is the
+// warp's ballot). ALL: every slotted brick of the simulations whose colliders changed;
+// otherwise the slots granted this step in the simulations that have colliders.
 template <bool ALL>
 __global__ void __launch_bounds__(128) k_build_solids(FpBatch bt) {
   const int kind = ALL ? FP_WORK_IDS : FP_WORK_FRESH;
@@ -388,19 +388,16 @@ __global__ void __launch_bounds__(128) k_build_solids(FpBatch bt) {
     int l = id & 63;
     int bx = rec.x * 4 + (l & 3), by = rec.y * 4 + ((l >> 2) & 3), bz = rec.z * 4 + (l >> 4);
     uint2 list = tileList(P, tile, 2);
-    for (int word = threadIdx.x; word < P.W; word += blockDim.x) {
-      uint32_t bits = 0;
-      for (int k = 0; k < 32; k++) {
-        int bit = word * 32 + k;
-        int x = bx * P.B + (bit & (P.B - 1)), y = by * P.B + ((bit >> P.shift) & (P.B - 1)),
-            z = bz * P.B + (bit >> (2 * P.shift));
-        for (uint32_t j = 0; j < list.y; j++)
-          if (insideCollider(P, P.colliders[P.tileLists[list.x + j]], x, y, z)) {
-            bits |= 1u << k;
-            break;
-          }
-      }
-      P.solids[(size_t)slot * P.W + word] = bits;
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    for (int word = threadIdx.x >> 5; word < P.W; word += warps) {
+      const int bit = word * 32 + lane;
+      const int x = bx * P.B + (bit & (P.B - 1)), y = by * P.B + ((bit >> P.shift) & (P.B - 1)),
+                z = bz * P.B + (bit >> (2 * P.shift));
+      bool inside = false;
+      for (uint32_t j = 0; j < list.y && !inside; j++)
+        inside = insideCollider(P, P.colliders[P.tileLists[list.x + j]], x, y, z);
+      const uint32_t bits = __ballot_sync(0xffffffffu, inside);
+      if (lane == 0) P.solids[(size_t)slot * P.W + word] = bits;
     }
   }
 }
@@ -444,8 +441,18 @@ __global__ void __launch_bounds__(256) k_readback(FpBatch bt) {
     const uint32_t* counters = reinterpret_cast<const uint32_t*>(P.counters);
     const uint32_t* solver = reinterpret_cast<const uint32_t*>(P.solver);
     const uint32_t* tiles = P.activity + (size_t)P.capacity * 64;
-    for (int k = threadIdx.x; k < cw + sw + P.capacity; k += blockDim.x)
-      P.readback[k] = k < cw ? counters[k] : (k < cw + sw ? solver[k - cw] : tiles[k - cw - sw]);
+    for (int k = threadIdx.x; k < cw + sw; k += blockDim.x) P.readback[k] = k < cw ? counters[k] : solver[k - cw];
+    // The tile words, four a store where the host-mapped words allow it (a few transactions over
+    // the bus rather than one a word).
+    uint32_t* out = P.readback + cw + sw;
+    const int n = P.capacity;
+    if ((reinterpret_cast<uintptr_t>(out) & 15u) == 0 && (reinterpret_cast<uintptr_t>(tiles) & 15u) == 0) {
+      for (int k = threadIdx.x; k < n / 4; k += blockDim.x)
+        reinterpret_cast<uint4*>(out)[k] = reinterpret_cast<const uint4*>(tiles)[k];
+      for (int k = (n / 4) * 4 + threadIdx.x; k < n; k += blockDim.x) out[k] = tiles[k];
+    } else {
+      for (int k = threadIdx.x; k < n; k += blockDim.x) out[k] = tiles[k];
+    }
     __syncthreads();
     if (threadIdx.x == 0) P.counters->failures = 0;
     uint32_t* clear = reinterpret_cast<uint32_t*>(P.solver);

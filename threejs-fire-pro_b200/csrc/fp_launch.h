@@ -21,7 +21,7 @@ void fp_launch_curl(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st);
 void fp_launch_forces(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st);
 // Divergence with the finest level's first iterate into p0[pSel]; projection with p0[pSel].
 void fp_launch_divergence(const FpBatch& bt, int pSel, int vd, int sms, cudaStream_t st);
-void fp_launch_project(const FpBatch& bt, int pSel, int B, int vd, int sms, cudaStream_t st);
+void fp_launch_project(const FpBatch& bt, int pSel, int vd, int sms, cudaStream_t st);
 void fp_launch_noise(float4* noise, cudaStream_t st);
 
 // Multigrid (pressure.wgsl). Levels below the brick levels live in brick slots, the rest in

@@ -1078,12 +1078,7 @@ __global__ void __launch_bounds__(THREADS, 6) k_divergence(FpBatch bt, int pSel)
 }
 
 // project (fluid-forces.wgsl:228-262) into the velocity pool of the next step.
-// Staged (8^3 bricks, one lattice): the pressure, whether each cell is a pressure unknown and
-// whether it is solid, over the brick and one cell beyond its upper faces (every cell the
-// brick's gradients read), evaluated once a cell into shared memory; same tests, same
-// arithmetic as the unstaged form.
-constexpr int PROJ_SIDE = 9, PROJ_CELLS = PROJ_SIDE * PROJ_SIDE * PROJ_SIDE;
-template <bool ONE, bool STAGED>
+template <bool ONE>
 FP_DEV void brick_project(const SimParams* __restrict__ Pp, uint32_t i, int pSel) {
   __shared__ int nslot[27];
   const SimParams& P = *Pp;
@@ -1092,41 +1087,6 @@ FP_DEV void brick_project(const SimParams* __restrict__ Pp, uint32_t i, int pSel
   Home H = enterBrick(P, P.active[i], nslot);
   size_t slot = (size_t)nslot[13];
   const size_t N = P.N;
-  if constexpr (STAGED) {
-    __shared__ float sp[PROJ_CELLS];
-    __shared__ uint8_t sflag[PROJ_CELLS];  // bit 0: pressure unknown, bit 1: solid
-    for (int q = threadIdx.x; q < PROJ_CELLS; q += blockDim.x) {
-      const int x = H.bx * 8 + q % PROJ_SIDE, y = H.by * 8 + (q / PROJ_SIDE) % PROJ_SIDE,
-                z = H.bz * 8 + q / (PROJ_SIDE * PROJ_SIDE);
-      sp[q] = cellAt(P, H, p, 1, 0, x, y, z);
-      sflag[q] = (uint8_t)((pressureUnknown(P, H, x, y, z) ? 1 : 0) | (solidCell<true>(P, H, x, y, z) ? 2 : 0));
-    }
-    __syncthreads();
-    for (int c = threadIdx.x; c < 512; c += blockDim.x) {
-      const int q = ((c >> 6) * PROJ_SIDE + ((c >> 3) & 7)) * PROJ_SIDE + (c & 7);
-      float res[3] = {0.f, 0.f, 0.f};
-      const uint8_t f = sflag[q];
-      if (!(f & 2)) {
-        const float cp = sp[q];
-        const bool pu = (f & 1) != 0;
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-          const int qn = q + (a == 0 ? 1 : (a == 1 ? PROJ_SIDE : PROJ_SIDE * PROJ_SIDE));
-          const uint8_t fn = sflag[qn];
-          const float v = P.velF[(slot * 3 + a) * N + c];
-          if (fn & 2)
-            res[a] = 0.f;
-          else if (!pu && !(fn & 1))
-            res[a] = 0.f;
-          else
-            res[a] = v - (sp[qn] - cp) / P.h;
-        }
-      }
-      for (int a = 0; a < 3; a++) P.velP[(slot * 3 + a) * N + c] = res[a];
-    }
-    __syncthreads();
-    return;
-  }
   for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
     int x, y, z;
     cellOf(P, H, c, x, y, z);
@@ -1152,13 +1112,13 @@ FP_DEV void brick_project(const SimParams* __restrict__ Pp, uint32_t i, int pSel
   }
   __syncthreads();
 }
-template <bool ONE, bool STAGED>
+template <bool ONE>
 __global__ void __launch_bounds__(THREADS) k_project(FpBatch bt, int pSel) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_project<ONE, STAGED>(ONE ? &P : P.vview, i, pSel);  // the velocity lattice
+    brick_project<ONE>(ONE ? &P : P.vview, i, pSel);  // the velocity lattice
   }
 }
 
@@ -1476,13 +1436,11 @@ void fp_launch_divergence(const FpBatch& bt, int pSel, int vd, int sms, cudaStre
   else
     k_divergence<false><<<sms * 6, THREADS, 0, st>>>(bt, pSel);
 }
-void fp_launch_project(const FpBatch& bt, int pSel, int B, int vd, int sms, cudaStream_t st) {
-  if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
-    k_project<true, true><<<sms * 4, THREADS, 0, st>>>(bt, pSel);
-  else if (vd == 1)
-    k_project<true, false><<<sms * 4, THREADS, 0, st>>>(bt, pSel);
+void fp_launch_project(const FpBatch& bt, int pSel, int vd, int sms, cudaStream_t st) {
+  if (vd == 1)
+    k_project<true><<<sms * 4, THREADS, 0, st>>>(bt, pSel);
   else
-    k_project<false, false><<<sms * 4, THREADS, 0, st>>>(bt, pSel);
+    k_project<false><<<sms * 4, THREADS, 0, st>>>(bt, pSel);
 }
 void fp_launch_noise(float4* noise, cudaStream_t st) { k_noise<<<64 * 64 * 64 / 256, 256, 0, st>>>(noise); }
 void fp_launch_post_divergence(const FpBatch& bt, int sms, cudaStream_t st) {

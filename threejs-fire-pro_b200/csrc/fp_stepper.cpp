@@ -559,7 +559,7 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   launches += mg;
   phaseEnd(PH_MULTIGRID, (int)mg);
   phaseBegin(PH_PROJECT);
-  fp_launch_project(bt, latest, B_, vd_, sms_, stream_);
+  fp_launch_project(bt, latest, vd_, sms_, stream_);
   launches++;
   if (measure) {
     fp_launch_post_divergence(bt, sms_, stream_);
