@@ -315,14 +315,15 @@ FP_DEV void predictVelocity(const SimParams& P, const Home& H, const Stage<SS>& 
 }
 // advectScalars (fluid-scalar-transport.wgsl:38-142) at field cell (x,y,z), offset c of its
 // brick's slot: P the field lattice, VP the velocity lattice the trace samples.
-template <int SS>
-FP_DEV void predictScalars(const SimParams& P, const SimParams& VP, const Home& H, const Stage<SS>& G, const Field& V,
-                           const Field& F, size_t slot, int c, int x, int y, int z) {
+// GV: the stage of the velocity (on VP's lattice), GF: the stage of the scalars (on P's).
+template <int SV, int SF>
+FP_DEV void predictScalars(const SimParams& P, const SimParams& VP, const Home& H, const Stage<SV>& GV, const Field& V,
+                           const Stage<SF>& GF, const Field& F, size_t slot, int c, int x, int y, int z) {
   const size_t N = P.N;
   // Scalars: a cell-centred RK2 back trace, the predictor and its donors' range.
   const float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-  float3 cv = VP.velDiv == 1 ? centreVelocity(VP, H, G, V, x, y, z) : velocityAt(VP, H, G, V, px, py, pz);
-  float3 vm = velocityAt(VP, H, G, V, px - 0.5f * P.dt * cv.x, py - 0.5f * P.dt * cv.y, pz - 0.5f * P.dt * cv.z);
+  float3 cv = VP.velDiv == 1 ? centreVelocity(VP, H, GV, V, x, y, z) : velocityAt(VP, H, GV, V, px, py, pz);
+  float3 vm = velocityAt(VP, H, GV, V, px - 0.5f * P.dt * cv.x, py - 0.5f * P.dt * cv.y, pz - 0.5f * P.dt * cv.z);
   float dx_ = px - P.dt * vm.x, dy_ = py - P.dt * vm.y, dz_ = pz - P.dt * vm.z;
   // The departure's trilinear block in cell units: corner `base`, fractions `fr`.
   const float dc[3] = {(float)x + (dx_ - px) * P.invH, (float)y + (dy_ - py) * P.invH,
@@ -335,13 +336,13 @@ FP_DEV void predictScalars(const SimParams& P, const SimParams& VP, const Home& 
     base[a] = (int)g;
     fr[a] = dc[a] - g;
   }
-  const float* blk = stagedBlock(G, F, base[0], base[1], base[2]);
+  const float* blk = stagedBlock(GF, F, base[0], base[1], base[2]);
   float out[4];
   float* sb = P.sb + slot * 8 * N;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     float t[8];
-    blockCells(P, H, G, F, k, blk, base[0], base[1], base[2], t);
+    blockCells(P, H, GF, F, k, blk, base[0], base[1], base[2], t);
     out[k] = blend8(t, fr[0], fr[1], fr[2]);
     if (P.maccormack) {
       // The donors' range; FP16-finite for smoke, heat and fuel, [0,1]-anchored for lifetime.
@@ -366,7 +367,32 @@ FP_DEV void predictScalars(const SimParams& P, const SimParams& VP, const Home& 
   for (int k = 0; k < 4; k++) P.fldP[(slot * 4 + k) * N + c] = out[k];
 }
 
-template <bool STAGED>
+// Transport kernels' forms. 0: unstaged (any grid). 1: staged, 8^3 bricks on one lattice.
+// 2: staged, a velocity lattice of 8^3 cells a brick under a finer field lattice (velocity
+// divisor d > 1 with 8 d field cells a brick side): the velocity is staged once over the brick
+// and a HALO-cell rim on its own lattice, the scalars per cube of 8^3 field cells and a HALO rim.
+constexpr int CUBE = 8;
+template <int SS>
+FP_DEV Stage<SS> stageAt(int ox, int oy, int oz) {
+  Stage<SS> G;
+  G.ox = ox;
+  G.oy = oy;
+  G.oz = oz;
+  return G;
+}
+// The velocity stage of form 2: the brick on the velocity lattice VP and a HALO rim.
+FP_DEV TransportStage<true> velocityStage(const SimParams& VP, const Home& H) {
+  return stageAt<8 + 2 * HALO>(H.bx * VP.B - HALO, H.by * VP.B - HALO, H.bz * VP.B - HALO);
+}
+// The cubes of 8^3 field cells of a brick of B field cells a side: cube k's first cell in the brick.
+FP_DEV void cubeOrigin(int B, int k, int& ox, int& oy, int& oz) {
+  const int per = B / CUBE;
+  ox = (k % per) * CUBE;
+  oy = ((k / per) % per) * CUBE;
+  oz = k / (per * per) * CUBE;
+}
+
+template <int MODE>
 FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
   extern __shared__ float smem[];
@@ -374,51 +400,82 @@ FP_DEV void brick_predict(const SimParams* __restrict__ Pp, uint32_t i) {
   uint32_t id = P.active[i];
   if (!homeOk(P, id)) return;  // the bounds-checked build only
   Home H = enterBrick(P, id, nslot);
-  TransportStage<STAGED> G = stageOf<STAGED>(P, H);
-  Field V{P.vel, 3, STAGED ? smem : nullptr};
-  Field F{P.fld, 4, STAGED ? smem + 3 * G.S3 : nullptr, P.scalarHalf != 0};
-  if (STAGED) {
-    stageField(P, H, G, smem, P.vel, 3);
-    stageField(P, H, G, smem + 3 * G.S3, P.fld, 4, F.half);
-    stageWait();
-  }
   size_t slot = (size_t)nslot[13];
-  if (STAGED || P.velDiv == 1) {
-    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
-      int x, y, z;
-      cellOf(P, H, c, x, y, z);
-      predictVelocity(P, H, G, V, slot, c, x, y, z);
-      predictScalars(P, P, H, G, V, F, slot, c, x, y, z);
-    }
-  } else {
-    // The velocity lattice's cells, then the field lattice's.
+  if constexpr (MODE == 2) {
     const SimParams& VP = *P.vview;
+    const TransportStage<true> GV = velocityStage(VP, H);
+    Field V{P.vel, 3, smem};
+    Field F{P.fld, 4, smem + 3 * GV.S3, P.scalarHalf != 0};
+    stageField(VP, H, GV, smem, P.vel, 3);
+    stageWait();
     for (int c = threadIdx.x; c < VP.N; c += blockDim.x) {
       int x, y, z;
       cellOf(VP, H, c, x, y, z);
-      predictVelocity(VP, H, G, V, slot, c, x, y, z);
+      predictVelocity(VP, H, GV, V, slot, c, x, y, z);
     }
-    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
-      int x, y, z;
-      cellOf(P, H, c, x, y, z);
-      predictScalars(P, VP, H, G, V, F, slot, c, x, y, z);
+    const int cubes = (P.B / CUBE) * (P.B / CUBE) * (P.B / CUBE);
+    for (int k = 0; k < cubes; k++) {
+      int ox, oy, oz;
+      cubeOrigin(P.B, k, ox, oy, oz);
+      const TransportStage<true> GF =
+          stageAt<8 + 2 * HALO>(H.bx * P.B + ox - HALO, H.by * P.B + oy - HALO, H.bz * P.B + oz - HALO);
+      __syncthreads();  // the previous cube's stage has been read
+      stageField(P, H, GF, smem + 3 * GV.S3, P.fld, 4, F.half);
+      stageWait();
+      for (int q = threadIdx.x; q < CUBE * CUBE * CUBE; q += blockDim.x) {
+        const int lx = ox + (q & 7), ly = oy + ((q >> 3) & 7), lz = oz + (q >> 6);
+        predictScalars(P, VP, H, GV, V, GF, F, slot, (lz * P.B + ly) * P.B + lx, H.bx * P.B + lx, H.by * P.B + ly,
+                       H.bz * P.B + lz);
+      }
+    }
+  } else {
+    constexpr bool STAGED = MODE == 1;
+    TransportStage<STAGED> G = stageOf<STAGED>(P, H);
+    Field V{P.vel, 3, STAGED ? smem : nullptr};
+    Field F{P.fld, 4, STAGED ? smem + 3 * G.S3 : nullptr, P.scalarHalf != 0};
+    if (STAGED) {
+      stageField(P, H, G, smem, P.vel, 3);
+      stageField(P, H, G, smem + 3 * G.S3, P.fld, 4, F.half);
+      stageWait();
+    }
+    if (STAGED || P.velDiv == 1) {
+      for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+        int x, y, z;
+        cellOf(P, H, c, x, y, z);
+        predictVelocity(P, H, G, V, slot, c, x, y, z);
+        predictScalars(P, P, H, G, V, G, F, slot, c, x, y, z);
+      }
+    } else {
+      // The velocity lattice's cells, then the field lattice's.
+      const SimParams& VP = *P.vview;
+      for (int c = threadIdx.x; c < VP.N; c += blockDim.x) {
+        int x, y, z;
+        cellOf(VP, H, c, x, y, z);
+        predictVelocity(VP, H, G, V, slot, c, x, y, z);
+      }
+      for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+        int x, y, z;
+        cellOf(P, H, c, x, y, z);
+        predictScalars(P, VP, H, G, V, G, F, slot, c, x, y, z);
+      }
     }
   }
   __syncthreads();
 }
-template <bool STAGED>
+template <int MODE>
 __global__ void __launch_bounds__(THREADS, FP_TRANSPORT_CTAS) k_predict(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_predict<STAGED>(&P, i);
+    brick_predict<MODE>(&P, i);
   }
 }
 
 // ---------------------------------------------------------------------------------------
 // correctVelocity (fluid-velocity-transport.wgsl:104-179): bounded MacCormack correction.
-template <bool STAGED>
+// ONE: the velocity lattice is the field lattice (velocity divisor 1), known at compile time.
+template <bool STAGED, bool ONE>
 FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
   extern __shared__ float smem[];
@@ -440,7 +497,7 @@ FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
     int x, y, z;
     cellOf(P, H, c, x, y, z);
     float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-    bool solid = solidCell<STAGED>(P, H, x, y, z);  // solidAt at the cell centre
+    bool solid = solidCell<ONE>(P, H, x, y, z);  // solidAt at the cell centre
     float3 orig = make_float3(nearCell(P, H, G, V, 0, x, y, z), nearCell(P, H, G, V, 1, x, y, z),
                               nearCell(P, H, G, V, 2, x, y, z));
 #pragma unroll
@@ -497,20 +554,21 @@ FP_DEV void brick_correct(const SimParams* __restrict__ Pp, uint32_t i) {
   }
   __syncthreads();
 }
-template <bool STAGED>
+template <int MODE>
 __global__ void __launch_bounds__(THREADS, FP_TRANSPORT_CTAS) k_correct(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_correct<STAGED>(STAGED ? &P : P.vview, i);  // the velocity lattice (staged: the only one)
+    // the velocity lattice, 8^3 cells a brick in the staged forms
+    brick_correct<MODE != 0, MODE == 1>(MODE == 1 ? &P : P.vview, i);
   }
 }
 
 // ---------------------------------------------------------------------------------------
 // evolveFields (fluid-field-evolution.wgsl:9-84) with correctedScalars
 // (fluid-scalar-transport.wgsl:144-199) and recordContent (fluid-content.wgsl:29-64).
-template <bool STAGED>
+template <int MODE>
 FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
   __shared__ uint32_t busyAll, expandsAll;
@@ -523,161 +581,185 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
   }
   if (!homeOk(P, id)) return;  // the bounds-checked build only
   Home H = enterBrick(P, id, nslot);
-  TransportStage<STAGED> G = stageOf<STAGED>(P, H);
-  const SimParams& VP = STAGED ? P : *P.vview;  // the velocity lattice the traces sample
+  constexpr bool STAGED = MODE != 0;
+  const SimParams& VP = MODE == 1 ? P : *P.vview;  // the velocity lattice the traces sample
   Field V{P.vel, 3, STAGED ? smem : nullptr};
-  Field Fp{P.fldP, 4, STAGED ? smem + 3 * G.S3 : nullptr, false};  // the predictor: FP32
-  const bool half = P.scalarHalf != 0;                             // the state pools
-  if (STAGED) {
-    stageField(P, H, G, smem, P.vel, 3);
-    stageField(P, H, G, smem + 3 * G.S3, P.fldP, 4);
-    stageWait();
-  }
+  Field Fp{P.fldP, 4, STAGED ? smem + 3 * TransportStage<true>::S3 : nullptr, false};  // the predictor: FP32
+  const bool half = P.scalarHalf != 0;  // the state pools
   size_t slot = (size_t)nslot[13];
   const size_t N = P.N;
   int tile = (int)(id >> 6);
   uint32_t busy = 0;
   bool expands = false;
-  for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
-    int x, y, z;
-    cellOf(P, H, c, x, y, z);
-    float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
-    bool solid = solidCell<STAGED>(P, H, x, y, z);  // solidAt at the cell centre
-    float value[4] = {0.f, 0.f, 0.f, 0.f};
-    float expansion = 0.f;
-    bool injected = false;
-    bool cvSampled = false;
-    float3 cv = make_float3(0.f, 0.f, 0.f);
-    if (!solid) {
-      float tr[4];
-      if (!P.maccormack) {
-        for (int k = 0; k < 4; k++) tr[k] = nearCell(P, H, G, Fp, k, x, y, z);
-      } else {
-        const float* b = P.sb + slot * 8 * N;
-        float mn0 = b[0 * N + c], mn1 = b[1 * N + c], mn3 = b[2 * N + c], lmin = b[3 * N + c];
-        float mx0 = b[4 * N + c], mx1 = b[5 * N + c], mx3 = b[6 * N + c], lmax = b[7 * N + c];
-        if (mn0 == mx0 && mn1 == mx1 && mn3 == mx3 && lmin == lmax) {
-          tr[0] = mn0;
-          tr[1] = mn1;
-          tr[2] = clamp01(lmin);
-          tr[3] = mn3;
+  // One field cell (x,y,z), offset c of the brick's slot; GV stages the velocity, GF the predictor.
+  auto cell = [&](const auto& GV, const auto& GF, int c, int x, int y, int z) {
+      float px = ((float)x + 0.5f) * P.h, py = ((float)y + 0.5f) * P.h, pz = ((float)z + 0.5f) * P.h;
+      bool solid = solidCell<MODE == 1>(P, H, x, y, z);  // solidAt at the cell centre
+      float value[4] = {0.f, 0.f, 0.f, 0.f};
+      float expansion = 0.f;
+      bool injected = false;
+      bool cvSampled = false;
+      float3 cv = make_float3(0.f, 0.f, 0.f);
+      if (!solid) {
+        float tr[4];
+        if (!P.maccormack) {
+          for (int k = 0; k < 4; k++) tr[k] = nearCell(P, H, GF, Fp, k, x, y, z);
         } else {
-          float a0 = nearCell(P, H, G, Fp, 0, x, y, z), a1 = nearCell(P, H, G, Fp, 1, x, y, z),
-                a2 = nearCell(P, H, G, Fp, 2, x, y, z), a3 = nearCell(P, H, G, Fp, 3, x, y, z);
-          cv = VP.velDiv == 1 ? centreVelocity(VP, H, G, V, x, y, z) : velocityAt(VP, H, G, V, px, py, pz);
-          cvSampled = true;
-          float3 vm = velocityAt(VP, H, G, V, px + 0.5f * P.dt * cv.x, py + 0.5f * P.dt * cv.y, pz + 0.5f * P.dt * cv.z);
-          float fx = px + P.dt * vm.x, fy = py + P.dt * vm.y, fz = pz + P.dt * vm.z;
-          const size_t o = slot * 4 * N + c;
-          float o0 = ldHalf(P.fld, o, half), o1 = ldHalf(P.fld, o + N, half), o2 = ldHalf(P.fld, o + 2 * N, half),
-                o3 = ldHalf(P.fld, o + 3 * N, half);
-          // The forward trace's trilinear block of the predictor, in cell units.
-          const float fc[3] = {(float)x + (fx - px) * P.invH, (float)y + (fy - py) * P.invH,
-                               (float)z + (fz - pz) * P.invH};
-          int base[3];
-          float fr[3];
-#pragma unroll
-          for (int a = 0; a < 3; a++) {
-            float g = floorf(fc[a]);
-            base[a] = (int)g;
-            fr[a] = fc[a] - g;
+          const float* b = P.sb + slot * 8 * N;
+          float mn0 = b[0 * N + c], mn1 = b[1 * N + c], mn3 = b[2 * N + c], lmin = b[3 * N + c];
+          float mx0 = b[4 * N + c], mx1 = b[5 * N + c], mx3 = b[6 * N + c], lmax = b[7 * N + c];
+          if (mn0 == mx0 && mn1 == mx1 && mn3 == mx3 && lmin == lmax) {
+            tr[0] = mn0;
+            tr[1] = mn1;
+            tr[2] = clamp01(lmin);
+            tr[3] = mn3;
+          } else {
+            float a0 = nearCell(P, H, GF, Fp, 0, x, y, z), a1 = nearCell(P, H, GF, Fp, 1, x, y, z),
+                  a2 = nearCell(P, H, GF, Fp, 2, x, y, z), a3 = nearCell(P, H, GF, Fp, 3, x, y, z);
+            cv = VP.velDiv == 1 ? centreVelocity(VP, H, GV, V, x, y, z) : velocityAt(VP, H, GV, V, px, py, pz);
+            cvSampled = true;
+            float3 vm = velocityAt(VP, H, GV, V, px + 0.5f * P.dt * cv.x, py + 0.5f * P.dt * cv.y, pz + 0.5f * P.dt * cv.z);
+            float fx = px + P.dt * vm.x, fy = py + P.dt * vm.y, fz = pz + P.dt * vm.z;
+            const size_t o = slot * 4 * N + c;
+            float o0 = ldHalf(P.fld, o, half), o1 = ldHalf(P.fld, o + N, half), o2 = ldHalf(P.fld, o + 2 * N, half),
+                  o3 = ldHalf(P.fld, o + 3 * N, half);
+            // The forward trace's trilinear block of the predictor, in cell units.
+            const float fc[3] = {(float)x + (fx - px) * P.invH, (float)y + (fy - py) * P.invH,
+                                 (float)z + (fz - pz) * P.invH};
+            int base[3];
+            float fr[3];
+  #pragma unroll
+            for (int a = 0; a < 3; a++) {
+              float g = floorf(fc[a]);
+              base[a] = (int)g;
+              fr[a] = fc[a] - g;
+            }
+            const float* blk = stagedBlock(GF, Fp, base[0], base[1], base[2]);
+            float rs[4];
+  #pragma unroll
+            for (int k = 0; k < 4; k++) {
+              float t[8];
+              blockCells(P, H, GF, Fp, k, blk, base[0], base[1], base[2], t);
+              rs[k] = blend8(t, fr[0], fr[1], fr[2]);
+            }
+            float r0 = rs[0], r1 = rs[1], r3 = rs[3];
+            float lifetime = a2;
+            if (lmin != lmax || a2 != lmin) {
+              float cl = a2 + 0.5f * (o2 - rs[2]);
+              lifetime = (cl < lmin || cl > lmax) ? a2 : cl;
+            }
+            float c0 = a0 + 0.5f * (o0 - r0), c1 = a1 + 0.5f * (o1 - r1), c3 = a3 + 0.5f * (o3 - r3);
+            tr[0] = (c0 < mn0 || c0 > mx0) ? a0 : c0;
+            tr[1] = (c1 < mn1 || c1 > mx1) ? a1 : c1;
+            tr[2] = clamp01(lifetime);
+            tr[3] = (c3 < mn3 || c3 > mx3) ? a3 : c3;
           }
-          const float* blk = stagedBlock(G, Fp, base[0], base[1], base[2]);
-          float rs[4];
-#pragma unroll
-          for (int k = 0; k < 4; k++) {
-            float t[8];
-            blockCells(P, H, G, Fp, k, blk, base[0], base[1], base[2], t);
-            rs[k] = blend8(t, fr[0], fr[1], fr[2]);
-          }
-          float r0 = rs[0], r1 = rs[1], r3 = rs[3];
-          float lifetime = a2;
-          if (lmin != lmax || a2 != lmin) {
-            float cl = a2 + 0.5f * (o2 - rs[2]);
-            lifetime = (cl < lmin || cl > lmax) ? a2 : cl;
-          }
-          float c0 = a0 + 0.5f * (o0 - r0), c1 = a1 + 0.5f * (o1 - r1), c3 = a3 + 0.5f * (o3 - r3);
-          tr[0] = (c0 < mn0 || c0 > mx0) ? a0 : c0;
-          tr[1] = (c1 < mn1 || c1 > mx1) ? a1 : c1;
-          tr[2] = clamp01(lifetime);
-          tr[3] = (c3 < mn3 || c3 > mx3) ? a3 : c3;
         }
-      }
-      // With coarse smoke the fine smoke channel stages only this step's source production
-      // (fluid-scalar-transport.wgsl:190-199).
-      if (P.smokeDiv > 1) tr[0] = 0.f;
-      float lifetime = tr[2];
-      float prodS = 0.f, prodH = 0.f, injectedFuel = 0.f;
-      uint2 list = tileList(P, tile, 0);
-      for (uint32_t j = 0; j < list.y; j++) {
-        const FpEmitter& e = P.emitters[P.tileLists[list.x + j]];
-        float w = emitterWeight(e, px, py, pz);
-        if (w == 0.f) continue;
-        float2 var = burstVariation(e, px, py, pz, P.seedBits);
-        lifetime = fmaxf(lifetime, e.flame * w * var.y);
-        prodS += e.smoke * w * P.dt;
-        prodH += e.heat * var.x * w * P.dt;
-        injectedFuel += e.fuel * w * P.dt;
-      }
-      // Mesh emission at this cell (fluid-field-evolution.wgsl:33-36).
-      if (const FpMeshSource* ms = meshSourceAt(P, H, x, y, z)) {
-        lifetime = fmaxf(lifetime, ms->scalar[0]);
-        prodS += ms->scalar[2] * P.dt;
-        prodH += ms->scalar[1] * P.dt;
-        injectedFuel += ms->scalar[3] * P.dt;
-      }
-      float remaining = 0.f, burned = 0.f;
-      if (P.fuelEnabled) {
-        remaining = tr[3] + injectedFuel;
-        if (tr[1] + prodH >= P.ignition) {
-          lifetime = fmaxf(lifetime, fminf(remaining, 1.f));
-          float unburned = remaining * expf(-P.burnRate * P.dt);
-          burned = remaining - unburned;
-          remaining = unburned;
+        // With coarse smoke the fine smoke channel stages only this step's source production
+        // (fluid-scalar-transport.wgsl:190-199).
+        if (P.smokeDiv > 1) tr[0] = 0.f;
+        float lifetime = tr[2];
+        float prodS = 0.f, prodH = 0.f, injectedFuel = 0.f;
+        uint2 list = tileList(P, tile, 0);
+        for (uint32_t j = 0; j < list.y; j++) {
+          const FpEmitter& e = P.emitters[P.tileLists[list.x + j]];
+          float w = emitterWeight(e, px, py, pz);
+          if (w == 0.f) continue;
+          float2 var = burstVariation(e, px, py, pz, P.seedBits);
+          lifetime = fmaxf(lifetime, e.flame * w * var.y);
+          prodS += e.smoke * w * P.dt;
+          prodH += e.heat * var.x * w * P.dt;
+          injectedFuel += e.fuel * w * P.dt;
         }
+        // Mesh emission at this cell (fluid-field-evolution.wgsl:33-36).
+        if (const FpMeshSource* ms = meshSourceAt(P, H, x, y, z)) {
+          lifetime = fmaxf(lifetime, ms->scalar[0]);
+          prodS += ms->scalar[2] * P.dt;
+          prodH += ms->scalar[1] * P.dt;
+          injectedFuel += ms->scalar[3] * P.dt;
+        }
+        float remaining = 0.f, burned = 0.f;
+        if (P.fuelEnabled) {
+          remaining = tr[3] + injectedFuel;
+          if (tr[1] + prodH >= P.ignition) {
+            lifetime = fmaxf(lifetime, fminf(remaining, 1.f));
+            float unburned = remaining * expf(-P.burnRate * P.dt);
+            burned = remaining - unburned;
+            remaining = unburned;
+          }
+        }
+        // evaluateFlame (flame-common.wgsl:30-42)
+        float before = clamp01(lifetime);
+        float after = 0.f, f0 = 0.f, f1 = 0.f, f2 = 0.f;
+        if (before > 0.f) {
+          const FpFlame& F = P.flame;
+          after = fmaxf(0.f, before - F.dt / F.lifespan);
+          f0 = F.smoke * F.lifespan * rampIntegral(F, 0, after, before);
+          f1 = F.heat * F.lifespan * rampIntegral(F, 1, after, before);
+          f2 = F.expansion * (F.lifespan * rampIntegral(F, 2, after, before) / F.dt);
+        }
+        expansion = f2 + P.flame.expansion * burned / P.dt;
+        float dS = tr[0] * expf(-P.dissipation * P.dt) + (prodS + f0) * expf(-P.dissipation * P.dt * 0.5f);
+        float dH = tr[1] * expf(-P.cooling * P.dt) + (prodH + f1) * expf(-P.cooling * P.dt * 0.5f);
+        value[0] = fmaxf(dS, 0.f);
+        value[1] = fmaxf(dH, 0.f);
+        value[2] = after;
+        value[3] = remaining;
+        injected = prodS > 0.f || prodH > 0.f || lifetime > tr[2] || injectedFuel > 0.f;
       }
-      // evaluateFlame (flame-common.wgsl:30-42)
-      float before = clamp01(lifetime);
-      float after = 0.f, f0 = 0.f, f1 = 0.f, f2 = 0.f;
-      if (before > 0.f) {
-        const FpFlame& F = P.flame;
-        after = fmaxf(0.f, before - F.dt / F.lifespan);
-        f0 = F.smoke * F.lifespan * rampIntegral(F, 0, after, before);
-        f1 = F.heat * F.lifespan * rampIntegral(F, 1, after, before);
-        f2 = F.expansion * (F.lifespan * rampIntegral(F, 2, after, before) / F.dt);
+      // clearDormant (fluid-common.wgsl:8-13)
+      if (!injected && value[2] == 0.f && value[0] < 0.001f && value[1] < 0.001f && value[3] < 0.001f)
+        value[0] = value[1] = value[2] = value[3] = 0.f;
+      for (int k = 0; k < 4; k++) stHalf(P.fldN, (slot * 4 + k) * N + c, value[k], half);
+      P.expn[slot * N + c] = expansion;
+      if (expansion != 0.f) expands = true;
+      // holdsContent and contentSupport (fluid-content.wgsl:22-39).
+      if (fmaxf(fmaxf(P.smokeDiv > 1 ? 0.f : value[0], value[2]), value[3]) > P.cutoff) {
+        if (!cvSampled) cv = VP.velDiv == 1 ? centreVelocity(VP, H, GV, V, x, y, z) : velocityAt(VP, H, GV, V, px, py, pz);
+        int idc[3] = {x, y, z};
+        float vv[3] = {cv.x, cv.y, cv.z};
+        bool low[3], high[3];
+        for (int a = 0; a < 3; a++) {
+          float side = (float)P.B;
+          float loc = (float)(idc[a] & (P.B - 1)) + 0.5f;
+          // two velocity cells of stencil (2 d field cells), and a step of motion
+          float pad = fminf(side, fmaxf(2.f, 2.f * (float)P.velDiv) + fabsf(vv[a]) * P.dt / P.h);
+          low[a] = loc < pad;
+          high[a] = loc + pad >= side;
+        }
+        uint32_t row = 2u | (low[0] ? 1u : 0u) | (high[0] ? 4u : 0u);
+        uint32_t plane = (row << 3u) | (low[1] ? row : 0u) | (high[1] ? (row << 6u) : 0u);
+        busy |= (plane << 9u) | (low[2] ? plane : 0u) | (high[2] ? (plane << 18u) : 0u);
       }
-      expansion = f2 + P.flame.expansion * burned / P.dt;
-      float dS = tr[0] * expf(-P.dissipation * P.dt) + (prodS + f0) * expf(-P.dissipation * P.dt * 0.5f);
-      float dH = tr[1] * expf(-P.cooling * P.dt) + (prodH + f1) * expf(-P.cooling * P.dt * 0.5f);
-      value[0] = fmaxf(dS, 0.f);
-      value[1] = fmaxf(dH, 0.f);
-      value[2] = after;
-      value[3] = remaining;
-      injected = prodS > 0.f || prodH > 0.f || lifetime > tr[2] || injectedFuel > 0.f;
+  };
+  if constexpr (MODE == 2) {
+    const TransportStage<true> GV = velocityStage(VP, H);
+    stageField(VP, H, GV, smem, P.vel, 3);
+    const int cubes = (P.B / CUBE) * (P.B / CUBE) * (P.B / CUBE);
+    for (int k = 0; k < cubes; k++) {
+      int ox, oy, oz;
+      cubeOrigin(P.B, k, ox, oy, oz);
+      const TransportStage<true> GF =
+          stageAt<8 + 2 * HALO>(H.bx * P.B + ox - HALO, H.by * P.B + oy - HALO, H.bz * P.B + oz - HALO);
+      if (k > 0) __syncthreads();  // the previous cube's stage has been read
+      stageField(P, H, GF, smem + 3 * GV.S3, P.fldP, 4);
+      stageWait();
+      for (int q = threadIdx.x; q < CUBE * CUBE * CUBE; q += blockDim.x) {
+        const int lx = ox + (q & 7), ly = oy + ((q >> 3) & 7), lz = oz + (q >> 6);
+        cell(GV, GF, (lz * P.B + ly) * P.B + lx, H.bx * P.B + lx, H.by * P.B + ly, H.bz * P.B + lz);
+      }
     }
-    // clearDormant (fluid-common.wgsl:8-13)
-    if (!injected && value[2] == 0.f && value[0] < 0.001f && value[1] < 0.001f && value[3] < 0.001f)
-      value[0] = value[1] = value[2] = value[3] = 0.f;
-    for (int k = 0; k < 4; k++) stHalf(P.fldN, (slot * 4 + k) * N + c, value[k], half);
-    P.expn[slot * N + c] = expansion;
-    if (expansion != 0.f) expands = true;
-    // holdsContent and contentSupport (fluid-content.wgsl:22-39).
-    if (fmaxf(fmaxf(P.smokeDiv > 1 ? 0.f : value[0], value[2]), value[3]) > P.cutoff) {
-      if (!cvSampled) cv = VP.velDiv == 1 ? centreVelocity(VP, H, G, V, x, y, z) : velocityAt(VP, H, G, V, px, py, pz);
-      int idc[3] = {x, y, z};
-      float vv[3] = {cv.x, cv.y, cv.z};
-      bool low[3], high[3];
-      for (int a = 0; a < 3; a++) {
-        float side = (float)P.B;
-        float loc = (float)(idc[a] & (P.B - 1)) + 0.5f;
-        // two velocity cells of stencil (2 d field cells), and a step of motion
-        float pad = fminf(side, fmaxf(2.f, 2.f * (float)P.velDiv) + fabsf(vv[a]) * P.dt / P.h);
-        low[a] = loc < pad;
-        high[a] = loc + pad >= side;
-      }
-      uint32_t row = 2u | (low[0] ? 1u : 0u) | (high[0] ? 4u : 0u);
-      uint32_t plane = (row << 3u) | (low[1] ? row : 0u) | (high[1] ? (row << 6u) : 0u);
-      busy |= (plane << 9u) | (low[2] ? plane : 0u) | (high[2] ? (plane << 18u) : 0u);
+  } else {
+    TransportStage<STAGED> G = stageOf<STAGED>(P, H);
+    if (STAGED) {
+      stageField(P, H, G, smem, P.vel, 3);
+      stageField(P, H, G, smem + 3 * G.S3, P.fldP, 4);
+      stageWait();
+    }
+    for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
+      int x, y, z;
+      cellOf(P, H, c, x, y, z);
+      cell(G, G, c, x, y, z);
     }
   }
   // recordContent (fluid-content.wgsl:43-64): one update per brick.
@@ -701,13 +783,13 @@ FP_DEV void brick_evolve(const SimParams* __restrict__ Pp, uint32_t i) {
   }
   __syncthreads();
 }
-template <bool STAGED>
+template <int MODE>
 __global__ void __launch_bounds__(THREADS, FP_TRANSPORT_CTAS) k_evolve(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_evolve<STAGED>(&P, i);
+    brick_evolve<MODE>(&P, i);
   }
 }
 
@@ -1391,30 +1473,44 @@ static size_t stagedBytes(int channels) {
 // Shared-memory limits of the step kernels, set once before any launch (and so before any
 // stream capture of one).
 void fp_step_configure(int B) {
-  cudaFuncSetAttribute(k_predict<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
-  cudaFuncSetAttribute(k_correct<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(6));
-  cudaFuncSetAttribute(k_evolve<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
+  cudaFuncSetAttribute(k_predict<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
+  cudaFuncSetAttribute(k_predict<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
+  cudaFuncSetAttribute(k_correct<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(6));
+  cudaFuncSetAttribute(k_correct<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(6));
+  cudaFuncSetAttribute(k_evolve<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
+  cudaFuncSetAttribute(k_evolve<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
   const size_t side = (size_t)(B < FORCE_SUB ? B : FORCE_SUB) + 1, smem = side * side * side * sizeof(float3);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_forces<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
+// The transport kernels' form for bricks of B field cells and velocity divisor vd.
+static int transportMode(int B, int vd) { return (B == 8 && vd == 1) ? 1 : ((vd > 1 && B == CUBE * vd) ? 2 : 0); }
 void fp_launch_predict(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
-  if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
-    k_predict<true><<<sms * FP_TRANSPORT_CTAS, THREADS, stagedBytes(7), st>>>(bt);
+  const int mode = transportMode(B, vd);
+  if (mode == 1)
+    k_predict<1><<<sms * FP_TRANSPORT_CTAS, THREADS, stagedBytes(7), st>>>(bt);
+  else if (mode == 2)
+    k_predict<2><<<sms * FP_TRANSPORT_CTAS, THREADS, stagedBytes(7), st>>>(bt);
   else
-    k_predict<false><<<sms * FP_TRANSPORT_CTAS, THREADS, 0, st>>>(bt);
+    k_predict<0><<<sms * FP_TRANSPORT_CTAS, THREADS, 0, st>>>(bt);
 }
 void fp_launch_correct(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
-  if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
-    k_correct<true><<<sms * FP_TRANSPORT_CTAS, THREADS, stagedBytes(6), st>>>(bt);
+  const int mode = transportMode(B, vd);
+  if (mode == 1)
+    k_correct<1><<<sms * FP_TRANSPORT_CTAS, THREADS, stagedBytes(6), st>>>(bt);
+  else if (mode == 2)
+    k_correct<2><<<sms * FP_TRANSPORT_CTAS, THREADS, stagedBytes(6), st>>>(bt);
   else
-    k_correct<false><<<sms * FP_TRANSPORT_CTAS, THREADS, 0, st>>>(bt);
+    k_correct<0><<<sms * FP_TRANSPORT_CTAS, THREADS, 0, st>>>(bt);
 }
 void fp_launch_evolve(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
-  if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
-    k_evolve<true><<<sms * FP_TRANSPORT_CTAS, THREADS, stagedBytes(7), st>>>(bt);
+  const int mode = transportMode(B, vd);
+  if (mode == 1)
+    k_evolve<1><<<sms * FP_TRANSPORT_CTAS, THREADS, stagedBytes(7), st>>>(bt);
+  else if (mode == 2)
+    k_evolve<2><<<sms * FP_TRANSPORT_CTAS, THREADS, stagedBytes(7), st>>>(bt);
   else
-    k_evolve<false><<<sms * FP_TRANSPORT_CTAS, THREADS, 0, st>>>(bt);
+    k_evolve<0><<<sms * FP_TRANSPORT_CTAS, THREADS, 0, st>>>(bt);
 }
 void fp_launch_curl(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
   if (B == 8 && vd == 1)  // staged: 8^3 bricks, one lattice
