@@ -524,6 +524,40 @@ def precision_form(local: int, steps: int = 30) -> dict:
     return out
 
 
+def profile_small_form(local: int, grow: int = 40) -> dict:
+    """A small case that runs every kernel family once inside the profiler window (for
+    `ncu --profile-from-start off`, one GPU): the force scene (colliders, every force kind) with
+    coarse smoke (smoke divisor 2) on 8^3 bricks, budget 2^20 voxels, grown `grow` steps, then
+    one step and a half-resolution render at 320x180 inside the window."""
+    import torch
+
+    from firepro import render, scenes
+    from firepro.engine import FluidSimulation
+
+    sc = scenes.ForceScene()
+    grid = sc.grid(budget=2 ** 20)
+    grid.smoke_divisor = 2
+    sim = FluidSimulation(grid, device=local)
+    sim.set_runtime(0.05, 2 ** 20, True)
+    for step in range(grow):
+        sim.step(sc.frame(step).frame)
+    cam = render.look_at((0.0, 1.0, 3.0), (0.0, 0.5, 0.0), 320, 180)
+    cam.half_resolution = 1
+    rs = render.default_settings(ray_steps=64, shadow_samples=8)
+    sim.render(cam, rs)  # the render pools and table, outside the window
+    sim.synchronize()
+    torch.cuda.profiler.start()
+    sim.step(sc.frame(grow).frame)
+    image = sim.render(cam, rs)
+    sim.synchronize()
+    torch.cuda.profiler.stop()
+    out = {"workload": f"force scene, 8^3 bricks, smoke divisor 2, budget 2^20 voxels, grown {grow} steps; one step "
+                       f"and a 320x180 half-resolution render in the profiler window",
+           "active_bricks": int(sim.stats().active_bricks), "covered": float((image[..., 3] > 0.01).mean())}
+    sim.dispose()
+    return out
+
+
 def stress_form(local: int, grow: int = 600, steps: int = 20, renders: int = 5) -> dict:
     """The stress workload: the 25 m/s jet scene grown `grow` steps (untimed) at the
     benchmark's budget, its step timed (plain FP32, the 6-level reference V-cycle), and the
@@ -819,8 +853,18 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and served workloads")
     ap.add_argument("--scene", default="large_scene", help="workload (default: the large single simulation)")
+    ap.add_argument("--form", default=None, choices=["batched", "served_64", "precision", "stress", "default_grid",
+                                                       "serving", "profile_small"],
+                    help="run one of the forms alone on GPU 0 and print its JSON")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.form:
+        forms = {"batched": lambda: batched_form(0), "served_64": lambda: served_form(0),
+                 "precision": lambda: precision_form(0), "stress": lambda: stress_form(0),
+                 "default_grid": lambda: default_grid_form(0), "serving": lambda: serving_forms(0),
+                 "profile_small": lambda: profile_small_form(0)}
+        print(json.dumps({"form": args.form, **forms[args.form]()}), flush=True)
+        return
     rank, world, local = dist_setup(args)
     try:
         if args.impl == "reference":

@@ -347,6 +347,7 @@ class Stepper {
   int cycle_ = 0;             // the V-cycle being enqueued
   bool fusedCoarse_ = false;  // the V-cycle below the first tile level runs as k_coarse
   bool anySmoke_ = false;     // a simulation of the launch keeps coarse smoke
+  int smokeDiv_ = 0;          // the finest coarse smoke grid's divisor among them (0: none)
   fp_solver_schedule schedule_{};  // the launch's pressure-solve schedule (its simulations')
   int rhs0Sel_ = 2;           // the finest level's right-hand side: the divergence, or the CG residual
   void vcycle(int level, int cur[], uint64_t& launches);

@@ -384,6 +384,12 @@ FP_DEV Stage<SS> stageAt(int ox, int oy, int oz) {
 FP_DEV TransportStage<true> velocityStage(const SimParams& VP, const Home& H) {
   return stageAt<8 + 2 * HALO>(H.bx * VP.B - HALO, H.by * VP.B - HALO, H.bz * VP.B - HALO);
 }
+// velocityStage when S, else no stage.
+template <bool S>
+FP_DEV TransportStage<S> velocityStageIf(const SimParams& VP, const Home& H) {
+  if constexpr (S) return velocityStage(VP, H);
+  else return TransportStage<false>{};
+}
 // The cubes of 8^3 field cells of a brick of B field cells a side: cube k's first cell in the brick.
 FP_DEV void cubeOrigin(int B, int k, int& ox, int& oy, int& oz) {
   const int per = B / CUBE;
@@ -1317,9 +1323,10 @@ FP_DEV SmokeCell smokeCellOf(const SimParams& P, const Home& H, int c) {
   return s;
 }
 // traceBack / traceForward (fluid-advection.wgsl:67-75) from `p` with centre velocity `cv`.
-FP_DEV float3 smokeTrace(const SimParams& P, const Home& H, const float* p, float3 cv, float sign) {
-  Stage<0> G{};
-  Field V{P.vel, 3, nullptr};
+// G and V: the velocity and its stage (on the velocity lattice), or no stage.
+template <int SS>
+FP_DEV float3 smokeTrace(const SimParams& P, const Home& H, const Stage<SS>& G, const Field& V, const float* p, float3 cv,
+                         float sign) {
   float3 vm = velocityAt(*P.vview, H, G, V, p[0] + sign * 0.5f * P.dt * cv.x, p[1] + sign * 0.5f * P.dt * cv.y,
                          p[2] + sign * 0.5f * P.dt * cv.z);
   return make_float3(p[0] + sign * P.dt * vm.x, p[1] + sign * P.dt * vm.y, p[2] + sign * P.dt * vm.z);
@@ -1327,8 +1334,13 @@ FP_DEV float3 smokeTrace(const SimParams& P, const Home& H, const float* p, floa
 
 // advectSmoke (smoke.wgsl:101-124): the predictor at the back-traced departure and, for
 // MacCormack, the donors' range (smokeDonorBounds :63-77: min from 1e30, max from 0).
-__global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_advect(FpBatch bt) {
+// VSTAGED: the velocity lattice has 8^3 cells a brick and the smoke grid 8^3 or more: the
+// velocity is staged once per brick over the brick and a HALO rim (256 threads a CTA); else
+// every velocity sample reads through the directory (64 threads a CTA).
+template <bool VSTAGED>
+__global__ void __launch_bounds__(VSTAGED ? 256 : SMOKE_THREADS) k_smoke_advect(FpBatch bt) {
   __shared__ int nslot[27];
+  extern __shared__ float smem[];
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
@@ -1339,14 +1351,18 @@ __global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_advect(FpBatch bt) {
     const size_t slot = (size_t)nslot[13], SN = (size_t)P.smokeCells;
     const float sp = P.h * (float)P.smokeDiv, invSp = 1.f / sp;
     const bool half = P.scalarHalf != 0;
-    Stage<0> G{};
-    Field V{P.vel, 3, nullptr};
+    const TransportStage<VSTAGED> G = velocityStageIf<VSTAGED>(*P.vview, H);
+    Field V{P.vel, 3, VSTAGED ? smem : nullptr};
+    if (VSTAGED) {
+      stageField(*P.vview, H, G, smem, P.vel, 3);
+      stageWait();
+    }
     for (int c = threadIdx.x; c < P.smokeCells; c += blockDim.x) {
       SmokeCell s = smokeCellOf(P, H, c);
       float density = 0.f;
       if (!solidAt(P, H, s.p[0], s.p[1], s.p[2])) {
         float3 cv = velocityAt(*P.vview, H, G, V, s.p[0], s.p[1], s.p[2]);
-        float3 dep = smokeTrace(P, H, s.p, cv, -1.f);
+        float3 dep = smokeTrace(P, H, G, V, s.p, cv, -1.f);
         density = smokeSample(P, H, P.smk, dep.x * invSp, dep.y * invSp, dep.z * invSp, half);
         if (P.maccormack) {
           // The donor block is an integer decision: divided, as the oracle does.
@@ -1389,9 +1405,11 @@ FP_DEV uint32_t smokeSupport(const SimParams& P, const int* q, float3 v) {
 // evolveSmoke (smoke.wgsl:126-178): the bounded MacCormack correction, decay, the volume
 // average of the evolved fine cells' source production (smokeProduction :23-38: the mean of
 // each 2x2x2 block, a trilinear sample at its shared corner), dormant clearing, content flags.
-__global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_evolve(FpBatch bt) {
+template <bool VSTAGED>
+__global__ void __launch_bounds__(VSTAGED ? 256 : SMOKE_THREADS) k_smoke_evolve(FpBatch bt) {
   __shared__ int nslot[27];
   __shared__ uint32_t busyAll;
+  extern __shared__ float smem[];
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
@@ -1405,8 +1423,12 @@ __global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_evolve(FpBatch bt) {
     const int d = P.smokeDiv, blocks = d / 2;
     const float sp = P.h * (float)d, invSp = 1.f / sp, volume = (float)(d * d * d / 8);
     const bool half = P.scalarHalf != 0;
-    Stage<0> G{};
-    Field V{P.vel, 3, nullptr};
+    const TransportStage<VSTAGED> G = velocityStageIf<VSTAGED>(*P.vview, H);
+    Field V{P.vel, 3, VSTAGED ? smem : nullptr};
+    if (VSTAGED) {
+      stageField(*P.vview, H, G, smem, P.vel, 3);
+      stageWait();
+    }
     uint32_t busy = 0;
     for (int c = threadIdx.x; c < P.smokeCells; c += blockDim.x) {
       SmokeCell s = smokeCellOf(P, H, c);
@@ -1419,7 +1441,7 @@ __global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_evolve(FpBatch bt) {
           const float lo = P.smkB[(slot * 2 + 0) * SN + c], hi = P.smkB[(slot * 2 + 1) * SN + c];
           if (lo != hi || predictor != lo) {
             const float original = ldHalf(P.smk, slot * SN + c, half);
-            float3 fwd = smokeTrace(P, H, s.p, cv, 1.f);
+            float3 fwd = smokeTrace(P, H, G, V, s.p, cv, 1.f);
             float reversed = smokeSample(P, H, P.smkP, fwd.x * invSp, fwd.y * invSp, fwd.z * invSp, false);
             float corrected = predictor + 0.5f * (original - reversed);
             bounded = (corrected < lo || corrected > hi) ? predictor : corrected;
@@ -1459,16 +1481,21 @@ __global__ void __launch_bounds__(SMOKE_THREADS) k_smoke_evolve(FpBatch bt) {
 
 }  // namespace
 
-void fp_launch_smoke(const FpBatch& bt, int sms, cudaStream_t st) {
-  k_smoke_advect<<<sms * 16, SMOKE_THREADS, 0, st>>>(bt);
-  k_smoke_evolve<<<sms * 16, SMOKE_THREADS, 0, st>>>(bt);
-}
-
 // Staged kernels for 8^3 bricks: `channels` staged fields over (8 + 2 HALO)^3 cells.
 static size_t stagedBytes(int channels) {
   const int S = 8 + 2 * HALO;
   return (size_t)channels * S * S * S * sizeof(float);
 }
+void fp_launch_smoke(const FpBatch& bt, int B, int vd, int sd, int sms, cudaStream_t st) {
+  if (B == CUBE * vd && B / sd >= CUBE) {  // the velocity lattice 8^3 a brick, the smoke grid 8^3 or finer
+    k_smoke_advect<true><<<sms * 3, 256, stagedBytes(3), st>>>(bt);
+    k_smoke_evolve<true><<<sms * 3, 256, stagedBytes(3), st>>>(bt);
+  } else {
+    k_smoke_advect<false><<<sms * 16, SMOKE_THREADS, 0, st>>>(bt);
+    k_smoke_evolve<false><<<sms * 16, SMOKE_THREADS, 0, st>>>(bt);
+  }
+}
+
 
 // Shared-memory limits of the step kernels, set once before any launch (and so before any
 // stream capture of one).

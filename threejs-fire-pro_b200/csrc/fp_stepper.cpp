@@ -227,12 +227,14 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
   int vcycles = 1;
   fusedCoarse_ = true;
   anySmoke_ = false;
+  smokeDiv_ = 0;
   pending_.clear();
   for (int i = 0; i < count; i++) {
     Engine* e = sims[i];
     uint32_t cap = (uint32_t)e->capacity();
     fusedCoarse_ = fusedCoarse_ && fp_coarse_fits(e->liveTiles());
     anySmoke_ = anySmoke_ || e->smokeDivisor() > 1;
+    if (e->smokeDivisor() > 1 && (smokeDiv_ == 0 || e->smokeDivisor() < smokeDiv_)) smokeDiv_ = e->smokeDivisor();
     rowBlocks[i] = blocks;
     rowTiles[i] = tiles;
     rowIds[i] = ids;
@@ -270,7 +272,7 @@ int Stepper::step(Engine* const* sims, const fp_frame* const* frames, const floa
                    ((uint64_t)anySmoke_ << 17) | ((uint64_t)schedule_.smoother << 18) |
                    ((uint64_t)schedule_.krylov << 19) | ((uint64_t)schedule_.levels << 20) |
                    ((uint64_t)schedule_.pre_sweeps << 24) | ((uint64_t)schedule_.post_sweeps << 28) |
-                   ((uint64_t)schedule_.bottom_sweeps << 32);
+                   ((uint64_t)schedule_.bottom_sweeps << 32) | ((uint64_t)smokeDiv_ << 40);
     auto it = graphs_.find(key);
     if (it == graphs_.end()) {
       GraphEntry ge{};
@@ -458,7 +460,7 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   fp_launch_evolve(bt, B_, vd_, sms_, stream_);
   // Coarse smoke evolves after the fine fields, whose source production it averages, and
   // records content before the measurement.
-  if (anySmoke_) fp_launch_smoke(bt, sms_, stream_);
+  if (anySmoke_) fp_launch_smoke(bt, B_, vd_, smokeDiv_, sms_, stream_);
   phaseEnd(PH_EVOLVE, anySmoke_ ? 3 : 1);
   launches += anySmoke_ ? 5 : 3;
 
