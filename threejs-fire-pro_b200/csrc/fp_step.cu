@@ -1322,6 +1322,52 @@ FP_DEV SmokeCell smokeCellOf(const SimParams& P, const Home& H, int c) {
   for (int a = 0; a < 3; a++) s.p[a] = ((float)s.q[a] + 0.5f) * sp;
   return s;
 }
+// The coarse smoke field of a brick of 8^3 smoke cells staged with a HALO rim (SmokeStage, on
+// the smoke lattice; `on` false: nothing staged). smokeCellS / smokeSampleS read the stage where
+// it holds the cell and the directory elsewhere: the same values as smokeCell / smokeSample.
+struct SmokeStage {
+  int ox, oy, oz;
+  bool on;
+  const float* st;
+  static constexpr int S = 8 + 2 * HALO, S3 = S * S * S;
+};
+FP_DEV SmokeStage stageSmoke(const SimParams& P, const Home& H, bool on, float* sm, const float* pool, bool half) {
+  SmokeStage G;
+  G.on = on;
+  G.st = sm;
+  G.ox = H.bx * 8 - HALO;
+  G.oy = H.by * 8 - HALO;
+  G.oz = H.bz * 8 - HALO;
+  if (!on) return G;
+  const int sh = P.smokeShift, m = (1 << sh) - 1;
+  for (int i = threadIdx.x; i < SmokeStage::S3; i += blockDim.x) {
+    const int x = G.ox + i % SmokeStage::S, y = G.oy + (i / SmokeStage::S) % SmokeStage::S,
+              z = G.oz + i / (SmokeStage::S * SmokeStage::S);
+    const int s = brickSlot(P, H, x >> sh, y >> sh, z >> sh);
+    sm[i] = s < 0 ? 0.f : ldHalf(pool, (size_t)s * P.smokeCells + ((((z & m) << sh) | (y & m)) << sh | (x & m)), half);
+  }
+  return G;
+}
+FP_DEV float smokeCellS(const SimParams& P, const Home& H, const SmokeStage& G, const float* pool, int x, int y, int z,
+                        bool half) {
+  if (G.on) {
+    const unsigned lx = (unsigned)(x - G.ox), ly = (unsigned)(y - G.oy), lz = (unsigned)(z - G.oz);
+    if (lx < (unsigned)SmokeStage::S && ly < (unsigned)SmokeStage::S && lz < (unsigned)SmokeStage::S)
+      return G.st[((int)lz * SmokeStage::S + (int)ly) * SmokeStage::S + (int)lx];
+  }
+  return smokeCell(P, H, pool, x, y, z, half);
+}
+FP_DEV float smokeSampleS(const SimParams& P, const Home& H, const SmokeStage& G, const float* pool, float px, float py,
+                          float pz, bool half) {
+  float qx = px - 0.5f, qy = py - 0.5f, qz = pz - 0.5f;
+  float gx = floorf(qx), gy = floorf(qy), gz = floorf(qz);
+  int x0 = (int)gx, y0 = (int)gy, z0 = (int)gz;
+  float t[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) t[j] = smokeCellS(P, H, G, pool, x0 + (j & 1), y0 + ((j >> 1) & 1), z0 + (j >> 2), half);
+  return blend8(t, qx - gx, qy - gy, qz - gz);
+}
+
 // traceBack / traceForward (fluid-advection.wgsl:67-75) from `p` with centre velocity `cv`.
 // G and V: the velocity and its stage (on the velocity lattice), or no stage.
 template <int SS>
@@ -1338,7 +1384,7 @@ FP_DEV float3 smokeTrace(const SimParams& P, const Home& H, const Stage<SS>& G, 
 // velocity is staged once per brick over the brick and a HALO rim (256 threads a CTA); else
 // every velocity sample reads through the directory (64 threads a CTA).
 template <bool VSTAGED>
-__global__ void __launch_bounds__(VSTAGED ? 256 : SMOKE_THREADS) k_smoke_advect(FpBatch bt) {
+__global__ void __launch_bounds__(VSTAGED ? 256 : SMOKE_THREADS, VSTAGED ? 3 : 8) k_smoke_advect(FpBatch bt) {
   __shared__ int nslot[27];
   extern __shared__ float smem[];
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
@@ -1353,6 +1399,7 @@ __global__ void __launch_bounds__(VSTAGED ? 256 : SMOKE_THREADS) k_smoke_advect(
     const bool half = P.scalarHalf != 0;
     const TransportStage<VSTAGED> G = velocityStageIf<VSTAGED>(*P.vview, H);
     Field V{P.vel, 3, VSTAGED ? smem : nullptr};
+    SmokeStage GS = stageSmoke(P, H, VSTAGED && P.smokeShift == 3, smem + 3 * G.S3, P.smk, half);
     if (VSTAGED) {
       stageField(*P.vview, H, G, smem, P.vel, 3);
       stageWait();
@@ -1363,14 +1410,14 @@ __global__ void __launch_bounds__(VSTAGED ? 256 : SMOKE_THREADS) k_smoke_advect(
       if (!solidAt(P, H, s.p[0], s.p[1], s.p[2])) {
         float3 cv = velocityAt(*P.vview, H, G, V, s.p[0], s.p[1], s.p[2]);
         float3 dep = smokeTrace(P, H, G, V, s.p, cv, -1.f);
-        density = smokeSample(P, H, P.smk, dep.x * invSp, dep.y * invSp, dep.z * invSp, half);
+        density = smokeSampleS(P, H, GS, P.smk, dep.x * invSp, dep.y * invSp, dep.z * invSp, half);
         if (P.maccormack) {
           // The donor block is an integer decision: divided, as the oracle does.
           int bx = (int)floorf(dep.x / sp - 0.5f), by = (int)floorf(dep.y / sp - 0.5f), bz = (int)floorf(dep.z / sp - 0.5f);
           float lo = 1e30f, hi = 0.f;
 #pragma unroll
           for (int k = 0; k < 8; k++) {
-            float v = smokeCell(P, H, P.smk, bx + (k & 1), by + ((k >> 1) & 1), bz + (k >> 2), half);
+            float v = smokeCellS(P, H, GS, P.smk, bx + (k & 1), by + ((k >> 1) & 1), bz + (k >> 2), half);
             lo = fminf(lo, v);
             hi = fmaxf(hi, v);
           }
@@ -1406,7 +1453,7 @@ FP_DEV uint32_t smokeSupport(const SimParams& P, const int* q, float3 v) {
 // average of the evolved fine cells' source production (smokeProduction :23-38: the mean of
 // each 2x2x2 block, a trilinear sample at its shared corner), dormant clearing, content flags.
 template <bool VSTAGED>
-__global__ void __launch_bounds__(VSTAGED ? 256 : SMOKE_THREADS) k_smoke_evolve(FpBatch bt) {
+__global__ void __launch_bounds__(VSTAGED ? 256 : SMOKE_THREADS, VSTAGED ? 3 : 8) k_smoke_evolve(FpBatch bt) {
   __shared__ int nslot[27];
   __shared__ uint32_t busyAll;
   extern __shared__ float smem[];
@@ -1425,6 +1472,7 @@ __global__ void __launch_bounds__(VSTAGED ? 256 : SMOKE_THREADS) k_smoke_evolve(
     const bool half = P.scalarHalf != 0;
     const TransportStage<VSTAGED> G = velocityStageIf<VSTAGED>(*P.vview, H);
     Field V{P.vel, 3, VSTAGED ? smem : nullptr};
+    SmokeStage GS = stageSmoke(P, H, VSTAGED && P.smokeShift == 3, smem + 3 * G.S3, P.smkP, false);
     if (VSTAGED) {
       stageField(*P.vview, H, G, smem, P.vel, 3);
       stageWait();
@@ -1442,7 +1490,7 @@ __global__ void __launch_bounds__(VSTAGED ? 256 : SMOKE_THREADS) k_smoke_evolve(
           if (lo != hi || predictor != lo) {
             const float original = ldHalf(P.smk, slot * SN + c, half);
             float3 fwd = smokeTrace(P, H, G, V, s.p, cv, 1.f);
-            float reversed = smokeSample(P, H, P.smkP, fwd.x * invSp, fwd.y * invSp, fwd.z * invSp, false);
+            float reversed = smokeSampleS(P, H, GS, P.smkP, fwd.x * invSp, fwd.y * invSp, fwd.z * invSp, false);
             float corrected = predictor + 0.5f * (original - reversed);
             bounded = (corrected < lo || corrected > hi) ? predictor : corrected;
           }
@@ -1453,8 +1501,18 @@ __global__ void __launch_bounds__(VSTAGED ? 256 : SMOKE_THREADS) k_smoke_evolve(
             for (int bx = 0; bx < blocks; bx++) {
               const float fx = (float)(s.q[0] * d + 2 * bx + 1), fy = (float)(s.q[1] * d + 2 * by + 1),
                           fz = (float)(s.q[2] * d + 2 * bz + 1);
+              // sampleCells at the shared corner of a 2x2x2 block of the brick's own field cells
+              // (fractions exactly one half): read from the slot directly.
+              const int x0 = (int)fx - 1, y0 = (int)fy - 1, z0 = (int)fz - 1;
 #pragma unroll
-              for (int k = 0; k < 4; k++) produced[k] += sampleCells(P, H, P.fldN, 4, k, fx, fy, fz, half);
+              for (int k = 0; k < 4; k++) {
+                float t[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                  t[j] = ldHalf(P.fldN, (slot * 4 + k) * (size_t)P.N + localCell(P, x0 + (j & 1), y0 + ((j >> 1) & 1), z0 + (j >> 2)),
+                                half);
+                produced[k] += blend8(t, 0.5f, 0.5f, 0.5f);
+              }
             }
 #pragma unroll
         for (int k = 0; k < 4; k++) produced[k] /= volume;
@@ -1488,8 +1546,8 @@ static size_t stagedBytes(int channels) {
 }
 void fp_launch_smoke(const FpBatch& bt, int B, int vd, int sd, int sms, cudaStream_t st) {
   if (B == CUBE * vd && B / sd >= CUBE) {  // the velocity lattice 8^3 a brick, the smoke grid 8^3 or finer
-    k_smoke_advect<true><<<sms * 3, 256, stagedBytes(3), st>>>(bt);
-    k_smoke_evolve<true><<<sms * 3, 256, stagedBytes(3), st>>>(bt);
+    k_smoke_advect<true><<<sms * 3, 256, stagedBytes(4), st>>>(bt);
+    k_smoke_evolve<true><<<sms * 3, 256, stagedBytes(4), st>>>(bt);
   } else {
     k_smoke_advect<false><<<sms * 16, SMOKE_THREADS, 0, st>>>(bt);
     k_smoke_evolve<false><<<sms * 16, SMOKE_THREADS, 0, st>>>(bt);
