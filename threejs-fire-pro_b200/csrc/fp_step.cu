@@ -1018,7 +1018,10 @@ FP_DEV float sourceVelocity(const SimParams& P, const Home& H, int tile, float v
 // The side of the cubes the force kernel walks a brick in: their force tiles fit shared memory.
 constexpr int FORCE_SUB = 16;
 
-template <bool STAGED>
+// MODE 1: 8^3 bricks on one lattice, curl and scalars staged. MODE 2: a velocity lattice of 8^3
+// cells a brick under a finer field lattice: the curl staged, the scalars' means (fieldAverage)
+// read through the directory. MODE 0: nothing staged.
+template <int MODE>
 FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   __shared__ int nslot[27];
   extern __shared__ float3 forceTile[];  // (SUB+1)^3, then the staged curl and scalars
@@ -1031,11 +1034,12 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   int tile = (int)(id >> 6);
   // The brick in cubes of SUB cells a side (one cube up to 16^3 bricks, 8 of them in a 32^3
   // brick), each with its centre forces on the cube and one cell beyond its upper faces.
-  const int SUB = STAGED ? 8 : min(P.B, FORCE_SUB), E = SUB + 1, E3 = E * E * E, per = STAGED ? 1 : P.B / SUB;
+  constexpr bool ONE = MODE == 1, CSTAGED = MODE != 0;
+  const int SUB = CSTAGED ? 8 : min(P.B, FORCE_SUB), E = SUB + 1, E3 = E * E * E, per = CSTAGED ? 1 : P.B / SUB;
   float* stage = reinterpret_cast<float*>(forceTile + E3);
   // Staged (8^3 bricks: E = 9): the curl over E + 2 cells a side, two scalars over E.
-  Stage<STAGED ? 11 : 0> Gc;
-  Stage<STAGED ? 9 : 0> Gs;
+  Stage<CSTAGED ? 11 : 0> Gc;
+  Stage<ONE ? 9 : 0> Gs;
   Gc.ox = H.bx * P.B - 1;
   Gc.oy = H.by * P.B - 1;
   Gc.oz = H.bz * P.B - 1;
@@ -1043,11 +1047,11 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
   Gs.oy = H.by * P.B;
   Gs.oz = H.bz * P.B;
   const bool half = P.scalarHalf != 0;
-  Field Fc{P.curl, 4, STAGED ? stage : nullptr};
-  Field Fs{P.fldN, 4, STAGED ? stage + 4 * Gc.S3 : nullptr, half};
-  if (STAGED) {
+  Field Fc{P.curl, 4, CSTAGED ? stage : nullptr};
+  Field Fs{P.fldN, 4, ONE ? stage + 4 * Gc.S3 : nullptr, half};
+  if (CSTAGED) {
     if (P.vorticity != 0.f) stageField(P, H, Gc, stage, P.curl, 4);
-    stageField(P, H, Gs, stage + 4 * Gc.S3, P.fldN, 4, half, 2);  // smoke, heat
+    if (ONE) stageField(P, H, Gs, stage + 4 * Gc.S3, P.fldN, 4, half, 2);  // smoke, heat
     stageWait();
   }
   const float decay = expf(-P.damping * P.dt);
@@ -1057,7 +1061,7 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
     for (int q = threadIdx.x; q < E3; q += blockDim.x) {
       int lx = q % E, ly = (q / E) % E, lz = q / (E * E);
       if ((lx == SUB) + (ly == SUB) + (lz == SUB) >= 2) continue;
-      forceTile[q] = cellForce<STAGED>(P, H, Gc, Fc, Gs, Fs, tile, ox + lx, oy + ly, oz + lz);
+      forceTile[q] = cellForce<ONE>(P, H, Gc, Fc, Gs, Fs, tile, ox + lx, oy + ly, oz + lz);
     }
     __syncthreads();
     for (int k = threadIdx.x; k < SUB * SUB * SUB; k += blockDim.x) {
@@ -1075,36 +1079,37 @@ FP_DEV void brick_forces(const SimParams* __restrict__ Pp, uint32_t i) {
         float face[3] = {px, py, pz};
         face[a] += 0.5f * P.h;
         // the face's field cell: (x + 1) d on its axis, x d + d/2 on the others (x + 1, x for d = 1)
-        const int d = STAGED ? 1 : P.velDiv, o = d >> 1;
-        out[a] = sourceVelocity<STAGED>(P, H, tile, v, face[0], face[1], face[2], a, a == 0 ? (x + 1) * d : x * d + o,
+        const int d = ONE ? 1 : P.velDiv, o = d >> 1;
+        out[a] = sourceVelocity<ONE>(P, H, tile, v, face[0], face[1], face[2], a, a == 0 ? (x + 1) * d : x * d + o,
                                         a == 1 ? (y + 1) * d : y * d + o, a == 2 ? (z + 1) * d : z * d + o);
       }
       // enforceFaces (fluid-forces.wgsl:15-31)
       // solidAt at a cell centre is solidCell of that cell: centre / h + 0.25 floors to it.
-      if (solidCell<STAGED>(P, H, x, y, z)) {
+      if (solidCell<ONE>(P, H, x, y, z)) {
         out[0] = out[1] = out[2] = 0.f;
       } else {
-        if (solidCell<STAGED>(P, H, x + 1, y, z)) out[0] = 0.f;
-        if (solidCell<STAGED>(P, H, x, y + 1, z)) out[1] = 0.f;
-        if (solidCell<STAGED>(P, H, x, y, z + 1)) out[2] = 0.f;
+        if (solidCell<ONE>(P, H, x + 1, y, z)) out[0] = 0.f;
+        if (solidCell<ONE>(P, H, x, y + 1, z)) out[1] = 0.f;
+        if (solidCell<ONE>(P, H, x, y, z + 1)) out[2] = 0.f;
       }
       for (int a = 0; a < 3; a++) P.velF[(slot * 3 + a) * N + c] = out[a];
     }
     __syncthreads();  // the tile is read before the next cube's forces overwrite it
   }
 }
-template <bool STAGED>
+template <int MODE>
 __global__ void __launch_bounds__(THREADS, FP_TRANSPORT_CTAS) k_forces(FpBatch bt) {
   uint32_t total = workTotal(bt, FP_WORK_ACTIVE);
   for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
     uint32_t i;
     const SimParams& P = workSim(bt, FP_WORK_ACTIVE, item, i);
-    brick_forces<STAGED>(STAGED ? &P : P.vview, i);  // the velocity lattice (staged: the only one)
+    brick_forces<MODE>(MODE == 1 ? &P : P.vview, i);  // the velocity lattice
   }
 }
 // Shared memory of the staged force kernel: the (B+1)^3 force tile, the curl over (B+3)^3,
 // two scalar channels over (B+1)^3.
 constexpr size_t FORCE_STAGED_BYTES = 729 * sizeof(float3) + (4 * 1331 + 2 * 729) * sizeof(float);
+constexpr size_t FORCE_CURL_STAGED_BYTES = 729 * sizeof(float3) + 4 * 1331 * sizeof(float);  // MODE 2
 
 // pressureUnknown (fluid-forces.wgsl:210-226): the cell's brick and those of its negative
 // neighbours compute.
@@ -1565,7 +1570,7 @@ void fp_step_configure(int B) {
   cudaFuncSetAttribute(k_evolve<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
   cudaFuncSetAttribute(k_evolve<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stagedBytes(7));
   const size_t side = (size_t)(B < FORCE_SUB ? B : FORCE_SUB) + 1, smem = side * side * side * sizeof(float3);
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_forces<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_forces<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 // The transport kernels' form for bricks of B field cells and velocity divisor vd.
@@ -1604,12 +1609,17 @@ void fp_launch_curl(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) 
     k_curl<false><<<sms * 6, THREADS, 0, st>>>(bt);
 }
 void fp_launch_forces(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st) {
-  if (B == 8 && vd == 1) {  // staged: 8^3 bricks, one lattice
-    k_forces<true><<<sms * FP_TRANSPORT_CTAS, THREADS, FORCE_STAGED_BYTES, st>>>(bt);
+  const int mode = transportMode(B, vd);
+  if (mode == 1) {  // staged: 8^3 bricks, one lattice
+    k_forces<1><<<sms * FP_TRANSPORT_CTAS, THREADS, FORCE_STAGED_BYTES, st>>>(bt);
+    return;
+  }
+  if (mode == 2) {  // the curl staged on a velocity lattice of 8^3 cells a brick
+    k_forces<2><<<sms * FP_TRANSPORT_CTAS, THREADS, FORCE_CURL_STAGED_BYTES, st>>>(bt);
     return;
   }
   const size_t side = (size_t)(B < FORCE_SUB ? B : FORCE_SUB) + 1, smem = side * side * side * sizeof(float3);
-  k_forces<false><<<sms * FP_TRANSPORT_CTAS, THREADS, smem, st>>>(bt);
+  k_forces<0><<<sms * FP_TRANSPORT_CTAS, THREADS, smem, st>>>(bt);
 }
 void fp_launch_divergence(const FpBatch& bt, int pSel, int vd, int sms, cudaStream_t st) {
   if (vd == 1)
