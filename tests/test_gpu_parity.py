@@ -288,3 +288,17 @@ def test_default_grid_large_scene():
     grid = sc.grid(budget=2 ** 22)
     grid.smoke_divisor = 2
     check(run(sc, 34, grid=grid, budget=2 ** 22), min_active=16)
+
+
+@pytest.mark.parametrize("brick,vd,sd", [(16, 2, 2), (32, 4, 4)])
+def test_staged_velocity_lattice_forms(brick, vd, sd):
+    """The staged forms on a velocity lattice of 8^3 cells a brick under a finer field lattice
+    (16^3 at divisor 2, 32^3 at divisor 4), with coarse smoke of 8^3 smoke cells a brick (staged
+    with the velocity): every force kind, colliders, a burst and a stopping emitter."""
+    sc = scenes.ForceScene()
+    sc.brick_size = brick
+    sc.velocity_divisor = vd
+    budget = 2 ** 22 if brick == 32 else 2 ** 21
+    grid = sc.grid(budget=budget)
+    grid.smoke_divisor = sd
+    check(run(sc, 14, grid=grid, budget=budget), min_active=4)

@@ -1124,6 +1124,36 @@ FP_DEV bool pressureUnknown(const SimParams& P, const Home& H, int x, int y, int
   return true;
 }
 
+// pressureUnknown of every cell of the home brick and of the layer past its upper faces, as a
+// table built once per brick: a cell's answer depends only on its brick (offset 0 or 1 from the
+// home on each axis) and on which axes its brick-local coordinate is 0 (then the brick below on
+// that axis must compute too). Bit ((oz*2 + oy)*2 + ox)*8 + (fz*2 + fy)*2 + fx; the ground's
+// rule as pressureUnknown's (bricks below y = 0 are not asked). Every thread of the CTA calls it.
+FP_DEV uint64_t unknownTable(const SimParams& P, const Home& H, uint32_t* words) {
+  const int t = threadIdx.x;
+  if (t < 64) {
+    const int ox = (t >> 3) & 1, oy = (t >> 4) & 1, oz = t >> 5, fx = t & 1, fy = (t >> 1) & 1, fz = (t >> 2) & 1;
+    bool u = true;
+    for (int dz = oz - fz; dz <= oz; dz++)
+      for (int dy = oy - fy; dy <= oy; dy++)
+        for (int dx = ox - fx; dx <= ox; dx++) {
+          if (P.ground && H.by + dy < 0) continue;
+          if (H.nslot[nbrIndex(dx, dy, dz)] < 0) u = false;
+        }
+    const uint32_t b = __ballot_sync(0xffffffffu, u);
+    if ((t & 31) == 0) words[t >> 5] = b;
+  }
+  __syncthreads();
+  return (uint64_t)words[0] | ((uint64_t)words[1] << 32);
+}
+// pressureUnknown of cell (x,y,z) of the home brick or of the layer past its upper faces.
+FP_DEV bool unknownIn(uint64_t table, const SimParams& P, const Home& H, int x, int y, int z) {
+  const int m = P.B - 1;
+  const int o = (((z >> P.shift) - H.bz) * 2 + ((y >> P.shift) - H.by)) * 2 + ((x >> P.shift) - H.bx);
+  const int f = (((z & m) == 0) * 2 + ((y & m) == 0)) * 2 + ((x & m) == 0);
+  return ((table >> (o * 8 + f)) & 1ull) != 0ull;
+}
+
 // computeDivergence (fluid-forces.wgsl:184-203) and the finest level's first Jacobi
 // iterate from zero (initializePressure, pressure.wgsl:485-505), fused: the iterate needs
 // only the cell's own right-hand side.
@@ -1131,10 +1161,12 @@ FP_DEV bool pressureUnknown(const SimParams& P, const Home& H, int x, int y, int
 template <bool ONE>
 FP_DEV void brick_divergence(const SimParams* __restrict__ Pp, uint32_t i, int pSel) {
   __shared__ int nslot[27];
+  __shared__ uint32_t unknownWords[2];
   const SimParams& P = *Pp;
   float* pOut = P.p0[pSel];
   if (!homeOk(P, P.active[i])) return;  // the bounds-checked build only
   Home H = enterBrick(P, P.active[i], nslot);
+  const uint64_t unknowns = unknownTable(P, H, unknownWords);
   size_t slot = (size_t)nslot[13];
   const size_t N = P.N;
   for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
@@ -1151,7 +1183,7 @@ FP_DEV void brick_divergence(const SimParams* __restrict__ Pp, uint32_t i, int p
     P.div[slot * N + c] = rhs;
     uint8_t t = P.topo[0][slot * N + c];
     float first = 0.f;
-    if (!(t & FP_STORED_SOLID) && pressureUnknown(P, H, x, y, z)) {
+    if (!(t & FP_STORED_SOLID) && unknownIn(unknowns, P, H, x, y, z)) {
       float diag = (float)((t >> 0) & 1) + (float)((t >> 1) & 1) + ((float)((t >> 2) & 1) + (float)((t >> 3) & 1)) +
                    ((float)((t >> 4) & 1) + (float)((t >> 5) & 1));
       first = mixf(0.f, (0.f - rhs) / fmaxf(diag, 1e-12f), 0.8f);
@@ -1174,10 +1206,12 @@ __global__ void __launch_bounds__(THREADS, 6) k_divergence(FpBatch bt, int pSel)
 template <bool ONE>
 FP_DEV void brick_project(const SimParams* __restrict__ Pp, uint32_t i, int pSel) {
   __shared__ int nslot[27];
+  __shared__ uint32_t unknownWords[2];
   const SimParams& P = *Pp;
   const float* p = P.p0[pSel];
   if (!homeOk(P, P.active[i])) return;  // the bounds-checked build only
   Home H = enterBrick(P, P.active[i], nslot);
+  const uint64_t unknowns = unknownTable(P, H, unknownWords);
   size_t slot = (size_t)nslot[13];
   const size_t N = P.N;
   for (int c = threadIdx.x; c < P.N; c += blockDim.x) {
@@ -1186,14 +1220,14 @@ FP_DEV void brick_project(const SimParams* __restrict__ Pp, uint32_t i, int pSel
     float res[3] = {0.f, 0.f, 0.f};
     if (!solidCell<ONE>(P, H, x, y, z)) {  // solidAt at the cell centre
       float cp = p[slot * N + c];
-      bool pu = pressureUnknown(P, H, x, y, z);
+      bool pu = unknownIn(unknowns, P, H, x, y, z);
       for (int a = 0; a < 3; a++) {
         int n[3] = {x, y, z};
         n[a] += 1;
         float v = P.velF[(slot * 3 + a) * N + c];
         if (solidCell<ONE>(P, H, n[0], n[1], n[2])) {
           res[a] = 0.f;
-        } else if (!pu && !pressureUnknown(P, H, n[0], n[1], n[2])) {
+        } else if (!pu && !unknownIn(unknowns, P, H, n[0], n[1], n[2])) {
           res[a] = 0.f;
         } else {
           float pn = cellAt(P, H, p, 1, 0, n[0], n[1], n[2]);
