@@ -300,6 +300,11 @@ class Stepper {
   int sms_ = 148;
   cudaStream_t stream_ = nullptr;
   cudaEvent_t readEvent_ = nullptr;
+  // A second stream the step forks work onto where nothing on the main stream depends on it yet:
+  // the multigrid topology (joined before the divergence) beside the transport kernels, the curl
+  // (joined before the forces) beside evolution. Not while profiling (phases stay serial).
+  cudaStream_t side_ = nullptr;
+  cudaEvent_t forkTopo_ = nullptr, joinTopo_ = nullptr, forkCurl_ = nullptr, joinCurl_ = nullptr;
   std::string error_;
   void* noise_ = nullptr;
 

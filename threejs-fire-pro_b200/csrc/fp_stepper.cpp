@@ -31,6 +31,9 @@ Stepper::~Stepper() {
   if (readH_) cudaFreeHost(readH_);
   if (noise_) cudaFree(noise_);
   if (readEvent_) cudaEventDestroy(readEvent_);
+  for (cudaEvent_t e : {forkTopo_, joinTopo_, forkCurl_, joinCurl_})
+    if (e) cudaEventDestroy(e);
+  if (side_) cudaStreamDestroy(side_);
   for (Phase& ph : phases_) {
     if (ph.a) cudaEventDestroy(ph.a);
     if (ph.b) cudaEventDestroy(ph.b);
@@ -50,6 +53,9 @@ int Stepper::initialize() {
   if ((rc = check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
   cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_);
   if ((rc = check(cudaEventCreateWithFlags(&readEvent_, cudaEventDisableTiming), "cudaEventCreate"))) return rc;
+  if ((rc = check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
+  for (cudaEvent_t* e : {&forkTopo_, &joinTopo_, &forkCurl_, &joinCurl_})
+    if ((rc = check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate"))) return rc;
   // The curl-noise table (CurlNoise.ts:5-51), once, shared by the simulations.
   if ((rc = check(cudaMalloc(&noise_, 64 * 64 * 64 * sizeof(float4)), "cudaMalloc"))) return rc;
   fp_launch_noise((float4*)noise_, stream_);
@@ -446,16 +452,34 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   launches += n;
   phaseEnd(PH_ALLOC, n);
   // Topology of the slots granted this step, or of everything after the geometry changed.
-  phaseBegin(PH_TOPO);
-  fp_launch_topology(bt, topoAll, sms_, stream_);
+  // Topology reads the allocation's tables and solids and writes only the multigrid's flags and
+  // masks, which nothing reads before the divergence: beside the transport kernels when not
+  // profiling.
+  const bool fork = !profiling_;
+  if (fork) {
+    cudaEventRecord(forkTopo_, stream_);
+    cudaStreamWaitEvent(side_, forkTopo_, 0);
+    fp_launch_topology(bt, topoAll, sms_, side_);
+    cudaEventRecord(joinTopo_, side_);
+  } else {
+    phaseBegin(PH_TOPO);
+    fp_launch_topology(bt, topoAll, sms_, stream_);
+    phaseEnd(PH_TOPO, topoAll ? 4 : 2);
+  }
   launches += topoAll ? 4 : 2;
-  phaseEnd(PH_TOPO, topoAll ? 4 : 2);
   phaseBegin(PH_PREDICT);
   fp_launch_predict(bt, B_, vd_, sms_, stream_);
   phaseEnd(PH_PREDICT, 1);
   phaseBegin(PH_CORRECT);
   fp_launch_correct(bt, B_, vd_, sms_, stream_);
   phaseEnd(PH_CORRECT, 1);
+  // The curl reads only the corrected velocity, and only the forces read it: beside evolution.
+  if (fork && curl) {
+    cudaEventRecord(forkCurl_, stream_);
+    cudaStreamWaitEvent(side_, forkCurl_, 0);
+    fp_launch_curl(bt, B_, vd_, sms_, side_);
+    cudaEventRecord(joinCurl_, side_);
+  }
   phaseBegin(PH_EVOLVE);
   fp_launch_evolve(bt, B_, vd_, sms_, stream_);
   // Coarse smoke evolves after the fine fields, whose source production it averages, and
@@ -476,10 +500,14 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
     cudaEventRecordWithFlags(readEvent_, stream_, cudaEventRecordExternal);
 
   if (curl) {
-    phaseBegin(PH_CURL);
-    fp_launch_curl(bt, B_, vd_, sms_, stream_);
+    if (fork) {
+      cudaStreamWaitEvent(stream_, joinCurl_, 0);
+    } else {
+      phaseBegin(PH_CURL);
+      fp_launch_curl(bt, B_, vd_, sms_, stream_);
+      phaseEnd(PH_CURL, 1);
+    }
     launches++;
-    phaseEnd(PH_CURL, 1);
   }
   phaseBegin(PH_FORCES);
   fp_launch_forces(bt, B_, vd_, sms_, stream_);
@@ -487,6 +515,7 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   phaseEnd(PH_FORCES, 1);
   // Cold start every step: the divergence writes the first iterate into p0[1].
   int cur[FP_MAX_LEVELS] = {0};
+  if (fork) cudaStreamWaitEvent(stream_, joinTopo_, 0);  // the first iterate reads the topology
   phaseBegin(PH_DIVERGENCE);
   fp_launch_divergence(bt, 1, vd_, sms_, stream_);
   launches++;
