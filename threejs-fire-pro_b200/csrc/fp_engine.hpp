@@ -304,7 +304,7 @@ class Stepper {
   // the multigrid topology (joined before the divergence) beside the transport kernels, the curl
   // (joined before the forces) beside evolution. Not while profiling (phases stay serial).
   cudaStream_t side_ = nullptr;
-  cudaEvent_t forkTopo_ = nullptr, joinTopo_ = nullptr, forkCurl_ = nullptr, joinCurl_ = nullptr;
+  cudaEvent_t forkTopo_ = nullptr, joinTopo_ = nullptr, forkCurl_ = nullptr, joinCurl_ = nullptr, joinSmoke_ = nullptr;
   std::string error_;
   void* noise_ = nullptr;
 

@@ -14,10 +14,12 @@ void fp_launch_readback(const FpBatch& bt, int sms, cudaStream_t st);
 void fp_launch_predict(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st);
 void fp_launch_correct(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st);
 void fp_launch_evolve(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st);
-// Coarse smoke (smoke_divisor > 1): advection with the donors' range, then evolution with
-// source production and content flags; simulations without coarse smoke skip both.
-// B field cells a brick side, vd the velocity divisor, sd the finest smoke divisor among them.
-void fp_launch_smoke(const FpBatch& bt, int B, int vd, int sd, int sms, cudaStream_t st);
+// Coarse smoke (smoke_divisor > 1): advection with the donors' range (it reads only the
+// start-of-step state), then evolution with source production and content flags (after the
+// fine fields' evolution); simulations without coarse smoke skip both. B field cells a brick
+// side, vd the velocity divisor, sd the finest smoke divisor among them.
+void fp_launch_smoke_advect(const FpBatch& bt, int B, int vd, int sd, int sms, cudaStream_t st);
+void fp_launch_smoke_evolve(const FpBatch& bt, int B, int vd, int sd, int sms, cudaStream_t st);
 void fp_launch_curl(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st);
 void fp_launch_forces(const FpBatch& bt, int B, int vd, int sms, cudaStream_t st);
 // Divergence with the finest level's first iterate into p0[pSel]; projection with p0[pSel].

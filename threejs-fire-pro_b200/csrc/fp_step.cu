@@ -1583,14 +1583,19 @@ static size_t stagedBytes(int channels) {
   const int S = 8 + 2 * HALO;
   return (size_t)channels * S * S * S * sizeof(float);
 }
-void fp_launch_smoke(const FpBatch& bt, int B, int vd, int sd, int sms, cudaStream_t st) {
-  if (B == CUBE * vd && B / sd >= CUBE) {  // the velocity lattice 8^3 a brick, the smoke grid 8^3 or finer
+// The velocity lattice 8^3 a brick and the smoke grid 8^3 or finer: the staged forms.
+static bool smokeStaged(int B, int vd, int sd) { return B == CUBE * vd && B / sd >= CUBE; }
+void fp_launch_smoke_advect(const FpBatch& bt, int B, int vd, int sd, int sms, cudaStream_t st) {
+  if (smokeStaged(B, vd, sd))
     k_smoke_advect<true><<<sms * 3, 256, stagedBytes(4), st>>>(bt);
-    k_smoke_evolve<true><<<sms * 3, 256, stagedBytes(4), st>>>(bt);
-  } else {
+  else
     k_smoke_advect<false><<<sms * 16, SMOKE_THREADS, 0, st>>>(bt);
+}
+void fp_launch_smoke_evolve(const FpBatch& bt, int B, int vd, int sd, int sms, cudaStream_t st) {
+  if (smokeStaged(B, vd, sd))
+    k_smoke_evolve<true><<<sms * 3, 256, stagedBytes(4), st>>>(bt);
+  else
     k_smoke_evolve<false><<<sms * 16, SMOKE_THREADS, 0, st>>>(bt);
-  }
 }
 
 

@@ -31,7 +31,7 @@ Stepper::~Stepper() {
   if (readH_) cudaFreeHost(readH_);
   if (noise_) cudaFree(noise_);
   if (readEvent_) cudaEventDestroy(readEvent_);
-  for (cudaEvent_t e : {forkTopo_, joinTopo_, forkCurl_, joinCurl_})
+  for (cudaEvent_t e : {forkTopo_, joinTopo_, forkCurl_, joinCurl_, joinSmoke_})
     if (e) cudaEventDestroy(e);
   if (side_) cudaStreamDestroy(side_);
   for (Phase& ph : phases_) {
@@ -54,7 +54,7 @@ int Stepper::initialize() {
   cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_);
   if ((rc = check(cudaEventCreateWithFlags(&readEvent_, cudaEventDisableTiming), "cudaEventCreate"))) return rc;
   if ((rc = check(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "cudaStreamCreate"))) return rc;
-  for (cudaEvent_t* e : {&forkTopo_, &joinTopo_, &forkCurl_, &joinCurl_})
+  for (cudaEvent_t* e : {&forkTopo_, &joinTopo_, &forkCurl_, &joinCurl_, &joinSmoke_})
     if ((rc = check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate"))) return rc;
   // The curl-noise table (CurlNoise.ts:5-51), once, shared by the simulations.
   if ((rc = check(cudaMalloc(&noise_, 64 * 64 * 64 * sizeof(float4)), "cudaMalloc"))) return rc;
@@ -461,6 +461,12 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
     cudaStreamWaitEvent(side_, forkTopo_, 0);
     fp_launch_topology(bt, topoAll, sms_, side_);
     cudaEventRecord(joinTopo_, side_);
+    // Coarse smoke's advection reads the start-of-step state only: beside the fine transport,
+    // joined before the coarse evolution.
+    if (anySmoke_) {
+      fp_launch_smoke_advect(bt, B_, vd_, smokeDiv_, sms_, side_);
+      cudaEventRecord(joinSmoke_, side_);
+    }
   } else {
     phaseBegin(PH_TOPO);
     fp_launch_topology(bt, topoAll, sms_, stream_);
@@ -484,7 +490,13 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   fp_launch_evolve(bt, B_, vd_, sms_, stream_);
   // Coarse smoke evolves after the fine fields, whose source production it averages, and
   // records content before the measurement.
-  if (anySmoke_) fp_launch_smoke(bt, B_, vd_, smokeDiv_, sms_, stream_);
+  if (anySmoke_) {
+    if (fork)
+      cudaStreamWaitEvent(stream_, joinSmoke_, 0);
+    else
+      fp_launch_smoke_advect(bt, B_, vd_, smokeDiv_, sms_, stream_);
+    fp_launch_smoke_evolve(bt, B_, vd_, smokeDiv_, sms_, stream_);
+  }
   phaseEnd(PH_EVOLVE, anySmoke_ ? 3 : 1);
   launches += anySmoke_ ? 5 : 3;
 
