@@ -324,8 +324,8 @@ class Stepper {
   double hostPrepareMs_ = 0, hostWaitMs_ = 0;
 
   // per-phase device timing (GpuProfiler.ts)
-  enum PhaseId { PH_ALLOC, PH_TOPO, PH_PREDICT, PH_CORRECT, PH_EVOLVE, PH_CURL, PH_FORCES, PH_DIVERGENCE,
-                 PH_MULTIGRID, PH_PROJECT, PH_COUNT };
+  enum PhaseId { PH_ALLOC, PH_TOPO, PH_PREDICT, PH_CORRECT, PH_EVOLVE, PH_SMOKE, PH_CURL, PH_FORCES, PH_DIVERGENCE,
+                 PH_MULTIGRID, PH_PROJECT, PH_COUNT };  // in the order the step runs them
   struct Phase {
     uint64_t launches = 0, stepLaunches = 0;
     double ms = 0, voxels = 0;

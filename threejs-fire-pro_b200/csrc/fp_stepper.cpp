@@ -332,8 +332,8 @@ int Stepper::setProfiling(bool on) {
 }
 
 int Stepper::readProfile(fp_phase* out, uint32_t* count) {
-  static const char* names[PH_COUNT] = {"allocation", "topology", "predict", "correct", "evolve", "curl",
-                                        "forces", "divergence", "multigrid", "project"};
+  static const char* names[PH_COUNT] = {"allocation", "topology", "predict", "correct", "evolve", "smoke",
+                                        "curl", "forces", "divergence", "multigrid", "project"};
   int rc = consume();
   if (rc) return rc;
   uint32_t cap = *count;
@@ -488,16 +488,18 @@ void Stepper::enqueue(bool solidsFresh, bool solidsAll, bool topoAll, bool curl,
   }
   phaseBegin(PH_EVOLVE);
   fp_launch_evolve(bt, B_, vd_, sms_, stream_);
+  phaseEnd(PH_EVOLVE, 1);
   // Coarse smoke evolves after the fine fields, whose source production it averages, and
   // records content before the measurement.
   if (anySmoke_) {
+    phaseBegin(PH_SMOKE);
     if (fork)
       cudaStreamWaitEvent(stream_, joinSmoke_, 0);
     else
       fp_launch_smoke_advect(bt, B_, vd_, smokeDiv_, sms_, stream_);
     fp_launch_smoke_evolve(bt, B_, vd_, smokeDiv_, sms_, stream_);
+    phaseEnd(PH_SMOKE, 2);
   }
-  phaseEnd(PH_EVOLVE, anySmoke_ ? 3 : 1);
   launches += anySmoke_ ? 5 : 3;
 
   // Measurement: counters and the tiles' content flags are final once evolution ran, so they
