@@ -20,16 +20,18 @@ namespace {
 
 constexpr int RTHREADS = 128;
 
-// A thread's current box (the pages its samples read) and its last brick lookup.
+// A thread's current box (the pages its samples read) and its last two brick lookups (samples
+// near a brick's face alternate between two bricks).
 struct SlotCache {
   int bx, by, bz, slot;
+  int bx2, by2, bz2, slot2;
   int lo[3], hi[3];  // the current box in bricks, inclusive
 };
 FP_DEV SlotCache noBox() {
   SlotCache c;
-  c.bx = 1 << 30;
-  c.by = c.bz = 0;
-  c.slot = -1;
+  c.bx = c.bx2 = 1 << 30;
+  c.by = c.bz = c.by2 = c.bz2 = 0;
+  c.slot = c.slot2 = -1;
   for (int a = 0; a < 3; a++) {
     c.lo[a] = 0;
     c.hi[a] = -1;
@@ -42,7 +44,7 @@ FP_DEV void useBox(const FpRender& R, SlotCache& c, int k) {
     c.lo[a] = R.boxes[6 * k + a];
     c.hi[a] = R.boxes[6 * k + 3 + a];
   }
-  c.bx = 1 << 30;
+  c.bx = c.bx2 = 1 << 30;
 }
 FP_DEV bool inBox(const SlotCache& c, int bx, int by, int bz) {
   return bx >= c.lo[0] && bx <= c.hi[0] && by >= c.lo[1] && by <= c.hi[1] && bz >= c.lo[2] && bz <= c.hi[2];
@@ -50,6 +52,11 @@ FP_DEV bool inBox(const SlotCache& c, int bx, int by, int bz) {
 // fireProPage: the slot of world brick b inside the current box, or -1.
 FP_DEV int slotAt(const SimParams& P, const FpRender& R, SlotCache& c, int bx, int by, int bz) {
   if (bx == c.bx && by == c.by && bz == c.bz) return c.slot;
+  if (bx == c.bx2 && by == c.by2 && bz == c.bz2) return c.slot2;
+  c.bx2 = c.bx;
+  c.by2 = c.by;
+  c.bz2 = c.bz;
+  c.slot2 = c.slot;
   int s = -1;
   if (inBox(c, bx, by, bz)) {
     int t = hashFind(P, bx >> 2, by >> 2, bz >> 2);
@@ -349,6 +356,78 @@ FP_DEV float4 incidentLight(const SimParams& P, const FpRender& R, SlotCache& c,
   return make_float4(glow.x, glow.y, glow.z, expf(-depth));
 }
 
+// incidentLight with a whole warp, every lane passing the same position (and its own copy of
+// the same cursor): the lanes take the shadow samples (32 at a time) and the six glow
+// directions, and every lane then adds their terms in the order of the serial loops, with the
+// serial early stop of the shadow sum, so all lanes return the serial result's value.
+FP_DEV float4 incidentLightWarp(const SimParams& P, const FpRender& R, SlotCache& c, float px, float py, float pz) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  float4 local = sampleWorld(P, R, c, px, py, pz);
+  if (local.x + glowOf(local.z) < 1e-5f) return make_float4(0.f, 0.f, 0.f, 1.f);
+  float ln = sqrtf(R.light[0] * R.light[0] + R.light[1] * R.light[1] + R.light[2] * R.light[2]);
+  float sx = R.light[0] / ln, sy = R.light[1] / ln, sz = R.light[2] / ln;
+  int count = R.shadowSamples;
+  float ds = exitDistance(P, c, px, py, pz, sx, sy, sz) / (float)count;
+  float depth = 0.f;
+  if (R.light[3] > 0.f) {
+    bool stop = false;
+    for (int base = 0; base < count && !stop; base += 32) {
+      const int i = base + lane;
+      float v = 0.f;
+      if (i < count) {
+        float t = ((float)i + .5f) * ds;
+        float4 f = sampleWorld(P, R, c, px + sx * t, py + sy * t, pz + sz * t);
+        v = (fmaxf(0.f, f.x) * R.optical[2] + glowOf(f.z) * R.flameOpacity) * ds;
+      }
+      const int n = min(32, count - base);
+      for (int j = 0; j < n; j++) {
+        const float vj = __shfl_sync(full, v, j);
+        if (!stop) {
+          depth += vj;
+          stop = depth > 9.f;
+        }
+      }
+    }
+  }
+  float3 glow = make_float3(0.f, 0.f, 0.f);
+  if (R.optical[1] > 0.f && local.x > 1e-5f) {
+    const float dirs[6][3] = {{.36f, .48f, -.8f}, {-.36f, -.48f, .8f}, {-.8f, .6f, 0.f},
+                              {.8f, -.6f, 0.f},   {.48f, .64f, .6f},   {-.48f, -.64f, -.6f}};
+    float ex[6], ey[6], ez[6], ew[6];  // lane d < 6: direction d's six steps
+#pragma unroll
+    for (int k = 0; k < 6; k++) ex[k] = ey[k] = ez[k] = ew[k] = 0.f;
+    if (lane < 6) {
+      float t = 0.f, interval = .075f, transmission = 1.f;
+#pragma unroll
+      for (int k = 0; k < 6; k++) {
+        float q = t + interval * .5f;
+        float4 f = sampleWorld(P, R, c, px + dirs[lane][0] * q, py + dirs[lane][1] * q, pz + dirs[lane][2] * q);
+        float ext = extinctionOf(R, f);
+        float att = expf(-ext * interval);
+        float3 e = emissionOf(R, f);
+        ew[k] = transmission * integratedTransmission(ext, interval, att) / 6.f;
+        ex[k] = e.x;
+        ey[k] = e.y;
+        ez[k] = e.z;
+        transmission *= att;
+        t += interval;
+        interval *= 1.65f;
+      }
+    }
+    for (int d = 0; d < 6; d++) {
+#pragma unroll
+      for (int k = 0; k < 6; k++) {
+        const float w = __shfl_sync(full, ew[k], d);
+        glow.x += __shfl_sync(full, ex[k], d) * w;
+        glow.y += __shfl_sync(full, ey[k], d) * w;
+        glow.z += __shfl_sync(full, ez[k], d) * w;
+      }
+    }
+  }
+  return make_float4(glow.x, glow.y, glow.z, expf(-depth));
+}
+
 // The brick of computing brick `i` inside a box, that box made the current one, with its
 // slot; false when no box holds it.
 FP_DEV bool boxBrick(const SimParams& P, const FpRender& R, SlotCache& c, uint32_t i, int& bx, int& by, int& bz,
@@ -468,16 +547,18 @@ __global__ void __launch_bounds__(RTHREADS) k_render_light(const SimParams* __re
       }
       __syncthreads();
     }
-    // The brick's texels of the lighting lattice.
-    for (int k = threadIdx.x; k < L3; k += blockDim.x) {
+    // The brick's texels of the lighting lattice, a warp a texel.
+    for (int k = threadIdx.x >> 5; k < L3; k += blockDim.x >> 5) {
       int lx = k % L, ly = (k / L) % L, lz = k / (L * L);
-      float4 light = incidentLight(P, R, c, ((float)(bx * L + lx) + .5f) * texel, ((float)(by * L + ly) + .5f) * texel,
-                                   ((float)(bz * L + lz) + .5f) * texel);
-      size_t o = (size_t)slot * 4 * L3 + k;
-      R.lighting[o] = light.x;
-      R.lighting[o + L3] = light.y;
-      R.lighting[o + 2 * L3] = light.z;
-      R.lighting[o + 3 * L3] = light.w;
+      float4 light = incidentLightWarp(P, R, c, ((float)(bx * L + lx) + .5f) * texel,
+                                       ((float)(by * L + ly) + .5f) * texel, ((float)(bz * L + lz) + .5f) * texel);
+      if ((threadIdx.x & 31) == 0) {
+        size_t o = (size_t)slot * 4 * L3 + k;
+        R.lighting[o] = light.x;
+        R.lighting[o + L3] = light.y;
+        R.lighting[o + 2 * L3] = light.z;
+        R.lighting[o + 3 * L3] = light.w;
+      }
     }
   }
 }
