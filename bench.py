@@ -703,6 +703,31 @@ def serving_forms(local: int, wall: float = 20.0) -> dict:
     return out
 
 
+FORM_ORDER = ("precision", "batched", "served_64", "stress", "default_grid", "serving")
+
+
+def run_forms(args) -> dict:
+    """Every form in a process of its own (`--form NAME`), so that no form runs in the state an
+    earlier one left (a served form measured after the batched one in the same process saw its
+    p99 latency triple). The precision form runs first: its V-cycle calibration of the accurate
+    solve is handed to the forms that use that solve."""
+    out = {}
+    for name in FORM_ORDER:
+        cmd = [sys.executable, str(ROOT / "bench.py"), "--form", name, "--steps", str(args.steps),
+               "--accurate-vcycles", str(ACCURATE["vcycles"])]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+        if r.returncode != 0 or not lines:
+            out[name] = {"error": (r.stderr or r.stdout)[-2000:]}
+            continue
+        d = json.loads(lines[-1])
+        d.pop("form", None)
+        out[name] = d
+        if name == "precision":
+            ACCURATE["vcycles"] = int(d["solver"]["vcycles"])
+    return out
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -827,12 +852,7 @@ def run_ours(args, rank, world, local):
         "clocks": clock,
     }
     if world == 1 and not args.no_forms:
-        line["forms"] = {"batched": batched_form(local, steps=max(10, min(args.steps, 60))),
-                         "served_64": served_form(local),
-                         "precision": precision_form(local),
-                         "stress": stress_form(local),
-                         "default_grid": default_grid_form(local),
-                         "serving": serving_forms(local)}
+        line["forms"] = run_forms(args)
     if world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         untimed = GROW_STEPS + args.warmup
@@ -856,10 +876,14 @@ def main():
     ap.add_argument("--form", default=None, choices=["batched", "served_64", "precision", "stress", "default_grid",
                                                        "serving", "profile_small"],
                     help="run one of the forms alone on GPU 0 and print its JSON")
+    ap.add_argument("--accurate-vcycles", type=int, default=None,
+                    help="the accurate solve's V-cycles a step (the precision form calibrates them)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.accurate_vcycles:
+        ACCURATE["vcycles"] = args.accurate_vcycles
     if args.form:
-        forms = {"batched": lambda: batched_form(0), "served_64": lambda: served_form(0),
+        forms = {"batched": lambda: batched_form(0, steps=max(10, min(args.steps, 60))), "served_64": lambda: served_form(0),
                  "precision": lambda: precision_form(0), "stress": lambda: stress_form(0),
                  "default_grid": lambda: default_grid_form(0), "serving": lambda: serving_forms(0),
                  "profile_small": lambda: profile_small_form(0)}
