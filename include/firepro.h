@@ -213,7 +213,7 @@ typedef struct fp_solver_stats {
  * brick entry or a neighbour record, a tile from the directory or its hash, a brick id from a
  * work list) against the table's size before using it. A bad index is counted, the first is
  * kept, and its access is skipped (it reads as "no slot"): no kernel traps or faults. No
- * reference counterpart (SURVEY's debug aid: WebGPU validation of the reference's bindings). */
+ * reference counterpart (the reference relies on WebGPU's validation of its bindings). */
 typedef struct fp_bounds {
   int32_t checked; /* 1: this library checks (the debug build); 0: the release build, nothing below */
   uint32_t count;  /* bad indices seen since the simulation was created or reset */

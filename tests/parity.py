@@ -12,7 +12,7 @@ import numpy as np
 from firepro import abi
 from oracle.fp_oracle import OracleSim
 
-# north_star tolerance: relative L2 <= 1e-3 against the FP64 oracle per field per step.
+# The parity tolerance: relative L2 <= 1e-3 against the FP64 oracle per field per step.
 REL_L2_TOL = 1e-3
 
 CHECK_FIELDS = {
