@@ -709,10 +709,10 @@ FORM_ORDER = ("served_64", "precision", "batched", "stress", "default_grid", "se
 def run_forms(args) -> dict:
     """Every form in a process of its own (`--form NAME`), so that no form runs in the state an
     earlier one left. The 64-session served form runs first: it keeps the GPU near saturation
-    (one launch after another at a 60 Hz request clock), so a few per cent of throughput lost to
-    the heat a long batched form leaves decides whether its queue drains (p99 11 ms measured
-    first, 30-70 ms right after the batched form). The precision form's V-cycle calibration of
-    the accurate solve is handed to the forms that use that solve."""
+    (one launch after another at a 60 Hz request clock), so a few per cent of throughput lost
+    after a long batched form (plausibly to the heat it leaves) decides whether its queue drains
+    (p99 11 ms measured first, 30-70 ms right after the batched form). The precision form's
+    V-cycle calibration of the accurate solve is handed to the forms that use that solve."""
     out = {}
     for name in FORM_ORDER:
         cmd = [sys.executable, str(ROOT / "bench.py"), "--form", name, "--steps", str(args.steps),
