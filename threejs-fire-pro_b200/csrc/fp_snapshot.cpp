@@ -311,6 +311,22 @@ int Engine::restore(const uint8_t* data, size_t bytes) {
                         sizes[46 + 4 * l] >= cells * coarseBytes();
     }
     if (!sane) return fail(FP_EINVAL, "the snapshot's tables do not match its sizes");
+    // The buffer selectors index the pools (a step only swaps two: permutations), and the live
+    // tiles are tile slots in ascending order, each at its own position in the slot ->
+    // position table (both lists are built together).
+    auto permutation = [](const int* v, int n) {
+      unsigned seen = 0;
+      for (int k = 0; k < n; k++) {
+        if (v[k] < 0 || v[k] >= n || ((seen >> v[k]) & 1u)) return false;
+        seen |= 1u << v[k];
+      }
+      return true;
+    };
+    bool consistent = permutation(velIdx, 4) && permutation(fldIdx, 3) && permutation(smokeIdx, 3);
+    for (size_t j = 0; consistent && j < liveTiles.size(); j++)
+      consistent = liveTiles[j] >= 0 && (size_t)liveTiles[j] < tileIndex.size() && tileIndex[liveTiles[j]] == (int)j &&
+                   (j == 0 || liveTiles[j] > liveTiles[j - 1]);
+    if (!consistent) return fail(FP_EINVAL, "the snapshot's buffer selectors or live tiles are inconsistent");
   }
 #define FP_LOAD(b)                                                                                      \
   {                                                                                                     \
