@@ -137,6 +137,26 @@ def test_empty_scene_holds_nothing(oracle_lib):
     assert o.info(8) == 0, "no tile without a source or content"
 
 
+@pytest.mark.parametrize("slots", [100, 150])
+def test_pool_exhaustion_conserves_demand(oracle_lib, slots):
+    # The plume's starting block wants 216 bricks; a budget of fewer slots grants every slot,
+    # counts the rest as failures and flags the pool as limited (poolLimited), step after step.
+    sc = scenes.SinglePlume()
+    o = _sim(sc, budget=slots * 512)
+    for s in range(3):
+        o.step(sc.frame(s).frame)
+        assert o.slots == slots and o.info(5) == slots, "every slot granted"
+        assert o.active_bricks == slots
+        assert o.info(5) + o.info(7) == 216, "granted + failed = wanted"
+        assert o.info(6) == 1
+    free = o.table(abi.FP_TABLE_FREE)
+    assert free[0] == 0 and free[1] == 216 - slots, "an empty free stack and the failure count"
+    active = o.table(abi.FP_TABLE_ACTIVE)
+    pages = o.table(abi.FP_TABLE_PAGES).view(np.int32)
+    ids = active[1:1 + int(active[0])]
+    assert np.array_equal(np.sort(pages[ids]), np.arange(slots)), "each slot held by one computing brick"
+
+
 def test_deterministic(oracle_lib):
     sc = scenes.SinglePlume()
     a, b = _sim(sc), _sim(sc)
