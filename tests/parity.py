@@ -166,3 +166,38 @@ def lockstep(scene, steps: int, gpu_factory, cutoff=0.05, budget=8e6, ground=Tru
     gpu.dispose()
     orc.close()
     return reports
+
+
+def brick_slots(sim) -> dict:
+    """World brick coordinates -> slot of every brick with one."""
+    entries = sim.table(abi.FP_TABLE_ENTRIES).view(np.int32)
+    tiles = sim.table(abi.FP_TABLE_TILES).view(np.int32).reshape(-1, 4)
+    ids = np.nonzero(entries >= 0)[0]
+    t, l = tiles[ids >> 6], ids & 63
+    coords = np.stack([t[:, 0] * 4 + (l & 3), t[:, 1] * 4 + ((l >> 2) & 3), t[:, 2] * 4 + (l >> 4)], 1)
+    return {tuple(int(v) for v in c): int(entries[i] & 0xFFFFFF) for i, c in zip(ids, coords)}
+
+
+def shift_frame(fd, dx: float, dz: float, cells: int):
+    """The frame's scene moved by (dx, 0, dz) metres (`cells` field cells for mesh-mask
+    colliders), with turbulence off: its noise is sampled at world positions."""
+    f = fd.frame
+    for k in range(f.force_count):
+        if f.forces[k].type == 1:
+            f.forces[k].strength = 0.0
+        f.forces[k].center[0] += dx
+        f.forces[k].center[2] += dz
+    for rows, n in ((f.sources, f.source_count), (f.force_targets, f.force_target_count)):
+        for k in range(n):
+            rows[k].position[0] += dx
+            rows[k].position[2] += dz
+    for k in range(f.collider_count):
+        c = f.colliders[k]
+        if c.shape == abi.FP_SHAPE_MESH:
+            c.lo[0] += cells
+            c.lo[2] += cells
+        else:
+            c.position[0] += dx
+            c.position[2] += dz
+    return fd
+

@@ -8,6 +8,7 @@ import pytest
 
 from firepro import abi, scenes
 from oracle.fp_oracle import OracleSim
+import parity
 
 BUDGET = 2 ** 19
 
@@ -321,40 +322,6 @@ def test_mesh_splat_single_sample():
         assert r.motion[1] == pytest.approx(60.0 * cover, rel=1e-6) and r.motion[3] == pytest.approx(60.0 * cover, rel=1e-6)
 
 
-def _brick_slots(o) -> dict:
-    """World brick coordinates -> slot of every brick with one."""
-    entries = o.table(abi.FP_TABLE_ENTRIES).view(np.int32)
-    tiles = o.table(abi.FP_TABLE_TILES).view(np.int32).reshape(-1, 4)
-    ids = np.nonzero(entries >= 0)[0]
-    t, l = tiles[ids >> 6], ids & 63
-    coords = np.stack([t[:, 0] * 4 + (l & 3), t[:, 1] * 4 + ((l >> 2) & 3), t[:, 2] * 4 + (l >> 4)], 1)
-    return {tuple(int(v) for v in c): int(entries[i] & 0xFFFFFF) for i, c in zip(ids, coords)}
-
-
-def _shift_frame(fd, dx: float, dz: float, cells: int):
-    """The force scene moved by (dx, 0, dz) metres (`cells` cells for the mesh mask), its
-    turbulence (noise at world positions) off."""
-    f = fd.frame
-    for k in range(f.force_count):
-        if f.forces[k].type == 1:
-            f.forces[k].strength = 0.0
-        f.forces[k].center[0] += dx
-        f.forces[k].center[2] += dz
-    for rows, n in ((f.sources, f.source_count), (f.force_targets, f.force_target_count)):
-        for k in range(n):
-            rows[k].position[0] += dx
-            rows[k].position[2] += dz
-    for k in range(f.collider_count):
-        c = f.colliders[k]
-        if c.shape == abi.FP_SHAPE_MESH:
-            c.lo[0] += cells
-            c.lo[2] += cells
-        else:
-            c.position[0] += dx
-            c.position[2] += dz
-    return fd
-
-
 def test_translation_by_a_tile_is_invariant(oracle_lib):
     # The force scene (colliders of every kind, wind, vortex, targeted radial force, a burst,
     # an emitter that stops) spans negative and positive brick coordinates; moved by one tile
@@ -367,9 +334,9 @@ def test_translation_by_a_tile_is_invariant(oracle_lib):
     a, b = _sim(sc, real=0, budget=budget), _sim(sc, real=0, budget=budget)
     metres, cells = 4 * sc.brick_size * sc.voxel_size, 4 * sc.brick_size
     for s in range(24):
-        a.step(_shift_frame(sc.frame(s), 0.0, 0.0, 0).frame)
-        b.step(_shift_frame(sc.frame(s), metres, metres, cells).frame)
-        sa, sb = _brick_slots(a), _brick_slots(b)
+        a.step(parity.shift_frame(sc.frame(s), 0.0, 0.0, 0).frame)
+        b.step(parity.shift_frame(sc.frame(s), metres, metres, cells).frame)
+        sa, sb = parity.brick_slots(a), parity.brick_slots(b)
         assert {(x + 4, y, z + 4): v for (x, y, z), v in sa.items()} == sb, f"step {s}: bricks and slots"
         keys = sorted(sa)
         for fid in (abi.FP_FIELD_VELOCITY, abi.FP_FIELD_SCALARS, abi.FP_FIELD_EXPANSION, abi.FP_FIELD_PRESSURE,
